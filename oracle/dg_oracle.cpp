@@ -1,0 +1,1182 @@
+// CPU oracle (test infrastructure): restatement of PHiLiP's explicit strong-form
+// DG/FR residual. Each function cites the reference file:line it follows.
+#include "dg_oracle.hpp"
+
+#include <algorithm>
+#include <cassert>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <stdexcept>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace oracle {
+
+static const double BIG_NUMBER = 1e100;   // physics.h:270
+static const double PI = 3.14159265358979323846;
+
+// ---------------------------------------------------------------------------------
+// 1-D quadrature and Lagrange bases (stand-ins for deal.II QGauss / QGaussLobatto /
+// FE_DGQ / FE_DGQArbitraryNodes, which the reference builds in dg_base.cpp:131-261).
+// ---------------------------------------------------------------------------------
+static void legendre(int n, double x, double& p, double& dp) {
+    // P_n(x) and P_n'(x) on [-1,1] by the three-term recurrence.
+    double p0 = 1.0, p1 = x;
+    if (n == 0) { p = 1.0; dp = 0.0; return; }
+    for (int k = 2; k <= n; ++k) {
+        double pk = ((2.0 * k - 1.0) * x * p1 - (k - 1.0) * p0) / k;
+        p0 = p1; p1 = pk;
+    }
+    p = p1;
+    dp = (std::fabs(x) < 1.0) ? n * (x * p1 - p0) / (x * x - 1.0) : 0.5 * n * (n + 1) * std::pow(x, n + 1);
+}
+
+void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
+    x.assign(n, 0.0); w.assign(n, 0.0);
+    for (int i = 0; i < n; ++i) {
+        double z = std::cos(PI * (i + 0.75) / (n + 0.5));
+        for (int it = 0; it < 100; ++it) {
+            double p, dp; legendre(n, z, p, dp);
+            double dz = p / dp; z -= dz;
+            if (std::fabs(dz) < 1e-16) break;
+        }
+        double p, dp; legendre(n, z, p, dp);
+        // ascending order on [0,1]
+        x[n - 1 - i] = 0.5 * (z + 1.0);
+        w[n - 1 - i] = 1.0 / ((1.0 - z * z) * dp * dp);   // (2/((1-z^2)P'^2)) / 2
+    }
+}
+
+void gauss_lobatto(int n, std::vector<double>& x, std::vector<double>& w) {
+    x.assign(n, 0.0); w.assign(n, 0.0);
+    if (n < 2) throw std::runtime_error("Gauss-Lobatto needs n >= 2");
+    const int m = n - 1;  // interior nodes are roots of P_m'
+    x[0] = 0.0; x[n - 1] = 1.0;
+    for (int i = 1; i < n - 1; ++i) {
+        double z = -std::cos(PI * i / m);   // Chebyshev-Gauss-Lobatto guess (ascending)
+        for (int it = 0; it < 100; ++it) {
+            // Newton on q(z) = P_m'(z); q' = (2 z P_m' - m(m+1) P_m)/(1-z^2)
+            double p, dp; legendre(m, z, p, dp);
+            double d2p = (2.0 * z * dp - m * (m + 1.0) * p) / (1.0 - z * z);
+            double dz = dp / d2p; z -= dz;
+            if (std::fabs(dz) < 1e-16) break;
+        }
+        x[i] = 0.5 * (z + 1.0);
+    }
+    for (int i = 0; i < n; ++i) {
+        double z = 2.0 * x[i] - 1.0, p, dp; legendre(m, z, p, dp);
+        w[i] = 1.0 / (m * (m + 1.0) * p * p);    // (2/(m(m+1)P_m^2)) / 2
+    }
+}
+
+void lagrange_eval(const std::vector<double>& nodes, double x, double* val, double* der) {
+    const int n = (int)nodes.size();
+    for (int j = 0; j < n; ++j) {
+        double v = 1.0, d = 0.0;
+        for (int m = 0; m < n; ++m) {
+            if (m == j) continue;
+            const double inv = 1.0 / (nodes[j] - nodes[m]);
+            d = d * (x - nodes[m]) * inv + v * inv;
+            v *= (x - nodes[m]) * inv;
+        }
+        if (val) val[j] = v;
+        if (der) der[j] = d;
+    }
+}
+
+static std::vector<double> matmul(const std::vector<double>& A, const std::vector<double>& B, int n, int k, int m) {
+    std::vector<double> C((size_t)n * m, 0.0);
+    for (int i = 0; i < n; ++i)
+        for (int l = 0; l < k; ++l)
+            for (int j = 0; j < m; ++j) C[i * m + j] += A[i * k + l] * B[l * m + j];
+    return C;
+}
+
+static std::vector<double> invert(std::vector<double> A, int n) {
+    // Gauss-Jordan with partial pivoting (deal.II FullMatrix::invert equivalent).
+    std::vector<double> I((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i) I[i * n + i] = 1.0;
+    for (int c = 0; c < n; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < n; ++r) if (std::fabs(A[r * n + c]) > std::fabs(A[piv * n + c])) piv = r;
+        if (piv != c) for (int j = 0; j < n; ++j) { std::swap(A[c * n + j], A[piv * n + j]); std::swap(I[c * n + j], I[piv * n + j]); }
+        const double d = 1.0 / A[c * n + c];
+        for (int j = 0; j < n; ++j) { A[c * n + j] *= d; I[c * n + j] *= d; }
+        for (int r = 0; r < n; ++r) {
+            if (r == c) continue;
+            const double f = A[r * n + c];
+            if (f == 0.0) continue;
+            for (int j = 0; j < n; ++j) { A[r * n + j] -= f * A[c * n + j]; I[r * n + j] -= f * I[c * n + j]; }
+        }
+    }
+    return I;
+}
+
+static double factorial(int k) { double f = 1.0; for (int i = 2; i <= k; ++i) f *= i; return f; }
+
+// FR correction parameter c (operators.cpp:1559-1661); reference element [0,1].
+double fr_correction_parameter(int fr_type, int p, double user_value) {
+    const double pf = factorial(p), pf2 = factorial(2 * p);
+    const double cp = pf2 / (pf * pf);
+    double c = 0.0;
+    switch (fr_type) {
+    case C_HU: case C_HU_LUMPED:
+        c = 2.0 * (p + 1) / (p * ((2.0 * p + 1.0) * std::pow(pf * cp, 2))); c /= 2.0; break;
+    case C_SD:
+        c = 2.0 * p / ((p + 1.0) * ((2.0 * p + 1.0) * std::pow(pf * cp, 2))); c /= 2.0; break;
+    case C_NEGATIVE:
+        c = -2.0 / std::pow((2.0 * p + 1.0) * std::pow(pf * cp, 2), 1.0); c /= 2.0; break;
+    case C_NEGATIVE2:
+        c = -2.0 / std::pow((2.0 * p + 1.0) * std::pow(pf * cp, 2), 1.0); c /= 2.0; c /= 2.0; break;
+    case C_DG: c = 0.0; break;
+    case C_10THOUSAND: c = 10000.0; break;
+    case C_PLUS:
+        if (p == 2) c = 0.186; else if (p == 3) c = 3.67e-3; else if (p == 4) c = 4.79e-5; else if (p == 5) c = 4.24e-7;
+        else throw std::runtime_error("cPlus defined for p=2..5 only");
+        c /= 2.0; c /= std::pow(std::pow(2.0, p), 2); break;
+    case C_USER:
+        c = user_value; c /= 2.0; c /= std::pow(std::pow(2.0, p), 2); break;
+    default: throw std::runtime_error("unknown FR type");
+    }
+    return c;
+}
+
+static double fr_aux_parameter(int k_type, int p) {
+    switch (k_type) {
+    case K_DG: return 0.0;
+    case K_SD: return fr_correction_parameter(C_SD, p, 0.0);
+    case K_HU: return fr_correction_parameter(C_HU, p, 0.0);
+    case K_NEGATIVE: return fr_correction_parameter(C_NEGATIVE, p, 0.0);
+    case K_NEGATIVE2: return fr_correction_parameter(C_NEGATIVE2, p, 0.0);
+    case K_PLUS: return fr_correction_parameter(C_PLUS, p, 0.0);
+    case K_10THOUSAND: return 10000.0;
+    }
+    throw std::runtime_error("unknown FR aux type");
+}
+
+Ops1D build_ops(const Params& prm) {
+    Ops1D o;
+    const int p = prm.poly_degree;
+    o.nd = p + 1;
+    o.nq = p + 1 + prm.overintegration;
+    if (prm.flux_nodes == GLL) gauss_lobatto(o.nq, o.xq, o.wq); else gauss_legendre(o.nq, o.xq, o.wq);
+    // FE_DGQ(p) support points: Gauss-Lobatto points of p+1 (0.5 for p=0).
+    if (p == 0) o.xs = {0.5};
+    else { std::vector<double> dummy; gauss_lobatto(o.nd, o.xs, dummy); }
+    const int nd = o.nd, nq = o.nq;
+    o.chi.assign((size_t)nq * nd, 0.0); o.dchi.assign((size_t)nq * nd, 0.0);
+    for (int q = 0; q < nq; ++q) lagrange_eval(o.xs, o.xq[q], &o.chi[q * nd], &o.dchi[q * nd]);
+    for (int s = 0; s < 2; ++s) { o.chi_s[s].assign(nd, 0.0); lagrange_eval(o.xs, (double)s, o.chi_s[s].data(), nullptr); }
+    o.phi.assign((size_t)nq * nq, 0.0); o.dphi.assign((size_t)nq * nq, 0.0);
+    for (int q = 0; q < nq; ++q) lagrange_eval(o.xq, o.xq[q], &o.phi[q * nq], &o.dphi[q * nq]);
+    for (int s = 0; s < 2; ++s) { o.phi_s[s].assign(nq, 0.0); lagrange_eval(o.xq, (double)s, o.phi_s[s].data(), nullptr); }
+    // stiffness S_ij = sum_q phi_i(x_q) phi_j'(x_q) w_q, skew = S - S^T (operators.cpp:1440-1477)
+    std::vector<double> S((size_t)nq * nq, 0.0);
+    for (int i = 0; i < nq; ++i)
+        for (int j = 0; j < nq; ++j) {
+            double v = 0.0;
+            for (int q = 0; q < nq; ++q) v += o.phi[q * nq + i] * o.dphi[q * nq + j] * o.wq[q];
+            S[i * nq + j] = v;
+        }
+    o.skew.assign((size_t)nq * nq, 0.0);
+    for (int i = 0; i < nq; ++i) for (int j = 0; j < nq; ++j) o.skew[i * nq + j] = S[i * nq + j] - S[j * nq + i];
+    // mass M_ij = sum_q chi_i chi_j w_q (operators.cpp:1354-1385)
+    std::vector<double> M((size_t)nd * nd, 0.0);
+    for (int i = 0; i < nd; ++i) for (int j = 0; j < nd; ++j) {
+        double v = 0.0;
+        for (int q = 0; q < nq; ++q) v += o.chi[q * nd + i] * o.chi[q * nd + j] * o.wq[q];
+        M[i * nd + j] = v;
+    }
+    // modal differential operator M^{-1} S_chi, p-th derivative (operators.cpp:1491-1540)
+    std::vector<double> Schi((size_t)nd * nd, 0.0);
+    for (int i = 0; i < nd; ++i) for (int j = 0; j < nd; ++j) {
+        double v = 0.0;
+        for (int q = 0; q < nq; ++q) v += o.chi[q * nd + i] * o.dchi[q * nd + j] * o.wq[q];
+        Schi[i * nd + j] = v;
+    }
+    std::vector<double> Minv = invert(M, nd);
+    std::vector<double> Dm = matmul(Minv, Schi, nd, nd, nd);
+    std::vector<double> Dp((size_t)nd * nd, 0.0);
+    for (int i = 0; i < nd; ++i) Dp[i * nd + i] = 1.0;
+    for (int k = 0; k < p; ++k) Dp = matmul(Dm, Dp, nd, nd, nd);
+    auto fr_oper = [&](double c) {   // K = c (D^p)^T M D^p  (operators.cpp:1663-1675)
+        std::vector<double> DpT((size_t)nd * nd);
+        for (int i = 0; i < nd; ++i) for (int j = 0; j < nd; ++j) DpT[i * nd + j] = c * Dp[j * nd + i];
+        return matmul(matmul(DpT, M, nd, nd, nd), Dp, nd, nd, nd);
+    };
+    const double c = fr_correction_parameter(prm.fr_type, p, prm.fr_user_value);
+    const double k = fr_aux_parameter(prm.fr_aux_type, p);
+    std::vector<double> K = fr_oper(c), Ka = fr_oper(k);
+    std::vector<double> MK(M), MKa(M);
+    for (size_t i = 0; i < M.size(); ++i) { MK[i] += K[i]; MKa[i] += Ka[i]; }
+    o.minv = invert(MK, nd);
+    o.minv_aux = invert(MKa, nd);
+    // projection Pi = M^{-1} chi^T W (operators.cpp:1864-1889), plain M (not FR)
+    o.proj.assign((size_t)nd * nq, 0.0);
+    for (int i = 0; i < nd; ++i) for (int q = 0; q < nq; ++q) {
+        double v = 0.0;
+        for (int j = 0; j < nd; ++j) v += Minv[i * nd + j] * o.chi[q * nd + j] * o.wq[q];
+        o.proj[i * nq + q] = v;
+    }
+    return o;
+}
+
+// ---------------------------------------------------------------------------------
+// Sum-factorised tensor-product application (operators.cpp:294-398, :575-636).
+// A_d is (r_d x c_d) row-major; input is c_z*c_y*c_x (x fastest), output r_z*r_y*r_x.
+// ---------------------------------------------------------------------------------
+static void apply3(const double* Ax, int rx, int cx, const double* Ay, int ry, int cy,
+                   const double* Az, int rz, int cz, const double* in, double* out,
+                   bool adding, double factor) {
+    std::vector<double> t1((size_t)rx * cy * cz), t2((size_t)rx * ry * cz);
+    for (int z = 0; z < cz; ++z) for (int y = 0; y < cy; ++y) for (int x = 0; x < rx; ++x) {
+        double v = 0.0;
+        for (int s = 0; s < cx; ++s) v += Ax[x * cx + s] * in[(z * cy + y) * cx + s];
+        t1[(z * cy + y) * rx + x] = v;
+    }
+    for (int z = 0; z < cz; ++z) for (int y = 0; y < ry; ++y) for (int x = 0; x < rx; ++x) {
+        double v = 0.0;
+        for (int s = 0; s < cy; ++s) v += Ay[y * cy + s] * t1[(z * cy + s) * rx + x];
+        t2[(z * ry + y) * rx + x] = v;
+    }
+    for (int z = 0; z < rz; ++z) for (int y = 0; y < ry; ++y) for (int x = 0; x < rx; ++x) {
+        double v = adding ? out[(z * ry + y) * rx + x] : 0.0;
+        for (int s = 0; s < cz; ++s) v += factor * Az[z * cz + s] * t2[(s * ry + y) * rx + x];
+        out[(z * ry + y) * rx + x] = v;
+    }
+}
+
+static std::vector<double> transpose(const double* A, int r, int c) {
+    std::vector<double> T((size_t)r * c);
+    for (int i = 0; i < r; ++i) for (int j = 0; j < c; ++j) T[j * r + i] = A[i * c + j];
+    return T;
+}
+
+// inner product: out = (Ax^T (x) Ay^T (x) Az^T)(in .* w)
+static void inner3(const double* Ax, int rx, int cx, const double* Ay, int ry, int cy,
+                   const double* Az, int rz, int cz, const double* in, const double* w, double* out,
+                   bool adding, double factor) {
+    const int n = rx * ry * rz;
+    std::vector<double> wi(n);
+    for (int i = 0; i < n; ++i) wi[i] = in[i] * (w ? w[i] : 1.0);
+    std::vector<double> Tx = transpose(Ax, rx, cx), Ty = transpose(Ay, ry, cy), Tz = transpose(Az, rz, cz);
+    apply3(Tx.data(), cx, rx, Ty.data(), cy, ry, Tz.data(), cz, rz, wi.data(), out, adding, factor);
+}
+
+// ---------------------------------------------------------------------------------
+// Physics (euler.cpp, navier_stokes.cpp)
+// ---------------------------------------------------------------------------------
+struct Physics {
+    const Params* prm;
+    double gam, gm1, mach2, temp_ratio;
+    int* status;
+    explicit Physics(const Params* p, int* st) : prm(p), status(st) {
+        gam = p->gamma; gm1 = gam - 1.0; mach2 = p->mach_inf * p->mach_inf;
+        temp_ratio = 110.4 / p->temperature_inf;     // navier_stokes.cpp:50-52
+    }
+    double positive(double q) const {   // euler.cpp:155-172 + physics.cpp:298-317
+        if (q < 0.0) {
+            if (status) __atomic_fetch_or(status, 1, __ATOMIC_RELAXED);
+            if (prm->non_physical == ABORT_RUN) { std::fprintf(stderr, "oracle: non-physical state\n"); std::abort(); }
+            return BIG_NUMBER;
+        }
+        return q;
+    }
+    double pressure(const double* u) const {   // euler.cpp:486-500
+        const double rho = u[0];
+        double v2 = 0.0;
+        for (int d = 0; d < 3; ++d) { const double v = u[1 + d] / rho; v2 = v2 + v * v; }
+        return positive(gm1 * (u[4] - 0.5 * rho * v2));
+    }
+    void primitive(const double* u, double* w) const {   // euler.cpp:177-198
+        const double rho = u[0];
+        for (int d = 0; d < 3; ++d) w[1 + d] = u[1 + d] / rho;
+        const double p = pressure(u);
+        w[0] = positive(rho);
+        w[4] = positive(p);
+    }
+    void conservative_from_primitive(const double* w, double* u) const {  // euler.cpp:207-222
+        const double rho = w[0];
+        u[0] = rho;
+        double v2 = 0.0;
+        for (int d = 0; d < 3; ++d) { u[1 + d] = rho * w[1 + d]; v2 += w[1 + d] * w[1 + d]; }
+        u[4] = w[4] / gm1 + 0.5 * rho * v2;
+    }
+    double sound(double rho, double p) const { return std::sqrt(p * gam / rho); }
+    void convective_flux(const double* u, double F[5][3]) const {   // euler.cpp:915-938
+        const double rho = u[0];
+        const double p = pressure(u);
+        double v[3]; for (int d = 0; d < 3; ++d) v[d] = u[1 + d] / rho;
+        const double H = u[4] / u[0] + p / rho;
+        for (int fd = 0; fd < 3; ++fd) {
+            F[0][fd] = u[1 + fd];
+            for (int vd = 0; vd < 3; ++vd) F[1 + vd][fd] = rho * v[fd] * v[vd];
+            F[1 + fd][fd] += p;
+            F[4][fd] = rho * v[fd] * H;
+        }
+    }
+    static double log_mean(double a, double b) {   // euler.cpp:628-646
+        const double zeta = a / b;
+        const double f = (zeta - 1.0) / (zeta + 1.0);
+        const double u = f * f;
+        double F;
+        if (u < 1.0e-2) F = 1.0 + u / 3.0 + u * u / 5.0 + u * u * u / 7.0;
+        else F = std::log(zeta) / 2.0 / f;
+        return (a + b) / (2.0 * F);
+    }
+    void two_point(const double* u1, const double* u2, double F[5][3]) const {   // euler.cpp:563-809
+        const int type = prm->two_point;
+        if (type == KG) {
+            const double rho = (u1[0] + u2[0]) / 2.;
+            const double p = (pressure(u1) + pressure(u2)) / 2.;
+            double v[3]; for (int d = 0; d < 3; ++d) v[d] = 0.5 * (u1[1 + d] / u1[0] + u2[1 + d] / u2[0]);
+            const double e = ((u1[4] / u1[0]) + (u2[4] / u2[0])) / 2.;
+            for (int fd = 0; fd < 3; ++fd) {
+                F[0][fd] = rho * v[fd];
+                for (int vd = 0; vd < 3; ++vd) F[1 + vd][fd] = rho * v[fd] * v[vd];
+                F[1 + fd][fd] += p;
+                F[4][fd] = rho * v[fd] * e + p * v[fd];
+            }
+        } else if (type == IR) {
+            double w1[5], w2[5], z1[5], z2[5];
+            primitive(u1, w1); primitive(u2, w2);
+            auto param = [](const double* w, double* z) {
+                z[0] = std::sqrt(w[0] / w[4]);
+                for (int d = 0; d < 3; ++d) z[1 + d] = z[0] * w[1 + d];
+                z[4] = std::sqrt(w[0] * w[4]);
+            };
+            param(w1, z1); param(w2, z2);
+            double avg[5], lm[5];
+            for (int s = 0; s < 5; ++s) avg[s] = 0.5 * (z1[s] + z2[s]);
+            for (int s = 0; s < 5; ++s) lm[s] = log_mean(z1[s], z2[s]);
+            double v[3];
+            const double rho = avg[0] * lm[4];
+            for (int d = 0; d < 3; ++d) v[d] = avg[1 + d] / avg[0];
+            const double p = avg[4] / avg[0];
+            double H = (gam + 1.0) * (lm[4] / lm[0]) + gm1 * p;
+            H /= 2.0 * gam;
+            H *= gam / (rho * gm1);
+            double vv = 0.0; for (int d = 0; d < 3; ++d) vv += v[d] * v[d];
+            H += 0.5 * vv;
+            for (int fd = 0; fd < 3; ++fd) {
+                F[0][fd] = rho * v[fd];
+                for (int vd = 0; vd < 3; ++vd) F[1 + vd][fd] = rho * v[fd] * v[vd];
+                F[1 + fd][fd] += p;
+                F[4][fd] = rho * v[fd] * H;
+            }
+        } else {   // CH or Ra
+            const bool ra = (type == RA);
+            const double rho_log = log_mean(u1[0], u2[0]);
+            const double p1 = pressure(u1), p2 = pressure(u2);
+            const double b1 = ra ? u1[0] / p1 : u1[0] / (2.0 * p1);
+            const double b2 = ra ? u2[0] / p2 : u2[0] / (2.0 * p2);
+            const double b_log = log_mean(b1, b2);
+            double v1[3], v2[3], va[3];
+            for (int d = 0; d < 3; ++d) { v1[d] = u1[1 + d] / u1[0]; v2[d] = u2[1 + d] / u2[0]; }
+            double p_hat = ra ? 0.5 * (p1 + p2) : 0.5 * (u1[0] + u2[0]) / (2.0 * 0.5 * (b1 + b2));
+            double vsq = 0.0;
+            for (int d = 0; d < 3; ++d) { va[d] = 0.5 * (v1[d] + v2[d]); vsq += (0.5 * (v1[d] + v2[d])) * (0.5 * (v1[d] + v2[d])); }
+            double H = ra ? 1.0 / (b_log * gm1) + vsq + 2.0 * p_hat / rho_log
+                          : 1.0 / (2.0 * b_log * gm1) + vsq + p_hat / rho_log;
+            for (int d = 0; d < 3; ++d) H -= 0.5 * (0.5 * (v1[d] * v1[d] + v2[d] * v2[d]));
+            for (int fd = 0; fd < 3; ++fd) {
+                F[0][fd] = rho_log * va[fd];
+                for (int vd = 0; vd < 3; ++vd) F[1 + vd][fd] = rho_log * va[fd] * va[vd];
+                F[1 + fd][fd] += p_hat;
+                F[4][fd] = rho_log * va[fd] * H;
+                if (ra) F[4][fd] -= (0.5 * (p1 * v1[fd] + p2 * v2[fd]));
+            }
+        }
+    }
+    void entropy_vars(const double* u, double* v) const {   // euler.cpp:811-830
+        const double rho = u[0];
+        const double p = pressure(u);
+        double s;
+        {   // compute_entropy (euler.cpp:510-531)
+            double rc = rho, pc = p;
+            rc = positive(rc); pc = positive(pc);
+            s = std::log(p * std::pow(rho, -gam));
+        }
+        const double rt = p / gm1;
+        v[0] = (rt * (gam + 1.0 - s) - u[4]) / rt;
+        for (int d = 0; d < 3; ++d) v[1 + d] = u[1 + d] / rt;
+        v[4] = -rho / rt;
+    }
+    void cons_from_entropy(const double* v, double* u) const {   // euler.cpp:833-855
+        double vv = 0.0;
+        for (int d = 0; d < 3; ++d) vv += v[1 + d] * v[1 + d];
+        const double s = gam - v[0] + 0.5 * vv / v[4];
+        const double rt = std::pow((gm1 / std::pow(-v[4], gam)), 1.0 / gm1) * std::exp(-s / gm1);
+        u[0] = -rt * v[4];
+        for (int d = 0; d < 3; ++d) u[1 + d] = rt * v[1 + d];
+        u[4] = rt * (1.0 - 0.5 * vv / v[4]);
+    }
+    double max_normal_eig(const double* u, const double* n) const {   // euler.cpp:1048-1063
+        double v[3]; for (int d = 0; d < 3; ++d) v[d] = u[1 + d] / u[0];
+        const double rho = positive(u[0]);
+        const double c = std::sqrt(pressure(u) * gam / rho);
+        double vn = 0.0; for (int d = 0; d < 3; ++d) vn += v[d] * n[d];
+        return std::fabs(vn) + c;
+    }
+    double max_eig(const double* u) const {   // euler.cpp:1034-1046
+        double v2 = 0.0; for (int d = 0; d < 3; ++d) { const double v = u[1 + d] / u[0]; v2 += v * v; }
+        const double rho = positive(u[0]);
+        const double c = std::sqrt(pressure(u) * gam / rho);
+        return std::sqrt(v2) + c;
+    }
+    // Navier-Stokes viscous flux, "LHS" sign (navier_stokes.cpp:1198-1350)
+    void viscous_flux(const double* u, const double g[5][3], double F[5][3]) const {
+        if (prm->pde != NAVIER_STOKES) { for (int s = 0; s < 5; ++s) for (int d = 0; d < 3; ++d) F[s][d] = 0.0; return; }
+        double w[5]; primitive(u, w);
+        const double rho = w[0];
+        double gw[5][3];
+        for (int d = 0; d < 3; ++d) gw[0][d] = g[0][d];
+        for (int a = 0; a < 3; ++a) for (int d = 0; d < 3; ++d) gw[1 + a][d] = (g[1 + a][d] - w[1 + a] * g[0][d]) / rho;
+        for (int d = 0; d < 3; ++d) {
+            gw[4][d] = g[4][d];
+            for (int k = 0; k < 3; ++k) gw[4][d] -= 0.5 * (w[1 + k] * g[1 + k][d] + u[1 + k] * gw[1 + k][d]);
+            gw[4][d] *= gm1;
+        }
+        const double T = gam * mach2 * (w[4] / rho);
+        double mu = prm->use_constant_viscosity ? 1.0 * prm->constant_viscosity
+                                                : ((1.0 + temp_ratio) / (T + temp_ratio)) * std::pow(T, 1.5);
+        mu = mu / prm->reynolds_inf;
+        const double kappa = mu / (gm1 * mach2 * prm->prandtl);
+        double S[3][3], div = 0.0;
+        for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) S[a][b] = 0.5 * (gw[1 + a][b] + gw[1 + b][a]);
+        for (int d = 0; d < 3; ++d) div += S[d][d];
+        double tau[3][3];
+        const double mu2 = (-2.0 / 3.0) * mu;
+        for (int a = 0; a < 3; ++a) {
+            for (int b = 0; b < 3; ++b) tau[a][b] = 2.0 * mu * S[a][b];
+            tau[a][a] += mu2 * div;
+        }
+        double q[3];
+        for (int d = 0; d < 3; ++d) {
+            const double dT = (gam * mach2 * gw[4][d] - T * gw[0][d]) / rho;
+            q[d] = -kappa * dT;
+        }
+        for (int fd = 0; fd < 3; ++fd) {
+            F[0][fd] = 0.0;
+            for (int sd = 0; sd < 3; ++sd) F[1 + sd][fd] = -tau[sd][fd];
+            F[4][fd] = 0.0;
+            for (int sd = 0; sd < 3; ++sd) F[4][fd] -= w[1 + sd] * tau[fd][sd];
+            F[4][fd] += q[fd];
+        }
+    }
+    void viscous_flux_dot_n(const double* u, const double g[5][3], const double* n, double* out) const {
+        double F[5][3]; viscous_flux(u, g, F);
+        for (int s = 0; s < 5; ++s) { out[s] = 0.0; for (int d = 0; d < 3; ++d) out[s] += F[s][d] * n[d]; }
+    }
+    // convective numerical flux dot n (convective_numerical_flux.cpp:35-480)
+    void conv_num_flux(const double* uL, const double* uR, const double* n, double* out) const {
+        const int t = prm->conv_flux;
+        double base[5] = {0, 0, 0, 0, 0};
+        if (t == TWO_POINT || t == TWO_POINT_LXF || t == TWO_POINT_ROE) {
+            double F[5][3]; two_point(uL, uR, F);
+            for (int s = 0; s < 5; ++s) { double v = 0.0; for (int d = 0; d < 3; ++d) v += F[s][d] * n[d]; base[s] = v; }
+        } else {
+            double FL[5][3], FR[5][3]; convective_flux(uL, FL); convective_flux(uR, FR);
+            for (int s = 0; s < 5; ++s) {
+                double v = 0.0;
+                for (int d = 0; d < 3; ++d) v += 0.5 * (FL[s][d] + FR[s][d]) * n[d];
+                base[s] = v;
+            }
+        }
+        double diss[5] = {0, 0, 0, 0, 0};
+        if (t == LAX_FRIEDRICHS || t == TWO_POINT_LXF) {
+            const double eL = max_normal_eig(uL, n), eR = max_normal_eig(uR, n);
+            const double e = (eL > eR) ? eL : eR;
+            for (int s = 0; s < 5; ++s) diss[s] = -0.5 * e * (uR[s] - uL[s]);
+        } else if (t == ROE || t == TWO_POINT_ROE) {
+            roe_dissipation(uL, uR, n, diss);
+        }
+        for (int s = 0; s < 5; ++s) out[s] = base[s] + diss[s];
+    }
+    void roe_dissipation(const double* uL, const double* uR, const double* n, double* out) const {
+        double wL[5], wR[5]; primitive(uL, wL); primitive(uR, wR);
+        const double rL = wL[0], pL = wL[4], rR = wR[0], pR = wR[4];
+        double vnL = 0.0, vnR = 0.0;
+        for (int d = 0; d < 3; ++d) { vnL += wL[1 + d] * n[d]; vnR += wR[1 + d] * n[d]; }
+        const double hL = (uL[4] + pL) / uL[0], hR = (uR[4] + pR) / uR[0];
+        const double r = std::sqrt(rR / rL), rp1 = r + 1.0;
+        const double rho_a = r * rL;
+        double va[3];
+        for (int d = 0; d < 3; ++d) va[d] = (r * wR[1 + d] + wL[1 + d]) / rp1;
+        const double ha = (r * hR + hL) / rp1;
+        double v2a = 0.0; for (int d = 0; d < 3; ++d) v2a = v2a + va[d] * va[d];
+        double vna = 0.0; for (int d = 0; d < 3; ++d) vna += va[d] * n[d];
+        const double c2a = gm1 * (ha - 0.5 * v2a);
+        double ca = 1e10;
+        if (c2a > 0.0) ca = std::sqrt(c2a);
+        double eig[3] = {std::fabs(vna - ca), std::fabs(vna), std::fabs(vna + ca)};
+        const double cL = sound(rL, pL), cR = sound(rR, pR);
+        const double eL[3] = {std::fabs(vnL - cL), std::fabs(vnL), std::fabs(vnL + cL)};
+        const double eR[3] = {std::fabs(vnR - cR), std::fabs(vnR), std::fabs(vnR + cR)};
+        const double dp = pR - pL, drho = rR - rL, dvn = vnR - vnL;
+        double dvt[3];
+        for (int d = 0; d < 3; ++d) dvt[d] = (wR[1 + d] - wL[1 + d]) - dvn * n[d];
+        for (int e = 0; e < 3; ++e) {   // Harten entropy fix (convective_numerical_flux.cpp:215-232)
+            const double eps = std::max(std::fabs(eig[e] - eL[e]), std::fabs(eR[e] - eig[e]));
+            if (eig[e] < eps) eig[e] = 0.5 * (eig[e] * eig[e] / eps + eps);
+        }
+        const double c0 = eig[0] * (dp - rho_a * ca * dvn) / (2.0 * c2a);
+        const double c1 = eig[1] * (drho - dp / c2a);
+        const double c2 = eig[1] * rho_a;
+        const double c3 = eig[2] * (dp + rho_a * ca * dvn) / (2.0 * c2a);
+        double A[5];
+        A[0] = c0 * 1.0;
+        for (int d = 0; d < 3; ++d) A[1 + d] = c0 * (va[d] - ca * n[d]);
+        A[4] = c0 * (ha - ca * vna);
+        A[0] += c1 * 1.0;
+        for (int d = 0; d < 3; ++d) A[1 + d] += c1 * va[d];
+        A[4] += c1 * v2a * 0.5;
+        A[0] += c2 * 0.0;
+        double dvtv = 0.0;
+        for (int d = 0; d < 3; ++d) { A[1 + d] += c2 * dvt[d]; dvtv += va[d] * dvt[d]; }
+        A[4] += c2 * dvtv;
+        A[0] += c3 * 1.0;
+        for (int d = 0; d < 3; ++d) A[1 + d] += c3 * (va[d] + ca * n[d]);
+        A[4] += c3 * (ha + ca * vna);
+        for (int s = 0; s < 5; ++s) out[s] = -0.5 * A[s];
+    }
+    // dissipative numerical (auxiliary) flux dot n (viscous_numerical_flux.cpp:146-328)
+    void diss_num_flux(const double* uL, const double* uR, const double gL[5][3], const double gR[5][3],
+                       const double* n, double penalty, double* out) const {
+        double fL[5], fR[5];
+        viscous_flux_dot_n(uL, gL, n, fL);
+        viscous_flux_dot_n(uR, gR, n, fR);
+        for (int s = 0; s < 5; ++s) out[s] = 0.5 * (fL[s] + fR[s]);
+        if (prm->diss_flux == SIPG) {
+            double jump[5][3];
+            for (int s = 0; s < 5; ++s) for (int d = 0; d < 3; ++d) jump[s][d] = (uL[s] - uR[s]) * n[d];
+            double aL[5], aR[5];
+            viscous_flux_dot_n(uL, jump, n, aL);
+            viscous_flux_dot_n(uR, jump, n, aR);
+            for (int s = 0; s < 5; ++s) out[s] = out[s] - penalty * (0.5 * (aL[s] + aR[s]));
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------------
+// Mesh: deal.II cell order for the periodic cube (straight_periodic_cube.cpp:17-68).
+// hyper_cube + refine_global(log2 n) gives recursive-child (Morton, child = x+2y+4z)
+// order; subdivided_hyper_cube(n) gives lexicographic order (x fastest).
+// ---------------------------------------------------------------------------------
+static bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+static double warp_map(double x0, double y0, double z0, int d, double a) {
+    const double s = a * std::sin(x0) * std::sin(y0) * std::sin(z0);
+    return (d == 0 ? x0 : d == 1 ? y0 : z0) + s;
+}
+
+Mesh build_periodic_cube(int n, double left, double right, int order, const Ops1D& ops,
+                         double warp, int grid_degree) {
+    Mesh m;
+    m.n = n; m.nc = n * n * n; m.left = left; m.right = right;
+    m.order = (order == ORDER_AUTO) ? (is_pow2(n) ? ORDER_MORTON : ORDER_LEXICOGRAPHIC) : order;
+    m.h = (right - left) / n;
+    m.ijk.resize(m.nc); m.cell_of.assign(m.nc, -1); m.nbr.resize(m.nc);
+    if (m.order == ORDER_MORTON) {
+        int levels = 0; while ((1 << levels) < n) ++levels;
+        for (int c = 0; c < m.nc; ++c) {
+            int ix = 0, iy = 0, iz = 0;
+            for (int l = 0; l < levels; ++l) {
+                const int child = (c >> (3 * (levels - 1 - l))) & 7;
+                ix = 2 * ix + (child & 1); iy = 2 * iy + ((child >> 1) & 1); iz = 2 * iz + ((child >> 2) & 1);
+            }
+            m.ijk[c] = {ix, iy, iz};
+        }
+    } else {
+        for (int c = 0; c < m.nc; ++c) m.ijk[c] = {c % n, (c / n) % n, c / (n * n)};
+    }
+    for (int c = 0; c < m.nc; ++c) { auto& t = m.ijk[c]; m.cell_of[(t[2] * n + t[1]) * n + t[0]] = c; }
+    for (int c = 0; c < m.nc; ++c) {
+        auto t = m.ijk[c];
+        for (int f = 0; f < 6; ++f) {
+            auto u = t; const int d = f / 2; const int s = (f % 2) ? 1 : -1;
+            u[d] = (u[d] + s + n) % n;
+            m.nbr[c][f] = m.cell_of[(u[2] * n + u[1]) * n + u[0]];
+        }
+    }
+    const int nq = ops.nq, nq3 = nq * nq * nq, nd = ops.nd;
+    m.cof.assign((size_t)m.nc * nq3 * 9, 0.0);
+    m.detj.assign((size_t)m.nc * nq3, 0.0);
+    m.cof_face.assign((size_t)m.nc * 6 * nq * nq * 9, 0.0);
+    m.xnode.assign((size_t)m.nc * nd * nd * nd * 3, 0.0);
+    m.warp = warp; m.grid_degree = grid_degree;
+    m.affine = (warp == 0.0);
+    if (!m.affine) throw std::runtime_error("oracle: curvilinear mesh not built here (see build_curvilinear)");
+    const double h = m.h;
+    for (int c = 0; c < m.nc; ++c) {
+        for (int q = 0; q < nq3; ++q) {
+            double* C = &m.cof[((size_t)c * nq3 + q) * 9];
+            C[0] = C[4] = C[8] = h * h;
+            m.detj[(size_t)c * nq3 + q] = h * h * h;
+        }
+        for (int f = 0; f < 6 * nq * nq; ++f) {
+            double* C = &m.cof_face[((size_t)c * 6 * nq * nq + f) * 9];
+            C[0] = C[4] = C[8] = h * h;
+        }
+        const auto t = m.ijk[c];
+        for (int k = 0; k < nd; ++k) for (int j = 0; j < nd; ++j) for (int i = 0; i < nd; ++i) {
+            double* X = &m.xnode[(((size_t)c * nd + k) * nd + j) * nd * 3 + i * 3];
+            X[0] = left + h * (t[0] + ops.xs[i]);
+            X[1] = left + h * (t[1] + ops.xs[j]);
+            X[2] = left + h * (t[2] + ops.xs[k]);
+        }
+    }
+    return m;
+}
+
+void Solver::init(const Params& p, int n, double left, double right, int order, double warp, int grid_degree) {
+    prm = p;
+    ops = build_ops(prm);
+    mesh = build_periodic_cube(n, left, right, order, ops, warp, grid_degree);
+    nd3 = ops.nd * ops.nd * ops.nd;
+    nq3 = ops.nq * ops.nq * ops.nq;
+    ndofs_cell = NSTATE * nd3;
+    aux.assign(3 * ndofs(), 0.0);
+    status = 0;
+}
+
+// ---------------------------------------------------------------------------------
+// Residual assembly
+// ---------------------------------------------------------------------------------
+namespace {
+
+struct Face {   // geometry helper for a face of the reference cube
+    int dn, side;
+};
+
+// surface interpolation: dir dn uses the 1 x c surface row; others the volume op
+inline void surf_apply(const Ops1D& o, const double* vol_op, int r, int c, const double* surf_row,
+                       int iface, const double* in, double* out, bool adding, double factor) {
+    const int dn = iface / 2;
+    const double* A[3] = {vol_op, vol_op, vol_op};
+    int R[3] = {r, r, r};
+    A[dn] = surf_row; R[dn] = 1;
+    (void)o;
+    apply3(A[0], R[0], c, A[1], R[1], c, A[2], R[2], c, in, out, adding, factor);
+}
+inline void surf_inner(const double* vol_op, int r, int c, const double* surf_row, int iface,
+                       const double* in, const double* w, double* out, bool adding, double factor) {
+    const int dn = iface / 2;
+    const double* A[3] = {vol_op, vol_op, vol_op};
+    int R[3] = {r, r, r};
+    A[dn] = surf_row; R[dn] = 1;
+    inner3(A[0], R[0], c, A[1], R[1], c, A[2], R[2], c, in, w, out, adding, factor);
+}
+// volume node on the normal line through face node f at position l
+inline int line_node(int dn, int f, int l, int n) {
+    int c[3];
+    const int t1 = (dn == 0) ? 1 : 0, t2 = (dn == 2) ? 1 : 2;
+    c[dn] = l; c[t1] = f % n; c[t2] = f / n;
+    return (c[2] * n + c[1]) * n + c[0];
+}
+
+} // namespace
+
+void Solver::assemble_residual(const double* U, double* R) {
+    const Ops1D& o = ops;
+    const int nd = o.nd, nq = o.nq, nf = nq * nq;
+    const int nc = mesh.nc;
+    const size_t ndc = (size_t)ndofs_cell;
+    Physics phys(&prm, &status);
+    const bool viscous = (prm.pde == NAVIER_STOKES);
+    const bool split = prm.use_split_form != 0;
+    const double* chi = o.chi.data();
+    const double* dphi = o.dphi.data();
+    const double* phi = o.phi.data();
+    std::vector<double> Wvol(nq3), Wface(nf), ones_vol(nq3, 1.0), ones_face(nf, 1.0);
+    for (int k = 0; k < nq; ++k) for (int j = 0; j < nq; ++j) for (int i = 0; i < nq; ++i)
+        Wvol[(k * nq + j) * nq + i] = o.wq[i] * o.wq[j] * o.wq[k];
+    for (int j = 0; j < nq; ++j) for (int i = 0; i < nq; ++i) Wface[j * nq + i] = o.wq[i] * o.wq[j];
+    const double* nref[6];
+    static const double NREF[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+    for (int f = 0; f < 6; ++f) nref[f] = NREF[f];
+
+    auto penalty_of = [&](int /*c*/, int /*f*/) {   // dg_base.cpp:397-413
+        const int p = prm.poly_degree;
+        const double degsq = (p == 0) ? 1.0 : (double)p * (p + 1);
+        return degsq / mesh.h * prm.sipg_penalty_factor;
+    };
+
+    // ------------------------------ auxiliary equation (strong_dg.cpp:498-1008)
+    if (viscous) {
+        std::vector<double> aux_rhs(3 * ndofs(), 0.0);
+#pragma omp parallel for schedule(static)
+        for (int c = 0; c < nc; ++c) {
+            const double* Uc = U + (size_t)c * ndc;
+            std::vector<double> uq(nq3), g(nq3), pg(nq3), rhs(nd3);
+            std::vector<std::vector<double>> rg(3, std::vector<double>(nq3));
+            double* out[3];
+            for (int d = 0; d < 3; ++d) out[d] = aux_rhs.data() + d * ndofs() + (size_t)c * ndc;
+            for (int s = 0; s < NSTATE; ++s) {
+                // volume part (strong_dg.cpp:666-724)
+                apply3(chi, nq, nd, chi, nq, nd, chi, nq, nd, Uc + s * nd3, uq.data(), false, 1.0);
+                apply3(dphi, nq, nq, phi, nq, nq, phi, nq, nq, uq.data(), rg[0].data(), false, 1.0);
+                apply3(phi, nq, nq, dphi, nq, nq, phi, nq, nq, uq.data(), rg[1].data(), false, 1.0);
+                apply3(phi, nq, nq, phi, nq, nq, dphi, nq, nq, uq.data(), rg[2].data(), false, 1.0);
+                for (int d = 0; d < 3; ++d) {
+                    for (int q = 0; q < nq3; ++q) {
+                        const double* C = &mesh.cof[((size_t)c * nq3 + q) * 9];
+                        double v = 0.0;
+                        for (int j = 0; j < 3; ++j) v += C[d * 3 + j] * rg[j][q];
+                        pg[q] = v;
+                    }
+                    inner3(chi, nq, nd, chi, nq, nd, chi, nq, nd, pg.data(), Wvol.data(), rhs.data(), false, 1.0);
+                    for (int i = 0; i < nd3; ++i) out[d][s * nd3 + i] += rhs[i];
+                }
+            }
+            // face part: this cell's side of each of its 6 faces (strong_dg.cpp:871-1008)
+            for (int f = 0; f < 6; ++f) {
+                const int cn = mesh.nbr[c][f];
+                const int fn = (f % 2) ? f - 1 : f + 1;
+                const double* Un = U + (size_t)cn * ndc;
+                // int = owner (lower index) as in dg_base.cpp:417-449; this cell may be either side
+                const bool owner = c < cn;
+                const int ci = owner ? c : cn, fi = owner ? f : fn, ce = owner ? cn : c, fe = owner ? fn : f;
+                const double* Ui = owner ? Uc : Un; const double* Ue = owner ? Un : Uc;
+                std::vector<double> si(NSTATE * nf), se(NSTATE * nf);
+                for (int s = 0; s < NSTATE; ++s) {
+                    surf_apply(o, chi, nq, nd, o.chi_s[fi % 2].data(), fi, Ui + s * nd3, &si[s * nf], false, 1.0);
+                    surf_apply(o, chi, nq, nd, o.chi_s[fe % 2].data(), fe, Ue + s * nd3, &se[s * nf], false, 1.0);
+                }
+                std::vector<double> term(nf);
+                for (int d = 0; d < 3; ++d) {
+                    for (int s = 0; s < NSTATE; ++s) {
+                        for (int q = 0; q < nf; ++q) {
+                            const double* C = &mesh.cof_face[(((size_t)ci * 6 + fi) * nf + q) * 9];
+                            double np[3];
+                            for (int a = 0; a < 3; ++a) { np[a] = 0.0; for (int b = 0; b < 3; ++b) np[a] += C[a * 3 + b] * nref[fi][b]; }
+                            double J = std::sqrt(np[0] * np[0] + np[1] * np[1] + np[2] * np[2]);
+                            for (int a = 0; a < 3; ++a) np[a] /= J;
+                            const double ustar = 0.5 * (si[s * nf + q] + se[s * nf + q]);
+                            if (owner) term[q] = (ustar - si[s * nf + q]) * np[d] * J;
+                            else term[q] = (ustar - se[s * nf + q]) * (-np[d]) * J;
+                        }
+                        const int fme = owner ? fi : fe;
+                        surf_inner(chi, nq, nd, o.chi_s[fme % 2].data(), fme, term.data(), Wface.data(), rhs.data(), false, 1.0);
+                        for (int i = 0; i < nd3; ++i) out[d][s * nd3 + i] += rhs[i];
+                    }
+                }
+                (void)ce;
+            }
+        }
+        // aux = M_aux^{-1} aux_rhs per dimension
+        for (int d = 0; d < 3; ++d) apply_inverse_mass(aux_rhs.data() + d * ndofs(), aux.data() + d * ndofs(), true);
+    }
+
+    // ------------------------------ primary equations
+    std::fill(R, R + ndofs(), 0.0);
+    // entropy-projected states per cell (volume nodes), computed once per cell
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int c = 0; c < nc; ++c) {
+        const double* Uc = U + (size_t)c * ndc;
+        double* Rc = R + (size_t)c * ndc;
+        auto auxc = [&](int cell, int d) { return aux.data() + d * ndofs() + (size_t)cell * ndc; };
+        // ---- volume term (strong_dg.cpp:1016-1579)
+        std::vector<double> uq(NSTATE * nq3), aq(NSTATE * 3 * nq3), ev(NSTATE * nq3), ecoef(nd3), pe(NSTATE * nq3);
+        for (int s = 0; s < NSTATE; ++s) {
+            apply3(chi, nq, nd, chi, nq, nd, chi, nq, nd, Uc + s * nd3, &uq[s * nq3], false, 1.0);
+            for (int d = 0; d < 3; ++d)
+                apply3(chi, nq, nd, chi, nq, nd, chi, nq, nd, auxc(c, d) + s * nd3, &aq[(s * 3 + d) * nq3], false, 1.0);
+        }
+        std::vector<double> ucons(NSTATE * nq3);   // conservative state from projected entropy variables
+        if (split) {
+            for (int q = 0; q < nq3; ++q) {
+                double u[5], v[5];
+                for (int s = 0; s < 5; ++s) u[s] = uq[s * nq3 + q];
+                phys.entropy_vars(u, v);
+                for (int s = 0; s < 5; ++s) ev[s * nq3 + q] = v[s];
+            }
+            for (int s = 0; s < NSTATE; ++s) {
+                apply3(o.proj.data(), nd, nq, o.proj.data(), nd, nq, o.proj.data(), nd, nq, &ev[s * nq3], ecoef.data(), false, 1.0);
+                apply3(chi, nq, nd, chi, nq, nd, chi, nq, nd, ecoef.data(), &pe[s * nq3], false, 1.0);
+            }
+            for (int q = 0; q < nq3; ++q) {
+                double v[5], u[5];
+                for (int s = 0; s < 5; ++s) v[s] = pe[s * nq3 + q];
+                phys.cons_from_entropy(v, u);
+                for (int s = 0; s < 5; ++s) ucons[s * nq3 + q] = u[s];
+            }
+        }
+        std::vector<double> conv_ref(NSTATE * 3 * nq3, 0.0), diff_ref(NSTATE * 3 * nq3, 0.0);
+        std::vector<double> twopt;
+        if (split) twopt.assign((size_t)NSTATE * 3 * nq3 * nq, 0.0);
+        for (int q = 0; q < nq3; ++q) {
+            double u[5], g[5][3];
+            for (int s = 0; s < 5; ++s) { u[s] = uq[s * nq3 + q]; for (int d = 0; d < 3; ++d) g[s][d] = aq[(s * 3 + d) * nq3 + q]; }
+            const double* Ci = &mesh.cof[((size_t)c * nq3 + q) * 9];
+            if (split) {
+                for (int s = 0; s < 5; ++s) u[s] = ucons[s * nq3 + q];
+                const int xi[3] = {q % nq, (q / nq) % nq, q / (nq * nq)};
+                for (int l = 0; l < nq; ++l) {
+                    for (int rd = 0; rd < 3; ++rd) {
+                        int xj[3] = {xi[0], xi[1], xi[2]}; xj[rd] = l;
+                        const int j = (xj[2] * nq + xj[1]) * nq + xj[0];
+                        const double* Cj = &mesh.cof[((size_t)c * nq3 + j) * 9];
+                        double uj[5]; for (int s = 0; s < 5; ++s) uj[s] = ucons[s * nq3 + j];
+                        double F[5][3]; phys.two_point(u, uj, F);
+                        for (int s = 0; s < 5; ++s) {
+                            double v = 0.0;
+                            for (int k = 0; k < 3; ++k) v += 0.5 * (Ci[k * 3 + rd] + Cj[k * 3 + rd]) * F[s][k];
+                            twopt[((size_t)(s * 3 + rd) * nq3 + q) * nq + l] = v;
+                        }
+                    }
+                }
+            } else {
+                double F[5][3]; phys.convective_flux(u, F);
+                for (int s = 0; s < 5; ++s) for (int d = 0; d < 3; ++d) {
+                    double v = 0.0; for (int k = 0; k < 3; ++k) v += Ci[k * 3 + d] * F[s][k];
+                    conv_ref[(s * 3 + d) * nq3 + q] = v;
+                }
+            }
+            if (viscous) {
+                double F[5][3]; phys.viscous_flux(u, g, F);
+                for (int s = 0; s < 5; ++s) for (int d = 0; d < 3; ++d) {
+                    double v = 0.0; for (int k = 0; k < 3; ++k) v += Ci[k * 3 + d] * F[s][k];
+                    diff_ref[(s * 3 + d) * nq3 + q] = v;
+                }
+            }
+        }
+        std::vector<double> div(nq3), ddiv(nq3), rhs(nd3);
+        for (int s = 0; s < NSTATE; ++s) {
+            if (split) {
+                for (int q = 0; q < nq3; ++q) {
+                    const int xi[3] = {q % nq, (q / nq) % nq, q / (nq * nq)};
+                    double v = 0.0;
+                    for (int rd = 0; rd < 3; ++rd) {
+                        const int a = (rd + 1) % 3, b = (rd + 2) % 3;
+                        // skew row of the node's coordinate in rd, times the two perpendicular weights
+                        for (int l = 0; l < nq; ++l) {
+                            const double Q = o.skew[xi[rd] * nq + l] * o.wq[xi[std::min(a, b)]] * o.wq[xi[std::max(a, b)]];
+                            v += Q * twopt[((size_t)(s * 3 + rd) * nq3 + q) * nq + l];
+                        }
+                    }
+                    div[q] = v;
+                }
+                inner3(chi, nq, nd, chi, nq, nd, chi, nq, nd, div.data(), ones_vol.data(), rhs.data(), false, -1.0);
+            } else {
+                apply3(dphi, nq, nq, phi, nq, nq, phi, nq, nq, &conv_ref[(s * 3 + 0) * nq3], div.data(), false, 1.0);
+                apply3(phi, nq, nq, dphi, nq, nq, phi, nq, nq, &conv_ref[(s * 3 + 1) * nq3], div.data(), true, 1.0);
+                apply3(phi, nq, nq, phi, nq, nq, dphi, nq, nq, &conv_ref[(s * 3 + 2) * nq3], div.data(), true, 1.0);
+                inner3(chi, nq, nd, chi, nq, nd, chi, nq, nd, div.data(), Wvol.data(), rhs.data(), false, -1.0);
+            }
+            if (viscous) {
+                apply3(dphi, nq, nq, phi, nq, nq, phi, nq, nq, &diff_ref[(s * 3 + 0) * nq3], ddiv.data(), false, 1.0);
+                apply3(phi, nq, nq, dphi, nq, nq, phi, nq, nq, &diff_ref[(s * 3 + 1) * nq3], ddiv.data(), true, 1.0);
+                apply3(phi, nq, nq, phi, nq, nq, dphi, nq, nq, &diff_ref[(s * 3 + 2) * nq3], ddiv.data(), true, 1.0);
+                inner3(chi, nq, nd, chi, nq, nd, chi, nq, nd, ddiv.data(), Wvol.data(), rhs.data(), true, -1.0);
+            } else {
+                // the reference adds -chi^T W div(F_v) with F_v == 0 for Euler: a no-op
+            }
+            for (int i = 0; i < nd3; ++i) Rc[s * nd3 + i] += rhs[i];
+        }
+
+        // ---- face terms (strong_dg.cpp:2367-3576); this cell's side of each face
+        for (int f = 0; f < 6; ++f) {
+            const int cn = mesh.nbr[c][f];
+            const int fn = (f % 2) ? f - 1 : f + 1;
+            const bool owner = c < cn;
+            const int ci = owner ? c : cn, fi = owner ? f : fn, ce = owner ? cn : c, fe = owner ? fn : f;
+            const double* Ui = U + (size_t)ci * ndc;
+            const double* Ue = U + (size_t)ce * ndc;
+            const int dni = fi / 2, dne = fe / 2;
+            // interpolations (strong_dg.cpp:2420-2470)
+            std::vector<double> vi(NSTATE * nq3), ve(NSTATE * nq3), si(NSTATE * nf), se(NSTATE * nf);
+            std::vector<double> avi(NSTATE * 3 * nq3), ave(NSTATE * 3 * nq3), asi(NSTATE * 3 * nf), ase(NSTATE * 3 * nf);
+            for (int s = 0; s < NSTATE; ++s) {
+                apply3(chi, nq, nd, chi, nq, nd, chi, nq, nd, Ui + s * nd3, &vi[s * nq3], false, 1.0);
+                apply3(chi, nq, nd, chi, nq, nd, chi, nq, nd, Ue + s * nd3, &ve[s * nq3], false, 1.0);
+                surf_apply(o, chi, nq, nd, o.chi_s[fi % 2].data(), fi, Ui + s * nd3, &si[s * nf], false, 1.0);
+                surf_apply(o, chi, nq, nd, o.chi_s[fe % 2].data(), fe, Ue + s * nd3, &se[s * nf], false, 1.0);
+                for (int d = 0; d < 3; ++d) {
+                    apply3(chi, nq, nd, chi, nq, nd, chi, nq, nd, auxc(ci, d) + s * nd3, &avi[(s * 3 + d) * nq3], false, 1.0);
+                    apply3(chi, nq, nd, chi, nq, nd, chi, nq, nd, auxc(ce, d) + s * nd3, &ave[(s * 3 + d) * nq3], false, 1.0);
+                    surf_apply(o, chi, nq, nd, o.chi_s[fi % 2].data(), fi, auxc(ci, d) + s * nd3, &asi[(s * 3 + d) * nf], false, 1.0);
+                    surf_apply(o, chi, nq, nd, o.chi_s[fe % 2].data(), fe, auxc(ce, d) + s * nd3, &ase[(s * 3 + d) * nf], false, 1.0);
+                }
+            }
+            // reference volume fluxes interpolated to the face, dotted with the unit reference normal (:2836-3041)
+            std::vector<double> cfi(NSTATE * nf, 0.0), cfe(NSTATE * nf, 0.0), dfi(NSTATE * nf, 0.0), dfe(NSTATE * nf, 0.0);
+            {
+                std::vector<double> cri(NSTATE * nq3), cre(NSTATE * nq3), dri(NSTATE * nq3), dre(NSTATE * nq3);
+                for (int side = 0; side < 2; ++side) {
+                    const int cc = side ? ce : ci; const int dn = side ? dne : dni;
+                    const std::vector<double>& vv = side ? ve : vi; const std::vector<double>& aa = side ? ave : avi;
+                    std::vector<double>& cr = side ? cre : cri; std::vector<double>& dr = side ? dre : dri;
+                    for (int q = 0; q < nq3; ++q) {
+                        double u[5], g[5][3];
+                        for (int s = 0; s < 5; ++s) { u[s] = vv[s * nq3 + q]; for (int d = 0; d < 3; ++d) g[s][d] = aa[(s * 3 + d) * nq3 + q]; }
+                        const double* C = &mesh.cof[((size_t)cc * nq3 + q) * 9];
+                        if (!split) {
+                            double F[5][3]; phys.convective_flux(u, F);
+                            for (int s = 0; s < 5; ++s) { double v = 0.0; for (int k = 0; k < 3; ++k) v += C[k * 3 + dn] * F[s][k]; cr[s * nq3 + q] = v; }
+                        }
+                        double F[5][3]; phys.viscous_flux(u, g, F);
+                        for (int s = 0; s < 5; ++s) { double v = 0.0; for (int k = 0; k < 3; ++k) v += C[k * 3 + dn] * F[s][k]; dr[s * nq3 + q] = v; }
+                    }
+                }
+                for (int s = 0; s < NSTATE; ++s) {
+                    if (!split) {
+                        surf_apply(o, phi, nq, nq, o.phi_s[fi % 2].data(), fi, &cri[s * nq3], &cfi[s * nf], false, nref[fi][dni]);
+                        surf_apply(o, phi, nq, nq, o.phi_s[fe % 2].data(), fe, &cre[s * nq3], &cfe[s * nf], false, nref[fe][dne]);
+                    }
+                    surf_apply(o, phi, nq, nq, o.phi_s[fi % 2].data(), fi, &dri[s * nq3], &dfi[s * nf], false, nref[fi][dni]);
+                    surf_apply(o, phi, nq, nq, o.phi_s[fe % 2].data(), fe, &dre[s * nq3], &dfe[s * nf], false, nref[fe][dne]);
+                }
+            }
+            // entropy projection (:3050-3142)
+            std::vector<double> pvi(NSTATE * nq3), pve(NSTATE * nq3), psi(NSTATE * nf), pse(NSTATE * nf);
+            {
+                std::vector<double> evi(NSTATE * nq3), eve(NSTATE * nq3), coef(nd3);
+                for (int q = 0; q < nq3; ++q) {
+                    double u[5], v[5];
+                    for (int s = 0; s < 5; ++s) u[s] = vi[s * nq3 + q];
+                    phys.entropy_vars(u, v);
+                    for (int s = 0; s < 5; ++s) evi[s * nq3 + q] = v[s];
+                    for (int s = 0; s < 5; ++s) u[s] = ve[s * nq3 + q];
+                    phys.entropy_vars(u, v);
+                    for (int s = 0; s < 5; ++s) eve[s * nq3 + q] = v[s];
+                }
+                for (int s = 0; s < NSTATE; ++s) {
+                    apply3(o.proj.data(), nd, nq, o.proj.data(), nd, nq, o.proj.data(), nd, nq, &evi[s * nq3], coef.data(), false, 1.0);
+                    apply3(chi, nq, nd, chi, nq, nd, chi, nq, nd, coef.data(), &pvi[s * nq3], false, 1.0);
+                    surf_apply(o, chi, nq, nd, o.chi_s[fi % 2].data(), fi, coef.data(), &psi[s * nf], false, 1.0);
+                    apply3(o.proj.data(), nd, nq, o.proj.data(), nd, nq, o.proj.data(), nd, nq, &eve[s * nq3], coef.data(), false, 1.0);
+                    apply3(chi, nq, nd, chi, nq, nd, chi, nq, nd, coef.data(), &pve[s * nq3], false, 1.0);
+                    surf_apply(o, chi, nq, nd, o.chi_s[fe % 2].data(), fe, coef.data(), &pse[s * nf], false, 1.0);
+                }
+            }
+            // hybrid surface-volume two-point terms (:3144-3350)
+            std::vector<double> hsi(NSTATE * nf, 0.0), hse(NSTATE * nf, 0.0), hvi(NSTATE * nq3, 0.0), hve(NSTATE * nq3, 0.0);
+            if (split) {
+                std::vector<double> s2i((size_t)NSTATE * nf * nq), s2e((size_t)NSTATE * nf * nq);
+                for (int q = 0; q < nf; ++q) {
+                    const double* Cs = &mesh.cof_face[(((size_t)ci * 6 + fi) * nf + q) * 9];
+                    double vfi[5], vfe[5], ufi[5], ufe[5];
+                    for (int s = 0; s < 5; ++s) { vfi[s] = psi[s * nf + q]; vfe[s] = pse[s * nf + q]; }
+                    phys.cons_from_entropy(vfi, ufi); phys.cons_from_entropy(vfe, ufe);
+                    for (int side = 0; side < 2; ++side) {
+                        const int dn = side ? dne : dni; const int cc = side ? ce : ci;
+                        const std::vector<double>& pv = side ? pve : pvi;
+                        const double* uf = side ? ufe : ufi;
+                        std::vector<double>& s2 = side ? s2e : s2i;
+                        for (int l = 0; l < nq; ++l) {
+                            const int jv = line_node(dn, q, l, nq);
+                            const double* Cv = &mesh.cof[((size_t)cc * nq3 + jv) * 9];
+                            double ev5[5], uv[5];
+                            for (int s = 0; s < 5; ++s) ev5[s] = pv[s * nq3 + jv];
+                            phys.cons_from_entropy(ev5, uv);
+                            double F[5][3]; phys.two_point(uv, uf, F);
+                            for (int s = 0; s < 5; ++s) {
+                                double v = 0.0;
+                                for (int k = 0; k < 3; ++k) v += 0.5 * (Cs[k * 3 + dn] + Cv[k * 3 + dn]) * F[s][k];
+                                s2[((size_t)s * nf + q) * nq + l] = v;
+                            }
+                        }
+                    }
+                }
+                for (int side = 0; side < 2; ++side) {
+                    const int ff = side ? fe : fi; const int dn = ff / 2;
+                    const std::vector<double>& s2 = side ? s2e : s2i;
+                    std::vector<double>& hs = side ? hse : hsi; std::vector<double>& hv = side ? hve : hvi;
+                    const double nn = nref[ff][dn];
+                    for (int s = 0; s < NSTATE; ++s)
+                        for (int q = 0; q < nf; ++q)
+                            for (int l = 0; l < nq; ++l) {
+                                const double Hop = o.phi_s[ff % 2][l] * o.wq[q % nq] * o.wq[q / nq];
+                                const double Hv = Hop * s2[((size_t)s * nf + q) * nq + l];
+                                hs[s * nf + q] -= Hv * nn;
+                                hv[s * nq3 + line_node(dn, q, l, nq)] += Hv * nn;
+                            }
+                }
+            }
+            // numerical fluxes at face nodes (:3354-3452)
+            std::vector<double> cn_(NSTATE * nf), dn_(NSTATE * nf);
+            const double pen = 0.5 * (penalty_of(ci, fi) + penalty_of(ce, fe));
+            for (int q = 0; q < nf; ++q) {
+                const double* Cs = &mesh.cof_face[(((size_t)ci * 6 + fi) * nf + q) * 9];
+                double ui[5], ue[5], ri[5], re[5], gi[5][3], ge[5][3];
+                for (int s = 0; s < 5; ++s) {
+                    ri[s] = si[s * nf + q]; re[s] = se[s * nf + q];
+                    for (int d = 0; d < 3; ++d) { gi[s][d] = asi[(s * 3 + d) * nf + q]; ge[s][d] = ase[(s * 3 + d) * nf + q]; }
+                }
+                {
+                    double vfi[5], vfe[5];
+                    for (int s = 0; s < 5; ++s) { vfi[s] = psi[s * nf + q]; vfe[s] = pse[s * nf + q]; }
+                    phys.cons_from_entropy(vfi, ui); phys.cons_from_entropy(vfe, ue);
+                }
+                if (!split) for (int s = 0; s < 5; ++s) { ui[s] = ri[s]; ue[s] = re[s]; }
+                double np[3];
+                for (int a = 0; a < 3; ++a) { np[a] = 0.0; for (int b = 0; b < 3; ++b) np[a] += Cs[a * 3 + b] * nref[fi][b]; }
+                double J = 0.0; for (int a = 0; a < 3; ++a) J += np[a] * np[a];
+                J = std::sqrt(J);
+                for (int a = 0; a < 3; ++a) np[a] /= J;
+                double cf[5], df[5] = {0, 0, 0, 0, 0};
+                phys.conv_num_flux(ui, ue, np, cf);
+                if (viscous) phys.diss_num_flux(ri, re, gi, ge, np, pen, df);
+                for (int s = 0; s < 5; ++s) { cn_[s * nf + q] = J * cf[s]; dn_[s * nf + q] = J * df[s]; }
+            }
+            // lift this cell's side (:3454-3576)
+            std::vector<double> r(nd3);
+            const bool me_int = owner;
+            const int fme = me_int ? fi : fe;
+            for (int s = 0; s < NSTATE; ++s) {
+                const double* crow = o.chi_s[fme % 2].data();
+                if (split) {
+                    surf_inner(chi, nq, nd, crow, fme, me_int ? &hsi[s * nf] : &hse[s * nf], ones_face.data(), r.data(), false, -1.0);
+                    inner3(chi, nq, nd, chi, nq, nd, chi, nq, nd, me_int ? &hvi[s * nq3] : &hve[s * nq3], ones_vol.data(), r.data(), true, -1.0);
+                } else {
+                    surf_inner(chi, nq, nd, crow, fme, me_int ? &cfi[s * nf] : &cfe[s * nf], Wface.data(), r.data(), false, 1.0);
+                }
+                surf_inner(chi, nq, nd, crow, fme, me_int ? &dfi[s * nf] : &dfe[s * nf], Wface.data(), r.data(), true, 1.0);
+                surf_inner(chi, nq, nd, crow, fme, &cn_[s * nf], Wface.data(), r.data(), true, me_int ? -1.0 : 1.0);
+                surf_inner(chi, nq, nd, crow, fme, &dn_[s * nf], Wface.data(), r.data(), true, me_int ? -1.0 : 1.0);
+                for (int i = 0; i < nd3; ++i) Rc[s * nd3 + i] += r[i];
+            }
+        }
+    }
+}
+
+void Solver::apply_inverse_mass(const double* in, double* out, bool aux_eq) {
+    // affine: (M+K)^{-1} (x) (M+K)^{-1} (x) (M+K)^{-1} / det J  (dg_base.cpp:4207-4219)
+    const int nd = ops.nd;
+    const double* Mi = aux_eq ? ops.minv_aux.data() : ops.minv.data();
+    const size_t ndc = (size_t)ndofs_cell;
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < mesh.nc; ++c) {
+        const double dj = mesh.detj[(size_t)c * nq3];
+        for (int s = 0; s < NSTATE; ++s)
+            apply3(Mi, nd, nd, Mi, nd, nd, Mi, nd, nd, in + c * ndc + s * nd3, out + c * ndc + s * nd3, false, 1.0 / dj);
+    }
+}
+
+void Solver::rk_step(double* U, double dt) {
+    // Butcher tableaux (runge_kutta_methods.cpp:7-47), stage loop (runge_kutta_base.cpp:21-39,
+    // runge_kutta_ode_solver.cpp:15-100)
+    int ns; double a[4][4] = {{0}}, b[4] = {0}, cc[4] = {0};
+    if (prm.rk_method == RK4) {
+        ns = 4; a[1][0] = 0.5; a[2][1] = 0.5; a[3][2] = 1.0;
+        b[0] = 1.0 / 6.0; b[1] = 1.0 / 3.0; b[2] = 1.0 / 3.0; b[3] = 1.0 / 6.0;
+        cc[1] = 0.5; cc[2] = 0.5; cc[3] = 1.0;
+    } else if (prm.rk_method == SSPRK3) {
+        ns = 3; a[1][0] = 1.0; a[2][0] = 0.25; a[2][1] = 0.25;
+        b[0] = 1.0 / 6.0; b[1] = 1.0 / 6.0; b[2] = 2.0 / 3.0;
+        cc[1] = 1.0; cc[2] = 0.5;
+    } else { ns = 1; b[0] = 1.0; }
+    const size_t N = ndofs();
+    std::vector<double> un(U, U + N), R(N);
+    std::vector<std::vector<double>> k(ns, std::vector<double>(N));
+    for (int i = 0; i < ns; ++i) {
+        std::vector<double>& st = k[i];
+        std::fill(st.begin(), st.end(), 0.0);
+        for (int j = 0; j < i; ++j)
+            if (a[i][j] != 0.0) for (size_t m = 0; m < N; ++m) st[m] += a[i][j] * k[j][m];
+        for (size_t m = 0; m < N; ++m) { st[m] *= dt; st[m] += 1.0 * un[m]; }
+        assemble_residual(st.data(), R.data());
+        apply_inverse_mass(R.data(), st.data());
+    }
+    for (int i = 0; i < ns; ++i)
+        for (size_t m = 0; m < N; ++m) un[m] += dt * b[i] * k[i][m];
+    std::copy(un.begin(), un.end(), U);
+    current_time += dt;
+    (void)cc;
+}
+
+void Solver::interpolate_ic(double* U, int ic, const double* icp) {
+    Physics phys(&prm, &status);
+    const int nd = ops.nd;
+    for (int c = 0; c < mesh.nc; ++c)
+        for (int i = 0; i < nd3; ++i) {
+            const double* X = &mesh.xnode[((size_t)c * nd3 + i) * 3];
+            double w[5], u[5];
+            if (ic == IC_TGV) {   // initial_condition_function.cpp:261-310
+                const double x = X[0], y = X[1], z = X[2];
+                w[0] = 1.0;
+                w[1] = std::sin(x) * std::cos(y) * std::cos(z);
+                w[2] = -std::cos(x) * std::sin(y) * std::cos(z);
+                w[3] = 0.0;
+                w[4] = 1.0 / (prm.gamma * prm.mach_inf * prm.mach_inf) + (1.0 / 16.0) * (std::cos(2.0 * x) + std::cos(2.0 * y)) * (std::cos(2.0 * z) + 2.0);
+                phys.conservative_from_primitive(w, u);
+            } else {
+                // isentropic vortex (initial_condition_function.cpp:643-690); IC_VORTEX_PARAM takes
+                // icp = {beta, mach, dir_x, dir_y, dir_z, x0, y0, t, L} and translates with the flow.
+                const double gam = prm.gamma;
+                double Minf, beta, dir[3], x0 = 0.0, y0 = 0.0, t = 0.0, L = 0.0;
+                if (ic == IC_ISENTROPIC_VORTEX) {
+                    Minf = std::sqrt(2.0 / gam);
+                    beta = Minf * 5 * std::sqrt(2.0) / 4.0 / PI * std::exp(1.0 / 2.0);
+                    dir[0] = std::cos(PI / 4); dir[1] = std::sin(PI / 4); dir[2] = 0.0;
+                } else {
+                    beta = icp[0]; Minf = icp[1]; dir[0] = icp[2]; dir[1] = icp[3]; dir[2] = icp[4];
+                    x0 = icp[5]; y0 = icp[6]; t = icp[7]; L = icp[8];
+                }
+                double x = X[0] - x0 - Minf * dir[0] * t, y = X[1] - y0 - Minf * dir[1] * t;
+                if (L > 0.0) { x -= L * std::round(x / L); y -= L * std::round(y / L); }
+                const double Om = beta * std::exp(-0.5 * (x * x + y * y));
+                const double dT = -(gam - 1.0) / 2.0 * Om * Om;
+                w[0] = std::pow(1 + dT, 1.0 / (gam - 1.0));
+                w[1] = Minf * dir[0] - y * Om;
+                w[2] = Minf * dir[1] + x * Om;
+                w[3] = Minf * dir[2];
+                w[4] = 1.0 / gam * std::pow(1 + dT, gam / (gam - 1.0));
+                phys.conservative_from_primitive(w, u);
+            }
+            for (int s = 0; s < 5; ++s) U[(size_t)c * ndofs_cell + s * nd3 + i] = u[s];
+        }
+}
+
+void Solver::integrals(const double* U, double* out) {
+    // periodic_turbulence.cpp:439-672 with QGauss(p+11) over-integration
+    Physics phys(&prm, &status);
+    const int nd = ops.nd;
+    const int ne = prm.poly_degree + 1 + 10;
+    std::vector<double> xe, we; gauss_legendre(ne, xe, we);
+    std::vector<double> B((size_t)ne * nd), dB((size_t)ne * nd);
+    for (int q = 0; q < ne; ++q) lagrange_eval(ops.xs, xe[q], &B[q * nd], &dB[q * nd]);
+    const int ne3 = ne * ne * ne;
+    double ke = 0.0, ens = 0.0, wave = 0.0;
+#pragma omp parallel for reduction(+ : ke, ens) reduction(max : wave)
+    for (int c = 0; c < mesh.nc; ++c) {
+        const double h = mesh.h, dj = h * h * h;
+        std::vector<double> uq(5 * ne3), gq(15 * ne3);
+        for (int s = 0; s < 5; ++s) {
+            const double* Uc = U + (size_t)c * ndofs_cell + s * nd3;
+            apply3(B.data(), ne, nd, B.data(), ne, nd, B.data(), ne, nd, Uc, &uq[s * ne3], false, 1.0);
+            apply3(dB.data(), ne, nd, B.data(), ne, nd, B.data(), ne, nd, Uc, &gq[(s * 3 + 0) * ne3], false, 1.0);
+            apply3(B.data(), ne, nd, dB.data(), ne, nd, B.data(), ne, nd, Uc, &gq[(s * 3 + 1) * ne3], false, 1.0);
+            apply3(B.data(), ne, nd, B.data(), ne, nd, dB.data(), ne, nd, Uc, &gq[(s * 3 + 2) * ne3], false, 1.0);
+        }
+        for (int q = 0; q < ne3; ++q) {
+            double u[5], g[5][3], w[5];
+            for (int s = 0; s < 5; ++s) {
+                u[s] = uq[s * ne3 + q];
+                for (int d = 0; d < 3; ++d) g[s][d] = (h * h) * gq[(s * 3 + d) * ne3 + q] / dj;
+            }
+            phys.primitive(u, w);
+            double v2 = 0.0; for (int d = 0; d < 3; ++d) v2 += w[1 + d] * w[1 + d];
+            const double kin = 0.5 * w[0] * v2;
+            double gv[3][3];
+            for (int a = 0; a < 3; ++a) for (int d = 0; d < 3; ++d) gv[a][d] = (g[1 + a][d] - w[1 + a] * g[0][d]) / w[0];
+            const double om0 = gv[2][1] - gv[1][2], om1 = gv[0][2] - gv[2][0], om2 = gv[1][0] - gv[0][1];
+            const double en = 0.5 * u[0] * (om0 * om0 + om1 * om1 + om2 * om2);
+            const double wt = we[q % ne] * we[(q / ne) % ne] * we[q / (ne * ne)] * dj;
+            ke += kin * wt; ens += en * wt;
+            const double mw = phys.max_eig(u);
+            if (mw > wave) wave = mw;
+        }
+    }
+    const double vol = std::pow(mesh.right - mesh.left, 3);
+    out[0] = ke / vol;
+    out[1] = ens / vol;
+    out[2] = (prm.pde == NAVIER_STOKES) ? 2.0 * out[1] / prm.reynolds_inf : 0.0;
+    out[3] = wave;
+}
+
+} // namespace oracle
