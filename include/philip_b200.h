@@ -1,0 +1,131 @@
+/*
+ * philip_b200 — C-ABI of the B200 explicit strong-form DG/FR residual and RK stage.
+ *
+ * Plain C types only (pointers, sizes, scalars); no exceptions cross this boundary.
+ * Every entry point returns 0 on success or a PH_ERR_* code; ph_last_error() gives
+ * the message of the calling thread's last failure.
+ *
+ * State layout (the reference's DoF order with do_renumber_dofs=false): cell-major in
+ * deal.II active-cell order, then conservative component (rho, rho u, rho v, rho w, E),
+ * then the (p+1)^3 GLL support points lexicographically with x fastest
+ * (local dof = istate*n_shape + ishape, src/dg/strong_dg.cpp:142-147).
+ *
+ * Thread-safety: one context per host thread; a context is bound to one CUDA stream.
+ */
+#ifndef PHILIP_B200_H
+#define PHILIP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ph_ctx ph_ctx;
+
+enum {
+    PH_OK = 0,
+    PH_ERR_INVALID = 1,      /* bad argument */
+    PH_ERR_UNSUPPORTED = 2,  /* configuration outside the GPU path (e.g. GL flux nodes) */
+    PH_ERR_CUDA = 3,         /* CUDA runtime failure */
+    PH_ERR_NOMEM = 4         /* device allocation failed */
+};
+
+enum { PH_HOST = 0, PH_DEVICE = 1 };                 /* where a pointer lives */
+enum { PH_FP64 = 0, PH_FP32_RESIDUAL = 1 };          /* arithmetic of the residual */
+
+/* .prm keys of the hot path (src/parameters/all_parameters.cpp:39-400,
+ * parameters_ode_solver.cpp, parameters_euler.cpp, parameters_navier_stokes.cpp).
+ * Enumerations use the reference's spelling order:
+ *   flux_nodes_type: 0 GL, 1 GLL            pde_type: 0 euler, 1 navier_stokes
+ *   two_point_num_flux_type: 0 KG, 1 IR, 2 CH, 3 Ra
+ *   conv_num_flux: 0 lax_friedrichs, 1 roe, 2 central_flux, 3 two_point_flux,
+ *                  4 two_point_flux_with_lax_friedrichs_dissipation,
+ *                  5 two_point_flux_with_roe_dissipation
+ *   diss_num_flux: 0 symm_internal_penalty, 1 bassi_rebay_2, 2 central_visc_flux
+ *   flux_reconstruction: 0 cDG, 1 cSD, 2 cHU, 3 cNegative, 4 cNegative2, 5 cPlus,
+ *                        6 c10Thousand, 7 cHULumped, 8 user_specified_value
+ *   flux_reconstruction_aux: 0 kDG (the GPU path supports kDG)
+ *   runge_kutta_method: 0 euler_ex, 1 ssprk3_ex, 2 rk4_ex
+ *   non_physical_behavior: 0 return_big_number, 1 abort_run, 2 print_warning */
+typedef struct ph_params {
+    int poly_degree;
+    int overintegration;
+    int flux_nodes_type;
+    int pde_type;
+    int use_split_form;
+    int two_point_num_flux_type;
+    int conv_num_flux;
+    int diss_num_flux;
+    int flux_reconstruction;
+    int flux_reconstruction_aux;
+    int runge_kutta_method;
+    int use_constant_viscosity;
+    int non_physical_behavior;
+    int precision;                        /* PH_FP64 or PH_FP32_RESIDUAL */
+    double FR_user_specified_correction_parameter_value;
+    double gamma_gas;
+    double mach_infinity;
+    double reynolds_number_inf;
+    double prandtl_number;
+    double temperature_inf;
+    double nondimensionalized_constant_viscosity;
+    double sipg_penalty_factor;
+} ph_params;
+
+/* Periodic cube [left,right]^3 with n^3 cells (PeriodicCubeFlow::generate_grid,
+ * src/flow_solver/flow_solver_cases/periodic_cube_flow.cpp:25-65). cell_order:
+ * 0 = as deal.II numbers it (recursive children when n is a power of two,
+ * lexicographic otherwise), 1 = lexicographic, 2 = recursive children. */
+typedef struct ph_mesh_desc {
+    int n_cells_per_direction;
+    int cell_order;
+    double left;
+    double right;
+} ph_mesh_desc;
+
+/* Builds host index maps, 1-D operators and device buffers (replaces DGFactory::
+ * create_discontinuous_galerkin + DGBase::allocate_system, src/dg/dg_factory.cpp:11,
+ * src/dg/dg_base.hpp:184, and ODESolverFactory::create_ODESolver + allocate_ode_system,
+ * src/ode_solver/ode_solver_factory.cpp:22, ode_solver_base.h:79).
+ * cuda_stream may be NULL (the default stream). */
+int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_stream, ph_ctx** out);
+int ph_ctx_destroy(ph_ctx* ctx);
+
+int64_t ph_ndofs(const ph_ctx* ctx);
+int ph_cell_ijk(const ph_ctx* ctx, int32_t* ijk /* 3 per cell */);
+
+/* DGBase::solution assignment / read-back (src/dg/dg_base.hpp:396). */
+int ph_set_state(ph_ctx* ctx, const double* U, int where);
+int ph_get_state(ph_ctx* ctx, double* U, int where);
+
+/* DGBase::assemble_residual (src/dg/dg_base.hpp:571, dg_base.cpp:2599-2915): R(U),
+ * the right-hand side before the inverse mass matrix, in the reference DoF order. */
+int ph_residual(ph_ctx* ctx, const double* U, double* R, int where);
+
+/* DGBase::apply_inverse_global_mass_matrix (src/dg/dg_base.hpp:267, dg_base.cpp:4089-4260). */
+int ph_apply_inverse_mass(ph_ctx* ctx, const double* R, double* out, int where);
+
+/* ODESolverBase::step_in_time for the explicit Butcher RK solver
+ * (src/ode_solver/ode_solver_base.h:70, runge_kutta_base.cpp:21-39), nsteps times
+ * with the same dt, on the context's state. Asynchronous on the context stream. */
+int ph_rk_step(ph_ctx* ctx, double dt, int nsteps);
+
+/* PeriodicTurbulence::compute_and_update_integrated_quantities subset
+ * (src/flow_solver/flow_solver_cases/periodic_turbulence.cpp:439-672):
+ * out[0] kinetic energy, out[1] enstrophy, out[2] vorticity-based dissipation rate,
+ * out[3] maximum convective wave speed; all divided by the domain volume except out[3]. */
+int ph_integrals(ph_ctx* ctx, double out[4]);
+
+/* Status word: bit 0 = a negative density or pressure was met (Euler::check_positive_quantity,
+ * src/physics/euler.cpp:155-172). Reading clears it. */
+int ph_status(ph_ctx* ctx, uint32_t* flags);
+
+int ph_sync(ph_ctx* ctx);
+const char* ph_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PHILIP_B200_H */

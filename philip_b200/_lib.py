@@ -1,0 +1,78 @@
+"""ctypes binding of the in-tree C-ABI library (include/philip_b200.h).
+
+The library is the product: there is no CPU fallback. Loading fails loudly when
+``libphilip_b200.so`` is missing or no CUDA device is visible.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libphilip_b200.so")
+
+PH_HOST, PH_DEVICE = 0, 1
+PH_FP64, PH_FP32_RESIDUAL = 0, 1
+ERRORS = {1: "invalid argument", 2: "unsupported configuration", 3: "CUDA error", 4: "out of device memory"}
+
+EXPORTED = ["ph_ctx_create", "ph_ctx_destroy", "ph_ndofs", "ph_cell_ijk", "ph_set_state", "ph_get_state",
+            "ph_residual", "ph_apply_inverse_mass", "ph_rk_step", "ph_integrals", "ph_status", "ph_sync",
+            "ph_last_error"]
+
+
+class PhParams(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in (
+        "poly_degree", "overintegration", "flux_nodes_type", "pde_type", "use_split_form",
+        "two_point_num_flux_type", "conv_num_flux", "diss_num_flux", "flux_reconstruction",
+        "flux_reconstruction_aux", "runge_kutta_method", "use_constant_viscosity", "non_physical_behavior",
+        "precision")] + [(n, ctypes.c_double) for n in (
+        "FR_user_specified_correction_parameter_value", "gamma_gas", "mach_infinity", "reynolds_number_inf",
+        "prandtl_number", "temperature_inf", "nondimensionalized_constant_viscosity", "sipg_penalty_factor")]
+
+
+class PhMeshDesc(ctypes.Structure):
+    _fields_ = [("n_cells_per_direction", ctypes.c_int), ("cell_order", ctypes.c_int),
+                ("left", ctypes.c_double), ("right", ctypes.c_double)]
+
+
+class PhError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def load(build_if_missing: bool = False):
+    """Load the library (optionally building it first); raises if it cannot be loaded."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        if not build_if_missing:
+            raise PhError(f"{LIB_PATH} is missing: run philip_b200.build.build() (or __graft_entry__.build())")
+        from . import build as _build
+        _build.build()
+    L = ctypes.CDLL(LIB_PATH)
+    vp = ctypes.c_void_p
+    dp = ctypes.POINTER(ctypes.c_double)
+    L.ph_ctx_create.argtypes = [ctypes.POINTER(PhMeshDesc), ctypes.POINTER(PhParams), vp, ctypes.POINTER(vp)]
+    L.ph_ctx_destroy.argtypes = [vp]
+    L.ph_ndofs.argtypes = [vp]; L.ph_ndofs.restype = ctypes.c_int64
+    L.ph_cell_ijk.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
+    L.ph_set_state.argtypes = [vp, vp, ctypes.c_int]
+    L.ph_get_state.argtypes = [vp, vp, ctypes.c_int]
+    L.ph_residual.argtypes = [vp, vp, vp, ctypes.c_int]
+    L.ph_apply_inverse_mass.argtypes = [vp, vp, vp, ctypes.c_int]
+    L.ph_rk_step.argtypes = [vp, ctypes.c_double, ctypes.c_int]
+    L.ph_integrals.argtypes = [vp, dp]
+    L.ph_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32)]
+    L.ph_sync.argtypes = [vp]
+    L.ph_last_error.restype = ctypes.c_char_p
+    _lib = L
+    return L
+
+
+def check(rc: int):
+    if rc != 0:
+        msg = _lib.ph_last_error().decode() if _lib is not None else ""
+        raise PhError(f"philip_b200 error {rc} ({ERRORS.get(rc, '?')}): {msg}")

@@ -1,0 +1,578 @@
+// C-ABI of the B200 strong-form DG/FR residual and explicit RK stage: context set-up
+// (host index maps, 1-D operators, device buffers) and stage orchestration.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/philip_b200.h"
+#include "ph_launch.cuh"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define PH_CUDA(call)                                                                         \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) return fail(PH_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// ---------------------------------------------------------------------------------------
+// 1-D nodes, bases and FR operators (host, double)
+// ---------------------------------------------------------------------------------------
+void legendre_pd(int n, double x, double& p, double& dp) {
+    double pm = 1.0, pc = x;
+    if (n == 0) { p = 1.0; dp = 0.0; return; }
+    for (int k = 2; k <= n; ++k) {
+        const double pn = ((2 * k - 1) * x * pc - (k - 1) * pm) / k;
+        pm = pc; pc = pn;
+    }
+    p = pc;
+    dp = n * (x * pc - pm) / (x * x - 1.0);
+}
+
+// Gauss-Lobatto-Legendre nodes/weights on [0,1], ascending (deal.II QGaussLobatto<1>)
+void gll(int n, std::vector<double>& x, std::vector<double>& w) {
+    x.assign(n, 0.0); w.assign(n, 0.0);
+    const int m = n - 1;
+    for (int i = 0; i < n; ++i) {
+        double z = -std::cos(M_PI * i / m);
+        if (i > 0 && i < m) {
+            for (int it = 0; it < 64; ++it) {
+                double p, dp; legendre_pd(m, z, p, dp);
+                const double d2p = (2.0 * z * dp - m * (m + 1.0) * p) / (1.0 - z * z);
+                const double dz = dp / d2p;
+                z -= dz;
+                if (std::fabs(dz) < 1e-17) break;
+            }
+        }
+        double p, dp; legendre_pd(m, z, p, dp);
+        x[i] = 0.5 * (z + 1.0);
+        w[i] = 1.0 / (m * (m + 1.0) * p * p);
+    }
+    x[0] = 0.0; x[m] = 1.0;
+}
+
+// Gauss-Legendre nodes/weights on [0,1], ascending (deal.II QGauss<1>)
+void gauss(int n, std::vector<double>& x, std::vector<double>& w) {
+    x.assign(n, 0.0); w.assign(n, 0.0);
+    for (int i = 0; i < n; ++i) {
+        double z = -std::cos(M_PI * (i + 0.75) / (n + 0.5));
+        for (int it = 0; it < 64; ++it) {
+            double p, dp; legendre_pd(n, z, p, dp);
+            const double dz = p / dp;
+            z -= dz;
+            if (std::fabs(dz) < 1e-17) break;
+        }
+        double p, dp; legendre_pd(n, z, p, dp);
+        x[i] = 0.5 * (z + 1.0);
+        w[i] = 1.0 / ((1.0 - z * z) * dp * dp);
+    }
+}
+
+// Lagrange basis on `nodes` at x: values and derivatives (product rule, exact at nodes)
+void lagrange(const std::vector<double>& nodes, double x, double* v, double* dv) {
+    const int n = (int)nodes.size();
+    for (int j = 0; j < n; ++j) {
+        double val = 1.0, der = 0.0;
+        for (int m = 0; m < n; ++m) {
+            if (m == j) continue;
+            const double r = 1.0 / (nodes[j] - nodes[m]);
+            der = der * (x - nodes[m]) * r + val * r;
+            val *= (x - nodes[m]) * r;
+        }
+        v[j] = val; dv[j] = der;
+    }
+}
+
+std::vector<double> mat_mul(const std::vector<double>& A, const std::vector<double>& B, int n) {
+    std::vector<double> C(n * n, 0.0);
+    for (int i = 0; i < n; ++i) for (int k = 0; k < n; ++k) for (int j = 0; j < n; ++j) C[i * n + j] += A[i * n + k] * B[k * n + j];
+    return C;
+}
+
+bool mat_inv(std::vector<double> A, int n, std::vector<double>& Ai) {
+    Ai.assign(n * n, 0.0);
+    for (int i = 0; i < n; ++i) Ai[i * n + i] = 1.0;
+    for (int c = 0; c < n; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < n; ++r) if (std::fabs(A[r * n + c]) > std::fabs(A[piv * n + c])) piv = r;
+        if (A[piv * n + c] == 0.0) return false;
+        for (int j = 0; j < n; ++j) { std::swap(A[c * n + j], A[piv * n + j]); std::swap(Ai[c * n + j], Ai[piv * n + j]); }
+        const double inv = 1.0 / A[c * n + c];
+        for (int j = 0; j < n; ++j) { A[c * n + j] *= inv; Ai[c * n + j] *= inv; }
+        for (int r = 0; r < n; ++r) if (r != c && A[r * n + c] != 0.0) {
+            const double f = A[r * n + c];
+            for (int j = 0; j < n; ++j) { A[r * n + j] -= f * A[c * n + j]; Ai[r * n + j] -= f * Ai[c * n + j]; }
+        }
+    }
+    return true;
+}
+
+double fact(int k) { double f = 1.0; for (int i = 2; i <= k; ++i) f *= i; return f; }
+
+// FR correction parameter for the reference element [0,1]
+// (local_Flux_Reconstruction_operator::get_FR_correction_parameter, operators.cpp:1559-1661)
+int fr_parameter(int type, int p, double user, double& c) {
+    const double pf = fact(p), cp = fact(2 * p) / (pf * pf);
+    switch (type) {
+    case 0: c = 0.0; return 0;                                                                          // cDG
+    case 1: c = 2.0 * p / ((p + 1.0) * ((2.0 * p + 1.0) * std::pow(pf * cp, 2))) / 2.0; return 0;     // cSD
+    case 2: case 7: c = 2.0 * (p + 1) / (p * ((2.0 * p + 1.0) * std::pow(pf * cp, 2))) / 2.0; return 0; // cHU
+    case 3: c = -2.0 / ((2.0 * p + 1.0) * std::pow(pf * cp, 2)) / 2.0; return 0;                        // cNegative
+    case 4: c = -2.0 / ((2.0 * p + 1.0) * std::pow(pf * cp, 2)) / 2.0 / 2.0; return 0;                  // cNegative2
+    case 5: {                                                                                            // cPlus
+        static const double tab[6] = {0, 0, 0.186, 3.67e-3, 4.79e-5, 4.24e-7};
+        if (p < 2 || p > 5) return 1;
+        c = tab[p] / 2.0 / std::pow(std::pow(2.0, p), 2);
+        return 0;
+    }
+    case 6: c = 10000.0; return 0;                                                                     // c10Thousand
+    case 8: c = user / 2.0 / std::pow(std::pow(2.0, p), 2); return 0;                                  // user value
+    }
+    return 1;
+}
+
+// deal.II active-cell order of the periodic cube: recursive children (child = x+2y+4z)
+// for hyper_cube + refine_global, lexicographic for subdivided_hyper_cube
+// (straight_periodic_cube.cpp:38-67).
+void cell_order(int n, int order, std::vector<int>& ijk) {
+    const int nc = n * n * n;
+    ijk.assign(3 * nc, 0);
+    const bool pow2 = n > 0 && (n & (n - 1)) == 0;
+    const bool morton = (order == 2) || (order == 0 && pow2);
+    int levels = 0;
+    while ((1 << levels) < n) ++levels;
+    for (int c = 0; c < nc; ++c) {
+        int ix, iy, iz;
+        if (morton) {
+            ix = iy = iz = 0;
+            for (int l = 0; l < levels; ++l) {
+                const int ch = (c >> (3 * (levels - 1 - l))) & 7;
+                ix = 2 * ix + (ch & 1); iy = 2 * iy + ((ch >> 1) & 1); iz = 2 * iz + ((ch >> 2) & 1);
+            }
+        } else {
+            ix = c % n; iy = (c / n) % n; iz = c / (n * n);
+        }
+        ijk[3 * c] = ix; ijk[3 * c + 1] = iy; ijk[3 * c + 2] = iz;
+    }
+}
+
+} // namespace
+
+struct ph_ctx {
+    ph_params prm{};
+    int n = 0, nc = 0, p = 0, N1 = 0, NP = 0;
+    double left = 0, right = 1, h = 1;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    bool visc = false, split = false, fp32 = false, fr = false;
+    size_t ndofs = 0;
+    std::vector<int> ijk;
+    int* d_nbr = nullptr;
+    ph::OpTab h_ops{};
+    ph::OpTab* d_ops = nullptr;
+    ph::IntegralTab* d_itab = nullptr;
+    double *d_sol = nullptr, *d_stA = nullptr, *d_stB = nullptr, *d_acc = nullptr, *d_carry = nullptr;
+    double *d_q = nullptr, *d_comp = nullptr, *d_tmpA = nullptr, *d_tmpB = nullptr, *d_partial = nullptr;
+    unsigned* d_status = nullptr;
+    ph::PhysConst pc{};
+    double pen = 0.0;
+    int ns = 0;
+    double A[4][4] = {{0}}, b[4] = {0};
+    std::vector<double> h_partial;
+};
+
+namespace {
+
+int dispatch_stage(ph_ctx* c, const ph::StageArgs& a) {
+    cudaError_t e;
+    switch (c->N1) {
+    case 2: e = ph::launch_stage<2>(a, c->fp32, c->visc, c->split, c->stream); break;
+    case 3: e = ph::launch_stage<3>(a, c->fp32, c->visc, c->split, c->stream); break;
+    case 4: e = ph::launch_stage<4>(a, c->fp32, c->visc, c->split, c->stream); break;
+    case 5: e = ph::launch_stage<5>(a, c->fp32, c->visc, c->split, c->stream); break;
+    case 6: e = ph::launch_stage<6>(a, c->fp32, c->visc, c->split, c->stream); break;
+    case 7: e = ph::launch_stage<7>(a, c->fp32, c->visc, c->split, c->stream); break;
+    default: return fail(PH_ERR_UNSUPPORTED, "polynomial degree outside 1..6");
+    }
+    if (e != cudaSuccess) return fail(PH_ERR_CUDA, std::string("residual launch: ") + cudaGetErrorString(e));
+    return PH_OK;
+}
+
+int dispatch_aux(ph_ctx* c, const double* U) {
+    cudaError_t e;
+    const double inv_h = 1.0 / c->h;
+    switch (c->N1) {
+    case 2: e = ph::launch_aux<2>(U, c->d_nbr, c->d_ops, c->nc, inv_h, c->d_q, c->stream); break;
+    case 3: e = ph::launch_aux<3>(U, c->d_nbr, c->d_ops, c->nc, inv_h, c->d_q, c->stream); break;
+    case 4: e = ph::launch_aux<4>(U, c->d_nbr, c->d_ops, c->nc, inv_h, c->d_q, c->stream); break;
+    case 5: e = ph::launch_aux<5>(U, c->d_nbr, c->d_ops, c->nc, inv_h, c->d_q, c->stream); break;
+    case 6: e = ph::launch_aux<6>(U, c->d_nbr, c->d_ops, c->nc, inv_h, c->d_q, c->stream); break;
+    case 7: e = ph::launch_aux<7>(U, c->d_nbr, c->d_ops, c->nc, inv_h, c->d_q, c->stream); break;
+    default: return fail(PH_ERR_UNSUPPORTED, "polynomial degree outside 1..6");
+    }
+    if (e != cudaSuccess) return fail(PH_ERR_CUDA, std::string("aux launch: ") + cudaGetErrorString(e));
+    return PH_OK;
+}
+
+ph::StageArgs base_args(ph_ctx* c, const double* U) {
+    ph::StageArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.U = U; a.Q = c->d_q; a.nbr = c->d_nbr; a.ops = c->d_ops; a.nc = c->nc;
+    a.h = c->h; a.inv_h = 1.0 / c->h; a.pen = c->pen; a.pc = c->pc; a.status = c->d_status;
+    a.fr = c->fr ? 1 : 0;
+    return a;
+}
+
+template <typename T>
+int dalloc(T** p, size_t count) {
+    if (cudaMalloc((void**)p, count * sizeof(T)) != cudaSuccess) { *p = nullptr; return 1; }
+    return 0;
+}
+
+} // namespace
+
+extern "C" {
+
+const char* ph_last_error(void) { return g_err.c_str(); }
+
+int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_stream, ph_ctx** out) {
+    if (!mesh || !prm || !out) return fail(PH_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (prm->flux_nodes_type != 1 || prm->overintegration != 0)
+        return fail(PH_ERR_UNSUPPORTED, "the GPU path is collocated: flux_nodes_type = GLL and overintegration = 0");
+    if (prm->poly_degree < 1 || prm->poly_degree > 6) return fail(PH_ERR_UNSUPPORTED, "poly_degree must be 1..6");
+    if (prm->flux_reconstruction_aux != 0) return fail(PH_ERR_UNSUPPORTED, "flux_reconstruction_aux must be kDG");
+    if (mesh->n_cells_per_direction < 1 || !(mesh->right > mesh->left)) return fail(PH_ERR_INVALID, "bad mesh");
+    if (prm->pde_type < 0 || prm->pde_type > 1 || prm->two_point_num_flux_type < 0 || prm->two_point_num_flux_type > 3 ||
+        prm->conv_num_flux < 0 || prm->conv_num_flux > 5 || prm->diss_num_flux < 0 || prm->diss_num_flux > 2 ||
+        prm->runge_kutta_method < 0 || prm->runge_kutta_method > 2)
+        return fail(PH_ERR_INVALID, "parameter out of range");
+    const bool ec = prm->conv_num_flux >= 3;
+    if (ec && !prm->use_split_form)
+        return fail(PH_ERR_INVALID, "two point flux and not using split form are not compatible");   // numerical_flux_factory.cpp
+    ph_ctx* c = new ph_ctx();
+    c->prm = *prm;
+    c->n = mesh->n_cells_per_direction;
+    c->nc = c->n * c->n * c->n;
+    c->p = prm->poly_degree;
+    c->N1 = c->p + 1;
+    c->NP = c->N1 * c->N1 * c->N1;
+    c->left = mesh->left; c->right = mesh->right;
+    c->h = (mesh->right - mesh->left) / c->n;
+    c->stream = (cudaStream_t)cuda_stream;
+    c->visc = prm->pde_type == 1;
+    c->split = prm->use_split_form != 0;
+    c->fp32 = prm->precision == PH_FP32_RESIDUAL;
+    c->ndofs = (size_t)c->nc * 5 * c->NP;
+    cudaGetDevice(&c->device);
+
+    // ---- 1-D operators on the GLL nodes
+    const int N1 = c->N1;
+    std::vector<double> x, w;
+    gll(N1, x, w);
+    std::vector<double> D(N1 * N1), v(N1), dv(N1);
+    for (int a = 0; a < N1; ++a) {
+        lagrange(x, x[a], v.data(), dv.data());
+        for (int l = 0; l < N1; ++l) D[a * N1 + l] = dv[l];
+    }
+    double cfr = 0.0;
+    if (fr_parameter(prm->flux_reconstruction, c->p, prm->FR_user_specified_correction_parameter_value, cfr)) {
+        delete c;
+        return fail(PH_ERR_UNSUPPORTED, "flux_reconstruction type not defined for this degree");
+    }
+    std::vector<double> Dp(N1 * N1, 0.0);
+    for (int i = 0; i < N1; ++i) Dp[i * N1 + i] = 1.0;
+    for (int k = 0; k < c->p; ++k) Dp = mat_mul(D, Dp, N1);
+    std::vector<double> MK(N1 * N1, 0.0);
+    for (int i = 0; i < N1; ++i)
+        for (int j = 0; j < N1; ++j) {
+            double kij = 0.0;
+            for (int q = 0; q < N1; ++q) kij += Dp[q * N1 + i] * w[q] * Dp[q * N1 + j];
+            MK[i * N1 + j] = (i == j ? w[i] : 0.0) + cfr * kij;
+        }
+    std::vector<double> Minv;
+    if (!mat_inv(MK, N1, Minv)) { delete c; return fail(PH_ERR_INVALID, "singular FR mass matrix"); }
+    c->fr = (cfr != 0.0);
+    std::memset(&c->h_ops, 0, sizeof(c->h_ops));
+    for (int a = 0; a < N1; ++a) {
+        c->h_ops.w[a] = w[a];
+        for (int l = 0; l < N1; ++l) {
+            c->h_ops.D[a * ph::MAXN1 + l] = D[a * N1 + l];
+            c->h_ops.Dsk[a * ph::MAXN1 + l] = (w[a] * D[a * N1 + l] - w[l] * D[l * N1 + a]) / w[a];
+            c->h_ops.Minv[a * ph::MAXN1 + l] = Minv[a * N1 + l];
+            c->h_ops.B[a * ph::MAXN1 + l] = Minv[a * N1 + l] * w[l];
+        }
+    }
+    // over-integration tables for the TGV integrals: QGauss(p + 11)
+    ph::IntegralTab itab;
+    std::memset(&itab, 0, sizeof(itab));
+    {
+        const int ne = c->p + 11;
+        std::vector<double> xe, we;
+        gauss(ne, xe, we);
+        for (int q = 0; q < ne; ++q) {
+            lagrange(x, xe[q], v.data(), dv.data());
+            for (int a = 0; a < N1; ++a) { itab.B[q * N1 + a] = v[a]; itab.dB[q * N1 + a] = dv[a]; }
+            itab.w[q] = we[q];
+        }
+    }
+
+    // ---- physics constants
+    ph::PhysConst& pc = c->pc;
+    pc.gam = prm->gamma_gas; pc.gm1 = prm->gamma_gas - 1.0;
+    pc.mach2 = prm->mach_infinity * prm->mach_infinity;
+    pc.temp_ratio = 110.4 / prm->temperature_inf;
+    pc.inv_re = 1.0 / prm->reynolds_number_inf;
+    pc.prandtl = prm->prandtl_number;
+    pc.const_visc = prm->nondimensionalized_constant_viscosity;
+    pc.use_const_visc = prm->use_constant_viscosity;
+    pc.two_point = prm->two_point_num_flux_type;
+    pc.conv_flux = prm->conv_num_flux;
+    pc.diss_flux = prm->diss_num_flux;
+    pc.navier_stokes = c->visc;
+    double sipg = prm->sipg_penalty_factor;
+    if (prm->diss_num_flux == 1) sipg = 0.0;   // all_parameters.cpp:611-614
+    pc.sipg_pen = sipg;
+    // SIPG penalty (dg_base.cpp:397-413), averaged over both (identical) cells
+    c->pen = (double)c->p * (c->p + 1) / c->h * sipg;
+
+    // ---- Butcher tableau (runge_kutta_methods.cpp:7-47)
+    if (prm->runge_kutta_method == 2) {
+        c->ns = 4; c->A[1][0] = 0.5; c->A[2][1] = 0.5; c->A[3][2] = 1.0;
+        c->b[0] = 1.0 / 6.0; c->b[1] = 1.0 / 3.0; c->b[2] = 1.0 / 3.0; c->b[3] = 1.0 / 6.0;
+    } else if (prm->runge_kutta_method == 1) {
+        c->ns = 3; c->A[1][0] = 1.0; c->A[2][0] = 0.25; c->A[2][1] = 0.25;
+        c->b[0] = 1.0 / 6.0; c->b[1] = 1.0 / 6.0; c->b[2] = 2.0 / 3.0;
+    } else {
+        c->ns = 1; c->b[0] = 1.0;
+    }
+
+    // ---- connectivity
+    cell_order(c->n, mesh->cell_order, c->ijk);
+    std::vector<int> lex2cell(c->nc), nbr(6 * c->nc);
+    const int n = c->n;
+    for (int cc = 0; cc < c->nc; ++cc) lex2cell[(c->ijk[3 * cc + 2] * n + c->ijk[3 * cc + 1]) * n + c->ijk[3 * cc]] = cc;
+    for (int cc = 0; cc < c->nc; ++cc)
+        for (int f = 0; f < 6; ++f) {
+            int t[3] = {c->ijk[3 * cc], c->ijk[3 * cc + 1], c->ijk[3 * cc + 2]};
+            const int d = f / 2;
+            t[d] = (t[d] + ((f & 1) ? 1 : -1) + n) % n;
+            nbr[6 * cc + f] = lex2cell[(t[2] * n + t[1]) * n + t[0]];
+        }
+
+    // ---- device buffers
+    const size_t N = c->ndofs;
+    int bad = 0;
+    bad |= dalloc(&c->d_nbr, nbr.size());
+    bad |= dalloc(&c->d_ops, 1);
+    bad |= dalloc(&c->d_itab, 1);
+    bad |= dalloc(&c->d_sol, N);
+    bad |= dalloc(&c->d_stA, N);
+    bad |= dalloc(&c->d_stB, N);
+    bad |= dalloc(&c->d_acc, N);
+    if (c->ns == 3) bad |= dalloc(&c->d_carry, N);
+    if (c->visc) bad |= dalloc(&c->d_q, 3 * N);
+    if (c->fp32) bad |= dalloc(&c->d_comp, N);
+    bad |= dalloc(&c->d_partial, 3 * (size_t)c->nc);
+    bad |= dalloc(&c->d_status, 1);
+    if (bad) { ph_ctx_destroy(c); return fail(PH_ERR_NOMEM, "device allocation failed"); }
+    cudaError_t e = cudaSuccess;
+    e = cudaMemcpy(c->d_nbr, nbr.data(), nbr.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(c->d_ops, &c->h_ops, sizeof(ph::OpTab), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(c->d_itab, &itab, sizeof(ph::IntegralTab), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(c->d_status, 0, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemset(c->d_sol, 0, N * sizeof(double));
+    if (e == cudaSuccess && c->d_comp) e = cudaMemset(c->d_comp, 0, N * sizeof(double));
+    if (e != cudaSuccess) { ph_ctx_destroy(c); return fail(PH_ERR_CUDA, cudaGetErrorString(e)); }
+    c->h_partial.resize(3 * (size_t)c->nc);
+    *out = c;
+    return PH_OK;
+}
+
+int ph_ctx_destroy(ph_ctx* c) {
+    if (!c) return PH_OK;
+    void* ptrs[] = {c->d_nbr, c->d_ops, c->d_itab, c->d_sol, c->d_stA, c->d_stB, c->d_acc, c->d_carry,
+                    c->d_q, c->d_comp, c->d_tmpA, c->d_tmpB, c->d_partial, c->d_status};
+    for (void* p : ptrs) if (p) cudaFree(p);
+    delete c;
+    return PH_OK;
+}
+
+int64_t ph_ndofs(const ph_ctx* c) { return c ? (int64_t)c->ndofs : -1; }
+
+int ph_cell_ijk(const ph_ctx* c, int32_t* ijk) {
+    if (!c || !ijk) return fail(PH_ERR_INVALID, "null argument");
+    std::memcpy(ijk, c->ijk.data(), c->ijk.size() * sizeof(int32_t));
+    return PH_OK;
+}
+
+int ph_set_state(ph_ctx* c, const double* U, int where) {
+    if (!c || !U) return fail(PH_ERR_INVALID, "null argument");
+    PH_CUDA(cudaMemcpyAsync(c->d_sol, U, c->ndofs * sizeof(double),
+                            where == PH_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, c->stream));
+    if (c->d_comp) PH_CUDA(cudaMemsetAsync(c->d_comp, 0, c->ndofs * sizeof(double), c->stream));
+    if (where == PH_HOST) PH_CUDA(cudaStreamSynchronize(c->stream));
+    return PH_OK;
+}
+
+int ph_get_state(ph_ctx* c, double* U, int where) {
+    if (!c || !U) return fail(PH_ERR_INVALID, "null argument");
+    PH_CUDA(cudaMemcpyAsync(U, c->d_sol, c->ndofs * sizeof(double),
+                            where == PH_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, c->stream));
+    if (where == PH_HOST) PH_CUDA(cudaStreamSynchronize(c->stream));
+    return PH_OK;
+}
+
+static int ensure_tmp(ph_ctx* c) {
+    if (!c->d_tmpA && dalloc(&c->d_tmpA, c->ndofs)) return fail(PH_ERR_NOMEM, "device allocation failed");
+    if (!c->d_tmpB && dalloc(&c->d_tmpB, c->ndofs)) return fail(PH_ERR_NOMEM, "device allocation failed");
+    return PH_OK;
+}
+
+int ph_residual(ph_ctx* c, const double* U, double* R, int where) {
+    if (!c || !U || !R) return fail(PH_ERR_INVALID, "null argument");
+    const double* dU = U;
+    double* dR = R;
+    if (where == PH_HOST) {
+        if (int rc = ensure_tmp(c)) return rc;
+        PH_CUDA(cudaMemcpyAsync(c->d_tmpA, U, c->ndofs * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        dU = c->d_tmpA; dR = c->d_tmpB;
+    }
+    if (c->visc) if (int rc = dispatch_aux(c, dU)) return rc;
+    ph::StageArgs a = base_args(c, dU);
+    a.mode = 0; a.out = dR;
+    if (int rc = dispatch_stage(c, a)) return rc;
+    if (where == PH_HOST) {
+        PH_CUDA(cudaMemcpyAsync(R, dR, c->ndofs * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        PH_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    return PH_OK;
+}
+
+int ph_apply_inverse_mass(ph_ctx* c, const double* R, double* out, int where) {
+    if (!c || !R || !out) return fail(PH_ERR_INVALID, "null argument");
+    const double* dR = R;
+    double* dO = out;
+    if (where == PH_HOST) {
+        if (int rc = ensure_tmp(c)) return rc;
+        PH_CUDA(cudaMemcpyAsync(c->d_tmpA, R, c->ndofs * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        dR = c->d_tmpA; dO = c->d_tmpB;
+    }
+    const double inv_detj = 1.0 / (c->h * c->h * c->h);
+    cudaError_t e;
+    switch (c->N1) {
+    case 2: e = ph::launch_inverse_mass<2>(dR, dO, c->d_ops, c->nc, inv_detj, c->stream); break;
+    case 3: e = ph::launch_inverse_mass<3>(dR, dO, c->d_ops, c->nc, inv_detj, c->stream); break;
+    case 4: e = ph::launch_inverse_mass<4>(dR, dO, c->d_ops, c->nc, inv_detj, c->stream); break;
+    case 5: e = ph::launch_inverse_mass<5>(dR, dO, c->d_ops, c->nc, inv_detj, c->stream); break;
+    case 6: e = ph::launch_inverse_mass<6>(dR, dO, c->d_ops, c->nc, inv_detj, c->stream); break;
+    case 7: e = ph::launch_inverse_mass<7>(dR, dO, c->d_ops, c->nc, inv_detj, c->stream); break;
+    default: return fail(PH_ERR_UNSUPPORTED, "polynomial degree");
+    }
+    if (e != cudaSuccess) return fail(PH_ERR_CUDA, cudaGetErrorString(e));
+    if (where == PH_HOST) {
+        PH_CUDA(cudaMemcpyAsync(out, dO, c->ndofs * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        PH_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    return PH_OK;
+}
+
+// One explicit Butcher step (RungeKuttaBase::step_in_time, runge_kutta_base.cpp:21-39):
+// stage i reads its stage state, computes k_i = M^{-1} R and, in the same kernel,
+// updates the running sum and writes the next stage state.
+static int rk_one_step(ph_ctx* c, double dt) {
+    const int ns = c->ns;
+    for (int i = 0; i < ns; ++i) {
+        const double* in = (i == 0) ? c->d_sol : ((i - 1) % 2 == 0 ? c->d_stA : c->d_stB);
+        if (c->visc) if (int rc = dispatch_aux(c, in)) return rc;
+        ph::StageArgs a = base_args(c, in);
+        a.mode = 2;
+        a.dt = dt;
+        a.Un = c->d_sol;
+        a.inc_mode = c->fp32 ? 1 : 0;
+        a.acc_in = (i == 0) ? nullptr : c->d_acc;
+        a.c_acc = dt * c->b[i];
+        const bool last = (i == ns - 1);
+        if (!last) {
+            a.acc_out = c->d_acc;
+            a.next = (i % 2 == 0) ? c->d_stA : c->d_stB;
+            a.a_next = c->A[i + 1][i];
+            if (c->d_carry && i >= 1 && c->A[i + 1][i - 1] != 0.0) a.carry_in = c->d_carry;
+            if (c->d_carry && i + 2 < ns && c->A[i + 2][i] != 0.0) { a.carry_out = c->d_carry; a.a_carry = c->A[i + 2][i]; }
+        } else {
+            // the stage input is read by neighbouring CTAs, so a one-stage method writes elsewhere
+            a.final_out = (ns == 1) ? c->d_stA : c->d_sol;
+            a.comp = c->d_comp;
+        }
+        if (int rc = dispatch_stage(c, a)) return rc;
+    }
+    if (ns == 1) std::swap(c->d_sol, c->d_stA);
+    return PH_OK;
+}
+
+int ph_rk_step(ph_ctx* c, double dt, int nsteps) {
+    if (!c || nsteps < 0) return fail(PH_ERR_INVALID, "bad argument");
+    for (int s = 0; s < nsteps; ++s)
+        if (int rc = rk_one_step(c, dt)) return rc;
+    return PH_OK;
+}
+
+int ph_integrals(ph_ctx* c, double out[4]) {
+    if (!c || !out) return fail(PH_ERR_INVALID, "null argument");
+    cudaError_t e;
+    const double gam = c->prm.gamma_gas, gm1 = gam - 1.0;
+    switch (c->N1) {
+    case 2: e = ph::launch_integrals<2>(c->d_sol, c->d_itab, c->nc, c->h, gam, gm1, c->d_partial, c->stream); break;
+    case 3: e = ph::launch_integrals<3>(c->d_sol, c->d_itab, c->nc, c->h, gam, gm1, c->d_partial, c->stream); break;
+    case 4: e = ph::launch_integrals<4>(c->d_sol, c->d_itab, c->nc, c->h, gam, gm1, c->d_partial, c->stream); break;
+    case 5: e = ph::launch_integrals<5>(c->d_sol, c->d_itab, c->nc, c->h, gam, gm1, c->d_partial, c->stream); break;
+    case 6: e = ph::launch_integrals<6>(c->d_sol, c->d_itab, c->nc, c->h, gam, gm1, c->d_partial, c->stream); break;
+    case 7: e = ph::launch_integrals<7>(c->d_sol, c->d_itab, c->nc, c->h, gam, gm1, c->d_partial, c->stream); break;
+    default: return fail(PH_ERR_UNSUPPORTED, "polynomial degree");
+    }
+    if (e != cudaSuccess) return fail(PH_ERR_CUDA, cudaGetErrorString(e));
+    PH_CUDA(cudaMemcpyAsync(c->h_partial.data(), c->d_partial, 3 * (size_t)c->nc * sizeof(double),
+                            cudaMemcpyDeviceToHost, c->stream));
+    PH_CUDA(cudaStreamSynchronize(c->stream));
+    double ke = 0.0, ens = 0.0, wave = 0.0;
+    for (int i = 0; i < c->nc; ++i) {
+        ke += c->h_partial[3 * i]; ens += c->h_partial[3 * i + 1];
+        wave = std::max(wave, c->h_partial[3 * i + 2]);
+    }
+    const double vol = std::pow(c->right - c->left, 3);
+    out[0] = ke / vol;
+    out[1] = ens / vol;
+    out[2] = 2.0 * out[1] / c->prm.reynolds_number_inf;
+    out[3] = wave;
+    return PH_OK;
+}
+
+int ph_status(ph_ctx* c, uint32_t* flags) {
+    if (!c || !flags) return fail(PH_ERR_INVALID, "null argument");
+    unsigned v = 0;
+    PH_CUDA(cudaMemcpyAsync(&v, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+    PH_CUDA(cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->stream));
+    PH_CUDA(cudaStreamSynchronize(c->stream));
+    *flags = v;
+    return PH_OK;
+}
+
+int ph_sync(ph_ctx* c) {
+    if (!c) return fail(PH_ERR_INVALID, "null argument");
+    PH_CUDA(cudaStreamSynchronize(c->stream));
+    return PH_OK;
+}
+
+}  // extern "C"

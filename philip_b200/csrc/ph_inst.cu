@@ -1,0 +1,108 @@
+// Explicit instantiation of the kernels for one polynomial order. Compiled once per
+// N1 (= p + 1) with -DPH_N1=<N1>.
+#include "ph_launch.cuh"
+
+#ifndef PH_N1
+#error "PH_N1 must be defined"
+#endif
+
+namespace ph {
+
+template <int N1> constexpr int cells_per_cta() { return N1 == 2 ? 16 : N1 == 3 ? 4 : N1 == 4 ? 2 : 1; }
+
+template <typename R, int N1, bool VISC, bool SPLIT>
+static cudaError_t launch_one(const StageArgs& a, cudaStream_t s) {
+    constexpr int CPC = cells_per_cta<N1>();
+    using L = Layout<R, N1, CPC, VISC, SPLIT>;
+    auto kern = residual_kernel<R, N1, CPC, VISC, SPLIT>;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static bool configured[64] = {false};
+    if (dev < 64 && !configured[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::bytes);
+        if (e != cudaSuccess) return e;
+        configured[dev] = true;
+    }
+    const int grid = (a.nc + CPC - 1) / CPC;
+    kern<<<grid, L::NT, L::bytes, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int N1>
+cudaError_t launch_stage(const StageArgs& a, int fp32, bool visc, bool split, cudaStream_t s) {
+    if (fp32) {
+        if (visc) return split ? launch_one<float, N1, true, true>(a, s) : launch_one<float, N1, true, false>(a, s);
+        return split ? launch_one<float, N1, false, true>(a, s) : launch_one<float, N1, false, false>(a, s);
+    }
+    if (visc) return split ? launch_one<double, N1, true, true>(a, s) : launch_one<double, N1, true, false>(a, s);
+    return split ? launch_one<double, N1, false, true>(a, s) : launch_one<double, N1, false, false>(a, s);
+}
+
+template <typename R, int N1, bool VISC, bool SPLIT>
+static void shape_one(int* threads, int* cpc, size_t* smem) {
+    constexpr int CPC = cells_per_cta<N1>();
+    using L = Layout<R, N1, CPC, VISC, SPLIT>;
+    *threads = L::NT; *cpc = CPC; *smem = L::bytes;
+}
+
+template <int N1>
+void stage_launch_shape(int fp32, bool visc, bool split, int* threads, int* cpc, size_t* smem) {
+    if (fp32) {
+        if (visc) split ? shape_one<float, N1, true, true>(threads, cpc, smem) : shape_one<float, N1, true, false>(threads, cpc, smem);
+        else split ? shape_one<float, N1, false, true>(threads, cpc, smem) : shape_one<float, N1, false, false>(threads, cpc, smem);
+    } else {
+        if (visc) split ? shape_one<double, N1, true, true>(threads, cpc, smem) : shape_one<double, N1, true, false>(threads, cpc, smem);
+        else split ? shape_one<double, N1, false, true>(threads, cpc, smem) : shape_one<double, N1, false, false>(threads, cpc, smem);
+    }
+}
+
+template <int N1>
+cudaError_t launch_aux(const double* U, const int* nbr, const OpTab* ops, int nc, double inv_h, double* Q,
+                       cudaStream_t s) {
+    constexpr int CPC = cells_per_cta<N1>();
+    using L = AuxLayout<N1, CPC>;
+    auto kern = aux_kernel<N1, CPC>;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static bool configured[64] = {false};
+    if (dev < 64 && !configured[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::bytes);
+        if (e != cudaSuccess) return e;
+        configured[dev] = true;
+    }
+    kern<<<(nc + CPC - 1) / CPC, L::NT, L::bytes, s>>>(U, nbr, ops, nc, inv_h, Q);
+    return cudaGetLastError();
+}
+
+template <int N1>
+cudaError_t launch_inverse_mass(const double* in, double* out, const OpTab* ops, int nc, double inv_detj,
+                                cudaStream_t s) {
+    inverse_mass_kernel<N1><<<nc, 128, 0, s>>>(in, out, ops, nc, inv_detj);
+    return cudaGetLastError();
+}
+
+template <int N1>
+cudaError_t launch_integrals(const double* U, const IntegralTab* tab, int nc, double h, double gam, double gm1,
+                             double* partial, cudaStream_t s) {
+    auto kern = integrals_kernel<N1>;
+    constexpr size_t bytes = integrals_smem_bytes<N1>();
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static bool configured[64] = {false};
+    if (dev < 64 && !configured[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (e != cudaSuccess) return e;
+        configured[dev] = true;
+    }
+    kern<<<nc, 256, bytes, s>>>(U, tab, nc, h, gam, gm1, partial);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_stage<PH_N1>(const StageArgs&, int, bool, bool, cudaStream_t);
+template void stage_launch_shape<PH_N1>(int, bool, bool, int*, int*, size_t*);
+template cudaError_t launch_aux<PH_N1>(const double*, const int*, const OpTab*, int, double, double*, cudaStream_t);
+template cudaError_t launch_inverse_mass<PH_N1>(const double*, double*, const OpTab*, int, double, cudaStream_t);
+template cudaError_t launch_integrals<PH_N1>(const double*, const IntegralTab*, int, double, double, double, double*,
+                                             cudaStream_t);
+
+} // namespace ph

@@ -1,0 +1,580 @@
+// sm_100a kernels of the GLL-collocated strong-form DG/FR residual, the auxiliary
+// (lifted-gradient) equation and the fused Runge-Kutta stage epilogue.
+//
+// Work decomposition. A CTA owns a tile of CPC cells. Every phase is a loop over
+// work items with a fixed owner, so all accumulation happens in a fixed order and
+// repeated runs are bitwise identical (no atomics on data):
+//   1. gather the neighbour face traces (state, and the auxiliary gradient when viscous)
+//   2. per node: FP64 positivity check, node quantities (rho, v, p, logs), viscous flux
+//   3. per face node: numerical flux at the canonical orientation (left cell = int,
+//      normal +e_d), lifted into this cell with the sign of its face
+//   4. per direction: one warp segment of N1 lanes owns one 1-D line; each lane
+//      evaluates the two-point flux with partner (pos+k) mod N1 and hands it to the
+//      partner through a warp shuffle, so each unordered pair is evaluated once
+//   5. per node: mass inverse (diagonal for cDG, B(x)B(x)B for FR) and the RK update
+//
+// Reference structure restated (GLL collocation makes chi = I and the entropy
+// projection the identity, and the hybrid surface-volume terms cancel exactly):
+//   volume split form ............ src/dg/strong_dg.cpp:1235-1543
+//   face term ..................... src/dg/strong_dg.cpp:2367-3576
+//   auxiliary equation ............ src/dg/strong_dg.cpp:498-1008
+//   inverse mass (affine) ......... src/dg/dg_base.cpp:4207-4219
+//   RK stage / sum ................ src/ode_solver/runge_kutta_ode_solver.cpp:15-100
+#pragma once
+#include "ph_physics.cuh"
+
+namespace ph {
+
+constexpr int MAXN1 = 8;
+
+// 1-D operator tables on the GLL nodes (double, row-major [a][l]).
+struct OpTab {
+    double D[MAXN1 * MAXN1];      // D[a][l] = l_l'(x_a)
+    double Dsk[MAXN1 * MAXN1];    // (w_a D[a][l] - w_l D[l][a]) / w_a
+    double B[MAXN1 * MAXN1];      // (M+K)^{-1} diag(w)  (FR mass inverse in G units)
+    double Minv[MAXN1 * MAXN1];   // (M+K)^{-1}
+    double w[MAXN1];              // GLL weights on [0,1]
+};
+
+struct StageArgs {
+    const double* U;          // stage input state [nc][5][NP]
+    const double* Q;          // auxiliary gradient [nc][3][5][NP] (viscous)
+    const int* nbr;           // [nc][6] neighbour cell per face
+    const OpTab* ops;
+    int nc;
+    double h, inv_h;
+    double pen;               // SIPG penalty p(p+1)/h * factor
+    PhysConst pc;
+    unsigned* status;
+    int mode;                 // 0: R (before M^-1), 1: k = M^-1 R, 2: RK stage
+    int fr;                   // apply the FR mass inverse B(x)B(x)B
+    double* out;              // modes 0,1
+    // RK stage epilogue (mode 2), all arrays in the state layout
+    const double* Un;         // u_n
+    const double* acc_in;     // running sum (nullptr on the first stage)
+    double* acc_out;          // acc_in (or base) + c_acc * k
+    double c_acc;
+    int inc_mode;             // acc holds the increment sum (precision form) instead of u_n + sum
+    double* comp;             // Kahan compensation of the final sum (precision form), or nullptr
+    double* final_out;        // last stage: u_{n+1}
+    double* next;             // next stage state: ((carry_in) + a_next k) dt + u_n
+    const double* carry_in;
+    double a_next;
+    double* carry_out;        // a_carry * k for the stage after next
+    double a_carry;
+    double dt;
+};
+
+template <typename R, int N1, int CPC, bool VISC, bool SPLIT>
+struct Layout {
+    static constexpr int NP = N1 * N1 * N1, NF = N1 * N1;
+    static constexpr int NQV = 10;                     // rho v0 v1 v2 p E a b la lb vsq -> packed 11
+    static constexpr int NQS = 11;
+    static constexpr int TR = VISC ? 9 : 5;            // trace values per face node: u (5) [+ ext viscous flux (4)]
+    static constexpr int NX = (VISC ? 12 : 0) + (SPLIT ? 0 : 15);
+    static constexpr int oOps = 0;                      // D, Dsk, B, w as R
+    static constexpr int nOps = 3 * N1 * N1 + N1;
+    static constexpr int oU = (oOps + nOps + 1) & ~1;
+    static constexpr int oD = oU + CPC * 5 * NP;
+    static constexpr int oT = oD + CPC * NQS * NP;
+    static constexpr int oA = oT + CPC * 6 * TR * NF;
+    static constexpr int oX = oA + CPC * 5 * NP;
+    static constexpr int total = oX + CPC * NX * NP;
+    static constexpr size_t bytes = (size_t)total * sizeof(R);
+    static constexpr int SPW = 32 / N1;                // lines per warp
+    static constexpr int WARPS_LINES = (CPC * NF + SPW - 1) / SPW;
+    static constexpr int NT = WARPS_LINES * 32;
+};
+
+template <int N1> __device__ __forceinline__ int node_of(int x, int y, int z) { return (z * N1 + y) * N1 + x; }
+
+// coordinates of face node `fn` of face f at boundary coordinate b
+template <int N1> __device__ __forceinline__ int face_node_volume_index(int f, int fn, int b) {
+    const int dn = f >> 1;
+    int c[3];
+    const int t1 = (dn == 0) ? 1 : 0, t2 = (dn == 2) ? 1 : 2;
+    c[dn] = b; c[t1] = fn % N1; c[t2] = fn / N1;
+    return node_of<N1>(c[0], c[1], c[2]);
+}
+
+template <typename R>
+__device__ __forceinline__ void store_q(R* sD, int NP, int idx, const NodeQ<R>& q) {
+    sD[0 * NP + idx] = q.rho; sD[1 * NP + idx] = q.v[0]; sD[2 * NP + idx] = q.v[1]; sD[3 * NP + idx] = q.v[2];
+    sD[4 * NP + idx] = q.p; sD[5 * NP + idx] = q.E; sD[6 * NP + idx] = q.a; sD[7 * NP + idx] = q.b;
+    sD[8 * NP + idx] = q.la; sD[9 * NP + idx] = q.lb; sD[10 * NP + idx] = q.vsq;
+}
+template <typename R>
+__device__ __forceinline__ void load_q(const R* sD, int NP, int idx, NodeQ<R>& q) {
+    q.rho = sD[0 * NP + idx]; q.v[0] = sD[1 * NP + idx]; q.v[1] = sD[2 * NP + idx]; q.v[2] = sD[3 * NP + idx];
+    q.p = sD[4 * NP + idx]; q.E = sD[5 * NP + idx]; q.a = sD[6 * NP + idx]; q.b = sD[7 * NP + idx];
+    q.la = sD[8 * NP + idx]; q.lb = sD[9 * NP + idx]; q.vsq = sD[10 * NP + idx];
+}
+
+// FP64 positivity check of a stored state (the check stays in FP64 for the precision form).
+__device__ __forceinline__ void check_state_fp64(double u[5], double gm1, unsigned* st) {
+    double v2 = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { const double v = u[1 + d] / u[0]; v2 = v2 + v * v; }
+    const double p = gm1 * (u[4] - 0.5 * u[0] * v2);
+    if (u[0] < 0.0 || p < 0.0) atomicOr(st, ST_NONPHYSICAL);
+}
+
+// One face node of phase 3: the numerical flux at the canonical orientation (the
+// left cell is the interior side, normal +e_D) lifted into this cell with its sign.
+template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int D>
+__device__ __forceinline__ void face_item(const Cst<R>& cst, int tp, int cf, int df, int ucv, const R* sU,
+                                          const R* sD, R* sT, const R* sX, int c, int f, int fn, R pen,
+                                          R inv_wend) {
+    using L = Layout<R, N1, CPC, VISC, SPLIT>;
+    constexpr int NP = L::NP, NF = L::NF, TR = L::TR, NQS = L::NQS;
+    const bool plus = (f & 1);                    // this cell is the left (minus) side
+    const R sgn = plus ? R(1) : R(-1);
+    const int node = face_node_volume_index<N1>(f, fn, plus ? N1 - 1 : 0);
+    R* tr = sT + (c * 6 + f) * TR * NF;
+    R uo[5], ue[5];
+#pragma unroll
+    for (int s = 0; s < 5; ++s) { uo[s] = sU[(c * 5 + s) * NP + node]; ue[s] = tr[s * NF + fn]; }
+    NodeQ<R> qo, qe;
+    load_q<R>(sD + c * NQS * NP, NP, node, qo);
+    node_prepare<R>(ue, tp, cst.gm1, qe, nullptr);
+    R Fs[5];
+    if (plus) conv_num_flux<R, D>(uo, ue, qo, qe, tp, cf, cst, Fs);
+    else conv_num_flux<R, D>(ue, uo, qe, qo, tp, cf, cst, Fs);
+    R term[5];
+#pragma unroll
+    for (int s = 0; s < 5; ++s) term[s] = -sgn * Fs[s];
+    const R* X = sX + c * L::NX * NP;
+    if constexpr (!SPLIT) {
+        constexpr int o = VISC ? 12 : 0;
+#pragma unroll
+        for (int s = 0; s < 5; ++s) term[s] += sgn * X[(o + D * 5 + s) * NP + node];
+    }
+    if constexpr (VISC) {
+        R Fo[4], Fn[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            Fo[k] = X[(D * 4 + k) * NP + node];
+            Fn[k] = R(0.5) * (Fo[k] + tr[(5 + k) * NF + fn]);
+        }
+        if (df == DF_SIPG) {
+            const R* uL = plus ? uo : ue;
+            const R* uR = plus ? ue : uo;
+            R gj[5][3];
+#pragma unroll
+            for (int s = 0; s < 5; ++s)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) gj[s][k] = (k == D) ? (uL[s] - uR[s]) : R(0);
+            R AL[3][4], AR[3][4];
+            viscous_flux<R>(uL, gj, ucv, cst, AL, 1 << D, nullptr);
+            viscous_flux<R>(uR, gj, ucv, cst, AR, 1 << D, nullptr);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) Fn[k] = Fn[k] - pen * (R(0.5) * (AL[D][k] + AR[D][k]));
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) term[1 + k] += sgn * (Fo[k] - Fn[k]);
+    }
+#pragma unroll
+    for (int s = 0; s < 5; ++s) tr[s * NF + fn] = term[s] * inv_wend;
+}
+
+// Phase 4 for direction D: warp segments of N1 lanes own 1-D lines along D.
+template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int D>
+__device__ __forceinline__ void volume_dir(const Cst<R>& cst, int tp, const R* sD, const R* sX, R* sA,
+                                           const R* sOpsD, const R* sOpsDsk, int lc, int lt, int pos, int seg,
+                                           bool lvalid) {
+    using L = Layout<R, N1, CPC, VISC, SPLIT>;
+    constexpr int NP = L::NP, NQS = L::NQS;
+    constexpr int st = (D == 0) ? 1 : (D == 1) ? N1 : N1 * N1;
+    constexpr int t1 = (D == 0) ? 1 : 0, t2 = (D == 2) ? 1 : 2;
+    int cc[3];
+    cc[D] = pos; cc[t1] = lt % N1; cc[t2] = lt / N1;
+    const int node = node_of<N1>(cc[0], cc[1], cc[2]);
+    const int base = node - pos * st;
+    R acc[5] = {R(0), R(0), R(0), R(0), R(0)};
+    if constexpr (SPLIT) {
+        const R* Dq = sD + lc * NQS * NP;
+        NodeQ<R> qi;
+        load_q<R>(Dq, NP, node, qi);
+#ifdef PH_ALL_ORDERED_PAIRS
+#pragma unroll
+        for (int l = 0; l < N1; ++l) {
+            if (l == pos) continue;
+            NodeQ<R> qj;
+            load_q<R>(Dq, NP, base + l * st, qj);
+            R F[5];
+            two_point_dir<R, D>(qi, qj, tp, cst, F);
+            const R cj = sOpsDsk[pos * N1 + l];
+#pragma unroll
+            for (int s = 0; s < 5; ++s) acc[s] += cj * F[s];
+        }
+#else
+        const int segbase = seg * N1;
+#pragma unroll
+        for (int k = 1; k <= N1 / 2; ++k) {
+            const int jp = (pos + k) % N1;
+            NodeQ<R> qj;
+            load_q<R>(Dq, NP, base + jp * st, qj);
+            R F[5];
+            two_point_dir<R, D>(qi, qj, tp, cst, F);
+            const R cj = sOpsDsk[pos * N1 + jp];
+            const int src = segbase + (pos - k + N1) % N1;
+            const R cr = sOpsDsk[pos * N1 + (pos - k + N1) % N1];
+            constexpr bool dup_possible = (N1 & 1) == 0;
+            const bool dup = dup_possible && (2 * k == N1);
+#pragma unroll
+            for (int s = 0; s < 5; ++s) {
+                const R fr = __shfl_sync(0xffffffffu, F[s], src);
+                acc[s] += cj * F[s];
+                if (!dup) acc[s] += cr * fr;
+            }
+        }
+#endif
+    }
+    if constexpr (VISC || !SPLIT) {
+        const R* X = sX + lc * L::NX * NP;
+#pragma unroll
+        for (int l = 0; l < N1; ++l) {
+            const int nl = base + l * st;
+            const R coef = sOpsD[pos * N1 + l];
+            if constexpr (VISC) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) acc[1 + k] += coef * X[(D * 4 + k) * NP + nl];
+            }
+            if constexpr (!SPLIT) {
+                constexpr int o = VISC ? 12 : 0;
+#pragma unroll
+                for (int s = 0; s < 5; ++s) acc[s] += coef * X[(o + D * 5 + s) * NP + nl];
+            }
+        }
+    }
+    if (lvalid) {
+        R* A = sA + lc * 5 * NP;
+#pragma unroll
+        for (int s = 0; s < 5; ++s) {
+            if (D == 0) A[s * NP + node] = acc[s];
+            else A[s * NP + node] += acc[s];
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Residual (+ mass inverse + RK epilogue) kernel
+// ------------------------------------------------------------------------------------
+template <typename R, int N1, int CPC, bool VISC, bool SPLIT>
+__global__ void __launch_bounds__(Layout<R, N1, CPC, VISC, SPLIT>::NT)
+residual_kernel(const StageArgs a) {
+    using L = Layout<R, N1, CPC, VISC, SPLIT>;
+    constexpr int NP = L::NP, NF = L::NF, NT = L::NT, TR = L::TR, NQS = L::NQS;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R* sm = reinterpret_cast<R*>(smem_raw);
+    R* sOpsD = sm + L::oOps;
+    R* sOpsDsk = sOpsD + N1 * N1;
+    R* sOpsB = sOpsDsk + N1 * N1;
+    R* sOpsW = sOpsB + N1 * N1;
+    R* sU = sm + L::oU;
+    R* sD = sm + L::oD;
+    R* sT = sm + L::oT;
+    R* sA = sm + L::oA;
+    R* sX = sm + L::oX;
+
+    Cst<R> cst; cst.load(a.pc);
+    const int tp = a.pc.two_point, cf = a.pc.conv_flux, df = a.pc.diss_flux, ucv = a.pc.use_const_visc;
+    const int tid = threadIdx.x;
+    const int cell0 = blockIdx.x * CPC;
+
+    for (int i = tid; i < N1 * N1; i += NT) {
+        sOpsD[i] = (R)a.ops->D[(i / N1) * MAXN1 + (i % N1)];
+        sOpsDsk[i] = (R)a.ops->Dsk[(i / N1) * MAXN1 + (i % N1)];
+        sOpsB[i] = (R)a.ops->B[(i / N1) * MAXN1 + (i % N1)];
+    }
+    for (int i = tid; i < N1; i += NT) sOpsW[i] = (R)a.ops->w[i];
+
+    // ---- phase 1: neighbour face traces (and the neighbour's viscous flux there)
+    for (int it = tid; it < CPC * 6 * NF; it += NT) {
+        const int fn = it % NF;
+        const int f = (it / NF) % 6;
+        const int c = it / (NF * 6);
+        int cell = cell0 + c; if (cell >= a.nc) cell = a.nc - 1;
+        const int cn = __ldg(&a.nbr[cell * 6 + f]);
+        const int nn = face_node_volume_index<N1>(f, fn, (f & 1) ? 0 : N1 - 1);
+        R* tr = sT + (c * 6 + f) * TR * NF;
+        R ue[5];
+#pragma unroll
+        for (int s = 0; s < 5; ++s) { ue[s] = (R)__ldg(&a.U[((size_t)cn * 5 + s) * NP + nn]); tr[s * NF + fn] = ue[s]; }
+        if constexpr (VISC) {
+            const int d = f >> 1;
+            R ge[5][3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+#pragma unroll
+                for (int s = 0; s < 5; ++s) ge[s][k] = (R)__ldg(&a.Q[(((size_t)cn * 3 + k) * 5 + s) * NP + nn]);
+            R Fe[3][4];
+            viscous_flux<R>(ue, ge, ucv, cst, Fe, 1 << d, nullptr);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) tr[(5 + k) * NF + fn] = Fe[d][k];
+        }
+    }
+
+    // ---- phase 2: node quantities (+ viscous / convective physical fluxes)
+    for (int it = tid; it < CPC * NP; it += NT) {
+        const int c = it / NP, node = it % NP;
+        int cell = cell0 + c;
+        const bool valid = cell < a.nc;
+        if (!valid) cell = a.nc - 1;
+        double ud[5];
+#pragma unroll
+        for (int s = 0; s < 5; ++s) ud[s] = __ldg(&a.U[((size_t)cell * 5 + s) * NP + node]);
+        if (valid) check_state_fp64(ud, a.pc.gm1, a.status);
+        R u[5];
+#pragma unroll
+        for (int s = 0; s < 5; ++s) { u[s] = (R)ud[s]; sU[(c * 5 + s) * NP + node] = u[s]; }
+        NodeQ<R> q;
+        node_prepare<R>(u, tp, cst.gm1, q, nullptr);
+        store_q<R>(sD + c * NQS * NP, NP, node, q);
+        R* X = sX + c * L::NX * NP;
+        if constexpr (VISC) {
+            R g[5][3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+#pragma unroll
+                for (int s = 0; s < 5; ++s) g[s][d] = (R)__ldg(&a.Q[(((size_t)cell * 3 + d) * 5 + s) * NP + node]);
+            R F[3][4];
+            viscous_flux<R>(u, g, ucv, cst, F, 7, nullptr);
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+#pragma unroll
+                for (int k = 0; k < 4; ++k) X[(d * 4 + k) * NP + node] = F[d][k];
+        }
+        if constexpr (!SPLIT) {
+            constexpr int o = VISC ? 12 : 0;
+            R F[5];
+            conv_flux_dir<R, 0>(q, F);
+#pragma unroll
+            for (int s = 0; s < 5; ++s) X[(o + 0 * 5 + s) * NP + node] = F[s];
+            conv_flux_dir<R, 1>(q, F);
+#pragma unroll
+            for (int s = 0; s < 5; ++s) X[(o + 1 * 5 + s) * NP + node] = F[s];
+            conv_flux_dir<R, 2>(q, F);
+#pragma unroll
+            for (int s = 0; s < 5; ++s) X[(o + 2 * 5 + s) * NP + node] = F[s];
+        }
+    }
+    __syncthreads();
+
+    // ---- phase 3: face fluxes (canonical orientation), lifted with 1/w_end
+    {
+        const R inv_wend = R(1) / sOpsW[0];
+        const R pen = (R)a.pen;
+        for (int it = tid; it < CPC * 6 * NF; it += NT) {
+            const int fn = it % NF;
+            const int f = (it / NF) % 6;
+            const int c = it / (NF * 6);
+            switch (f >> 1) {
+            case 0: face_item<R, N1, CPC, VISC, SPLIT, 0>(cst, tp, cf, df, ucv, sU, sD, sT, sX, c, f, fn, pen, inv_wend); break;
+            case 1: face_item<R, N1, CPC, VISC, SPLIT, 1>(cst, tp, cf, df, ucv, sU, sD, sT, sX, c, f, fn, pen, inv_wend); break;
+            default: face_item<R, N1, CPC, VISC, SPLIT, 2>(cst, tp, cf, df, ucv, sU, sD, sT, sX, c, f, fn, pen, inv_wend); break;
+            }
+        }
+    }
+
+    // ---- phase 4: volume terms, one direction at a time
+    {
+        constexpr int SPW = L::SPW;
+        const int warp = tid >> 5, lane = tid & 31;
+        const int seg = lane / N1, pos = lane % N1;
+        const int line = warp * SPW + seg;
+        const bool lvalid = (seg < SPW) && (line < CPC * NF);
+        const int lc = lvalid ? line / NF : 0;
+        const int lt = lvalid ? line % NF : 0;
+        __syncthreads();
+        volume_dir<R, N1, CPC, VISC, SPLIT, 0>(cst, tp, sD, sX, sA, sOpsD, sOpsDsk, lc, lt, pos, seg, lvalid);
+        __syncthreads();
+        volume_dir<R, N1, CPC, VISC, SPLIT, 1>(cst, tp, sD, sX, sA, sOpsD, sOpsDsk, lc, lt, pos, seg, lvalid);
+        __syncthreads();
+        volume_dir<R, N1, CPC, VISC, SPLIT, 2>(cst, tp, sD, sX, sA, sOpsD, sOpsDsk, lc, lt, pos, seg, lvalid);
+        __syncthreads();
+    }
+
+    // ---- phase 5: G = -volume + lifted faces; mass inverse; outputs
+    for (int it = tid; it < CPC * NP; it += NT) {
+        const int c = it / NP, node = it % NP;
+        const int x = node % N1, y = (node / N1) % N1, z = node / (N1 * N1);
+        const int cx[3] = {x, y, z};
+        R* A = sA + c * 5 * NP;
+        R G[5];
+#pragma unroll
+        for (int s = 0; s < 5; ++s) G[s] = -A[s * NP + node];
+#pragma unroll
+        for (int f = 0; f < 6; ++f) {
+            const int dn = f >> 1;
+            const int b = (f & 1) ? N1 - 1 : 0;
+            if (cx[dn] != b) continue;
+            const int t1 = (dn == 0) ? 1 : 0, t2 = (dn == 2) ? 1 : 2;
+            const int fn = cx[t2] * N1 + cx[t1];
+            const R* tr = sT + (c * 6 + f) * TR * NF;
+#pragma unroll
+            for (int s = 0; s < 5; ++s) G[s] += tr[s * NF + fn];
+        }
+#pragma unroll
+        for (int s = 0; s < 5; ++s) A[s * NP + node] = G[s];
+    }
+    if (a.mode != 0 && a.fr) {
+        // B (x) B (x) B applied direction by direction, ping-pong between sA and sD
+        R* src = sA; R* dst = sD;
+        for (int d = 0; d < 3; ++d) {
+            __syncthreads();
+            const int st = (d == 0) ? 1 : (d == 1) ? N1 : N1 * N1;
+            for (int it = tid; it < CPC * NP; it += NT) {
+                const int c = it / NP, node = it % NP;
+                const int pos = (node / st) % N1;
+                const int base = node - pos * st;
+                for (int s = 0; s < 5; ++s) {
+                    R v = R(0);
+                    for (int l = 0; l < N1; ++l) v += sOpsB[pos * N1 + l] * src[(c * 5 + s) * NP + base + l * st];
+                    dst[(c * 5 + s) * NP + node] = v;
+                }
+            }
+            R* t = src; src = dst; dst = t;
+        }
+        __syncthreads();
+        if (src != sA) {
+            for (int it = tid; it < CPC * 5 * NP; it += NT) sA[it] = src[it];
+        }
+    }
+    __syncthreads();
+    for (int it = tid; it < CPC * 5 * NP; it += NT) {
+        const int c = it / (5 * NP);
+        const int rem = it % (5 * NP);
+        const int node = rem % NP;
+        const int cell = cell0 + c;
+        if (cell >= a.nc) continue;
+        const size_t dof = (size_t)cell * 5 * NP + rem;
+        const double G = (double)sA[it];
+        if (a.mode == 0) {
+            const int x = node % N1, y = (node / N1) % N1, z = node / (N1 * N1);
+            const double W = a.ops->w[x] * a.ops->w[y] * a.ops->w[z];
+            a.out[dof] = W * a.h * a.h * G;
+            continue;
+        }
+        const double k = G * a.inv_h;
+        if (a.mode == 1) { a.out[dof] = k; continue; }
+        const double un = a.Un[dof];
+        const double base = a.acc_in ? a.acc_in[dof] : (a.inc_mode ? 0.0 : un);
+        const double sum = base + a.c_acc * k;
+        if (a.acc_out) a.acc_out[dof] = sum;
+        if (a.final_out) {
+            if (a.comp) {   // compensated u_{n+1} = u_n + increment
+                const double y = sum - a.comp[dof];
+                const double t = un + y;
+                a.comp[dof] = (t - un) - y;
+                a.final_out[dof] = t;
+            } else {
+                a.final_out[dof] = a.inc_mode ? un + sum : sum;
+            }
+        }
+        if (a.next) {
+            const double cin = a.carry_in ? a.carry_in[dof] : 0.0;
+            a.next[dof] = (cin + a.a_next * k) * a.dt + un;
+        }
+        if (a.carry_out) a.carry_out[dof] = a.a_carry * k;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Auxiliary equation: lifted gradient q = M^{-1}[ vol grad + face (u* - u) n ] (kDG)
+// ------------------------------------------------------------------------------------
+template <int N1, int CPC>
+struct AuxLayout {
+    static constexpr int NP = N1 * N1 * N1, NF = N1 * N1;
+    static constexpr int NT = ((CPC * NP + 31) / 32) * 32 > 512 ? 512 : ((CPC * NP + 31) / 32) * 32;
+    static constexpr size_t bytes = sizeof(double) * ((size_t)CPC * 5 * NP + (size_t)CPC * 6 * 5 * NF + N1 * N1 + N1);
+};
+
+template <int N1, int CPC>
+__global__ void __launch_bounds__(AuxLayout<N1, CPC>::NT)
+aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, const OpTab* ops, int nc,
+           double inv_h, double* __restrict__ Q) {
+    using L = AuxLayout<N1, CPC>;
+    constexpr int NP = L::NP, NF = L::NF, NT = L::NT;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* sU = reinterpret_cast<double*>(smem_raw);
+    double* sT = sU + CPC * 5 * NP;
+    double* sDm = sT + CPC * 6 * 5 * NF;
+    double* sW = sDm + N1 * N1;
+    const int tid = threadIdx.x;
+    const int cell0 = blockIdx.x * CPC;
+    for (int i = tid; i < N1 * N1; i += NT) sDm[i] = ops->D[(i / N1) * MAXN1 + (i % N1)];
+    for (int i = tid; i < N1; i += NT) sW[i] = ops->w[i];
+    for (int it = tid; it < CPC * 5 * NP; it += NT) {
+        int cell = cell0 + it / (5 * NP); if (cell >= nc) cell = nc - 1;
+        sU[it] = __ldg(&U[(size_t)cell * 5 * NP + it % (5 * NP)]);
+    }
+    for (int it = tid; it < CPC * 6 * 5 * NF; it += NT) {
+        const int fn = it % NF, s = (it / NF) % 5, f = (it / (5 * NF)) % 6, c = it / (30 * NF);
+        int cell = cell0 + c; if (cell >= nc) cell = nc - 1;
+        const int cn = __ldg(&nbr[cell * 6 + f]);
+        const int nn = face_node_volume_index<N1>(f, fn, (f & 1) ? 0 : N1 - 1);
+        sT[it] = __ldg(&U[((size_t)cn * 5 + s) * NP + nn]);
+    }
+    __syncthreads();
+    const double inv_wend = 1.0 / sW[0];
+    for (int it = tid; it < CPC * NP; it += NT) {
+        const int c = it / NP, node = it % NP;
+        const int cell = cell0 + c;
+        if (cell >= nc) continue;
+        const int cx[3] = {node % N1, (node / N1) % N1, node / (N1 * N1)};
+        const double* u = sU + c * 5 * NP;
+        for (int d = 0; d < 3; ++d) {
+            const int st = (d == 0) ? 1 : (d == 1) ? N1 : N1 * N1;
+            const int pos = cx[d];
+            const int base = node - pos * st;
+            const int t1 = (d == 0) ? 1 : 0, t2 = (d == 2) ? 1 : 2;
+            const int fn = cx[t2] * N1 + cx[t1];
+#pragma unroll
+            for (int s = 0; s < 5; ++s) {
+                double g = 0.0;
+#pragma unroll
+                for (int l = 0; l < N1; ++l) g += sDm[pos * N1 + l] * u[s * NP + base + l * st];
+                if (pos == 0) {
+                    const double ue = sT[((c * 6 + 2 * d) * 5 + s) * NF + fn];
+                    g += inv_wend * (-(0.5 * (u[s * NP + node] + ue) - u[s * NP + node]));
+                }
+                if (pos == N1 - 1) {
+                    const double ue = sT[((c * 6 + 2 * d + 1) * 5 + s) * NF + fn];
+                    g += inv_wend * ((0.5 * (u[s * NP + node] + ue) - u[s * NP + node]));
+                }
+                Q[(((size_t)cell * 3 + d) * 5 + s) * NP + node] = g * inv_h;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Inverse mass on its own (DGBase::apply_inverse_global_mass_matrix, affine cells)
+// ------------------------------------------------------------------------------------
+template <int N1>
+__global__ void inverse_mass_kernel(const double* __restrict__ in, double* __restrict__ out, const OpTab* ops,
+                                    int nc, double inv_detj) {
+    constexpr int NP = N1 * N1 * N1;
+    __shared__ double s0[5 * NP], s1[5 * NP], sM[N1 * N1];
+    const int cell = blockIdx.x;
+    for (int i = threadIdx.x; i < N1 * N1; i += blockDim.x) sM[i] = ops->Minv[(i / N1) * MAXN1 + (i % N1)];
+    for (int i = threadIdx.x; i < 5 * NP; i += blockDim.x) s0[i] = in[(size_t)cell * 5 * NP + i];
+    double* src = s0; double* dst = s1;
+    for (int d = 0; d < 3; ++d) {
+        __syncthreads();
+        const int st = (d == 0) ? 1 : (d == 1) ? N1 : N1 * N1;
+        for (int i = threadIdx.x; i < 5 * NP; i += blockDim.x) {
+            const int node = i % NP, s = i / NP;
+            const int pos = (node / st) % N1, base = node - pos * st;
+            double v = 0.0;
+            for (int l = 0; l < N1; ++l) v += sM[pos * N1 + l] * src[s * NP + base + l * st];
+            dst[i] = v;
+        }
+        double* t = src; src = dst; dst = t;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 5 * NP; i += blockDim.x) out[(size_t)cell * 5 * NP + i] = src[i] * inv_detj;
+}
+
+} // namespace ph

@@ -1,0 +1,323 @@
+// Device-side Euler / Navier-Stokes physics and numerical fluxes for the GLL
+// collocated strong-form DG/FR residual. Templated on the arithmetic type `R`
+// (double for the plain path, float for the precision form).
+//
+// Reference behaviour followed:
+//   pressure / primitive conversions ........ src/physics/euler.cpp:177-500
+//   two-point split fluxes KG/IR/CH/Ra ...... src/physics/euler.cpp:563-809
+//   Ismail-Roe logarithmic mean ............. src/physics/euler.cpp:628-646
+//   convective flux ......................... src/physics/euler.cpp:915-938
+//   Roe-Pike dissipation + Harten fix ....... src/numerical_flux/convective_numerical_flux.cpp:215-480
+//   Lax-Friedrichs dissipation .............. src/numerical_flux/convective_numerical_flux.cpp:190-214
+//   viscous flux (Sutherland, Stokes) ....... src/physics/navier_stokes.cpp:241-395, :755-830, :1198-1350
+//   SIPG / BR2 auxiliary fluxes ............. src/numerical_flux/viscous_numerical_flux.cpp:146-328
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+
+namespace ph {
+
+enum TwoPointType { TP_KG = 0, TP_IR = 1, TP_CH = 2, TP_RA = 3 };
+enum ConvFluxType { CF_LXF = 0, CF_ROE = 1, CF_CENTRAL = 2, CF_EC = 3, CF_EC_LXF = 4, CF_EC_ROE = 5 };
+enum DissFluxType { DF_SIPG = 0, DF_BR2 = 1, DF_CENTRAL = 2 };
+
+// status bits written by kernels (host reads them through ph_status)
+enum StatusBits : unsigned { ST_NONPHYSICAL = 1u };
+
+constexpr double BIG_NUMBER = 1e100;   // physics.h:270
+
+struct PhysConst {
+    double gam, gm1, mach2, temp_ratio, inv_re, prandtl, const_visc, sipg_pen;
+    int use_const_visc, two_point, conv_flux, diss_flux, navier_stokes;
+};
+
+template <typename R> struct Cst {
+    R gam, gm1, mach2, temp_ratio, inv_re, prandtl, const_visc, kappa_fac;
+    __device__ __forceinline__ void load(const PhysConst& c) {
+        gam = (R)c.gam; gm1 = (R)c.gm1; mach2 = (R)c.mach2; temp_ratio = (R)c.temp_ratio;
+        inv_re = (R)c.inv_re; prandtl = (R)c.prandtl; const_visc = (R)c.const_visc;
+        kappa_fac = (R)(1.0 / (c.gm1 * c.mach2 * c.prandtl));
+    }
+};
+
+template <typename R> __device__ __forceinline__ R rlog(R x);
+template <> __device__ __forceinline__ double rlog<double>(double x) { return log(x); }
+template <> __device__ __forceinline__ float rlog<float>(float x) { return logf(x); }
+template <typename R> __device__ __forceinline__ R rsqrt_(R x);
+template <> __device__ __forceinline__ double rsqrt_<double>(double x) { return sqrt(x); }
+template <> __device__ __forceinline__ float rsqrt_<float>(float x) { return sqrtf(x); }
+template <typename R> __device__ __forceinline__ R rpow(R x, R y);
+template <> __device__ __forceinline__ double rpow<double>(double x, double y) { return pow(x, y); }
+template <> __device__ __forceinline__ float rpow<float>(float x, float y) { return powf(x, y); }
+template <typename R> __device__ __forceinline__ R rabs(R x) { return x < R(0) ? -x : x; }
+
+// Non-physical handling: a negative density/pressure sets a status bit and is
+// replaced by BIG_NUMBER, as check_positive_quantity does (euler.cpp:155-172).
+template <typename R> __device__ __forceinline__ R positive(R q, unsigned* status) {
+    if (q < R(0)) {
+        if (status) atomicOr(status, ST_NONPHYSICAL);
+        return (R)BIG_NUMBER;
+    }
+    return q;
+}
+
+template <typename R> __device__ __forceinline__ R pressure(const R u[5], R gm1, unsigned* st) {
+    const R rho = u[0];
+    R v2 = R(0);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { const R v = u[1 + d] / rho; v2 = v2 + v * v; }
+    return positive<R>(gm1 * (u[4] - R(0.5) * rho * v2), st);
+}
+
+// Per-node quantities reused by every two-point flux that touches the node.
+template <typename R> struct NodeQ {
+    R rho, v[3], p, E;
+    R a, b, la, lb;   // log-mean arguments and their logarithms (type dependent)
+    R vsq;            // |v|^2 (CH, Ra) or specific total energy (KG)
+};
+
+template <typename R>
+__device__ __forceinline__ void node_prepare(const R u[5], int tp, R gm1, NodeQ<R>& q, unsigned* st) {
+    q.rho = u[0];
+    R v2 = R(0);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { q.v[d] = u[1 + d] / u[0]; v2 = v2 + q.v[d] * q.v[d]; }
+    q.E = u[4];
+    q.p = positive<R>(gm1 * (u[4] - R(0.5) * u[0] * v2), st);
+    if (tp == TP_CH) {
+        q.a = q.rho; q.b = q.rho / (R(2) * q.p);
+        q.la = rlog<R>(q.a); q.lb = rlog<R>(q.b);
+        q.vsq = q.v[0] * q.v[0] + q.v[1] * q.v[1] + q.v[2] * q.v[2];
+    } else if (tp == TP_RA) {
+        q.a = q.rho; q.b = q.rho / q.p;
+        q.la = rlog<R>(q.a); q.lb = rlog<R>(q.b);
+        q.vsq = q.v[0] * q.v[0] + q.v[1] * q.v[1] + q.v[2] * q.v[2];
+    } else if (tp == TP_IR) {
+        const R rho = positive<R>(q.rho, st);
+        q.a = rsqrt_<R>(rho / q.p);      // z_0
+        q.b = rsqrt_<R>(rho * q.p);      // z_4
+        q.la = rlog<R>(q.a); q.lb = rlog<R>(q.b);
+        q.vsq = R(0);
+    } else {   // KG
+        q.a = q.b = q.la = q.lb = R(0);
+        q.vsq = q.E / q.rho;
+    }
+}
+
+// Logarithmic mean with the Ismail-Roe series branch (euler.cpp:628-646). The
+// logarithms of the two arguments are taken once per node, so the log of the ratio
+// is their difference; the branch test uses the reference's own ratio form.
+template <typename R>
+__device__ __forceinline__ R log_mean(R a, R b, R la, R lb) {
+    const R zeta = a / b;
+    const R f = (zeta - R(1)) / (zeta + R(1));
+    const R u = f * f;
+    if (u < R(1.0e-2)) {
+        const R F = R(1) + u / R(3) + u * u / R(5) + u * u * u / R(7);
+        return (a + b) / (R(2) * F);
+    }
+    return (a - b) / (la - lb);
+}
+
+// Two-point flux component along direction d (compile time) for all 5 equations.
+template <typename R, int d>
+__device__ __forceinline__ void two_point_dir(const NodeQ<R>& i, const NodeQ<R>& j, int tp,
+                                              const Cst<R>& c, R F[5]) {
+    if (tp == TP_CH || tp == TP_RA) {
+        const R rho_log = log_mean<R>(i.a, j.a, i.la, j.la);
+        const R b_log = log_mean<R>(i.b, j.b, i.lb, j.lb);
+        R va[3], vsq = R(0);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { va[k] = R(0.5) * (i.v[k] + j.v[k]); vsq += va[k] * va[k]; }
+        R p_hat, H;
+        if (tp == TP_CH) {
+            p_hat = R(0.5) * (i.rho + j.rho) / (R(2) * R(0.5) * (i.b + j.b));
+            H = R(1) / (R(2) * b_log * c.gm1) + vsq + p_hat / rho_log;
+        } else {
+            p_hat = R(0.5) * (i.p + j.p);
+            H = R(1) / (b_log * c.gm1) + vsq + R(2) * p_hat / rho_log;
+        }
+        H -= R(0.5) * (R(0.5) * (i.vsq + j.vsq));
+        const R m = rho_log * va[d];
+        F[0] = m;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) F[1 + k] = m * va[k];
+        F[1 + d] += p_hat;
+        F[4] = m * H;
+        if (tp == TP_RA) F[4] -= R(0.5) * (i.p * i.v[d] + j.p * j.v[d]);
+    } else if (tp == TP_IR) {
+        const R z0a = R(0.5) * (i.a + j.a), z4a = R(0.5) * (i.b + j.b);
+        const R l0 = log_mean<R>(i.a, j.a, i.la, j.la);
+        const R l4 = log_mean<R>(i.b, j.b, i.lb, j.lb);
+        const R rho = z0a * l4;
+        R v[3], vv = R(0);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const R zk = R(0.5) * (i.a * i.v[k] + j.a * j.v[k]);
+            v[k] = zk / z0a; vv += v[k] * v[k];
+        }
+        const R p = z4a / z0a;
+        R H = (c.gam + R(1)) * (l4 / l0) + c.gm1 * p;
+        H /= R(2) * c.gam;
+        H *= c.gam / (rho * c.gm1);
+        H += R(0.5) * vv;
+        const R m = rho * v[d];
+        F[0] = m;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) F[1 + k] = m * v[k];
+        F[1 + d] += p;
+        F[4] = m * H;
+    } else {   // KG
+        const R rho = (i.rho + j.rho) / R(2);
+        const R p = (i.p + j.p) / R(2);
+        R v[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) v[k] = R(0.5) * (i.v[k] + j.v[k]);
+        const R e = (i.vsq + j.vsq) / R(2);
+        const R m = rho * v[d];
+        F[0] = m;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) F[1 + k] = m * v[k];
+        F[1 + d] += p;
+        F[4] = m * e + p * v[d];
+    }
+}
+
+// Physical convective flux along direction d.
+template <typename R, int d>
+__device__ __forceinline__ void conv_flux_dir(const NodeQ<R>& q, R F[5]) {
+    const R H = q.E / q.rho + q.p / q.rho;
+    const R m = q.rho * q.v[d];
+    F[0] = m;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) F[1 + k] = m * q.v[k];
+    F[1 + d] += q.p;
+    F[4] = m * H;
+}
+
+// Roe-Pike dissipation -1/2 |A_roe| (uR - uL) for the axis normal n = +e_d.
+template <typename R, int d>
+__device__ __forceinline__ void roe_dissipation(const NodeQ<R>& L, const NodeQ<R>& Rq,
+                                                const Cst<R>& c, R out[5]) {
+    const R n[3] = {R(d == 0), R(d == 1), R(d == 2)};
+    const R vnL = L.v[d], vnR = Rq.v[d];
+    const R hL = (L.E + L.p) / L.rho, hR = (Rq.E + Rq.p) / Rq.rho;
+    const R r = rsqrt_<R>(Rq.rho / L.rho), rp1 = r + R(1);
+    const R rho_a = r * L.rho;
+    R va[3], v2a = R(0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { va[k] = (r * Rq.v[k] + L.v[k]) / rp1; v2a = v2a + va[k] * va[k]; }
+    const R ha = (r * hR + hL) / rp1;
+    const R vna = va[d];
+    const R c2a = c.gm1 * (ha - R(0.5) * v2a);
+    R ca = R(1e10);
+    if (c2a > R(0)) ca = rsqrt_<R>(c2a);
+    R eig[3] = {rabs(vna - ca), rabs(vna), rabs(vna + ca)};
+    const R cL = rsqrt_<R>(L.p * c.gam / L.rho), cR = rsqrt_<R>(Rq.p * c.gam / Rq.rho);
+    const R eL[3] = {rabs(vnL - cL), rabs(vnL), rabs(vnL + cL)};
+    const R eR[3] = {rabs(vnR - cR), rabs(vnR), rabs(vnR + cR)};
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+        const R a1 = rabs(eig[e] - eL[e]), a2 = rabs(eR[e] - eig[e]);
+        const R eps = a1 > a2 ? a1 : a2;
+        if (eig[e] < eps) eig[e] = R(0.5) * (eig[e] * eig[e] / eps + eps);
+    }
+    const R dp = Rq.p - L.p, drho = Rq.rho - L.rho, dvn = vnR - vnL;
+    R dvt[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) dvt[k] = (Rq.v[k] - L.v[k]) - dvn * n[k];
+    const R c0 = eig[0] * (dp - rho_a * ca * dvn) / (R(2) * c2a);
+    const R c1 = eig[1] * (drho - dp / c2a);
+    const R c2 = eig[1] * rho_a;
+    const R c3 = eig[2] * (dp + rho_a * ca * dvn) / (R(2) * c2a);
+    R A[5];
+    A[0] = c0 + c1 + c3;
+    R dvtv = R(0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        A[1 + k] = c0 * (va[k] - ca * n[k]) + c1 * va[k] + c2 * dvt[k] + c3 * (va[k] + ca * n[k]);
+        dvtv += va[k] * dvt[k];
+    }
+    A[4] = c0 * (ha - ca * vna) + c1 * v2a * R(0.5) + c2 * dvtv + c3 * (ha + ca * vna);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) out[k] = R(-0.5) * A[k];
+}
+
+// Convective numerical flux dot n for n = +e_d, evaluated with L = minus side.
+// (convective_numerical_flux.cpp:35-54 composition of baseline + dissipation)
+template <typename R, int d>
+__device__ __forceinline__ void conv_num_flux(const R uL[5], const R uR[5], const NodeQ<R>& L, const NodeQ<R>& Rq,
+                                              int tp, int cf, const Cst<R>& c, R out[5]) {
+    if (cf == CF_EC || cf == CF_EC_LXF || cf == CF_EC_ROE) {
+        two_point_dir<R, d>(L, Rq, tp, c, out);
+    } else {
+        R FL[5], FR[5];
+        conv_flux_dir<R, d>(L, FL);
+        conv_flux_dir<R, d>(Rq, FR);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) out[k] = R(0.5) * (FL[k] + FR[k]);
+    }
+    if (cf == CF_LXF || cf == CF_EC_LXF) {
+        const R eLv = rabs(L.v[d]) + rsqrt_<R>(L.p * c.gam / L.rho);
+        const R eRv = rabs(Rq.v[d]) + rsqrt_<R>(Rq.p * c.gam / Rq.rho);
+        const R e = eLv > eRv ? eLv : eRv;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) out[k] += R(-0.5) * e * (uR[k] - uL[k]);
+    } else if (cf == CF_ROE || cf == CF_EC_ROE) {
+        R diss[5];
+        roe_dissipation<R, d>(L, Rq, c, diss);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) out[k] += diss[k];
+    }
+}
+
+// Navier-Stokes viscous flux ("LHS" sign) for state u and conservative gradient
+// g[s][k] (navier_stokes.cpp:1198-1350). F[d][0..3] = (momentum x3, energy) along
+// direction d; the density component is zero. `dmask` selects the directions.
+template <typename R>
+__device__ __forceinline__ void viscous_flux(const R u[5], const R g[5][3], int use_const_visc,
+                                             const Cst<R>& c, R F[3][4], int dmask, unsigned* st) {
+    const R rho_raw = u[0];
+    R w[5];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) w[1 + k] = u[1 + k] / rho_raw;
+    R v2 = R(0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) v2 = v2 + w[1 + k] * w[1 + k];
+    w[4] = positive<R>(positive<R>(c.gm1 * (u[4] - R(0.5) * rho_raw * v2), st), st);
+    w[0] = positive<R>(rho_raw, st);
+    const R rho = w[0];
+    R gv[3][3], gp[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) gv[a][k] = (g[1 + a][k] - w[1 + a] * g[0][k]) / rho;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        R t = g[4][k];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) t -= R(0.5) * (w[1 + m] * g[1 + m][k] + u[1 + m] * gv[m][k]);
+        gp[k] = t * c.gm1;
+    }
+    const R T = c.gam * c.mach2 * (w[4] / rho);
+    R mu = use_const_visc ? c.const_visc : ((R(1) + c.temp_ratio) / (T + c.temp_ratio)) * rpow<R>(T, R(1.5));
+    mu = mu * c.inv_re;
+    const R kappa = mu * c.kappa_fac;
+    const R div = gv[0][0] + gv[1][1] + gv[2][2];
+    const R mu2 = (R(-2) / R(3)) * mu;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        if (!(dmask & (1 << d))) continue;
+        R tau_d[3];   // tau[k][d] (symmetric)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) tau_d[k] = R(2) * mu * (R(0.5) * (gv[k][d] + gv[d][k]));
+        tau_d[d] += mu2 * div;
+        const R dT = (c.gam * c.mach2 * gp[d] - T * g[0][d]) / rho;
+        const R q = -kappa * dT;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) F[d][k] = -tau_d[k];
+        F[d][3] = -(w[1] * tau_d[0] + w[2] * tau_d[1] + w[3] * tau_d[2]) + q;
+    }
+}
+
+} // namespace ph

@@ -1,0 +1,258 @@
+"""Host-side mirror of the reference's DGBase/DGStrong, RungeKuttaODESolver and
+FlowSolver surface over the C-ABI library.
+
+Reference interfaces mirrored (same names and argument meaning):
+  DGBase::solution / right_hand_side ............ src/dg/dg_base.hpp:396, :409
+  DGBase::assemble_residual ..................... src/dg/dg_base.hpp:571
+  DGBase::apply_inverse_global_mass_matrix ...... src/dg/dg_base.hpp:267
+  DGBase::set_current_time ...................... src/dg/dg_base.hpp
+  ODESolverBase::step_in_time / advance_solution_time  src/ode_solver/ode_solver_base.h:70, .cpp:262-322
+  FlowSolver::run (unsteady loop) ............... src/flow_solver/flow_solver.cpp:427-600
+  PeriodicTurbulence::get_constant_time_step .... src/flow_solver/flow_solver_cases/periodic_turbulence.cpp:115-127
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+
+from . import _lib
+from .prm import Parameters
+
+
+def _ptr(a: np.ndarray) -> int:
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data
+
+
+def gll_nodes(n: int) -> np.ndarray:
+    """Gauss-Lobatto nodes on [0,1] (the FE_DGQ support points)."""
+    if n == 1:
+        return np.array([0.5])
+    m = n - 1
+    z = -np.cos(np.pi * np.arange(n) / m)
+    for _ in range(100):
+        # Newton on P_m'(z) at the interior points
+        p0, p1 = np.ones_like(z), z.copy()
+        for k in range(2, m + 1):
+            p0, p1 = p1, ((2 * k - 1) * z * p1 - (k - 1) * p0) / k
+        with np.errstate(divide="ignore", invalid="ignore"):
+            dp = m * (z * p1 - p0) / (z * z - 1.0)
+            d2p = (2.0 * z * dp - m * (m + 1.0) * p1) / (1.0 - z * z)
+            dz = np.where(np.abs(np.abs(z) - 1.0) < 1e-15, 0.0, dp / d2p)
+        z = z - dz
+        if np.max(np.abs(dz)) < 1e-16:
+            break
+    x = 0.5 * (z + 1.0)
+    x[0], x[-1] = 0.0, 1.0
+    return x
+
+
+class DGStrong:
+    """Strong-form DG/FR discretisation on a periodic cube, evaluated on the B200."""
+
+    def __init__(self, parameters: Parameters, precision: int = _lib.PH_FP64, cell_order: int = 0,
+                 stream: int | None = None):
+        self.L = _lib.load()
+        self.parameters = parameters
+        self.params = parameters.to_ph_params(precision)
+        left, right = parameters.grid_bounds
+        self.mesh = _lib.PhMeshDesc(parameters.n_cells, cell_order, left, right)
+        h = ctypes.c_void_p()
+        _lib.check(self.L.ph_ctx_create(ctypes.byref(self.mesh), ctypes.byref(self.params),
+                                        ctypes.c_void_p(stream) if stream else None, ctypes.byref(h)))
+        self._h = h
+        self.n_dofs = int(self.L.ph_ndofs(h))
+        self.poly_degree = parameters.poly_degree
+        self.n_cells = parameters.n_cells ** 3
+        self.n_shape = (self.poly_degree + 1) ** 3
+        self.right_hand_side = np.zeros(self.n_dofs)
+        self.current_time = 0.0
+
+    def __del__(self):
+        if getattr(self, "_h", None) is not None:
+            self.L.ph_ctx_destroy(self._h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    # -- state
+    @property
+    def solution(self) -> np.ndarray:
+        U = np.empty(self.n_dofs)
+        _lib.check(self.L.ph_get_state(self._h, _ptr(U), _lib.PH_HOST))
+        return U
+
+    @solution.setter
+    def solution(self, U: np.ndarray):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        if U.size != self.n_dofs:
+            raise ValueError("state size mismatch")
+        _lib.check(self.L.ph_set_state(self._h, _ptr(U), _lib.PH_HOST))
+
+    def set_current_time(self, t: float):
+        self.current_time = t
+
+    # -- residual and mass inverse
+    def assemble_residual(self, compute_dRdW: bool = False, compute_dRdX: bool = False,
+                          compute_d2R: bool = False, CFL_mass: float = 0.0):
+        if compute_dRdW or compute_dRdX or compute_d2R:
+            raise NotImplementedError("implicit/adjoint derivatives are outside the explicit path")
+        U = self.solution
+        _lib.check(self.L.ph_residual(self._h, _ptr(U), _ptr(self.right_hand_side), _lib.PH_HOST))
+
+    def residual_of(self, U: np.ndarray) -> np.ndarray:
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        R = np.empty(self.n_dofs)
+        _lib.check(self.L.ph_residual(self._h, _ptr(U), _ptr(R), _lib.PH_HOST))
+        return R
+
+    def apply_inverse_global_mass_matrix(self, input_vector: np.ndarray, output_vector: np.ndarray,
+                                         use_auxiliary_eq: bool = False):
+        if use_auxiliary_eq:
+            raise NotImplementedError("the auxiliary mass inverse is applied inside the residual")
+        inp = np.ascontiguousarray(input_vector, dtype=np.float64)
+        if not (output_vector.dtype == np.float64 and output_vector.flags["C_CONTIGUOUS"]):
+            raise ValueError("output_vector must be a contiguous float64 array")
+        _lib.check(self.L.ph_apply_inverse_mass(self._h, _ptr(inp), _ptr(output_vector), _lib.PH_HOST))
+
+    # -- geometry
+    def cell_ijk(self) -> np.ndarray:
+        out = np.empty((self.n_cells, 3), dtype=np.int32)
+        _lib.check(self.L.ph_cell_ijk(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))))
+        return out
+
+    def node_coordinates(self) -> np.ndarray:
+        """Physical coordinates of the solution support points, [cell][node][3]."""
+        n1 = self.poly_degree + 1
+        xs = gll_nodes(n1)
+        left, right = self.parameters.grid_bounds
+        h = (right - left) / self.parameters.n_cells
+        ijk = self.cell_ijk().astype(np.float64)
+        k, j, i = np.meshgrid(np.arange(n1), np.arange(n1), np.arange(n1), indexing="ij")
+        local = np.stack([xs[i].ravel(), xs[j].ravel(), xs[k].ravel()], axis=-1)
+        return left + h * (ijk[:, None, :] + local[None, :, :])
+
+    # -- diagnostics
+    def integrals(self) -> np.ndarray:
+        out = np.zeros(4)
+        _lib.check(self.L.ph_integrals(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out
+
+    def status(self) -> int:
+        v = ctypes.c_uint32(0)
+        _lib.check(self.L.ph_status(self._h, ctypes.byref(v)))
+        return int(v.value)
+
+
+class RungeKuttaODESolver:
+    """Explicit Butcher RK stepping on the device-resident state (RungeKuttaODESolver)."""
+
+    def __init__(self, dg: DGStrong):
+        self.dg = dg
+        self.current_time = 0.0
+        self.current_iteration = 0
+
+    def step_in_time(self, dt: float, pseudotime: bool = False, nsteps: int = 1):
+        if pseudotime:
+            raise NotImplementedError("pseudotime stepping belongs to the steady solvers")
+        _lib.check(self.dg.L.ph_rk_step(self.dg.handle, dt, nsteps))
+        self.current_iteration += nsteps
+        self.current_time += dt * nsteps
+        self.dg.set_current_time(self.current_time)
+
+    def advance_solution_time(self, time_advance: float, dt: float):
+        """ODESolverBase::advance_solution_time: steps of dt, the last one clipped."""
+        final = self.current_time + time_advance
+        while self.current_time < final:
+            step = min(dt, final - self.current_time)
+            self.step_in_time(step)
+
+
+# --------------------------------------------------------------------------------
+# Flow cases (periodic cube): Taylor-Green vortex and isentropic vortex
+# --------------------------------------------------------------------------------
+def tgv_primitive(x, y, z, gamma, mach):
+    """InitialConditionFunction_TaylorGreenVortex (initial_condition_function.cpp:261-310)."""
+    rho = np.ones_like(x)
+    u = np.sin(x) * np.cos(y) * np.cos(z)
+    v = -np.cos(x) * np.sin(y) * np.cos(z)
+    w = np.zeros_like(x)
+    p = 1.0 / (gamma * mach * mach) + (1.0 / 16.0) * (np.cos(2.0 * x) + np.cos(2.0 * y)) * (np.cos(2.0 * z) + 2.0)
+    return rho, u, v, w, p
+
+
+def isentropic_vortex_primitive(x, y, z, gamma, beta, mach, direction, center=(0.0, 0.0), t=0.0, period=0.0):
+    """Isentropic vortex translated with the free stream (initial_condition_function.cpp:643-690,
+    with strength, Mach number and direction as parameters)."""
+    dx = x - center[0] - mach * direction[0] * t
+    dy = y - center[1] - mach * direction[1] * t
+    if period > 0.0:
+        dx = dx - period * np.round(dx / period)
+        dy = dy - period * np.round(dy / period)
+    om = beta * np.exp(-0.5 * (dx * dx + dy * dy))
+    dT = -(gamma - 1.0) / 2.0 * om * om
+    rho = (1.0 + dT) ** (1.0 / (gamma - 1.0))
+    u = mach * direction[0] - dy * om
+    v = mach * direction[1] + dx * om
+    w = mach * direction[2] * np.ones_like(x)
+    p = 1.0 / gamma * (1.0 + dT) ** (gamma / (gamma - 1.0))
+    return rho, u, v, w, p
+
+
+def conservative_state(dg: DGStrong, prim) -> np.ndarray:
+    """Nodal interpolation (VectorTools::interpolate) into the reference DoF layout."""
+    rho, u, v, w, p = prim
+    gamma = dg.params.gamma_gas
+    E = p / (gamma - 1.0) + 0.5 * rho * (u * u + v * v + w * w)
+    cons = np.stack([rho, rho * u, rho * v, rho * w, E], axis=1)   # [cell][state][node]
+    return np.ascontiguousarray(cons.reshape(-1))
+
+
+class FlowSolver:
+    """FlowSolver::run for the periodic-cube cases (TGV; isentropic vortex)."""
+
+    def __init__(self, parameters: Parameters, precision: int = _lib.PH_FP64, cell_order: int = 0):
+        self.parameters = parameters
+        self.dg = DGStrong(parameters, precision=precision, cell_order=cell_order)
+        self.ode_solver = RungeKuttaODESolver(self.dg)
+        self.flow_case = parameters.get("flow_solver/flow_case_type")
+        X = self.dg.node_coordinates()
+        gamma, mach = self.dg.params.gamma_gas, self.dg.params.mach_infinity
+        if self.flow_case == "taylor_green_vortex":
+            prim = tgv_primitive(X[..., 0], X[..., 1], X[..., 2], gamma, mach)
+        elif self.flow_case == "isentropic_vortex":
+            m = math.sqrt(2.0 / gamma)
+            beta = m * 5 * math.sqrt(2.0) / 4.0 / math.pi * math.exp(0.5)
+            prim = isentropic_vortex_primitive(X[..., 0], X[..., 1], X[..., 2], gamma, beta, m,
+                                               (math.cos(math.pi / 4), math.sin(math.pi / 4), 0.0))
+        else:
+            raise ValueError(f"flow_case_type {self.flow_case!r} is outside the periodic-cube cases")
+        self.dg.solution = conservative_state(self.dg, prim)
+        self.unsteady_data = []
+
+    def constant_time_step(self) -> float:
+        cst = float(self.parameters.get("flow_solver/constant_time_step"))
+        if cst > 0.0:
+            return cst
+        left, right = self.parameters.grid_bounds
+        ndof_per_state = self.dg.n_dofs // 5
+        return float(self.parameters.get("flow_solver/courant_friedrichs_lewy_number")) * \
+            (right - left) / ndof_per_state ** (1.0 / 3.0)
+
+    def run(self, record_every: int = 1):
+        final_time = float(self.parameters.get("flow_solver/final_time"))
+        end_exact = self.parameters.get("flow_solver/end_exactly_at_final_time").lower() == "true"
+        dt = self.constant_time_step()
+        self.unsteady_data.append((self.ode_solver.current_time, *self.dg.integrals()))
+        while self.ode_solver.current_time < final_time:
+            step = dt
+            if self.ode_solver.current_time + step > final_time and end_exact:
+                step = final_time - self.ode_solver.current_time
+            self.ode_solver.step_in_time(step)
+            if self.ode_solver.current_iteration % record_every == 0:
+                self.unsteady_data.append((self.ode_solver.current_time, *self.dg.integrals()))
+        return 0
