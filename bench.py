@@ -1,0 +1,364 @@
+#!/usr/bin/env python
+"""Benchmark of the explicit strong-form DG/FR residual + RK4 stage on the B200.
+
+Workload (default): viscous Taylor-Green vortex, Re=1600, Pr=0.71, Mach 0.1, on the
+periodic cube [0, 2 pi]^3 with 24^3 hex cells, p = 5 on GLL nodes (216 nodes/cell,
+14,929,920 DOFs), Chandrashekar split-form volume flux, Roe face dissipation, BR2
+viscous flux, classical RK4. Synthetic data: the TGV initial condition, interpolated
+at the nodes.
+
+A "step" is one RK4 time step (4 stages). The metric is DOF-updates per second per
+stage = N_DOF x stages / time, aggregated over all GPUs (each GPU integrates its own
+copy of the cube: replicas, weak scaling).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload tgv_viscous_24_p5|tgv_inviscid_8_p3|tgv_viscous_32_p3]
+                  [--precision fp64|fp32]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+TWO_PI = 6.28318530717958623200
+
+WORKLOADS = {
+    # name: (poly_degree, cells per direction, pde, diss flux, description)
+    "tgv_viscous_24_p5": (5, 24, "navier_stokes", "bassi_rebay_2",
+                          "viscous TGV Re=1600, 24^3 cells, p=5 GLL, CH split + Roe, BR2, RK4"),
+    "tgv_inviscid_8_p3": (3, 8, "euler", "symm_internal_penalty",
+                          "inviscid TGV, 8^3 cells, p=3 GLL, CH split + Roe, RK4"),
+    "tgv_viscous_32_p3": (3, 32, "navier_stokes", "bassi_rebay_2",
+                          "viscous TGV Re=1600, 32^3 cells, p=3 GLL, CH split + Roe, BR2, RK4"),
+    # reduced size of the default workload, for ncu captures (still larger than L2)
+    "tgv_viscous_16_p5": (5, 16, "navier_stokes", "bassi_rebay_2",
+                          "viscous TGV Re=1600, 16^3 cells, p=5 GLL, CH split + Roe, BR2, RK4"),
+}
+
+
+def prm_for(workload: str) -> dict:
+    p, n, pde, diss, _ = WORKLOADS[workload]
+    return {
+        "dimension": 3, "pde_type": pde, "use_weak_form": False, "flux_nodes_type": "GLL",
+        "use_split_form": True, "two_point_num_flux_type": "CH",
+        "conv_num_flux": "two_point_flux_with_roe_dissipation", "diss_num_flux": diss,
+        "flux_reconstruction": "cDG", "use_inverse_mass_on_the_fly": True,
+        "all_boundaries_are_periodic": True, "do_renumber_dofs": False,
+        "ODE solver/ode_solver_type": "runge_kutta", "ODE solver/runge_kutta_method": "rk4_ex",
+        "euler/mach_infinity": 0.1, "navier_stokes/reynolds_number_inf": 1600.0,
+        "navier_stokes/prandtl_number": 0.71,
+        "flow_solver/flow_case_type": "taylor_green_vortex", "flow_solver/poly_degree": p,
+        "flow_solver/final_time": 2.0, "flow_solver/courant_friedrichs_lewy_number": 0.1,
+        # CFL x spacing / max wave speed (the reference's adaptive_time_step formula); the
+        # constant formula CFL x spacing ignores the sound speed and is unstable at Mach 0.1
+        "flow_solver/adaptive_time_step": True,
+        "flow_solver/grid/grid_left_bound": 0.0, "flow_solver/grid/grid_right_bound": TWO_PI,
+        "flow_solver/grid/number_of_grid_elements_per_dimension": n,
+    }
+
+
+def bytes_per_dof_stage(viscous: bool) -> dict:
+    """Algorithmic HBM bytes per DOF of the stage kernel, averaged over the 4 RK4 stages.
+
+    Stage kernel (FP64 state): reads the stage input (8 B), u_n (8 B, stages 1-3... see
+    below), the running sum (8 B, stages 2-4) and writes the running sum (8 B, stages 1-3),
+    the next stage state (8 B, stages 1-3) or u_{n+1} (8 B, stage 4):
+      stage 1: U_in + acc_out + next            = 24 B
+      stage 2,3: U_in + u_n + acc_in + acc_out + next = 40 B
+      stage 4: U_in + acc_in + u_{n+1}          = 24 B      -> mean 32 B
+    Viscous: the stage kernel also reads the lifted gradient q (3 x 8 B); the auxiliary
+    kernel reads U_in (8 B) and writes q (24 B). Neighbour face traces are not counted
+    (they are re-reads of data the neighbouring CTA streams, served from L2).
+    """
+    stage = 32.0 + (24.0 if viscous else 0.0)
+    aux = 32.0 if viscous else 0.0
+    return {"stage": stage, "aux": aux}
+
+
+def flops_per_dof_stage(p: int, viscous: bool) -> float:
+    """Algorithmic FP64 operations per DOF per stage (counted from the kernel source:
+    add/mul/fma = 1, divide = 1, sqrt = 1, log = 1). Two-point fluxes with pair symmetry:
+    1.5 (n1 - 1) unique CH pairs per node at ~46 ops each, plus per-node preparation
+    (~30 ops + 2 logs), the face numerical flux (Roe, ~170 ops per face node, evaluated by
+    both neighbours: 6 n1^2 per cell) and the viscous terms (~150 ops per node for the
+    flux, 2 x 3 x n1 x 4 FMA for its divergence and 3 x n1 x 5 for the gradient)."""
+    n1 = p + 1
+    per_node = 1.5 * (n1 - 1) * 46 + 32 + 6.0 * n1 * n1 * 170 / n1 ** 3 + 5 * 3 * 2 * n1
+    if viscous:
+        per_node += 150 + 2 * 3 * n1 * 4 + 3 * n1 * 5 + 6.0 * n1 * n1 * 2 * 150 / n1 ** 3
+    return per_node / 5.0
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._thr = None
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._thr = threading.Thread(target=self._run, daemon=True)
+        self._thr.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._thr.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "", 1).isdigit()]
+        smax = [float(s[1]) for s in self.samples if s[1].replace(".", "", 1).isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 3 + i and "Active" in s[3 + i]
+                          and not s[3 + i].startswith("Not")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback 6.65 TB/s"
+
+
+def ncu_traffic(workload: str):
+    path = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d.get(workload)
+    return None
+
+
+def cpu_baseline(workload: str, n_threads: int | None = None):
+    """Time the CPU oracle (a port of the reference path) on one RK stage of the workload."""
+    from oracle.oracle import Oracle, lib as orc_lib
+    from philip_b200.prm import Parameters
+    prm = Parameters.from_dict(prm_for(workload))
+    if n_threads:
+        Oracle.set_threads(n_threads)
+    cores = int(orc_lib().orc_max_threads())
+    orc = Oracle(prm.oracle_cfg(), prm.n_cells, *prm.grid_bounds)
+    U = orc.initial_condition("tgv")
+    t0 = time.perf_counter()
+    R = orc.residual(U)
+    k = orc.inverse_mass(R)
+    U += 1e-4 * k
+    dt = time.perf_counter() - t0
+    return {"value": orc.ndofs / dt, "unit": "DOF-updates/s/stage", "cores": cores, "kind": "port",
+            "sample": f"one RK stage (assemble_residual + inverse mass + update) of the full {workload} "
+                      f"mesh ({orc.ndofs} DOFs) on {cores} OpenMP threads, {dt:.2f} s"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    from oracle.oracle import Oracle, lib as orc_lib
+    from philip_b200.prm import Parameters
+    prm = Parameters.from_dict(prm_for(args.workload))
+    cores = int(orc_lib().orc_max_threads())
+    orc = Oracle(prm.oracle_cfg(), prm.n_cells, *prm.grid_bounds)
+    U = orc.initial_condition("tgv")
+    # one RK stage of the full mesh per step; the CPU needs no warm-up beyond one stage
+    for _ in range(min(args.warmup, 1)):
+        orc.inverse_mass(orc.residual(U))
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        k = orc.inverse_mass(orc.residual(U))
+        U += 1e-6 * k
+    el = time.perf_counter() - t0
+    value = orc.ndofs * args.steps / el
+    _, _, _, _, desc = WORKLOADS[args.workload]
+    line = {
+        "impl": "reference", "metric": "TGV DOF-updates/s/stage", "value": value, "unit": "DOF-updates/s/stage",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (Taylor-Green initial condition interpolated at the GLL nodes)",
+        "config": {"workload": args.workload, "description": desc, "ndofs": orc.ndofs,
+                   "step": "one RK stage on the host (reference arm)"},
+        "cpu_baseline": {"value": value, "unit": "DOF-updates/s/stage", "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} RK stages of the full mesh on {cores} OpenMP threads "
+                                   "(the reference itself cannot be built: deal.II/MPI/Trilinos/p4est absent)"},
+        "e2e": {"value": value, "unit": "DOF-updates/s/stage", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="tgv_viscous_24_p5", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from philip_b200 import _lib
+    from philip_b200.dg import FlowSolver
+    from philip_b200.prm import Parameters
+
+    if args.warmup < 3:
+        args.warmup = 3
+    prm = Parameters.from_dict(prm_for(args.workload))
+    prec = _lib.PH_FP32_RESIDUAL if args.precision == "fp32" else _lib.PH_FP64
+    fs = FlowSolver(prm, precision=prec)
+    dg = fs.dg
+    L, h = dg.L, dg.handle
+    dt = fs.adaptive_time_step()
+    p, n, pde, _, desc = WORKLOADS[args.workload]
+    viscous = pde == "navier_stokes"
+    stages = 4
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # ---- warm-up
+    _lib.check(L.ph_rk_step(h, dt, args.warmup))
+    torch.cuda.synchronize()
+
+    # ---- device-timed region (inputs resident in HBM; the working set is larger than L2)
+    _lib.check(L.ph_set_timing(h, 0))
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(); torch.cuda.synchronize()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ev0.record()
+        _lib.check(L.ph_rk_step(h, dt, args.steps))
+        ev1.record()
+        torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    tm = np.zeros(7)
+    _lib.check(L.ph_get_timing(h, tm.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+    launches = int(tm[6])
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = world * dg.n_dofs * stages * args.steps / (ms * 1e-3)
+
+    # ---- per-kernel launch durations (CUDA events on the launching stream)
+    _lib.check(L.ph_set_timing(h, 1))
+    _lib.check(L.ph_rk_step(h, dt, 2))
+    _lib.check(L.ph_get_timing(h, tm.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+    _lib.check(L.ph_set_timing(h, 0))
+    stage_ms = tm[0] / max(tm[1], 1)
+    aux_ms = tm[2] / max(tm[3], 1)
+
+    # ---- end to end through the C-ABI with host buffers (pinned), every step:
+    # H2D of the state, one RK4 step, D2H of the state
+    U_host = torch.empty(dg.n_dofs, dtype=torch.float64, pin_memory=True)
+    _lib.check(L.ph_get_state(h, U_host.data_ptr(), _lib.PH_HOST))
+    barrier(); torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        _lib.check(L.ph_set_state(h, U_host.data_ptr(), _lib.PH_HOST))
+        _lib.check(L.ph_rk_step(h, dt, 1))
+        _lib.check(L.ph_get_state(h, U_host.data_ptr(), _lib.PH_HOST))
+    e1.record(); torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e = world * dg.n_dofs * stages * args.steps / (ms_e2e * 1e-3)
+    status = dg.status()
+
+    if rank == 0:
+        peak, peak_src = measured_peaks()
+        bpd = bytes_per_dof_stage(viscous)
+        if args.precision == "fp32":
+            pass   # the state stays FP64, so the stage bytes are the same (+8 B/DOF Kahan term at the last stage)
+        bytes_launch = bpd["stage"] * dg.n_dofs
+        achieved = bytes_launch / (stage_ms * 1e-3) / 1e9
+        traffic = ncu_traffic(args.workload + ("" if args.precision == "fp64" else "_fp32"))
+        line = {
+            "metric": "TGV DOF-updates/s/stage", "value": value, "unit": "DOF-updates/s/stage",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32-residual/f64-state",
+            "data": "synthetic (Taylor-Green initial condition interpolated at the GLL nodes)",
+            "config": {"workload": args.workload, "description": desc, "ndofs": dg.n_dofs,
+                       "cells": n ** 3, "poly_degree": p, "stages_per_step": stages, "dt": dt,
+                       "l2": "inputs larger than L2 (state 120 MB/vector, working set > 600 MB)"
+                       if args.workload != "tgv_inviscid_8_p3" else "L2-resident (6.6 MB/vector)",
+                       "parallelism": f"replicas x{world}", "status_flags": status},
+            "e2e": {"value": e2e, "unit": "DOF-updates/s/stage",
+                    "h2d_bytes_per_step": 8 * dg.n_dofs, "d2h_bytes_per_step": 8 * dg.n_dofs,
+                    "path": "ph_set_state(host pinned) + ph_rk_step + ph_get_state(host pinned) per step"},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "residual_kernel (stage: residual + mass inverse + RK update)",
+                         "kernel_ms": stage_ms, "aux_kernel_ms": aux_ms,
+                         "alg_bytes_per_dof": bpd, "peak_source": peak_src,
+                         "fp64_alg_flops_per_dof_stage": flops_per_dof_stage(p, viscous)},
+            "clocks": clk.summary(),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                line["cpu_baseline"] = cpu_baseline(args.workload)
+            except Exception as e:  # the checker must not hide a failure of the GPU arm
+                line["cpu_baseline"] = {"value": None, "error": str(e)}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -122,6 +122,15 @@ int ph_integrals(ph_ctx* ctx, double out[4]);
  * src/physics/euler.cpp:155-172). Reading clears it. */
 int ph_status(ph_ctx* ctx, uint32_t* flags);
 
+/* Measurement hooks (no counterpart in the reference, which times with dealii::Timer,
+ * src/flow_solver/flow_solver.cpp:690-711). With timing enabled every kernel launch is
+ * bracketed by CUDA events on the context stream and the stream is synchronised after
+ * it. out[0..5] = {stage-kernel ms, stage launches, auxiliary-kernel ms, auxiliary
+ * launches, other ms, other launches}, out[6] = kernel launches counted since the last
+ * ph_set_timing call (counted with timing enabled or not). */
+int ph_set_timing(ph_ctx* ctx, int enable);
+int ph_get_timing(ph_ctx* ctx, double out[7]);
+
 int ph_sync(ph_ctx* ctx);
 const char* ph_last_error(void);
 

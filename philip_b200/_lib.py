@@ -17,7 +17,7 @@ ERRORS = {1: "invalid argument", 2: "unsupported configuration", 3: "CUDA error"
 
 EXPORTED = ["ph_ctx_create", "ph_ctx_destroy", "ph_ndofs", "ph_cell_ijk", "ph_set_state", "ph_get_state",
             "ph_residual", "ph_apply_inverse_mass", "ph_rk_step", "ph_integrals", "ph_status", "ph_sync",
-            "ph_last_error"]
+            "ph_set_timing", "ph_get_timing", "ph_last_error"]
 
 
 class PhParams(ctypes.Structure):
@@ -67,6 +67,8 @@ def load(build_if_missing: bool = False):
     L.ph_integrals.argtypes = [vp, dp]
     L.ph_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32)]
     L.ph_sync.argtypes = [vp]
+    L.ph_set_timing.argtypes = [vp, ctypes.c_int]
+    L.ph_get_timing.argtypes = [vp, dp]
     L.ph_last_error.restype = ctypes.c_char_p
     _lib = L
     return L

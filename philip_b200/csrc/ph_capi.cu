@@ -184,19 +184,40 @@ struct ph_ctx {
     ph::OpTab* d_ops = nullptr;
     ph::IntegralTab* d_itab = nullptr;
     double *d_sol = nullptr, *d_stA = nullptr, *d_stB = nullptr, *d_acc = nullptr, *d_carry = nullptr;
-    double *d_q = nullptr, *d_comp = nullptr, *d_tmpA = nullptr, *d_tmpB = nullptr, *d_partial = nullptr;
+    double *d_fv = nullptr, *d_comp = nullptr, *d_tmpA = nullptr, *d_tmpB = nullptr, *d_partial = nullptr;
     unsigned* d_status = nullptr;
     ph::PhysConst pc{};
     double pen = 0.0;
     int ns = 0;
     double A[4][4] = {{0}}, b[4] = {0};
     std::vector<double> h_partial;
+    // optional per-kernel timing (CUDA events on the context stream)
+    bool timing = false;
+    double t_ms[3] = {0, 0, 0};      // residual/stage kernel, auxiliary kernel, other
+    long long t_n[3] = {0, 0, 0};
+    long long launches = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
 namespace {
 
+void timer_begin(ph_ctx* c) {
+    if (c->timing) cudaEventRecord(c->ev0, c->stream);
+}
+void timer_end(ph_ctx* c, int cls) {
+    ++c->launches;
+    if (!c->timing) return;
+    cudaEventRecord(c->ev1, c->stream);
+    cudaEventSynchronize(c->ev1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    c->t_ms[cls] += ms;
+    c->t_n[cls] += 1;
+}
+
 int dispatch_stage(ph_ctx* c, const ph::StageArgs& a) {
     cudaError_t e;
+    timer_begin(c);
     switch (c->N1) {
     case 2: e = ph::launch_stage<2>(a, c->fp32, c->visc, c->split, c->stream); break;
     case 3: e = ph::launch_stage<3>(a, c->fp32, c->visc, c->split, c->stream); break;
@@ -207,29 +228,32 @@ int dispatch_stage(ph_ctx* c, const ph::StageArgs& a) {
     default: return fail(PH_ERR_UNSUPPORTED, "polynomial degree outside 1..6");
     }
     if (e != cudaSuccess) return fail(PH_ERR_CUDA, std::string("residual launch: ") + cudaGetErrorString(e));
+    timer_end(c, 0);
     return PH_OK;
 }
 
 int dispatch_aux(ph_ctx* c, const double* U) {
     cudaError_t e;
     const double inv_h = 1.0 / c->h;
+    timer_begin(c);
     switch (c->N1) {
-    case 2: e = ph::launch_aux<2>(U, c->d_nbr, c->d_ops, c->nc, inv_h, c->d_q, c->stream); break;
-    case 3: e = ph::launch_aux<3>(U, c->d_nbr, c->d_ops, c->nc, inv_h, c->d_q, c->stream); break;
-    case 4: e = ph::launch_aux<4>(U, c->d_nbr, c->d_ops, c->nc, inv_h, c->d_q, c->stream); break;
-    case 5: e = ph::launch_aux<5>(U, c->d_nbr, c->d_ops, c->nc, inv_h, c->d_q, c->stream); break;
-    case 6: e = ph::launch_aux<6>(U, c->d_nbr, c->d_ops, c->nc, inv_h, c->d_q, c->stream); break;
-    case 7: e = ph::launch_aux<7>(U, c->d_nbr, c->d_ops, c->nc, inv_h, c->d_q, c->stream); break;
+    case 2: e = ph::launch_aux<2>(U, c->d_nbr, c->d_ops, c->nc, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
+    case 3: e = ph::launch_aux<3>(U, c->d_nbr, c->d_ops, c->nc, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
+    case 4: e = ph::launch_aux<4>(U, c->d_nbr, c->d_ops, c->nc, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
+    case 5: e = ph::launch_aux<5>(U, c->d_nbr, c->d_ops, c->nc, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
+    case 6: e = ph::launch_aux<6>(U, c->d_nbr, c->d_ops, c->nc, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
+    case 7: e = ph::launch_aux<7>(U, c->d_nbr, c->d_ops, c->nc, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
     default: return fail(PH_ERR_UNSUPPORTED, "polynomial degree outside 1..6");
     }
     if (e != cudaSuccess) return fail(PH_ERR_CUDA, std::string("aux launch: ") + cudaGetErrorString(e));
+    timer_end(c, 1);
     return PH_OK;
 }
 
 ph::StageArgs base_args(ph_ctx* c, const double* U) {
     ph::StageArgs a;
     std::memset(&a, 0, sizeof(a));
-    a.U = U; a.Q = c->d_q; a.nbr = c->d_nbr; a.ops = c->d_ops; a.nc = c->nc;
+    a.U = U; a.Fv = c->d_fv; a.nbr = c->d_nbr; a.ops = c->d_ops; a.nc = c->nc;
     a.h = c->h; a.inv_h = 1.0 / c->h; a.pen = c->pen; a.pc = c->pc; a.status = c->d_status;
     a.fr = c->fr ? 1 : 0;
     return a;
@@ -383,7 +407,7 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
     bad |= dalloc(&c->d_stB, N);
     bad |= dalloc(&c->d_acc, N);
     if (c->ns == 3) bad |= dalloc(&c->d_carry, N);
-    if (c->visc) bad |= dalloc(&c->d_q, 3 * N);
+    if (c->visc) bad |= dalloc(&c->d_fv, (size_t)12 * c->nc * c->NP);   // viscous flux scratch
     if (c->fp32) bad |= dalloc(&c->d_comp, N);
     bad |= dalloc(&c->d_partial, 3 * (size_t)c->nc);
     bad |= dalloc(&c->d_status, 1);
@@ -404,8 +428,10 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
 int ph_ctx_destroy(ph_ctx* c) {
     if (!c) return PH_OK;
     void* ptrs[] = {c->d_nbr, c->d_ops, c->d_itab, c->d_sol, c->d_stA, c->d_stB, c->d_acc, c->d_carry,
-                    c->d_q, c->d_comp, c->d_tmpA, c->d_tmpB, c->d_partial, c->d_status};
+                    c->d_fv, c->d_comp, c->d_tmpA, c->d_tmpB, c->d_partial, c->d_status};
     for (void* p : ptrs) if (p) cudaFree(p);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
     delete c;
     return PH_OK;
 }
@@ -566,6 +592,25 @@ int ph_status(ph_ctx* c, uint32_t* flags) {
     PH_CUDA(cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->stream));
     PH_CUDA(cudaStreamSynchronize(c->stream));
     *flags = v;
+    return PH_OK;
+}
+
+int ph_set_timing(ph_ctx* c, int enable) {
+    if (!c) return fail(PH_ERR_INVALID, "null argument");
+    if (enable && !c->ev0) {
+        PH_CUDA(cudaEventCreate(&c->ev0));
+        PH_CUDA(cudaEventCreate(&c->ev1));
+    }
+    c->timing = enable != 0;
+    for (int i = 0; i < 3; ++i) { c->t_ms[i] = 0.0; c->t_n[i] = 0; }
+    c->launches = 0;
+    return PH_OK;
+}
+
+int ph_get_timing(ph_ctx* c, double out[7]) {
+    if (!c || !out) return fail(PH_ERR_INVALID, "null argument");
+    for (int i = 0; i < 3; ++i) { out[2 * i] = c->t_ms[i]; out[2 * i + 1] = (double)c->t_n[i]; }
+    out[6] = (double)c->launches;
     return PH_OK;
 }
 

@@ -10,11 +10,11 @@ namespace ph {
 
 template <int N1> constexpr int cells_per_cta() { return N1 == 2 ? 16 : N1 == 3 ? 4 : N1 == 4 ? 2 : 1; }
 
-template <typename R, int N1, bool VISC, bool SPLIT>
+template <typename R, int N1, bool VISC, bool SPLIT, int FS>
 static cudaError_t launch_one(const StageArgs& a, cudaStream_t s) {
     constexpr int CPC = cells_per_cta<N1>();
     using L = Layout<R, N1, CPC, VISC, SPLIT>;
-    auto kern = residual_kernel<R, N1, CPC, VISC, SPLIT>;
+    auto kern = residual_kernel<R, N1, CPC, VISC, SPLIT, FS>;
     int dev = 0;
     cudaGetDevice(&dev);
     static bool configured[64] = {false};
@@ -28,18 +28,26 @@ static cudaError_t launch_one(const StageArgs& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+template <typename R, int N1>
+static cudaError_t launch_prec(const StageArgs& a, bool visc, bool split, cudaStream_t s) {
+    // the Chandrashekar + EC/Roe (+ BR2) combination has its own compile-time instance
+    const bool hot = split && a.pc.two_point == TP_CH && a.pc.conv_flux == CF_EC_ROE &&
+                     (!visc || a.pc.diss_flux == DF_BR2);
+    if (visc) {
+        if (split) return hot ? launch_one<R, N1, true, true, 1>(a, s) : launch_one<R, N1, true, true, 0>(a, s);
+        return launch_one<R, N1, true, false, 0>(a, s);
+    }
+    if (split) return hot ? launch_one<R, N1, false, true, 1>(a, s) : launch_one<R, N1, false, true, 0>(a, s);
+    return launch_one<R, N1, false, false, 0>(a, s);
+}
+
 template <int N1>
 cudaError_t launch_stage(const StageArgs& a, int fp32, bool visc, bool split, cudaStream_t s) {
-    if (fp32) {
-        if (visc) return split ? launch_one<float, N1, true, true>(a, s) : launch_one<float, N1, true, false>(a, s);
-        return split ? launch_one<float, N1, false, true>(a, s) : launch_one<float, N1, false, false>(a, s);
-    }
-    if (visc) return split ? launch_one<double, N1, true, true>(a, s) : launch_one<double, N1, true, false>(a, s);
-    return split ? launch_one<double, N1, false, true>(a, s) : launch_one<double, N1, false, false>(a, s);
+    return fp32 ? launch_prec<float, N1>(a, visc, split, s) : launch_prec<double, N1>(a, visc, split, s);
 }
 
 template <typename R, int N1, bool VISC, bool SPLIT>
-static void shape_one(int* threads, int* cpc, size_t* smem) {
+static void shape_one(int* threads, int* cpc, size_t* smem) {  // same shape for every flux set
     constexpr int CPC = cells_per_cta<N1>();
     using L = Layout<R, N1, CPC, VISC, SPLIT>;
     *threads = L::NT; *cpc = CPC; *smem = L::bytes;
@@ -56,22 +64,30 @@ void stage_launch_shape(int fp32, bool visc, bool split, int* threads, int* cpc,
     }
 }
 
-template <int N1>
-cudaError_t launch_aux(const double* U, const int* nbr, const OpTab* ops, int nc, double inv_h, double* Q,
-                       cudaStream_t s) {
+template <typename R, int N1>
+static cudaError_t launch_aux_prec(const double* U, const int* nbr, const OpTab* ops, int nc, double inv_h,
+                                   const PhysConst& pc, double* Fv, cudaStream_t s) {
     constexpr int CPC = cells_per_cta<N1>();
     using L = AuxLayout<N1, CPC>;
-    auto kern = aux_kernel<N1, CPC>;
+    constexpr size_t bytes = L::template bytes<R>();
+    auto kern = aux_kernel<R, N1, CPC>;
     int dev = 0;
     cudaGetDevice(&dev);
     static bool configured[64] = {false};
     if (dev < 64 && !configured[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::bytes);
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         if (e != cudaSuccess) return e;
         configured[dev] = true;
     }
-    kern<<<(nc + CPC - 1) / CPC, L::NT, L::bytes, s>>>(U, nbr, ops, nc, inv_h, Q);
+    kern<<<(nc + CPC - 1) / CPC, L::NT, bytes, s>>>(U, nbr, ops, nc, inv_h, pc, Fv);
     return cudaGetLastError();
+}
+
+template <int N1>
+cudaError_t launch_aux(const double* U, const int* nbr, const OpTab* ops, int nc, double inv_h,
+                       const PhysConst& pc, int fp32, double* Fv, cudaStream_t s) {
+    return fp32 ? launch_aux_prec<float, N1>(U, nbr, ops, nc, inv_h, pc, Fv, s)
+                : launch_aux_prec<double, N1>(U, nbr, ops, nc, inv_h, pc, Fv, s);
 }
 
 template <int N1>
@@ -100,7 +116,8 @@ cudaError_t launch_integrals(const double* U, const IntegralTab* tab, int nc, do
 
 template cudaError_t launch_stage<PH_N1>(const StageArgs&, int, bool, bool, cudaStream_t);
 template void stage_launch_shape<PH_N1>(int, bool, bool, int*, int*, size_t*);
-template cudaError_t launch_aux<PH_N1>(const double*, const int*, const OpTab*, int, double, double*, cudaStream_t);
+template cudaError_t launch_aux<PH_N1>(const double*, const int*, const OpTab*, int, double, const PhysConst&, int,
+                                       double*, cudaStream_t);
 template cudaError_t launch_inverse_mass<PH_N1>(const double*, double*, const OpTab*, int, double, cudaStream_t);
 template cudaError_t launch_integrals<PH_N1>(const double*, const IntegralTab*, int, double, double, double, double*,
                                              cudaStream_t);

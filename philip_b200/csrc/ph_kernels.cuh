@@ -23,6 +23,10 @@
 #pragma once
 #include "ph_physics.cuh"
 
+#ifndef PH_P5_MINB
+#define PH_P5_MINB 3
+#endif
+
 namespace ph {
 
 constexpr int MAXN1 = 8;
@@ -38,7 +42,7 @@ struct OpTab {
 
 struct StageArgs {
     const double* U;          // stage input state [nc][5][NP]
-    const double* Q;          // auxiliary gradient [nc][3][5][NP] (viscous)
+    const double* Fv;         // viscous flux [nc][3 dirs x 4][NP] from the auxiliary kernel (viscous)
     const int* nbr;           // [nc][6] neighbour cell per face
     const OpTab* ops;
     int nc;
@@ -84,6 +88,8 @@ struct Layout {
     static constexpr int SPW = 32 / N1;                // lines per warp
     static constexpr int WARPS_LINES = (CPC * NF + SPW - 1) / SPW;
     static constexpr int NT = WARPS_LINES * 32;
+    // p = 5 tiles are one cell per CTA: ask for PH_P5_MINB resident CTAs per SM
+    static constexpr int MINB = (N1 == 6) ? PH_P5_MINB : 1;
 };
 
 template <int N1> __device__ __forceinline__ int node_of(int x, int y, int z) { return (z * N1 + y) * N1 + x; }
@@ -103,6 +109,27 @@ __device__ __forceinline__ void store_q(R* sD, int NP, int idx, const NodeQ<R>& 
     sD[4 * NP + idx] = q.p; sD[5 * NP + idx] = q.E; sD[6 * NP + idx] = q.a; sD[7 * NP + idx] = q.b;
     sD[8 * NP + idx] = q.la; sD[9 * NP + idx] = q.lb; sD[10 * NP + idx] = q.vsq;
 }
+// Node quantities with the velocity expressed in the frame (e_d, e_{d+1}, e_{d+2}):
+// every flux along direction d is then evaluated by the x-direction code.
+template <typename R>
+__device__ __forceinline__ void load_q_rot(const R* sD, int NP, int idx, int d, NodeQ<R>& q) {
+    const int d1 = (d + 1) % 3, d2 = (d + 2) % 3;
+    q.rho = sD[0 * NP + idx]; q.v[0] = sD[(1 + d) * NP + idx]; q.v[1] = sD[(1 + d1) * NP + idx];
+    q.v[2] = sD[(1 + d2) * NP + idx];
+    q.p = sD[4 * NP + idx]; q.E = sD[5 * NP + idx]; q.a = sD[6 * NP + idx]; q.b = sD[7 * NP + idx];
+    q.la = sD[8 * NP + idx]; q.lb = sD[9 * NP + idx]; q.vsq = sD[10 * NP + idx];
+}
+template <typename R>
+__device__ __forceinline__ void rotate_state(const R u[5], int d, R r[5]) {
+    r[0] = u[0]; r[1] = u[1 + d]; r[2] = u[1 + (d + 1) % 3]; r[3] = u[1 + (d + 2) % 3]; r[4] = u[4];
+}
+// back from the rotated frame: F (rotated components) -> out (x, y, z components)
+template <typename R>
+__device__ __forceinline__ void unrotate_flux(const R F[5], int d, R out[5]) {
+    out[0] = F[0]; out[4] = F[4];
+    out[1 + d] = F[1]; out[1 + (d + 1) % 3] = F[2]; out[1 + (d + 2) % 3] = F[3];
+}
+
 template <typename R>
 __device__ __forceinline__ void load_q(const R* sD, int NP, int idx, NodeQ<R>& q) {
     q.rho = sD[0 * NP + idx]; q.v[0] = sD[1 * NP + idx]; q.v[1] = sD[2 * NP + idx]; q.v[2] = sD[3 * NP + idx];
@@ -120,13 +147,15 @@ __device__ __forceinline__ void check_state_fp64(double u[5], double gm1, unsign
 }
 
 // One face node of phase 3: the numerical flux at the canonical orientation (the
-// left cell is the interior side, normal +e_D) lifted into this cell with its sign.
-template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int D>
+// left cell is the interior side, normal +e_d) lifted into this cell with its sign.
+// The convective flux is evaluated in the frame whose x axis is the face normal.
+template <typename R, int N1, int CPC, bool VISC, bool SPLIT>
 __device__ __forceinline__ void face_item(const Cst<R>& cst, int tp, int cf, int df, int ucv, const R* sU,
                                           const R* sD, R* sT, const R* sX, int c, int f, int fn, R pen,
                                           R inv_wend) {
     using L = Layout<R, N1, CPC, VISC, SPLIT>;
     constexpr int NP = L::NP, NF = L::NF, TR = L::TR, NQS = L::NQS;
+    const int d = f >> 1;
     const bool plus = (f & 1);                    // this cell is the left (minus) side
     const R sgn = plus ? R(1) : R(-1);
     const int node = face_node_volume_index<N1>(f, fn, plus ? N1 - 1 : 0);
@@ -134,12 +163,16 @@ __device__ __forceinline__ void face_item(const Cst<R>& cst, int tp, int cf, int
     R uo[5], ue[5];
 #pragma unroll
     for (int s = 0; s < 5; ++s) { uo[s] = sU[(c * 5 + s) * NP + node]; ue[s] = tr[s * NF + fn]; }
+    R ro[5], re[5];
+    rotate_state<R>(uo, d, ro);
+    rotate_state<R>(ue, d, re);
     NodeQ<R> qo, qe;
-    load_q<R>(sD + c * NQS * NP, NP, node, qo);
-    node_prepare<R>(ue, tp, cst.gm1, qe, nullptr);
-    R Fs[5];
-    if (plus) conv_num_flux<R, D>(uo, ue, qo, qe, tp, cf, cst, Fs);
-    else conv_num_flux<R, D>(ue, uo, qe, qo, tp, cf, cst, Fs);
+    load_q_rot<R>(sD + c * NQS * NP, NP, node, d, qo);
+    node_prepare<R>(re, tp, cst.gm1, qe, nullptr);
+    R Fr[5], Fs[5];
+    if (plus) conv_num_flux<R, 0>(ro, re, qo, qe, tp, cf, cst, Fr);
+    else conv_num_flux<R, 0>(re, ro, qe, qo, tp, cf, cst, Fr);
+    unrotate_flux<R>(Fr, d, Fs);
     R term[5];
 #pragma unroll
     for (int s = 0; s < 5; ++s) term[s] = -sgn * Fs[s];
@@ -147,13 +180,13 @@ __device__ __forceinline__ void face_item(const Cst<R>& cst, int tp, int cf, int
     if constexpr (!SPLIT) {
         constexpr int o = VISC ? 12 : 0;
 #pragma unroll
-        for (int s = 0; s < 5; ++s) term[s] += sgn * X[(o + D * 5 + s) * NP + node];
+        for (int s = 0; s < 5; ++s) term[s] += sgn * X[(o + d * 5 + s) * NP + node];
     }
     if constexpr (VISC) {
         R Fo[4], Fn[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            Fo[k] = X[(D * 4 + k) * NP + node];
+            Fo[k] = X[(d * 4 + k) * NP + node];
             Fn[k] = R(0.5) * (Fo[k] + tr[(5 + k) * NF + fn]);
         }
         if (df == DF_SIPG) {
@@ -163,12 +196,16 @@ __device__ __forceinline__ void face_item(const Cst<R>& cst, int tp, int cf, int
 #pragma unroll
             for (int s = 0; s < 5; ++s)
 #pragma unroll
-                for (int k = 0; k < 3; ++k) gj[s][k] = (k == D) ? (uL[s] - uR[s]) : R(0);
+                for (int k = 0; k < 3; ++k) gj[s][k] = (k == d) ? (uL[s] - uR[s]) : R(0);
             R AL[3][4], AR[3][4];
-            viscous_flux<R>(uL, gj, ucv, cst, AL, 1 << D, nullptr);
-            viscous_flux<R>(uR, gj, ucv, cst, AR, 1 << D, nullptr);
+            viscous_flux<R>(uL, gj, ucv, cst, AL, 7, nullptr);
+            viscous_flux<R>(uR, gj, ucv, cst, AR, 7, nullptr);
 #pragma unroll
-            for (int k = 0; k < 4; ++k) Fn[k] = Fn[k] - pen * (R(0.5) * (AL[D][k] + AR[D][k]));
+            for (int k = 0; k < 4; ++k) {
+                const R al = d == 0 ? AL[0][k] : d == 1 ? AL[1][k] : AL[2][k];
+                const R ar = d == 0 ? AR[0][k] : d == 1 ? AR[1][k] : AR[2][k];
+                Fn[k] = Fn[k] - pen * (R(0.5) * (al + ar));
+            }
         }
 #pragma unroll
         for (int k = 0; k < 4; ++k) term[1 + k] += sgn * (Fo[k] - Fn[k]);
@@ -177,58 +214,61 @@ __device__ __forceinline__ void face_item(const Cst<R>& cst, int tp, int cf, int
     for (int s = 0; s < 5; ++s) tr[s * NF + fn] = term[s] * inv_wend;
 }
 
-// Phase 4 for direction D: warp segments of N1 lanes own 1-D lines along D.
-template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int D>
-__device__ __forceinline__ void volume_dir(const Cst<R>& cst, int tp, const R* sD, const R* sX, R* sA,
+// Phase 4 for direction d: warp segments of N1 lanes own 1-D lines along d. The
+// two-point flux is evaluated in the frame whose x axis is e_d.
+template <typename R, int N1, int CPC, bool VISC, bool SPLIT>
+__device__ __forceinline__ void volume_dir(int d, const Cst<R>& cst, int tp, const R* sD, const R* sX, R* sA,
                                            const R* sOpsD, const R* sOpsDsk, int lc, int lt, int pos, int seg,
                                            bool lvalid) {
     using L = Layout<R, N1, CPC, VISC, SPLIT>;
     constexpr int NP = L::NP, NQS = L::NQS;
-    constexpr int st = (D == 0) ? 1 : (D == 1) ? N1 : N1 * N1;
-    constexpr int t1 = (D == 0) ? 1 : 0, t2 = (D == 2) ? 1 : 2;
+    const int st = (d == 0) ? 1 : (d == 1) ? N1 : N1 * N1;
+    const int t1 = (d == 0) ? 1 : 0, t2 = (d == 2) ? 1 : 2;
     int cc[3];
-    cc[D] = pos; cc[t1] = lt % N1; cc[t2] = lt / N1;
-    const int node = node_of<N1>(cc[0], cc[1], cc[2]);
+    cc[0] = cc[1] = cc[2] = 0;
+    cc[t1] = lt % N1; cc[t2] = lt / N1;
+    const int node = node_of<N1>(d == 0 ? pos : cc[0], d == 1 ? pos : cc[1], d == 2 ? pos : cc[2]);
     const int base = node - pos * st;
     R acc[5] = {R(0), R(0), R(0), R(0), R(0)};
     if constexpr (SPLIT) {
         const R* Dq = sD + lc * NQS * NP;
         NodeQ<R> qi;
-        load_q<R>(Dq, NP, node, qi);
+        load_q_rot<R>(Dq, NP, node, d, qi);
+        R accr[5] = {R(0), R(0), R(0), R(0), R(0)};
 #ifdef PH_ALL_ORDERED_PAIRS
-#pragma unroll
+#pragma unroll 1
         for (int l = 0; l < N1; ++l) {
             if (l == pos) continue;
             NodeQ<R> qj;
-            load_q<R>(Dq, NP, base + l * st, qj);
+            load_q_rot<R>(Dq, NP, base + l * st, d, qj);
             R F[5];
-            two_point_dir<R, D>(qi, qj, tp, cst, F);
+            two_point_dir<R, 0>(qi, qj, tp, cst, F);
             const R cj = sOpsDsk[pos * N1 + l];
 #pragma unroll
-            for (int s = 0; s < 5; ++s) acc[s] += cj * F[s];
+            for (int s = 0; s < 5; ++s) accr[s] += cj * F[s];
         }
 #else
         const int segbase = seg * N1;
-#pragma unroll
+#pragma unroll 1
         for (int k = 1; k <= N1 / 2; ++k) {
             const int jp = (pos + k) % N1;
             NodeQ<R> qj;
-            load_q<R>(Dq, NP, base + jp * st, qj);
+            load_q_rot<R>(Dq, NP, base + jp * st, d, qj);
             R F[5];
-            two_point_dir<R, D>(qi, qj, tp, cst, F);
+            two_point_dir<R, 0>(qi, qj, tp, cst, F);
             const R cj = sOpsDsk[pos * N1 + jp];
             const int src = segbase + (pos - k + N1) % N1;
             const R cr = sOpsDsk[pos * N1 + (pos - k + N1) % N1];
-            constexpr bool dup_possible = (N1 & 1) == 0;
-            const bool dup = dup_possible && (2 * k == N1);
+            const bool dup = ((N1 & 1) == 0) && (2 * k == N1);
 #pragma unroll
             for (int s = 0; s < 5; ++s) {
                 const R fr = __shfl_sync(0xffffffffu, F[s], src);
-                acc[s] += cj * F[s];
-                if (!dup) acc[s] += cr * fr;
+                accr[s] += cj * F[s];
+                if (!dup) accr[s] += cr * fr;
             }
         }
 #endif
+        unrotate_flux<R>(accr, d, acc);
     }
     if constexpr (VISC || !SPLIT) {
         const R* X = sX + lc * L::NX * NP;
@@ -238,12 +278,12 @@ __device__ __forceinline__ void volume_dir(const Cst<R>& cst, int tp, const R* s
             const R coef = sOpsD[pos * N1 + l];
             if constexpr (VISC) {
 #pragma unroll
-                for (int k = 0; k < 4; ++k) acc[1 + k] += coef * X[(D * 4 + k) * NP + nl];
+                for (int k = 0; k < 4; ++k) acc[1 + k] += coef * X[(d * 4 + k) * NP + nl];
             }
             if constexpr (!SPLIT) {
                 constexpr int o = VISC ? 12 : 0;
 #pragma unroll
-                for (int s = 0; s < 5; ++s) acc[s] += coef * X[(o + D * 5 + s) * NP + nl];
+                for (int s = 0; s < 5; ++s) acc[s] += coef * X[(o + d * 5 + s) * NP + nl];
             }
         }
     }
@@ -251,7 +291,7 @@ __device__ __forceinline__ void volume_dir(const Cst<R>& cst, int tp, const R* s
         R* A = sA + lc * 5 * NP;
 #pragma unroll
         for (int s = 0; s < 5; ++s) {
-            if (D == 0) A[s * NP + node] = acc[s];
+            if (d == 0) A[s * NP + node] = acc[s];
             else A[s * NP + node] += acc[s];
         }
     }
@@ -260,8 +300,12 @@ __device__ __forceinline__ void volume_dir(const Cst<R>& cst, int tp, const R* s
 // ------------------------------------------------------------------------------------
 // Residual (+ mass inverse + RK epilogue) kernel
 // ------------------------------------------------------------------------------------
-template <typename R, int N1, int CPC, bool VISC, bool SPLIT>
-__global__ void __launch_bounds__(Layout<R, N1, CPC, VISC, SPLIT>::NT)
+// FS selects the flux set: 0 = any (two-point / convective / dissipative types read at
+// run time), 1 = Chandrashekar split flux + entropy-conserving baseline with Roe
+// dissipation (+ BR2 when viscous) fixed at compile time, which removes the unused
+// variants from the instruction stream.
+template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int FS>
+__global__ void __launch_bounds__(Layout<R, N1, CPC, VISC, SPLIT>::NT, Layout<R, N1, CPC, VISC, SPLIT>::MINB)
 residual_kernel(const StageArgs a) {
     using L = Layout<R, N1, CPC, VISC, SPLIT>;
     constexpr int NP = L::NP, NF = L::NF, NT = L::NT, TR = L::TR, NQS = L::NQS;
@@ -278,7 +322,10 @@ residual_kernel(const StageArgs a) {
     R* sX = sm + L::oX;
 
     Cst<R> cst; cst.load(a.pc);
-    const int tp = a.pc.two_point, cf = a.pc.conv_flux, df = a.pc.diss_flux, ucv = a.pc.use_const_visc;
+    const int tp = FS == 1 ? (int)TP_CH : a.pc.two_point;
+    const int cf = FS == 1 ? (int)CF_EC_ROE : a.pc.conv_flux;
+    const int df = FS == 1 ? (int)DF_BR2 : a.pc.diss_flux;
+    const int ucv = a.pc.use_const_visc;
     const int tid = threadIdx.x;
     const int cell0 = blockIdx.x * CPC;
 
@@ -303,15 +350,8 @@ residual_kernel(const StageArgs a) {
         for (int s = 0; s < 5; ++s) { ue[s] = (R)__ldg(&a.U[((size_t)cn * 5 + s) * NP + nn]); tr[s * NF + fn] = ue[s]; }
         if constexpr (VISC) {
             const int d = f >> 1;
-            R ge[5][3];
 #pragma unroll
-            for (int k = 0; k < 3; ++k)
-#pragma unroll
-                for (int s = 0; s < 5; ++s) ge[s][k] = (R)__ldg(&a.Q[(((size_t)cn * 3 + k) * 5 + s) * NP + nn]);
-            R Fe[3][4];
-            viscous_flux<R>(ue, ge, ucv, cst, Fe, 1 << d, nullptr);
-#pragma unroll
-            for (int k = 0; k < 4; ++k) tr[(5 + k) * NF + fn] = Fe[d][k];
+            for (int k = 0; k < 4; ++k) tr[(5 + k) * NF + fn] = (R)__ldg(&a.Fv[((size_t)cn * 12 + d * 4 + k) * NP + nn]);
         }
     }
 
@@ -333,17 +373,8 @@ residual_kernel(const StageArgs a) {
         store_q<R>(sD + c * NQS * NP, NP, node, q);
         R* X = sX + c * L::NX * NP;
         if constexpr (VISC) {
-            R g[5][3];
 #pragma unroll
-            for (int d = 0; d < 3; ++d)
-#pragma unroll
-                for (int s = 0; s < 5; ++s) g[s][d] = (R)__ldg(&a.Q[(((size_t)cell * 3 + d) * 5 + s) * NP + node]);
-            R F[3][4];
-            viscous_flux<R>(u, g, ucv, cst, F, 7, nullptr);
-#pragma unroll
-            for (int d = 0; d < 3; ++d)
-#pragma unroll
-                for (int k = 0; k < 4; ++k) X[(d * 4 + k) * NP + node] = F[d][k];
+            for (int i = 0; i < 12; ++i) X[i * NP + node] = (R)__ldg(&a.Fv[((size_t)cell * 12 + i) * NP + node]);
         }
         if constexpr (!SPLIT) {
             constexpr int o = VISC ? 12 : 0;
@@ -369,11 +400,7 @@ residual_kernel(const StageArgs a) {
             const int fn = it % NF;
             const int f = (it / NF) % 6;
             const int c = it / (NF * 6);
-            switch (f >> 1) {
-            case 0: face_item<R, N1, CPC, VISC, SPLIT, 0>(cst, tp, cf, df, ucv, sU, sD, sT, sX, c, f, fn, pen, inv_wend); break;
-            case 1: face_item<R, N1, CPC, VISC, SPLIT, 1>(cst, tp, cf, df, ucv, sU, sD, sT, sX, c, f, fn, pen, inv_wend); break;
-            default: face_item<R, N1, CPC, VISC, SPLIT, 2>(cst, tp, cf, df, ucv, sU, sD, sT, sX, c, f, fn, pen, inv_wend); break;
-            }
+            face_item<R, N1, CPC, VISC, SPLIT>(cst, tp, cf, df, ucv, sU, sD, sT, sX, c, f, fn, pen, inv_wend);
         }
     }
 
@@ -386,12 +413,11 @@ residual_kernel(const StageArgs a) {
         const bool lvalid = (seg < SPW) && (line < CPC * NF);
         const int lc = lvalid ? line / NF : 0;
         const int lt = lvalid ? line % NF : 0;
-        __syncthreads();
-        volume_dir<R, N1, CPC, VISC, SPLIT, 0>(cst, tp, sD, sX, sA, sOpsD, sOpsDsk, lc, lt, pos, seg, lvalid);
-        __syncthreads();
-        volume_dir<R, N1, CPC, VISC, SPLIT, 1>(cst, tp, sD, sX, sA, sOpsD, sOpsDsk, lc, lt, pos, seg, lvalid);
-        __syncthreads();
-        volume_dir<R, N1, CPC, VISC, SPLIT, 2>(cst, tp, sD, sX, sA, sOpsD, sOpsDsk, lc, lt, pos, seg, lvalid);
+#pragma unroll 1
+        for (int d = 0; d < 3; ++d) {
+            __syncthreads();
+            volume_dir<R, N1, CPC, VISC, SPLIT>(d, cst, tp, sD, sX, sA, sOpsD, sOpsDsk, lc, lt, pos, seg, lvalid);
+        }
         __syncthreads();
     }
 
@@ -481,49 +507,58 @@ residual_kernel(const StageArgs a) {
 }
 
 // ------------------------------------------------------------------------------------
-// Auxiliary equation: lifted gradient q = M^{-1}[ vol grad + face (u* - u) n ] (kDG)
+// Auxiliary equation: lifted gradient q = M^{-1}[ vol grad + face (u* - u) n ] (kDG),
+// then the viscous flux F_v(u, q) at every node, which is all the stage kernel needs
+// (the split form evaluates it at the entropy-projected state, the nodal state for GLL).
 // ------------------------------------------------------------------------------------
 template <int N1, int CPC>
 struct AuxLayout {
     static constexpr int NP = N1 * N1 * N1, NF = N1 * N1;
     static constexpr int NT = ((CPC * NP + 31) / 32) * 32 > 512 ? 512 : ((CPC * NP + 31) / 32) * 32;
-    static constexpr size_t bytes = sizeof(double) * ((size_t)CPC * 5 * NP + (size_t)CPC * 6 * 5 * NF + N1 * N1 + N1);
+    template <typename R>
+    static constexpr size_t bytes() {
+        return sizeof(R) * ((size_t)CPC * 5 * NP + (size_t)CPC * 6 * 5 * NF + N1 * N1 + N1);
+    }
 };
 
-template <int N1, int CPC>
+template <typename R, int N1, int CPC>
 __global__ void __launch_bounds__(AuxLayout<N1, CPC>::NT)
 aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, const OpTab* ops, int nc,
-           double inv_h, double* __restrict__ Q) {
+           double inv_h, PhysConst pc, double* __restrict__ Fv) {
     using L = AuxLayout<N1, CPC>;
     constexpr int NP = L::NP, NF = L::NF, NT = L::NT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double* sU = reinterpret_cast<double*>(smem_raw);
-    double* sT = sU + CPC * 5 * NP;
-    double* sDm = sT + CPC * 6 * 5 * NF;
-    double* sW = sDm + N1 * N1;
+    R* sU = reinterpret_cast<R*>(smem_raw);
+    R* sT = sU + CPC * 5 * NP;
+    R* sDm = sT + CPC * 6 * 5 * NF;
+    R* sW = sDm + N1 * N1;
+    Cst<R> cst; cst.load(pc);
     const int tid = threadIdx.x;
     const int cell0 = blockIdx.x * CPC;
-    for (int i = tid; i < N1 * N1; i += NT) sDm[i] = ops->D[(i / N1) * MAXN1 + (i % N1)];
-    for (int i = tid; i < N1; i += NT) sW[i] = ops->w[i];
+    for (int i = tid; i < N1 * N1; i += NT) sDm[i] = (R)ops->D[(i / N1) * MAXN1 + (i % N1)];
+    for (int i = tid; i < N1; i += NT) sW[i] = (R)ops->w[i];
     for (int it = tid; it < CPC * 5 * NP; it += NT) {
         int cell = cell0 + it / (5 * NP); if (cell >= nc) cell = nc - 1;
-        sU[it] = __ldg(&U[(size_t)cell * 5 * NP + it % (5 * NP)]);
+        sU[it] = (R)__ldg(&U[(size_t)cell * 5 * NP + it % (5 * NP)]);
     }
     for (int it = tid; it < CPC * 6 * 5 * NF; it += NT) {
         const int fn = it % NF, s = (it / NF) % 5, f = (it / (5 * NF)) % 6, c = it / (30 * NF);
         int cell = cell0 + c; if (cell >= nc) cell = nc - 1;
         const int cn = __ldg(&nbr[cell * 6 + f]);
         const int nn = face_node_volume_index<N1>(f, fn, (f & 1) ? 0 : N1 - 1);
-        sT[it] = __ldg(&U[((size_t)cn * 5 + s) * NP + nn]);
+        sT[it] = (R)__ldg(&U[((size_t)cn * 5 + s) * NP + nn]);
     }
     __syncthreads();
-    const double inv_wend = 1.0 / sW[0];
+    const R inv_wend = R(1) / sW[0];
+    const R ih = (R)inv_h;
     for (int it = tid; it < CPC * NP; it += NT) {
         const int c = it / NP, node = it % NP;
         const int cell = cell0 + c;
         if (cell >= nc) continue;
         const int cx[3] = {node % N1, (node / N1) % N1, node / (N1 * N1)};
-        const double* u = sU + c * 5 * NP;
+        const R* u = sU + c * 5 * NP;
+        R g[5][3];
+#pragma unroll
         for (int d = 0; d < 3; ++d) {
             const int st = (d == 0) ? 1 : (d == 1) ? N1 : N1 * N1;
             const int pos = cx[d];
@@ -532,20 +567,29 @@ aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, const OpTa
             const int fn = cx[t2] * N1 + cx[t1];
 #pragma unroll
             for (int s = 0; s < 5; ++s) {
-                double g = 0.0;
+                R v = R(0);
 #pragma unroll
-                for (int l = 0; l < N1; ++l) g += sDm[pos * N1 + l] * u[s * NP + base + l * st];
+                for (int l = 0; l < N1; ++l) v += sDm[pos * N1 + l] * u[s * NP + base + l * st];
                 if (pos == 0) {
-                    const double ue = sT[((c * 6 + 2 * d) * 5 + s) * NF + fn];
-                    g += inv_wend * (-(0.5 * (u[s * NP + node] + ue) - u[s * NP + node]));
+                    const R ue = sT[((c * 6 + 2 * d) * 5 + s) * NF + fn];
+                    v += inv_wend * (-(R(0.5) * (u[s * NP + node] + ue) - u[s * NP + node]));
                 }
                 if (pos == N1 - 1) {
-                    const double ue = sT[((c * 6 + 2 * d + 1) * 5 + s) * NF + fn];
-                    g += inv_wend * ((0.5 * (u[s * NP + node] + ue) - u[s * NP + node]));
+                    const R ue = sT[((c * 6 + 2 * d + 1) * 5 + s) * NF + fn];
+                    v += inv_wend * ((R(0.5) * (u[s * NP + node] + ue) - u[s * NP + node]));
                 }
-                Q[(((size_t)cell * 3 + d) * 5 + s) * NP + node] = g * inv_h;
+                g[s][d] = v * ih;
             }
         }
+        R un[5];
+#pragma unroll
+        for (int s = 0; s < 5; ++s) un[s] = u[s * NP + node];
+        R F[3][4];
+        viscous_flux<R>(un, g, pc.use_const_visc, cst, F, 7, nullptr);
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) Fv[((size_t)cell * 12 + d * 4 + k) * NP + node] = (double)F[d][k];
     }
 }
 

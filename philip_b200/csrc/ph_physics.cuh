@@ -107,16 +107,20 @@ __device__ __forceinline__ void node_prepare(const R u[5], int tp, R gm1, NodeQ<
 // Logarithmic mean with the Ismail-Roe series branch (euler.cpp:628-646). The
 // logarithms of the two arguments are taken once per node, so the log of the ratio
 // is their difference; the branch test uses the reference's own ratio form.
+//
+// Division count: f = (a-b)/(a+b) equals the reference's (zeta-1)/(zeta+1) with
+// zeta = a/b up to rounding, the series is evaluated in Horner form with the constant
+// reciprocals, and (a+b) f / log(zeta) = (a-b)/(log a - log b); two divisions per call.
 template <typename R>
 __device__ __forceinline__ R log_mean(R a, R b, R la, R lb) {
-    const R zeta = a / b;
-    const R f = (zeta - R(1)) / (zeta + R(1));
+    const R s = a + b, d = a - b;
+    const R f = d / s;
     const R u = f * f;
     if (u < R(1.0e-2)) {
-        const R F = R(1) + u / R(3) + u * u / R(5) + u * u * u / R(7);
-        return (a + b) / (R(2) * F);
+        const R F = R(1) + u * (R(1.0 / 3.0) + u * (R(1.0 / 5.0) + u * R(1.0 / 7.0)));
+        return s / (R(2) * F);
     }
-    return (a - b) / (la - lb);
+    return d / (la - lb);
 }
 
 // Two-point flux component along direction d (compile time) for all 5 equations.
@@ -131,11 +135,14 @@ __device__ __forceinline__ void two_point_dir(const NodeQ<R>& i, const NodeQ<R>&
         for (int k = 0; k < 3; ++k) { va[k] = R(0.5) * (i.v[k] + j.v[k]); vsq += va[k] * va[k]; }
         R p_hat, H;
         if (tp == TP_CH) {
-            p_hat = R(0.5) * (i.rho + j.rho) / (R(2) * R(0.5) * (i.b + j.b));
-            H = R(1) / (R(2) * b_log * c.gm1) + vsq + p_hat / rho_log;
+            // 1/(2 b_log gm1) + p_hat/rho_log over one common denominator
+            p_hat = (i.rho + j.rho) / (R(2) * (i.b + j.b));
+            const R g2b = R(2) * b_log * c.gm1;
+            H = (rho_log + g2b * p_hat) / (g2b * rho_log) + vsq;
         } else {
             p_hat = R(0.5) * (i.p + j.p);
-            H = R(1) / (b_log * c.gm1) + vsq + R(2) * p_hat / rho_log;
+            const R gb = b_log * c.gm1;
+            H = (rho_log + R(2) * gb * p_hat) / (gb * rho_log) + vsq;
         }
         H -= R(0.5) * (R(0.5) * (i.vsq + j.vsq));
         const R m = rho_log * va[d];
@@ -300,7 +307,8 @@ __device__ __forceinline__ void viscous_flux(const R u[5], const R g[5][3], int 
         gp[k] = t * c.gm1;
     }
     const R T = c.gam * c.mach2 * (w[4] / rho);
-    R mu = use_const_visc ? c.const_visc : ((R(1) + c.temp_ratio) / (T + c.temp_ratio)) * rpow<R>(T, R(1.5));
+    // Sutherland's law mu = (1 + T_r)/(T + T_r) T^{3/2}, with T^{3/2} = T sqrt(T)
+    R mu = use_const_visc ? c.const_visc : ((R(1) + c.temp_ratio) / (T + c.temp_ratio)) * (T * rsqrt_<R>(T));
     mu = mu * c.inv_re;
     const R kappa = mu * c.kappa_fac;
     const R div = gv[0][0] + gv[1][1] + gv[2][2];

@@ -234,25 +234,44 @@ class FlowSolver:
         self.dg.solution = conservative_state(self.dg, prim)
         self.unsteady_data = []
 
+    def _grid_spacing(self) -> float:
+        left, right = self.parameters.grid_bounds
+        ndof_per_state = self.dg.n_dofs // 5
+        return (right - left) / ndof_per_state ** (1.0 / 3.0)
+
     def constant_time_step(self) -> float:
+        """PeriodicTurbulence::get_constant_time_step (periodic_turbulence.cpp:115-127)."""
         cst = float(self.parameters.get("flow_solver/constant_time_step"))
         if cst > 0.0:
             return cst
-        left, right = self.parameters.grid_bounds
-        ndof_per_state = self.dg.n_dofs // 5
-        return float(self.parameters.get("flow_solver/courant_friedrichs_lewy_number")) * \
-            (right - left) / ndof_per_state ** (1.0 / 3.0)
+        return float(self.parameters.get("flow_solver/courant_friedrichs_lewy_number")) * self._grid_spacing()
+
+    def adaptive_time_step(self) -> float:
+        """PeriodicTurbulence::get_adaptive_time_step (periodic_turbulence.cpp:361-369):
+        CFL x spacing / maximum convective wave speed (|v| + c) of the current state."""
+        wave = self.dg.integrals()[3]
+        return float(self.parameters.get("flow_solver/courant_friedrichs_lewy_number")) * self._grid_spacing() / wave
+
+    def time_step(self) -> float:
+        if self.parameters.get("flow_solver/adaptive_time_step").lower() == "true":
+            return self.adaptive_time_step()
+        return self.constant_time_step()
 
     def run(self, record_every: int = 1):
         final_time = float(self.parameters.get("flow_solver/final_time"))
         end_exact = self.parameters.get("flow_solver/end_exactly_at_final_time").lower() == "true"
-        dt = self.constant_time_step()
+        adaptive = self.parameters.get("flow_solver/adaptive_time_step").lower() == "true"
+        dt = self.time_step()
         self.unsteady_data.append((self.ode_solver.current_time, *self.dg.integrals()))
         while self.ode_solver.current_time < final_time:
             step = dt
             if self.ode_solver.current_time + step > final_time and end_exact:
                 step = final_time - self.ode_solver.current_time
             self.ode_solver.step_in_time(step)
-            if self.ode_solver.current_iteration % record_every == 0:
-                self.unsteady_data.append((self.ode_solver.current_time, *self.dg.integrals()))
+            if adaptive or self.ode_solver.current_iteration % record_every == 0:
+                q = self.dg.integrals()
+                self.unsteady_data.append((self.ode_solver.current_time, *q))
+                if adaptive:
+                    dt = float(self.parameters.get("flow_solver/courant_friedrichs_lewy_number")) * \
+                        self._grid_spacing() / q[3]
         return 0

@@ -105,3 +105,27 @@ def test_nonphysical_status_flag():
     dg.assemble_residual()
     assert dg.status() & 1
     assert dg.status() == 0   # reading clears it
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rk", ["rk4_ex", "ssprk3_ex"])
+@pytest.mark.parametrize("visc", [False, True])
+def test_multistep_parity_and_clean_status(rk, visc):
+    """Several steps at the TGV time step: the state follows the oracle and no
+    non-physical state is flagged."""
+    kw = dict(poly_degree=3, n_cells=4, rk=rk, pde="navier_stokes" if visc else "euler",
+              diss="bassi_rebay_2")
+    prm, orc, dg = _pair(kw)
+    U = orc.initial_condition("tgv")
+    dg.solution = U
+    dt = 0.1 * 6.28318530717958623200 / (4 * 4) / 11.0   # acoustic CFL 0.1 (|v| + c ~ 11)
+    ode = RungeKuttaODESolver(dg)
+    for step in range(6):
+        orc.rk_step(U, dt)
+        ode.step_in_time(dt)
+        st = dg.status()
+        Ug = dg.solution
+        err = rel_max_err(Ug, U)
+        print(f"{rk} visc={visc} step {step}: rel err {err:.3e} status {st}")
+        assert st == 0
+        assert err <= 1e-12
