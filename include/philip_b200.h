@@ -131,6 +131,11 @@ int ph_status(ph_ctx* ctx, uint32_t* flags);
 int ph_set_timing(ph_ctx* ctx, int enable);
 int ph_get_timing(ph_ctx* ctx, double out[7]);
 
+/* Self-test of the quotient used inside the flux kernels against IEEE division on n
+ * pseudo-random operand pairs; out[0] = max relative error in FP64, out[1] in FP32.
+ * No counterpart in the reference. */
+int ph_quotient_selftest(uint64_t seed, int n, double out[2]);
+
 int ph_sync(ph_ctx* ctx);
 const char* ph_last_error(void);
 

@@ -614,6 +614,22 @@ int ph_get_timing(ph_ctx* c, double out[7]) {
     return PH_OK;
 }
 
+int ph_quotient_selftest(uint64_t seed, int n, double out[2]) {
+    if (n <= 0 || !out) return fail(PH_ERR_INVALID, "bad argument");
+    const int blocks = (n + 255) / 256;
+    double* d = nullptr;
+    PH_CUDA(cudaMalloc(&d, 2 * (size_t)blocks * sizeof(double)));
+    ph::quotient_selftest_kernel<<<blocks, 256>>>(seed, n, d);
+    cudaError_t e = cudaGetLastError();
+    std::vector<double> h(2 * (size_t)blocks);
+    if (e == cudaSuccess) e = cudaMemcpy(h.data(), d, h.size() * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(PH_ERR_CUDA, cudaGetErrorString(e));
+    out[0] = out[1] = 0.0;
+    for (int b = 0; b < blocks; ++b) { out[0] = std::max(out[0], h[2 * b]); out[1] = std::max(out[1], h[2 * b + 1]); }
+    return PH_OK;
+}
+
 int ph_sync(ph_ctx* c) {
     if (!c) return fail(PH_ERR_INVALID, "null argument");
     PH_CUDA(cudaStreamSynchronize(c->stream));

@@ -594,6 +594,43 @@ aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, const OpTa
 }
 
 // ------------------------------------------------------------------------------------
+// Self-test of the flux quotient against IEEE division on pseudo-random operands
+// (one thread per sample, operands from a 64-bit LCG; out[0/1] = max relative error
+// in FP64 / FP32 over this block, reduced by the host).
+// ------------------------------------------------------------------------------------
+static __global__ void quotient_selftest_kernel(unsigned long long seed, int n, double* out) {
+    __shared__ double m64[256];
+    __shared__ double m32[256];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double e64 = 0.0, e32 = 0.0;
+    if (i < n) {
+        unsigned long long s = seed + 0x9E3779B97F4A7C15ull * (unsigned long long)(i + 1);
+        s = s * 6364136223846793005ull + 1442695040888963407ull;
+        const double u = (double)(s >> 11) * (1.0 / 9007199254740992.0);
+        s = s * 6364136223846793005ull + 1442695040888963407ull;
+        const double v = (double)(s >> 11) * (1.0 / 9007199254740992.0);
+        const double a = (u - 0.5) * exp2(40.0 * v - 20.0);
+        const double b = (v + 0.01) * exp2(40.0 * u - 20.0) * ((s >> 3) & 1 ? 1.0 : -1.0);
+        const double q = a / b, qq = qdiv<double>(a, b);
+        e64 = q != 0.0 ? fabs(qq - q) / fabs(q) : 0.0;
+        const float af = (float)a, bf = (float)b;
+        const float qf = af / bf, qqf = qdiv<float>(af, bf);
+        e32 = qf != 0.0f ? fabs((double)qqf - (double)qf) / fabs((double)qf) : 0.0;
+    }
+    m64[threadIdx.x] = e64;
+    m32[threadIdx.x] = e32;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            m64[threadIdx.x] = fmax(m64[threadIdx.x], m64[threadIdx.x + o]);
+            m32[threadIdx.x] = fmax(m32[threadIdx.x], m32[threadIdx.x + o]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { out[2 * blockIdx.x] = m64[0]; out[2 * blockIdx.x + 1] = m32[0]; }
+}
+
+// ------------------------------------------------------------------------------------
 // Inverse mass on its own (DGBase::apply_inverse_global_mass_matrix, affine cells)
 // ------------------------------------------------------------------------------------
 template <int N1>

@@ -51,6 +51,44 @@ template <> __device__ __forceinline__ double rpow<double>(double x, double y) {
 template <> __device__ __forceinline__ float rpow<float>(float x, float y) { return powf(x, y); }
 template <typename R> __device__ __forceinline__ R rabs(R x) { return x < R(0) ? -x : x; }
 
+// Quotient used inside the flux functions. PH_FAST_DIV=0: IEEE division. Otherwise the
+// numerator times the hardware approximate reciprocal (PTX rcp.approx.ftz.f64/.f32,
+// relative error about 1e-6 in FP64) refined by Newton-Raphson steps
+// r <- r + r (1 - b r), each of which squares the relative error: two steps in FP64
+// (about 2 ulp, measured against IEEE division in tests/test_gpu_quotient.py), none
+// in FP32 (the f32 approximation is within about 1 ulp already).
+#ifndef PH_FAST_DIV
+#define PH_FAST_DIV 1
+#endif
+__device__ __forceinline__ double rcp_approx(double x) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    return r;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+template <typename R> __device__ __forceinline__ R qdiv(R a, R b);
+template <> __device__ __forceinline__ double qdiv<double>(double a, double b) {
+#if PH_FAST_DIV == 0
+    return a / b;
+#else
+    double r = rcp_approx(b);
+    r = fma(r, fma(-b, r, 1.0), r);
+    r = fma(r, fma(-b, r, 1.0), r);
+    return a * r;
+#endif
+}
+template <> __device__ __forceinline__ float qdiv<float>(float a, float b) {
+#if PH_FAST_DIV == 0
+    return a / b;
+#else
+    return a * rcp_approx(b);
+#endif
+}
+
 // Non-physical handling: a negative density/pressure sets a status bit and is
 // replaced by BIG_NUMBER, as check_positive_quantity does (euler.cpp:155-172).
 template <typename R> __device__ __forceinline__ R positive(R q, unsigned* status) {
@@ -65,7 +103,7 @@ template <typename R> __device__ __forceinline__ R pressure(const R u[5], R gm1,
     const R rho = u[0];
     R v2 = R(0);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) { const R v = u[1 + d] / rho; v2 = v2 + v * v; }
+    for (int d = 0; d < 3; ++d) { const R v = qdiv<R>(u[1 + d], rho); v2 = v2 + v * v; }
     return positive<R>(gm1 * (u[4] - R(0.5) * rho * v2), st);
 }
 
@@ -81,26 +119,26 @@ __device__ __forceinline__ void node_prepare(const R u[5], int tp, R gm1, NodeQ<
     q.rho = u[0];
     R v2 = R(0);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) { q.v[d] = u[1 + d] / u[0]; v2 = v2 + q.v[d] * q.v[d]; }
+    for (int d = 0; d < 3; ++d) { q.v[d] = qdiv<R>(u[1 + d], u[0]); v2 = v2 + q.v[d] * q.v[d]; }
     q.E = u[4];
     q.p = positive<R>(gm1 * (u[4] - R(0.5) * u[0] * v2), st);
     if (tp == TP_CH) {
-        q.a = q.rho; q.b = q.rho / (R(2) * q.p);
+        q.a = q.rho; q.b = qdiv<R>(q.rho, R(2) * q.p);
         q.la = rlog<R>(q.a); q.lb = rlog<R>(q.b);
         q.vsq = q.v[0] * q.v[0] + q.v[1] * q.v[1] + q.v[2] * q.v[2];
     } else if (tp == TP_RA) {
-        q.a = q.rho; q.b = q.rho / q.p;
+        q.a = q.rho; q.b = qdiv<R>(q.rho, q.p);
         q.la = rlog<R>(q.a); q.lb = rlog<R>(q.b);
         q.vsq = q.v[0] * q.v[0] + q.v[1] * q.v[1] + q.v[2] * q.v[2];
     } else if (tp == TP_IR) {
         const R rho = positive<R>(q.rho, st);
-        q.a = rsqrt_<R>(rho / q.p);      // z_0
+        q.a = rsqrt_<R>(qdiv<R>(rho, q.p));      // z_0
         q.b = rsqrt_<R>(rho * q.p);      // z_4
         q.la = rlog<R>(q.a); q.lb = rlog<R>(q.b);
         q.vsq = R(0);
     } else {   // KG
         q.a = q.b = q.la = q.lb = R(0);
-        q.vsq = q.E / q.rho;
+        q.vsq = qdiv<R>(q.E, q.rho);
     }
 }
 
@@ -114,13 +152,13 @@ __device__ __forceinline__ void node_prepare(const R u[5], int tp, R gm1, NodeQ<
 template <typename R>
 __device__ __forceinline__ R log_mean(R a, R b, R la, R lb) {
     const R s = a + b, d = a - b;
-    const R f = d / s;
+    const R f = qdiv<R>(d, s);
     const R u = f * f;
     if (u < R(1.0e-2)) {
         const R F = R(1) + u * (R(1.0 / 3.0) + u * (R(1.0 / 5.0) + u * R(1.0 / 7.0)));
-        return s / (R(2) * F);
+        return qdiv<R>(s, R(2) * F);
     }
-    return d / (la - lb);
+    return qdiv<R>(d, la - lb);
 }
 
 // Two-point flux component along direction d (compile time) for all 5 equations.
@@ -136,13 +174,13 @@ __device__ __forceinline__ void two_point_dir(const NodeQ<R>& i, const NodeQ<R>&
         R p_hat, H;
         if (tp == TP_CH) {
             // 1/(2 b_log gm1) + p_hat/rho_log over one common denominator
-            p_hat = (i.rho + j.rho) / (R(2) * (i.b + j.b));
+            p_hat = qdiv<R>(i.rho + j.rho, R(2) * (i.b + j.b));
             const R g2b = R(2) * b_log * c.gm1;
-            H = (rho_log + g2b * p_hat) / (g2b * rho_log) + vsq;
+            H = qdiv<R>(rho_log + g2b * p_hat, g2b * rho_log) + vsq;
         } else {
             p_hat = R(0.5) * (i.p + j.p);
             const R gb = b_log * c.gm1;
-            H = (rho_log + R(2) * gb * p_hat) / (gb * rho_log) + vsq;
+            H = qdiv<R>(rho_log + R(2) * gb * p_hat, gb * rho_log) + vsq;
         }
         H -= R(0.5) * (R(0.5) * (i.vsq + j.vsq));
         const R m = rho_log * va[d];
@@ -161,12 +199,12 @@ __device__ __forceinline__ void two_point_dir(const NodeQ<R>& i, const NodeQ<R>&
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             const R zk = R(0.5) * (i.a * i.v[k] + j.a * j.v[k]);
-            v[k] = zk / z0a; vv += v[k] * v[k];
+            v[k] = qdiv<R>(zk, z0a); vv += v[k] * v[k];
         }
-        const R p = z4a / z0a;
-        R H = (c.gam + R(1)) * (l4 / l0) + c.gm1 * p;
+        const R p = qdiv<R>(z4a, z0a);
+        R H = (c.gam + R(1)) * qdiv<R>(l4, l0) + c.gm1 * p;
         H /= R(2) * c.gam;
-        H *= c.gam / (rho * c.gm1);
+        H *= qdiv<R>(c.gam, rho * c.gm1);
         H += R(0.5) * vv;
         const R m = rho * v[d];
         F[0] = m;
@@ -193,7 +231,7 @@ __device__ __forceinline__ void two_point_dir(const NodeQ<R>& i, const NodeQ<R>&
 // Physical convective flux along direction d.
 template <typename R, int d>
 __device__ __forceinline__ void conv_flux_dir(const NodeQ<R>& q, R F[5]) {
-    const R H = q.E / q.rho + q.p / q.rho;
+    const R H = qdiv<R>(q.E, q.rho) + qdiv<R>(q.p, q.rho);
     const R m = q.rho * q.v[d];
     F[0] = m;
 #pragma unroll
@@ -208,35 +246,36 @@ __device__ __forceinline__ void roe_dissipation(const NodeQ<R>& L, const NodeQ<R
                                                 const Cst<R>& c, R out[5]) {
     const R n[3] = {R(d == 0), R(d == 1), R(d == 2)};
     const R vnL = L.v[d], vnR = Rq.v[d];
-    const R hL = (L.E + L.p) / L.rho, hR = (Rq.E + Rq.p) / Rq.rho;
-    const R r = rsqrt_<R>(Rq.rho / L.rho), rp1 = r + R(1);
+    const R hL = qdiv<R>(L.E + L.p, L.rho), hR = qdiv<R>(Rq.E + Rq.p, Rq.rho);
+    const R r = rsqrt_<R>(qdiv<R>(Rq.rho, L.rho)), rp1 = r + R(1);
     const R rho_a = r * L.rho;
     R va[3], v2a = R(0);
 #pragma unroll
-    for (int k = 0; k < 3; ++k) { va[k] = (r * Rq.v[k] + L.v[k]) / rp1; v2a = v2a + va[k] * va[k]; }
-    const R ha = (r * hR + hL) / rp1;
+    for (int k = 0; k < 3; ++k) { va[k] = qdiv<R>(r * Rq.v[k] + L.v[k], rp1); v2a = v2a + va[k] * va[k]; }
+    const R ha = qdiv<R>(r * hR + hL, rp1);
     const R vna = va[d];
     const R c2a = c.gm1 * (ha - R(0.5) * v2a);
     R ca = R(1e10);
     if (c2a > R(0)) ca = rsqrt_<R>(c2a);
     R eig[3] = {rabs(vna - ca), rabs(vna), rabs(vna + ca)};
-    const R cL = rsqrt_<R>(L.p * c.gam / L.rho), cR = rsqrt_<R>(Rq.p * c.gam / Rq.rho);
+    const R cL = rsqrt_<R>(qdiv<R>(L.p * c.gam, L.rho)), cR = rsqrt_<R>(qdiv<R>(Rq.p * c.gam, Rq.rho));
     const R eL[3] = {rabs(vnL - cL), rabs(vnL), rabs(vnL + cL)};
     const R eR[3] = {rabs(vnR - cR), rabs(vnR), rabs(vnR + cR)};
 #pragma unroll
     for (int e = 0; e < 3; ++e) {
         const R a1 = rabs(eig[e] - eL[e]), a2 = rabs(eR[e] - eig[e]);
         const R eps = a1 > a2 ? a1 : a2;
-        if (eig[e] < eps) eig[e] = R(0.5) * (eig[e] * eig[e] / eps + eps);
+        if (eig[e] < eps) eig[e] = R(0.5) * (qdiv<R>(eig[e] * eig[e], eps) + eps);
     }
     const R dp = Rq.p - L.p, drho = Rq.rho - L.rho, dvn = vnR - vnL;
     R dvt[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) dvt[k] = (Rq.v[k] - L.v[k]) - dvn * n[k];
-    const R c0 = eig[0] * (dp - rho_a * ca * dvn) / (R(2) * c2a);
-    const R c1 = eig[1] * (drho - dp / c2a);
+    const R inv2c2 = qdiv<R>(R(1), R(2) * c2a);
+    const R c0 = eig[0] * (dp - rho_a * ca * dvn) * inv2c2;
+    const R c1 = eig[1] * (drho - R(2) * dp * inv2c2);
     const R c2 = eig[1] * rho_a;
-    const R c3 = eig[2] * (dp + rho_a * ca * dvn) / (R(2) * c2a);
+    const R c3 = eig[2] * (dp + rho_a * ca * dvn) * inv2c2;
     R A[5];
     A[0] = c0 + c1 + c3;
     R dvtv = R(0);
@@ -265,8 +304,8 @@ __device__ __forceinline__ void conv_num_flux(const R uL[5], const R uR[5], cons
         for (int k = 0; k < 5; ++k) out[k] = R(0.5) * (FL[k] + FR[k]);
     }
     if (cf == CF_LXF || cf == CF_EC_LXF) {
-        const R eLv = rabs(L.v[d]) + rsqrt_<R>(L.p * c.gam / L.rho);
-        const R eRv = rabs(Rq.v[d]) + rsqrt_<R>(Rq.p * c.gam / Rq.rho);
+        const R eLv = rabs(L.v[d]) + rsqrt_<R>(qdiv<R>(L.p * c.gam, L.rho));
+        const R eRv = rabs(Rq.v[d]) + rsqrt_<R>(qdiv<R>(Rq.p * c.gam, Rq.rho));
         const R e = eLv > eRv ? eLv : eRv;
 #pragma unroll
         for (int k = 0; k < 5; ++k) out[k] += R(-0.5) * e * (uR[k] - uL[k]);
@@ -287,18 +326,19 @@ __device__ __forceinline__ void viscous_flux(const R u[5], const R g[5][3], int 
     const R rho_raw = u[0];
     R w[5];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) w[1 + k] = u[1 + k] / rho_raw;
+    for (int k = 0; k < 3; ++k) w[1 + k] = qdiv<R>(u[1 + k], rho_raw);
     R v2 = R(0);
 #pragma unroll
     for (int k = 0; k < 3; ++k) v2 = v2 + w[1 + k] * w[1 + k];
     w[4] = positive<R>(positive<R>(c.gm1 * (u[4] - R(0.5) * rho_raw * v2), st), st);
     w[0] = positive<R>(rho_raw, st);
     const R rho = w[0];
+    const R inv_rho = qdiv<R>(R(1), rho);
     R gv[3][3], gp[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a)
 #pragma unroll
-        for (int k = 0; k < 3; ++k) gv[a][k] = (g[1 + a][k] - w[1 + a] * g[0][k]) / rho;
+        for (int k = 0; k < 3; ++k) gv[a][k] = (g[1 + a][k] - w[1 + a] * g[0][k]) * inv_rho;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         R t = g[4][k];
@@ -306,9 +346,9 @@ __device__ __forceinline__ void viscous_flux(const R u[5], const R g[5][3], int 
         for (int m = 0; m < 3; ++m) t -= R(0.5) * (w[1 + m] * g[1 + m][k] + u[1 + m] * gv[m][k]);
         gp[k] = t * c.gm1;
     }
-    const R T = c.gam * c.mach2 * (w[4] / rho);
+    const R T = c.gam * c.mach2 * (w[4] * inv_rho);
     // Sutherland's law mu = (1 + T_r)/(T + T_r) T^{3/2}, with T^{3/2} = T sqrt(T)
-    R mu = use_const_visc ? c.const_visc : ((R(1) + c.temp_ratio) / (T + c.temp_ratio)) * (T * rsqrt_<R>(T));
+    R mu = use_const_visc ? c.const_visc : qdiv<R>(R(1) + c.temp_ratio, T + c.temp_ratio) * (T * rsqrt_<R>(T));
     mu = mu * c.inv_re;
     const R kappa = mu * c.kappa_fac;
     const R div = gv[0][0] + gv[1][1] + gv[2][2];
@@ -320,7 +360,7 @@ __device__ __forceinline__ void viscous_flux(const R u[5], const R g[5][3], int 
 #pragma unroll
         for (int k = 0; k < 3; ++k) tau_d[k] = R(2) * mu * (R(0.5) * (gv[k][d] + gv[d][k]));
         tau_d[d] += mu2 * div;
-        const R dT = (c.gam * c.mach2 * gp[d] - T * g[0][d]) / rho;
+        const R dT = (c.gam * c.mach2 * gp[d] - T * g[0][d]) * inv_rho;
         const R q = -kappa * dT;
 #pragma unroll
         for (int k = 0; k < 3; ++k) F[d][k] = -tau_d[k];
