@@ -131,6 +131,19 @@ int ph_status(ph_ctx* ctx, uint32_t* flags);
 int ph_set_timing(ph_ctx* ctx, int enable);
 int ph_get_timing(ph_ctx* ctx, double out[7]);
 
+/* R(U) as ph_residual computes it, on caller-owned DEVICE buffers U and R, without a
+ * context and without allocating device memory. No counterpart in the reference: it
+ * exists for callers that cannot call cudaMalloc (loops that must not synchronise the
+ * device, or a framework that owns all device memory). U and R need no initialisation
+ * beyond U's values. Its scratch lives in fixed file-scope device arrays: at most 32768 cells, and
+ * for Navier-Stokes at most 12 x cells x (p+1)^3 <= 4 Mi doubles of viscous-flux scratch
+ * (32 MiB); larger meshes are rejected with PH_ERR_INVALID. The first call on a device
+ * resolves the arrays' device addresses and should come before any stream capture.
+ * Every call shares the same arrays: calls that overlap on the GPU (other streams or
+ * threads) race, so serialise them. Asynchronous on cuda_stream (NULL = default). */
+int ph_residual_noalloc(const ph_mesh_desc* mesh, const ph_params* prm, const double* U, double* R,
+                        void* cuda_stream);
+
 /* Self-test of the quotient used inside the flux kernels against IEEE division on n
  * pseudo-random operand pairs; out[0] = max relative error in FP64, out[1] in FP32.
  * No counterpart in the reference. */

@@ -17,7 +17,7 @@ ERRORS = {1: "invalid argument", 2: "unsupported configuration", 3: "CUDA error"
 
 EXPORTED = ["ph_ctx_create", "ph_ctx_destroy", "ph_ndofs", "ph_cell_ijk", "ph_set_state", "ph_get_state",
             "ph_residual", "ph_apply_inverse_mass", "ph_rk_step", "ph_integrals", "ph_status", "ph_sync",
-            "ph_set_timing", "ph_get_timing", "ph_quotient_selftest", "ph_last_error"]
+            "ph_set_timing", "ph_get_timing", "ph_quotient_selftest", "ph_residual_noalloc", "ph_last_error"]
 
 
 class PhParams(ctypes.Structure):
@@ -70,6 +70,7 @@ def load(build_if_missing: bool = False):
     L.ph_set_timing.argtypes = [vp, ctypes.c_int]
     L.ph_get_timing.argtypes = [vp, dp]
     L.ph_quotient_selftest.argtypes = [ctypes.c_uint64, ctypes.c_int, dp]
+    L.ph_residual_noalloc.argtypes = [ctypes.POINTER(PhMeshDesc), ctypes.POINTER(PhParams), vp, vp, vp]
     L.ph_last_error.restype = ctypes.c_char_p
     _lib = L
     return L

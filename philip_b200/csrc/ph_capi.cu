@@ -637,3 +637,256 @@ int ph_sync(ph_ctx* c) {
 }
 
 }  // extern "C"
+
+// =======================================================================================
+// Residual evaluation that allocates no device memory.
+//
+// Some callers cannot call cudaMalloc: solver loops that must never synchronise the
+// device (cudaMalloc and cudaFree may), and host frameworks that reserve the device memory
+// up front through their own pool and forbid any later allocation. For them
+// ph_residual_noalloc computes R(U) on caller-owned device buffers without a context:
+// its scratch (the nodal viscous flux between the auxiliary and residual kernels), the
+// neighbour table and the operator tables live in file-scope device arrays of fixed
+// size, which every GPU that loads this library holds until the process exits.
+// Nothing has to start at zero: each call rebuilds the tables, clears the status word,
+// writes the whole viscous-flux scratch before reading it and writes every entry of R.
+// All calls share these arrays, so calls that overlap on the GPU race.
+// =======================================================================================
+namespace {
+
+constexpr size_t NOALLOC_FV_DOUBLES = (size_t)4 << 20;      // 4 Mi doubles = 32 MiB viscous-flux scratch
+constexpr int NOALLOC_MAX_CELLS = 32768;                     // 32^3 cells (neighbour table 768 KiB)
+
+static __device__ __align__(256) double g_noalloc_fv[NOALLOC_FV_DOUBLES];
+static __device__ __align__(256) int g_noalloc_nbr[6 * NOALLOC_MAX_CELLS];
+static __device__ __align__(256) ph::OpTab g_noalloc_ops;
+static __device__ __align__(256) unsigned g_noalloc_status;
+
+// Device addresses of the arrays above, resolved once per device with that device current.
+// In host code the array names are host-side stand-ins, never device addresses.
+struct NoallocSymbols {
+    bool ready = false;
+    double* fv = nullptr;
+    int* nbr = nullptr;
+    ph::OpTab* ops = nullptr;
+    unsigned* status = nullptr;
+};
+NoallocSymbols g_noalloc_sym[64];
+
+int noalloc_setup(int dev) {
+    if (dev < 0 || dev >= 64) return fail(PH_ERR_INVALID, "device ordinal out of range");
+    NoallocSymbols& s = g_noalloc_sym[dev];
+    if (s.ready) return PH_OK;
+    PH_CUDA(cudaGetSymbolAddress((void**)&s.fv, g_noalloc_fv));
+    PH_CUDA(cudaGetSymbolAddress((void**)&s.nbr, g_noalloc_nbr));
+    PH_CUDA(cudaGetSymbolAddress((void**)&s.ops, g_noalloc_ops));
+    PH_CUDA(cudaGetSymbolAddress((void**)&s.status, g_noalloc_status));
+    s.ready = true;
+    return PH_OK;
+}
+
+// fixed-size versions of the 1-D helpers (no heap allocation)
+void noalloc_gll(int n, double* x, double* w) {
+    const int m = n - 1;
+    for (int i = 0; i < n; ++i) {
+        double z = -std::cos(M_PI * i / m);
+        if (i > 0 && i < m) {
+            for (int it = 0; it < 64; ++it) {
+                double p, dp; legendre_pd(m, z, p, dp);
+                const double d2p = (2.0 * z * dp - m * (m + 1.0) * p) / (1.0 - z * z);
+                const double dz = dp / d2p;
+                z -= dz;
+                if (std::fabs(dz) < 1e-17) break;
+            }
+        }
+        double p, dp; legendre_pd(m, z, p, dp);
+        x[i] = 0.5 * (z + 1.0);
+        w[i] = 1.0 / (m * (m + 1.0) * p * p);
+    }
+    x[0] = 0.0; x[m] = 1.0;
+}
+void noalloc_lagrange_derivative(const double* nodes, int n, double xx, double* dv) {
+    for (int j = 0; j < n; ++j) {
+        double val = 1.0, der = 0.0;
+        for (int m = 0; m < n; ++m) {
+            if (m == j) continue;
+            const double r = 1.0 / (nodes[j] - nodes[m]);
+            der = der * (xx - nodes[m]) * r + val * r;
+            val *= (xx - nodes[m]) * r;
+        }
+        dv[j] = der;
+    }
+}
+bool noalloc_invert(const double* A0, int n, double* Ai) {
+    double A[ph::MAXN1 * ph::MAXN1];
+    for (int i = 0; i < n * n; ++i) { A[i] = A0[i]; Ai[i] = (i % (n + 1) == 0) ? 1.0 : 0.0; }
+    for (int c = 0; c < n; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < n; ++r) if (std::fabs(A[r * n + c]) > std::fabs(A[piv * n + c])) piv = r;
+        if (A[piv * n + c] == 0.0) return false;
+        for (int j = 0; j < n; ++j) { std::swap(A[c * n + j], A[piv * n + j]); std::swap(Ai[c * n + j], Ai[piv * n + j]); }
+        const double inv = 1.0 / A[c * n + c];
+        for (int j = 0; j < n; ++j) { A[c * n + j] *= inv; Ai[c * n + j] *= inv; }
+        for (int r = 0; r < n; ++r) if (r != c && A[r * n + c] != 0.0) {
+            const double f = A[r * n + c];
+            for (int j = 0; j < n; ++j) { A[r * n + j] -= f * A[c * n + j]; Ai[r * n + j] -= f * Ai[c * n + j]; }
+        }
+    }
+    return true;
+}
+
+// neighbour table of the periodic cube in deal.II cell order, built on the device
+__global__ void noalloc_neighbours(int n, int morton, int levels, int* nbr) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nc = n * n * n;
+    if (c >= nc) return;
+    int t[3];
+    if (morton) {
+        t[0] = t[1] = t[2] = 0;
+        for (int l = 0; l < levels; ++l) {
+            const int ch = (c >> (3 * (levels - 1 - l))) & 7;
+            t[0] = 2 * t[0] + (ch & 1); t[1] = 2 * t[1] + ((ch >> 1) & 1); t[2] = 2 * t[2] + ((ch >> 2) & 1);
+        }
+    } else {
+        t[0] = c % n; t[1] = (c / n) % n; t[2] = c / (n * n);
+    }
+    for (int f = 0; f < 6; ++f) {
+        int u[3] = {t[0], t[1], t[2]};
+        const int d = f >> 1;
+        u[d] = (u[d] + ((f & 1) ? 1 : -1) + n) % n;
+        int id;
+        if (morton) {
+            id = 0;
+            for (int l = 0; l < levels; ++l) {
+                const int b = levels - 1 - l;
+                const int ch = ((u[0] >> b) & 1) | (((u[1] >> b) & 1) << 1) | (((u[2] >> b) & 1) << 2);
+                id = (id << 3) | ch;
+            }
+        } else {
+            id = (u[2] * n + u[1]) * n + u[0];
+        }
+        nbr[6 * c + f] = id;
+    }
+}
+
+} // namespace
+
+extern "C" int ph_residual_noalloc(const ph_mesh_desc* mesh, const ph_params* prm, const double* U, double* R,
+                                   void* cuda_stream) {
+    if (!mesh || !prm || !U || !R) return fail(PH_ERR_INVALID, "null argument");
+    if (prm->flux_nodes_type != 1 || prm->overintegration != 0)
+        return fail(PH_ERR_UNSUPPORTED, "the GPU path is collocated: flux_nodes_type = GLL and overintegration = 0");
+    if (prm->poly_degree < 1 || prm->poly_degree > 6) return fail(PH_ERR_UNSUPPORTED, "poly_degree must be 1..6");
+    if (prm->flux_reconstruction_aux != 0) return fail(PH_ERR_UNSUPPORTED, "flux_reconstruction_aux must be kDG");
+    if (prm->conv_num_flux >= 3 && !prm->use_split_form)
+        return fail(PH_ERR_INVALID, "two point flux and not using split form are not compatible");
+    const int n = mesh->n_cells_per_direction;
+    if (n < 1 || !(mesh->right > mesh->left)) return fail(PH_ERR_INVALID, "bad mesh");
+    const long long nc = (long long)n * n * n;
+    const int N1 = prm->poly_degree + 1, NP = N1 * N1 * N1;
+    const bool visc = prm->pde_type == 1;
+    if (nc > NOALLOC_MAX_CELLS)
+        return fail(PH_ERR_INVALID, "ph_residual_noalloc: " + std::to_string(nc) + " cells exceed the fixed limit of " +
+                                        std::to_string(NOALLOC_MAX_CELLS));
+    if (visc && (size_t)12 * nc * NP > NOALLOC_FV_DOUBLES)
+        return fail(PH_ERR_INVALID, "ph_residual_noalloc: the viscous-flux scratch needs " +
+                                        std::to_string((size_t)12 * nc * NP) + " doubles, above the fixed " +
+                                        std::to_string(NOALLOC_FV_DOUBLES));
+    int dev = 0;
+    PH_CUDA(cudaGetDevice(&dev));
+    if (int rc = noalloc_setup(dev)) return rc;
+    const NoallocSymbols& sym = g_noalloc_sym[dev];
+    cudaStream_t stream = (cudaStream_t)cuda_stream;
+    const double h = (mesh->right - mesh->left) / n;
+
+    // 1-D operators (the construction of ph_ctx_create, on fixed-size stack arrays so that
+    // this entry point makes no heap allocation either)
+    double x[ph::MAXN1], w[ph::MAXN1], D[ph::MAXN1 * ph::MAXN1], Dp[ph::MAXN1 * ph::MAXN1];
+    double MK[ph::MAXN1 * ph::MAXN1], Minv[ph::MAXN1 * ph::MAXN1], tmp[ph::MAXN1 * ph::MAXN1];
+    noalloc_gll(N1, x, w);
+    for (int a = 0; a < N1; ++a) noalloc_lagrange_derivative(x, N1, x[a], &D[a * N1]);
+    double cfr = 0.0;
+    if (fr_parameter(prm->flux_reconstruction, prm->poly_degree, prm->FR_user_specified_correction_parameter_value, cfr))
+        return fail(PH_ERR_UNSUPPORTED, "flux_reconstruction type not defined for this degree");
+    for (int i = 0; i < N1 * N1; ++i) Dp[i] = (i % (N1 + 1) == 0) ? 1.0 : 0.0;
+    for (int k = 0; k < prm->poly_degree; ++k) {
+        for (int i = 0; i < N1; ++i)
+            for (int j = 0; j < N1; ++j) {
+                double acc = 0.0;
+                for (int m = 0; m < N1; ++m) acc += D[i * N1 + m] * Dp[m * N1 + j];
+                tmp[i * N1 + j] = acc;
+            }
+        for (int i = 0; i < N1 * N1; ++i) Dp[i] = tmp[i];
+    }
+    for (int i = 0; i < N1; ++i)
+        for (int j = 0; j < N1; ++j) {
+            double kij = 0.0;
+            for (int q = 0; q < N1; ++q) kij += Dp[q * N1 + i] * w[q] * Dp[q * N1 + j];
+            MK[i * N1 + j] = (i == j ? w[i] : 0.0) + cfr * kij;
+        }
+    if (!noalloc_invert(MK, N1, Minv)) return fail(PH_ERR_INVALID, "singular FR mass matrix");
+    ph::OpTab tab;
+    std::memset(&tab, 0, sizeof(tab));
+    for (int a = 0; a < N1; ++a) {
+        tab.w[a] = w[a];
+        for (int l = 0; l < N1; ++l) {
+            tab.D[a * ph::MAXN1 + l] = D[a * N1 + l];
+            tab.Dsk[a * ph::MAXN1 + l] = (w[a] * D[a * N1 + l] - w[l] * D[l * N1 + a]) / w[a];
+            tab.Minv[a * ph::MAXN1 + l] = Minv[a * N1 + l];
+            tab.B[a * ph::MAXN1 + l] = Minv[a * N1 + l] * w[l];
+        }
+    }
+    PH_CUDA(cudaMemcpyToSymbolAsync(g_noalloc_ops, &tab, sizeof(tab), 0, cudaMemcpyHostToDevice, stream));
+    PH_CUDA(cudaMemsetAsync(sym.status, 0, sizeof(unsigned), stream));
+    const bool pow2 = (n & (n - 1)) == 0;
+    const bool morton = (mesh->cell_order == 2) || (mesh->cell_order == 0 && pow2);
+    int levels = 0;
+    while ((1 << levels) < n) ++levels;
+    noalloc_neighbours<<<(int)((nc + 127) / 128), 128, 0, stream>>>(n, morton ? 1 : 0, levels, sym.nbr);
+    PH_CUDA(cudaGetLastError());
+
+    ph::PhysConst pc{};
+    pc.gam = prm->gamma_gas; pc.gm1 = prm->gamma_gas - 1.0;
+    pc.mach2 = prm->mach_infinity * prm->mach_infinity;
+    pc.temp_ratio = 110.4 / prm->temperature_inf;
+    pc.inv_re = 1.0 / prm->reynolds_number_inf;
+    pc.prandtl = prm->prandtl_number;
+    pc.const_visc = prm->nondimensionalized_constant_viscosity;
+    pc.use_const_visc = prm->use_constant_viscosity;
+    pc.two_point = prm->two_point_num_flux_type;
+    pc.conv_flux = prm->conv_num_flux;
+    pc.diss_flux = prm->diss_num_flux;
+    pc.navier_stokes = visc;
+    const double sipg = prm->diss_num_flux == 1 ? 0.0 : prm->sipg_penalty_factor;
+    pc.sipg_pen = sipg;
+    const int fp32 = prm->precision == PH_FP32_RESIDUAL;
+
+    cudaError_t e = cudaSuccess;
+    if (visc) {
+        switch (N1) {
+        case 2: e = ph::launch_aux<2>(U, sym.nbr, sym.ops, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
+        case 3: e = ph::launch_aux<3>(U, sym.nbr, sym.ops, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
+        case 4: e = ph::launch_aux<4>(U, sym.nbr, sym.ops, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
+        case 5: e = ph::launch_aux<5>(U, sym.nbr, sym.ops, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
+        case 6: e = ph::launch_aux<6>(U, sym.nbr, sym.ops, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
+        default: e = ph::launch_aux<7>(U, sym.nbr, sym.ops, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
+        }
+        if (e != cudaSuccess) return fail(PH_ERR_CUDA, std::string("aux launch: ") + cudaGetErrorString(e));
+    }
+    ph::StageArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.U = U; a.Fv = sym.fv; a.nbr = sym.nbr; a.ops = sym.ops; a.nc = (int)nc;
+    a.h = h; a.inv_h = 1.0 / h; a.pen = (double)prm->poly_degree * (prm->poly_degree + 1) / h * sipg;
+    a.pc = pc; a.status = sym.status; a.mode = 0; a.fr = cfr != 0.0; a.out = R;
+    const bool split = prm->use_split_form != 0;
+    switch (N1) {
+    case 2: e = ph::launch_stage<2>(a, fp32, visc, split, stream); break;
+    case 3: e = ph::launch_stage<3>(a, fp32, visc, split, stream); break;
+    case 4: e = ph::launch_stage<4>(a, fp32, visc, split, stream); break;
+    case 5: e = ph::launch_stage<5>(a, fp32, visc, split, stream); break;
+    case 6: e = ph::launch_stage<6>(a, fp32, visc, split, stream); break;
+    default: e = ph::launch_stage<7>(a, fp32, visc, split, stream); break;
+    }
+    if (e != cudaSuccess) return fail(PH_ERR_CUDA, std::string("residual launch: ") + cudaGetErrorString(e));
+    return PH_OK;
+}
