@@ -152,13 +152,37 @@ def measured_peaks():
     return 6650.0, "fallback 6.65 TB/s"
 
 
-def ncu_traffic(workload: str):
+def fp64_dgemm_peak(torch):
+    """Measured FP64 denominator: cuBLAS DGEMM 8192^3 (2 N^3 flops), best of 3, CUDA events.
+    Run outside the timed region."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    c = a @ b
+    best = float("inf")
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(); torch.matmul(a, b, out=c); e1.record(); torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b, c
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def ncu_traffic(p: int, viscous: bool, precision: str, ndofs: int):
+    """DRAM bytes (read + write) of one stage-kernel launch, from the ncu capture summarised
+    in profiles/dram_traffic.json (bytes per DOF of a smaller case of the same order and
+    physics, scaled by the DOFs of this workload), or None when no capture matches."""
     path = os.path.join(ROOT, "profiles", "dram_traffic.json")
-    if os.path.exists(path):
-        with open(path) as f:
-            d = json.load(f)
-        return d.get(workload)
-    return None
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    e = d.get(f"residual_kernel/{'navier_stokes' if viscous else 'euler'}/p{p}/{precision}")
+    if not e:
+        return None
+    return {"bytes_per_launch": e["bytes_per_dof"] * ndofs, "bytes_per_dof": e["bytes_per_dof"],
+            "alg_bytes_per_dof_same_stage": e["alg_bytes_per_dof_same_stage"], "captured": e["captured"]}
 
 
 def cpu_baseline(workload: str, n_threads: int | None = None):
@@ -337,7 +361,10 @@ def main():
             pass   # the state stays FP64, so the stage bytes are the same (+8 B/DOF Kahan term at the last stage)
         bytes_launch = bpd["stage"] * dg.n_dofs
         achieved = bytes_launch / (stage_ms * 1e-3) / 1e9
-        traffic = ncu_traffic(args.workload + ("" if args.precision == "fp64" else "_fp32"))
+        traffic = ncu_traffic(p, viscous, args.precision, dg.n_dofs)
+        flops_dof = flops_per_dof_stage(p, viscous)
+        fp64_tflops = flops_dof * dg.n_dofs / (stage_ms * 1e-3) / 1e12
+        dgemm_tflops = fp64_dgemm_peak(torch)
         line = {
             "metric": "TGV DOF-updates/s/stage", "value": value, "unit": "DOF-updates/s/stage",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -358,7 +385,11 @@ def main():
                          "kernel": "residual_kernel (stage: residual + mass inverse + RK update)",
                          "kernel_ms": stage_ms, "aux_kernel_ms": aux_ms,
                          "alg_bytes_per_dof": bpd, "peak_source": peak_src,
-                         "fp64_alg_flops_per_dof_stage": flops_per_dof_stage(p, viscous)},
+                         "fp64": {"alg_flops_per_dof_stage": flops_dof, "achieved_tflops": fp64_tflops,
+                                  "peak_tflops": dgemm_tflops, "frac": fp64_tflops / dgemm_tflops,
+                                  "peak_source": "measured here: cuBLAS DGEMM 8192^3, best of 3"
+                                                 + ("" if args.precision == "fp64" else
+                                                    " (the precision form computes its fluxes in FP32)")}},
             "clocks": clk.summary(),
         }
         if world == 1 and not args.no_cpu_baseline:
