@@ -83,6 +83,15 @@ typedef struct ph_mesh_desc {
     int cell_order;
     double left;
     double right;
+    /* Curvilinear cube when warp != 0: every coordinate of the straight-sided mesh is moved
+     * by warp (L/2pi) sin(2pi(x-l)/L) sin(2pi(y-l)/L) sin(2pi(z-l)/L) (L = right - left,
+     * l = left; zero on the cube's faces, so periodic faces still match), through a mapping
+     * of degree grid_degree on GLL support points. The GPU path takes grid_degree =
+     * poly_degree, split-form Euler and cDG on curvilinear meshes. Not a reference grid:
+     * the construction follows the reference's curved periodic grids
+     * (src/mesh/grids/curved_periodic_grid.cpp) with this warp. */
+    double warp;
+    int grid_degree;
 } ph_mesh_desc;
 
 /* Builds host index maps, 1-D operators and device buffers (replaces DGFactory::
@@ -94,6 +103,10 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
 int ph_ctx_destroy(ph_ctx* ctx);
 
 int64_t ph_ndofs(const ph_ctx* ctx);
+/* Physical coordinates of the solution nodes, [cell][node][3] in the state's cell and node
+ * order (the points VectorTools::interpolate evaluates an initial condition at,
+ * src/solution/set_initial_condition.cpp:51). */
+int ph_node_xyz(const ph_ctx* ctx, double* xyz);
 int ph_cell_ijk(const ph_ctx* ctx, int32_t* ijk /* 3 per cell */);
 
 /* DGBase::solution assignment / read-back (src/dg/dg_base.hpp:396). */
@@ -114,7 +127,8 @@ int ph_rk_step(ph_ctx* ctx, double dt, int nsteps);
 
 /* PeriodicTurbulence::compute_and_update_integrated_quantities subset
  * (src/flow_solver/flow_solver_cases/periodic_turbulence.cpp:439-672):
- * out[0] kinetic energy, out[1] enstrophy, out[2] vorticity-based dissipation rate,
+ * out[0] kinetic energy, out[1] enstrophy, out[2] vorticity-based dissipation rate
+ * (2 enstrophy / Re; zero for the Euler equations),
  * out[3] maximum convective wave speed; all divided by the domain volume except out[3]. */
 int ph_integrals(ph_ctx* ctx, double out[4]);
 

@@ -568,9 +568,129 @@ struct Physics {
 // ---------------------------------------------------------------------------------
 static bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 
-static double warp_map(double x0, double y0, double z0, int d, double a) {
-    const double s = a * std::sin(x0) * std::sin(y0) * std::sin(z0);
-    return (d == 0 ? x0 : d == 1 ? y0 : z0) + s;
+// Sine warp of the periodic cube [l, r]^3 (L = r - l, k = 2 pi / L): every coordinate is
+// moved by the same amount a/k sin(k(x-l)) sin(k(y-l)) sin(k(z-l)), which vanishes on the
+// cube's faces, so periodic faces still match (for [0, 2 pi]^3: x_i += a sin x sin y sin z).
+// Not a reference grid: the reference's curved periodic grids (curved_periodic_grid.cpp,
+// nonsymmetric_curved_periodic_grid.cpp) use other warps; the construction is the same:
+// the mapping support points are the manifold's images of the straight-sided points.
+static void warp_point(double left, double right, double a, double X[3]) {
+    const double k = 2.0 * PI / (right - left);
+    const double s = a / k * std::sin(k * (X[0] - left)) * std::sin(k * (X[1] - left)) * std::sin(k * (X[2] - left));
+    X[0] += s; X[1] += s; X[2] += s;
+}
+
+// Metric cofactor by the conservative curl form (operators.cpp:2738-2884) at the points
+// selected by the 1-D operators A[d] (mapping basis values there, r[d] rows each) and
+// dA[d] (their derivatives). P holds the nine products X_l dX_m/dxi_j at the grid nodes:
+// P[0..2] = z dy/dxi_j, P[3..5] = x dz/dxi_j, P[6..8] = y dx/dxi_j. C is [npts][9].
+static void cofactor_at(const double* const A[3], const double* const dA[3], const int r[3], int ng,
+                        const std::vector<double> P[9], double* C) {
+    const int npts = r[0] * r[1] * r[2];
+    std::vector<double> t(npts), acc(npts);
+    auto D = [&](int e, const std::vector<double>& f, bool adding, double factor) {
+        const double* B[3] = {A[0], A[1], A[2]};
+        B[e] = dA[e];
+        apply3(B[0], r[0], ng, B[1], r[1], ng, B[2], r[2], ng, f.data(), acc.data(), adding, factor);
+    };
+    // row l of C from the products of row l: C[l][0] = -D_eta(f_zeta) + D_zeta(f_eta),
+    // C[l][1] = D_xi(f_zeta) - D_zeta(f_xi), C[l][2] = -D_xi(f_eta) + D_eta(f_xi)
+    for (int l = 0; l < 3; ++l) {
+        const std::vector<double>* f = &P[3 * l];
+        D(1, f[2], false, -1.0); D(2, f[1], true, 1.0);
+        for (int q = 0; q < npts; ++q) C[q * 9 + l * 3 + 0] = acc[q];
+        D(0, f[2], false, 1.0); D(2, f[0], true, -1.0);
+        for (int q = 0; q < npts; ++q) C[q * 9 + l * 3 + 1] = acc[q];
+        D(0, f[1], false, -1.0); D(1, f[0], true, 1.0);
+        for (int q = 0; q < npts; ++q) C[q * 9 + l * 3 + 2] = acc[q];
+    }
+}
+
+static double det3(const double J[3][3]) {
+    return J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) - J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+           J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+}
+
+// Curvilinear metric terms of cell c: mapping support points on the GLL points of degree
+// grid_degree (FE_Q support points in lexicographic order, strong_dg.cpp:68-75), det J at
+// the volume flux nodes (operators.cpp:2591-2672), cofactor at the volume flux nodes and
+// at every face's flux nodes (operators.cpp:2444-2589), and the physical positions of the
+// solution support points.
+static void build_curvilinear_cell(Mesh& m, const Ops1D& ops, int c) {
+    const int ng = m.grid_degree + 1, ng3 = ng * ng * ng;
+    const int nq = ops.nq, nd = ops.nd, nq3 = nq * nq * nq, nf = nq * nq;
+    std::vector<double> xg, wg; gauss_lobatto(ng, xg, wg);
+    std::vector<double> Bg(ng * ng), dBg(ng * ng), Bf(nq * ng), dBf(nq * ng), Bx(nd * ng);
+    std::vector<double> Bs[2] = {std::vector<double>(ng), std::vector<double>(ng)};
+    std::vector<double> dBs[2] = {std::vector<double>(ng), std::vector<double>(ng)};
+    for (int a = 0; a < ng; ++a) lagrange_eval(xg, xg[a], &Bg[a * ng], &dBg[a * ng]);
+    for (int q = 0; q < nq; ++q) lagrange_eval(xg, ops.xq[q], &Bf[q * ng], &dBf[q * ng]);
+    for (int i = 0; i < nd; ++i) lagrange_eval(xg, ops.xs[i], &Bx[i * ng], nullptr);
+    lagrange_eval(xg, 0.0, Bs[0].data(), dBs[0].data());
+    lagrange_eval(xg, 1.0, Bs[1].data(), dBs[1].data());
+    const auto t = m.ijk[c];
+    std::vector<double> X[3] = {std::vector<double>(ng3), std::vector<double>(ng3), std::vector<double>(ng3)};
+    for (int k = 0; k < ng; ++k) for (int j = 0; j < ng; ++j) for (int i = 0; i < ng; ++i) {
+        double p[3] = {m.left + m.h * (t[0] + xg[i]), m.left + m.h * (t[1] + xg[j]), m.left + m.h * (t[2] + xg[k])};
+        warp_point(m.left, m.right, m.warp, p);
+        for (int d = 0; d < 3; ++d) X[d][(k * ng + j) * ng + i] = p[d];
+    }
+    // gradient of the support points at the grid nodes (the Jacobian there)
+    std::vector<double> GX[3][3];
+    for (int mm = 0; mm < 3; ++mm)
+        for (int j = 0; j < 3; ++j) {
+            GX[mm][j].resize(ng3);
+            const double* B[3] = {Bg.data(), Bg.data(), Bg.data()};
+            B[j] = dBg.data();
+            apply3(B[0], ng, ng, B[1], ng, ng, B[2], ng, ng, X[mm].data(), GX[mm][j].data(), false, 1.0);
+        }
+    std::vector<double> P[9];
+    for (int j = 0; j < 3; ++j) {
+        P[j].resize(ng3); P[3 + j].resize(ng3); P[6 + j].resize(ng3);
+        for (int g = 0; g < ng3; ++g) {
+            P[j][g] = X[2][g] * GX[1][j][g];        // z dy/dxi_j
+            P[3 + j][g] = X[0][g] * GX[2][j][g];    // x dz/dxi_j
+            P[6 + j][g] = X[1][g] * GX[0][j][g];    // y dx/dxi_j
+        }
+    }
+    // volume flux nodes
+    {
+        const double* A[3] = {Bf.data(), Bf.data(), Bf.data()};
+        const double* dA[3] = {dBf.data(), dBf.data(), dBf.data()};
+        const int r[3] = {nq, nq, nq};
+        cofactor_at(A, dA, r, ng, P, &m.cof[(size_t)c * nq3 * 9]);
+        std::vector<double> Jm[3][3];
+        for (int mm = 0; mm < 3; ++mm)
+            for (int j = 0; j < 3; ++j) {
+                Jm[mm][j].resize(nq3);
+                const double* B[3] = {Bf.data(), Bf.data(), Bf.data()};
+                B[j] = dBf.data();
+                apply3(B[0], nq, ng, B[1], nq, ng, B[2], nq, ng, X[mm].data(), Jm[mm][j].data(), false, 1.0);
+            }
+        for (int q = 0; q < nq3; ++q) {
+            double J[3][3];
+            for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) J[a][b] = Jm[a][b][q];
+            const double dj = det3(J);
+            if (dj <= 1e-14) throw std::runtime_error("oracle: non-positive det J (operators.cpp:2667-2670)");
+            m.detj[(size_t)c * nq3 + q] = dj;
+        }
+    }
+    // facet flux nodes of each face, interior side (operators.cpp:2501-2589)
+    for (int f = 0; f < 6; ++f) {
+        const int dn = f / 2, side = f % 2;
+        const double* A[3] = {Bf.data(), Bf.data(), Bf.data()};
+        const double* dA[3] = {dBf.data(), dBf.data(), dBf.data()};
+        int r[3] = {nq, nq, nq};
+        A[dn] = Bs[side].data(); dA[dn] = dBs[side].data(); r[dn] = 1;
+        cofactor_at(A, dA, r, ng, P, &m.cof_face[((size_t)c * 6 + f) * nf * 9]);
+    }
+    // solution support points in physical space
+    const int nd3 = nd * nd * nd;
+    std::vector<double> xs(nd3);
+    for (int d = 0; d < 3; ++d) {
+        apply3(Bx.data(), nd, ng, Bx.data(), nd, ng, Bx.data(), nd, ng, X[d].data(), xs.data(), false, 1.0);
+        for (int i = 0; i < nd3; ++i) m.xnode[((size_t)c * nd3 + i) * 3 + d] = xs[i];
+    }
 }
 
 Mesh build_periodic_cube(int n, double left, double right, int order, const Ops1D& ops,
@@ -609,7 +729,12 @@ Mesh build_periodic_cube(int n, double left, double right, int order, const Ops1
     m.xnode.assign((size_t)m.nc * nd * nd * nd * 3, 0.0);
     m.warp = warp; m.grid_degree = grid_degree;
     m.affine = (warp == 0.0);
-    if (!m.affine) throw std::runtime_error("oracle: curvilinear mesh not built here (see build_curvilinear)");
+    if (!m.affine) {
+        if (grid_degree < 1) throw std::runtime_error("oracle: grid_degree must be >= 1");
+#pragma omp parallel for schedule(static)
+        for (int c = 0; c < m.nc; ++c) build_curvilinear_cell(m, ops, c);
+        return m;
+    }
     const double h = m.h;
     for (int c = 0; c < m.nc; ++c) {
         for (int q = 0; q < nq3; ++q) {
@@ -1049,6 +1174,33 @@ void Solver::apply_inverse_mass(const double* in, double* out, bool aux_eq) {
     const int nd = ops.nd;
     const double* Mi = aux_eq ? ops.minv_aux.data() : ops.minv.data();
     const size_t ndc = (size_t)ndofs_cell;
+    if (!mesh.affine) {
+        // curvilinear: weight-adjusted inverse P diag(1/(w J)) P^T with the FR projection
+        // P = (M+K)^{-1} chi^T W (dg_base.cpp:4217-4249, operators.cpp:1909-1932)
+        const int nq = ops.nq;
+        std::vector<double> P((size_t)nd * nq, 0.0);
+        for (int i = 0; i < nd; ++i)
+            for (int q = 0; q < nq; ++q) {
+                double v = 0.0;
+                for (int j = 0; j < nd; ++j) v += Mi[i * nd + j] * ops.chi[q * nd + j];
+                P[i * nq + q] = v * ops.wq[q];
+            }
+        const std::vector<double> PT = transpose(P.data(), nd, nq);
+#pragma omp parallel for schedule(static)
+        for (int c = 0; c < mesh.nc; ++c) {
+            std::vector<double> t(nq3), jw(nq3);
+            for (int k = 0; k < nq; ++k) for (int j = 0; j < nq; ++j) for (int i = 0; i < nq; ++i) {
+                const int q = (k * nq + j) * nq + i;
+                jw[q] = 1.0 / (ops.wq[i] * ops.wq[j] * ops.wq[k] * mesh.detj[(size_t)c * nq3 + q]);
+            }
+            for (int s = 0; s < NSTATE; ++s) {
+                apply3(PT.data(), nq, nd, PT.data(), nq, nd, PT.data(), nq, nd, in + c * ndc + s * nd3, t.data(), false, 1.0);
+                for (int q = 0; q < nq3; ++q) t[q] *= jw[q];
+                apply3(P.data(), nd, nq, P.data(), nd, nq, P.data(), nd, nq, t.data(), out + c * ndc + s * nd3, false, 1.0);
+            }
+        }
+        return;
+    }
 #pragma omp parallel for schedule(static)
     for (int c = 0; c < mesh.nc; ++c) {
         const double dj = mesh.detj[(size_t)c * nq3];
@@ -1141,10 +1293,53 @@ void Solver::integrals(const double* U, double* out) {
     std::vector<double> B((size_t)ne * nd), dB((size_t)ne * nd);
     for (int q = 0; q < ne; ++q) lagrange_eval(ops.xs, xe[q], &B[q * nd], &dB[q * nd]);
     const int ne3 = ne * ne * ne;
+    // curvilinear: the mapping (degree grid_degree on its GLL support points) at the Gauss points
+    const int ng = mesh.grid_degree + 1, ng3 = ng * ng * ng;
+    std::vector<double> xg, wg, Bm, dBm;
+    if (!mesh.affine) {
+        gauss_lobatto(ng, xg, wg);
+        Bm.resize((size_t)ne * ng); dBm.resize((size_t)ne * ng);
+        for (int q = 0; q < ne; ++q) lagrange_eval(xg, xe[q], &Bm[q * ng], &dBm[q * ng]);
+    }
     double ke = 0.0, ens = 0.0, wave = 0.0;
 #pragma omp parallel for reduction(+ : ke, ens) reduction(max : wave)
     for (int c = 0; c < mesh.nc; ++c) {
         const double h = mesh.h, dj = h * h * h;
+        std::vector<double> jac, dje;      // curvilinear: J^{-1} [ne3][3][3] and det J at the Gauss points
+        if (!mesh.affine) {
+            std::vector<double> X(ng3), Jm((size_t)9 * ne3);
+            const auto t = mesh.ijk[c];
+            for (int mm = 0; mm < 3; ++mm) {
+                for (int k = 0; k < ng; ++k) for (int j = 0; j < ng; ++j) for (int i = 0; i < ng; ++i) {
+                    double p[3] = {mesh.left + h * (t[0] + xg[i]), mesh.left + h * (t[1] + xg[j]), mesh.left + h * (t[2] + xg[k])};
+                    warp_point(mesh.left, mesh.right, mesh.warp, p);
+                    X[(k * ng + j) * ng + i] = p[mm];
+                }
+                for (int j = 0; j < 3; ++j) {
+                    const double* B[3] = {Bm.data(), Bm.data(), Bm.data()};
+                    B[j] = dBm.data();
+                    apply3(B[0], ne, ng, B[1], ne, ng, B[2], ne, ng, X.data(), &Jm[(size_t)(mm * 3 + j) * ne3], false, 1.0);
+                }
+            }
+            jac.resize((size_t)9 * ne3); dje.resize(ne3);
+            for (int q = 0; q < ne3; ++q) {
+                double J[3][3];
+                for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) J[a][b] = Jm[(size_t)(a * 3 + b) * ne3 + q];
+                const double d = det3(J);
+                dje[q] = d;
+                // inverse by the cofactor (adjugate) formula
+                double* I = &jac[(size_t)q * 9];
+                I[0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) / d;
+                I[1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / d;
+                I[2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / d;
+                I[3] = (J[1][2] * J[2][0] - J[1][0] * J[2][2]) / d;
+                I[4] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / d;
+                I[5] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / d;
+                I[6] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) / d;
+                I[7] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / d;
+                I[8] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / d;
+            }
+        }
         std::vector<double> uq(5 * ne3), gq(15 * ne3);
         for (int s = 0; s < 5; ++s) {
             const double* Uc = U + (size_t)c * ndofs_cell + s * nd3;
@@ -1157,7 +1352,16 @@ void Solver::integrals(const double* U, double* out) {
             double u[5], g[5][3], w[5];
             for (int s = 0; s < 5; ++s) {
                 u[s] = uq[s * ne3 + q];
-                for (int d = 0; d < 3; ++d) g[s][d] = (h * h) * gq[(s * 3 + d) * ne3 + q] / dj;
+                if (mesh.affine) {
+                    for (int d = 0; d < 3; ++d) g[s][d] = (h * h) * gq[(s * 3 + d) * ne3 + q] / dj;
+                } else {   // d/dx_d = sum_j (J^{-1})[j][d] d/dxi_j
+                    const double* I = &jac[(size_t)q * 9];
+                    for (int d = 0; d < 3; ++d) {
+                        double v = 0.0;
+                        for (int j = 0; j < 3; ++j) v += I[j * 3 + d] * gq[(s * 3 + j) * ne3 + q];
+                        g[s][d] = v;
+                    }
+                }
             }
             phys.primitive(u, w);
             double v2 = 0.0; for (int d = 0; d < 3; ++d) v2 += w[1 + d] * w[1 + d];
@@ -1166,7 +1370,7 @@ void Solver::integrals(const double* U, double* out) {
             for (int a = 0; a < 3; ++a) for (int d = 0; d < 3; ++d) gv[a][d] = (g[1 + a][d] - w[1 + a] * g[0][d]) / w[0];
             const double om0 = gv[2][1] - gv[1][2], om1 = gv[0][2] - gv[2][0], om2 = gv[1][0] - gv[0][1];
             const double en = 0.5 * u[0] * (om0 * om0 + om1 * om1 + om2 * om2);
-            const double wt = we[q % ne] * we[(q / ne) % ne] * we[q / (ne * ne)] * dj;
+            const double wt = we[q % ne] * we[(q / ne) % ne] * we[q / (ne * ne)] * (mesh.affine ? dj : dje[q]);
             ke += kin * wt; ens += en * wt;
             const double mw = phys.max_eig(u);
             if (mw > wave) wave = mw;

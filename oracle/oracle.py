@@ -57,6 +57,8 @@ def lib():
         vp, dp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
         L.orc_create.argtypes = [ctypes.POINTER(OrcParams), ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                  ctypes.c_int, ctypes.POINTER(vp)]
+        L.orc_create_curved.argtypes = [ctypes.POINTER(OrcParams), ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.POINTER(vp)]
         L.orc_destroy.argtypes = [vp]
         L.orc_ndofs.argtypes = [vp]; L.orc_ndofs.restype = ctypes.c_longlong
         L.orc_nd.argtypes = [vp]; L.orc_nq.argtypes = [vp]; L.orc_status.argtypes = [vp]
@@ -111,11 +113,20 @@ def make_params(cfg: dict) -> OrcParams:
 class Oracle:
     """One DG discretisation on a periodic cube, evaluated on the CPU."""
 
-    def __init__(self, cfg: dict, n_cells: int, left: float, right: float, order: str = "auto"):
+    def __init__(self, cfg: dict, n_cells: int, left: float, right: float, order: str = "auto",
+                 warp: float = 0.0, grid_degree: int | None = None):
+        """warp != 0: the sine-warped periodic cube (every coordinate moved by
+        warp (L/2pi) sin(2pi(x-l)/L) sin(2pi(y-l)/L) sin(2pi(z-l)/L)) with a mapping of degree
+        grid_degree (default: the polynomial degree)."""
         self.cfg = dict(cfg)
         self._p = make_params(cfg)
         h = ctypes.c_void_p()
-        rc = lib().orc_create(ctypes.byref(self._p), n_cells, left, right, ORDER[order], ctypes.byref(h))
+        if warp != 0.0:
+            g = cfg["poly_degree"] if grid_degree is None else grid_degree
+            rc = lib().orc_create_curved(ctypes.byref(self._p), n_cells, left, right, ORDER[order], warp, g,
+                                         ctypes.byref(h))
+        else:
+            rc = lib().orc_create(ctypes.byref(self._p), n_cells, left, right, ORDER[order], ctypes.byref(h))
         if rc != 0:
             raise RuntimeError("oracle creation failed")
         self.h = h

@@ -46,6 +46,19 @@ int orc_create(const orc_params* p, int n, double left, double right, int order,
         return 1;
     }
 }
+// curvilinear periodic cube: sine warp of amplitude `warp`, mapping of degree grid_degree
+int orc_create_curved(const orc_params* p, int n, double left, double right, int order, double warp,
+                      int grid_degree, void** out) {
+    try {
+        Solver* s = new Solver();
+        s->init(to_params(p), n, left, right, order, warp, grid_degree);
+        *out = s;
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "orc_create_curved: %s\n", e.what());
+        return 1;
+    }
+}
 void orc_destroy(void* h) { delete static_cast<Solver*>(h); }
 long long orc_ndofs(void* h) { return (long long)static_cast<Solver*>(h)->ndofs(); }
 int orc_nd(void* h) { return static_cast<Solver*>(h)->ops.nd; }

@@ -17,7 +17,8 @@ ERRORS = {1: "invalid argument", 2: "unsupported configuration", 3: "CUDA error"
 
 EXPORTED = ["ph_ctx_create", "ph_ctx_destroy", "ph_ndofs", "ph_cell_ijk", "ph_set_state", "ph_get_state",
             "ph_residual", "ph_apply_inverse_mass", "ph_rk_step", "ph_integrals", "ph_status", "ph_sync",
-            "ph_set_timing", "ph_get_timing", "ph_quotient_selftest", "ph_residual_noalloc", "ph_last_error"]
+            "ph_set_timing", "ph_get_timing", "ph_quotient_selftest", "ph_residual_noalloc", "ph_node_xyz",
+            "ph_last_error"]
 
 
 class PhParams(ctypes.Structure):
@@ -32,7 +33,8 @@ class PhParams(ctypes.Structure):
 
 class PhMeshDesc(ctypes.Structure):
     _fields_ = [("n_cells_per_direction", ctypes.c_int), ("cell_order", ctypes.c_int),
-                ("left", ctypes.c_double), ("right", ctypes.c_double)]
+                ("left", ctypes.c_double), ("right", ctypes.c_double),
+                ("warp", ctypes.c_double), ("grid_degree", ctypes.c_int)]
 
 
 class PhError(RuntimeError):
@@ -70,6 +72,7 @@ def load(build_if_missing: bool = False):
     L.ph_set_timing.argtypes = [vp, ctypes.c_int]
     L.ph_get_timing.argtypes = [vp, dp]
     L.ph_quotient_selftest.argtypes = [ctypes.c_uint64, ctypes.c_int, dp]
+    L.ph_node_xyz.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     L.ph_residual_noalloc.argtypes = [ctypes.POINTER(PhMeshDesc), ctypes.POINTER(PhParams), vp, vp, vp]
     L.ph_last_error.restype = ctypes.c_char_p
     _lib = L

@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/philip_b200.h"
@@ -168,6 +169,82 @@ void cell_order(int n, int order, std::vector<int>& ijk) {
     }
 }
 
+// Sine warp of the periodic cube [l, r]^3: each coordinate moves by
+// a/k sin(k(x-l)) sin(k(y-l)) sin(k(z-l)), k = 2 pi / (r - l); zero on the cube's faces.
+void warp_point(double l, double r, double a, double X[3]) {
+    const double k = 2.0 * M_PI / (r - l);
+    const double s = a / k * std::sin(k * (X[0] - l)) * std::sin(k * (X[1] - l)) * std::sin(k * (X[2] - l));
+    X[0] += s; X[1] += s; X[2] += s;
+}
+
+// d/dxi_dir of a nodal field f on the N1^3 GLL nodes (x fastest): out = (D along dir) f
+void nodal_derivative(const std::vector<double>& D, int N1, int dir, const double* f, double* out) {
+    const int st = dir == 0 ? 1 : dir == 1 ? N1 : N1 * N1;
+    const int NP = N1 * N1 * N1;
+    for (int node = 0; node < NP; ++node) {
+        const int pos = (node / st) % N1, base = node - pos * st;
+        double v = 0.0;
+        for (int l = 0; l < N1; ++l) v += D[pos * N1 + l] * f[base + l * st];
+        out[node] = v;
+    }
+}
+
+// Metric terms of one curvilinear cell whose mapping has the solution's degree, so the
+// mapping support points, the flux nodes and the solution nodes are the same GLL points
+// and every tensor-product operator is a 1-D derivative along one direction.
+// Cofactor by the conservative curl form (operators.cpp:2738-2884):
+//   C[l][0] = d_zeta(f_eta) - d_eta(f_zeta), C[l][1] = d_xi(f_zeta) - d_zeta(f_xi),
+//   C[l][2] = d_eta(f_xi) - d_xi(f_eta),
+// with f_j = z dy/dxi_j (l = 0), x dz/dxi_j (l = 1), y dx/dxi_j (l = 2); det J of the
+// mapping Jacobian (operators.cpp:2629-2672). Writes metric rows 0..8 (C[k][d] at k*3+d),
+// row 9 = 1 / det J, and the node coordinates; returns false on a non-positive det J.
+bool curvilinear_cell(const std::vector<double>& x, const std::vector<double>& D, int N1, double h, double left,
+                      double right, double warp, const int ijk[3], double* metric, double* xyz) {
+    const int NP = N1 * N1 * N1;
+    std::vector<double> X(3 * NP), G(9 * NP), P(9 * NP), t(NP);
+    for (int node = 0; node < NP; ++node) {
+        const int i = node % N1, j = (node / N1) % N1, k = node / (N1 * N1);
+        double p[3] = {left + h * (ijk[0] + x[i]), left + h * (ijk[1] + x[j]), left + h * (ijk[2] + x[k])};
+        warp_point(left, right, warp, p);
+        for (int d = 0; d < 3; ++d) { X[d * NP + node] = p[d]; xyz[node * 3 + d] = p[d]; }
+    }
+    for (int m = 0; m < 3; ++m)
+        for (int j = 0; j < 3; ++j) nodal_derivative(D, N1, j, &X[m * NP], &G[(m * 3 + j) * NP]);
+    // products at the nodes: row l uses (X_a, dX_b) = (z, y), (x, z), (y, x)
+    const int pa[3] = {2, 0, 1}, pb[3] = {1, 2, 0};
+    for (int l = 0; l < 3; ++l)
+        for (int j = 0; j < 3; ++j)
+            for (int node = 0; node < NP; ++node)
+                P[(l * 3 + j) * NP + node] = X[pa[l] * NP + node] * G[(pb[l] * 3 + j) * NP + node];
+    for (int l = 0; l < 3; ++l) {
+        const double* f0 = &P[(l * 3 + 0) * NP];
+        const double* f1 = &P[(l * 3 + 1) * NP];
+        const double* f2 = &P[(l * 3 + 2) * NP];
+        double* C0 = metric + (l * 3 + 0) * NP;
+        double* C1 = metric + (l * 3 + 1) * NP;
+        double* C2 = metric + (l * 3 + 2) * NP;
+        nodal_derivative(D, N1, 1, f2, C0);
+        nodal_derivative(D, N1, 2, f1, t.data());
+        for (int q = 0; q < NP; ++q) C0[q] = t[q] - C0[q];
+        nodal_derivative(D, N1, 0, f2, C1);
+        nodal_derivative(D, N1, 2, f0, t.data());
+        for (int q = 0; q < NP; ++q) C1[q] = C1[q] - t[q];
+        nodal_derivative(D, N1, 0, f1, C2);
+        nodal_derivative(D, N1, 1, f0, t.data());
+        for (int q = 0; q < NP; ++q) C2[q] = t[q] - C2[q];
+    }
+    for (int q = 0; q < NP; ++q) {
+        double J[3][3];
+        for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) J[a][b] = G[(a * 3 + b) * NP + q];
+        const double dj = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) -
+                          J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+                          J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+        if (!(dj > 1e-14)) return false;
+        metric[9 * NP + q] = 1.0 / dj;
+    }
+    return true;
+}
+
 } // namespace
 
 struct ph_ctx {
@@ -176,7 +253,11 @@ struct ph_ctx {
     double left = 0, right = 1, h = 1;
     cudaStream_t stream = nullptr;
     int device = 0;
-    bool visc = false, split = false, fp32 = false, fr = false;
+    bool visc = false, split = false, fp32 = false, fr = false, curv = false;
+    double warp = 0.0;
+    std::vector<double> xyz;            // physical node coordinates [cell][node][3]
+    double* d_metric = nullptr;         // curvilinear: [nc][10][NP] cofactor rows + 1/det J
+    double* d_xnode = nullptr;          // curvilinear: node coordinates [nc][3][NP] (integrals)
     size_t ndofs = 0;
     std::vector<int> ijk;
     int* d_nbr = nullptr;
@@ -256,6 +337,7 @@ ph::StageArgs base_args(ph_ctx* c, const double* U) {
     a.U = U; a.Fv = c->d_fv; a.nbr = c->d_nbr; a.ops = c->d_ops; a.nc = c->nc;
     a.h = c->h; a.inv_h = 1.0 / c->h; a.pen = c->pen; a.pc = c->pc; a.status = c->d_status;
     a.fr = c->fr ? 1 : 0;
+    a.metric = c->d_metric;
     return a;
 }
 
@@ -300,7 +382,17 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
     c->split = prm->use_split_form != 0;
     c->fp32 = prm->precision == PH_FP32_RESIDUAL;
     c->ndofs = (size_t)c->nc * 5 * c->NP;
+    c->warp = mesh->warp;
+    c->curv = mesh->warp != 0.0;
     cudaGetDevice(&c->device);
+    if (c->curv) {
+        const int g = mesh->grid_degree;
+        const char* why = (g != c->p) ? "curvilinear meshes take grid_degree = poly_degree"
+                          : c->visc ? "curvilinear meshes take the Euler equations"
+                          : !c->split ? "curvilinear meshes take the split form"
+                          : (prm->flux_reconstruction != 0) ? "curvilinear meshes take cDG" : nullptr;
+        if (why) { delete c; return fail(PH_ERR_UNSUPPORTED, why); }
+    }
 
     // ---- 1-D operators on the GLL nodes
     const int N1 = c->N1;
@@ -396,6 +488,35 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
             nbr[6 * cc + f] = lex2cell[(t[2] * n + t[1]) * n + t[0]];
         }
 
+    // ---- node coordinates and (curvilinear) metric terms, cells in parallel on the host
+    c->xyz.assign((size_t)c->nc * c->NP * 3, 0.0);
+    std::vector<double> metric;
+    if (c->curv) metric.assign((size_t)c->nc * 10 * c->NP, 0.0);
+    {
+        const unsigned nthr = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+        std::vector<std::thread> pool;
+        std::vector<int> ok(nthr, 1);
+        for (unsigned tI = 0; tI < nthr; ++tI)
+            pool.emplace_back([&, tI]() {
+                for (int cc = (int)tI; cc < c->nc; cc += (int)nthr) {
+                    const int* t = &c->ijk[3 * cc];
+                    double* xyz = &c->xyz[(size_t)cc * c->NP * 3];
+                    if (c->curv) {
+                        if (!curvilinear_cell(x, D, N1, c->h, c->left, c->right, c->warp, t,
+                                              &metric[(size_t)cc * 10 * c->NP], xyz)) ok[tI] = 0;
+                    } else {
+                        for (int node = 0; node < c->NP; ++node) {
+                            const int ii[3] = {node % N1, (node / N1) % N1, node / (N1 * N1)};
+                            for (int d = 0; d < 3; ++d) xyz[node * 3 + d] = c->left + c->h * (t[d] + x[ii[d]]);
+                        }
+                    }
+                }
+            });
+        for (auto& th : pool) th.join();
+        for (int v : ok)
+            if (!v) { delete c; return fail(PH_ERR_INVALID, "non-positive det J: the warp folds a cell"); }
+    }
+
     // ---- device buffers
     const size_t N = c->ndofs;
     int bad = 0;
@@ -411,6 +532,8 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
     if (c->fp32) bad |= dalloc(&c->d_comp, N);
     bad |= dalloc(&c->d_partial, 3 * (size_t)c->nc);
     bad |= dalloc(&c->d_status, 1);
+    if (c->curv) bad |= dalloc(&c->d_metric, metric.size());
+    if (c->curv) bad |= dalloc(&c->d_xnode, (size_t)3 * c->nc * c->NP);
     if (bad) { ph_ctx_destroy(c); return fail(PH_ERR_NOMEM, "device allocation failed"); }
     cudaError_t e = cudaSuccess;
     e = cudaMemcpy(c->d_nbr, nbr.data(), nbr.size() * sizeof(int), cudaMemcpyHostToDevice);
@@ -419,6 +542,16 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
     if (e == cudaSuccess) e = cudaMemset(c->d_status, 0, sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMemset(c->d_sol, 0, N * sizeof(double));
     if (e == cudaSuccess && c->d_comp) e = cudaMemset(c->d_comp, 0, N * sizeof(double));
+    if (e == cudaSuccess && c->d_metric)
+        e = cudaMemcpy(c->d_metric, metric.data(), metric.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && c->d_xnode) {
+        std::vector<double> xn((size_t)3 * c->nc * c->NP);
+        for (int cc = 0; cc < c->nc; ++cc)
+            for (int d = 0; d < 3; ++d)
+                for (int node = 0; node < c->NP; ++node)
+                    xn[((size_t)cc * 3 + d) * c->NP + node] = c->xyz[((size_t)cc * c->NP + node) * 3 + d];
+        e = cudaMemcpy(c->d_xnode, xn.data(), xn.size() * sizeof(double), cudaMemcpyHostToDevice);
+    }
     if (e != cudaSuccess) { ph_ctx_destroy(c); return fail(PH_ERR_CUDA, cudaGetErrorString(e)); }
     c->h_partial.resize(3 * (size_t)c->nc);
     *out = c;
@@ -428,7 +561,7 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
 int ph_ctx_destroy(ph_ctx* c) {
     if (!c) return PH_OK;
     void* ptrs[] = {c->d_nbr, c->d_ops, c->d_itab, c->d_sol, c->d_stA, c->d_stB, c->d_acc, c->d_carry,
-                    c->d_fv, c->d_comp, c->d_tmpA, c->d_tmpB, c->d_partial, c->d_status};
+                    c->d_fv, c->d_comp, c->d_tmpA, c->d_tmpB, c->d_partial, c->d_status, c->d_metric, c->d_xnode};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -437,6 +570,12 @@ int ph_ctx_destroy(ph_ctx* c) {
 }
 
 int64_t ph_ndofs(const ph_ctx* c) { return c ? (int64_t)c->ndofs : -1; }
+
+int ph_node_xyz(const ph_ctx* c, double* xyz) {
+    if (!c || !xyz) return fail(PH_ERR_INVALID, "null argument");
+    std::memcpy(xyz, c->xyz.data(), c->xyz.size() * sizeof(double));
+    return PH_OK;
+}
 
 int ph_cell_ijk(const ph_ctx* c, int32_t* ijk) {
     if (!c || !ijk) return fail(PH_ERR_INVALID, "null argument");
@@ -499,12 +638,12 @@ int ph_apply_inverse_mass(ph_ctx* c, const double* R, double* out, int where) {
     const double inv_detj = 1.0 / (c->h * c->h * c->h);
     cudaError_t e;
     switch (c->N1) {
-    case 2: e = ph::launch_inverse_mass<2>(dR, dO, c->d_ops, c->nc, inv_detj, c->stream); break;
-    case 3: e = ph::launch_inverse_mass<3>(dR, dO, c->d_ops, c->nc, inv_detj, c->stream); break;
-    case 4: e = ph::launch_inverse_mass<4>(dR, dO, c->d_ops, c->nc, inv_detj, c->stream); break;
-    case 5: e = ph::launch_inverse_mass<5>(dR, dO, c->d_ops, c->nc, inv_detj, c->stream); break;
-    case 6: e = ph::launch_inverse_mass<6>(dR, dO, c->d_ops, c->nc, inv_detj, c->stream); break;
-    case 7: e = ph::launch_inverse_mass<7>(dR, dO, c->d_ops, c->nc, inv_detj, c->stream); break;
+    case 2: e = ph::launch_inverse_mass<2>(dR, dO, c->d_ops, c->nc, inv_detj, c->d_metric, c->stream); break;
+    case 3: e = ph::launch_inverse_mass<3>(dR, dO, c->d_ops, c->nc, inv_detj, c->d_metric, c->stream); break;
+    case 4: e = ph::launch_inverse_mass<4>(dR, dO, c->d_ops, c->nc, inv_detj, c->d_metric, c->stream); break;
+    case 5: e = ph::launch_inverse_mass<5>(dR, dO, c->d_ops, c->nc, inv_detj, c->d_metric, c->stream); break;
+    case 6: e = ph::launch_inverse_mass<6>(dR, dO, c->d_ops, c->nc, inv_detj, c->d_metric, c->stream); break;
+    case 7: e = ph::launch_inverse_mass<7>(dR, dO, c->d_ops, c->nc, inv_detj, c->d_metric, c->stream); break;
     default: return fail(PH_ERR_UNSUPPORTED, "polynomial degree");
     }
     if (e != cudaSuccess) return fail(PH_ERR_CUDA, cudaGetErrorString(e));
@@ -560,12 +699,12 @@ int ph_integrals(ph_ctx* c, double out[4]) {
     cudaError_t e;
     const double gam = c->prm.gamma_gas, gm1 = gam - 1.0;
     switch (c->N1) {
-    case 2: e = ph::launch_integrals<2>(c->d_sol, c->d_itab, c->nc, c->h, gam, gm1, c->d_partial, c->stream); break;
-    case 3: e = ph::launch_integrals<3>(c->d_sol, c->d_itab, c->nc, c->h, gam, gm1, c->d_partial, c->stream); break;
-    case 4: e = ph::launch_integrals<4>(c->d_sol, c->d_itab, c->nc, c->h, gam, gm1, c->d_partial, c->stream); break;
-    case 5: e = ph::launch_integrals<5>(c->d_sol, c->d_itab, c->nc, c->h, gam, gm1, c->d_partial, c->stream); break;
-    case 6: e = ph::launch_integrals<6>(c->d_sol, c->d_itab, c->nc, c->h, gam, gm1, c->d_partial, c->stream); break;
-    case 7: e = ph::launch_integrals<7>(c->d_sol, c->d_itab, c->nc, c->h, gam, gm1, c->d_partial, c->stream); break;
+    case 2: e = ph::launch_integrals<2>(c->d_sol, c->d_xnode, c->d_itab, c->nc, c->h, gam, gm1, c->d_partial, c->stream); break;
+    case 3: e = ph::launch_integrals<3>(c->d_sol, c->d_xnode, c->d_itab, c->nc, c->h, gam, gm1, c->d_partial, c->stream); break;
+    case 4: e = ph::launch_integrals<4>(c->d_sol, c->d_xnode, c->d_itab, c->nc, c->h, gam, gm1, c->d_partial, c->stream); break;
+    case 5: e = ph::launch_integrals<5>(c->d_sol, c->d_xnode, c->d_itab, c->nc, c->h, gam, gm1, c->d_partial, c->stream); break;
+    case 6: e = ph::launch_integrals<6>(c->d_sol, c->d_xnode, c->d_itab, c->nc, c->h, gam, gm1, c->d_partial, c->stream); break;
+    case 7: e = ph::launch_integrals<7>(c->d_sol, c->d_xnode, c->d_itab, c->nc, c->h, gam, gm1, c->d_partial, c->stream); break;
     default: return fail(PH_ERR_UNSUPPORTED, "polynomial degree");
     }
     if (e != cudaSuccess) return fail(PH_ERR_CUDA, cudaGetErrorString(e));
@@ -580,7 +719,9 @@ int ph_integrals(ph_ctx* c, double out[4]) {
     const double vol = std::pow(c->right - c->left, 3);
     out[0] = ke / vol;
     out[1] = ens / vol;
-    out[2] = 2.0 * out[1] / c->prm.reynolds_number_inf;
+    // zero for inviscid flow (PeriodicTurbulence::get_vorticity_based_dissipation_rate,
+    // periodic_turbulence.cpp:717-725)
+    out[2] = c->visc ? 2.0 * out[1] / c->prm.reynolds_number_inf : 0.0;
     out[3] = wave;
     return PH_OK;
 }
@@ -774,6 +915,7 @@ __global__ void noalloc_neighbours(int n, int morton, int levels, int* nbr) {
 extern "C" int ph_residual_noalloc(const ph_mesh_desc* mesh, const ph_params* prm, const double* U, double* R,
                                    void* cuda_stream) {
     if (!mesh || !prm || !U || !R) return fail(PH_ERR_INVALID, "null argument");
+    if (mesh->warp != 0.0) return fail(PH_ERR_UNSUPPORTED, "ph_residual_noalloc: affine meshes only (warp = 0)");
     if (prm->flux_nodes_type != 1 || prm->overintegration != 0)
         return fail(PH_ERR_UNSUPPORTED, "the GPU path is collocated: flux_nodes_type = GLL and overintegration = 0");
     if (prm->poly_degree < 1 || prm->poly_degree > 6) return fail(PH_ERR_UNSUPPORTED, "poly_degree must be 1..6");

@@ -10,11 +10,11 @@ namespace ph {
 
 template <int N1> constexpr int cells_per_cta() { return N1 == 2 ? 16 : N1 == 3 ? 4 : N1 == 4 ? 2 : 1; }
 
-template <typename R, int N1, bool VISC, bool SPLIT, int FS>
+template <typename R, int N1, bool VISC, bool SPLIT, int FS, bool CURV = false>
 static cudaError_t launch_one(const StageArgs& a, cudaStream_t s) {
     constexpr int CPC = cells_per_cta<N1>();
-    using L = Layout<R, N1, CPC, VISC, SPLIT>;
-    auto kern = residual_kernel<R, N1, CPC, VISC, SPLIT, FS>;
+    using L = Layout<R, N1, CPC, VISC, SPLIT, CURV>;
+    auto kern = residual_kernel<R, N1, CPC, VISC, SPLIT, FS, CURV>;
     int dev = 0;
     cudaGetDevice(&dev);
     static bool configured[64] = {false};
@@ -33,6 +33,10 @@ static cudaError_t launch_prec(const StageArgs& a, bool visc, bool split, cudaSt
     // the Chandrashekar + EC/Roe (+ BR2) combination has its own compile-time instance
     const bool hot = split && a.pc.two_point == TP_CH && a.pc.conv_flux == CF_EC_ROE &&
                      (!visc || a.pc.diss_flux == DF_BR2);
+    if (a.metric) {   // curvilinear cells: split-form Euler (checked by the host)
+        if (visc || !split) return cudaErrorInvalidValue;
+        return hot ? launch_one<R, N1, false, true, 1, true>(a, s) : launch_one<R, N1, false, true, 0, true>(a, s);
+    }
     if (visc) {
         if (split) return hot ? launch_one<R, N1, true, true, 1>(a, s) : launch_one<R, N1, true, true, 0>(a, s);
         return launch_one<R, N1, true, false, 0>(a, s);
@@ -92,16 +96,16 @@ cudaError_t launch_aux(const double* U, const int* nbr, const OpTab* ops, int nc
 
 template <int N1>
 cudaError_t launch_inverse_mass(const double* in, double* out, const OpTab* ops, int nc, double inv_detj,
-                                cudaStream_t s) {
-    inverse_mass_kernel<N1><<<nc, 128, 0, s>>>(in, out, ops, nc, inv_detj);
+                                const double* metric, cudaStream_t s) {
+    inverse_mass_kernel<N1><<<nc, 128, 0, s>>>(in, out, ops, nc, inv_detj, metric);
     return cudaGetLastError();
 }
 
-template <int N1>
-cudaError_t launch_integrals(const double* U, const IntegralTab* tab, int nc, double h, double gam, double gm1,
-                             double* partial, cudaStream_t s) {
-    auto kern = integrals_kernel<N1>;
-    constexpr size_t bytes = integrals_smem_bytes<N1>();
+template <int N1, bool CURV>
+static cudaError_t launch_integrals_one(const double* U, const double* X, const IntegralTab* tab, int nc, double h,
+                                       double gam, double gm1, double* partial, cudaStream_t s) {
+    auto kern = integrals_kernel<N1, CURV>;
+    constexpr size_t bytes = integrals_smem_bytes<N1, CURV>();
     int dev = 0;
     cudaGetDevice(&dev);
     static bool configured[64] = {false};
@@ -110,16 +114,24 @@ cudaError_t launch_integrals(const double* U, const IntegralTab* tab, int nc, do
         if (e != cudaSuccess) return e;
         configured[dev] = true;
     }
-    kern<<<nc, 256, bytes, s>>>(U, tab, nc, h, gam, gm1, partial);
+    kern<<<nc, 256, bytes, s>>>(U, X, tab, nc, h, gam, gm1, partial);
     return cudaGetLastError();
+}
+
+template <int N1>
+cudaError_t launch_integrals(const double* U, const double* X, const IntegralTab* tab, int nc, double h, double gam,
+                             double gm1, double* partial, cudaStream_t s) {
+    return X ? launch_integrals_one<N1, true>(U, X, tab, nc, h, gam, gm1, partial, s)
+             : launch_integrals_one<N1, false>(U, X, tab, nc, h, gam, gm1, partial, s);
 }
 
 template cudaError_t launch_stage<PH_N1>(const StageArgs&, int, bool, bool, cudaStream_t);
 template void stage_launch_shape<PH_N1>(int, bool, bool, int*, int*, size_t*);
 template cudaError_t launch_aux<PH_N1>(const double*, const int*, const OpTab*, int, double, const PhysConst&, int,
                                        double*, cudaStream_t);
-template cudaError_t launch_inverse_mass<PH_N1>(const double*, double*, const OpTab*, int, double, cudaStream_t);
-template cudaError_t launch_integrals<PH_N1>(const double*, const IntegralTab*, int, double, double, double, double*,
-                                             cudaStream_t);
+template cudaError_t launch_inverse_mass<PH_N1>(const double*, double*, const OpTab*, int, double, const double*,
+                                                cudaStream_t);
+template cudaError_t launch_integrals<PH_N1>(const double*, const double*, const IntegralTab*, int, double, double,
+                                             double, double*, cudaStream_t);
 
 } // namespace ph

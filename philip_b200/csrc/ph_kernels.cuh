@@ -67,15 +67,20 @@ struct StageArgs {
     double* carry_out;        // a_carry * k for the stage after next
     double a_carry;
     double dt;
+    // curvilinear cells: [nc][10][NP], rows k*3+d = metric cofactor C[k][d] at the
+    // volume nodes, row 9 = 1 / det J (nullptr on affine meshes)
+    const double* metric;
 };
 
-template <typename R, int N1, int CPC, bool VISC, bool SPLIT>
+// CURV: curvilinear cells (split-form Euler): the per-node metric cofactor (9 values)
+// takes the place of the precomputed flux rows in sX.
+template <typename R, int N1, int CPC, bool VISC, bool SPLIT, bool CURV = false>
 struct Layout {
     static constexpr int NP = N1 * N1 * N1, NF = N1 * N1;
     static constexpr int NQV = 10;                     // rho v0 v1 v2 p E a b la lb vsq -> packed 11
     static constexpr int NQS = 11;
     static constexpr int TR = VISC ? 9 : 5;            // trace values per face node: u (5) [+ ext viscous flux (4)]
-    static constexpr int NX = (VISC ? 12 : 0) + (SPLIT ? 0 : 15);
+    static constexpr int NX = (VISC ? 12 : 0) + (SPLIT ? 0 : 15) + (CURV ? 9 : 0);
     static constexpr int oOps = 0;                      // D, Dsk, B, w as R
     static constexpr int nOps = 3 * N1 * N1 + N1;
     static constexpr int oU = (oOps + nOps + 1) & ~1;
@@ -149,11 +154,11 @@ __device__ __forceinline__ void check_state_fp64(double u[5], double gm1, unsign
 // One face node of phase 3: the numerical flux at the canonical orientation (the
 // left cell is the interior side, normal +e_d) lifted into this cell with its sign.
 // The convective flux is evaluated in the frame whose x axis is the face normal.
-template <typename R, int N1, int CPC, bool VISC, bool SPLIT>
+template <typename R, int N1, int CPC, bool VISC, bool SPLIT, bool CURV>
 __device__ __forceinline__ void face_item(const Cst<R>& cst, int tp, int cf, int df, int ucv, const R* sU,
                                           const R* sD, R* sT, const R* sX, int c, int f, int fn, R pen,
                                           R inv_wend) {
-    using L = Layout<R, N1, CPC, VISC, SPLIT>;
+    using L = Layout<R, N1, CPC, VISC, SPLIT, CURV>;
     constexpr int NP = L::NP, NF = L::NF, TR = L::TR, NQS = L::NQS;
     const int d = f >> 1;
     const bool plus = (f & 1);                    // this cell is the left (minus) side
@@ -163,6 +168,23 @@ __device__ __forceinline__ void face_item(const Cst<R>& cst, int tp, int cf, int
     R uo[5], ue[5];
 #pragma unroll
     for (int s = 0; s < 5; ++s) { uo[s] = sU[(c * 5 + s) * NP + node]; ue[s] = tr[s * NF + fn]; }
+    if constexpr (CURV) {
+        // normal metric C[:, d] at this face node: the canonical normal (from the left cell
+        // into the right one) is the same vector seen from either side; |C n| scales the flux
+        const R* X = sX + c * L::NX * NP;
+        const R m[3] = {X[(0 * 3 + d) * NP + node], X[(1 * 3 + d) * NP + node], X[(2 * 3 + d) * NP + node]};
+        const R J = rsqrt_<R>(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+        const R nrm[3] = {qdiv<R>(m[0], J), qdiv<R>(m[1], J), qdiv<R>(m[2], J)};
+        NodeQ<R> qo, qe;
+        load_q<R>(sD + c * NQS * NP, NP, node, qo);
+        node_prepare<R>(ue, tp, cst.gm1, qe, nullptr);
+        R F[5];
+        if (plus) conv_num_flux_n<R>(uo, ue, qo, qe, nrm, tp, cf, cst, F);
+        else conv_num_flux_n<R>(ue, uo, qe, qo, nrm, tp, cf, cst, F);
+#pragma unroll
+        for (int s = 0; s < 5; ++s) tr[s * NF + fn] = -sgn * J * F[s] * inv_wend;
+        return;
+    }
     R ro[5], re[5];
     rotate_state<R>(uo, d, ro);
     rotate_state<R>(ue, d, re);
@@ -216,11 +238,11 @@ __device__ __forceinline__ void face_item(const Cst<R>& cst, int tp, int cf, int
 
 // Phase 4 for direction d: warp segments of N1 lanes own 1-D lines along d. The
 // two-point flux is evaluated in the frame whose x axis is e_d.
-template <typename R, int N1, int CPC, bool VISC, bool SPLIT>
+template <typename R, int N1, int CPC, bool VISC, bool SPLIT, bool CURV>
 __device__ __forceinline__ void volume_dir(int d, const Cst<R>& cst, int tp, const R* sD, const R* sX, R* sA,
                                            const R* sOpsD, const R* sOpsDsk, int lc, int lt, int pos, int seg,
                                            bool lvalid) {
-    using L = Layout<R, N1, CPC, VISC, SPLIT>;
+    using L = Layout<R, N1, CPC, VISC, SPLIT, CURV>;
     constexpr int NP = L::NP, NQS = L::NQS;
     const int st = (d == 0) ? 1 : (d == 1) ? N1 : N1 * N1;
     const int t1 = (d == 0) ? 1 : 0, t2 = (d == 2) ? 1 : 2;
@@ -230,7 +252,37 @@ __device__ __forceinline__ void volume_dir(int d, const Cst<R>& cst, int tp, con
     const int node = node_of<N1>(d == 0 ? pos : cc[0], d == 1 ? pos : cc[1], d == 2 ? pos : cc[2]);
     const int base = node - pos * st;
     R acc[5] = {R(0), R(0), R(0), R(0), R(0)};
-    if constexpr (SPLIT) {
+    if constexpr (CURV) {
+        // curvilinear: the pair flux is dotted with the averaged metric column
+        // 1/2 (C_i[:, d] + C_j[:, d]), symmetric in (i, j) like the flux itself
+        const R* Dq = sD + lc * NQS * NP;
+        const R* X = sX + lc * L::NX * NP;
+        NodeQ<R> qi;
+        load_q<R>(Dq, NP, node, qi);
+        const R mi[3] = {X[(0 * 3 + d) * NP + node], X[(1 * 3 + d) * NP + node], X[(2 * 3 + d) * NP + node]};
+        const int segbase = seg * N1;
+#pragma unroll 1
+        for (int k = 1; k <= N1 / 2; ++k) {
+            const int jp = (pos + k) % N1;
+            const int nj = base + jp * st;
+            NodeQ<R> qj;
+            load_q<R>(Dq, NP, nj, qj);
+            const R nv[3] = {R(0.5) * (mi[0] + X[(0 * 3 + d) * NP + nj]), R(0.5) * (mi[1] + X[(1 * 3 + d) * NP + nj]),
+                             R(0.5) * (mi[2] + X[(2 * 3 + d) * NP + nj])};
+            R F[5];
+            two_point_n<R>(qi, qj, nv, tp, cst, F);
+            const R cj = sOpsDsk[pos * N1 + jp];
+            const int src = segbase + (pos - k + N1) % N1;
+            const R cr = sOpsDsk[pos * N1 + (pos - k + N1) % N1];
+            const bool dup = ((N1 & 1) == 0) && (2 * k == N1);
+#pragma unroll
+            for (int s = 0; s < 5; ++s) {
+                const R fr = __shfl_sync(0xffffffffu, F[s], src);
+                acc[s] += cj * F[s];
+                if (!dup) acc[s] += cr * fr;
+            }
+        }
+    } else if constexpr (SPLIT) {
         const R* Dq = sD + lc * NQS * NP;
         NodeQ<R> qi;
         load_q_rot<R>(Dq, NP, node, d, qi);
@@ -304,10 +356,11 @@ __device__ __forceinline__ void volume_dir(int d, const Cst<R>& cst, int tp, con
 // run time), 1 = Chandrashekar split flux + entropy-conserving baseline with Roe
 // dissipation (+ BR2 when viscous) fixed at compile time, which removes the unused
 // variants from the instruction stream.
-template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int FS>
-__global__ void __launch_bounds__(Layout<R, N1, CPC, VISC, SPLIT>::NT, Layout<R, N1, CPC, VISC, SPLIT>::MINB)
+template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int FS, bool CURV = false>
+__global__ void __launch_bounds__(Layout<R, N1, CPC, VISC, SPLIT, CURV>::NT, Layout<R, N1, CPC, VISC, SPLIT, CURV>::MINB)
 residual_kernel(const StageArgs a) {
-    using L = Layout<R, N1, CPC, VISC, SPLIT>;
+    static_assert(!CURV || (SPLIT && !VISC), "curvilinear cells: split-form Euler only");
+    using L = Layout<R, N1, CPC, VISC, SPLIT, CURV>;
     constexpr int NP = L::NP, NF = L::NF, NT = L::NT, TR = L::TR, NQS = L::NQS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R* sm = reinterpret_cast<R*>(smem_raw);
@@ -376,6 +429,10 @@ residual_kernel(const StageArgs a) {
 #pragma unroll
             for (int i = 0; i < 12; ++i) X[i * NP + node] = (R)__ldg(&a.Fv[((size_t)cell * 12 + i) * NP + node]);
         }
+        if constexpr (CURV) {
+#pragma unroll
+            for (int i = 0; i < 9; ++i) X[i * NP + node] = (R)__ldg(&a.metric[((size_t)cell * 10 + i) * NP + node]);
+        }
         if constexpr (!SPLIT) {
             constexpr int o = VISC ? 12 : 0;
             R F[5];
@@ -400,7 +457,7 @@ residual_kernel(const StageArgs a) {
             const int fn = it % NF;
             const int f = (it / NF) % 6;
             const int c = it / (NF * 6);
-            face_item<R, N1, CPC, VISC, SPLIT>(cst, tp, cf, df, ucv, sU, sD, sT, sX, c, f, fn, pen, inv_wend);
+            face_item<R, N1, CPC, VISC, SPLIT, CURV>(cst, tp, cf, df, ucv, sU, sD, sT, sX, c, f, fn, pen, inv_wend);
         }
     }
 
@@ -416,7 +473,7 @@ residual_kernel(const StageArgs a) {
 #pragma unroll 1
         for (int d = 0; d < 3; ++d) {
             __syncthreads();
-            volume_dir<R, N1, CPC, VISC, SPLIT>(d, cst, tp, sD, sX, sA, sOpsD, sOpsDsk, lc, lt, pos, seg, lvalid);
+            volume_dir<R, N1, CPC, VISC, SPLIT, CURV>(d, cst, tp, sD, sX, sA, sOpsD, sOpsDsk, lc, lt, pos, seg, lvalid);
         }
         __syncthreads();
     }
@@ -479,10 +536,11 @@ residual_kernel(const StageArgs a) {
         if (a.mode == 0) {
             const int x = node % N1, y = (node / N1) % N1, z = node / (N1 * N1);
             const double W = a.ops->w[x] * a.ops->w[y] * a.ops->w[z];
-            a.out[dof] = W * a.h * a.h * G;
+            a.out[dof] = CURV ? W * G : W * a.h * a.h * G;
             continue;
         }
-        const double k = G * a.inv_h;
+        // affine: M^-1 R = G / h; curvilinear (cDG): R / (W det J) = G / det J
+        const double k = CURV ? G * __ldg(&a.metric[((size_t)cell * 10 + 9) * NP + node]) : G * a.inv_h;
         if (a.mode == 1) { a.out[dof] = k; continue; }
         const double un = a.Un[dof];
         const double base = a.acc_in ? a.acc_in[dof] : (a.inc_mode ? 0.0 : un);
@@ -634,8 +692,10 @@ static __global__ void quotient_selftest_kernel(unsigned long long seed, int n, 
 // Inverse mass on its own (DGBase::apply_inverse_global_mass_matrix, affine cells)
 // ------------------------------------------------------------------------------------
 template <int N1>
+// metric != nullptr: curvilinear cDG cells, M^-1 = 1 / (W det J) per node (the weight-adjusted
+// inverse of dg_base.cpp:4217-4249 on collocated GLL nodes)
 __global__ void inverse_mass_kernel(const double* __restrict__ in, double* __restrict__ out, const OpTab* ops,
-                                    int nc, double inv_detj) {
+                                    int nc, double inv_detj, const double* __restrict__ metric) {
     constexpr int NP = N1 * N1 * N1;
     __shared__ double s0[5 * NP], s1[5 * NP], sM[N1 * N1];
     const int cell = blockIdx.x;
@@ -655,7 +715,8 @@ __global__ void inverse_mass_kernel(const double* __restrict__ in, double* __res
         double* t = src; src = dst; dst = t;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < 5 * NP; i += blockDim.x) out[(size_t)cell * 5 * NP + i] = src[i] * inv_detj;
+    for (int i = threadIdx.x; i < 5 * NP; i += blockDim.x)
+        out[(size_t)cell * 5 * NP + i] = src[i] * (metric ? metric[((size_t)cell * 10 + 9) * NP + i % NP] : inv_detj);
 }
 
 } // namespace ph

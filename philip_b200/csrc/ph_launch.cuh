@@ -17,11 +17,12 @@ cudaError_t launch_aux(const double* U, const int* nbr, const OpTab* ops, int nc
 // DGBase::apply_inverse_global_mass_matrix on its own
 template <int N1>
 cudaError_t launch_inverse_mass(const double* in, double* out, const OpTab* ops, int nc, double inv_detj,
-                                cudaStream_t s);
+                                const double* metric, cudaStream_t s);
 // Taylor-Green integrals, per-cell partial sums
+// X: node coordinates [nc][3][NP] of curvilinear cells, nullptr on affine meshes
 template <int N1>
-cudaError_t launch_integrals(const double* U, const IntegralTab* tab, int nc, double h, double gam, double gm1,
-                             double* partial, cudaStream_t s);
+cudaError_t launch_integrals(const double* U, const double* X, const IntegralTab* tab, int nc, double h, double gam,
+                             double gm1, double* partial, cudaStream_t s);
 // shared memory and threads of the residual kernel (for reporting / tests)
 template <int N1>
 void stage_launch_shape(int fp32, bool visc, bool split, int* threads, int* cells_per_cta, size_t* smem);

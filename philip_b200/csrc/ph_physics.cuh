@@ -317,6 +317,170 @@ __device__ __forceinline__ void conv_num_flux(const R uL[5], const R uR[5], cons
     }
 }
 
+// ---- general-normal forms, for curvilinear cells: the flux dotted with a vector n
+// (sum_k n_k F_k), with n the metric-averaged reference direction in the volume and the
+// unit physical normal on faces (strong_dg.cpp:1235-1515, :3354-3452).
+
+// Two-point flux dotted with n.
+template <typename R>
+__device__ __forceinline__ void two_point_n(const NodeQ<R>& i, const NodeQ<R>& j, const R n[3], int tp,
+                                            const Cst<R>& c, R F[5]) {
+    if (tp == TP_CH || tp == TP_RA) {
+        const R rho_log = log_mean<R>(i.a, j.a, i.la, j.la);
+        const R b_log = log_mean<R>(i.b, j.b, i.lb, j.lb);
+        R va[3], vsq = R(0), vn = R(0);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { va[k] = R(0.5) * (i.v[k] + j.v[k]); vsq += va[k] * va[k]; vn += va[k] * n[k]; }
+        R p_hat, H;
+        if (tp == TP_CH) {
+            p_hat = qdiv<R>(i.rho + j.rho, R(2) * (i.b + j.b));
+            const R g2b = R(2) * b_log * c.gm1;
+            H = qdiv<R>(rho_log + g2b * p_hat, g2b * rho_log) + vsq;
+        } else {
+            p_hat = R(0.5) * (i.p + j.p);
+            const R gb = b_log * c.gm1;
+            H = qdiv<R>(rho_log + R(2) * gb * p_hat, gb * rho_log) + vsq;
+        }
+        H -= R(0.5) * (R(0.5) * (i.vsq + j.vsq));
+        const R m = rho_log * vn;
+        F[0] = m;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) F[1 + k] = m * va[k] + p_hat * n[k];
+        F[4] = m * H;
+        if (tp == TP_RA) {
+            R vni = R(0), vnj = R(0);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) { vni += i.v[k] * n[k]; vnj += j.v[k] * n[k]; }
+            F[4] -= R(0.5) * (i.p * vni + j.p * vnj);
+        }
+    } else if (tp == TP_IR) {
+        const R z0a = R(0.5) * (i.a + j.a), z4a = R(0.5) * (i.b + j.b);
+        const R l0 = log_mean<R>(i.a, j.a, i.la, j.la);
+        const R l4 = log_mean<R>(i.b, j.b, i.lb, j.lb);
+        const R rho = z0a * l4;
+        R v[3], vv = R(0), vn = R(0);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const R zk = R(0.5) * (i.a * i.v[k] + j.a * j.v[k]);
+            v[k] = qdiv<R>(zk, z0a); vv += v[k] * v[k]; vn += v[k] * n[k];
+        }
+        const R p = qdiv<R>(z4a, z0a);
+        R H = (c.gam + R(1)) * qdiv<R>(l4, l0) + c.gm1 * p;
+        H /= R(2) * c.gam;
+        H *= qdiv<R>(c.gam, rho * c.gm1);
+        H += R(0.5) * vv;
+        const R m = rho * vn;
+        F[0] = m;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) F[1 + k] = m * v[k] + p * n[k];
+        F[4] = m * H;
+    } else {   // KG
+        const R rho = (i.rho + j.rho) / R(2);
+        const R p = (i.p + j.p) / R(2);
+        R v[3], vn = R(0);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { v[k] = R(0.5) * (i.v[k] + j.v[k]); vn += v[k] * n[k]; }
+        const R e = (i.vsq + j.vsq) / R(2);
+        const R m = rho * vn;
+        F[0] = m;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) F[1 + k] = m * v[k] + p * n[k];
+        F[4] = m * e + p * vn;
+    }
+}
+
+// Physical convective flux dotted with n.
+template <typename R>
+__device__ __forceinline__ void conv_flux_n(const NodeQ<R>& q, const R n[3], R F[5]) {
+    const R H = qdiv<R>(q.E, q.rho) + qdiv<R>(q.p, q.rho);
+    const R vn = q.v[0] * n[0] + q.v[1] * n[1] + q.v[2] * n[2];
+    const R m = q.rho * vn;
+    F[0] = m;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) F[1 + k] = m * q.v[k] + q.p * n[k];
+    F[4] = m * H;
+}
+
+// Roe-Pike dissipation -1/2 |A_roe(n)| (uR - uL) for a unit normal n
+// (convective_numerical_flux.cpp:333-480 with the entropy fix of :215-232).
+template <typename R>
+__device__ __forceinline__ void roe_dissipation_n(const NodeQ<R>& L, const NodeQ<R>& Rq, const R n[3],
+                                                  const Cst<R>& c, R out[5]) {
+    const R vnL = L.v[0] * n[0] + L.v[1] * n[1] + L.v[2] * n[2];
+    const R vnR = Rq.v[0] * n[0] + Rq.v[1] * n[1] + Rq.v[2] * n[2];
+    const R hL = qdiv<R>(L.E + L.p, L.rho), hR = qdiv<R>(Rq.E + Rq.p, Rq.rho);
+    const R r = rsqrt_<R>(qdiv<R>(Rq.rho, L.rho)), rp1 = r + R(1);
+    const R rho_a = r * L.rho;
+    R va[3], v2a = R(0), vna = R(0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        va[k] = qdiv<R>(r * Rq.v[k] + L.v[k], rp1); v2a = v2a + va[k] * va[k]; vna = vna + va[k] * n[k];
+    }
+    const R ha = qdiv<R>(r * hR + hL, rp1);
+    const R c2a = c.gm1 * (ha - R(0.5) * v2a);
+    R ca = R(1e10);
+    if (c2a > R(0)) ca = rsqrt_<R>(c2a);
+    R eig[3] = {rabs(vna - ca), rabs(vna), rabs(vna + ca)};
+    const R cL = rsqrt_<R>(qdiv<R>(L.p * c.gam, L.rho)), cR = rsqrt_<R>(qdiv<R>(Rq.p * c.gam, Rq.rho));
+    const R eL[3] = {rabs(vnL - cL), rabs(vnL), rabs(vnL + cL)};
+    const R eR[3] = {rabs(vnR - cR), rabs(vnR), rabs(vnR + cR)};
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+        const R a1 = rabs(eig[e] - eL[e]), a2 = rabs(eR[e] - eig[e]);
+        const R eps = a1 > a2 ? a1 : a2;
+        if (eig[e] < eps) eig[e] = R(0.5) * (qdiv<R>(eig[e] * eig[e], eps) + eps);
+    }
+    const R dp = Rq.p - L.p, drho = Rq.rho - L.rho, dvn = vnR - vnL;
+    R dvt[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) dvt[k] = (Rq.v[k] - L.v[k]) - dvn * n[k];
+    const R inv2c2 = qdiv<R>(R(1), R(2) * c2a);
+    const R c0 = eig[0] * (dp - rho_a * ca * dvn) * inv2c2;
+    const R c1 = eig[1] * (drho - R(2) * dp * inv2c2);
+    const R c2 = eig[1] * rho_a;
+    const R c3 = eig[2] * (dp + rho_a * ca * dvn) * inv2c2;
+    R A[5];
+    A[0] = c0 + c1 + c3;
+    R dvtv = R(0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        A[1 + k] = c0 * (va[k] - ca * n[k]) + c1 * va[k] + c2 * dvt[k] + c3 * (va[k] + ca * n[k]);
+        dvtv += va[k] * dvt[k];
+    }
+    A[4] = c0 * (ha - ca * vna) + c1 * v2a * R(0.5) + c2 * dvtv + c3 * (ha + ca * vna);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) out[k] = R(-0.5) * A[k];
+}
+
+// Convective numerical flux dotted with the unit normal n (L = the side n points away from).
+template <typename R>
+__device__ __forceinline__ void conv_num_flux_n(const R uL[5], const R uR[5], const NodeQ<R>& L, const NodeQ<R>& Rq,
+                                                const R n[3], int tp, int cf, const Cst<R>& c, R out[5]) {
+    if (cf == CF_EC || cf == CF_EC_LXF || cf == CF_EC_ROE) {
+        two_point_n<R>(L, Rq, n, tp, c, out);
+    } else {
+        R FL[5], FR[5];
+        conv_flux_n<R>(L, n, FL);
+        conv_flux_n<R>(Rq, n, FR);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) out[k] = R(0.5) * (FL[k] + FR[k]);
+    }
+    if (cf == CF_LXF || cf == CF_EC_LXF) {
+        const R vnL = L.v[0] * n[0] + L.v[1] * n[1] + L.v[2] * n[2];
+        const R vnR = Rq.v[0] * n[0] + Rq.v[1] * n[1] + Rq.v[2] * n[2];
+        const R eLv = rabs(vnL) + rsqrt_<R>(qdiv<R>(L.p * c.gam, L.rho));
+        const R eRv = rabs(vnR) + rsqrt_<R>(qdiv<R>(Rq.p * c.gam, Rq.rho));
+        const R e = eLv > eRv ? eLv : eRv;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) out[k] += R(-0.5) * e * (uR[k] - uL[k]);
+    } else if (cf == CF_ROE || cf == CF_EC_ROE) {
+        R diss[5];
+        roe_dissipation_n<R>(L, Rq, n, c, diss);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) out[k] += diss[k];
+    }
+}
+
 // Navier-Stokes viscous flux ("LHS" sign) for state u and conservative gradient
 // g[s][k] (navier_stokes.cpp:1198-1350). F[d][0..3] = (momentum x3, energy) along
 // direction d; the density component is zero. `dmask` selects the directions.

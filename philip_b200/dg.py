@@ -53,12 +53,15 @@ class DGStrong:
     """Strong-form DG/FR discretisation on a periodic cube, evaluated on the B200."""
 
     def __init__(self, parameters: Parameters, precision: int = _lib.PH_FP64, cell_order: int = 0,
-                 stream: int | None = None):
+                 stream: int | None = None, warp: float = 0.0):
+        """warp != 0 gives the sine-warped (curvilinear) cube: every coordinate moves by
+        warp (L/2pi) sin(2pi(x-l)/L) sin(2pi(y-l)/L) sin(2pi(z-l)/L), mapping degree = p."""
         self.L = _lib.load()
         self.parameters = parameters
         self.params = parameters.to_ph_params(precision)
         left, right = parameters.grid_bounds
-        self.mesh = _lib.PhMeshDesc(parameters.n_cells, cell_order, left, right)
+        self.warp = float(warp)
+        self.mesh = _lib.PhMeshDesc(parameters.n_cells, cell_order, left, right, self.warp, parameters.poly_degree)
         h = ctypes.c_void_p()
         _lib.check(self.L.ph_ctx_create(ctypes.byref(self.mesh), ctypes.byref(self.params),
                                         ctypes.c_void_p(stream) if stream else None, ctypes.byref(h)))
@@ -127,14 +130,9 @@ class DGStrong:
 
     def node_coordinates(self) -> np.ndarray:
         """Physical coordinates of the solution support points, [cell][node][3]."""
-        n1 = self.poly_degree + 1
-        xs = gll_nodes(n1)
-        left, right = self.parameters.grid_bounds
-        h = (right - left) / self.parameters.n_cells
-        ijk = self.cell_ijk().astype(np.float64)
-        k, j, i = np.meshgrid(np.arange(n1), np.arange(n1), np.arange(n1), indexing="ij")
-        local = np.stack([xs[i].ravel(), xs[j].ravel(), xs[k].ravel()], axis=-1)
-        return left + h * (ijk[:, None, :] + local[None, :, :])
+        out = np.empty((self.n_cells, self.n_shape, 3))
+        _lib.check(self.L.ph_node_xyz(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out
 
     # -- diagnostics
     def integrals(self) -> np.ndarray:
