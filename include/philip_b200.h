@@ -163,6 +163,52 @@ int ph_residual_noalloc(const ph_mesh_desc* mesh, const ph_params* prm, const do
  * No counterpart in the reference. */
 int ph_quotient_selftest(uint64_t seed, int n, double out[2]);
 
+/* ---- Batch of independent solves (the parameter-swept snapshot solves of
+ * AdaptiveSamplingBase::solveSnapshotFOM, src/reduced_order/adaptive_sampling_base.cpp:255-265,
+ * served together). No single counterpart in the reference, which runs one FlowSolver per
+ * snapshot. Every admitted solve keeps its state resident in a device arena reserved once
+ * (the HBM budget); each RK stage of all admitted solves of one order runs as one persistent
+ * kernel over a tile list, the stages of all orders form one CUDA graph per step, and solves
+ * join and leave between steps (continuous batching). Split-form Euler, GLL, rk4_ex or
+ * ssprk3_ex; affine or curvilinear meshes; one precision per batch. A solve's result is
+ * bitwise the one ph_rk_step gives for it alone. Calls on one batch are not thread-safe. */
+typedef struct ph_batch ph_batch;
+int ph_batch_create(size_t hbm_budget_bytes, int precision, void* cuda_stream, ph_batch** out);
+int ph_batch_destroy(ph_batch* b);
+/* device bytes one solve takes from the budget */
+int ph_batch_bytes(const ph_mesh_desc* mesh, const ph_params* prm, size_t* bytes);
+/* Admit one solve with initial state U0 (host, the reference DoF order), time step dt and
+ * nsteps steps. *slot receives its id. PH_ERR_NOMEM when the budget has no room now. */
+int ph_batch_admit(ph_batch* b, const ph_mesh_desc* mesh, const ph_params* prm, const double* U0, double dt,
+                   int nsteps, int* slot);
+/* Advance every unfinished solve by up to nsteps steps (each stops at its own count).
+ * Asynchronous on the batch stream. */
+int ph_batch_step(ph_batch* b, int nsteps);
+/* steps done and steps asked of a solve; *active = number of unfinished solves */
+int ph_batch_progress(ph_batch* b, int slot, int* steps_done, int* nsteps);
+int ph_batch_active(ph_batch* b, int* active);
+/* state of a solve (host; a finished solve waits for its own last step only), status word
+ * (read clears) */
+int ph_batch_get_state(ph_batch* b, int slot, double* U);
+int ph_batch_status(ph_batch* b, int slot, uint32_t* flags);
+/* return a solve's memory to the budget (a finished or an abandoned solve) */
+int ph_batch_release(ph_batch* b, int slot);
+/* *complete = 1 once the GPU has finished the solve's last step (non-blocking) */
+int ph_batch_poll(ph_batch* b, int slot, int* complete);
+/* fence after the work queued so far; wait for a fence (bounds the work in flight) */
+int ph_batch_fence(ph_batch* b, long long* ticket);
+int ph_batch_fence_wait(ph_batch* b, long long ticket);
+/* physical coordinates of the solution nodes of a mesh, [cell][node][3] (no context) */
+int ph_mesh_node_xyz(const ph_mesh_desc* mesh, int poly_degree, double* xyz);
+/* Tile-shape autotuner: times every cells-per-CTA variant of the batched stage kernel for
+ * (poly_degree, curvilinear) on a synthetic periodic-cube solve and keeps the fastest for
+ * this process; ms[] (up to 4) receives each variant's time per stage, *best the choice.
+ * A batch tunes each new (order, mesh kind) on first use unless a choice is already set. */
+int ph_batch_autotune(int poly_degree, int precision, int curvilinear, int* best, double ms[4], int* nvariants);
+int ph_batch_set_variant(int poly_degree, int precision, int curvilinear, int variant);
+/* launches of this library's kernels issued by ph_batch_step so far (graph nodes counted) */
+int ph_batch_launches(ph_batch* b, long long* launches);
+
 int ph_sync(ph_ctx* ctx);
 const char* ph_last_error(void);
 

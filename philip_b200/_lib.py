@@ -13,12 +13,16 @@ LIB_PATH = os.environ.get("PHILIP_B200_LIB", os.path.join(_HERE, "libphilip_b200
 
 PH_HOST, PH_DEVICE = 0, 1
 PH_FP64, PH_FP32_RESIDUAL = 0, 1
+PH_OK, PH_ERR_INVALID, PH_ERR_UNSUPPORTED, PH_ERR_CUDA, PH_ERR_NOMEM = 0, 1, 2, 3, 4
 ERRORS = {1: "invalid argument", 2: "unsupported configuration", 3: "CUDA error", 4: "out of device memory"}
 
 EXPORTED = ["ph_ctx_create", "ph_ctx_destroy", "ph_ndofs", "ph_cell_ijk", "ph_set_state", "ph_get_state",
             "ph_residual", "ph_apply_inverse_mass", "ph_rk_step", "ph_integrals", "ph_status", "ph_sync",
             "ph_set_timing", "ph_get_timing", "ph_quotient_selftest", "ph_residual_noalloc", "ph_node_xyz",
-            "ph_last_error"]
+            "ph_batch_create", "ph_batch_destroy", "ph_batch_bytes", "ph_batch_admit", "ph_batch_step",
+            "ph_batch_progress", "ph_batch_active", "ph_batch_get_state", "ph_batch_status", "ph_batch_release",
+            "ph_batch_poll", "ph_batch_fence", "ph_batch_fence_wait", "ph_batch_autotune", "ph_batch_set_variant",
+            "ph_batch_launches", "ph_mesh_node_xyz", "ph_last_error"]
 
 
 class PhParams(ctypes.Structure):
@@ -72,6 +76,26 @@ def load(build_if_missing: bool = False):
     L.ph_set_timing.argtypes = [vp, ctypes.c_int]
     L.ph_get_timing.argtypes = [vp, dp]
     L.ph_quotient_selftest.argtypes = [ctypes.c_uint64, ctypes.c_int, dp]
+    sz = ctypes.c_size_t
+    L.ph_batch_create.argtypes = [sz, ctypes.c_int, vp, ctypes.POINTER(vp)]
+    L.ph_batch_destroy.argtypes = [vp]
+    L.ph_batch_bytes.argtypes = [ctypes.POINTER(PhMeshDesc), ctypes.POINTER(PhParams), ctypes.POINTER(sz)]
+    L.ph_batch_admit.argtypes = [vp, ctypes.POINTER(PhMeshDesc), ctypes.POINTER(PhParams), ctypes.POINTER(ctypes.c_double),
+                                 ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    L.ph_batch_step.argtypes = [vp, ctypes.c_int]
+    L.ph_batch_progress.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+    L.ph_batch_active.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
+    L.ph_batch_get_state.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    L.ph_batch_status.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_uint32)]
+    L.ph_batch_release.argtypes = [vp, ctypes.c_int]
+    L.ph_batch_poll.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    L.ph_batch_fence.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.ph_batch_fence_wait.argtypes = [vp, ctypes.c_longlong]
+    L.ph_batch_autotune.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                    ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]
+    L.ph_batch_set_variant.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.ph_batch_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.ph_mesh_node_xyz.argtypes = [ctypes.POINTER(PhMeshDesc), ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     L.ph_node_xyz.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     L.ph_residual_noalloc.argtypes = [ctypes.POINTER(PhMeshDesc), ctypes.POINTER(PhParams), vp, vp, vp]
     L.ph_last_error.restype = ctypes.c_char_p

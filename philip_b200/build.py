@@ -2,7 +2,7 @@
 
 The kernels are instantiated once per polynomial order (``ph_inst.cu`` with
 ``-DPH_N1=<p+1>``); the orders compile in parallel and are linked with the C-ABI
-(``ph_capi.cu``) into one shared library. nvcc cross-compiles without a GPU.
+(``ph_capi.cu``, ``ph_batch.cu``) into one shared library. nvcc cross-compiles without a GPU.
 """
 from __future__ import annotations
 
@@ -17,6 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libphilip_b200.so")
 N1_RANGE = range(2, 8)          # p = 1 .. 6
+HOST_UNITS = ("ph_capi", "ph_batch")   # C-ABI: single-solve context, batch of solves
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -33,7 +34,7 @@ def _nvcc() -> str:
 
 
 def _sources():
-    return [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh"))] + \
+    return [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".hpp"))] + \
         [os.path.join(HERE, "..", "include", "philip_b200.h")]
 
 
@@ -65,12 +66,14 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
     for n1 in N1_RANGE:
         obj = os.path.join(BUILD, f"ph_inst_{n1}.o")
         jobs.append([nvcc, *NVCC_FLAGS, *extra, f"-DPH_N1={n1}", "-c", os.path.join(CSRC, "ph_inst.cu"), "-o", obj])
-    jobs.append([nvcc, *NVCC_FLAGS, "-c", os.path.join(CSRC, "ph_capi.cu"), "-o", os.path.join(BUILD, "ph_capi.o")])
+    for unit in HOST_UNITS:
+        jobs.append([nvcc, *NVCC_FLAGS, "-c", os.path.join(CSRC, unit + ".cu"), "-o", os.path.join(BUILD, unit + ".o")])
     logs = []
     with cf.ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 4)) as ex:
         for out in ex.map(lambda c: _run(c, verbose), jobs):
             logs.append(out)
-    objs = [os.path.join(BUILD, f"ph_inst_{n1}.o") for n1 in N1_RANGE] + [os.path.join(BUILD, "ph_capi.o")]
+    objs = [os.path.join(BUILD, f"ph_inst_{n1}.o") for n1 in N1_RANGE] + \
+        [os.path.join(BUILD, unit + ".o") for unit in HOST_UNITS]
     tmp = LIB + ".tmp"
     _run([nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp, *objs, "-lcudart"], verbose)
     os.replace(tmp, LIB)

@@ -11,9 +11,10 @@
 #include <vector>
 
 #include "../../include/philip_b200.h"
+#include "ph_internal.hpp"
 #include "ph_launch.cuh"
 
-namespace {
+namespace ph_host {
 
 thread_local std::string g_err;
 
@@ -245,7 +246,185 @@ bool curvilinear_cell(const std::vector<double>& x, const std::vector<double>& D
     return true;
 }
 
-} // namespace
+
+const char* unsupported_reason(const ph_mesh_desc* mesh, const ph_params* prm) {
+    if (prm->flux_nodes_type != 1 || prm->overintegration != 0)
+        return "the GPU path is collocated: flux_nodes_type = GLL and overintegration = 0";
+    if (prm->poly_degree < 1 || prm->poly_degree > 6) return "poly_degree must be 1..6";
+    if (prm->flux_reconstruction_aux != 0) return "flux_reconstruction_aux must be kDG";
+    if (mesh->warp != 0.0) {
+        if (mesh->grid_degree != prm->poly_degree) return "curvilinear meshes take grid_degree = poly_degree";
+        if (prm->pde_type != 0) return "curvilinear meshes take the Euler equations";
+        if (!prm->use_split_form) return "curvilinear meshes take the split form";
+        if (prm->flux_reconstruction != 0) return "curvilinear meshes take cDG";
+    }
+    return nullptr;
+}
+
+int build_operators(const ph_params* prm, ph::OpTab& tab, bool& fr, std::vector<double>& x, std::vector<double>& D) {
+    const int N1 = prm->poly_degree + 1;
+    std::vector<double> w;
+    gll(N1, x, w);
+    D.assign(N1 * N1, 0.0);
+    std::vector<double> v(N1), dv(N1);
+    for (int a = 0; a < N1; ++a) {
+        lagrange(x, x[a], v.data(), dv.data());
+        for (int l = 0; l < N1; ++l) D[a * N1 + l] = dv[l];
+    }
+    double cfr = 0.0;
+    if (fr_parameter(prm->flux_reconstruction, prm->poly_degree, prm->FR_user_specified_correction_parameter_value, cfr))
+        return fail(PH_ERR_UNSUPPORTED, "flux_reconstruction type not defined for this degree");
+    std::vector<double> Dp(N1 * N1, 0.0);
+    for (int i = 0; i < N1; ++i) Dp[i * N1 + i] = 1.0;
+    for (int k = 0; k < prm->poly_degree; ++k) Dp = mat_mul(D, Dp, N1);
+    std::vector<double> MK(N1 * N1, 0.0);
+    for (int i = 0; i < N1; ++i)
+        for (int j = 0; j < N1; ++j) {
+            double kij = 0.0;
+            for (int q = 0; q < N1; ++q) kij += Dp[q * N1 + i] * w[q] * Dp[q * N1 + j];
+            MK[i * N1 + j] = (i == j ? w[i] : 0.0) + cfr * kij;
+        }
+    std::vector<double> Minv;
+    if (!mat_inv(MK, N1, Minv)) return fail(PH_ERR_INVALID, "singular FR mass matrix");
+    fr = (cfr != 0.0);
+    std::memset(&tab, 0, sizeof(tab));
+    for (int a = 0; a < N1; ++a) {
+        tab.w[a] = w[a];
+        for (int l = 0; l < N1; ++l) {
+            tab.D[a * ph::MAXN1 + l] = D[a * N1 + l];
+            tab.Dsk[a * ph::MAXN1 + l] = (w[a] * D[a * N1 + l] - w[l] * D[l * N1 + a]) / w[a];
+            tab.Minv[a * ph::MAXN1 + l] = Minv[a * N1 + l];
+            tab.B[a * ph::MAXN1 + l] = Minv[a * N1 + l] * w[l];
+        }
+    }
+    return PH_OK;
+}
+
+void build_integral_table(const std::vector<double>& x, int p, ph::IntegralTab& itab) {
+    const int N1 = p + 1, ne = p + 11;
+    std::memset(&itab, 0, sizeof(itab));
+    std::vector<double> xe, we, v(N1), dv(N1);
+    gauss(ne, xe, we);
+    for (int q = 0; q < ne; ++q) {
+        lagrange(x, xe[q], v.data(), dv.data());
+        for (int a = 0; a < N1; ++a) { itab.B[q * N1 + a] = v[a]; itab.dB[q * N1 + a] = dv[a]; }
+        itab.w[q] = we[q];
+    }
+}
+
+ph::PhysConst physics_constants(const ph_params* prm, double h, double& penalty) {
+    ph::PhysConst pc{};
+    pc.gam = prm->gamma_gas; pc.gm1 = prm->gamma_gas - 1.0;
+    pc.mach2 = prm->mach_infinity * prm->mach_infinity;
+    pc.temp_ratio = 110.4 / prm->temperature_inf;
+    pc.inv_re = 1.0 / prm->reynolds_number_inf;
+    pc.prandtl = prm->prandtl_number;
+    pc.const_visc = prm->nondimensionalized_constant_viscosity;
+    pc.use_const_visc = prm->use_constant_viscosity;
+    pc.two_point = prm->two_point_num_flux_type;
+    pc.conv_flux = prm->conv_num_flux;
+    pc.diss_flux = prm->diss_num_flux;
+    pc.navier_stokes = prm->pde_type == 1;
+    double sipg = prm->sipg_penalty_factor;
+    if (prm->diss_num_flux == 1) sipg = 0.0;   // all_parameters.cpp:611-614
+    pc.sipg_pen = sipg;
+    // SIPG penalty (dg_base.cpp:397-413), averaged over both (identical) cells
+    penalty = (double)prm->poly_degree * (prm->poly_degree + 1) / h * sipg;
+    return pc;
+}
+
+void periodic_connectivity(int n, int order, std::vector<int>& ijk, std::vector<int>& nbr) {
+    const int nc = n * n * n;
+    cell_order(n, order, ijk);
+    std::vector<int> lex2cell(nc);
+    nbr.assign(6 * (size_t)nc, 0);
+    for (int cc = 0; cc < nc; ++cc) lex2cell[(ijk[3 * cc + 2] * n + ijk[3 * cc + 1]) * n + ijk[3 * cc]] = cc;
+    for (int cc = 0; cc < nc; ++cc)
+        for (int f = 0; f < 6; ++f) {
+            int t[3] = {ijk[3 * cc], ijk[3 * cc + 1], ijk[3 * cc + 2]};
+            const int d = f / 2;
+            t[d] = (t[d] + ((f & 1) ? 1 : -1) + n) % n;
+            nbr[6 * cc + f] = lex2cell[(t[2] * n + t[1]) * n + t[0]];
+        }
+}
+
+int node_geometry(int n, const std::vector<int>& ijk, const std::vector<double>& x, const std::vector<double>& D,
+                  double left, double right, double warp, std::vector<double>& xyz, std::vector<double>& metric) {
+    const int N1 = (int)x.size(), NP = N1 * N1 * N1, nc = n * n * n;
+    const double h = (right - left) / n;
+    const bool curv = warp != 0.0;
+    xyz.assign((size_t)nc * NP * 3, 0.0);
+    if (curv) metric.assign((size_t)nc * 10 * NP, 0.0);
+    else metric.clear();
+    const unsigned nthr = std::max(1u, std::min(32u, std::min(std::thread::hardware_concurrency(), (unsigned)nc)));
+    std::vector<std::thread> pool;
+    std::vector<int> ok(nthr, 1);
+    for (unsigned tI = 0; tI < nthr; ++tI)
+        pool.emplace_back([&, tI]() {
+            for (int cc = (int)tI; cc < nc; cc += (int)nthr) {
+                const int* t = &ijk[3 * cc];
+                double* X = &xyz[(size_t)cc * NP * 3];
+                if (curv) {
+                    if (!curvilinear_cell(x, D, N1, h, left, right, warp, t, &metric[(size_t)cc * 10 * NP], X)) ok[tI] = 0;
+                } else {
+                    for (int node = 0; node < NP; ++node) {
+                        const int ii[3] = {node % N1, (node / N1) % N1, node / (N1 * N1)};
+                        for (int d = 0; d < 3; ++d) X[node * 3 + d] = left + h * (t[d] + x[ii[d]]);
+                    }
+                }
+            }
+        });
+    for (auto& th : pool) th.join();
+    for (int v : ok)
+        if (!v) return fail(PH_ERR_INVALID, "non-positive det J: the warp folds a cell");
+    return PH_OK;
+}
+
+void rk_tableau(int method, int& ns, double A[4][4], double b[4]) {
+    for (int i = 0; i < 4; ++i) { b[i] = 0.0; for (int j = 0; j < 4; ++j) A[i][j] = 0.0; }
+    if (method == 2) {
+        ns = 4; A[1][0] = 0.5; A[2][1] = 0.5; A[3][2] = 1.0;
+        b[0] = 1.0 / 6.0; b[1] = 1.0 / 3.0; b[2] = 1.0 / 3.0; b[3] = 1.0 / 6.0;
+    } else if (method == 1) {
+        ns = 3; A[1][0] = 1.0; A[2][0] = 0.25; A[2][1] = 0.25;
+        b[0] = 1.0 / 6.0; b[1] = 1.0 / 6.0; b[2] = 2.0 / 3.0;
+    } else {
+        ns = 1; b[0] = 1.0;
+    }
+}
+
+const double* rk_stage_input(const RkBuffers& B, int i) {
+    return (i == 0) ? B.sol : ((i - 1) % 2 == 0 ? B.stA : B.stB);
+}
+
+// Stage i of RungeKuttaODESolver::step_in_time (runge_kutta_ode_solver.cpp:15-100) fused
+// into the residual epilogue: u_{i+1} = u_n + dt sum_j a_{i+1,j} k_j written as the next
+// stage input, the b-weighted sum accumulated in acc, u_{n+1} written by the last stage.
+void rk_stage_args(ph::StageArgs& a, const RkBuffers& B, int i, int ns, const double A[4][4], const double b[4],
+                   double dt, bool fp32) {
+    a.mode = 2;
+    a.dt = dt;
+    a.Un = B.sol;
+    a.inc_mode = fp32 ? 1 : 0;
+    a.acc_in = (i == 0) ? nullptr : B.acc;
+    a.c_acc = dt * b[i];
+    const bool last = (i == ns - 1);
+    if (!last) {
+        a.acc_out = B.acc;
+        a.next = (i % 2 == 0) ? B.stA : B.stB;
+        a.a_next = A[i + 1][i];
+        if (B.carry && i >= 1 && A[i + 1][i - 1] != 0.0) a.carry_in = B.carry;
+        if (B.carry && i + 2 < ns && A[i + 2][i] != 0.0) { a.carry_out = B.carry; a.a_carry = A[i + 2][i]; }
+    } else {
+        // the stage input is read by neighbouring CTAs, so a one-stage method writes elsewhere
+        a.final_out = (ns == 1) ? B.stA : B.sol;
+        a.comp = B.comp;
+    }
+}
+
+} // namespace ph_host
+
+using namespace ph_host;
 
 struct ph_ctx {
     ph_params prm{};
@@ -356,15 +535,12 @@ const char* ph_last_error(void) { return g_err.c_str(); }
 int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_stream, ph_ctx** out) {
     if (!mesh || !prm || !out) return fail(PH_ERR_INVALID, "null argument");
     *out = nullptr;
-    if (prm->flux_nodes_type != 1 || prm->overintegration != 0)
-        return fail(PH_ERR_UNSUPPORTED, "the GPU path is collocated: flux_nodes_type = GLL and overintegration = 0");
-    if (prm->poly_degree < 1 || prm->poly_degree > 6) return fail(PH_ERR_UNSUPPORTED, "poly_degree must be 1..6");
-    if (prm->flux_reconstruction_aux != 0) return fail(PH_ERR_UNSUPPORTED, "flux_reconstruction_aux must be kDG");
     if (mesh->n_cells_per_direction < 1 || !(mesh->right > mesh->left)) return fail(PH_ERR_INVALID, "bad mesh");
     if (prm->pde_type < 0 || prm->pde_type > 1 || prm->two_point_num_flux_type < 0 || prm->two_point_num_flux_type > 3 ||
         prm->conv_num_flux < 0 || prm->conv_num_flux > 5 || prm->diss_num_flux < 0 || prm->diss_num_flux > 2 ||
         prm->runge_kutta_method < 0 || prm->runge_kutta_method > 2)
         return fail(PH_ERR_INVALID, "parameter out of range");
+    if (const char* why = unsupported_reason(mesh, prm)) return fail(PH_ERR_UNSUPPORTED, why);
     const bool ec = prm->conv_num_flux >= 3;
     if (ec && !prm->use_split_form)
         return fail(PH_ERR_INVALID, "two point flux and not using split form are not compatible");   // numerical_flux_factory.cpp
@@ -385,137 +561,18 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
     c->warp = mesh->warp;
     c->curv = mesh->warp != 0.0;
     cudaGetDevice(&c->device);
-    if (c->curv) {
-        const int g = mesh->grid_degree;
-        const char* why = (g != c->p) ? "curvilinear meshes take grid_degree = poly_degree"
-                          : c->visc ? "curvilinear meshes take the Euler equations"
-                          : !c->split ? "curvilinear meshes take the split form"
-                          : (prm->flux_reconstruction != 0) ? "curvilinear meshes take cDG" : nullptr;
-        if (why) { delete c; return fail(PH_ERR_UNSUPPORTED, why); }
-    }
 
-    // ---- 1-D operators on the GLL nodes
-    const int N1 = c->N1;
-    std::vector<double> x, w;
-    gll(N1, x, w);
-    std::vector<double> D(N1 * N1), v(N1), dv(N1);
-    for (int a = 0; a < N1; ++a) {
-        lagrange(x, x[a], v.data(), dv.data());
-        for (int l = 0; l < N1; ++l) D[a * N1 + l] = dv[l];
-    }
-    double cfr = 0.0;
-    if (fr_parameter(prm->flux_reconstruction, c->p, prm->FR_user_specified_correction_parameter_value, cfr)) {
-        delete c;
-        return fail(PH_ERR_UNSUPPORTED, "flux_reconstruction type not defined for this degree");
-    }
-    std::vector<double> Dp(N1 * N1, 0.0);
-    for (int i = 0; i < N1; ++i) Dp[i * N1 + i] = 1.0;
-    for (int k = 0; k < c->p; ++k) Dp = mat_mul(D, Dp, N1);
-    std::vector<double> MK(N1 * N1, 0.0);
-    for (int i = 0; i < N1; ++i)
-        for (int j = 0; j < N1; ++j) {
-            double kij = 0.0;
-            for (int q = 0; q < N1; ++q) kij += Dp[q * N1 + i] * w[q] * Dp[q * N1 + j];
-            MK[i * N1 + j] = (i == j ? w[i] : 0.0) + cfr * kij;
-        }
-    std::vector<double> Minv;
-    if (!mat_inv(MK, N1, Minv)) { delete c; return fail(PH_ERR_INVALID, "singular FR mass matrix"); }
-    c->fr = (cfr != 0.0);
-    std::memset(&c->h_ops, 0, sizeof(c->h_ops));
-    for (int a = 0; a < N1; ++a) {
-        c->h_ops.w[a] = w[a];
-        for (int l = 0; l < N1; ++l) {
-            c->h_ops.D[a * ph::MAXN1 + l] = D[a * N1 + l];
-            c->h_ops.Dsk[a * ph::MAXN1 + l] = (w[a] * D[a * N1 + l] - w[l] * D[l * N1 + a]) / w[a];
-            c->h_ops.Minv[a * ph::MAXN1 + l] = Minv[a * N1 + l];
-            c->h_ops.B[a * ph::MAXN1 + l] = Minv[a * N1 + l] * w[l];
-        }
-    }
-    // over-integration tables for the TGV integrals: QGauss(p + 11)
+    // ---- 1-D operators, integral tables, physics, RK tableau, connectivity, geometry
+    std::vector<double> x, D;
+    if (int rc = build_operators(prm, c->h_ops, c->fr, x, D)) { delete c; return rc; }
     ph::IntegralTab itab;
-    std::memset(&itab, 0, sizeof(itab));
-    {
-        const int ne = c->p + 11;
-        std::vector<double> xe, we;
-        gauss(ne, xe, we);
-        for (int q = 0; q < ne; ++q) {
-            lagrange(x, xe[q], v.data(), dv.data());
-            for (int a = 0; a < N1; ++a) { itab.B[q * N1 + a] = v[a]; itab.dB[q * N1 + a] = dv[a]; }
-            itab.w[q] = we[q];
-        }
-    }
-
-    // ---- physics constants
-    ph::PhysConst& pc = c->pc;
-    pc.gam = prm->gamma_gas; pc.gm1 = prm->gamma_gas - 1.0;
-    pc.mach2 = prm->mach_infinity * prm->mach_infinity;
-    pc.temp_ratio = 110.4 / prm->temperature_inf;
-    pc.inv_re = 1.0 / prm->reynolds_number_inf;
-    pc.prandtl = prm->prandtl_number;
-    pc.const_visc = prm->nondimensionalized_constant_viscosity;
-    pc.use_const_visc = prm->use_constant_viscosity;
-    pc.two_point = prm->two_point_num_flux_type;
-    pc.conv_flux = prm->conv_num_flux;
-    pc.diss_flux = prm->diss_num_flux;
-    pc.navier_stokes = c->visc;
-    double sipg = prm->sipg_penalty_factor;
-    if (prm->diss_num_flux == 1) sipg = 0.0;   // all_parameters.cpp:611-614
-    pc.sipg_pen = sipg;
-    // SIPG penalty (dg_base.cpp:397-413), averaged over both (identical) cells
-    c->pen = (double)c->p * (c->p + 1) / c->h * sipg;
-
-    // ---- Butcher tableau (runge_kutta_methods.cpp:7-47)
-    if (prm->runge_kutta_method == 2) {
-        c->ns = 4; c->A[1][0] = 0.5; c->A[2][1] = 0.5; c->A[3][2] = 1.0;
-        c->b[0] = 1.0 / 6.0; c->b[1] = 1.0 / 3.0; c->b[2] = 1.0 / 3.0; c->b[3] = 1.0 / 6.0;
-    } else if (prm->runge_kutta_method == 1) {
-        c->ns = 3; c->A[1][0] = 1.0; c->A[2][0] = 0.25; c->A[2][1] = 0.25;
-        c->b[0] = 1.0 / 6.0; c->b[1] = 1.0 / 6.0; c->b[2] = 2.0 / 3.0;
-    } else {
-        c->ns = 1; c->b[0] = 1.0;
-    }
-
-    // ---- connectivity
-    cell_order(c->n, mesh->cell_order, c->ijk);
-    std::vector<int> lex2cell(c->nc), nbr(6 * c->nc);
-    const int n = c->n;
-    for (int cc = 0; cc < c->nc; ++cc) lex2cell[(c->ijk[3 * cc + 2] * n + c->ijk[3 * cc + 1]) * n + c->ijk[3 * cc]] = cc;
-    for (int cc = 0; cc < c->nc; ++cc)
-        for (int f = 0; f < 6; ++f) {
-            int t[3] = {c->ijk[3 * cc], c->ijk[3 * cc + 1], c->ijk[3 * cc + 2]};
-            const int d = f / 2;
-            t[d] = (t[d] + ((f & 1) ? 1 : -1) + n) % n;
-            nbr[6 * cc + f] = lex2cell[(t[2] * n + t[1]) * n + t[0]];
-        }
-
-    // ---- node coordinates and (curvilinear) metric terms, cells in parallel on the host
-    c->xyz.assign((size_t)c->nc * c->NP * 3, 0.0);
+    build_integral_table(x, c->p, itab);
+    c->pc = physics_constants(prm, c->h, c->pen);
+    rk_tableau(prm->runge_kutta_method, c->ns, c->A, c->b);
+    std::vector<int> nbr;
+    periodic_connectivity(c->n, mesh->cell_order, c->ijk, nbr);
     std::vector<double> metric;
-    if (c->curv) metric.assign((size_t)c->nc * 10 * c->NP, 0.0);
-    {
-        const unsigned nthr = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-        std::vector<std::thread> pool;
-        std::vector<int> ok(nthr, 1);
-        for (unsigned tI = 0; tI < nthr; ++tI)
-            pool.emplace_back([&, tI]() {
-                for (int cc = (int)tI; cc < c->nc; cc += (int)nthr) {
-                    const int* t = &c->ijk[3 * cc];
-                    double* xyz = &c->xyz[(size_t)cc * c->NP * 3];
-                    if (c->curv) {
-                        if (!curvilinear_cell(x, D, N1, c->h, c->left, c->right, c->warp, t,
-                                              &metric[(size_t)cc * 10 * c->NP], xyz)) ok[tI] = 0;
-                    } else {
-                        for (int node = 0; node < c->NP; ++node) {
-                            const int ii[3] = {node % N1, (node / N1) % N1, node / (N1 * N1)};
-                            for (int d = 0; d < 3; ++d) xyz[node * 3 + d] = c->left + c->h * (t[d] + x[ii[d]]);
-                        }
-                    }
-                }
-            });
-        for (auto& th : pool) th.join();
-        for (int v : ok)
-            if (!v) { delete c; return fail(PH_ERR_INVALID, "non-positive det J: the warp folds a cell"); }
-    }
+    if (int rc = node_geometry(c->n, c->ijk, x, D, c->left, c->right, c->warp, c->xyz, metric)) { delete c; return rc; }
 
     // ---- device buffers
     const size_t N = c->ndofs;
@@ -659,28 +716,12 @@ int ph_apply_inverse_mass(ph_ctx* c, const double* R, double* out, int where) {
 // updates the running sum and writes the next stage state.
 static int rk_one_step(ph_ctx* c, double dt) {
     const int ns = c->ns;
+    const RkBuffers B{c->d_sol, c->d_stA, c->d_stB, c->d_acc, c->d_carry, c->d_comp};
     for (int i = 0; i < ns; ++i) {
-        const double* in = (i == 0) ? c->d_sol : ((i - 1) % 2 == 0 ? c->d_stA : c->d_stB);
+        const double* in = rk_stage_input(B, i);
         if (c->visc) if (int rc = dispatch_aux(c, in)) return rc;
         ph::StageArgs a = base_args(c, in);
-        a.mode = 2;
-        a.dt = dt;
-        a.Un = c->d_sol;
-        a.inc_mode = c->fp32 ? 1 : 0;
-        a.acc_in = (i == 0) ? nullptr : c->d_acc;
-        a.c_acc = dt * c->b[i];
-        const bool last = (i == ns - 1);
-        if (!last) {
-            a.acc_out = c->d_acc;
-            a.next = (i % 2 == 0) ? c->d_stA : c->d_stB;
-            a.a_next = c->A[i + 1][i];
-            if (c->d_carry && i >= 1 && c->A[i + 1][i - 1] != 0.0) a.carry_in = c->d_carry;
-            if (c->d_carry && i + 2 < ns && c->A[i + 2][i] != 0.0) { a.carry_out = c->d_carry; a.a_carry = c->A[i + 2][i]; }
-        } else {
-            // the stage input is read by neighbouring CTAs, so a one-stage method writes elsewhere
-            a.final_out = (ns == 1) ? c->d_stA : c->d_sol;
-            a.comp = c->d_comp;
-        }
+        rk_stage_args(a, B, i, ns, c->A, c->b, dt, c->fp32);
         if (int rc = dispatch_stage(c, a)) return rc;
     }
     if (ns == 1) std::swap(c->d_sol, c->d_stA);

@@ -50,6 +50,93 @@ cudaError_t launch_stage(const StageArgs& a, int fp32, bool visc, bool split, cu
     return fp32 ? launch_prec<float, N1>(a, visc, split, s) : launch_prec<double, N1>(a, visc, split, s);
 }
 
+// ---- batched stage kernels: tile-shape variants per order (cells per CTA)
+template <int N1> constexpr int batched_variants() { return (N1 == 2 || N1 >= 6) ? 1 : 2; }
+template <int N1, int V> constexpr int batched_cpc() {
+    return N1 == 2 ? 16 : N1 == 3 ? (V == 0 ? 4 : 8) : N1 == 4 ? (V == 0 ? 2 : 4) : N1 == 5 ? (V == 0 ? 1 : 2) : 1;
+}
+
+template <typename R, int N1, int V, int FS, bool CURV>
+static cudaError_t launch_batched_one(const StageArgs* inst, const BatchTile* tiles, int ntiles, int grid,
+                                      cudaStream_t s) {
+    constexpr int CPC = batched_cpc<N1, V>();
+    using L = Layout<R, N1, CPC, false, true, CURV>;
+    auto kern = residual_kernel_batched<R, N1, CPC, false, true, FS, CURV>;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static bool configured[64] = {false};
+    static int resident[64] = {0};
+    if (dev < 64 && !configured[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::bytes);
+        if (e != cudaSuccess) return e;
+        int per_sm = 0, sms = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, L::NT, L::bytes);
+        if (e != cudaSuccess) return e;
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+        resident[dev] = per_sm * sms;
+        configured[dev] = true;
+    }
+    if (ntiles <= 0) return cudaSuccess;
+    if (grid <= 0) grid = resident[dev < 64 ? dev : 0];
+    if (grid <= 0 || grid > ntiles) grid = ntiles;
+    kern<<<grid, L::NT, L::bytes, s>>>(inst, tiles, ntiles);
+    return cudaGetLastError();
+}
+
+template <typename R, int N1, int V>
+static cudaError_t launch_batched_v(const StageArgs* inst, const BatchTile* tiles, int ntiles, bool curv, bool hot,
+                                    int grid, cudaStream_t s) {
+    if (curv) return hot ? launch_batched_one<R, N1, V, 1, true>(inst, tiles, ntiles, grid, s)
+                         : launch_batched_one<R, N1, V, 0, true>(inst, tiles, ntiles, grid, s);
+    return hot ? launch_batched_one<R, N1, V, 1, false>(inst, tiles, ntiles, grid, s)
+               : launch_batched_one<R, N1, V, 0, false>(inst, tiles, ntiles, grid, s);
+}
+
+template <typename R, int N1>
+static cudaError_t launch_batched_prec(const StageArgs* inst, const BatchTile* tiles, int ntiles, bool curv, bool hot,
+                                       int variant, int grid, cudaStream_t s) {
+    if constexpr (batched_variants<N1>() > 1) {
+        if (variant == 1) return launch_batched_v<R, N1, 1>(inst, tiles, ntiles, curv, hot, grid, s);
+    }
+    if (variant != 0) return cudaErrorInvalidValue;
+    return launch_batched_v<R, N1, 0>(inst, tiles, ntiles, curv, hot, grid, s);
+}
+
+template <int N1>
+cudaError_t launch_stage_batched(const StageArgs* inst, const BatchTile* tiles, int ntiles, int fp32, bool curv,
+                                 bool hot, int variant, int grid, cudaStream_t s) {
+    return fp32 ? launch_batched_prec<float, N1>(inst, tiles, ntiles, curv, hot, variant, grid, s)
+                : launch_batched_prec<double, N1>(inst, tiles, ntiles, curv, hot, variant, grid, s);
+}
+
+template <typename R, int N1, int V, bool CURV>
+static bool batched_shape_one(int* cpc, int* threads, size_t* smem, int* ctas_per_sm) {
+    constexpr int CPC = batched_cpc<N1, V>();
+    using L = Layout<R, N1, CPC, false, true, CURV>;
+    *cpc = CPC; *threads = L::NT; *smem = L::bytes;
+    auto kern = residual_kernel_batched<R, N1, CPC, false, true, 1, CURV>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::bytes) != cudaSuccess) return false;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, kern, L::NT, L::bytes) == cudaSuccess;
+}
+
+template <typename R, int N1>
+static bool batched_shape_prec(bool curv, int variant, int* cpc, int* threads, size_t* smem, int* ctas_per_sm) {
+    if constexpr (batched_variants<N1>() > 1) {
+        if (variant == 1) return curv ? batched_shape_one<R, N1, 1, true>(cpc, threads, smem, ctas_per_sm)
+                                      : batched_shape_one<R, N1, 1, false>(cpc, threads, smem, ctas_per_sm);
+    }
+    if (variant != 0) return false;
+    return curv ? batched_shape_one<R, N1, 0, true>(cpc, threads, smem, ctas_per_sm)
+                : batched_shape_one<R, N1, 0, false>(cpc, threads, smem, ctas_per_sm);
+}
+
+template <int N1>
+bool batched_shape(int fp32, bool curv, int variant, int* cpc, int* threads, size_t* smem, int* ctas_per_sm) {
+    return fp32 ? batched_shape_prec<float, N1>(curv, variant, cpc, threads, smem, ctas_per_sm)
+                : batched_shape_prec<double, N1>(curv, variant, cpc, threads, smem, ctas_per_sm);
+}
+
 template <typename R, int N1, bool VISC, bool SPLIT>
 static void shape_one(int* threads, int* cpc, size_t* smem) {  // same shape for every flux set
     constexpr int CPC = cells_per_cta<N1>();
@@ -127,6 +214,9 @@ cudaError_t launch_integrals(const double* U, const double* X, const IntegralTab
 
 template cudaError_t launch_stage<PH_N1>(const StageArgs&, int, bool, bool, cudaStream_t);
 template void stage_launch_shape<PH_N1>(int, bool, bool, int*, int*, size_t*);
+template cudaError_t launch_stage_batched<PH_N1>(const StageArgs*, const BatchTile*, int, int, bool, bool, int, int,
+                                                 cudaStream_t);
+template bool batched_shape<PH_N1>(int, bool, int, int*, int*, size_t*, int*);
 template cudaError_t launch_aux<PH_N1>(const double*, const int*, const OpTab*, int, double, const PhysConst&, int,
                                        double*, cudaStream_t);
 template cudaError_t launch_inverse_mass<PH_N1>(const double*, double*, const OpTab*, int, double, const double*,

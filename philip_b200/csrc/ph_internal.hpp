@@ -1,0 +1,57 @@
+// Host-side building blocks shared by the single-solve context (ph_capi.cu) and the
+// batch of solves (ph_batch.cu): parameter checks, 1-D operators, physics constants,
+// periodic-cube connectivity, node geometry / curvilinear metric terms and the RK
+// stage arguments. Not part of the C-ABI.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "../../include/philip_b200.h"
+#include "ph_integrals.cuh"
+#include "ph_kernels.cuh"
+
+namespace ph_host {
+
+int fail(int code, const std::string& msg);   // records the message for ph_last_error
+
+// Configuration checks shared by every entry point that builds a discretisation;
+// returns nullptr when the configuration is on the GPU path, else the reason.
+const char* unsupported_reason(const ph_mesh_desc* mesh, const ph_params* prm);
+
+// 1-D operators on the GLL nodes: D, skew D, FR mass inverse (M+K)^-1 and B = (M+K)^-1 W.
+// x, D are the nodes and derivative matrix (N1 and N1 x N1). Returns PH_OK or an error.
+int build_operators(const ph_params* prm, ph::OpTab& tab, bool& fr, std::vector<double>& x, std::vector<double>& D);
+
+// QGauss(p + 11) tables of the TGV integrals for solution nodes x
+void build_integral_table(const std::vector<double>& x, int p, ph::IntegralTab& tab);
+
+// Physics constants of the kernels; the SIPG penalty (dg_base.cpp:397-413) for cell size h.
+ph::PhysConst physics_constants(const ph_params* prm, double h, double& penalty);
+
+// deal.II cell order (ijk, 3 per cell) and the 6 periodic neighbours of each cell.
+void periodic_connectivity(int n, int order, std::vector<int>& ijk, std::vector<int>& nbr);
+
+// Node coordinates [cell][node][3] and, for warp != 0, the metric rows [cell][10][NP];
+// cells are processed by host threads. Returns PH_OK or an error (folded cell).
+int node_geometry(int n, const std::vector<int>& ijk, const std::vector<double>& x, const std::vector<double>& D,
+                  double left, double right, double warp, std::vector<double>& xyz, std::vector<double>& metric);
+
+// Butcher tableau of the explicit RK method (runge_kutta_methods.cpp:7-47).
+void rk_tableau(int method, int& ns, double A[4][4], double b[4]);
+
+// Device vectors of one explicit RK integration of one discretisation.
+struct RkBuffers {
+    double* sol;     // u_n, and u_{n+1} after the last stage
+    double* stA;     // stage inputs (ping-pong)
+    double* stB;
+    double* acc;     // running sum of the stage derivatives
+    double* carry;   // SSPRK3 carry (nullptr otherwise)
+    double* comp;    // Kahan compensation of the precision form (nullptr otherwise)
+};
+
+// Stage input of stage i, and the RK epilogue arguments of stage i (mode 2) into a.
+const double* rk_stage_input(const RkBuffers& B, int i);
+void rk_stage_args(ph::StageArgs& a, const RkBuffers& B, int i, int ns, const double A[4][4], const double b[4],
+                   double dt, bool fp32);
+
+} // namespace ph_host

@@ -356,9 +356,12 @@ __device__ __forceinline__ void volume_dir(int d, const Cst<R>& cst, int tp, con
 // run time), 1 = Chandrashekar split flux + entropy-conserving baseline with Roe
 // dissipation (+ BR2 when viscous) fixed at compile time, which removes the unused
 // variants from the instruction stream.
-template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int FS, bool CURV = false>
-__global__ void __launch_bounds__(Layout<R, N1, CPC, VISC, SPLIT, CURV>::NT, Layout<R, N1, CPC, VISC, SPLIT, CURV>::MINB)
-residual_kernel(const StageArgs a) {
+//
+// residual_tile does the work of one CTA on the tile of CPC cells starting at cell0;
+// residual_kernel runs one tile per CTA of one discretisation, residual_kernel_batched
+// runs the tiles of many independent discretisations (a batch of solves) from a tile list.
+template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int FS, bool CURV>
+__device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell0) {
     static_assert(!CURV || (SPLIT && !VISC), "curvilinear cells: split-form Euler only");
     using L = Layout<R, N1, CPC, VISC, SPLIT, CURV>;
     constexpr int NP = L::NP, NF = L::NF, NT = L::NT, TR = L::TR, NQS = L::NQS;
@@ -380,7 +383,6 @@ residual_kernel(const StageArgs a) {
     const int df = FS == 1 ? (int)DF_BR2 : a.pc.diss_flux;
     const int ucv = a.pc.use_const_visc;
     const int tid = threadIdx.x;
-    const int cell0 = blockIdx.x * CPC;
 
     for (int i = tid; i < N1 * N1; i += NT) {
         sOpsD[i] = (R)a.ops->D[(i / N1) * MAXN1 + (i % N1)];
@@ -561,6 +563,38 @@ residual_kernel(const StageArgs a) {
             a.next[dof] = (cin + a.a_next * k) * a.dt + un;
         }
         if (a.carry_out) a.carry_out[dof] = a.a_carry * k;
+    }
+}
+
+template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int FS, bool CURV = false>
+__global__ void __launch_bounds__(Layout<R, N1, CPC, VISC, SPLIT, CURV>::NT, Layout<R, N1, CPC, VISC, SPLIT, CURV>::MINB)
+residual_kernel(const StageArgs a) {
+    residual_tile<R, N1, CPC, VISC, SPLIT, FS, CURV>(a, blockIdx.x * CPC);
+}
+
+// One tile of a batch: instance index and its first cell.
+struct BatchTile {
+    int inst;
+    int cell0;
+};
+
+// Persistent batched stage kernel: every CTA walks the tile list with a grid stride; the
+// tile's discretisation (state pointers, physics, dt, RK coefficients of this stage) is
+// staged from the instance table into shared memory. The per-tile work is the same code as
+// residual_kernel, so a solve gives bitwise the same result alone and inside a batch.
+template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int FS, bool CURV = false>
+__global__ void __launch_bounds__(Layout<R, N1, CPC, VISC, SPLIT, CURV>::NT, Layout<R, N1, CPC, VISC, SPLIT, CURV>::MINB)
+residual_kernel_batched(const StageArgs* __restrict__ inst, const BatchTile* __restrict__ tiles, int ntiles) {
+    static_assert(sizeof(StageArgs) % sizeof(int) == 0, "StageArgs is copied as ints");
+    __shared__ __align__(16) StageArgs sa;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const BatchTile tile = tiles[t];
+        const int* src = reinterpret_cast<const int*>(inst + tile.inst);
+        int* dst = reinterpret_cast<int*>(&sa);
+        for (int i = threadIdx.x; i < (int)(sizeof(StageArgs) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+        __syncthreads();
+        residual_tile<R, N1, CPC, VISC, SPLIT, FS, CURV>(sa, tile.cell0);
+        __syncthreads();
     }
 }
 

@@ -23,6 +23,16 @@ cudaError_t launch_inverse_mass(const double* in, double* out, const OpTab* ops,
 template <int N1>
 cudaError_t launch_integrals(const double* U, const double* X, const IntegralTab* tab, int nc, double h, double gam,
                              double gm1, double* partial, cudaStream_t s);
+// Batched (many-solve) stage: split-form Euler tiles of several discretisations of the same
+// order. `variant` selects the cells-per-CTA tile shape (batched_shape lists them); grid <= 0
+// sizes the persistent grid to the resident CTAs of the whole GPU.
+template <int N1>
+cudaError_t launch_stage_batched(const StageArgs* inst, const BatchTile* tiles, int ntiles, int fp32, bool curv,
+                                 bool hot, int variant, int grid, cudaStream_t s);
+// tile shape of a batched variant: cells per CTA, threads, dynamic shared memory and resident
+// CTAs per SM; returns false when the variant does not exist
+template <int N1>
+bool batched_shape(int fp32, bool curv, int variant, int* cpc, int* threads, size_t* smem, int* ctas_per_sm);
 // shared memory and threads of the residual kernel (for reporting / tests)
 template <int N1>
 void stage_launch_shape(int fp32, bool visc, bool split, int* threads, int* cells_per_cta, size_t* smem);
