@@ -27,6 +27,8 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -255,13 +257,139 @@ def run_reference(args, rank, world):
     return 0
 
 
+# ------------------------------------------------------------------------------------------
+# Batched and served forms (many independent Euler solves on one GPU)
+# ------------------------------------------------------------------------------------------
+MANY = {
+    "vortex_batch_256": "256 isentropic-vortex solves on [0,10]^3, n^3 cells with n in {4,6,8,12,16}, p in 2..5, "
+                        "beta ~ U[1,5], Mach ~ U[0.1,0.5], random direction, to t=1; all admitted at once",
+    "served_stream": "Poisson arrivals (50/s) of Euler solves on sine-warped periodic cubes (x_i += 0.1 sin x sin y "
+                     "sin z), TGV or isentropic vortex 50/50, Mach ~ U[0.1,0.4], n in 6..20, p in 2..5, to t=1",
+}
+
+
+def many_requests(kind: str, count: int, seed: int = 20261203):
+    from philip_b200.serve import SolveRequest
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(count):
+        d = rng.standard_normal(3)
+        d /= np.linalg.norm(d)
+        if kind == "vortex_batch_256":
+            reqs.append(SolveRequest("isentropic_vortex", n_cells=int(rng.choice([4, 6, 8, 12, 16])),
+                                     poly_degree=int(rng.integers(2, 6)), mach=float(rng.uniform(0.1, 0.5)),
+                                     beta=float(rng.uniform(1.0, 5.0)), direction=tuple(d), final_time=1.0))
+        else:
+            tgv = rng.random() < 0.5
+            reqs.append(SolveRequest("taylor_green_vortex" if tgv else "isentropic_vortex",
+                                     n_cells=int(rng.integers(6, 21)), poly_degree=int(rng.integers(2, 6)),
+                                     left=0.0, right=TWO_PI if tgv else 10.0, warp=0.1,
+                                     mach=float(rng.uniform(0.1, 0.4)), beta=float(rng.uniform(1.0, 5.0)),
+                                     direction=tuple(d), final_time=1.0))
+    return reqs
+
+
+def one_at_a_time(reqs):
+    """The same solves one after another through the single-solve context in FP64
+    (ph_ctx_create, ph_set_state, ph_rk_step, ph_get_state per solve)."""
+    import torch
+    from philip_b200 import _lib
+    from philip_b200.dg import DGStrong
+    prepared = [(r, *r.prepare()) for r in reqs]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    work = 0
+    for r, U0, dt, nsteps in prepared:
+        dg = DGStrong(r.parameters(), precision=_lib.PH_FP64, warp=r.warp)
+        dg.solution = U0
+        _lib.check(dg.L.ph_rk_step(dg.handle, dt, nsteps))
+        dg.solution   # read back (synchronises)
+        work += r.ndofs * 4 * nsteps
+        del dg
+    el = time.perf_counter() - t0
+    return {"solves": len(reqs), "seconds": el, "solves_per_s": len(reqs) / el,
+            "dof_updates_per_s_stage": work / el, "dtype": "f64", "path": "single-solve context per solve"}
+
+
+def run_many(args):
+    """Batched (all admitted at t=0) or served (Poisson arrivals, continuous batching) form."""
+    import torch
+    from philip_b200 import _lib
+    from philip_b200.serve import Batch, SnapshotServer, autotune, poisson_arrivals, solve_bytes
+    torch.cuda.set_device(0)
+    prec = _lib.PH_FP32_RESIDUAL if args.precision == "fp32" else _lib.PH_FP64
+    count = args.requests or (256 if args.workload == "vortex_batch_256" else 64)
+    reqs = many_requests(args.workload, count)
+    tuned = {}
+    for r in reqs:   # tile shapes per (order, mesh kind), before the clock starts
+        key = (r.poly_degree, r.warp != 0.0)
+        if key not in tuned:
+            tuned[key] = autotune(r.poly_degree, prec, key[1])
+    for r in reqs:   # the requests' payload (initial state, time step), before the clock starts
+        r.prepare()
+    budget = int(args.budget_gb * (1 << 30))
+    rng = np.random.default_rng(7)
+    arrivals = [0.0] * count if args.workload == "vortex_batch_256" else list(poisson_arrivals(args.rate, count, rng))
+    # warm-up: one small solve through the same batch machinery
+    warm = Batch(1 << 28, prec)
+    SnapshotServer(warm, chunk=args.chunk, precision=prec).run([(0.0, many_requests(args.workload, 1, seed=1)[0])])
+    warm.close()
+    batch = Batch(budget, prec)
+    with ClockSampler(0) as clk:
+        srv = SnapshotServer(batch, chunk=args.chunk, keep_states=args.workload == "vortex_batch_256", precision=prec)
+        stats = srv.run(list(zip(arrivals, reqs)))
+    launches = batch.launches
+    batch.close()
+    work = sum(c.request.ndofs * 4 * c.steps for c in stats.completed)
+    line = {
+        "metric": "served solves/s" if args.workload == "served_stream" else "batched DOF-updates/s/stage",
+        "unit": "solves/s" if args.workload == "served_stream" else "DOF-updates/s/stage",
+        "value": stats.solves_per_s if args.workload == "served_stream" else work / stats.makespan,
+        "n_gpus": 1, "steps": None, "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32-residual/f64-state" if prec == _lib.PH_FP32_RESIDUAL else "f64",
+        "data": "synthetic (seeded requests; exact initial conditions)",
+        "config": {"workload": args.workload, "description": MANY[args.workload], "requests": count,
+                   "budget_gb": args.budget_gb, "chunk_steps": args.chunk,
+                   "arrival_rate_per_s": None if args.workload == "vortex_batch_256" else args.rate,
+                   "total_dofs": int(sum(r.ndofs for r in reqs)),
+                   "tile_variants": {f"p{k[0]}{'c' if k[1] else 'a'}": v for k, v in tuned.items()}},
+        "solves_per_s": stats.solves_per_s, "dof_updates_per_s_stage": work / stats.makespan,
+        "makespan_s": stats.makespan,
+        "latency_ms": {"p50": 1e3 * stats.percentile(50), "p99": 1e3 * stats.percentile(99),
+                       "max": 1e3 * max(c.latency for c in stats.completed)},
+        "max_resident": stats.max_in_flight, "gpu_launches": launches,
+        "status_flags": int(np.bitwise_or.reduce([c.status for c in stats.completed])),
+        "clocks": clk.summary(),
+    }
+    if args.workload == "vortex_batch_256":
+        errs = []
+        for c in stats.completed:
+            ex = c.request.exact_state()
+            errs.append(float(np.max(np.abs(c.state - ex)) / np.max(np.abs(ex))))
+        line["vortex_rel_max_error"] = {"median": float(np.median(errs)), "max": float(np.max(errs))}
+    if not args.no_cpu_baseline:
+        sample = reqs[: args.baseline_sample] if args.baseline_sample else reqs
+        base = one_at_a_time(sample)
+        base["sample"] = f"first {len(sample)} of the {count} requests, run back to back (no arrival gaps)"
+        line["one_at_a_time"] = base
+        line["speedup_vs_one_at_a_time"] = (line["dof_updates_per_s_stage"] / base["dof_updates_per_s_stage"])
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="tgv_viscous_24_p5", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="tgv_viscous_24_p5", choices=sorted(WORKLOADS) + sorted(MANY))
+    ap.add_argument("--requests", type=int, default=0, help="batched / served forms: number of solves")
+    ap.add_argument("--rate", type=float, default=50.0, help="served form: Poisson arrival rate per second")
+    ap.add_argument("--budget-gb", type=float, default=96.0, help="batched / served forms: HBM budget")
+    ap.add_argument("--chunk", type=int, default=16, help="batched / served forms: RK steps per enqueue")
+    ap.add_argument("--baseline-sample", type=int, default=0,
+                    help="batched / served forms: solves in the one-at-a-time FP64 comparison (0 = all)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -269,6 +397,15 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload in MANY:
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the batched and served forms have no reference "
+                              "counterpart (the reference runs one FlowSolver per snapshot); their baseline is the "
+                              "one-at-a-time line inside this arm's output"}), flush=True)
+            return 0
+        if args.precision == "fp64" and "--precision" not in sys.argv:
+            args.precision = "fp32"   # the batched and served forms run the precision form by default
+        return run_many(args)
     if args.impl == "reference":
         return run_reference(args, rank, world)
 

@@ -214,6 +214,13 @@ class SolveRequest:
         nsteps = max(1, int(math.ceil(self.final_time / dt - 1e-12)))
         return self.final_time / nsteps, nsteps
 
+    def prepare(self):
+        """Initial state and time step, computed once (the request's payload)."""
+        if getattr(self, "_prepared", None) is None:
+            U0 = self.initial_state()
+            self._prepared = (U0, *self.time_step(U0))
+        return self._prepared
+
     def exact_state(self) -> np.ndarray:
         """Exact solution at final_time (the vortex translated with the free stream)."""
         if self.flow_case != "isentropic_vortex":
@@ -266,16 +273,16 @@ class SnapshotServer:
     """
 
     def __init__(self, batch, chunk: int = 16, keep_states: bool = False, clock=time.perf_counter,
-                 precision: int = _lib.PH_FP32_RESIDUAL):
+                 precision: int = _lib.PH_FP32_RESIDUAL, admit_slice: float = 0.004):
         self.batch = batch
         self.chunk = chunk
         self.keep_states = keep_states
         self.clock = clock
         self.precision = precision
+        self.admit_slice = admit_slice   # host time per loop spent admitting while solves are resident
 
     def _prepare(self, req: SolveRequest):
-        U0 = req.initial_state()
-        dt, nsteps = req.time_step(U0)
+        U0, dt, nsteps = req.prepare()
         return req.mesh(), req.parameters().to_ph_params(self.precision), U0, dt, nsteps
 
     def run(self, arrivals):
@@ -289,16 +296,21 @@ class SnapshotServer:
         while pending or queue or resident:
             now = self.clock() - t0
             while pending and pending[0][0] <= now:
-                arr, req = pending.popleft()
-                queue.append((arr, req, self._prepare(req)))
-            while queue:
-                arr, req, (mesh, prm, U0, dt, nsteps) = queue[0]
+                queue.append(pending.popleft())
+            # admit in FIFO order; while solves are resident, only for a slice of host time, so
+            # the queued GPU work keeps running while the host sets up the newcomers
+            t_end = self.clock() + self.admit_slice if resident else float("inf")
+            while queue and self.clock() < t_end:
+                arr, req = queue[0]
+                mesh, prm, U0, dt, nsteps = self._prepare(req)
                 slot = self.batch.admit(mesh, prm, U0, dt, nsteps)
                 if slot is None:
                     stats.admissions_deferred += 1
                     break
                 queue.popleft()
                 resident[slot] = (req, arr, self.clock() - t0, nsteps)
+                if len(resident) == 1:
+                    t_end = self.clock() + self.admit_slice
             stats.max_in_flight = max(stats.max_in_flight, len(resident))
             if not resident:
                 if pending:

@@ -57,7 +57,7 @@ class FakeBatch:
 
 
 class FakeServer(SnapshotServer):
-    def _prepare(self, req):
+    def _prepare(self, req):   # the fake request carries (bytes, nsteps)
         return req.tag[0], None, None, 1.0, req.tag[1]    # (bytes, -, -, dt, nsteps)
 
 
