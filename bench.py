@@ -311,15 +311,28 @@ def one_at_a_time(reqs):
             "dof_updates_per_s_stage": work / el, "dtype": "f64", "path": "single-solve context per solve"}
 
 
-def run_many(args):
-    """Batched (all admitted at t=0) or served (Poisson arrivals, continuous batching) form."""
+def run_many(args, rank: int = 0, world: int = 1, local_rank: int = 0):
+    """Batched (all admitted at t=0) or served (Poisson arrivals, continuous batching) form.
+    With N GPUs every rank serves a cost-balanced share of the same requests (by solve; no
+    exchange between ranks), so the total work is fixed (strong scaling)."""
     import torch
     from philip_b200 import _lib
-    from philip_b200.serve import Batch, SnapshotServer, autotune, poisson_arrivals, solve_bytes
-    torch.cuda.set_device(0)
+    from philip_b200.serve import Batch, SnapshotServer, autotune, poisson_arrivals
+    from philip_b200.shard import reduce_max, reduce_sum, request_cost, shard_by_cost
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     prec = _lib.PH_FP32_RESIDUAL if args.precision == "fp32" else _lib.PH_FP64
     count = args.requests or (256 if args.workload == "vortex_batch_256" else 64)
-    reqs = many_requests(args.workload, count)
+    all_reqs = many_requests(args.workload, count)
+    rng0 = np.random.default_rng(7)
+    all_arrivals = [0.0] * count if args.workload == "vortex_batch_256" else list(poisson_arrivals(args.rate, count, rng0))
+    mine = shard_by_cost([request_cost(r) for r in all_reqs], world)[rank] if world > 1 else list(range(count))
+    reqs = [all_reqs[i] for i in mine]
+    arrivals = [all_arrivals[i] for i in mine]
     tuned = {}
     for r in reqs:   # tile shapes per (order, mesh kind), before the clock starts
         key = (r.poly_degree, r.warp != 0.0)
@@ -328,24 +341,43 @@ def run_many(args):
     for r in reqs:   # the requests' payload (initial state, time step), before the clock starts
         r.prepare()
     budget = int(args.budget_gb * (1 << 30))
-    rng = np.random.default_rng(7)
-    arrivals = [0.0] * count if args.workload == "vortex_batch_256" else list(poisson_arrivals(args.rate, count, rng))
     # warm-up: one small solve through the same batch machinery
     warm = Batch(1 << 28, prec)
     SnapshotServer(warm, chunk=args.chunk, precision=prec).run([(0.0, many_requests(args.workload, 1, seed=1)[0])])
     warm.close()
     batch = Batch(budget, prec)
-    with ClockSampler(0) as clk:
+    if dist is not None:
+        dist.barrier()
+    with ClockSampler(local_rank) as clk:
         srv = SnapshotServer(batch, chunk=args.chunk, keep_states=args.workload == "vortex_batch_256", precision=prec)
         stats = srv.run(list(zip(arrivals, reqs)))
     launches = batch.launches
     batch.close()
     work = sum(c.request.ndofs * 4 * c.steps for c in stats.completed)
+    if dist is not None:   # whole job: all ranks' solves and work over the slowest rank's makespan
+        lat = [None] * world
+        dist.all_gather_object(lat, [c.latency for c in stats.completed])
+        makespan = reduce_max(stats.makespan, dist, "cuda")
+        work = reduce_sum(work, dist, "cuda")
+        launches = int(reduce_sum(launches, dist, "cuda"))
+        latencies = sorted(x for part in lat for x in part)
+        stats.makespan = makespan
+        stats.completed_all = latencies
+        if rank != 0:
+            dist.barrier()
+            dist.destroy_process_group()
+            return 0
+    else:
+        latencies = sorted(c.latency for c in stats.completed)
+
+    def pct(q):
+        k = min(len(latencies) - 1, max(0, int(np.ceil(q / 100.0 * len(latencies))) - 1))
+        return latencies[k]
     line = {
         "metric": "served solves/s" if args.workload == "served_stream" else "batched DOF-updates/s/stage",
         "unit": "solves/s" if args.workload == "served_stream" else "DOF-updates/s/stage",
-        "value": stats.solves_per_s if args.workload == "served_stream" else work / stats.makespan,
-        "n_gpus": 1, "steps": None, "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "value": len(latencies) / stats.makespan if args.workload == "served_stream" else work / stats.makespan,
+        "n_gpus": world, "steps": None, "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32-residual/f64-state" if prec == _lib.PH_FP32_RESIDUAL else "f64",
         "data": "synthetic (seeded requests; exact initial conditions)",
         "config": {"workload": args.workload, "description": MANY[args.workload], "requests": count,
@@ -353,10 +385,10 @@ def run_many(args):
                    "arrival_rate_per_s": None if args.workload == "vortex_batch_256" else args.rate,
                    "total_dofs": int(sum(r.ndofs for r in reqs)),
                    "tile_variants": {f"p{k[0]}{'c' if k[1] else 'a'}": v for k, v in tuned.items()}},
-        "solves_per_s": stats.solves_per_s, "dof_updates_per_s_stage": work / stats.makespan,
+        "solves_per_s": len(latencies) / stats.makespan, "dof_updates_per_s_stage": work / stats.makespan,
         "makespan_s": stats.makespan,
-        "latency_ms": {"p50": 1e3 * stats.percentile(50), "p99": 1e3 * stats.percentile(99),
-                       "max": 1e3 * max(c.latency for c in stats.completed)},
+        "latency_ms": {"p50": 1e3 * pct(50), "p99": 1e3 * pct(99), "max": 1e3 * latencies[-1]},
+        "parallelism": f"solves sharded over {world} GPU(s)" if world > 1 else "one GPU",
         "max_resident": stats.max_in_flight, "gpu_launches": launches,
         "status_flags": int(np.bitwise_or.reduce([c.status for c in stats.completed])),
         "clocks": clk.summary(),
@@ -367,13 +399,16 @@ def run_many(args):
             ex = c.request.exact_state()
             errs.append(float(np.max(np.abs(c.state - ex)) / np.max(np.abs(ex))))
         line["vortex_rel_max_error"] = {"median": float(np.median(errs)), "max": float(np.max(errs))}
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and world == 1:
         sample = reqs[: args.baseline_sample] if args.baseline_sample else reqs
         base = one_at_a_time(sample)
         base["sample"] = f"first {len(sample)} of the {count} requests, run back to back (no arrival gaps)"
         line["one_at_a_time"] = base
         line["speedup_vs_one_at_a_time"] = (line["dof_updates_per_s_stage"] / base["dof_updates_per_s_stage"])
     print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
     return 0
 
 
@@ -405,7 +440,7 @@ def main():
             return 0
         if args.precision == "fp64" and "--precision" not in sys.argv:
             args.precision = "fp32"   # the batched and served forms run the precision form by default
-        return run_many(args)
+        return run_many(args, rank, world, local_rank)
     if args.impl == "reference":
         return run_reference(args, rank, world)
 
@@ -421,6 +456,7 @@ def main():
     from philip_b200 import _lib
     from philip_b200.dg import FlowSolver
     from philip_b200.prm import Parameters
+    from philip_b200.shard import reduce_max
 
     if args.warmup < 3:
         args.warmup = 3
@@ -456,10 +492,7 @@ def main():
     tm = np.zeros(7)
     _lib.check(L.ph_get_timing(h, tm.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
     launches = int(tm[6])
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = reduce_max(ms, dist, "cuda")
     ms_per_step = ms / args.steps
     value = world * dg.n_dofs * stages * args.steps / (ms * 1e-3)
 
@@ -484,10 +517,7 @@ def main():
         _lib.check(L.ph_get_state(h, U_host.data_ptr(), _lib.PH_HOST))
     e1.record(); torch.cuda.synchronize()
     ms_e2e = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([ms_e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
+    ms_e2e = reduce_max(ms_e2e, dist, "cuda")
     e2e = world * dg.n_dofs * stages * args.steps / (ms_e2e * 1e-3)
     status = dg.status()
 

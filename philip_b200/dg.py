@@ -210,12 +210,47 @@ def conservative_state(dg: DGStrong, prim) -> np.ndarray:
     return np.ascontiguousarray(cons.reshape(-1))
 
 
-class FlowSolver:
-    """FlowSolver::run for the periodic-cube cases (TGV; isentropic vortex)."""
+RESTART_MAGIC = b"PHB2RST1"
 
-    def __init__(self, parameters: Parameters, precision: int = _lib.PH_FP64, cell_order: int = 0):
+
+def restart_filename_without_extension(index: int) -> str:
+    """FlowSolver::get_restart_filename_without_extension (flow_solver.cpp:168-180)."""
+    return f"restart-{index:05d}"
+
+
+def write_restart_state(path: str, U: np.ndarray, time: float, iteration: int, dt: float):
+    """Device-state checkpoint: magic, DOF count, time, iteration, time step, then the state in
+    the reference DoF order (little-endian float64). It stands in for deal.II's
+    triangulation + SolutionTransfer serialisation, which this path does not link."""
+    with open(path, "wb") as f:
+        f.write(RESTART_MAGIC)
+        np.array([U.size, iteration], dtype="<i8").tofile(f)
+        np.array([time, dt], dtype="<f8").tofile(f)
+        np.ascontiguousarray(U, dtype="<f8").tofile(f)
+
+
+def read_restart_state(path: str):
+    with open(path, "rb") as f:
+        if f.read(8) != RESTART_MAGIC:
+            raise ValueError(f"{path}: not a restart state file")
+        n, iteration = np.fromfile(f, dtype="<i8", count=2)
+        time, dt = np.fromfile(f, dtype="<f8", count=2)
+        U = np.fromfile(f, dtype="<f8", count=int(n))
+    if U.size != n:
+        raise ValueError(f"{path}: truncated")
+    return U, float(time), int(iteration), float(dt)
+
+
+class FlowSolver:
+    """FlowSolver::run for the periodic-cube cases (TGV; isentropic vortex), with the
+    reference's restart files (flow_solver.cpp:240-395): restart-NNNNN.prm (the input
+    parameters with the ODE solver's initial time / iteration / time step and the restart
+    switches updated), the unsteady data table, and the state checkpoint."""
+
+    def __init__(self, parameters: Parameters, precision: int = _lib.PH_FP64, cell_order: int = 0,
+                 warp: float = 0.0):
         self.parameters = parameters
-        self.dg = DGStrong(parameters, precision=precision, cell_order=cell_order)
+        self.dg = DGStrong(parameters, precision=precision, cell_order=cell_order, warp=warp)
         self.ode_solver = RungeKuttaODESolver(self.dg)
         self.flow_case = parameters.get("flow_solver/flow_case_type")
         X = self.dg.node_coordinates()
@@ -231,6 +266,58 @@ class FlowSolver:
             raise ValueError(f"flow_case_type {self.flow_case!r} is outside the periodic-cube cases")
         self.dg.solution = conservative_state(self.dg, prim)
         self.unsteady_data = []
+        self.restart_dt = None
+        if parameters.get("flow_solver/restart_computation_from_file").lower() == "true":
+            self._restart_from_file()
+
+    def _restart_dir(self) -> str:
+        return self.parameters.get("flow_solver/restart_files_directory_name")
+
+    def _table_name(self, index: int) -> str:
+        return (self.parameters.get("flow_solver/unsteady_data_table_filename") + "-" +
+                restart_filename_without_extension(index) + ".txt")
+
+    def _restart_from_file(self):
+        """FlowSolver constructor's restart branch (flow_solver.cpp:58-100, :452-541)."""
+        import os
+        idx = int(self.parameters.get("flow_solver/restart_file_index"))
+        base = os.path.join(self._restart_dir(), restart_filename_without_extension(idx))
+        U, t, it, dt = read_restart_state(base + ".sol")
+        if U.size != self.dg.n_dofs:
+            raise ValueError("restart state does not match the discretisation")
+        self.dg.solution = U
+        self.ode_solver.current_time = float(self.parameters.get("ODE solver/initial_time"))
+        self.ode_solver.current_iteration = int(self.parameters.get("ODE solver/initial_iteration"))
+        self.dg.set_current_time(self.ode_solver.current_time)
+        self.restart_dt = float(self.parameters.get("ODE solver/initial_time_step"))
+        table = os.path.join(self._restart_dir(), self._table_name(idx))
+        if os.path.exists(table):
+            rows = np.loadtxt(table, skiprows=1, ndmin=2)
+            self.unsteady_data = [tuple(r) for r in rows]
+
+    def output_restart_files(self, index: int, dt: float):
+        """FlowSolver::output_restart_files + write_restart_parameter_file (flow_solver.cpp:240-395)."""
+        import os
+        d = self._restart_dir()
+        base = os.path.join(d, restart_filename_without_extension(index))
+        write_restart_state(base + ".sol", self.dg.solution, self.ode_solver.current_time,
+                            self.ode_solver.current_iteration, dt)
+        with open(os.path.join(d, self._table_name(index)), "w") as f:
+            f.write("time kinetic_energy enstrophy vorticity_based_dissipation_rate max_wave_speed\n")
+            for row in self.unsteady_data:
+                f.write(" ".join(repr(float(v)) for v in row) + "\n")
+        prm = self.parameters.with_values({
+            "ODE solver/initial_desired_time_for_output_solution_every_dt_time_intervals":
+                f"{self.ode_solver.current_time:.16e}",
+            "ODE solver/initial_iteration": str(self.ode_solver.current_iteration),
+            "ODE solver/initial_time": f"{self.ode_solver.current_time:.16e}",
+            "ODE solver/initial_time_step": f"{dt:.16e}",
+            "flow_solver/output_restart_files": "true",
+            "flow_solver/restart_computation_from_file": "true",
+            "flow_solver/restart_file_index": str(index),
+        })
+        with open(base + ".prm", "w") as f:   # written last, after the data it points to
+            f.write(prm.to_text())
 
     def _grid_spacing(self) -> float:
         left, right = self.parameters.grid_bounds
@@ -259,8 +346,15 @@ class FlowSolver:
         final_time = float(self.parameters.get("flow_solver/final_time"))
         end_exact = self.parameters.get("flow_solver/end_exactly_at_final_time").lower() == "true"
         adaptive = self.parameters.get("flow_solver/adaptive_time_step").lower() == "true"
-        dt = self.time_step()
-        self.unsteady_data.append((self.ode_solver.current_time, *self.dg.integrals()))
+        write_restart = self.parameters.get("flow_solver/output_restart_files").lower() == "true"
+        every_x = int(self.parameters.get("flow_solver/output_restart_files_every_x_steps"))
+        every_dt = float(self.parameters.get("flow_solver/output_restart_files_every_dt_time_intervals"))
+        restart_index = int(self.parameters.get("flow_solver/restart_file_index")) + 1 \
+            if self.restart_dt is not None else 1
+        next_restart_time = self.ode_solver.current_time + every_dt
+        dt = self.restart_dt if self.restart_dt is not None else self.time_step()
+        if not self.unsteady_data:
+            self.unsteady_data.append((self.ode_solver.current_time, *self.dg.integrals()))
         while self.ode_solver.current_time < final_time:
             step = dt
             if self.ode_solver.current_time + step > final_time and end_exact:
@@ -272,4 +366,12 @@ class FlowSolver:
                 if adaptive:
                     dt = float(self.parameters.get("flow_solver/courant_friedrichs_lewy_number")) * \
                         self._grid_spacing() / q[3]
+            if write_restart:   # flow_solver.cpp:605-632: every dt time interval, or every x steps
+                if every_dt > 0.0:
+                    if self.ode_solver.current_time >= next_restart_time:
+                        self.output_restart_files(restart_index, dt)
+                        restart_index += 1
+                        next_restart_time += every_dt
+                elif self.ode_solver.current_iteration % every_x == 0:
+                    self.output_restart_files(self.ode_solver.current_iteration // every_x, dt)
         return 0

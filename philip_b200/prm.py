@@ -44,6 +44,13 @@ DEFAULTS = {
     "flow_solver/end_exactly_at_final_time": "true",
     "flow_solver/grid/grid_left_bound": "0.0", "flow_solver/grid/grid_right_bound": "1.0",
     "flow_solver/grid/number_of_grid_elements_per_dimension": "4",
+    "ODE solver/initial_time": "0.0", "ODE solver/initial_iteration": "0", "ODE solver/initial_time_step": "100.0",
+    "ODE solver/initial_desired_time_for_output_solution_every_dt_time_intervals": "0.0",
+    "flow_solver/unsteady_data_table_filename": "unsteady_data_table",
+    "flow_solver/output_restart_files": "false", "flow_solver/restart_computation_from_file": "false",
+    "flow_solver/restart_files_directory_name": ".", "flow_solver/restart_file_index": "1",
+    "flow_solver/output_restart_files_every_x_steps": "1",
+    "flow_solver/output_restart_files_every_dt_time_intervals": "0.0",
     "flow_solver/taylor_green_vortex/expected_kinetic_energy_at_final_time": "0",
     "flow_solver/taylor_green_vortex/expected_theoretical_dissipation_rate_at_final_time": "0",
 }
@@ -74,6 +81,32 @@ def parse_text(text: str) -> dict:
     if stack:
         raise ValueError(f"unterminated subsection(s): {stack}")
     return out
+
+
+def format_text(values: dict) -> str:
+    """The inverse of parse_text: a .prm text with one ``set`` line per key, subsections
+    nested in the order their keys first appear."""
+    tree: dict = {}
+    for key, val in values.items():
+        node = tree
+        *subs, leaf = key.split("/")
+        for sub in subs:
+            node = node.setdefault(("sub", sub), {})
+        node[("set", leaf)] = val
+    lines: list = []
+
+    def emit(node, depth):
+        pad = "  " * depth
+        for (kind, name), v in node.items():
+            if kind == "set":
+                lines.append(f"{pad}set {name} = {v}")
+        for (kind, name), v in node.items():
+            if kind == "sub":
+                lines.append(f"{pad}subsection {name}")
+                emit(v, depth + 1)
+                lines.append(f"{pad}end")
+    emit(tree, 0)
+    return "\n".join(lines) + "\n"
 
 
 def parse_file(path: str) -> dict:
@@ -107,6 +140,16 @@ class Parameters:
     @classmethod
     def from_file(cls, path: str) -> "Parameters":
         return cls(parse_file(path))
+
+    def with_values(self, updates: dict) -> "Parameters":
+        """A copy with the given keys set (values as the .prm spells them)."""
+        raw = dict(self.raw)
+        for k, v in updates.items():
+            raw[k] = str(v).lower() if isinstance(v, bool) else str(v)
+        return Parameters(raw)
+
+    def to_text(self) -> str:
+        return format_text(self.raw)
 
     @classmethod
     def from_dict(cls, d: dict) -> "Parameters":
