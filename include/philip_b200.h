@@ -92,6 +92,12 @@ typedef struct ph_mesh_desc {
      * (src/mesh/grids/curved_periodic_grid.cpp) with this warp. */
     double warp;
     int grid_degree;
+    /* Optional: physical coordinates of every cell's mapping support points, [cell][3][(p+1)^3]
+     * (GLL points, x fastest, cells in the state's order). When set, the mesh is curvilinear
+     * with this mapping (any curved periodic grid, e.g. the reference's curved_periodic_grid
+     * or nonsymmetric_curved_periodic_grid with grid_degree = poly_degree) and warp is
+     * ignored. The caller keeps the array alive during ph_ctx_create / ph_batch_admit. */
+    const double* mapping_support_points;
 } ph_mesh_desc;
 
 /* Builds host index maps, 1-D operators and device buffers (replaces DGFactory::

@@ -38,7 +38,8 @@ class PhParams(ctypes.Structure):
 class PhMeshDesc(ctypes.Structure):
     _fields_ = [("n_cells_per_direction", ctypes.c_int), ("cell_order", ctypes.c_int),
                 ("left", ctypes.c_double), ("right", ctypes.c_double),
-                ("warp", ctypes.c_double), ("grid_degree", ctypes.c_int)]
+                ("warp", ctypes.c_double), ("grid_degree", ctypes.c_int),
+                ("mapping_support_points", ctypes.POINTER(ctypes.c_double))]
 
 
 class PhError(RuntimeError):

@@ -416,7 +416,7 @@ int ph_batch_bytes(const ph_mesh_desc* mesh, const ph_params* prm, size_t* bytes
     if (!mesh || !prm || !bytes) return fail(PH_ERR_INVALID, "null argument");
     if (int rc = check_batch_params(nullptr, mesh, prm)) return rc;
     const int n = mesh->n_cells_per_direction, nc = n * n * n, N1 = prm->poly_degree + 1, NP = N1 * N1 * N1;
-    const SlotLayout L = slot_layout((size_t)nc * 5 * NP, nc, NP, mesh->warp != 0.0, prm->runge_kutta_method == 1,
+    const SlotLayout L = slot_layout((size_t)nc * 5 * NP, nc, NP, is_curvilinear(mesh), prm->runge_kutta_method == 1,
                                      prm->precision == PH_FP32_RESIDUAL);
     *bytes = L.total;
     return PH_OK;
@@ -429,7 +429,7 @@ int ph_batch_admit(ph_batch* b, const ph_mesh_desc* mesh, const ph_params* prm, 
     if (int rc = check_batch_params(b, mesh, prm)) return rc;
     if (nsteps < 0 || !(dt > 0.0)) return fail(PH_ERR_INVALID, "dt must be > 0 and nsteps >= 0");
     const int n = mesh->n_cells_per_direction, nc = n * n * n, N1 = prm->poly_degree + 1, NP = N1 * N1 * N1;
-    const bool curv = mesh->warp != 0.0;
+    const bool curv = is_curvilinear(mesh);
     const size_t ndofs = (size_t)nc * 5 * NP;
     int ns = 0;
     double A[4][4], bw[4];
@@ -453,7 +453,7 @@ int ph_batch_admit(ph_batch* b, const ph_mesh_desc* mesh, const ph_params* prm, 
     int rc = build_operators(prm, ops, fr, x, D);
     if (!rc) {
         periodic_connectivity(n, mesh->cell_order, ijk, nbr);
-        rc = node_geometry(n, ijk, x, D, mesh->left, mesh->right, mesh->warp, xyz, metric);
+        rc = node_geometry(n, ijk, x, D, mesh->left, mesh->right, mesh->warp, xyz, metric, mesh->mapping_support_points);
     }
     if (rc) { arena_free(b, off, L.total); return rc; }
     int s = -1;
@@ -635,7 +635,8 @@ int ph_mesh_node_xyz(const ph_mesh_desc* mesh, int poly_degree, double* xyz) {
     std::vector<int> ijk, nbr;
     if (int rc = build_operators(&prm, ops, fr, x, D)) return rc;
     periodic_connectivity(mesh->n_cells_per_direction, mesh->cell_order, ijk, nbr);
-    if (int rc = node_geometry(mesh->n_cells_per_direction, ijk, x, D, mesh->left, mesh->right, mesh->warp, X, metric))
+    if (int rc = node_geometry(mesh->n_cells_per_direction, ijk, x, D, mesh->left, mesh->right, mesh->warp, X, metric,
+                               mesh->mapping_support_points))
         return rc;
     std::memcpy(xyz, X.data(), X.size() * sizeof(double));
     return PH_OK;
@@ -666,7 +667,7 @@ int ph_batch_autotune(int poly_degree, int precision, int curvilinear, int* best
     if (nvariants) *nvariants = nv;
     // synthetic solve: TGV on the periodic cube, large enough to fill the GPU several times
     const int n = poly_degree <= 3 ? 24 : 16;
-    ph_mesh_desc mesh{n, 0, 0.0, 2.0 * M_PI, curv ? 0.1 : 0.0, poly_degree};
+    ph_mesh_desc mesh{n, 0, 0.0, 2.0 * M_PI, curv ? 0.1 : 0.0, poly_degree, nullptr};
     ph_params prm{};
     prm.poly_degree = poly_degree; prm.flux_nodes_type = 1; prm.pde_type = 0; prm.use_split_form = 1;
     prm.two_point_num_flux_type = ph::TP_CH; prm.conv_num_flux = ph::CF_EC_ROE; prm.diss_num_flux = 0;

@@ -200,13 +200,15 @@ void nodal_derivative(const std::vector<double>& D, int N1, int dir, const doubl
 // mapping Jacobian (operators.cpp:2629-2672). Writes metric rows 0..8 (C[k][d] at k*3+d),
 // row 9 = 1 / det J, and the node coordinates; returns false on a non-positive det J.
 bool curvilinear_cell(const std::vector<double>& x, const std::vector<double>& D, int N1, double h, double left,
-                      double right, double warp, const int ijk[3], double* metric, double* xyz) {
+                      double right, double warp, const int ijk[3], double* metric, double* xyz,
+                      const double* support /* [3][NP] or nullptr */) {
     const int NP = N1 * N1 * N1;
     std::vector<double> X(3 * NP), G(9 * NP), P(9 * NP), t(NP);
     for (int node = 0; node < NP; ++node) {
         const int i = node % N1, j = (node / N1) % N1, k = node / (N1 * N1);
         double p[3] = {left + h * (ijk[0] + x[i]), left + h * (ijk[1] + x[j]), left + h * (ijk[2] + x[k])};
-        warp_point(left, right, warp, p);
+        if (support) { for (int d = 0; d < 3; ++d) p[d] = support[d * NP + node]; }
+        else warp_point(left, right, warp, p);
         for (int d = 0; d < 3; ++d) { X[d * NP + node] = p[d]; xyz[node * 3 + d] = p[d]; }
     }
     for (int m = 0; m < 3; ++m)
@@ -252,8 +254,9 @@ const char* unsupported_reason(const ph_mesh_desc* mesh, const ph_params* prm) {
         return "the GPU path is collocated: flux_nodes_type = GLL and overintegration = 0";
     if (prm->poly_degree < 1 || prm->poly_degree > 6) return "poly_degree must be 1..6";
     if (prm->flux_reconstruction_aux != 0) return "flux_reconstruction_aux must be kDG";
-    if (mesh->warp != 0.0) {
-        if (mesh->grid_degree != prm->poly_degree) return "curvilinear meshes take grid_degree = poly_degree";
+    if (is_curvilinear(mesh)) {
+        if (mesh->mapping_support_points == nullptr && mesh->grid_degree != prm->poly_degree)
+            return "curvilinear meshes take grid_degree = poly_degree";
         if (prm->pde_type != 0) return "curvilinear meshes take the Euler equations";
         if (!prm->use_split_form) return "curvilinear meshes take the split form";
         if (prm->flux_reconstruction != 0) return "curvilinear meshes take cDG";
@@ -349,10 +352,11 @@ void periodic_connectivity(int n, int order, std::vector<int>& ijk, std::vector<
 }
 
 int node_geometry(int n, const std::vector<int>& ijk, const std::vector<double>& x, const std::vector<double>& D,
-                  double left, double right, double warp, std::vector<double>& xyz, std::vector<double>& metric) {
+                  double left, double right, double warp, std::vector<double>& xyz, std::vector<double>& metric,
+                  const double* support) {
     const int N1 = (int)x.size(), NP = N1 * N1 * N1, nc = n * n * n;
     const double h = (right - left) / n;
-    const bool curv = warp != 0.0;
+    const bool curv = warp != 0.0 || support != nullptr;
     xyz.assign((size_t)nc * NP * 3, 0.0);
     if (curv) metric.assign((size_t)nc * 10 * NP, 0.0);
     else metric.clear();
@@ -365,7 +369,9 @@ int node_geometry(int n, const std::vector<int>& ijk, const std::vector<double>&
                 const int* t = &ijk[3 * cc];
                 double* X = &xyz[(size_t)cc * NP * 3];
                 if (curv) {
-                    if (!curvilinear_cell(x, D, N1, h, left, right, warp, t, &metric[(size_t)cc * 10 * NP], X)) ok[tI] = 0;
+                    if (!curvilinear_cell(x, D, N1, h, left, right, warp, t, &metric[(size_t)cc * 10 * NP], X,
+                                          support ? support + (size_t)cc * 3 * NP : nullptr))
+                        ok[tI] = 0;
                 } else {
                     for (int node = 0; node < NP; ++node) {
                         const int ii[3] = {node % N1, (node / N1) % N1, node / (N1 * N1)};
@@ -559,7 +565,7 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
     c->fp32 = prm->precision == PH_FP32_RESIDUAL;
     c->ndofs = (size_t)c->nc * 5 * c->NP;
     c->warp = mesh->warp;
-    c->curv = mesh->warp != 0.0;
+    c->curv = is_curvilinear(mesh);
     cudaGetDevice(&c->device);
 
     // ---- 1-D operators, integral tables, physics, RK tableau, connectivity, geometry
@@ -572,7 +578,8 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
     std::vector<int> nbr;
     periodic_connectivity(c->n, mesh->cell_order, c->ijk, nbr);
     std::vector<double> metric;
-    if (int rc = node_geometry(c->n, c->ijk, x, D, c->left, c->right, c->warp, c->xyz, metric)) { delete c; return rc; }
+    if (int rc = node_geometry(c->n, c->ijk, x, D, c->left, c->right, c->warp, c->xyz, metric,
+                               mesh->mapping_support_points)) { delete c; return rc; }
 
     // ---- device buffers
     const size_t N = c->ndofs;
@@ -956,7 +963,7 @@ __global__ void noalloc_neighbours(int n, int morton, int levels, int* nbr) {
 extern "C" int ph_residual_noalloc(const ph_mesh_desc* mesh, const ph_params* prm, const double* U, double* R,
                                    void* cuda_stream) {
     if (!mesh || !prm || !U || !R) return fail(PH_ERR_INVALID, "null argument");
-    if (mesh->warp != 0.0) return fail(PH_ERR_UNSUPPORTED, "ph_residual_noalloc: affine meshes only (warp = 0)");
+    if (is_curvilinear(mesh)) return fail(PH_ERR_UNSUPPORTED, "ph_residual_noalloc: affine meshes only");
     if (prm->flux_nodes_type != 1 || prm->overintegration != 0)
         return fail(PH_ERR_UNSUPPORTED, "the GPU path is collocated: flux_nodes_type = GLL and overintegration = 0");
     if (prm->poly_degree < 1 || prm->poly_degree > 6) return fail(PH_ERR_UNSUPPORTED, "poly_degree must be 1..6");

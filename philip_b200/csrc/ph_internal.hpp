@@ -31,10 +31,17 @@ ph::PhysConst physics_constants(const ph_params* prm, double h, double& penalty)
 // deal.II cell order (ijk, 3 per cell) and the 6 periodic neighbours of each cell.
 void periodic_connectivity(int n, int order, std::vector<int>& ijk, std::vector<int>& nbr);
 
-// Node coordinates [cell][node][3] and, for warp != 0, the metric rows [cell][10][NP];
+// Node coordinates [cell][node][3] and, for a curvilinear mesh (warp != 0 or given support
+// points [cell][3][NP]), the metric rows [cell][10][NP];
 // cells are processed by host threads. Returns PH_OK or an error (folded cell).
 int node_geometry(int n, const std::vector<int>& ijk, const std::vector<double>& x, const std::vector<double>& D,
-                  double left, double right, double warp, std::vector<double>& xyz, std::vector<double>& metric);
+                  double left, double right, double warp, std::vector<double>& xyz, std::vector<double>& metric,
+                  const double* support = nullptr);
+
+// a curvilinear mesh: warped, or given by its mapping support points
+inline bool is_curvilinear(const ph_mesh_desc* mesh) {
+    return mesh->warp != 0.0 || mesh->mapping_support_points != nullptr;
+}
 
 // Butcher tableau of the explicit RK method (runge_kutta_methods.cpp:7-47).
 void rk_tableau(int method, int& ns, double A[4][4], double b[4]);

@@ -53,15 +53,19 @@ class DGStrong:
     """Strong-form DG/FR discretisation on a periodic cube, evaluated on the B200."""
 
     def __init__(self, parameters: Parameters, precision: int = _lib.PH_FP64, cell_order: int = 0,
-                 stream: int | None = None, warp: float = 0.0):
+                 stream: int | None = None, warp: float = 0.0, mapping_support_points: np.ndarray | None = None):
         """warp != 0 gives the sine-warped (curvilinear) cube: every coordinate moves by
-        warp (L/2pi) sin(2pi(x-l)/L) sin(2pi(y-l)/L) sin(2pi(z-l)/L), mapping degree = p."""
+        warp (L/2pi) sin(2pi(x-l)/L) sin(2pi(y-l)/L) sin(2pi(z-l)/L), mapping degree = p.
+        mapping_support_points ([cell][3][(p+1)^3], GLL points) gives any other curved mapping."""
         self.L = _lib.load()
         self.parameters = parameters
         self.params = parameters.to_ph_params(precision)
         left, right = parameters.grid_bounds
         self.warp = float(warp)
         self.mesh = _lib.PhMeshDesc(parameters.n_cells, cell_order, left, right, self.warp, parameters.poly_degree)
+        if mapping_support_points is not None:
+            self._support = np.ascontiguousarray(mapping_support_points, dtype=np.float64)
+            self.mesh.mapping_support_points = self._support.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
         h = ctypes.c_void_p()
         _lib.check(self.L.ph_ctx_create(ctypes.byref(self.mesh), ctypes.byref(self.params),
                                         ctypes.c_void_p(stream) if stream else None, ctypes.byref(h)))

@@ -135,3 +135,42 @@ def test_curvilinear_precision_form():
     err = rel_max_err(dg.residual_of(U), orc.residual(U))
     print(f"curvilinear fp32 residual rel err {err:.3e}")
     assert err <= 1e-5
+
+
+def _support_points(xyz, nd):
+    """[cell][node][3] -> [cell][3][node]"""
+    return np.ascontiguousarray(np.transpose(xyz.reshape(-1, nd ** 3, 3), (0, 2, 1)))
+
+
+@pytest.mark.gpu
+def test_explicit_support_points_match_the_warp():
+    from philip_b200.dg import DGStrong
+    kw = dict(poly_degree=3, n_cells=3)
+    prm, orc = _oracle(kw, WARP)
+    X = _support_points(orc.node_xyz(), orc.nd)
+    dg = DGStrong(prm, mapping_support_points=X)
+    U = perturbed_tgv(orc, seed=9)
+    err = rel_max_err(dg.residual_of(U), orc.residual(U))
+    print(f"support points from the warp: rel max err {err:.3e}")
+    assert err <= RTOL
+
+
+@pytest.mark.gpu
+def test_reference_style_curved_periodic_grid_preserves_free_stream():
+    """The chart map of the reference's PeriodicSineManifold (curved_periodic_grid.cpp:64-90:
+    x += 0.2 sin(pi y), y += 0.2 sin(pi z), z += 0.2 sin(pi x) on the unit cube), given as
+    mapping support points: a uniform flow stays uniform (metric identities of the curl form)."""
+    from philip_b200.dg import DGStrong
+    kw = dict(poly_degree=4, n_cells=2, left=0.0, right=1.0)
+    prm, orc = _oracle(kw, 0.0)
+    P = orc.node_xyz().reshape(-1, 3).copy()
+    x, y, z = P[:, 0].copy(), P[:, 1].copy(), P[:, 2].copy()
+    P[:, 0] = x + 0.2 * np.sin(np.pi * y)
+    P[:, 1] = y + 0.2 * np.sin(np.pi * z)
+    P[:, 2] = z + 0.2 * np.sin(np.pi * x)
+    dg = DGStrong(prm, mapping_support_points=_support_points(P, orc.nd))
+    assert np.allclose(dg.node_coordinates().reshape(-1, 3), P, rtol=0, atol=1e-15)
+    U = _uniform_state(orc)
+    R = dg.residual_of(U)
+    print(f"reference-style curved grid, uniform flow: max |R| {np.max(np.abs(R)):.3e}")
+    assert np.max(np.abs(R)) <= 1e-11
