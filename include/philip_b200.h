@@ -156,7 +156,7 @@ int ph_get_timing(ph_ctx* ctx, double out[7]);
  * exists for callers that cannot call cudaMalloc (loops that must not synchronise the
  * device, or a framework that owns all device memory). U and R need no initialisation
  * beyond U's values. Its scratch lives in fixed file-scope device arrays: at most 32768 cells, and
- * for Navier-Stokes at most 12 x cells x (p+1)^3 <= 4 Mi doubles of viscous-flux scratch
+ * for Navier-Stokes at most cells x (4 (p+1)^3 + 24 (p+1)^2) <= 4 Mi doubles of viscous-term scratch
  * (32 MiB); larger meshes are rejected with PH_ERR_INVALID. The first call on a device
  * resolves the arrays' device addresses and should come before any stream capture.
  * Every call shares the same arrays: calls that overlap on the GPU (other streams or

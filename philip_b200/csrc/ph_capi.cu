@@ -592,7 +592,7 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
     bad |= dalloc(&c->d_stB, N);
     bad |= dalloc(&c->d_acc, N);
     if (c->ns == 3) bad |= dalloc(&c->d_carry, N);
-    if (c->visc) bad |= dalloc(&c->d_fv, (size_t)12 * c->nc * c->NP);   // viscous flux scratch
+    if (c->visc) bad |= dalloc(&c->d_fv, (size_t)c->nc * (4 * c->NP + 24 * c->N1 * c->N1));   // viscous terms
     if (c->fp32) bad |= dalloc(&c->d_comp, N);
     bad |= dalloc(&c->d_partial, 3 * (size_t)c->nc);
     bad |= dalloc(&c->d_status, 1);
@@ -834,7 +834,7 @@ int ph_sync(ph_ctx* c) {
 // device (cudaMalloc and cudaFree may), and host frameworks that reserve the device memory
 // up front through their own pool and forbid any later allocation. For them
 // ph_residual_noalloc computes R(U) on caller-owned device buffers without a context:
-// its scratch (the nodal viscous flux between the auxiliary and residual kernels), the
+// its scratch (the viscous terms between the auxiliary and residual kernels), the
 // neighbour table and the operator tables live in file-scope device arrays of fixed
 // size, which every GPU that loads this library holds until the process exits.
 // Nothing has to start at zero: each call rebuilds the tables, clears the status word,
@@ -843,7 +843,7 @@ int ph_sync(ph_ctx* c) {
 // =======================================================================================
 namespace {
 
-constexpr size_t NOALLOC_FV_DOUBLES = (size_t)4 << 20;      // 4 Mi doubles = 32 MiB viscous-flux scratch
+constexpr size_t NOALLOC_FV_DOUBLES = (size_t)4 << 20;      // 4 Mi doubles = 32 MiB viscous-term scratch
 constexpr int NOALLOC_MAX_CELLS = 32768;                     // 32^3 cells (neighbour table 768 KiB)
 
 static __device__ __align__(256) double g_noalloc_fv[NOALLOC_FV_DOUBLES];
@@ -978,9 +978,10 @@ extern "C" int ph_residual_noalloc(const ph_mesh_desc* mesh, const ph_params* pr
     if (nc > NOALLOC_MAX_CELLS)
         return fail(PH_ERR_INVALID, "ph_residual_noalloc: " + std::to_string(nc) + " cells exceed the fixed limit of " +
                                         std::to_string(NOALLOC_MAX_CELLS));
-    if (visc && (size_t)12 * nc * NP > NOALLOC_FV_DOUBLES)
-        return fail(PH_ERR_INVALID, "ph_residual_noalloc: the viscous-flux scratch needs " +
-                                        std::to_string((size_t)12 * nc * NP) + " doubles, above the fixed " +
+    const size_t fv_doubles = (size_t)nc * (4 * NP + 24 * N1 * N1);
+    if (visc && fv_doubles > NOALLOC_FV_DOUBLES)
+        return fail(PH_ERR_INVALID, "ph_residual_noalloc: the viscous-term scratch needs " +
+                                        std::to_string(fv_doubles) + " doubles, above the fixed " +
                                         std::to_string(NOALLOC_FV_DOUBLES));
     int dev = 0;
     PH_CUDA(cudaGetDevice(&dev));

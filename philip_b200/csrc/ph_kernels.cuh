@@ -25,8 +25,19 @@
 
 #include "ph_physics.cuh"
 
+// resident CTAs per SM asked of the compiler (register budget) for the p = 3 and p = 5
+// stage tiles, FP64 and FP32 (measured choices; see the Layout)
 #ifndef PH_P5_MINB
-#define PH_P5_MINB 3
+#define PH_P5_MINB 4
+#endif
+#ifndef PH_P5_MINB_F32
+#define PH_P5_MINB_F32 6
+#endif
+#ifndef PH_P3_MINB
+#define PH_P3_MINB 6
+#endif
+#ifndef PH_P3_MINB_F32
+#define PH_P3_MINB_F32 8
 #endif
 
 namespace ph {
@@ -44,7 +55,7 @@ struct OpTab {
 
 struct StageArgs {
     const double* U;          // stage input state [nc][5][NP]
-    const double* Fv;         // viscous flux [nc][3 dirs x 4][NP] from the auxiliary kernel (viscous)
+    const double* Fv;         // viscous terms from the auxiliary kernel, viscous_terms_per_cell<N1>() per cell
     const int* nbr;           // [nc][6] neighbour cell per face
     const OpTab* ops;
     int nc;
@@ -74,6 +85,14 @@ struct StageArgs {
     const double* metric;
 };
 
+// Viscous terms per cell written by the auxiliary kernel and read by the stage kernel:
+// [4][NP] the volume divergence sum_d D_d F_v,d of the momentum and energy rows, then
+// [6 faces][4][NF] the face-normal viscous flux F_v,d(f) at each face's nodes (a cell reads
+// its neighbour's block of the opposite face, whose nodes come in the same order).
+template <int N1> __host__ __device__ constexpr int viscous_terms_per_cell() {
+    return 4 * N1 * N1 * N1 + 24 * N1 * N1;
+}
+
 // CURV: curvilinear cells (split-form Euler): the per-node metric cofactor (9 values)
 // takes the place of the precomputed flux rows in sX.
 template <typename R, int N1, int CPC, bool VISC, bool SPLIT, bool CURV = false>
@@ -82,7 +101,7 @@ struct Layout {
     static constexpr int NQV = 10;                     // rho v0 v1 v2 p E a b la lb vsq -> packed 11
     static constexpr int NQS = 11;
     static constexpr int TR = VISC ? 9 : 5;            // trace values per face node: u (5) [+ ext viscous flux (4)]
-    static constexpr int NX = (VISC ? 12 : 0) + (SPLIT ? 0 : 15) + (CURV ? 9 : 0);
+    static constexpr int NX = (VISC ? 4 : 0) + (SPLIT ? 0 : 15) + (CURV ? 9 : 0);
     static constexpr int oOps = 0;                      // D, Dsk, B, w as R
     static constexpr int nOps = 3 * N1 * N1 + N1;
     static constexpr int oU = (oOps + nOps + 1) & ~1;
@@ -96,10 +115,12 @@ struct Layout {
     static constexpr int SPW = 32 / N1;                // lines per warp
     static constexpr int WARPS_LINES = (CPC * NF + SPW - 1) / SPW;
     static constexpr int NT = WARPS_LINES * 32;
-    // p = 5 tiles are one cell per CTA: ask for PH_P5_MINB resident CTAs per SM with the
-    // viscous flux in shared memory (3: shared memory allows no more), 4 without it
-    // (64 registers; measured 5 % faster than 3 for the FP64 Euler stage)
-    static constexpr int MINB = (N1 == 6) ? (VISC ? PH_P5_MINB : 4) : 1;
+    // register budgets from timing the stage kernel on B200: p = 5 (one cell, 256 threads
+    // per CTA) 4 CTAs per SM in FP64 (2-5 % faster than 3), 6 in FP32 (3-4 % faster than 4);
+    // p = 3 (two cells, 128 threads) 6 in FP64 and 8 in FP32 (3 % faster than unbounded)
+    static constexpr bool F32 = sizeof(R) == 4;
+    static constexpr int MINB = (N1 == 6) ? (F32 ? PH_P5_MINB_F32 : PH_P5_MINB)
+                              : (N1 == 4) ? (F32 ? PH_P3_MINB_F32 : PH_P3_MINB) : 1;
 };
 
 template <int N1> __device__ __forceinline__ int node_of(int x, int y, int z) { return (z * N1 + y) * N1 + x; }
@@ -159,10 +180,11 @@ __device__ __forceinline__ void check_state_fp64(double u[5], double gm1, unsign
 // One face node of phase 3: the numerical flux at the canonical orientation (the
 // left cell is the interior side, normal +e_d) lifted into this cell with its sign.
 // The convective flux is evaluated in the frame whose x axis is the face normal.
+// fvface: this cell's face blocks of the viscous terms (viscous only).
 template <typename R, int N1, int CPC, bool VISC, bool SPLIT, bool CURV>
 __device__ __forceinline__ void face_item(const Cst<R>& cst, int tp, int cf, int df, int ucv, const R* sU,
                                           const R* sD, R* sT, const R* sX, int c, int f, int fn, R pen,
-                                          R inv_wend) {
+                                          R inv_wend, const double* __restrict__ fvface) {
     using L = Layout<R, N1, CPC, VISC, SPLIT, CURV>;
     constexpr int NP = L::NP, NF = L::NF, TR = L::TR, NQS = L::NQS;
     const int d = f >> 1;
@@ -205,7 +227,7 @@ __device__ __forceinline__ void face_item(const Cst<R>& cst, int tp, int cf, int
     for (int s = 0; s < 5; ++s) term[s] = -sgn * Fs[s];
     const R* X = sX + c * L::NX * NP;
     if constexpr (!SPLIT) {
-        constexpr int o = VISC ? 12 : 0;
+        constexpr int o = VISC ? 4 : 0;
 #pragma unroll
         for (int s = 0; s < 5; ++s) term[s] += sgn * X[(o + d * 5 + s) * NP + node];
     }
@@ -213,7 +235,7 @@ __device__ __forceinline__ void face_item(const Cst<R>& cst, int tp, int cf, int
         R Fo[4], Fn[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            Fo[k] = X[(d * 4 + k) * NP + node];
+            Fo[k] = (R)__ldg(&fvface[(f * 4 + k) * NF + fn]);
             Fn[k] = R(0.5) * (Fo[k] + tr[(5 + k) * NF + fn]);
         }
         if (df == DF_SIPG) {
@@ -327,21 +349,15 @@ __device__ __forceinline__ void volume_dir(int d, const Cst<R>& cst, int tp, con
 #endif
         unrotate_flux<R>(accr, d, acc);
     }
-    if constexpr (VISC || !SPLIT) {
+    if constexpr (!SPLIT) {   // (the viscous divergence comes precomputed from the auxiliary kernel)
         const R* X = sX + lc * L::NX * NP;
+        constexpr int o = VISC ? 4 : 0;
 #pragma unroll
         for (int l = 0; l < N1; ++l) {
             const int nl = base + l * st;
             const R coef = sOpsD[pos * N1 + l];
-            if constexpr (VISC) {
 #pragma unroll
-                for (int k = 0; k < 4; ++k) acc[1 + k] += coef * X[(d * 4 + k) * NP + nl];
-            }
-            if constexpr (!SPLIT) {
-                constexpr int o = VISC ? 12 : 0;
-#pragma unroll
-                for (int s = 0; s < 5; ++s) acc[s] += coef * X[(o + d * 5 + s) * NP + nl];
-            }
+            for (int s = 0; s < 5; ++s) acc[s] += coef * X[(o + d * 5 + s) * NP + nl];
         }
     }
     if (lvalid) {
@@ -408,10 +424,10 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
         R ue[5];
 #pragma unroll
         for (int s = 0; s < 5; ++s) { ue[s] = (R)__ldg(&a.U[((size_t)cn * 5 + s) * NP + nn]); tr[s * NF + fn] = ue[s]; }
-        if constexpr (VISC) {
-            const int d = f >> 1;
+        if constexpr (VISC) {   // the neighbour's block of the opposite face: same node order, contiguous
+            const double* fb = a.Fv + (size_t)cn * viscous_terms_per_cell<N1>() + 4 * NP + (f ^ 1) * 4 * NF;
 #pragma unroll
-            for (int k = 0; k < 4; ++k) tr[(5 + k) * NF + fn] = (R)__ldg(&a.Fv[((size_t)cn * 12 + d * 4 + k) * NP + nn]);
+            for (int k = 0; k < 4; ++k) tr[(5 + k) * NF + fn] = (R)__ldg(&fb[k * NF + fn]);
         }
     }
 
@@ -439,15 +455,16 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
         store_q<R>(sD + c * NQS * NP, NP, node, q);
         R* X = sX + c * L::NX * NP;
         if constexpr (VISC) {
+            const double* dv = a.Fv + (size_t)cell * viscous_terms_per_cell<N1>();
 #pragma unroll
-            for (int i = 0; i < 12; ++i) X[i * NP + node] = (R)__ldg(&a.Fv[((size_t)cell * 12 + i) * NP + node]);
+            for (int k = 0; k < 4; ++k) X[k * NP + node] = (R)__ldg(&dv[k * NP + node]);
         }
         if constexpr (CURV) {
 #pragma unroll
             for (int i = 0; i < 9; ++i) X[i * NP + node] = (R)__ldg(&a.metric[((size_t)cell * 10 + i) * NP + node]);
         }
         if constexpr (!SPLIT) {
-            constexpr int o = VISC ? 12 : 0;
+            constexpr int o = VISC ? 4 : 0;
             R F[5];
             conv_flux_dir<R, 0>(q, F);
 #pragma unroll
@@ -470,7 +487,13 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
             const int fn = it % NF;
             const int f = (it / NF) % 6;
             const int c = it / (NF * 6);
-            face_item<R, N1, CPC, VISC, SPLIT, CURV>(cst, tp, cf, df, ucv, sU, sD, sT, sX, c, f, fn, pen, inv_wend);
+            const double* fvface = nullptr;
+            if constexpr (VISC) {
+                int cell = cell0 + c; if (cell >= a.nc) cell = a.nc - 1;
+                fvface = a.Fv + (size_t)cell * viscous_terms_per_cell<N1>() + 4 * NP;
+            }
+            face_item<R, N1, CPC, VISC, SPLIT, CURV>(cst, tp, cf, df, ucv, sU, sD, sT, sX, c, f, fn, pen, inv_wend,
+                                                    fvface);
         }
     }
 
@@ -500,6 +523,11 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
         R G[5];
 #pragma unroll
         for (int s = 0; s < 5; ++s) G[s] = -A[s * NP + node];
+        if constexpr (VISC) {
+            const R* X = sX + c * L::NX * NP;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) G[1 + k] -= X[k * NP + node];
+        }
 #pragma unroll
         for (int f = 0; f < 6; ++f) {
             const int dn = f >> 1;
@@ -611,8 +639,10 @@ residual_kernel_batched(const StageArgs* __restrict__ inst, const BatchTile* __r
 
 // ------------------------------------------------------------------------------------
 // Auxiliary equation: lifted gradient q = M^{-1}[ vol grad + face (u* - u) n ] (kDG),
-// then the viscous flux F_v(u, q) at every node, which is all the stage kernel needs
-// (the split form evaluates it at the entropy-projected state, the nodal state for GLL).
+// then the viscous flux F_v(u, q) at every node (the split form evaluates it at the
+// entropy-projected state, the nodal state for GLL), reduced to what the stage kernel
+// needs: its volume divergence and its face-normal component on each face
+// (viscous_terms_per_cell).
 // ------------------------------------------------------------------------------------
 template <int N1, int CPC>
 struct AuxLayout {
@@ -620,7 +650,7 @@ struct AuxLayout {
     static constexpr int NT = ((CPC * NP + 31) / 32) * 32 > 512 ? 512 : ((CPC * NP + 31) / 32) * 32;
     template <typename R>
     static constexpr size_t bytes() {
-        return sizeof(R) * ((size_t)CPC * 5 * NP + (size_t)CPC * 6 * 5 * NF + N1 * N1 + N1);
+        return sizeof(R) * ((size_t)CPC * 5 * NP + (size_t)CPC * 6 * 5 * NF + N1 * N1 + N1 + (size_t)CPC * 12 * NP);
     }
 };
 
@@ -635,6 +665,7 @@ aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, const OpTa
     R* sT = sU + CPC * 5 * NP;
     R* sDm = sT + CPC * 6 * 5 * NF;
     R* sW = sDm + N1 * N1;
+    R* sF = sW + N1;                        // [c][3 dirs x 4][NP] nodal viscous flux
     Cst<R> cst; cst.load(pc);
     const int tid = threadIdx.x;
     const int cell0 = blockIdx.x * CPC;
@@ -692,7 +723,39 @@ aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, const OpTa
 #pragma unroll
         for (int d = 0; d < 3; ++d)
 #pragma unroll
-            for (int k = 0; k < 4; ++k) Fv[((size_t)cell * 12 + d * 4 + k) * NP + node] = (double)F[d][k];
+            for (int k = 0; k < 4; ++k) sF[(c * 12 + d * 4 + k) * NP + node] = F[d][k];
+    }
+    __syncthreads();
+    // volume divergence sum_d D_d F_d and the face-normal blocks
+    for (int it = tid; it < CPC * NP; it += NT) {
+        const int c = it / NP, node = it % NP;
+        const int cell = cell0 + c;
+        if (cell >= nc) continue;
+        const int cx[3] = {node % N1, (node / N1) % N1, node / (N1 * N1)};
+        const R* Fc = sF + c * 12 * NP;
+        double* out = Fv + (size_t)cell * viscous_terms_per_cell<N1>();
+        R div[4] = {R(0), R(0), R(0), R(0)};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const int st = (d == 0) ? 1 : (d == 1) ? N1 : N1 * N1;
+            const int pos = cx[d];
+            const int base = node - pos * st;
+#pragma unroll
+            for (int l = 0; l < N1; ++l) {
+                const R coef = sDm[pos * N1 + l];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) div[k] += coef * Fc[(d * 4 + k) * NP + base + l * st];
+            }
+            if (pos == 0 || pos == N1 - 1) {
+                const int f = 2 * d + (pos == 0 ? 0 : 1);
+                const int t1 = (d == 0) ? 1 : 0, t2 = (d == 2) ? 1 : 2;
+                const int fn = cx[t2] * N1 + cx[t1];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) out[4 * NP + (f * 4 + k) * NF + fn] = (double)Fc[(d * 4 + k) * NP + node];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) out[k * NP + node] = (double)div[k];
     }
 }
 

@@ -60,15 +60,16 @@ def test_noalloc_residual_matches_context_residual(name, kw):
 def test_noalloc_rejects_meshes_above_its_limits():
     import torch
     L = _lib.load()
-    prm = Parameters.from_dict(prm_dict(poly_degree=5, n_cells=12, pde="navier_stokes", diss="bassi_rebay_2"))
+    # 14^3 cells at p = 5: 2744 x (4 x 216 + 24 x 36) doubles of viscous terms > 4 Mi
+    prm = Parameters.from_dict(prm_dict(poly_degree=5, n_cells=14, pde="navier_stokes", diss="bassi_rebay_2"))
     p = prm.to_ph_params()
-    mesh = _lib.PhMeshDesc(12, 0, 0.0, 6.28318530717958623200)
-    dU = torch.zeros(5 * 216 * 12 ** 3, dtype=torch.float64, device="cuda")
+    mesh = _lib.PhMeshDesc(14, 0, 0.0, 6.28318530717958623200)
+    dU = torch.zeros(5 * 216 * 14 ** 3, dtype=torch.float64, device="cuda")
     dR = torch.zeros_like(dU)
     rc = L.ph_residual_noalloc(ctypes.byref(mesh), ctypes.byref(p), ctypes.c_void_p(dU.data_ptr()),
                                ctypes.c_void_p(dR.data_ptr()), None)
     assert rc == 1
-    assert b"viscous-flux scratch" in L.ph_last_error()
+    assert b"viscous-term scratch" in L.ph_last_error()
     mesh.n_cells_per_direction = 40
     rc = L.ph_residual_noalloc(ctypes.byref(mesh), ctypes.byref(p), ctypes.c_void_p(dU.data_ptr()),
                                ctypes.c_void_p(dR.data_ptr()), None)
