@@ -69,20 +69,23 @@ def prm_for(workload: str) -> dict:
     }
 
 
-def bytes_per_dof_stage(viscous: bool) -> dict:
+def bytes_per_dof_stage(viscous: bool, p: int = 5) -> dict:
     """Algorithmic HBM bytes per DOF of the stage kernel, averaged over the 4 RK4 stages.
 
     Stage kernel (FP64 state), per DOF:
       stage 1:   U_in + acc_out + next                   = 24 B
       stage 2,3: U_in + u_n + acc_in + acc_out + next    = 40 B
       stage 4:   U_in + acc_in + u_{n+1}                 = 24 B      -> mean 32 B
-    Viscous: the stage kernel also reads the nodal viscous flux (12 doubles per node =
-    2.4 per DOF = 19.2 B); the auxiliary kernel reads U_in (8 B) and writes that flux
-    (19.2 B). Neighbour face traces are not counted: they are re-reads of data the
-    neighbouring CTA streams, served from L2.
+    Viscous: the auxiliary kernel reads U_in (8 B) and writes the viscous terms per cell:
+    the divergence (4 NP doubles) and the six face blocks (24 NF doubles); the stage kernel
+    reads the divergence, its own face blocks and its neighbours' (48 NF doubles). Per DOF
+    (5 NP DOFs per cell). Neighbour state traces are not counted: they are re-reads of data
+    the neighbouring CTA streams, served from L2.
     """
-    stage = 32.0 + (19.2 if viscous else 0.0)
-    aux = 27.2 if viscous else 0.0
+    n1 = p + 1
+    NP, NF = n1 ** 3, n1 ** 2
+    stage = 32.0 + ((4 * NP + 48 * NF) * 8.0 / (5 * NP) if viscous else 0.0)
+    aux = (8.0 + (4 * NP + 24 * NF) * 8.0 / (5 * NP)) if viscous else 0.0
     return {"stage": stage, "aux": aux}
 
 
@@ -523,7 +526,7 @@ def main():
 
     if rank == 0:
         peak, peak_src = measured_peaks()
-        bpd = bytes_per_dof_stage(viscous)
+        bpd = bytes_per_dof_stage(viscous, p)
         if args.precision == "fp32":
             pass   # the state stays FP64, so the stage bytes are the same (+8 B/DOF Kahan term at the last stage)
         bytes_launch = bpd["stage"] * dg.n_dofs
