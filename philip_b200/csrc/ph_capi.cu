@@ -592,7 +592,10 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
     bad |= dalloc(&c->d_stB, N);
     bad |= dalloc(&c->d_acc, N);
     if (c->ns == 3) bad |= dalloc(&c->d_carry, N);
-    if (c->visc) bad |= dalloc(&c->d_fv, (size_t)c->nc * (4 * c->NP + 24 * c->N1 * c->N1));   // viscous terms
+    if (c->visc) {   // viscous terms, stored in the arithmetic type (floats in the precision form)
+        const size_t vt = (size_t)c->nc * (4 * c->NP + 24 * c->N1 * c->N1);
+        bad |= dalloc(&c->d_fv, c->fp32 ? (vt + 1) / 2 : vt);
+    }
     if (c->fp32) bad |= dalloc(&c->d_comp, N);
     bad |= dalloc(&c->d_partial, 3 * (size_t)c->nc);
     bad |= dalloc(&c->d_status, 1);

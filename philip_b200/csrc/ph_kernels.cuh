@@ -55,7 +55,8 @@ struct OpTab {
 
 struct StageArgs {
     const double* U;          // stage input state [nc][5][NP]
-    const double* Fv;         // viscous terms from the auxiliary kernel, viscous_terms_per_cell<N1>() per cell
+    const void* Fv;           // viscous terms from the auxiliary kernel, viscous_terms_per_cell<N1>() per
+                              // cell, stored in the arithmetic type R (FP32 in the precision form)
     const int* nbr;           // [nc][6] neighbour cell per face
     const OpTab* ops;
     int nc;
@@ -184,7 +185,7 @@ __device__ __forceinline__ void check_state_fp64(double u[5], double gm1, unsign
 template <typename R, int N1, int CPC, bool VISC, bool SPLIT, bool CURV>
 __device__ __forceinline__ void face_item(const Cst<R>& cst, int tp, int cf, int df, int ucv, const R* sU,
                                           const R* sD, R* sT, const R* sX, int c, int f, int fn, R pen,
-                                          R inv_wend, const double* __restrict__ fvface) {
+                                          R inv_wend, const R* __restrict__ fvface) {
     using L = Layout<R, N1, CPC, VISC, SPLIT, CURV>;
     constexpr int NP = L::NP, NF = L::NF, TR = L::TR, NQS = L::NQS;
     const int d = f >> 1;
@@ -235,7 +236,7 @@ __device__ __forceinline__ void face_item(const Cst<R>& cst, int tp, int cf, int
         R Fo[4], Fn[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            Fo[k] = (R)__ldg(&fvface[(f * 4 + k) * NF + fn]);
+            Fo[k] = __ldg(&fvface[(f * 4 + k) * NF + fn]);
             Fn[k] = R(0.5) * (Fo[k] + tr[(5 + k) * NF + fn]);
         }
         if (df == DF_SIPG) {
@@ -425,7 +426,8 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
 #pragma unroll
         for (int s = 0; s < 5; ++s) { ue[s] = (R)__ldg(&a.U[((size_t)cn * 5 + s) * NP + nn]); tr[s * NF + fn] = ue[s]; }
         if constexpr (VISC) {   // the neighbour's block of the opposite face: same node order, contiguous
-            const double* fb = a.Fv + (size_t)cn * viscous_terms_per_cell<N1>() + 4 * NP + (f ^ 1) * 4 * NF;
+            const R* fb = static_cast<const R*>(a.Fv) + (size_t)cn * viscous_terms_per_cell<N1>() + 4 * NP +
+                          (f ^ 1) * 4 * NF;
 #pragma unroll
             for (int k = 0; k < 4; ++k) tr[(5 + k) * NF + fn] = (R)__ldg(&fb[k * NF + fn]);
         }
@@ -455,9 +457,9 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
         store_q<R>(sD + c * NQS * NP, NP, node, q);
         R* X = sX + c * L::NX * NP;
         if constexpr (VISC) {
-            const double* dv = a.Fv + (size_t)cell * viscous_terms_per_cell<N1>();
+            const R* dv = static_cast<const R*>(a.Fv) + (size_t)cell * viscous_terms_per_cell<N1>();
 #pragma unroll
-            for (int k = 0; k < 4; ++k) X[k * NP + node] = (R)__ldg(&dv[k * NP + node]);
+            for (int k = 0; k < 4; ++k) X[k * NP + node] = __ldg(&dv[k * NP + node]);
         }
         if constexpr (CURV) {
 #pragma unroll
@@ -487,10 +489,10 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
             const int fn = it % NF;
             const int f = (it / NF) % 6;
             const int c = it / (NF * 6);
-            const double* fvface = nullptr;
+            const R* fvface = nullptr;
             if constexpr (VISC) {
                 int cell = cell0 + c; if (cell >= a.nc) cell = a.nc - 1;
-                fvface = a.Fv + (size_t)cell * viscous_terms_per_cell<N1>() + 4 * NP;
+                fvface = static_cast<const R*>(a.Fv) + (size_t)cell * viscous_terms_per_cell<N1>() + 4 * NP;
             }
             face_item<R, N1, CPC, VISC, SPLIT, CURV>(cst, tp, cf, df, ucv, sU, sD, sT, sX, c, f, fn, pen, inv_wend,
                                                     fvface);
@@ -657,7 +659,7 @@ struct AuxLayout {
 template <typename R, int N1, int CPC>
 __global__ void __launch_bounds__(AuxLayout<N1, CPC>::NT)
 aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, const OpTab* ops, int nc,
-           double inv_h, PhysConst pc, double* __restrict__ Fv) {
+           double inv_h, PhysConst pc, R* __restrict__ Fv) {
     using L = AuxLayout<N1, CPC>;
     constexpr int NP = L::NP, NF = L::NF, NT = L::NT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -733,7 +735,7 @@ aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, const OpTa
         if (cell >= nc) continue;
         const int cx[3] = {node % N1, (node / N1) % N1, node / (N1 * N1)};
         const R* Fc = sF + c * 12 * NP;
-        double* out = Fv + (size_t)cell * viscous_terms_per_cell<N1>();
+        R* out = Fv + (size_t)cell * viscous_terms_per_cell<N1>();
         R div[4] = {R(0), R(0), R(0), R(0)};
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
@@ -751,11 +753,11 @@ aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, const OpTa
                 const int t1 = (d == 0) ? 1 : 0, t2 = (d == 2) ? 1 : 2;
                 const int fn = cx[t2] * N1 + cx[t1];
 #pragma unroll
-                for (int k = 0; k < 4; ++k) out[4 * NP + (f * 4 + k) * NF + fn] = (double)Fc[(d * 4 + k) * NP + node];
+                for (int k = 0; k < 4; ++k) out[4 * NP + (f * 4 + k) * NF + fn] = Fc[(d * 4 + k) * NP + node];
             }
         }
 #pragma unroll
-        for (int k = 0; k < 4; ++k) out[k * NP + node] = (double)div[k];
+        for (int k = 0; k < 4; ++k) out[k * NP + node] = div[k];
     }
 }
 

@@ -13,7 +13,7 @@ cudaError_t launch_stage(const StageArgs& a, int fp32, bool visc, bool split, cu
 // auxiliary (lifted gradient) equation, emitting the nodal viscous flux
 template <int N1>
 cudaError_t launch_aux(const double* U, const int* nbr, const OpTab* ops, int nc, double inv_h,
-                       const PhysConst& pc, int fp32, double* Fv, cudaStream_t s);
+                       const PhysConst& pc, int fp32, void* Fv, cudaStream_t s);
 // DGBase::apply_inverse_global_mass_matrix on its own
 template <int N1>
 cudaError_t launch_inverse_mass(const double* in, double* out, const OpTab* ops, int nc, double inv_detj,
