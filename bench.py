@@ -465,7 +465,10 @@ def main():
         args.warmup = 3
     prm = Parameters.from_dict(prm_for(args.workload))
     prec = _lib.PH_FP32_RESIDUAL if args.precision == "fp32" else _lib.PH_FP64
-    fs = FlowSolver(prm, precision=prec)
+    # the context runs on its own stream (multi-step calls then replay a captured RK step);
+    # every CUDA event below is recorded on that stream
+    stream = torch.cuda.Stream()
+    fs = FlowSolver(prm, precision=prec, stream=stream.cuda_stream)
     dg = fs.dg
     L, h = dg.L, dg.handle
     dt = fs.adaptive_time_step()
@@ -486,9 +489,9 @@ def main():
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier(); torch.cuda.synchronize()
     with ClockSampler(torch.cuda.current_device()) as clk:
-        ev0.record()
+        ev0.record(stream)
         _lib.check(L.ph_rk_step(h, dt, args.steps))
-        ev1.record()
+        ev1.record(stream)
         torch.cuda.synchronize()
     barrier()
     ms = ev0.elapsed_time(ev1)
@@ -513,12 +516,12 @@ def main():
     _lib.check(L.ph_get_state(h, U_host.data_ptr(), _lib.PH_HOST))
     barrier(); torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
+    e0.record(stream)
     for _ in range(args.steps):
         _lib.check(L.ph_set_state(h, U_host.data_ptr(), _lib.PH_HOST))
         _lib.check(L.ph_rk_step(h, dt, 1))
         _lib.check(L.ph_get_state(h, U_host.data_ptr(), _lib.PH_HOST))
-    e1.record(); torch.cuda.synchronize()
+    e1.record(stream); torch.cuda.synchronize()
     ms_e2e = e0.elapsed_time(e1)
     ms_e2e = reduce_max(ms_e2e, dist, "cuda")
     e2e = world * dg.n_dofs * stages * args.steps / (ms_e2e * 1e-3)

@@ -47,7 +47,7 @@ enum { PH_FP64 = 0, PH_FP32_RESIDUAL = 1 };          /* arithmetic of the residu
  *   flux_reconstruction: 0 cDG, 1 cSD, 2 cHU, 3 cNegative, 4 cNegative2, 5 cPlus,
  *                        6 c10Thousand, 7 cHULumped, 8 user_specified_value
  *   flux_reconstruction_aux: 0 kDG (the GPU path supports kDG)
- *   runge_kutta_method: 0 euler_ex, 1 ssprk3_ex, 2 rk4_ex
+ *   runge_kutta_method: 0 rk4_ex, 1 ssprk3_ex, 2 heun2_ex, 3 euler_ex (4-6 implicit: not on this path)
  *   non_physical_behavior: 0 return_big_number, 1 abort_run, 2 print_warning */
 typedef struct ph_params {
     int poly_degree;

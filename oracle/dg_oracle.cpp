@@ -1221,6 +1221,8 @@ void Solver::rk_step(double* U, double dt) {
         ns = 3; a[1][0] = 1.0; a[2][0] = 0.25; a[2][1] = 0.25;
         b[0] = 1.0 / 6.0; b[1] = 1.0 / 6.0; b[2] = 2.0 / 3.0;
         cc[1] = 1.0; cc[2] = 0.5;
+    } else if (prm.rk_method == HEUN2) {   // HeunExplicit (runge_kutta_methods.cpp:73-92)
+        ns = 2; a[1][0] = 1.0; b[0] = 0.5; b[1] = 0.5; cc[1] = 1.0;
     } else { ns = 1; b[0] = 1.0; }
     const size_t N = ndofs();
     std::vector<double> un(U, U + N), R(N);
@@ -1243,7 +1245,6 @@ void Solver::rk_step(double* U, double dt) {
 
 void Solver::interpolate_ic(double* U, int ic, const double* icp) {
     Physics phys(&prm, &status);
-    const int nd = ops.nd;
     for (int c = 0; c < mesh.nc; ++c)
         for (int i = 0; i < nd3; ++i) {
             const double* X = &mesh.xnode[((size_t)c * nd3 + i) * 3];

@@ -27,7 +27,7 @@ enum Pde { EULER = 0, NAVIER_STOKES = 1 };
 enum TwoPoint { KG = 0, IR = 1, CH = 2, RA = 3 };
 enum ConvFlux { LAX_FRIEDRICHS = 0, ROE = 1, CENTRAL = 2, TWO_POINT = 3, TWO_POINT_LXF = 4, TWO_POINT_ROE = 5 };
 enum DissFlux { SIPG = 0, BR2 = 1, CENTRAL_VISC = 2 };
-enum RkMethod { RK_EULER = 0, SSPRK3 = 1, RK4 = 2 };
+enum RkMethod { RK_EULER = 0, SSPRK3 = 1, RK4 = 2, HEUN2 = 3 };
 enum FrType { C_DG = 0, C_SD = 1, C_HU = 2, C_NEGATIVE = 3, C_NEGATIVE2 = 4, C_PLUS = 5, C_10THOUSAND = 6, C_HU_LUMPED = 7, C_USER = 8 };
 enum FrAuxType { K_DG = 0, K_SD = 1, K_HU = 2, K_NEGATIVE = 3, K_NEGATIVE2 = 4, K_PLUS = 5, K_10THOUSAND = 6 };
 enum CellOrder { ORDER_AUTO = 0, ORDER_LEXICOGRAPHIC = 1, ORDER_MORTON = 2 };

@@ -24,7 +24,7 @@ CONV_FLUX = {"lax_friedrichs": 0, "roe": 1, "central_flux": 2, "two_point_flux":
              "two_point_flux_with_lax_friedrichs_dissipation": 4,
              "two_point_flux_with_roe_dissipation": 5}
 DISS_FLUX = {"symm_internal_penalty": 0, "bassi_rebay_2": 1, "central_visc_flux": 2}
-RK = {"euler_ex": 0, "ssprk3_ex": 1, "rk4_ex": 2}
+RK = {"euler_ex": 0, "ssprk3_ex": 1, "rk4_ex": 2, "heun2_ex": 3}
 FR = {"cDG": 0, "cSD": 1, "cHU": 2, "cNegative": 3, "cNegative2": 4, "cPlus": 5,
       "c10Thousand": 6, "cHULumped": 7, "user_specified_value": 8}
 FR_AUX = {"kDG": 0, "kSD": 1, "kHU": 2, "kNegative": 3, "kNegative2": 4, "kPlus": 5, "k10Thousand": 6}

@@ -337,8 +337,8 @@ int check_batch_params(const ph_batch* b, const ph_mesh_desc* mesh, const ph_par
     if (const char* why = unsupported_reason(mesh, prm)) return fail(PH_ERR_UNSUPPORTED, why);
     if (prm->pde_type != 0 || !prm->use_split_form)
         return fail(PH_ERR_UNSUPPORTED, "a batch takes split-form Euler solves");
-    if (prm->runge_kutta_method != 1 && prm->runge_kutta_method != 2)
-        return fail(PH_ERR_UNSUPPORTED, "a batch takes rk4_ex or ssprk3_ex");
+    if (prm->runge_kutta_method < 0 || prm->runge_kutta_method > 2)
+        return fail(PH_ERR_UNSUPPORTED, "a batch takes rk4_ex, ssprk3_ex or heun2_ex");
     if (prm->two_point_num_flux_type < 0 || prm->two_point_num_flux_type > 3 || prm->conv_num_flux < 0 ||
         prm->conv_num_flux > 5)
         return fail(PH_ERR_INVALID, "parameter out of range");
@@ -671,7 +671,7 @@ int ph_batch_autotune(int poly_degree, int precision, int curvilinear, int* best
     ph_params prm{};
     prm.poly_degree = poly_degree; prm.flux_nodes_type = 1; prm.pde_type = 0; prm.use_split_form = 1;
     prm.two_point_num_flux_type = ph::TP_CH; prm.conv_num_flux = ph::CF_EC_ROE; prm.diss_num_flux = 0;
-    prm.runge_kutta_method = 2; prm.precision = precision; prm.gamma_gas = 1.4; prm.mach_infinity = 0.1;
+    prm.runge_kutta_method = 0; prm.precision = precision; prm.gamma_gas = 1.4; prm.mach_infinity = 0.1;
     prm.reynolds_number_inf = 1600.0; prm.prandtl_number = 0.71; prm.temperature_inf = 273.15;
     prm.sipg_penalty_factor = 1.0; prm.nondimensionalized_constant_viscosity = 1.0;
     size_t bytes = 0;

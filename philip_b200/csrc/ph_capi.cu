@@ -388,13 +388,16 @@ int node_geometry(int n, const std::vector<int>& ijk, const std::vector<double>&
 
 void rk_tableau(int method, int& ns, double A[4][4], double b[4]) {
     for (int i = 0; i < 4; ++i) { b[i] = 0.0; for (int j = 0; j < 4; ++j) A[i][j] = 0.0; }
-    if (method == 2) {
+    if (method == 0) {          // rk4_ex
         ns = 4; A[1][0] = 0.5; A[2][1] = 0.5; A[3][2] = 1.0;
         b[0] = 1.0 / 6.0; b[1] = 1.0 / 3.0; b[2] = 1.0 / 3.0; b[3] = 1.0 / 6.0;
-    } else if (method == 1) {
+    } else if (method == 1) {   // ssprk3_ex
         ns = 3; A[1][0] = 1.0; A[2][0] = 0.25; A[2][1] = 0.25;
         b[0] = 1.0 / 6.0; b[1] = 1.0 / 6.0; b[2] = 2.0 / 3.0;
-    } else {
+    } else if (method == 2) {   // heun2_ex
+        ns = 2; A[1][0] = 1.0;
+        b[0] = 0.5; b[1] = 0.5;
+    } else {                    // euler_ex
         ns = 1; b[0] = 1.0;
     }
 }
@@ -463,6 +466,11 @@ struct ph_ctx {
     long long t_n[3] = {0, 0, 0};
     long long launches = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // one RK step captured as a CUDA graph, replayed by ph_rk_step while dt stays the same
+    // (only on a caller-given stream: the legacy default stream cannot be captured)
+    cudaGraphExec_t step_graph = nullptr;
+    double step_graph_dt = 0.0;
+    int step_graph_launches = 0;
 };
 
 namespace {
@@ -544,7 +552,7 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
     if (mesh->n_cells_per_direction < 1 || !(mesh->right > mesh->left)) return fail(PH_ERR_INVALID, "bad mesh");
     if (prm->pde_type < 0 || prm->pde_type > 1 || prm->two_point_num_flux_type < 0 || prm->two_point_num_flux_type > 3 ||
         prm->conv_num_flux < 0 || prm->conv_num_flux > 5 || prm->diss_num_flux < 0 || prm->diss_num_flux > 2 ||
-        prm->runge_kutta_method < 0 || prm->runge_kutta_method > 2)
+        prm->runge_kutta_method < 0 || prm->runge_kutta_method > 3)
         return fail(PH_ERR_INVALID, "parameter out of range");
     if (const char* why = unsupported_reason(mesh, prm)) return fail(PH_ERR_UNSUPPORTED, why);
     const bool ec = prm->conv_num_flux >= 3;
@@ -627,6 +635,10 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
 
 int ph_ctx_destroy(ph_ctx* c) {
     if (!c) return PH_OK;
+    if (c->step_graph) {
+        if (c->stream) cudaStreamSynchronize(c->stream);
+        cudaGraphExecDestroy(c->step_graph);
+    }
     void* ptrs[] = {c->d_nbr, c->d_ops, c->d_itab, c->d_sol, c->d_stA, c->d_stB, c->d_acc, c->d_carry,
                     c->d_fv, c->d_comp, c->d_tmpA, c->d_tmpB, c->d_partial, c->d_status, c->d_metric, c->d_xnode};
     for (void* p : ptrs) if (p) cudaFree(p);
@@ -738,8 +750,47 @@ static int rk_one_step(ph_ctx* c, double dt) {
     return PH_OK;
 }
 
+// Capture one RK step (all stages, auxiliary kernels included) as a graph for this dt.
+static int capture_step_graph(ph_ctx* c, double dt) {
+    if (c->step_graph) { cudaGraphExecDestroy(c->step_graph); c->step_graph = nullptr; }
+    const long long before = c->launches;
+    cudaGraph_t g = nullptr;
+    PH_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = rk_one_step(c, dt);
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (rc || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        c->launches = before;
+        return rc ? rc : fail(PH_ERR_CUDA, std::string("step capture: ") + cudaGetErrorString(e));
+    }
+    const cudaError_t e2 = cudaGraphInstantiate(&c->step_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e2 != cudaSuccess) { c->step_graph = nullptr; return fail(PH_ERR_CUDA, cudaGetErrorString(e2)); }
+    c->step_graph_launches = (int)(c->launches - before);
+    c->launches = before;
+    c->step_graph_dt = dt;
+    return PH_OK;
+}
+
 int ph_rk_step(ph_ctx* c, double dt, int nsteps) {
     if (!c || nsteps < 0) return fail(PH_ERR_INVALID, "bad argument");
+    // several steps of one dt on a caller-given stream replay a graph of one step; the
+    // per-launch timing mode and one-stage methods (which swap buffers) launch directly
+    const bool graph = c->stream != nullptr && !c->timing && c->ns > 1 && nsteps > 1;
+    if (graph) {
+        int s = 0;
+        if (!c->step_graph || c->step_graph_dt != dt) {
+            // the first step runs directly, so every kernel is configured before the capture
+            if (int rc = rk_one_step(c, dt)) return rc;
+            s = 1;
+            if (int rc = capture_step_graph(c, dt)) return rc;
+        }
+        for (; s < nsteps; ++s) {
+            PH_CUDA(cudaGraphLaunch(c->step_graph, c->stream));
+            c->launches += c->step_graph_launches;
+        }
+        return PH_OK;
+    }
     for (int s = 0; s < nsteps; ++s)
         if (int rc = rk_one_step(c, dt)) return rc;
     return PH_OK;

@@ -252,9 +252,9 @@ class FlowSolver:
     switches updated), the unsteady data table, and the state checkpoint."""
 
     def __init__(self, parameters: Parameters, precision: int = _lib.PH_FP64, cell_order: int = 0,
-                 warp: float = 0.0):
+                 warp: float = 0.0, stream: int | None = None):
         self.parameters = parameters
-        self.dg = DGStrong(parameters, precision=precision, cell_order=cell_order, warp=warp)
+        self.dg = DGStrong(parameters, precision=precision, cell_order=cell_order, warp=warp, stream=stream)
         self.ode_solver = RungeKuttaODESolver(self.dg)
         self.flow_case = parameters.get("flow_solver/flow_case_type")
         X = self.dg.node_coordinates()

@@ -22,7 +22,7 @@ DISS_FLUX = {"symm_internal_penalty": 0, "bassi_rebay_2": 1, "central_visc_flux"
 FR = {"cDG": 0, "cSD": 1, "cHU": 2, "cNegative": 3, "cNegative2": 4, "cPlus": 5, "c10Thousand": 6,
       "cHULumped": 7, "user_specified_value": 8}
 FR_AUX = {"kDG": 0}
-RK = {"euler_ex": 0, "ssprk3_ex": 1, "rk4_ex": 2}
+RK = {"rk4_ex": 0, "ssprk3_ex": 1, "heun2_ex": 2, "euler_ex": 3}   # parameters_ode_solver.h:66-78 order
 NON_PHYSICAL = {"return_big_number": 0, "abort_run": 1, "print_warning": 2}
 
 DEFAULTS = {

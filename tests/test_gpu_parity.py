@@ -69,7 +69,7 @@ def test_inverse_mass_and_rk_step_parity(fr):
     k_gpu = np.empty_like(R)
     dg.apply_inverse_global_mass_matrix(R, k_gpu)
     assert rel_max_err(k_gpu, k_orc) <= RTOL
-    for rk in ("rk4_ex", "ssprk3_ex", "euler_ex"):
+    for rk in ("rk4_ex", "ssprk3_ex", "heun2_ex", "euler_ex"):
         kw2 = dict(kw, rk=rk)
         prm, orc, dg = _pair(kw2)
         U0 = perturbed_tgv(orc, seed=3)
@@ -108,7 +108,7 @@ def test_nonphysical_status_flag():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("rk", ["rk4_ex", "ssprk3_ex"])
+@pytest.mark.parametrize("rk", ["rk4_ex", "ssprk3_ex", "heun2_ex"])
 @pytest.mark.parametrize("visc", [False, True])
 def test_multistep_parity_and_clean_status(rk, visc):
     """Several steps at the TGV time step: the state follows the oracle and no
@@ -129,3 +129,26 @@ def test_multistep_parity_and_clean_status(rk, visc):
         print(f"{rk} visc={visc} step {step}: rel err {err:.3e} status {st}")
         assert st == 0
         assert err <= 1e-12
+
+
+@pytest.mark.gpu
+def test_graph_replayed_steps_match_direct_steps():
+    """ph_rk_step on a caller-given stream replays one captured RK step; the result is bitwise
+    the directly launched steps'."""
+    import torch
+    kw = dict(poly_degree=3, n_cells=4, pde="navier_stokes", diss="bassi_rebay_2")
+    prm = Parameters.from_dict(prm_dict(**kw))
+    orc = Oracle(prm.oracle_cfg(), prm.n_cells, *prm.grid_bounds)
+    U0 = orc.initial_condition("tgv")
+    dt = 0.1 * 6.28318530717958623200 / 16 / 11.0
+    direct = DGStrong(prm)                       # legacy default stream: direct launches
+    direct.solution = U0
+    RungeKuttaODESolver(direct).step_in_time(dt, nsteps=5)
+    s = torch.cuda.Stream()
+    graphed = DGStrong(prm, stream=s.cuda_stream)
+    graphed.solution = U0
+    RungeKuttaODESolver(graphed).step_in_time(dt, nsteps=5)
+    RungeKuttaODESolver(graphed).step_in_time(dt, nsteps=3)    # replays the cached graph
+    RungeKuttaODESolver(direct).step_in_time(dt, nsteps=3)
+    s.synchronize()
+    assert np.array_equal(graphed.solution, direct.solution)
