@@ -47,7 +47,9 @@ enum { PH_FP64 = 0, PH_FP32_RESIDUAL = 1 };          /* arithmetic of the residu
  *   flux_reconstruction: 0 cDG, 1 cSD, 2 cHU, 3 cNegative, 4 cNegative2, 5 cPlus,
  *                        6 c10Thousand, 7 cHULumped, 8 user_specified_value
  *   flux_reconstruction_aux: 0 kDG (the GPU path supports kDG)
- *   runge_kutta_method: 0 rk4_ex, 1 ssprk3_ex, 2 heun2_ex, 3 euler_ex (4-6 implicit: not on this path)
+ *   runge_kutta_method: 0 rk4_ex, 1 ssprk3_ex, 2 heun2_ex, 3 euler_ex (4-6 implicit: not on this path),
+ *                       7 RK4_3_5_3SStar, 8 RK3_2_5F_3SStarPlus, 9 RK4_3_9F_3SStarPlus,
+ *                       10 RK5_4_10F_3SStarPlus (low-storage, with an embedded error estimate)
  *   non_physical_behavior: 0 return_big_number, 1 abort_run, 2 print_warning */
 typedef struct ph_params {
     int poly_degree;
@@ -72,6 +74,8 @@ typedef struct ph_params {
     double temperature_inf;
     double nondimensionalized_constant_viscosity;
     double sipg_penalty_factor;
+    double rk_atol;                       /* low-storage RK error estimate: absolute and relative */
+    double rk_rtol;                       /* tolerances (ODE solver atol / rtol) */
 } ph_params;
 
 /* Periodic cube [left,right]^3 with n^3 cells (PeriodicCubeFlow::generate_grid,
@@ -130,6 +134,13 @@ int ph_apply_inverse_mass(ph_ctx* ctx, const double* R, double* out, int where);
  * (src/ode_solver/ode_solver_base.h:70, runge_kutta_base.cpp:21-39), nsteps times
  * with the same dt, on the context's state. Asynchronous on the context stream. */
 int ph_rk_step(ph_ctx* ctx, double dt, int nsteps);
+
+/* Weighted RMS error estimate of the last low-storage RK step,
+ * sqrt(mean(((S1 - S_embedded) / (atol + rtol max(|S1|, |S_embedded|)))^2)) over all DOFs
+ * (LowStorageRungeKuttaODESolver::get_automatic_error_adaptive_step_size,
+ * src/ode_solver/low_storage_runge_kutta_ode_solver.cpp:80-110, before the step-size
+ * controller). Synchronises the context stream. */
+int ph_rk_error_norm(ph_ctx* ctx, double* w);
 
 /* PeriodicTurbulence::compute_and_update_integrated_quantities subset
  * (src/flow_solver/flow_solver_cases/periodic_turbulence.cpp:439-672):

@@ -27,7 +27,8 @@ enum Pde { EULER = 0, NAVIER_STOKES = 1 };
 enum TwoPoint { KG = 0, IR = 1, CH = 2, RA = 3 };
 enum ConvFlux { LAX_FRIEDRICHS = 0, ROE = 1, CENTRAL = 2, TWO_POINT = 3, TWO_POINT_LXF = 4, TWO_POINT_ROE = 5 };
 enum DissFlux { SIPG = 0, BR2 = 1, CENTRAL_VISC = 2 };
-enum RkMethod { RK_EULER = 0, SSPRK3 = 1, RK4 = 2, HEUN2 = 3 };
+enum RkMethod { RK_EULER = 0, SSPRK3 = 1, RK4 = 2, HEUN2 = 3,
+                LS_RK4_3_5 = 4, LS_RK3_2_5F = 5, LS_RK4_3_9F = 6, LS_RK5_4_10F = 7 };
 enum FrType { C_DG = 0, C_SD = 1, C_HU = 2, C_NEGATIVE = 3, C_NEGATIVE2 = 4, C_PLUS = 5, C_10THOUSAND = 6, C_HU_LUMPED = 7, C_USER = 8 };
 enum FrAuxType { K_DG = 0, K_SD = 1, K_HU = 2, K_NEGATIVE = 3, K_NEGATIVE2 = 4, K_PLUS = 5, K_10THOUSAND = 6 };
 enum CellOrder { ORDER_AUTO = 0, ORDER_LEXICOGRAPHIC = 1, ORDER_MORTON = 2 };
@@ -56,6 +57,7 @@ struct Params {
     double constant_viscosity = 1.0;
     double sipg_penalty_factor = 1.0;
     int non_physical = RETURN_BIG_NUMBER;
+    double atol = 1e-3, rtol = 1e-3;   // low-storage error estimate
 };
 
 // One-dimensional operators on the reference interval [0,1]
@@ -112,6 +114,7 @@ struct Solver {
     int nd3 = 0, nq3 = 0, ndofs_cell = 0;
     std::vector<double> aux;     // 3 * ndofs (auxiliary gradient, dof-major per dimension)
     int status = 0;              // bit 0: non-physical state met
+    double last_error = 0.0;     // weighted RMS error estimate of the last low-storage step
     double current_time = 0.0;
     int nthreads = 0;
 
@@ -124,6 +127,8 @@ struct Solver {
     void apply_inverse_mass(const double* in, double* out, bool aux_eq = false);
     // one explicit Butcher RK step (runge_kutta_base.cpp:21-39)
     void rk_step(double* U, double dt);
+    // one low-storage 3S* / 3S*+ step, leaving its error estimate in last_error
+    void lsrk_step(double* U, double dt);
     // nodal interpolation of an initial condition (set_initial_condition.cpp:51)
     void interpolate_ic(double* U, int ic, const double* ic_params);
     // TGV integrated quantities (periodic_turbulence.cpp:439-672):

@@ -24,7 +24,8 @@ CONV_FLUX = {"lax_friedrichs": 0, "roe": 1, "central_flux": 2, "two_point_flux":
              "two_point_flux_with_lax_friedrichs_dissipation": 4,
              "two_point_flux_with_roe_dissipation": 5}
 DISS_FLUX = {"symm_internal_penalty": 0, "bassi_rebay_2": 1, "central_visc_flux": 2}
-RK = {"euler_ex": 0, "ssprk3_ex": 1, "rk4_ex": 2, "heun2_ex": 3}
+RK = {"euler_ex": 0, "ssprk3_ex": 1, "rk4_ex": 2, "heun2_ex": 3, "RK4_3_5_3SStar": 4, "RK3_2_5F_3SStarPlus": 5,
+      "RK4_3_9F_3SStarPlus": 6, "RK5_4_10F_3SStarPlus": 7}
 FR = {"cDG": 0, "cSD": 1, "cHU": 2, "cNegative": 3, "cNegative2": 4, "cPlus": 5,
       "c10Thousand": 6, "cHULumped": 7, "user_specified_value": 8}
 FR_AUX = {"kDG": 0, "kSD": 1, "kHU": 2, "kNegative": 3, "kNegative2": 4, "kPlus": 5, "k10Thousand": 6}
@@ -38,7 +39,7 @@ class OrcParams(ctypes.Structure):
         "conv_flux", "diss_flux", "fr_type", "fr_aux_type", "rk_method", "use_constant_viscosity",
         "non_physical", "pad0")] + [(n, ctypes.c_double) for n in (
         "fr_user_value", "gamma", "mach_inf", "reynolds_inf", "prandtl", "temperature_inf",
-        "constant_viscosity", "sipg_penalty_factor")]
+        "constant_viscosity", "sipg_penalty_factor", "atol", "rtol")]
 
 
 _lib = None
@@ -73,6 +74,7 @@ def lib():
         L.orc_inverse_mass.argtypes = [vp, dp, dp]
         L.orc_rk_step.argtypes = [vp, dp, ctypes.c_double]
         L.orc_integrals.argtypes = [vp, dp, dp]
+        L.orc_rk_error.argtypes = [vp]; L.orc_rk_error.restype = ctypes.c_double
         _lib = L
     return _lib
 
@@ -107,6 +109,8 @@ def make_params(cfg: dict) -> OrcParams:
         sipg = 0.0   # all_parameters.cpp:611-614
     p.sipg_penalty_factor = sipg
     p.non_physical = {"return_big_number": 0, "abort_run": 1, "print_warning": 2}[cfg.get("non_physical_behavior", "return_big_number")]
+    p.atol = cfg.get("atol", 1e-3)
+    p.rtol = cfg.get("rtol", 1e-3)
     return p
 
 
@@ -185,6 +189,10 @@ class Oracle:
 
     def rk_step(self, U, dt):
         lib().orc_rk_step(self.h, _dp(U), dt)
+
+    def rk_error(self) -> float:
+        """Weighted RMS error estimate of the last low-storage step."""
+        return float(lib().orc_rk_error(self.h))
 
     def integrals(self, U):
         out = np.zeros(4)

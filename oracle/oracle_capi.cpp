@@ -19,7 +19,7 @@ struct orc_params {
     int poly_degree, overintegration, flux_nodes, pde, use_split_form, two_point, conv_flux, diss_flux;
     int fr_type, fr_aux_type, rk_method, use_constant_viscosity, non_physical, pad0;
     double fr_user_value, gamma, mach_inf, reynolds_inf, prandtl, temperature_inf, constant_viscosity,
-        sipg_penalty_factor;
+        sipg_penalty_factor, atol, rtol;
 };
 
 static Params to_params(const orc_params* p) {
@@ -32,6 +32,7 @@ static Params to_params(const orc_params* p) {
     q.temperature_inf = p->temperature_inf; q.use_constant_viscosity = p->use_constant_viscosity;
     q.constant_viscosity = p->constant_viscosity; q.sipg_penalty_factor = p->sipg_penalty_factor;
     q.non_physical = p->non_physical;
+    q.atol = p->atol; q.rtol = p->rtol;
     return q;
 }
 
@@ -59,6 +60,8 @@ int orc_create_curved(const orc_params* p, int n, double left, double right, int
         return 1;
     }
 }
+// weighted RMS error estimate of the last low-storage step
+double orc_rk_error(void* h) { return static_cast<Solver*>(h)->last_error; }
 void orc_destroy(void* h) { delete static_cast<Solver*>(h); }
 long long orc_ndofs(void* h) { return (long long)static_cast<Solver*>(h)->ndofs(); }
 int orc_nd(void* h) { return static_cast<Solver*>(h)->ops.nd; }

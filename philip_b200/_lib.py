@@ -22,7 +22,7 @@ EXPORTED = ["ph_ctx_create", "ph_ctx_destroy", "ph_ndofs", "ph_cell_ijk", "ph_se
             "ph_batch_create", "ph_batch_destroy", "ph_batch_bytes", "ph_batch_admit", "ph_batch_step",
             "ph_batch_progress", "ph_batch_active", "ph_batch_get_state", "ph_batch_status", "ph_batch_release",
             "ph_batch_poll", "ph_batch_fence", "ph_batch_fence_wait", "ph_batch_autotune", "ph_batch_set_variant",
-            "ph_batch_launches", "ph_mesh_node_xyz", "ph_last_error"]
+            "ph_batch_launches", "ph_mesh_node_xyz", "ph_rk_error_norm", "ph_last_error"]
 
 
 class PhParams(ctypes.Structure):
@@ -32,7 +32,8 @@ class PhParams(ctypes.Structure):
         "flux_reconstruction_aux", "runge_kutta_method", "use_constant_viscosity", "non_physical_behavior",
         "precision")] + [(n, ctypes.c_double) for n in (
         "FR_user_specified_correction_parameter_value", "gamma_gas", "mach_infinity", "reynolds_number_inf",
-        "prandtl_number", "temperature_inf", "nondimensionalized_constant_viscosity", "sipg_penalty_factor")]
+        "prandtl_number", "temperature_inf", "nondimensionalized_constant_viscosity", "sipg_penalty_factor",
+        "rk_atol", "rk_rtol")]
 
 
 class PhMeshDesc(ctypes.Structure):
@@ -97,6 +98,7 @@ def load(build_if_missing: bool = False):
     L.ph_batch_set_variant.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.ph_batch_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.ph_mesh_node_xyz.argtypes = [ctypes.POINTER(PhMeshDesc), ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    L.ph_rk_error_norm.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     L.ph_node_xyz.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     L.ph_residual_noalloc.argtypes = [ctypes.POINTER(PhMeshDesc), ctypes.POINTER(PhParams), vp, vp, vp]
     L.ph_last_error.restype = ctypes.c_char_p

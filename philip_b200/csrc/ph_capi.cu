@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
+#include <initializer_list>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -431,6 +433,147 @@ void rk_stage_args(ph::StageArgs& a, const RkBuffers& B, int i, int ns, const do
     }
 }
 
+// Low-storage tableaux: published coefficients (restated from
+// src/ode_solver/runge_kutta_methods/low_storage_runge_kutta_methods.cpp).
+bool low_storage_tableau(int method, LowStorageTableau& t) {
+    t = LowStorageTableau();
+    auto set = [&](int ns, int nd, int order, bool plus, std::initializer_list<std::array<double, 3>> g,
+                   std::initializer_list<double> b, std::initializer_list<double> d, std::initializer_list<double> bh) {
+        t.ns = ns; t.num_delta = nd; t.order = order; t.plus = plus;
+        int i = 0;
+        for (const auto& row : g) { t.gamma[i][0] = row[0]; t.gamma[i][1] = row[1]; t.gamma[i][2] = row[2]; ++i; }
+        i = 0; for (double v : b) t.beta[i++] = v;
+        i = 0; for (double v : d) t.delta[i++] = v;
+        i = 0; for (double v : bh) t.bhat[i++] = v;
+    };
+    switch (method) {
+    case 7:   // RK4(3)5[3S*]
+        set(5, 7, 4, false,
+            {{0.0, 0.0, 0.0}, {0.0, 1.0, 0.0}, {-0.497531095840104, 1.384996869124138, 0.0},
+             {1.010070514199942, 3.878155713328178, 0.0}, {-3.196559004608766, -2.324512951813145, 1.642598936063715},
+             {1.717835630267259, -0.514633322274467, 0.188295940828347}},
+            {0.0, 0.075152045700771, 0.211361016946069, 1.100713347634329, 0.728537814675568, 0.393172889823198},
+            {1.0, 0.081252332929194, -1.083849060586449, -1.096110881845602, 2.859440022030827, -0.655568367959557,
+             -0.194421504490852},
+            {0.0, 0.0, 0.0, 0.0, 0.0, 0.0});
+        return true;
+    case 8:   // RK3(2)5F[3S*+]
+        set(5, 5, 3, true,
+            {{0.0, 0.0, 0.0}, {0.0, 1.0, 0.0},
+             {0.2587771979725733308135192812685323706, 0.5528354909301389892439698870483746541, 0.0},
+             {-0.1324380360140723382965420909764953437, 0.6731871608203061824849561782794643600, 0.0},
+             {0.05056033948190826045833606441415585735, 0.2803103963297672407841316576323901761,
+              0.2752563273304676380891217287572780582},
+             {0.5670532000739313812633197158607642990, 0.5521525447020610386070346724931300367,
+              -0.8950526174674033822276061734289327568}},
+            {0.0, 0.2300298624518076223899418286314123354, 0.3021434166948288809034402119555380003,
+             0.8025606185416310937583009085873554681, 0.4362158943603440930655148245148766471, 0.11292725304550591},
+            {1.0, 0.34076558793345252, 0.34143826550033862, 0.72292753667879872, 0.0},
+            {0.094841667050357029, 0.17263713394303537, 0.39982431890843712, 0.17180168075801786,
+             0.058819144221557401, 0.1020760551185952388626787099944507877});
+        return true;
+    case 9:   // RK4(3)9F[3S*+]
+        set(9, 9, 4, true,
+            {{0.0, 0.0, 0.0}, {0.0, 1.0, 0.0},
+             {-4.655641447335068552684422206224169103, 2.499262792574495009336242992898153462, 0.0},
+             {-0.7720265099645871829248487209517314217, 0.5866820377718875577451517985847920081, 0.0},
+             {-4.024436690519806086742256154738379161, 1.205146086523094569925592464380295241,
+              0.7621006678721315291614677352949377871},
+             {-0.02129676284018530966221583708648634733, 0.3474793722186732780030762737753849272,
+              -0.1981182504339400567765766904309673119},
+             {-2.435022509790109546199372365866450709, 1.321346060965113109321230804210670518,
+              -0.6228959218699007450469629366684127462},
+             {0.01985627297131987000579523283542615256, 0.3119636464694193615946633676950358444,
+              -0.3752248380775956442989480369774937099},
+             {-0.2810791146791038566946663374735713961, 0.4351419539684379261368971206040518552,
+              -0.3355438309135169811915662336248989661},
+             {0.1689434168754859644351230590422137972, 0.2359698130028753572503744518147537768,
+              -0.04560955005031121479972862973705108039}},
+            {0.0, 0.2836343005184365275160654678626695428, 0.9736500104654741223716056170419660217,
+             0.3382359225242515288768487569778320563, -0.3584943611106183357043212309791897386,
+             -0.004113944068471528211627210454497620358, 1.427968894048586363415504654313371031,
+             0.01808470948394314017665968411915568633, 0.1605770645946802213926893453819236685,
+             0.2952227015964591648775833803635147962},
+            {1.0, 1.262923876648114432874834923838556100, 0.7574967189685911558308119415539596711,
+             0.5163589453140728104667573195005629833, -0.02746327421802609557034437892013640319,
+             -0.4382673178127944142238606608356542890, 1.273587294602656522645691372699677063,
+             -0.6294740283927400326554066998751383342, 0.0},
+            {0.02483675912451591196775756814283216443, 0.1866327774562103796990092260942180726,
+             0.05671080795936984495604436622517631183, -0.003447695439149287702616943808570747099,
+             0.003602245056516636472203469198006404016, 0.4545570622145088936800484247980581766,
+             -0.0002434665289427612407531544765622888855, 0.06642755361103549971517945063138312147,
+             0.1613697079523505006226025497715177578, 0.04955424859358438183052504342394102722});
+        return true;
+    case 10:  // RK5(4)10F[3S*+]
+        set(10, 10, 5, true,
+            {{0.0, 0.0, 0.0}, {0.0, 1.0, 0.0},
+             {0.4043660121685749695640462197806189975, 0.6871467028161416909922221357014564412, 0.0},
+             {-0.8503427289575839690883191973980814832, 1.093024748914750833700799552463885117, 0.0},
+             {-6.950894175262117526410215315179482885, 3.225975379607193001678365742708874597,
+              -2.393405133244194727221124311276648940},
+             {0.9238765192731084931855438934978371889, 1.041153702510101386914019859778740444,
+              -1.902854422421760920850597670305403139},
+             {-2.563178056509891340215942413817786020, 1.292821487912164945157744726076279306,
+              -2.820042207399977261483046412236557428},
+             {0.2545744879365226143946122067064118430, 0.7391462755788122847651304143259254381,
+              -1.832698465277380999601896111079977378},
+             {0.3125831707411998258746812355492206137, 0.1239129251371800313941948224441873274,
+              -0.2199094483084671192328083958346519535},
+             {-0.7007114414440507927791249989236719346, 0.1842753472370123193132193302369345580,
+              -0.4082430635847870963724591602173546218},
+             {0.4839621016023833375810172323297465039, 0.05712788998796583446479387686662738843,
+              -0.1377669797880289713535665985132703979}},
+            {0.0, 0.2597883554788674084039539165398464630, 0.01777008889438867858759149597539211023,
+             0.2481636629715501931294746189266601496, 0.7941736871152005775821844297293296135,
+             0.3885391285642019129575902994397298066, 0.1455051657916305055730603387469193768,
+             0.1587517385964749337690916959584348979, 0.1650605617880053419242434594242509601,
+             0.2118093284937153836908655490906875007, 0.1559392342362059886106995325687547506},
+            {1.0, -0.1331778419508803397033287009506932673, 0.8260422814750207498262063505871077303,
+             1.513700425755728332485300719652378197, -1.305810059935023735972298885749903694,
+             3.036678802924163246003321318996156380, -1.449458274398895177922690618003584514,
+             3.834313899176362315089976408899373409, 4.122293760012985409330881631526514714, 0.0},
+            {-0.02019255440012066080909442770590267512, 0.02737903480959184339932730854141598275,
+             0.3028818636145965534365173822296811090, -0.03656843880622222190071445247906780540,
+             0.3982664774676767729863101188528827405, -0.05715959421140685436681459970502471634,
+             0.09849855103848558320961101178888983150, 0.06654601552456084978615342374581437947,
+             0.09073479542748112726465375642050504556, 0.08432289325330803924891866923939606351,
+             0.04529095628204896774513180907141004447});
+        return true;
+    }
+    return false;
+}
+
+const double* lsrk_stage_args(ph::StageArgs& a, const RkBuffers& B, int i, const LowStorageTableau& t, double dt,
+                              double atol, double rtol, double* err_partial) {
+    const int ns = t.ns;
+    a.mode = 3;
+    a.dt = dt;
+    a.atol = atol; a.rtol = rtol;
+    a.ls_s2 = B.acc; a.ls_s3 = B.sol; a.ls_s4 = t.plus ? B.carry : nullptr;
+    if (i == ns) {   // 3S*+: the first-same-as-last evaluation at u_{n+1} feeds the error register only
+        a.ls_s1_out = nullptr;
+        a.ls_bhat = t.bhat[ns];
+        a.err_partial = err_partial;
+        return B.sol;
+    }
+    const double* in = (i == 0) ? B.sol : ((i - 1) % 2 == 0 ? B.stA : B.stB);
+    a.ls_s1_out = (i == ns - 1) ? B.sol : (i % 2 == 0 ? B.stA : B.stB);
+    a.ls_g0 = t.gamma[i + 1][0]; a.ls_g1 = t.gamma[i + 1][1]; a.ls_g2 = t.gamma[i + 1][2];
+    a.ls_beta = t.beta[i + 1];
+    a.ls_delta = t.delta[i];
+    a.ls_bhat = t.bhat[i];
+    a.ls_first = (i == 0);
+    if (!t.plus && i == ns - 1) {
+        double sum = 0.0;
+        for (int j = 0; j < t.num_delta; ++j) sum += t.delta[j];
+        a.ls_embedded = 1;
+        a.ls_delta_s = t.delta[ns]; a.ls_delta_s1 = t.delta[ns + 1];
+        a.ls_inv_sum_delta = 1.0 / sum;
+        a.err_partial = err_partial;
+    }
+    return in;
+}
+
 } // namespace ph_host
 
 using namespace ph_host;
@@ -459,6 +602,10 @@ struct ph_ctx {
     double pen = 0.0;
     int ns = 0;
     double A[4][4] = {{0}}, b[4] = {0};
+    bool lowstorage = false;            // 3S* / 3S*+ low-storage method
+    LowStorageTableau ls;
+    double* d_err = nullptr;            // per-tile squared scaled errors of the last low-storage step
+    int err_tiles = 0;
     std::vector<double> h_partial;
     // optional per-kernel timing (CUDA events on the context stream)
     bool timing = false;
@@ -552,7 +699,8 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
     if (mesh->n_cells_per_direction < 1 || !(mesh->right > mesh->left)) return fail(PH_ERR_INVALID, "bad mesh");
     if (prm->pde_type < 0 || prm->pde_type > 1 || prm->two_point_num_flux_type < 0 || prm->two_point_num_flux_type > 3 ||
         prm->conv_num_flux < 0 || prm->conv_num_flux > 5 || prm->diss_num_flux < 0 || prm->diss_num_flux > 2 ||
-        prm->runge_kutta_method < 0 || prm->runge_kutta_method > 3)
+        prm->runge_kutta_method < 0 || prm->runge_kutta_method > 10 ||
+        (prm->runge_kutta_method >= 4 && prm->runge_kutta_method <= 6))
         return fail(PH_ERR_INVALID, "parameter out of range");
     if (const char* why = unsupported_reason(mesh, prm)) return fail(PH_ERR_UNSUPPORTED, why);
     const bool ec = prm->conv_num_flux >= 3;
@@ -582,7 +730,12 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
     ph::IntegralTab itab;
     build_integral_table(x, c->p, itab);
     c->pc = physics_constants(prm, c->h, c->pen);
-    rk_tableau(prm->runge_kutta_method, c->ns, c->A, c->b);
+    if (low_storage_tableau(prm->runge_kutta_method, c->ls)) {
+        c->lowstorage = true;
+        c->ns = c->ls.ns;
+    } else {
+        rk_tableau(prm->runge_kutta_method, c->ns, c->A, c->b);
+    }
     std::vector<int> nbr;
     periodic_connectivity(c->n, mesh->cell_order, c->ijk, nbr);
     std::vector<double> metric;
@@ -599,7 +752,8 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
     bad |= dalloc(&c->d_stA, N);
     bad |= dalloc(&c->d_stB, N);
     bad |= dalloc(&c->d_acc, N);
-    if (c->ns == 3) bad |= dalloc(&c->d_carry, N);
+    if (c->ns == 3 || (c->lowstorage && c->ls.plus)) bad |= dalloc(&c->d_carry, N);   // SSPRK3 carry / 3S*+ S4
+    if (c->lowstorage) bad |= dalloc(&c->d_err, (size_t)c->nc);
     if (c->visc) {   // viscous terms, stored in the arithmetic type (floats in the precision form)
         const size_t vt = (size_t)c->nc * (4 * c->NP + 24 * c->N1 * c->N1);
         bad |= dalloc(&c->d_fv, c->fp32 ? (vt + 1) / 2 : vt);
@@ -640,7 +794,7 @@ int ph_ctx_destroy(ph_ctx* c) {
         cudaGraphExecDestroy(c->step_graph);
     }
     void* ptrs[] = {c->d_nbr, c->d_ops, c->d_itab, c->d_sol, c->d_stA, c->d_stB, c->d_acc, c->d_carry,
-                    c->d_fv, c->d_comp, c->d_tmpA, c->d_tmpB, c->d_partial, c->d_status, c->d_metric, c->d_xnode};
+                    c->d_fv, c->d_comp, c->d_tmpA, c->d_tmpB, c->d_partial, c->d_status, c->d_metric, c->d_xnode, c->d_err};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -739,6 +893,17 @@ int ph_apply_inverse_mass(ph_ctx* c, const double* R, double* out, int where) {
 static int rk_one_step(ph_ctx* c, double dt) {
     const int ns = c->ns;
     const RkBuffers B{c->d_sol, c->d_stA, c->d_stB, c->d_acc, c->d_carry, c->d_comp};
+    if (c->lowstorage) {   // LowStorageRungeKuttaODESolver: ns stages (+ the FSAL evaluation of 3S*+)
+        const int last = c->ls.plus ? ns : ns - 1;
+        for (int i = 0; i <= last; ++i) {
+            ph::StageArgs a = base_args(c, nullptr);
+            const double* in = lsrk_stage_args(a, B, i, c->ls, dt, c->prm.rk_atol, c->prm.rk_rtol, c->d_err);
+            a.U = in;
+            if (c->visc) if (int rc = dispatch_aux(c, in)) return rc;
+            if (int rc = dispatch_stage(c, a)) return rc;
+        }
+        return PH_OK;
+    }
     for (int i = 0; i < ns; ++i) {
         const double* in = rk_stage_input(B, i);
         if (c->visc) if (int rc = dispatch_aux(c, in)) return rc;
@@ -825,6 +990,29 @@ int ph_integrals(ph_ctx* c, double out[4]) {
     // periodic_turbulence.cpp:717-725)
     out[2] = c->visc ? 2.0 * out[1] / c->prm.reynolds_number_inf : 0.0;
     out[3] = wave;
+    return PH_OK;
+}
+
+int ph_rk_error_norm(ph_ctx* c, double* w) {
+    if (!c || !w) return fail(PH_ERR_INVALID, "null argument");
+    if (!c->lowstorage) return fail(PH_ERR_INVALID, "the error estimate belongs to the low-storage methods");
+    int threads = 0, cpc = 1;
+    size_t smem = 0;
+    switch (c->N1) {
+    case 2: ph::stage_launch_shape<2>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
+    case 3: ph::stage_launch_shape<3>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
+    case 4: ph::stage_launch_shape<4>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
+    case 5: ph::stage_launch_shape<5>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
+    case 6: ph::stage_launch_shape<6>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
+    default: ph::stage_launch_shape<7>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
+    }
+    const int tiles = (c->nc + cpc - 1) / cpc;
+    std::vector<double> part(tiles);
+    PH_CUDA(cudaMemcpyAsync(part.data(), c->d_err, tiles * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    PH_CUDA(cudaStreamSynchronize(c->stream));
+    double sum = 0.0;
+    for (double v : part) sum += v;   // tile order: deterministic
+    *w = std::sqrt(sum / (double)c->ndofs);
     return PH_OK;
 }
 

@@ -46,6 +46,21 @@ inline bool is_curvilinear(const ph_mesh_desc* mesh) {
 // Butcher tableau of the explicit RK method (runge_kutta_methods.cpp:7-47).
 void rk_tableau(int method, int& ns, double A[4][4], double b[4]);
 
+// Low-storage 3S* / 3S*+ tableau (low_storage_runge_kutta_methods.cpp; Ketcheson 2010 for
+// RK4(3)5[3S*], Ranocha, Dalcin, Parsani and Ketcheson 2021 for the [3S*+] methods).
+struct LowStorageTableau {
+    int ns = 0;                 // stages
+    int num_delta = 0;          // delta entries summed for the embedded solution (3S*)
+    int order = 0;
+    bool plus = false;          // 3S*+: FSAL error register S4
+    double gamma[11][3] = {};
+    double beta[11] = {};
+    double delta[11] = {};
+    double bhat[11] = {};
+};
+// false when `method` is not a low-storage method (parameters_ode_solver.h:66-78 numbering)
+bool low_storage_tableau(int method, LowStorageTableau& t);
+
 // Device vectors of one explicit RK integration of one discretisation.
 struct RkBuffers {
     double* sol;     // u_n, and u_{n+1} after the last stage
@@ -60,5 +75,9 @@ struct RkBuffers {
 const double* rk_stage_input(const RkBuffers& B, int i);
 void rk_stage_args(ph::StageArgs& a, const RkBuffers& B, int i, int ns, const double A[4][4], const double b[4],
                    double dt, bool fp32);
+// Stage i of a low-storage step (i == ns: the 3S*+ FSAL evaluation). S2 lives in B.acc,
+// S4 in B.carry, S3 = u_n = B.sol. Returns the stage input.
+const double* lsrk_stage_args(ph::StageArgs& a, const RkBuffers& B, int i, const LowStorageTableau& t, double dt,
+                              double atol, double rtol, double* err_partial);
 
 } // namespace ph_host

@@ -84,6 +84,18 @@ struct StageArgs {
     // curvilinear cells: [nc][10][NP], rows k*3+d = metric cofactor C[k][d] at the
     // volume nodes, row 9 = 1 / det J (nullptr on affine meshes)
     const double* metric;
+    // low-storage 3S* / 3S*+ stage (mode 3): S1 = the stage input U, S2 and S4 updated in
+    // place, S3 = u_n, S1 of the next stage written to ls_s1_out
+    double* ls_s2;
+    const double* ls_s3;
+    double* ls_s4;              // 3S*+ error register (nullptr for 3S*)
+    double* ls_s1_out;          // nullptr on the FSAL evaluation
+    double ls_g0, ls_g1, ls_g2, ls_beta, ls_delta, ls_bhat;
+    int ls_first;               // stage 0: S2 starts at 0, S4 at u_n
+    int ls_embedded;            // last 3S* stage: S2 = (S2 + d_s S1 + d_s1 S3) / sum(delta)
+    double ls_delta_s, ls_delta_s1, ls_inv_sum_delta;
+    double* err_partial;        // per-tile sums of the squared scaled error (or nullptr)
+    double atol, rtol;
 };
 
 // Viscous terms per cell written by the auxiliary kernel and read by the stage kernel:
@@ -568,6 +580,7 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
         }
     }
     __syncthreads();
+    double err2 = 0.0;   // low-storage error estimate: this thread's share of the tile
     for (int it = tid; it < CPC * 5 * NP; it += NT) {
         const int c = it / (5 * NP);
         const int rem = it % (5 * NP);
@@ -585,6 +598,37 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
         // affine: M^-1 R = G / h; curvilinear (cDG): R / (W det J) = G / det J
         const double k = CURV ? G * __ldg(&a.metric[((size_t)cell * 10 + 9) * NP + node]) : G * a.inv_h;
         if (a.mode == 1) { a.out[dof] = k; continue; }
+        if (a.mode == 3) {
+            // LowStorageRungeKuttaODESolver stage (low_storage_runge_kutta_ode_solver.cpp:22-100):
+            // S2 += delta_i S1; S1 = g0 S1 + g1 S2 + g2 S3 + beta dt k; S4 += bhat_i dt k
+            const double s1 = a.U[dof];
+            const double s3 = a.ls_s3[dof];
+            const double kdt = a.dt * k;
+            double e = 0.0, ref = 0.0;
+            bool have_err = false;
+            if (a.ls_s1_out) {
+                const double s2 = (a.ls_first ? 0.0 : a.ls_s2[dof]) + a.ls_delta * s1;
+                const double s1n = ((a.ls_g0 * s1 + a.ls_g1 * s2) + a.ls_g2 * s3) + a.ls_beta * kdt;
+                a.ls_s1_out[dof] = s1n;
+                if (a.ls_embedded) {   // embedded solution of the last 3S* stage
+                    const double s2e = ((s2 + a.ls_delta_s * s1n) + a.ls_delta_s1 * s3) * a.ls_inv_sum_delta;
+                    a.ls_s2[dof] = s2e;
+                    e = s1n - s2e; ref = fmax(fabs(s1n), fabs(s2e)); have_err = true;
+                } else {
+                    a.ls_s2[dof] = s2;
+                }
+            }
+            if (a.ls_s4) {
+                const double s4 = (a.ls_first ? s3 : a.ls_s4[dof]) + a.ls_bhat * kdt;
+                a.ls_s4[dof] = s4;
+                if (!a.ls_s1_out) { e = s1 - s4; ref = fmax(fabs(s1), fabs(s4)); have_err = true; }
+            }
+            if (have_err && a.err_partial) {
+                const double r = e / (a.atol + a.rtol * ref);
+                err2 += r * r;
+            }
+            continue;
+        }
         const double un = a.Un[dof];
         const double base = a.acc_in ? a.acc_in[dof] : (a.inc_mode ? 0.0 : un);
         const double sum = base + a.c_acc * k;
@@ -604,6 +648,18 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
             a.next[dof] = (cin + a.a_next * k) * a.dt + un;
         }
         if (a.carry_out) a.carry_out[dof] = a.a_carry * k;
+    }
+    if (a.mode == 3 && a.err_partial) {   // tile sum of the squared scaled error, fixed order
+        __shared__ double red[32];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) err2 += __shfl_down_sync(0xffffffffu, err2, o);
+        if ((tid & 31) == 0) red[tid >> 5] = err2;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int w = 0; w < (NT + 31) / 32; ++w) t += red[w];
+            a.err_partial[cell0 / CPC] = t;
+        }
     }
 }
 

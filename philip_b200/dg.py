@@ -151,20 +151,61 @@ class DGStrong:
 
 
 class RungeKuttaODESolver:
-    """Explicit Butcher RK stepping on the device-resident state (RungeKuttaODESolver)."""
+    """Explicit RK stepping on the device-resident state: the Butcher methods of
+    RungeKuttaODESolver and the low-storage methods of LowStorageRungeKuttaODESolver
+    (src/ode_solver/low_storage_runge_kutta_ode_solver.cpp), with the latter's error-based
+    step-size control."""
 
     def __init__(self, dg: DGStrong):
         self.dg = dg
         self.current_time = 0.0
         self.current_iteration = 0
+        self.epsilon = [1.0, 1.0, 1.0]   # step-size controller history (low_storage_runge_kutta_ode_solver.cpp:11)
 
     def step_in_time(self, dt: float, pseudotime: bool = False, nsteps: int = 1):
         if pseudotime:
             raise NotImplementedError("pseudotime stepping belongs to the steady solvers")
         _lib.check(self.dg.L.ph_rk_step(self.dg.handle, dt, nsteps))
-        self.current_iteration += nsteps
-        self.current_time += dt * nsteps
+        for _ in range(nsteps):
+            self.current_iteration += 1
+            self.current_time += dt
         self.dg.set_current_time(self.current_time)
+
+    def error_norm(self) -> float:
+        """Weighted RMS error estimate of the last low-storage step."""
+        w = ctypes.c_double(0.0)
+        _lib.check(self.dg.L.ph_rk_error_norm(self.dg.handle, ctypes.byref(w)))
+        return float(w.value)
+
+    def get_automatic_error_adaptive_step_size(self, dt: float) -> float:
+        """LowStorageRungeKuttaODESolver::get_automatic_error_adaptive_step_size
+        (low_storage_runge_kutta_ode_solver.cpp:80-110): PID controller on eps = 1 / w."""
+        from .prm import RK_ORDER
+        prm = self.dg.parameters
+        order = RK_ORDER[prm.get("ODE solver/runge_kutta_method")]
+        b1, b2, b3 = (float(prm.get(f"ODE solver/beta{i}")) for i in (1, 2, 3))
+        w = self.error_norm()
+        self.epsilon = [1.0 / w, self.epsilon[0], self.epsilon[1]]
+        e0, e1, e2 = self.epsilon
+        return e0 ** (b1 / order) * e1 ** (b2 / order) * e2 ** (b3 / order) * dt
+
+    def get_automatic_initial_step_size(self, dt: float = 0.0) -> float:
+        """LowStorageRungeKuttaODESolver::get_automatic_initial_step_size
+        (low_storage_runge_kutta_ode_solver.cpp:112-175)."""
+        u_n = self.dg.solution
+        n = u_n.size
+        rhs = np.empty(n)
+        self.dg.apply_inverse_global_mass_matrix(self.dg.residual_of(u_n), rhs)
+        d0 = float(np.max(np.abs(u_n)))
+        d1 = float(np.max(np.abs(rhs)))
+        h0 = 1e-6 if (d0 < 1e-5 or d1 < 1e-5) else 0.01 * d0 / d1
+        u1 = u_n + h0 * rhs
+        rhs1 = np.empty(n)
+        self.dg.apply_inverse_global_mass_matrix(self.dg.residual_of(u1), rhs1)
+        d2 = float(np.max(np.abs(rhs1 - rhs))) / h0
+        h1 = max(1e-6, h0 * 1e-3) if max(d1, d2) <= 1e-15 else 0.01 / max(d1, d2)
+        self.dg.solution = u_n
+        return min(100.0 * h0, h1)
 
     def advance_solution_time(self, time_advance: float, dt: float):
         """ODESolverBase::advance_solution_time: steps of dt, the last one clipped."""
@@ -350,13 +391,21 @@ class FlowSolver:
         final_time = float(self.parameters.get("flow_solver/final_time"))
         end_exact = self.parameters.get("flow_solver/end_exactly_at_final_time").lower() == "true"
         adaptive = self.parameters.get("flow_solver/adaptive_time_step").lower() == "true"
+        error_adaptive = self.parameters.get("flow_solver/error_adaptive_time_step").lower() == "true"
+        if adaptive and error_adaptive:
+            raise ValueError("CFL-adaptation and error-adaptation cannot be used at the same time")
         write_restart = self.parameters.get("flow_solver/output_restart_files").lower() == "true"
         every_x = int(self.parameters.get("flow_solver/output_restart_files_every_x_steps"))
         every_dt = float(self.parameters.get("flow_solver/output_restart_files_every_dt_time_intervals"))
         restart_index = int(self.parameters.get("flow_solver/restart_file_index")) + 1 \
             if self.restart_dt is not None else 1
         next_restart_time = self.ode_solver.current_time + every_dt
-        dt = self.restart_dt if self.restart_dt is not None else self.time_step()
+        if self.restart_dt is not None:
+            dt = self.restart_dt
+        elif error_adaptive:   # flow_solver.cpp:495-510
+            dt = self.ode_solver.get_automatic_initial_step_size()
+        else:
+            dt = self.time_step()
         if not self.unsteady_data:
             self.unsteady_data.append((self.ode_solver.current_time, *self.dg.integrals()))
         while self.ode_solver.current_time < final_time:
@@ -370,6 +419,8 @@ class FlowSolver:
                 if adaptive:
                     dt = float(self.parameters.get("flow_solver/courant_friedrichs_lewy_number")) * \
                         self._grid_spacing() / q[3]
+            if error_adaptive:   # flow_solver.cpp:603-607
+                dt = self.ode_solver.get_automatic_error_adaptive_step_size(step)
             if write_restart:   # flow_solver.cpp:605-632: every dt time interval, or every x steps
                 if every_dt > 0.0:
                     if self.ode_solver.current_time >= next_restart_time:

@@ -22,7 +22,10 @@ DISS_FLUX = {"symm_internal_penalty": 0, "bassi_rebay_2": 1, "central_visc_flux"
 FR = {"cDG": 0, "cSD": 1, "cHU": 2, "cNegative": 3, "cNegative2": 4, "cPlus": 5, "c10Thousand": 6,
       "cHULumped": 7, "user_specified_value": 8}
 FR_AUX = {"kDG": 0}
-RK = {"rk4_ex": 0, "ssprk3_ex": 1, "heun2_ex": 2, "euler_ex": 3}   # parameters_ode_solver.h:66-78 order
+RK = {"rk4_ex": 0, "ssprk3_ex": 1, "heun2_ex": 2, "euler_ex": 3,   # parameters_ode_solver.h:66-78 order
+      "RK4_3_5_3SStar": 7, "RK3_2_5F_3SStarPlus": 8, "RK4_3_9F_3SStarPlus": 9, "RK5_4_10F_3SStarPlus": 10}
+RK_ORDER = {"rk4_ex": 4, "ssprk3_ex": 3, "heun2_ex": 2, "euler_ex": 1, "RK4_3_5_3SStar": 4,
+            "RK3_2_5F_3SStarPlus": 3, "RK4_3_9F_3SStarPlus": 4, "RK5_4_10F_3SStarPlus": 5}
 NON_PHYSICAL = {"return_big_number": 0, "abort_run": 1, "print_warning": 2}
 
 DEFAULTS = {
@@ -44,6 +47,8 @@ DEFAULTS = {
     "flow_solver/end_exactly_at_final_time": "true",
     "flow_solver/grid/grid_left_bound": "0.0", "flow_solver/grid/grid_right_bound": "1.0",
     "flow_solver/grid/number_of_grid_elements_per_dimension": "4",
+    "ODE solver/atol": "0.001", "ODE solver/rtol": "0.001", "ODE solver/beta1": "0.70",
+    "ODE solver/beta2": "-0.23", "ODE solver/beta3": "0.0", "flow_solver/error_adaptive_time_step": "false",
     "ODE solver/initial_time": "0.0", "ODE solver/initial_iteration": "0", "ODE solver/initial_time_step": "100.0",
     "ODE solver/initial_desired_time_for_output_solution_every_dt_time_intervals": "0.0",
     "flow_solver/unsteady_data_table_filename": "unsteady_data_table",
@@ -205,6 +210,8 @@ class Parameters:
         p.sipg_penalty_factor = sipg
         p.non_physical_behavior = NON_PHYSICAL[self.get("non_physical_behavior")]
         p.precision = precision
+        p.rk_atol = float(self.get("ODE solver/atol"))
+        p.rk_rtol = float(self.get("ODE solver/rtol"))
         return p
 
     def oracle_cfg(self) -> dict:
@@ -224,4 +231,5 @@ class Parameters:
             "use_constant_viscosity": _b(self.get("navier_stokes/use_constant_viscosity")),
             "sipg_penalty_factor": float(self.get("sipg_penalty_factor")),
             "FR_user_specified_correction_parameter_value": float(self.get("FR_user_specified_correction_parameter_value")),
+            "atol": float(self.get("ODE solver/atol")), "rtol": float(self.get("ODE solver/rtol")),
         }
