@@ -149,6 +149,29 @@ int ph_rk_error_norm(ph_ctx* ctx, double* w);
  * out[3] maximum convective wave speed; all divided by the domain volume except out[3]. */
 int ph_integrals(ph_ctx* ctx, double out[4]);
 
+/* All nine integrated quantities of PeriodicTurbulence::compute_and_update_integrated_quantities
+ * (periodic_turbulence.cpp:439-672), in the order of its IntegratedQuantitiesEnum
+ * (periodic_turbulence.h:176-186), each divided by the domain volume. The integrands are the
+ * NavierStokes physics' whatever the PDE (navier_stokes.cpp:399-740, euler.cpp:378-402); the
+ * palinstrophy differentiates the vorticity after its L2 projection onto the solution basis;
+ * the angular momentum (0.5 |x|^2 |omega|) is always computed, where the reference computes it
+ * only under do_compute_angular_momentum. Derived rates, as the reference forms them:
+ * pressure-dilatation-based dissipation = -out[2]; deviatoric / strain-rate based =
+ * 2 out[3] / Re and 2 out[4] / Re (zero for the Euler equations). */
+enum {
+    PH_IQ_KINETIC_ENERGY = 0,
+    PH_IQ_ENSTROPHY = 1,
+    PH_IQ_PRESSURE_DILATATION = 2,
+    PH_IQ_VISCOSITY_TIMES_DEVIATORIC_STRAIN_RATE_SQR = 3,
+    PH_IQ_VISCOSITY_TIMES_STRAIN_RATE_SQR = 4,
+    PH_IQ_INCOMPRESSIBLE_KINETIC_ENERGY = 5,
+    PH_IQ_INCOMPRESSIBLE_ENSTROPHY = 6,
+    PH_IQ_INCOMPRESSIBLE_PALINSTROPHY = 7,
+    PH_IQ_ANGULAR_MOMENTUM = 8,
+    PH_N_INTEGRATED_QUANTITIES = 9
+};
+int ph_integrated_quantities(ph_ctx* ctx, double out[PH_N_INTEGRATED_QUANTITIES]);
+
 /* Status word: bit 0 = a negative density or pressure was met (Euler::check_positive_quantity,
  * src/physics/euler.cpp:155-172). Reading clears it. */
 int ph_status(ph_ctx* ctx, uint32_t* flags);

@@ -1442,14 +1442,28 @@ void Solver::interpolate_ic(double* U, int ic, const double* icp) {
         }
 }
 
-void Solver::integrals(const double* U, double* out) {
-    // periodic_turbulence.cpp:439-672 with QGauss(p+11) over-integration
+void Solver::integrated_quantities(const double* U, double* out) {
+    // PeriodicTurbulence::compute_and_update_integrated_quantities (periodic_turbulence.cpp:439-672)
+    // with QGauss(p+11) over-integration. The integrands follow the NavierStokes physics of
+    // navier_stokes.cpp:399-740 and euler.cpp:378-402; the palinstrophy takes the gradient of the
+    // vorticity after its L2 projection onto the solution basis on the reference cell
+    // (vol_projection_operator, operators.cpp:1865-1889).
     Physics phys(&prm, &status);
     const int nd = ops.nd;
     const int ne = prm.poly_degree + 1 + 10;
     std::vector<double> xe, we; gauss_legendre(ne, xe, we);
     std::vector<double> B((size_t)ne * nd), dB((size_t)ne * nd);
     for (int q = 0; q < ne; ++q) lagrange_eval(ops.xs, xe[q], &B[q * nd], &dB[q * nd]);
+    // 1-D projection P = M^-1 (W B)^T with the mass matrix of the same quadrature
+    std::vector<double> M((size_t)nd * nd, 0.0), P((size_t)nd * ne);
+    for (int i = 0; i < nd; ++i) for (int j = 0; j < nd; ++j)
+        for (int q = 0; q < ne; ++q) M[i * nd + j] += we[q] * B[q * nd + i] * B[q * nd + j];
+    const std::vector<double> Minv = invert(M, nd);
+    for (int i = 0; i < nd; ++i) for (int q = 0; q < ne; ++q) {
+        double v = 0.0;
+        for (int j = 0; j < nd; ++j) v += Minv[i * nd + j] * we[q] * B[q * nd + j];
+        P[i * ne + q] = v;
+    }
     const int ne3 = ne * ne * ne;
     // curvilinear: the mapping (degree grid_degree on its GLL support points) at the Gauss points
     const int ng = mesh.grid_degree + 1, ng3 = ng * ng * ng;
@@ -1459,24 +1473,30 @@ void Solver::integrals(const double* U, double* out) {
         Bm.resize((size_t)ne * ng); dBm.resize((size_t)ne * ng);
         for (int q = 0; q < ne; ++q) lagrange_eval(xg, xe[q], &Bm[q * ng], &dBm[q * ng]);
     }
-    double ke = 0.0, ens = 0.0, wave = 0.0;
-#pragma omp parallel for reduction(+ : ke, ens) reduction(max : wave)
+    const double gam = prm.gamma, mach2 = prm.mach_inf * prm.mach_inf;
+    const double temp_ratio = 110.4 / prm.temperature_inf;   // navier_stokes.cpp:50-52
+    double acc[NUM_INTEGRATED] = {0.0};
+    double wave = 0.0;
+    const int nq = NUM_INTEGRATED;
+#pragma omp parallel for reduction(+ : acc[:nq]) reduction(max : wave)
     for (int c = 0; c < mesh.nc; ++c) {
         const double h = mesh.h, dj = h * h * h;
-        std::vector<double> jac, dje;      // curvilinear: J^{-1} [ne3][3][3] and det J at the Gauss points
+        const auto t = mesh.ijk[c];
+        std::vector<double> jac, dje, xq;   // curvilinear: J^{-1} [ne3][3][3], det J, positions [3][ne3]
         if (!mesh.affine) {
             std::vector<double> X(ng3), Jm((size_t)9 * ne3);
-            const auto t = mesh.ijk[c];
+            xq.resize((size_t)3 * ne3);
             for (int mm = 0; mm < 3; ++mm) {
                 for (int k = 0; k < ng; ++k) for (int j = 0; j < ng; ++j) for (int i = 0; i < ng; ++i) {
                     double p[3] = {mesh.left + h * (t[0] + xg[i]), mesh.left + h * (t[1] + xg[j]), mesh.left + h * (t[2] + xg[k])};
                     warp_point(mesh.left, mesh.right, mesh.warp, p);
                     X[(k * ng + j) * ng + i] = p[mm];
                 }
+                apply3(Bm.data(), ne, ng, Bm.data(), ne, ng, Bm.data(), ne, ng, X.data(), &xq[(size_t)mm * ne3], false, 1.0);
                 for (int j = 0; j < 3; ++j) {
-                    const double* B[3] = {Bm.data(), Bm.data(), Bm.data()};
-                    B[j] = dBm.data();
-                    apply3(B[0], ne, ng, B[1], ne, ng, B[2], ne, ng, X.data(), &Jm[(size_t)(mm * 3 + j) * ne3], false, 1.0);
+                    const double* Bd[3] = {Bm.data(), Bm.data(), Bm.data()};
+                    Bd[j] = dBm.data();
+                    apply3(Bd[0], ne, ng, Bd[1], ne, ng, Bd[2], ne, ng, X.data(), &Jm[(size_t)(mm * 3 + j) * ne3], false, 1.0);
                 }
             }
             jac.resize((size_t)9 * ne3); dje.resize(ne3);
@@ -1498,47 +1518,104 @@ void Solver::integrals(const double* U, double* out) {
                 I[8] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / d;
             }
         }
-        std::vector<double> uq(5 * ne3), gq(15 * ne3);
-        for (int s = 0; s < 5; ++s) {
-            const double* Uc = U + (size_t)c * ndofs_cell + s * nd3;
-            apply3(B.data(), ne, nd, B.data(), ne, nd, B.data(), ne, nd, Uc, &uq[s * ne3], false, 1.0);
-            apply3(dB.data(), ne, nd, B.data(), ne, nd, B.data(), ne, nd, Uc, &gq[(s * 3 + 0) * ne3], false, 1.0);
-            apply3(B.data(), ne, nd, dB.data(), ne, nd, B.data(), ne, nd, Uc, &gq[(s * 3 + 1) * ne3], false, 1.0);
-            apply3(B.data(), ne, nd, B.data(), ne, nd, dB.data(), ne, nd, Uc, &gq[(s * 3 + 2) * ne3], false, 1.0);
-        }
+        // physical gradient of a field from its reference gradient at cubature point q
+        auto physical = [&](const double* gref, int q, double* g) {
+            if (mesh.affine) {
+                for (int d = 0; d < 3; ++d) g[d] = (h * h) * gref[d] / dj;
+            } else {   // d/dx_d = sum_j (J^{-1})[j][d] d/dxi_j
+                const double* I = &jac[(size_t)q * 9];
+                for (int d = 0; d < 3; ++d) {
+                    double v = 0.0;
+                    for (int j = 0; j < 3; ++j) v += I[j * 3 + d] * gref[j];
+                    g[d] = v;
+                }
+            }
+        };
+        auto gradient_at_points = [&](const double* coef, double* val, double* grad) {
+            apply3(B.data(), ne, nd, B.data(), ne, nd, B.data(), ne, nd, coef, val, false, 1.0);
+            apply3(dB.data(), ne, nd, B.data(), ne, nd, B.data(), ne, nd, coef, &grad[0], false, 1.0);
+            apply3(B.data(), ne, nd, dB.data(), ne, nd, B.data(), ne, nd, coef, &grad[ne3], false, 1.0);
+            apply3(B.data(), ne, nd, B.data(), ne, nd, dB.data(), ne, nd, coef, &grad[2 * (size_t)ne3], false, 1.0);
+        };
+        std::vector<double> uq(5 * ne3), gq(15 * ne3), omq(3 * ne3);
+        for (int s = 0; s < 5; ++s)
+            gradient_at_points(U + (size_t)c * ndofs_cell + s * nd3, &uq[s * ne3], &gq[(size_t)s * 3 * ne3]);
+        double loc[NUM_INTEGRATED] = {0.0};
         for (int q = 0; q < ne3; ++q) {
             double u[5], g[5][3], w[5];
             for (int s = 0; s < 5; ++s) {
                 u[s] = uq[s * ne3 + q];
-                if (mesh.affine) {
-                    for (int d = 0; d < 3; ++d) g[s][d] = (h * h) * gq[(s * 3 + d) * ne3 + q] / dj;
-                } else {   // d/dx_d = sum_j (J^{-1})[j][d] d/dxi_j
-                    const double* I = &jac[(size_t)q * 9];
-                    for (int d = 0; d < 3; ++d) {
-                        double v = 0.0;
-                        for (int j = 0; j < 3; ++j) v += I[j * 3 + d] * gq[(s * 3 + j) * ne3 + q];
-                        g[s][d] = v;
-                    }
-                }
+                const double gref[3] = {gq[(s * 3 + 0) * ne3 + q], gq[(s * 3 + 1) * ne3 + q], gq[(s * 3 + 2) * ne3 + q]};
+                physical(gref, q, g[s]);
             }
             phys.primitive(u, w);
             double v2 = 0.0; for (int d = 0; d < 3; ++d) v2 += w[1 + d] * w[1 + d];
-            const double kin = 0.5 * w[0] * v2;
             double gv[3][3];
             for (int a = 0; a < 3; ++a) for (int d = 0; d < 3; ++d) gv[a][d] = (g[1 + a][d] - w[1 + a] * g[0][d]) / w[0];
-            const double om0 = gv[2][1] - gv[1][2], om1 = gv[0][2] - gv[2][0], om2 = gv[1][0] - gv[0][1];
-            const double en = 0.5 * u[0] * (om0 * om0 + om1 * om1 + om2 * om2);
+            const double om[3] = {gv[2][1] - gv[1][2], gv[0][2] - gv[2][0], gv[1][0] - gv[0][1]};
+            const double om2 = om[0] * om[0] + om[1] * om[1] + om[2] * om[2];
+            for (int d = 0; d < 3; ++d) omq[d * ne3 + q] = om[d];
+            double S[3][3], dil = 0.0;
+            for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) S[a][b] = 0.5 * (gv[a][b] + gv[b][a]);
+            for (int d = 0; d < 3; ++d) dil += gv[d][d];
+            double s2 = 0.0, sd2 = 0.0;
+            for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) {
+                const double dv = S[a][b] - (a == b ? dil / 3.0 : 0.0);
+                s2 += S[a][b] * S[a][b];
+                sd2 += dv * dv;
+            }
+            const double T = gam * mach2 * (w[4] / w[0]);
+            const double mu = prm.use_constant_viscosity ? 1.0 * prm.constant_viscosity
+                                                         : ((1.0 + temp_ratio) / (T + temp_ratio)) * std::pow(T, 1.5);
+            double r2 = 0.0;
+            for (int d = 0; d < 3; ++d) {
+                const double x = mesh.affine ? mesh.left + h * (t[d] + xe[d == 0 ? q % ne : d == 1 ? (q / ne) % ne : q / (ne * ne)])
+                                             : xq[(size_t)d * ne3 + q];
+                r2 += x * x;
+            }
+            const double val[NUM_INTEGRATED] = {
+                0.5 * w[0] * v2,                 // kinetic energy
+                0.5 * w[0] * om2,                // enstrophy
+                w[4] * dil,                      // pressure dilatation
+                mu * sd2,                        // viscosity x |deviatoric strain rate|^2
+                mu * s2,                         // viscosity x |strain rate|^2
+                0.5 * v2,                        // incompressible kinetic energy
+                0.5 * om2,                       // incompressible enstrophy
+                0.0,                             // incompressible palinstrophy (below)
+                0.5 * r2 * std::sqrt(om2)};      // angular momentum
             const double wt = we[q % ne] * we[(q / ne) % ne] * we[q / (ne * ne)] * (mesh.affine ? dj : dje[q]);
-            ke += kin * wt; ens += en * wt;
+            for (int i = 0; i < NUM_INTEGRATED; ++i) loc[i] += val[i] * wt;
             const double mw = phys.max_eig(u);
             if (mw > wave) wave = mw;
         }
+        // palinstrophy: project the vorticity onto the solution basis, then take its gradient
+        std::vector<double> coef(nd3), oval(ne3), ograd(3 * (size_t)ne3);
+        for (int d = 0; d < 3; ++d) {
+            apply3(P.data(), nd, ne, P.data(), nd, ne, P.data(), nd, ne, &omq[(size_t)d * ne3], coef.data(), false, 1.0);
+            gradient_at_points(coef.data(), oval.data(), ograd.data());
+            for (int q = 0; q < ne3; ++q) {
+                const double gref[3] = {ograd[q], ograd[ne3 + q], ograd[2 * (size_t)ne3 + q]};
+                double g[3];
+                physical(gref, q, g);
+                const double wt = we[q % ne] * we[(q / ne) % ne] * we[q / (ne * ne)] * (mesh.affine ? dj : dje[q]);
+                loc[7] += 0.5 * (g[0] * g[0] + g[1] * g[1] + g[2] * g[2]) * wt;
+            }
+        }
+        for (int i = 0; i < NUM_INTEGRATED; ++i) acc[i] += loc[i];
     }
     const double vol = std::pow(mesh.right - mesh.left, 3);
-    out[0] = ke / vol;
-    out[1] = ens / vol;
+    for (int i = 0; i < NUM_INTEGRATED; ++i) out[i] = acc[i] / vol;
+    out[NUM_INTEGRATED] = wave;
+}
+
+void Solver::integrals(const double* U, double* out) {
+    double q[NUM_INTEGRATED + 1];
+    integrated_quantities(U, q);
+    out[0] = q[0];
+    out[1] = q[1];
+    // zero for inviscid flow (periodic_turbulence.cpp:717-725)
     out[2] = (prm.pde == NAVIER_STOKES) ? 2.0 * out[1] / prm.reynolds_inf : 0.0;
-    out[3] = wave;
+    out[3] = q[NUM_INTEGRATED];
 }
 
 } // namespace oracle

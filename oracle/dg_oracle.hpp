@@ -107,6 +107,8 @@ Mesh build_periodic_cube(int n, double left, double right, int order, const Ops1
                          double warp = 0.0, int grid_degree = 1);
 
 // DG discretisation state.
+constexpr int NUM_INTEGRATED = 9;   // PeriodicTurbulence::IntegratedQuantitiesEnum
+
 struct Solver {
     Params prm;
     Ops1D ops;
@@ -134,6 +136,10 @@ struct Solver {
     // TGV integrated quantities (periodic_turbulence.cpp:439-672):
     // out[0]=KE, out[1]=enstrophy, out[2]=vorticity dissipation rate, out[3]=max wave speed
     void integrals(const double* U, double* out);
+    // out[0..8]: the nine integrated quantities in the order of PeriodicTurbulence's
+    // IntegratedQuantitiesEnum (periodic_turbulence.h:176-186), each over the domain volume
+    // (angular momentum always computed); out[9] = max wave speed
+    void integrated_quantities(const double* U, double* out);
 };
 
 enum InitialCondition { IC_TGV = 0, IC_ISENTROPIC_VORTEX = 1, IC_VORTEX_PARAM = 2 };

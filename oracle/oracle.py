@@ -74,6 +74,7 @@ def lib():
         L.orc_inverse_mass.argtypes = [vp, dp, dp]
         L.orc_rk_step.argtypes = [vp, dp, ctypes.c_double]
         L.orc_integrals.argtypes = [vp, dp, dp]
+        L.orc_integrated_quantities.argtypes = [vp, dp, dp]
         L.orc_rk_error.argtypes = [vp]; L.orc_rk_error.restype = ctypes.c_double
         _lib = L
     return _lib
@@ -197,6 +198,13 @@ class Oracle:
     def integrals(self, U):
         out = np.zeros(4)
         lib().orc_integrals(self.h, _dp(np.ascontiguousarray(U)), _dp(out))
+        return out
+
+    def integrated_quantities(self, U):
+        """The nine PeriodicTurbulence integrated quantities (IntegratedQuantitiesEnum order, each
+        over the domain volume) and the max wave speed as a tenth entry."""
+        out = np.zeros(10)
+        lib().orc_integrated_quantities(self.h, _dp(np.ascontiguousarray(U)), _dp(out))
         return out
 
     def status(self):

@@ -109,5 +109,8 @@ void orc_aux(void* h, double* out) {
 void orc_inverse_mass(void* h, const double* in, double* out) { static_cast<Solver*>(h)->apply_inverse_mass(in, out); }
 void orc_rk_step(void* h, double* U, double dt) { static_cast<Solver*>(h)->rk_step(U, dt); }
 void orc_integrals(void* h, const double* U, double* out) { static_cast<Solver*>(h)->integrals(U, out); }
+void orc_integrated_quantities(void* h, const double* U, double* out) {
+    static_cast<Solver*>(h)->integrated_quantities(U, out);
+}
 
 }  // extern "C"

@@ -14,6 +14,11 @@ LIB_PATH = os.environ.get("PHILIP_B200_LIB", os.path.join(_HERE, "libphilip_b200
 PH_HOST, PH_DEVICE = 0, 1
 PH_FP64, PH_FP32_RESIDUAL = 0, 1
 PH_OK, PH_ERR_INVALID, PH_ERR_UNSUPPORTED, PH_ERR_CUDA, PH_ERR_NOMEM = 0, 1, 2, 3, 4
+# PeriodicTurbulence::IntegratedQuantitiesEnum (periodic_turbulence.h:176-186)
+INTEGRATED_QUANTITIES = ("kinetic_energy", "enstrophy", "pressure_dilatation",
+                         "viscosity_times_deviatoric_strain_rate_tensor_magnitude_sqr",
+                         "viscosity_times_strain_rate_tensor_magnitude_sqr", "incompressible_kinetic_energy",
+                         "incompressible_enstrophy", "incompressible_palinstrophy", "angular_momentum")
 ERRORS = {1: "invalid argument", 2: "unsupported configuration", 3: "CUDA error", 4: "out of device memory"}
 
 EXPORTED = ["ph_ctx_create", "ph_ctx_destroy", "ph_ndofs", "ph_cell_ijk", "ph_set_state", "ph_get_state",
@@ -22,7 +27,8 @@ EXPORTED = ["ph_ctx_create", "ph_ctx_destroy", "ph_ndofs", "ph_cell_ijk", "ph_se
             "ph_batch_create", "ph_batch_destroy", "ph_batch_bytes", "ph_batch_admit", "ph_batch_step",
             "ph_batch_progress", "ph_batch_active", "ph_batch_get_state", "ph_batch_status", "ph_batch_release",
             "ph_batch_poll", "ph_batch_fence", "ph_batch_fence_wait", "ph_batch_autotune", "ph_batch_set_variant",
-            "ph_batch_launches", "ph_mesh_node_xyz", "ph_rk_error_norm", "ph_last_error"]
+            "ph_batch_launches", "ph_mesh_node_xyz", "ph_rk_error_norm", "ph_last_error",
+            "ph_integrated_quantities"]
 
 
 class PhParams(ctypes.Structure):
@@ -73,6 +79,7 @@ def load(build_if_missing: bool = False):
     L.ph_apply_inverse_mass.argtypes = [vp, vp, vp, ctypes.c_int]
     L.ph_rk_step.argtypes = [vp, ctypes.c_double, ctypes.c_int]
     L.ph_integrals.argtypes = [vp, dp]
+    L.ph_integrated_quantities.argtypes = [vp, dp]
     L.ph_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32)]
     L.ph_sync.argtypes = [vp]
     L.ph_set_timing.argtypes = [vp, ctypes.c_int]

@@ -314,7 +314,21 @@ void build_integral_table(const std::vector<double>& x, int p, ph::IntegralTab& 
         lagrange(x, xe[q], v.data(), dv.data());
         for (int a = 0; a < N1; ++a) { itab.B[q * N1 + a] = v[a]; itab.dB[q * N1 + a] = dv[a]; }
         itab.w[q] = we[q];
+        itab.x[q] = xe[q];
     }
+    // 1-D L2 projection onto the solution basis, P = M^-1 (W B)^T with the mass matrix of the
+    // same quadrature (vol_projection_operator::build_1D_volume_operator, operators.cpp:1873-1889)
+    std::vector<double> M((size_t)N1 * N1, 0.0), Mi;
+    for (int i = 0; i < N1; ++i)
+        for (int j = 0; j < N1; ++j)
+            for (int q = 0; q < ne; ++q) M[i * N1 + j] += we[q] * itab.B[q * N1 + i] * itab.B[q * N1 + j];
+    mat_inv(M, N1, Mi);   // a Gauss mass matrix of the Lagrange basis: symmetric positive definite
+    for (int i = 0; i < N1; ++i)
+        for (int q = 0; q < ne; ++q) {
+            double acc = 0.0;
+            for (int j = 0; j < N1; ++j) acc += Mi[i * N1 + j] * we[q] * itab.B[q * N1 + j];
+            itab.P[i * ne + q] = acc;
+        }
 }
 
 ph::PhysConst physics_constants(const ph_params* prm, double h, double& penalty) {
@@ -589,6 +603,7 @@ struct ph_ctx {
     std::vector<double> xyz;            // physical node coordinates [cell][node][3]
     double* d_metric = nullptr;         // curvilinear: [nc][10][NP] cofactor rows + 1/det J
     double* d_xnode = nullptr;          // curvilinear: node coordinates [nc][3][NP] (integrals)
+    double* d_origin = nullptr;         // affine: lower corner of each cell [nc][3] (integrals)
     size_t ndofs = 0;
     std::vector<int> ijk;
     int* d_nbr = nullptr;
@@ -759,10 +774,11 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
         bad |= dalloc(&c->d_fv, c->fp32 ? (vt + 1) / 2 : vt);
     }
     if (c->fp32) bad |= dalloc(&c->d_comp, N);
-    bad |= dalloc(&c->d_partial, 3 * (size_t)c->nc);
+    bad |= dalloc(&c->d_partial, (size_t)ph::integral_partials<true>() * c->nc);
     bad |= dalloc(&c->d_status, 1);
     if (c->curv) bad |= dalloc(&c->d_metric, metric.size());
     if (c->curv) bad |= dalloc(&c->d_xnode, (size_t)3 * c->nc * c->NP);
+    else bad |= dalloc(&c->d_origin, (size_t)3 * c->nc);
     if (bad) { ph_ctx_destroy(c); return fail(PH_ERR_NOMEM, "device allocation failed"); }
     cudaError_t e = cudaSuccess;
     e = cudaMemcpy(c->d_nbr, nbr.data(), nbr.size() * sizeof(int), cudaMemcpyHostToDevice);
@@ -781,8 +797,14 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
                     xn[((size_t)cc * 3 + d) * c->NP + node] = c->xyz[((size_t)cc * c->NP + node) * 3 + d];
         e = cudaMemcpy(c->d_xnode, xn.data(), xn.size() * sizeof(double), cudaMemcpyHostToDevice);
     }
+    if (e == cudaSuccess && c->d_origin) {   // node 0 sits at the cell's lower corner
+        std::vector<double> o((size_t)3 * c->nc);
+        for (int cc = 0; cc < c->nc; ++cc)
+            for (int d = 0; d < 3; ++d) o[(size_t)cc * 3 + d] = c->xyz[(size_t)cc * c->NP * 3 + d];
+        e = cudaMemcpy(c->d_origin, o.data(), o.size() * sizeof(double), cudaMemcpyHostToDevice);
+    }
     if (e != cudaSuccess) { ph_ctx_destroy(c); return fail(PH_ERR_CUDA, cudaGetErrorString(e)); }
-    c->h_partial.resize(3 * (size_t)c->nc);
+    c->h_partial.resize((size_t)ph::integral_partials<true>() * c->nc);
     *out = c;
     return PH_OK;
 }
@@ -794,7 +816,7 @@ int ph_ctx_destroy(ph_ctx* c) {
         cudaGraphExecDestroy(c->step_graph);
     }
     void* ptrs[] = {c->d_nbr, c->d_ops, c->d_itab, c->d_sol, c->d_stA, c->d_stB, c->d_acc, c->d_carry,
-                    c->d_fv, c->d_comp, c->d_tmpA, c->d_tmpB, c->d_partial, c->d_status, c->d_metric, c->d_xnode, c->d_err};
+                    c->d_fv, c->d_comp, c->d_tmpA, c->d_tmpB, c->d_partial, c->d_status, c->d_metric, c->d_xnode, c->d_origin, c->d_err};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -961,23 +983,33 @@ int ph_rk_step(ph_ctx* c, double dt, int nsteps) {
     return PH_OK;
 }
 
-int ph_integrals(ph_ctx* c, double out[4]) {
-    if (!c || !out) return fail(PH_ERR_INVALID, "null argument");
+static int run_integrals(ph_ctx* c, bool full) {
+    ph::IntegralConst ic{};
+    ic.h = c->h;
+    ic.gam = c->prm.gamma_gas; ic.gm1 = ic.gam - 1.0;
+    ic.mach2 = c->pc.mach2; ic.temp_ratio = c->pc.temp_ratio;
+    ic.const_visc = c->pc.const_visc; ic.use_const_visc = c->pc.use_const_visc;
     cudaError_t e;
-    const double gam = c->prm.gamma_gas, gm1 = gam - 1.0;
     switch (c->N1) {
-    case 2: e = ph::launch_integrals<2>(c->d_sol, c->d_xnode, c->d_itab, c->nc, c->h, gam, gm1, c->d_partial, c->stream); break;
-    case 3: e = ph::launch_integrals<3>(c->d_sol, c->d_xnode, c->d_itab, c->nc, c->h, gam, gm1, c->d_partial, c->stream); break;
-    case 4: e = ph::launch_integrals<4>(c->d_sol, c->d_xnode, c->d_itab, c->nc, c->h, gam, gm1, c->d_partial, c->stream); break;
-    case 5: e = ph::launch_integrals<5>(c->d_sol, c->d_xnode, c->d_itab, c->nc, c->h, gam, gm1, c->d_partial, c->stream); break;
-    case 6: e = ph::launch_integrals<6>(c->d_sol, c->d_xnode, c->d_itab, c->nc, c->h, gam, gm1, c->d_partial, c->stream); break;
-    case 7: e = ph::launch_integrals<7>(c->d_sol, c->d_xnode, c->d_itab, c->nc, c->h, gam, gm1, c->d_partial, c->stream); break;
+#define PH_INTEGRALS_CASE(n)                                                                                   \
+    case n: e = ph::launch_integrals<n>(c->d_sol, c->d_xnode, c->d_origin, c->d_itab, c->nc, ic, full, c->d_partial, \
+                                        c->stream); break;
+    PH_INTEGRALS_CASE(2) PH_INTEGRALS_CASE(3) PH_INTEGRALS_CASE(4) PH_INTEGRALS_CASE(5) PH_INTEGRALS_CASE(6)
+    PH_INTEGRALS_CASE(7)
+#undef PH_INTEGRALS_CASE
     default: return fail(PH_ERR_UNSUPPORTED, "polynomial degree");
     }
     if (e != cudaSuccess) return fail(PH_ERR_CUDA, cudaGetErrorString(e));
-    PH_CUDA(cudaMemcpyAsync(c->h_partial.data(), c->d_partial, 3 * (size_t)c->nc * sizeof(double),
+    const size_t nq = full ? ph::integral_partials<true>() : ph::integral_partials<false>();
+    PH_CUDA(cudaMemcpyAsync(c->h_partial.data(), c->d_partial, nq * c->nc * sizeof(double),
                             cudaMemcpyDeviceToHost, c->stream));
     PH_CUDA(cudaStreamSynchronize(c->stream));
+    return PH_OK;
+}
+
+int ph_integrals(ph_ctx* c, double out[4]) {
+    if (!c || !out) return fail(PH_ERR_INVALID, "null argument");
+    if (int rc = run_integrals(c, false)) return rc;
     double ke = 0.0, ens = 0.0, wave = 0.0;
     for (int i = 0; i < c->nc; ++i) {
         ke += c->h_partial[3 * i]; ens += c->h_partial[3 * i + 1];
@@ -990,6 +1022,19 @@ int ph_integrals(ph_ctx* c, double out[4]) {
     // periodic_turbulence.cpp:717-725)
     out[2] = c->visc ? 2.0 * out[1] / c->prm.reynolds_number_inf : 0.0;
     out[3] = wave;
+    return PH_OK;
+}
+
+int ph_integrated_quantities(ph_ctx* c, double out[PH_N_INTEGRATED_QUANTITIES]) {
+    if (!c || !out) return fail(PH_ERR_INVALID, "null argument");
+    if (int rc = run_integrals(c, true)) return rc;
+    constexpr int NQ = ph::integral_partials<true>();
+    static_assert(NQ == PH_N_INTEGRATED_QUANTITIES + 1, "partials: the quantities then the wave speed");
+    double acc[PH_N_INTEGRATED_QUANTITIES] = {0.0};
+    for (int i = 0; i < c->nc; ++i)
+        for (int q = 0; q < PH_N_INTEGRATED_QUANTITIES; ++q) acc[q] += c->h_partial[(size_t)NQ * i + q];
+    const double vol = std::pow(c->right - c->left, 3);
+    for (int q = 0; q < PH_N_INTEGRATED_QUANTITIES; ++q) out[q] = acc[q] / vol;
     return PH_OK;
 }
 

@@ -188,11 +188,11 @@ cudaError_t launch_inverse_mass(const double* in, double* out, const OpTab* ops,
     return cudaGetLastError();
 }
 
-template <int N1, bool CURV>
-static cudaError_t launch_integrals_one(const double* U, const double* X, const IntegralTab* tab, int nc, double h,
-                                       double gam, double gm1, double* partial, cudaStream_t s) {
-    auto kern = integrals_kernel<N1, CURV>;
-    constexpr size_t bytes = integrals_smem_bytes<N1, CURV>();
+template <int N1, bool CURV, bool FULL>
+static cudaError_t launch_integrals_one(const double* U, const double* X, const double* origin, const IntegralTab* tab,
+                                       int nc, const IntegralConst& ic, double* partial, cudaStream_t s) {
+    auto kern = integrals_kernel<N1, CURV, FULL>;
+    constexpr size_t bytes = integrals_smem_bytes<N1, CURV, FULL>();
     int dev = 0;
     cudaGetDevice(&dev);
     static bool configured[64] = {false};
@@ -201,15 +201,18 @@ static cudaError_t launch_integrals_one(const double* U, const double* X, const 
         if (e != cudaSuccess) return e;
         configured[dev] = true;
     }
-    kern<<<nc, 256, bytes, s>>>(U, X, tab, nc, h, gam, gm1, partial);
+    kern<<<nc, 256, bytes, s>>>(U, X, origin, tab, nc, ic, partial);
     return cudaGetLastError();
 }
 
 template <int N1>
-cudaError_t launch_integrals(const double* U, const double* X, const IntegralTab* tab, int nc, double h, double gam,
-                             double gm1, double* partial, cudaStream_t s) {
-    return X ? launch_integrals_one<N1, true>(U, X, tab, nc, h, gam, gm1, partial, s)
-             : launch_integrals_one<N1, false>(U, X, tab, nc, h, gam, gm1, partial, s);
+cudaError_t launch_integrals(const double* U, const double* X, const double* origin, const IntegralTab* tab, int nc,
+                             const IntegralConst& ic, bool full, double* partial, cudaStream_t s) {
+    if (full)
+        return X ? launch_integrals_one<N1, true, true>(U, X, origin, tab, nc, ic, partial, s)
+                 : launch_integrals_one<N1, false, true>(U, X, origin, tab, nc, ic, partial, s);
+    return X ? launch_integrals_one<N1, true, false>(U, X, origin, tab, nc, ic, partial, s)
+             : launch_integrals_one<N1, false, false>(U, X, origin, tab, nc, ic, partial, s);
 }
 
 template cudaError_t launch_stage<PH_N1>(const StageArgs&, int, bool, bool, cudaStream_t);
@@ -221,7 +224,7 @@ template cudaError_t launch_aux<PH_N1>(const double*, const int*, const OpTab*, 
                                        void*, cudaStream_t);
 template cudaError_t launch_inverse_mass<PH_N1>(const double*, double*, const OpTab*, int, double, const double*,
                                                 cudaStream_t);
-template cudaError_t launch_integrals<PH_N1>(const double*, const double*, const IntegralTab*, int, double, double,
-                                             double, double*, cudaStream_t);
+template cudaError_t launch_integrals<PH_N1>(const double*, const double*, const double*, const IntegralTab*, int,
+                                             const IntegralConst&, bool, double*, cudaStream_t);
 
 } // namespace ph

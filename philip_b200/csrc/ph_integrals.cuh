@@ -11,6 +11,14 @@
 // through the same contractions; their derivatives at a cubature point are the mapping
 // Jacobian there (the mapping has the solution's degree), which gives det J for the
 // weights and J^-1 for the physical gradients.
+//
+// FULL: all nine quantities of the reference's IntegratedQuantitiesEnum
+// (periodic_turbulence.h:176-186) with the integrands of navier_stokes.cpp:399-740 and
+// euler.cpp:378-402. The palinstrophy needs the gradient of the vorticity after its L2
+// projection onto the solution basis (vol_projection_operator, operators.cpp:1865-1889):
+// each column thread accumulates the qz-projection of the vorticity while it walks qz,
+// the qy and qx projections follow in shared memory, and a second pass over the
+// cubature points differentiates the projected vorticity.
 #pragma once
 #include "ph_kernels.cuh"
 
@@ -21,35 +29,119 @@ constexpr int MAXNE = 20;
 struct IntegralTab {
     double B[MAXNE * MAXN1];
     double dB[MAXNE * MAXN1];
+    double P[MAXN1 * MAXNE];   // 1-D L2 projection onto the solution basis, [node][cubature point]
     double w[MAXNE];
+    double x[MAXNE];           // cubature points on [0, 1]
 };
 
-template <int N1, bool CURV>
+// Viscosity and gas constants of the integrands (the reference evaluates them with a
+// NavierStokes physics object whatever the PDE).
+struct IntegralConst {
+    double h, gam, gm1, mach2, temp_ratio, const_visc;
+    int use_const_visc;
+};
+
+// partial sums per cell: FULL = the nine quantities then the max wave speed;
+// otherwise kinetic energy, enstrophy, max wave speed
+template <bool FULL> __host__ __device__ constexpr int integral_partials() { return FULL ? 10 : 3; }
+
+template <int N1, bool CURV, bool FULL>
 __host__ __device__ constexpr size_t integrals_smem_bytes() {
     constexpr int NFLD = CURV ? 8 : 5;
-    return sizeof(double) * (NFLD * N1 * N1 * N1 + 2 * NFLD * N1 * N1 * (N1 + 10));
+    constexpr int NE = N1 + 10;
+    constexpr size_t base = NFLD * N1 * N1 * N1 + 2 * NFLD * N1 * N1 * NE;
+    constexpr size_t proj = FULL ? 3 * NE * NE * N1 + 3 * NE * N1 * N1 : 0;
+    return sizeof(double) * (base + proj);
 }
 
-template <int N1, bool CURV>
-__global__ void integrals_kernel(const double* __restrict__ U, const double* __restrict__ X, const IntegralTab* tab,
-                                 int nc, double h, double gam, double gm1, double* __restrict__ partial) {
+// Physical gradient of nf nodal fields at one cubature point from the x-contracted values
+// and x-derivatives (sT0, sT1); fields listed in fld[].
+template <int N1, int NE, int NF>
+__device__ __forceinline__ void point_fields(const double* sT0, const double* sT1, const double* sB, const double* sdB,
+                                             const int (&fld)[NF], int qx, int qy, int qz, double (&u)[NF],
+                                             double (&g)[NF][3]) {
+    constexpr int NT2 = N1 * N1 * NE;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+        const int s = fld[f];
+        double v = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+#pragma unroll
+        for (int k = 0; k < N1; ++k) {
+            double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+#pragma unroll
+            for (int j = 0; j < N1; ++j) {
+                const double t0 = sT0[s * NT2 + (k * N1 + j) * NE + qx];
+                const double t1 = sT1[s * NT2 + (k * N1 + j) * NE + qx];
+                a0 += sB[qy * N1 + j] * t0;
+                a1 += sB[qy * N1 + j] * t1;
+                a2 += sdB[qy * N1 + j] * t0;
+            }
+            const double b = sB[qz * N1 + k], db = sdB[qz * N1 + k];
+            v += b * a0; gx += b * a1; gy += b * a2; gz += db * a0;
+        }
+        u[f] = v; g[f][0] = gx; g[f][1] = gy; g[f][2] = gz;
+    }
+}
+
+// J^-1 and det J from the reference gradients of the three coordinate fields
+// (J[m][j] = dX_m/dxi_j; physical gradient = reference gradient times J^-1).
+__device__ __forceinline__ double inverse_jacobian(const double (&gx)[3][3], double (&I)[3][3]) {
+    const double(&J)[3][3] = gx;
+    const double dj = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) -
+                      J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+                      J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+    I[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) / dj;
+    I[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / dj;
+    I[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / dj;
+    I[1][0] = (J[1][2] * J[2][0] - J[1][0] * J[2][2]) / dj;
+    I[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / dj;
+    I[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / dj;
+    I[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) / dj;
+    I[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / dj;
+    I[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / dj;
+    return dj;
+}
+
+template <int NF>
+__device__ __forceinline__ void to_physical(double (&g)[NF][3], int nf, const double (&I)[3][3]) {
+#pragma unroll
+    for (int s = 0; s < NF; ++s) {
+        if (s >= nf) break;
+        const double r0 = g[s][0], r1 = g[s][1], r2 = g[s][2];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) g[s][d] = r0 * I[0][d] + r1 * I[1][d] + r2 * I[2][d];
+    }
+}
+
+template <int N1, bool CURV, bool FULL>
+__global__ void integrals_kernel(const double* __restrict__ U, const double* __restrict__ X,
+                                 const double* __restrict__ origin, const IntegralTab* tab, int nc, IntegralConst ic,
+                                 double* __restrict__ partial) {
     constexpr int NE = N1 + 10;
     constexpr int NP = N1 * N1 * N1;
     constexpr int NT2 = N1 * N1 * NE;
     constexpr int NFLD = CURV ? 8 : 5;   // state (+ node coordinates)
-    __shared__ double sB[NE * N1], sdB[NE * N1], sw[NE];
-    __shared__ double red[3][32];
+    constexpr int NQ = integral_partials<FULL>();
+    constexpr int NACC = FULL ? 9 : 2;   // summed quantities (the wave speed is a max)
+    __shared__ double sB[NE * N1], sdB[NE * N1], sP[FULL ? N1 * NE : 1], sw[NE], sx[NE];
+    __shared__ double red[NQ][32];
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* sU = reinterpret_cast<double*>(smem_raw);
     double* sT0 = sU + NFLD * NP;       // [s][(k*N1 + j)*NE + qx], x-contracted values
     double* sT1 = sT0 + NFLD * NT2;     // x-contracted x-derivatives
+    double* sWz = sT1 + NFLD * NT2;     // FULL: vorticity projected in z, [c][qy*NE + qx][k]
+    double* sWy = sWz + 3 * NE * NE * N1;   // FULL: ... and in y, [c][(k*N1 + j)*NE + qx]
     const int cell = blockIdx.x;
     const int tid = threadIdx.x;
     for (int i = tid; i < NE * N1; i += blockDim.x) { sB[i] = tab->B[i]; sdB[i] = tab->dB[i]; }
-    for (int i = tid; i < NE; i += blockDim.x) sw[i] = tab->w[i];
+    if constexpr (FULL) {
+        for (int i = tid; i < N1 * NE; i += blockDim.x) sP[i] = tab->P[i];
+    }
+    for (int i = tid; i < NE; i += blockDim.x) { sw[i] = tab->w[i]; sx[i] = tab->x[i]; }
     for (int i = tid; i < 5 * NP; i += blockDim.x) sU[i] = U[(size_t)cell * 5 * NP + i];
-    if constexpr (CURV)
+    if constexpr (CURV) {
         for (int i = tid; i < 3 * NP; i += blockDim.x) sU[5 * NP + i] = X[(size_t)cell * 3 * NP + i];
+    }
     __syncthreads();
     for (int i = tid; i < NFLD * NT2; i += blockDim.x) {
         const int qx = i % NE, kj = (i / NE) % (N1 * N1), s = i / NT2;
@@ -63,97 +155,197 @@ __global__ void integrals_kernel(const double* __restrict__ U, const double* __r
         sT1[i] = dv;
     }
     __syncthreads();
-    const double inv_h = 1.0 / h, detj = h * h * h;
-    double ke = 0.0, ens = 0.0, wave = 0.0;
-    for (int pt = tid; pt < NE * NE * NE; pt += blockDim.x) {
-        const int qx = pt % NE, qy = (pt / NE) % NE, qz = pt / (NE * NE);
-        double u[NFLD], g[NFLD][3];
+    const double h = ic.h, inv_h = 1.0 / h, detj = h * h * h;
+    const double gam = ic.gam, gm1 = ic.gm1;
+    double acc[NACC];
 #pragma unroll
-        for (int s = 0; s < NFLD; ++s) {
-            double v = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+    for (int i = 0; i < NACC; ++i) acc[i] = 0.0;
+    double wave = 0.0;
+    double o0rg[3] = {0.0, 0.0, 0.0};
+    if constexpr (FULL && !CURV) {
+        for (int d = 0; d < 3; ++d) o0rg[d] = origin[3 * cell + d];
+    }
+    int fld[NFLD];
 #pragma unroll
-            for (int k = 0; k < N1; ++k) {
-                double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (int s = 0; s < NFLD; ++s) fld[s] = s;
+    for (int col = tid; col < NE * NE; col += blockDim.x) {
+        const int qx = col % NE, qy = col / NE;
+        double zp[FULL ? 3 : 1][FULL ? N1 : 1];   // FULL: vorticity projected along this column
 #pragma unroll
-                for (int j = 0; j < N1; ++j) {
-                    const double t0 = sT0[s * NT2 + (k * N1 + j) * NE + qx];
-                    const double t1 = sT1[s * NT2 + (k * N1 + j) * NE + qx];
-                    a0 += sB[qy * N1 + j] * t0;
-                    a1 += sB[qy * N1 + j] * t1;
-                    a2 += sdB[qy * N1 + j] * t0;
+        for (int c = 0; c < (FULL ? 3 : 1); ++c)
+#pragma unroll
+            for (int k = 0; k < (FULL ? N1 : 1); ++k) zp[c][k] = 0.0;
+        for (int qz = 0; qz < NE; ++qz) {
+            double u[NFLD], g[NFLD][3];
+            point_fields<N1, NE, NFLD>(sT0, sT1, sB, sdB, fld, qx, qy, qz, u, g);
+            double wdet = detj;
+            if constexpr (CURV) {
+                const double gx[3][3] = {{g[5][0], g[5][1], g[5][2]}, {g[6][0], g[6][1], g[6][2]},
+                                         {g[7][0], g[7][1], g[7][2]}};
+                double I[3][3];
+                wdet = inverse_jacobian(gx, I);
+                to_physical<NFLD>(g, 5, I);
+            } else {
+#pragma unroll
+                for (int s = 0; s < 5; ++s)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) g[s][d] *= inv_h;
+            }
+            const double rho = u[0];
+            double v[3], v2 = 0.0;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) { v[d] = u[1 + d] / rho; v2 += v[d] * v[d]; }
+            double gv[3][3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) gv[a][d] = (g[1 + a][d] - v[a] * g[0][d]) / rho;
+            const double o0 = gv[2][1] - gv[1][2], o1 = gv[0][2] - gv[2][0], o2 = gv[1][0] - gv[0][1];
+            const double om2 = o0 * o0 + o1 * o1 + o2 * o2;
+            const double wt = sw[qx] * sw[qy] * sw[qz] * wdet;
+            acc[0] += 0.5 * rho * v2 * wt;
+            acc[1] += 0.5 * rho * om2 * wt;
+            const double p = gm1 * (u[4] - 0.5 * rho * v2);
+            if constexpr (FULL) {
+                double S[3][3], dil = 0.0;
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                    for (int b = 0; b < 3; ++b) S[a][b] = 0.5 * (gv[a][b] + gv[b][a]);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) dil += gv[d][d];
+                double s2 = 0.0, sd2 = 0.0;
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                    for (int b = 0; b < 3; ++b) {
+                        const double dv = S[a][b] - (a == b ? dil / 3.0 : 0.0);
+                        s2 += S[a][b] * S[a][b];
+                        sd2 += dv * dv;
+                    }
+                // Sutherland's law in the nondimensional temperature (navier_stokes.cpp:241-300)
+                const double T = gam * ic.mach2 * (p / rho);
+                const double mu = ic.use_const_visc ? 1.0 * ic.const_visc
+                                                    : ((1.0 + ic.temp_ratio) / (T + ic.temp_ratio)) * pow(T, 1.5);
+                double r2 = 0.0;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    double xd;
+                    if constexpr (CURV) xd = u[5 + d];
+                    else xd = o0rg[d] + h * sx[d == 0 ? qx : d == 1 ? qy : qz];
+                    r2 += xd * xd;
                 }
-                const double b = sB[qz * N1 + k], db = sdB[qz * N1 + k];
-                v += b * a0; gx += b * a1; gy += b * a2; gz += db * a0;
+                acc[2] += p * dil * wt;
+                acc[3] += mu * sd2 * wt;
+                acc[4] += mu * s2 * wt;
+                acc[5] += 0.5 * v2 * wt;
+                acc[6] += 0.5 * om2 * wt;
+                acc[8] += 0.5 * r2 * sqrt(om2) * wt;
+#pragma unroll
+                for (int k = 0; k < N1; ++k) {
+                    const double pk = sP[k * NE + qz];
+                    zp[0][k] += pk * o0; zp[1][k] += pk * o1; zp[2][k] += pk * o2;
+                }
             }
-            u[s] = v; g[s][0] = gx; g[s][1] = gy; g[s][2] = gz;
+            const double c = sqrt(p * gam / rho);
+            const double ws = sqrt(v2) + c;
+            wave = ws > wave ? ws : wave;
         }
-        double wdet = detj;
-        if constexpr (CURV) {
-            // J[m][j] = dX_m/dxi_j; physical gradient = reference gradient times J^-1
-            double J[3][3];
+        if constexpr (FULL) {
 #pragma unroll
-            for (int m = 0; m < 3; ++m)
+            for (int c = 0; c < 3; ++c)
 #pragma unroll
-                for (int j = 0; j < 3; ++j) J[m][j] = g[5 + m][j];
-            const double dj = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) -
-                              J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
-                              J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
-            double I[3][3];
-            I[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) / dj;
-            I[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / dj;
-            I[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / dj;
-            I[1][0] = (J[1][2] * J[2][0] - J[1][0] * J[2][2]) / dj;
-            I[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / dj;
-            I[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / dj;
-            I[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) / dj;
-            I[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / dj;
-            I[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / dj;
-#pragma unroll
-            for (int s = 0; s < 5; ++s) {
-                const double r0 = g[s][0], r1 = g[s][1], r2 = g[s][2];
-#pragma unroll
-                for (int d = 0; d < 3; ++d) g[s][d] = r0 * I[0][d] + r1 * I[1][d] + r2 * I[2][d];
+                for (int k = 0; k < N1; ++k) sWz[(c * NE * NE + col) * N1 + k] = zp[c][k];
+        }
+    }
+    if constexpr (FULL) {
+        __syncthreads();
+        // projection in y: sWy[c][(k*N1 + j)*NE + qx] = sum_qy P[j][qy] sWz[c][qy*NE + qx][k]
+        for (int i = tid; i < 3 * N1 * N1 * NE; i += blockDim.x) {
+            const int qx = i % NE, j = (i / NE) % N1, k = (i / (NE * N1)) % N1, c = i / (NE * N1 * N1);
+            double v = 0.0;
+            for (int qy = 0; qy < NE; ++qy) v += sP[j * NE + qy] * sWz[(c * NE * NE + qy * NE + qx) * N1 + k];
+            sWy[i] = v;
+        }
+        __syncthreads();
+        // projection in x: coefficients into the (no longer needed) state slots 0..2 of sU
+        for (int i = tid; i < 3 * NP; i += blockDim.x) {
+            const int a = i % N1, kj = (i / N1) % (N1 * N1), c = i / NP;
+            double v = 0.0;
+            for (int qx = 0; qx < NE; ++qx) v += sP[a * NE + qx] * sWy[(c * N1 * N1 + kj) * NE + qx];
+            sU[i] = v;
+        }
+        __syncthreads();
+        // x-contraction of the projected vorticity into slots 0..2 (coordinates stay in 5..7)
+        for (int i = tid; i < 3 * NT2; i += blockDim.x) {
+            const int qx = i % NE, kj = (i / NE) % (N1 * N1), s = i / NT2;
+            double v = 0.0, dv = 0.0;
+            for (int a = 0; a < N1; ++a) {
+                const double u = sU[s * NP + kj * N1 + a];
+                v += sB[qx * N1 + a] * u;
+                dv += sdB[qx * N1 + a] * u;
             }
-            wdet = dj;
-        } else {
-#pragma unroll
-            for (int s = 0; s < 5; ++s)
-#pragma unroll
-                for (int d = 0; d < 3; ++d) g[s][d] *= inv_h;
+            sT0[i] = v;
+            sT1[i] = dv;
         }
-        const double rho = u[0];
-        double v[3], v2 = 0.0;
+        __syncthreads();
+        constexpr int NF2 = CURV ? 6 : 3;
+        int fld2[NF2];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) { v[d] = u[1 + d] / rho; v2 += v[d] * v[d]; }
-        double gv[3][3];
+        for (int f = 0; f < NF2; ++f) fld2[f] = f < 3 ? f : f + 2;
+        double pal = 0.0;
+        for (int pt = tid; pt < NE * NE * NE; pt += blockDim.x) {
+            const int qx = pt % NE, qy = (pt / NE) % NE, qz = pt / (NE * NE);
+            double u[NF2], g[NF2][3];
+            point_fields<N1, NE, NF2>(sT0, sT1, sB, sdB, fld2, qx, qy, qz, u, g);
+            double wdet = detj;
+            if constexpr (CURV) {
+                const double gx[3][3] = {{g[3][0], g[3][1], g[3][2]}, {g[4][0], g[4][1], g[4][2]},
+                                         {g[5][0], g[5][1], g[5][2]}};
+                double I[3][3];
+                wdet = inverse_jacobian(gx, I);
+                to_physical<NF2>(g, 3, I);
+            } else {
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
+                for (int s = 0; s < 3; ++s)
 #pragma unroll
-            for (int d = 0; d < 3; ++d) gv[a][d] = (g[1 + a][d] - v[a] * g[0][d]) / rho;
-        const double o0 = gv[2][1] - gv[1][2], o1 = gv[0][2] - gv[2][0], o2 = gv[1][0] - gv[0][1];
-        const double wt = sw[qx] * sw[qy] * sw[qz] * wdet;
-        ke += 0.5 * rho * v2 * wt;
-        ens += 0.5 * rho * (o0 * o0 + o1 * o1 + o2 * o2) * wt;
-        const double p = gm1 * (u[4] - 0.5 * rho * v2);
-        const double c = sqrt(p * gam / rho);
-        const double ws = sqrt(v2) + c;
-        wave = ws > wave ? ws : wave;
+                    for (int d = 0; d < 3; ++d) g[s][d] *= inv_h;
+            }
+            double gg = 0.0;
+#pragma unroll
+            for (int s = 0; s < 3; ++s)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) gg += g[s][d] * g[s][d];
+            pal += 0.5 * gg * sw[qx] * sw[qy] * sw[qz] * wdet;
+        }
+        acc[7] = pal;
     }
     // block reduction in a fixed order (warp shuffles, then warp 0)
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        ke += __shfl_down_sync(0xffffffffu, ke, o);
-        ens += __shfl_down_sync(0xffffffffu, ens, o);
+#pragma unroll
+        for (int i = 0; i < NACC; ++i) acc[i] += __shfl_down_sync(0xffffffffu, acc[i], o);
         const double wo = __shfl_down_sync(0xffffffffu, wave, o);
         wave = wo > wave ? wo : wave;
     }
     const int warp = tid >> 5, lane = tid & 31, nw = (blockDim.x + 31) >> 5;
-    if (lane == 0) { red[0][warp] = ke; red[1][warp] = ens; red[2][warp] = wave; }
+    if (lane == 0) {
+#pragma unroll
+        for (int i = 0; i < NACC; ++i) red[i][warp] = acc[i];
+        red[NQ - 1][warp] = wave;
+    }
     __syncthreads();
     if (tid == 0) {
-        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-        for (int w = 0; w < nw; ++w) { a0 += red[0][w]; a1 += red[1][w]; a2 = red[2][w] > a2 ? red[2][w] : a2; }
-        partial[3 * cell + 0] = a0; partial[3 * cell + 1] = a1; partial[3 * cell + 2] = a2;
+        double a[NQ];
+#pragma unroll
+        for (int i = 0; i < NQ; ++i) a[i] = 0.0;
+        for (int w = 0; w < nw; ++w) {
+#pragma unroll
+            for (int i = 0; i < NACC; ++i) a[i] += red[i][w];
+            a[NQ - 1] = red[NQ - 1][w] > a[NQ - 1] ? red[NQ - 1][w] : a[NQ - 1];
+        }
+#pragma unroll
+        for (int i = 0; i < NQ; ++i) partial[(size_t)NQ * cell + i] = a[i];
     }
 }
 

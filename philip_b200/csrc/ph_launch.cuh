@@ -18,11 +18,12 @@ cudaError_t launch_aux(const double* U, const int* nbr, const OpTab* ops, int nc
 template <int N1>
 cudaError_t launch_inverse_mass(const double* in, double* out, const OpTab* ops, int nc, double inv_detj,
                                 const double* metric, cudaStream_t s);
-// Taylor-Green integrals, per-cell partial sums
-// X: node coordinates [nc][3][NP] of curvilinear cells, nullptr on affine meshes
+// Taylor-Green integrals, per-cell partial sums (integral_partials<full>() per cell)
+// X: node coordinates [nc][3][NP] of curvilinear cells, nullptr on affine meshes;
+// origin: lower corner [nc][3] of affine cells (the full set's angular momentum)
 template <int N1>
-cudaError_t launch_integrals(const double* U, const double* X, const IntegralTab* tab, int nc, double h, double gam,
-                             double gm1, double* partial, cudaStream_t s);
+cudaError_t launch_integrals(const double* U, const double* X, const double* origin, const IntegralTab* tab, int nc,
+                             const IntegralConst& ic, bool full, double* partial, cudaStream_t s);
 // Batched (many-solve) stage: split-form Euler tiles of several discretisations of the same
 // order. `variant` selects the cells-per-CTA tile shape (batched_shape lists them); grid <= 0
 // sizes the persistent grid to the resident CTAs of the whole GPU.

@@ -144,6 +144,14 @@ class DGStrong:
         _lib.check(self.L.ph_integrals(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
         return out
 
+    def integrated_quantities(self) -> np.ndarray:
+        """The nine quantities of PeriodicTurbulence::compute_and_update_integrated_quantities
+        (periodic_turbulence.cpp:439-672) in IntegratedQuantitiesEnum order
+        (_lib.INTEGRATED_QUANTITIES), each over the domain volume."""
+        out = np.zeros(len(_lib.INTEGRATED_QUANTITIES))
+        _lib.check(self.L.ph_integrated_quantities(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out
+
     def status(self) -> int:
         v = ctypes.c_uint32(0)
         _lib.check(self.L.ph_status(self._h, ctypes.byref(v)))
@@ -363,6 +371,28 @@ class FlowSolver:
         })
         with open(base + ".prm", "w") as f:   # written last, after the data it points to
             f.write(prm.to_text())
+
+    def unsteady_data_row(self) -> dict:
+        """One row of PeriodicTurbulence's unsteady data table (compute_unsteady_data_and_write_to_table,
+        periodic_turbulence.cpp:925-972): the integrated quantities and the dissipation rates
+        derived from them, under the reference's column names; the viscous-only columns only
+        for Navier-Stokes, the angular momentum only when asked for."""
+        q = dict(zip(_lib.INTEGRATED_QUANTITIES, self.dg.integrated_quantities()))
+        viscous = self.parameters.get("pde_type") != "euler"
+        re = float(self.parameters.get("navier_stokes/reynolds_number_inf"))
+        row = {"time": self.ode_solver.current_time,
+               "kinetic_energy": q["kinetic_energy"], "enstrophy": q["enstrophy"]}
+        if viscous:
+            row["eps_vorticity"] = 2.0 * q["enstrophy"] / re
+        row["eps_pressure"] = -q["pressure_dilatation"]
+        if viscous:
+            row["eps_strain"] = 2.0 * q["viscosity_times_strain_rate_tensor_magnitude_sqr"] / re
+            row["eps_dev_strain"] = 2.0 * q["viscosity_times_deviatoric_strain_rate_tensor_magnitude_sqr"] / re
+        for k in ("incompressible_kinetic_energy", "incompressible_enstrophy", "incompressible_palinstrophy"):
+            row[k] = q[k]
+        if self.parameters.get("flow_solver/dipole_wall_collision/do_compute_angular_momentum").lower() == "true":
+            row["angular_momentum"] = q["angular_momentum"]
+        return row
 
     def _grid_spacing(self) -> float:
         left, right = self.parameters.grid_bounds
