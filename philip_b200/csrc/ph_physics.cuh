@@ -32,11 +32,12 @@ struct PhysConst {
 };
 
 template <typename R> struct Cst {
-    R gam, gm1, mach2, temp_ratio, inv_re, prandtl, const_visc, kappa_fac;
+    R gam, gm1, mach2, temp_ratio, inv_re, prandtl, const_visc, kappa_fac, inv2gm1;
     __device__ __forceinline__ void load(const PhysConst& c) {
         gam = (R)c.gam; gm1 = (R)c.gm1; mach2 = (R)c.mach2; temp_ratio = (R)c.temp_ratio;
         inv_re = (R)c.inv_re; prandtl = (R)c.prandtl; const_visc = (R)c.const_visc;
         kappa_fac = (R)(1.0 / (c.gm1 * c.mach2 * c.prandtl));
+        inv2gm1 = (R)(0.5 / c.gm1);
     }
 };
 
@@ -70,22 +71,29 @@ __device__ __forceinline__ float rcp_approx(float x) {
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
 }
-template <typename R> __device__ __forceinline__ R qdiv(R a, R b);
-template <> __device__ __forceinline__ double qdiv<double>(double a, double b) {
+template <typename R> __device__ __forceinline__ R qrcp(R b);
+template <> __device__ __forceinline__ double qrcp<double>(double b) {
 #if PH_FAST_DIV == 0
-    return a / b;
+    return 1.0 / b;
 #else
     double r = rcp_approx(b);
     r = fma(r, fma(-b, r, 1.0), r);
     r = fma(r, fma(-b, r, 1.0), r);
-    return a * r;
+    return r;
 #endif
 }
-template <> __device__ __forceinline__ float qdiv<float>(float a, float b) {
+template <> __device__ __forceinline__ float qrcp<float>(float b) {
+#if PH_FAST_DIV == 0
+    return 1.0f / b;
+#else
+    return rcp_approx(b);
+#endif
+}
+template <typename R> __device__ __forceinline__ R qdiv(R a, R b) {
 #if PH_FAST_DIV == 0
     return a / b;
 #else
-    return a * rcp_approx(b);
+    return a * qrcp<R>(b);
 #endif
 }
 
@@ -161,35 +169,79 @@ __device__ __forceinline__ R log_mean(R a, R b, R la, R lb) {
     return qdiv<R>(d, la - lb);
 }
 
+// The series of log_mean: F(u) = 1 + u/3 + u^2/5 + u^3/7, Horner form.
+template <typename R> __device__ __forceinline__ R log_mean_series(R u) {
+    return R(1) + u * (R(1.0 / 3.0) + u * (R(1.0 / 5.0) + u * R(1.0 / 7.0)));
+}
+
+// Averages of the Chandrashekar flux (Euler::compute_chandrashekar_flux, euler.cpp): the
+// logarithmic mean rho_log of the density, p_hat = mean(rho) / (2 mean(b)) and the scalar
+// part of the enthalpy, h0 = 1 / (2 (gamma - 1) b_log) + p_hat / rho_log - mean(|v|^2) / 2.
+// Both logarithmic means follow log_mean (the same branch test, series for u < 1e-2), with
+// the quotients rearranged to share reciprocals: three when both means take the series
+// branch (smooth flow), at most five, where the plain form divides six times.
+template <typename R>
+__device__ __forceinline__ void ch_means(const NodeQ<R>& i, const NodeQ<R>& j, const Cst<R>& c, R& rho_log,
+                                         R& p_hat, R& h0) {
+    const R srho = i.rho + j.rho, drho = i.rho - j.rho;
+    const R sb = i.b + j.b, db = i.b - j.b;
+    const R rsb = qrcp<R>(sb);
+    p_hat = R(0.5) * srho * rsb;
+    R inv_blog;
+    {
+        const R f = db * rsb, u = f * f;
+        if (u < R(1.0e-2)) inv_blog = R(2) * log_mean_series<R>(u) * rsb;
+        else inv_blog = (i.lb - j.lb) * qrcp<R>(db);
+    }
+    R inv_rlog;
+    {
+        const R rs = qrcp<R>(srho);
+        const R f = drho * rs, u = f * f;
+        if (u < R(1.0e-2)) {
+            const R F = log_mean_series<R>(u);
+            inv_rlog = R(2) * F * rs;
+            rho_log = R(0.5) * srho * qrcp<R>(F);
+        } else {
+            const R dl = i.la - j.la;
+            rho_log = drho * qrcp<R>(dl);
+            inv_rlog = dl * qrcp<R>(drho);
+        }
+    }
+    h0 = inv_blog * c.inv2gm1 + p_hat * inv_rlog - R(0.25) * (i.vsq + j.vsq);
+}
+
 // Two-point flux component along direction d (compile time) for all 5 equations.
 template <typename R, int d>
 __device__ __forceinline__ void two_point_dir(const NodeQ<R>& i, const NodeQ<R>& j, int tp,
                                               const Cst<R>& c, R F[5]) {
-    if (tp == TP_CH || tp == TP_RA) {
+    if (tp == TP_CH) {
+        R rho_log, p_hat, h0;
+        ch_means<R>(i, j, c, rho_log, p_hat, h0);
+        R va[3], vsq = R(0);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { va[k] = R(0.5) * (i.v[k] + j.v[k]); vsq += va[k] * va[k]; }
+        const R m = rho_log * va[d];
+        F[0] = m;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) F[1 + k] = m * va[k];
+        F[1 + d] += p_hat;
+        F[4] = m * (h0 + vsq);
+    } else if (tp == TP_RA) {
         const R rho_log = log_mean<R>(i.a, j.a, i.la, j.la);
         const R b_log = log_mean<R>(i.b, j.b, i.lb, j.lb);
         R va[3], vsq = R(0);
 #pragma unroll
         for (int k = 0; k < 3; ++k) { va[k] = R(0.5) * (i.v[k] + j.v[k]); vsq += va[k] * va[k]; }
-        R p_hat, H;
-        if (tp == TP_CH) {
-            // 1/(2 b_log gm1) + p_hat/rho_log over one common denominator
-            p_hat = qdiv<R>(i.rho + j.rho, R(2) * (i.b + j.b));
-            const R g2b = R(2) * b_log * c.gm1;
-            H = qdiv<R>(rho_log + g2b * p_hat, g2b * rho_log) + vsq;
-        } else {
-            p_hat = R(0.5) * (i.p + j.p);
-            const R gb = b_log * c.gm1;
-            H = qdiv<R>(rho_log + R(2) * gb * p_hat, gb * rho_log) + vsq;
-        }
+        const R p_hat = R(0.5) * (i.p + j.p);
+        const R gb = b_log * c.gm1;
+        R H = qdiv<R>(rho_log + R(2) * gb * p_hat, gb * rho_log) + vsq;
         H -= R(0.5) * (R(0.5) * (i.vsq + j.vsq));
         const R m = rho_log * va[d];
         F[0] = m;
 #pragma unroll
         for (int k = 0; k < 3; ++k) F[1 + k] = m * va[k];
         F[1 + d] += p_hat;
-        F[4] = m * H;
-        if (tp == TP_RA) F[4] -= R(0.5) * (i.p * i.v[d] + j.p * j.v[d]);
+        F[4] = m * H - R(0.5) * (i.p * i.v[d] + j.p * j.v[d]);
     } else if (tp == TP_IR) {
         const R z0a = R(0.5) * (i.a + j.a), z4a = R(0.5) * (i.b + j.b);
         const R l0 = log_mean<R>(i.a, j.a, i.la, j.la);
@@ -325,34 +377,36 @@ __device__ __forceinline__ void conv_num_flux(const R uL[5], const R uR[5], cons
 template <typename R>
 __device__ __forceinline__ void two_point_n(const NodeQ<R>& i, const NodeQ<R>& j, const R n[3], int tp,
                                             const Cst<R>& c, R F[5]) {
-    if (tp == TP_CH || tp == TP_RA) {
+    if (tp == TP_CH) {
+        R rho_log, p_hat, h0;
+        ch_means<R>(i, j, c, rho_log, p_hat, h0);
+        R va[3], vsq = R(0), vn = R(0);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { va[k] = R(0.5) * (i.v[k] + j.v[k]); vsq += va[k] * va[k]; vn += va[k] * n[k]; }
+        const R m = rho_log * vn;
+        F[0] = m;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) F[1 + k] = m * va[k] + p_hat * n[k];
+        F[4] = m * (h0 + vsq);
+    } else if (tp == TP_RA) {
         const R rho_log = log_mean<R>(i.a, j.a, i.la, j.la);
         const R b_log = log_mean<R>(i.b, j.b, i.lb, j.lb);
         R va[3], vsq = R(0), vn = R(0);
 #pragma unroll
         for (int k = 0; k < 3; ++k) { va[k] = R(0.5) * (i.v[k] + j.v[k]); vsq += va[k] * va[k]; vn += va[k] * n[k]; }
-        R p_hat, H;
-        if (tp == TP_CH) {
-            p_hat = qdiv<R>(i.rho + j.rho, R(2) * (i.b + j.b));
-            const R g2b = R(2) * b_log * c.gm1;
-            H = qdiv<R>(rho_log + g2b * p_hat, g2b * rho_log) + vsq;
-        } else {
-            p_hat = R(0.5) * (i.p + j.p);
-            const R gb = b_log * c.gm1;
-            H = qdiv<R>(rho_log + R(2) * gb * p_hat, gb * rho_log) + vsq;
-        }
+        const R p_hat = R(0.5) * (i.p + j.p);
+        const R gb = b_log * c.gm1;
+        R H = qdiv<R>(rho_log + R(2) * gb * p_hat, gb * rho_log) + vsq;
         H -= R(0.5) * (R(0.5) * (i.vsq + j.vsq));
         const R m = rho_log * vn;
         F[0] = m;
 #pragma unroll
         for (int k = 0; k < 3; ++k) F[1 + k] = m * va[k] + p_hat * n[k];
         F[4] = m * H;
-        if (tp == TP_RA) {
-            R vni = R(0), vnj = R(0);
+        R vni = R(0), vnj = R(0);
 #pragma unroll
-            for (int k = 0; k < 3; ++k) { vni += i.v[k] * n[k]; vnj += j.v[k] * n[k]; }
-            F[4] -= R(0.5) * (i.p * vni + j.p * vnj);
-        }
+        for (int k = 0; k < 3; ++k) { vni += i.v[k] * n[k]; vnj += j.v[k] * n[k]; }
+        F[4] -= R(0.5) * (i.p * vni + j.p * vnj);
     } else if (tp == TP_IR) {
         const R z0a = R(0.5) * (i.a + j.a), z4a = R(0.5) * (i.b + j.b);
         const R l0 = log_mean<R>(i.a, j.a, i.la, j.la);
