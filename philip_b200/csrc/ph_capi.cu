@@ -673,12 +673,12 @@ int dispatch_aux(ph_ctx* c, const double* U) {
     const double inv_h = 1.0 / c->h;
     timer_begin(c);
     switch (c->N1) {
-    case 2: e = ph::launch_aux<2>(U, c->d_nbr, c->d_ops, c->nc, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
-    case 3: e = ph::launch_aux<3>(U, c->d_nbr, c->d_ops, c->nc, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
-    case 4: e = ph::launch_aux<4>(U, c->d_nbr, c->d_ops, c->nc, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
-    case 5: e = ph::launch_aux<5>(U, c->d_nbr, c->d_ops, c->nc, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
-    case 6: e = ph::launch_aux<6>(U, c->d_nbr, c->d_ops, c->nc, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
-    case 7: e = ph::launch_aux<7>(U, c->d_nbr, c->d_ops, c->nc, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
+    case 2: e = ph::launch_aux<2>(U, c->d_nbr, c->h_ops, c->nc, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
+    case 3: e = ph::launch_aux<3>(U, c->d_nbr, c->h_ops, c->nc, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
+    case 4: e = ph::launch_aux<4>(U, c->d_nbr, c->h_ops, c->nc, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
+    case 5: e = ph::launch_aux<5>(U, c->d_nbr, c->h_ops, c->nc, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
+    case 6: e = ph::launch_aux<6>(U, c->d_nbr, c->h_ops, c->nc, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
+    case 7: e = ph::launch_aux<7>(U, c->d_nbr, c->h_ops, c->nc, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
     default: return fail(PH_ERR_UNSUPPORTED, "polynomial degree outside 1..6");
     }
     if (e != cudaSuccess) return fail(PH_ERR_CUDA, std::string("aux launch: ") + cudaGetErrorString(e));
@@ -1342,12 +1342,12 @@ extern "C" int ph_residual_noalloc(const ph_mesh_desc* mesh, const ph_params* pr
     cudaError_t e = cudaSuccess;
     if (visc) {
         switch (N1) {
-        case 2: e = ph::launch_aux<2>(U, sym.nbr, sym.ops, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
-        case 3: e = ph::launch_aux<3>(U, sym.nbr, sym.ops, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
-        case 4: e = ph::launch_aux<4>(U, sym.nbr, sym.ops, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
-        case 5: e = ph::launch_aux<5>(U, sym.nbr, sym.ops, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
-        case 6: e = ph::launch_aux<6>(U, sym.nbr, sym.ops, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
-        default: e = ph::launch_aux<7>(U, sym.nbr, sym.ops, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
+        case 2: e = ph::launch_aux<2>(U, sym.nbr, tab, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
+        case 3: e = ph::launch_aux<3>(U, sym.nbr, tab, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
+        case 4: e = ph::launch_aux<4>(U, sym.nbr, tab, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
+        case 5: e = ph::launch_aux<5>(U, sym.nbr, tab, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
+        case 6: e = ph::launch_aux<6>(U, sym.nbr, tab, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
+        default: e = ph::launch_aux<7>(U, sym.nbr, tab, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
         }
         if (e != cudaSuccess) return fail(PH_ERR_CUDA, std::string("aux launch: ") + cudaGetErrorString(e));
     }

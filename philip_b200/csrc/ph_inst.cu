@@ -156,7 +156,7 @@ void stage_launch_shape(int fp32, bool visc, bool split, int* threads, int* cpc,
 }
 
 template <typename R, int N1>
-static cudaError_t launch_aux_prec(const double* U, const int* nbr, const OpTab* ops, int nc, double inv_h,
+static cudaError_t launch_aux_prec(const double* U, const int* nbr, const OpTab& ops, int nc, double inv_h,
                                    const PhysConst& pc, void* Fv, cudaStream_t s) {
     constexpr int CPC = cells_per_cta<N1>();
     using L = AuxLayout<N1, CPC>;
@@ -170,12 +170,15 @@ static cudaError_t launch_aux_prec(const double* U, const int* nbr, const OpTab*
         if (e != cudaSuccess) return e;
         configured[dev] = true;
     }
-    kern<<<(nc + CPC - 1) / CPC, L::NT, bytes, s>>>(U, nbr, ops, nc, inv_h, pc, static_cast<R*>(Fv));
+    AuxCoef<R> co{};
+    for (int i = 0; i < MAXN1 * MAXN1; ++i) co.D[i] = (R)ops.D[i];
+    co.inv_wend = R(1) / (R)ops.w[0];
+    kern<<<(nc + CPC - 1) / CPC, L::NT, bytes, s>>>(U, nbr, nc, (R)inv_h, pc, co, static_cast<R*>(Fv));
     return cudaGetLastError();
 }
 
 template <int N1>
-cudaError_t launch_aux(const double* U, const int* nbr, const OpTab* ops, int nc, double inv_h,
+cudaError_t launch_aux(const double* U, const int* nbr, const OpTab& ops, int nc, double inv_h,
                        const PhysConst& pc, int fp32, void* Fv, cudaStream_t s) {
     return fp32 ? launch_aux_prec<float, N1>(U, nbr, ops, nc, inv_h, pc, Fv, s)
                 : launch_aux_prec<double, N1>(U, nbr, ops, nc, inv_h, pc, Fv, s);
@@ -220,7 +223,7 @@ template void stage_launch_shape<PH_N1>(int, bool, bool, int*, int*, size_t*);
 template cudaError_t launch_stage_batched<PH_N1>(const StageArgs*, const BatchTile*, int, int, bool, bool, int, int,
                                                  cudaStream_t);
 template bool batched_shape<PH_N1>(int, bool, int, int*, int*, size_t*, int*);
-template cudaError_t launch_aux<PH_N1>(const double*, const int*, const OpTab*, int, double, const PhysConst&, int,
+template cudaError_t launch_aux<PH_N1>(const double*, const int*, const OpTab&, int, double, const PhysConst&, int,
                                        void*, cudaStream_t);
 template cudaError_t launch_inverse_mass<PH_N1>(const double*, double*, const OpTab*, int, double, const double*,
                                                 cudaStream_t);

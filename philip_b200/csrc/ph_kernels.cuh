@@ -616,6 +616,53 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
         }
     }
     __syncthreads();
+    if (a.mode == 2) {
+        // Butcher RK stage: the thread's inputs (u_n and the running sum) for all its DOFs
+        // are loaded before its first store, so that the loads are in flight together
+        // (the outputs may alias the inputs, but only DOF by DOF)
+        constexpr int TOT = CPC * 5 * NP, PER = (TOT + NT - 1) / NT;
+        double un[PER], bs[PER];
+#pragma unroll
+        for (int r = 0; r < PER; ++r) {
+            const int it = tid + r * NT;
+            un[r] = bs[r] = 0.0;
+            if (it < TOT && cell0 + it / (5 * NP) < a.nc) {
+                const size_t dof = (size_t)cell0 * 5 * NP + it;
+                un[r] = a.Un[dof];
+                bs[r] = a.acc_in ? a.acc_in[dof] : (a.inc_mode ? 0.0 : un[r]);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < PER; ++r) {
+            const int it = tid + r * NT;
+            if (it >= TOT) break;
+            const int cell = cell0 + it / (5 * NP);
+            if (cell >= a.nc) break;
+            const int node = (it % (5 * NP)) % NP;
+            const size_t dof = (size_t)cell0 * 5 * NP + it;
+            const double G = (double)sA[it];
+            const double k = CURV ? G * __ldg(&a.metric[((size_t)cell * 10 + 9) * NP + node]) : G * a.inv_h;
+            const double sum = bs[r] + a.c_acc * k;
+            if (a.acc_out) a.acc_out[dof] = sum;
+            if (a.final_out) {
+                if (a.comp) {   // compensated u_{n+1} = u_n + increment
+                    const double y = sum - a.comp[dof];
+                    const double t = un[r] + y;
+                    a.comp[dof] = (t - un[r]) - y;
+                    a.final_out[dof] = t;
+                } else {
+                    a.final_out[dof] = a.inc_mode ? un[r] + sum : sum;
+                }
+            }
+            if (a.next) {
+                const double cin = a.carry_in ? a.carry_in[dof] : 0.0;
+                a.next[dof] = (cin + a.a_next * k) * a.dt + un[r];
+            }
+            if (a.carry_out) a.carry_out[dof] = a.a_carry * k;
+        }
+        return;
+    }
+    // residual (mode 0), k = M^-1 R (mode 1), low-storage stage (mode 3)
     double err2 = 0.0;   // low-storage error estimate: this thread's share of the tile
     for (int it = tid; it < CPC * 5 * NP; it += NT) {
         const int c = it / (5 * NP);
@@ -665,25 +712,6 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
             }
             continue;
         }
-        const double un = a.Un[dof];
-        const double base = a.acc_in ? a.acc_in[dof] : (a.inc_mode ? 0.0 : un);
-        const double sum = base + a.c_acc * k;
-        if (a.acc_out) a.acc_out[dof] = sum;
-        if (a.final_out) {
-            if (a.comp) {   // compensated u_{n+1} = u_n + increment
-                const double y = sum - a.comp[dof];
-                const double t = un + y;
-                a.comp[dof] = (t - un) - y;
-                a.final_out[dof] = t;
-            } else {
-                a.final_out[dof] = a.inc_mode ? un + sum : sum;
-            }
-        }
-        if (a.next) {
-            const double cin = a.carry_in ? a.carry_in[dof] : 0.0;
-            a.next[dof] = (cin + a.a_next * k) * a.dt + un;
-        }
-        if (a.carry_out) a.carry_out[dof] = a.a_carry * k;
     }
     if (a.mode == 3 && a.err_partial) {   // tile sum of the squared scaled error, fixed order
         __shared__ double red[32];
@@ -738,37 +766,64 @@ residual_kernel_batched(const StageArgs* __restrict__ inst, const BatchTile* __r
 // needs: its volume divergence and its face-normal component on each face
 // (viscous_terms_per_cell).
 // ------------------------------------------------------------------------------------
+// Two forms of the same arithmetic, chosen per precision and order from timings on B200:
+//  line form (FP64, p >= 4): one thread per (direction, state, line) differentiates the
+//    line held in registers; every coefficient is a parameter-bank operand, the gradient
+//    and then the nodal flux share one buffer, the divergence runs direction by direction;
+//  node form (FP32, and FP64 at p <= 3): one thread per node, coefficients from shared
+//    memory (fewer barriers and less shared memory, which wins at low order and in FP32).
+// Both sum every node's terms in the same order (over l, then over directions).
+template <typename R, int N1> __host__ __device__ constexpr bool aux_line_form() {
+    return sizeof(R) == 8 && N1 >= 5;
+}
+
 template <int N1, int CPC>
 struct AuxLayout {
     static constexpr int NP = N1 * N1 * N1, NF = N1 * N1;
     static constexpr int NT = ((CPC * NP + 31) / 32) * 32 > 512 ? 512 : ((CPC * NP + 31) / 32) * 32;
+    // state, neighbour traces, then (line form) the gradient / nodal flux or (node form) the
+    // differentiation matrix and the nodal flux
     template <typename R>
     static constexpr size_t bytes() {
-        return sizeof(R) * ((size_t)CPC * 5 * NP + (size_t)CPC * 6 * 5 * NF + N1 * N1 + N1 + (size_t)CPC * 12 * NP);
+        return sizeof(R) * ((size_t)CPC * 5 * NP + (size_t)CPC * 6 * 5 * NF +
+                            (aux_line_form<R, N1>() ? (size_t)CPC * 15 * NP : N1 * N1 + (size_t)CPC * 12 * NP));
     }
 };
 
+// The 1-D differentiation matrix and the lifting weight 1/w_end of the auxiliary kernel,
+// passed by value (in the line form each coefficient is then a parameter-bank operand).
+template <typename R> struct AuxCoef {
+    R D[MAXN1 * MAXN1];   // D[pos][l] = l_l'(x_pos)
+    R inv_wend;
+};
+
+// node index of position pos along direction d on the line whose transverse coordinates
+// are (line % N1, line / N1) (the lower transverse direction first, as face node order)
+template <int N1> __device__ __forceinline__ int line_node(int d, int line, int pos) {
+    const int a = line % N1, b = line / N1;
+    return d == 0 ? node_of<N1>(pos, a, b) : d == 1 ? node_of<N1>(a, pos, b) : node_of<N1>(a, b, pos);
+}
+
 template <typename R, int N1, int CPC>
 __global__ void __launch_bounds__(AuxLayout<N1, CPC>::NT)
-aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, const OpTab* ops, int nc,
-           double inv_h, PhysConst pc, R* __restrict__ Fv) {
+aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, int nc, R inv_h, PhysConst pc,
+           AuxCoef<R> co, R* __restrict__ Fv) {
     using L = AuxLayout<N1, CPC>;
     constexpr int NP = L::NP, NF = L::NF, NT = L::NT;
+    constexpr int VT = viscous_terms_per_cell<N1>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    R* sU = reinterpret_cast<R*>(smem_raw);
-    R* sT = sU + CPC * 5 * NP;
-    R* sDm = sT + CPC * 6 * 5 * NF;
-    R* sW = sDm + N1 * N1;
-    R* sF = sW + N1;                        // [c][3 dirs x 4][NP] nodal viscous flux
+    R* sU = reinterpret_cast<R*>(smem_raw);   // [c][5][NP] state
+    R* sT = sU + CPC * 5 * NP;                // [c][face][5][NF] neighbour traces
     Cst<R> cst; cst.load(pc);
     const int tid = threadIdx.x;
     const int cell0 = blockIdx.x * CPC;
-    for (int i = tid; i < N1 * N1; i += NT) sDm[i] = (R)ops->D[(i / N1) * MAXN1 + (i % N1)];
-    for (int i = tid; i < N1; i += NT) sW[i] = (R)ops->w[i];
+    // loads unrolled so that all of a thread's loads are in flight before the first store
+#pragma unroll
     for (int it = tid; it < CPC * 5 * NP; it += NT) {
         int cell = cell0 + it / (5 * NP); if (cell >= nc) cell = nc - 1;
         sU[it] = (R)__ldg(&U[(size_t)cell * 5 * NP + it % (5 * NP)]);
     }
+#pragma unroll
     for (int it = tid; it < CPC * 6 * 5 * NF; it += NT) {
         const int fn = it % NF, s = (it / NF) % 5, f = (it / (5 * NF)) % 6, c = it / (30 * NF);
         int cell = cell0 + c; if (cell >= nc) cell = nc - 1;
@@ -776,80 +831,164 @@ aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, const OpTa
         const int nn = face_node_volume_index<N1>(f, fn, (f & 1) ? 0 : N1 - 1);
         sT[it] = (R)__ldg(&U[((size_t)cn * 5 + s) * NP + nn]);
     }
-    __syncthreads();
-    const R inv_wend = R(1) / sW[0];
-    const R ih = (R)inv_h;
-    for (int it = tid; it < CPC * NP; it += NT) {
-        const int c = it / NP, node = it % NP;
-        const int cell = cell0 + c;
-        if (cell >= nc) continue;
-        const int cx[3] = {node % N1, (node / N1) % N1, node / (N1 * N1)};
-        const R* u = sU + c * 5 * NP;
-        R g[5][3];
+    if constexpr (aux_line_form<R, N1>()) {
+        R* sG = sT + CPC * 6 * 5 * NF;   // [c][d][5][NP] gradient, later [c][d][4][NP] flux
+        __syncthreads();
+        // lifted gradient: D u along the line, the lifting u* - u = (u_ext - u)/2 at both ends
+        for (int task = tid; task < CPC * 15 * NF; task += NT) {
+            const int c = task / (15 * NF), r = task % (15 * NF);
+            const int line = r % NF, s = (r / NF) % 5, d = r / (5 * NF);
+            const R* u = sU + (c * 5 + s) * NP;
+            R v[N1];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            const int st = (d == 0) ? 1 : (d == 1) ? N1 : N1 * N1;
-            const int pos = cx[d];
-            const int base = node - pos * st;
-            const int t1 = (d == 0) ? 1 : 0, t2 = (d == 2) ? 1 : 2;
-            const int fn = cx[t2] * N1 + cx[t1];
+            for (int l = 0; l < N1; ++l) v[l] = u[line_node<N1>(d, line, l)];
+            const R ue0 = sT[((c * 6 + 2 * d) * 5 + s) * NF + line];
+            const R ue1 = sT[((c * 6 + 2 * d + 1) * 5 + s) * NF + line];
+            R* g = sG + (c * 15 + d * 5 + s) * NP;
 #pragma unroll
-            for (int s = 0; s < 5; ++s) {
-                R v = R(0);
+            for (int pos = 0; pos < N1; ++pos) {
+                R acc = R(0);
 #pragma unroll
-                for (int l = 0; l < N1; ++l) v += sDm[pos * N1 + l] * u[s * NP + base + l * st];
-                if (pos == 0) {
-                    const R ue = sT[((c * 6 + 2 * d) * 5 + s) * NF + fn];
-                    v += inv_wend * (-(R(0.5) * (u[s * NP + node] + ue) - u[s * NP + node]));
-                }
-                if (pos == N1 - 1) {
-                    const R ue = sT[((c * 6 + 2 * d + 1) * 5 + s) * NF + fn];
-                    v += inv_wend * ((R(0.5) * (u[s * NP + node] + ue) - u[s * NP + node]));
-                }
-                g[s][d] = v * ih;
+                for (int l = 0; l < N1; ++l) acc += co.D[pos * MAXN1 + l] * v[l];
+                if (pos == 0) acc += co.inv_wend * (-(R(0.5) * (v[0] + ue0) - v[0]));
+                if (pos == N1 - 1) acc += co.inv_wend * ((R(0.5) * (v[N1 - 1] + ue1) - v[N1 - 1]));
+                g[line_node<N1>(d, line, pos)] = acc * inv_h;
             }
         }
-        R un[5];
+        __syncthreads();
+        // viscous flux per node; it replaces the node's own gradient entries
+        for (int it = tid; it < CPC * NP; it += NT) {
+            const int c = it / NP, node = it % NP;
+            R g[5][3];
 #pragma unroll
-        for (int s = 0; s < 5; ++s) un[s] = u[s * NP + node];
-        R F[3][4];
-        viscous_flux<R>(un, g, pc.use_const_visc, cst, F, 7, nullptr);
+            for (int d = 0; d < 3; ++d)
 #pragma unroll
-        for (int d = 0; d < 3; ++d)
+                for (int s = 0; s < 5; ++s) g[s][d] = sG[(c * 15 + d * 5 + s) * NP + node];
+            R un[5];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) sF[(c * 12 + d * 4 + k) * NP + node] = F[d][k];
-    }
-    __syncthreads();
-    // volume divergence sum_d D_d F_d and the face-normal blocks
-    for (int it = tid; it < CPC * NP; it += NT) {
-        const int c = it / NP, node = it % NP;
-        const int cell = cell0 + c;
-        if (cell >= nc) continue;
-        const int cx[3] = {node % N1, (node / N1) % N1, node / (N1 * N1)};
-        const R* Fc = sF + c * 12 * NP;
-        R* out = Fv + (size_t)cell * viscous_terms_per_cell<N1>();
-        R div[4] = {R(0), R(0), R(0), R(0)};
+            for (int s = 0; s < 5; ++s) un[s] = sU[(c * 5 + s) * NP + node];
+            R F[3][4];
+            viscous_flux<R>(un, g, pc.use_const_visc, cst, F, 7, nullptr);
 #pragma unroll
+            for (int d = 0; d < 3; ++d)
+#pragma unroll
+                for (int k = 0; k < 4; ++k) sG[(c * 15 + d * 4 + k) * NP + node] = F[d][k];
+        }
+        // divergence sum_d D_d F_d into the state's rows (the state is no longer read), one
+        // direction after the other, one thread per (component, line)
+#pragma unroll 1
         for (int d = 0; d < 3; ++d) {
-            const int st = (d == 0) ? 1 : (d == 1) ? N1 : N1 * N1;
-            const int pos = cx[d];
-            const int base = node - pos * st;
+            __syncthreads();
+            for (int task = tid; task < CPC * 4 * NF; task += NT) {
+                const int c = task / (4 * NF), r = task % (4 * NF);
+                const int line = r % NF, k = r / NF;
+                const R* f = sG + (c * 15 + d * 4 + k) * NP;
+                R* dv = sU + (c * 4 + k) * NP;
+                R v[N1];
 #pragma unroll
-            for (int l = 0; l < N1; ++l) {
-                const R coef = sDm[pos * N1 + l];
+                for (int l = 0; l < N1; ++l) v[l] = f[line_node<N1>(d, line, l)];
 #pragma unroll
-                for (int k = 0; k < 4; ++k) div[k] += coef * Fc[(d * 4 + k) * NP + base + l * st];
+                for (int pos = 0; pos < N1; ++pos) {
+                    const int node = line_node<N1>(d, line, pos);
+                    R acc = d == 0 ? R(0) : dv[node];
+#pragma unroll
+                    for (int l = 0; l < N1; ++l) acc += co.D[pos * MAXN1 + l] * v[l];
+                    dv[node] = acc;
+                }
             }
-            if (pos == 0 || pos == N1 - 1) {
-                const int f = 2 * d + (pos == 0 ? 0 : 1);
+        }
+        __syncthreads();
+        for (int it = tid; it < CPC * 4 * NP; it += NT) {
+            const int c = it / (4 * NP);
+            const int cell = cell0 + c;
+            if (cell >= nc) continue;
+            Fv[(size_t)cell * VT + it % (4 * NP)] = sU[c * 4 * NP + it % (4 * NP)];
+        }
+        for (int it = tid; it < CPC * 24 * NF; it += NT) {
+            const int c = it / (24 * NF), j = it % (24 * NF);
+            const int cell = cell0 + c;
+            if (cell >= nc) continue;
+            const int f = j / (4 * NF), k = (j / NF) % 4, fn = j % NF;
+            const int d = f >> 1;
+            const int node = line_node<N1>(d, fn, (f & 1) ? N1 - 1 : 0);
+            Fv[(size_t)cell * VT + 4 * NP + j] = sG[(c * 15 + d * 4 + k) * NP + node];
+        }
+    } else {
+        R* sDm = sT + CPC * 6 * 5 * NF;
+        R* sF = sDm + N1 * N1;   // [c][3 dirs x 4][NP] nodal viscous flux
+        for (int i = tid; i < N1 * N1; i += NT) sDm[i] = co.D[(i / N1) * MAXN1 + (i % N1)];
+        __syncthreads();
+        for (int it = tid; it < CPC * NP; it += NT) {
+            const int c = it / NP, node = it % NP;
+            const int cell = cell0 + c;
+            if (cell >= nc) continue;
+            const int cx[3] = {node % N1, (node / N1) % N1, node / (N1 * N1)};
+            const R* u = sU + c * 5 * NP;
+            R g[5][3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const int st = (d == 0) ? 1 : (d == 1) ? N1 : N1 * N1;
+                const int pos = cx[d];
+                const int base = node - pos * st;
                 const int t1 = (d == 0) ? 1 : 0, t2 = (d == 2) ? 1 : 2;
                 const int fn = cx[t2] * N1 + cx[t1];
 #pragma unroll
-                for (int k = 0; k < 4; ++k) out[4 * NP + (f * 4 + k) * NF + fn] = Fc[(d * 4 + k) * NP + node];
-            }
-        }
+                for (int s = 0; s < 5; ++s) {
+                    R v = R(0);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) out[k * NP + node] = div[k];
+                    for (int l = 0; l < N1; ++l) v += sDm[pos * N1 + l] * u[s * NP + base + l * st];
+                    if (pos == 0) {
+                        const R ue = sT[((c * 6 + 2 * d) * 5 + s) * NF + fn];
+                        v += co.inv_wend * (-(R(0.5) * (u[s * NP + node] + ue) - u[s * NP + node]));
+                    }
+                    if (pos == N1 - 1) {
+                        const R ue = sT[((c * 6 + 2 * d + 1) * 5 + s) * NF + fn];
+                        v += co.inv_wend * ((R(0.5) * (u[s * NP + node] + ue) - u[s * NP + node]));
+                    }
+                    g[s][d] = v * inv_h;
+                }
+            }
+            R un[5];
+#pragma unroll
+            for (int s = 0; s < 5; ++s) un[s] = u[s * NP + node];
+            R F[3][4];
+            viscous_flux<R>(un, g, pc.use_const_visc, cst, F, 7, nullptr);
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+#pragma unroll
+                for (int k = 0; k < 4; ++k) sF[(c * 12 + d * 4 + k) * NP + node] = F[d][k];
+        }
+        __syncthreads();
+        for (int it = tid; it < CPC * NP; it += NT) {
+            const int c = it / NP, node = it % NP;
+            const int cell = cell0 + c;
+            if (cell >= nc) continue;
+            const int cx[3] = {node % N1, (node / N1) % N1, node / (N1 * N1)};
+            const R* Fc = sF + c * 12 * NP;
+            R* out = Fv + (size_t)cell * VT;
+            R div[4] = {R(0), R(0), R(0), R(0)};
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const int st = (d == 0) ? 1 : (d == 1) ? N1 : N1 * N1;
+                const int pos = cx[d];
+                const int base = node - pos * st;
+#pragma unroll
+                for (int l = 0; l < N1; ++l) {
+                    const R coef = sDm[pos * N1 + l];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) div[k] += coef * Fc[(d * 4 + k) * NP + base + l * st];
+                }
+                if (pos == 0 || pos == N1 - 1) {
+                    const int f = 2 * d + (pos == 0 ? 0 : 1);
+                    const int t1 = (d == 0) ? 1 : 0, t2 = (d == 2) ? 1 : 2;
+                    const int fn = cx[t2] * N1 + cx[t1];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) out[4 * NP + (f * 4 + k) * NF + fn] = Fc[(d * 4 + k) * NP + node];
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) out[k * NP + node] = div[k];
+        }
     }
 }
 
