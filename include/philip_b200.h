@@ -172,6 +172,16 @@ enum {
 };
 int ph_integrated_quantities(ph_ctx* ctx, double out[PH_N_INTEGRATED_QUANTITIES]);
 
+/* The time loop of FlowSolver::run (src/flow_solver/flow_solver.cpp:540-620) with the
+ * periodic-turbulence unsteady data (PeriodicTurbulence::compute_unsteady_data_and_write_to_table,
+ * periodic_turbulence.cpp:923-972) on the device: nsteps steps of dt as ph_rk_step takes
+ * them; after every record_every-th step the four values of ph_integrals are reduced on the
+ * device into a table, which is copied once, at the end, to rows (nsteps / record_every
+ * rows of 4 doubles: kinetic energy, enstrophy, vorticity-based dissipation rate, max wave
+ * speed). record_every = 0 records nothing. On a caller-given stream each record interval
+ * replays one captured graph (steps, integrals, row). Synchronises the context stream. */
+int ph_run(ph_ctx* ctx, double dt, int nsteps, int record_every, double* rows);
+
 /* Status word: bit 0 = a negative density or pressure was met (Euler::check_positive_quantity,
  * src/physics/euler.cpp:155-172). Reading clears it. */
 int ph_status(ph_ctx* ctx, uint32_t* flags);

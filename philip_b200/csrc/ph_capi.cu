@@ -633,6 +633,15 @@ struct ph_ctx {
     cudaGraphExec_t step_graph = nullptr;
     double step_graph_dt = 0.0;
     int step_graph_launches = 0;
+    // ph_run: device table of integrals rows, its row counter, and the captured graph of one
+    // record interval (record_every steps, the integrals and the row reduction)
+    double* d_table = nullptr;
+    int table_rows = 0;
+    int* d_counter = nullptr;
+    cudaGraphExec_t run_graph = nullptr;
+    double run_graph_dt = 0.0;
+    int run_graph_every = 0;
+    int run_graph_launches = 0;
 };
 
 namespace {
@@ -811,12 +820,14 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
 
 int ph_ctx_destroy(ph_ctx* c) {
     if (!c) return PH_OK;
-    if (c->step_graph) {
+    if (c->step_graph || c->run_graph) {
         if (c->stream) cudaStreamSynchronize(c->stream);
-        cudaGraphExecDestroy(c->step_graph);
+        if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+        if (c->run_graph) cudaGraphExecDestroy(c->run_graph);
     }
     void* ptrs[] = {c->d_nbr, c->d_ops, c->d_itab, c->d_sol, c->d_stA, c->d_stB, c->d_acc, c->d_carry,
-                    c->d_fv, c->d_comp, c->d_tmpA, c->d_tmpB, c->d_partial, c->d_status, c->d_metric, c->d_xnode, c->d_origin, c->d_err};
+                    c->d_fv, c->d_comp, c->d_tmpA, c->d_tmpB, c->d_partial, c->d_status, c->d_metric, c->d_xnode, c->d_origin, c->d_err,
+                    c->d_table, c->d_counter};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -983,7 +994,7 @@ int ph_rk_step(ph_ctx* c, double dt, int nsteps) {
     return PH_OK;
 }
 
-static int run_integrals(ph_ctx* c, bool full) {
+static int launch_integrals_async(ph_ctx* c, bool full) {
     ph::IntegralConst ic{};
     ic.h = c->h;
     ic.gam = c->prm.gamma_gas; ic.gm1 = ic.gam - 1.0;
@@ -1000,6 +1011,12 @@ static int run_integrals(ph_ctx* c, bool full) {
     default: return fail(PH_ERR_UNSUPPORTED, "polynomial degree");
     }
     if (e != cudaSuccess) return fail(PH_ERR_CUDA, cudaGetErrorString(e));
+    ++c->launches;
+    return PH_OK;
+}
+
+static int run_integrals(ph_ctx* c, bool full) {
+    if (int rc = launch_integrals_async(c, full)) return rc;
     const size_t nq = full ? ph::integral_partials<true>() : ph::integral_partials<false>();
     PH_CUDA(cudaMemcpyAsync(c->h_partial.data(), c->d_partial, nq * c->nc * sizeof(double),
                             cudaMemcpyDeviceToHost, c->stream));
@@ -1035,6 +1052,96 @@ int ph_integrated_quantities(ph_ctx* c, double out[PH_N_INTEGRATED_QUANTITIES]) 
         for (int q = 0; q < PH_N_INTEGRATED_QUANTITIES; ++q) acc[q] += c->h_partial[(size_t)NQ * i + q];
     const double vol = std::pow(c->right - c->left, 3);
     for (int q = 0; q < PH_N_INTEGRATED_QUANTITIES; ++q) out[q] = acc[q] / vol;
+    return PH_OK;
+}
+
+// One record interval: record_every RK steps, then the integrals and their row on the device.
+static int run_interval(ph_ctx* c, double dt, int record_every) {
+    for (int s = 0; s < record_every; ++s)
+        if (int rc = rk_one_step(c, dt)) return rc;
+    if (int rc = launch_integrals_async(c, false)) return rc;
+    const double vol = std::pow(c->right - c->left, 3);
+    ph::integrals_row_kernel<<<1, ph::ROW_THREADS, 0, c->stream>>>(
+        c->d_partial, c->nc, vol, c->visc ? c->prm.reynolds_number_inf : 0.0, c->d_counter, c->table_rows,
+        c->d_table);
+    PH_CUDA(cudaGetLastError());
+    ++c->launches;
+    return PH_OK;
+}
+
+static int capture_run_graph(ph_ctx* c, double dt, int record_every) {
+    if (c->run_graph) { cudaGraphExecDestroy(c->run_graph); c->run_graph = nullptr; }
+    const long long before = c->launches;
+    cudaGraph_t g = nullptr;
+    PH_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = run_interval(c, dt, record_every);
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (rc || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        c->launches = before;
+        return rc ? rc : fail(PH_ERR_CUDA, std::string("run capture: ") + cudaGetErrorString(e));
+    }
+    const cudaError_t e2 = cudaGraphInstantiate(&c->run_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e2 != cudaSuccess) { c->run_graph = nullptr; return fail(PH_ERR_CUDA, cudaGetErrorString(e2)); }
+    c->run_graph_launches = (int)(c->launches - before);
+    c->launches = before;
+    c->run_graph_dt = dt;
+    c->run_graph_every = record_every;
+    return PH_OK;
+}
+
+int ph_run(ph_ctx* c, double dt, int nsteps, int record_every, double* rows) {
+    if (!c || nsteps < 0 || record_every < 0) return fail(PH_ERR_INVALID, "bad argument");
+    const int nrec = record_every > 0 ? nsteps / record_every : 0;
+    if (nrec > 0 && !rows) return fail(PH_ERR_INVALID, "null rows");
+    if (nrec > c->table_rows) {   // grow the device table (synchronises the stream)
+        if (c->run_graph) {
+            PH_CUDA(cudaStreamSynchronize(c->stream));
+            cudaGraphExecDestroy(c->run_graph);
+            c->run_graph = nullptr;
+        }
+        if (c->d_table) cudaFree(c->d_table);
+        c->d_table = nullptr;
+        c->table_rows = 0;
+        if (cudaMalloc(&c->d_table, (size_t)nrec * 4 * sizeof(double)) != cudaSuccess) {
+            c->d_table = nullptr;
+            return fail(PH_ERR_NOMEM, "integrals table");
+        }
+        c->table_rows = nrec;
+    }
+    if (nrec > 0 && !c->d_counter) {
+        if (cudaMalloc(&c->d_counter, sizeof(int)) != cudaSuccess) {
+            c->d_counter = nullptr;
+            return fail(PH_ERR_NOMEM, "row counter");
+        }
+    }
+    if (nrec > 0) PH_CUDA(cudaMemsetAsync(c->d_counter, 0, sizeof(int), c->stream));
+    // intervals on a caller-given stream replay a captured graph (the first one runs
+    // directly so that every kernel is configured before the capture)
+    const bool graph = c->stream != nullptr && !c->timing && c->ns > 1 && nrec > 1;
+    int r = 0;
+    if (graph) {
+        if (!c->run_graph || c->run_graph_dt != dt || c->run_graph_every != record_every) {
+            if (int rc = run_interval(c, dt, record_every)) return rc;
+            r = 1;
+            if (int rc = capture_run_graph(c, dt, record_every)) return rc;
+        }
+        for (; r < nrec; ++r) {
+            PH_CUDA(cudaGraphLaunch(c->run_graph, c->stream));
+            c->launches += c->run_graph_launches;
+        }
+    } else {
+        for (; r < nrec; ++r)
+            if (int rc = run_interval(c, dt, record_every)) return rc;
+    }
+    for (int s = nrec * record_every; s < nsteps; ++s)
+        if (int rc = rk_one_step(c, dt)) return rc;
+    if (nrec > 0) {
+        PH_CUDA(cudaMemcpyAsync(rows, c->d_table, (size_t)nrec * 4 * sizeof(double), cudaMemcpyDeviceToHost,
+                                c->stream));
+    }
+    PH_CUDA(cudaStreamSynchronize(c->stream));
     return PH_OK;
 }
 

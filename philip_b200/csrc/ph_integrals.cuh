@@ -349,4 +349,46 @@ __global__ void integrals_kernel(const double* __restrict__ U, const double* __r
     }
 }
 
+// One row of the integrals table on the device: the per-cell partials of integrals_kernel
+// (not FULL: kinetic energy, enstrophy, max wave speed per cell) reduced to
+// {KE / V, enstrophy / V, 2 enstrophy / (Re V) (re > 0; zero otherwise), max wave speed}, the
+// values ph_integrals returns. One block of ROW_THREADS: each thread sums a fixed strided share of the cells in
+// order, then a fixed-order tree, so a row is the same on every run. The row index comes
+// from a device counter that the kernel advances, so one captured launch serves every row.
+constexpr int ROW_THREADS = 512;
+static __global__ void __launch_bounds__(ROW_THREADS)
+integrals_row_kernel(const double* __restrict__ partial, int nc, double vol, double re, int* __restrict__ counter,
+                     int max_rows, double* __restrict__ table) {
+    __shared__ double ske[ROW_THREADS], sen[ROW_THREADS], swv[ROW_THREADS];
+    const int tid = threadIdx.x;
+    double ke = 0.0, en = 0.0, wv = 0.0;
+    for (int i = tid; i < nc; i += ROW_THREADS) {
+        ke += partial[3 * (size_t)i];
+        en += partial[3 * (size_t)i + 1];
+        const double w = partial[3 * (size_t)i + 2];
+        wv = w > wv ? w : wv;
+    }
+    ske[tid] = ke; sen[tid] = en; swv[tid] = wv;
+    __syncthreads();
+    for (int h = ROW_THREADS / 2; h > 0; h >>= 1) {
+        if (tid < h) {
+            ske[tid] += ske[tid + h];
+            sen[tid] += sen[tid + h];
+            swv[tid] = swv[tid + h] > swv[tid] ? swv[tid + h] : swv[tid];
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        const int r = *counter;
+        if (r < max_rows) {
+            double* row = table + 4 * (size_t)r;
+            row[0] = ske[0] / vol;
+            row[1] = sen[0] / vol;
+            row[2] = re > 0.0 ? 2.0 * row[1] / re : 0.0;
+            row[3] = swv[0];
+        }
+        *counter = r + 1;
+    }
+}
+
 } // namespace ph

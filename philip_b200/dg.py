@@ -179,6 +179,23 @@ class RungeKuttaODESolver:
             self.current_time += dt
         self.dg.set_current_time(self.current_time)
 
+    def step_in_time_with_records(self, dt: float, nsteps: int, record_every: int):
+        """nsteps steps of dt with the four ph_integrals values reduced on the device after
+        every record_every-th step (ph_run); returns [(time, KE, enstrophy, eps, wave)] with
+        the times this solver's clock shows after those steps."""
+        nrec = nsteps // record_every if record_every > 0 else 0
+        rows = np.zeros((max(nrec, 1), 4))
+        _lib.check(self.dg.L.ph_run(self.dg.handle, dt, nsteps, record_every,
+                                    rows.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        out = []
+        for s in range(nsteps):
+            self.current_iteration += 1
+            self.current_time += dt
+            if record_every > 0 and (s + 1) % record_every == 0 and (s + 1) // record_every <= nrec:
+                out.append((self.current_time, *rows[(s + 1) // record_every - 1]))
+        self.dg.set_current_time(self.current_time)
+        return out
+
     def error_norm(self) -> float:
         """Weighted RMS error estimate of the last low-storage step."""
         w = ctypes.c_double(0.0)
@@ -438,6 +455,16 @@ class FlowSolver:
             dt = self.time_step()
         if not self.unsteady_data:
             self.unsteady_data.append((self.ode_solver.current_time, *self.dg.integrals()))
+        if (not adaptive and not error_adaptive and not write_restart and record_every > 0
+                and self.ode_solver.current_iteration % record_every == 0):
+            # the whole steps of dt run on the device with the records reduced there (ph_run);
+            # the count follows the loop below step by step, so the clock is the same
+            t, n = self.ode_solver.current_time, 0
+            while t < final_time and not (end_exact and t + dt > final_time):
+                t += dt
+                n += 1
+            # records after iterations that are multiples of record_every, as the loop below
+            self.unsteady_data.extend(self.ode_solver.step_in_time_with_records(dt, n, record_every))
         while self.ode_solver.current_time < final_time:
             step = dt
             if self.ode_solver.current_time + step > final_time and end_exact:
