@@ -415,13 +415,85 @@ def run_many(args, rank: int = 0, world: int = 1, local_rank: int = 0):
     return 0
 
 
+PRECISION_CHECK = "tgv_precision_check_32_p3"
+
+
+def run_precision_check(args, rank: int = 0, world: int = 1, local_rank: int = 0):
+    """The precision form's error against the FP64 path on the viscous TGV at 32^3 cells, p=3
+    over t in [0, t_final] (default 5): both forms take the same constant time step (the
+    adaptive formula evaluated once at t=0) and record kinetic energy and enstrophy every 10
+    steps on the device (ph_run). Reports the relative max errors of the kinetic-energy
+    dissipation rate -dKE/dt (central differences of the KE rows), of the vorticity-based
+    dissipation rate 2 enstrophy / Re and of the KE itself, and the two forms' rates with the
+    rows included. Independent replicas on every rank (no exchange)."""
+    import torch
+    from philip_b200 import _lib
+    from philip_b200.dg import FlowSolver
+    from philip_b200.prm import Parameters
+    torch.cuda.set_device(local_rank)
+    prm = Parameters.from_dict(prm_for("tgv_viscous_32_p3"))
+    t_final = args.final_time
+    record_every = 10
+    out = {}
+    dt = None
+    for name, prec in (("fp64", _lib.PH_FP64), ("fp32", _lib.PH_FP32_RESIDUAL)):
+        stream = torch.cuda.Stream()
+        fs = FlowSolver(prm, precision=prec, stream=stream.cuda_stream)
+        if dt is None:
+            dt = fs.adaptive_time_step()
+        nsteps = int(round(t_final / dt))
+        q0 = fs.dg.integrals()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        rows = fs.ode_solver.step_in_time_with_records(dt, nsteps, record_every)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        out[name] = dict(t=np.array([0.0] + [r[0] for r in rows]), ke=np.array([q0[0]] + [r[1] for r in rows]),
+                         eps_w=np.array([q0[2]] + [r[3] for r in rows]), ms=ev0.elapsed_time(ev1),
+                         nsteps=nsteps, status=fs.dg.status(), ndofs=fs.dg.n_dofs)
+        del fs
+        torch.cuda.empty_cache()
+    a, b = out["fp64"], out["fp32"]
+
+    def rel(x, y):
+        return float(np.max(np.abs(x - y)) / np.max(np.abs(x)))
+
+    dke_a = -np.gradient(a["ke"], a["t"])
+    dke_b = -np.gradient(b["ke"], b["t"])
+
+    def rate(o):
+        return o["ndofs"] * 4 * o["nsteps"] / (o["ms"] * 1e-3)
+
+    if rank == 0:
+        line = {
+            "metric": "KE-dissipation-rate rel error, precision form vs FP64 (viscous TGV 32^3 p3)",
+            "value": rel(dke_a, dke_b), "unit": "relative max error", "higher_is_better": False,
+            "n_gpus": world, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32-residual/f64-state vs f64", "data": "synthetic (Taylor-Green initial condition)",
+            "config": {"workload": PRECISION_CHECK, "t_final": t_final, "dt": dt, "steps": a["nsteps"],
+                       "record_every": record_every, "rows": len(a["t"]) - 1},
+            "errors": {"ke_dissipation_rate_minus_dKE_dt": rel(dke_a, dke_b),
+                       "vorticity_dissipation_rate_2_enstrophy_over_Re": rel(a["eps_w"], b["eps_w"]),
+                       "kinetic_energy": rel(a["ke"], b["ke"])},
+            "rates_with_rows": {"fp64": rate(a), "fp32": rate(b), "ratio": rate(b) / rate(a),
+                                "unit": "DOF-updates/s/stage"},
+            "status_flags": [a["status"], b["status"]],
+            "ke_final": [float(a["ke"][-1]), float(b["ke"][-1])],
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="tgv_viscous_24_p5", choices=sorted(WORKLOADS) + sorted(MANY))
+    ap.add_argument("--workload", default="tgv_viscous_24_p5",
+                    choices=sorted(WORKLOADS) + sorted(MANY) + [PRECISION_CHECK])
+    ap.add_argument("--final-time", type=float, default=5.0, help="precision check: end of the compared window")
     ap.add_argument("--requests", type=int, default=0, help="batched / served forms: number of solves")
     ap.add_argument("--rate", type=float, default=50.0, help="served form: Poisson arrival rate per second")
     ap.add_argument("--budget-gb", type=float, default=96.0, help="batched / served forms: HBM budget")
@@ -435,6 +507,12 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload == PRECISION_CHECK:
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the precision check compares this build's two "
+                              "forms with each other; the reference has no precision form"}), flush=True)
+            return 0
+        return run_precision_check(args, rank, world, local_rank)
     if args.workload in MANY:
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the batched and served forms have no reference "

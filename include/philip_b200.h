@@ -76,6 +76,13 @@ typedef struct ph_params {
     double sipg_penalty_factor;
     double rk_atol;                       /* low-storage RK error estimate: absolute and relative */
     double rk_rtol;                       /* tolerances (ODE solver atol / rtol) */
+    /* Precision form only (no counterpart in the reference's parameters): a constant reference
+     * pressure subtracted from the pressure in every momentum flux. A constant pressure adds
+     * the same amount to the volume and the face terms, which cancel, so the residual is
+     * unchanged in exact arithmetic; in FP32 the mean pressure of a low-Mach flow
+     * (1/(gamma M^2) in the Taylor-Green scaling, 1/gamma in the isentropic vortex's) would
+     * otherwise swamp its O(1) variations. 0 = no shift. Ignored by the FP64 path. */
+    double pressure_shift;
 } ph_params;
 
 /* Periodic cube [left,right]^3 with n^3 cells (PeriodicCubeFlow::generate_grid,

@@ -39,7 +39,7 @@ class PhParams(ctypes.Structure):
         "precision")] + [(n, ctypes.c_double) for n in (
         "FR_user_specified_correction_parameter_value", "gamma_gas", "mach_infinity", "reynolds_number_inf",
         "prandtl_number", "temperature_inf", "nondimensionalized_constant_viscosity", "sipg_penalty_factor",
-        "rk_atol", "rk_rtol")]
+        "rk_atol", "rk_rtol", "pressure_shift")]
 
 
 class PhMeshDesc(ctypes.Structure):

@@ -675,6 +675,7 @@ int ph_batch_autotune(int poly_degree, int precision, int curvilinear, int* best
     prm.reynolds_number_inf = 1600.0; prm.prandtl_number = 0.71; prm.temperature_inf = 273.15;
     prm.sipg_penalty_factor = 1.0; prm.nondimensionalized_constant_viscosity = 1.0;
     prm.rk_atol = 1e-3; prm.rk_rtol = 1e-3;
+    prm.pressure_shift = 1.0 / (1.4 * 0.1 * 0.1);
     size_t bytes = 0;
     if (int rc = ph_batch_bytes(&mesh, &prm, &bytes)) return rc;
     cudaStream_t s = nullptr;

@@ -340,6 +340,7 @@ ph::PhysConst physics_constants(const ph_params* prm, double h, double& penalty)
     pc.prandtl = prm->prandtl_number;
     pc.const_visc = prm->nondimensionalized_constant_viscosity;
     pc.use_const_visc = prm->use_constant_viscosity;
+    pc.pressure_shift = prm->pressure_shift;
     pc.two_point = prm->two_point_num_flux_type;
     pc.conv_flux = prm->conv_num_flux;
     pc.diss_flux = prm->diss_num_flux;
@@ -1438,6 +1439,7 @@ extern "C" int ph_residual_noalloc(const ph_mesh_desc* mesh, const ph_params* pr
     pc.prandtl = prm->prandtl_number;
     pc.const_visc = prm->nondimensionalized_constant_viscosity;
     pc.use_const_visc = prm->use_constant_viscosity;
+    pc.pressure_shift = prm->pressure_shift;
     pc.two_point = prm->two_point_num_flux_type;
     pc.conv_flux = prm->conv_num_flux;
     pc.diss_flux = prm->diss_num_flux;

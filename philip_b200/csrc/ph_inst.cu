@@ -211,6 +211,22 @@ static cudaError_t launch_integrals_one(const double* U, const double* X, const 
 template <int N1>
 cudaError_t launch_integrals(const double* U, const double* X, const double* origin, const IntegralTab* tab, int nc,
                              const IntegralConst& ic, bool full, double* partial, cudaStream_t s) {
+    if constexpr (integrals_affine_fits<N1>()) {
+        if (!full && !X) {   // affine cells, the three partials: the hoisted-contraction kernel
+            auto kern = integrals_affine_kernel<N1>;
+            constexpr size_t bytes = integrals_affine_smem_bytes<N1>();
+            int dev = 0;
+            cudaGetDevice(&dev);
+            static bool configured[64] = {false};
+            if (dev < 64 && !configured[dev]) {
+                cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+                if (e != cudaSuccess) return e;
+                configured[dev] = true;
+            }
+            kern<<<nc, AFF_THREADS, bytes, s>>>(U, tab, nc, ic, partial);
+            return cudaGetLastError();
+        }
+    }
     if (full)
         return X ? launch_integrals_one<N1, true, true>(U, X, origin, tab, nc, ic, partial, s)
                  : launch_integrals_one<N1, false, true>(U, X, origin, tab, nc, ic, partial, s);

@@ -349,6 +349,140 @@ __global__ void integrals_kernel(const double* __restrict__ U, const double* __r
     }
 }
 
+// Kinetic energy, enstrophy and wave speed on affine cells (the integrals_kernel's partials
+// without FULL) with the y-contraction hoisted out of the point loop: the x- and then the
+// y-contracted values (and x-, y-derivatives of the four fields whose gradient the enstrophy
+// needs) of all columns are built once per cell in shared memory, so a cubature point only
+// contracts along z (4 N1-term sums per field instead of N1 (3 N1 + 4)). Each point's values
+// are the same products summed in the same order as in integrals_kernel. Used while two CTAs
+// fit an SM (p <= 3: 82 KB at p = 3): 2.5 ms against 3.9 ms per evaluation at 32^3 cells,
+// p = 3 on B200; at p = 5 (178 KB, one CTA per SM) it was slower than integrals_kernel.
+constexpr int AFF_THREADS = 256;
+template <int N1> __host__ __device__ constexpr size_t integrals_affine_smem_bytes() {
+    constexpr int NE = N1 + 10;
+    return sizeof(double) * (5 * N1 * N1 * N1 + 2 * N1 * N1 * NE + 13 * N1 * NE * NE);
+}
+template <int N1> __host__ __device__ constexpr bool integrals_affine_fits() {
+    return integrals_affine_smem_bytes<N1>() <= 100 * 1024;
+}
+
+template <int N1>
+__global__ void __launch_bounds__(AFF_THREADS)
+integrals_affine_kernel(const double* __restrict__ U, const IntegralTab* tab, int nc, IntegralConst ic,
+                        double* __restrict__ partial) {
+    constexpr int NE = N1 + 10;
+    constexpr int NP = N1 * N1 * N1;
+    constexpr int NT2 = N1 * N1 * NE;    // x-contracted entries of one field
+    constexpr int NY = N1 * NE * NE;     // x- and y-contracted entries of one field
+    __shared__ double sB[NE * N1], sdB[NE * N1], sw[NE];
+    __shared__ double red[3][32];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* sU = reinterpret_cast<double*>(smem_raw);   // [5][NP]
+    double* sTv = sU + 5 * NP;                          // [(k*N1 + j)*NE + qx], one field at a time
+    double* sTx = sTv + NT2;
+    // rows 0-4: values of the five fields; 5-8: x-derivatives and 9-12: y-derivatives of
+    // density and momentum; each row [k][qy*NE + qx]
+    double* sY = sTx + NT2;
+    const int cell = blockIdx.x;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < NE * N1; i += AFF_THREADS) { sB[i] = tab->B[i]; sdB[i] = tab->dB[i]; }
+    for (int i = tid; i < NE; i += AFF_THREADS) sw[i] = tab->w[i];
+    for (int i = tid; i < 5 * NP; i += AFF_THREADS) sU[i] = U[(size_t)cell * 5 * NP + i];
+    __syncthreads();
+    for (int f = 0; f < 5; ++f) {
+        for (int i = tid; i < NT2; i += AFF_THREADS) {
+            const int qx = i % NE, kj = i / NE;
+            double v = 0.0, dv = 0.0;
+            for (int a = 0; a < N1; ++a) {
+                const double u = sU[f * NP + kj * N1 + a];
+                v += sB[qx * N1 + a] * u;
+                dv += sdB[qx * N1 + a] * u;
+            }
+            sTv[i] = v;
+            sTx[i] = dv;
+        }
+        __syncthreads();
+        for (int i = tid; i < NY; i += AFF_THREADS) {
+            const int qx = i % NE, qy = (i / NE) % NE, k = i / (NE * NE);
+            double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+#pragma unroll
+            for (int j = 0; j < N1; ++j) {
+                const double t0 = sTv[(k * N1 + j) * NE + qx];
+                const double t1 = sTx[(k * N1 + j) * NE + qx];
+                a0 += sB[qy * N1 + j] * t0;
+                a1 += sB[qy * N1 + j] * t1;
+                a2 += sdB[qy * N1 + j] * t0;
+            }
+            sY[f * NY + i] = a0;
+            if (f < 4) { sY[(5 + f) * NY + i] = a1; sY[(9 + f) * NY + i] = a2; }
+        }
+        __syncthreads();
+    }
+    const double inv_h = 1.0 / ic.h, detj = ic.h * ic.h * ic.h;
+    const double gam = ic.gam, gm1 = ic.gm1;
+    double ke = 0.0, ens = 0.0, wave = 0.0;
+    for (int pt = tid; pt < NE * NE * NE; pt += AFF_THREADS) {
+        const int col = pt % (NE * NE), qz = pt / (NE * NE);
+        const int qx = col % NE, qy = col / NE;
+        double u[5], g[4][3];
+#pragma unroll
+        for (int f = 0; f < 5; ++f) {
+            double v = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+#pragma unroll
+            for (int k = 0; k < N1; ++k) {
+                const double b = sB[qz * N1 + k], db = sdB[qz * N1 + k];
+                const double a0 = sY[f * NY + k * NE * NE + col];
+                if (f < 4) {
+                    const double a1 = sY[(5 + f) * NY + k * NE * NE + col];
+                    const double a2 = sY[(9 + f) * NY + k * NE * NE + col];
+                    v += b * a0; gx += b * a1; gy += b * a2; gz += db * a0;
+                } else {
+                    v += b * a0;
+                }
+            }
+            u[f] = v;
+            if (f < 4) { g[f][0] = gx * inv_h; g[f][1] = gy * inv_h; g[f][2] = gz * inv_h; }
+        }
+        const double rho = u[0];
+        double v[3], v2 = 0.0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) { v[d] = u[1 + d] / rho; v2 += v[d] * v[d]; }
+        double gv[3][3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) gv[a][d] = (g[1 + a][d] - v[a] * g[0][d]) / rho;
+        const double o0 = gv[2][1] - gv[1][2], o1 = gv[0][2] - gv[2][0], o2 = gv[1][0] - gv[0][1];
+        const double wt = sw[qx] * sw[qy] * sw[qz] * detj;
+        ke += 0.5 * rho * v2 * wt;
+        ens += 0.5 * rho * (o0 * o0 + o1 * o1 + o2 * o2) * wt;
+        const double p = gm1 * (u[4] - 0.5 * rho * v2);
+        const double c = sqrt(p * gam / rho);
+        const double ws = sqrt(v2) + c;
+        wave = ws > wave ? ws : wave;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        ke += __shfl_down_sync(0xffffffffu, ke, o);
+        ens += __shfl_down_sync(0xffffffffu, ens, o);
+        const double wo = __shfl_down_sync(0xffffffffu, wave, o);
+        wave = wo > wave ? wo : wave;
+    }
+    const int warp = tid >> 5, lane = tid & 31;
+    if (lane == 0) { red[0][warp] = ke; red[1][warp] = ens; red[2][warp] = wave; }
+    __syncthreads();
+    if (tid == 0) {
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        for (int w = 0; w < AFF_THREADS / 32; ++w) {
+            a0 += red[0][w]; a1 += red[1][w];
+            a2 = red[2][w] > a2 ? red[2][w] : a2;
+        }
+        partial[3 * (size_t)cell + 0] = a0;
+        partial[3 * (size_t)cell + 1] = a1;
+        partial[3 * (size_t)cell + 2] = a2;
+    }
+}
+
 // One row of the integrals table on the device: the per-cell partials of integrals_kernel
 // (not FULL: kinetic energy, enstrophy, max wave speed per cell) reduced to
 // {KE / V, enstrophy / V, 2 enstrophy / (Re V) (re > 0; zero otherwise), max wave speed}, the

@@ -516,13 +516,13 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
         if constexpr (!SPLIT) {
             constexpr int o = VISC ? 4 : 0;
             R F[5];
-            conv_flux_dir<R, 0>(q, F);
+            conv_flux_dir<R, 0>(q, cst.p0, F);
 #pragma unroll
             for (int s = 0; s < 5; ++s) X[(o + 0 * 5 + s) * NP + node] = F[s];
-            conv_flux_dir<R, 1>(q, F);
+            conv_flux_dir<R, 1>(q, cst.p0, F);
 #pragma unroll
             for (int s = 0; s < 5; ++s) X[(o + 1 * 5 + s) * NP + node] = F[s];
-            conv_flux_dir<R, 2>(q, F);
+            conv_flux_dir<R, 2>(q, cst.p0, F);
 #pragma unroll
             for (int s = 0; s < 5; ++s) X[(o + 2 * 5 + s) * NP + node] = F[s];
         }
@@ -768,15 +768,16 @@ residual_kernel_batched(const StageArgs* __restrict__ inst, const BatchTile* __r
 // needs: its volume divergence and its face-normal component on each face
 // (viscous_terms_per_cell).
 // ------------------------------------------------------------------------------------
-// Two forms of the same arithmetic, chosen per precision and order from timings on B200:
-//  line form (FP64, p >= 4): one thread per (direction, state, line) differentiates the
-//    line held in registers; every coefficient is a parameter-bank operand, the gradient
-//    and then the nodal flux share one buffer, the divergence runs direction by direction;
-//  node form (FP32, and FP64 at p <= 3): one thread per node, coefficients from shared
-//    memory (fewer barriers and less shared memory, which wins at low order and in FP32).
+// Two forms of the same arithmetic, chosen per order from timings on B200:
+//  line form (p >= 4): one thread per (direction, state, line) differentiates the line held
+//    in registers; every coefficient is a parameter-bank operand, the gradient and then the
+//    nodal flux share one buffer, the divergence runs direction by direction (at p = 5 it
+//    takes 0.170 ms against 0.262 ms for the node form in FP64, 0.124 against 0.162 in FP32);
+//  node form (p <= 3): one thread per node, coefficients from shared memory (fewer barriers
+//    and less shared memory, which wins at low order).
 // Both sum every node's terms in the same order (over l, then over directions).
 template <typename R, int N1> __host__ __device__ constexpr bool aux_line_form() {
-    return sizeof(R) == 8 && N1 >= 5;
+    return N1 >= 5;
 }
 
 template <int N1, int CPC>

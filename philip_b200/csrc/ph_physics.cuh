@@ -28,16 +28,23 @@ constexpr double BIG_NUMBER = 1e100;   // physics.h:270
 
 struct PhysConst {
     double gam, gm1, mach2, temp_ratio, inv_re, prandtl, const_visc, sipg_pen;
+    double pressure_shift;   // precision form: reference pressure taken out of the momentum fluxes
     int use_const_visc, two_point, conv_flux, diss_flux, navier_stokes;
 };
 
 template <typename R> struct Cst {
-    R gam, gm1, mach2, temp_ratio, inv_re, prandtl, const_visc, kappa_fac, inv2gm1;
+    // p0: the constant subtracted from the pressure in every momentum flux of the precision
+    // form. A constant pressure adds the same amount to the volume and the face terms, which
+    // cancel exactly, so the residual is unchanged; in FP32 the large mean pressure of a
+    // low-Mach flow (1/(gamma M^2) = 71 at M = 0.1) no longer swamps its O(1) variations.
+    // Zero in FP64, whose arithmetic stays the reference's.
+    R gam, gm1, mach2, temp_ratio, inv_re, prandtl, const_visc, kappa_fac, inv2gm1, p0;
     __device__ __forceinline__ void load(const PhysConst& c) {
         gam = (R)c.gam; gm1 = (R)c.gm1; mach2 = (R)c.mach2; temp_ratio = (R)c.temp_ratio;
         inv_re = (R)c.inv_re; prandtl = (R)c.prandtl; const_visc = (R)c.const_visc;
         kappa_fac = (R)(1.0 / (c.gm1 * c.mach2 * c.prandtl));
         inv2gm1 = (R)(0.5 / c.gm1);
+        p0 = sizeof(R) == 4 ? (R)c.pressure_shift : R(0);
     }
 };
 
@@ -224,7 +231,7 @@ __device__ __forceinline__ void two_point_dir(const NodeQ<R>& i, const NodeQ<R>&
         F[0] = m;
 #pragma unroll
         for (int k = 0; k < 3; ++k) F[1 + k] = m * va[k];
-        F[1 + d] += p_hat;
+        F[1 + d] += p_hat - c.p0;
         F[4] = m * (h0 + vsq);
     } else if (tp == TP_RA) {
         const R rho_log = log_mean<R>(i.a, j.a, i.la, j.la);
@@ -240,7 +247,7 @@ __device__ __forceinline__ void two_point_dir(const NodeQ<R>& i, const NodeQ<R>&
         F[0] = m;
 #pragma unroll
         for (int k = 0; k < 3; ++k) F[1 + k] = m * va[k];
-        F[1 + d] += p_hat;
+        F[1 + d] += p_hat - c.p0;
         F[4] = m * H - R(0.5) * (i.p * i.v[d] + j.p * j.v[d]);
     } else if (tp == TP_IR) {
         const R z0a = R(0.5) * (i.a + j.a), z4a = R(0.5) * (i.b + j.b);
@@ -262,7 +269,7 @@ __device__ __forceinline__ void two_point_dir(const NodeQ<R>& i, const NodeQ<R>&
         F[0] = m;
 #pragma unroll
         for (int k = 0; k < 3; ++k) F[1 + k] = m * v[k];
-        F[1 + d] += p;
+        F[1 + d] += p - c.p0;
         F[4] = m * H;
     } else {   // KG
         const R rho = (i.rho + j.rho) / R(2);
@@ -275,20 +282,20 @@ __device__ __forceinline__ void two_point_dir(const NodeQ<R>& i, const NodeQ<R>&
         F[0] = m;
 #pragma unroll
         for (int k = 0; k < 3; ++k) F[1 + k] = m * v[k];
-        F[1 + d] += p;
+        F[1 + d] += p - c.p0;
         F[4] = m * e + p * v[d];
     }
 }
 
-// Physical convective flux along direction d.
+// Physical convective flux along direction d (p0: the precision form's pressure shift).
 template <typename R, int d>
-__device__ __forceinline__ void conv_flux_dir(const NodeQ<R>& q, R F[5]) {
+__device__ __forceinline__ void conv_flux_dir(const NodeQ<R>& q, R p0, R F[5]) {
     const R H = qdiv<R>(q.E, q.rho) + qdiv<R>(q.p, q.rho);
     const R m = q.rho * q.v[d];
     F[0] = m;
 #pragma unroll
     for (int k = 0; k < 3; ++k) F[1 + k] = m * q.v[k];
-    F[1 + d] += q.p;
+    F[1 + d] += q.p - p0;
     F[4] = m * H;
 }
 
@@ -350,8 +357,8 @@ __device__ __forceinline__ void conv_num_flux(const R uL[5], const R uR[5], cons
         two_point_dir<R, d>(L, Rq, tp, c, out);
     } else {
         R FL[5], FR[5];
-        conv_flux_dir<R, d>(L, FL);
-        conv_flux_dir<R, d>(Rq, FR);
+        conv_flux_dir<R, d>(L, c.p0, FL);
+        conv_flux_dir<R, d>(Rq, c.p0, FR);
 #pragma unroll
         for (int k = 0; k < 5; ++k) out[k] = R(0.5) * (FL[k] + FR[k]);
     }
@@ -386,7 +393,7 @@ __device__ __forceinline__ void two_point_n(const NodeQ<R>& i, const NodeQ<R>& j
         const R m = rho_log * vn;
         F[0] = m;
 #pragma unroll
-        for (int k = 0; k < 3; ++k) F[1 + k] = m * va[k] + p_hat * n[k];
+        for (int k = 0; k < 3; ++k) F[1 + k] = m * va[k] + (p_hat - c.p0) * n[k];
         F[4] = m * (h0 + vsq);
     } else if (tp == TP_RA) {
         const R rho_log = log_mean<R>(i.a, j.a, i.la, j.la);
@@ -401,7 +408,7 @@ __device__ __forceinline__ void two_point_n(const NodeQ<R>& i, const NodeQ<R>& j
         const R m = rho_log * vn;
         F[0] = m;
 #pragma unroll
-        for (int k = 0; k < 3; ++k) F[1 + k] = m * va[k] + p_hat * n[k];
+        for (int k = 0; k < 3; ++k) F[1 + k] = m * va[k] + (p_hat - c.p0) * n[k];
         F[4] = m * H;
         R vni = R(0), vnj = R(0);
 #pragma unroll
@@ -426,7 +433,7 @@ __device__ __forceinline__ void two_point_n(const NodeQ<R>& i, const NodeQ<R>& j
         const R m = rho * vn;
         F[0] = m;
 #pragma unroll
-        for (int k = 0; k < 3; ++k) F[1 + k] = m * v[k] + p * n[k];
+        for (int k = 0; k < 3; ++k) F[1 + k] = m * v[k] + (p - c.p0) * n[k];
         F[4] = m * H;
     } else {   // KG
         const R rho = (i.rho + j.rho) / R(2);
@@ -438,20 +445,20 @@ __device__ __forceinline__ void two_point_n(const NodeQ<R>& i, const NodeQ<R>& j
         const R m = rho * vn;
         F[0] = m;
 #pragma unroll
-        for (int k = 0; k < 3; ++k) F[1 + k] = m * v[k] + p * n[k];
+        for (int k = 0; k < 3; ++k) F[1 + k] = m * v[k] + (p - c.p0) * n[k];
         F[4] = m * e + p * vn;
     }
 }
 
 // Physical convective flux dotted with n.
 template <typename R>
-__device__ __forceinline__ void conv_flux_n(const NodeQ<R>& q, const R n[3], R F[5]) {
+__device__ __forceinline__ void conv_flux_n(const NodeQ<R>& q, const R n[3], R p0, R F[5]) {
     const R H = qdiv<R>(q.E, q.rho) + qdiv<R>(q.p, q.rho);
     const R vn = q.v[0] * n[0] + q.v[1] * n[1] + q.v[2] * n[2];
     const R m = q.rho * vn;
     F[0] = m;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) F[1 + k] = m * q.v[k] + q.p * n[k];
+    for (int k = 0; k < 3; ++k) F[1 + k] = m * q.v[k] + (q.p - p0) * n[k];
     F[4] = m * H;
 }
 
@@ -514,8 +521,8 @@ __device__ __forceinline__ void conv_num_flux_n(const R uL[5], const R uR[5], co
         two_point_n<R>(L, Rq, n, tp, c, out);
     } else {
         R FL[5], FR[5];
-        conv_flux_n<R>(L, n, FL);
-        conv_flux_n<R>(Rq, n, FR);
+        conv_flux_n<R>(L, n, c.p0, FL);
+        conv_flux_n<R>(Rq, n, c.p0, FR);
 #pragma unroll
         for (int k = 0; k < 5; ++k) out[k] = R(0.5) * (FL[k] + FR[k]);
     }

@@ -213,7 +213,22 @@ class Parameters:
         p.precision = precision
         p.rk_atol = float(self.get("ODE solver/atol"))
         p.rk_rtol = float(self.get("ODE solver/rtol"))
+        p.pressure_shift = self.reference_pressure()
         return p
+
+    def reference_pressure(self) -> float:
+        """The flow case's free-stream pressure in its nondimensional scaling, which the
+        precision form takes out of its momentum fluxes: 1/(gamma M^2) for the Taylor-Green
+        vortex (initial_condition_function.cpp:261-310), 1/gamma for the isentropic vortex
+        (:643-690); 0 (no shift) otherwise."""
+        gamma = float(self.get("euler/gamma_gas"))
+        case = self.get("flow_solver/flow_case_type")
+        if case == "taylor_green_vortex":
+            mach = float(self.get("euler/mach_infinity"))
+            return 1.0 / (gamma * mach * mach)
+        if case == "isentropic_vortex":
+            return 1.0 / gamma
+        return 0.0
 
     def oracle_cfg(self) -> dict:
         """The same settings in the key set the CPU oracle's wrapper takes (tests only)."""

@@ -3,8 +3,11 @@ FP64 positivity checks and metric scaling.
 
 Tolerances (stated here, measured against the FP64 oracle / FP64 GPU path):
   residual, relative max-norm vs the FP64 oracle ............ 1e-5
-  TGV kinetic energy history over 200 steps, relative ....... 1e-5
-  vorticity-based dissipation rate history, relative ........ 1e-5
+  TGV kinetic energy history over 200 steps, relative ....... 2e-7
+  vorticity-based dissipation rate history, relative ........ 1e-6
+(the history bounds hold with the flow's mean pressure taken out of the FP32 momentum
+fluxes, ph_params.pressure_shift, which the flow-case parameters set; without it they were
+3e-6 and 1e-6)
 """
 import numpy as np
 import pytest
@@ -46,5 +49,6 @@ def test_fp32_tgv_energy_history():
     ke_err = np.max(np.abs(h32[:, 1] - h64[:, 1])) / np.max(np.abs(h64[:, 1]))
     eps_err = np.max(np.abs(h32[:, 3] - h64[:, 3])) / np.max(np.abs(h64[:, 3]))
     print(f"fp32 KE rel err {ke_err:.3e}, dissipation-rate rel err {eps_err:.3e}")
-    assert ke_err <= 1e-5
-    assert eps_err <= 1e-5
+    # with the mean pressure taken out of the FP32 momentum fluxes (ph_params.pressure_shift)
+    assert ke_err <= 2e-7
+    assert eps_err <= 1e-6
