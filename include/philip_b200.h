@@ -83,6 +83,12 @@ typedef struct ph_params {
      * (1/(gamma M^2) in the Taylor-Green scaling, 1/gamma in the isentropic vortex's) would
      * otherwise swamp its O(1) variations. 0 = no shift. Ignored by the FP64 path. */
     double pressure_shift;
+    /* Relaxation Runge-Kutta, root-finding form for the Euler / Navier-Stokes entropy
+     * (ODE solver/rrk root solver: use_relaxation_runge_kutta, relaxation_runge_kutta_root_tolerance;
+     * src/ode_solver/relaxation_runge_kutta/root_finding_rrk_ode_solver.cpp). The Butcher methods
+     * in FP64, two-point fluxes other than KG. */
+    int use_relaxation_runge_kutta;
+    double relaxation_runge_kutta_root_tolerance;
 } ph_params;
 
 /* Periodic cube [left,right]^3 with n^3 cells (PeriodicCubeFlow::generate_grid,
@@ -141,6 +147,13 @@ int ph_apply_inverse_mass(ph_ctx* ctx, const double* R, double* out, int where);
  * (src/ode_solver/ode_solver_base.h:70, runge_kutta_base.cpp:21-39), nsteps times
  * with the same dt, on the context's state. Asynchronous on the context stream. */
 int ph_rk_step(ph_ctx* ctx, double dt, int nsteps);
+
+/* Relaxation RK: the relaxation parameter gamma of the last step (RRKODESolverBase::
+ * update_relaxation_parameter, rrk_ode_solver_base.cpp:13-33) and the time the state advanced
+ * over the last ph_rk_step call, sum over its steps of gamma dt (RungeKuttaODESolver::
+ * adjust_time_step, runge_kutta_ode_solver.cpp:102-110). gamma = 1 and elapsed = nsteps dt
+ * without relaxation. */
+int ph_rk_relaxation(ph_ctx* ctx, double* gamma, double* elapsed);
 
 /* Weighted RMS error estimate of the last low-storage RK step,
  * sqrt(mean(((S1 - S_embedded) / (atol + rtol max(|S1|, |S_embedded|)))^2)) over all DOFs

@@ -1384,6 +1384,7 @@ void Solver::rk_step(double* U, double dt) {
     const size_t N = ndofs();
     std::vector<double> un(U, U + N), R(N);
     std::vector<std::vector<double>> k(ns, std::vector<double>(N));
+    double est = 0.0;   // relaxation RK: dt sum_i b_i v(u_i)^T M k_i
     for (int i = 0; i < ns; ++i) {
         std::vector<double>& st = k[i];
         std::fill(st.begin(), st.end(), 0.0);
@@ -1391,13 +1392,129 @@ void Solver::rk_step(double* U, double dt) {
             if (a[i][j] != 0.0) for (size_t m = 0; m < N; ++m) st[m] += a[i][j] * k[j][m];
         for (size_t m = 0; m < N; ++m) { st[m] *= dt; st[m] += 1.0 * un[m]; }
         assemble_residual(st.data(), R.data());
+        if (prm.use_rrk) est += b[i] * entropy_vars_dot_mass(st.data(), R.data());
         apply_inverse_mass(R.data(), st.data());
     }
+    double step = dt;
+    if (prm.use_rrk) step = dt * relaxation_parameter(un.data(), k, b, ns, dt, dt * est);
     for (int i = 0; i < ns; ++i)
-        for (size_t m = 0; m < N; ++m) un[m] += dt * b[i] * k[i][m];
+        for (size_t m = 0; m < N; ++m) un[m] += step * b[i] * k[i][m];
     std::copy(un.begin(), un.end(), U);
-    current_time += dt;
+    current_time += step;
     (void)cc;
+}
+
+// ---- relaxation Runge-Kutta, root-finding form for the Euler / Navier-Stokes entropy
+// (RootFindingRRKODESolver, root_finding_rrk_ode_solver.cpp:15-180, :182-390;
+// RKNumEntropy::compute_entropy_vars, runge_kutta_store_entropy.cpp:27-100). GLL flux nodes:
+// the volume quadrature is the solution nodes, so the entropy variables' projection onto the
+// solution basis is the identity and the mass matrix of the M norm is diag(W det J).
+
+// Euler::compute_entropy (euler.cpp:512-530) and compute_numerical_entropy_function (:437-447)
+static double numerical_entropy_fn(const double u[5], double gam) {
+    const double p = (gam - 1.0) * (u[4] - 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0]);
+    const double s = std::log(p * std::pow(u[0], -gam));
+    return -u[0] * s;
+}
+
+// Euler::compute_entropy_variables (euler.cpp:811-829)
+static void entropy_variables(const double u[5], double gam, double v[5]) {
+    const double p = (gam - 1.0) * (u[4] - 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0]);
+    const double s = std::log(p * std::pow(u[0], -gam));
+    const double rt = p / (gam - 1.0);
+    v[0] = (rt * (gam + 1.0 - s) - u[4]) / rt;
+    for (int d = 0; d < 3; ++d) v[1 + d] = u[1 + d] / rt;
+    v[4] = -u[0] / rt;
+}
+
+// W det J of every solution node of cell c (GLL collocation)
+static double node_mass(const Mesh& mesh, const Ops1D& ops, int c, int node) {
+    const int nd = ops.nd;
+    const double W = ops.wq[node % nd] * ops.wq[(node / nd) % nd] * ops.wq[node / (nd * nd)];
+    const double J = mesh.affine ? mesh.h * mesh.h * mesh.h : mesh.detj[(size_t)c * nd * nd * nd + node];
+    return W * J;
+}
+
+double Solver::numerical_entropy(const double* U) const {
+    double sum = 0.0;
+    for (int c = 0; c < mesh.nc; ++c)
+        for (int i = 0; i < nd3; ++i) {
+            double u[5];
+            for (int s = 0; s < 5; ++s) u[s] = U[(size_t)c * ndofs_cell + s * nd3 + i];
+            sum += node_mass(mesh, ops, c, i) * numerical_entropy_fn(u, prm.gamma);
+        }
+    return sum;
+}
+
+// v(u)^T M k with M k = R for the residual R of this stage: M (M+K)^{-1} R is R for cDG; the
+// reference's M-norm form applies M to k, which for FR differs from R, so it is M k here.
+double Solver::entropy_vars_dot_mass(const double* st, const double* R) {
+    std::vector<double> kk((size_t)ndofs());
+    apply_inverse_mass(R, kk.data());
+    double sum = 0.0;
+    for (int c = 0; c < mesh.nc; ++c)
+        for (int i = 0; i < nd3; ++i) {
+            double u[5], v[5];
+            for (int s = 0; s < 5; ++s) u[s] = st[(size_t)c * ndofs_cell + s * nd3 + i];
+            entropy_variables(u, prm.gamma, v);
+            const double m = node_mass(mesh, ops, c, i);
+            for (int s = 0; s < 5; ++s) sum += v[s] * m * kk[(size_t)c * ndofs_cell + s * nd3 + i];
+        }
+    return sum;
+}
+
+double Solver::relaxation_parameter(const double* un, const std::vector<std::vector<double>>& k, const double* b,
+                                    int ns, double dt, double est) {
+    if (prm.flux_nodes != GLL) throw std::runtime_error("relaxation RK: GLL flux nodes only");
+    const size_t N = ndofs();
+    std::vector<double> d(N, 0.0), tmp(N);
+    for (int i = 0; i < ns; ++i)
+        for (size_t m = 0; m < N; ++m) d[m] += b[i] * k[i][m];
+    for (size_t m = 0; m < N; ++m) d[m] *= dt;
+    const double eta_n = numerical_entropy(un);
+    auto root = [&](double g) {
+        for (size_t m = 0; m < N; ++m) tmp[m] = un[m] + g * d[m];
+        return numerical_entropy(tmp.data()) - eta_n - g * est;
+    };
+    // secant from the previous parameter, with the reference's safeguards; bisection if it fails
+    const int iter_limit = 100;
+    int iter = 0;
+    double g_kp1 = 0.0;
+    bool secant_failed = false;
+    {
+        double residual = 1.0;
+        double g_k = rrk_gamma + 1e-5, g_km1 = rrk_gamma - 1e-5;
+        double r_k = root(g_k), r_km1 = root(g_km1);
+        while (residual > prm.rrk_tol && iter < iter_limit) {
+            if (r_km1 == r_k) { g_k *= 1.001; r_km1 = root(g_km1); r_k = root(g_k); }
+            if (g_k < 0.5 || g_k > 1.5) { g_k = 1.0; r_k = root(g_k); }
+            g_kp1 = g_k - r_k * (g_k - g_km1) / (r_k - r_km1);
+            residual = std::fabs(g_kp1 - g_k);
+            ++iter;
+            g_km1 = g_k; g_k = g_kp1; r_km1 = r_k; r_k = root(g_k);
+            if (std::isnan(g_k) || std::isnan(g_km1)) {
+                g_k = 1.0 - 1e-5; r_k = root(g_k); g_km1 = 1.0 + 1e-5; r_km1 = root(g_km1); residual = 1.0;
+            }
+        }
+        if (iter == iter_limit) secant_failed = true;
+    }
+    if (secant_failed) {
+        iter = 0;
+        double lo = rrk_gamma - 0.1, hi = rrk_gamma + 0.1;
+        double r_lo = root(lo), r_hi = root(hi), residual = 1.0;
+        while (residual > prm.rrk_tol && iter < iter_limit) {
+            if (r_lo * r_hi > 0) { lo -= 0.1; hi += 0.1; }
+            g_kp1 = 0.5 * (lo + hi);
+            const double r = root(g_kp1);
+            if (r < 0) { lo = g_kp1; r_lo = r; } else { hi = g_kp1; r_hi = r; }
+            residual = hi - lo;
+            ++iter;
+        }
+        if (iter == iter_limit) throw std::runtime_error("relaxation RK: root finding failed");
+    }
+    if (g_kp1 < 0.5) throw std::runtime_error("relaxation RK: no reasonable relaxation factor");
+    rrk_gamma = g_kp1;
+    return g_kp1;
 }
 
 void Solver::interpolate_ic(double* U, int ic, const double* icp) {

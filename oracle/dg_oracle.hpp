@@ -58,6 +58,8 @@ struct Params {
     double sipg_penalty_factor = 1.0;
     int non_physical = RETURN_BIG_NUMBER;
     double atol = 1e-3, rtol = 1e-3;   // low-storage error estimate
+    int use_rrk = 0;                   // relaxation Runge-Kutta (root-finding, entropy)
+    double rrk_tol = 5e-10;            // relaxation_runge_kutta_root_tolerance
 };
 
 // One-dimensional operators on the reference interval [0,1]
@@ -131,6 +133,13 @@ struct Solver {
     void rk_step(double* U, double dt);
     // one low-storage 3S* / 3S*+ step, leaving its error estimate in last_error
     void lsrk_step(double* U, double dt);
+    // relaxation Runge-Kutta: the last step's relaxation parameter (also the next step's
+    // initial guess, rrk_ode_solver_base.h:28) and the integrated numerical entropy
+    double rrk_gamma = 1.0;
+    double numerical_entropy(const double* U) const;
+    double entropy_vars_dot_mass(const double* st, const double* R);
+    double relaxation_parameter(const double* un, const std::vector<std::vector<double>>& k, const double* b,
+                                int ns, double dt, double est);
     // nodal interpolation of an initial condition (set_initial_condition.cpp:51)
     void interpolate_ic(double* U, int ic, const double* ic_params);
     // TGV integrated quantities (periodic_turbulence.cpp:439-672):

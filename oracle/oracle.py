@@ -37,9 +37,9 @@ class OrcParams(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in (
         "poly_degree", "overintegration", "flux_nodes", "pde", "use_split_form", "two_point",
         "conv_flux", "diss_flux", "fr_type", "fr_aux_type", "rk_method", "use_constant_viscosity",
-        "non_physical", "pad0")] + [(n, ctypes.c_double) for n in (
+        "non_physical", "use_rrk")] + [(n, ctypes.c_double) for n in (
         "fr_user_value", "gamma", "mach_inf", "reynolds_inf", "prandtl", "temperature_inf",
-        "constant_viscosity", "sipg_penalty_factor", "atol", "rtol")]
+        "constant_viscosity", "sipg_penalty_factor", "atol", "rtol", "rrk_tol")]
 
 
 _lib = None
@@ -72,10 +72,12 @@ def lib():
         L.orc_residual.argtypes = [vp, dp, dp]
         L.orc_aux.argtypes = [vp, dp]
         L.orc_inverse_mass.argtypes = [vp, dp, dp]
-        L.orc_rk_step.argtypes = [vp, dp, ctypes.c_double]
+        L.orc_rk_step.argtypes = [vp, dp, ctypes.c_double]; L.orc_rk_step.restype = ctypes.c_int
         L.orc_integrals.argtypes = [vp, dp, dp]
         L.orc_integrated_quantities.argtypes = [vp, dp, dp]
         L.orc_rk_error.argtypes = [vp]; L.orc_rk_error.restype = ctypes.c_double
+        L.orc_rrk_gamma.argtypes = [vp]; L.orc_rrk_gamma.restype = ctypes.c_double
+        L.orc_numerical_entropy.argtypes = [vp, dp]; L.orc_numerical_entropy.restype = ctypes.c_double
         _lib = L
     return _lib
 
@@ -112,6 +114,8 @@ def make_params(cfg: dict) -> OrcParams:
     p.non_physical = {"return_big_number": 0, "abort_run": 1, "print_warning": 2}[cfg.get("non_physical_behavior", "return_big_number")]
     p.atol = cfg.get("atol", 1e-3)
     p.rtol = cfg.get("rtol", 1e-3)
+    p.use_rrk = int(cfg.get("use_relaxation_runge_kutta", False))
+    p.rrk_tol = cfg.get("relaxation_runge_kutta_root_tolerance", 5e-10)
     return p
 
 
@@ -189,7 +193,16 @@ class Oracle:
         return out
 
     def rk_step(self, U, dt):
-        lib().orc_rk_step(self.h, _dp(U), dt)
+        if lib().orc_rk_step(self.h, _dp(U), dt) != 0:
+            raise RuntimeError("oracle RK step failed (relaxation root finding)")
+
+    def rrk_gamma(self) -> float:
+        """Relaxation parameter of the last relaxation-RK step (1 before the first)."""
+        return float(lib().orc_rrk_gamma(self.h))
+
+    def numerical_entropy(self, U) -> float:
+        """Integrated numerical entropy sum W det J (-rho log(p rho^-gamma)) over the nodes."""
+        return float(lib().orc_numerical_entropy(self.h, _dp(np.ascontiguousarray(U))))
 
     def rk_error(self) -> float:
         """Weighted RMS error estimate of the last low-storage step."""

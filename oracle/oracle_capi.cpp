@@ -17,9 +17,9 @@ extern "C" {
 
 struct orc_params {
     int poly_degree, overintegration, flux_nodes, pde, use_split_form, two_point, conv_flux, diss_flux;
-    int fr_type, fr_aux_type, rk_method, use_constant_viscosity, non_physical, pad0;
+    int fr_type, fr_aux_type, rk_method, use_constant_viscosity, non_physical, use_rrk;
     double fr_user_value, gamma, mach_inf, reynolds_inf, prandtl, temperature_inf, constant_viscosity,
-        sipg_penalty_factor, atol, rtol;
+        sipg_penalty_factor, atol, rtol, rrk_tol;
 };
 
 static Params to_params(const orc_params* p) {
@@ -33,6 +33,7 @@ static Params to_params(const orc_params* p) {
     q.constant_viscosity = p->constant_viscosity; q.sipg_penalty_factor = p->sipg_penalty_factor;
     q.non_physical = p->non_physical;
     q.atol = p->atol; q.rtol = p->rtol;
+    q.use_rrk = p->use_rrk; q.rrk_tol = p->rrk_tol;
     return q;
 }
 
@@ -62,6 +63,8 @@ int orc_create_curved(const orc_params* p, int n, double left, double right, int
 }
 // weighted RMS error estimate of the last low-storage step
 double orc_rk_error(void* h) { return static_cast<Solver*>(h)->last_error; }
+double orc_rrk_gamma(void* h) { return static_cast<Solver*>(h)->rrk_gamma; }
+double orc_numerical_entropy(void* h, const double* U) { return static_cast<Solver*>(h)->numerical_entropy(U); }
 void orc_destroy(void* h) { delete static_cast<Solver*>(h); }
 long long orc_ndofs(void* h) { return (long long)static_cast<Solver*>(h)->ndofs(); }
 int orc_nd(void* h) { return static_cast<Solver*>(h)->ops.nd; }
@@ -107,7 +110,15 @@ void orc_aux(void* h, double* out) {
     std::memcpy(out, s->aux.data(), s->aux.size() * sizeof(double));
 }
 void orc_inverse_mass(void* h, const double* in, double* out) { static_cast<Solver*>(h)->apply_inverse_mass(in, out); }
-void orc_rk_step(void* h, double* U, double dt) { static_cast<Solver*>(h)->rk_step(U, dt); }
+int orc_rk_step(void* h, double* U, double dt) {
+    try {
+        static_cast<Solver*>(h)->rk_step(U, dt);
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "oracle: %s\n", e.what());
+        return 1;
+    }
+}
 void orc_integrals(void* h, const double* U, double* out) { static_cast<Solver*>(h)->integrals(U, out); }
 void orc_integrated_quantities(void* h, const double* U, double* out) {
     static_cast<Solver*>(h)->integrated_quantities(U, out);

@@ -28,7 +28,7 @@ EXPORTED = ["ph_ctx_create", "ph_ctx_destroy", "ph_ndofs", "ph_cell_ijk", "ph_se
             "ph_batch_progress", "ph_batch_active", "ph_batch_get_state", "ph_batch_status", "ph_batch_release",
             "ph_batch_poll", "ph_batch_fence", "ph_batch_fence_wait", "ph_batch_autotune", "ph_batch_set_variant",
             "ph_batch_launches", "ph_mesh_node_xyz", "ph_rk_error_norm", "ph_last_error",
-            "ph_integrated_quantities", "ph_run"]
+            "ph_integrated_quantities", "ph_run", "ph_rk_relaxation"]
 
 
 class PhParams(ctypes.Structure):
@@ -39,7 +39,8 @@ class PhParams(ctypes.Structure):
         "precision")] + [(n, ctypes.c_double) for n in (
         "FR_user_specified_correction_parameter_value", "gamma_gas", "mach_infinity", "reynolds_number_inf",
         "prandtl_number", "temperature_inf", "nondimensionalized_constant_viscosity", "sipg_penalty_factor",
-        "rk_atol", "rk_rtol", "pressure_shift")]
+        "rk_atol", "rk_rtol", "pressure_shift")] + [
+        ("use_relaxation_runge_kutta", ctypes.c_int), ("relaxation_runge_kutta_root_tolerance", ctypes.c_double)]
 
 
 class PhMeshDesc(ctypes.Structure):
@@ -81,6 +82,7 @@ def load(build_if_missing: bool = False):
     L.ph_integrals.argtypes = [vp, dp]
     L.ph_integrated_quantities.argtypes = [vp, dp]
     L.ph_run.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, dp]
+    L.ph_rk_relaxation.argtypes = [vp, dp, dp]
     L.ph_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32)]
     L.ph_sync.argtypes = [vp]
     L.ph_set_timing.argtypes = [vp, ctypes.c_int]

@@ -622,6 +622,14 @@ struct ph_ctx {
     LowStorageTableau ls;
     double* d_err = nullptr;            // per-tile squared scaled errors of the last low-storage step
     int err_tiles = 0;
+    // relaxation RK: per-stage per-tile sums of v^T M k, per-cell entropy partials, the last
+    // parameter (the next step's initial guess) and the time advanced by the last call
+    bool rrk = false;
+    double* d_ent = nullptr;
+    double* d_ent_cell = nullptr;
+    int ent_tiles = 0;
+    double rrk_gamma = 1.0, rrk_elapsed = 0.0;
+    std::vector<double> h_ent;
     std::vector<double> h_partial;
     // optional per-kernel timing (CUDA events on the context stream)
     bool timing = false;
@@ -731,6 +739,16 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
     const bool ec = prm->conv_num_flux >= 3;
     if (ec && !prm->use_split_form)
         return fail(PH_ERR_INVALID, "two point flux and not using split form are not compatible");   // numerical_flux_factory.cpp
+    if (prm->use_relaxation_runge_kutta) {
+        // ode_solver_factory.cpp:343-369: Euler / Navier-Stokes take the root-finding form, KG has no
+        // assigned numerical entropy
+        if (prm->two_point_num_flux_type == ph::TP_KG)
+            return fail(PH_ERR_UNSUPPORTED, "relaxation RK: the KG two-point flux has no numerical entropy");
+        if (prm->runge_kutta_method >= 7) return fail(PH_ERR_UNSUPPORTED, "relaxation RK: the Butcher methods");
+        if (prm->precision != PH_FP64) return fail(PH_ERR_UNSUPPORTED, "relaxation RK: the FP64 path");
+        if (!(prm->relaxation_runge_kutta_root_tolerance > 0.0))
+            return fail(PH_ERR_INVALID, "relaxation_runge_kutta_root_tolerance must be positive");
+    }
     ph_ctx* c = new ph_ctx();
     c->prm = *prm;
     c->n = mesh->n_cells_per_direction;
@@ -779,6 +797,12 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
     bad |= dalloc(&c->d_acc, N);
     if (c->ns == 3 || (c->lowstorage && c->ls.plus)) bad |= dalloc(&c->d_carry, N);   // SSPRK3 carry / 3S*+ S4
     if (c->lowstorage) bad |= dalloc(&c->d_err, (size_t)c->nc);
+    c->rrk = prm->use_relaxation_runge_kutta != 0;
+    if (c->rrk) {
+        c->ent_tiles = c->nc;   // at most one tile per cell
+        bad |= dalloc(&c->d_ent, (size_t)c->ns * c->ent_tiles);
+        bad |= dalloc(&c->d_ent_cell, (size_t)c->nc);
+    }
     if (c->visc) {   // viscous terms, stored in the arithmetic type (floats in the precision form)
         const size_t vt = (size_t)c->nc * (4 * c->NP + 24 * c->N1 * c->N1);
         bad |= dalloc(&c->d_fv, c->fp32 ? (vt + 1) / 2 : vt);
@@ -828,7 +852,7 @@ int ph_ctx_destroy(ph_ctx* c) {
     }
     void* ptrs[] = {c->d_nbr, c->d_ops, c->d_itab, c->d_sol, c->d_stA, c->d_stB, c->d_acc, c->d_carry,
                     c->d_fv, c->d_comp, c->d_tmpA, c->d_tmpB, c->d_partial, c->d_status, c->d_metric, c->d_xnode, c->d_origin, c->d_err,
-                    c->d_table, c->d_counter};
+                    c->d_table, c->d_counter, c->d_ent, c->d_ent_cell};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -949,6 +973,136 @@ static int rk_one_step(ph_ctx* c, double dt) {
     return PH_OK;
 }
 
+// tiles (CTAs) of one stage-kernel launch
+static int stage_tiles(const ph_ctx* c) {
+    int threads = 0, cpc = 1;
+    size_t smem = 0;
+    switch (c->N1) {
+    case 2: ph::stage_launch_shape<2>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
+    case 3: ph::stage_launch_shape<3>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
+    case 4: ph::stage_launch_shape<4>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
+    case 5: ph::stage_launch_shape<5>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
+    case 6: ph::stage_launch_shape<6>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
+    default: ph::stage_launch_shape<7>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
+    }
+    return (c->nc + cpc - 1) / cpc;
+}
+
+static __global__ void rrk_apply_kernel(double* __restrict__ sol, const double* __restrict__ u1, double g, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        sol[i] = sol[i] + g * (u1[i] - sol[i]);
+}
+
+// Integrated numerical entropy of u_n + g (u1 - u_n): per-cell partials on the device,
+// summed on the host in cell order (the same value on every run).
+static int rrk_entropy(ph_ctx* c, const double* u1, double g, double* out) {
+    const double h3 = c->h * c->h * c->h;
+    const double* metric = c->curv ? c->d_metric : nullptr;
+    cudaError_t e;
+    switch (c->N1) {
+#define PH_RRK_CASE(n) \
+    case n: e = ph::launch_rrk_entropy<n>(c->d_sol, u1, g, c->d_ops, c->nc, h3, metric, c->prm.gamma_gas, c->d_ent_cell, \
+                                          c->stream); break;
+    PH_RRK_CASE(2) PH_RRK_CASE(3) PH_RRK_CASE(4) PH_RRK_CASE(5) PH_RRK_CASE(6) PH_RRK_CASE(7)
+#undef PH_RRK_CASE
+    default: return fail(PH_ERR_UNSUPPORTED, "polynomial degree");
+    }
+    if (e != cudaSuccess) return fail(PH_ERR_CUDA, cudaGetErrorString(e));
+    ++c->launches;
+    c->h_ent.resize((size_t)c->nc);
+    PH_CUDA(cudaMemcpyAsync(c->h_ent.data(), c->d_ent_cell, c->nc * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    PH_CUDA(cudaStreamSynchronize(c->stream));
+    double sum = 0.0;
+    for (int i = 0; i < c->nc; ++i) sum += c->h_ent[i];
+    *out = sum;
+    return PH_OK;
+}
+
+// One relaxation-RK step (RungeKuttaBase::step_in_time with RootFindingRRKODESolver,
+// runge_kutta_base.cpp:21-39, root_finding_rrk_ode_solver.cpp:15-180): the stages as
+// rk_one_step takes them, with v(u_i)^T M k_i reduced in each stage's epilogue and the last
+// stage's u_n + dt sum b_i k_i written beside u_n; the relaxation parameter gamma is the root of
+// eta(u_n + gamma d) - eta(u_n) - gamma dt sum_i b_i v_i^T M k_i (secant from the previous
+// gamma, the reference's safeguards, bisection as the fallback), and u_{n+1} = u_n + gamma d.
+static int rrk_one_step(ph_ctx* c, double dt) {
+    const int ns = c->ns;
+    const RkBuffers B{c->d_sol, c->d_stA, c->d_stB, c->d_acc, c->d_carry, c->d_comp};
+    // the last stage reads stA (ns even) or stB (ns odd, > 1); its output goes to the other one
+    double* u1 = (ns == 1) ? B.stA : ((ns - 2) % 2 == 0 ? B.stB : B.stA);
+    const int tiles = stage_tiles(c);
+    for (int i = 0; i < ns; ++i) {
+        const double* in = rk_stage_input(B, i);
+        if (c->visc) if (int rc = dispatch_aux(c, in)) return rc;
+        ph::StageArgs a = base_args(c, in);
+        rk_stage_args(a, B, i, ns, c->A, c->b, dt, c->fp32);
+        if (i == ns - 1) a.final_out = u1;
+        a.ent_partial = c->d_ent + (size_t)i * c->ent_tiles;
+        if (int rc = dispatch_stage(c, a)) return rc;
+    }
+    std::vector<double> part((size_t)ns * c->ent_tiles);
+    PH_CUDA(cudaMemcpyAsync(part.data(), c->d_ent, part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    PH_CUDA(cudaStreamSynchronize(c->stream));
+    double est = 0.0;
+    for (int i = 0; i < ns; ++i) {
+        double si = 0.0;
+        for (int t = 0; t < tiles; ++t) si += part[(size_t)i * c->ent_tiles + t];
+        est += c->b[i] * si;
+    }
+    est *= dt;
+    double eta_n = 0.0;
+    if (int rc = rrk_entropy(c, u1, 0.0, &eta_n)) return rc;
+    int rc = PH_OK;
+    auto root = [&](double g) {
+        double eta = 0.0;
+        if (!rc) rc = rrk_entropy(c, u1, g, &eta);
+        return eta - eta_n - g * est;
+    };
+    const double tol = c->prm.relaxation_runge_kutta_root_tolerance;
+    const int iter_limit = 100;
+    int iter = 0;
+    double g_kp1 = 0.0;
+    bool secant_failed = false;
+    {
+        double residual = 1.0;
+        double g_k = c->rrk_gamma + 1e-5, g_km1 = c->rrk_gamma - 1e-5;
+        double r_k = root(g_k), r_km1 = root(g_km1);
+        while (residual > tol && iter < iter_limit && !rc) {
+            if (r_km1 == r_k) { g_k *= 1.001; r_km1 = root(g_km1); r_k = root(g_k); }
+            if (g_k < 0.5 || g_k > 1.5) { g_k = 1.0; r_k = root(g_k); }
+            g_kp1 = g_k - r_k * (g_k - g_km1) / (r_k - r_km1);
+            residual = std::fabs(g_kp1 - g_k);
+            ++iter;
+            g_km1 = g_k; g_k = g_kp1; r_km1 = r_k; r_k = root(g_k);
+            if (std::isnan(g_k) || std::isnan(g_km1)) {
+                g_k = 1.0 - 1e-5; r_k = root(g_k); g_km1 = 1.0 + 1e-5; r_km1 = root(g_km1); residual = 1.0;
+            }
+        }
+        if (iter == iter_limit) secant_failed = true;
+    }
+    if (secant_failed && !rc) {
+        iter = 0;
+        double lo = c->rrk_gamma - 0.1, hi = c->rrk_gamma + 0.1;
+        double r_lo = root(lo), r_hi = root(hi), residual = 1.0;
+        while (residual > tol && iter < iter_limit && !rc) {
+            if (r_lo * r_hi > 0) { lo -= 0.1; hi += 0.1; }
+            g_kp1 = 0.5 * (lo + hi);
+            const double r = root(g_kp1);
+            if (r < 0) { lo = g_kp1; r_lo = r; } else { hi = g_kp1; r_hi = r; }
+            residual = hi - lo;
+            ++iter;
+        }
+        if (iter == iter_limit && !rc) return fail(PH_ERR_INVALID, "relaxation RK: root finding did not converge");
+    }
+    if (rc) return rc;
+    if (!(g_kp1 >= 0.5)) return fail(PH_ERR_INVALID, "relaxation RK: no reasonable relaxation parameter (< 0.5)");
+    rrk_apply_kernel<<<1184, 256, 0, c->stream>>>(c->d_sol, u1, g_kp1, c->ndofs);
+    PH_CUDA(cudaGetLastError());
+    ++c->launches;
+    c->rrk_gamma = g_kp1;
+    c->rrk_elapsed += g_kp1 * dt;
+    return PH_OK;
+}
+
 // Capture one RK step (all stages, auxiliary kernels included) as a graph for this dt.
 static int capture_step_graph(ph_ctx* c, double dt) {
     if (c->step_graph) { cudaGraphExecDestroy(c->step_graph); c->step_graph = nullptr; }
@@ -973,6 +1127,13 @@ static int capture_step_graph(ph_ctx* c, double dt) {
 
 int ph_rk_step(ph_ctx* c, double dt, int nsteps) {
     if (!c || nsteps < 0) return fail(PH_ERR_INVALID, "bad argument");
+    if (c->rrk) {   // the root finding reads sums back after every step: direct launches
+        c->rrk_elapsed = 0.0;
+        for (int s = 0; s < nsteps; ++s)
+            if (int rc = rrk_one_step(c, dt)) return rc;
+        return PH_OK;
+    }
+    c->rrk_elapsed = dt * nsteps;
     // several steps of one dt on a caller-given stream replay a graph of one step; the
     // per-launch timing mode and one-stage methods (which swap buffers) launch directly
     const bool graph = c->stream != nullptr && !c->timing && c->ns > 1 && nsteps > 1;
@@ -1092,8 +1253,16 @@ static int capture_run_graph(ph_ctx* c, double dt, int record_every) {
     return PH_OK;
 }
 
+int ph_rk_relaxation(ph_ctx* c, double* gamma, double* elapsed) {
+    if (!c || !gamma || !elapsed) return fail(PH_ERR_INVALID, "null argument");
+    *gamma = c->rrk ? c->rrk_gamma : 1.0;
+    *elapsed = c->rrk_elapsed;
+    return PH_OK;
+}
+
 int ph_run(ph_ctx* c, double dt, int nsteps, int record_every, double* rows) {
     if (!c || nsteps < 0 || record_every < 0) return fail(PH_ERR_INVALID, "bad argument");
+    if (c->rrk) return fail(PH_ERR_UNSUPPORTED, "ph_run: relaxation RK steps have variable length; use ph_rk_step");
     const int nrec = record_every > 0 ? nsteps / record_every : 0;
     if (nrec > 0 && !rows) return fail(PH_ERR_INVALID, "null rows");
     if (nrec > c->table_rows) {   // grow the device table (synchronises the stream)

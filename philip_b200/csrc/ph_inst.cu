@@ -30,9 +30,10 @@ static cudaError_t launch_one(const StageArgs& a, cudaStream_t s) {
 
 template <typename R, int N1>
 static cudaError_t launch_prec(const StageArgs& a, bool visc, bool split, cudaStream_t s) {
-    // the Chandrashekar + EC/Roe (+ BR2) combination has its own compile-time instance
+    // the Chandrashekar + EC/Roe (+ BR2) combination has its own compile-time instance; the
+    // relaxation RK's entropy estimate lives in the generic instance only
     const bool hot = split && a.pc.two_point == TP_CH && a.pc.conv_flux == CF_EC_ROE &&
-                     (!visc || a.pc.diss_flux == DF_BR2);
+                     (!visc || a.pc.diss_flux == DF_BR2) && a.ent_partial == nullptr;
     if (a.metric) {   // curvilinear cells: split-form Euler (checked by the host)
         if (visc || !split) return cudaErrorInvalidValue;
         return hot ? launch_one<R, N1, false, true, 1, true>(a, s) : launch_one<R, N1, false, true, 0, true>(a, s);
@@ -234,6 +235,16 @@ cudaError_t launch_integrals(const double* U, const double* X, const double* ori
              : launch_integrals_one<N1, false, false>(U, X, origin, tab, nc, ic, partial, s);
 }
 
+template <int N1>
+cudaError_t launch_rrk_entropy(const double* Un, const double* U1, double gamma, const OpTab* ops, int nc, double h3,
+                               const double* metric, double gam, double* partial, cudaStream_t s) {
+    constexpr int NP = N1 * N1 * N1;
+    rrk_entropy_kernel<N1><<<nc, ((NP + 31) / 32) * 32, 0, s>>>(Un, U1, gamma, ops, nc, h3, metric, gam, partial);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_rrk_entropy<PH_N1>(const double*, const double*, double, const OpTab*, int, double,
+                                               const double*, double, double*, cudaStream_t);
 template cudaError_t launch_stage<PH_N1>(const StageArgs&, int, bool, bool, cudaStream_t);
 template void stage_launch_shape<PH_N1>(int, bool, bool, int*, int*, size_t*);
 template cudaError_t launch_stage_batched<PH_N1>(const StageArgs*, const BatchTile*, int, int, bool, bool, int, int,

@@ -96,6 +96,9 @@ struct StageArgs {
     double ls_delta_s, ls_delta_s1, ls_inv_sum_delta;
     double* err_partial;        // per-tile sums of the squared scaled error (or nullptr)
     double atol, rtol;
+    // relaxation RK (mode 2): per-tile sums of v(u)^T M k, v the entropy variables of the
+    // stage input (or nullptr; the generic flux-set kernel, FS = 0, computes them)
+    double* ent_partial;
 };
 
 // Viscous terms per cell written by the auxiliary kernel and read by the stage kernel:
@@ -385,6 +388,92 @@ __device__ __forceinline__ void volume_dir(int d, const Cst<R>& cst, int tp, con
     }
 }
 
+// Entropy of the relaxation RK method (FP64): component s of the entropy variables
+// (Euler::compute_entropy_variables, euler.cpp:811-829) and the numerical entropy function
+// -rho log(p rho^-gamma) (compute_numerical_entropy_function, :437-447; compute_entropy,
+// :512-530), from the conservative state.
+__device__ __forceinline__ double entropy_variable(const double u[5], int s, double gam) {
+    const double p = (gam - 1.0) * (u[4] - 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0]);
+    const double ent = log(p * pow(u[0], -gam));
+    const double rt = p / (gam - 1.0);
+    if (s == 0) return (rt * (gam + 1.0 - ent) - u[4]) / rt;
+    if (s == 4) return -u[0] / rt;
+    return u[s] / rt;
+}
+__device__ __forceinline__ double numerical_entropy_fn(const double u[5], double gam) {
+    const double p = (gam - 1.0) * (u[4] - 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0]);
+    return -u[0] * log(p * pow(u[0], -gam));
+}
+
+// Integrated numerical entropy of u_n + gamma (u1 - u_n), per cell: sum over the nodes of
+// W det J eta (GLL collocation: the volume quadrature is the solution nodes). One CTA per
+// cell, fixed-order reduction.
+template <int N1>
+__global__ void rrk_entropy_kernel(const double* __restrict__ Un, const double* __restrict__ U1, double gamma,
+                                   const OpTab* __restrict__ ops, int nc, double h3,
+                                   const double* __restrict__ metric, double gam, double* __restrict__ partial) {
+    constexpr int NP = N1 * N1 * N1;
+    const int cell = blockIdx.x, node = threadIdx.x;
+    double e = 0.0;
+    if (node < NP) {
+        double u[5];
+#pragma unroll
+        for (int s = 0; s < 5; ++s) {
+            const size_t i = ((size_t)cell * 5 + s) * NP + node;
+            u[s] = Un[i] + gamma * (U1[i] - Un[i]);
+        }
+        const int x = node % N1, y = (node / N1) % N1, z = node / (N1 * N1);
+        const double W = ops->w[x] * ops->w[y] * ops->w[z];
+        const double J = metric ? 1.0 / metric[((size_t)cell * 10 + 9) * NP + node] : h3;
+        e = W * J * numerical_entropy_fn(u, gam);
+    }
+    __shared__ double red[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = e;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)((blockDim.x + 31) / 32); ++w) t += red[w];
+        partial[cell] = t;
+    }
+}
+
+// Relaxation RK: this tile's share of v(u_i)^T M k_i, the entropy variables of the stage
+// input (FP64, from the state) times M k = W det J k = W (h^2, or 1 on curvilinear cells) G
+// (RootFindingRRKODESolver::compute_entropy_change_estimate, root_finding_rrk_ode_solver.cpp:
+// 355-390), written to a.ent_partial[tile]. Compiled into the generic flux-set kernels only
+// (relaxed steps dispatch there), so the hot kernel's register allocation does not see it.
+template <typename R, int N1, int CPC, int NT, bool CURV>
+__device__ __forceinline__ void entropy_estimate_tile(const StageArgs& a, const R* sA, int cell0) {
+    constexpr int NP = N1 * N1 * N1;
+    const int tid = threadIdx.x;
+    double ent = 0.0;
+    for (int it = tid; it < CPC * 5 * NP; it += NT) {
+        const int c = it / (5 * NP), rem = it % (5 * NP), s = rem / NP, node = rem % NP;
+        const int cell = cell0 + c;
+        if (cell >= a.nc) continue;
+        double u[5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) u[q] = a.U[((size_t)cell * 5 + q) * NP + node];
+        const double v = entropy_variable(u, s, a.pc.gam);
+        const int x = node % N1, y = (node / N1) % N1, z = node / (N1 * N1);
+        const double W = a.ops->w[x] * a.ops->w[y] * a.ops->w[z];
+        const double G = (double)sA[it];
+        ent += v * (CURV ? W * G : W * a.h * a.h * G);
+    }
+    __shared__ double ered[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ent += __shfl_down_sync(0xffffffffu, ent, o);
+    if ((tid & 31) == 0) ered[tid >> 5] = ent;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (NT + 31) / 32; ++w) t += ered[w];
+        a.ent_partial[cell0 / CPC] = t;
+    }
+}
+
 // Warms L2 with the inputs a tile reads after its first phase: its own stage state, the
 // RK registers the epilogue reads (u_n, running sum, carry, Kahan term) and its block of
 // viscous terms. One L2 prefetch per 128-byte line, addresses clamped inside the tile's
@@ -516,13 +605,13 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
         if constexpr (!SPLIT) {
             constexpr int o = VISC ? 4 : 0;
             R F[5];
-            conv_flux_dir<R, 0>(q, cst.p0, F);
+            conv_flux_dir<R, 0>(q, cst.shift(), F);
 #pragma unroll
             for (int s = 0; s < 5; ++s) X[(o + 0 * 5 + s) * NP + node] = F[s];
-            conv_flux_dir<R, 1>(q, cst.p0, F);
+            conv_flux_dir<R, 1>(q, cst.shift(), F);
 #pragma unroll
             for (int s = 0; s < 5; ++s) X[(o + 1 * 5 + s) * NP + node] = F[s];
-            conv_flux_dir<R, 2>(q, cst.p0, F);
+            conv_flux_dir<R, 2>(q, cst.shift(), F);
 #pragma unroll
             for (int s = 0; s < 5; ++s) X[(o + 2 * 5 + s) * NP + node] = F[s];
         }
@@ -661,6 +750,9 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
                 a.next[dof] = (cin + a.a_next * k) * a.dt + un[r];
             }
             if (a.carry_out) a.carry_out[dof] = a.a_carry * k;
+        }
+        if constexpr (FS == 0) {
+            if (a.ent_partial) entropy_estimate_tile<R, N1, CPC, NT, CURV>(a, sA, cell0);
         }
         return;
     }

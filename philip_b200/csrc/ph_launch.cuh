@@ -25,6 +25,10 @@ cudaError_t launch_inverse_mass(const double* in, double* out, const OpTab* ops,
 template <int N1>
 cudaError_t launch_integrals(const double* U, const double* X, const double* origin, const IntegralTab* tab, int nc,
                              const IntegralConst& ic, bool full, double* partial, cudaStream_t s);
+// Relaxation RK: integrated numerical entropy of u_n + gamma (u1 - u_n), per cell
+template <int N1>
+cudaError_t launch_rrk_entropy(const double* Un, const double* U1, double gamma, const OpTab* ops, int nc, double h3,
+                               const double* metric, double gam, double* partial, cudaStream_t s);
 // Batched (many-solve) stage: split-form Euler tiles of several discretisations of the same
 // order. `variant` selects the cells-per-CTA tile shape (batched_shape lists them); grid <= 0
 // sizes the persistent grid to the resident CTAs of the whole GPU.

@@ -46,6 +46,8 @@ template <typename R> struct Cst {
         inv2gm1 = (R)(0.5 / c.gm1);
         p0 = sizeof(R) == 4 ? (R)c.pressure_shift : R(0);
     }
+    // the shift as the flux code uses it: a compile-time zero in FP64
+    __device__ __forceinline__ R shift() const { return sizeof(R) == 4 ? p0 : R(0); }
 };
 
 template <typename R> __device__ __forceinline__ R rlog(R x);
@@ -231,7 +233,7 @@ __device__ __forceinline__ void two_point_dir(const NodeQ<R>& i, const NodeQ<R>&
         F[0] = m;
 #pragma unroll
         for (int k = 0; k < 3; ++k) F[1 + k] = m * va[k];
-        F[1 + d] += p_hat - c.p0;
+        F[1 + d] += p_hat - c.shift();
         F[4] = m * (h0 + vsq);
     } else if (tp == TP_RA) {
         const R rho_log = log_mean<R>(i.a, j.a, i.la, j.la);
@@ -247,7 +249,7 @@ __device__ __forceinline__ void two_point_dir(const NodeQ<R>& i, const NodeQ<R>&
         F[0] = m;
 #pragma unroll
         for (int k = 0; k < 3; ++k) F[1 + k] = m * va[k];
-        F[1 + d] += p_hat - c.p0;
+        F[1 + d] += p_hat - c.shift();
         F[4] = m * H - R(0.5) * (i.p * i.v[d] + j.p * j.v[d]);
     } else if (tp == TP_IR) {
         const R z0a = R(0.5) * (i.a + j.a), z4a = R(0.5) * (i.b + j.b);
@@ -269,7 +271,7 @@ __device__ __forceinline__ void two_point_dir(const NodeQ<R>& i, const NodeQ<R>&
         F[0] = m;
 #pragma unroll
         for (int k = 0; k < 3; ++k) F[1 + k] = m * v[k];
-        F[1 + d] += p - c.p0;
+        F[1 + d] += p - c.shift();
         F[4] = m * H;
     } else {   // KG
         const R rho = (i.rho + j.rho) / R(2);
@@ -282,7 +284,7 @@ __device__ __forceinline__ void two_point_dir(const NodeQ<R>& i, const NodeQ<R>&
         F[0] = m;
 #pragma unroll
         for (int k = 0; k < 3; ++k) F[1 + k] = m * v[k];
-        F[1 + d] += p - c.p0;
+        F[1 + d] += p - c.shift();
         F[4] = m * e + p * v[d];
     }
 }
@@ -357,8 +359,8 @@ __device__ __forceinline__ void conv_num_flux(const R uL[5], const R uR[5], cons
         two_point_dir<R, d>(L, Rq, tp, c, out);
     } else {
         R FL[5], FR[5];
-        conv_flux_dir<R, d>(L, c.p0, FL);
-        conv_flux_dir<R, d>(Rq, c.p0, FR);
+        conv_flux_dir<R, d>(L, c.shift(), FL);
+        conv_flux_dir<R, d>(Rq, c.shift(), FR);
 #pragma unroll
         for (int k = 0; k < 5; ++k) out[k] = R(0.5) * (FL[k] + FR[k]);
     }
@@ -393,7 +395,7 @@ __device__ __forceinline__ void two_point_n(const NodeQ<R>& i, const NodeQ<R>& j
         const R m = rho_log * vn;
         F[0] = m;
 #pragma unroll
-        for (int k = 0; k < 3; ++k) F[1 + k] = m * va[k] + (p_hat - c.p0) * n[k];
+        for (int k = 0; k < 3; ++k) F[1 + k] = m * va[k] + (p_hat - c.shift()) * n[k];
         F[4] = m * (h0 + vsq);
     } else if (tp == TP_RA) {
         const R rho_log = log_mean<R>(i.a, j.a, i.la, j.la);
@@ -408,7 +410,7 @@ __device__ __forceinline__ void two_point_n(const NodeQ<R>& i, const NodeQ<R>& j
         const R m = rho_log * vn;
         F[0] = m;
 #pragma unroll
-        for (int k = 0; k < 3; ++k) F[1 + k] = m * va[k] + (p_hat - c.p0) * n[k];
+        for (int k = 0; k < 3; ++k) F[1 + k] = m * va[k] + (p_hat - c.shift()) * n[k];
         F[4] = m * H;
         R vni = R(0), vnj = R(0);
 #pragma unroll
@@ -433,7 +435,7 @@ __device__ __forceinline__ void two_point_n(const NodeQ<R>& i, const NodeQ<R>& j
         const R m = rho * vn;
         F[0] = m;
 #pragma unroll
-        for (int k = 0; k < 3; ++k) F[1 + k] = m * v[k] + (p - c.p0) * n[k];
+        for (int k = 0; k < 3; ++k) F[1 + k] = m * v[k] + (p - c.shift()) * n[k];
         F[4] = m * H;
     } else {   // KG
         const R rho = (i.rho + j.rho) / R(2);
@@ -445,7 +447,7 @@ __device__ __forceinline__ void two_point_n(const NodeQ<R>& i, const NodeQ<R>& j
         const R m = rho * vn;
         F[0] = m;
 #pragma unroll
-        for (int k = 0; k < 3; ++k) F[1 + k] = m * v[k] + (p - c.p0) * n[k];
+        for (int k = 0; k < 3; ++k) F[1 + k] = m * v[k] + (p - c.shift()) * n[k];
         F[4] = m * e + p * vn;
     }
 }
@@ -521,8 +523,8 @@ __device__ __forceinline__ void conv_num_flux_n(const R uL[5], const R uR[5], co
         two_point_n<R>(L, Rq, n, tp, c, out);
     } else {
         R FL[5], FR[5];
-        conv_flux_n<R>(L, n, c.p0, FL);
-        conv_flux_n<R>(Rq, n, c.p0, FR);
+        conv_flux_n<R>(L, n, c.shift(), FL);
+        conv_flux_n<R>(Rq, n, c.shift(), FR);
 #pragma unroll
         for (int k = 0; k < 5; ++k) out[k] = R(0.5) * (FL[k] + FR[k]);
     }

@@ -169,14 +169,23 @@ class RungeKuttaODESolver:
         self.current_time = 0.0
         self.current_iteration = 0
         self.epsilon = [1.0, 1.0, 1.0]   # step-size controller history (low_storage_runge_kutta_ode_solver.cpp:11)
+        self.relaxation_parameter = 1.0  # relaxation RK: the last step's gamma
 
     def step_in_time(self, dt: float, pseudotime: bool = False, nsteps: int = 1):
         if pseudotime:
             raise NotImplementedError("pseudotime stepping belongs to the steady solvers")
         _lib.check(self.dg.L.ph_rk_step(self.dg.handle, dt, nsteps))
-        for _ in range(nsteps):
-            self.current_iteration += 1
-            self.current_time += dt
+        if self.dg.parameters.use_relaxation_runge_kutta:
+            # each step advanced gamma dt (RungeKuttaODESolver::adjust_time_step)
+            g, elapsed = ctypes.c_double(1.0), ctypes.c_double(0.0)
+            _lib.check(self.dg.L.ph_rk_relaxation(self.dg.handle, ctypes.byref(g), ctypes.byref(elapsed)))
+            self.relaxation_parameter = float(g.value)
+            self.current_iteration += nsteps
+            self.current_time += float(elapsed.value)
+        else:
+            for _ in range(nsteps):
+                self.current_iteration += 1
+                self.current_time += dt
         self.dg.set_current_time(self.current_time)
 
     def step_in_time_with_records(self, dt: float, nsteps: int, record_every: int):
@@ -208,7 +217,7 @@ class RungeKuttaODESolver:
         from .prm import RK_ORDER
         prm = self.dg.parameters
         order = RK_ORDER[prm.get("ODE solver/runge_kutta_method")]
-        b1, b2, b3 = (float(prm.get(f"ODE solver/beta{i}")) for i in (1, 2, 3))
+        b1, b2, b3 = (float(prm.get(f"ODE solver/low-storage rk solver/beta{i}")) for i in (1, 2, 3))
         w = self.error_norm()
         self.epsilon = [1.0 / w, self.epsilon[0], self.epsilon[1]]
         e0, e1, e2 = self.epsilon
@@ -456,6 +465,7 @@ class FlowSolver:
         if not self.unsteady_data:
             self.unsteady_data.append((self.ode_solver.current_time, *self.dg.integrals()))
         if (not adaptive and not error_adaptive and not write_restart and record_every > 0
+                and not self.parameters.use_relaxation_runge_kutta
                 and self.ode_solver.current_iteration % record_every == 0):
             # the whole steps of dt run on the device with the records reduced there (ph_run);
             # the count follows the loop below step by step, so the clock is the same

@@ -47,8 +47,11 @@ DEFAULTS = {
     "flow_solver/end_exactly_at_final_time": "true",
     "flow_solver/grid/grid_left_bound": "0.0", "flow_solver/grid/grid_right_bound": "1.0",
     "flow_solver/grid/number_of_grid_elements_per_dimension": "4",
-    "ODE solver/atol": "0.001", "ODE solver/rtol": "0.001", "ODE solver/beta1": "0.70",
-    "ODE solver/beta2": "-0.23", "ODE solver/beta3": "0.0", "flow_solver/error_adaptive_time_step": "false",
+    "ODE solver/low-storage rk solver/atol": "0.001", "ODE solver/low-storage rk solver/rtol": "0.001", "ODE solver/low-storage rk solver/beta1": "0.70",
+    "ODE solver/low-storage rk solver/beta2": "-0.23", "ODE solver/low-storage rk solver/beta3": "0.0", "flow_solver/error_adaptive_time_step": "false",
+    "ODE solver/rrk root solver/use_relaxation_runge_kutta": "false",
+    "ODE solver/rrk root solver/relaxation_runge_kutta_root_tolerance": "5e-10",
+    "ODE solver/rrk root solver/rrk_root_solver_output": "quiet",
     "ODE solver/initial_time": "0.0", "ODE solver/initial_iteration": "0", "ODE solver/initial_time_step": "100.0",
     "ODE solver/initial_desired_time_for_output_solution_every_dt_time_intervals": "0.0",
     "flow_solver/unsteady_data_table_filename": "unsteady_data_table",
@@ -171,6 +174,13 @@ class Parameters:
         return int(self.get("flow_solver/grid/number_of_grid_elements_per_dimension"))
 
     @property
+    def use_relaxation_runge_kutta(self) -> bool:
+        """ODE solver/rrk root solver/use_relaxation_runge_kutta, or the deprecated
+        ode_solver_type = rrk_explicit (parameters_ode_solver.cpp:299-315)."""
+        return (_b(self.get("ODE solver/rrk root solver/use_relaxation_runge_kutta"))
+                or self.get("ODE solver/ode_solver_type") == "rrk_explicit")
+
+    @property
     def grid_bounds(self):
         return float(self.get("flow_solver/grid/grid_left_bound")), float(self.get("flow_solver/grid/grid_right_bound"))
 
@@ -195,8 +205,8 @@ class Parameters:
             raise ValueError(f"flux_reconstruction_aux {aux!r}: the B200 path implements kDG")
         p.flux_reconstruction_aux = FR_AUX[aux]
         p.FR_user_specified_correction_parameter_value = float(self.get("FR_user_specified_correction_parameter_value"))
-        if self.get("ODE solver/ode_solver_type") != "runge_kutta":
-            raise ValueError("ode_solver_type must be runge_kutta (explicit Butcher RK)")
+        if self.get("ODE solver/ode_solver_type") not in ("runge_kutta", "rrk_explicit"):
+            raise ValueError("ode_solver_type must be runge_kutta (explicit RK)")
         p.runge_kutta_method = RK[self.get("ODE solver/runge_kutta_method")]
         p.gamma_gas = float(self.get("euler/gamma_gas"))
         p.mach_infinity = float(self.get("euler/mach_infinity"))
@@ -211,8 +221,11 @@ class Parameters:
         p.sipg_penalty_factor = sipg
         p.non_physical_behavior = NON_PHYSICAL[self.get("non_physical_behavior")]
         p.precision = precision
-        p.rk_atol = float(self.get("ODE solver/atol"))
-        p.rk_rtol = float(self.get("ODE solver/rtol"))
+        p.rk_atol = float(self.get("ODE solver/low-storage rk solver/atol"))
+        p.rk_rtol = float(self.get("ODE solver/low-storage rk solver/rtol"))
+        p.use_relaxation_runge_kutta = int(self.use_relaxation_runge_kutta)
+        p.relaxation_runge_kutta_root_tolerance = float(
+            self.get("ODE solver/rrk root solver/relaxation_runge_kutta_root_tolerance"))
         p.pressure_shift = self.reference_pressure()
         return p
 
@@ -247,5 +260,8 @@ class Parameters:
             "use_constant_viscosity": _b(self.get("navier_stokes/use_constant_viscosity")),
             "sipg_penalty_factor": float(self.get("sipg_penalty_factor")),
             "FR_user_specified_correction_parameter_value": float(self.get("FR_user_specified_correction_parameter_value")),
-            "atol": float(self.get("ODE solver/atol")), "rtol": float(self.get("ODE solver/rtol")),
+            "atol": float(self.get("ODE solver/low-storage rk solver/atol")), "rtol": float(self.get("ODE solver/low-storage rk solver/rtol")),
+            "use_relaxation_runge_kutta": self.use_relaxation_runge_kutta,
+            "relaxation_runge_kutta_root_tolerance": float(
+                self.get("ODE solver/rrk root solver/relaxation_runge_kutta_root_tolerance")),
         }
