@@ -37,7 +37,7 @@
 #define PH_P3_MINB 6
 #endif
 #ifndef PH_P3_MINB_F32
-#define PH_P3_MINB_F32 8
+#define PH_P3_MINB_F32 10
 #endif
 
 namespace ph {
@@ -133,7 +133,7 @@ struct Layout {
     static constexpr int NT = WARPS_LINES * 32;
     // register budgets from timing the stage kernel on B200: p = 5 (one cell, 256 threads
     // per CTA) 4 CTAs per SM in FP64 (2-5 % faster than 3), 6 in FP32 (3-4 % faster than 4);
-    // p = 3 (two cells, 128 threads) 6 in FP64 and 8 in FP32 (3 % faster than unbounded)
+    // p = 3 (two cells, 128 threads) 6 in FP64 and 10 in FP32 (3 % faster than 8)
     static constexpr bool F32 = sizeof(R) == 4;
     static constexpr int MINB = (N1 == 6) ? (F32 ? PH_P5_MINB_F32 : PH_P5_MINB)
                               : (N1 == 4) ? (F32 ? PH_P3_MINB_F32 : PH_P3_MINB) : 1;
