@@ -135,8 +135,10 @@ struct Layout {
     // per CTA) 4 CTAs per SM in FP64 (2-5 % faster than 3), 6 in FP32 (3-4 % faster than 4);
     // p = 3 (two cells, 128 threads) 6 in FP64 and 10 in FP32 (3 % faster than 8)
     static constexpr bool F32 = sizeof(R) == 4;
-    static constexpr int MINB = (N1 == 6) ? (F32 ? PH_P5_MINB_F32 : PH_P5_MINB)
-                              : (N1 == 4) ? (F32 ? PH_P3_MINB_F32 : PH_P3_MINB) : 1;
+    static constexpr int MINB_ASKED = (N1 == 6) ? (F32 ? PH_P5_MINB_F32 : PH_P5_MINB)
+                                    : (N1 == 4) ? (F32 ? PH_P3_MINB_F32 : PH_P3_MINB) : 1;
+    // never more CTAs than 2048 threads per SM hold (the batched tile shapes are wider)
+    static constexpr int MINB = MINB_ASKED * NT > 2048 ? 2048 / NT : MINB_ASKED;
 };
 
 template <int N1> __device__ __forceinline__ int node_of(int x, int y, int z) { return (z * N1 + y) * N1 + x; }
