@@ -29,7 +29,8 @@ enum {
     PH_ERR_INVALID = 1,      /* bad argument */
     PH_ERR_UNSUPPORTED = 2,  /* configuration outside the GPU path (e.g. GL flux nodes) */
     PH_ERR_CUDA = 3,         /* CUDA runtime failure */
-    PH_ERR_NOMEM = 4         /* device allocation failed */
+    PH_ERR_NOMEM = 4,        /* device allocation failed */
+    PH_ERR_EXCHANGE = 5      /* the halo exchange callback of a slab context failed */
 };
 
 enum { PH_HOST = 0, PH_DEVICE = 1 };                 /* where a pointer lives */
@@ -214,6 +215,54 @@ int ph_status(ph_ctx* ctx, uint32_t* flags);
  * ph_set_timing call (counted with timing enabled or not). */
 int ph_set_timing(ph_ctx* ctx, int enable);
 int ph_get_timing(ph_ctx* ctx, double out[7]);
+
+/* ---- One mesh over several GPUs: slabs of cell layers and a halo exchange ----
+ * The reference distributes the triangulation over MPI ranks and refreshes the ghost values
+ * of the solution before every residual (DGBase::assemble_residual, src/dg/dg_base.cpp:2742)
+ * and of the auxiliary solution before the viscous face terms (src/dg/strong_dg.cpp:648).
+ * Here a rank owns the cell layers z_first .. z_first + z_count - 1 (periodically) of the
+ * affine periodic cube and keeps one ghost layer below and one above. Before each residual
+ * evaluation the library packs, for each partition face, only what the neighbour's kernels
+ * read: the state at the face nodes (5 (p+1)^2 doubles per cell) and, for Navier-Stokes, after
+ * the auxiliary kernel, the face-normal viscous flux (4 (p+1)^2 values per cell in the
+ * arithmetic type). The transfer itself is the caller's (NCCL, CUDA-aware MPI, peer copies),
+ * through the callback below; the cells that read no ghost data are computed while the
+ * transfer is in flight.
+ *
+ * Owned cells are numbered lexicographically (x fastest, then y, then z from z_first; see
+ * ph_cell_ijk), whatever mesh->cell_order says; the state, ph_ndofs and the integrals cover
+ * the owned cells only (ph_integrals / ph_integrated_quantities give this rank's share of
+ * each volume average: sum them over ranks, and take the max of the wave speed). Slab
+ * contexts take affine meshes, no relaxation RK, and launch directly (no step graph,
+ * ph_run refused). z_count = n is the whole mesh without ghosts. */
+enum { PH_HALO_STATE = 0, PH_HALO_VISCOUS = 1 };   /* what is exchanged */
+enum { PH_HALO_BEGIN = 0, PH_HALO_END = 1 };        /* phase of the exchange */
+
+/* Called twice per exchange, on the host thread that called the library:
+ *   phase PH_HALO_BEGIN: send_lo (the first owned layer's data, for the rank that owns the layer
+ *     below) and send_hi (the last layer's, for the rank above) are packed in stream order on
+ *     cuda_stream; the callback starts the transfer of send_lo to the rank below and of send_hi to
+ *     the rank above, and the receipt into recv_lo (from the rank below, its send_hi) and recv_hi
+ *     (from the rank above, its send_lo). Ordered after the packing (e.g. NCCL send/recv enqueued
+ *     on, or made to wait on, cuda_stream). With two ranks the rank below and above are the same:
+ *     deliver the downward pair (send_lo -> recv_hi) before the upward pair.
+ *   phase PH_HALO_END: the receive buffers must be complete in cuda_stream order when it returns
+ *     (a stream wait on the transfer, or a synchronous copy), and the send buffers free for reuse.
+ * bytes: the size of each of the four buffers (device memory, the library's). A nonzero return
+ * fails the calling entry point with PH_ERR_EXCHANGE. */
+typedef int (*ph_halo_fn)(void* user, int what, int phase, const void* send_lo, const void* send_hi,
+                          void* recv_lo, void* recv_hi, size_t bytes, void* cuda_stream);
+
+/* A context for the slab z_first .. z_first + z_count - 1 of mesh (1 <= z_count <= n). */
+int ph_ctx_create_slab(const ph_mesh_desc* mesh, const ph_params* prm, int z_first, int z_count,
+                       void* cuda_stream, ph_ctx** out);
+/* Registers the exchange; every slab context with z_count < n needs one before it steps. */
+int ph_set_halo_exchange(ph_ctx* ctx, ph_halo_fn fn, void* user);
+/* Host only (no device work): the owned cells' (i, j, k) [z_count n^2][3] and neighbour table
+ * [z_count n^2][6] (faces x-, x+, y-, y+, z-, z+) of a slab. A neighbour index below z_count n^2
+ * is an owned cell; z_count n^2 + j n + i is the lower ghost (the cell (i, j) of layer
+ * z_first - 1, filled from the rank below), z_count n^2 + n^2 + j n + i the upper ghost. */
+int ph_slab_connectivity(int n, int z_first, int z_count, int32_t* ijk, int32_t* nbr);
 
 /* R(U) as ph_residual computes it, on caller-owned DEVICE buffers U and R, without a
  * context and without allocating device memory. No counterpart in the reference: it

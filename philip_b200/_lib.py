@@ -13,13 +13,16 @@ LIB_PATH = os.environ.get("PHILIP_B200_LIB", os.path.join(_HERE, "libphilip_b200
 
 PH_HOST, PH_DEVICE = 0, 1
 PH_FP64, PH_FP32_RESIDUAL = 0, 1
-PH_OK, PH_ERR_INVALID, PH_ERR_UNSUPPORTED, PH_ERR_CUDA, PH_ERR_NOMEM = 0, 1, 2, 3, 4
+PH_OK, PH_ERR_INVALID, PH_ERR_UNSUPPORTED, PH_ERR_CUDA, PH_ERR_NOMEM, PH_ERR_EXCHANGE = 0, 1, 2, 3, 4, 5
+PH_HALO_STATE, PH_HALO_VISCOUS = 0, 1
+PH_HALO_BEGIN, PH_HALO_END = 0, 1
 # PeriodicTurbulence::IntegratedQuantitiesEnum (periodic_turbulence.h:176-186)
 INTEGRATED_QUANTITIES = ("kinetic_energy", "enstrophy", "pressure_dilatation",
                          "viscosity_times_deviatoric_strain_rate_tensor_magnitude_sqr",
                          "viscosity_times_strain_rate_tensor_magnitude_sqr", "incompressible_kinetic_energy",
                          "incompressible_enstrophy", "incompressible_palinstrophy", "angular_momentum")
-ERRORS = {1: "invalid argument", 2: "unsupported configuration", 3: "CUDA error", 4: "out of device memory"}
+ERRORS = {1: "invalid argument", 2: "unsupported configuration", 3: "CUDA error", 4: "out of device memory",
+          5: "halo exchange failed"}
 
 EXPORTED = ["ph_ctx_create", "ph_ctx_destroy", "ph_ndofs", "ph_cell_ijk", "ph_set_state", "ph_get_state",
             "ph_residual", "ph_apply_inverse_mass", "ph_rk_step", "ph_integrals", "ph_status", "ph_sync",
@@ -28,7 +31,12 @@ EXPORTED = ["ph_ctx_create", "ph_ctx_destroy", "ph_ndofs", "ph_cell_ijk", "ph_se
             "ph_batch_progress", "ph_batch_active", "ph_batch_get_state", "ph_batch_status", "ph_batch_release",
             "ph_batch_poll", "ph_batch_fence", "ph_batch_fence_wait", "ph_batch_autotune", "ph_batch_set_variant",
             "ph_batch_launches", "ph_mesh_node_xyz", "ph_rk_error_norm", "ph_last_error",
-            "ph_integrated_quantities", "ph_run", "ph_rk_relaxation"]
+            "ph_integrated_quantities", "ph_run", "ph_rk_relaxation", "ph_ctx_create_slab", "ph_set_halo_exchange",
+            "ph_slab_connectivity"]
+
+# ph_halo_fn(user, what, phase, send_lo, send_hi, recv_lo, recv_hi, bytes, cuda_stream)
+HALO_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)
 
 
 class PhParams(ctypes.Structure):
@@ -111,6 +119,11 @@ def load(build_if_missing: bool = False):
     L.ph_rk_error_norm.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     L.ph_node_xyz.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     L.ph_residual_noalloc.argtypes = [ctypes.POINTER(PhMeshDesc), ctypes.POINTER(PhParams), vp, vp, vp]
+    L.ph_ctx_create_slab.argtypes = [ctypes.POINTER(PhMeshDesc), ctypes.POINTER(PhParams), ctypes.c_int, ctypes.c_int,
+                                     vp, ctypes.POINTER(vp)]
+    L.ph_set_halo_exchange.argtypes = [vp, HALO_FN, vp]
+    L.ph_slab_connectivity.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int32),
+                                       ctypes.POINTER(ctypes.c_int32)]
     L.ph_last_error.restype = ctypes.c_char_p
     _lib = L
     return L

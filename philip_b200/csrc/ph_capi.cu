@@ -368,10 +368,40 @@ void periodic_connectivity(int n, int order, std::vector<int>& ijk, std::vector<
         }
 }
 
+// Slab z0 .. z0 + nz - 1 of the periodic cube, owned cells lexicographic (x, y, then z from
+// z0). With nz < n the lower ghost layer (layer z0 - 1) follows the owned cells, then the
+// upper one (layer z0 + nz), each in (y, x) order; a ghost's own row names itself (no kernel
+// evaluates a ghost). With nz = n the slab wraps onto itself and has no ghosts.
+void slab_connectivity(int n, int z0, int nz, std::vector<int>& ijk, std::vector<int>& nbr) {
+    const int L = n * n, nown = nz * L;
+    const bool ghosts = nz < n;
+    const int ntot = nown + (ghosts ? 2 * L : 0);
+    ijk.assign(3 * (size_t)nown, 0);
+    nbr.assign(6 * (size_t)ntot, 0);
+    for (int cc = 0; cc < nown; ++cc) {
+        const int i = cc % n, j = (cc / n) % n, kz = cc / L;
+        ijk[3 * cc] = i; ijk[3 * cc + 1] = j; ijk[3 * cc + 2] = (z0 + kz) % n;
+        const int in = j * n + i;
+        nbr[6 * cc + 0] = kz * L + j * n + (i + n - 1) % n;
+        nbr[6 * cc + 1] = kz * L + j * n + (i + 1) % n;
+        nbr[6 * cc + 2] = kz * L + ((j + n - 1) % n) * n + i;
+        nbr[6 * cc + 3] = kz * L + ((j + 1) % n) * n + i;
+        if (ghosts) {
+            nbr[6 * cc + 4] = kz > 0 ? cc - L : nown + in;
+            nbr[6 * cc + 5] = kz < nz - 1 ? cc + L : nown + L + in;
+        } else {
+            nbr[6 * cc + 4] = ((kz + nz - 1) % nz) * L + in;
+            nbr[6 * cc + 5] = ((kz + 1) % nz) * L + in;
+        }
+    }
+    for (int g = nown; g < ntot; ++g)
+        for (int f = 0; f < 6; ++f) nbr[6 * (size_t)g + f] = g;
+}
+
 int node_geometry(int n, const std::vector<int>& ijk, const std::vector<double>& x, const std::vector<double>& D,
                   double left, double right, double warp, std::vector<double>& xyz, std::vector<double>& metric,
                   const double* support) {
-    const int N1 = (int)x.size(), NP = N1 * N1 * N1, nc = n * n * n;
+    const int N1 = (int)x.size(), NP = N1 * N1 * N1, nc = (int)(ijk.size() / 3);
     const double h = (right - left) / n;
     const bool curv = warp != 0.0 || support != nullptr;
     xyz.assign((size_t)nc * NP * 3, 0.0);
@@ -651,6 +681,19 @@ struct ph_ctx {
     double run_graph_dt = 0.0;
     int run_graph_every = 0;
     int run_graph_launches = 0;
+    // slab of a mesh shared by several GPUs: the owned layers z_first .. z_first + z_count - 1,
+    // the ghost layers (2 n^2 cells, face data only) stored after the owned cells in every
+    // stage-input state buffer and in the viscous terms
+    bool slab = false;
+    int z_first = 0, z_count = 0, layer = 0, nc_ghost = 0;
+    size_t nalloc = 0;                  // doubles per stage-input buffer, ghost slots included
+    // stage tiles [0, lo_end) and [hi_begin, nc) read ghost data (CPC-aligned, so the tiles and
+    // their partial sums are those of one launch over all cells); [lo_end, hi_begin) do not
+    int lo_end = 0, hi_begin = 0;
+    ph_halo_fn halo_fn = nullptr;
+    void* halo_user = nullptr;
+    unsigned char* d_halo = nullptr;    // send_lo | send_hi | recv_lo | recv_hi, halo_stride bytes each
+    size_t halo_stride = 0, halo_state_bytes = 0, halo_visc_bytes = 0;
 };
 
 namespace {
@@ -686,21 +729,97 @@ int dispatch_stage(ph_ctx* c, const ph::StageArgs& a) {
     return PH_OK;
 }
 
-int dispatch_aux(ph_ctx* c, const double* U) {
+int dispatch_aux(ph_ctx* c, const double* U, int cell_begin, int cell_end) {
     cudaError_t e;
     const double inv_h = 1.0 / c->h;
     timer_begin(c);
     switch (c->N1) {
-    case 2: e = ph::launch_aux<2>(U, c->d_nbr, c->h_ops, c->nc, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
-    case 3: e = ph::launch_aux<3>(U, c->d_nbr, c->h_ops, c->nc, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
-    case 4: e = ph::launch_aux<4>(U, c->d_nbr, c->h_ops, c->nc, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
-    case 5: e = ph::launch_aux<5>(U, c->d_nbr, c->h_ops, c->nc, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
-    case 6: e = ph::launch_aux<6>(U, c->d_nbr, c->h_ops, c->nc, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
-    case 7: e = ph::launch_aux<7>(U, c->d_nbr, c->h_ops, c->nc, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
+    case 2: e = ph::launch_aux<2>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
+    case 3: e = ph::launch_aux<3>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
+    case 4: e = ph::launch_aux<4>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
+    case 5: e = ph::launch_aux<5>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
+    case 6: e = ph::launch_aux<6>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
+    case 7: e = ph::launch_aux<7>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
     default: return fail(PH_ERR_UNSUPPORTED, "polynomial degree outside 1..6");
     }
     if (e != cudaSuccess) return fail(PH_ERR_CUDA, std::string("aux launch: ") + cudaGetErrorString(e));
     timer_end(c, 1);
+    return PH_OK;
+}
+
+// Halo copy of a slab context: rows of `width` 8-byte words for both partition faces at once
+// (blockIdx.y = side), from a strided source to a strided destination.
+struct HaloCopy {
+    const unsigned long long* src[2];
+    unsigned long long* dst[2];
+    long long src_pitch, dst_pitch;   // words between rows
+    int rows, width;
+};
+
+__global__ void halo_copy_kernel(const HaloCopy h) {
+    const int side = blockIdx.y;
+    const long long total = (long long)h.rows * h.width;
+    const unsigned long long* __restrict__ src = h.src[side];
+    unsigned long long* __restrict__ dst = h.dst[side];
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        const long long r = i / h.width, w = i - r * h.width;
+        dst[r * h.dst_pitch + w] = src[r * h.src_pitch + w];
+    }
+}
+
+// Packs (pack = true) the first owned layer's bottom-face data into send_lo and the last
+// layer's top-face data into send_hi, or unpacks recv_lo into the lower ghost layer (its top
+// face, read by the first layer's z- faces) and recv_hi into the upper ghost layer (its
+// bottom face). STATE: the 5 components at the face's (p+1)^2 nodes of the state buffer U;
+// VISCOUS: the face's block of the viscous terms (4 (p+1)^2 values of the arithmetic type).
+int halo_copy(ph_ctx* c, int what, bool pack, const double* U) {
+    const int N1 = c->N1, NF = N1 * N1, NP = c->NP, L = c->layer, nc = c->nc;
+    unsigned char* hb = c->d_halo;
+    unsigned long long* buf[4];
+    for (int i = 0; i < 4; ++i) buf[i] = reinterpret_cast<unsigned long long*>(hb + i * c->halo_stride);
+    HaloCopy h{};
+    const unsigned long long* vol[2];
+    unsigned long long* volw[2];
+    long long vpitch;
+    if (what == PH_HALO_STATE) {
+        auto* w = reinterpret_cast<unsigned long long*>(const_cast<double*>(U));
+        h.rows = 5 * L; h.width = NF; vpitch = NP;
+        if (pack) { vol[0] = w; vol[1] = w + (size_t)(nc - L) * 5 * NP + (size_t)(N1 - 1) * NF; }
+        else { volw[0] = w + (size_t)nc * 5 * NP + (size_t)(N1 - 1) * NF; volw[1] = w + (size_t)(nc + L) * 5 * NP; }
+    } else {
+        const size_t es = c->fp32 ? sizeof(float) : sizeof(double);
+        const size_t VT = (size_t)4 * NP + (size_t)24 * NF;
+        auto* w = reinterpret_cast<unsigned long long*>(c->d_fv);
+        const size_t vtw = VT * es / 8, blk = (size_t)4 * NF * es / 8;
+        auto off = [&](int f) { return ((size_t)4 * NP + (size_t)f * 4 * NF) * es / 8; };
+        h.rows = L; h.width = (int)blk; vpitch = (long long)vtw;
+        if (pack) { vol[0] = w + off(4); vol[1] = w + (size_t)(nc - L) * vtw + off(5); }
+        else { volw[0] = w + (size_t)nc * vtw + off(5); volw[1] = w + (size_t)(nc + L) * vtw + off(4); }
+    }
+    if (pack) {
+        h.src[0] = vol[0]; h.src[1] = vol[1]; h.dst[0] = buf[0]; h.dst[1] = buf[1];
+        h.src_pitch = vpitch; h.dst_pitch = h.width;
+    } else {
+        h.src[0] = buf[2]; h.src[1] = buf[3]; h.dst[0] = volw[0]; h.dst[1] = volw[1];
+        h.src_pitch = h.width; h.dst_pitch = vpitch;
+    }
+    const long long total = (long long)h.rows * h.width;
+    const int gx = (int)std::min<long long>((total + 255) / 256, 4 * 148);
+    timer_begin(c);
+    halo_copy_kernel<<<dim3(gx, 2), 256, 0, c->stream>>>(h);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(PH_ERR_CUDA, std::string("halo copy: ") + cudaGetErrorString(e));
+    timer_end(c, 2);
+    return PH_OK;
+}
+
+int halo_call(ph_ctx* c, int what, int phase) {
+    if (!c->halo_fn) return fail(PH_ERR_INVALID, "a slab context needs ph_set_halo_exchange before it evaluates a residual");
+    unsigned char* b = c->d_halo;
+    const size_t st = c->halo_stride;
+    const size_t bytes = what == PH_HALO_STATE ? c->halo_state_bytes : c->halo_visc_bytes;
+    const int rc = c->halo_fn(c->halo_user, what, phase, b, b + st, b + 2 * st, b + 3 * st, bytes, (void*)c->stream);
+    if (rc) return fail(PH_ERR_EXCHANGE, "halo exchange callback returned " + std::to_string(rc));
     return PH_OK;
 }
 
@@ -720,13 +839,54 @@ int dalloc(T** p, size_t count) {
     return 0;
 }
 
+int stage_range(ph_ctx* c, ph::StageArgs a, int begin, int end) {
+    if (begin >= end) return PH_OK;
+    a.cell_begin = begin; a.nc = end;
+    return dispatch_stage(c, a);
+}
+
+// One residual evaluation on the stage input `in` (auxiliary kernel, then the stage kernel with
+// the epilogue `a` asks for). In a slab context with neighbours the ghost layers of `in` and of
+// the viscous terms are refreshed through the halo callback; the cells that read no ghost data
+// run while each transfer is in flight, the first and last layer after it. Every cell runs the
+// same code on the same inputs as in one launch over all cells.
+int eval_residual(ph_ctx* c, const double* in, ph::StageArgs a) {
+    a.U = in;
+    if (!c->nc_ghost) {
+        if (c->visc) if (int rc = dispatch_aux(c, in, 0, c->nc)) return rc;
+        return stage_range(c, a, 0, c->nc);
+    }
+    const int lo = c->lo_end, hi = c->hi_begin, nc = c->nc;
+    if (int rc = halo_copy(c, PH_HALO_STATE, true, in)) return rc;
+    if (int rc = halo_call(c, PH_HALO_STATE, PH_HALO_BEGIN)) return rc;
+    if (lo < hi) {
+        if (c->visc) { if (int rc = dispatch_aux(c, in, lo, hi)) return rc; }
+        else if (int rc = stage_range(c, a, lo, hi)) return rc;
+    }
+    if (int rc = halo_call(c, PH_HALO_STATE, PH_HALO_END)) return rc;
+    if (int rc = halo_copy(c, PH_HALO_STATE, false, in)) return rc;
+    if (c->visc) {
+        if (int rc = dispatch_aux(c, in, 0, lo)) return rc;
+        if (hi < nc) if (int rc = dispatch_aux(c, in, hi, nc)) return rc;
+        if (int rc = halo_copy(c, PH_HALO_VISCOUS, true, in)) return rc;
+        if (int rc = halo_call(c, PH_HALO_VISCOUS, PH_HALO_BEGIN)) return rc;
+        if (int rc = stage_range(c, a, lo, hi)) return rc;
+        if (int rc = halo_call(c, PH_HALO_VISCOUS, PH_HALO_END)) return rc;
+        if (int rc = halo_copy(c, PH_HALO_VISCOUS, false, in)) return rc;
+    }
+    if (int rc = stage_range(c, a, 0, lo)) return rc;
+    return stage_range(c, a, hi, nc);
+}
+
 } // namespace
 
 extern "C" {
 
 const char* ph_last_error(void) { return g_err.c_str(); }
 
-int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_stream, ph_ctx** out) {
+// ph_ctx_create (nz = 0: the whole mesh in mesh->cell_order) and ph_ctx_create_slab
+static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_stream, int z0, int nz,
+                          ph_ctx** out) {
     if (!mesh || !prm || !out) return fail(PH_ERR_INVALID, "null argument");
     *out = nullptr;
     if (mesh->n_cells_per_direction < 1 || !(mesh->right > mesh->left)) return fail(PH_ERR_INVALID, "bad mesh");
@@ -749,10 +909,23 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
         if (!(prm->relaxation_runge_kutta_root_tolerance > 0.0))
             return fail(PH_ERR_INVALID, "relaxation_runge_kutta_root_tolerance must be positive");
     }
+    const bool slab = nz > 0;
+    if (slab) {
+        if (z0 < 0 || z0 >= mesh->n_cells_per_direction || nz > mesh->n_cells_per_direction)
+            return fail(PH_ERR_INVALID, "slab outside the mesh: 0 <= z_first < n and 1 <= z_count <= n");
+        if (is_curvilinear(mesh)) return fail(PH_ERR_UNSUPPORTED, "slab contexts take affine meshes");
+        if (prm->use_relaxation_runge_kutta)
+            return fail(PH_ERR_UNSUPPORTED, "slab contexts: relaxation RK needs global entropy sums per root iterate");
+    }
     ph_ctx* c = new ph_ctx();
     c->prm = *prm;
     c->n = mesh->n_cells_per_direction;
-    c->nc = c->n * c->n * c->n;
+    c->slab = slab;
+    c->layer = c->n * c->n;
+    c->z_first = slab ? z0 : 0;
+    c->z_count = slab ? nz : c->n;
+    c->nc = c->z_count * c->layer;
+    c->nc_ghost = (slab && nz < c->n) ? 2 * c->layer : 0;
     c->p = prm->poly_degree;
     c->N1 = c->p + 1;
     c->NP = c->N1 * c->N1 * c->N1;
@@ -763,6 +936,7 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
     c->split = prm->use_split_form != 0;
     c->fp32 = prm->precision == PH_FP32_RESIDUAL;
     c->ndofs = (size_t)c->nc * 5 * c->NP;
+    c->nalloc = (size_t)(c->nc + c->nc_ghost) * 5 * c->NP;
     c->warp = mesh->warp;
     c->curv = is_curvilinear(mesh);
     cudaGetDevice(&c->device);
@@ -780,7 +954,8 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
         rk_tableau(prm->runge_kutta_method, c->ns, c->A, c->b);
     }
     std::vector<int> nbr;
-    periodic_connectivity(c->n, mesh->cell_order, c->ijk, nbr);
+    if (slab) slab_connectivity(c->n, c->z_first, c->z_count, c->ijk, nbr);
+    else periodic_connectivity(c->n, mesh->cell_order, c->ijk, nbr);
     std::vector<double> metric;
     if (int rc = node_geometry(c->n, c->ijk, x, D, c->left, c->right, c->warp, c->xyz, metric,
                                mesh->mapping_support_points)) { delete c; return rc; }
@@ -791,9 +966,9 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
     bad |= dalloc(&c->d_nbr, nbr.size());
     bad |= dalloc(&c->d_ops, 1);
     bad |= dalloc(&c->d_itab, 1);
-    bad |= dalloc(&c->d_sol, N);
-    bad |= dalloc(&c->d_stA, N);
-    bad |= dalloc(&c->d_stB, N);
+    bad |= dalloc(&c->d_sol, c->nalloc);
+    bad |= dalloc(&c->d_stA, c->nalloc);
+    bad |= dalloc(&c->d_stB, c->nalloc);
     bad |= dalloc(&c->d_acc, N);
     if (c->ns == 3 || (c->lowstorage && c->ls.plus)) bad |= dalloc(&c->d_carry, N);   // SSPRK3 carry / 3S*+ S4
     if (c->lowstorage) bad |= dalloc(&c->d_err, (size_t)c->nc);
@@ -804,12 +979,19 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
         bad |= dalloc(&c->d_ent_cell, (size_t)c->nc);
     }
     if (c->visc) {   // viscous terms, stored in the arithmetic type (floats in the precision form)
-        const size_t vt = (size_t)c->nc * (4 * c->NP + 24 * c->N1 * c->N1);
+        const size_t vt = (size_t)(c->nc + c->nc_ghost) * (4 * c->NP + 24 * c->N1 * c->N1);
         bad |= dalloc(&c->d_fv, c->fp32 ? (vt + 1) / 2 : vt);
     }
     if (c->fp32) bad |= dalloc(&c->d_comp, N);
     bad |= dalloc(&c->d_partial, (size_t)ph::integral_partials<true>() * c->nc);
     bad |= dalloc(&c->d_status, 1);
+    if (c->nc_ghost) {   // per side: the face state (5 NF doubles) or viscous block (4 NF values) per layer cell
+        const int NF = c->N1 * c->N1;
+        c->halo_state_bytes = (size_t)c->layer * 5 * NF * sizeof(double);
+        c->halo_visc_bytes = c->visc ? (size_t)c->layer * 4 * NF * (c->fp32 ? sizeof(float) : sizeof(double)) : 0;
+        c->halo_stride = (std::max(c->halo_state_bytes, c->halo_visc_bytes) + 255) / 256 * 256;
+        bad |= dalloc(&c->d_halo, 4 * c->halo_stride);
+    }
     if (c->curv) bad |= dalloc(&c->d_metric, metric.size());
     if (c->curv) bad |= dalloc(&c->d_xnode, (size_t)3 * c->nc * c->NP);
     else bad |= dalloc(&c->d_origin, (size_t)3 * c->nc);
@@ -819,7 +1001,7 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
     if (e == cudaSuccess) e = cudaMemcpy(c->d_ops, &c->h_ops, sizeof(ph::OpTab), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(c->d_itab, &itab, sizeof(ph::IntegralTab), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(c->d_status, 0, sizeof(unsigned));
-    if (e == cudaSuccess) e = cudaMemset(c->d_sol, 0, N * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemset(c->d_sol, 0, c->nalloc * sizeof(double));
     if (e == cudaSuccess && c->d_comp) e = cudaMemset(c->d_comp, 0, N * sizeof(double));
     if (e == cudaSuccess && c->d_metric)
         e = cudaMemcpy(c->d_metric, metric.data(), metric.size() * sizeof(double), cudaMemcpyHostToDevice);
@@ -839,7 +1021,49 @@ int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_str
     }
     if (e != cudaSuccess) { ph_ctx_destroy(c); return fail(PH_ERR_CUDA, cudaGetErrorString(e)); }
     c->h_partial.resize((size_t)ph::integral_partials<true>() * c->nc);
+    {   // stage tiles that read ghost data: the first and last layer, rounded out to whole tiles
+        int threads = 0, cpc = 1;
+        size_t smem = 0;
+        switch (c->N1) {
+        case 2: ph::stage_launch_shape<2>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
+        case 3: ph::stage_launch_shape<3>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
+        case 4: ph::stage_launch_shape<4>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
+        case 5: ph::stage_launch_shape<5>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
+        case 6: ph::stage_launch_shape<6>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
+        default: ph::stage_launch_shape<7>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
+        }
+        c->lo_end = (c->layer + cpc - 1) / cpc * cpc;
+        c->hi_begin = (c->nc - c->layer) / cpc * cpc;
+        if (c->lo_end >= c->hi_begin) c->lo_end = c->hi_begin = c->nc;   // no cell is free of ghost data
+    }
     *out = c;
+    return PH_OK;
+}
+
+int ph_ctx_create(const ph_mesh_desc* mesh, const ph_params* prm, void* cuda_stream, ph_ctx** out) {
+    return create_context(mesh, prm, cuda_stream, 0, 0, out);
+}
+
+int ph_ctx_create_slab(const ph_mesh_desc* mesh, const ph_params* prm, int z_first, int z_count, void* cuda_stream,
+                       ph_ctx** out) {
+    if (z_count < 1) return fail(PH_ERR_INVALID, "slab outside the mesh: 0 <= z_first < n and 1 <= z_count <= n");
+    return create_context(mesh, prm, cuda_stream, z_first, z_count, out);
+}
+
+int ph_set_halo_exchange(ph_ctx* c, ph_halo_fn fn, void* user) {
+    if (!c) return fail(PH_ERR_INVALID, "null argument");
+    c->halo_fn = fn;
+    c->halo_user = user;
+    return PH_OK;
+}
+
+int ph_slab_connectivity(int n, int z_first, int z_count, int32_t* ijk, int32_t* nbr) {
+    if (n < 1 || z_first < 0 || z_first >= n || z_count < 1 || z_count > n || !ijk || !nbr)
+        return fail(PH_ERR_INVALID, "bad slab");
+    std::vector<int> h_ijk, h_nbr;
+    slab_connectivity(n, z_first, z_count, h_ijk, h_nbr);
+    std::memcpy(ijk, h_ijk.data(), h_ijk.size() * sizeof(int32_t));
+    std::memcpy(nbr, h_nbr.data(), (size_t)6 * z_count * n * n * sizeof(int32_t));
     return PH_OK;
 }
 
@@ -852,7 +1076,7 @@ int ph_ctx_destroy(ph_ctx* c) {
     }
     void* ptrs[] = {c->d_nbr, c->d_ops, c->d_itab, c->d_sol, c->d_stA, c->d_stB, c->d_acc, c->d_carry,
                     c->d_fv, c->d_comp, c->d_tmpA, c->d_tmpB, c->d_partial, c->d_status, c->d_metric, c->d_xnode, c->d_origin, c->d_err,
-                    c->d_table, c->d_counter, c->d_ent, c->d_ent_cell};
+                    c->d_table, c->d_counter, c->d_ent, c->d_ent_cell, c->d_halo};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -892,8 +1116,8 @@ int ph_get_state(ph_ctx* c, double* U, int where) {
 }
 
 static int ensure_tmp(ph_ctx* c) {
-    if (!c->d_tmpA && dalloc(&c->d_tmpA, c->ndofs)) return fail(PH_ERR_NOMEM, "device allocation failed");
-    if (!c->d_tmpB && dalloc(&c->d_tmpB, c->ndofs)) return fail(PH_ERR_NOMEM, "device allocation failed");
+    if (!c->d_tmpA && dalloc(&c->d_tmpA, c->nalloc)) return fail(PH_ERR_NOMEM, "device allocation failed");
+    if (!c->d_tmpB && dalloc(&c->d_tmpB, c->nalloc)) return fail(PH_ERR_NOMEM, "device allocation failed");
     return PH_OK;
 }
 
@@ -905,11 +1129,14 @@ int ph_residual(ph_ctx* c, const double* U, double* R, int where) {
         if (int rc = ensure_tmp(c)) return rc;
         PH_CUDA(cudaMemcpyAsync(c->d_tmpA, U, c->ndofs * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         dU = c->d_tmpA; dR = c->d_tmpB;
+    } else if (c->nc_ghost) {   // the ghost layers need room after the owned cells
+        if (int rc = ensure_tmp(c)) return rc;
+        PH_CUDA(cudaMemcpyAsync(c->d_tmpA, U, c->ndofs * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+        dU = c->d_tmpA;
     }
-    if (c->visc) if (int rc = dispatch_aux(c, dU)) return rc;
     ph::StageArgs a = base_args(c, dU);
     a.mode = 0; a.out = dR;
-    if (int rc = dispatch_stage(c, a)) return rc;
+    if (int rc = eval_residual(c, dU, a)) return rc;
     if (where == PH_HOST) {
         PH_CUDA(cudaMemcpyAsync(R, dR, c->ndofs * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         PH_CUDA(cudaStreamSynchronize(c->stream));
@@ -956,18 +1183,15 @@ static int rk_one_step(ph_ctx* c, double dt) {
         for (int i = 0; i <= last; ++i) {
             ph::StageArgs a = base_args(c, nullptr);
             const double* in = lsrk_stage_args(a, B, i, c->ls, dt, c->prm.rk_atol, c->prm.rk_rtol, c->d_err);
-            a.U = in;
-            if (c->visc) if (int rc = dispatch_aux(c, in)) return rc;
-            if (int rc = dispatch_stage(c, a)) return rc;
+            if (int rc = eval_residual(c, in, a)) return rc;
         }
         return PH_OK;
     }
     for (int i = 0; i < ns; ++i) {
         const double* in = rk_stage_input(B, i);
-        if (c->visc) if (int rc = dispatch_aux(c, in)) return rc;
         ph::StageArgs a = base_args(c, in);
         rk_stage_args(a, B, i, ns, c->A, c->b, dt, c->fp32);
-        if (int rc = dispatch_stage(c, a)) return rc;
+        if (int rc = eval_residual(c, in, a)) return rc;
     }
     if (ns == 1) std::swap(c->d_sol, c->d_stA);
     return PH_OK;
@@ -1032,12 +1256,11 @@ static int rrk_one_step(ph_ctx* c, double dt) {
     const int tiles = stage_tiles(c);
     for (int i = 0; i < ns; ++i) {
         const double* in = rk_stage_input(B, i);
-        if (c->visc) if (int rc = dispatch_aux(c, in)) return rc;
         ph::StageArgs a = base_args(c, in);
         rk_stage_args(a, B, i, ns, c->A, c->b, dt, c->fp32);
         if (i == ns - 1) a.final_out = u1;
         a.ent_partial = c->d_ent + (size_t)i * c->ent_tiles;
-        if (int rc = dispatch_stage(c, a)) return rc;
+        if (int rc = eval_residual(c, in, a)) return rc;
     }
     std::vector<double> part((size_t)ns * c->ent_tiles);
     PH_CUDA(cudaMemcpyAsync(part.data(), c->d_ent, part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -1136,7 +1359,7 @@ int ph_rk_step(ph_ctx* c, double dt, int nsteps) {
     c->rrk_elapsed = dt * nsteps;
     // several steps of one dt on a caller-given stream replay a graph of one step; the
     // per-launch timing mode and one-stage methods (which swap buffers) launch directly
-    const bool graph = c->stream != nullptr && !c->timing && c->ns > 1 && nsteps > 1;
+    const bool graph = c->stream != nullptr && !c->timing && c->ns > 1 && nsteps > 1 && !c->nc_ghost;
     if (graph) {
         int s = 0;
         if (!c->step_graph || c->step_graph_dt != dt) {
@@ -1263,6 +1486,7 @@ int ph_rk_relaxation(ph_ctx* c, double* gamma, double* elapsed) {
 int ph_run(ph_ctx* c, double dt, int nsteps, int record_every, double* rows) {
     if (!c || nsteps < 0 || record_every < 0) return fail(PH_ERR_INVALID, "bad argument");
     if (c->rrk) return fail(PH_ERR_UNSUPPORTED, "ph_run: relaxation RK steps have variable length; use ph_rk_step");
+    if (c->nc_ghost) return fail(PH_ERR_UNSUPPORTED, "ph_run: slab contexts exchange halos on the host; use ph_rk_step");
     const int nrec = record_every > 0 ? nsteps / record_every : 0;
     if (nrec > 0 && !rows) return fail(PH_ERR_INVALID, "null rows");
     if (nrec > c->table_rows) {   // grow the device table (synchronises the stream)
@@ -1620,12 +1844,12 @@ extern "C" int ph_residual_noalloc(const ph_mesh_desc* mesh, const ph_params* pr
     cudaError_t e = cudaSuccess;
     if (visc) {
         switch (N1) {
-        case 2: e = ph::launch_aux<2>(U, sym.nbr, tab, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
-        case 3: e = ph::launch_aux<3>(U, sym.nbr, tab, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
-        case 4: e = ph::launch_aux<4>(U, sym.nbr, tab, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
-        case 5: e = ph::launch_aux<5>(U, sym.nbr, tab, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
-        case 6: e = ph::launch_aux<6>(U, sym.nbr, tab, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
-        default: e = ph::launch_aux<7>(U, sym.nbr, tab, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
+        case 2: e = ph::launch_aux<2>(U, sym.nbr, tab, 0, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
+        case 3: e = ph::launch_aux<3>(U, sym.nbr, tab, 0, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
+        case 4: e = ph::launch_aux<4>(U, sym.nbr, tab, 0, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
+        case 5: e = ph::launch_aux<5>(U, sym.nbr, tab, 0, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
+        case 6: e = ph::launch_aux<6>(U, sym.nbr, tab, 0, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
+        default: e = ph::launch_aux<7>(U, sym.nbr, tab, 0, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
         }
         if (e != cudaSuccess) return fail(PH_ERR_CUDA, std::string("aux launch: ") + cudaGetErrorString(e));
     }

@@ -23,7 +23,8 @@ static cudaError_t launch_one(const StageArgs& a, cudaStream_t s) {
         if (e != cudaSuccess) return e;
         configured[dev] = true;
     }
-    const int grid = (a.nc + CPC - 1) / CPC;
+    const int grid = (a.nc - a.cell_begin + CPC - 1) / CPC;
+    if (grid <= 0) return cudaErrorInvalidValue;
     kern<<<grid, L::NT, L::bytes, s>>>(a);
     return cudaGetLastError();
 }
@@ -157,8 +158,8 @@ void stage_launch_shape(int fp32, bool visc, bool split, int* threads, int* cpc,
 }
 
 template <typename R, int N1>
-static cudaError_t launch_aux_prec(const double* U, const int* nbr, const OpTab& ops, int nc, double inv_h,
-                                   const PhysConst& pc, void* Fv, cudaStream_t s) {
+static cudaError_t launch_aux_prec(const double* U, const int* nbr, const OpTab& ops, int cell_begin, int nc,
+                                   double inv_h, const PhysConst& pc, void* Fv, cudaStream_t s) {
     constexpr int CPC = cells_per_cta<N1>();
     using L = AuxLayout<N1, CPC>;
     constexpr size_t bytes = L::template bytes<R>();
@@ -174,15 +175,17 @@ static cudaError_t launch_aux_prec(const double* U, const int* nbr, const OpTab&
     AuxCoef<R> co{};
     for (int i = 0; i < MAXN1 * MAXN1; ++i) co.D[i] = (R)ops.D[i];
     co.inv_wend = R(1) / (R)ops.w[0];
-    kern<<<(nc + CPC - 1) / CPC, L::NT, bytes, s>>>(U, nbr, nc, (R)inv_h, pc, co, static_cast<R*>(Fv));
+    const int grid = (nc - cell_begin + CPC - 1) / CPC;
+    if (grid <= 0) return cudaErrorInvalidValue;
+    kern<<<grid, L::NT, bytes, s>>>(U, nbr, cell_begin, nc, (R)inv_h, pc, co, static_cast<R*>(Fv));
     return cudaGetLastError();
 }
 
 template <int N1>
-cudaError_t launch_aux(const double* U, const int* nbr, const OpTab& ops, int nc, double inv_h,
+cudaError_t launch_aux(const double* U, const int* nbr, const OpTab& ops, int cell_begin, int nc, double inv_h,
                        const PhysConst& pc, int fp32, void* Fv, cudaStream_t s) {
-    return fp32 ? launch_aux_prec<float, N1>(U, nbr, ops, nc, inv_h, pc, Fv, s)
-                : launch_aux_prec<double, N1>(U, nbr, ops, nc, inv_h, pc, Fv, s);
+    return fp32 ? launch_aux_prec<float, N1>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, s)
+                : launch_aux_prec<double, N1>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, s);
 }
 
 template <int N1>
@@ -250,7 +253,7 @@ template void stage_launch_shape<PH_N1>(int, bool, bool, int*, int*, size_t*);
 template cudaError_t launch_stage_batched<PH_N1>(const StageArgs*, const BatchTile*, int, int, bool, bool, int, int,
                                                  cudaStream_t);
 template bool batched_shape<PH_N1>(int, bool, int, int*, int*, size_t*, int*);
-template cudaError_t launch_aux<PH_N1>(const double*, const int*, const OpTab&, int, double, const PhysConst&, int,
+template cudaError_t launch_aux<PH_N1>(const double*, const int*, const OpTab&, int, int, double, const PhysConst&, int,
                                        void*, cudaStream_t);
 template cudaError_t launch_inverse_mass<PH_N1>(const double*, double*, const OpTab*, int, double, const double*,
                                                 cudaStream_t);

@@ -59,7 +59,8 @@ struct StageArgs {
                               // cell, stored in the arithmetic type R (FP32 in the precision form)
     const int* nbr;           // [nc][6] neighbour cell per face
     const OpTab* ops;
-    int nc;
+    int nc;                   // one past the last cell of this launch
+    int cell_begin;           // first cell of this launch (a multiple of the cells per tile)
     double h, inv_h;
     double pen;               // SIPG penalty p(p+1)/h * factor
     PhysConst pc;
@@ -826,7 +827,7 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
 template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int FS, bool CURV = false>
 __global__ void __launch_bounds__(Layout<R, N1, CPC, VISC, SPLIT, CURV>::NT, Layout<R, N1, CPC, VISC, SPLIT, CURV>::MINB)
 residual_kernel(const StageArgs a) {
-    residual_tile<R, N1, CPC, VISC, SPLIT, FS, CURV>(a, blockIdx.x * CPC);
+    residual_tile<R, N1, CPC, VISC, SPLIT, FS, CURV>(a, a.cell_begin + blockIdx.x * CPC);
 }
 
 // One tile of a batch: instance index and its first cell.
@@ -903,7 +904,7 @@ template <int N1> __device__ __forceinline__ int line_node(int d, int line, int 
 
 template <typename R, int N1, int CPC>
 __global__ void __launch_bounds__(AuxLayout<N1, CPC>::NT)
-aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, int nc, R inv_h, PhysConst pc,
+aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, int cell_begin, int nc, R inv_h, PhysConst pc,
            AuxCoef<R> co, R* __restrict__ Fv) {
     using L = AuxLayout<N1, CPC>;
     constexpr int NP = L::NP, NF = L::NF, NT = L::NT;
@@ -913,7 +914,7 @@ aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, int nc, R 
     R* sT = sU + CPC * 5 * NP;                // [c][face][5][NF] neighbour traces
     Cst<R> cst; cst.load(pc);
     const int tid = threadIdx.x;
-    const int cell0 = blockIdx.x * CPC;
+    const int cell0 = cell_begin + blockIdx.x * CPC;
     // loads unrolled so that all of a thread's loads are in flight before the first store
 #pragma unroll
     for (int it = tid; it < CPC * 5 * NP; it += NT) {

@@ -7,13 +7,13 @@
 
 namespace ph {
 
-// residual / mass-inverse / RK stage for one stage input
+// residual / mass-inverse / RK stage for one stage input, cells [a.cell_begin, a.nc)
 template <int N1>
 cudaError_t launch_stage(const StageArgs& a, int fp32, bool visc, bool split, cudaStream_t s);
 // auxiliary (lifted gradient) equation, emitting the viscous terms of the stage kernel
-// (viscous_terms_per_cell); ops: the host copy of the operator table
+// (viscous_terms_per_cell) of cells [cell_begin, nc); ops: the host copy of the operator table
 template <int N1>
-cudaError_t launch_aux(const double* U, const int* nbr, const OpTab& ops, int nc, double inv_h,
+cudaError_t launch_aux(const double* U, const int* nbr, const OpTab& ops, int cell_begin, int nc, double inv_h,
                        const PhysConst& pc, int fp32, void* Fv, cudaStream_t s);
 // DGBase::apply_inverse_global_mass_matrix on its own
 template <int N1>

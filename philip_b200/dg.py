@@ -53,10 +53,13 @@ class DGStrong:
     """Strong-form DG/FR discretisation on a periodic cube, evaluated on the B200."""
 
     def __init__(self, parameters: Parameters, precision: int = _lib.PH_FP64, cell_order: int = 0,
-                 stream: int | None = None, warp: float = 0.0, mapping_support_points: np.ndarray | None = None):
+                 stream: int | None = None, warp: float = 0.0, mapping_support_points: np.ndarray | None = None,
+                 slab: tuple[int, int] | None = None, halo=None):
         """warp != 0 gives the sine-warped (curvilinear) cube: every coordinate moves by
         warp (L/2pi) sin(2pi(x-l)/L) sin(2pi(y-l)/L) sin(2pi(z-l)/L), mapping degree = p.
-        mapping_support_points ([cell][3][(p+1)^3], GLL points) gives any other curved mapping."""
+        mapping_support_points ([cell][3][(p+1)^3], GLL points) gives any other curved mapping.
+        slab = (z_first, z_count): this process's layers of a mesh shared by several GPUs
+        (philip_b200.slab); halo: the object whose `callback` exchanges the partition faces."""
         self.L = _lib.load()
         self.parameters = parameters
         self.params = parameters.to_ph_params(precision)
@@ -67,12 +70,20 @@ class DGStrong:
             self._support = np.ascontiguousarray(mapping_support_points, dtype=np.float64)
             self.mesh.mapping_support_points = self._support.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
         h = ctypes.c_void_p()
-        _lib.check(self.L.ph_ctx_create(ctypes.byref(self.mesh), ctypes.byref(self.params),
-                                        ctypes.c_void_p(stream) if stream else None, ctypes.byref(h)))
+        st = ctypes.c_void_p(stream) if stream else None
+        if slab is None:
+            _lib.check(self.L.ph_ctx_create(ctypes.byref(self.mesh), ctypes.byref(self.params), st, ctypes.byref(h)))
+        else:
+            _lib.check(self.L.ph_ctx_create_slab(ctypes.byref(self.mesh), ctypes.byref(self.params), int(slab[0]),
+                                                 int(slab[1]), st, ctypes.byref(h)))
         self._h = h
+        self.slab = slab
+        self.halo = halo
+        if halo is not None:
+            _lib.check(self.L.ph_set_halo_exchange(h, halo.callback, None))
         self.n_dofs = int(self.L.ph_ndofs(h))
         self.poly_degree = parameters.poly_degree
-        self.n_cells = parameters.n_cells ** 3
+        self.n_cells = parameters.n_cells ** 2 * (slab[1] if slab is not None else parameters.n_cells)
         self.n_shape = (self.poly_degree + 1) ** 3
         self.right_hand_side = np.zeros(self.n_dofs)
         self.current_time = 0.0

@@ -1,0 +1,359 @@
+"""One mesh over several ranks: slabs of cell layers with a halo exchange of the partition
+faces (the reference's ghost-value refresh before each residual, DGBase::assemble_residual,
+src/dg/dg_base.cpp:2742, and of the auxiliary solution, src/dg/strong_dg.cpp:648).
+
+CPU (gloo, 2 and 3 ranks): the slab plan names, for every owned cell's face, either the owned
+neighbour or a ghost slot, and the exchange through philip_b200.slab.DistributedHalo fills each
+ghost slot with the data of the cell that the periodic cube puts there.
+GPU (one device): the slabs of a mesh run as contexts in threads of one process, exchanging
+through device copies between host barriers (no kernel waits on another context); their
+residuals and RK steps are bitwise those of one context over the whole mesh.
+"""
+import ctypes
+import os
+import socket
+import threading
+
+import numpy as np
+import pytest
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+from philip_b200 import _lib
+from philip_b200.slab import DistributedHalo, global_integrals, slab_bounds
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _plan(n, z0, nz):
+    L = _lib.load()
+    nown = nz * n * n
+    ijk = np.zeros((nown, 3), np.int32)
+    nbr = np.zeros((nown, 6), np.int32)
+    _lib.check(L.ph_slab_connectivity(n, z0, nz, ijk.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                      nbr.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))))
+    return ijk, nbr
+
+
+def _gid(n, i, j, k):
+    return (k * n + j) * n + i
+
+
+def test_slab_bounds_cover_the_layers():
+    for n in (1, 4, 7, 24):
+        for world in range(1, n + 1):
+            spans = [slab_bounds(n, world, r) for r in range(world)]
+            layers = [z for z0, nz in spans for z in range(z0, z0 + nz)]
+            assert layers == list(range(n))
+            assert max(s[1] for s in spans) - min(s[1] for s in spans) <= 1
+    with pytest.raises(ValueError):
+        slab_bounds(3, 4, 0)
+
+
+@pytest.mark.parametrize("n,z0,nz", [(4, 0, 2), (4, 3, 1), (3, 1, 2), (5, 2, 5), (2, 0, 1)])
+def test_slab_plan_names_the_periodic_neighbours(n, z0, nz):
+    ijk, nbr = _plan(n, z0, nz)
+    nown = nz * n * n
+    assert sorted(ijk[:, 2].tolist()) == sorted([(z0 + k) % n for k in range(nz) for _ in range(n * n)])
+    for c in range(nown):
+        for f in range(6):
+            t = list(ijk[c]); d = f // 2
+            t[d] = (t[d] + (1 if f & 1 else -1)) % n
+            g = int(nbr[c, f])
+            if g < nown:
+                assert list(ijk[g]) == t
+            else:                               # ghost slot: only z faces of the first / last layer
+                assert nz < n and d == 2
+                side, ii = divmod(g - nown, n * n)
+                layer = (z0 - 1) % n if side == 0 else (z0 + nz) % n
+                assert (ii % n, ii // n, layer) == tuple(t)
+
+
+def _exchange_worker(rank, world, port, n, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        z0, nz = slab_bounds(n, world, rank)
+        ijk, nbr = _plan(n, z0, nz)
+        nown, L2, m = nz * n * n, n * n, 3
+        halo = DistributedHalo(device="cpu")
+        ok = True
+        for what in (_lib.PH_HALO_STATE, _lib.PH_HALO_VISCOUS):
+            # the packed layout: one record of m values per cell of the layer, (y, x) order
+            bufs = [np.zeros((L2, m)) for _ in range(4)]
+            for ii in range(L2):
+                i, j = ii % n, ii // n
+                bufs[0][ii] = _gid(n, i, j, z0) + 0.25 * what
+                bufs[1][ii] = _gid(n, i, j, (z0 + nz - 1) % n) + 0.25 * what
+            ptr = [b.ctypes.data for b in bufs]
+            halo.begin(what, *ptr, bufs[0].nbytes)
+            halo.end()
+            recv_lo, recv_hi = bufs[2], bufs[3]
+            for c in range(nown):
+                for f in (4, 5):
+                    g = int(nbr[c, f])
+                    if g < nown:
+                        continue
+                    side, ii = divmod(g - nown, L2)
+                    t = list(ijk[c]); t[2] = (t[2] + (1 if f & 1 else -1)) % n
+                    want = _gid(n, *t) + 0.25 * what
+                    ok &= bool(np.all((recv_lo if side == 0 else recv_hi)[ii] == want))
+        # the volume averages of the slabs add up, the wave speed is the largest
+        tot = global_integrals([1.0 + rank, 2.0, 0.5, 3.0 + rank], dist)
+        out[rank] = (ok, tot)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,n", [(2, 4), (3, 4), (2, 2)])
+def test_halo_exchange_fills_the_ghost_layers(world, n):
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        mp.spawn(_exchange_worker, args=(world, _free_port(), n, out), nprocs=world, join=True)
+        res = dict(out)
+    for r in range(world):
+        ok, tot = res[r]
+        assert ok
+        assert tot == [sum(1.0 + q for q in range(world)), 2.0 * world, 0.5 * world, 3.0 + world - 1]
+
+
+def test_slab_refusals_without_a_gpu():
+    from helpers import prm_dict
+    from philip_b200.prm import Parameters
+    L = _lib.load()
+    prm = Parameters.from_dict(prm_dict(poly_degree=2, n_cells=4))
+    p = prm.to_ph_params()
+    h = ctypes.c_void_p()
+
+    def create(z0, nz, warp=0.0, edit=None):
+        q = prm.to_ph_params()
+        if edit:
+            edit(q)
+        m = _lib.PhMeshDesc(4, 0, 0.0, 6.283185307179586, warp, 2)
+        return L.ph_ctx_create_slab(ctypes.byref(m), ctypes.byref(q), z0, nz, None, ctypes.byref(h))
+
+    assert create(4, 1) == _lib.PH_ERR_INVALID
+    assert create(0, 0) == _lib.PH_ERR_INVALID
+    assert create(1, 5) == _lib.PH_ERR_INVALID
+    assert create(0, 2, warp=0.1) == _lib.PH_ERR_UNSUPPORTED and b"affine" in L.ph_last_error()
+    assert create(0, 2, edit=lambda q: setattr(q, "use_relaxation_runge_kutta", 1)) == _lib.PH_ERR_UNSUPPORTED
+    del p
+
+
+# ------------------------------------------------------------------------------- GPU
+
+class ThreadHalo:
+    """The exchange of `world` slab contexts of one process, each stepped by its own thread:
+    every rank synchronises its stream, publishes its send buffers, and after a barrier copies
+    its neighbours' into its receive buffers on its stream; a second barrier keeps the send
+    buffers until every rank has copied. Host barriers only: no kernel waits on another."""
+
+    def __init__(self, world, state):
+        self.world = world
+        self.state = state              # shared: barrier and published pointers
+
+    def for_rank(self, rank):
+        h = ThreadHalo(self.world, self.state)
+        h.rank = rank
+        h.callback = _lib.HALO_FN(h._call)
+        return h
+
+    @staticmethod
+    def shared(world):
+        return {"barrier": threading.Barrier(world, timeout=120), "send": {}}
+
+    def _call(self, user, what, phase, send_lo, send_hi, recv_lo, recv_hi, nbytes, stream):
+        import torch
+        from philip_b200.slab import _as_tensor
+        try:
+            if phase == _lib.PH_HALO_END:
+                return 0
+            s = torch.cuda.ExternalStream(stream) if stream else torch.cuda.default_stream()
+            s.synchronize()
+            st = self.state
+            st["send"][self.rank] = (send_lo, send_hi)
+            st["barrier"].wait()
+            lo, hi = (self.rank - 1) % self.world, (self.rank + 1) % self.world
+            with torch.cuda.stream(s):
+                _as_tensor(recv_lo, nbytes, "cuda").copy_(_as_tensor(st["send"][lo][1], nbytes, "cuda"))
+                _as_tensor(recv_hi, nbytes, "cuda").copy_(_as_tensor(st["send"][hi][0], nbytes, "cuda"))
+            s.synchronize()
+            st["barrier"].wait()
+            return 0
+        except Exception:
+            import traceback
+            traceback.print_exc()
+            try:
+                self.state["barrier"].abort()
+            except Exception:
+                pass
+            return 1
+
+
+def _slabs(prm, world, precision=_lib.PH_FP64):
+    import torch
+    from philip_b200.dg import DGStrong
+    shared = ThreadHalo.shared(world)
+    base = ThreadHalo(world, shared)
+    out = []
+    for r in range(world):
+        s = torch.cuda.Stream()
+        halo = base.for_rank(r)
+        dg = DGStrong(prm, precision=precision, stream=s.cuda_stream,
+                      slab=slab_bounds(prm.n_cells, world, r), halo=halo)
+        out.append((dg, s))
+    return out
+
+
+def _in_threads(fns):
+    errs = [None] * len(fns)
+    res = [None] * len(fns)
+
+    def run(k):
+        try:
+            res[k] = fns[k]()
+        except Exception as e:          # noqa: BLE001
+            errs[k] = e
+
+    th = [threading.Thread(target=run, args=(k,)) for k in range(len(fns))]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    for e in errs:
+        if e is not None:
+            raise e
+    return res
+
+
+def _slice_map(whole, part):
+    """Cell indices of `part`'s owned cells in `whole`'s order."""
+    pos = {tuple(r): i for i, r in enumerate(whole.cell_ijk())}
+    return np.array([pos[tuple(r)] for r in part.cell_ijk()])
+
+
+def _gather(whole, parts, vecs):
+    nd = 5 * whole.n_shape
+    U = np.empty(whole.n_dofs)
+    for dg, v in zip(parts, vecs):
+        idx = _slice_map(whole, dg)
+        U.reshape(-1, nd)[idx] = v.reshape(-1, nd)
+    return U
+
+
+def _scatter(whole, parts, U):
+    nd = 5 * whole.n_shape
+    return [U.reshape(-1, nd)[_slice_map(whole, dg)].reshape(-1).copy() for dg in parts]
+
+
+SLAB_CASES = [
+    ("ns_br2_p3_two_slabs", dict(poly_degree=3, n_cells=4, pde="navier_stokes", diss="bassi_rebay_2"), 2),
+    ("ns_sipg_p2_three_slabs", dict(poly_degree=2, n_cells=4, pde="navier_stokes"), 3),
+    ("euler_ch_p5_two_slabs", dict(poly_degree=5, n_cells=3), 2),
+    ("ns_p4_one_layer_each", dict(poly_degree=4, n_cells=3, pde="navier_stokes", diss="bassi_rebay_2"), 3),
+    ("euler_p1_interior_overlap", dict(poly_degree=1, n_cells=8), 2),
+    ("ns_br2_p2_interior_overlap", dict(poly_degree=2, n_cells=6, pde="navier_stokes", diss="bassi_rebay_2"), 2),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,kw,world", SLAB_CASES, ids=[c[0] for c in SLAB_CASES])
+def test_slab_residual_is_the_whole_mesh_residual(name, kw, world):
+    from oracle.oracle import Oracle
+    from philip_b200.dg import DGStrong
+    from philip_b200.prm import Parameters
+    from helpers import perturbed_tgv, prm_dict
+    prm = Parameters.from_dict(prm_dict(**kw))
+    whole = DGStrong(prm)
+    orc = Oracle(prm.oracle_cfg(), prm.n_cells, *prm.grid_bounds)
+    U = perturbed_tgv(orc, seed=len(name))
+    R_whole = whole.residual_of(U)
+    parts = _slabs(prm, world)
+    Us = _scatter(whole, [p for p, _ in parts], U)
+    Rs = _in_threads([lambda k=k: parts[k][0].residual_of(Us[k]) for k in range(world)])
+    R = _gather(whole, [p for p, _ in parts], Rs)
+    print(f"{name}: max |R_slabs - R_whole| = {np.max(np.abs(R - R_whole)):.3e}")
+    assert np.array_equal(R, R_whole)
+
+
+STEP_CASES = [
+    ("ns_br2_rk4_p3", dict(poly_degree=3, n_cells=6, pde="navier_stokes", diss="bassi_rebay_2"), 2, _lib.PH_FP64),
+    ("euler_ssprk3_p2", dict(poly_degree=2, n_cells=4, rk="ssprk3_ex"), 3, _lib.PH_FP64),
+    ("euler_forward_euler_p2", dict(poly_degree=2, n_cells=3, rk="euler_ex"), 2, _lib.PH_FP64),
+    ("ns_lsrk_p3", dict(poly_degree=3, n_cells=4, pde="navier_stokes", rk="RK3_2_5F_3SStarPlus"), 2, _lib.PH_FP64),
+    ("ns_br2_precision_form_p5", dict(poly_degree=5, n_cells=6, pde="navier_stokes", diss="bassi_rebay_2"), 2,
+     _lib.PH_FP32_RESIDUAL),
+    ("euler_precision_form_p3_one_layer_each", dict(poly_degree=3, n_cells=3), 3, _lib.PH_FP32_RESIDUAL),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,kw,world,precision", STEP_CASES, ids=[c[0] for c in STEP_CASES])
+def test_slab_steps_are_the_whole_mesh_steps(name, kw, world, precision):
+    from oracle.oracle import Oracle
+    from philip_b200.dg import DGStrong, RungeKuttaODESolver
+    from philip_b200.prm import Parameters
+    from helpers import TWO_PI, prm_dict
+    prm = Parameters.from_dict(prm_dict(**kw))
+    whole = DGStrong(prm, precision=precision)
+    U0 = Oracle(prm.oracle_cfg(), prm.n_cells, *prm.grid_bounds).initial_condition("tgv")
+    whole.solution = U0
+    dt = 0.1 * TWO_PI / prm.n_cells / (prm.poly_degree + 1) / 11.0
+    ode = RungeKuttaODESolver(whole)
+    ode.step_in_time(dt, nsteps=3)
+    parts = _slabs(prm, world, precision)
+    dgs = [p for p, _ in parts]
+    for dg, u in zip(dgs, _scatter(whole, dgs, U0)):
+        dg.solution = u
+
+    def steps(k):
+        o = RungeKuttaODESolver(dgs[k])
+        o.step_in_time(dt, nsteps=3)
+        parts[k][1].synchronize()
+        return dgs[k].solution, dgs[k].integrals(), (o.error_norm() if "lsrk" in name else 0.0)
+
+    res = _in_threads([lambda k=k: steps(k) for k in range(world)])
+    U = _gather(whole, dgs, [r[0] for r in res])
+    print(f"{name}: max |U_slabs - U_whole| = {np.max(np.abs(U - whole.solution)):.3e}")
+    assert np.array_equal(U, whole.solution)
+    assert all(dg.status() == 0 for dg in dgs)
+    # the slabs' shares of the volume averages add up to the whole mesh's
+    q = np.array([r[1] for r in res])
+    qw = whole.integrals()
+    assert np.allclose(q[:, :3].sum(axis=0), qw[:3], rtol=1e-13, atol=0.0)
+    assert q[:, 3].max() == qw[3]
+    if "lsrk" in name:   # the error norm: the RMS over the slabs' DOFs
+        w = np.sqrt(sum(r[2] ** 2 * dg.n_dofs for r, dg in zip(res, dgs)) / whole.n_dofs)
+        assert abs(w - ode.error_norm()) <= 1e-13 * ode.error_norm()
+
+
+@pytest.mark.gpu
+def test_slab_exchange_failures_are_reported():
+    from philip_b200.dg import DGStrong
+    from philip_b200.prm import Parameters
+    from helpers import prm_dict
+    prm = Parameters.from_dict(prm_dict(poly_degree=2, n_cells=4))
+    lonely = DGStrong(prm, slab=(0, 2))
+    U = np.zeros(lonely.n_dofs) + 1.0
+    with pytest.raises(_lib.PhError, match="ph_set_halo_exchange"):
+        lonely.residual_of(U)
+
+    class Failing:
+        def __init__(self):
+            self.callback = _lib.HALO_FN(lambda *a: 7)
+
+    dg = DGStrong(prm, slab=(0, 2), halo=Failing())
+    with pytest.raises(_lib.PhError, match="returned 7"):
+        dg.residual_of(U)
+    # the whole mesh as one slab needs no exchange
+    one = DGStrong(prm, slab=(0, 4))
+    whole = DGStrong(prm)
+    from oracle.oracle import Oracle
+    U0 = Oracle(prm.oracle_cfg(), prm.n_cells, *prm.grid_bounds).initial_condition("tgv")
+    one.solution = _scatter(whole, [one], U0)[0]
+    assert np.array_equal(_gather(whole, [one], [one.residual_of(one.solution)]), whole.residual_of(U0))
