@@ -9,11 +9,13 @@ at the nodes.
 
 A "step" is one RK4 time step (4 stages). The metric is DOF-updates per second per
 stage = N_DOF x stages / time, aggregated over all GPUs (each GPU integrates its own
-copy of the cube: replicas, weak scaling).
+copy of the cube: replicas, weak scaling). With --shard slab the GPUs share one cube
+instead, each owning a slab of cell layers and exchanging the partition faces with its
+neighbours every stage (strong scaling).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--workload tgv_viscous_24_p5|tgv_inviscid_8_p3|tgv_viscous_32_p3]
-                  [--precision fp64|fp32]
+                  [--precision fp64|fp32] [--shard replicas|slab]
 """
 from __future__ import annotations
 
@@ -502,6 +504,8 @@ def main():
                     help="batched / served forms: solves in the one-at-a-time FP64 comparison (0 = all)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shard", default="replicas", choices=["replicas", "slab"],
+                    help="N > 1: a copy of the cube per GPU, or one cube in slabs of cell layers")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -546,8 +550,17 @@ def main():
     # the context runs on its own stream (multi-step calls then replay a captured RK step);
     # every CUDA event below is recorded on that stream
     stream = torch.cuda.Stream()
-    fs = FlowSolver(prm, precision=prec, stream=stream.cuda_stream)
+    slab = args.shard == "slab"
+    if slab:   # this rank's layers of the one cube, the partition faces over NCCL
+        from philip_b200.slab import DistributedHalo, slab_bounds
+        fs = FlowSolver(prm, precision=prec, stream=stream.cuda_stream,
+                        slab=slab_bounds(prm.n_cells, world, rank),
+                        halo=DistributedHalo() if world > 1 else None, dist=dist)
+    else:
+        fs = FlowSolver(prm, precision=prec, stream=stream.cuda_stream)
     dg = fs.dg
+    # DOFs that one timed step updates over the whole job
+    job_dofs = prm.n_cells ** 3 * 5 * dg.n_shape if slab else world * dg.n_dofs
     L, h = dg.L, dg.handle
     dt = fs.adaptive_time_step()
     p, n, pde, _, desc = WORKLOADS[args.workload]
@@ -578,29 +591,33 @@ def main():
     launches = int(tm[6])
     ms = reduce_max(ms, dist, "cuda")
     ms_per_step = ms / args.steps
-    value = world * dg.n_dofs * stages * args.steps / (ms * 1e-3)
+    value = job_dofs * stages * args.steps / (ms * 1e-3)
 
     # ---- the same steps through the device time loop with the kinetic energy / enstrophy
     # rows every 10 steps (ph_run: the integrals reduced on the device, one copy at the end)
     record_every = 10
     rows = np.zeros((max(args.steps // record_every, 2), 4))
-    # warm-up: captures the graph of one record interval
-    _lib.check(L.ph_run(h, dt, 2 * record_every, record_every, rows.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
-    barrier(); torch.cuda.synchronize()
-    r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    r0.record(stream)
-    _lib.check(L.ph_run(h, dt, args.steps, record_every, rows.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
-    r1.record(stream); torch.cuda.synchronize()
-    ms_rec = reduce_max(r0.elapsed_time(r1), dist, "cuda")
-    value_rec = world * dg.n_dofs * stages * args.steps / (ms_rec * 1e-3)
+    exchange = slab and world > 1   # the slabs step through ph_rk_step (ph_run is one GPU's loop)
+    if not exchange:
+        # warm-up: captures the graph of one record interval
+        _lib.check(L.ph_run(h, dt, 2 * record_every, record_every,
+                            rows.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        barrier(); torch.cuda.synchronize()
+        r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        r0.record(stream)
+        _lib.check(L.ph_run(h, dt, args.steps, record_every, rows.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        r1.record(stream); torch.cuda.synchronize()
+        ms_rec = reduce_max(r0.elapsed_time(r1), dist, "cuda")
+        value_rec = job_dofs * stages * args.steps / (ms_rec * 1e-3)
 
     # ---- per-kernel launch durations (CUDA events on the launching stream)
     _lib.check(L.ph_set_timing(h, 1))
     _lib.check(L.ph_rk_step(h, dt, 2))
     _lib.check(L.ph_get_timing(h, tm.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
     _lib.check(L.ph_set_timing(h, 0))
-    stage_ms = tm[0] / max(tm[1], 1)
-    aux_ms = tm[2] / max(tm[3], 1)
+    # per stage (a slab with neighbours splits each stage into interior and boundary launches)
+    stage_ms = tm[0] / (2 * stages)
+    aux_ms = tm[2] / (2 * stages)
 
     # ---- end to end through the C-ABI with host buffers (pinned), every step:
     # H2D of the state, one RK4 step, D2H of the state
@@ -616,7 +633,7 @@ def main():
     e1.record(stream); torch.cuda.synchronize()
     ms_e2e = e0.elapsed_time(e1)
     ms_e2e = reduce_max(ms_e2e, dist, "cuda")
-    e2e = world * dg.n_dofs * stages * args.steps / (ms_e2e * 1e-3)
+    e2e = job_dofs * stages * args.steps / (ms_e2e * 1e-3)
     status = dg.status()
 
     if rank == 0:
@@ -633,14 +650,15 @@ def main():
         line = {
             "metric": "TGV DOF-updates/s/stage", "value": value, "unit": "DOF-updates/s/stage",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True, "scaling": "strong" if slab else "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f32-residual/f64-state",
             "data": "synthetic (Taylor-Green initial condition interpolated at the GLL nodes)",
-            "config": {"workload": args.workload, "description": desc, "ndofs": dg.n_dofs,
+            "config": {"workload": args.workload, "description": desc, "ndofs": n ** 3 * 5 * dg.n_shape,
                        "cells": n ** 3, "poly_degree": p, "stages_per_step": stages, "dt": dt,
                        "l2": "inputs larger than L2 (state 120 MB/vector, working set > 600 MB)"
                        if args.workload != "tgv_inviscid_8_p3" else "L2-resident (6.6 MB/vector)",
-                       "parallelism": f"replicas x{world}", "status_flags": status},
+                       "parallelism": f"slabs x{world}" if slab else f"replicas x{world}",
+                       "status_flags": status},
             "e2e": {"value": e2e, "unit": "DOF-updates/s/stage",
                     "h2d_bytes_per_step": 8 * dg.n_dofs, "d2h_bytes_per_step": 8 * dg.n_dofs,
                     "path": "ph_set_state(host pinned) + ph_rk_step + ph_get_state(host pinned) per step"},
@@ -648,7 +666,8 @@ def main():
             "with_integrals": {"record_every": record_every, "value": value_rec, "ms_per_step": ms_rec / args.steps,
                                "rows": int(args.steps // record_every),
                                "path": "ph_run: the same steps with kinetic energy, enstrophy, dissipation rate "
-                                       "and wave speed reduced on the device every 10 steps"},
+                                       "and wave speed reduced on the device every 10 steps"}
+            if not exchange else {"skipped": "the slabs of a shared cube step through ph_rk_step"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": "residual_kernel (stage: residual + mass inverse + RK update)",

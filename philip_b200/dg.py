@@ -54,12 +54,14 @@ class DGStrong:
 
     def __init__(self, parameters: Parameters, precision: int = _lib.PH_FP64, cell_order: int = 0,
                  stream: int | None = None, warp: float = 0.0, mapping_support_points: np.ndarray | None = None,
-                 slab: tuple[int, int] | None = None, halo=None):
+                 slab: tuple[int, int] | None = None, halo=None, dist=None):
         """warp != 0 gives the sine-warped (curvilinear) cube: every coordinate moves by
         warp (L/2pi) sin(2pi(x-l)/L) sin(2pi(y-l)/L) sin(2pi(z-l)/L), mapping degree = p.
         mapping_support_points ([cell][3][(p+1)^3], GLL points) gives any other curved mapping.
         slab = (z_first, z_count): this process's layers of a mesh shared by several GPUs
-        (philip_b200.slab); halo: the object whose `callback` exchanges the partition faces."""
+        (philip_b200.slab); halo: the object whose `callback` exchanges the partition faces;
+        dist: the torch.distributed module (initialised) over which the integrals, maxima and
+        error norms of the slabs are combined into the mesh's (None: this slab's share)."""
         self.L = _lib.load()
         self.parameters = parameters
         self.params = parameters.to_ph_params(precision)
@@ -79,6 +81,8 @@ class DGStrong:
         self._h = h
         self.slab = slab
         self.halo = halo
+        self.dist = dist if (slab is not None and dist is not None and dist.is_initialized()
+                             and dist.get_world_size() > 1) else None
         if halo is not None:
             _lib.check(self.L.ph_set_halo_exchange(h, halo.callback, None))
         self.n_dofs = int(self.L.ph_ndofs(h))
@@ -149,10 +153,30 @@ class DGStrong:
         _lib.check(self.L.ph_node_xyz(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
         return out
 
+    # -- reductions over the slabs of a shared mesh (identity on a whole mesh)
+    def _allreduce(self, values, op: str) -> np.ndarray:
+        if self.dist is None:
+            return np.asarray(values, dtype=np.float64)
+        import torch
+        dev = "cuda" if self.dist.get_backend() == "nccl" else "cpu"
+        t = torch.tensor(np.asarray(values, dtype=np.float64), device=dev)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM if op == "sum" else self.dist.ReduceOp.MAX)
+        return t.cpu().numpy()
+
+    def global_max(self, value: float) -> float:
+        return float(self._allreduce([value], "max")[0])
+
+    def global_sum(self, value: float) -> float:
+        return float(self._allreduce([value], "sum")[0])
+
     # -- diagnostics
     def integrals(self) -> np.ndarray:
+        """Kinetic energy, enstrophy, vorticity-based dissipation rate (volume averages) and the
+        maximum wave speed; a slab's share of the first three without `dist`."""
         out = np.zeros(4)
         _lib.check(self.L.ph_integrals(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        if self.dist is not None:
+            out = np.concatenate([self._allreduce(out[:3], "sum"), self._allreduce(out[3:], "max")])
         return out
 
     def integrated_quantities(self) -> np.ndarray:
@@ -161,7 +185,7 @@ class DGStrong:
         (_lib.INTEGRATED_QUANTITIES), each over the domain volume."""
         out = np.zeros(len(_lib.INTEGRATED_QUANTITIES))
         _lib.check(self.L.ph_integrated_quantities(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
-        return out
+        return self._allreduce(out, "sum") if self.dist is not None else out
 
     def status(self) -> int:
         v = ctypes.c_uint32(0)
@@ -217,10 +241,14 @@ class RungeKuttaODESolver:
         return out
 
     def error_norm(self) -> float:
-        """Weighted RMS error estimate of the last low-storage step."""
+        """Weighted RMS error estimate of the last low-storage step (over the whole mesh when
+        the slabs of a shared mesh combine their sums)."""
         w = ctypes.c_double(0.0)
         _lib.check(self.dg.L.ph_rk_error_norm(self.dg.handle, ctypes.byref(w)))
-        return float(w.value)
+        if self.dg.dist is None:
+            return float(w.value)
+        s = self.dg._allreduce([w.value ** 2 * self.dg.n_dofs, float(self.dg.n_dofs)], "sum")
+        return float(math.sqrt(s[0] / s[1]))
 
     def get_automatic_error_adaptive_step_size(self, dt: float) -> float:
         """LowStorageRungeKuttaODESolver::get_automatic_error_adaptive_step_size
@@ -241,13 +269,14 @@ class RungeKuttaODESolver:
         n = u_n.size
         rhs = np.empty(n)
         self.dg.apply_inverse_global_mass_matrix(self.dg.residual_of(u_n), rhs)
-        d0 = float(np.max(np.abs(u_n)))
-        d1 = float(np.max(np.abs(rhs)))
+        gmax = self.dg.global_max
+        d0 = gmax(float(np.max(np.abs(u_n))))
+        d1 = gmax(float(np.max(np.abs(rhs))))
         h0 = 1e-6 if (d0 < 1e-5 or d1 < 1e-5) else 0.01 * d0 / d1
         u1 = u_n + h0 * rhs
         rhs1 = np.empty(n)
         self.dg.apply_inverse_global_mass_matrix(self.dg.residual_of(u1), rhs1)
-        d2 = float(np.max(np.abs(rhs1 - rhs))) / h0
+        d2 = gmax(float(np.max(np.abs(rhs1 - rhs)))) / h0
         h1 = max(1e-6, h0 * 1e-3) if max(d1, d2) <= 1e-15 else 0.01 / max(d1, d2)
         self.dg.solution = u_n
         return min(100.0 * h0, h1)
@@ -338,9 +367,13 @@ class FlowSolver:
     switches updated), the unsteady data table, and the state checkpoint."""
 
     def __init__(self, parameters: Parameters, precision: int = _lib.PH_FP64, cell_order: int = 0,
-                 warp: float = 0.0, stream: int | None = None):
+                 warp: float = 0.0, stream: int | None = None, slab: tuple[int, int] | None = None,
+                 halo=None, dist=None):
+        """slab / halo / dist: this process's share of a mesh over several GPUs (DGStrong);
+        the time steps, integrals and table rows are then the whole mesh's on every rank."""
         self.parameters = parameters
-        self.dg = DGStrong(parameters, precision=precision, cell_order=cell_order, warp=warp, stream=stream)
+        self.dg = DGStrong(parameters, precision=precision, cell_order=cell_order, warp=warp, stream=stream,
+                           slab=slab, halo=halo, dist=dist)
         self.ode_solver = RungeKuttaODESolver(self.dg)
         self.flow_case = parameters.get("flow_solver/flow_case_type")
         X = self.dg.node_coordinates()
@@ -433,7 +466,7 @@ class FlowSolver:
 
     def _grid_spacing(self) -> float:
         left, right = self.parameters.grid_bounds
-        ndof_per_state = self.dg.n_dofs // 5
+        ndof_per_state = self.parameters.n_cells ** 3 * self.dg.n_shape   # the whole mesh's
         return (right - left) / ndof_per_state ** (1.0 / 3.0)
 
     def constant_time_step(self) -> float:
@@ -462,6 +495,8 @@ class FlowSolver:
         if adaptive and error_adaptive:
             raise ValueError("CFL-adaptation and error-adaptation cannot be used at the same time")
         write_restart = self.parameters.get("flow_solver/output_restart_files").lower() == "true"
+        if write_restart and self.dg.slab is not None:
+            raise ValueError("restart files hold the whole mesh's state: not written from the slabs of a shared mesh")
         every_x = int(self.parameters.get("flow_solver/output_restart_files_every_x_steps"))
         every_dt = float(self.parameters.get("flow_solver/output_restart_files_every_dt_time_intervals"))
         restart_index = int(self.parameters.get("flow_solver/restart_file_index")) + 1 \
@@ -476,7 +511,7 @@ class FlowSolver:
         if not self.unsteady_data:
             self.unsteady_data.append((self.ode_solver.current_time, *self.dg.integrals()))
         if (not adaptive and not error_adaptive and not write_restart and record_every > 0
-                and not self.parameters.use_relaxation_runge_kutta
+                and not self.parameters.use_relaxation_runge_kutta and self.dg.slab is None
                 and self.ode_solver.current_iteration % record_every == 0):
             # the whole steps of dt run on the device with the records reduced there (ph_run);
             # the count follows the loop below step by step, so the clock is the same
