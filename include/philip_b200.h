@@ -234,7 +234,8 @@ int ph_get_timing(ph_ctx* ctx, double out[7]);
  * the owned cells only (ph_integrals / ph_integrated_quantities give this rank's share of
  * each volume average: sum them over ranks, and take the max of the wave speed). Slab
  * contexts take affine meshes, no relaxation RK, and launch directly (no step graph,
- * ph_run refused). z_count = n is the whole mesh without ghosts. */
+ * ph_run refused). z_count = n is the whole mesh on one rank: its ghost layers are its own last
+ * and first layers (a halo that copies send_hi to recv_lo and send_lo to recv_hi). */
 enum { PH_HALO_STATE = 0, PH_HALO_VISCOUS = 1 };   /* what is exchanged */
 enum { PH_HALO_BEGIN = 0, PH_HALO_END = 1 };        /* phase of the exchange */
 
@@ -256,7 +257,7 @@ typedef int (*ph_halo_fn)(void* user, int what, int phase, const void* send_lo, 
 /* A context for the slab z_first .. z_first + z_count - 1 of mesh (1 <= z_count <= n). */
 int ph_ctx_create_slab(const ph_mesh_desc* mesh, const ph_params* prm, int z_first, int z_count,
                        void* cuda_stream, ph_ctx** out);
-/* Registers the exchange; every slab context with z_count < n needs one before it steps. */
+/* Registers the exchange; every slab context needs one before it evaluates a residual. */
 int ph_set_halo_exchange(ph_ctx* ctx, ph_halo_fn fn, void* user);
 /* Host only (no device work): the owned cells' (i, j, k) [z_count n^2][3] and neighbour table
  * [z_count n^2][6] (faces x-, x+, y-, y+, z-, z+) of a slab. A neighbour index below z_count n^2

@@ -369,13 +369,12 @@ void periodic_connectivity(int n, int order, std::vector<int>& ijk, std::vector<
 }
 
 // Slab z0 .. z0 + nz - 1 of the periodic cube, owned cells lexicographic (x, y, then z from
-// z0). With nz < n the lower ghost layer (layer z0 - 1) follows the owned cells, then the
-// upper one (layer z0 + nz), each in (y, x) order; a ghost's own row names itself (no kernel
-// evaluates a ghost). With nz = n the slab wraps onto itself and has no ghosts.
+// z0). The lower ghost layer (layer z0 - 1) follows the owned cells, then the upper one
+// (layer z0 + nz), each in (y, x) order; a ghost's own row names itself (no kernel evaluates
+// a ghost). With nz = n the ghosts stand for the slab's own last and first layers.
 void slab_connectivity(int n, int z0, int nz, std::vector<int>& ijk, std::vector<int>& nbr) {
     const int L = n * n, nown = nz * L;
-    const bool ghosts = nz < n;
-    const int ntot = nown + (ghosts ? 2 * L : 0);
+    const int ntot = nown + 2 * L;
     ijk.assign(3 * (size_t)nown, 0);
     nbr.assign(6 * (size_t)ntot, 0);
     for (int cc = 0; cc < nown; ++cc) {
@@ -386,13 +385,8 @@ void slab_connectivity(int n, int z0, int nz, std::vector<int>& ijk, std::vector
         nbr[6 * cc + 1] = kz * L + j * n + (i + 1) % n;
         nbr[6 * cc + 2] = kz * L + ((j + n - 1) % n) * n + i;
         nbr[6 * cc + 3] = kz * L + ((j + 1) % n) * n + i;
-        if (ghosts) {
-            nbr[6 * cc + 4] = kz > 0 ? cc - L : nown + in;
-            nbr[6 * cc + 5] = kz < nz - 1 ? cc + L : nown + L + in;
-        } else {
-            nbr[6 * cc + 4] = ((kz + nz - 1) % nz) * L + in;
-            nbr[6 * cc + 5] = ((kz + 1) % nz) * L + in;
-        }
+        nbr[6 * cc + 4] = kz > 0 ? cc - L : nown + in;
+        nbr[6 * cc + 5] = kz < nz - 1 ? cc + L : nown + L + in;
     }
     for (int g = nown; g < ntot; ++g)
         for (int f = 0; f < 6; ++f) nbr[6 * (size_t)g + f] = g;
@@ -925,7 +919,7 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
     c->z_first = slab ? z0 : 0;
     c->z_count = slab ? nz : c->n;
     c->nc = c->z_count * c->layer;
-    c->nc_ghost = (slab && nz < c->n) ? 2 * c->layer : 0;
+    c->nc_ghost = slab ? 2 * c->layer : 0;
     c->p = prm->poly_degree;
     c->N1 = c->p + 1;
     c->NP = c->N1 * c->N1 * c->N1;

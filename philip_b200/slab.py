@@ -101,6 +101,31 @@ class DistributedHalo:
             return 1
 
 
+class LoopbackHalo:
+    """ph_halo_fn of a slab that owns every layer (one rank): its lower ghost layer is its own
+    last layer and its upper ghost its own first, so recv_lo <- send_hi and recv_hi <- send_lo,
+    two device copies on the context stream (no host synchronisation)."""
+
+    def __init__(self, device: str = "cuda"):
+        self.device = device
+        self.callback = _lib.HALO_FN(self._call)
+
+    def _call(self, user, what, phase, send_lo, send_hi, recv_lo, recv_hi, nbytes, stream):
+        try:
+            if phase == _lib.PH_HALO_BEGIN:
+                import contextlib
+                import torch
+                ctx = contextlib.nullcontext() if self.device == "cpu" else torch.cuda.stream(
+                    torch.cuda.ExternalStream(stream) if stream else torch.cuda.default_stream())
+                with ctx:
+                    _as_tensor(recv_lo, nbytes, self.device).copy_(_as_tensor(send_hi, nbytes, self.device))
+                    _as_tensor(recv_hi, nbytes, self.device).copy_(_as_tensor(send_lo, nbytes, self.device))
+            return 0
+        except Exception:
+            traceback.print_exc(file=sys.stderr)
+            return 1
+
+
 def global_integrals(local, dist=None, device: str = "cpu"):
     """The mesh's ph_integrals values from every slab's: the three volume averages summed,
     the wave speed maximised."""

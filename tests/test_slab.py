@@ -67,7 +67,7 @@ def test_slab_plan_names_the_periodic_neighbours(n, z0, nz):
             if g < nown:
                 assert list(ijk[g]) == t
             else:                               # ghost slot: only z faces of the first / last layer
-                assert nz < n and d == 2
+                assert d == 2
                 side, ii = divmod(g - nown, n * n)
                 layer = (z0 - 1) % n if side == 0 else (z0 + nz) % n
                 assert (ii % n, ii // n, layer) == tuple(t)
@@ -120,6 +120,16 @@ def test_halo_exchange_fills_the_ghost_layers(world, n):
         ok, tot = res[r]
         assert ok
         assert tot == [sum(1.0 + q for q in range(world)), 2.0 * world, 0.5 * world, 3.0 + world - 1]
+
+
+def test_loopback_halo_feeds_a_slab_its_own_layers():
+    from philip_b200.slab import LoopbackHalo
+    bufs = [np.arange(6.0) + 10 * k for k in range(4)]
+    halo = LoopbackHalo(device="cpu")
+    ptr = [b.ctypes.data for b in bufs]
+    assert halo.callback(None, _lib.PH_HALO_STATE, _lib.PH_HALO_BEGIN, *ptr, bufs[0].nbytes, None) == 0
+    assert halo.callback(None, _lib.PH_HALO_STATE, _lib.PH_HALO_END, *ptr, bufs[0].nbytes, None) == 0
+    assert np.array_equal(bufs[2], np.arange(6.0) + 10) and np.array_equal(bufs[3], np.arange(6.0))
 
 
 def test_slab_refusals_without_a_gpu():
@@ -350,10 +360,27 @@ def test_slab_exchange_failures_are_reported():
     dg = DGStrong(prm, slab=(0, 2), halo=Failing())
     with pytest.raises(_lib.PhError, match="returned 7"):
         dg.residual_of(U)
-    # the whole mesh as one slab needs no exchange
-    one = DGStrong(prm, slab=(0, 4))
-    whole = DGStrong(prm)
+
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kw", [dict(poly_degree=3, n_cells=4, pde="navier_stokes", diss="bassi_rebay_2"),
+                                dict(poly_degree=5, n_cells=3)], ids=["ns_br2_p3", "euler_p5"])
+def test_one_slab_with_its_own_ghosts_is_the_whole_mesh(kw):
+    """The whole mesh as one slab exchanges with itself (LoopbackHalo, stream-ordered device
+    copies): residual and RK4 steps bitwise the whole-mesh context's."""
     from oracle.oracle import Oracle
+    from philip_b200.dg import DGStrong, RungeKuttaODESolver
+    from philip_b200.prm import Parameters
+    from philip_b200.slab import LoopbackHalo
+    from helpers import prm_dict
+    prm = Parameters.from_dict(prm_dict(**kw))
+    whole = DGStrong(prm)
+    one = DGStrong(prm, slab=(0, prm.n_cells), halo=LoopbackHalo())
     U0 = Oracle(prm.oracle_cfg(), prm.n_cells, *prm.grid_bounds).initial_condition("tgv")
     one.solution = _scatter(whole, [one], U0)[0]
     assert np.array_equal(_gather(whole, [one], [one.residual_of(one.solution)]), whole.residual_of(U0))
+    whole.solution = U0
+    RungeKuttaODESolver(whole).step_in_time(1e-3, nsteps=2)
+    RungeKuttaODESolver(one).step_in_time(1e-3, nsteps=2)
+    assert np.array_equal(_gather(whole, [one], [one.solution]), whole.solution)
