@@ -688,6 +688,10 @@ struct ph_ctx {
     void* halo_user = nullptr;
     unsigned char* d_halo = nullptr;    // send_lo | send_hi | recv_lo | recv_hi, halo_stride bytes each
     size_t halo_stride = 0, halo_state_bytes = 0, halo_visc_bytes = 0;
+    // the interior cells' kernels run on a second stream, concurrently with the exchange and the
+    // first and last layers' kernels; events fork it from and join it to the context stream
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_aux = nullptr, ev_join = nullptr;
 };
 
 namespace {
@@ -844,6 +848,23 @@ int stage_range(ph_ctx* c, ph::StageArgs a, int begin, int end) {
 // the viscous terms are refreshed through the halo callback; the cells that read no ghost data
 // run while each transfer is in flight, the first and last layer after it. Every cell runs the
 // same code on the same inputs as in one launch over all cells.
+// Runs `launch` on the interior stream after everything queued so far on the context stream
+// (or on the context stream itself when `fork` is false); `done`, when given, is recorded on
+// the interior stream after it.
+template <typename F>
+int on_interior(ph_ctx* c, bool fork, F launch, cudaEvent_t done) {
+    if (!fork) return launch();
+    PH_CUDA(cudaEventRecord(c->ev_fork, c->stream));
+    PH_CUDA(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
+    cudaStream_t main = c->stream;
+    c->stream = c->side;
+    const int rc = launch();
+    c->stream = main;
+    if (rc) return rc;
+    if (done) PH_CUDA(cudaEventRecord(done, c->side));
+    return PH_OK;
+}
+
 int eval_residual(ph_ctx* c, const double* in, ph::StageArgs a) {
     a.U = in;
     if (!c->nc_ghost) {
@@ -851,11 +872,16 @@ int eval_residual(ph_ctx* c, const double* in, ph::StageArgs a) {
         return stage_range(c, a, 0, c->nc);
     }
     const int lo = c->lo_end, hi = c->hi_begin, nc = c->nc;
+    // the interior runs concurrently unless there is none or every launch is being timed
+    const bool fork = lo < hi && !c->timing;
     if (int rc = halo_copy(c, PH_HALO_STATE, true, in)) return rc;
     if (int rc = halo_call(c, PH_HALO_STATE, PH_HALO_BEGIN)) return rc;
     if (lo < hi) {
-        if (c->visc) { if (int rc = dispatch_aux(c, in, lo, hi)) return rc; }
-        else if (int rc = stage_range(c, a, lo, hi)) return rc;
+        if (c->visc) {
+            if (int rc = on_interior(c, fork, [&] { return dispatch_aux(c, in, lo, hi); }, c->ev_aux)) return rc;
+        } else if (int rc = on_interior(c, fork, [&] { return stage_range(c, a, lo, hi); }, c->ev_join)) {
+            return rc;
+        }
     }
     if (int rc = halo_call(c, PH_HALO_STATE, PH_HALO_END)) return rc;
     if (int rc = halo_copy(c, PH_HALO_STATE, false, in)) return rc;
@@ -864,12 +890,17 @@ int eval_residual(ph_ctx* c, const double* in, ph::StageArgs a) {
         if (hi < nc) if (int rc = dispatch_aux(c, in, hi, nc)) return rc;
         if (int rc = halo_copy(c, PH_HALO_VISCOUS, true, in)) return rc;
         if (int rc = halo_call(c, PH_HALO_VISCOUS, PH_HALO_BEGIN)) return rc;
-        if (int rc = stage_range(c, a, lo, hi)) return rc;
+        // the interior stage reads the first and last layers' viscous terms: forked after them
+        if (int rc = on_interior(c, fork, [&] { return stage_range(c, a, lo, hi); }, c->ev_join)) return rc;
         if (int rc = halo_call(c, PH_HALO_VISCOUS, PH_HALO_END)) return rc;
         if (int rc = halo_copy(c, PH_HALO_VISCOUS, false, in)) return rc;
+        // ... and the first and last layers read the interior's
+        if (fork) PH_CUDA(cudaStreamWaitEvent(c->stream, c->ev_aux, 0));
     }
     if (int rc = stage_range(c, a, 0, lo)) return rc;
-    return stage_range(c, a, hi, nc);
+    if (int rc = stage_range(c, a, hi, nc)) return rc;
+    if (fork) PH_CUDA(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+    return PH_OK;
 }
 
 } // namespace
@@ -1030,6 +1061,13 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
         c->hi_begin = (c->nc - c->layer) / cpc * cpc;
         if (c->lo_end >= c->hi_begin) c->lo_end = c->hi_begin = c->nc;   // no cell is free of ghost data
     }
+    if (c->nc_ghost) {
+        cudaError_t se = cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking);
+        if (se == cudaSuccess) se = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+        if (se == cudaSuccess) se = cudaEventCreateWithFlags(&c->ev_aux, cudaEventDisableTiming);
+        if (se == cudaSuccess) se = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
+        if (se != cudaSuccess) { ph_ctx_destroy(c); return fail(PH_ERR_CUDA, cudaGetErrorString(se)); }
+    }
     *out = c;
     return PH_OK;
 }
@@ -1071,7 +1109,10 @@ int ph_ctx_destroy(ph_ctx* c) {
     void* ptrs[] = {c->d_nbr, c->d_ops, c->d_itab, c->d_sol, c->d_stA, c->d_stB, c->d_acc, c->d_carry,
                     c->d_fv, c->d_comp, c->d_tmpA, c->d_tmpB, c->d_partial, c->d_status, c->d_metric, c->d_xnode, c->d_origin, c->d_err,
                     c->d_table, c->d_counter, c->d_ent, c->d_ent_cell, c->d_halo};
+    if (c->side) cudaStreamSynchronize(c->side);
     for (void* p : ptrs) if (p) cudaFree(p);
+    if (c->side) cudaStreamDestroy(c->side);
+    for (cudaEvent_t ev : {c->ev_fork, c->ev_aux, c->ev_join}) if (ev) cudaEventDestroy(ev);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     delete c;
