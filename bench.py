@@ -106,15 +106,47 @@ def flops_per_dof_stage(p: int, viscous: bool) -> float:
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    """Samples the SM clock and the clock-event (throttle) reasons during the timed region:
+    through NVML every 5 ms (the device found by its PCI bus id), else nvidia-smi every 50 ms.
+    Reads only."""
 
     def __init__(self, device_index: int):
         self.idx = device_index
         self.samples = []
+        self.source = "nvidia-smi"
         self._stop = threading.Event()
         self._thr = None
+        self._nvml = None
+        try:
+            import pynvml
+            import torch
+            pr = torch.cuda.get_device_properties(device_index)
+            pynvml.nvmlInit()
+            bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+            self._handle = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            self._max = float(pynvml.nvmlDeviceGetMaxClockInfo(self._handle, pynvml.NVML_CLOCK_SM))
+            self._nvml = pynvml
+            self.source = "nvml"
+        except Exception:
+            self._nvml = None
+
+    def _run_nvml(self):
+        n = self._nvml
+        bits = [n.nvmlClocksEventReasonHwSlowdown, n.nvmlClocksEventReasonHwThermalSlowdown,
+                n.nvmlClocksEventReasonSwThermalSlowdown, n.nvmlClocksEventReasonSwPowerCap]
+        while not self._stop.is_set():
+            try:
+                sm = float(n.nvmlDeviceGetClockInfo(self._handle, n.NVML_CLOCK_SM))
+                r = int(n.nvmlDeviceGetCurrentClocksEventReasons(self._handle))
+                self.samples.append([str(sm), str(self._max), ""] +
+                                    ["Active" if r & b else "Not Active" for b in bits])
+            except Exception:
+                pass
+            self._stop.wait(0.005)
 
     def _run(self):
+        if self._nvml is not None:
+            return self._run_nvml()
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
@@ -147,7 +179,7 @@ class ClockSampler:
         reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 3 + i and "Active" in s[3 + i]
                           and not s[3 + i].startswith("Not")})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": reasons, "samples": len(self.samples)}
+                "reasons": reasons, "samples": len(self.samples), "source": self.source}
 
 
 def measured_peaks():
