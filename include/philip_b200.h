@@ -329,6 +329,34 @@ int ph_batch_set_variant(int poly_degree, int precision, int curvilinear, int va
 /* launches of this library's kernels issued by ph_batch_step so far (graph nodes counted) */
 int ph_batch_launches(ph_batch* b, long long* launches);
 
+/* ---- Served solves: continuous batching behind a submission queue. Callers on any host
+ * thread submit solves and collect results; one worker thread owns a ph_batch (HBM budget,
+ * precision) and, pass after pass, admits queued solves in FIFO order while the budget holds
+ * them (a solve that does not fit waits and holds the ones behind it), enqueues chunk_steps RK
+ * steps of every resident solve with at most two chunks in flight, and retires each solve
+ * whose last step the GPU has finished (final state and status word copied to host memory,
+ * arena range released). The solves are the batch's (split-form Euler, ...), with the batch's
+ * results. No counterpart in the reference, which runs one FlowSolver per snapshot
+ * (AdaptiveSamplingBase::solveSnapshotFOM, src/reduced_order/adaptive_sampling_base.cpp:255-265). */
+typedef struct ph_server ph_server;
+enum { PH_SOLVE_QUEUED = 0, PH_SOLVE_RUNNING = 1, PH_SOLVE_DONE = 2, PH_SOLVE_FAILED = 3 };
+int ph_server_create(size_t hbm_budget_bytes, int precision, int chunk_steps, ph_server** out);
+/* Copies mesh (and its mapping support points), parameters and U0 (host, n^3 5 (p+1)^3
+ * doubles); returns at once with a ticket. Thread-safe. */
+int ph_server_submit(ph_server* s, const ph_mesh_desc* mesh, const ph_params* prm, const double* U0, double dt,
+                     int nsteps, long long* ticket);
+int ph_server_poll(ph_server* s, long long ticket, int* state);
+/* blocks until the solve is done or failed, or timeout_s passes; *state as ph_server_poll */
+int ph_server_wait(ph_server* s, long long ticket, double timeout_s, int* state);
+/* A finished solve: final state into U (may be NULL), status word, seconds from submission to
+ * admission and to completion; the ticket is then forgotten. A failed solve returns its error. */
+int ph_server_result(ph_server* s, long long ticket, double* U, uint32_t* flags, double seconds[2]);
+/* out = {solves queued now, admissions deferred for lack of room so far, most solves resident} */
+int ph_server_stats(ph_server* s, long long out[3]);
+/* Cancels the solves not yet admitted (they fail), lets the resident ones finish, then frees
+ * everything. */
+int ph_server_destroy(ph_server* s);
+
 int ph_sync(ph_ctx* ctx);
 const char* ph_last_error(void);
 

@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libphilip_b200.so")
 N1_RANGE = range(2, 8)          # p = 1 .. 6
-HOST_UNITS = ("ph_capi", "ph_batch")   # C-ABI: single-solve context, batch of solves
+HOST_UNITS = ("ph_capi", "ph_batch", "ph_server")   # C-ABI: single-solve context, batch of solves, server
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

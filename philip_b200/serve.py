@@ -10,6 +10,9 @@ each of which runs FlowSolver::run, src/flow_solver/flow_solver.cpp:427-600).
   SnapshotServer ..... continuous batching: requests that arrive while others run are admitted
                        as the HBM budget frees up, stepped in chunks with a bounded amount of
                        work in flight, retired as they finish; records per-solve latency
+  Server ............. the same loop in native code behind a thread-safe submission queue
+                       (ph_server_*): submit from any thread, poll / wait, collect results
+  serve_native ....... a stream of timed arrivals through a Server, with per-solve latency
   autotune ........... the tile-shape autotuner of the batched stage kernel
 """
 from __future__ import annotations
@@ -335,6 +338,106 @@ class SnapshotServer:
                     self.batch.wait(tickets.popleft())
         stats.makespan = self.clock() - t0
         return stats
+
+
+class Server:
+    """ph_server_*: a worker thread of the library runs the continuous-batching loop over its
+    own batch; submissions return a ticket at once and may come from any thread."""
+
+    def __init__(self, budget_bytes: int, precision: int = _lib.PH_FP32_RESIDUAL, chunk: int = 16):
+        self.L = _lib.load()
+        h = ctypes.c_void_p()
+        _lib.check(self.L.ph_server_create(ctypes.c_size_t(int(budget_bytes)), precision, chunk, ctypes.byref(h)))
+        self._h = h
+        self.precision = precision
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            self.L.ph_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def submit(self, mesh, params, U0: np.ndarray, dt: float, nsteps: int) -> int:
+        t = ctypes.c_longlong(0)
+        U0 = np.ascontiguousarray(U0, dtype=np.float64)
+        _lib.check(self.L.ph_server_submit(self._h, ctypes.byref(mesh), ctypes.byref(params), _dp(U0), dt, nsteps,
+                                           ctypes.byref(t)))
+        return int(t.value)
+
+    def submit_request(self, req: SolveRequest) -> int:
+        U0, dt, nsteps = req.prepare()
+        return self.submit(req.mesh(), req.parameters().to_ph_params(self.precision), U0, dt, nsteps)
+
+    def poll(self, ticket: int) -> int:
+        st = ctypes.c_int(0)
+        _lib.check(self.L.ph_server_poll(self._h, ticket, ctypes.byref(st)))
+        return int(st.value)
+
+    def wait(self, ticket: int, timeout: float = 3600.0) -> int:
+        st = ctypes.c_int(0)
+        _lib.check(self.L.ph_server_wait(self._h, ticket, timeout, ctypes.byref(st)))
+        return int(st.value)
+
+    def result(self, ticket: int, ndofs: int):
+        """(final state, status word, (seconds to admission, seconds to completion)); raises
+        PhError for a failed solve."""
+        U = np.empty(ndofs)
+        flags = ctypes.c_uint32(0)
+        sec = (ctypes.c_double * 2)()
+        _lib.check(self.L.ph_server_result(self._h, ticket, _dp(U), ctypes.byref(flags), sec))
+        return U, int(flags.value), (float(sec[0]), float(sec[1]))
+
+    def stats(self):
+        out = (ctypes.c_longlong * 3)()
+        _lib.check(self.L.ph_server_stats(self._h, out))
+        return {"queued": int(out[0]), "admissions_deferred": int(out[1]), "max_resident": int(out[2])}
+
+
+def serve_native(server: Server, arrivals, keep_states: bool = False, clock=time.perf_counter):
+    """arrivals: list of (arrival time in s from start, SolveRequest). Each request is prepared
+    (initial state, time step) and submitted at its arrival time; the results are collected as
+    they finish. Latency = completion - arrival. Returns ServeStats."""
+    import threading
+    stats = ServeStats()
+    order = sorted(arrivals, key=lambda a: a[0])
+    submitted = []                 # (ticket, request, arrival, seconds after start at submission)
+    lock = threading.Lock()
+    t0 = clock()
+
+    def submitter():
+        for arr, req in order:
+            delay = arr - (clock() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            ticket = server.submit_request(req)
+            with lock:
+                submitted.append((ticket, req, arr, clock() - t0))
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    done = 0
+    while done < len(order):
+        with lock:
+            pending = list(submitted)
+            submitted.clear()
+        if not pending:
+            time.sleep(0.001)
+            continue
+        for ticket, req, arr, t_sub in pending:
+            server.wait(ticket)
+            U, flags, (t_adm, t_done) = server.result(ticket, req.ndofs)
+            _, _, nsteps = req.prepare()
+            stats.completed.append(Completed(req, arr, t_sub + t_adm, t_sub + t_done, nsteps,
+                                             U if keep_states else None, flags))
+            done += 1
+    th.join()
+    stats.makespan = max(c.done for c in stats.completed) if stats.completed else 0.0
+    s = server.stats()
+    stats.max_in_flight = s["max_resident"]
+    stats.admissions_deferred = s["admissions_deferred"]
+    return stats
 
 
 def poisson_arrivals(rate: float, count: int, rng: np.random.Generator):
