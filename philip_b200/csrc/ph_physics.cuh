@@ -326,7 +326,14 @@ __device__ __forceinline__ void roe_dissipation(const NodeQ<R>& L, const NodeQ<R
     for (int e = 0; e < 3; ++e) {
         const R a1 = rabs(eig[e] - eL[e]), a2 = rabs(eR[e] - eig[e]);
         const R eps = a1 > a2 ? a1 : a2;
-        if (eig[e] < eps) eig[e] = R(0.5) * (qdiv<R>(eig[e] * eig[e], eps) + eps);
+        if (eig[e] < eps) {
+            // eig^2 / eps < eps; when eps is below the normal range the flushed approximate
+            // reciprocal is infinite and the quotient inf or NaN (0 * inf): the term is then
+            // below eps and is dropped (IEEE division would give a value of order eps too)
+            R t = qdiv<R>(eig[e] * eig[e], eps);
+            if (!(t <= R(2) * eps)) t = R(0);
+            eig[e] = R(0.5) * (t + eps);
+        }
     }
     const R dp = Rq.p - L.p, drho = Rq.rho - L.rho, dvn = vnR - vnL;
     R dvt[3];

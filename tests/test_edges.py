@@ -144,3 +144,25 @@ def test_device_time_loop_refuses_relaxed_steps():
     rows = np.zeros((2, 4))
     rc = dg.L.ph_run(dg.handle, 1e-3, 4, 2, rows.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
     assert rc == _lib.PH_ERR_UNSUPPORTED and b"relaxation" in dg.L.ph_last_error()
+
+
+@pytest.mark.gpu
+def test_roe_entropy_fix_with_vanishing_wave_speed_differences():
+    """A z-extruded isentropic vortex in the precision form: at the z faces the normal
+    velocities and their differences are below FP32's normal range, where the Harten fix's
+    eps^-1 (an approximate reciprocal that flushes to zero) is infinite; the fix then keeps
+    eps / 2 (the quotient it drops is smaller than eps), so the step stays finite and close to
+    the FP64 step (before this guard two nodes per corner cell turned NaN after one step)."""
+    from philip_b200.dg import DGStrong, RungeKuttaODESolver
+    from philip_b200.serve import SolveRequest
+    req = SolveRequest("isentropic_vortex", n_cells=3, poly_degree=4, mach=0.4, final_time=0.02)
+    U0, dt, nsteps = req.prepare()
+    out = {}
+    for prec in (_lib.PH_FP64, _lib.PH_FP32_RESIDUAL):
+        dg = DGStrong(req.parameters(), precision=prec)
+        dg.solution = U0
+        RungeKuttaODESolver(dg).step_in_time(dt, nsteps=nsteps)
+        out[prec] = dg.solution
+        assert dg.status() == 0
+    assert np.all(np.isfinite(out[_lib.PH_FP32_RESIDUAL]))
+    assert rel_max_err(out[_lib.PH_FP32_RESIDUAL], out[_lib.PH_FP64]) <= 1e-5
