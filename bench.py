@@ -354,7 +354,7 @@ def run_many(args, rank: int = 0, world: int = 1, local_rank: int = 0):
     exchange between ranks), so the total work is fixed (strong scaling)."""
     import torch
     from philip_b200 import _lib
-    from philip_b200.serve import Batch, SnapshotServer, autotune, poisson_arrivals
+    from philip_b200.serve import Batch, Server, SnapshotServer, autotune, poisson_arrivals, serve_native
     from philip_b200.shard import reduce_max, reduce_sum, request_cost, shard_by_cost
     torch.cuda.set_device(local_rank)
     dist = None
@@ -378,17 +378,28 @@ def run_many(args, rank: int = 0, world: int = 1, local_rank: int = 0):
     for r in reqs:   # the requests' payload (initial state, time step), before the clock starts
         r.prepare()
     budget = int(args.budget_gb * (1 << 30))
+    keep = args.workload == "vortex_batch_256"
+    native = args.server == "native"
     # warm-up: one small solve through the same batch machinery
-    warm = Batch(1 << 28, prec)
-    SnapshotServer(warm, chunk=args.chunk, precision=prec).run([(0.0, many_requests(args.workload, 1, seed=1)[0])])
-    warm.close()
-    batch = Batch(budget, prec)
+    warm_req = many_requests(args.workload, 1, seed=1)[0]
+    if native:
+        warm = Server(1 << 28, prec, chunk=args.chunk)
+        serve_native(warm, [(0.0, warm_req)])
+        warm.close()
+    else:
+        warm = Batch(1 << 28, prec)
+        SnapshotServer(warm, chunk=args.chunk, precision=prec).run([(0.0, warm_req)])
+        warm.close()
+    batch = Server(budget, prec, chunk=args.chunk) if native else Batch(budget, prec)
     if dist is not None:
         dist.barrier()
     with ClockSampler(local_rank) as clk:
-        srv = SnapshotServer(batch, chunk=args.chunk, keep_states=args.workload == "vortex_batch_256", precision=prec)
-        stats = srv.run(list(zip(arrivals, reqs)))
-    launches = batch.launches
+        if native:   # the loop in the library's worker thread; requests submitted as they arrive
+            stats = serve_native(batch, list(zip(arrivals, reqs)), keep_states=keep)
+        else:
+            srv = SnapshotServer(batch, chunk=args.chunk, keep_states=keep, precision=prec)
+            stats = srv.run(list(zip(arrivals, reqs)))
+    launches = batch.stats()["launches"] if native else batch.launches
     batch.close()
     work = sum(c.request.ndofs * 4 * c.steps for c in stats.completed)
     if dist is not None:   # whole job: all ranks' solves and work over the slowest rank's makespan
@@ -419,6 +430,7 @@ def run_many(args, rank: int = 0, world: int = 1, local_rank: int = 0):
         "data": "synthetic (seeded requests; exact initial conditions)",
         "config": {"workload": args.workload, "description": MANY[args.workload], "requests": count,
                    "budget_gb": args.budget_gb, "chunk_steps": args.chunk,
+                   "server": "ph_server (native worker thread)" if native else "SnapshotServer (Python loop)",
                    "arrival_rate_per_s": None if args.workload == "vortex_batch_256" else args.rate,
                    "total_dofs": int(sum(r.ndofs for r in reqs)),
                    "tile_variants": {f"p{k[0]}{'c' if k[1] else 'a'}": v for k, v in tuned.items()}},
@@ -536,6 +548,8 @@ def main():
                     help="batched / served forms: solves in the one-at-a-time FP64 comparison (0 = all)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--server", default="native", choices=["native", "python"],
+                    help="batched / served forms: the library's serving loop or the Python one")
     ap.add_argument("--shard", default="replicas", choices=["replicas", "slab"],
                     help="N > 1: a copy of the cube per GPU, or one cube in slabs of cell layers")
     args = ap.parse_args()

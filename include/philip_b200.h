@@ -351,8 +351,9 @@ int ph_server_wait(ph_server* s, long long ticket, double timeout_s, int* state)
 /* A finished solve: final state into U (may be NULL), status word, seconds from submission to
  * admission and to completion; the ticket is then forgotten. A failed solve returns its error. */
 int ph_server_result(ph_server* s, long long ticket, double* U, uint32_t* flags, double seconds[2]);
-/* out = {solves queued now, admissions deferred for lack of room so far, most solves resident} */
-int ph_server_stats(ph_server* s, long long out[3]);
+/* out = {solves queued now, admissions deferred for lack of room so far, most solves resident,
+ * kernel launches issued so far (graph nodes counted)} */
+int ph_server_stats(ph_server* s, long long out[4]);
 /* Cancels the solves not yet admitted (they fail), lets the resident ones finish, then frees
  * everything. */
 int ph_server_destroy(ph_server* s);

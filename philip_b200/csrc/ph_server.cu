@@ -64,6 +64,7 @@ struct ph_server {
     bool stop = false;
     long long admissions_deferred = 0;
     int max_resident = 0;
+    long long launches = 0;            // kernel launches the batch has issued (graph nodes counted)
     std::thread worker;
 
     void run();
@@ -127,6 +128,10 @@ void ph_server::run() {
             long long t = 0;
             if (ph_batch_step(batch, chunk) == PH_OK && ph_batch_fence(batch, &t) == PH_OK) fences.push_back(t);
             if (fences.size() > 2) { ph_batch_fence_wait(batch, fences.front()); fences.pop_front(); }
+            long long n = 0;
+            ph_batch_launches(batch, &n);
+            std::lock_guard<std::mutex> lk(mu);
+            launches = n;
         }
         for (auto it = resident.begin(); it != resident.end();) {
             int complete = 0;
@@ -248,12 +253,13 @@ int ph_server_result(ph_server* s, long long ticket, double* U, uint32_t* flags,
     return rc;
 }
 
-int ph_server_stats(ph_server* s, long long out[3]) {
+int ph_server_stats(ph_server* s, long long out[4]) {
     if (!s || !out) return fail(PH_ERR_INVALID, "null argument");
     std::lock_guard<std::mutex> lk(s->mu);
     out[0] = (long long)s->queue.size();
     out[1] = s->admissions_deferred;
     out[2] = s->max_resident;
+    out[3] = s->launches;
     return PH_OK;
 }
 

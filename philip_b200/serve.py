@@ -390,9 +390,10 @@ class Server:
         return U, int(flags.value), (float(sec[0]), float(sec[1]))
 
     def stats(self):
-        out = (ctypes.c_longlong * 3)()
+        out = (ctypes.c_longlong * 4)()
         _lib.check(self.L.ph_server_stats(self._h, out))
-        return {"queued": int(out[0]), "admissions_deferred": int(out[1]), "max_resident": int(out[2])}
+        return {"queued": int(out[0]), "admissions_deferred": int(out[1]), "max_resident": int(out[2]),
+                "launches": int(out[3])}
 
 
 def serve_native(server: Server, arrivals, keep_states: bool = False, clock=time.perf_counter):
