@@ -332,7 +332,8 @@ int ph_batch_launches(ph_batch* b, long long* launches);
 /* ---- Served solves: continuous batching behind a submission queue. Callers on any host
  * thread submit solves and collect results; one worker thread owns a ph_batch (HBM budget,
  * precision) and, pass after pass, admits queued solves in FIFO order while the budget holds
- * them (a solve that does not fit waits and holds the ones behind it), enqueues chunk_steps RK
+ * them (a solve that does not fit waits and holds the ones behind it) for at most admit_slice_s of
+ * host time while solves are resident, enqueues chunk_steps RK
  * steps of every resident solve with at most two chunks in flight, and retires each solve
  * whose last step the GPU has finished (final state and status word copied to host memory,
  * arena range released). The solves are the batch's (split-form Euler, ...), with the batch's
@@ -340,9 +341,12 @@ int ph_batch_launches(ph_batch* b, long long* launches);
  * (AdaptiveSamplingBase::solveSnapshotFOM, src/reduced_order/adaptive_sampling_base.cpp:255-265). */
 typedef struct ph_server ph_server;
 enum { PH_SOLVE_QUEUED = 0, PH_SOLVE_RUNNING = 1, PH_SOLVE_DONE = 2, PH_SOLVE_FAILED = 3 };
-int ph_server_create(size_t hbm_budget_bytes, int precision, int chunk_steps, ph_server** out);
-/* Copies mesh (and its mapping support points), parameters and U0 (host, n^3 5 (p+1)^3
- * doubles); returns at once with a ticket. Thread-safe. */
+/* admit_slice_s: host time per pass the worker may spend admitting while solves are resident
+ * (an admission builds the solve's geometry on the host; e.g. 0.004) */
+int ph_server_create(size_t hbm_budget_bytes, int precision, int chunk_steps, double admit_slice_s, ph_server** out);
+/* Checks the solve, builds its host-side set-up (operators, connectivity, geometry) on the
+ * calling thread, copies U0 (host, n^3 5 (p+1)^3 doubles) and returns a ticket without waiting
+ * for the GPU. Thread-safe. */
 int ph_server_submit(ph_server* s, const ph_mesh_desc* mesh, const ph_params* prm, const double* U0, double dt,
                      int nsteps, long long* ticket);
 int ph_server_poll(ph_server* s, long long ticket, int* state);

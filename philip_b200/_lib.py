@@ -127,7 +127,7 @@ def load(build_if_missing: bool = False):
     L.ph_slab_connectivity.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int32),
                                        ctypes.POINTER(ctypes.c_int32)]
     ll = ctypes.c_longlong
-    L.ph_server_create.argtypes = [sz, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
+    L.ph_server_create.argtypes = [sz, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.POINTER(vp)]
     L.ph_server_submit.argtypes = [vp, ctypes.POINTER(PhMeshDesc), ctypes.POINTER(PhParams), dp, ctypes.c_double,
                                    ctypes.c_int, ctypes.POINTER(ll)]
     L.ph_server_poll.argtypes = [vp, ll, ctypes.POINTER(ctypes.c_int)]

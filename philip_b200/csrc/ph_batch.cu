@@ -424,8 +424,25 @@ int ph_batch_bytes(const ph_mesh_desc* mesh, const ph_params* prm, size_t* bytes
     return PH_OK;
 }
 
-int ph_batch_admit(ph_batch* b, const ph_mesh_desc* mesh, const ph_params* prm, const double* U0, double dt,
-                   int nsteps, int* slot) {
+}  // extern "C"
+
+int ph_host::batch_prepare(const ph_mesh_desc* mesh, const ph_params* prm, BatchPrep& out) {
+    if (!mesh || !prm) return fail(PH_ERR_INVALID, "null argument");
+    if (int rc = check_batch_params(nullptr, mesh, prm)) return rc;
+    std::vector<double> x, D, xyz;
+    std::vector<int> ijk;
+    int rc = build_operators(prm, out.ops, out.fr, x, D);
+    if (!rc) {
+        periodic_connectivity(mesh->n_cells_per_direction, mesh->cell_order, ijk, out.nbr);
+        rc = node_geometry(mesh->n_cells_per_direction, ijk, x, D, mesh->left, mesh->right, mesh->warp, xyz,
+                           out.metric, mesh->mapping_support_points);
+    }
+    out.ready = rc == PH_OK;
+    return rc;
+}
+
+int ph_host::batch_admit_prepared(ph_batch* b, const ph_mesh_desc* mesh, const ph_params* prm, const BatchPrep* prep,
+                                  const double* U0, double dt, int nsteps, int* slot) {
     if (!b || !mesh || !prm || !U0 || !slot) return fail(PH_ERR_INVALID, "null argument");
     *slot = -1;
     if (int rc = check_batch_params(b, mesh, prm)) return rc;
@@ -447,17 +464,16 @@ int ph_batch_admit(ph_batch* b, const ph_mesh_desc* mesh, const ph_params* prm, 
         if (ph_batch_autotune(prm->poly_degree, b->fp32 ? PH_FP32_RESIDUAL : PH_FP64, curv ? 1 : 0, &best, ms, &nv))
             set_variant(N1, b->fp32, curv, 0);
     }
-    // host set-up: operators, connectivity, geometry
-    ph::OpTab ops;
-    bool fr = false;
-    std::vector<double> x, D, xyz, metric;
-    std::vector<int> ijk, nbr;
-    int rc = build_operators(prm, ops, fr, x, D);
-    if (!rc) {
-        periodic_connectivity(n, mesh->cell_order, ijk, nbr);
-        rc = node_geometry(n, ijk, x, D, mesh->left, mesh->right, mesh->warp, xyz, metric, mesh->mapping_support_points);
+    // host set-up: operators, connectivity, geometry (here, unless the caller prepared them)
+    BatchPrep local;
+    if (!prep || !prep->ready) {
+        if (int rc = batch_prepare(mesh, prm, local)) { arena_free(b, off, L.total); return rc; }
+        prep = &local;
     }
-    if (rc) { arena_free(b, off, L.total); return rc; }
+    const ph::OpTab& ops = prep->ops;
+    const bool fr = prep->fr;
+    const std::vector<int>& nbr = prep->nbr;
+    const std::vector<double>& metric = prep->metric;
     int s = -1;
     for (int i = 0; i < (int)b->slots.size(); ++i)
         if (!b->slots[i].used) { s = i; break; }
@@ -513,6 +529,13 @@ int ph_batch_admit(ph_batch* b, const ph_mesh_desc* mesh, const ph_params* prm, 
     if (!sl.finished) b->dirty = true;
     *slot = s;
     return PH_OK;
+}
+
+extern "C" {
+
+int ph_batch_admit(ph_batch* b, const ph_mesh_desc* mesh, const ph_params* prm, const double* U0, double dt,
+                   int nsteps, int* slot) {
+    return batch_admit_prepared(b, mesh, prm, nullptr, U0, dt, nsteps, slot);
 }
 
 int ph_batch_step(ph_batch* b, int nsteps) {

@@ -38,6 +38,20 @@ int node_geometry(int n, const std::vector<int>& ijk, const std::vector<double>&
                   double left, double right, double warp, std::vector<double>& xyz, std::vector<double>& metric,
                   const double* support = nullptr);
 
+// A solve's host-side set-up for a batch (operators, connectivity, geometry / metric terms),
+// computed without the batch, so that it can run on the thread that submits the solve.
+struct BatchPrep {
+    ph::OpTab ops{};
+    bool fr = false;
+    bool ready = false;
+    std::vector<int> nbr;
+    std::vector<double> metric;
+};
+int batch_prepare(const ph_mesh_desc* mesh, const ph_params* prm, BatchPrep& out);
+// ph_batch_admit with the set-up done beforehand (prep may be nullptr: done here)
+int batch_admit_prepared(ph_batch* b, const ph_mesh_desc* mesh, const ph_params* prm, const BatchPrep* prep,
+                         const double* U0, double dt, int nsteps, int* slot);
+
 // a curvilinear mesh: warped, or given by its mapping support points
 inline bool is_curvilinear(const ph_mesh_desc* mesh) {
     return mesh->warp != 0.0 || mesh->mapping_support_points != nullptr;

@@ -37,6 +37,7 @@ struct Job {
     std::vector<double> U;           // initial state, then the final state
     double dt = 0.0;
     int nsteps = 0;
+    BatchPrep prep;                  // host set-up, built on the submitting thread
     int state = PH_SOLVE_QUEUED;
     int rc = PH_OK;
     std::string error;
@@ -55,6 +56,7 @@ struct ph_server {
     ph_batch* batch = nullptr;
     int device = 0;
     int chunk = 16;
+    double admit_slice = 0.004;        // seconds of host time per pass spent admitting while solves run
     std::mutex mu;
     std::condition_variable work_cv;   // the worker waits here for submissions
     std::condition_variable done_cv;   // callers of ph_server_wait wait here
@@ -95,12 +97,17 @@ void ph_server::run() {
             }
             if (!queue.empty()) head = queue.front();
         }
-        // admission, FIFO; the batch is touched by this thread only
-        while (head) {
+        // admission, FIFO; the batch is touched by this thread only. While solves are resident it
+        // takes at most admit_slice of host time per pass (an admission builds the solve's
+        // geometry on the host), so the loop returns to queue steps before the GPU runs dry.
+        auto slice_end = Clock::now() + std::chrono::duration_cast<Clock::duration>(
+                                            std::chrono::duration<double>(admit_slice));
+        while (head && (resident.empty() || Clock::now() < slice_end)) {
             const double* u0 = head->U.data();
             if (!head->support.empty()) head->mesh.mapping_support_points = head->support.data();
             int slot = -1;
-            const int rc = ph_batch_admit(batch, &head->mesh, &head->prm, u0, head->dt, head->nsteps, &slot);
+            const int rc = batch_admit_prepared(batch, &head->mesh, &head->prm, &head->prep, u0, head->dt, head->nsteps,
+                                                &slot);
             std::unique_lock<std::mutex> lk(mu);
             if (rc == PH_ERR_NOMEM && !resident.empty()) {   // no room now: retry once solves retire
                 ++admissions_deferred;
@@ -116,6 +123,9 @@ void ph_server::run() {
             } else {
                 head->state = PH_SOLVE_RUNNING;
                 head->admitted = Clock::now();
+                if (resident.empty())   // the first resident solve opens the slice
+                    slice_end = head->admitted + std::chrono::duration_cast<Clock::duration>(
+                                                     std::chrono::duration<double>(admit_slice));
                 resident[slot] = head;
                 if ((int)resident.size() > max_resident) max_resident = (int)resident.size();
             }
@@ -160,14 +170,16 @@ void ph_server::run() {
 
 extern "C" {
 
-int ph_server_create(size_t hbm_budget_bytes, int precision, int chunk_steps, ph_server** out) {
+int ph_server_create(size_t hbm_budget_bytes, int precision, int chunk_steps, double admit_slice_s, ph_server** out) {
     if (!out) return fail(PH_ERR_INVALID, "null argument");
     *out = nullptr;
     if (chunk_steps < 1) return fail(PH_ERR_INVALID, "chunk_steps must be positive");
+    if (!(admit_slice_s >= 0.0)) return fail(PH_ERR_INVALID, "admit_slice_s must be >= 0");
     if (precision != PH_FP64 && precision != PH_FP32_RESIDUAL) return fail(PH_ERR_INVALID, "precision");
     if (hbm_budget_bytes == 0) return fail(PH_ERR_INVALID, "budget too small");
     ph_server* s = new ph_server();
     s->chunk = chunk_steps;
+    s->admit_slice = admit_slice_s;
     cudaGetDevice(&s->device);
     if (int rc = ph_batch_create(hbm_budget_bytes, precision, nullptr, &s->batch)) { delete s; return rc; }
     s->worker = std::thread([s] { s->run(); });
@@ -191,8 +203,11 @@ int ph_server_submit(ph_server* s, const ph_mesh_desc* mesh, const ph_params* pr
         const size_t ns = n / 5 * 3;   // [cell][3][(p+1)^3]
         j->support.assign(mesh->mapping_support_points, mesh->mapping_support_points + ns);
     }
-    j->mesh.mapping_support_points = nullptr;
+    j->mesh.mapping_support_points = j->support.empty() ? nullptr : j->support.data();
     j->submitted = Clock::now();
+    // the solve's geometry on this thread, not on the worker's (which keeps the GPU fed)
+    if (int rc = batch_prepare(&j->mesh, &j->prm, j->prep)) { delete j; return rc; }
+    j->mesh.mapping_support_points = nullptr;
     {
         std::lock_guard<std::mutex> lk(s->mu);
         if (s->stop) { delete j; return fail(PH_ERR_INVALID, "server is stopping"); }

@@ -344,10 +344,12 @@ class Server:
     """ph_server_*: a worker thread of the library runs the continuous-batching loop over its
     own batch; submissions return a ticket at once and may come from any thread."""
 
-    def __init__(self, budget_bytes: int, precision: int = _lib.PH_FP32_RESIDUAL, chunk: int = 16):
+    def __init__(self, budget_bytes: int, precision: int = _lib.PH_FP32_RESIDUAL, chunk: int = 16,
+                 admit_slice: float = 0.004):
         self.L = _lib.load()
         h = ctypes.c_void_p()
-        _lib.check(self.L.ph_server_create(ctypes.c_size_t(int(budget_bytes)), precision, chunk, ctypes.byref(h)))
+        _lib.check(self.L.ph_server_create(ctypes.c_size_t(int(budget_bytes)), precision, chunk, admit_slice,
+                                           ctypes.byref(h)))
         self._h = h
         self.precision = precision
 

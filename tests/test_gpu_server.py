@@ -31,9 +31,10 @@ def test_server_refuses_bad_arguments_without_a_gpu():
     import ctypes
     L = _lib.load()
     h = ctypes.c_void_p()
-    assert L.ph_server_create(ctypes.c_size_t(1 << 20), _lib.PH_FP64, 0, ctypes.byref(h)) == _lib.PH_ERR_INVALID
-    assert L.ph_server_create(ctypes.c_size_t(0), _lib.PH_FP64, 4, ctypes.byref(h)) == _lib.PH_ERR_INVALID
-    assert L.ph_server_create(ctypes.c_size_t(1 << 20), 7, 4, ctypes.byref(h)) == _lib.PH_ERR_INVALID
+    assert L.ph_server_create(ctypes.c_size_t(1 << 20), _lib.PH_FP64, 0, 0.004, ctypes.byref(h)) == _lib.PH_ERR_INVALID
+    assert L.ph_server_create(ctypes.c_size_t(0), _lib.PH_FP64, 4, 0.004, ctypes.byref(h)) == _lib.PH_ERR_INVALID
+    assert L.ph_server_create(ctypes.c_size_t(1 << 20), 7, 4, 0.004, ctypes.byref(h)) == _lib.PH_ERR_INVALID
+    assert L.ph_server_create(ctypes.c_size_t(1 << 20), _lib.PH_FP64, 4, -1.0, ctypes.byref(h)) == _lib.PH_ERR_INVALID
 
 
 def _alone(req):
