@@ -362,6 +362,33 @@ int ph_server_stats(ph_server* s, long long out[4]);
  * everything. */
 int ph_server_destroy(ph_server* s);
 
+/* ---- Snapshot matrix on the device and its POD basis (OnlinePOD::addSnapshot / computeBasis,
+ * src/reduced_order/pod_basis_online.cpp:28-89; fed by FlowSolver::run every
+ * output_snapshot_every_x_timesteps, src/flow_solver/flow_solver.cpp:110-120, :675-679, and by
+ * the snapshot solves of adaptive sampling, adaptive_sampling_base.cpp:249). The snapshots are
+ * the columns of an ndofs x capacity matrix resident on the device; a context's or a batch
+ * solve's state is appended by a device copy ordered after that solver's queued work. */
+typedef struct ph_snapshots ph_snapshots;
+int ph_snapshots_create(int64_t ndofs, int capacity, ph_snapshots** out);
+int ph_snapshots_destroy(ph_snapshots* s);
+/* appending to a full matrix doubles its capacity (PH_ERR_NOMEM when that allocation fails) */
+int ph_snapshots_add(ph_snapshots* s, const double* U, int where);
+int ph_snapshots_add_state(ph_snapshots* s, ph_ctx* ctx);            /* the context's current solution */
+int ph_snapshots_add_batch(ph_snapshots* s, ph_batch* b, int slot);  /* a batch solve's state */
+int ph_snapshots_count(const ph_snapshots* s, int* m);
+/* the matrix, column-major: S[j * ndofs + i] = DOF i of snapshot j */
+int ph_snapshots_get(ph_snapshots* s, double* S, int where);
+/* OnlinePOD::computeBasis: reference_state = the row mean (ndofs), the snapshots centred on it,
+ * and the thin SVD of the centred matrix: singular_values (m, descending) and basis (the left
+ * singular vectors, column-major ndofs x rank). By the method of snapshots: G = Sc^T Sc on the
+ * device (cuBLAS DSYRK), its eigenvectors on the host (Jacobi rotations), U = Sc V / sigma
+ * (cuBLAS DGEMM); a singular value below rel_tol x the largest is reported as 0 and its vector
+ * is not formed (*rank counts those kept). Each vector's entry of largest magnitude is positive.
+ * Output pointers may be NULL; where = PH_HOST or PH_DEVICE for reference_state and basis.
+ * Accuracy: sigma_k carries a relative error of about 1e-16 (sigma_1 / sigma_k)^2. */
+int ph_snapshots_pod(ph_snapshots* s, double rel_tol, double* reference_state, double* singular_values, double* basis,
+                     int where, int* rank);
+
 int ph_sync(ph_ctx* ctx);
 const char* ph_last_error(void);
 

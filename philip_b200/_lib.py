@@ -33,7 +33,9 @@ EXPORTED = ["ph_ctx_create", "ph_ctx_destroy", "ph_ndofs", "ph_cell_ijk", "ph_se
             "ph_batch_launches", "ph_mesh_node_xyz", "ph_rk_error_norm", "ph_last_error",
             "ph_integrated_quantities", "ph_run", "ph_rk_relaxation", "ph_ctx_create_slab", "ph_set_halo_exchange",
             "ph_slab_connectivity", "ph_server_create", "ph_server_submit", "ph_server_poll", "ph_server_wait",
-            "ph_server_result", "ph_server_stats", "ph_server_destroy"]
+            "ph_server_result", "ph_server_stats", "ph_server_destroy", "ph_snapshots_create", "ph_snapshots_destroy",
+            "ph_snapshots_add", "ph_snapshots_add_state", "ph_snapshots_add_batch", "ph_snapshots_count",
+            "ph_snapshots_get", "ph_snapshots_pod"]
 PH_SOLVE_QUEUED, PH_SOLVE_RUNNING, PH_SOLVE_DONE, PH_SOLVE_FAILED = 0, 1, 2, 3
 
 # ph_halo_fn(user, what, phase, send_lo, send_hi, recv_lo, recv_hi, bytes, cuda_stream)
@@ -135,6 +137,14 @@ def load(build_if_missing: bool = False):
     L.ph_server_result.argtypes = [vp, ll, dp, ctypes.POINTER(ctypes.c_uint32), dp]
     L.ph_server_stats.argtypes = [vp, ctypes.POINTER(ll)]
     L.ph_server_destroy.argtypes = [vp]
+    L.ph_snapshots_create.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.POINTER(vp)]
+    L.ph_snapshots_destroy.argtypes = [vp]
+    L.ph_snapshots_add.argtypes = [vp, vp, ctypes.c_int]
+    L.ph_snapshots_add_state.argtypes = [vp, vp]
+    L.ph_snapshots_add_batch.argtypes = [vp, vp, ctypes.c_int]
+    L.ph_snapshots_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
+    L.ph_snapshots_get.argtypes = [vp, vp, ctypes.c_int]
+    L.ph_snapshots_pod.argtypes = [vp, ctypes.c_double, vp, vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.ph_last_error.restype = ctypes.c_char_p
     _lib = L
     return L

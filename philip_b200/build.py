@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libphilip_b200.so")
 N1_RANGE = range(2, 8)          # p = 1 .. 6
-HOST_UNITS = ("ph_capi", "ph_batch", "ph_server")   # C-ABI: single-solve context, batch of solves, server
+HOST_UNITS = ("ph_capi", "ph_batch", "ph_server", "ph_snapshots")   # C-ABI units
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -75,7 +75,8 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
     objs = [os.path.join(BUILD, f"ph_inst_{n1}.o") for n1 in N1_RANGE] + \
         [os.path.join(BUILD, unit + ".o") for unit in HOST_UNITS]
     tmp = LIB + ".tmp"
-    _run([nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp, *objs, "-lcudart"], verbose)
+    _run([nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp, *objs, "-lcudart", "-lcublas"],
+         verbose)
     os.replace(tmp, LIB)
     if ptxas_info:
         sys.stdout.write("\n".join(logs))

@@ -531,6 +531,12 @@ int ph_host::batch_admit_prepared(ph_batch* b, const ph_mesh_desc* mesh, const p
     return PH_OK;
 }
 
+int ph_host::batch_state(ph_batch* b, int slot, const double** d, size_t* n, cudaStream_t* stream) {
+    if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].used) return fail(PH_ERR_INVALID, "bad slot");
+    *d = b->slots[slot].B.sol; *n = b->slots[slot].ndofs; *stream = b->stream;
+    return PH_OK;
+}
+
 extern "C" {
 
 int ph_batch_admit(ph_batch* b, const ph_mesh_desc* mesh, const ph_params* prm, const double* U0, double dt,

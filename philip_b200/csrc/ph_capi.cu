@@ -1121,6 +1121,16 @@ int ph_ctx_destroy(ph_ctx* c) {
 
 int64_t ph_ndofs(const ph_ctx* c) { return c ? (int64_t)c->ndofs : -1; }
 
+}  // extern "C"
+
+int ph_host::ctx_state(ph_ctx* c, const double** d, size_t* n, cudaStream_t* stream) {
+    if (!c) return fail(PH_ERR_INVALID, "null argument");
+    *d = c->d_sol; *n = c->ndofs; *stream = c->stream;
+    return PH_OK;
+}
+
+extern "C" {
+
 int ph_node_xyz(const ph_ctx* c, double* xyz) {
     if (!c || !xyz) return fail(PH_ERR_INVALID, "null argument");
     std::memcpy(xyz, c->xyz.data(), c->xyz.size() * sizeof(double));

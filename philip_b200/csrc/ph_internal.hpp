@@ -3,6 +3,8 @@
 // periodic-cube connectivity, node geometry / curvilinear metric terms and the RK
 // stage arguments. Not part of the C-ABI.
 #pragma once
+#include <cuda_runtime.h>
+
 #include <string>
 #include <vector>
 
@@ -51,6 +53,11 @@ int batch_prepare(const ph_mesh_desc* mesh, const ph_params* prm, BatchPrep& out
 // ph_batch_admit with the set-up done beforehand (prep may be nullptr: done here)
 int batch_admit_prepared(ph_batch* b, const ph_mesh_desc* mesh, const ph_params* prm, const BatchPrep* prep,
                          const double* U0, double dt, int nsteps, int* slot);
+
+// Device state of a context (its current solution, ndofs doubles) and the stream it is ordered on;
+// of a batch slot likewise (the batch stream). For the snapshot matrix's device-to-device copies.
+int ctx_state(ph_ctx* c, const double** d, size_t* n, cudaStream_t* stream);
+int batch_state(ph_batch* b, int slot, const double** d, size_t* n, cudaStream_t* stream);
 
 // a curvilinear mesh: warped, or given by its mapping support points
 inline bool is_curvilinear(const ph_mesh_desc* mesh) {

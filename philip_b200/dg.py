@@ -390,6 +390,13 @@ class FlowSolver:
         self.dg.solution = conservative_state(self.dg, prim)
         self.unsteady_data = []
         self.restart_dt = None
+        # time POD (flow_solver.cpp:110-120): the snapshot matrix stays on the device
+        self.snapshot_every = int(parameters.get("reduced order/output_snapshot_every_x_timesteps"))
+        self.time_pod = None
+        if self.snapshot_every != 0:
+            from .pod import OnlinePOD
+            self.time_pod = OnlinePOD(self.dg.n_dofs, 16)
+            self.time_pod.addSnapshot(self.dg)
         if parameters.get("flow_solver/restart_computation_from_file").lower() == "true":
             self._restart_from_file()
 
@@ -512,6 +519,7 @@ class FlowSolver:
             self.unsteady_data.append((self.ode_solver.current_time, *self.dg.integrals()))
         if (not adaptive and not error_adaptive and not write_restart and record_every > 0
                 and not self.parameters.use_relaxation_runge_kutta and self.dg.slab is None
+                and self.time_pod is None
                 and self.ode_solver.current_iteration % record_every == 0):
             # the whole steps of dt run on the device with the records reduced there (ph_run);
             # the count follows the loop below step by step, so the clock is the same
@@ -534,6 +542,8 @@ class FlowSolver:
                         self._grid_spacing() / q[3]
             if error_adaptive:   # flow_solver.cpp:603-607
                 dt = self.ode_solver.get_automatic_error_adaptive_step_size(step)
+            if self.time_pod is not None and self.ode_solver.current_iteration % self.snapshot_every == 0:
+                self.time_pod.addSnapshot(self.dg)   # flow_solver.cpp:675-679, a device copy
             if write_restart:   # flow_solver.cpp:605-632: every dt time interval, or every x steps
                 if every_dt > 0.0:
                     if self.ode_solver.current_time >= next_restart_time:
@@ -542,4 +552,8 @@ class FlowSolver:
                         next_restart_time += every_dt
                 elif self.ode_solver.current_iteration % every_x == 0:
                     self.output_restart_files(self.ode_solver.current_iteration // every_x, dt)
+        if self.time_pod is not None:   # flow_solver.cpp:683-688
+            from .pod import write_snapshot_matrix
+            write_snapshot_matrix(f"solution_snapshots_iteration_{self.ode_solver.current_iteration}.txt",
+                                  self.time_pod.getSnapshotMatrix())
         return 0

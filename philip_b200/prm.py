@@ -56,6 +56,7 @@ DEFAULTS = {
     "ODE solver/initial_desired_time_for_output_solution_every_dt_time_intervals": "0.0",
     "flow_solver/unsteady_data_table_filename": "unsteady_data_table",
     "flow_solver/dipole_wall_collision/do_compute_angular_momentum": "false",
+    "reduced order/output_snapshot_every_x_timesteps": "0",
     "flow_solver/output_restart_files": "false", "flow_solver/restart_computation_from_file": "false",
     "flow_solver/restart_files_directory_name": ".", "flow_solver/restart_file_index": "1",
     "flow_solver/output_restart_files_every_x_steps": "1",
