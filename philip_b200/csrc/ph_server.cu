@@ -136,8 +136,25 @@ void ph_server::run() {
         ph_batch_active(batch, &active);
         if (active > 0) {
             long long t = 0;
-            if (ph_batch_step(batch, chunk) == PH_OK && ph_batch_fence(batch, &t) == PH_OK) fences.push_back(t);
-            if (fences.size() > 2) { ph_batch_fence_wait(batch, fences.front()); fences.pop_front(); }
+            int rc = ph_batch_step(batch, chunk);
+            if (rc == PH_OK) rc = ph_batch_fence(batch, &t);
+            if (rc == PH_OK) fences.push_back(t);
+            if (rc == PH_OK && fences.size() > 2) { rc = ph_batch_fence_wait(batch, fences.front()); fences.pop_front(); }
+            if (rc != PH_OK) {   // the batch cannot advance: every resident solve fails with its error
+                const std::string why = ph_last_error();
+                for (auto& kv : resident) {
+                    ph_batch_release(batch, kv.first);
+                    std::lock_guard<std::mutex> lk(mu);
+                    kv.second->rc = rc;
+                    kv.second->error = "stepping failed: " + why;
+                    kv.second->state = PH_SOLVE_FAILED;
+                    kv.second->completed = Clock::now();
+                }
+                resident.clear();
+                fences.clear();
+                done_cv.notify_all();
+                continue;
+            }
             long long n = 0;
             ph_batch_launches(batch, &n);
             std::lock_guard<std::mutex> lk(mu);
