@@ -629,6 +629,9 @@ def main():
         ev0.record(stream)
         _lib.check(L.ph_rk_step(h, dt, args.steps))
         ev1.record(stream)
+        # wait inside the library (ctypes releases the interpreter lock there, so the clock
+        # sampler thread keeps sampling while the GPU runs), then on the device as a whole
+        _lib.check(L.ph_sync(h))
         torch.cuda.synchronize()
     barrier()
     ms = ev0.elapsed_time(ev1)
