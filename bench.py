@@ -717,7 +717,9 @@ def main():
                                        "and wave speed reduced on the device every 10 steps"}
             if not slab else {"skipped": "slab contexts step through ph_rk_step"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
+                         "frac": achieved / peak,
+                         "traffic": traffic["bytes_per_launch"] if traffic else None,   # DRAM bytes per launch
+                         "traffic_detail": traffic,
                          "kernel": "residual_kernel (stage: residual + mass inverse + RK update)",
                          "kernel_ms": stage_ms, "aux_kernel_ms": aux_ms,
                          "alg_bytes_per_dof": bpd, "peak_source": peak_src,
