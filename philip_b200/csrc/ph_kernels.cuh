@@ -28,7 +28,7 @@
 // resident CTAs per SM asked of the compiler (register budget) for the p = 3 and p = 5
 // stage tiles, FP64 and FP32 (measured choices; see the Layout)
 #ifndef PH_P5_MINB
-#define PH_P5_MINB 4
+#define PH_P5_MINB 3
 #endif
 #ifndef PH_P5_MINB_F32
 #define PH_P5_MINB_F32 6
@@ -282,9 +282,11 @@ __device__ __forceinline__ void face_item(const Cst<R>& cst, int tp, int cf, int
     for (int s = 0; s < 5; ++s) tr[s * NF + fn] = term[s] * inv_wend;
 }
 
-// unroll count of the volume phase's partner loop (k = 1 .. N1/2)
+// unroll count of the volume phase's partner loop (k = 1 .. N1/2): unrolled where B200 timings
+// favour it (FP32 at every order; FP64 at p = 3 and p = 5, the latter with 3 CTAs per SM), rolled
+// at the other FP64 orders, which were not measured unrolled
 template <typename R, int N1> __host__ __device__ constexpr int PAIR_UNROLL() {
-    return sizeof(R) == 4 ? N1 / 2 : 1;
+    return (sizeof(R) == 4 || N1 == 4 || N1 == 6) ? N1 / 2 : 1;
 }
 
 // Phase 4 for direction d: warp segments of N1 lanes own 1-D lines along d. The
@@ -353,9 +355,10 @@ __device__ __forceinline__ void volume_dir(int d, const Cst<R>& cst, int tp, con
         }
 #else
         const int segbase = seg * N1;
-        // the partner loop is unrolled in FP32 (the independent pair fluxes interleave: the
-        // p = 5 stage kernel takes 0.276 ms instead of 0.294 ms on B200) and kept rolled in FP64
-        // (0.533 ms instead of 0.515: the unrolled FP64 body spills at the 64-register bound)
+        // the partner loop is unrolled (PAIR_UNROLL): the independent pair fluxes interleave.
+        // At p = 5 on B200 the FP32 stage kernel takes 0.276 ms instead of 0.294 ms, the FP64
+        // one 0.496 ms instead of 0.515 with 3 CTAs per SM (at 4 CTAs per SM the unrolled FP64
+        // body spills at the 64-register bound and takes 0.533 ms)
 #pragma unroll(PAIR_UNROLL<R, N1>())
         for (int k = 1; k <= N1 / 2; ++k) {
             const int jp = pos + k < N1 ? pos + k : pos + k - N1;      // (pos + k) mod N1
