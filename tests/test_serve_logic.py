@@ -99,3 +99,54 @@ def test_fifo_admission_waits_for_room():
     assert done[(6, 5)].admitted >= done[(6, 30)].done
     assert done[(1, 5)].admitted >= done[(6, 5)].admitted
     assert stats.admissions_deferred > 0
+
+
+class FakeNativeServer:
+    """Stand-in for serve.Server (the native loop): every solve is admitted at once and done
+    `steps * 1 ms` after its submission; records the order and times of the submissions."""
+
+    def __init__(self):
+        import time
+        self.t0 = time.perf_counter()
+        self.jobs, self.order = {}, []
+
+    def submit_request(self, req):
+        import time
+        t = len(self.jobs) + 1
+        _, _, nsteps = req.prepare()
+        self.jobs[t] = (req, time.perf_counter() - self.t0, nsteps)
+        self.order.append(t)
+        return t
+
+    def wait(self, ticket, timeout=3600.0):
+        return 2
+
+    def result(self, ticket, ndofs):
+        req, sub, nsteps = self.jobs.pop(ticket)
+        return np.zeros(ndofs), 0, (0.0, 1e-3 * nsteps)
+
+    def stats(self):
+        return {"queued": 0, "admissions_deferred": 0, "max_resident": 1, "launches": 0}
+
+
+class _Req:
+    def __init__(self, nsteps):
+        self.nsteps, self.ndofs = nsteps, 4
+
+    def prepare(self):
+        return None, 0.1, self.nsteps
+
+
+def test_native_serving_loop_accounting():
+    from philip_b200.serve import serve_native
+    arrivals = [(0.0, _Req(5)), (0.02, _Req(3)), (0.01, _Req(7))]
+    srv = FakeNativeServer()
+    stats = serve_native(srv, arrivals)
+    assert len(stats.completed) == 3 and not srv.jobs           # every ticket collected once
+    # submitted in arrival order, each no earlier than its arrival time
+    assert [c.request.nsteps for c in sorted(stats.completed, key=lambda c: c.admitted)] == [5, 7, 3]
+    for c in stats.completed:
+        assert c.admitted >= c.arrival - 1e-9
+        assert abs((c.done - c.admitted) - 1e-3 * c.steps) < 1e-12
+        assert c.latency >= 1e-3 * c.steps - 1e-9
+    assert stats.makespan == max(c.done for c in stats.completed)
