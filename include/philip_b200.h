@@ -208,9 +208,15 @@ int ph_run(ph_ctx* ctx, double dt, int nsteps, int record_every, double* rows);
 int ph_status(ph_ctx* ctx, uint32_t* flags);
 
 /* Measurement hooks (no counterpart in the reference, which times with dealii::Timer,
- * src/flow_solver/flow_solver.cpp:690-711). With timing enabled every kernel launch is
- * bracketed by CUDA events on the context stream and the stream is synchronised after
- * it. out[0..5] = {stage-kernel ms, stage launches, auxiliary-kernel ms, auxiliary
+ * src/flow_solver/flow_solver.cpp:690-711). enable = 1: every kernel launch is bracketed
+ * by CUDA events on the context stream and the stream is synchronised after it (steps
+ * launch directly). enable = 2: the captured RK step that ph_rk_step replays carries an
+ * event-record node before its first kernel and after each kernel, and every replay
+ * records a fresh set of events, so the kernels are timed inside the replayed steps
+ * themselves (each duration includes the launch gap before the kernel); changing to or
+ * from mode 2 drops the captured step, which the next multi-step ph_rk_step captures
+ * again (its first step runs directly and is not timed). Every call resets the sums.
+ * out[0..5] = {stage-kernel ms, stage launches, auxiliary-kernel ms, auxiliary
  * launches, other ms, other launches}, out[6] = kernel launches counted since the last
  * ph_set_timing call (counted with timing enabled or not). */
 int ph_set_timing(ph_ctx* ctx, int enable);
@@ -271,12 +277,17 @@ int ph_slab_connectivity(int n, int z_first, int z_count, int32_t* ijk, int32_t*
  * device, or a framework that owns all device memory). U and R need no initialisation
  * beyond U's values. Its scratch lives in fixed file-scope device arrays: at most 32768 cells, and
  * for Navier-Stokes at most cells x (4 (p+1)^3 + 24 (p+1)^2) <= 4 Mi doubles of viscous-term scratch
- * (32 MiB); larger meshes are rejected with PH_ERR_INVALID. The first call on a device
+ * (32 MiB); larger meshes are rejected with PH_ERR_INVALID. The mesh and parameters pass the
+ * checks of ph_ctx_create before anything is launched. The first call on a device
  * resolves the arrays' device addresses and should come before any stream capture.
  * Every call shares the same arrays: calls that overlap on the GPU (other streams or
  * threads) race, so serialise them. Asynchronous on cuda_stream (NULL = default). */
 int ph_residual_noalloc(const ph_mesh_desc* mesh, const ph_params* prm, const double* U, double* R,
                         void* cuda_stream);
+/* The status word of the last ph_residual_noalloc on this device (bit 0: a non-positive density
+ * or pressure was met; the residual then holds the non-physical branch's values, as ph_status
+ * reports for a context). Each ph_residual_noalloc clears it first. Waits for cuda_stream. */
+int ph_residual_noalloc_status(void* cuda_stream, uint32_t* flags);
 
 /* Self-test of the quotient used inside the flux kernels against IEEE division on n
  * pseudo-random operand pairs; out[0] = max relative error in FP64, out[1] in FP32.

@@ -26,7 +26,7 @@ ERRORS = {1: "invalid argument", 2: "unsupported configuration", 3: "CUDA error"
 
 EXPORTED = ["ph_ctx_create", "ph_ctx_destroy", "ph_ndofs", "ph_cell_ijk", "ph_set_state", "ph_get_state",
             "ph_residual", "ph_apply_inverse_mass", "ph_rk_step", "ph_integrals", "ph_status", "ph_sync",
-            "ph_set_timing", "ph_get_timing", "ph_quotient_selftest", "ph_residual_noalloc", "ph_node_xyz",
+            "ph_set_timing", "ph_get_timing", "ph_quotient_selftest", "ph_residual_noalloc", "ph_residual_noalloc_status", "ph_node_xyz",
             "ph_batch_create", "ph_batch_destroy", "ph_batch_bytes", "ph_batch_admit", "ph_batch_step",
             "ph_batch_progress", "ph_batch_active", "ph_batch_get_state", "ph_batch_status", "ph_batch_release",
             "ph_batch_poll", "ph_batch_fence", "ph_batch_fence_wait", "ph_batch_autotune", "ph_batch_set_variant",
@@ -123,6 +123,7 @@ def load(build_if_missing: bool = False):
     L.ph_rk_error_norm.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     L.ph_node_xyz.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     L.ph_residual_noalloc.argtypes = [ctypes.POINTER(PhMeshDesc), ctypes.POINTER(PhParams), vp, vp, vp]
+    L.ph_residual_noalloc_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32)]
     L.ph_ctx_create_slab.argtypes = [ctypes.POINTER(PhMeshDesc), ctypes.POINTER(PhParams), ctypes.c_int, ctypes.c_int,
                                      vp, ctypes.POINTER(vp)]
     L.ph_set_halo_exchange.argtypes = [vp, HALO_FN, vp]

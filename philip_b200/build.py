@@ -75,7 +75,7 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
     objs = [os.path.join(BUILD, f"ph_inst_{n1}.o") for n1 in N1_RANGE] + \
         [os.path.join(BUILD, unit + ".o") for unit in HOST_UNITS]
     tmp = LIB + ".tmp"
-    _run([nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp, *objs, "-lcudart", "-lcublas"],
+    _run([nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp, *objs, "-lcudart", "-lcublas", "-ldl"],
          verbose)
     os.replace(tmp, LIB)
     if ptxas_info:

@@ -333,7 +333,7 @@ int rebuild(ph_batch* b) {
 }
 
 int check_batch_params(const ph_batch* b, const ph_mesh_desc* mesh, const ph_params* prm) {
-    if (mesh->n_cells_per_direction < 1 || !(mesh->right > mesh->left)) return fail(PH_ERR_INVALID, "bad mesh");
+    if (int rc = check_mesh(mesh)) return rc;
     if (const char* why = unsupported_reason(mesh, prm)) return fail(PH_ERR_UNSUPPORTED, why);
     if (prm->pde_type != 0 || !prm->use_split_form)
         return fail(PH_ERR_UNSUPPORTED, "a batch takes split-form Euler solves");
@@ -657,7 +657,7 @@ int ph_batch_fence_wait(ph_batch* b, long long ticket) {
 int ph_mesh_node_xyz(const ph_mesh_desc* mesh, int poly_degree, double* xyz) {
     if (!mesh || !xyz) return fail(PH_ERR_INVALID, "null argument");
     if (poly_degree < 1 || poly_degree > 6) return fail(PH_ERR_UNSUPPORTED, "poly_degree must be 1..6");
-    if (mesh->n_cells_per_direction < 1 || !(mesh->right > mesh->left)) return fail(PH_ERR_INVALID, "bad mesh");
+    if (int rc = check_mesh(mesh)) return rc;
     ph_params prm{};
     prm.poly_degree = poly_degree;
     ph::OpTab ops;

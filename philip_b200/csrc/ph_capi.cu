@@ -1,13 +1,16 @@
 // C-ABI of the B200 strong-form DG/FR residual and explicit RK stage: context set-up
 // (host index maps, 1-D operators, device buffers) and stage orchestration.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <initializer_list>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -250,6 +253,26 @@ bool curvilinear_cell(const std::vector<double>& x, const std::vector<double>& D
     return true;
 }
 
+
+int check_mesh(const ph_mesh_desc* mesh) {
+    const int n = mesh->n_cells_per_direction;
+    if (n < 1 || !(mesh->right > mesh->left)) return fail(PH_ERR_INVALID, "bad mesh");
+    if (mesh->cell_order < 0 || mesh->cell_order > 2) return fail(PH_ERR_INVALID, "cell_order must be 0, 1 or 2");
+    // the recursive-children order exists only for hyper_cube + refine_global: n = 2^levels
+    if (mesh->cell_order == 2 && (n & (n - 1)) != 0)
+        return fail(PH_ERR_INVALID, "cell_order 2 (recursive children) needs n_cells_per_direction a power of two");
+    return PH_OK;
+}
+
+int check_param_ranges(const ph_params* prm) {
+    if (prm->pde_type < 0 || prm->pde_type > 1 || prm->two_point_num_flux_type < 0 || prm->two_point_num_flux_type > 3 ||
+        prm->conv_num_flux < 0 || prm->conv_num_flux > 5 || prm->diss_num_flux < 0 || prm->diss_num_flux > 2 ||
+        prm->runge_kutta_method < 0 || prm->runge_kutta_method > 10 ||
+        (prm->runge_kutta_method >= 4 && prm->runge_kutta_method <= 6) || prm->precision < 0 || prm->precision > 1 ||
+        prm->flux_nodes_type < 0 || prm->flux_nodes_type > 1)
+        return fail(PH_ERR_INVALID, "parameter out of range");
+    return PH_OK;
+}
 
 const char* unsupported_reason(const ph_mesh_desc* mesh, const ph_params* prm) {
     if (prm->flux_nodes_type != 1 || prm->overintegration != 0)
@@ -655,15 +678,24 @@ struct ph_ctx {
     double rrk_gamma = 1.0, rrk_elapsed = 0.0;
     std::vector<double> h_ent;
     std::vector<double> h_partial;
-    // optional per-kernel timing (CUDA events on the context stream)
-    bool timing = false;
+    // optional per-kernel timing: 1 = CUDA events around every direct launch, the stream
+    // synchronised after each; 2 = event-record nodes between the kernels of the captured
+    // RK step, a fresh set of events for every replay (the replays themselves are timed)
+    int timing = 0;
     double t_ms[3] = {0, 0, 0};      // residual/stage kernel, auxiliary kernel, other
     long long t_n[3] = {0, 0, 0};
     long long launches = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool capturing = false;                        // inside capture_step_graph
+    std::vector<cudaEvent_t> tcap;                 // mode 2: events recorded at capture, kernels + 1
+    std::vector<int> tcls;                         // mode 2: class of kernel j of the step
+    std::vector<cudaGraphNode_t> tnodes;           // mode 2: the event-record node of tcap[j]
+    std::vector<std::vector<cudaEvent_t>> tpool;   // mode 2: the events of replay r
+    size_t treplays = 0;                           // mode 2: replays since the last reset
     // one RK step captured as a CUDA graph, replayed by ph_rk_step while dt stays the same
     // (only on a caller-given stream: the legacy default stream cannot be captured)
     cudaGraphExec_t step_graph = nullptr;
+    cudaGraph_t step_graph_src = nullptr;          // mode 2: kept for its node handles
     double step_graph_dt = 0.0;
     int step_graph_launches = 0;
     // ph_run: device table of integrals rows, its row counter, and the captured graph of one
@@ -696,12 +728,38 @@ struct ph_ctx {
 
 namespace {
 
+// NVTX range for the profilers' timelines (a no-op unless a tool is attached): one per RK
+// step, per stage and per kernel launch
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
+constexpr size_t TIMED_KERNELS_PER_STEP = 64;
+
+void drop_step_graph(ph_ctx* c) {
+    if (c->step_graph) { cudaGraphExecDestroy(c->step_graph); c->step_graph = nullptr; }
+    if (c->step_graph_src) { cudaGraphDestroy(c->step_graph_src); c->step_graph_src = nullptr; }
+    c->tnodes.clear();
+}
+
 void timer_begin(ph_ctx* c) {
-    if (c->timing) cudaEventRecord(c->ev0, c->stream);
+    if (c->timing == 1) cudaEventRecord(c->ev0, c->stream);
+    else if (c->timing == 2 && c->capturing && c->tcls.empty())   // an event-record node of the graph
+        cudaEventRecordWithFlags(c->tcap[0], c->stream, cudaEventRecordExternal);
 }
 void timer_end(ph_ctx* c, int cls) {
     ++c->launches;
-    if (!c->timing) return;
+    if (c->timing == 2) {
+        if (c->capturing && c->tcls.size() + 1 < c->tcap.size()) {
+            c->tcls.push_back(cls);
+            cudaEventRecordWithFlags(c->tcap[c->tcls.size()], c->stream, cudaEventRecordExternal);
+        }
+        return;
+    }
+    if (c->timing != 1) return;
     cudaEventRecord(c->ev1, c->stream);
     cudaEventSynchronize(c->ev1);
     float ms = 0.f;
@@ -711,6 +769,7 @@ void timer_end(ph_ctx* c, int cls) {
 }
 
 int dispatch_stage(ph_ctx* c, const ph::StageArgs& a) {
+    NvtxRange nvtx("stage kernel");
     cudaError_t e;
     timer_begin(c);
     switch (c->N1) {
@@ -728,6 +787,7 @@ int dispatch_stage(ph_ctx* c, const ph::StageArgs& a) {
 }
 
 int dispatch_aux(ph_ctx* c, const double* U, int cell_begin, int cell_end) {
+    NvtxRange nvtx("auxiliary kernel");
     cudaError_t e;
     const double inv_h = 1.0 / c->h;
     timer_begin(c);
@@ -873,7 +933,7 @@ int eval_residual(ph_ctx* c, const double* in, ph::StageArgs a) {
     }
     const int lo = c->lo_end, hi = c->hi_begin, nc = c->nc;
     // the interior runs concurrently unless there is none or every launch is being timed
-    const bool fork = lo < hi && !c->timing;
+    const bool fork = lo < hi && c->timing != 1;
     if (int rc = halo_copy(c, PH_HALO_STATE, true, in)) return rc;
     if (int rc = halo_call(c, PH_HALO_STATE, PH_HALO_BEGIN)) return rc;
     if (lo < hi) {
@@ -914,12 +974,8 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
                           ph_ctx** out) {
     if (!mesh || !prm || !out) return fail(PH_ERR_INVALID, "null argument");
     *out = nullptr;
-    if (mesh->n_cells_per_direction < 1 || !(mesh->right > mesh->left)) return fail(PH_ERR_INVALID, "bad mesh");
-    if (prm->pde_type < 0 || prm->pde_type > 1 || prm->two_point_num_flux_type < 0 || prm->two_point_num_flux_type > 3 ||
-        prm->conv_num_flux < 0 || prm->conv_num_flux > 5 || prm->diss_num_flux < 0 || prm->diss_num_flux > 2 ||
-        prm->runge_kutta_method < 0 || prm->runge_kutta_method > 10 ||
-        (prm->runge_kutta_method >= 4 && prm->runge_kutta_method <= 6))
-        return fail(PH_ERR_INVALID, "parameter out of range");
+    if (int rc = check_mesh(mesh)) return rc;
+    if (int rc = check_param_ranges(prm)) return rc;
     if (const char* why = unsupported_reason(mesh, prm)) return fail(PH_ERR_UNSUPPORTED, why);
     const bool ec = prm->conv_num_flux >= 3;
     if (ec && !prm->use_split_form)
@@ -1103,9 +1159,11 @@ int ph_ctx_destroy(ph_ctx* c) {
     if (!c) return PH_OK;
     if (c->step_graph || c->run_graph) {
         if (c->stream) cudaStreamSynchronize(c->stream);
-        if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+        drop_step_graph(c);
         if (c->run_graph) cudaGraphExecDestroy(c->run_graph);
     }
+    for (cudaEvent_t ev : c->tcap) if (ev) cudaEventDestroy(ev);
+    for (auto& set : c->tpool) for (cudaEvent_t ev : set) if (ev) cudaEventDestroy(ev);
     void* ptrs[] = {c->d_nbr, c->d_ops, c->d_itab, c->d_sol, c->d_stA, c->d_stB, c->d_acc, c->d_carry,
                     c->d_fv, c->d_comp, c->d_tmpA, c->d_tmpB, c->d_partial, c->d_status, c->d_metric, c->d_xnode, c->d_origin, c->d_err,
                     c->d_table, c->d_counter, c->d_ent, c->d_ent_cell, c->d_halo};
@@ -1168,6 +1226,7 @@ static int ensure_tmp(ph_ctx* c) {
 
 int ph_residual(ph_ctx* c, const double* U, double* R, int where) {
     if (!c || !U || !R) return fail(PH_ERR_INVALID, "null argument");
+    NvtxRange nvtx("ph_residual");
     const double* dU = U;
     double* dR = R;
     if (where == PH_HOST) {
@@ -1221,11 +1280,16 @@ int ph_apply_inverse_mass(ph_ctx* c, const double* R, double* out, int where) {
 // stage i reads its stage state, computes k_i = M^{-1} R and, in the same kernel,
 // updates the running sum and writes the next stage state.
 static int rk_one_step(ph_ctx* c, double dt) {
+    static const char* const kStage[] = {"RK stage 0", "RK stage 1", "RK stage 2", "RK stage 3", "RK stage 4",
+                                         "RK stage 5", "RK stage 6", "RK stage 7", "RK stage 8", "RK stage 9",
+                                         "RK stage 10"};
+    NvtxRange nvtx("RK step");
     const int ns = c->ns;
     const RkBuffers B{c->d_sol, c->d_stA, c->d_stB, c->d_acc, c->d_carry, c->d_comp};
     if (c->lowstorage) {   // LowStorageRungeKuttaODESolver: ns stages (+ the FSAL evaluation of 3S*+)
         const int last = c->ls.plus ? ns : ns - 1;
         for (int i = 0; i <= last; ++i) {
+            NvtxRange stage(kStage[i < 10 ? i : 10]);
             ph::StageArgs a = base_args(c, nullptr);
             const double* in = lsrk_stage_args(a, B, i, c->ls, dt, c->prm.rk_atol, c->prm.rk_rtol, c->d_err);
             if (int rc = eval_residual(c, in, a)) return rc;
@@ -1233,6 +1297,7 @@ static int rk_one_step(ph_ctx* c, double dt) {
         return PH_OK;
     }
     for (int i = 0; i < ns; ++i) {
+        NvtxRange stage(kStage[i]);
         const double* in = rk_stage_input(B, i);
         ph::StageArgs a = base_args(c, in);
         rk_stage_args(a, B, i, ns, c->A, c->b, dt, c->fp32);
@@ -1372,21 +1437,50 @@ static int rrk_one_step(ph_ctx* c, double dt) {
 }
 
 // Capture one RK step (all stages, auxiliary kernels included) as a graph for this dt.
+// Timing mode 2: the event-record nodes of the captured step, in kernel order (matched to the
+// capture events they record).
+static int find_timing_nodes(ph_ctx* c, cudaGraph_t g) {
+    size_t n = 0;
+    PH_CUDA(cudaGraphGetNodes(g, nullptr, &n));
+    std::vector<cudaGraphNode_t> nodes(n);
+    PH_CUDA(cudaGraphGetNodes(g, nodes.data(), &n));
+    c->tnodes.assign(c->tcls.size() + 1, nullptr);
+    for (cudaGraphNode_t node : nodes) {
+        cudaGraphNodeType type;
+        PH_CUDA(cudaGraphNodeGetType(node, &type));
+        if (type != cudaGraphNodeTypeEventRecord) continue;
+        cudaEvent_t ev = nullptr;
+        PH_CUDA(cudaGraphEventRecordNodeGetEvent(node, &ev));
+        for (size_t j = 0; j < c->tnodes.size(); ++j)
+            if (c->tcap[j] == ev) c->tnodes[j] = node;
+    }
+    for (cudaGraphNode_t node : c->tnodes)
+        if (!node) return fail(PH_ERR_CUDA, "step capture: a timing event node is missing");
+    return PH_OK;
+}
+
 static int capture_step_graph(ph_ctx* c, double dt) {
-    if (c->step_graph) { cudaGraphExecDestroy(c->step_graph); c->step_graph = nullptr; }
+    drop_step_graph(c);
     const long long before = c->launches;
     cudaGraph_t g = nullptr;
+    c->tcls.clear();
     PH_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    c->capturing = true;
     const int rc = rk_one_step(c, dt);
+    c->capturing = false;
     const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
     if (rc || e != cudaSuccess) {
         if (g) cudaGraphDestroy(g);
         c->launches = before;
         return rc ? rc : fail(PH_ERR_CUDA, std::string("step capture: ") + cudaGetErrorString(e));
     }
+    if (c->timing == 2) {
+        if (int rc2 = find_timing_nodes(c, g)) { cudaGraphDestroy(g); return rc2; }
+    }
     const cudaError_t e2 = cudaGraphInstantiate(&c->step_graph, g, 0);
-    cudaGraphDestroy(g);
-    if (e2 != cudaSuccess) { c->step_graph = nullptr; return fail(PH_ERR_CUDA, cudaGetErrorString(e2)); }
+    if (c->timing == 2) c->step_graph_src = g;
+    else cudaGraphDestroy(g);
+    if (e2 != cudaSuccess) { c->step_graph = nullptr; drop_step_graph(c); return fail(PH_ERR_CUDA, cudaGetErrorString(e2)); }
     c->step_graph_launches = (int)(c->launches - before);
     c->launches = before;
     c->step_graph_dt = dt;
@@ -1395,6 +1489,7 @@ static int capture_step_graph(ph_ctx* c, double dt) {
 
 int ph_rk_step(ph_ctx* c, double dt, int nsteps) {
     if (!c || nsteps < 0) return fail(PH_ERR_INVALID, "bad argument");
+    NvtxRange nvtx("ph_rk_step");
     if (c->rrk) {   // the root finding reads sums back after every step: direct launches
         c->rrk_elapsed = 0.0;
         for (int s = 0; s < nsteps; ++s)
@@ -1404,7 +1499,7 @@ int ph_rk_step(ph_ctx* c, double dt, int nsteps) {
     c->rrk_elapsed = dt * nsteps;
     // several steps of one dt on a caller-given stream replay a graph of one step; the
     // per-launch timing mode and one-stage methods (which swap buffers) launch directly
-    const bool graph = c->stream != nullptr && !c->timing && c->ns > 1 && nsteps > 1 && !c->nc_ghost;
+    const bool graph = c->stream != nullptr && c->timing != 1 && c->ns > 1 && nsteps > 1 && !c->nc_ghost;
     if (graph) {
         int s = 0;
         if (!c->step_graph || c->step_graph_dt != dt) {
@@ -1414,6 +1509,16 @@ int ph_rk_step(ph_ctx* c, double dt, int nsteps) {
             if (int rc = capture_step_graph(c, dt)) return rc;
         }
         for (; s < nsteps; ++s) {
+            if (c->timing == 2) {   // this replay records its own events
+                if (c->tpool.size() <= c->treplays) {
+                    c->tpool.emplace_back(c->tnodes.size(), nullptr);
+                    for (cudaEvent_t& ev : c->tpool.back()) PH_CUDA(cudaEventCreate(&ev));
+                }
+                std::vector<cudaEvent_t>& evs = c->tpool[c->treplays];
+                for (size_t j = 0; j < c->tnodes.size(); ++j)
+                    PH_CUDA(cudaGraphExecEventRecordNodeSetEvent(c->step_graph, c->tnodes[j], evs[j]));
+                ++c->treplays;
+            }
             PH_CUDA(cudaGraphLaunch(c->step_graph, c->stream));
             c->launches += c->step_graph_launches;
         }
@@ -1558,7 +1663,7 @@ int ph_run(ph_ctx* c, double dt, int nsteps, int record_every, double* rows) {
     if (nrec > 0) PH_CUDA(cudaMemsetAsync(c->d_counter, 0, sizeof(int), c->stream));
     // intervals on a caller-given stream replay a captured graph (the first one runs
     // directly so that every kernel is configured before the capture)
-    const bool graph = c->stream != nullptr && !c->timing && c->ns > 1 && nrec > 1;
+    const bool graph = c->stream != nullptr && c->timing == 0 && c->ns > 1 && nrec > 1;
     int r = 0;
     if (graph) {
         if (!c->run_graph || c->run_graph_dt != dt || c->run_graph_every != record_every) {
@@ -1619,18 +1724,40 @@ int ph_status(ph_ctx* c, uint32_t* flags) {
 
 int ph_set_timing(ph_ctx* c, int enable) {
     if (!c) return fail(PH_ERR_INVALID, "null argument");
-    if (enable && !c->ev0) {
+    if (enable < 0 || enable > 2) return fail(PH_ERR_INVALID, "timing mode must be 0, 1 or 2");
+    if (enable == 1 && !c->ev0) {
         PH_CUDA(cudaEventCreate(&c->ev0));
         PH_CUDA(cudaEventCreate(&c->ev1));
     }
-    c->timing = enable != 0;
+    if (enable == 2 && c->tcap.empty()) {
+        c->tcap.assign(TIMED_KERNELS_PER_STEP + 1, nullptr);
+        for (cudaEvent_t& ev : c->tcap) PH_CUDA(cudaEventCreate(&ev));
+    }
+    // a step graph captured in another mode has (or lacks) the timing nodes: capture again
+    if ((enable == 2) != (c->timing == 2) && c->step_graph) {
+        PH_CUDA(cudaStreamSynchronize(c->stream));
+        drop_step_graph(c);
+    }
+    c->timing = enable;
     for (int i = 0; i < 3; ++i) { c->t_ms[i] = 0.0; c->t_n[i] = 0; }
+    c->treplays = 0;
     c->launches = 0;
     return PH_OK;
 }
 
 int ph_get_timing(ph_ctx* c, double out[7]) {
     if (!c || !out) return fail(PH_ERR_INVALID, "null argument");
+    if (c->timing == 2 && c->treplays) {   // the replays' kernel durations, summed per class
+        PH_CUDA(cudaStreamSynchronize(c->stream));
+        for (int i = 0; i < 3; ++i) { c->t_ms[i] = 0.0; c->t_n[i] = 0; }
+        for (size_t r = 0; r < c->treplays; ++r)
+            for (size_t j = 0; j < c->tcls.size(); ++j) {
+                float ms = 0.f;
+                PH_CUDA(cudaEventElapsedTime(&ms, c->tpool[r][j], c->tpool[r][j + 1]));
+                c->t_ms[c->tcls[j]] += ms;
+                c->t_n[c->tcls[j]] += 1;
+            }
+    }
     for (int i = 0; i < 3; ++i) { out[2 * i] = c->t_ms[i]; out[2 * i + 1] = (double)c->t_n[i]; }
     out[6] = (double)c->launches;
     return PH_OK;
@@ -1672,7 +1799,9 @@ int ph_sync(ph_ctx* c) {
 // size, which every GPU that loads this library holds until the process exits.
 // Nothing has to start at zero: each call rebuilds the tables, clears the status word,
 // writes the whole viscous-flux scratch before reading it and writes every entry of R.
-// All calls share these arrays, so calls that overlap on the GPU race.
+// The status word keeps the call's non-physical flag until the next call
+// (ph_residual_noalloc_status reads it). All calls share these arrays, so calls that
+// overlap on the GPU race.
 // =======================================================================================
 namespace {
 
@@ -1685,26 +1814,39 @@ static __device__ __align__(256) ph::OpTab g_noalloc_ops;
 static __device__ __align__(256) unsigned g_noalloc_status;
 
 // Device addresses of the arrays above, resolved once per device with that device current.
-// In host code the array names are host-side stand-ins, never device addresses.
+// In host code the array names are host-side stand-ins, never device addresses. The first
+// call on a device takes the mutex; later calls see `ready` set (release / acquire).
 struct NoallocSymbols {
-    bool ready = false;
+    std::atomic<bool> ready{false};
     double* fv = nullptr;
     int* nbr = nullptr;
     ph::OpTab* ops = nullptr;
     unsigned* status = nullptr;
 };
 NoallocSymbols g_noalloc_sym[64];
+std::mutex g_noalloc_setup_mutex;
 
 int noalloc_setup(int dev) {
     if (dev < 0 || dev >= 64) return fail(PH_ERR_INVALID, "device ordinal out of range");
     NoallocSymbols& s = g_noalloc_sym[dev];
-    if (s.ready) return PH_OK;
+    if (s.ready.load(std::memory_order_acquire)) return PH_OK;
+    std::lock_guard<std::mutex> lock(g_noalloc_setup_mutex);
+    if (s.ready.load(std::memory_order_relaxed)) return PH_OK;
     PH_CUDA(cudaGetSymbolAddress((void**)&s.fv, g_noalloc_fv));
     PH_CUDA(cudaGetSymbolAddress((void**)&s.nbr, g_noalloc_nbr));
     PH_CUDA(cudaGetSymbolAddress((void**)&s.ops, g_noalloc_ops));
     PH_CUDA(cudaGetSymbolAddress((void**)&s.status, g_noalloc_status));
-    s.ready = true;
+    s.ready.store(true, std::memory_order_release);
     return PH_OK;
+}
+
+// Writes this call's operator table and clears the status word. The table travels as a
+// kernel argument (copied into the launch), so no host buffer has to outlive the call.
+__global__ void noalloc_set_tables(const ph::OpTab tab) {
+    const double* src = reinterpret_cast<const double*>(&tab);
+    double* dst = reinterpret_cast<double*>(&g_noalloc_ops);
+    for (int i = threadIdx.x; i < (int)(sizeof(ph::OpTab) / sizeof(double)); i += blockDim.x) dst[i] = src[i];
+    if (threadIdx.x == 0) g_noalloc_status = 0u;
 }
 
 // fixed-size versions of the 1-D helpers (no heap allocation)
@@ -1796,15 +1938,14 @@ __global__ void noalloc_neighbours(int n, int morton, int levels, int* nbr) {
 extern "C" int ph_residual_noalloc(const ph_mesh_desc* mesh, const ph_params* prm, const double* U, double* R,
                                    void* cuda_stream) {
     if (!mesh || !prm || !U || !R) return fail(PH_ERR_INVALID, "null argument");
+    // the checks of ph_ctx_create, before anything is launched
+    if (int rc = check_mesh(mesh)) return rc;
+    if (int rc = check_param_ranges(prm)) return rc;
     if (is_curvilinear(mesh)) return fail(PH_ERR_UNSUPPORTED, "ph_residual_noalloc: affine meshes only");
-    if (prm->flux_nodes_type != 1 || prm->overintegration != 0)
-        return fail(PH_ERR_UNSUPPORTED, "the GPU path is collocated: flux_nodes_type = GLL and overintegration = 0");
-    if (prm->poly_degree < 1 || prm->poly_degree > 6) return fail(PH_ERR_UNSUPPORTED, "poly_degree must be 1..6");
-    if (prm->flux_reconstruction_aux != 0) return fail(PH_ERR_UNSUPPORTED, "flux_reconstruction_aux must be kDG");
+    if (const char* why = unsupported_reason(mesh, prm)) return fail(PH_ERR_UNSUPPORTED, why);
     if (prm->conv_num_flux >= 3 && !prm->use_split_form)
         return fail(PH_ERR_INVALID, "two point flux and not using split form are not compatible");
     const int n = mesh->n_cells_per_direction;
-    if (n < 1 || !(mesh->right > mesh->left)) return fail(PH_ERR_INVALID, "bad mesh");
     const long long nc = (long long)n * n * n;
     const int N1 = prm->poly_degree + 1, NP = N1 * N1 * N1;
     const bool visc = prm->pde_type == 1;
@@ -1860,8 +2001,8 @@ extern "C" int ph_residual_noalloc(const ph_mesh_desc* mesh, const ph_params* pr
             tab.B[a * ph::MAXN1 + l] = Minv[a * N1 + l] * w[l];
         }
     }
-    PH_CUDA(cudaMemcpyToSymbolAsync(g_noalloc_ops, &tab, sizeof(tab), 0, cudaMemcpyHostToDevice, stream));
-    PH_CUDA(cudaMemsetAsync(sym.status, 0, sizeof(unsigned), stream));
+    noalloc_set_tables<<<1, 128, 0, stream>>>(tab);
+    PH_CUDA(cudaGetLastError());
     const bool pow2 = (n & (n - 1)) == 0;
     const bool morton = (mesh->cell_order == 2) || (mesh->cell_order == 0 && pow2);
     int levels = 0;
@@ -1913,5 +2054,18 @@ extern "C" int ph_residual_noalloc(const ph_mesh_desc* mesh, const ph_params* pr
     default: e = ph::launch_stage<7>(a, fp32, visc, split, stream); break;
     }
     if (e != cudaSuccess) return fail(PH_ERR_CUDA, std::string("residual launch: ") + cudaGetErrorString(e));
+    return PH_OK;
+}
+
+extern "C" int ph_residual_noalloc_status(void* cuda_stream, uint32_t* flags) {
+    if (!flags) return fail(PH_ERR_INVALID, "null argument");
+    int dev = 0;
+    PH_CUDA(cudaGetDevice(&dev));
+    if (int rc = noalloc_setup(dev)) return rc;
+    unsigned v = 0;
+    cudaStream_t stream = (cudaStream_t)cuda_stream;
+    PH_CUDA(cudaMemcpyAsync(&v, g_noalloc_sym[dev].status, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+    PH_CUDA(cudaStreamSynchronize(stream));
+    *flags = v;
     return PH_OK;
 }

@@ -16,6 +16,12 @@ namespace ph_host {
 
 int fail(int code, const std::string& msg);   // records the message for ph_last_error
 
+// Argument checks shared by every entry point that takes a mesh / parameters: PH_OK, or
+// PH_ERR_INVALID with the message recorded (mesh size and bounds, cell_order 0..2 and the
+// recursive-children order only for a power-of-two n; enumerations within their ranges).
+int check_mesh(const ph_mesh_desc* mesh);
+int check_param_ranges(const ph_params* prm);
+
 // Configuration checks shared by every entry point that builds a discretisation;
 // returns nullptr when the configuration is on the GPU path, else the reason.
 const char* unsupported_reason(const ph_mesh_desc* mesh, const ph_params* prm);

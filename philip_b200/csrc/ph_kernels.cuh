@@ -133,7 +133,8 @@ struct Layout {
     static constexpr int WARPS_LINES = (CPC * NF + SPW - 1) / SPW;
     static constexpr int NT = WARPS_LINES * 32;
     // register budgets from timing the stage kernel on B200: p = 5 (one cell, 256 threads
-    // per CTA) 4 CTAs per SM in FP64 (2-5 % faster than 3), 6 in FP32 (3-4 % faster than 4);
+    // per CTA) 3 CTAs per SM in FP64 (the unrolled partner loop needs 80 registers; at 4 CTAs
+    // it spills and takes 0.533 ms against 0.496), 6 in FP32 (3-4 % faster than 4);
     // p = 3 (two cells, 128 threads) 6 in FP64 and 10 in FP32 (3 % faster than 8)
     static constexpr bool F32 = sizeof(R) == 4;
     static constexpr int MINB_ASKED = (N1 == 6) ? (F32 ? PH_P5_MINB_F32 : PH_P5_MINB)

@@ -1,8 +1,8 @@
 """Extracts the Taylor-Green energy-check golden values from the reference's own
 integration-test parameter files into tests/golden/tgv_energy_check.json.
 
-Run in the build container (the reference tree is not present on the GPU box):
-    python tests/golden/make_golden.py /root/reference
+Run where a checkout of the reference is present, giving the path of its root:
+    python tests/golden/make_golden.py <path-to-PHiLiP-checkout>
 Only parameter values and expected numbers are copied, not the files.
 """
 import json
@@ -41,4 +41,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <path-to-PHiLiP-checkout>")
+    main(sys.argv[1])

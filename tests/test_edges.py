@@ -66,6 +66,50 @@ def test_curvilinear_navier_stokes_is_refused():
     assert rc == _lib.PH_ERR_UNSUPPORTED and "Euler" in msg
 
 
+BAD_MESHES = [
+    ("recursive_order_n3", dict(n_cells_per_direction=3, cell_order=2), "power of two"),
+    ("cell_order_3", dict(cell_order=3), "cell_order"),
+    ("cell_order_negative", dict(cell_order=-1), "cell_order"),
+    ("no_cells", dict(n_cells_per_direction=0), "bad mesh"),
+]
+
+
+@pytest.mark.parametrize("name,mesh_kw,text", BAD_MESHES, ids=[b[0] for b in BAD_MESHES])
+def test_bad_meshes_are_refused_by_every_entry_point(name, mesh_kw, text):
+    """A cell order the connectivity cannot build (the recursive-children order of a cube whose
+    side is not a power of two would number cells past the mesh) is refused with
+    PH_ERR_INVALID before any device work by ph_ctx_create, ph_residual_noalloc and
+    ph_batch_bytes."""
+    rc, msg = _create(mesh_kw=mesh_kw)
+    assert rc == _lib.PH_ERR_INVALID and text in msg, (rc, msg)
+    L = _lib.load()
+    prm = Parameters.from_dict(prm_dict())
+    p = prm.to_ph_params()
+    m = _lib.PhMeshDesc(prm.n_cells, 0, *prm.grid_bounds)
+    for k, v in mesh_kw.items():
+        setattr(m, k, v)
+    dummy = ctypes.c_void_p(16)   # never dereferenced: the checks come first
+    rc = L.ph_residual_noalloc(ctypes.byref(m), ctypes.byref(p), dummy, dummy, None)
+    assert rc == _lib.PH_ERR_INVALID and text in L.ph_last_error().decode()
+    nbytes = ctypes.c_size_t()
+    rc = L.ph_batch_bytes(ctypes.byref(m), ctypes.byref(p), ctypes.byref(nbytes))
+    assert rc == _lib.PH_ERR_INVALID and text in L.ph_last_error().decode()
+
+
+def test_noalloc_refuses_what_the_context_refuses():
+    """ph_residual_noalloc applies ph_ctx_create's parameter checks before any launch."""
+    L = _lib.load()
+    prm = Parameters.from_dict(prm_dict())
+    m = _lib.PhMeshDesc(prm.n_cells, 0, *prm.grid_bounds)
+    dummy = ctypes.c_void_p(16)
+    for field, value in (("pde_type", 2), ("two_point_num_flux_type", 7), ("conv_num_flux", 9), ("precision", 3),
+                         ("poly_degree", 7)):
+        p = prm.to_ph_params()
+        setattr(p, field, value)
+        rc = L.ph_residual_noalloc(ctypes.byref(m), ctypes.byref(p), dummy, dummy, None)
+        assert rc in (_lib.PH_ERR_INVALID, _lib.PH_ERR_UNSUPPORTED), field
+
+
 # ------------------------------------------------------------------------------- GPU
 
 SMALL = [

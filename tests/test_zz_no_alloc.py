@@ -1,11 +1,18 @@
 """ph_residual_noalloc: R(U) on caller-owned device buffers with no device allocation.
 
-Callers that cannot call cudaMalloc (inside CUDA-graph capture, in loops that must not
-synchronise the device, or under a framework that owns all device memory) use this entry
-point; its scratch is a fixed file-scope device array. It must give the same residual as
-ph_residual (tolerance 1e-12 relative max-norm, as the other parity tests), on two calls
-in a row (the shared scratch keeps the previous call's contents), and reject meshes above
-its fixed limits with an error. Collected last on purpose (file name).
+Some callers of this library cannot allocate device memory: a solver loop that must never
+synchronise the device (cudaMalloc and cudaFree may synchronise), or a host framework that
+reserves all device memory for its own pool up front and forbids allocations behind its
+back. They call this entry point; its scratch is fixed file-scope device arrays shared by
+every call.
+
+Checked here, through the C-ABI: the same residual as ph_residual on a context (tolerance
+1e-12 relative max-norm in FP64, the other parity tests' bound; 1e-5 in the precision form,
+the precision tests' bound) on two calls in a row (the shared scratch keeps the previous
+call's contents), on the default stream and on a side stream; free device memory unchanged
+by a warm call; the non-physical flag of the last call readable through
+ph_residual_noalloc_status and cleared by the next call; meshes above the fixed limits
+rejected with an error. Collected last on purpose (file name).
 """
 import ctypes
 
@@ -35,25 +42,95 @@ def _state(dg, seed):
     return U * (1.0 + 0.02 * rng.standard_normal(U.shape))
 
 
+def _noalloc(dg, dU, dR, stream=None):
+    rc = dg.L.ph_residual_noalloc(ctypes.byref(dg.mesh), ctypes.byref(dg.params), ctypes.c_void_p(dU.data_ptr()),
+                                  ctypes.c_void_p(dR.data_ptr()), stream)
+    _lib.check(rc)
+
+
+def _status(L, stream=None):
+    flags = ctypes.c_uint32(0xFFFFFFFF)
+    _lib.check(L.ph_residual_noalloc_status(stream, ctypes.byref(flags)))
+    return flags.value
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("name,kw", CASES, ids=[c[0] for c in CASES])
 def test_noalloc_residual_matches_context_residual(name, kw):
     import torch
     prm = Parameters.from_dict(prm_dict(**kw))
     dg = DGStrong(prm)
-    L = dg.L
     for call in range(2):
         U = _state(dg, seed=call + len(name))
         R_ref = dg.residual_of(U)
         dU = torch.from_numpy(U).cuda()
         dR = torch.full_like(dU, float("nan"))
-        rc = L.ph_residual_noalloc(ctypes.byref(dg.mesh), ctypes.byref(dg.params), ctypes.c_void_p(dU.data_ptr()),
-                                   ctypes.c_void_p(dR.data_ptr()), None)
-        _lib.check(rc)
+        _noalloc(dg, dU, dR)
         torch.cuda.synchronize()
         err = rel_max_err(dR.cpu().numpy(), R_ref)
         print(f"{name} call {call}: no-alloc vs context residual rel err {err:.3e}")
         assert err <= 1e-12
+        assert _status(dg.L) == 0
+
+
+@pytest.mark.gpu
+def test_noalloc_precision_form_matches_context_residual():
+    import torch
+    prm = Parameters.from_dict(prm_dict(poly_degree=3, n_cells=4, pde="navier_stokes", diss="bassi_rebay_2"))
+    dg = DGStrong(prm, precision=_lib.PH_FP32_RESIDUAL)
+    for call in range(2):
+        U = _state(dg, seed=11 + call)
+        R_ref = dg.residual_of(U)
+        dU = torch.from_numpy(U).cuda()
+        dR = torch.full_like(dU, float("nan"))
+        _noalloc(dg, dU, dR)
+        torch.cuda.synchronize()
+        err = rel_max_err(dR.cpu().numpy(), R_ref)
+        print(f"precision form call {call}: no-alloc vs context residual rel err {err:.3e}")
+        assert err <= 1e-5
+
+
+@pytest.mark.gpu
+def test_noalloc_on_a_side_stream_allocates_nothing():
+    import torch
+    prm = Parameters.from_dict(prm_dict(poly_degree=4, n_cells=4, pde="navier_stokes", diss="bassi_rebay_2"))
+    dg = DGStrong(prm)
+    U = _state(dg, seed=5)
+    R_ref = dg.residual_of(U)
+    side = torch.cuda.Stream()
+    dU = torch.from_numpy(U).cuda()
+    dR = torch.full_like(dU, float("nan"))
+    torch.cuda.synchronize()
+    handle = ctypes.c_void_p(side.cuda_stream)
+    _noalloc(dg, dU, dR, handle)        # warm call: the device's first call resolves the arrays' addresses
+    side.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    dR.fill_(float("nan"))
+    torch.cuda.synchronize()
+    _noalloc(dg, dU, dR, handle)
+    side.synchronize()
+    free_after = torch.cuda.mem_get_info()[0]
+    err = rel_max_err(dR.cpu().numpy(), R_ref)
+    print(f"side stream: rel err {err:.3e}, free memory {free_before} -> {free_after}")
+    assert err <= 1e-12
+    assert free_after == free_before
+
+
+@pytest.mark.gpu
+def test_noalloc_reports_a_non_physical_state():
+    import torch
+    prm = Parameters.from_dict(prm_dict(poly_degree=3, n_cells=2))
+    dg = DGStrong(prm)
+    U = _state(dg, seed=3)
+    bad = U.copy()
+    bad[0] = -abs(bad[0])               # density of node 0 of cell 0
+    dU = torch.from_numpy(bad).cuda()
+    dR = torch.zeros_like(dU)
+    _noalloc(dg, dU, dR)
+    assert _status(dg.L) & 1
+    dU.copy_(torch.from_numpy(U))
+    _noalloc(dg, dU, dR)                # the next call clears the flag
+    assert _status(dg.L) == 0
 
 
 @pytest.mark.gpu
