@@ -274,9 +274,23 @@ int check_param_ranges(const ph_params* prm) {
     return PH_OK;
 }
 
+bool uncollocated(const ph_params* prm) { return prm->flux_nodes_type != 1 || prm->overintegration != 0; }
+
+const char* uncollocated_reason(const ph_mesh_desc* mesh, const ph_params* prm) {
+    if (prm->overintegration < 0 || prm->overintegration > 2) return "overintegration must be 0, 1 or 2";
+    if (prm->poly_degree < 1 || prm->poly_degree + 1 + prm->overintegration > ph::GL_MAXQ)
+        return "uncollocated flux nodes: poly_degree >= 1 and poly_degree + 1 + overintegration <= 7";
+    if (prm->flux_reconstruction_aux != 0) return "flux_reconstruction_aux must be kDG";
+    if (is_curvilinear(mesh)) return "uncollocated flux nodes take affine meshes";
+    if (prm->precision != PH_FP64) return "uncollocated flux nodes take the FP64 path";
+    if (prm->runge_kutta_method > 3) return "uncollocated flux nodes take the Butcher RK methods";
+    if (prm->use_relaxation_runge_kutta) return "uncollocated flux nodes: no relaxation RK";
+    return nullptr;
+}
+
 const char* unsupported_reason(const ph_mesh_desc* mesh, const ph_params* prm) {
-    if (prm->flux_nodes_type != 1 || prm->overintegration != 0)
-        return "the GPU path is collocated: flux_nodes_type = GLL and overintegration = 0";
+    if (uncollocated(prm))
+        return "this entry point is collocated: flux_nodes_type = GLL and overintegration = 0 (contexts take both)";
     if (prm->poly_degree < 1 || prm->poly_degree > 6) return "poly_degree must be 1..6";
     if (prm->flux_reconstruction_aux != 0) return "flux_reconstruction_aux must be kDG";
     if (is_curvilinear(mesh)) {
@@ -325,6 +339,91 @@ int build_operators(const ph_params* prm, ph::OpTab& tab, bool& fr, std::vector<
             tab.B[a * ph::MAXN1 + l] = Minv[a * N1 + l] * w[l];
         }
     }
+    return PH_OK;
+}
+
+// 1-D operators of the uncollocated path (GL flux nodes, or overintegration): solution basis
+// on the p + 1 GLL support points, nq flux nodes (QGauss, or QGaussLobatto with
+// overintegration); the sets of DGBase::create_collection_tuple (dg_base.cpp:131-261) and
+// OPERATOR::basis_functions / local_mass / local_basis_stiffness / vol_projection_operator /
+// local_Flux_Reconstruction_operator (operators.cpp:1206-2005): chi, its face rows, the
+// flux-node derivative and skew operator, M = chi^T W chi, the projection chi M^-1 chi^T W,
+// and (M + K)^-1 with K = c (D^p)^T M D^p, D = M^-1 chi^T W chi'. The FR mass inverse also
+// goes into ops.Minv for ph_apply_inverse_mass.
+int build_gl_operators(const ph_params* prm, ph::GlTab& t, ph::OpTab& ops) {
+    const int p = prm->poly_degree, nd = p + 1, nq = p + 1 + prm->overintegration;
+    std::vector<double> xs, ws, xq, wq;
+    gll(nd, xs, ws);
+    if (prm->flux_nodes_type == 1) gll(nq, xq, wq); else gauss(nq, xq, wq);
+    std::memset(&t, 0, sizeof(t));
+    std::vector<double> chi((size_t)nq * nd), dchi((size_t)nq * nd), phi(nq), dph(nq);
+    for (int q = 0; q < nq; ++q) {
+        lagrange(xs, xq[q], &chi[q * nd], &dchi[q * nd]);
+        lagrange(xq, xq[q], phi.data(), dph.data());
+        for (int l = 0; l < nq; ++l) t.dphi[q * nq + l] = dph[l];
+        t.wq[q] = wq[q];
+    }
+    for (int i = 0; i < nq * nd; ++i) t.chi[i] = chi[i];
+    std::vector<double> tmp(std::max(nd, nq)), dtmp(std::max(nd, nq));
+    for (int side = 0; side < 2; ++side) {
+        lagrange(xs, (double)side, tmp.data(), dtmp.data());
+        for (int i = 0; i < nd; ++i) t.chis[side][i] = tmp[i];
+        lagrange(xq, (double)side, tmp.data(), dtmp.data());
+        for (int l = 0; l < nq; ++l) t.phis[side][l] = tmp[l];
+    }
+    // S_ij = sum_q phi_i(x_q) phi_j'(x_q) w_q = w_i dphi[i][j] on the flux nodes
+    for (int i = 0; i < nq; ++i)
+        for (int j = 0; j < nq; ++j) t.skew[i * nq + j] = wq[i] * t.dphi[i * nq + j] - wq[j] * t.dphi[j * nq + i];
+    std::vector<double> M((size_t)nd * nd, 0.0), Schi((size_t)nd * nd, 0.0);
+    for (int i = 0; i < nd; ++i)
+        for (int j = 0; j < nd; ++j)
+            for (int q = 0; q < nq; ++q) {
+                M[i * nd + j] += chi[q * nd + i] * chi[q * nd + j] * wq[q];
+                Schi[i * nd + j] += chi[q * nd + i] * dchi[q * nd + j] * wq[q];
+            }
+    std::vector<double> Mi;
+    if (!mat_inv(M, nd, Mi)) return fail(PH_ERR_INVALID, "singular mass matrix");
+    // projection M^-1 chi^T W (nd x nq), then P = chi proj and the face rows chis proj
+    std::vector<double> proj((size_t)nd * nq, 0.0);
+    for (int i = 0; i < nd; ++i)
+        for (int q = 0; q < nq; ++q) {
+            double v = 0.0;
+            for (int j = 0; j < nd; ++j) v += Mi[i * nd + j] * chi[q * nd + j] * wq[q];
+            proj[i * nq + q] = v;
+        }
+    for (int a = 0; a < nq; ++a)
+        for (int q = 0; q < nq; ++q) {
+            double v = 0.0;
+            for (int i = 0; i < nd; ++i) v += chi[a * nd + i] * proj[i * nq + q];
+            t.P[a * nq + q] = v;
+        }
+    for (int side = 0; side < 2; ++side)
+        for (int q = 0; q < nq; ++q) {
+            double v = 0.0;
+            for (int i = 0; i < nd; ++i) v += t.chis[side][i] * proj[i * nq + q];
+            t.ps[side][q] = v;
+        }
+    // FR: D = M^-1 Schi, K = c (D^p)^T M D^p; kDG for the auxiliary equation (K = 0)
+    double cfr = 0.0;
+    if (fr_parameter(prm->flux_reconstruction, p, prm->FR_user_specified_correction_parameter_value, cfr))
+        return fail(PH_ERR_UNSUPPORTED, "flux_reconstruction type not defined for this degree");
+    const std::vector<double> Dm = mat_mul(Mi, Schi, nd);
+    std::vector<double> Dp((size_t)nd * nd, 0.0);
+    for (int i = 0; i < nd; ++i) Dp[i * nd + i] = 1.0;
+    for (int k = 0; k < p; ++k) Dp = mat_mul(Dm, Dp, nd);
+    std::vector<double> MK(M);
+    for (int i = 0; i < nd; ++i)
+        for (int j = 0; j < nd; ++j) {
+            double kij = 0.0;
+            for (int a = 0; a < nd; ++a)
+                for (int b = 0; b < nd; ++b) kij += Dp[a * nd + i] * M[a * nd + b] * Dp[b * nd + j];
+            MK[i * nd + j] += cfr * kij;
+        }
+    std::vector<double> MKi;
+    if (!mat_inv(MK, nd, MKi)) return fail(PH_ERR_INVALID, "singular FR mass matrix");
+    for (int i = 0; i < nd * nd; ++i) { t.minv[i] = MKi[i]; t.minv_aux[i] = Mi[i]; }
+    for (int a = 0; a < nd; ++a)
+        for (int l = 0; l < nd; ++l) ops.Minv[a * ph::MAXN1 + l] = MKi[a * nd + l];
     return PH_OK;
 }
 
@@ -678,6 +777,15 @@ struct ph_ctx {
     double rrk_gamma = 1.0, rrk_elapsed = 0.0;
     std::vector<double> h_ent;
     std::vector<double> h_partial;
+    // uncollocated path (GL flux nodes / overintegration): nq flux nodes per direction, the
+    // operator table and the face / viscous buffers of its kernels
+    bool gl = false;
+    int NQ = 0;
+    ph::GlTab h_gl{};
+    ph::GlTab* d_gl = nullptr;
+    double* d_t1 = nullptr;
+    double* d_t2 = nullptr;
+    double* d_vis = nullptr;
     // optional per-kernel timing: 1 = CUDA events around every direct launch, the stream
     // synchronised after each; 2 = event-record nodes between the kernels of the captured
     // RK step, a fresh set of events for every replay (the replays themselves are timed)
@@ -805,6 +913,28 @@ int dispatch_aux(ph_ctx* c, const double* U, int cell_begin, int cell_end) {
     return PH_OK;
 }
 
+// One kernel of the uncollocated path on the stage input a.U: 0 face values, 1 auxiliary
+// equation, 2 residual / RK stage (timing classes: other, auxiliary, stage).
+int dispatch_gl(ph_ctx* c, int kernel, const ph::StageArgs& a) {
+    static const char* const kName[] = {"face-value kernel", "auxiliary kernel", "stage kernel"};
+    NvtxRange nvtx(kName[kernel]);
+    const ph::GlArgs g{c->d_gl, c->d_t1, c->d_t2, c->d_vis};
+    cudaError_t e;
+    timer_begin(c);
+    switch (c->N1) {
+    case 2: e = ph::launch_gl<2>(kernel, c->NQ, a, g, c->visc, c->split, c->stream); break;
+    case 3: e = ph::launch_gl<3>(kernel, c->NQ, a, g, c->visc, c->split, c->stream); break;
+    case 4: e = ph::launch_gl<4>(kernel, c->NQ, a, g, c->visc, c->split, c->stream); break;
+    case 5: e = ph::launch_gl<5>(kernel, c->NQ, a, g, c->visc, c->split, c->stream); break;
+    case 6: e = ph::launch_gl<6>(kernel, c->NQ, a, g, c->visc, c->split, c->stream); break;
+    case 7: e = ph::launch_gl<7>(kernel, c->NQ, a, g, c->visc, c->split, c->stream); break;
+    default: return fail(PH_ERR_UNSUPPORTED, "polynomial degree outside 1..6");
+    }
+    if (e != cudaSuccess) return fail(PH_ERR_CUDA, std::string(kName[kernel]) + " launch: " + cudaGetErrorString(e));
+    timer_end(c, kernel == 2 ? 0 : kernel == 1 ? 1 : 2);
+    return PH_OK;
+}
+
 // Halo copy of a slab context: rows of `width` 8-byte words for both partition faces at once
 // (blockIdx.y = side), from a strided source to a strided destination.
 struct HaloCopy {
@@ -927,6 +1057,12 @@ int on_interior(ph_ctx* c, bool fork, F launch, cudaEvent_t done) {
 
 int eval_residual(ph_ctx* c, const double* in, ph::StageArgs a) {
     a.U = in;
+    if (c->gl) {   // face values, (auxiliary equation,) residual: every kernel over all cells
+        a.cell_begin = 0; a.nc = c->nc;
+        if (int rc = dispatch_gl(c, 0, a)) return rc;
+        if (c->visc) if (int rc = dispatch_gl(c, 1, a)) return rc;
+        return dispatch_gl(c, 2, a);
+    }
     if (!c->nc_ghost) {
         if (c->visc) if (int rc = dispatch_aux(c, in, 0, c->nc)) return rc;
         return stage_range(c, a, 0, c->nc);
@@ -976,7 +1112,9 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
     *out = nullptr;
     if (int rc = check_mesh(mesh)) return rc;
     if (int rc = check_param_ranges(prm)) return rc;
-    if (const char* why = unsupported_reason(mesh, prm)) return fail(PH_ERR_UNSUPPORTED, why);
+    const bool gl = uncollocated(prm);
+    if (const char* why = gl ? uncollocated_reason(mesh, prm) : unsupported_reason(mesh, prm))
+        return fail(PH_ERR_UNSUPPORTED, why);
     const bool ec = prm->conv_num_flux >= 3;
     if (ec && !prm->use_split_form)
         return fail(PH_ERR_INVALID, "two point flux and not using split form are not compatible");   // numerical_flux_factory.cpp
@@ -995,6 +1133,7 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
         if (z0 < 0 || z0 >= mesh->n_cells_per_direction || nz > mesh->n_cells_per_direction)
             return fail(PH_ERR_INVALID, "slab outside the mesh: 0 <= z_first < n and 1 <= z_count <= n");
         if (is_curvilinear(mesh)) return fail(PH_ERR_UNSUPPORTED, "slab contexts take affine meshes");
+        if (gl) return fail(PH_ERR_UNSUPPORTED, "slab contexts take GLL flux nodes without overintegration");
         if (prm->use_relaxation_runge_kutta)
             return fail(PH_ERR_UNSUPPORTED, "slab contexts: relaxation RK needs global entropy sums per root iterate");
     }
@@ -1025,6 +1164,11 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
     // ---- 1-D operators, integral tables, physics, RK tableau, connectivity, geometry
     std::vector<double> x, D;
     if (int rc = build_operators(prm, c->h_ops, c->fr, x, D)) { delete c; return rc; }
+    c->gl = gl;
+    if (gl) {
+        c->NQ = c->N1 + prm->overintegration;
+        if (int rc = build_gl_operators(prm, c->h_gl, c->h_ops)) { delete c; return rc; }
+    }
     ph::IntegralTab itab;
     build_integral_table(x, c->p, itab);
     c->pc = physics_constants(prm, c->h, c->pen);
@@ -1073,6 +1217,15 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
         c->halo_stride = (std::max(c->halo_state_bytes, c->halo_visc_bytes) + 255) / 256 * 256;
         bad |= dalloc(&c->d_halo, 4 * c->halo_stride);
     }
+    if (gl) {
+        const size_t faces = (size_t)c->nc * 6 * c->NQ * c->NQ;
+        bad |= dalloc(&c->d_gl, 1);
+        bad |= dalloc(&c->d_t1, faces * (c->split ? 10 : 5));
+        if (c->visc) {
+            bad |= dalloc(&c->d_t2, faces * ph::GL_T2W);
+            bad |= dalloc(&c->d_vis, (size_t)c->nc * 4 * c->NP);
+        }
+    }
     if (c->curv) bad |= dalloc(&c->d_metric, metric.size());
     if (c->curv) bad |= dalloc(&c->d_xnode, (size_t)3 * c->nc * c->NP);
     else bad |= dalloc(&c->d_origin, (size_t)3 * c->nc);
@@ -1081,6 +1234,7 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
     e = cudaMemcpy(c->d_nbr, nbr.data(), nbr.size() * sizeof(int), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(c->d_ops, &c->h_ops, sizeof(ph::OpTab), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(c->d_itab, &itab, sizeof(ph::IntegralTab), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && c->d_gl) e = cudaMemcpy(c->d_gl, &c->h_gl, sizeof(ph::GlTab), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(c->d_status, 0, sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMemset(c->d_sol, 0, c->nalloc * sizeof(double));
     if (e == cudaSuccess && c->d_comp) e = cudaMemset(c->d_comp, 0, N * sizeof(double));
@@ -1166,7 +1320,8 @@ int ph_ctx_destroy(ph_ctx* c) {
     for (auto& set : c->tpool) for (cudaEvent_t ev : set) if (ev) cudaEventDestroy(ev);
     void* ptrs[] = {c->d_nbr, c->d_ops, c->d_itab, c->d_sol, c->d_stA, c->d_stB, c->d_acc, c->d_carry,
                     c->d_fv, c->d_comp, c->d_tmpA, c->d_tmpB, c->d_partial, c->d_status, c->d_metric, c->d_xnode, c->d_origin, c->d_err,
-                    c->d_table, c->d_counter, c->d_ent, c->d_ent_cell, c->d_halo};
+                    c->d_table, c->d_counter, c->d_ent, c->d_ent_cell, c->d_halo, c->d_gl, c->d_t1, c->d_t2,
+                    c->d_vis};
     if (c->side) cudaStreamSynchronize(c->side);
     for (void* p : ptrs) if (p) cudaFree(p);
     if (c->side) cudaStreamDestroy(c->side);

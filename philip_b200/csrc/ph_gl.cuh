@@ -1,0 +1,792 @@
+// sm_100a kernels of the uncollocated strong-form DG/FR residual: solution on the (p+1)^3
+// GLL support points of FE_DGQ(p), volume and face integrals on nq = p + 1 +
+// overintegration flux nodes per direction (Gauss-Legendre, the reference's default
+// flux_nodes_type, or Gauss-Lobatto with overintegration), affine periodic cells, FP64.
+//
+// Here the 1-D operators are dense: the interpolation chi (nq x nd) from the solution
+// nodes to the flux nodes, its face rows, the entropy projection (chi M^-1 chi^T W), the
+// flux-node differentiation and the FR mass inverse (M + K)^-1 with M = chi^T W chi. Every
+// one is applied direction by direction (sum factorisation, operators.cpp:294-649).
+//
+// Three kernels per residual evaluation (one CTA per cell each):
+//   gl_trace_kernel  the state's face values (chi_s (x) chi (x) chi U) and, for the split
+//                    form, the face values of the projected entropy variables, per face
+//   gl_aux_kernel    (Navier-Stokes) the lifted gradient q = (M_aux)^-1 [chi^T W D(chi u)
+//                    + face (u* - u) n], then the viscous volume term -chi^T W div(F_v), the
+//                    face values of q and the face-normal volume viscous flux
+//   gl_stage_kernel  volume term (two-point split form with the skew operator on flux-node
+//                    lines, or the conservative divergence), hybrid surface-volume two-point
+//                    terms, numerical fluxes, lifts, (M+K)^-1 and the RK stage update
+// The face data of a neighbour come from the buffers the earlier kernels wrote, so every
+// face's numerical flux sees the same two states from either side.
+//
+// Reference structure restated (the oracle's Solver::assemble_residual follows the same lines):
+//   auxiliary equation ................ src/dg/strong_dg.cpp:498-1008
+//   volume term, split and conservative src/dg/strong_dg.cpp:1016-1579
+//   entropy projection ................ src/dg/strong_dg.cpp:1235-1330, :3044-3142
+//   hybrid surface-volume two-point ... src/dg/strong_dg.cpp:3144-3350
+//   numerical fluxes and lifts ........ src/dg/strong_dg.cpp:3354-3576
+//   inverse mass (affine) ............. src/dg/dg_base.cpp:4207-4219
+#pragma once
+#include "ph_kernels.cuh"
+
+namespace ph {
+
+constexpr int GL_MAXQ = 7;   // flux nodes per direction
+constexpr int GL_MAXD = 7;   // solution nodes per direction
+
+// 1-D operators, packed row-major with the actual sizes (nq, nd).
+struct GlTab {
+    double chi[GL_MAXQ * GL_MAXD];    // [q][i] solution basis l_i at flux node q
+    double chis[2][GL_MAXD];          // solution basis at xi = 0 and xi = 1
+    double phis[2][GL_MAXQ];          // flux-node Lagrange basis at xi = 0 and xi = 1
+    double dphi[GL_MAXQ * GL_MAXQ];   // [q][l] derivative of flux-node basis l at flux node q
+    double skew[GL_MAXQ * GL_MAXQ];   // S - S^T, S_ij = sum_q phi_i phi_j' w_q (operators.cpp:1440-1477)
+    double wq[GL_MAXQ];               // flux-node weights on [0, 1]
+    double P[GL_MAXQ * GL_MAXQ];      // chi M^-1 chi^T W: flux values -> projected -> flux values
+    double ps[2][GL_MAXQ];            // chis[side] M^-1 chi^T W: face value of the projection
+    double minv[GL_MAXD * GL_MAXD];   // (M + K)^-1
+    double minv_aux[GL_MAXD * GL_MAXD];
+};
+
+// Device buffers of the uncollocated path (per cell, reference units).
+struct GlArgs {
+    const GlTab* tab;
+    double* t1;    // [nc][6][T1W][nq^2]: state at the face nodes (5), projected entropy variables (5, split)
+    double* t2;    // [nc][6][19][nq^2]: lifted gradient q (15, s*3+d), face-normal volume viscous flux (4)
+    double* vis;   // [nc][4][nd^3]: -chi^T W div(F_v), momentum and energy rows
+};
+
+template <bool SPLIT> __host__ __device__ constexpr int gl_t1_width() { return SPLIT ? 10 : 5; }
+constexpr int GL_T2W = 19;
+
+// temporaries of the sum-factorised passes on 5 components (and of the six faces' arrays)
+template <int ND, int NQ> __host__ __device__ constexpr int gl_temp() {
+    constexpr int a = 5 * NQ * NQ * NQ, b = 30 * NQ * NQ, c = 30 * NQ * ND, d = 30 * ND * ND;
+    constexpr int ab = a > b ? a : b, cd = c > d ? c : d;
+    return ab > cd ? ab : cd;
+}
+
+template <int NQ> __host__ __device__ constexpr int gl_threads() {
+    return NQ * NQ * NQ <= 64 ? 64 : NQ * NQ * NQ <= 128 ? 128 : 256;
+}
+
+// Entropy variables of a conservative state (Euler::compute_entropy_variables, euler.cpp:811-830)
+// and the conservative state of entropy variables (:833-855), FP64.
+__device__ __forceinline__ void gl_entropy_vars(const double u[5], double gam, double gm1, double v[5],
+                                                unsigned* st) {
+    const double rho = u[0];
+    double v2 = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { const double w = u[1 + d] / rho; v2 = v2 + w * w; }
+    const double p = positive<double>(gm1 * (u[4] - 0.5 * rho * v2), st);
+    const double s = log(p * pow(rho, -gam));
+    const double rt = p / gm1;
+    v[0] = (rt * (gam + 1.0 - s) - u[4]) / rt;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) v[1 + d] = u[1 + d] / rt;
+    v[4] = -rho / rt;
+}
+__device__ __forceinline__ void gl_cons_from_entropy(const double v[5], double gam, double gm1, double u[5]) {
+    double vv = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) vv += v[1 + d] * v[1 + d];
+    const double s = gam - v[0] + 0.5 * vv / v[4];
+    const double rt = pow(gm1 / pow(-v[4], gam), 1.0 / gm1) * exp(-s / gm1);
+    u[0] = -rt * v[4];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) u[1 + d] = rt * v[1 + d];
+    u[4] = rt * (1.0 - 0.5 * vv / v[4]);
+}
+
+// One sum-factorised pass along direction d: out[s][o] (+)= scale * sum_l A[r * cols + l] in[s][o, r -> l]
+// with r the output's coordinate along d. Input dims (n0, n1, n2), n_d = cols; output dims the
+// same with n_d = rows. x is the fastest index.
+template <int NT>
+__device__ __forceinline__ void gl_pass(const double* A, int rows, int cols, int d, int n0, int n1, int n2,
+                                        const double* in, int in_ss, double* out, int out_ss, int ns, double scale,
+                                        bool acc) {
+    const int m0 = d == 0 ? rows : n0, m1 = d == 1 ? rows : n1, m2 = d == 2 ? rows : n2;
+    const int osz = m0 * m1 * m2;
+    const int st = d == 0 ? 1 : d == 1 ? n0 : n0 * n1;
+    for (int it = threadIdx.x; it < ns * osz; it += NT) {
+        const int s = it / osz, o = it - s * osz;
+        const int x = o % m0, y = (o / m0) % m1, z = o / (m0 * m1);
+        const int r = d == 0 ? x : d == 1 ? y : z;
+        const int base = ((d == 2 ? 0 : z) * n1 + (d == 1 ? 0 : y)) * n0 + (d == 0 ? 0 : x);
+        const double* ip = in + s * in_ss + base;
+        const double* ar = A + r * cols;
+        double v = 0.0;
+        for (int l = 0; l < cols; ++l) v += ar[l] * ip[l * st];
+        double* op = out + s * out_ss + o;
+        *op = acc ? *op + scale * v : scale * v;
+    }
+}
+
+// out = (Az (x) Ay (x) Az) in, x first: input cubes of n_in per direction, output n_out per
+// direction; t0, t1 hold ns * n_out * n_in^2 and ns * n_out^2 * n_in values. Ends with a barrier.
+template <int NT>
+__device__ __forceinline__ void gl_apply3(const double* A, int n_out, int n_in, const double* in, int in_ss,
+                                          double* out, int out_ss, int ns, double* t0, double* t1, double scale,
+                                          bool acc) {
+    const int s0 = n_out * n_in * n_in, s1 = n_out * n_out * n_in;
+    gl_pass<NT>(A, n_out, n_in, 0, n_in, n_in, n_in, in, in_ss, t0, s0, ns, 1.0, false);
+    __syncthreads();
+    gl_pass<NT>(A, n_out, n_in, 1, n_out, n_in, n_in, t0, s0, t1, s1, ns, 1.0, false);
+    __syncthreads();
+    gl_pass<NT>(A, n_out, n_in, 2, n_out, n_out, n_in, t1, s1, out, out_ss, ns, scale, acc);
+    __syncthreads();
+}
+
+// The transpose: out = (A^T (x) A^T (x) A^T) in for A (n_in x n_out) stored row-major, i.e.
+// out[i] = sum_q A[q][i] in[q] per direction (an inner product with the rows of A).
+template <int NT>
+__device__ __forceinline__ void gl_passT(const double* A, int rows_out, int cols_in, int d, int n0, int n1, int n2,
+                                         const double* in, int in_ss, double* out, int out_ss, int ns, double scale,
+                                         bool acc) {
+    // A is (cols_in x rows_out): out coordinate r sums A[l][r] in[l]
+    const int m0 = d == 0 ? rows_out : n0, m1 = d == 1 ? rows_out : n1, m2 = d == 2 ? rows_out : n2;
+    const int osz = m0 * m1 * m2;
+    const int st = d == 0 ? 1 : d == 1 ? n0 : n0 * n1;
+    for (int it = threadIdx.x; it < ns * osz; it += NT) {
+        const int s = it / osz, o = it - s * osz;
+        const int x = o % m0, y = (o / m0) % m1, z = o / (m0 * m1);
+        const int r = d == 0 ? x : d == 1 ? y : z;
+        const int base = ((d == 2 ? 0 : z) * n1 + (d == 1 ? 0 : y)) * n0 + (d == 0 ? 0 : x);
+        const double* ip = in + s * in_ss + base;
+        double v = 0.0;
+        for (int l = 0; l < cols_in; ++l) v += A[l * rows_out + r] * ip[l * st];
+        double* op = out + s * out_ss + o;
+        *op = acc ? *op + scale * v : scale * v;
+    }
+}
+template <int NT>
+__device__ __forceinline__ void gl_apply3T(const double* A, int n_out, int n_in, const double* in, int in_ss,
+                                           double* out, int out_ss, int ns, double* t0, double* t1, double scale,
+                                           bool acc) {
+    const int s0 = n_out * n_in * n_in, s1 = n_out * n_out * n_in;
+    gl_passT<NT>(A, n_out, n_in, 0, n_in, n_in, n_in, in, in_ss, t0, s0, ns, 1.0, false);
+    __syncthreads();
+    gl_passT<NT>(A, n_out, n_in, 1, n_out, n_in, n_in, t0, s0, t1, s1, ns, 1.0, false);
+    __syncthreads();
+    gl_passT<NT>(A, n_out, n_in, 2, n_out, n_out, n_in, t1, s1, out, out_ss, ns, scale, acc);
+    __syncthreads();
+}
+
+// Face values on all six faces of a cube of values: for face f (normal direction dn = f/2,
+// side f&1) out[f][s][q2] = sum over the cube of row[side][i_dn] T[q_t1][i_t1] T[q_t2][i_t2]
+// src[s][i] (the surface interpolation of operators.cpp:355-398 with the face's row along the
+// normal). q2 = q_t2 * n_out + q_t1, t1 < t2 the tangential directions: the same face-node order
+// on both sides of a face. row: two rows of n_in; T: n_out x n_in (nullptr: identity, n_out =
+// n_in). w0: 6 ns n_in^2 values, w1: 6 ns n_out n_in. out[f][s] at out + f * out_fs + s * out_ss.
+template <int NT>
+__device__ __forceinline__ void gl_face_values(const double* src, int src_ss, int ns, int n_in,
+                                               const double* row0, const double* row1, const double* T, int n_out,
+                                               double* w0, double* w1, double* out, int out_fs, int out_ss) {
+    const int n2 = n_in * n_in;
+    // along the normal: w0[f][s][b * n_in + a] (a along t1, b along t2)
+    for (int it = threadIdx.x; it < 6 * ns * n2; it += NT) {
+        const int f = it / (ns * n2), r = it - f * ns * n2, s = r / n2, ab = r - s * n2;
+        const int a = ab % n_in, b = ab / n_in, dn = f >> 1;
+        const double* rw = (f & 1) ? row1 : row0;
+        const int st = dn == 0 ? 1 : dn == 1 ? n_in : n2;
+        const int base = dn == 0 ? (b * n_in + a) * n_in : dn == 1 ? b * n2 + a : b * n_in + a;
+        const double* ip = src + s * src_ss + base;
+        double v = 0.0;
+        for (int l = 0; l < n_in; ++l) v += rw[l] * ip[l * st];
+        w0[it] = v;
+    }
+    __syncthreads();
+    if (T == nullptr) {
+        for (int it = threadIdx.x; it < 6 * ns * n2; it += NT) {
+            const int f = it / (ns * n2), r = it - f * ns * n2, s = r / n2, q2 = r - s * n2;
+            out[f * out_fs + s * out_ss + q2] = w0[it];
+        }
+        __syncthreads();
+        return;
+    }
+    const int m1 = n_out * n_in;
+    for (int it = threadIdx.x; it < 6 * ns * m1; it += NT) {   // along t1: w1[f][s][b * n_out + q1]
+        const int fs = it / m1, bq = it - fs * m1, q1 = bq % n_out, b = bq / n_out;
+        const double* ip = w0 + fs * n2 + b * n_in;
+        double v = 0.0;
+        for (int l = 0; l < n_in; ++l) v += T[q1 * n_in + l] * ip[l];
+        w1[it] = v;
+    }
+    __syncthreads();
+    const int m2 = n_out * n_out;
+    for (int it = threadIdx.x; it < 6 * ns * m2; it += NT) {   // along t2
+        const int fs = it / m2, q2 = it - fs * m2, q1 = q2 % n_out, qq = q2 / n_out;
+        const int f = fs / ns, s = fs - f * ns;
+        const double* ip = w1 + fs * m1 + q1;
+        double v = 0.0;
+        for (int l = 0; l < n_in; ++l) v += T[qq * n_in + l] * ip[l * n_out];
+        out[f * out_fs + s * out_ss + q2] = v;
+    }
+    __syncthreads();
+}
+
+// The lift of six face arrays into the cube: dst[s][node] (+)= sum_f row[side][i_dn]
+// sum_{q1,q2} T[q1][i_t1] T[q2][i_t2] face[f][s][q2] (the surface inner products of
+// operators.cpp:575-636 with the solution basis; T is n_q x n_d). Only the faces in mask
+// (bit f) contribute; per_dir: dst holds one cube per normal direction (dst + dn * dst_ds).
+template <int NT>
+__device__ __forceinline__ void gl_lift_faces(const double* face, int face_fs, int face_ss, int ns, int nq, int nd,
+                                              const double* row0, const double* row1, const double* T, double* w0,
+                                              double* w1, double* dst, int dst_ss, int dst_ds, double scale) {
+    const int mq = nq * nq, m1 = nq * nd, m2 = nd * nd;
+    for (int it = threadIdx.x; it < 6 * ns * m1; it += NT) {   // along t1: w0[f][s][q2 * nd + a]
+        const int fs = it / m1, r = it - fs * m1, a = r % nd, q2 = r / nd;
+        const int f = fs / ns, s = fs - f * ns;
+        const double* ip = face + f * face_fs + s * face_ss + q2 * nq;
+        double v = 0.0;
+        for (int l = 0; l < nq; ++l) v += T[l * nd + a] * ip[l];
+        w0[it] = v;
+    }
+    __syncthreads();
+    for (int it = threadIdx.x; it < 6 * ns * m2; it += NT) {   // along t2: w1[f][s][b * nd + a]
+        const int fs = it / m2, r = it - fs * m2, a = r % nd, b = r / nd;
+        const double* ip = w0 + fs * m1 + a;
+        double v = 0.0;
+        for (int l = 0; l < nq; ++l) v += T[l * nd + b] * ip[l * nd];
+        w1[it] = v;
+    }
+    __syncthreads();
+    const int nd3 = m2 * nd;
+    for (int it = threadIdx.x; it < ns * nd3; it += NT) {
+        const int s = it / nd3, node = it - s * nd3;
+        const int c[3] = {node % nd, (node / nd) % nd, node / m2};
+#pragma unroll
+        for (int dn = 0; dn < 3; ++dn) {
+            const int t1 = dn == 0 ? 1 : 0, t2 = dn == 2 ? 1 : 2;
+            const int ab = c[t2] * nd + c[t1];
+            const double v = row0[c[dn]] * w1[((2 * dn) * ns + s) * m2 + ab] +
+                             row1[c[dn]] * w1[((2 * dn + 1) * ns + s) * m2 + ab];
+            double* op = dst + (dst_ds ? dn * dst_ds : 0) + s * dst_ss + node;
+            *op += scale * v;
+        }
+    }
+    __syncthreads();
+    (void)mq;
+}
+
+// Shared-memory copy of the operator table.
+__device__ __forceinline__ void gl_load_tab(const GlTab* g, GlTab* s, int nt) {
+    const double* src = reinterpret_cast<const double*>(g);
+    double* dst = reinterpret_cast<double*>(s);
+    for (int i = threadIdx.x; i < (int)(sizeof(GlTab) / sizeof(double)); i += nt) dst[i] = src[i];
+}
+
+// ------------------------------------------------------------------------------------
+// Face values of the state (and of the projected entropy variables)
+// ------------------------------------------------------------------------------------
+template <int ND, int NQ, bool SPLIT>
+struct GlTraceLayout {
+    static constexpr int NT = gl_threads<NQ>();
+    static constexpr int D3 = ND * ND * ND, Q3 = NQ * NQ * NQ;
+    static constexpr int oTab = 0, nTab = (int)(sizeof(GlTab) / sizeof(double));
+    static constexpr int oU = nTab;                                 // 5 ND^3
+    static constexpr int oQ = oU + 5 * D3;                          // 5 NQ^3 (flux-node values / entropy variables)
+    static constexpr int nW = gl_temp<ND, NQ>();
+    static constexpr int oW0 = oQ + 5 * Q3, oW1 = oW0 + nW;
+    static constexpr int total = oW1 + nW;
+    static constexpr size_t bytes = (size_t)total * sizeof(double);
+};
+
+template <int ND, int NQ, bool SPLIT>
+__global__ void __launch_bounds__(gl_threads<NQ>()) gl_trace_kernel(const StageArgs a, const GlArgs g) {
+    using L = GlTraceLayout<ND, NQ, SPLIT>;
+    constexpr int NT = L::NT, D3 = L::D3, Q3 = L::Q3, T1W = gl_t1_width<SPLIT>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* sm = reinterpret_cast<double*>(smem_raw);
+    GlTab* tab = reinterpret_cast<GlTab*>(sm + L::oTab);
+    double* sU = sm + L::oU;
+    double* sQ = sm + L::oQ;
+    double* w0 = sm + L::oW0;
+    double* w1 = sm + L::oW1;
+    const int cell = a.cell_begin + blockIdx.x;
+    gl_load_tab(g.tab, tab, NT);
+    for (int i = threadIdx.x; i < 5 * D3; i += NT) sU[i] = __ldg(&a.U[(size_t)cell * 5 * D3 + i]);
+    __syncthreads();
+    double* out = g.t1 + (size_t)cell * 6 * T1W * NQ * NQ;
+    gl_face_values<NT>(sU, D3, 5, ND, tab->chis[0], tab->chis[1], tab->chi, NQ, w0, w1, out, T1W * NQ * NQ, NQ * NQ);
+    if constexpr (SPLIT) {
+        gl_apply3<NT>(tab->chi, NQ, ND, sU, D3, sQ, Q3, 5, w0, w1, 1.0, false);
+        const double gam = a.pc.gam, gm1 = a.pc.gm1;
+        for (int q = threadIdx.x; q < Q3; q += NT) {
+            double u[5], v[5];
+#pragma unroll
+            for (int s = 0; s < 5; ++s) u[s] = sQ[s * Q3 + q];
+            gl_entropy_vars(u, gam, gm1, v, a.status);
+#pragma unroll
+            for (int s = 0; s < 5; ++s) sQ[s * Q3 + q] = v[s];
+        }
+        __syncthreads();
+        gl_face_values<NT>(sQ, Q3, 5, NQ, tab->ps[0], tab->ps[1], tab->P, NQ, w0, w1, out + 5 * NQ * NQ,
+                           T1W * NQ * NQ, NQ * NQ);
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Auxiliary equation and the viscous terms (Navier-Stokes)
+// ------------------------------------------------------------------------------------
+template <int ND, int NQ, bool SPLIT>
+struct GlAuxLayout {
+    static constexpr int NT = gl_threads<NQ>();
+    static constexpr int D3 = ND * ND * ND, Q3 = NQ * NQ * NQ;
+    static constexpr int nTab = (int)(sizeof(GlTab) / sizeof(double));
+    static constexpr int oU = nTab;                      // 5 NQ^3: the state, later the projected state
+    static constexpr int oQ = oU + 5 * Q3;               // 5 NQ^3: state at the flux nodes
+    // aux right-hand side (15 ND^3) and lifted gradient (15 ND^3); later the volume viscous
+    // flux (12 NQ^3) over both
+    static constexpr int nRA = 30 * D3 > 12 * Q3 ? 30 * D3 : 12 * Q3;
+    static constexpr int oR = oQ + 5 * Q3;
+    static constexpr int oA = oR + 15 * D3;
+    static constexpr int oAQ = oR + nRA;                 // 15 NQ^3: lifted gradient at the flux nodes
+    static constexpr int nT = gl_temp<ND, NQ>();
+    static constexpr int oT0 = oAQ + 15 * Q3, oT1 = oT0 + nT;
+    static constexpr int total = oT1 + nT;
+    static constexpr size_t bytes = (size_t)total * sizeof(double);
+};
+
+template <int ND, int NQ, bool SPLIT>
+__global__ void __launch_bounds__(gl_threads<NQ>()) gl_aux_kernel(const StageArgs a, const GlArgs g) {
+    using L = GlAuxLayout<ND, NQ, SPLIT>;
+    constexpr int NT = L::NT, D3 = L::D3, Q3 = L::Q3, NF = NQ * NQ, T1W = gl_t1_width<SPLIT>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* sm = reinterpret_cast<double*>(smem_raw);
+    GlTab* tab = reinterpret_cast<GlTab*>(sm);
+    double* sU = sm + L::oU;
+    double* sQ = sm + L::oQ;
+    double* sR = sm + L::oR;
+    double* sA = sm + L::oA;
+    double* sAQ = sm + L::oAQ;
+    double* t0 = sm + L::oT0;
+    double* t1 = sm + L::oT1;
+    const int cell = a.cell_begin + blockIdx.x;
+    Cst<double> cst; cst.load(a.pc);
+    const int ucv = a.pc.use_const_visc;
+    gl_load_tab(g.tab, tab, NT);
+    for (int i = threadIdx.x; i < 5 * D3; i += NT) sU[i] = __ldg(&a.U[(size_t)cell * 5 * D3 + i]);
+    __syncthreads();
+    gl_apply3<NT>(tab->chi, NQ, ND, sU, D3, sQ, Q3, 5, t0, t1, 1.0, false);
+    // volume part: rhs_d = chi^T W D_d (chi u)   (strong_dg.cpp:666-724; C = h^2 I folded into 1/h below)
+    for (int d = 0; d < 3; ++d) {
+        gl_pass<NT>(tab->dphi, NQ, NQ, d, NQ, NQ, NQ, sQ, Q3, t0, Q3, 5, 1.0, false);
+        __syncthreads();
+        for (int i = threadIdx.x; i < 5 * Q3; i += NT) {
+            const int q = i % Q3;
+            t0[i] *= tab->wq[q % NQ] * tab->wq[(q / NQ) % NQ] * tab->wq[q / (NQ * NQ)];
+        }
+        __syncthreads();
+        // chi^T (x3) into sR[s * 3 + d]: strided over the 15 rows
+        gl_passT<NT>(tab->chi, ND, NQ, 0, NQ, NQ, NQ, t0, Q3, t1, ND * NQ * NQ, 5, 1.0, false);
+        __syncthreads();
+        gl_passT<NT>(tab->chi, ND, NQ, 1, ND, NQ, NQ, t1, ND * NQ * NQ, t0, ND * ND * NQ, 5, 1.0, false);
+        __syncthreads();
+        gl_passT<NT>(tab->chi, ND, NQ, 2, ND, ND, NQ, t0, ND * ND * NQ, sR + d * D3, 3 * D3, 5, 1.0, false);
+        __syncthreads();
+    }
+    // face part: (u* - u) n_d with u* the average of both sides' face values (strong_dg.cpp:871-1008)
+    {
+        double* face = t0;   // [f][s][q2]: W_face (u* - u) n_dn
+        for (int it = threadIdx.x; it < 6 * 5 * NF; it += NT) {
+            const int f = it / (5 * NF), s = (it / NF) % 5, q2 = it % NF;
+            const int cn = __ldg(&a.nbr[cell * 6 + f]);
+            const double uo = __ldg(&g.t1[(((size_t)cell * 6 + f) * T1W + s) * NF + q2]);
+            const double ue = __ldg(&g.t1[(((size_t)cn * 6 + (f ^ 1)) * T1W + s) * NF + q2]);
+            const double sgn = (f & 1) ? 1.0 : -1.0;
+            face[it] = tab->wq[q2 % NQ] * tab->wq[q2 / NQ] * ((0.5 * (uo + ue) - uo) * sgn);
+        }
+        __syncthreads();
+        // added into rhs_dn: sR[s*3 + dn] = sR + dn * D3 + s * 3 * D3 (sA, not yet written,
+        // holds the second pass: 30 ND^2 <= 15 ND^3)
+        gl_lift_faces<NT>(face, 5 * NF, NF, 5, NQ, ND, tab->chis[0], tab->chis[1], tab->chi, t1, sA, sR, 3 * D3, D3,
+                          1.0);
+    }
+    // lifted gradient q = (1/h) M_aux^-1 rhs   (dg_base.cpp:4089-4260, use_auxiliary_eq), then its
+    // face values for the dissipative numerical flux of both neighbours and its values at the
+    // flux nodes; five rows at a time
+    double* tout = g.t2 + (size_t)cell * 6 * GL_T2W * NF;
+    for (int b = 0; b < 3; ++b) {
+        gl_apply3<NT>(tab->minv_aux, ND, ND, sR + b * 5 * D3, D3, sA + b * 5 * D3, D3, 5, t0, t1, a.inv_h, false);
+        gl_face_values<NT>(sA + b * 5 * D3, D3, 5, ND, tab->chis[0], tab->chis[1], tab->chi, NQ, t0, t1,
+                           tout + b * 5 * NF, GL_T2W * NF, NF);
+        gl_apply3<NT>(tab->chi, NQ, ND, sA + b * 5 * D3, D3, sAQ + b * 5 * Q3, Q3, 5, t0, t1, 1.0, false);
+    }
+    // the split form evaluates the volume viscous flux at the entropy-projected state
+    // (strong_dg.cpp:1328 before :1392); the face-normal flux interpolated to the faces uses
+    // the state itself (:2836-3041)
+    if constexpr (SPLIT) {
+        for (int q = threadIdx.x; q < Q3; q += NT) {
+            double u[5], v[5];
+#pragma unroll
+            for (int s = 0; s < 5; ++s) u[s] = sQ[s * Q3 + q];
+            gl_entropy_vars(u, cst.gam, cst.gm1, v, a.status);
+#pragma unroll
+            for (int s = 0; s < 5; ++s) t0[s * Q3 + q] = v[s];
+        }
+        __syncthreads();
+        gl_apply3<NT>(tab->P, NQ, NQ, t0, Q3, sU, Q3, 5, t1, sR, 1.0, false);   // sR is free until the fluxes
+        for (int q = threadIdx.x; q < Q3; q += NT) {
+            double v[5], u[5];
+#pragma unroll
+            for (int s = 0; s < 5; ++s) v[s] = sU[s * Q3 + q];
+            gl_cons_from_entropy(v, cst.gam, cst.gm1, u);
+#pragma unroll
+            for (int s = 0; s < 5; ++s) sU[s * Q3 + q] = u[s];
+        }
+        __syncthreads();
+    }
+    double* sF = sR;   // [d][k][Q3] volume viscous flux, over the dead right-hand side and q
+    for (int q = threadIdx.x; q < Q3; q += NT) {
+        double u[5], gq[5][3];
+#pragma unroll
+        for (int s = 0; s < 5; ++s) {
+            u[s] = SPLIT ? sU[s * Q3 + q] : sQ[s * Q3 + q];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) gq[s][d] = sAQ[(s * 3 + d) * Q3 + q];
+        }
+        double F[3][4];
+        viscous_flux<double>(u, gq, ucv, cst, F, 7, nullptr);
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) sF[(d * 4 + k) * Q3 + q] = F[d][k];
+    }
+    __syncthreads();
+    // -chi^T W sum_d D_d F_d, momentum and energy rows
+    gl_pass<NT>(tab->dphi, NQ, NQ, 0, NQ, NQ, NQ, sF, Q3, t0, Q3, 4, 1.0, false);
+    __syncthreads();
+    gl_pass<NT>(tab->dphi, NQ, NQ, 1, NQ, NQ, NQ, sF + 4 * Q3, Q3, t0, Q3, 4, 1.0, true);
+    __syncthreads();
+    gl_pass<NT>(tab->dphi, NQ, NQ, 2, NQ, NQ, NQ, sF + 8 * Q3, Q3, t0, Q3, 4, 1.0, true);
+    __syncthreads();
+    for (int i = threadIdx.x; i < 4 * Q3; i += NT) {
+        const int q = i % Q3;
+        t0[i] *= tab->wq[q % NQ] * tab->wq[(q / NQ) % NQ] * tab->wq[q / (NQ * NQ)];
+    }
+    __syncthreads();
+    // (the state rows sU are free now: the fluxes stay in sF for the face values below)
+    gl_passT<NT>(tab->chi, ND, NQ, 0, NQ, NQ, NQ, t0, Q3, t1, ND * NQ * NQ, 4, 1.0, false);
+    __syncthreads();
+    gl_passT<NT>(tab->chi, ND, NQ, 1, ND, NQ, NQ, t1, ND * NQ * NQ, sU, ND * ND * NQ, 4, 1.0, false);
+    __syncthreads();
+    gl_passT<NT>(tab->chi, ND, NQ, 2, ND, ND, NQ, sU, ND * ND * NQ, g.vis + (size_t)cell * 4 * D3, D3, 4, -1.0, false);
+    // face-normal volume viscous flux at the faces: n_dn sum_l phi_l(side) F_dn(u_l) (state not
+    // projected)
+    if constexpr (SPLIT) {
+        __syncthreads();
+        for (int q = threadIdx.x; q < Q3; q += NT) {
+            double u[5], gq[5][3];
+#pragma unroll
+            for (int s = 0; s < 5; ++s) {
+                u[s] = sQ[s * Q3 + q];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) gq[s][d] = sAQ[(s * 3 + d) * Q3 + q];
+            }
+            double F[3][4];
+            viscous_flux<double>(u, gq, ucv, cst, F, 7, nullptr);
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+#pragma unroll
+                for (int k = 0; k < 4; ++k) sF[(d * 4 + k) * Q3 + q] = F[d][k];
+        }
+    }
+    __syncthreads();
+    for (int it = threadIdx.x; it < 6 * 4 * NF; it += NT) {
+        const int f = it / (4 * NF), k = (it / NF) % 4, q2 = it % NF;
+        const int dn = f >> 1, side = f & 1;
+        const int t1c = q2 % NQ, t2c = q2 / NQ;
+        double v = 0.0;
+        for (int l = 0; l < NQ; ++l) {
+            const int node = dn == 0 ? (t2c * NQ + t1c) * NQ + l : dn == 1 ? (t2c * NQ + l) * NQ + t1c
+                                                                           : (l * NQ + t2c) * NQ + t1c;
+            v += tab->phis[side][l] * sF[(dn * 4 + k) * Q3 + node];
+        }
+        g.t2[(((size_t)cell * 6 + f) * GL_T2W + 15 + k) * NF + q2] = side ? v : -v;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Residual (+ mass inverse + RK epilogue)
+// ------------------------------------------------------------------------------------
+template <int ND, int NQ, bool VISC, bool SPLIT>
+struct GlStageLayout {
+    static constexpr int NT = gl_threads<NQ>();
+    static constexpr int D3 = ND * ND * ND, Q3 = NQ * NQ * NQ, NF = NQ * NQ;
+    static constexpr int nTab = (int)(sizeof(GlTab) / sizeof(double));
+    static constexpr int oU = nTab;                       // 5 ND^3 state, later the right-hand side
+    static constexpr int oQ = oU + 5 * D3;                // 5 NQ^3 state at the flux nodes (split: projected)
+    static constexpr int oN = oQ + 5 * Q3;                // node quantities (11 NQ^3) or fluxes (15 NQ^3)
+    static constexpr int oDiv = oN + 15 * Q3;             // 5 NQ^3 volume divergence (+ hybrid volume terms)
+    static constexpr int oF = oDiv + 5 * Q3;              // 6 x 5 x NF face arrays
+    static constexpr int nT = gl_temp<ND, NQ>();
+    static constexpr int oT0 = oF + 30 * NF, oT1 = oT0 + nT;
+    static constexpr int total = oT1 + nT;
+    static constexpr size_t bytes = (size_t)total * sizeof(double);
+};
+
+template <int ND, int NQ, bool VISC, bool SPLIT>
+__global__ void __launch_bounds__(gl_threads<NQ>()) gl_stage_kernel(const StageArgs a, const GlArgs g) {
+    using L = GlStageLayout<ND, NQ, VISC, SPLIT>;
+    constexpr int NT = L::NT, D3 = L::D3, Q3 = L::Q3, NF = L::NF, T1W = gl_t1_width<SPLIT>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* sm = reinterpret_cast<double*>(smem_raw);
+    GlTab* tab = reinterpret_cast<GlTab*>(sm);
+    double* sU = sm + L::oU;
+    double* sQ = sm + L::oQ;
+    double* sN = sm + L::oN;
+    double* sDiv = sm + L::oDiv;
+    double* sF = sm + L::oF;
+    double* t0 = sm + L::oT0;
+    double* t1 = sm + L::oT1;
+    const int cell = a.cell_begin + blockIdx.x;
+    Cst<double> cst; cst.load(a.pc);
+    const int tp = a.pc.two_point, cf = a.pc.conv_flux, df = a.pc.diss_flux, ucv = a.pc.use_const_visc;
+    gl_load_tab(g.tab, tab, NT);
+    for (int i = threadIdx.x; i < 5 * D3; i += NT) sU[i] = __ldg(&a.U[(size_t)cell * 5 * D3 + i]);
+    __syncthreads();
+    gl_apply3<NT>(tab->chi, NQ, ND, sU, D3, sQ, Q3, 5, t0, t1, 1.0, false);
+    if constexpr (SPLIT) {
+        // entropy projection at the flux nodes: u = u(P (x3) v(chi u))  (strong_dg.cpp:1235-1330)
+        for (int q = threadIdx.x; q < Q3; q += NT) {
+            double u[5], v[5];
+#pragma unroll
+            for (int s = 0; s < 5; ++s) u[s] = sQ[s * Q3 + q];
+            gl_entropy_vars(u, cst.gam, cst.gm1, v, a.status);
+#pragma unroll
+            for (int s = 0; s < 5; ++s) t0[s * Q3 + q] = v[s];
+        }
+        __syncthreads();
+        gl_apply3<NT>(tab->P, NQ, NQ, t0, Q3, sQ, Q3, 5, t1, sDiv, 1.0, false);
+        for (int q = threadIdx.x; q < Q3; q += NT) {
+            double v[5], u[5];
+#pragma unroll
+            for (int s = 0; s < 5; ++s) v[s] = sQ[s * Q3 + q];
+            gl_cons_from_entropy(v, cst.gam, cst.gm1, u);
+#pragma unroll
+            for (int s = 0; s < 5; ++s) sQ[s * Q3 + q] = u[s];
+            NodeQ<double> nq;
+            node_prepare<double>(u, tp, cst.gm1, nq, a.status);
+            store_q<double>(sN, Q3, q, nq);
+        }
+        __syncthreads();
+        // two-point volume term: sum over the node's three flux-node lines of
+        // skew[x_d][l] w_a w_b F(u_i, u_l) . e_d   (operators.cpp:983-1062)
+        for (int q = threadIdx.x; q < Q3; q += NT) {
+            const int xi[3] = {q % NQ, (q / NQ) % NQ, q / NF};
+            NodeQ<double> qi;
+            load_q<double>(sN, Q3, q, qi);
+            double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+            for (int rd = 0; rd < 3; ++rd) {
+                const int ra = rd == 0 ? 1 : 0, rb = rd == 2 ? 1 : 2;
+                const double wab = tab->wq[xi[ra]] * tab->wq[xi[rb]];
+                const double nv[3] = {rd == 0 ? 1.0 : 0.0, rd == 1 ? 1.0 : 0.0, rd == 2 ? 1.0 : 0.0};
+                const int st = rd == 0 ? 1 : rd == 1 ? NQ : NF;
+                const int base = q - xi[rd] * st;
+                for (int l = 0; l < NQ; ++l) {
+                    if (l == xi[rd]) continue;
+                    NodeQ<double> qj;
+                    load_q<double>(sN, Q3, base + l * st, qj);
+                    double F[5];
+                    two_point_n<double>(qi, qj, nv, tp, cst, F);
+                    const double Qc = tab->skew[xi[rd] * NQ + l] * wab;
+#pragma unroll
+                    for (int s = 0; s < 5; ++s) acc[s] += Qc * F[s];
+                }
+            }
+#pragma unroll
+            for (int s = 0; s < 5; ++s) sDiv[s * Q3 + q] = acc[s];
+        }
+        __syncthreads();
+    } else {
+        // conservative: W div(F(chi u)) by the flux-node derivative   (strong_dg.cpp:1546)
+        for (int q = threadIdx.x; q < Q3; q += NT) {
+            double u[5];
+#pragma unroll
+            for (int s = 0; s < 5; ++s) u[s] = sQ[s * Q3 + q];
+            NodeQ<double> nq;
+            node_prepare<double>(u, TP_KG, cst.gm1, nq, a.status);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const double nv[3] = {d == 0 ? 1.0 : 0.0, d == 1 ? 1.0 : 0.0, d == 2 ? 1.0 : 0.0};
+                double F[5];
+                conv_flux_n<double>(nq, nv, 0.0, F);
+#pragma unroll
+                for (int s = 0; s < 5; ++s) sN[(d * 5 + s) * Q3 + q] = F[s];
+            }
+        }
+        __syncthreads();
+        gl_pass<NT>(tab->dphi, NQ, NQ, 0, NQ, NQ, NQ, sN, Q3, sDiv, Q3, 5, 1.0, false);
+        __syncthreads();
+        gl_pass<NT>(tab->dphi, NQ, NQ, 1, NQ, NQ, NQ, sN + 5 * Q3, Q3, sDiv, Q3, 5, 1.0, true);
+        __syncthreads();
+        gl_pass<NT>(tab->dphi, NQ, NQ, 2, NQ, NQ, NQ, sN + 10 * Q3, Q3, sDiv, Q3, 5, 1.0, true);
+        __syncthreads();
+        for (int i = threadIdx.x; i < 5 * Q3; i += NT) {
+            const int q = i % Q3;
+            sDiv[i] *= tab->wq[q % NQ] * tab->wq[(q / NQ) % NQ] * tab->wq[q / NF];
+        }
+        __syncthreads();
+    }
+
+    // ---- faces: numerical fluxes (canonical orientation: the left state is the cell whose
+    // +e_dn face it is, the normal +e_dn), and this cell's face array
+    // W_face (F_vol.n + F_v,vol.n -/+ F*_conv -/+ F*_diss) [- hybrid surface terms]
+    for (int it = threadIdx.x; it < 6 * NF; it += NT) {
+        const int f = it / NF, q2 = it % NF;
+        const int dn = f >> 1, side = f & 1;
+        const double sgn = side ? 1.0 : -1.0;
+        const int cn = __ldg(&a.nbr[cell * 6 + f]);
+        const double* to = g.t1 + ((size_t)cell * 6 + f) * T1W * NF + q2;
+        const double* te = g.t1 + ((size_t)cn * 6 + (f ^ 1)) * T1W * NF + q2;
+        double uo[5], ue[5], ro[5], re[5];
+#pragma unroll
+        for (int s = 0; s < 5; ++s) { ro[s] = __ldg(&to[s * NF]); re[s] = __ldg(&te[s * NF]); }
+        if constexpr (SPLIT) {
+            double vo[5], ve[5];
+#pragma unroll
+            for (int s = 0; s < 5; ++s) { vo[s] = __ldg(&to[(5 + s) * NF]); ve[s] = __ldg(&te[(5 + s) * NF]); }
+            gl_cons_from_entropy(vo, cst.gam, cst.gm1, uo);
+            gl_cons_from_entropy(ve, cst.gam, cst.gm1, ue);
+        } else {
+#pragma unroll
+            for (int s = 0; s < 5; ++s) { uo[s] = ro[s]; ue[s] = re[s]; }
+        }
+        const double nv[3] = {dn == 0 ? 1.0 : 0.0, dn == 1 ? 1.0 : 0.0, dn == 2 ? 1.0 : 0.0};
+        const double* uL = side ? uo : ue;
+        const double* uR = side ? ue : uo;
+        NodeQ<double> qL, qR;
+        node_prepare<double>(uL, tp, cst.gm1, qL, nullptr);
+        node_prepare<double>(uR, tp, cst.gm1, qR, nullptr);
+        double Fc[5];
+        conv_num_flux_n<double>(uL, uR, qL, qR, nv, tp, cf, cst, Fc);
+        double term[5];
+#pragma unroll
+        for (int s = 0; s < 5; ++s) term[s] = -sgn * Fc[s];
+        if constexpr (VISC) {
+            const double* ao = g.t2 + ((size_t)cell * 6 + f) * GL_T2W * NF + q2;
+            const double* ae = g.t2 + ((size_t)cn * 6 + (f ^ 1)) * GL_T2W * NF + q2;
+            double go[5][3], ge[5][3];
+#pragma unroll
+            for (int s = 0; s < 5; ++s)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) { go[s][d] = __ldg(&ao[(s * 3 + d) * NF]); ge[s][d] = __ldg(&ae[(s * 3 + d) * NF]); }
+            const double* rL = side ? ro : re;
+            const double* rR = side ? re : ro;
+            double FL[3][4], FR[3][4];
+            viscous_flux<double>(rL, side ? go : ge, ucv, cst, FL, 1 << dn, nullptr);
+            viscous_flux<double>(rR, side ? ge : go, ucv, cst, FR, 1 << dn, nullptr);
+            double Fd[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) Fd[k] = 0.5 * (FL[dn][k] + FR[dn][k]);
+            if (df == DF_SIPG) {
+                double jump[5][3];
+#pragma unroll
+                for (int s = 0; s < 5; ++s)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) jump[s][d] = d == dn ? rL[s] - rR[s] : 0.0;
+                double AL[3][4], AR[3][4];
+                viscous_flux<double>(rL, jump, ucv, cst, AL, 1 << dn, nullptr);
+                viscous_flux<double>(rR, jump, ucv, cst, AR, 1 << dn, nullptr);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) Fd[k] = Fd[k] - a.pen * (0.5 * (AL[dn][k] + AR[dn][k]));
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) term[1 + k] += -sgn * Fd[k] + __ldg(&ao[(15 + k) * NF]);
+        }
+        if constexpr (!SPLIT) {   // the cell's own convective volume flux at the face: n . sum_l phi_l F(u_l)
+            const int t1c = q2 % NQ, t2c = q2 / NQ;
+#pragma unroll
+            for (int s = 0; s < 5; ++s) {
+                double v = 0.0;
+                for (int l = 0; l < NQ; ++l) {
+                    const int node = dn == 0 ? (t2c * NQ + t1c) * NQ + l : dn == 1 ? (t2c * NQ + l) * NQ + t1c
+                                                                                   : (l * NQ + t2c) * NQ + t1c;
+                    v += tab->phis[side][l] * sN[(dn * 5 + s) * Q3 + node];
+                }
+                term[s] += sgn * v;
+            }
+        }
+        const double wf = tab->wq[q2 % NQ] * tab->wq[q2 / NQ];
+#pragma unroll
+        for (int s = 0; s < 5; ++s) sF[(f * 5 + s) * NF + q2] = wf * term[s];
+    }
+    __syncthreads();
+    if constexpr (SPLIT) {
+        // hybrid surface-volume two-point terms (strong_dg.cpp:3144-3350): between each face node
+        // (its projected state) and the flux nodes of the normal line through it; one face at a
+        // time, since the faces of one direction share the volume nodes
+        for (int f = 0; f < 6; ++f) {
+            const int dn = f >> 1, side = f & 1;
+            const double sgn = side ? 1.0 : -1.0;
+            const double nv[3] = {dn == 0 ? 1.0 : 0.0, dn == 1 ? 1.0 : 0.0, dn == 2 ? 1.0 : 0.0};
+            for (int q2 = threadIdx.x; q2 < NF; q2 += NT) {
+                const double* to = g.t1 + ((size_t)cell * 6 + f) * T1W * NF + q2;
+                double vo[5], uf[5];
+#pragma unroll
+                for (int s = 0; s < 5; ++s) vo[s] = __ldg(&to[(5 + s) * NF]);
+                gl_cons_from_entropy(vo, cst.gam, cst.gm1, uf);
+                NodeQ<double> qf;
+                node_prepare<double>(uf, tp, cst.gm1, qf, nullptr);
+                const int t1c = q2 % NQ, t2c = q2 / NQ;
+                const double wf = tab->wq[t1c] * tab->wq[t2c];
+                double hs[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+                for (int l = 0; l < NQ; ++l) {
+                    const int node = dn == 0 ? (t2c * NQ + t1c) * NQ + l : dn == 1 ? (t2c * NQ + l) * NQ + t1c
+                                                                                   : (l * NQ + t2c) * NQ + t1c;
+                    NodeQ<double> qv;
+                    load_q<double>(sN, Q3, node, qv);
+                    double F[5];
+                    two_point_n<double>(qv, qf, nv, tp, cst, F);
+                    const double Hop = tab->phis[side][l] * wf * sgn;
+#pragma unroll
+                    for (int s = 0; s < 5; ++s) {
+                        hs[s] -= Hop * F[s];
+                        sDiv[s * Q3 + node] += Hop * F[s];
+                    }
+                }
+#pragma unroll
+                for (int s = 0; s < 5; ++s) sF[(f * 5 + s) * NF + q2] -= hs[s];
+            }
+            __syncthreads();
+        }
+    }
+    // ---- assembly: r = -chi^T (x3) [div (+ hybrid)] + sum_f lift(face array) (+ viscous volume)
+    gl_apply3T<NT>(tab->chi, ND, NQ, sDiv, Q3, sU, D3, 5, t0, t1, -1.0, false);
+    gl_lift_faces<NT>(sF, 5 * NF, NF, 5, NQ, ND, tab->chis[0], tab->chis[1], tab->chi, t0, t1, sU, D3, 0, 1.0);
+    if constexpr (VISC) {
+        for (int i = threadIdx.x; i < 4 * D3; i += NT) sU[D3 + i] += __ldg(&g.vis[(size_t)cell * 4 * D3 + i]);
+        __syncthreads();
+    }
+    // sU = R / h^2 (the affine metric C = h^2 I and J = h^2 factored out)
+    if (a.mode == 0) {
+        const double h2 = a.h * a.h;
+        for (int i = threadIdx.x; i < 5 * D3; i += NT) a.out[(size_t)cell * 5 * D3 + i] = h2 * sU[i];
+        return;
+    }
+    // k = M^-1 R = (1/h) (M+K)^-1 (x3) (R / h^2)
+    gl_apply3<NT>(tab->minv, ND, ND, sU, D3, sQ, D3, 5, t0, t1, a.inv_h, false);
+    if (a.mode == 1) {
+        for (int i = threadIdx.x; i < 5 * D3; i += NT) a.out[(size_t)cell * 5 * D3 + i] = sQ[i];
+        return;
+    }
+    // Butcher RK stage (as the collocated kernel's epilogue)
+    for (int i = threadIdx.x; i < 5 * D3; i += NT) {
+        const size_t dof = (size_t)cell * 5 * D3 + i;
+        const double k = sQ[i];
+        const double un = a.Un[dof];
+        const double bs = a.acc_in ? a.acc_in[dof] : (a.inc_mode ? 0.0 : un);
+        const double sum = bs + a.c_acc * k;
+        if (a.acc_out) a.acc_out[dof] = sum;
+        if (a.final_out) a.final_out[dof] = a.inc_mode ? un + sum : sum;
+        if (a.next) {
+            const double cin = a.carry_in ? a.carry_in[dof] : 0.0;
+            a.next[dof] = (cin + a.a_next * k) * a.dt + un;
+        }
+        if (a.carry_out) a.carry_out[dof] = a.a_carry * k;
+    }
+}
+
+} // namespace ph

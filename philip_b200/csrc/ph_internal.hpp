@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/philip_b200.h"
+#include "ph_gl.cuh"
 #include "ph_integrals.cuh"
 #include "ph_kernels.cuh"
 
@@ -24,7 +25,13 @@ int check_param_ranges(const ph_params* prm);
 
 // Configuration checks shared by every entry point that builds a discretisation;
 // returns nullptr when the configuration is on the GPU path, else the reason.
+// unsupported_reason: the collocated kernels (GLL flux nodes, no overintegration);
+// uncollocated_reason: a context on GL flux nodes or with overintegration.
 const char* unsupported_reason(const ph_mesh_desc* mesh, const ph_params* prm);
+bool uncollocated(const ph_params* prm);
+const char* uncollocated_reason(const ph_mesh_desc* mesh, const ph_params* prm);
+// 1-D operators of the uncollocated path; also sets ops.Minv to its FR mass inverse
+int build_gl_operators(const ph_params* prm, ph::GlTab& t, ph::OpTab& ops);
 
 // 1-D operators on the GLL nodes: D, skew D, FR mass inverse (M+K)^-1 and B = (M+K)^-1 W.
 // x, D are the nodes and derivative matrix (N1 and N1 x N1). Returns PH_OK or an error.

@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include "ph_kernels.cuh"
+#include "ph_gl.cuh"
 #include "ph_integrals.cuh"
 
 namespace ph {
@@ -39,6 +40,12 @@ cudaError_t launch_stage_batched(const StageArgs* inst, const BatchTile* tiles, 
 // CTAs per SM; returns false when the variant does not exist
 template <int N1>
 bool batched_shape(int fp32, bool curv, int variant, int* cpc, int* threads, size_t* smem, int* ctas_per_sm);
+// Uncollocated path (GL flux nodes / overintegration), N1 = p + 1 solution nodes and nq flux
+// nodes per direction (N1 <= nq <= min(N1 + 2, 7)): kernel 0 = face values (gl_trace_kernel),
+// 1 = auxiliary equation and viscous terms (gl_aux_kernel), 2 = residual / RK stage
+// (gl_stage_kernel); one CTA per cell of [a.cell_begin, a.nc).
+template <int N1>
+cudaError_t launch_gl(int kernel, int nq, const StageArgs& a, const GlArgs& g, bool visc, bool split, cudaStream_t s);
 // shared memory and threads of the residual kernel (for reporting / tests)
 template <int N1>
 void stage_launch_shape(int fp32, bool visc, bool split, int* threads, int* cells_per_cta, size_t* smem);

@@ -40,7 +40,14 @@ def _create(prm_kw=None, mesh_kw=None, edit=None):
 
 
 REFUSED = [
-    ("gl_flux_nodes", lambda p: setattr(p, "flux_nodes_type", 0), _lib.PH_ERR_UNSUPPORTED, "GLL"),
+    ("gl_flux_nodes_precision_form", lambda p: (setattr(p, "flux_nodes_type", 0), setattr(p, "precision", 1)),
+     _lib.PH_ERR_UNSUPPORTED, "FP64"),
+    ("gl_flux_nodes_low_storage_rk", lambda p: (setattr(p, "flux_nodes_type", 0), setattr(p, "runge_kutta_method", 7)),
+     _lib.PH_ERR_UNSUPPORTED, "Butcher"),
+    ("overintegration_3", lambda p: setattr(p, "overintegration", 3), _lib.PH_ERR_UNSUPPORTED, "overintegration"),
+    ("gl_flux_nodes_p6_overintegration", lambda p: (setattr(p, "flux_nodes_type", 0), setattr(p, "poly_degree", 6),
+                                                    setattr(p, "overintegration", 1)),
+     _lib.PH_ERR_UNSUPPORTED, "<= 7"),
     ("degree_7", lambda p: setattr(p, "poly_degree", 7), _lib.PH_ERR_UNSUPPORTED, "poly_degree"),
     ("implicit_rk", lambda p: setattr(p, "runge_kutta_method", 4), _lib.PH_ERR_INVALID, "out of range"),
     ("ec_flux_without_split_form", lambda p: (setattr(p, "use_split_form", 0), setattr(p, "conv_num_flux", 3)),
@@ -64,6 +71,25 @@ def test_configurations_outside_the_path_are_refused(name, edit, code, text):
 def test_curvilinear_navier_stokes_is_refused():
     rc, msg = _create(prm_kw=dict(pde="navier_stokes"), mesh_kw=dict(warp=0.1))
     assert rc == _lib.PH_ERR_UNSUPPORTED and "Euler" in msg
+
+
+def test_curvilinear_gl_flux_nodes_are_refused():
+    rc, msg = _create(mesh_kw=dict(warp=0.1), edit=lambda p: setattr(p, "flux_nodes_type", 0))
+    assert rc == _lib.PH_ERR_UNSUPPORTED and "affine" in msg
+
+
+def test_entry_points_without_contexts_refuse_gl_flux_nodes():
+    """The batch, the server and the no-allocation residual run the collocated kernels only."""
+    L = _lib.load()
+    prm = Parameters.from_dict(prm_dict())
+    p = prm.to_ph_params()
+    p.flux_nodes_type = 0
+    m = _lib.PhMeshDesc(prm.n_cells, 0, *prm.grid_bounds)
+    dummy = ctypes.c_void_p(16)
+    assert L.ph_residual_noalloc(ctypes.byref(m), ctypes.byref(p), dummy, dummy, None) == _lib.PH_ERR_UNSUPPORTED
+    nbytes = ctypes.c_size_t()
+    assert L.ph_batch_bytes(ctypes.byref(m), ctypes.byref(p), ctypes.byref(nbytes)) == _lib.PH_ERR_UNSUPPORTED
+    assert b"collocated" in L.ph_last_error()
 
 
 BAD_MESHES = [

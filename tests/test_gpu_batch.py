@@ -150,6 +150,35 @@ def test_served_mix_and_vortex_error():
         assert _same_as_single(c.state, _alone(c.request, prec)[0], prec)
 
 
+@pytest.mark.parametrize("p", [2, 3])
+def test_batched_vortex_converges_at_the_design_order(p):
+    """h-refinement of the translated isentropic vortex in one FP64 batch (all meshes together):
+    the RMS nodal error against the exact solution falls by at least 2^(p + 1/2) per halving of
+    the cell size (DG of degree p on a smooth solution: order p + 1, here measured between the
+    two finest meshes), so a wrong-but-stable solve fails."""
+    prec = _lib.PH_FP64
+    ns = [6, 12, 24]
+    reqs = [SolveRequest("isentropic_vortex", n_cells=n, poly_degree=p, mach=0.3, beta=3.0,
+                         direction=(0.6, 0.8, 0.0), final_time=0.5, cfl=0.05) for n in ns]
+    b = Batch(4 << 30, prec)
+    slots = []
+    for r in reqs:
+        U0 = r.initial_state()
+        dt, nsteps = r.time_step(U0)
+        slots.append(b.admit(r.mesh(), r.parameters().to_ph_params(prec), U0, dt, nsteps))
+    b.step(10 ** 6)
+    errs = []
+    for r, s in zip(reqs, slots):
+        U = b.state(s, r.ndofs)
+        ex = r.exact_state()
+        errs.append(float(np.sqrt(np.mean((U - ex) ** 2)) / np.sqrt(np.mean(ex ** 2))))
+    b.close()
+    orders = [np.log2(errs[i] / errs[i + 1]) for i in range(len(ns) - 1)]
+    print(f"p={p}: RMS errors {['%.3e' % e for e in errs]}, observed orders {['%.2f' % o for o in orders]}")
+    assert orders[-1] >= p + 0.5
+    assert all(e2 < e1 for e1, e2 in zip(errs, errs[1:]))
+
+
 def test_autotuner_picks_a_variant():
     best, ms = autotune(3, _lib.PH_FP32_RESIDUAL, False)
     print("p=3 variants ms:", ms, "best", best)
