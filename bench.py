@@ -91,18 +91,37 @@ def bytes_per_dof_stage(viscous: bool, p: int = 5) -> dict:
     return {"stage": stage, "aux": aux}
 
 
-def flops_per_dof_stage(p: int, viscous: bool) -> float:
-    """Algorithmic FP64 operations per DOF per stage (counted from the kernel source:
-    add/mul/fma = 1, divide = 1, sqrt = 1, log = 1). Two-point fluxes with pair symmetry:
-    1.5 (n1 - 1) unique CH pairs per node at ~46 ops each, plus per-node preparation
-    (~30 ops + 2 logs), the face numerical flux (Roe, ~170 ops per face node, evaluated by
-    both neighbours: 6 n1^2 per cell) and the viscous terms (~150 ops per node for the
-    flux, 2 x 3 x n1 x 4 FMA for its divergence and 3 x n1 x 5 for the gradient)."""
+def flops_per_dof_stage(p: int, viscous: bool) -> dict:
+    """Algorithmic FP64 operations per DOF of one stage-kernel launch (Chandrashekar split form,
+    EC + Roe faces, BR2 when viscous, classical RK4 epilogue), counted from the kernel source:
+    add / mul = 1, fma = 2, division / square root / logarithm = 1 each. Each unordered pair of
+    nodes on a line is counted once (1.5 (n1 - 1) pair fluxes per node; the skew operator's
+    diagonal is zero, operators.cpp:1466-1476) and each face once (3 n1^2 face nodes per cell).
+    The viscous flux, gradient and divergence belong to the auxiliary kernel, not to this one.
+      pair flux (Chandrashekar means, momentum and energy fluxes) ........ 56
+      its accumulation into both nodes (2 x 5 fma) ........................ 20
+      node quantities (velocity, pressure, beta, two logarithms) .......... 22
+      face node: EC flux 56 + Roe-Pike dissipation with Harten's fix 118 +
+        the neighbour's node quantities 22 + lift 10 (+ BR2 average 20) .. 206 (226)
+      epilogue: face terms, 1/h, RK4 running sum and next stage input .... 45 per node
+    """
     n1 = p + 1
-    per_node = 1.5 * (n1 - 1) * 46 + 32 + 6.0 * n1 * n1 * 170 / n1 ** 3 + 5 * 3 * 2 * n1
-    if viscous:
-        per_node += 150 + 2 * 3 * n1 * 4 + 3 * n1 * 5 + 6.0 * n1 * n1 * 2 * 150 / n1 ** 3
-    return per_node / 5.0
+    pair = 56 + 20
+    face_node = 206 + (20 if viscous else 0)
+    per_node = 1.5 * (n1 - 1) * pair + 22 + 3.0 * n1 * n1 * face_node / n1 ** 3 + 45
+    return {"per_dof": per_node / 5.0, "pair_flux": pair, "face_node": face_node,
+            "rule": "add/mul 1, fma 2, div/sqrt/log 1; each node pair and each face once"}
+
+
+def measured_fp64_mix(p: int, viscous: bool, precision: str):
+    """Executed FP64 operations and FP64-pipe activity of the stage kernel from an ncu capture
+    (profiles/fp64_mix.json), or None."""
+    path = os.path.join(ROOT, "profiles", "fp64_mix.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    return d.get(f"residual_kernel/{'navier_stokes' if viscous else 'euler'}/p{p}/{precision}")
 
 
 class ClockSampler:
@@ -191,18 +210,21 @@ def measured_peaks():
     return 6650.0, "fallback 6.65 TB/s"
 
 
-def fp64_dgemm_peak(torch):
-    """Measured FP64 denominator: cuBLAS DGEMM 8192^3 (2 N^3 flops), best of 3, CUDA events.
-    Run outside the timed region."""
+def gemm_peak(torch, dtype):
+    """Measured FP64 (or FP32, TF32 off) denominator: a cuBLAS GEMM 8192^3 (2 N^3 flops), best of
+    3, CUDA events. Run outside the timed region."""
     n = 8192
-    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
-    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    tf32 = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    a = torch.randn(n, n, dtype=dtype, device="cuda")
+    b = torch.randn(n, n, dtype=dtype, device="cuda")
     c = a @ b
     best = float("inf")
     for _ in range(3):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(); torch.matmul(a, b, out=c); e1.record(); torch.cuda.synchronize()
         best = min(best, e0.elapsed_time(e1))
+    torch.backends.cuda.matmul.allow_tf32 = tf32
     del a, b, c
     torch.cuda.empty_cache()
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
@@ -469,9 +491,10 @@ def run_precision_check(args, rank: int = 0, world: int = 1, local_rank: int = 0
     over t in [0, t_final] (default 5): both forms take the same constant time step (the
     adaptive formula evaluated once at t=0) and record kinetic energy and enstrophy every 10
     steps on the device (ph_run). Reports the relative max errors of the kinetic-energy
-    dissipation rate -dKE/dt (central differences of the KE rows), of the vorticity-based
-    dissipation rate 2 enstrophy / Re and of the KE itself, and the two forms' rates with the
-    rows included. Independent replicas on every rank (no exchange)."""
+    dissipation rate -dKE/dt (from each recorded state and its time derivative M^-1 R(u), on
+    the device; also by central differences of the KE rows, which amplify the rows' rounding),
+    of the vorticity-based dissipation rate 2 enstrophy / Re and of the KE itself, and the two
+    forms' rates with the rows included. Independent replicas on every rank (no exchange)."""
     import torch
     from philip_b200 import _lib
     from philip_b200.dg import FlowSolver
@@ -487,7 +510,7 @@ def run_precision_check(args, rank: int = 0, world: int = 1, local_rank: int = 0
         fs = FlowSolver(prm, precision=prec, stream=stream.cuda_stream)
         if dt is None:
             dt = fs.adaptive_time_step()
-        nsteps = int(round(t_final / dt))
+        nsteps = int(round(t_final / dt)) // record_every * record_every
         q0 = fs.dg.integrals()
         torch.cuda.synchronize()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -495,9 +518,19 @@ def run_precision_check(args, rank: int = 0, world: int = 1, local_rank: int = 0
         rows = fs.ode_solver.step_in_time_with_records(dt, nsteps, record_every)
         ev1.record(stream)
         torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        status = fs.dg.status()
+        del fs
+        # the same steps again, with -dKE/dt from each recorded state's time derivative
+        # M^-1 R(u) on the device (ph_kinetic_energy_rate) after every record interval
+        fs = FlowSolver(prm, precision=prec, stream=stream.cuda_stream)
+        rates = [-fs.dg.kinetic_energy_rate()]
+        for _ in range(nsteps // record_every):
+            fs.ode_solver.step_in_time_with_records(dt, record_every, record_every)
+            rates.append(-fs.dg.kinetic_energy_rate())
         out[name] = dict(t=np.array([0.0] + [r[0] for r in rows]), ke=np.array([q0[0]] + [r[1] for r in rows]),
-                         eps_w=np.array([q0[2]] + [r[3] for r in rows]), ms=ev0.elapsed_time(ev1),
-                         nsteps=nsteps, status=fs.dg.status(), ndofs=fs.dg.n_dofs)
+                         eps_w=np.array([q0[2]] + [r[3] for r in rows]), ms=ms, rate=np.array(rates),
+                         nsteps=nsteps, status=status, ndofs=fs.dg.n_dofs)
         del fs
         torch.cuda.empty_cache()
     a, b = out["fp64"], out["fp32"]
@@ -514,12 +547,13 @@ def run_precision_check(args, rank: int = 0, world: int = 1, local_rank: int = 0
     if rank == 0:
         line = {
             "metric": "KE-dissipation-rate rel error, precision form vs FP64 (viscous TGV 32^3 p3)",
-            "value": rel(dke_a, dke_b), "unit": "relative max error", "higher_is_better": False,
+            "value": rel(a["rate"], b["rate"]), "unit": "relative max error", "higher_is_better": False,
             "n_gpus": world, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32-residual/f64-state vs f64", "data": "synthetic (Taylor-Green initial condition)",
             "config": {"workload": PRECISION_CHECK, "t_final": t_final, "dt": dt, "steps": a["nsteps"],
                        "record_every": record_every, "rows": len(a["t"]) - 1},
-            "errors": {"ke_dissipation_rate_minus_dKE_dt": rel(dke_a, dke_b),
+            "errors": {"ke_dissipation_rate_minus_dKE_dt": rel(a["rate"], b["rate"]),
+                       "ke_dissipation_rate_by_central_differences_of_rows": rel(dke_a, dke_b),
                        "vorticity_dissipation_rate_2_enstrophy_over_Re": rel(a["eps_w"], b["eps_w"]),
                        "kinetic_energy": rel(a["ke"], b["ke"])},
             "rates_with_rows": {"fp64": rate(a), "fp32": rate(b), "ratio": rate(b) / rate(a),
@@ -699,11 +733,13 @@ def main():
         if args.precision == "fp32":
             pass   # the state stays FP64, so the stage bytes are the same (+8 B/DOF Kahan term at the last stage)
         bytes_launch = bpd["stage"] * dg.n_dofs
-        achieved = bytes_launch / (stage_ms * 1e-3) / 1e9
+        achieved_gbs = bytes_launch / (stage_ms * 1e-3) / 1e9
         traffic = ncu_traffic(p, viscous, args.precision, dg.n_dofs)
-        flops_dof = flops_per_dof_stage(p, viscous)
-        fp64_tflops = flops_dof * dg.n_dofs / (stage_ms * 1e-3) / 1e12
-        dgemm_tflops = fp64_dgemm_peak(torch)
+        flops = flops_per_dof_stage(p, viscous)
+        alg_tflops = flops["per_dof"] * dg.n_dofs / (stage_ms * 1e-3) / 1e12
+        fp32 = args.precision == "fp32"
+        gemm_tflops = gemm_peak(torch, torch.float32 if fp32 else torch.float64)
+        mix = measured_fp64_mix(p, viscous, args.precision)
         line = {
             "metric": "TGV DOF-updates/s/stage", "value": value, "unit": "DOF-updates/s/stage",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -725,18 +761,23 @@ def main():
                                "path": "ph_run: the same steps with kinetic energy, enstrophy, dissipation rate "
                                        "and wave speed reduced on the device every 10 steps"}
             if not slab else {"skipped": "slab contexts step through ph_rk_step"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak,
+            # the binding roof of the stage kernel is its floating-point pipe (arithmetic intensity
+            # above the HBM ridge); the HBM figures are kept beside it
+            "roofline": {"bound": "fp32" if fp32 else "fp64", "achieved": alg_tflops, "peak": gemm_tflops,
+                         "unit": "TFLOP/s", "frac": alg_tflops / gemm_tflops,
                          "traffic": traffic["bytes_per_launch"] if traffic else None,   # DRAM bytes per launch
                          "traffic_detail": traffic,
                          "kernel": "residual_kernel (stage: residual + mass inverse + RK update)",
                          "kernel_ms": stage_ms, "aux_kernel_ms": aux_ms,
-                         "alg_bytes_per_dof": bpd, "peak_source": peak_src,
-                         "fp64": {"alg_flops_per_dof_stage": flops_dof, "achieved_tflops": fp64_tflops,
-                                  "peak_tflops": dgemm_tflops, "frac": fp64_tflops / dgemm_tflops,
-                                  "peak_source": "measured here: cuBLAS DGEMM 8192^3, best of 3"
-                                                 + ("" if args.precision == "fp64" else
-                                                    " (the precision form computes its fluxes in FP32)")}},
+                         "kernel_ms_source": "mean over the timed steps: CUDA events recorded by graph nodes "
+                                             "around each kernel of every replayed RK step (ph_set_timing mode 2)"
+                                             if not slab else "per-launch CUDA events after the timed steps",
+                         "alg_flops_per_dof": flops,
+                         "peak_source": ("measured here: cuBLAS " + ("SGEMM (TF32 off)" if fp32 else "DGEMM")
+                                         + " 8192^3, best of 3; MEASURED_PEAKS.json holds no FP64/FP32 figure"),
+                         "executed": mix,
+                         "hbm": {"achieved": achieved_gbs, "peak": peak, "unit": "GB/s", "frac": achieved_gbs / peak,
+                                 "alg_bytes_per_dof": bpd, "peak_source": peak_src}},
             "clocks": clk.summary(),
         }
         if world == 1 and not args.no_cpu_baseline:

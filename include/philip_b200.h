@@ -90,6 +90,14 @@ typedef struct ph_params {
      * in FP64, two-point fluxes other than KG. */
     int use_relaxation_runge_kutta;
     double relaxation_runge_kutta_root_tolerance;
+    /* limiter/bound_preserving_limiter (src/parameters/parameters_limiter.cpp:17-30):
+     * 0 none, 1 maximum_principle (scalar equations: not on this path),
+     * 2 positivity_preservingZhang2010, 3 positivity_preservingWang2012; and limiter/min_density.
+     * A positivity limiter is applied to every RK stage solution and to the new solution
+     * (Butcher methods), and with it the non-physical replacement of negative densities and
+     * pressures is off, as in the reference (Euler::check_positive_quantity). */
+    int bound_preserving_limiter;
+    double min_density;
 } ph_params;
 
 /* Periodic cube [left,right]^3 with n^3 cells (PeriodicCubeFlow::generate_grid,
@@ -204,8 +212,22 @@ int ph_integrated_quantities(ph_ctx* ctx, double out[PH_N_INTEGRATED_QUANTITIES]
 int ph_run(ph_ctx* ctx, double dt, int nsteps, int record_every, double* rows);
 
 /* Status word: bit 0 = a negative density or pressure was met (Euler::check_positive_quantity,
- * src/physics/euler.cpp:155-172). Reading clears it. */
+ * src/physics/euler.cpp:155-172); bit 1 = a bulk copy into shared memory did not complete within
+ * a kernel's wait limit (that launch's outputs were not written). Reading clears it. */
 int ph_status(ph_ctx* ctx, uint32_t* flags);
+
+/* Rate of change of the volume-averaged kinetic energy at the current solution,
+ * dKE/dt = (1/|Omega|) integral of (v . dm/dt - |v|^2/2 drho/dt) with dU/dt = M^-1 R(U) evaluated
+ * by the residual kernel of the context's precision and the QGauss(p+11) cubature of the kinetic
+ * energy (periodic_turbulence.cpp:439-672). No counterpart in the reference, whose dissipation
+ * rates come from the enstrophy and strain integrals; this one measures the precision form's
+ * kinetic-energy dissipation directly. Whole affine meshes. Synchronises the context stream. */
+int ph_kinetic_energy_rate(ph_ctx* ctx, double* out);
+
+/* PositivityPreservingLimiter::limit (src/limiter/positivity_preserving_limiter.cpp:381-678) on the
+ * context's solution for a stage of time step dt, as set_initial_condition.cpp:56 applies it to
+ * an initial condition. Requires bound_preserving_limiter 2 or 3. */
+int ph_limit(ph_ctx* ctx, double dt);
 
 /* Measurement hooks (no counterpart in the reference, which times with dealii::Timer,
  * src/flow_solver/flow_solver.cpp:690-711). enable = 1: every kernel launch is bracketed

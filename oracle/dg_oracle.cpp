@@ -279,6 +279,9 @@ struct Physics {
         temp_ratio = 110.4 / p->temperature_inf;     // navier_stokes.cpp:50-52
     }
     double positive(double q) const {   // euler.cpp:155-172 + physics.cpp:298-317
+        // with a positivity-preserving limiter selected the check passes every value through
+        // unchanged (check_positive_quantity, euler.cpp:153-172)
+        if (prm->limiter == PPL_ZHANG2010 || prm->limiter == PPL_WANG2012) return q;
         if (q < 0.0) {
             if (status) __atomic_fetch_or(status, 1, __ATOMIC_RELAXED);
             if (prm->non_physical == ABORT_RUN) { std::fprintf(stderr, "oracle: non-physical state\n"); std::abort(); }
@@ -1211,6 +1214,176 @@ void Solver::apply_inverse_mass(const double* in, double* out, bool aux_eq) {
 }
 
 // ---------------------------------------------------------------------------------
+// Positivity-preserving limiter (PositivityPreservingLimiter, limiter/positivity_preserving_limiter.cpp),
+// restated with its index behaviour: the solution is interpolated to three mixed point sets
+// (GLL along direction d, GL along the other two; the sum-factorised interpolation applies its
+// first operator along x, operators.cpp:355-395), and each directional "cell average" loops
+// over GLL/GL weights with an unbraced innermost loop, so its point index advances once per
+// (i, j) pair: the average of set d sums the first n^2 points only (the z = 0 plane), with the
+// weight of the loop's i on y and of its j on x (:264-298). The averages are combined with the
+// wave-speed weights of Zhang & Shu (:300-345).
+// ---------------------------------------------------------------------------------
+namespace {
+
+// Smallest-modulus root of s3 + s2 t + s1 t^2, real part (Eigen::PolynomialSolver<double,2>
+// smallestRoot().real(), as get_theta2_Zhang2010 takes it, :95-98)
+double smallest_root_real(double s3, double s2, double s1) {
+    if (s1 == 0.0) return -s3 / s2;
+    const double disc = s2 * s2 - 4.0 * s1 * s3;
+    if (disc < 0.0) return -s2 / (2.0 * s1);      // complex pair: equal moduli, same real part
+    const double q = -0.5 * (s2 + (s2 >= 0.0 ? std::sqrt(disc) : -std::sqrt(disc)));
+    const double r1 = q / s1, r2 = (q != 0.0) ? s3 / q : r1;
+    return std::fabs(r1) <= std::fabs(r2) ? r1 : r2;
+}
+
+}  // namespace
+
+void Solver::limit(double* U, double dt) {
+    if (prm.limiter != PPL_ZHANG2010 && prm.limiter != PPL_WANG2012) return;
+    const int n = ops.nd, n3 = n * n * n;
+    std::vector<double> xgl, wgl, xgll, wgll;
+    gauss_legendre(n, xgl, wgl);
+    gauss_lobatto(n, xgll, wgll);
+    std::vector<double> Bgl((size_t)n * n), Bgll((size_t)n * n);   // FE_DGQ basis at the GL / GLL points
+    for (int q = 0; q < n; ++q) {
+        lagrange_eval(ops.xs, xgl[q], &Bgl[q * n], nullptr);
+        lagrange_eval(ops.xs, xgll[q], &Bgll[q * n], nullptr);
+    }
+    const double dx = mesh.h;   // (right - left) / cells, the same in every direction
+    const double lam = dt / dx;
+    const double gam = prm.gamma, gm1 = gam - 1.0;
+    auto pressure = [&](const double* u) {   // compute_pressure, no non-physical replacement here
+        const double rho = u[0];
+        double v2 = 0.0;
+        for (int d = 0; d < 3; ++d) { const double v = u[1 + d] / rho; v2 = v2 + v * v; }
+        return gm1 * (u[4] - 0.5 * rho * v2);
+    };
+    auto max_eig = [&](const double* u) {   // max_convective_eigenvalue (euler.cpp:1034-1046)
+        double v2 = 0.0;
+        for (int d = 0; d < 3; ++d) { const double v = u[1 + d] / u[0]; v2 += v * v; }
+        return std::sqrt(v2) + std::sqrt(pressure(u) * gam / u[0]);
+    };
+    const bool zhang = prm.limiter == PPL_ZHANG2010;
+    const double lower = prm.min_density;
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < mesh.nc; ++c) {
+        double* Uc = U + (size_t)c * ndofs_cell;
+        std::vector<double> coeff(Uc, Uc + ndofs_cell);
+        bool nan = false;
+        for (double v : coeff) nan |= std::isnan(v);
+        if (nan) continue;   // the reference aborts here (:430-442)
+        // the three mixed point sets: q[d][s][n3]
+        std::vector<double> q[3];
+        auto interp = [&](int d, int s) {
+            const double* A[3] = {d == 0 ? Bgll.data() : Bgl.data(), d == 1 ? Bgll.data() : Bgl.data(),
+                                  d == 2 ? Bgll.data() : Bgl.data()};
+            apply3(A[0], n, n, A[1], n, n, A[2], n, n, &coeff[(size_t)s * n3], &q[d][(size_t)s * n3], false, 1.0);
+        };
+        for (int d = 0; d < 3; ++d) { q[d].assign((size_t)NSTATE * n3, 0.0); for (int s = 0; s < NSTATE; ++s) interp(d, s); }
+        double min_rho = 1e6;
+        for (int d = 0; d < 3; ++d)
+            for (int i = 0; i < n3; ++i) {
+                if (coeff[i] < min_rho) min_rho = coeff[i];
+                if (q[d][i] < min_rho) min_rho = q[d][i];
+            }
+        // directional averages with the reference's point indexing (see above)
+        double avg_dim[3][NSTATE] = {};
+        for (int s = 0; s < NSTATE; ++s) {
+            int qp = 0;
+            for (int i = 0; i < n; ++i) for (int j = 0; j < n; ++j) {
+                for (int k = 0; k < n; ++k) avg_dim[0][s] += wgll[i] * wgl[j] * wgl[k] * q[0][(size_t)s * n3 + qp];
+                qp++;
+            }
+            qp = 0;
+            for (int i = 0; i < n; ++i) for (int j = 0; j < n; ++j) {
+                for (int k = 0; k < n; ++k) avg_dim[1][s] += wgl[i] * wgll[j] * wgl[k] * q[1][(size_t)s * n3 + qp];
+                qp++;
+            }
+            qp = 0;
+            for (int i = 0; i < n; ++i) for (int j = 0; j < n; ++j) {
+                for (int k = 0; k < n; ++k) avg_dim[2][s] += wgl[i] * wgl[j] * wgll[k] * q[2][(size_t)s * n3 + qp];
+                qp++;
+            }
+        }
+        double ws[3] = {0.0, 0.0, 0.0};
+        for (int i = 0; i < n3; ++i)
+            for (int d = 0; d < 3; ++d) {
+                double u[NSTATE];
+                for (int s = 0; s < NSTATE; ++s) u[s] = q[d][(size_t)s * n3 + i];
+                const double w = max_eig(u);
+                if (w > ws[d]) ws[d] = w;
+            }
+        const double mu = ws[0] * lam + ws[1] * lam + ws[2] * lam;
+        const double aw[3] = {(ws[0] * lam) / mu, (ws[1] * lam) / mu, (ws[2] * lam) / mu};
+        double avg[NSTATE];
+        for (int s = 0; s < NSTATE; ++s) {
+            avg[s] = aw[0] * avg_dim[0][s] + aw[1] * avg_dim[1][s];
+            avg[s] += aw[2] * avg_dim[2][s];
+        }
+        const double p_avg = pressure(avg);
+        // get_density_scaling_value (:170-186)
+        double eps = std::min({lower, avg[0], p_avg});
+        if (eps < 0) eps = lower;
+        double theta = 1.0;
+        if (avg[0] - min_rho > 1e-13)
+            theta = (avg[0] - min_rho == 0) ? 1.0 : std::min((avg[0] - eps) / (avg[0] - min_rho), 1.0);
+        if (theta < 0 || theta > 1) theta = 0;
+        for (int i = 0; i < n3; ++i) coeff[i] = theta * (coeff[i] - avg[0]) + avg[0];
+        for (int d = 0; d < 3; ++d) interp(d, 0);
+        if (!zhang) {   // Wang 2012 (:597-618)
+            auto theta2_of = [&](const double* base) {
+                double th = 1.0;
+                for (int i = 0; i < n3; ++i) {
+                    double u[NSTATE];
+                    for (int s = 0; s < NSTATE; ++s) u[s] = base[(size_t)s * n3 + i];
+                    const double pl = pressure(u);
+                    const double t2 = (pl >= 0) ? 1.0 : p_avg / (p_avg - pl);
+                    if (t2 != 1 && t2 >= 0 && t2 <= 1 && t2 < th) th = t2;
+                }
+                return th;
+            };
+            double theta2 = 1.0;
+            for (int d = 0; d < 3; ++d) theta2 = std::min(theta2, theta2_of(q[d].data()));
+            const double t_soln = theta2_of(coeff.data());
+            if (t_soln < theta2) theta2 = t_soln;
+            for (int s = 0; s < NSTATE; ++s)
+                for (int i = 0; i < n3; ++i) coeff[(size_t)s * n3 + i] = theta2 * (coeff[(size_t)s * n3 + i] - avg[s]) + avg[s];
+        } else {   // Zhang 2010 (:620-668); gamma 1.4 as the reference passes it
+            auto theta2_of = [&](const double* base, double* out) {
+                const double e = lower / 1.4;
+                for (int i = 0; i < n3; ++i) {
+                    double u[NSTATE];
+                    for (int s = 0; s < NSTATE; ++s) u[s] = base[(size_t)s * n3 + i];
+                    if (pressure(u) >= lower) { out[i] = 1.0; continue; }
+                    double s1 = (u[4] - avg[4]) * (u[0] - avg[0]) - 0.5 * std::pow(u[1] - avg[1], 2);
+                    double s2 = avg[0] * (u[4] - avg[4]) + avg[4] * (u[0] - avg[0]) - avg[1] * (u[1] - avg[1]) -
+                                e * (u[0] - avg[0]);
+                    double s3 = (avg[4] * avg[0]) - 0.5 * std::pow(avg[1], 2) - e * avg[0];
+                    s1 -= 0.5 * std::pow(u[2] - avg[2], 2);
+                    s2 -= avg[2] * (u[2] - avg[2]);
+                    s3 -= 0.5 * std::pow(avg[2], 2);
+                    s1 -= 0.5 * std::pow(u[3] - avg[3], 2);
+                    s2 -= avg[3] * (u[3] - avg[3]);
+                    s3 -= 0.5 * std::pow(avg[3], 2);
+                    out[i] = smallest_root_real(s3, s2, s1);
+                }
+            };
+            std::vector<double> tq((size_t)3 * n3), tsol(n3);
+            for (int d = 0; d < 3; ++d) theta2_of(q[d].data(), &tq[(size_t)d * n3]);
+            theta2_of(coeff.data(), tsol.data());
+            for (int s = 0; s < NSTATE; ++s)
+                for (int i = 0; i < n3; ++i) {
+                    double mq = 1e6;
+                    for (int d = 0; d < 3; ++d) if (tq[(size_t)d * n3 + i] < mq) mq = tq[(size_t)d * n3 + i];
+                    const double th = std::min(mq, tsol[i]);
+                    coeff[(size_t)s * n3 + i] = th * (coeff[(size_t)s * n3 + i] - avg[s]) + avg[s];
+                }
+        }
+        std::copy(coeff.begin(), coeff.end(), Uc);
+    }
+}
+
+// ---------------------------------------------------------------------------------
 // Low-storage 3S* / 3S*+ step (LowStorageRungeKuttaODESolver,
 // low_storage_runge_kutta_ode_solver.cpp:20-110; tableaux low_storage_runge_kutta_methods.cpp,
 // the published RK4(3)5[3S*] of Ketcheson 2010 and the [3S*+] family of Ranocha et al. 2021).
@@ -1391,6 +1564,7 @@ void Solver::rk_step(double* U, double dt) {
         for (int j = 0; j < i; ++j)
             if (a[i][j] != 0.0) for (size_t m = 0; m < N; ++m) st[m] += a[i][j] * k[j][m];
         for (size_t m = 0; m < N; ++m) { st[m] *= dt; st[m] += 1.0 * un[m]; }
+        limit(st.data(), dt);   // RungeKuttaBase::apply_limiter at every stage (runge_kutta_base.cpp:26)
         assemble_residual(st.data(), R.data());
         if (prm.use_rrk) est += b[i] * entropy_vars_dot_mass(st.data(), R.data());
         apply_inverse_mass(R.data(), st.data());
@@ -1400,6 +1574,7 @@ void Solver::rk_step(double* U, double dt) {
     for (int i = 0; i < ns; ++i)
         for (size_t m = 0; m < N; ++m) un[m] += step * b[i] * k[i][m];
     std::copy(un.begin(), un.end(), U);
+    limit(U, dt);   // and on the new solution (runge_kutta_base.cpp:34)
     current_time += step;
     (void)cc;
 }

@@ -33,6 +33,8 @@ enum FrType { C_DG = 0, C_SD = 1, C_HU = 2, C_NEGATIVE = 3, C_NEGATIVE2 = 4, C_P
 enum FrAuxType { K_DG = 0, K_SD = 1, K_HU = 2, K_NEGATIVE = 3, K_NEGATIVE2 = 4, K_PLUS = 5, K_10THOUSAND = 6 };
 enum CellOrder { ORDER_AUTO = 0, ORDER_LEXICOGRAPHIC = 1, ORDER_MORTON = 2 };
 enum NonPhysical { RETURN_BIG_NUMBER = 0, ABORT_RUN = 1, PRINT_WARNING = 2 };
+// limiter/bound_preserving_limiter (parameters_limiter.cpp:17-30); the positivity-preserving ones
+enum Limiter { LIMITER_NONE = 0, LIMITER_MAXIMUM_PRINCIPLE = 1, PPL_ZHANG2010 = 2, PPL_WANG2012 = 3 };
 
 // Plain parameter block (mirrors the .prm keys of the hot path).
 struct Params {
@@ -60,6 +62,8 @@ struct Params {
     double atol = 1e-3, rtol = 1e-3;   // low-storage error estimate
     int use_rrk = 0;                   // relaxation Runge-Kutta (root-finding, entropy)
     double rrk_tol = 5e-10;            // relaxation_runge_kutta_root_tolerance
+    int limiter = LIMITER_NONE;        // limiter/bound_preserving_limiter
+    double min_density = 1e-13;        // limiter/min_density
 };
 
 // One-dimensional operators on the reference interval [0,1]
@@ -140,6 +144,9 @@ struct Solver {
     double entropy_vars_dot_mass(const double* st, const double* R);
     double relaxation_parameter(const double* un, const std::vector<std::vector<double>>& k, const double* b,
                                 int ns, double dt, double est);
+    // PositivityPreservingLimiter::limit (positivity_preserving_limiter.cpp:381-678) on a state,
+    // for the stage solution of time step dt; no-op unless prm.limiter is a positivity limiter
+    void limit(double* U, double dt);
     // nodal interpolation of an initial condition (set_initial_condition.cpp:51)
     void interpolate_ic(double* U, int ic, const double* ic_params);
     // TGV integrated quantities (periodic_turbulence.cpp:439-672):

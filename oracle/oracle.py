@@ -31,6 +31,7 @@ FR = {"cDG": 0, "cSD": 1, "cHU": 2, "cNegative": 3, "cNegative2": 4, "cPlus": 5,
 FR_AUX = {"kDG": 0, "kSD": 1, "kHU": 2, "kNegative": 3, "kNegative2": 4, "kPlus": 5, "k10Thousand": 6}
 ORDER = {"auto": 0, "lexicographic": 1, "morton": 2}
 IC = {"tgv": 0, "isentropic_vortex": 1, "vortex_param": 2}
+LIMITER = {"none": 0, "maximum_principle": 1, "positivity_preservingZhang2010": 2, "positivity_preservingWang2012": 3}
 
 
 class OrcParams(ctypes.Structure):
@@ -39,7 +40,8 @@ class OrcParams(ctypes.Structure):
         "conv_flux", "diss_flux", "fr_type", "fr_aux_type", "rk_method", "use_constant_viscosity",
         "non_physical", "use_rrk")] + [(n, ctypes.c_double) for n in (
         "fr_user_value", "gamma", "mach_inf", "reynolds_inf", "prandtl", "temperature_inf",
-        "constant_viscosity", "sipg_penalty_factor", "atol", "rtol", "rrk_tol")]
+        "constant_viscosity", "sipg_penalty_factor", "atol", "rtol", "rrk_tol")] + [
+        ("limiter", ctypes.c_int), ("min_density", ctypes.c_double)]
 
 
 _lib = None
@@ -74,6 +76,7 @@ def lib():
         L.orc_inverse_mass.argtypes = [vp, dp, dp]
         L.orc_rk_step.argtypes = [vp, dp, ctypes.c_double]; L.orc_rk_step.restype = ctypes.c_int
         L.orc_integrals.argtypes = [vp, dp, dp]
+        L.orc_limit.argtypes = [vp, dp, ctypes.c_double]
         L.orc_integrated_quantities.argtypes = [vp, dp, dp]
         L.orc_rk_error.argtypes = [vp]; L.orc_rk_error.restype = ctypes.c_double
         L.orc_rrk_gamma.argtypes = [vp]; L.orc_rrk_gamma.restype = ctypes.c_double
@@ -116,6 +119,8 @@ def make_params(cfg: dict) -> OrcParams:
     p.rtol = cfg.get("rtol", 1e-3)
     p.use_rrk = int(cfg.get("use_relaxation_runge_kutta", False))
     p.rrk_tol = cfg.get("relaxation_runge_kutta_root_tolerance", 5e-10)
+    p.limiter = LIMITER[cfg.get("bound_preserving_limiter", "none")]
+    p.min_density = cfg.get("min_density", 1e-13)
     return p
 
 
@@ -207,6 +212,10 @@ class Oracle:
     def rk_error(self) -> float:
         """Weighted RMS error estimate of the last low-storage step."""
         return float(lib().orc_rk_error(self.h))
+
+    def limit(self, U, dt):
+        """PositivityPreservingLimiter::limit on U in place (for a stage of time step dt)."""
+        lib().orc_limit(self.h, _dp(U), dt)
 
     def integrals(self, U):
         out = np.zeros(4)

@@ -20,6 +20,8 @@ struct orc_params {
     int fr_type, fr_aux_type, rk_method, use_constant_viscosity, non_physical, use_rrk;
     double fr_user_value, gamma, mach_inf, reynolds_inf, prandtl, temperature_inf, constant_viscosity,
         sipg_penalty_factor, atol, rtol, rrk_tol;
+    int limiter;
+    double min_density;
 };
 
 static Params to_params(const orc_params* p) {
@@ -34,6 +36,7 @@ static Params to_params(const orc_params* p) {
     q.non_physical = p->non_physical;
     q.atol = p->atol; q.rtol = p->rtol;
     q.use_rrk = p->use_rrk; q.rrk_tol = p->rrk_tol;
+    q.limiter = p->limiter; q.min_density = p->min_density;
     return q;
 }
 
@@ -120,6 +123,7 @@ int orc_rk_step(void* h, double* U, double dt) {
     }
 }
 void orc_integrals(void* h, const double* U, double* out) { static_cast<Solver*>(h)->integrals(U, out); }
+void orc_limit(void* h, double* U, double dt) { static_cast<Solver*>(h)->limit(U, dt); }
 void orc_integrated_quantities(void* h, const double* U, double* out) {
     static_cast<Solver*>(h)->integrated_quantities(U, out);
 }

@@ -35,7 +35,7 @@ EXPORTED = ["ph_ctx_create", "ph_ctx_destroy", "ph_ndofs", "ph_cell_ijk", "ph_se
             "ph_slab_connectivity", "ph_server_create", "ph_server_submit", "ph_server_poll", "ph_server_wait",
             "ph_server_result", "ph_server_stats", "ph_server_destroy", "ph_snapshots_create", "ph_snapshots_destroy",
             "ph_snapshots_add", "ph_snapshots_add_state", "ph_snapshots_add_batch", "ph_snapshots_count",
-            "ph_snapshots_get", "ph_snapshots_pod"]
+            "ph_snapshots_get", "ph_snapshots_pod", "ph_limit", "ph_kinetic_energy_rate"]
 PH_SOLVE_QUEUED, PH_SOLVE_RUNNING, PH_SOLVE_DONE, PH_SOLVE_FAILED = 0, 1, 2, 3
 
 # ph_halo_fn(user, what, phase, send_lo, send_hi, recv_lo, recv_hi, bytes, cuda_stream)
@@ -52,7 +52,8 @@ class PhParams(ctypes.Structure):
         "FR_user_specified_correction_parameter_value", "gamma_gas", "mach_infinity", "reynolds_number_inf",
         "prandtl_number", "temperature_inf", "nondimensionalized_constant_viscosity", "sipg_penalty_factor",
         "rk_atol", "rk_rtol", "pressure_shift")] + [
-        ("use_relaxation_runge_kutta", ctypes.c_int), ("relaxation_runge_kutta_root_tolerance", ctypes.c_double)]
+        ("use_relaxation_runge_kutta", ctypes.c_int), ("relaxation_runge_kutta_root_tolerance", ctypes.c_double),
+        ("bound_preserving_limiter", ctypes.c_int), ("min_density", ctypes.c_double)]
 
 
 class PhMeshDesc(ctypes.Structure):
@@ -96,6 +97,8 @@ def load(build_if_missing: bool = False):
     L.ph_run.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, dp]
     L.ph_rk_relaxation.argtypes = [vp, dp, dp]
     L.ph_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32)]
+    L.ph_limit.argtypes = [vp, ctypes.c_double]
+    L.ph_kinetic_energy_rate.argtypes = [vp, dp]
     L.ph_sync.argtypes = [vp]
     L.ph_set_timing.argtypes = [vp, ctypes.c_int]
     L.ph_get_timing.argtypes = [vp, dp]

@@ -341,6 +341,7 @@ int check_batch_params(const ph_batch* b, const ph_mesh_desc* mesh, const ph_par
         return fail(PH_ERR_UNSUPPORTED, "a batch takes rk4_ex, ssprk3_ex or heun2_ex");
     if (prm->use_relaxation_runge_kutta)
         return fail(PH_ERR_UNSUPPORTED, "a batch takes fixed-step solves (no relaxation RK)");
+    if (prm->bound_preserving_limiter != 0) return fail(PH_ERR_UNSUPPORTED, "a batch takes solves without a limiter");
     if (prm->two_point_num_flux_type < 0 || prm->two_point_num_flux_type > 3 || prm->conv_num_flux < 0 ||
         prm->conv_num_flux > 5)
         return fail(PH_ERR_INVALID, "parameter out of range");

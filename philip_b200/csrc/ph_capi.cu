@@ -777,6 +777,9 @@ struct ph_ctx {
     double rrk_gamma = 1.0, rrk_elapsed = 0.0;
     std::vector<double> h_ent;
     std::vector<double> h_partial;
+    // positivity-preserving limiter (2 Zhang 2010, 3 Wang 2012; 0 none) and its 1-D tables
+    int limiter = 0;
+    ph::LimiterTab* d_ltab = nullptr;
     // uncollocated path (GL flux nodes / overintegration): nq flux nodes per direction, the
     // operator table and the face / viscous buffers of its kernels
     bool gl = false;
@@ -932,6 +935,26 @@ int dispatch_gl(ph_ctx* c, int kernel, const ph::StageArgs& a) {
     }
     if (e != cudaSuccess) return fail(PH_ERR_CUDA, std::string(kName[kernel]) + " launch: " + cudaGetErrorString(e));
     timer_end(c, kernel == 2 ? 0 : kernel == 1 ? 1 : 2);
+    return PH_OK;
+}
+
+// The positivity-preserving limiter on a state of this context (in place), for a stage of dt.
+int dispatch_limiter(ph_ctx* c, double* U, double dt) {
+    NvtxRange nvtx("limiter kernel");
+    ph::LimiterArgs la{U, c->d_ltab, c->nc, dt / c->h, c->prm.gamma_gas, c->prm.min_density, c->limiter == 2 ? 1 : 0};
+    cudaError_t e;
+    timer_begin(c);
+    switch (c->N1) {
+    case 2: e = ph::launch_limiter<2>(la, c->stream); break;
+    case 3: e = ph::launch_limiter<3>(la, c->stream); break;
+    case 4: e = ph::launch_limiter<4>(la, c->stream); break;
+    case 5: e = ph::launch_limiter<5>(la, c->stream); break;
+    case 6: e = ph::launch_limiter<6>(la, c->stream); break;
+    case 7: e = ph::launch_limiter<7>(la, c->stream); break;
+    default: return fail(PH_ERR_UNSUPPORTED, "polynomial degree outside 1..6");
+    }
+    if (e != cudaSuccess) return fail(PH_ERR_CUDA, std::string("limiter launch: ") + cudaGetErrorString(e));
+    timer_end(c, 2);
     return PH_OK;
 }
 
@@ -1128,6 +1151,16 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
         if (!(prm->relaxation_runge_kutta_root_tolerance > 0.0))
             return fail(PH_ERR_INVALID, "relaxation_runge_kutta_root_tolerance must be positive");
     }
+    if (prm->bound_preserving_limiter < 0 || prm->bound_preserving_limiter > 3)
+        return fail(PH_ERR_INVALID, "bound_preserving_limiter out of range");
+    if (prm->bound_preserving_limiter == 1)
+        return fail(PH_ERR_UNSUPPORTED, "the maximum-principle limiter applies to scalar equations, not Euler / Navier-Stokes");
+    if (prm->bound_preserving_limiter >= 2) {
+        if (prm->runge_kutta_method > 3 || prm->use_relaxation_runge_kutta)
+            return fail(PH_ERR_UNSUPPORTED, "the positivity-preserving limiter: Butcher RK methods without relaxation");
+        if (!(prm->min_density > 0.0)) return fail(PH_ERR_INVALID, "min_density must be positive");
+        if (is_curvilinear(mesh)) return fail(PH_ERR_UNSUPPORTED, "the positivity-preserving limiter: affine meshes");
+    }
     const bool slab = nz > 0;
     if (slab) {
         if (z0 < 0 || z0 >= mesh->n_cells_per_direction || nz > mesh->n_cells_per_direction)
@@ -1217,6 +1250,8 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
         c->halo_stride = (std::max(c->halo_state_bytes, c->halo_visc_bytes) + 255) / 256 * 256;
         bad |= dalloc(&c->d_halo, 4 * c->halo_stride);
     }
+    c->limiter = prm->bound_preserving_limiter;
+    if (c->limiter) bad |= dalloc(&c->d_ltab, 1);
     if (gl) {
         const size_t faces = (size_t)c->nc * 6 * c->NQ * c->NQ;
         bad |= dalloc(&c->d_gl, 1);
@@ -1235,6 +1270,22 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
     if (e == cudaSuccess) e = cudaMemcpy(c->d_ops, &c->h_ops, sizeof(ph::OpTab), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(c->d_itab, &itab, sizeof(ph::IntegralTab), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && c->d_gl) e = cudaMemcpy(c->d_gl, &c->h_gl, sizeof(ph::GlTab), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && c->d_ltab) {   // the FE_DGQ basis at the Gauss and Gauss-Lobatto points of p + 1
+        ph::LimiterTab lt;
+        std::memset(&lt, 0, sizeof(lt));
+        std::vector<double> xg, wg, xl, wl, v(c->N1), dv(c->N1);
+        gauss(c->N1, xg, wg);
+        gll(c->N1, xl, wl);
+        for (int q = 0; q < c->N1; ++q) {
+            lagrange(x, xg[q], v.data(), dv.data());
+            for (int i = 0; i < c->N1; ++i) lt.Bgl[q * c->N1 + i] = v[i];
+            lagrange(x, xl[q], v.data(), dv.data());
+            for (int i = 0; i < c->N1; ++i) lt.Bgll[q * c->N1 + i] = v[i];
+            lt.wgl[q] = wg[q];
+            lt.wgll[q] = wl[q];
+        }
+        e = cudaMemcpy(c->d_ltab, &lt, sizeof(lt), cudaMemcpyHostToDevice);
+    }
     if (e == cudaSuccess) e = cudaMemset(c->d_status, 0, sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMemset(c->d_sol, 0, c->nalloc * sizeof(double));
     if (e == cudaSuccess && c->d_comp) e = cudaMemset(c->d_comp, 0, N * sizeof(double));
@@ -1321,7 +1372,7 @@ int ph_ctx_destroy(ph_ctx* c) {
     void* ptrs[] = {c->d_nbr, c->d_ops, c->d_itab, c->d_sol, c->d_stA, c->d_stB, c->d_acc, c->d_carry,
                     c->d_fv, c->d_comp, c->d_tmpA, c->d_tmpB, c->d_partial, c->d_status, c->d_metric, c->d_xnode, c->d_origin, c->d_err,
                     c->d_table, c->d_counter, c->d_ent, c->d_ent_cell, c->d_halo, c->d_gl, c->d_t1, c->d_t2,
-                    c->d_vis};
+                    c->d_vis, c->d_ltab};
     if (c->side) cudaStreamSynchronize(c->side);
     for (void* p : ptrs) if (p) cudaFree(p);
     if (c->side) cudaStreamDestroy(c->side);
@@ -1454,9 +1505,22 @@ static int rk_one_step(ph_ctx* c, double dt) {
     for (int i = 0; i < ns; ++i) {
         NvtxRange stage(kStage[i]);
         const double* in = rk_stage_input(B, i);
+        if (c->limiter && i == 0) {
+            // RungeKuttaBase::step_in_time limits every stage solution before its derivative
+            // (runge_kutta_base.cpp:24-28): stage 0's is u_n, limited in a copy (stB is free
+            // during stage 0) so that the step's sum still starts from u_n itself
+            PH_CUDA(cudaMemcpyAsync(c->d_stB, c->d_sol, c->ndofs * sizeof(double), cudaMemcpyDeviceToDevice,
+                                    c->stream));
+            if (int rc = dispatch_limiter(c, c->d_stB, dt)) return rc;
+            in = c->d_stB;
+        }
         ph::StageArgs a = base_args(c, in);
         rk_stage_args(a, B, i, ns, c->A, c->b, dt, c->fp32);
         if (int rc = eval_residual(c, in, a)) return rc;
+        if (c->limiter) {   // the next stage's solution, or the new solution (runge_kutta_base.cpp:34)
+            double* out = (i == ns - 1) ? a.final_out : a.next;
+            if (int rc = dispatch_limiter(c, out, dt)) return rc;
+        }
     }
     if (ns == 1) std::swap(c->d_sol, c->d_stA);
     return PH_OK;
@@ -1874,6 +1938,42 @@ int ph_status(ph_ctx* c, uint32_t* flags) {
     PH_CUDA(cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->stream));
     PH_CUDA(cudaStreamSynchronize(c->stream));
     *flags = v;
+    return PH_OK;
+}
+
+int ph_kinetic_energy_rate(ph_ctx* c, double* out) {
+    if (!c || !out) return fail(PH_ERR_INVALID, "null argument");
+    if (c->curv || c->nc_ghost) return fail(PH_ERR_UNSUPPORTED, "ph_kinetic_energy_rate: whole affine meshes");
+    if (int rc = ensure_tmp(c)) return rc;
+    // K = M^-1 R(u) of the current solution, by the stage kernel's mode 1
+    ph::StageArgs a = base_args(c, c->d_sol);
+    a.mode = 1; a.out = c->d_tmpB;
+    if (int rc = eval_residual(c, c->d_sol, a)) return rc;
+    cudaError_t e;
+    const double h3 = c->h * c->h * c->h;
+    switch (c->N1) {
+#define PH_KE_CASE(n) case n: e = ph::launch_ke_rate<n>(c->d_sol, c->d_tmpB, c->d_itab, c->nc, h3, c->d_partial, c->stream); break;
+    PH_KE_CASE(2) PH_KE_CASE(3) PH_KE_CASE(4) PH_KE_CASE(5) PH_KE_CASE(6) PH_KE_CASE(7)
+#undef PH_KE_CASE
+    default: return fail(PH_ERR_UNSUPPORTED, "polynomial degree");
+    }
+    if (e != cudaSuccess) return fail(PH_ERR_CUDA, std::string("kinetic energy rate: ") + cudaGetErrorString(e));
+    ++c->launches;
+    PH_CUDA(cudaMemcpyAsync(c->h_partial.data(), c->d_partial, c->nc * sizeof(double), cudaMemcpyDeviceToHost,
+                            c->stream));
+    PH_CUDA(cudaStreamSynchronize(c->stream));
+    double sum = 0.0;
+    for (int i = 0; i < c->nc; ++i) sum += c->h_partial[i];
+    const double L = c->right - c->left;
+    *out = sum / (L * L * L);
+    return PH_OK;
+}
+
+int ph_limit(ph_ctx* c, double dt) {
+    if (!c) return fail(PH_ERR_INVALID, "null argument");
+    if (!c->limiter) return fail(PH_ERR_INVALID, "the context has no positivity-preserving limiter");
+    if (c->nc_ghost) return fail(PH_ERR_UNSUPPORTED, "ph_limit on a slab context");
+    if (int rc = dispatch_limiter(c, c->d_sol, dt)) return rc;
     return PH_OK;
 }
 

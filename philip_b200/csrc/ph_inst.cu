@@ -320,4 +320,42 @@ cudaError_t launch_gl(int kernel, int nq, const StageArgs& a, const GlArgs& g, b
 }
 template cudaError_t launch_gl<PH_N1>(int, int, const StageArgs&, const GlArgs&, bool, bool, cudaStream_t);
 
+template <int N1>
+cudaError_t launch_limiter(const LimiterArgs& a, cudaStream_t s) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static bool configured[64] = {false};
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!configured[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(limiter_kernel<N1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)limiter_smem<N1>());
+        if (e != cudaSuccess) return e;
+        configured[dev] = true;
+    }
+    if (a.nc <= 0) return cudaErrorInvalidValue;
+    limiter_kernel<N1><<<a.nc, limiter_threads<N1>(), limiter_smem<N1>(), s>>>(a);
+    return cudaGetLastError();
+}
+template cudaError_t launch_limiter<PH_N1>(const LimiterArgs&, cudaStream_t);
+
+template <int N1>
+cudaError_t launch_ke_rate(const double* U, const double* K, const IntegralTab* tab, int nc, double h3,
+                           double* partial, cudaStream_t s) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static bool configured[64] = {false};
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!configured[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(ke_rate_kernel<N1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)ke_rate_smem<N1>());
+        if (e != cudaSuccess) return e;
+        configured[dev] = true;
+    }
+    if (nc <= 0) return cudaErrorInvalidValue;
+    ke_rate_kernel<N1><<<nc, ke_rate_threads<N1>(), ke_rate_smem<N1>(), s>>>(U, K, tab, nc, h3, partial);
+    return cudaGetLastError();
+}
+template cudaError_t launch_ke_rate<PH_N1>(const double*, const double*, const IntegralTab*, int, double, double*,
+                                           cudaStream_t);
+
 } // namespace ph

@@ -525,4 +525,80 @@ integrals_row_kernel(const double* __restrict__ partial, int nc, double vol, dou
     }
 }
 
+// ------------------------------------------------------------------------------------
+// Rate of change of the kinetic energy, dKE/dt = integral of dKE/dU . dU/dt over the cell with
+// the same QGauss(p+11) cubature as the kinetic energy itself (so its time integral is that
+// KE), from a state U and its time derivative K = M^-1 R(U): the integrand is
+// v . K_m - |v|^2 / 2 K_rho (rho |v|^2 / 2 with m = rho v; the energy does not enter). Affine
+// cells; per-cell partial sums (W det J included), summed on the host in cell order. One CTA
+// per cell; one thread per (qx, qy) column walks qz.
+// ------------------------------------------------------------------------------------
+template <int N1> __host__ __device__ constexpr int ke_rate_threads() {
+    return (N1 + 10) * (N1 + 10) <= 256 ? 256 : 512;
+}
+template <int N1> __host__ __device__ constexpr size_t ke_rate_smem() {
+    constexpr int NE = N1 + 10;
+    return sizeof(double) * (8 * (size_t)N1 * N1 * N1 + 8 * (size_t)N1 * N1 * NE + 8 * (size_t)N1 * NE * NE);
+}
+
+template <int N1>
+__global__ void __launch_bounds__(ke_rate_threads<N1>())
+ke_rate_kernel(const double* __restrict__ U, const double* __restrict__ K, const IntegralTab* __restrict__ tab,
+               int nc, double h3, double* __restrict__ partial) {
+    constexpr int NE = N1 + 10, NP = N1 * N1 * N1, NT = ke_rate_threads<N1>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* sF = reinterpret_cast<double*>(smem_raw);   // [8][NP]: rho, m (3) of U, then of K
+    double* t0 = sF + 8 * NP;                           // [8][N1][N1][NE] after x
+    double* t1 = t0 + 8 * N1 * N1 * NE;                 // [8][N1][NE][NE] after y
+    __shared__ double sB[NE * N1], sw[NE], red[NT / 32];
+    const int cell = blockIdx.x, tid = threadIdx.x;
+    for (int i = tid; i < NE * N1; i += NT) sB[i] = tab->B[i];
+    for (int i = tid; i < NE; i += NT) sw[i] = tab->w[i];
+    for (int i = tid; i < 8 * NP; i += NT) {
+        const int f = i / NP, node = i % NP;
+        const double* src = f < 4 ? U : K;
+        sF[i] = src[((size_t)cell * 5 + (f % 4)) * NP + node];
+    }
+    __syncthreads();
+    for (int i = tid; i < 8 * N1 * N1 * NE; i += NT) {   // x: [f][z][y][qx]
+        const int qx = i % NE, r = i / NE;              // r = (f * N1 + z) * N1 + y
+        double v = 0.0;
+        for (int a = 0; a < N1; ++a) v += sB[qx * N1 + a] * sF[r * N1 + a];
+        t0[i] = v;
+    }
+    __syncthreads();
+    for (int i = tid; i < 8 * N1 * NE * NE; i += NT) {   // y: [f][z][qy][qx]
+        const int qx = i % NE, qy = (i / NE) % NE, fz = i / (NE * NE);
+        double v = 0.0;
+        for (int b = 0; b < N1; ++b) v += sB[qy * N1 + b] * t0[(fz * N1 + b) * NE + qx];
+        t1[i] = v;
+    }
+    __syncthreads();
+    double acc = 0.0;
+    for (int col = tid; col < NE * NE; col += NT) {
+        const int qx = col % NE, qy = col / NE;
+        for (int qz = 0; qz < NE; ++qz) {
+            double f[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                double v = 0.0;
+                for (int c = 0; c < N1; ++c) v += sB[qz * N1 + c] * t1[((k * N1 + c) * NE + qy) * NE + qx];
+                f[k] = v;
+            }
+            const double v0 = f[1] / f[0], v1 = f[2] / f[0], v2 = f[3] / f[0];
+            const double rate = v0 * f[5] + v1 * f[6] + v2 * f[7] - 0.5 * (v0 * v0 + v1 * v1 + v2 * v2) * f[4];
+            acc += sw[qx] * sw[qy] * sw[qz] * rate;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((tid & 31) == 0) red[tid >> 5] = acc;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+        for (int w = 0; w < NT / 32; ++w) t += red[w];
+        partial[cell] = t * h3;
+    }
+}
+
 } // namespace ph

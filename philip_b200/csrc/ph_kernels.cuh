@@ -39,6 +39,17 @@
 #ifndef PH_P3_MINB_F32
 #define PH_P3_MINB_F32 10
 #endif
+// 1: the pair fluxes between opposite nodes of a line (offset N1/2, even N1), which both lanes of
+// the pair would evaluate, are computed once per pair in a pass of their own and read back by
+// both nodes' lanes
+#ifndef PH_PAIR_DEDUP
+#define PH_PAIR_DEDUP 1
+#endif
+// 1: the FP64 stage kernel (even N1, affine cells) stages its tile's state and viscous
+// divergence into shared memory with bulk copies (cp.async.bulk, completion on an mbarrier)
+#ifndef PH_BULK_TILE
+#define PH_BULK_TILE 0
+#endif
 
 namespace ph {
 
@@ -127,7 +138,11 @@ struct Layout {
     // the volume accumulator reuses the state's space: the state is read last by the face phase
     static constexpr int oA = oU;
     static constexpr int oX = oT + CPC * 6 * TR * NF;
-    static constexpr int total = oX + CPC * NX * NP;
+    // opposite-node pair fluxes: [direction][cell][line][pair][5] (split form on affine cells,
+    // even N1; in the frame of the line's direction)
+    static constexpr int HP = (PH_PAIR_DEDUP && SPLIT && !CURV && (N1 % 2 == 0)) ? N1 / 2 : 0;
+    static constexpr int oH = oX + CPC * NX * NP;
+    static constexpr int total = oH + 3 * CPC * NF * HP * 5;
     static constexpr size_t bytes = (size_t)total * sizeof(R);
     static constexpr int SPW = 32 / N1;                // lines per warp
     static constexpr int WARPS_LINES = (CPC * NF + SPW - 1) / SPW;
@@ -144,6 +159,33 @@ struct Layout {
 };
 
 template <int N1> __device__ __forceinline__ int node_of(int x, int y, int z) { return (z * N1 + y) * N1 + x; }
+
+// ---- bulk copies global -> shared with mbarrier completion (this CTA's own shared memory, no
+// multicast). Sizes and both addresses are multiples of 16 bytes.
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(ok) : "r"(smem_addr(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+// Bounded wait on phase `parity`: true when the phase completed within `limit` polls.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity, long long limit) {
+    for (long long i = 0; i < limit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
 
 // coordinates of face node `fn` of face f at boundary coordinate b
 template <int N1> __device__ __forceinline__ int face_node_volume_index(int f, int fn, int b) {
@@ -294,8 +336,8 @@ template <typename R, int N1> __host__ __device__ constexpr int PAIR_UNROLL() {
 // two-point flux is evaluated in the frame whose x axis is e_d.
 template <typename R, int N1, int CPC, bool VISC, bool SPLIT, bool CURV>
 __device__ __forceinline__ void volume_dir(int d, const Cst<R>& cst, int tp, const R* sD, const R* sX, R* sA,
-                                           const R* sOpsD, const R* sOpsDsk, int lc, int lt, int pos, int seg,
-                                           bool lvalid) {
+                                           const R* sOpsD, const R* sOpsDsk, const R* sH, int lc, int lt, int pos,
+                                           int seg, bool lvalid) {
     using L = Layout<R, N1, CPC, VISC, SPLIT, CURV>;
     constexpr int NP = L::NP, NQS = L::NQS;
     const int st = (d == 0) ? 1 : (d == 1) ? N1 : N1 * N1;
@@ -364,14 +406,21 @@ __device__ __forceinline__ void volume_dir(int d, const Cst<R>& cst, int tp, con
         for (int k = 1; k <= N1 / 2; ++k) {
             const int jp = pos + k < N1 ? pos + k : pos + k - N1;      // (pos + k) mod N1
             const int jm = pos - k >= 0 ? pos - k : pos - k + N1;      // (pos - k) mod N1
+            const bool dup = ((N1 & 1) == 0) && (2 * k == N1);
+            const R cj = sOpsDsk[pos * N1 + jp];
+            if (L::HP > 0 && dup) {   // the opposite node's pair flux, from the pair pass
+                const int hp = pos < L::HP ? pos : pos - L::HP;
+                const R* h = sH + ((((size_t)d * CPC + lc) * L::NF + lt) * L::HP + hp) * 5;
+#pragma unroll
+                for (int s = 0; s < 5; ++s) accr[s] += cj * h[s];
+                continue;
+            }
             NodeQ<R> qj;
             load_q_rot<R>(Dq, NP, base + jp * st, d, qj);
             R F[5];
             two_point_dir<R, 0>(qi, qj, tp, cst, F);
-            const R cj = sOpsDsk[pos * N1 + jp];
             const int src = segbase + jm;
             const R cr = sOpsDsk[pos * N1 + jm];
-            const bool dup = ((N1 & 1) == 0) && (2 * k == N1);
 #pragma unroll
             for (int s = 0; s < 5; ++s) {
                 const R fr = __shfl_sync(0xffffffffu, F[s], src);
@@ -533,9 +582,10 @@ __device__ __forceinline__ void prefetch_tile_l2(const StageArgs& a, int cell0) 
 // residual_tile does the work of one CTA on the tile of CPC cells starting at cell0;
 // residual_kernel runs one tile per CTA of one discretisation, residual_kernel_batched
 // runs the tiles of many independent discretisations (a batch of solves) from a tile list.
-template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int FS, bool CURV>
+template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int FS, bool CURV, bool BULK = false>
 __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell0) {
     static_assert(!CURV || (SPLIT && !VISC), "curvilinear cells: split-form Euler only");
+    static_assert(!BULK || (std::is_same<R, double>::value && N1 % 2 == 0 && !CURV), "bulk staging: FP64, even N1");
     using L = Layout<R, N1, CPC, VISC, SPLIT, CURV>;
     constexpr int NP = L::NP, NF = L::NF, NT = L::NT, TR = L::TR, NQS = L::NQS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -567,6 +617,26 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
     }
     for (int i = tid; i < N1; i += NT) sOpsW[i] = (R)a.ops->w[i];
 
+    // bulk staging: the tile's state (cells contiguous) into sU and each cell's viscous
+    // divergence into its sX rows, issued before the neighbour gathers so both overlap
+    __shared__ __align__(8) unsigned long long tile_bar;
+    const int ncell = (a.nc - cell0) < CPC ? (a.nc - cell0) : CPC;
+    if constexpr (BULK) {
+        if (tid == 0) {
+            mbar_init(&tile_bar, 1);
+            const unsigned ubytes = (unsigned)(ncell * 5 * NP * sizeof(double));
+            const unsigned vbytes = VISC ? (unsigned)(4 * NP * sizeof(double)) : 0u;
+            mbar_expect_tx(&tile_bar, ubytes + ncell * vbytes);
+            bulk_copy_g2s(sU, a.U + (size_t)cell0 * 5 * NP, ubytes, &tile_bar);
+            if constexpr (VISC) {
+                for (int c = 0; c < ncell; ++c)
+                    bulk_copy_g2s(sX + c * L::NX * NP,
+                                  static_cast<const double*>(a.Fv) + (size_t)(cell0 + c) * viscous_terms_per_cell<N1>(),
+                                  vbytes, &tile_bar);
+            }
+        }
+    }
+
     // ---- phase 1: neighbour face traces (and the neighbour's viscous flux there)
     for (int it = tid; it < CPC * 6 * NF; it += NT) {
         const int fn = it % NF;
@@ -587,6 +657,16 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
         }
     }
 
+    if constexpr (BULK) {   // bounded wait for the staged tile; on a timeout no output is written
+        __syncthreads();    // the barrier's initialisation is visible to every thread
+        bool done = mbar_wait_bounded(&tile_bar, 0, 1ll << 22);
+        if (!done && tid == 0) atomicOr(a.status, ST_COPY_TIMEOUT);
+        if (__syncthreads_or(!done)) {
+            if (!done) mbar_wait_bounded(&tile_bar, 0, 1ll << 22);   // the copies in flight, again bounded
+            return;
+        }
+    }
+
     // ---- phase 2: node quantities (+ viscous / convective physical fluxes)
     for (int it = tid; it < CPC * NP; it += NT) {
         const int c = it / NP, node = it % NP;
@@ -594,8 +674,14 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
         const bool valid = cell < a.nc;
         if (!valid) cell = a.nc - 1;
         double ud[5];
+        if constexpr (BULK) {   // from the staged tile (a missing cell of the last tile: its first cell)
+            const int cs = valid ? c : 0;
 #pragma unroll
-        for (int s = 0; s < 5; ++s) ud[s] = __ldg(&a.U[((size_t)cell * 5 + s) * NP + node]);
+            for (int s = 0; s < 5; ++s) ud[s] = (double)sU[(cs * 5 + s) * NP + node];
+        } else {
+#pragma unroll
+            for (int s = 0; s < 5; ++s) ud[s] = __ldg(&a.U[((size_t)cell * 5 + s) * NP + node]);
+        }
         // positivity in FP64: the FP64 path checks the pressure it computes anyway, the
         // precision form checks the FP64 state before rounding it
         if constexpr (!std::is_same<R, double>::value) {
@@ -605,15 +691,23 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
         }
         R u[5];
 #pragma unroll
-        for (int s = 0; s < 5; ++s) { u[s] = (R)ud[s]; sU[(c * 5 + s) * NP + node] = u[s]; }
+        for (int s = 0; s < 5; ++s) { u[s] = (R)ud[s]; if constexpr (!BULK) sU[(c * 5 + s) * NP + node] = u[s]; }
+        if constexpr (BULK) {
+            if (!valid) {
+#pragma unroll
+                for (int s = 0; s < 5; ++s) sU[(c * 5 + s) * NP + node] = u[s];
+            }
+        }
         NodeQ<R> q;
         node_prepare<R>(u, tp, cst.gm1, q, std::is_same<R, double>::value && valid ? a.status : nullptr);
         store_q<R>(sD + c * NQS * NP, NP, node, q);
         R* X = sX + c * L::NX * NP;
         if constexpr (VISC) {
-            const R* dv = static_cast<const R*>(a.Fv) + (size_t)cell * viscous_terms_per_cell<N1>();
+            if (!BULK || !valid) {   // (staged by the bulk copy for the tile's cells)
+                const R* dv = static_cast<const R*>(a.Fv) + (size_t)cell * viscous_terms_per_cell<N1>();
 #pragma unroll
-            for (int k = 0; k < 4; ++k) X[k * NP + node] = __ldg(&dv[k * NP + node]);
+                for (int k = 0; k < 4; ++k) X[k * NP + node] = __ldg(&dv[k * NP + node]);
+            }
         }
         if constexpr (CURV) {
 #pragma unroll
@@ -652,6 +746,28 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
                                                     fvface);
         }
     }
+    // ---- opposite-node pair fluxes (even N1): each evaluated once, read by both lanes in phase 4
+    if constexpr (L::HP > 0) {
+        constexpr int HP = L::HP, PER_D = CPC * NF * HP;
+        R* sH = sm + L::oH;
+        for (int t = tid; t < 3 * PER_D; t += NT) {
+            const int d = t / PER_D, r = t - d * PER_D;
+            const int c = r / (NF * HP), lt = (r / HP) % NF, i = r % HP;
+            const int st = (d == 0) ? 1 : (d == 1) ? N1 : N1 * N1;
+            const int t1 = (d == 0) ? 1 : 0, t2 = (d == 2) ? 1 : 2;
+            int cc[3] = {0, 0, 0};
+            cc[t1] = lt % N1; cc[t2] = lt / N1;
+            const int base = node_of<N1>(cc[0], cc[1], cc[2]);
+            const R* Dq = sD + c * NQS * NP;
+            NodeQ<R> qi, qj;
+            load_q_rot<R>(Dq, NP, base + i * st, d, qi);
+            load_q_rot<R>(Dq, NP, base + (i + HP) * st, d, qj);
+            R F[5];
+            two_point_dir<R, 0>(qi, qj, tp, cst, F);
+#pragma unroll
+            for (int s = 0; s < 5; ++s) sH[(size_t)t * 5 + s] = F[s];
+        }
+    }
 
     // ---- phase 4: volume terms, one direction at a time
     {
@@ -667,7 +783,8 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             __syncthreads();
-            volume_dir<R, N1, CPC, VISC, SPLIT, CURV>(d, cst, tp, sD, sX, sA, sOpsD, sOpsDsk, lc, lt, pos, seg, lvalid);
+            volume_dir<R, N1, CPC, VISC, SPLIT, CURV>(d, cst, tp, sD, sX, sA, sOpsD, sOpsDsk, sm + L::oH, lc, lt, pos,
+                                                     seg, lvalid);
         }
         __syncthreads();
     }
@@ -838,10 +955,16 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
     }
 }
 
+template <typename R, int N1, int CPC, bool VISC, bool SPLIT, bool CURV>
+__host__ __device__ constexpr bool stage_bulk() {
+    return PH_BULK_TILE && std::is_same<R, double>::value && N1 % 2 == 0 && !CURV;
+}
+
 template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int FS, bool CURV = false>
 __global__ void __launch_bounds__(Layout<R, N1, CPC, VISC, SPLIT, CURV>::NT, Layout<R, N1, CPC, VISC, SPLIT, CURV>::MINB)
 residual_kernel(const StageArgs a) {
-    residual_tile<R, N1, CPC, VISC, SPLIT, FS, CURV>(a, a.cell_begin + blockIdx.x * CPC);
+    residual_tile<R, N1, CPC, VISC, SPLIT, FS, CURV, stage_bulk<R, N1, CPC, VISC, SPLIT, CURV>()>(
+        a, a.cell_begin + blockIdx.x * CPC);
 }
 
 // One tile of a batch: instance index and its first cell.

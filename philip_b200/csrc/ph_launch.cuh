@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include "ph_kernels.cuh"
 #include "ph_gl.cuh"
+#include "ph_limiter.cuh"
 #include "ph_integrals.cuh"
 
 namespace ph {
@@ -46,6 +47,13 @@ bool batched_shape(int fp32, bool curv, int variant, int* cpc, int* threads, siz
 // (gl_stage_kernel); one CTA per cell of [a.cell_begin, a.nc).
 template <int N1>
 cudaError_t launch_gl(int kernel, int nq, const StageArgs& a, const GlArgs& g, bool visc, bool split, cudaStream_t s);
+// dKE/dt of state U with time derivative K, per-cell partial sums (affine cells)
+template <int N1>
+cudaError_t launch_ke_rate(const double* U, const double* K, const IntegralTab* tab, int nc, double h3,
+                           double* partial, cudaStream_t s);
+// positivity-preserving limiter on a.U, one CTA per cell
+template <int N1>
+cudaError_t launch_limiter(const LimiterArgs& a, cudaStream_t s);
 // shared memory and threads of the residual kernel (for reporting / tests)
 template <int N1>
 void stage_launch_shape(int fp32, bool visc, bool split, int* threads, int* cells_per_cta, size_t* smem);

@@ -22,7 +22,9 @@ enum ConvFluxType { CF_LXF = 0, CF_ROE = 1, CF_CENTRAL = 2, CF_EC = 3, CF_EC_LXF
 enum DissFluxType { DF_SIPG = 0, DF_BR2 = 1, DF_CENTRAL = 2 };
 
 // status bits written by kernels (host reads them through ph_status)
-enum StatusBits : unsigned { ST_NONPHYSICAL = 1u };
+// ST_COPY_TIMEOUT: a bulk copy into shared memory did not complete within the kernel's wait
+// limit (the tile's outputs were not written)
+enum StatusBits : unsigned { ST_NONPHYSICAL = 1u, ST_COPY_TIMEOUT = 2u };
 
 constexpr double BIG_NUMBER = 1e100;   // physics.h:270
 

@@ -187,6 +187,17 @@ class DGStrong:
         _lib.check(self.L.ph_integrated_quantities(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
         return self._allreduce(out, "sum") if self.dist is not None else out
 
+    def kinetic_energy_rate(self) -> float:
+        """dKE/dt of the current solution from its time derivative M^-1 R (ph_kinetic_energy_rate)."""
+        v = ctypes.c_double(0.0)
+        _lib.check(self.L.ph_kinetic_energy_rate(self._h, ctypes.byref(v)))
+        return float(v.value)
+
+    def apply_limiter(self, dt: float):
+        """BoundPreservingLimiter::limit on the current solution for a stage of time step dt
+        (the context's positivity-preserving limiter, limiter/bound_preserving_limiter)."""
+        _lib.check(self.L.ph_limit(self._h, dt))
+
     def status(self) -> int:
         v = ctypes.c_uint32(0)
         _lib.check(self.L.ph_status(self._h, ctypes.byref(v)))
@@ -388,6 +399,10 @@ class FlowSolver:
         else:
             raise ValueError(f"flow_case_type {self.flow_case!r} is outside the periodic-cube cases")
         self.dg.solution = conservative_state(self.dg, prim)
+        # SetInitialCondition::interpolate_initial_condition limits the interpolated state with the
+        # Wang 2012 limiter (set_initial_condition.cpp:54-67), for a stage of the initial time step
+        if parameters.get("limiter/bound_preserving_limiter") == "positivity_preservingWang2012":
+            self.dg.apply_limiter(float(parameters.get("ODE solver/initial_time_step")))
         self.unsteady_data = []
         self.restart_dt = None
         # time POD (flow_solver.cpp:110-120): the snapshot matrix stays on the device

@@ -27,6 +27,7 @@ RK = {"rk4_ex": 0, "ssprk3_ex": 1, "heun2_ex": 2, "euler_ex": 3,   # parameters_
 RK_ORDER = {"rk4_ex": 4, "ssprk3_ex": 3, "heun2_ex": 2, "euler_ex": 1, "RK4_3_5_3SStar": 4,
             "RK3_2_5F_3SStarPlus": 3, "RK4_3_9F_3SStarPlus": 4, "RK5_4_10F_3SStarPlus": 5}
 NON_PHYSICAL = {"return_big_number": 0, "abort_run": 1, "print_warning": 2}
+LIMITER = {"none": 0, "maximum_principle": 1, "positivity_preservingZhang2010": 2, "positivity_preservingWang2012": 3}
 
 DEFAULTS = {
     "dimension": "-1", "pde_type": "advection", "use_weak_form": "true", "flux_nodes_type": "GL",
@@ -61,6 +62,7 @@ DEFAULTS = {
     "flow_solver/restart_files_directory_name": ".", "flow_solver/restart_file_index": "1",
     "flow_solver/output_restart_files_every_x_steps": "1",
     "flow_solver/output_restart_files_every_dt_time_intervals": "0.0",
+    "limiter/bound_preserving_limiter": "none", "limiter/min_density": "1e-13",
     "flow_solver/taylor_green_vortex/expected_kinetic_energy_at_final_time": "0",
     "flow_solver/taylor_green_vortex/expected_theoretical_dissipation_rate_at_final_time": "0",
 }
@@ -228,6 +230,8 @@ class Parameters:
         p.relaxation_runge_kutta_root_tolerance = float(
             self.get("ODE solver/rrk root solver/relaxation_runge_kutta_root_tolerance"))
         p.pressure_shift = self.reference_pressure()
+        p.bound_preserving_limiter = LIMITER[self.get("limiter/bound_preserving_limiter")]
+        p.min_density = float(self.get("limiter/min_density"))
         return p
 
     def reference_pressure(self) -> float:
@@ -265,4 +269,6 @@ class Parameters:
             "use_relaxation_runge_kutta": self.use_relaxation_runge_kutta,
             "relaxation_runge_kutta_root_tolerance": float(
                 self.get("ODE solver/rrk root solver/relaxation_runge_kutta_root_tolerance")),
+            "bound_preserving_limiter": self.get("limiter/bound_preserving_limiter"),
+            "min_density": float(self.get("limiter/min_density")),
         }

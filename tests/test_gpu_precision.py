@@ -52,3 +52,30 @@ def test_fp32_tgv_energy_history():
     # with the mean pressure taken out of the FP32 momentum fluxes (ph_params.pressure_shift)
     assert ke_err <= 2e-7
     assert eps_err <= 1e-6
+
+
+@pytest.mark.gpu
+def test_kinetic_energy_rate_from_the_time_derivative():
+    """ph_kinetic_energy_rate: dKE/dt from the state and M^-1 R(u) equals the central difference
+    of the kinetic energy along that direction (tolerance 1e-7, the difference's truncation and
+    rounding), and the precision form's rate is within 1e-5 of the FP64 one at the same state
+    (its residual's own bound)."""
+    prm = Parameters.from_dict(prm_dict(poly_degree=3, n_cells=4, pde="navier_stokes", diss="bassi_rebay_2"))
+    orc = Oracle(prm.oracle_cfg(), prm.n_cells, *prm.grid_bounds)
+    U = perturbed_tgv(orc, seed=9, amp=0.01)
+    dg = DGStrong(prm)
+    dg.solution = U
+    rate = dg.kinetic_energy_rate()
+    K = orc.inverse_mass(orc.residual(U))
+    eps = 1e-4 / np.max(np.abs(K))
+    ke = []
+    for sgn in (1.0, -1.0):
+        dg.solution = U + sgn * eps * K
+        ke.append(dg.integrals()[0])
+    fd = (ke[0] - ke[1]) / (2.0 * eps)
+    dg32 = DGStrong(prm, precision=_lib.PH_FP32_RESIDUAL)
+    dg32.solution = U
+    rate32 = dg32.kinetic_energy_rate()
+    print(f"dKE/dt {rate:.12e}, central difference {fd:.12e}, precision form {rate32:.12e}")
+    assert abs(rate - fd) <= 1e-7 * abs(rate)
+    assert abs(rate32 - rate) <= 1e-5 * abs(rate)

@@ -1,0 +1,166 @@
+"""Positivity-preserving limiter (PositivityPreservingLimiter, limiter/positivity_preserving_limiter.cpp).
+
+CPU: the oracle's restatement keeps the reference's index behaviour, pinned here against an
+independent numpy restatement of the same steps: each directional "cell average" sums only the
+first n^2 points of its mixed point set (the innermost weight loop has no braces, :264-298), so
+the average the limiter scales towards is not the cell's mean. The average is recovered from
+the oracle's output (every limited density is theta * (rho - avg) + avg) and compared.
+GPU: the limiter kernel and the limited RK steps against the oracle (1e-12).
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from philip_b200.prm import Parameters
+
+from helpers import prm_dict, rel_max_err
+
+
+def _params(limiter, **kw):
+    d = prm_dict(**kw)
+    d["limiter/bound_preserving_limiter"] = limiter
+    return Parameters.from_dict(d)
+
+
+def _gauss(n):
+    x, w = np.polynomial.legendre.leggauss(n)
+    return 0.5 * (x + 1.0), 0.5 * w
+
+
+def _gauss_lobatto(n):
+    m = n - 1
+    P = np.polynomial.legendre.Legendre.basis(m)
+    x = np.concatenate([[-1.0], np.sort(P.deriv().roots()), [1.0]])
+    w = 2.0 / (m * (m + 1) * P(x) ** 2)
+    return 0.5 * (x + 1.0), 0.5 * w
+
+
+def _lagrange(nodes, x):
+    B = np.ones((len(x), len(nodes)))
+    for j, xj in enumerate(nodes):
+        for m, xm in enumerate(nodes):
+            if m != j:
+                B[:, j] *= (x - xm) / (xj - xm)
+    return B
+
+
+def _reference_average(U_cell, n, lam, gamma):
+    """The average of PositivityPreservingLimiter::get_soln_cell_avg_PPL (3-D), steps restated."""
+    xs, _ = _gauss_lobatto(n)
+    xg, wg = _gauss(n)
+    xl, wl = _gauss_lobatto(n)
+    Bg, Bl = _lagrange(xs, xg), _lagrange(xs, xl)
+    C = U_cell.reshape(5, n, n, n)          # [s][z][y][x]
+    sets = []
+    for d in range(3):
+        Ax = Bl if d == 0 else Bg
+        Ay = Bl if d == 1 else Bg
+        Az = Bl if d == 2 else Bg
+        sets.append(np.einsum("ax,by,cz,szyx->scba", Ax, Ay, Az, C).reshape(5, -1))
+    wi = [wl, wg, wg]
+    wj = [wg, wl, wg]
+    wk = [wg, wg, wl]
+    avg_dim = np.zeros((3, 5))
+    for d in range(3):
+        for s in range(5):
+            qp = 0
+            for i in range(n):
+                for j in range(n):
+                    for k in range(n):
+                        avg_dim[d, s] += wi[d][i] * wj[d][j] * wk[d][k] * sets[d][s, qp]
+                    qp += 1
+    ws = []
+    for d in range(3):
+        rho, m = sets[d][0], sets[d][1:4]
+        v = m / rho
+        p = (gamma - 1.0) * (sets[d][4] - 0.5 * rho * np.sum(v * v, axis=0))
+        ws.append(np.max(np.sqrt(np.sum(v * v, axis=0)) + np.sqrt(p * gamma / rho)))
+    mu = sum(w * lam for w in ws)
+    return sum((ws[d] * lam / mu) * avg_dim[d] for d in range(3))
+
+
+@pytest.mark.parametrize("limiter", ["positivity_preservingWang2012", "positivity_preservingZhang2010"])
+def test_oracle_limiter_scales_towards_the_reference_average(limiter):
+    prm = _params(limiter, poly_degree=3, n_cells=2)
+    orc = Oracle(prm.oracle_cfg(), prm.n_cells, *prm.grid_bounds)
+    U = orc.initial_condition("tgv")
+    n, ncell = 4, 5 * 64
+    U[3] = -0.2            # a negative density at one node of cell 0
+    dt = 0.01
+    V = U.copy()
+    orc.limit(V, dt)
+    rho, out = U[:64], V[:64]
+    s, c = np.polyfit(rho, out, 1)
+    assert np.max(np.abs(out - (s * rho + c))) < 1e-13 and s < 1.0
+    avg = c / (1.0 - s)
+    h = prm.grid_bounds[1] / prm.n_cells
+    ref = _reference_average(U[:ncell], n, dt / h, 1.4)
+    xs, ws = _gauss_lobatto(n)          # the cell's true mean density: GLL quadrature of the nodal values
+    true_avg = np.einsum("z,y,x,zyx->", ws, ws, ws, U[:64].reshape(n, n, n))
+    print(f"{limiter}: recovered average {avg:.15f}, restated {ref[0]:.15f}, cell mean {true_avg:.15f}")
+    assert abs(avg - ref[0]) <= 1e-12 * abs(ref[0])
+    assert abs(ref[0] - true_avg) > 1e-6         # the average is the reference's, not the cell mean
+    assert np.min(V.reshape(-1, 5, 64)[:, 0]) >= 0.0
+    # cells without a negative density or pressure change only by the rounding of
+    # theta (u - avg) + avg with theta = 1
+    assert rel_max_err(V[ncell:], U[ncell:]) <= 1e-14
+
+
+def test_oracle_limiter_is_off_by_default():
+    prm = Parameters.from_dict(prm_dict(poly_degree=2, n_cells=2))
+    orc = Oracle(prm.oracle_cfg(), prm.n_cells, *prm.grid_bounds)
+    U = orc.initial_condition("tgv")
+    U[0] = -0.5
+    V = U.copy()
+    orc.limit(V, 0.01)
+    assert np.array_equal(U, V)
+
+
+# ------------------------------------------------------------------------------- GPU
+
+def _negative_state(orc, seed):
+    U = orc.initial_condition("tgv")
+    rng = np.random.default_rng(seed)
+    nd3 = orc.nd ** 3
+    W = U.reshape(-1, 5, nd3)
+    for c in rng.choice(W.shape[0], size=3, replace=False):
+        W[c, 0, rng.integers(nd3)] = -0.05                     # negative density
+        W[c, 4, rng.integers(nd3)] *= -0.5                      # negative energy -> negative pressure
+    return U
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("limiter", ["positivity_preservingWang2012", "positivity_preservingZhang2010"])
+@pytest.mark.parametrize("p", [2, 3, 5])
+def test_gpu_limiter_matches_oracle(limiter, p):
+    from philip_b200.dg import DGStrong
+    prm = _params(limiter, poly_degree=p, n_cells=3)
+    orc = Oracle(prm.oracle_cfg(), prm.n_cells, *prm.grid_bounds)
+    dg = DGStrong(prm)
+    U = _negative_state(orc, seed=p)
+    dg.solution = U
+    dg.apply_limiter(0.003)
+    orc.limit(U, 0.003)
+    err = rel_max_err(dg.solution, U)
+    print(f"{limiter} p={p}: limited state rel err {err:.3e}")
+    assert err <= 1e-12
+    assert np.min(U.reshape(-1, 5, (p + 1) ** 3)[:, 0]) >= 0.0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("limiter,rk", [("positivity_preservingWang2012", "ssprk3_ex"),
+                                        ("positivity_preservingZhang2010", "rk4_ex")])
+def test_gpu_limited_rk_steps_match_oracle(limiter, rk):
+    from philip_b200.dg import DGStrong, RungeKuttaODESolver
+    prm = _params(limiter, poly_degree=3, n_cells=3, rk=rk)
+    orc = Oracle(prm.oracle_cfg(), prm.n_cells, *prm.grid_bounds)
+    dg = DGStrong(prm)
+    U = _negative_state(orc, seed=11)
+    dg.solution = U
+    ode = RungeKuttaODESolver(dg)
+    for _ in range(3):
+        ode.step_in_time(1e-4)
+        orc.rk_step(U, 1e-4)
+    err = rel_max_err(dg.solution, U)
+    print(f"{limiter} {rk}: three limited steps rel err {err:.3e}")
+    assert err <= 1e-12
