@@ -41,14 +41,17 @@
 #endif
 // 1: the pair fluxes between opposite nodes of a line (offset N1/2, even N1), which both lanes of
 // the pair would evaluate, are computed once per pair in a pass of their own and read back by
-// both nodes' lanes
+// both nodes' lanes. Off: on B200 the extra shared memory costs more than the saved pair fluxes
+// (24^3 p5 FP64 stage 0.505 ms against 0.494, 32^3 p3 0.425 against 0.396: one CTA per SM fewer)
 #ifndef PH_PAIR_DEDUP
-#define PH_PAIR_DEDUP 1
+#define PH_PAIR_DEDUP 0
 #endif
-// 1: the FP64 stage kernel (even N1, affine cells) stages its tile's state and viscous
-// divergence into shared memory with bulk copies (cp.async.bulk, completion on an mbarrier)
+// 1: the FP64 viscous stage kernel (even N1, affine cells) stages its tile's state and viscous
+// divergence into shared memory with bulk copies (cp.async.bulk, completion on an mbarrier),
+// issued before the neighbour gathers (B200: 24^3 p5 0.499 ms against 0.505, 32^3 p3 0.421
+// against 0.425; the L2-resident 8^3 p3 inviscid case is 5 % slower with it, so only viscous)
 #ifndef PH_BULK_TILE
-#define PH_BULK_TILE 0
+#define PH_BULK_TILE 1
 #endif
 
 namespace ph {
@@ -957,7 +960,7 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
 
 template <typename R, int N1, int CPC, bool VISC, bool SPLIT, bool CURV>
 __host__ __device__ constexpr bool stage_bulk() {
-    return PH_BULK_TILE && std::is_same<R, double>::value && N1 % 2 == 0 && !CURV;
+    return PH_BULK_TILE && std::is_same<R, double>::value && N1 % 2 == 0 && !CURV && VISC;
 }
 
 template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int FS, bool CURV = false>
