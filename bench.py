@@ -47,13 +47,18 @@ WORKLOADS = {
     # reduced size of the default workload, for ncu captures (still larger than L2)
     "tgv_viscous_16_p5": (5, 16, "navier_stokes", "bassi_rebay_2",
                           "viscous TGV Re=1600, 16^3 cells, p=5 GLL, CH split + Roe, BR2, RK4"),
+    # the default workload on Gauss-Legendre flux nodes (the reference's default flux_nodes_type):
+    # dense interpolation, entropy projection and FR operators
+    "tgv_viscous_gl_24_p5": (5, 24, "navier_stokes", "bassi_rebay_2",
+                             "viscous TGV Re=1600, 24^3 cells, p=5 on GL flux nodes, CH split + Roe, BR2, RK4"),
 }
 
 
 def prm_for(workload: str) -> dict:
     p, n, pde, diss, _ = WORKLOADS[workload]
     return {
-        "dimension": 3, "pde_type": pde, "use_weak_form": False, "flux_nodes_type": "GLL",
+        "dimension": 3, "pde_type": pde, "use_weak_form": False,
+        "flux_nodes_type": "GL" if "_gl_" in workload else "GLL",
         "use_split_form": True, "two_point_num_flux_type": "CH",
         "conv_num_flux": "two_point_flux_with_roe_dissipation", "diss_num_flux": diss,
         "flux_reconstruction": "cDG", "use_inverse_mass_on_the_fly": True,
@@ -740,6 +745,8 @@ def main():
         fp32 = args.precision == "fp32"
         gemm_tflops = gemm_peak(torch, torch.float32 if fp32 else torch.float64)
         mix = measured_fp64_mix(p, viscous, args.precision)
+        if "_gl_" in args.workload:   # the byte and flop models above are the collocated kernel's
+            flops = dict(flops, applies_to="collocated (GLL) stage kernel; this workload runs the GL kernels")
         line = {
             "metric": "TGV DOF-updates/s/stage", "value": value, "unit": "DOF-updates/s/stage",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,

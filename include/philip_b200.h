@@ -233,9 +233,10 @@ int ph_limit(ph_ctx* ctx, double dt);
  * src/flow_solver/flow_solver.cpp:690-711). enable = 1: every kernel launch is bracketed
  * by CUDA events on the context stream and the stream is synchronised after it (steps
  * launch directly). enable = 2: the captured RK step that ph_rk_step replays carries an
- * event-record node before its first kernel and after each kernel, and every replay
- * records a fresh set of events, so the kernels are timed inside the replayed steps
- * themselves (each duration includes the launch gap before the kernel); changing to or
+ * event-record node before its first kernel and after each kernel, on a side branch of the
+ * graph that the kernels do not wait for, and every replay records a fresh set of events, so
+ * the kernels are timed inside the replayed steps themselves (each duration includes the
+ * launch gap before the kernel); changing to or
  * from mode 2 drops the captured step, which the next multi-step ph_rk_step captures
  * again (its first step runs directly and is not timed). Every call resets the sums.
  * out[0..5] = {stage-kernel ms, stage launches, auxiliary-kernel ms, auxiliary

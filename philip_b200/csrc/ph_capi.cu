@@ -798,6 +798,8 @@ struct ph_ctx {
     long long launches = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool capturing = false;                        // inside capture_step_graph
+    cudaStream_t tside = nullptr;                  // mode 2: the event nodes' side branch of the graph
+    cudaEvent_t tfork = nullptr;                   // mode 2: fork / join points of that branch
     std::vector<cudaEvent_t> tcap;                 // mode 2: events recorded at capture, kernels + 1
     std::vector<int> tcls;                         // mode 2: class of kernel j of the step
     std::vector<cudaGraphNode_t> tnodes;           // mode 2: the event-record node of tcap[j]
@@ -856,17 +858,24 @@ void drop_step_graph(ph_ctx* c) {
     c->tnodes.clear();
 }
 
+// Mode 2: an event-record node of the captured graph on a side branch that forks from the
+// context stream at this point, so the kernels that follow do not wait for the event.
+void timer_mark(ph_ctx* c, cudaEvent_t ev) {
+    cudaEventRecord(c->tfork, c->stream);
+    cudaStreamWaitEvent(c->tside, c->tfork, 0);
+    cudaEventRecordWithFlags(ev, c->tside, cudaEventRecordExternal);
+}
+
 void timer_begin(ph_ctx* c) {
     if (c->timing == 1) cudaEventRecord(c->ev0, c->stream);
-    else if (c->timing == 2 && c->capturing && c->tcls.empty())   // an event-record node of the graph
-        cudaEventRecordWithFlags(c->tcap[0], c->stream, cudaEventRecordExternal);
+    else if (c->timing == 2 && c->capturing && c->tcls.empty()) timer_mark(c, c->tcap[0]);
 }
 void timer_end(ph_ctx* c, int cls) {
     ++c->launches;
     if (c->timing == 2) {
         if (c->capturing && c->tcls.size() + 1 < c->tcap.size()) {
             c->tcls.push_back(cls);
-            cudaEventRecordWithFlags(c->tcap[c->tcls.size()], c->stream, cudaEventRecordExternal);
+            timer_mark(c, c->tcap[c->tcls.size()]);
         }
         return;
     }
@@ -1368,6 +1377,8 @@ int ph_ctx_destroy(ph_ctx* c) {
         if (c->run_graph) cudaGraphExecDestroy(c->run_graph);
     }
     for (cudaEvent_t ev : c->tcap) if (ev) cudaEventDestroy(ev);
+    if (c->tfork) cudaEventDestroy(c->tfork);
+    if (c->tside) cudaStreamDestroy(c->tside);
     for (auto& set : c->tpool) for (cudaEvent_t ev : set) if (ev) cudaEventDestroy(ev);
     void* ptrs[] = {c->d_nbr, c->d_ops, c->d_itab, c->d_sol, c->d_stA, c->d_stB, c->d_acc, c->d_carry,
                     c->d_fv, c->d_comp, c->d_tmpA, c->d_tmpB, c->d_partial, c->d_status, c->d_metric, c->d_xnode, c->d_origin, c->d_err,
@@ -1685,8 +1696,12 @@ static int capture_step_graph(ph_ctx* c, double dt) {
     c->tcls.clear();
     PH_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     c->capturing = true;
-    const int rc = rk_one_step(c, dt);
+    int rc = rk_one_step(c, dt);
     c->capturing = false;
+    if (c->timing == 2 && !c->tcls.empty()) {   // join the event branch back before the capture ends
+        cudaEventRecord(c->tfork, c->tside);
+        cudaStreamWaitEvent(c->stream, c->tfork, 0);
+    }
     const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
     if (rc || e != cudaSuccess) {
         if (g) cudaGraphDestroy(g);
@@ -1987,6 +2002,8 @@ int ph_set_timing(ph_ctx* c, int enable) {
     if (enable == 2 && c->tcap.empty()) {
         c->tcap.assign(TIMED_KERNELS_PER_STEP + 1, nullptr);
         for (cudaEvent_t& ev : c->tcap) PH_CUDA(cudaEventCreate(&ev));
+        PH_CUDA(cudaStreamCreateWithFlags(&c->tside, cudaStreamNonBlocking));
+        PH_CUDA(cudaEventCreateWithFlags(&c->tfork, cudaEventDisableTiming));
     }
     // a step graph captured in another mode has (or lacks) the timing nodes: capture again
     if ((enable == 2) != (c->timing == 2) && c->step_graph) {

@@ -103,9 +103,9 @@ __device__ __forceinline__ void gl_cons_from_entropy(const double v[5], double g
 // with r the output's coordinate along d. Input dims (n0, n1, n2), n_d = cols; output dims the
 // same with n_d = rows. x is the fastest index.
 template <int NT>
-__device__ __forceinline__ void gl_pass(const double* A, int rows, int cols, int d, int n0, int n1, int n2,
-                                        const double* in, int in_ss, double* out, int out_ss, int ns, double scale,
-                                        bool acc) {
+__device__ __forceinline__ void gl_pass_fma(const double* A, int rows, int cols, int d, int n0, int n1, int n2,
+                                            const double* in, int in_ss, double* out, int out_ss, int ns,
+                                            double scale, bool acc) {
     const int m0 = d == 0 ? rows : n0, m1 = d == 1 ? rows : n1, m2 = d == 2 ? rows : n2;
     const int osz = m0 * m1 * m2;
     const int st = d == 0 ? 1 : d == 1 ? n0 : n0 * n1;
@@ -122,6 +122,89 @@ __device__ __forceinline__ void gl_pass(const double* A, int rows, int cols, int
         *op = acc ? *op + scale * v : scale * v;
     }
 }
+
+// 1: the sum-factorised passes run on the FP64 tensor-core instruction (mma.sync m8n8k4 f64):
+// a pass is the product of the 1-D operator (rows x cols, both <= 8, zero-padded to 8 x 8) with
+// the matrix whose columns are the input's lines, eight lines per warp-level product
+#ifndef PH_GL_DMMA
+#define PH_GL_DMMA 0
+#endif
+
+template <int NT>
+__device__ __forceinline__ void gl_pass_mma(const double* A, int rows, int cols, int d, int n0, int n1, int n2,
+                                            const double* in, int in_ss, double* out, int out_ss, int ns, double scale,
+                                            bool acc);
+template <int NT>
+__device__ __forceinline__ void gl_pass(const double* A, int rows, int cols, int d, int n0, int n1, int n2,
+                                        const double* in, int in_ss, double* out, int out_ss, int ns, double scale,
+                                        bool acc) {
+#if PH_GL_DMMA
+    gl_pass_mma<NT>(A, rows, cols, d, n0, n1, n2, in, in_ss, out, out_ss, ns, scale, acc);
+#else
+    gl_pass_fma<NT>(A, rows, cols, d, n0, n1, n2, in, in_ss, out, out_ss, ns, scale, acc);
+#endif
+}
+
+#if PH_GL_DMMA
+// D (8x8) += A (8x4, row-major) B (4x8, column-major); per lane: A[lane/4][lane%4],
+// B[lane%4][lane/4], D[lane/4][2 (lane%4) + {0, 1}]
+__device__ __forceinline__ void dmma_8x8x4(double a, double b, double& d0, double& d1) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
+}
+
+// gl_pass with the products on the tensor cores (see PH_GL_DMMA)
+template <int NT>
+__device__ __forceinline__ void gl_pass_mma(const double* A, int rows, int cols, int d, int n0, int n1, int n2,
+                                            const double* in, int in_ss, double* out, int out_ss, int ns, double scale,
+                                            bool acc) {
+    const int m0 = d == 0 ? rows : n0, m1 = d == 1 ? rows : n1, m2 = d == 2 ? rows : n2;
+    const int osz = m0 * m1 * m2;
+    const int st = d == 0 ? 1 : d == 1 ? n0 : n0 * n1;
+    const int ost = d == 0 ? 1 : d == 1 ? m0 : m0 * m1;
+    // lines: the coordinates other than d, then the state
+    const int pa = d == 0 ? n1 : n0;                 // extent of the first other coordinate
+    const int pb = d == 2 ? n1 : n2;                 // of the second
+    const int lines_per_state = pa * pb;
+    const int nlines = ns * lines_per_state;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int r = lane >> 2, kq = lane & 3;
+    double a0 = 0.0, a1 = 0.0;
+    if (r < rows) {
+        if (kq < cols) a0 = A[r * cols + kq];
+        if (kq + 4 < cols) a1 = A[r * cols + kq + 4];
+    }
+    for (int tile = warp; tile * 8 < nlines; tile += NT / 32) {
+        const int j = tile * 8 + (lane >> 2);        // this lane's B column (line)
+        double b0 = 0.0, b1 = 0.0;
+        if (j < nlines) {
+            const int s = j / lines_per_state, t = j - s * lines_per_state;
+            const int ca = t % pa, cb = t / pa;
+            const int x = d == 0 ? 0 : ca, y = d == 1 ? 0 : (d == 0 ? ca : cb), z = d == 2 ? 0 : cb;
+            const double* ip = in + s * in_ss + (z * n1 + y) * n0 + x;
+            if (kq < cols) b0 = ip[kq * st];
+            if (kq + 4 < cols) b1 = ip[(kq + 4) * st];
+        }
+        double d0 = 0.0, d1 = 0.0;
+        dmma_8x8x4(a0, b0, d0, d1);
+        dmma_8x8x4(a1, b1, d0, d1);
+        // write D[r][lines 2 kq, 2 kq + 1 of the tile]
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int jj = tile * 8 + 2 * kq + i;
+            if (r < rows && jj < nlines) {
+                const int s = jj / lines_per_state, t = jj - s * lines_per_state;
+                const int ca = t % pa, cb = t / pa;
+                const int x = d == 0 ? r : ca, y = d == 1 ? r : (d == 0 ? ca : cb), z = d == 2 ? r : cb;
+                double* op = out + s * out_ss + (z * m1 + y) * m0 + x;
+                const double v = i ? d1 : d0;
+                *op = acc ? *op + scale * v : scale * v;
+            }
+        }
+    }
+    (void)osz; (void)ost;
+}
+#endif
 
 // out = (Az (x) Ay (x) Az) in, x first: input cubes of n_in per direction, output n_out per
 // direction; t0, t1 hold ns * n_out * n_in^2 and ns * n_out^2 * n_in values. Ends with a barrier.
