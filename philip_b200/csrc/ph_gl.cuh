@@ -311,23 +311,26 @@ __device__ __forceinline__ void gl_face_values(const double* src, int src_ss, in
 
 // The lift of six face arrays into the cube: dst[s][node] (+)= sum_f row[side][i_dn]
 // sum_{q1,q2} T[q1][i_t1] T[q2][i_t2] face[f][s][q2] (the surface inner products of
-// operators.cpp:575-636 with the solution basis; T is n_q x n_d). Only the faces in mask
-// (bit f) contribute; per_dir: dst holds one cube per normal direction (dst + dn * dst_ds).
+// operators.cpp:575-636 with the solution basis; T is n_q x n_d). dst_ds != 0: dst holds one
+// cube per normal direction (dst + dn * dst_ds). only_dn >= 0: only the two faces of that
+// direction, given as face[0..1] (faces 2 only_dn and 2 only_dn + 1).
 template <int NT>
 __device__ __forceinline__ void gl_lift_faces(const double* face, int face_fs, int face_ss, int ns, int nq, int nd,
                                               const double* row0, const double* row1, const double* T, double* w0,
-                                              double* w1, double* dst, int dst_ss, int dst_ds, double scale) {
+                                              double* w1, double* dst, int dst_ss, int dst_ds, double scale,
+                                              int only_dn = -1) {
     const int mq = nq * nq, m1 = nq * nd, m2 = nd * nd;
-    for (int it = threadIdx.x; it < 6 * ns * m1; it += NT) {   // along t1: w0[f][s][q2 * nd + a]
+    const int f0 = only_dn < 0 ? 0 : 2 * only_dn, nfc = only_dn < 0 ? 6 : 2;   // the faces lifted
+    for (int it = threadIdx.x; it < nfc * ns * m1; it += NT) {   // along t1: w0[f][s][q2 * nd + a]
         const int fs = it / m1, r = it - fs * m1, a = r % nd, q2 = r / nd;
-        const int f = fs / ns, s = fs - f * ns;
-        const double* ip = face + f * face_fs + s * face_ss + q2 * nq;
+        const int f = f0 + fs / ns, s = fs % ns;
+        const double* ip = face + (f - f0) * face_fs + s * face_ss + q2 * nq;   // only_dn: two faces given
         double v = 0.0;
         for (int l = 0; l < nq; ++l) v += T[l * nd + a] * ip[l];
         w0[it] = v;
     }
     __syncthreads();
-    for (int it = threadIdx.x; it < 6 * ns * m2; it += NT) {   // along t2: w1[f][s][b * nd + a]
+    for (int it = threadIdx.x; it < nfc * ns * m2; it += NT) {   // along t2: w1[f][s][b * nd + a]
         const int fs = it / m2, r = it - fs * m2, a = r % nd, b = r / nd;
         const double* ip = w0 + fs * m1 + a;
         double v = 0.0;
@@ -341,10 +344,11 @@ __device__ __forceinline__ void gl_lift_faces(const double* face, int face_fs, i
         const int c[3] = {node % nd, (node / nd) % nd, node / m2};
 #pragma unroll
         for (int dn = 0; dn < 3; ++dn) {
+            if (only_dn >= 0 && dn != only_dn) continue;
             const int t1 = dn == 0 ? 1 : 0, t2 = dn == 2 ? 1 : 2;
             const int ab = c[t2] * nd + c[t1];
-            const double v = row0[c[dn]] * w1[((2 * dn) * ns + s) * m2 + ab] +
-                             row1[c[dn]] * w1[((2 * dn + 1) * ns + s) * m2 + ab];
+            const int fb = only_dn < 0 ? 2 * dn : 0;   // first of the direction's two faces in w1
+            const double v = row0[c[dn]] * w1[(fb * ns + s) * m2 + ab] + row1[c[dn]] * w1[((fb + 1) * ns + s) * m2 + ab];
             double* op = dst + (dst_ds ? dn * dst_ds : 0) + s * dst_ss + node;
             *op += scale * v;
         }
@@ -420,20 +424,22 @@ struct GlAuxLayout {
     static constexpr int nTab = (int)(sizeof(GlTab) / sizeof(double));
     static constexpr int oU = nTab;                      // 5 NQ^3: the state, later the projected state
     static constexpr int oQ = oU + 5 * Q3;               // 5 NQ^3: state at the flux nodes
-    // aux right-hand side (15 ND^3) and lifted gradient (15 ND^3); later the volume viscous
-    // flux (12 NQ^3) over both
-    static constexpr int nRA = 30 * D3 > 12 * Q3 ? 30 * D3 : 12 * Q3;
+    // one direction's aux right-hand side and lifted gradient (5 ND^3 each; the lift's second
+    // pass, 30 ND^2, also goes there), the lifted gradient at the flux nodes (15 NQ^3) and the
+    // volume viscous flux (12 NQ^3)
+    static constexpr int nR = 5 * D3 > 30 * ND * ND ? 5 * D3 : 30 * ND * ND;
     static constexpr int oR = oQ + 5 * Q3;
-    static constexpr int oA = oR + 15 * D3;
-    static constexpr int oAQ = oR + nRA;                 // 15 NQ^3: lifted gradient at the flux nodes
+    static constexpr int oA = oR + nR;
+    static constexpr int oAQ = oA + 5 * D3;
+    static constexpr int oF = oAQ + 15 * Q3;
     static constexpr int nT = gl_temp<ND, NQ>();
-    static constexpr int oT0 = oAQ + 15 * Q3, oT1 = oT0 + nT;
+    static constexpr int oT0 = oF + 12 * Q3, oT1 = oT0 + nT;
     static constexpr int total = oT1 + nT;
     static constexpr size_t bytes = (size_t)total * sizeof(double);
 };
 
 template <int ND, int NQ, bool SPLIT>
-__global__ void __launch_bounds__(gl_threads<NQ>()) gl_aux_kernel(const StageArgs a, const GlArgs g) {
+__global__ void __launch_bounds__(gl_threads<NQ>(), 2) gl_aux_kernel(const StageArgs a, const GlArgs g) {
     using L = GlAuxLayout<ND, NQ, SPLIT>;
     constexpr int NT = L::NT, D3 = L::D3, Q3 = L::Q3, NF = NQ * NQ, T1W = gl_t1_width<SPLIT>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -444,6 +450,7 @@ __global__ void __launch_bounds__(gl_threads<NQ>()) gl_aux_kernel(const StageArg
     double* sR = sm + L::oR;
     double* sA = sm + L::oA;
     double* sAQ = sm + L::oAQ;
+    double* sF = sm + L::oF;
     double* t0 = sm + L::oT0;
     double* t1 = sm + L::oT1;
     const int cell = a.cell_begin + blockIdx.x;
@@ -453,7 +460,12 @@ __global__ void __launch_bounds__(gl_threads<NQ>()) gl_aux_kernel(const StageArg
     for (int i = threadIdx.x; i < 5 * D3; i += NT) sU[i] = __ldg(&a.U[(size_t)cell * 5 * D3 + i]);
     __syncthreads();
     gl_apply3<NT>(tab->chi, NQ, ND, sU, D3, sQ, Q3, 5, t0, t1, 1.0, false);
-    // volume part: rhs_d = chi^T W D_d (chi u)   (strong_dg.cpp:666-724; C = h^2 I folded into 1/h below)
+    // q_d = (1/h) M_aux^-1 [chi^T W D_d (chi u) + face lifts of (u* - u) n_d], one direction at
+    // a time (strong_dg.cpp:498-1008, dg_base.cpp:4089-4260 with use_auxiliary_eq; C = h^2 I),
+    // then its face values for both neighbours' dissipative fluxes and its values at the flux
+    // nodes, row s * 3 + d of each
+    double* tout = g.t2 + (size_t)cell * 6 * GL_T2W * NF;
+    double* face = sF;   // [2][s][q2]: W_face (u* - u) n_d on faces 2d and 2d + 1 (sF is free here)
     for (int d = 0; d < 3; ++d) {
         gl_pass<NT>(tab->dphi, NQ, NQ, d, NQ, NQ, NQ, sQ, Q3, t0, Q3, 5, 1.0, false);
         __syncthreads();
@@ -462,19 +474,13 @@ __global__ void __launch_bounds__(gl_threads<NQ>()) gl_aux_kernel(const StageArg
             t0[i] *= tab->wq[q % NQ] * tab->wq[(q / NQ) % NQ] * tab->wq[q / (NQ * NQ)];
         }
         __syncthreads();
-        // chi^T (x3) into sR[s * 3 + d]: strided over the 15 rows
         gl_passT<NT>(tab->chi, ND, NQ, 0, NQ, NQ, NQ, t0, Q3, t1, ND * NQ * NQ, 5, 1.0, false);
         __syncthreads();
         gl_passT<NT>(tab->chi, ND, NQ, 1, ND, NQ, NQ, t1, ND * NQ * NQ, t0, ND * ND * NQ, 5, 1.0, false);
         __syncthreads();
-        gl_passT<NT>(tab->chi, ND, NQ, 2, ND, ND, NQ, t0, ND * ND * NQ, sR + d * D3, 3 * D3, 5, 1.0, false);
-        __syncthreads();
-    }
-    // face part: (u* - u) n_d with u* the average of both sides' face values (strong_dg.cpp:871-1008)
-    {
-        double* face = t0;   // [f][s][q2]: W_face (u* - u) n_dn
-        for (int it = threadIdx.x; it < 6 * 5 * NF; it += NT) {
-            const int f = it / (5 * NF), s = (it / NF) % 5, q2 = it % NF;
+        gl_passT<NT>(tab->chi, ND, NQ, 2, ND, ND, NQ, t0, ND * ND * NQ, sR, D3, 5, 1.0, false);
+        for (int it = threadIdx.x; it < 2 * 5 * NF; it += NT) {   // faces 2d, 2d + 1
+            const int f = 2 * d + it / (5 * NF), s = (it / NF) % 5, q2 = it % NF;
             const int cn = __ldg(&a.nbr[cell * 6 + f]);
             const double uo = __ldg(&g.t1[(((size_t)cell * 6 + f) * T1W + s) * NF + q2]);
             const double ue = __ldg(&g.t1[(((size_t)cn * 6 + (f ^ 1)) * T1W + s) * NF + q2]);
@@ -482,20 +488,12 @@ __global__ void __launch_bounds__(gl_threads<NQ>()) gl_aux_kernel(const StageArg
             face[it] = tab->wq[q2 % NQ] * tab->wq[q2 / NQ] * ((0.5 * (uo + ue) - uo) * sgn);
         }
         __syncthreads();
-        // added into rhs_dn: sR[s*3 + dn] = sR + dn * D3 + s * 3 * D3 (sA, not yet written,
-        // holds the second pass: 30 ND^2 <= 15 ND^3)
-        gl_lift_faces<NT>(face, 5 * NF, NF, 5, NQ, ND, tab->chis[0], tab->chis[1], tab->chi, t1, sA, sR, 3 * D3, D3,
-                          1.0);
-    }
-    // lifted gradient q = (1/h) M_aux^-1 rhs   (dg_base.cpp:4089-4260, use_auxiliary_eq), then its
-    // face values for the dissipative numerical flux of both neighbours and its values at the
-    // flux nodes; five rows at a time
-    double* tout = g.t2 + (size_t)cell * 6 * GL_T2W * NF;
-    for (int b = 0; b < 3; ++b) {
-        gl_apply3<NT>(tab->minv_aux, ND, ND, sR + b * 5 * D3, D3, sA + b * 5 * D3, D3, 5, t0, t1, a.inv_h, false);
-        gl_face_values<NT>(sA + b * 5 * D3, D3, 5, ND, tab->chis[0], tab->chis[1], tab->chi, NQ, t0, t1,
-                           tout + b * 5 * NF, GL_T2W * NF, NF);
-        gl_apply3<NT>(tab->chi, NQ, ND, sA + b * 5 * D3, D3, sAQ + b * 5 * Q3, Q3, 5, t0, t1, 1.0, false);
+        gl_lift_faces<NT>(face, 5 * NF, NF, 5, NQ, ND, tab->chis[0], tab->chis[1], tab->chi, t1, sA, sR, D3, 0, 1.0,
+                          d);
+        gl_apply3<NT>(tab->minv_aux, ND, ND, sR, D3, sA, D3, 5, t0, t1, a.inv_h, false);
+        gl_face_values<NT>(sA, D3, 5, ND, tab->chis[0], tab->chis[1], tab->chi, NQ, t0, t1, tout + d * NF,
+                           GL_T2W * NF, 3 * NF);
+        gl_apply3<NT>(tab->chi, NQ, ND, sA, D3, sAQ + d * Q3, 3 * Q3, 5, t0, t1, 1.0, false);
     }
     // the split form evaluates the volume viscous flux at the entropy-projected state
     // (strong_dg.cpp:1328 before :1392); the face-normal flux interpolated to the faces uses
@@ -521,7 +519,7 @@ __global__ void __launch_bounds__(gl_threads<NQ>()) gl_aux_kernel(const StageArg
         }
         __syncthreads();
     }
-    double* sF = sR;   // [d][k][Q3] volume viscous flux, over the dead right-hand side and q
+    // sF: [d][k][Q3] volume viscous flux
     for (int q = threadIdx.x; q < Q3; q += NT) {
         double u[5], gq[5][3];
 #pragma unroll
@@ -606,12 +604,14 @@ struct GlStageLayout {
     static constexpr int oF = oDiv + 5 * Q3;              // 6 x 5 x NF face arrays
     static constexpr int nT = gl_temp<ND, NQ>();
     static constexpr int oT0 = oF + 30 * NF, oT1 = oT0 + nT;
-    static constexpr int total = oT1 + nT;
+    static constexpr int oQF = oT1 + nT;                 // split: the node quantities of two faces' nodes
+    static constexpr int total = oQF + (SPLIT ? 2 * NF * 11 : 0);
     static constexpr size_t bytes = (size_t)total * sizeof(double);
+    static_assert(2 * nT >= 2 * NF * NQ * 5, "the hybrid pair fluxes of one direction fit the temporaries");
 };
 
 template <int ND, int NQ, bool VISC, bool SPLIT>
-__global__ void __launch_bounds__(gl_threads<NQ>()) gl_stage_kernel(const StageArgs a, const GlArgs g) {
+__global__ void __launch_bounds__(gl_threads<NQ>(), 2) gl_stage_kernel(const StageArgs a, const GlArgs g) {
     using L = GlStageLayout<ND, NQ, VISC, SPLIT>;
     constexpr int NT = L::NT, D3 = L::D3, Q3 = L::Q3, NF = L::NF, T1W = gl_t1_width<SPLIT>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -799,39 +799,67 @@ __global__ void __launch_bounds__(gl_threads<NQ>()) gl_stage_kernel(const StageA
     __syncthreads();
     if constexpr (SPLIT) {
         // hybrid surface-volume two-point terms (strong_dg.cpp:3144-3350): between each face node
-        // (its projected state) and the flux nodes of the normal line through it; one face at a
-        // time, since the faces of one direction share the volume nodes
-        for (int f = 0; f < 6; ++f) {
-            const int dn = f >> 1, side = f & 1;
-            const double sgn = side ? 1.0 : -1.0;
+        // (its projected state) and the flux nodes of the normal line through it. One direction at
+        // a time (its two faces share the volume nodes): the face nodes' quantities, then every
+        // (face node, line node) pair flux, then the face sums and the volume sums, in the order
+        // face 2 dn before face 2 dn + 1 and line position by position.
+        double* sQF = sm + L::oQF;   // [11][2 NF]
+        double* s2 = t0;             // [2][NF][NQ][5] (t0 and t1 are contiguous)
+        for (int dn = 0; dn < 3; ++dn) {
             const double nv[3] = {dn == 0 ? 1.0 : 0.0, dn == 1 ? 1.0 : 0.0, dn == 2 ? 1.0 : 0.0};
-            for (int q2 = threadIdx.x; q2 < NF; q2 += NT) {
-                const double* to = g.t1 + ((size_t)cell * 6 + f) * T1W * NF + q2;
+            for (int it = threadIdx.x; it < 2 * NF; it += NT) {
+                const int side = it / NF, q2 = it % NF;
+                const double* to = g.t1 + ((size_t)cell * 6 + 2 * dn + side) * T1W * NF + q2;
                 double vo[5], uf[5];
 #pragma unroll
                 for (int s = 0; s < 5; ++s) vo[s] = __ldg(&to[(5 + s) * NF]);
                 gl_cons_from_entropy(vo, cst.gam, cst.gm1, uf);
                 NodeQ<double> qf;
                 node_prepare<double>(uf, tp, cst.gm1, qf, nullptr);
+                store_q<double>(sQF, 2 * NF, it, qf);
+            }
+            __syncthreads();
+            for (int it = threadIdx.x; it < 2 * NF * NQ; it += NT) {
+                const int side = it / (NF * NQ), r = it % (NF * NQ), q2 = r / NQ, l = r % NQ;
                 const int t1c = q2 % NQ, t2c = q2 / NQ;
-                const double wf = tab->wq[t1c] * tab->wq[t2c];
+                const int node = dn == 0 ? (t2c * NQ + t1c) * NQ + l : dn == 1 ? (t2c * NQ + l) * NQ + t1c
+                                                                               : (l * NQ + t2c) * NQ + t1c;
+                NodeQ<double> qv, qf;
+                load_q<double>(sN, Q3, node, qv);
+                load_q<double>(sQF, 2 * NF, side * NF + q2, qf);
+                double F[5];
+                two_point_n<double>(qv, qf, nv, tp, cst, F);
+#pragma unroll
+                for (int s = 0; s < 5; ++s) s2[(size_t)it * 5 + s] = F[s];
+            }
+            __syncthreads();
+            for (int it = threadIdx.x; it < 2 * NF; it += NT) {   // face sums
+                const int side = it / NF, q2 = it % NF, f = 2 * dn + side;
+                const double sgn = side ? 1.0 : -1.0;
+                const double wf = tab->wq[q2 % NQ] * tab->wq[q2 / NQ];
                 double hs[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
                 for (int l = 0; l < NQ; ++l) {
-                    const int node = dn == 0 ? (t2c * NQ + t1c) * NQ + l : dn == 1 ? (t2c * NQ + l) * NQ + t1c
-                                                                                   : (l * NQ + t2c) * NQ + t1c;
-                    NodeQ<double> qv;
-                    load_q<double>(sN, Q3, node, qv);
-                    double F[5];
-                    two_point_n<double>(qv, qf, nv, tp, cst, F);
                     const double Hop = tab->phis[side][l] * wf * sgn;
+                    const double* F = s2 + ((size_t)(side * NF + q2) * NQ + l) * 5;
 #pragma unroll
-                    for (int s = 0; s < 5; ++s) {
-                        hs[s] -= Hop * F[s];
-                        sDiv[s * Q3 + node] += Hop * F[s];
-                    }
+                    for (int s = 0; s < 5; ++s) hs[s] -= Hop * F[s];
                 }
 #pragma unroll
                 for (int s = 0; s < 5; ++s) sF[(f * 5 + s) * NF + q2] -= hs[s];
+            }
+            for (int it = threadIdx.x; it < NF * NQ; it += NT) {   // volume sums (other outputs)
+                const int q2 = it / NQ, l = it % NQ;
+                const int t1c = q2 % NQ, t2c = q2 / NQ;
+                const int node = dn == 0 ? (t2c * NQ + t1c) * NQ + l : dn == 1 ? (t2c * NQ + l) * NQ + t1c
+                                                                               : (l * NQ + t2c) * NQ + t1c;
+                const double wf = tab->wq[t1c] * tab->wq[t2c];
+#pragma unroll
+                for (int side = 0; side < 2; ++side) {
+                    const double Hop = tab->phis[side][l] * wf * (side ? 1.0 : -1.0);
+                    const double* F = s2 + ((size_t)(side * NF + q2) * NQ + l) * 5;
+#pragma unroll
+                    for (int s = 0; s < 5; ++s) sDiv[s * Q3 + node] += Hop * F[s];
+                }
             }
             __syncthreads();
         }
