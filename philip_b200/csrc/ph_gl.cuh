@@ -72,7 +72,11 @@ template <int NQ> __host__ __device__ constexpr int gl_threads() {
 }
 
 // Entropy variables of a conservative state (Euler::compute_entropy_variables, euler.cpp:811-830)
-// and the conservative state of entropy variables (:833-855), FP64.
+// and the conservative state of entropy variables (:833-855), FP64. The powers are taken through
+// logarithms: s = log(p rho^-gamma) = log p - gamma log rho, and
+// rho e = (gm1 / (-v4)^gamma)^(1/gm1) exp(-s / gm1) = exp((log gm1 - gamma log(-v4) - s) / gm1),
+// one exponential and one or two logarithms instead of the powers' own logarithm-exponential
+// pairs (the same values to rounding).
 __device__ __forceinline__ void gl_entropy_vars(const double u[5], double gam, double gm1, double v[5],
                                                 unsigned* st) {
     const double rho = u[0];
@@ -80,23 +84,25 @@ __device__ __forceinline__ void gl_entropy_vars(const double u[5], double gam, d
 #pragma unroll
     for (int d = 0; d < 3; ++d) { const double w = u[1 + d] / rho; v2 = v2 + w * w; }
     const double p = positive<double>(gm1 * (u[4] - 0.5 * rho * v2), st);
-    const double s = log(p * pow(rho, -gam));
+    const double s = log(p) - gam * log(rho);
     const double rt = p / gm1;
-    v[0] = (rt * (gam + 1.0 - s) - u[4]) / rt;
+    const double irt = 1.0 / rt;
+    v[0] = (rt * (gam + 1.0 - s) - u[4]) * irt;
 #pragma unroll
-    for (int d = 0; d < 3; ++d) v[1 + d] = u[1 + d] / rt;
-    v[4] = -rho / rt;
+    for (int d = 0; d < 3; ++d) v[1 + d] = u[1 + d] * irt;
+    v[4] = -rho * irt;
 }
 __device__ __forceinline__ void gl_cons_from_entropy(const double v[5], double gam, double gm1, double u[5]) {
     double vv = 0.0;
 #pragma unroll
     for (int d = 0; d < 3; ++d) vv += v[1 + d] * v[1 + d];
-    const double s = gam - v[0] + 0.5 * vv / v[4];
-    const double rt = pow(gm1 / pow(-v[4], gam), 1.0 / gm1) * exp(-s / gm1);
+    const double iv4 = 1.0 / v[4];
+    const double s = gam - v[0] + 0.5 * vv * iv4;
+    const double rt = exp((log(gm1) - gam * log(-v[4]) - s) / gm1);
     u[0] = -rt * v[4];
 #pragma unroll
     for (int d = 0; d < 3; ++d) u[1 + d] = rt * v[1 + d];
-    u[4] = rt * (1.0 - 0.5 * vv / v[4]);
+    u[4] = rt * (1.0 - 0.5 * vv * iv4);
 }
 
 // One sum-factorised pass along direction d: out[s][o] (+)= scale * sum_l A[r * cols + l] in[s][o, r -> l]
@@ -508,7 +514,7 @@ __global__ void __launch_bounds__(gl_threads<NQ>(), 2) gl_aux_kernel(const Stage
             for (int s = 0; s < 5; ++s) t0[s * Q3 + q] = v[s];
         }
         __syncthreads();
-        gl_apply3<NT>(tab->P, NQ, NQ, t0, Q3, sU, Q3, 5, t1, sR, 1.0, false);   // sR is free until the fluxes
+        gl_apply3<NT>(tab->P, NQ, NQ, t0, Q3, sU, Q3, 5, t1, sF, 1.0, false);   // sF is free until the fluxes
         for (int q = threadIdx.x; q < Q3; q += NT) {
             double v[5], u[5];
 #pragma unroll
