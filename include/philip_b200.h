@@ -47,7 +47,8 @@ enum { PH_FP64 = 0, PH_FP32_RESIDUAL = 1 };          /* arithmetic of the residu
  *   diss_num_flux: 0 symm_internal_penalty, 1 bassi_rebay_2, 2 central_visc_flux
  *   flux_reconstruction: 0 cDG, 1 cSD, 2 cHU, 3 cNegative, 4 cNegative2, 5 cPlus,
  *                        6 c10Thousand, 7 cHULumped, 8 user_specified_value
- *   flux_reconstruction_aux: 0 kDG (the GPU path supports kDG)
+ *   flux_reconstruction_aux: 0 kDG, 1 kSD, 2 kHU, 3 kNegative, 4 kNegative2, 5 kPlus (p = 2..5),
+ *                            6 k10Thousand
  *   runge_kutta_method: 0 rk4_ex, 1 ssprk3_ex, 2 heun2_ex, 3 euler_ex (4-6 implicit: not on this path),
  *                       7 RK4_3_5_3SStar, 8 RK3_2_5F_3SStarPlus, 9 RK4_3_9F_3SStarPlus,
  *                       10 RK5_4_10F_3SStarPlus (low-storage, with an embedded error estimate)

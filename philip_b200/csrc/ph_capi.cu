@@ -150,6 +150,15 @@ int fr_parameter(int type, int p, double user, double& c) {
     return 1;
 }
 
+// FR auxiliary correction parameter (local_Flux_Reconstruction_operator_aux::
+// get_FR_aux_correction_parameter, operators.cpp:1809-1835): kDG, kSD, kHU, kNegative, kNegative2,
+// kPlus, k10Thousand (indices 0..6) take the values of cDG, cSD, cHU, cNegative, cNegative2, cPlus,
+// c10Thousand, which have the same indices in fr_parameter
+int fr_aux_parameter(int type, int p, double& k) {
+    if (type < 0 || type > 6) return 1;
+    return fr_parameter(type, p, 0.0, k);
+}
+
 // deal.II active-cell order of the periodic cube: recursive children (child = x+2y+4z)
 // for hyper_cube + refine_global, lexicographic for subdivided_hyper_cube
 // (straight_periodic_cube.cpp:38-67).
@@ -269,7 +278,8 @@ int check_param_ranges(const ph_params* prm) {
         prm->conv_num_flux < 0 || prm->conv_num_flux > 5 || prm->diss_num_flux < 0 || prm->diss_num_flux > 2 ||
         prm->runge_kutta_method < 0 || prm->runge_kutta_method > 10 ||
         (prm->runge_kutta_method >= 4 && prm->runge_kutta_method <= 6) || prm->precision < 0 || prm->precision > 1 ||
-        prm->flux_nodes_type < 0 || prm->flux_nodes_type > 1)
+        prm->flux_nodes_type < 0 || prm->flux_nodes_type > 1 || prm->flux_reconstruction_aux < 0 ||
+        prm->flux_reconstruction_aux > 6)
         return fail(PH_ERR_INVALID, "parameter out of range");
     return PH_OK;
 }
@@ -280,7 +290,6 @@ const char* uncollocated_reason(const ph_mesh_desc* mesh, const ph_params* prm) 
     if (prm->overintegration < 0 || prm->overintegration > 2) return "overintegration must be 0, 1 or 2";
     if (prm->poly_degree < 1 || prm->poly_degree + 1 + prm->overintegration > ph::GL_MAXQ)
         return "uncollocated flux nodes: poly_degree >= 1 and poly_degree + 1 + overintegration <= 7";
-    if (prm->flux_reconstruction_aux != 0) return "flux_reconstruction_aux must be kDG";
     if (is_curvilinear(mesh)) return "uncollocated flux nodes take affine meshes";
     if (prm->precision != PH_FP64) return "uncollocated flux nodes take the FP64 path";
     if (prm->runge_kutta_method > 3) return "uncollocated flux nodes take the Butcher RK methods";
@@ -292,7 +301,6 @@ const char* unsupported_reason(const ph_mesh_desc* mesh, const ph_params* prm) {
     if (uncollocated(prm))
         return "this entry point is collocated: flux_nodes_type = GLL and overintegration = 0 (contexts take both)";
     if (prm->poly_degree < 1 || prm->poly_degree > 6) return "poly_degree must be 1..6";
-    if (prm->flux_reconstruction_aux != 0) return "flux_reconstruction_aux must be kDG";
     if (is_curvilinear(mesh)) {
         if (mesh->mapping_support_points == nullptr && mesh->grid_degree != prm->poly_degree)
             return "curvilinear meshes take grid_degree = poly_degree";
@@ -313,23 +321,30 @@ int build_operators(const ph_params* prm, ph::OpTab& tab, bool& fr, std::vector<
         lagrange(x, x[a], v.data(), dv.data());
         for (int l = 0; l < N1; ++l) D[a * N1 + l] = dv[l];
     }
-    double cfr = 0.0;
+    double cfr = 0.0, kaux = 0.0;
     if (fr_parameter(prm->flux_reconstruction, prm->poly_degree, prm->FR_user_specified_correction_parameter_value, cfr))
         return fail(PH_ERR_UNSUPPORTED, "flux_reconstruction type not defined for this degree");
+    if (fr_aux_parameter(prm->flux_reconstruction_aux, prm->poly_degree, kaux))
+        return fail(PH_ERR_UNSUPPORTED, "flux_reconstruction_aux type not defined for this degree");
     std::vector<double> Dp(N1 * N1, 0.0);
     for (int i = 0; i < N1; ++i) Dp[i * N1 + i] = 1.0;
     for (int k = 0; k < prm->poly_degree; ++k) Dp = mat_mul(D, Dp, N1);
-    std::vector<double> MK(N1 * N1, 0.0);
+    // K = (D^p)^T M D^p without its parameter; M + c K for the primary equation, M + k K for the
+    // auxiliary one (local_Flux_Reconstruction_operator(_aux)::build_1D_volume_operator)
+    std::vector<double> MK(N1 * N1, 0.0), MKa(N1 * N1, 0.0);
     for (int i = 0; i < N1; ++i)
         for (int j = 0; j < N1; ++j) {
             double kij = 0.0;
             for (int q = 0; q < N1; ++q) kij += Dp[q * N1 + i] * w[q] * Dp[q * N1 + j];
             MK[i * N1 + j] = (i == j ? w[i] : 0.0) + cfr * kij;
+            MKa[i * N1 + j] = (i == j ? w[i] : 0.0) + kaux * kij;
         }
-    std::vector<double> Minv;
+    std::vector<double> Minv, Minva;
     if (!mat_inv(MK, N1, Minv)) return fail(PH_ERR_INVALID, "singular FR mass matrix");
+    if (!mat_inv(MKa, N1, Minva)) return fail(PH_ERR_INVALID, "singular auxiliary FR mass matrix");
     fr = (cfr != 0.0);
     std::memset(&tab, 0, sizeof(tab));
+    tab.aux_fr = kaux != 0.0;
     for (int a = 0; a < N1; ++a) {
         tab.w[a] = w[a];
         for (int l = 0; l < N1; ++l) {
@@ -337,6 +352,7 @@ int build_operators(const ph_params* prm, ph::OpTab& tab, bool& fr, std::vector<
             tab.Dsk[a * ph::MAXN1 + l] = (w[a] * D[a * N1 + l] - w[l] * D[l * N1 + a]) / w[a];
             tab.Minv[a * ph::MAXN1 + l] = Minv[a * N1 + l];
             tab.B[a * ph::MAXN1 + l] = Minv[a * N1 + l] * w[l];
+            tab.Baux[a * ph::MAXN1 + l] = Minva[a * N1 + l] * w[l];
         }
     }
     return PH_OK;
@@ -403,25 +419,30 @@ int build_gl_operators(const ph_params* prm, ph::GlTab& t, ph::OpTab& ops) {
             for (int i = 0; i < nd; ++i) v += t.chis[side][i] * proj[i * nq + q];
             t.ps[side][q] = v;
         }
-    // FR: D = M^-1 Schi, K = c (D^p)^T M D^p; kDG for the auxiliary equation (K = 0)
-    double cfr = 0.0;
+    // FR: D = M^-1 Schi, K = c (D^p)^T M D^p; the auxiliary equation's K_aux takes k for c
+    double cfr = 0.0, kaux = 0.0;
     if (fr_parameter(prm->flux_reconstruction, p, prm->FR_user_specified_correction_parameter_value, cfr))
         return fail(PH_ERR_UNSUPPORTED, "flux_reconstruction type not defined for this degree");
+    if (fr_aux_parameter(prm->flux_reconstruction_aux, p, kaux))
+        return fail(PH_ERR_UNSUPPORTED, "flux_reconstruction_aux type not defined for this degree");
     const std::vector<double> Dm = mat_mul(Mi, Schi, nd);
     std::vector<double> Dp((size_t)nd * nd, 0.0);
     for (int i = 0; i < nd; ++i) Dp[i * nd + i] = 1.0;
     for (int k = 0; k < p; ++k) Dp = mat_mul(Dm, Dp, nd);
-    std::vector<double> MK(M);
+    std::vector<double> MK(M), MKa(M);
     for (int i = 0; i < nd; ++i)
         for (int j = 0; j < nd; ++j) {
             double kij = 0.0;
             for (int a = 0; a < nd; ++a)
                 for (int b = 0; b < nd; ++b) kij += Dp[a * nd + i] * M[a * nd + b] * Dp[b * nd + j];
             MK[i * nd + j] += cfr * kij;
+            MKa[i * nd + j] += kaux * kij;
         }
-    std::vector<double> MKi;
+    std::vector<double> MKi, MKai;
     if (!mat_inv(MK, nd, MKi)) return fail(PH_ERR_INVALID, "singular FR mass matrix");
-    for (int i = 0; i < nd * nd; ++i) { t.minv[i] = MKi[i]; t.minv_aux[i] = Mi[i]; }
+    if (kaux == 0.0) MKai = Mi;
+    else if (!mat_inv(MKa, nd, MKai)) return fail(PH_ERR_INVALID, "singular auxiliary FR mass matrix");
+    for (int i = 0; i < nd * nd; ++i) { t.minv[i] = MKi[i]; t.minv_aux[i] = MKai[i]; }
     for (int a = 0; a < nd; ++a)
         for (int l = 0; l < nd; ++l) ops.Minv[a * ph::MAXN1 + l] = MKi[a * nd + l];
     return PH_OK;
@@ -2240,11 +2261,14 @@ extern "C" int ph_residual_noalloc(const ph_mesh_desc* mesh, const ph_params* pr
     // this entry point makes no heap allocation either)
     double x[ph::MAXN1], w[ph::MAXN1], D[ph::MAXN1 * ph::MAXN1], Dp[ph::MAXN1 * ph::MAXN1];
     double MK[ph::MAXN1 * ph::MAXN1], Minv[ph::MAXN1 * ph::MAXN1], tmp[ph::MAXN1 * ph::MAXN1];
+    double MKa[ph::MAXN1 * ph::MAXN1], Minva[ph::MAXN1 * ph::MAXN1];
     noalloc_gll(N1, x, w);
     for (int a = 0; a < N1; ++a) noalloc_lagrange_derivative(x, N1, x[a], &D[a * N1]);
-    double cfr = 0.0;
+    double cfr = 0.0, kaux = 0.0;
     if (fr_parameter(prm->flux_reconstruction, prm->poly_degree, prm->FR_user_specified_correction_parameter_value, cfr))
         return fail(PH_ERR_UNSUPPORTED, "flux_reconstruction type not defined for this degree");
+    if (fr_aux_parameter(prm->flux_reconstruction_aux, prm->poly_degree, kaux))
+        return fail(PH_ERR_UNSUPPORTED, "flux_reconstruction_aux type not defined for this degree");
     for (int i = 0; i < N1 * N1; ++i) Dp[i] = (i % (N1 + 1) == 0) ? 1.0 : 0.0;
     for (int k = 0; k < prm->poly_degree; ++k) {
         for (int i = 0; i < N1; ++i)
@@ -2260,10 +2284,13 @@ extern "C" int ph_residual_noalloc(const ph_mesh_desc* mesh, const ph_params* pr
             double kij = 0.0;
             for (int q = 0; q < N1; ++q) kij += Dp[q * N1 + i] * w[q] * Dp[q * N1 + j];
             MK[i * N1 + j] = (i == j ? w[i] : 0.0) + cfr * kij;
+            MKa[i * N1 + j] = (i == j ? w[i] : 0.0) + kaux * kij;
         }
     if (!noalloc_invert(MK, N1, Minv)) return fail(PH_ERR_INVALID, "singular FR mass matrix");
+    if (!noalloc_invert(MKa, N1, Minva)) return fail(PH_ERR_INVALID, "singular auxiliary FR mass matrix");
     ph::OpTab tab;
     std::memset(&tab, 0, sizeof(tab));
+    tab.aux_fr = kaux != 0.0;
     for (int a = 0; a < N1; ++a) {
         tab.w[a] = w[a];
         for (int l = 0; l < N1; ++l) {
@@ -2271,6 +2298,7 @@ extern "C" int ph_residual_noalloc(const ph_mesh_desc* mesh, const ph_params* pr
             tab.Dsk[a * ph::MAXN1 + l] = (w[a] * D[a * N1 + l] - w[l] * D[l * N1 + a]) / w[a];
             tab.Minv[a * ph::MAXN1 + l] = Minv[a * N1 + l];
             tab.B[a * ph::MAXN1 + l] = Minv[a * N1 + l] * w[l];
+            tab.Baux[a * ph::MAXN1 + l] = Minva[a * N1 + l] * w[l];
         }
     }
     noalloc_set_tables<<<1, 128, 0, stream>>>(tab);

@@ -157,13 +157,13 @@ void stage_launch_shape(int fp32, bool visc, bool split, int* threads, int* cpc,
     }
 }
 
-template <typename R, int N1>
+template <typename R, int N1, bool FRA>
 static cudaError_t launch_aux_prec(const double* U, const int* nbr, const OpTab& ops, int cell_begin, int nc,
                                    double inv_h, const PhysConst& pc, void* Fv, cudaStream_t s) {
     constexpr int CPC = cells_per_cta<N1>();
-    using L = AuxLayout<N1, CPC>;
+    using L = AuxLayout<N1, CPC, FRA>;
     constexpr size_t bytes = L::template bytes<R>();
-    auto kern = aux_kernel<R, N1, CPC>;
+    auto kern = aux_kernel<R, N1, CPC, FRA>;
     int dev = 0;
     cudaGetDevice(&dev);
     static bool configured[64] = {false};
@@ -173,7 +173,7 @@ static cudaError_t launch_aux_prec(const double* U, const int* nbr, const OpTab&
         configured[dev] = true;
     }
     AuxCoef<R> co{};
-    for (int i = 0; i < MAXN1 * MAXN1; ++i) co.D[i] = (R)ops.D[i];
+    for (int i = 0; i < MAXN1 * MAXN1; ++i) { co.D[i] = (R)ops.D[i]; co.Ba[i] = (R)ops.Baux[i]; }
     co.inv_wend = R(1) / (R)ops.w[0];
     const int grid = (nc - cell_begin + CPC - 1) / CPC;
     if (grid <= 0) return cudaErrorInvalidValue;
@@ -184,8 +184,11 @@ static cudaError_t launch_aux_prec(const double* U, const int* nbr, const OpTab&
 template <int N1>
 cudaError_t launch_aux(const double* U, const int* nbr, const OpTab& ops, int cell_begin, int nc, double inv_h,
                        const PhysConst& pc, int fp32, void* Fv, cudaStream_t s) {
-    return fp32 ? launch_aux_prec<float, N1>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, s)
-                : launch_aux_prec<double, N1>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, s);
+    if (ops.aux_fr)
+        return fp32 ? launch_aux_prec<float, N1, true>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, s)
+                    : launch_aux_prec<double, N1, true>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, s);
+    return fp32 ? launch_aux_prec<float, N1, false>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, s)
+                : launch_aux_prec<double, N1, false>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, s);
 }
 
 template <int N1>

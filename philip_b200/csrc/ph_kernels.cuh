@@ -65,6 +65,8 @@ struct OpTab {
     double B[MAXN1 * MAXN1];      // (M+K)^{-1} diag(w)  (FR mass inverse in G units)
     double Minv[MAXN1 * MAXN1];   // (M+K)^{-1}
     double w[MAXN1];              // GLL weights on [0,1]
+    double Baux[MAXN1 * MAXN1];   // (M+K_aux)^{-1} diag(w), the auxiliary equation's FR mass inverse
+    int aux_fr;                   // K_aux != 0: the auxiliary kernel applies Baux(x)Baux(x)Baux
 };
 
 struct StageArgs {
@@ -1011,11 +1013,13 @@ residual_kernel_batched(const StageArgs* __restrict__ inst, const BatchTile* __r
 //  node form (p <= 3): one thread per node, coefficients from shared memory (fewer barriers
 //    and less shared memory, which wins at low order).
 // Both sum every node's terms in the same order (over l, then over directions).
-template <typename R, int N1> __host__ __device__ constexpr bool aux_line_form() {
-    return N1 >= 5;
+// An FR auxiliary correction (K_aux != 0) multiplies the gradient by Baux(x)Baux(x)Baux before
+// the flux; it needs the whole gradient in shared memory, so it always takes the line form.
+template <typename R, int N1, bool FRA = false> __host__ __device__ constexpr bool aux_line_form() {
+    return N1 >= 5 || FRA;
 }
 
-template <int N1, int CPC>
+template <int N1, int CPC, bool FRA = false>
 struct AuxLayout {
     static constexpr int NP = N1 * N1 * N1, NF = N1 * N1;
     static constexpr int NT = ((CPC * NP + 31) / 32) * 32 > 512 ? 512 : ((CPC * NP + 31) / 32) * 32;
@@ -1024,14 +1028,15 @@ struct AuxLayout {
     template <typename R>
     static constexpr size_t bytes() {
         return sizeof(R) * ((size_t)CPC * 5 * NP + (size_t)CPC * 6 * 5 * NF +
-                            (aux_line_form<R, N1>() ? (size_t)CPC * 15 * NP : N1 * N1 + (size_t)CPC * 12 * NP));
+                            (aux_line_form<R, N1, FRA>() ? (size_t)CPC * 15 * NP : N1 * N1 + (size_t)CPC * 12 * NP));
     }
 };
 
 // The 1-D differentiation matrix and the lifting weight 1/w_end of the auxiliary kernel,
 // passed by value (in the line form each coefficient is then a parameter-bank operand).
 template <typename R> struct AuxCoef {
-    R D[MAXN1 * MAXN1];   // D[pos][l] = l_l'(x_pos)
+    R D[MAXN1 * MAXN1];    // D[pos][l] = l_l'(x_pos)
+    R Ba[MAXN1 * MAXN1];   // (M+K_aux)^{-1} diag(w) (read only with an FR auxiliary correction)
     R inv_wend;
 };
 
@@ -1042,11 +1047,11 @@ template <int N1> __device__ __forceinline__ int line_node(int d, int line, int 
     return d == 0 ? node_of<N1>(pos, a, b) : d == 1 ? node_of<N1>(a, pos, b) : node_of<N1>(a, b, pos);
 }
 
-template <typename R, int N1, int CPC>
-__global__ void __launch_bounds__(AuxLayout<N1, CPC>::NT)
+template <typename R, int N1, int CPC, bool FRA>
+__global__ void __launch_bounds__(AuxLayout<N1, CPC, FRA>::NT)
 aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, int cell_begin, int nc, R inv_h, PhysConst pc,
            AuxCoef<R> co, R* __restrict__ Fv) {
-    using L = AuxLayout<N1, CPC>;
+    using L = AuxLayout<N1, CPC, FRA>;
     constexpr int NP = L::NP, NF = L::NF, NT = L::NT;
     constexpr int VT = viscous_terms_per_cell<N1>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1069,7 +1074,7 @@ aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, int cell_b
         const int nn = face_node_volume_index<N1>(f, fn, (f & 1) ? 0 : N1 - 1);
         sT[it] = (R)__ldg(&U[((size_t)cn * 5 + s) * NP + nn]);
     }
-    if constexpr (aux_line_form<R, N1>()) {
+    if constexpr (aux_line_form<R, N1, FRA>()) {
         R* sG = sT + CPC * 6 * 5 * NF;   // [c][d][5][NP] gradient, later [c][d][4][NP] flux
         __syncthreads();
         // lifted gradient: D u along the line, the lifting u* - u = (u_ext - u)/2 at both ends;
@@ -1100,6 +1105,31 @@ aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, int cell_b
             }
         }
         __syncthreads();
+        if constexpr (FRA) {
+            // FR auxiliary correction (M+K_aux)^{-1} in three directions, applied to the DG
+            // gradient diag(w)^{-1} r as Baux = (M+K_aux)^{-1} diag(w) along x, then y, then z
+            // (the order of the sum-factorised inverse mass); one thread per (component, line)
+#pragma unroll
+            for (int e = 0; e < 3; ++e) {
+                const int st = e == 0 ? 1 : e == 1 ? N1 : N1 * N1;
+                for (int task = tid; task < CPC * 15 * NF; task += NT) {
+                    const int c = task / (15 * NF), r = task % (15 * NF);
+                    const int line = r % NF, k = r / NF;
+                    R* g = sG + (c * 15 + k) * NP + line_node<N1>(e, line, 0);
+                    R v[N1];
+#pragma unroll
+                    for (int l = 0; l < N1; ++l) v[l] = g[l * st];
+#pragma unroll
+                    for (int pos = 0; pos < N1; ++pos) {
+                        R acc = R(0);
+#pragma unroll
+                        for (int l = 0; l < N1; ++l) acc += co.Ba[pos * MAXN1 + l] * v[l];
+                        g[pos * st] = acc;
+                    }
+                }
+                __syncthreads();
+            }
+        }
         // viscous flux per node; it replaces the node's own gradient entries
         for (int it = tid; it < CPC * NP; it += NT) {
             const int c = it / NP, node = it % NP;

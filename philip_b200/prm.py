@@ -21,7 +21,8 @@ CONV_FLUX = {"lax_friedrichs": 0, "roe": 1, "central_flux": 2, "two_point_flux":
 DISS_FLUX = {"symm_internal_penalty": 0, "bassi_rebay_2": 1, "central_visc_flux": 2}
 FR = {"cDG": 0, "cSD": 1, "cHU": 2, "cNegative": 3, "cNegative2": 4, "cPlus": 5, "c10Thousand": 6,
       "cHULumped": 7, "user_specified_value": 8}
-FR_AUX = {"kDG": 0}
+FR_AUX = {"kDG": 0, "kSD": 1, "kHU": 2, "kNegative": 3, "kNegative2": 4, "kPlus": 5,   # all_parameters.h:299
+          "k10Thousand": 6}
 RK = {"rk4_ex": 0, "ssprk3_ex": 1, "heun2_ex": 2, "euler_ex": 3,   # parameters_ode_solver.h:66-78 order
       "RK4_3_5_3SStar": 7, "RK3_2_5F_3SStarPlus": 8, "RK4_3_9F_3SStarPlus": 9, "RK5_4_10F_3SStarPlus": 10}
 RK_ORDER = {"rk4_ex": 4, "ssprk3_ex": 3, "heun2_ex": 2, "euler_ex": 1, "RK4_3_5_3SStar": 4,
@@ -205,7 +206,7 @@ class Parameters:
         p.flux_reconstruction = FR[self.get("flux_reconstruction")]
         aux = self.get("flux_reconstruction_aux")
         if aux not in FR_AUX:
-            raise ValueError(f"flux_reconstruction_aux {aux!r}: the B200 path implements kDG")
+            raise ValueError(f"flux_reconstruction_aux {aux!r} is not a reference value")
         p.flux_reconstruction_aux = FR_AUX[aux]
         p.FR_user_specified_correction_parameter_value = float(self.get("FR_user_specified_correction_parameter_value"))
         if self.get("ODE solver/ode_solver_type") not in ("runge_kutta", "rrk_explicit"):
@@ -257,6 +258,7 @@ class Parameters:
             "two_point_num_flux_type": self.get("two_point_num_flux_type"),
             "conv_num_flux": self.get("conv_num_flux"), "diss_num_flux": self.get("diss_num_flux"),
             "flux_reconstruction": self.get("flux_reconstruction"),
+            "flux_reconstruction_aux": self.get("flux_reconstruction_aux"),
             "runge_kutta_method": self.get("ODE solver/runge_kutta_method"),
             "gamma_gas": float(self.get("euler/gamma_gas")), "mach_infinity": float(self.get("euler/mach_infinity")),
             "reynolds_number_inf": float(self.get("navier_stokes/reynolds_number_inf")),

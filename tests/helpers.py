@@ -10,12 +10,13 @@ TWO_PI = 6.28318530717958623200
 
 def prm_dict(poly_degree=3, n_cells=4, pde="euler", split=True, two_point="CH",
              conv="two_point_flux_with_roe_dissipation", diss="symm_internal_penalty", fr="cDG",
-             rk="rk4_ex", mach=0.1, reynolds=1600.0, prandtl=0.71, left=0.0, right=TWO_PI,
+             fr_aux="kDG", rk="rk4_ex", mach=0.1, reynolds=1600.0, prandtl=0.71, left=0.0, right=TWO_PI,
              cfl=0.1, final_time=1.0, flow_case="taylor_green_vortex"):
     return {
         "dimension": 3, "pde_type": pde, "use_weak_form": False, "flux_nodes_type": "GLL",
         "use_split_form": split, "two_point_num_flux_type": two_point, "conv_num_flux": conv,
-        "diss_num_flux": diss, "flux_reconstruction": fr, "all_boundaries_are_periodic": True,
+        "diss_num_flux": diss, "flux_reconstruction": fr, "flux_reconstruction_aux": fr_aux,
+        "all_boundaries_are_periodic": True,
         "do_renumber_dofs": False,
         "ODE solver/ode_solver_type": "runge_kutta", "ODE solver/runge_kutta_method": rk,
         "euler/mach_infinity": mach, "navier_stokes/reynolds_number_inf": reynolds,

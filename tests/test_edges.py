@@ -58,6 +58,9 @@ REFUSED = [
      _lib.PH_ERR_UNSUPPORTED, "Butcher"),
     ("rrk_in_precision_form", lambda p: (setattr(p, "use_relaxation_runge_kutta", 1), setattr(p, "precision", 1)),
      _lib.PH_ERR_UNSUPPORTED, "FP64"),
+    ("kplus_aux_at_degree_6", lambda p: (setattr(p, "poly_degree", 6), setattr(p, "flux_reconstruction_aux", 5)),
+     _lib.PH_ERR_UNSUPPORTED, "flux_reconstruction_aux"),
+    ("aux_fr_type_7", lambda p: setattr(p, "flux_reconstruction_aux", 7), _lib.PH_ERR_INVALID, "out of range"),
 ]
 
 

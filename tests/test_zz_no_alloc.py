@@ -31,6 +31,7 @@ CASES = [
     ("euler_CH_roe_p5", dict(poly_degree=5, n_cells=2)),
     ("ns_conservative_cHU_p4", dict(poly_degree=4, n_cells=3, pde="navier_stokes", split=False, conv="roe",
                                     fr="cHU")),
+    ("ns_CH_kSD_aux_p3", dict(poly_degree=3, n_cells=3, pde="navier_stokes", fr_aux="kSD")),
 ]
 
 
