@@ -443,6 +443,18 @@ int build_gl_operators(const ph_params* prm, ph::GlTab& t, ph::OpTab& ops) {
     if (kaux == 0.0) MKai = Mi;
     else if (!mat_inv(MKa, nd, MKai)) return fail(PH_ERR_INVALID, "singular auxiliary FR mass matrix");
     for (int i = 0; i < nd * nd; ++i) { t.minv[i] = MKi[i]; t.minv_aux[i] = MKai[i]; }
+    // chi (M + K_aux)^-1 chi^T (nq x nq): the auxiliary equation's inverse mass seen from the flux
+    // nodes (solution values at the flux nodes of (M + K_aux)^-1 chi^T applied to flux-node data)
+    for (int a = 0; a < nq; ++a)
+        for (int b = 0; b < nq; ++b) {
+            double v = 0.0;
+            for (int i = 0; i < nd; ++i) {
+                double w = 0.0;
+                for (int j = 0; j < nd; ++j) w += MKai[i * nd + j] * chi[b * nd + j];
+                v += chi[a * nd + i] * w;
+            }
+            t.haux[a * nq + b] = v;
+        }
     for (int a = 0; a < nd; ++a)
         for (int l = 0; l < nd; ++l) ops.Minv[a * ph::MAXN1 + l] = MKi[a * nd + l];
     return PH_OK;
@@ -955,12 +967,12 @@ int dispatch_gl(ph_ctx* c, int kernel, const ph::StageArgs& a) {
     cudaError_t e;
     timer_begin(c);
     switch (c->N1) {
-    case 2: e = ph::launch_gl<2>(kernel, c->NQ, a, g, c->visc, c->split, c->stream); break;
-    case 3: e = ph::launch_gl<3>(kernel, c->NQ, a, g, c->visc, c->split, c->stream); break;
-    case 4: e = ph::launch_gl<4>(kernel, c->NQ, a, g, c->visc, c->split, c->stream); break;
-    case 5: e = ph::launch_gl<5>(kernel, c->NQ, a, g, c->visc, c->split, c->stream); break;
-    case 6: e = ph::launch_gl<6>(kernel, c->NQ, a, g, c->visc, c->split, c->stream); break;
-    case 7: e = ph::launch_gl<7>(kernel, c->NQ, a, g, c->visc, c->split, c->stream); break;
+    case 2: e = ph::launch_gl<2>(kernel, c->NQ, a, g, c->h_gl, c->visc, c->split, c->stream); break;
+    case 3: e = ph::launch_gl<3>(kernel, c->NQ, a, g, c->h_gl, c->visc, c->split, c->stream); break;
+    case 4: e = ph::launch_gl<4>(kernel, c->NQ, a, g, c->h_gl, c->visc, c->split, c->stream); break;
+    case 5: e = ph::launch_gl<5>(kernel, c->NQ, a, g, c->h_gl, c->visc, c->split, c->stream); break;
+    case 6: e = ph::launch_gl<6>(kernel, c->NQ, a, g, c->h_gl, c->visc, c->split, c->stream); break;
+    case 7: e = ph::launch_gl<7>(kernel, c->NQ, a, g, c->h_gl, c->visc, c->split, c->stream); break;
     default: return fail(PH_ERR_UNSUPPORTED, "polynomial degree outside 1..6");
     }
     if (e != cudaSuccess) return fail(PH_ERR_CUDA, std::string(kName[kernel]) + " launch: " + cudaGetErrorString(e));

@@ -6,14 +6,18 @@
 // Here the 1-D operators are dense: the interpolation chi (nq x nd) from the solution
 // nodes to the flux nodes, its face rows, the entropy projection (chi M^-1 chi^T W), the
 // flux-node differentiation and the FR mass inverse (M + K)^-1 with M = chi^T W chi. Every
-// one is applied direction by direction (sum factorisation, operators.cpp:294-649).
+// one is applied direction by direction (sum factorisation, operators.cpp:294-649): one thread
+// per 1-D line holds the line in registers, and the operator, a kernel parameter, is read with
+// compile-time indices (the extents are template arguments), so its entries are operands of
+// the FMAs rather than memory loads.
 //
 // Three kernels per residual evaluation (one CTA per cell each):
 //   gl_trace_kernel  the state's face values (chi_s (x) chi (x) chi U) and, for the split
 //                    form, the face values of the projected entropy variables, per face
 //   gl_aux_kernel    (Navier-Stokes) the lifted gradient q = (M_aux)^-1 [chi^T W D(chi u)
-//                    + face (u* - u) n], then the viscous volume term -chi^T W div(F_v), the
-//                    face values of q and the face-normal volume viscous flux
+//                    + face (u* - u) n], kept at the flux nodes, then the viscous volume term
+//                    -chi^T W div(F_v), and per face node F_v(u, q) . n and the face-normal
+//                    volume viscous flux
 //   gl_stage_kernel  volume term (two-point split form with the skew operator on flux-node
 //                    lines, or the conservative divergence), hybrid surface-volume two-point
 //                    terms, numerical fluxes, lifts, (M+K)^-1 and the RK stage update
@@ -47,18 +51,20 @@ struct GlTab {
     double ps[2][GL_MAXQ];            // chis[side] M^-1 chi^T W: face value of the projection
     double minv[GL_MAXD * GL_MAXD];   // (M + K)^-1
     double minv_aux[GL_MAXD * GL_MAXD];
+    double haux[GL_MAXQ * GL_MAXQ];   // chi (M + K_aux)^-1 chi^T
 };
 
 // Device buffers of the uncollocated path (per cell, reference units).
 struct GlArgs {
     const GlTab* tab;
     double* t1;    // [nc][6][T1W][nq^2]: state at the face nodes (5), projected entropy variables (5, split)
-    double* t2;    // [nc][6][19][nq^2]: lifted gradient q (15, s*3+d), face-normal volume viscous flux (4)
+    double* t2;    // [nc][6][8][nq^2]: the cell's F_v(u, q) . e_dn at its face nodes (4) and its face-normal
+                   // volume viscous flux interpolated to them, signed by the side (4)
     double* vis;   // [nc][4][nd^3]: -chi^T W div(F_v), momentum and energy rows
 };
 
 template <bool SPLIT> __host__ __device__ constexpr int gl_t1_width() { return SPLIT ? 10 : 5; }
-constexpr int GL_T2W = 19;
+constexpr int GL_T2W = 8;
 
 // temporaries of the sum-factorised passes on 5 components (and of the six faces' arrays)
 template <int ND, int NQ> __host__ __device__ constexpr int gl_temp() {
@@ -109,7 +115,7 @@ __device__ __forceinline__ void gl_cons_from_entropy(const double v[5], double g
 // with r the output's coordinate along d. Input dims (n0, n1, n2), n_d = cols; output dims the
 // same with n_d = rows. x is the fastest index.
 template <int NT>
-__device__ __forceinline__ void gl_pass_fma(const double* A, int rows, int cols, int d, int n0, int n1, int n2,
+__device__ __forceinline__ void gl_pass(const double* A, int rows, int cols, int d, int n0, int n1, int n2,
                                             const double* in, int in_ss, double* out, int out_ss, int ns,
                                             double scale, bool acc) {
     const int m0 = d == 0 ? rows : n0, m1 = d == 1 ? rows : n1, m2 = d == 2 ? rows : n2;
@@ -129,241 +135,189 @@ __device__ __forceinline__ void gl_pass_fma(const double* A, int rows, int cols,
     }
 }
 
-// 1: the sum-factorised passes run on the FP64 tensor-core instruction (mma.sync m8n8k4 f64):
-// a pass is the product of the 1-D operator (rows x cols, both <= 8, zero-padded to 8 x 8) with
-// the matrix whose columns are the input's lines, eight lines per warp-level product
-#ifndef PH_GL_DMMA
-#define PH_GL_DMMA 0
-#endif
-
-template <int NT>
-__device__ __forceinline__ void gl_pass_mma(const double* A, int rows, int cols, int d, int n0, int n1, int n2,
-                                            const double* in, int in_ss, double* out, int out_ss, int ns, double scale,
-                                            bool acc);
-template <int NT>
-__device__ __forceinline__ void gl_pass(const double* A, int rows, int cols, int d, int n0, int n1, int n2,
-                                        const double* in, int in_ss, double* out, int out_ss, int ns, double scale,
-                                        bool acc) {
-#if PH_GL_DMMA
-    gl_pass_mma<NT>(A, rows, cols, d, n0, n1, n2, in, in_ss, out, out_ss, ns, scale, acc);
-#else
-    gl_pass_fma<NT>(A, rows, cols, d, n0, n1, n2, in, in_ss, out, out_ss, ns, scale, acc);
-#endif
-}
-
-#if PH_GL_DMMA
-// D (8x8) += A (8x4, row-major) B (4x8, column-major); per lane: A[lane/4][lane%4],
-// B[lane%4][lane/4], D[lane/4][2 (lane%4) + {0, 1}]
-__device__ __forceinline__ void dmma_8x8x4(double a, double b, double& d0, double& d1) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-                 : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
-}
-
-// gl_pass with the products on the tensor cores (see PH_GL_DMMA)
-template <int NT>
-__device__ __forceinline__ void gl_pass_mma(const double* A, int rows, int cols, int d, int n0, int n1, int n2,
-                                            const double* in, int in_ss, double* out, int out_ss, int ns, double scale,
-                                            bool acc) {
-    const int m0 = d == 0 ? rows : n0, m1 = d == 1 ? rows : n1, m2 = d == 2 ? rows : n2;
-    const int osz = m0 * m1 * m2;
-    const int st = d == 0 ? 1 : d == 1 ? n0 : n0 * n1;
-    const int ost = d == 0 ? 1 : d == 1 ? m0 : m0 * m1;
-    // lines: the coordinates other than d, then the state
-    const int pa = d == 0 ? n1 : n0;                 // extent of the first other coordinate
-    const int pb = d == 2 ? n1 : n2;                 // of the second
-    const int lines_per_state = pa * pb;
-    const int nlines = ns * lines_per_state;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int r = lane >> 2, kq = lane & 3;
-    double a0 = 0.0, a1 = 0.0;
-    if (r < rows) {
-        if (kq < cols) a0 = A[r * cols + kq];
-        if (kq + 4 < cols) a1 = A[r * cols + kq + 4];
-    }
-    for (int tile = warp; tile * 8 < nlines; tile += NT / 32) {
-        const int j = tile * 8 + (lane >> 2);        // this lane's B column (line)
-        double b0 = 0.0, b1 = 0.0;
-        if (j < nlines) {
-            const int s = j / lines_per_state, t = j - s * lines_per_state;
-            const int ca = t % pa, cb = t / pa;
-            const int x = d == 0 ? 0 : ca, y = d == 1 ? 0 : (d == 0 ? ca : cb), z = d == 2 ? 0 : cb;
-            const double* ip = in + s * in_ss + (z * n1 + y) * n0 + x;
-            if (kq < cols) b0 = ip[kq * st];
-            if (kq + 4 < cols) b1 = ip[(kq + 4) * st];
-        }
-        double d0 = 0.0, d1 = 0.0;
-        dmma_8x8x4(a0, b0, d0, d1);
-        dmma_8x8x4(a1, b1, d0, d1);
-        // write D[r][lines 2 kq, 2 kq + 1 of the tile]
+// ------------------------------------------------------------------------------------
+// Compile-time sum-factorised passes
+// ------------------------------------------------------------------------------------
+// One pass along direction D of NS arrays with input extents (N0, N1, N2), N_D = COLS, and
+// output extents the same with N_D = ROWS (x fastest): one thread per line reads the COLS
+// inputs into registers and writes out[o] (+)= scale * sum_l A(o, l) in[l] for each of the ROWS
+// outputs, A(o, l) = A[o * COLS + l], or A[l * ROWS + o] with TRANS (the transposed operator
+// stored as cols x rows). Summation in ascending l from zero. A line's inputs are all read
+// before its outputs are written, so in == out is allowed when ROWS == COLS.
+template <int NT, int ROWS, int COLS, int D, int N0, int N1, int N2, int NS, bool TRANS = false>
+__device__ __forceinline__ void gl_line(const double* __restrict__ A, const double* in, int in_ss, double* out,
+                                        int out_ss, double scale, bool acc) {
+    static_assert((D == 0 ? N0 : D == 1 ? N1 : N2) == COLS, "the input extent along D is COLS");
+    constexpr int PA = D == 0 ? N1 : N0, PB = D == 2 ? N1 : N2;   // the other two extents, lower first
+    constexpr int IST = D == 0 ? 1 : D == 1 ? N0 : N0 * N1;
+    constexpr int M0 = D == 0 ? ROWS : N0, M1 = D == 1 ? ROWS : N1;
+    constexpr int OST = D == 0 ? 1 : D == 1 ? M0 : M0 * M1;
+    constexpr int NL = NS * PA * PB;
+#pragma unroll 1
+    for (int t = threadIdx.x; t < NL; t += NT) {
+        const int s = t / (PA * PB), r = t - s * (PA * PB);
+        const int ca = r % PA, cb = r / PA;
+        int ib, ob;
+        if constexpr (D == 0) { ib = (cb * N1 + ca) * N0; ob = (cb * M1 + ca) * M0; }
+        else if constexpr (D == 1) { ib = cb * N1 * N0 + ca; ob = cb * M1 * M0 + ca; }
+        else { ib = cb * N0 + ca; ob = ib; }
+        const double* ip = in + s * in_ss + ib;
+        double* op = out + s * out_ss + ob;
+        double v[COLS];
 #pragma unroll
-        for (int i = 0; i < 2; ++i) {
-            const int jj = tile * 8 + 2 * kq + i;
-            if (r < rows && jj < nlines) {
-                const int s = jj / lines_per_state, t = jj - s * lines_per_state;
-                const int ca = t % pa, cb = t / pa;
-                const int x = d == 0 ? r : ca, y = d == 1 ? r : (d == 0 ? ca : cb), z = d == 2 ? r : cb;
-                double* op = out + s * out_ss + (z * m1 + y) * m0 + x;
-                const double v = i ? d1 : d0;
-                *op = acc ? *op + scale * v : scale * v;
-            }
+        for (int l = 0; l < COLS; ++l) v[l] = ip[l * IST];
+#pragma unroll
+        for (int o = 0; o < ROWS; ++o) {
+            double x = 0.0;
+#pragma unroll
+            for (int l = 0; l < COLS; ++l) x += (TRANS ? A[l * ROWS + o] : A[o * COLS + l]) * v[l];
+            op[o * OST] = acc ? op[o * OST] + scale * x : scale * x;
         }
     }
-    (void)osz; (void)ost;
 }
-#endif
 
-// out = (Az (x) Ay (x) Az) in, x first: input cubes of n_in per direction, output n_out per
-// direction; t0, t1 hold ns * n_out * n_in^2 and ns * n_out^2 * n_in values. Ends with a barrier.
-template <int NT>
-__device__ __forceinline__ void gl_apply3(const double* A, int n_out, int n_in, const double* in, int in_ss,
-                                          double* out, int out_ss, int ns, double* t0, double* t1, double scale,
-                                          bool acc) {
-    const int s0 = n_out * n_in * n_in, s1 = n_out * n_out * n_in;
-    gl_pass<NT>(A, n_out, n_in, 0, n_in, n_in, n_in, in, in_ss, t0, s0, ns, 1.0, false);
+// out = (A (x) A (x) A) in, x first (TRANS: the transpose of A stored NI x NO): input cubes of
+// NI per direction, output NO per direction; t0, t1 hold NS NO NI^2 and NS NO^2 NI values.
+// Ends with a barrier.
+template <int NT, int NO, int NI, int NS, bool TRANS = false>
+__device__ __forceinline__ void gl_apply3(const double* A, const double* in, int in_ss, double* out, int out_ss,
+                                          double* t0, double* t1, double scale, bool acc) {
+    constexpr int S0 = NO * NI * NI, S1 = NO * NO * NI;
+    gl_line<NT, NO, NI, 0, NI, NI, NI, NS, TRANS>(A, in, in_ss, t0, S0, 1.0, false);
     __syncthreads();
-    gl_pass<NT>(A, n_out, n_in, 1, n_out, n_in, n_in, t0, s0, t1, s1, ns, 1.0, false);
+    gl_line<NT, NO, NI, 1, NO, NI, NI, NS, TRANS>(A, t0, S0, t1, S1, 1.0, false);
     __syncthreads();
-    gl_pass<NT>(A, n_out, n_in, 2, n_out, n_out, n_in, t1, s1, out, out_ss, ns, scale, acc);
+    gl_line<NT, NO, NI, 2, NO, NO, NI, NS, TRANS>(A, t1, S1, out, out_ss, scale, acc);
     __syncthreads();
 }
 
-// The transpose: out = (A^T (x) A^T (x) A^T) in for A (n_in x n_out) stored row-major, i.e.
-// out[i] = sum_q A[q][i] in[q] per direction (an inner product with the rows of A).
-template <int NT>
-__device__ __forceinline__ void gl_passT(const double* A, int rows_out, int cols_in, int d, int n0, int n1, int n2,
-                                         const double* in, int in_ss, double* out, int out_ss, int ns, double scale,
-                                         bool acc) {
-    // A is (cols_in x rows_out): out coordinate r sums A[l][r] in[l]
-    const int m0 = d == 0 ? rows_out : n0, m1 = d == 1 ? rows_out : n1, m2 = d == 2 ? rows_out : n2;
-    const int osz = m0 * m1 * m2;
-    const int st = d == 0 ? 1 : d == 1 ? n0 : n0 * n1;
-    for (int it = threadIdx.x; it < ns * osz; it += NT) {
-        const int s = it / osz, o = it - s * osz;
-        const int x = o % m0, y = (o / m0) % m1, z = o / (m0 * m1);
-        const int r = d == 0 ? x : d == 1 ? y : z;
-        const int base = ((d == 2 ? 0 : z) * n1 + (d == 1 ? 0 : y)) * n0 + (d == 0 ? 0 : x);
-        const double* ip = in + s * in_ss + base;
-        double v = 0.0;
-        for (int l = 0; l < cols_in; ++l) v += A[l * rows_out + r] * ip[l * st];
-        double* op = out + s * out_ss + o;
-        *op = acc ? *op + scale * v : scale * v;
-    }
-}
-template <int NT>
-__device__ __forceinline__ void gl_apply3T(const double* A, int n_out, int n_in, const double* in, int in_ss,
-                                           double* out, int out_ss, int ns, double* t0, double* t1, double scale,
-                                           bool acc) {
-    const int s0 = n_out * n_in * n_in, s1 = n_out * n_out * n_in;
-    gl_passT<NT>(A, n_out, n_in, 0, n_in, n_in, n_in, in, in_ss, t0, s0, ns, 1.0, false);
-    __syncthreads();
-    gl_passT<NT>(A, n_out, n_in, 1, n_out, n_in, n_in, t0, s0, t1, s1, ns, 1.0, false);
-    __syncthreads();
-    gl_passT<NT>(A, n_out, n_in, 2, n_out, n_out, n_in, t1, s1, out, out_ss, ns, scale, acc);
-    __syncthreads();
+// node index of position l along direction dn on the face-node line q2 = t2 * N + t1 (t1 < t2
+// the tangential directions: the face-node order of both sides of a face)
+template <int N> __device__ __forceinline__ int gl_line_node(int dn, int q2, int l) {
+    const int t1c = q2 % N, t2c = q2 / N;
+    return dn == 0 ? (t2c * N + t1c) * N + l : dn == 1 ? (t2c * N + l) * N + t1c : (l * N + t2c) * N + t1c;
 }
 
-// Face values on all six faces of a cube of values: for face f (normal direction dn = f/2,
-// side f&1) out[f][s][q2] = sum over the cube of row[side][i_dn] T[q_t1][i_t1] T[q_t2][i_t2]
-// src[s][i] (the surface interpolation of operators.cpp:355-398 with the face's row along the
-// normal). q2 = q_t2 * n_out + q_t1, t1 < t2 the tangential directions: the same face-node order
-// on both sides of a face. row: two rows of n_in; T: n_out x n_in (nullptr: identity, n_out =
-// n_in). w0: 6 ns n_in^2 values, w1: 6 ns n_out n_in. out[f][s] at out + f * out_fs + s * out_ss.
-template <int NT>
-__device__ __forceinline__ void gl_face_values(const double* src, int src_ss, int ns, int n_in,
-                                               const double* row0, const double* row1, const double* T, int n_out,
-                                               double* w0, double* w1, double* out, int out_fs, int out_ss) {
-    const int n2 = n_in * n_in;
-    // along the normal: w0[f][s][b * n_in + a] (a along t1, b along t2)
-    for (int it = threadIdx.x; it < 6 * ns * n2; it += NT) {
-        const int f = it / (ns * n2), r = it - f * ns * n2, s = r / n2, ab = r - s * n2;
-        const int a = ab % n_in, b = ab / n_in, dn = f >> 1;
+// Face values on all six faces of NS cubes of NIN^3 values: for face f (normal dn = f / 2,
+// side f & 1) out[f][s][q2] = sum row[side][i_dn] T[q_t1][i_t1] T[q_t2][i_t2] src[s][i]
+// (the surface interpolation of operators.cpp:355-398 with the face's row along the normal),
+// q2 = q_t2 * NOUT + q_t1. row0 / row1 (NIN values) are read with run-time indices (shared
+// memory); T (NOUT x NIN, a kernel parameter) only with compile-time ones; without HAS_T the
+// tangential operator is the identity (NOUT = NIN). w0: 6 NS NIN^2 values, w1: 6 NS NOUT NIN.
+// Ends with a barrier.
+template <int NT, int NIN, int NOUT, int NS, bool HAS_T>
+__device__ __forceinline__ void gl_face_values(const double* src, int src_ss, const double* row0, const double* row1,
+                                               const double* T, double* w0, double* w1, double* out, int out_fs,
+                                               int out_ss) {
+    constexpr int N2 = NIN * NIN;
+    for (int it = threadIdx.x; it < 6 * NS * N2; it += NT) {   // along the normal: w0[f][s][b * NIN + a]
+        const int f = it / (NS * N2), r = it - f * NS * N2, s = r / N2, ab = r - s * N2;
+        const int a = ab % NIN, b = ab / NIN, dn = f >> 1;
         const double* rw = (f & 1) ? row1 : row0;
-        const int st = dn == 0 ? 1 : dn == 1 ? n_in : n2;
-        const int base = dn == 0 ? (b * n_in + a) * n_in : dn == 1 ? b * n2 + a : b * n_in + a;
+        const int st = dn == 0 ? 1 : dn == 1 ? NIN : N2;
+        const int base = dn == 0 ? (b * NIN + a) * NIN : dn == 1 ? b * N2 + a : b * NIN + a;
         const double* ip = src + s * src_ss + base;
         double v = 0.0;
-        for (int l = 0; l < n_in; ++l) v += rw[l] * ip[l * st];
-        w0[it] = v;
+#pragma unroll
+        for (int l = 0; l < NIN; ++l) v += rw[l] * ip[l * st];
+        if constexpr (HAS_T) w0[it] = v;
+        else out[f * out_fs + s * out_ss + ab] = v;
     }
     __syncthreads();
-    if (T == nullptr) {
-        for (int it = threadIdx.x; it < 6 * ns * n2; it += NT) {
-            const int f = it / (ns * n2), r = it - f * ns * n2, s = r / n2, q2 = r - s * n2;
-            out[f * out_fs + s * out_ss + q2] = w0[it];
+    if constexpr (HAS_T) {
+        for (int it = threadIdx.x; it < 6 * NS * NIN; it += NT) {   // along t1: w1[f][s][b * NOUT + q1]
+            const double* ip = w0 + it * NIN;
+            double v[NIN];
+#pragma unroll
+            for (int l = 0; l < NIN; ++l) v[l] = ip[l];
+            double* op = w1 + it * NOUT;
+#pragma unroll
+            for (int o = 0; o < NOUT; ++o) {
+                double x = 0.0;
+#pragma unroll
+                for (int l = 0; l < NIN; ++l) x += T[o * NIN + l] * v[l];
+                op[o] = x;
+            }
         }
         __syncthreads();
-        return;
+        for (int it = threadIdx.x; it < 6 * NS * NOUT; it += NT) {   // along t2
+            const int fs = it / NOUT, q1 = it - fs * NOUT, f = fs / NS, s = fs - f * NS;
+            const double* ip = w1 + fs * NOUT * NIN + q1;
+            double v[NIN];
+#pragma unroll
+            for (int l = 0; l < NIN; ++l) v[l] = ip[l * NOUT];
+            double* op = out + f * out_fs + s * out_ss + q1;
+#pragma unroll
+            for (int o = 0; o < NOUT; ++o) {
+                double x = 0.0;
+#pragma unroll
+                for (int l = 0; l < NIN; ++l) x += T[o * NIN + l] * v[l];
+                op[o * NOUT] = x;
+            }
+        }
+        __syncthreads();
     }
-    const int m1 = n_out * n_in;
-    for (int it = threadIdx.x; it < 6 * ns * m1; it += NT) {   // along t1: w1[f][s][b * n_out + q1]
-        const int fs = it / m1, bq = it - fs * m1, q1 = bq % n_out, b = bq / n_out;
-        const double* ip = w0 + fs * n2 + b * n_in;
-        double v = 0.0;
-        for (int l = 0; l < n_in; ++l) v += T[q1 * n_in + l] * ip[l];
-        w1[it] = v;
-    }
-    __syncthreads();
-    const int m2 = n_out * n_out;
-    for (int it = threadIdx.x; it < 6 * ns * m2; it += NT) {   // along t2
-        const int fs = it / m2, q2 = it - fs * m2, q1 = q2 % n_out, qq = q2 / n_out;
-        const int f = fs / ns, s = fs - f * ns;
-        const double* ip = w1 + fs * m1 + q1;
-        double v = 0.0;
-        for (int l = 0; l < n_in; ++l) v += T[qq * n_in + l] * ip[l * n_out];
-        out[f * out_fs + s * out_ss + q2] = v;
-    }
-    __syncthreads();
 }
 
-// The lift of six face arrays into the cube: dst[s][node] (+)= sum_f row[side][i_dn]
+// The lift of six face arrays into NS cubes of ND^3: dst[s][node] (+)= sum_f row[side][i_dn]
 // sum_{q1,q2} T[q1][i_t1] T[q2][i_t2] face[f][s][q2] (the surface inner products of
-// operators.cpp:575-636 with the solution basis; T is n_q x n_d). dst_ds != 0: dst holds one
-// cube per normal direction (dst + dn * dst_ds). only_dn >= 0: only the two faces of that
-// direction, given as face[0..1] (faces 2 only_dn and 2 only_dn + 1).
-template <int NT>
-__device__ __forceinline__ void gl_lift_faces(const double* face, int face_fs, int face_ss, int ns, int nq, int nd,
-                                              const double* row0, const double* row1, const double* T, double* w0,
-                                              double* w1, double* dst, int dst_ss, int dst_ds, double scale,
-                                              int only_dn = -1) {
-    const int mq = nq * nq, m1 = nq * nd, m2 = nd * nd;
-    const int f0 = only_dn < 0 ? 0 : 2 * only_dn, nfc = only_dn < 0 ? 6 : 2;   // the faces lifted
-    for (int it = threadIdx.x; it < nfc * ns * m1; it += NT) {   // along t1: w0[f][s][q2 * nd + a]
-        const int fs = it / m1, r = it - fs * m1, a = r % nd, q2 = r / nd;
-        const int f = f0 + fs / ns, s = fs % ns;
-        const double* ip = face + (f - f0) * face_fs + s * face_ss + q2 * nq;   // only_dn: two faces given
-        double v = 0.0;
-        for (int l = 0; l < nq; ++l) v += T[l * nd + a] * ip[l];
-        w0[it] = v;
+// operators.cpp:575-636 with the solution basis; T is NQ x ND, a kernel parameter; row0 / row1
+// in shared memory). w0: 6 NS NQ ND, w1: 6 NS ND^2 values. Ends with a barrier.
+template <int NT, int NQ, int ND, int NS>
+__device__ __forceinline__ void gl_lift_faces(const double* face, int face_fs, int face_ss, const double* row0,
+                                              const double* row1, const double* T, double* w0, double* w1, double* dst,
+                                              int dst_ss, double scale) {
+    constexpr int MQ = NQ * NQ, D2 = ND * ND, D3 = D2 * ND;
+    for (int it = threadIdx.x; it < 6 * NS * NQ; it += NT) {   // along t1: w0[f][s][q2][a]
+        const int fs = it / NQ, q2 = it - fs * NQ, f = fs / NS, s = fs - f * NS;
+        const double* ip = face + f * face_fs + s * face_ss + q2 * NQ;
+        double v[NQ];
+#pragma unroll
+        for (int l = 0; l < NQ; ++l) v[l] = ip[l];
+        double* op = w0 + (fs * NQ + q2) * ND;
+#pragma unroll
+        for (int o = 0; o < ND; ++o) {
+            double x = 0.0;
+#pragma unroll
+            for (int l = 0; l < NQ; ++l) x += T[l * ND + o] * v[l];
+            op[o] = x;
+        }
     }
     __syncthreads();
-    for (int it = threadIdx.x; it < nfc * ns * m2; it += NT) {   // along t2: w1[f][s][b * nd + a]
-        const int fs = it / m2, r = it - fs * m2, a = r % nd, b = r / nd;
-        const double* ip = w0 + fs * m1 + a;
-        double v = 0.0;
-        for (int l = 0; l < nq; ++l) v += T[l * nd + b] * ip[l * nd];
-        w1[it] = v;
+    for (int it = threadIdx.x; it < 6 * NS * ND; it += NT) {   // along t2: w1[f][s][b * ND + a]
+        const int fs = it / ND, a = it - fs * ND;
+        const double* ip = w0 + fs * NQ * ND + a;
+        double v[NQ];
+#pragma unroll
+        for (int l = 0; l < NQ; ++l) v[l] = ip[l * ND];
+        double* op = w1 + fs * D2 + a;
+#pragma unroll
+        for (int o = 0; o < ND; ++o) {
+            double x = 0.0;
+#pragma unroll
+            for (int l = 0; l < NQ; ++l) x += T[l * ND + o] * v[l];
+            op[o * ND] = x;
+        }
     }
     __syncthreads();
-    const int nd3 = m2 * nd;
-    for (int it = threadIdx.x; it < ns * nd3; it += NT) {
-        const int s = it / nd3, node = it - s * nd3;
-        const int c[3] = {node % nd, (node / nd) % nd, node / m2};
+    for (int it = threadIdx.x; it < NS * D3; it += NT) {
+        const int s = it / D3, node = it - s * D3;
+        const int c[3] = {node % ND, (node / ND) % ND, node / D2};
+        double* op = dst + s * dst_ss + node;
 #pragma unroll
         for (int dn = 0; dn < 3; ++dn) {
-            if (only_dn >= 0 && dn != only_dn) continue;
             const int t1 = dn == 0 ? 1 : 0, t2 = dn == 2 ? 1 : 2;
-            const int ab = c[t2] * nd + c[t1];
-            const int fb = only_dn < 0 ? 2 * dn : 0;   // first of the direction's two faces in w1
-            const double v = row0[c[dn]] * w1[(fb * ns + s) * m2 + ab] + row1[c[dn]] * w1[((fb + 1) * ns + s) * m2 + ab];
-            double* op = dst + (dst_ds ? dn * dst_ds : 0) + s * dst_ss + node;
+            const int ab = c[t2] * ND + c[t1];
+            const double v = row0[c[dn]] * w1[((2 * dn) * NS + s) * D2 + ab] +
+                             row1[c[dn]] * w1[((2 * dn + 1) * NS + s) * D2 + ab];
             *op += scale * v;
         }
     }
     __syncthreads();
-    (void)mq;
+    (void)MQ;
 }
 
-// Shared-memory copy of the operator table.
+// Shared-memory copy of the operator table (for the reads with run-time indices).
 __device__ __forceinline__ void gl_load_tab(const GlTab* g, GlTab* s, int nt) {
     const double* src = reinterpret_cast<const double*>(g);
     double* dst = reinterpret_cast<double*>(s);
@@ -387,7 +341,8 @@ struct GlTraceLayout {
 };
 
 template <int ND, int NQ, bool SPLIT>
-__global__ void __launch_bounds__(gl_threads<NQ>()) gl_trace_kernel(const StageArgs a, const GlArgs g) {
+__global__ void __launch_bounds__(gl_threads<NQ>())
+gl_trace_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab T) {
     using L = GlTraceLayout<ND, NQ, SPLIT>;
     constexpr int NT = L::NT, D3 = L::D3, Q3 = L::Q3, T1W = gl_t1_width<SPLIT>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -402,9 +357,10 @@ __global__ void __launch_bounds__(gl_threads<NQ>()) gl_trace_kernel(const StageA
     for (int i = threadIdx.x; i < 5 * D3; i += NT) sU[i] = __ldg(&a.U[(size_t)cell * 5 * D3 + i]);
     __syncthreads();
     double* out = g.t1 + (size_t)cell * 6 * T1W * NQ * NQ;
-    gl_face_values<NT>(sU, D3, 5, ND, tab->chis[0], tab->chis[1], tab->chi, NQ, w0, w1, out, T1W * NQ * NQ, NQ * NQ);
+    gl_face_values<NT, ND, NQ, 5, true>(sU, D3, tab->chis[0], tab->chis[1], T.chi, w0, w1, out, T1W * NQ * NQ,
+                                        NQ * NQ);
     if constexpr (SPLIT) {
-        gl_apply3<NT>(tab->chi, NQ, ND, sU, D3, sQ, Q3, 5, w0, w1, 1.0, false);
+        gl_apply3<NT, NQ, ND, 5>(T.chi, sU, D3, sQ, Q3, w0, w1, 1.0, false);
         const double gam = a.pc.gam, gm1 = a.pc.gm1;
         for (int q = threadIdx.x; q < Q3; q += NT) {
             double u[5], v[5];
@@ -415,46 +371,78 @@ __global__ void __launch_bounds__(gl_threads<NQ>()) gl_trace_kernel(const StageA
             for (int s = 0; s < 5; ++s) sQ[s * Q3 + q] = v[s];
         }
         __syncthreads();
-        gl_face_values<NT>(sQ, Q3, 5, NQ, tab->ps[0], tab->ps[1], tab->P, NQ, w0, w1, out + 5 * NQ * NQ,
-                           T1W * NQ * NQ, NQ * NQ);
+        gl_face_values<NT, NQ, NQ, 5, true>(sQ, Q3, tab->ps[0], tab->ps[1], T.P, w0, w1, out + 5 * NQ * NQ,
+                                            T1W * NQ * NQ, NQ * NQ);
     }
 }
 
 // ------------------------------------------------------------------------------------
 // Auxiliary equation and the viscous terms (Navier-Stokes)
 // ------------------------------------------------------------------------------------
+// The lifted gradient is formed at the flux nodes: with H = chi (M + K_aux)^-1 chi^T and
+// chi_side = chi^T phi_side (the solution basis is interpolated exactly by the flux-node basis),
+//   chi (x3) q_d = (1/h) (H (x) H (x) H) [W D_d (chi u) + sum_side phi_side (x) W_face (u* - u) n_d]
+// which is the reference's q_d = (M_aux)^-1 [chi^T W D_d (chi u) + face lifts] taken to the
+// flux nodes (strong_dg.cpp:498-1008, dg_base.cpp:4089-4260 with use_auxiliary_eq; C = h^2 I):
+// four passes per direction instead of ten. The face values of q are the flux-node values along
+// the normal contracted with phi_side (exact for the degree-p gradient).
 template <int ND, int NQ, bool SPLIT>
 struct GlAuxLayout {
     static constexpr int NT = gl_threads<NQ>();
-    static constexpr int D3 = ND * ND * ND, Q3 = NQ * NQ * NQ;
+    static constexpr int D3 = ND * ND * ND, Q3 = NQ * NQ * NQ, NF = NQ * NQ;
     static constexpr int nTab = (int)(sizeof(GlTab) / sizeof(double));
     static constexpr int oU = nTab;                      // 5 NQ^3: the state, later the projected state
     static constexpr int oQ = oU + 5 * Q3;               // 5 NQ^3: state at the flux nodes
-    // one direction's aux right-hand side and lifted gradient (5 ND^3 each; the lift's second
-    // pass, 30 ND^2, also goes there), the lifted gradient at the flux nodes (15 NQ^3) and the
-    // volume viscous flux (12 NQ^3)
-    static constexpr int nR = 5 * D3 > 30 * ND * ND ? 5 * D3 : 30 * ND * ND;
-    static constexpr int oR = oQ + 5 * Q3;
-    static constexpr int oA = oR + nR;
-    static constexpr int oAQ = oA + 5 * D3;
-    static constexpr int oF = oAQ + 15 * Q3;
+    static constexpr int oG = oQ + 5 * Q3;               // 5 NQ^3: one direction's bracket [.] above
+    static constexpr int oAQ = oG + 5 * Q3;              // 15 NQ^3: lifted gradient at the flux nodes
+    static constexpr int oF = oAQ + 15 * Q3;             // 12 NQ^3: volume viscous flux (first: face terms)
     static constexpr int nT = gl_temp<ND, NQ>();
     static constexpr int oT0 = oF + 12 * Q3, oT1 = oT0 + nT;
     static constexpr int total = oT1 + nT;
     static constexpr size_t bytes = (size_t)total * sizeof(double);
+    static_assert(12 * Q3 >= 10 * NF, "the face terms of one direction fit the flux buffer");
 };
 
-template <int ND, int NQ, bool SPLIT>
-__global__ void __launch_bounds__(gl_threads<NQ>(), 2) gl_aux_kernel(const StageArgs a, const GlArgs g) {
+// one direction of the lifted gradient (see above); ends with a barrier
+template <int ND, int NQ, bool SPLIT, int D>
+__device__ __forceinline__ void gl_aux_direction(const StageArgs& a, const GlArgs& g, const GlTab& T,
+                                                 const GlTab* tab, int cell, const double* sQ, double* sG,
+                                                 double* face, double* sAQ, double* t0, double* t1) {
     using L = GlAuxLayout<ND, NQ, SPLIT>;
-    constexpr int NT = L::NT, D3 = L::D3, Q3 = L::Q3, NF = NQ * NQ, T1W = gl_t1_width<SPLIT>();
+    constexpr int NT = L::NT, Q3 = L::Q3, NF = L::NF, T1W = gl_t1_width<SPLIT>();
+    gl_line<NT, NQ, NQ, D, NQ, NQ, NQ, 5>(T.dphi, sQ, Q3, sG, Q3, 1.0, false);
+    for (int it = threadIdx.x; it < 2 * 5 * NF; it += NT) {   // faces 2D, 2D + 1: W_face (u* - u) n_D
+        const int f = 2 * D + it / (5 * NF), s = (it / NF) % 5, q2 = it % NF;
+        const int cn = __ldg(&a.nbr[cell * 6 + f]);
+        const double uo = __ldg(&g.t1[(((size_t)cell * 6 + f) * T1W + s) * NF + q2]);
+        const double ue = __ldg(&g.t1[(((size_t)cn * 6 + (f ^ 1)) * T1W + s) * NF + q2]);
+        const double sgn = (f & 1) ? 1.0 : -1.0;
+        face[it] = tab->wq[q2 % NQ] * tab->wq[q2 / NQ] * ((0.5 * (uo + ue) - uo) * sgn);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 5 * Q3; i += NT) {
+        const int s = i / Q3, q = i - s * Q3;
+        const int c[3] = {q % NQ, (q / NQ) % NQ, q / NF};
+        constexpr int A1 = D == 0 ? 1 : 0, A2 = D == 2 ? 1 : 2;
+        const int q2 = c[A2] * NQ + c[A1];
+        sG[i] = tab->wq[c[0]] * tab->wq[c[1]] * tab->wq[c[2]] * sG[i] + tab->phis[0][c[D]] * face[s * NF + q2] +
+                tab->phis[1][c[D]] * face[(5 + s) * NF + q2];
+    }
+    __syncthreads();
+    gl_apply3<NT, NQ, NQ, 5>(T.haux, sG, Q3, sAQ + D * Q3, 3 * Q3, t0, t1, a.inv_h, false);
+}
+
+template <int ND, int NQ, bool SPLIT>
+__global__ void __launch_bounds__(gl_threads<NQ>(), 2)
+gl_aux_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab T) {
+    using L = GlAuxLayout<ND, NQ, SPLIT>;
+    constexpr int NT = L::NT, D3 = L::D3, Q3 = L::Q3, NF = L::NF, T1W = gl_t1_width<SPLIT>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* sm = reinterpret_cast<double*>(smem_raw);
     GlTab* tab = reinterpret_cast<GlTab*>(sm);
     double* sU = sm + L::oU;
     double* sQ = sm + L::oQ;
-    double* sR = sm + L::oR;
-    double* sA = sm + L::oA;
+    double* sG = sm + L::oG;
     double* sAQ = sm + L::oAQ;
     double* sF = sm + L::oF;
     double* t0 = sm + L::oT0;
@@ -465,41 +453,34 @@ __global__ void __launch_bounds__(gl_threads<NQ>(), 2) gl_aux_kernel(const Stage
     gl_load_tab(g.tab, tab, NT);
     for (int i = threadIdx.x; i < 5 * D3; i += NT) sU[i] = __ldg(&a.U[(size_t)cell * 5 * D3 + i]);
     __syncthreads();
-    gl_apply3<NT>(tab->chi, NQ, ND, sU, D3, sQ, Q3, 5, t0, t1, 1.0, false);
-    // q_d = (1/h) M_aux^-1 [chi^T W D_d (chi u) + face lifts of (u* - u) n_d], one direction at
-    // a time (strong_dg.cpp:498-1008, dg_base.cpp:4089-4260 with use_auxiliary_eq; C = h^2 I),
-    // then its face values for both neighbours' dissipative fluxes and its values at the flux
-    // nodes, row s * 3 + d of each
+    gl_apply3<NT, NQ, ND, 5>(T.chi, sU, D3, sQ, Q3, t0, t1, 1.0, false);
+    gl_aux_direction<ND, NQ, SPLIT, 0>(a, g, T, tab, cell, sQ, sG, sF, sAQ, t0, t1);
+    gl_aux_direction<ND, NQ, SPLIT, 1>(a, g, T, tab, cell, sQ, sG, sF, sAQ, t0, t1);
+    gl_aux_direction<ND, NQ, SPLIT, 2>(a, g, T, tab, cell, sQ, sG, sF, sAQ, t0, t1);
+    // per face node of the cell: F_v(u, q) . e_dn with the state's and the gradient's face values
+    // (each side's half of the dissipative numerical flux, strong_dg.cpp:3354-3452)
     double* tout = g.t2 + (size_t)cell * 6 * GL_T2W * NF;
-    double* face = sF;   // [2][s][q2]: W_face (u* - u) n_d on faces 2d and 2d + 1 (sF is free here)
-    for (int d = 0; d < 3; ++d) {
-        gl_pass<NT>(tab->dphi, NQ, NQ, d, NQ, NQ, NQ, sQ, Q3, t0, Q3, 5, 1.0, false);
-        __syncthreads();
-        for (int i = threadIdx.x; i < 5 * Q3; i += NT) {
-            const int q = i % Q3;
-            t0[i] *= tab->wq[q % NQ] * tab->wq[(q / NQ) % NQ] * tab->wq[q / (NQ * NQ)];
+    for (int it = threadIdx.x; it < 6 * NF; it += NT) {
+        const int f = it / NF, q2 = it - f * NF, dn = f >> 1, side = f & 1;
+        const double* rw = tab->phis[side];
+        double gq[5][3], r[5];
+#pragma unroll
+        for (int s = 0; s < 5; ++s) {
+            r[s] = __ldg(&g.t1[(((size_t)cell * 6 + f) * T1W + s) * NF + q2]);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const double* row = sAQ + (s * 3 + d) * Q3;
+                double v = 0.0;
+#pragma unroll
+                for (int l = 0; l < NQ; ++l) v += rw[l] * row[gl_line_node<NQ>(dn, q2, l)];
+                gq[s][d] = v;
+            }
         }
-        __syncthreads();
-        gl_passT<NT>(tab->chi, ND, NQ, 0, NQ, NQ, NQ, t0, Q3, t1, ND * NQ * NQ, 5, 1.0, false);
-        __syncthreads();
-        gl_passT<NT>(tab->chi, ND, NQ, 1, ND, NQ, NQ, t1, ND * NQ * NQ, t0, ND * ND * NQ, 5, 1.0, false);
-        __syncthreads();
-        gl_passT<NT>(tab->chi, ND, NQ, 2, ND, ND, NQ, t0, ND * ND * NQ, sR, D3, 5, 1.0, false);
-        for (int it = threadIdx.x; it < 2 * 5 * NF; it += NT) {   // faces 2d, 2d + 1
-            const int f = 2 * d + it / (5 * NF), s = (it / NF) % 5, q2 = it % NF;
-            const int cn = __ldg(&a.nbr[cell * 6 + f]);
-            const double uo = __ldg(&g.t1[(((size_t)cell * 6 + f) * T1W + s) * NF + q2]);
-            const double ue = __ldg(&g.t1[(((size_t)cn * 6 + (f ^ 1)) * T1W + s) * NF + q2]);
-            const double sgn = (f & 1) ? 1.0 : -1.0;
-            face[it] = tab->wq[q2 % NQ] * tab->wq[q2 / NQ] * ((0.5 * (uo + ue) - uo) * sgn);
-        }
-        __syncthreads();
-        gl_lift_faces<NT>(face, 5 * NF, NF, 5, NQ, ND, tab->chis[0], tab->chis[1], tab->chi, t1, sA, sR, D3, 0, 1.0,
-                          d);
-        gl_apply3<NT>(tab->minv_aux, ND, ND, sR, D3, sA, D3, 5, t0, t1, a.inv_h, false);
-        gl_face_values<NT>(sA, D3, 5, ND, tab->chis[0], tab->chis[1], tab->chi, NQ, t0, t1, tout + d * NF,
-                           GL_T2W * NF, 3 * NF);
-        gl_apply3<NT>(tab->chi, NQ, ND, sA, D3, sAQ + d * Q3, 3 * Q3, 5, t0, t1, 1.0, false);
+        double F[3][4];
+        viscous_flux<double>(r, gq, ucv, cst, F, 1 << dn, nullptr);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)   // (selects, not a run-time index, keep F in registers)
+            tout[(f * GL_T2W + k) * NF + q2] = dn == 0 ? F[0][k] : dn == 1 ? F[1][k] : F[2][k];
     }
     // the split form evaluates the volume viscous flux at the entropy-projected state
     // (strong_dg.cpp:1328 before :1392); the face-normal flux interpolated to the faces uses
@@ -514,7 +495,7 @@ __global__ void __launch_bounds__(gl_threads<NQ>(), 2) gl_aux_kernel(const Stage
             for (int s = 0; s < 5; ++s) t0[s * Q3 + q] = v[s];
         }
         __syncthreads();
-        gl_apply3<NT>(tab->P, NQ, NQ, t0, Q3, sU, Q3, 5, t1, sF, 1.0, false);   // sF is free until the fluxes
+        gl_apply3<NT, NQ, NQ, 5>(T.P, t0, Q3, sU, Q3, t1, sF, 1.0, false);   // sF is free until the fluxes
         for (int q = threadIdx.x; q < Q3; q += NT) {
             double v[5], u[5];
 #pragma unroll
@@ -543,23 +524,24 @@ __global__ void __launch_bounds__(gl_threads<NQ>(), 2) gl_aux_kernel(const Stage
     }
     __syncthreads();
     // -chi^T W sum_d D_d F_d, momentum and energy rows
-    gl_pass<NT>(tab->dphi, NQ, NQ, 0, NQ, NQ, NQ, sF, Q3, t0, Q3, 4, 1.0, false);
+    gl_line<NT, NQ, NQ, 0, NQ, NQ, NQ, 4>(T.dphi, sF, Q3, t0, Q3, 1.0, false);
     __syncthreads();
-    gl_pass<NT>(tab->dphi, NQ, NQ, 1, NQ, NQ, NQ, sF + 4 * Q3, Q3, t0, Q3, 4, 1.0, true);
+    gl_line<NT, NQ, NQ, 1, NQ, NQ, NQ, 4>(T.dphi, sF + 4 * Q3, Q3, t0, Q3, 1.0, true);
     __syncthreads();
-    gl_pass<NT>(tab->dphi, NQ, NQ, 2, NQ, NQ, NQ, sF + 8 * Q3, Q3, t0, Q3, 4, 1.0, true);
+    gl_line<NT, NQ, NQ, 2, NQ, NQ, NQ, 4>(T.dphi, sF + 8 * Q3, Q3, t0, Q3, 1.0, true);
     __syncthreads();
     for (int i = threadIdx.x; i < 4 * Q3; i += NT) {
         const int q = i % Q3;
-        t0[i] *= tab->wq[q % NQ] * tab->wq[(q / NQ) % NQ] * tab->wq[q / (NQ * NQ)];
+        t0[i] *= tab->wq[q % NQ] * tab->wq[(q / NQ) % NQ] * tab->wq[q / NF];
     }
     __syncthreads();
     // (the state rows sU are free now: the fluxes stay in sF for the face values below)
-    gl_passT<NT>(tab->chi, ND, NQ, 0, NQ, NQ, NQ, t0, Q3, t1, ND * NQ * NQ, 4, 1.0, false);
+    gl_line<NT, ND, NQ, 0, NQ, NQ, NQ, 4, true>(T.chi, t0, Q3, t1, ND * NQ * NQ, 1.0, false);
     __syncthreads();
-    gl_passT<NT>(tab->chi, ND, NQ, 1, ND, NQ, NQ, t1, ND * NQ * NQ, sU, ND * ND * NQ, 4, 1.0, false);
+    gl_line<NT, ND, NQ, 1, ND, NQ, NQ, 4, true>(T.chi, t1, ND * NQ * NQ, sU, ND * ND * NQ, 1.0, false);
     __syncthreads();
-    gl_passT<NT>(tab->chi, ND, NQ, 2, ND, ND, NQ, sU, ND * ND * NQ, g.vis + (size_t)cell * 4 * D3, D3, 4, -1.0, false);
+    gl_line<NT, ND, NQ, 2, ND, ND, NQ, 4, true>(T.chi, sU, ND * ND * NQ, g.vis + (size_t)cell * 4 * D3, D3, -1.0,
+                                                false);
     // face-normal volume viscous flux at the faces: n_dn sum_l phi_l(side) F_dn(u_l) (state not
     // projected)
     if constexpr (SPLIT) {
@@ -584,14 +566,12 @@ __global__ void __launch_bounds__(gl_threads<NQ>(), 2) gl_aux_kernel(const Stage
     for (int it = threadIdx.x; it < 6 * 4 * NF; it += NT) {
         const int f = it / (4 * NF), k = (it / NF) % 4, q2 = it % NF;
         const int dn = f >> 1, side = f & 1;
-        const int t1c = q2 % NQ, t2c = q2 / NQ;
+        const double* rw = tab->phis[side];
+        const double* row = sF + (dn * 4 + k) * Q3;
         double v = 0.0;
-        for (int l = 0; l < NQ; ++l) {
-            const int node = dn == 0 ? (t2c * NQ + t1c) * NQ + l : dn == 1 ? (t2c * NQ + l) * NQ + t1c
-                                                                           : (l * NQ + t2c) * NQ + t1c;
-            v += tab->phis[side][l] * sF[(dn * 4 + k) * Q3 + node];
-        }
-        g.t2[(((size_t)cell * 6 + f) * GL_T2W + 15 + k) * NF + q2] = side ? v : -v;
+#pragma unroll
+        for (int l = 0; l < NQ; ++l) v += rw[l] * row[gl_line_node<NQ>(dn, q2, l)];
+        tout[(f * GL_T2W + 4 + k) * NF + q2] = side ? v : -v;
     }
 }
 
@@ -617,7 +597,8 @@ struct GlStageLayout {
 };
 
 template <int ND, int NQ, bool VISC, bool SPLIT>
-__global__ void __launch_bounds__(gl_threads<NQ>(), 2) gl_stage_kernel(const StageArgs a, const GlArgs g) {
+__global__ void __launch_bounds__(gl_threads<NQ>(), 2)
+gl_stage_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab T) {
     using L = GlStageLayout<ND, NQ, VISC, SPLIT>;
     constexpr int NT = L::NT, D3 = L::D3, Q3 = L::Q3, NF = L::NF, T1W = gl_t1_width<SPLIT>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -636,7 +617,7 @@ __global__ void __launch_bounds__(gl_threads<NQ>(), 2) gl_stage_kernel(const Sta
     gl_load_tab(g.tab, tab, NT);
     for (int i = threadIdx.x; i < 5 * D3; i += NT) sU[i] = __ldg(&a.U[(size_t)cell * 5 * D3 + i]);
     __syncthreads();
-    gl_apply3<NT>(tab->chi, NQ, ND, sU, D3, sQ, Q3, 5, t0, t1, 1.0, false);
+    gl_apply3<NT, NQ, ND, 5>(T.chi, sU, D3, sQ, Q3, t0, t1, 1.0, false);
     if constexpr (SPLIT) {
         // entropy projection at the flux nodes: u = u(P (x3) v(chi u))  (strong_dg.cpp:1235-1330)
         for (int q = threadIdx.x; q < Q3; q += NT) {
@@ -648,7 +629,7 @@ __global__ void __launch_bounds__(gl_threads<NQ>(), 2) gl_stage_kernel(const Sta
             for (int s = 0; s < 5; ++s) t0[s * Q3 + q] = v[s];
         }
         __syncthreads();
-        gl_apply3<NT>(tab->P, NQ, NQ, t0, Q3, sQ, Q3, 5, t1, sDiv, 1.0, false);
+        gl_apply3<NT, NQ, NQ, 5>(T.P, t0, Q3, sQ, Q3, t1, sDiv, 1.0, false);
         for (int q = threadIdx.x; q < Q3; q += NT) {
             double v[5], u[5];
 #pragma unroll
@@ -668,6 +649,7 @@ __global__ void __launch_bounds__(gl_threads<NQ>(), 2) gl_stage_kernel(const Sta
             NodeQ<double> qi;
             load_q<double>(sN, Q3, q, qi);
             double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
             for (int rd = 0; rd < 3; ++rd) {
                 const int ra = rd == 0 ? 1 : 0, rb = rd == 2 ? 1 : 2;
                 const double wab = tab->wq[xi[ra]] * tab->wq[xi[rb]];
@@ -707,11 +689,11 @@ __global__ void __launch_bounds__(gl_threads<NQ>(), 2) gl_stage_kernel(const Sta
             }
         }
         __syncthreads();
-        gl_pass<NT>(tab->dphi, NQ, NQ, 0, NQ, NQ, NQ, sN, Q3, sDiv, Q3, 5, 1.0, false);
+        gl_line<NT, NQ, NQ, 0, NQ, NQ, NQ, 5>(T.dphi, sN, Q3, sDiv, Q3, 1.0, false);
         __syncthreads();
-        gl_pass<NT>(tab->dphi, NQ, NQ, 1, NQ, NQ, NQ, sN + 5 * Q3, Q3, sDiv, Q3, 5, 1.0, true);
+        gl_line<NT, NQ, NQ, 1, NQ, NQ, NQ, 5>(T.dphi, sN + 5 * Q3, Q3, sDiv, Q3, 1.0, true);
         __syncthreads();
-        gl_pass<NT>(tab->dphi, NQ, NQ, 2, NQ, NQ, NQ, sN + 10 * Q3, Q3, sDiv, Q3, 5, 1.0, true);
+        gl_line<NT, NQ, NQ, 2, NQ, NQ, NQ, 5>(T.dphi, sN + 10 * Q3, Q3, sDiv, Q3, 1.0, true);
         __syncthreads();
         for (int i = threadIdx.x; i < 5 * Q3; i += NT) {
             const int q = i % Q3;
@@ -755,21 +737,19 @@ __global__ void __launch_bounds__(gl_threads<NQ>(), 2) gl_stage_kernel(const Sta
 #pragma unroll
         for (int s = 0; s < 5; ++s) term[s] = -sgn * Fc[s];
         if constexpr (VISC) {
+            // each side's F_v(u, q) . e_dn at the face node, from the auxiliary kernel
             const double* ao = g.t2 + ((size_t)cell * 6 + f) * GL_T2W * NF + q2;
             const double* ae = g.t2 + ((size_t)cn * 6 + (f ^ 1)) * GL_T2W * NF + q2;
-            double go[5][3], ge[5][3];
+            double Fo[4], Fe[4];
 #pragma unroll
-            for (int s = 0; s < 5; ++s)
-#pragma unroll
-                for (int d = 0; d < 3; ++d) { go[s][d] = __ldg(&ao[(s * 3 + d) * NF]); ge[s][d] = __ldg(&ae[(s * 3 + d) * NF]); }
+            for (int k = 0; k < 4; ++k) { Fo[k] = __ldg(&ao[k * NF]); Fe[k] = __ldg(&ae[k * NF]); }
             const double* rL = side ? ro : re;
             const double* rR = side ? re : ro;
-            double FL[3][4], FR[3][4];
-            viscous_flux<double>(rL, side ? go : ge, ucv, cst, FL, 1 << dn, nullptr);
-            viscous_flux<double>(rR, side ? ge : go, ucv, cst, FR, 1 << dn, nullptr);
+            const double* FL = side ? Fo : Fe;
+            const double* FR = side ? Fe : Fo;
             double Fd[4];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) Fd[k] = 0.5 * (FL[dn][k] + FR[dn][k]);
+            for (int k = 0; k < 4; ++k) Fd[k] = 0.5 * (FL[k] + FR[k]);
             if (df == DF_SIPG) {
                 double jump[5][3];
 #pragma unroll
@@ -780,21 +760,23 @@ __global__ void __launch_bounds__(gl_threads<NQ>(), 2) gl_stage_kernel(const Sta
                 viscous_flux<double>(rL, jump, ucv, cst, AL, 1 << dn, nullptr);
                 viscous_flux<double>(rR, jump, ucv, cst, AR, 1 << dn, nullptr);
 #pragma unroll
-                for (int k = 0; k < 4; ++k) Fd[k] = Fd[k] - a.pen * (0.5 * (AL[dn][k] + AR[dn][k]));
+                for (int k = 0; k < 4; ++k) {
+                    const double al = dn == 0 ? AL[0][k] : dn == 1 ? AL[1][k] : AL[2][k];
+                    const double ar = dn == 0 ? AR[0][k] : dn == 1 ? AR[1][k] : AR[2][k];
+                    Fd[k] = Fd[k] - a.pen * (0.5 * (al + ar));
+                }
             }
 #pragma unroll
-            for (int k = 0; k < 4; ++k) term[1 + k] += -sgn * Fd[k] + __ldg(&ao[(15 + k) * NF]);
+            for (int k = 0; k < 4; ++k) term[1 + k] += -sgn * Fd[k] + __ldg(&ao[(4 + k) * NF]);
         }
         if constexpr (!SPLIT) {   // the cell's own convective volume flux at the face: n . sum_l phi_l F(u_l)
-            const int t1c = q2 % NQ, t2c = q2 / NQ;
+            const double* rw = tab->phis[side];
 #pragma unroll
             for (int s = 0; s < 5; ++s) {
+                const double* row = sN + (dn * 5 + s) * Q3;
                 double v = 0.0;
-                for (int l = 0; l < NQ; ++l) {
-                    const int node = dn == 0 ? (t2c * NQ + t1c) * NQ + l : dn == 1 ? (t2c * NQ + l) * NQ + t1c
-                                                                                   : (l * NQ + t2c) * NQ + t1c;
-                    v += tab->phis[side][l] * sN[(dn * 5 + s) * Q3 + node];
-                }
+#pragma unroll
+                for (int l = 0; l < NQ; ++l) v += rw[l] * row[gl_line_node<NQ>(dn, q2, l)];
                 term[s] += sgn * v;
             }
         }
@@ -811,6 +793,7 @@ __global__ void __launch_bounds__(gl_threads<NQ>(), 2) gl_stage_kernel(const Sta
         // face 2 dn before face 2 dn + 1 and line position by position.
         double* sQF = sm + L::oQF;   // [11][2 NF]
         double* s2 = t0;             // [2][NF][NQ][5] (t0 and t1 are contiguous)
+#pragma unroll 1
         for (int dn = 0; dn < 3; ++dn) {
             const double nv[3] = {dn == 0 ? 1.0 : 0.0, dn == 1 ? 1.0 : 0.0, dn == 2 ? 1.0 : 0.0};
             for (int it = threadIdx.x; it < 2 * NF; it += NT) {
@@ -827,9 +810,7 @@ __global__ void __launch_bounds__(gl_threads<NQ>(), 2) gl_stage_kernel(const Sta
             __syncthreads();
             for (int it = threadIdx.x; it < 2 * NF * NQ; it += NT) {
                 const int side = it / (NF * NQ), r = it % (NF * NQ), q2 = r / NQ, l = r % NQ;
-                const int t1c = q2 % NQ, t2c = q2 / NQ;
-                const int node = dn == 0 ? (t2c * NQ + t1c) * NQ + l : dn == 1 ? (t2c * NQ + l) * NQ + t1c
-                                                                               : (l * NQ + t2c) * NQ + t1c;
+                const int node = gl_line_node<NQ>(dn, q2, l);
                 NodeQ<double> qv, qf;
                 load_q<double>(sN, Q3, node, qv);
                 load_q<double>(sQF, 2 * NF, side * NF + q2, qf);
@@ -844,6 +825,7 @@ __global__ void __launch_bounds__(gl_threads<NQ>(), 2) gl_stage_kernel(const Sta
                 const double sgn = side ? 1.0 : -1.0;
                 const double wf = tab->wq[q2 % NQ] * tab->wq[q2 / NQ];
                 double hs[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
                 for (int l = 0; l < NQ; ++l) {
                     const double Hop = tab->phis[side][l] * wf * sgn;
                     const double* F = s2 + ((size_t)(side * NF + q2) * NQ + l) * 5;
@@ -856,8 +838,7 @@ __global__ void __launch_bounds__(gl_threads<NQ>(), 2) gl_stage_kernel(const Sta
             for (int it = threadIdx.x; it < NF * NQ; it += NT) {   // volume sums (other outputs)
                 const int q2 = it / NQ, l = it % NQ;
                 const int t1c = q2 % NQ, t2c = q2 / NQ;
-                const int node = dn == 0 ? (t2c * NQ + t1c) * NQ + l : dn == 1 ? (t2c * NQ + l) * NQ + t1c
-                                                                               : (l * NQ + t2c) * NQ + t1c;
+                const int node = gl_line_node<NQ>(dn, q2, l);
                 const double wf = tab->wq[t1c] * tab->wq[t2c];
 #pragma unroll
                 for (int side = 0; side < 2; ++side) {
@@ -871,8 +852,8 @@ __global__ void __launch_bounds__(gl_threads<NQ>(), 2) gl_stage_kernel(const Sta
         }
     }
     // ---- assembly: r = -chi^T (x3) [div (+ hybrid)] + sum_f lift(face array) (+ viscous volume)
-    gl_apply3T<NT>(tab->chi, ND, NQ, sDiv, Q3, sU, D3, 5, t0, t1, -1.0, false);
-    gl_lift_faces<NT>(sF, 5 * NF, NF, 5, NQ, ND, tab->chis[0], tab->chis[1], tab->chi, t0, t1, sU, D3, 0, 1.0);
+    gl_apply3<NT, ND, NQ, 5, true>(T.chi, sDiv, Q3, sU, D3, t0, t1, -1.0, false);
+    gl_lift_faces<NT, NQ, ND, 5>(sF, 5 * NF, NF, tab->chis[0], tab->chis[1], T.chi, t0, t1, sU, D3, 1.0);
     if constexpr (VISC) {
         for (int i = threadIdx.x; i < 4 * D3; i += NT) sU[D3 + i] += __ldg(&g.vis[(size_t)cell * 4 * D3 + i]);
         __syncthreads();
@@ -884,7 +865,7 @@ __global__ void __launch_bounds__(gl_threads<NQ>(), 2) gl_stage_kernel(const Sta
         return;
     }
     // k = M^-1 R = (1/h) (M+K)^-1 (x3) (R / h^2)
-    gl_apply3<NT>(tab->minv, ND, ND, sU, D3, sQ, D3, 5, t0, t1, a.inv_h, false);
+    gl_apply3<NT, ND, ND, 5>(T.minv, sU, D3, sQ, D3, t0, t1, a.inv_h, false);
     if (a.mode == 1) {
         for (int i = threadIdx.x; i < 5 * D3; i += NT) a.out[(size_t)cell * 5 * D3 + i] = sQ[i];
         return;

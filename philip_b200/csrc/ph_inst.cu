@@ -266,7 +266,7 @@ template cudaError_t launch_integrals<PH_N1>(const double*, const double*, const
 // ---- uncollocated path
 template <typename K>
 static cudaError_t launch_gl_kernel(K kern, size_t bytes, int threads, const StageArgs& a, const GlArgs& g,
-                                   bool& configured, cudaStream_t s) {
+                                   const GlTab& ht, bool& configured, cudaStream_t s) {
     if (!configured) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         if (e != cudaSuccess) return e;
@@ -274,54 +274,56 @@ static cudaError_t launch_gl_kernel(K kern, size_t bytes, int threads, const Sta
     }
     const int grid = a.nc - a.cell_begin;
     if (grid <= 0) return cudaErrorInvalidValue;
-    kern<<<grid, threads, bytes, s>>>(a, g);
+    kern<<<grid, threads, bytes, s>>>(a, g, ht);
     return cudaGetLastError();
 }
 
 template <int ND, int NQ>
-static cudaError_t launch_gl_nq(int kernel, const StageArgs& a, const GlArgs& g, bool visc, bool split,
-                                cudaStream_t s) {
+static cudaError_t launch_gl_nq(int kernel, const StageArgs& a, const GlArgs& g, const GlTab& ht, bool visc,
+                                bool split, cudaStream_t s) {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     constexpr int NT = gl_threads<NQ>();
     static bool cfg[8][64] = {};
     if (kernel == 0) {
-        if (split) return launch_gl_kernel(gl_trace_kernel<ND, NQ, true>, GlTraceLayout<ND, NQ, true>::bytes, NT, a, g,
+        if (split) return launch_gl_kernel(gl_trace_kernel<ND, NQ, true>, GlTraceLayout<ND, NQ, true>::bytes, NT, a, g, ht,
                                            cfg[0][dev], s);
-        return launch_gl_kernel(gl_trace_kernel<ND, NQ, false>, GlTraceLayout<ND, NQ, false>::bytes, NT, a, g,
+        return launch_gl_kernel(gl_trace_kernel<ND, NQ, false>, GlTraceLayout<ND, NQ, false>::bytes, NT, a, g, ht,
                                 cfg[1][dev], s);
     }
     if (kernel == 1) {
-        if (split) return launch_gl_kernel(gl_aux_kernel<ND, NQ, true>, GlAuxLayout<ND, NQ, true>::bytes, NT, a, g,
+        if (split) return launch_gl_kernel(gl_aux_kernel<ND, NQ, true>, GlAuxLayout<ND, NQ, true>::bytes, NT, a, g, ht,
                                            cfg[2][dev], s);
-        return launch_gl_kernel(gl_aux_kernel<ND, NQ, false>, GlAuxLayout<ND, NQ, false>::bytes, NT, a, g,
+        return launch_gl_kernel(gl_aux_kernel<ND, NQ, false>, GlAuxLayout<ND, NQ, false>::bytes, NT, a, g, ht,
                                 cfg[3][dev], s);
     }
     if (visc) {
         if (split) return launch_gl_kernel(gl_stage_kernel<ND, NQ, true, true>, GlStageLayout<ND, NQ, true, true>::bytes,
-                                           NT, a, g, cfg[4][dev], s);
+                                           NT, a, g, ht, cfg[4][dev], s);
         return launch_gl_kernel(gl_stage_kernel<ND, NQ, true, false>, GlStageLayout<ND, NQ, true, false>::bytes, NT, a,
-                                g, cfg[5][dev], s);
+                                g, ht, cfg[5][dev], s);
     }
     if (split) return launch_gl_kernel(gl_stage_kernel<ND, NQ, false, true>, GlStageLayout<ND, NQ, false, true>::bytes,
-                                       NT, a, g, cfg[6][dev], s);
+                                       NT, a, g, ht, cfg[6][dev], s);
     return launch_gl_kernel(gl_stage_kernel<ND, NQ, false, false>, GlStageLayout<ND, NQ, false, false>::bytes, NT, a,
-                            g, cfg[7][dev], s);
+                            g, ht, cfg[7][dev], s);
 }
 
 template <int N1>
-cudaError_t launch_gl(int kernel, int nq, const StageArgs& a, const GlArgs& g, bool visc, bool split, cudaStream_t s) {
-    if (nq == N1) return launch_gl_nq<N1, N1>(kernel, a, g, visc, split, s);
+cudaError_t launch_gl(int kernel, int nq, const StageArgs& a, const GlArgs& g, const GlTab& ht, bool visc, bool split,
+                      cudaStream_t s) {
+    if (nq == N1) return launch_gl_nq<N1, N1>(kernel, a, g, ht, visc, split, s);
     if constexpr (N1 + 1 <= GL_MAXQ) {
-        if (nq == N1 + 1) return launch_gl_nq<N1, N1 + 1>(kernel, a, g, visc, split, s);
+        if (nq == N1 + 1) return launch_gl_nq<N1, N1 + 1>(kernel, a, g, ht, visc, split, s);
     }
     if constexpr (N1 + 2 <= GL_MAXQ) {
-        if (nq == N1 + 2) return launch_gl_nq<N1, N1 + 2>(kernel, a, g, visc, split, s);
+        if (nq == N1 + 2) return launch_gl_nq<N1, N1 + 2>(kernel, a, g, ht, visc, split, s);
     }
     return cudaErrorInvalidValue;
 }
-template cudaError_t launch_gl<PH_N1>(int, int, const StageArgs&, const GlArgs&, bool, bool, cudaStream_t);
+template cudaError_t launch_gl<PH_N1>(int, int, const StageArgs&, const GlArgs&, const GlTab&, bool, bool,
+                                      cudaStream_t);
 
 template <int N1>
 cudaError_t launch_limiter(const LimiterArgs& a, cudaStream_t s) {

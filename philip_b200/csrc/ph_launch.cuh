@@ -46,7 +46,8 @@ bool batched_shape(int fp32, bool curv, int variant, int* cpc, int* threads, siz
 // 1 = auxiliary equation and viscous terms (gl_aux_kernel), 2 = residual / RK stage
 // (gl_stage_kernel); one CTA per cell of [a.cell_begin, a.nc).
 template <int N1>
-cudaError_t launch_gl(int kernel, int nq, const StageArgs& a, const GlArgs& g, bool visc, bool split, cudaStream_t s);
+cudaError_t launch_gl(int kernel, int nq, const StageArgs& a, const GlArgs& g, const GlTab& ht, bool visc, bool split,
+                      cudaStream_t s);
 // dKE/dt of state U with time derivative K, per-cell partial sums (affine cells)
 template <int N1>
 cudaError_t launch_ke_rate(const double* U, const double* K, const IntegralTab* tab, int nc, double h3,
