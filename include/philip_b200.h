@@ -263,8 +263,9 @@ int ph_get_timing(ph_ctx* ctx, double out[7]);
  * ph_cell_ijk), whatever mesh->cell_order says; the state, ph_ndofs and the integrals cover
  * the owned cells only (ph_integrals / ph_integrated_quantities give this rank's share of
  * each volume average: sum them over ranks, and take the max of the wave speed). Slab
- * contexts take affine meshes, no relaxation RK, and launch directly (no step graph,
- * ph_run refused). z_count = n is the whole mesh on one rank: its ghost layers are its own last
+ * contexts take GLL flux nodes without overintegration, no relaxation RK, and launch directly
+ * (no step graph, ph_run refused); on a curvilinear mesh mapping_support_points, when given,
+ * covers the slab's own cells in the slab's state order. z_count = n is the whole mesh on one rank: its ghost layers are its own last
  * and first layers (a halo that copies send_hi to recv_lo and send_lo to recv_hi). */
 enum { PH_HALO_STATE = 0, PH_HALO_VISCOUS = 1 };   /* what is exchanged */
 enum { PH_HALO_BEGIN = 0, PH_HALO_END = 1 };        /* phase of the exchange */

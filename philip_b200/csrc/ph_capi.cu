@@ -1207,7 +1207,6 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
     if (slab) {
         if (z0 < 0 || z0 >= mesh->n_cells_per_direction || nz > mesh->n_cells_per_direction)
             return fail(PH_ERR_INVALID, "slab outside the mesh: 0 <= z_first < n and 1 <= z_count <= n");
-        if (is_curvilinear(mesh)) return fail(PH_ERR_UNSUPPORTED, "slab contexts take affine meshes");
         if (gl) return fail(PH_ERR_UNSUPPORTED, "slab contexts take GLL flux nodes without overintegration");
         if (prm->use_relaxation_runge_kutta)
             return fail(PH_ERR_UNSUPPORTED, "slab contexts: relaxation RK needs global entropy sums per root iterate");

@@ -643,34 +643,60 @@ gl_stage_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab
         }
         __syncthreads();
         // two-point volume term: sum over the node's three flux-node lines of
-        // skew[x_d][l] w_a w_b F(u_i, u_l) . e_d   (operators.cpp:983-1062)
-        for (int q = threadIdx.x; q < Q3; q += NT) {
-            const int xi[3] = {q % NQ, (q / NQ) % NQ, q / NF};
-            NodeQ<double> qi;
-            load_q<double>(sN, Q3, q, qi);
-            double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        // skew[x_d][l] w_a w_b F(u_i, u_l) . e_d   (operators.cpp:983-1062), pair-symmetric on
+        // warp segments as in the collocated kernel: segments of NQ lanes own the lines along
+        // rd; lane pos evaluates the pairs (pos, pos + k), k = 1 .. NQ / 2, in the frame whose x
+        // axis is e_rd and receives the pair (pos - k, pos) from lane pos - k of its segment (the
+        // two-point fluxes are symmetric); w_a w_b, the same along a line, scales the sum.
+        constexpr int SPW = 32 / NQ, NSEG = (NT / 32) * SPW;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        const int lseg = lane / NQ, pos = lane - lseg * NQ, segbase = lseg * NQ;
+#pragma unroll 1
+        for (int rd = 0; rd < 3; ++rd) {
+            const int st = rd == 0 ? 1 : rd == 1 ? NQ : NF;
+#pragma unroll 1
+            for (int l0 = 0; l0 < NF; l0 += NSEG) {
+                const int lt = l0 + warp * SPW + lseg;
+                const bool valid = lseg < SPW && lt < NF;
+                const int node = gl_line_node<NQ>(rd, valid ? lt : 0, pos);
+                const int base = node - pos * st;
+                NodeQ<double> qi;
+                load_q_rot<double>(sN, Q3, node, rd, qi);
+                double accr[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-            for (int rd = 0; rd < 3; ++rd) {
-                const int ra = rd == 0 ? 1 : 0, rb = rd == 2 ? 1 : 2;
-                const double wab = tab->wq[xi[ra]] * tab->wq[xi[rb]];
-                const double nv[3] = {rd == 0 ? 1.0 : 0.0, rd == 1 ? 1.0 : 0.0, rd == 2 ? 1.0 : 0.0};
-                const int st = rd == 0 ? 1 : rd == 1 ? NQ : NF;
-                const int base = q - xi[rd] * st;
-                for (int l = 0; l < NQ; ++l) {
-                    if (l == xi[rd]) continue;
+                for (int k = 1; k <= NQ / 2; ++k) {
+                    const int jp = pos + k < NQ ? pos + k : pos + k - NQ;   // (pos + k) mod NQ
+                    const int jm = pos - k >= 0 ? pos - k : pos - k + NQ;   // (pos - k) mod NQ
+                    const bool dup = ((NQ & 1) == 0) && (2 * k == NQ);
                     NodeQ<double> qj;
-                    load_q<double>(sN, Q3, base + l * st, qj);
+                    load_q_rot<double>(sN, Q3, base + jp * st, rd, qj);
                     double F[5];
-                    two_point_n<double>(qi, qj, nv, tp, cst, F);
-                    const double Qc = tab->skew[xi[rd] * NQ + l] * wab;
+                    two_point_dir<double, 0>(qi, qj, tp, cst, F);
+                    const double cj = tab->skew[pos * NQ + jp], cr = tab->skew[pos * NQ + jm];
 #pragma unroll
-                    for (int s = 0; s < 5; ++s) acc[s] += Qc * F[s];
+                    for (int s = 0; s < 5; ++s) {
+                        const double fr = __shfl_sync(0xffffffffu, F[s], segbase + jm);
+                        accr[s] += cj * F[s];
+                        if (!dup) accr[s] += cr * fr;
+                    }
+                }
+                // back to (x, y, z) components by selects (a run-time index would put acc in
+                // local memory)
+                const double acc[5] = {accr[0], rd == 0 ? accr[1] : rd == 1 ? accr[3] : accr[2],
+                                       rd == 0 ? accr[2] : rd == 1 ? accr[1] : accr[3],
+                                       rd == 0 ? accr[3] : rd == 1 ? accr[2] : accr[1], accr[4]};
+                if (valid) {
+                    const int t1c = lt % NQ, t2c = lt / NQ;
+                    const double wab = tab->wq[t1c] * tab->wq[t2c];
+#pragma unroll
+                    for (int s = 0; s < 5; ++s) {
+                        double* o = sDiv + s * Q3 + node;
+                        *o = rd == 0 ? wab * acc[s] : *o + wab * acc[s];
+                    }
                 }
             }
-#pragma unroll
-            for (int s = 0; s < 5; ++s) sDiv[s * Q3 + q] = acc[s];
+            __syncthreads();
         }
-        __syncthreads();
     } else {
         // conservative: W div(F(chi u)) by the flux-node derivative   (strong_dg.cpp:1546)
         for (int q = threadIdx.x; q < Q3; q += NT) {

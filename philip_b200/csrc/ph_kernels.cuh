@@ -1066,13 +1066,18 @@ aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, int cell_b
         int cell = cell0 + it / (5 * NP); if (cell >= nc) cell = nc - 1;
         sU[it] = (R)__ldg(&U[(size_t)cell * 5 * NP + it % (5 * NP)]);
     }
+    // neighbour traces: one thread per (cell, face, face node) finds the node once and loads
+    // its five components
 #pragma unroll
-    for (int it = tid; it < CPC * 6 * 5 * NF; it += NT) {
-        const int fn = it % NF, s = (it / NF) % 5, f = (it / (5 * NF)) % 6, c = it / (30 * NF);
+    for (int it = tid; it < CPC * 6 * NF; it += NT) {
+        const int fn = it % NF, f = (it / NF) % 6, c = it / (6 * NF);
         int cell = cell0 + c; if (cell >= nc) cell = nc - 1;
         const int cn = __ldg(&nbr[cell * 6 + f]);
         const int nn = face_node_volume_index<N1>(f, fn, (f & 1) ? 0 : N1 - 1);
-        sT[it] = (R)__ldg(&U[((size_t)cn * 5 + s) * NP + nn]);
+        const double* src = U + (size_t)cn * 5 * NP + nn;
+        R* dst = sT + (c * 6 + f) * 5 * NF + fn;
+#pragma unroll
+        for (int s = 0; s < 5; ++s) dst[s * NF] = (R)__ldg(&src[s * NP]);
     }
     if constexpr (aux_line_form<R, N1, FRA>()) {
         R* sG = sT + CPC * 6 * 5 * NF;   // [c][d][5][NP] gradient, later [c][d][4][NP] flux
@@ -1179,14 +1184,17 @@ aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, int cell_b
             if (cell >= nc) continue;
             Fv[(size_t)cell * VT + it % (4 * NP)] = sU[c * 4 * NP + it % (4 * NP)];
         }
-        for (int it = tid; it < CPC * 24 * NF; it += NT) {
-            const int c = it / (24 * NF), j = it % (24 * NF);
+        for (int it = tid; it < CPC * 6 * NF; it += NT) {   // one thread per (cell, face, face node)
+            const int c = it / (6 * NF), j = it % (6 * NF);
             const int cell = cell0 + c;
             if (cell >= nc) continue;
-            const int f = j / (4 * NF), k = (j / NF) % 4, fn = j % NF;
+            const int f = j / NF, fn = j % NF;
             const int d = f >> 1;
             const int node = line_node<N1>(d, fn, (f & 1) ? N1 - 1 : 0);
-            Fv[(size_t)cell * VT + 4 * NP + j] = sG[(c * 15 + d * 4 + k) * NP + node];
+            R* dst = Fv + (size_t)cell * VT + 4 * NP + f * 4 * NF + fn;
+            const R* src = sG + (c * 15 + d * 4) * NP + node;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) dst[k * NF] = src[k * NP];
         }
     } else {
         R* sDm = sT + CPC * 6 * 5 * NF;

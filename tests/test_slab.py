@@ -150,7 +150,8 @@ def test_slab_refusals_without_a_gpu():
     assert create(4, 1) == _lib.PH_ERR_INVALID
     assert create(0, 0) == _lib.PH_ERR_INVALID
     assert create(1, 5) == _lib.PH_ERR_INVALID
-    assert create(0, 2, warp=0.1) == _lib.PH_ERR_UNSUPPORTED and b"affine" in L.ph_last_error()
+    assert create(0, 2, edit=lambda q: setattr(q, "flux_nodes_type", 0)) == _lib.PH_ERR_UNSUPPORTED
+    assert b"GLL" in L.ph_last_error()
     assert create(0, 2, edit=lambda q: setattr(q, "use_relaxation_runge_kutta", 1)) == _lib.PH_ERR_UNSUPPORTED
     del p
 
@@ -205,7 +206,7 @@ class ThreadHalo:
             return 1
 
 
-def _slabs(prm, world, precision=_lib.PH_FP64):
+def _slabs(prm, world, precision=_lib.PH_FP64, warp=0.0):
     import torch
     from philip_b200.dg import DGStrong
     shared = ThreadHalo.shared(world)
@@ -215,7 +216,7 @@ def _slabs(prm, world, precision=_lib.PH_FP64):
         s = torch.cuda.Stream()
         halo = base.for_rank(r)
         dg = DGStrong(prm, precision=precision, stream=s.cuda_stream,
-                      slab=slab_bounds(prm.n_cells, world, r), halo=halo)
+                      slab=slab_bounds(prm.n_cells, world, r), halo=halo, warp=warp)
         out.append((dg, s))
     return out
 
@@ -384,3 +385,53 @@ def test_one_slab_with_its_own_ghosts_is_the_whole_mesh(kw):
     RungeKuttaODESolver(whole).step_in_time(1e-3, nsteps=2)
     RungeKuttaODESolver(one).step_in_time(1e-3, nsteps=2)
     assert np.array_equal(_gather(whole, [one], [one.solution]), whole.solution)
+
+
+CURV_CASES = [
+    ("euler_ch_p3_two_slabs", dict(poly_degree=3, n_cells=4), 2, _lib.PH_FP64),
+    ("euler_ir_p2_three_slabs", dict(poly_degree=2, n_cells=4, two_point="IR", conv="two_point_flux"), 3,
+     _lib.PH_FP64),
+    ("euler_ch_p4_precision_form", dict(poly_degree=4, n_cells=4), 2, _lib.PH_FP32_RESIDUAL),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,kw,world,precision", CURV_CASES, ids=[c[0] for c in CURV_CASES])
+def test_curvilinear_slabs_are_the_whole_curvilinear_mesh(name, kw, world, precision):
+    """Slabs of the sine-warped cube (warp 0.1): each slab builds the metric terms of its own
+    cells, and its faces use the metric of their own side, so the residual, three RK4 steps and
+    the integrals are bitwise (the sums to rounding) the whole curvilinear mesh's."""
+    from oracle.oracle import Oracle
+    from philip_b200.dg import DGStrong, RungeKuttaODESolver
+    from philip_b200.prm import Parameters
+    from helpers import TWO_PI, perturbed_tgv, prm_dict
+    warp = 0.1
+    prm = Parameters.from_dict(prm_dict(**kw))
+    whole = DGStrong(prm, precision=precision, warp=warp)
+    U0 = perturbed_tgv(Oracle(prm.oracle_cfg(), prm.n_cells, *prm.grid_bounds), seed=len(name))
+    parts = _slabs(prm, world, precision, warp=warp)
+    dgs = [p for p, _ in parts]
+    Us = _scatter(whole, dgs, U0)
+    Rs = _in_threads([lambda k=k: dgs[k].residual_of(Us[k]) for k in range(world)])
+    R = _gather(whole, dgs, Rs)
+    print(f"{name}: max |R_slabs - R_whole| = {np.max(np.abs(R - whole.residual_of(U0))):.3e}")
+    assert np.array_equal(R, whole.residual_of(U0))
+    dt = 0.1 * TWO_PI / prm.n_cells / (prm.poly_degree + 1) / 11.0
+    whole.solution = U0
+    RungeKuttaODESolver(whole).step_in_time(dt, nsteps=3)
+    for dg, u in zip(dgs, Us):
+        dg.solution = u
+
+    def steps(k):
+        RungeKuttaODESolver(dgs[k]).step_in_time(dt, nsteps=3)
+        parts[k][1].synchronize()
+        return dgs[k].solution, dgs[k].integrals()
+
+    res = _in_threads([lambda k=k: steps(k) for k in range(world)])
+    U = _gather(whole, dgs, [r[0] for r in res])
+    print(f"{name}: max |U_slabs - U_whole| = {np.max(np.abs(U - whole.solution)):.3e}")
+    assert np.array_equal(U, whole.solution)
+    q = np.array([r[1] for r in res])
+    qw = whole.integrals()
+    assert np.allclose(q[:, :3].sum(axis=0), qw[:3], rtol=1e-13, atol=0.0)
+    assert q[:, 3].max() == qw[3]
