@@ -263,8 +263,8 @@ int ph_get_timing(ph_ctx* ctx, double out[7]);
  * ph_cell_ijk), whatever mesh->cell_order says; the state, ph_ndofs and the integrals cover
  * the owned cells only (ph_integrals / ph_integrated_quantities give this rank's share of
  * each volume average: sum them over ranks, and take the max of the wave speed). Slab
- * contexts take GLL flux nodes without overintegration, no relaxation RK, and launch directly
- * (no step graph, ph_run refused); on a curvilinear mesh mapping_support_points, when given,
+ * contexts take GLL flux nodes without overintegration and launch directly (no step graph,
+ * ph_run refused); with relaxation RK they need ph_set_rank_sum; on a curvilinear mesh mapping_support_points, when given,
  * covers the slab's own cells in the slab's state order. z_count = n is the whole mesh on one rank: its ghost layers are its own last
  * and first layers (a halo that copies send_hi to recv_lo and send_lo to recv_hi). */
 enum { PH_HALO_STATE = 0, PH_HALO_VISCOUS = 1 };   /* what is exchanged */
@@ -290,6 +290,16 @@ int ph_ctx_create_slab(const ph_mesh_desc* mesh, const ph_params* prm, int z_fir
                        void* cuda_stream, ph_ctx** out);
 /* Registers the exchange; every slab context needs one before it evaluates a residual. */
 int ph_set_halo_exchange(ph_ctx* ctx, ph_halo_fn fn, void* user);
+/* Sum over the ranks of one mesh, for relaxation RK on slab contexts (the root of the
+ * relaxation parameter needs the mesh's entropy integrals, RootFindingRRKODESolver,
+ * root_finding_rrk_ode_solver.cpp:15-180, where the reference's MPI vector reductions give
+ * them): on the host thread that called the library, replace values[0..count-1] by their sum
+ * over every rank's values, the same result on every rank (an all-reduce). Every rank makes
+ * the same calls in the same order. A nonzero return fails the calling entry point with
+ * PH_ERR_EXCHANGE. */
+typedef int (*ph_rank_sum_fn)(void* user, double* values, int count);
+/* Registers the sum; a slab context with relaxation RK needs one before its first step. */
+int ph_set_rank_sum(ph_ctx* ctx, ph_rank_sum_fn fn, void* user);
 /* Host only (no device work): the owned cells' (i, j, k) [z_count n^2][3] and neighbour table
  * [z_count n^2][6] (faces x-, x+, y-, y+, z-, z+) of a slab. A neighbour index below z_count n^2
  * is an owned cell; z_count n^2 + j n + i is the lower ghost (the cell (i, j) of layer

@@ -32,6 +32,7 @@ EXPORTED = ["ph_ctx_create", "ph_ctx_destroy", "ph_ndofs", "ph_cell_ijk", "ph_se
             "ph_batch_poll", "ph_batch_fence", "ph_batch_fence_wait", "ph_batch_autotune", "ph_batch_set_variant",
             "ph_batch_launches", "ph_mesh_node_xyz", "ph_rk_error_norm", "ph_last_error",
             "ph_integrated_quantities", "ph_run", "ph_rk_relaxation", "ph_ctx_create_slab", "ph_set_halo_exchange",
+            "ph_set_rank_sum",
             "ph_slab_connectivity", "ph_server_create", "ph_server_submit", "ph_server_poll", "ph_server_wait",
             "ph_server_result", "ph_server_stats", "ph_server_destroy", "ph_snapshots_create", "ph_snapshots_destroy",
             "ph_snapshots_add", "ph_snapshots_add_state", "ph_snapshots_add_batch", "ph_snapshots_count",
@@ -41,6 +42,8 @@ PH_SOLVE_QUEUED, PH_SOLVE_RUNNING, PH_SOLVE_DONE, PH_SOLVE_FAILED = 0, 1, 2, 3
 # ph_halo_fn(user, what, phase, send_lo, send_hi, recv_lo, recv_hi, bytes, cuda_stream)
 HALO_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)
+# ph_rank_sum_fn(user, values, count)
+RANK_SUM_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int)
 
 
 class PhParams(ctypes.Structure):
@@ -130,6 +133,7 @@ def load(build_if_missing: bool = False):
     L.ph_ctx_create_slab.argtypes = [ctypes.POINTER(PhMeshDesc), ctypes.POINTER(PhParams), ctypes.c_int, ctypes.c_int,
                                      vp, ctypes.POINTER(vp)]
     L.ph_set_halo_exchange.argtypes = [vp, HALO_FN, vp]
+    L.ph_set_rank_sum.argtypes = [vp, RANK_SUM_FN, vp]
     L.ph_slab_connectivity.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int32),
                                        ctypes.POINTER(ctypes.c_int32)]
     ll = ctypes.c_longlong

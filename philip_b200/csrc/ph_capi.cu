@@ -864,6 +864,8 @@ struct ph_ctx {
     int lo_end = 0, hi_begin = 0;
     ph_halo_fn halo_fn = nullptr;
     void* halo_user = nullptr;
+    ph_rank_sum_fn sum_fn = nullptr;    // slab contexts with relaxation RK
+    void* sum_user = nullptr;
     unsigned char* d_halo = nullptr;    // send_lo | send_hi | recv_lo | recv_hi, halo_stride bytes each
     size_t halo_stride = 0, halo_state_bytes = 0, halo_visc_bytes = 0;
     // the interior cells' kernels run on a second stream, concurrently with the exchange and the
@@ -1076,6 +1078,15 @@ int halo_call(ph_ctx* c, int what, int phase) {
     return PH_OK;
 }
 
+// values[0..n) summed over the ranks of the mesh (slab contexts; a whole mesh is its own sum)
+int rank_sum(ph_ctx* c, double* values, int n) {
+    if (!c->nc_ghost) return PH_OK;
+    if (!c->sum_fn) return fail(PH_ERR_INVALID, "a slab context with relaxation RK needs ph_set_rank_sum");
+    const int rc = c->sum_fn(c->sum_user, values, n);
+    if (rc) return fail(PH_ERR_EXCHANGE, "rank sum callback returned " + std::to_string(rc));
+    return PH_OK;
+}
+
 ph::StageArgs base_args(ph_ctx* c, const double* U) {
     ph::StageArgs a;
     std::memset(&a, 0, sizeof(a));
@@ -1208,8 +1219,6 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
         if (z0 < 0 || z0 >= mesh->n_cells_per_direction || nz > mesh->n_cells_per_direction)
             return fail(PH_ERR_INVALID, "slab outside the mesh: 0 <= z_first < n and 1 <= z_count <= n");
         if (gl) return fail(PH_ERR_UNSUPPORTED, "slab contexts take GLL flux nodes without overintegration");
-        if (prm->use_relaxation_runge_kutta)
-            return fail(PH_ERR_UNSUPPORTED, "slab contexts: relaxation RK needs global entropy sums per root iterate");
     }
     ph_ctx* c = new ph_ctx();
     c->prm = *prm;
@@ -1388,6 +1397,13 @@ int ph_set_halo_exchange(ph_ctx* c, ph_halo_fn fn, void* user) {
     if (!c) return fail(PH_ERR_INVALID, "null argument");
     c->halo_fn = fn;
     c->halo_user = user;
+    return PH_OK;
+}
+
+int ph_set_rank_sum(ph_ctx* c, ph_rank_sum_fn fn, void* user) {
+    if (!c) return fail(PH_ERR_INVALID, "null argument");
+    c->sum_fn = fn;
+    c->sum_user = user;
     return PH_OK;
 }
 
@@ -1610,6 +1626,7 @@ static int rrk_entropy(ph_ctx* c, const double* u1, double g, double* out) {
     PH_CUDA(cudaStreamSynchronize(c->stream));
     double sum = 0.0;
     for (int i = 0; i < c->nc; ++i) sum += c->h_ent[i];
+    if (int rc = rank_sum(c, &sum, 1)) return rc;   // a slab's share -> the mesh's
     *out = sum;
     return PH_OK;
 }
@@ -1637,12 +1654,12 @@ static int rrk_one_step(ph_ctx* c, double dt) {
     std::vector<double> part((size_t)ns * c->ent_tiles);
     PH_CUDA(cudaMemcpyAsync(part.data(), c->d_ent, part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     PH_CUDA(cudaStreamSynchronize(c->stream));
+    double si[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int i = 0; i < ns; ++i)
+        for (int t = 0; t < tiles; ++t) si[i] += part[(size_t)i * c->ent_tiles + t];
+    if (int rc = rank_sum(c, si, ns)) return rc;
     double est = 0.0;
-    for (int i = 0; i < ns; ++i) {
-        double si = 0.0;
-        for (int t = 0; t < tiles; ++t) si += part[(size_t)i * c->ent_tiles + t];
-        est += c->b[i] * si;
-    }
+    for (int i = 0; i < ns; ++i) est += c->b[i] * si[i];
     est *= dt;
     double eta_n = 0.0;
     if (int rc = rrk_entropy(c, u1, 0.0, &eta_n)) return rc;

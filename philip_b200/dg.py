@@ -59,7 +59,9 @@ class DGStrong:
         warp (L/2pi) sin(2pi(x-l)/L) sin(2pi(y-l)/L) sin(2pi(z-l)/L), mapping degree = p.
         mapping_support_points ([cell][3][(p+1)^3], GLL points) gives any other curved mapping.
         slab = (z_first, z_count): this process's layers of a mesh shared by several GPUs
-        (philip_b200.slab); halo: the object whose `callback` exchanges the partition faces;
+        (philip_b200.slab); halo: the object whose `callback` exchanges the partition faces
+        (and whose `sum_callback`, when present, sums the relaxation RK entropy integrals over
+        the ranks);
         dist: the torch.distributed module (initialised) over which the integrals, maxima and
         error norms of the slabs are combined into the mesh's (None: this slab's share)."""
         self.L = _lib.load()
@@ -85,6 +87,8 @@ class DGStrong:
                              and dist.get_world_size() > 1) else None
         if halo is not None:
             _lib.check(self.L.ph_set_halo_exchange(h, halo.callback, None))
+            if getattr(halo, "sum_callback", None) is not None:   # relaxation RK: the mesh's entropy sums
+                _lib.check(self.L.ph_set_rank_sum(h, halo.sum_callback, None))
         self.n_dofs = int(self.L.ph_ndofs(h))
         self.poly_degree = parameters.poly_degree
         self.n_cells = parameters.n_cells ** 2 * (slab[1] if slab is not None else parameters.n_cells)

@@ -64,6 +64,7 @@ class DistributedHalo:
         self.hi = glob((self.rank + 1) % self.world)
         self._pending = None
         self.callback = _lib.HALO_FN(self._call)    # referenced for as long as the halo lives
+        self.sum_callback = _lib.RANK_SUM_FN(self._sum)
 
     def _stream_ctx(self, stream):
         import contextlib
@@ -100,6 +101,23 @@ class DistributedHalo:
             traceback.print_exc(file=sys.stderr)
             return 1
 
+    def sum(self, values):
+        """values summed over the ranks (all-reduce of a float64 vector), as a list."""
+        import torch
+        t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM, group=self.group)
+        return t.cpu().tolist()
+
+    def _sum(self, user, values, count):   # ph_rank_sum_fn
+        try:
+            out = self.sum([values[i] for i in range(count)])
+            for i in range(count):
+                values[i] = out[i]
+            return 0
+        except Exception:
+            traceback.print_exc(file=sys.stderr)
+            return 1
+
 
 class LoopbackHalo:
     """ph_halo_fn of a slab that owns every layer (one rank): its lower ghost layer is its own
@@ -109,6 +127,7 @@ class LoopbackHalo:
     def __init__(self, device: str = "cuda"):
         self.device = device
         self.callback = _lib.HALO_FN(self._call)
+        self.sum_callback = _lib.RANK_SUM_FN(lambda user, values, count: 0)   # one rank: its own sum
 
     def _call(self, user, what, phase, send_lo, send_hi, recv_lo, recv_hi, nbytes, stream):
         try:

@@ -105,7 +105,10 @@ def _exchange_worker(rank, world, port, n, out):
                     ok &= bool(np.all((recv_lo if side == 0 else recv_hi)[ii] == want))
         # the volume averages of the slabs add up, the wave speed is the largest
         tot = global_integrals([1.0 + rank, 2.0, 0.5, 3.0 + rank], dist)
-        out[rank] = (ok, tot)
+        # the relaxation RK sum through the library's callback type: in place, on every rank
+        vals = (ctypes.c_double * 3)(1.0 + rank, -0.5 * rank, 0.25)
+        rc = halo.sum_callback(None, vals, 3)
+        out[rank] = (ok, tot, rc, list(vals))
     finally:
         dist.destroy_process_group()
 
@@ -117,9 +120,11 @@ def test_halo_exchange_fills_the_ghost_layers(world, n):
         mp.spawn(_exchange_worker, args=(world, _free_port(), n, out), nprocs=world, join=True)
         res = dict(out)
     for r in range(world):
-        ok, tot = res[r]
+        ok, tot, rc, sums = res[r]
         assert ok
         assert tot == [sum(1.0 + q for q in range(world)), 2.0 * world, 0.5 * world, 3.0 + world - 1]
+        assert rc == 0 and sums == [sum(1.0 + q for q in range(world)), sum(-0.5 * q for q in range(world)),
+                                    0.25 * world]
 
 
 def test_loopback_halo_feeds_a_slab_its_own_layers():
@@ -152,7 +157,6 @@ def test_slab_refusals_without_a_gpu():
     assert create(1, 5) == _lib.PH_ERR_INVALID
     assert create(0, 2, edit=lambda q: setattr(q, "flux_nodes_type", 0)) == _lib.PH_ERR_UNSUPPORTED
     assert b"GLL" in L.ph_last_error()
-    assert create(0, 2, edit=lambda q: setattr(q, "use_relaxation_runge_kutta", 1)) == _lib.PH_ERR_UNSUPPORTED
     del p
 
 
@@ -172,11 +176,36 @@ class ThreadHalo:
         h = ThreadHalo(self.world, self.state)
         h.rank = rank
         h.callback = _lib.HALO_FN(h._call)
+        h.sum_callback = _lib.RANK_SUM_FN(h._sum)
         return h
 
     @staticmethod
     def shared(world):
-        return {"barrier": threading.Barrier(world, timeout=120), "send": {}}
+        return {"barrier": threading.Barrier(world, timeout=120), "send": {}, "sums": {}}
+
+    def _sum(self, user, values, count):
+        """ph_rank_sum_fn: every rank publishes its values and, after a barrier, sums all ranks'
+        in rank order (the same result on every rank); a second barrier keeps them published
+        until all have read."""
+        try:
+            st = self.state
+            st["sums"][self.rank] = [values[i] for i in range(count)]
+            st["barrier"].wait()
+            for i in range(count):
+                acc = 0.0
+                for r in range(self.world):
+                    acc += st["sums"][r][i]
+                values[i] = acc
+            st["barrier"].wait()
+            return 0
+        except Exception:
+            import traceback
+            traceback.print_exc()
+            try:
+                self.state["barrier"].abort()
+            except Exception:
+                pass
+            return 1
 
     def _call(self, user, what, phase, send_lo, send_hi, recv_lo, recv_hi, nbytes, stream):
         import torch
@@ -435,3 +464,67 @@ def test_curvilinear_slabs_are_the_whole_curvilinear_mesh(name, kw, world, preci
     qw = whole.integrals()
     assert np.allclose(q[:, :3].sum(axis=0), qw[:3], rtol=1e-13, atol=0.0)
     assert q[:, 3].max() == qw[3]
+
+
+RRK_CASES = [
+    ("entropy_conservative_p3_two_slabs", dict(poly_degree=3, n_cells=4, two_point="CH", conv="two_point_flux"), 2),
+    ("roe_dissipation_p2_three_slabs", dict(poly_degree=2, n_cells=4), 3),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,kw,world", RRK_CASES, ids=[c[0] for c in RRK_CASES])
+def test_relaxation_rk_on_slabs(name, kw, world):
+    """Relaxation RK on slabs: the entropy integrals of every root iterate and the stage
+    estimates are summed over the ranks (ph_set_rank_sum), so every slab takes the same
+    relaxation parameter as the whole mesh up to the summation order of those integrals (the
+    bounds of the GPU-vs-oracle relaxation test: 1e-5 on gamma, 5e-9 on the state); with the
+    entropy-conservative scheme the slabs' relaxed steps conserve the mesh's numerical entropy to
+    rounding. A slab without the sum is refused at its first step."""
+    from oracle.oracle import Oracle
+    from philip_b200.dg import DGStrong, RungeKuttaODESolver
+    from philip_b200.prm import Parameters
+    from philip_b200.slab import LoopbackHalo
+    from helpers import prm_dict
+    d = prm_dict(**kw)
+    d["ODE solver/rrk root solver/use_relaxation_runge_kutta"] = "true"
+    prm = Parameters.from_dict(d)
+    orc = Oracle(prm.oracle_cfg(), prm.n_cells, *prm.grid_bounds)
+    U0 = orc.initial_condition("tgv")
+    dt = 0.02
+    whole = DGStrong(prm)
+    whole.solution = U0
+    ode = RungeKuttaODESolver(whole)
+    parts = _slabs(prm, world)
+    dgs = [p for p, _ in parts]
+    for dg, u in zip(dgs, _scatter(whole, dgs, U0)):
+        dg.solution = u
+    odes = [RungeKuttaODESolver(dg) for dg in dgs]
+    e0 = orc.numerical_entropy(U0)
+    for step in range(4):
+        ode.step_in_time(dt)
+        _in_threads([lambda k=k: (odes[k].step_in_time(dt), parts[k][1].synchronize()) for k in range(world)])
+        gam = [o.relaxation_parameter for o in odes]
+        U = _gather(whole, dgs, [dg.solution for dg in dgs])
+        err = float(np.max(np.abs(U - whole.solution)) / np.max(np.abs(whole.solution)))
+        g_err = max(abs(g - ode.relaxation_parameter) for g in gam) / ode.relaxation_parameter
+        print(f"{name} step {step}: gamma {gam[0]:.15f} (whole {ode.relaxation_parameter:.15f}, rel {g_err:.2e}), "
+              f"state rel err {err:.2e}")
+        assert len(set(gam)) == 1          # every rank took the same root
+        assert g_err <= 1e-5 and err <= 5e-9
+    assert abs(odes[0].current_time - ode.current_time) <= 1e-5 * ode.current_time
+    drift = (orc.numerical_entropy(U) - e0) / abs(e0)
+    print(f"{name}: entropy change over 4 relaxed slab steps {drift:.3e}")
+    if kw.get("conv") == "two_point_flux":
+        assert abs(drift) <= 1e-12
+    else:
+        assert drift < 0.0
+
+    class NoSum:
+        def __init__(self, halo):
+            self.callback = halo.callback
+
+    lonely = DGStrong(prm, slab=(0, prm.n_cells), halo=NoSum(LoopbackHalo()))
+    lonely.solution = _scatter(whole, [lonely], U0)[0]
+    with pytest.raises(_lib.PhError, match="ph_set_rank_sum"):
+        RungeKuttaODESolver(lonely).step_in_time(dt)
