@@ -304,7 +304,11 @@ const char* unsupported_reason(const ph_mesh_desc* mesh, const ph_params* prm) {
     if (is_curvilinear(mesh)) {
         if (mesh->mapping_support_points == nullptr && mesh->grid_degree != prm->poly_degree)
             return "curvilinear meshes take grid_degree = poly_degree";
-        if (prm->pde_type != 0) return "curvilinear meshes take the Euler equations";
+        if (prm->pde_type != 0 && prm->diss_num_flux == 0)
+            return "curvilinear Navier-Stokes takes bassi_rebay_2 or central_visc_flux (the SIPG penalty's cell "
+                   "extent on curved cells is not restated)";
+        if (prm->pde_type != 0 && prm->flux_reconstruction_aux != 0)
+            return "curvilinear Navier-Stokes takes flux_reconstruction_aux = kDG";
         if (!prm->use_split_form) return "curvilinear meshes take the split form";
         if (prm->flux_reconstruction != 0) return "curvilinear meshes take cDG";
     }
@@ -947,12 +951,12 @@ int dispatch_aux(ph_ctx* c, const double* U, int cell_begin, int cell_end) {
     const double inv_h = 1.0 / c->h;
     timer_begin(c);
     switch (c->N1) {
-    case 2: e = ph::launch_aux<2>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
-    case 3: e = ph::launch_aux<3>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
-    case 4: e = ph::launch_aux<4>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
-    case 5: e = ph::launch_aux<5>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
-    case 6: e = ph::launch_aux<6>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
-    case 7: e = ph::launch_aux<7>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->stream); break;
+    case 2: e = ph::launch_aux<2>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->curv ? c->d_metric : nullptr, c->stream); break;
+    case 3: e = ph::launch_aux<3>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->curv ? c->d_metric : nullptr, c->stream); break;
+    case 4: e = ph::launch_aux<4>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->curv ? c->d_metric : nullptr, c->stream); break;
+    case 5: e = ph::launch_aux<5>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->curv ? c->d_metric : nullptr, c->stream); break;
+    case 6: e = ph::launch_aux<6>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->curv ? c->d_metric : nullptr, c->stream); break;
+    case 7: e = ph::launch_aux<7>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->curv ? c->d_metric : nullptr, c->stream); break;
     default: return fail(PH_ERR_UNSUPPORTED, "polynomial degree outside 1..6");
     }
     if (e != cudaSuccess) return fail(PH_ERR_CUDA, std::string("aux launch: ") + cudaGetErrorString(e));
@@ -2358,12 +2362,12 @@ extern "C" int ph_residual_noalloc(const ph_mesh_desc* mesh, const ph_params* pr
     cudaError_t e = cudaSuccess;
     if (visc) {
         switch (N1) {
-        case 2: e = ph::launch_aux<2>(U, sym.nbr, tab, 0, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
-        case 3: e = ph::launch_aux<3>(U, sym.nbr, tab, 0, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
-        case 4: e = ph::launch_aux<4>(U, sym.nbr, tab, 0, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
-        case 5: e = ph::launch_aux<5>(U, sym.nbr, tab, 0, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
-        case 6: e = ph::launch_aux<6>(U, sym.nbr, tab, 0, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
-        default: e = ph::launch_aux<7>(U, sym.nbr, tab, 0, (int)nc, 1.0 / h, pc, fp32, sym.fv, stream); break;
+        case 2: e = ph::launch_aux<2>(U, sym.nbr, tab, 0, (int)nc, 1.0 / h, pc, fp32, sym.fv, nullptr, stream); break;
+        case 3: e = ph::launch_aux<3>(U, sym.nbr, tab, 0, (int)nc, 1.0 / h, pc, fp32, sym.fv, nullptr, stream); break;
+        case 4: e = ph::launch_aux<4>(U, sym.nbr, tab, 0, (int)nc, 1.0 / h, pc, fp32, sym.fv, nullptr, stream); break;
+        case 5: e = ph::launch_aux<5>(U, sym.nbr, tab, 0, (int)nc, 1.0 / h, pc, fp32, sym.fv, nullptr, stream); break;
+        case 6: e = ph::launch_aux<6>(U, sym.nbr, tab, 0, (int)nc, 1.0 / h, pc, fp32, sym.fv, nullptr, stream); break;
+        default: e = ph::launch_aux<7>(U, sym.nbr, tab, 0, (int)nc, 1.0 / h, pc, fp32, sym.fv, nullptr, stream); break;
         }
         if (e != cudaSuccess) return fail(PH_ERR_CUDA, std::string("aux launch: ") + cudaGetErrorString(e));
     }

@@ -35,8 +35,9 @@ static cudaError_t launch_prec(const StageArgs& a, bool visc, bool split, cudaSt
     // relaxation RK's entropy estimate lives in the generic instance only
     const bool hot = split && a.pc.two_point == TP_CH && a.pc.conv_flux == CF_EC_ROE &&
                      (!visc || a.pc.diss_flux == DF_BR2) && a.ent_partial == nullptr;
-    if (a.metric) {   // curvilinear cells: split-form Euler (checked by the host)
-        if (visc || !split) return cudaErrorInvalidValue;
+    if (a.metric) {   // curvilinear cells: the split form (checked by the host)
+        if (!split) return cudaErrorInvalidValue;
+        if (visc) return hot ? launch_one<R, N1, true, true, 1, true>(a, s) : launch_one<R, N1, true, true, 0, true>(a, s);
         return hot ? launch_one<R, N1, false, true, 1, true>(a, s) : launch_one<R, N1, false, true, 0, true>(a, s);
     }
     if (visc) {
@@ -157,13 +158,13 @@ void stage_launch_shape(int fp32, bool visc, bool split, int* threads, int* cpc,
     }
 }
 
-template <typename R, int N1, bool FRA>
+template <typename R, int N1, bool FRA, bool CURV>
 static cudaError_t launch_aux_prec(const double* U, const int* nbr, const OpTab& ops, int cell_begin, int nc,
-                                   double inv_h, const PhysConst& pc, void* Fv, cudaStream_t s) {
+                                   double inv_h, const PhysConst& pc, void* Fv, const double* metric, cudaStream_t s) {
     constexpr int CPC = cells_per_cta<N1>();
     using L = AuxLayout<N1, CPC, FRA>;
     constexpr size_t bytes = L::template bytes<R>();
-    auto kern = aux_kernel<R, N1, CPC, FRA>;
+    auto kern = aux_kernel<R, N1, CPC, FRA, CURV>;
     int dev = 0;
     cudaGetDevice(&dev);
     static bool configured[64] = {false};
@@ -177,18 +178,24 @@ static cudaError_t launch_aux_prec(const double* U, const int* nbr, const OpTab&
     co.inv_wend = R(1) / (R)ops.w[0];
     const int grid = (nc - cell_begin + CPC - 1) / CPC;
     if (grid <= 0) return cudaErrorInvalidValue;
-    kern<<<grid, L::NT, bytes, s>>>(U, nbr, cell_begin, nc, (R)inv_h, pc, co, static_cast<R*>(Fv));
+    kern<<<grid, L::NT, bytes, s>>>(U, nbr, cell_begin, nc, CURV ? R(1) : (R)inv_h, pc, co, static_cast<R*>(Fv),
+                                    metric);
     return cudaGetLastError();
 }
 
 template <int N1>
 cudaError_t launch_aux(const double* U, const int* nbr, const OpTab& ops, int cell_begin, int nc, double inv_h,
-                       const PhysConst& pc, int fp32, void* Fv, cudaStream_t s) {
+                       const PhysConst& pc, int fp32, void* Fv, const double* metric, cudaStream_t s) {
+    if (metric) {   // curvilinear cells (kDG, checked by the host)
+        if (ops.aux_fr) return cudaErrorInvalidValue;
+        return fp32 ? launch_aux_prec<float, N1, false, true>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, metric, s)
+                    : launch_aux_prec<double, N1, false, true>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, metric, s);
+    }
     if (ops.aux_fr)
-        return fp32 ? launch_aux_prec<float, N1, true>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, s)
-                    : launch_aux_prec<double, N1, true>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, s);
-    return fp32 ? launch_aux_prec<float, N1, false>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, s)
-                : launch_aux_prec<double, N1, false>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, s);
+        return fp32 ? launch_aux_prec<float, N1, true, false>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, nullptr, s)
+                    : launch_aux_prec<double, N1, true, false>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, nullptr, s);
+    return fp32 ? launch_aux_prec<float, N1, false, false>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, nullptr, s)
+                : launch_aux_prec<double, N1, false, false>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, nullptr, s);
 }
 
 template <int N1>
@@ -257,7 +264,7 @@ template cudaError_t launch_stage_batched<PH_N1>(const StageArgs*, const BatchTi
                                                  cudaStream_t);
 template bool batched_shape<PH_N1>(int, bool, int, int*, int*, size_t*, int*);
 template cudaError_t launch_aux<PH_N1>(const double*, const int*, const OpTab&, int, int, double, const PhysConst&, int,
-                                       void*, cudaStream_t);
+                                       void*, const double*, cudaStream_t);
 template cudaError_t launch_inverse_mass<PH_N1>(const double*, double*, const OpTab*, int, double, const double*,
                                                 cudaStream_t);
 template cudaError_t launch_integrals<PH_N1>(const double*, const double*, const double*, const IntegralTab*, int,

@@ -126,8 +126,8 @@ template <int N1> __host__ __device__ constexpr int viscous_terms_per_cell() {
     return 4 * N1 * N1 * N1 + 24 * N1 * N1;
 }
 
-// CURV: curvilinear cells (split-form Euler): the per-node metric cofactor (9 values)
-// takes the place of the precomputed flux rows in sX.
+// CURV: curvilinear cells (split form, Euler or Navier-Stokes): the per-node metric cofactor
+// (9 values) in sX, after the viscous rows.
 template <typename R, int N1, int CPC, bool VISC, bool SPLIT, bool CURV = false>
 struct Layout {
     static constexpr int NP = N1 * N1 * N1, NF = N1 * N1;
@@ -135,6 +135,7 @@ struct Layout {
     static constexpr int NQS = 11;
     static constexpr int TR = VISC ? 9 : 5;            // trace values per face node: u (5) [+ ext viscous flux (4)]
     static constexpr int NX = (VISC ? 4 : 0) + (SPLIT ? 0 : 15) + (CURV ? 9 : 0);
+    static constexpr int OM = VISC ? 4 : 0;            // curvilinear: first metric row of X (after the viscous rows)
     static constexpr int oOps = 0;                      // D, Dsk, B, w as R
     static constexpr int nOps = 3 * N1 * N1 + N1;
     static constexpr int oU = (oOps + nOps + 1) & ~1;
@@ -266,7 +267,9 @@ __device__ __forceinline__ void face_item(const Cst<R>& cst, int tp, int cf, int
         // normal metric C[:, d] at this face node: the canonical normal (from the left cell
         // into the right one) is the same vector seen from either side; |C n| scales the flux
         const R* X = sX + c * L::NX * NP;
-        const R m[3] = {X[(0 * 3 + d) * NP + node], X[(1 * 3 + d) * NP + node], X[(2 * 3 + d) * NP + node]};
+        constexpr int OM = L::OM;
+        const R m[3] = {X[(OM + 0 * 3 + d) * NP + node], X[(OM + 1 * 3 + d) * NP + node],
+                        X[(OM + 2 * 3 + d) * NP + node]};
         const R J = rsqrt_<R>(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
         const R nrm[3] = {qdiv<R>(m[0], J), qdiv<R>(m[1], J), qdiv<R>(m[2], J)};
         NodeQ<R> qo, qe;
@@ -275,8 +278,21 @@ __device__ __forceinline__ void face_item(const Cst<R>& cst, int tp, int cf, int
         R F[5];
         if (plus) conv_num_flux_n<R>(uo, ue, qo, qe, nrm, tp, cf, cst, F);
         else conv_num_flux_n<R>(ue, uo, qe, qo, nrm, tp, cf, cst, F);
+        R term[5];
 #pragma unroll
-        for (int s = 0; s < 5; ++s) tr[s * NF + fn] = -sgn * J * F[s] * inv_wend;
+        for (int s = 0; s < 5; ++s) term[s] = -sgn * J * F[s];
+        if constexpr (VISC) {
+            // the metric-scaled normal viscous flux F~_d = sum_k C[k][d] F_k of both sides (the
+            // auxiliary kernels' face blocks; BR2 / central: their average, strong_dg.cpp:3354-3452)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const R Fo = __ldg(&fvface[(f * 4 + k) * NF + fn]);
+                const R Fn = R(0.5) * (Fo + tr[(5 + k) * NF + fn]);
+                term[1 + k] += sgn * (Fo - Fn);
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < 5; ++s) tr[s * NF + fn] = term[s] * inv_wend;
         return;
     }
     R ro[5], re[5];
@@ -357,7 +373,7 @@ __device__ __forceinline__ void volume_dir(int d, const Cst<R>& cst, int tp, con
         // curvilinear: the pair flux is dotted with the averaged metric column
         // 1/2 (C_i[:, d] + C_j[:, d]), symmetric in (i, j) like the flux itself
         const R* Dq = sD + lc * NQS * NP;
-        const R* X = sX + lc * L::NX * NP;
+        const R* X = sX + (lc * L::NX + L::OM) * NP;   // the metric rows
         NodeQ<R> qi;
         load_q<R>(Dq, NP, node, qi);
         const R mi[3] = {X[(0 * 3 + d) * NP + node], X[(1 * 3 + d) * NP + node], X[(2 * 3 + d) * NP + node]};
@@ -589,7 +605,7 @@ __device__ __forceinline__ void prefetch_tile_l2(const StageArgs& a, int cell0) 
 // runs the tiles of many independent discretisations (a batch of solves) from a tile list.
 template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int FS, bool CURV, bool BULK = false>
 __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell0) {
-    static_assert(!CURV || (SPLIT && !VISC), "curvilinear cells: split-form Euler only");
+    static_assert(!CURV || SPLIT, "curvilinear cells: split form only");
     static_assert(!BULK || (std::is_same<R, double>::value && N1 % 2 == 0 && !CURV), "bulk staging: FP64, even N1");
     using L = Layout<R, N1, CPC, VISC, SPLIT, CURV>;
     constexpr int NP = L::NP, NF = L::NF, NT = L::NT, TR = L::TR, NQS = L::NQS;
@@ -716,7 +732,7 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
         }
         if constexpr (CURV) {
 #pragma unroll
-            for (int i = 0; i < 9; ++i) X[i * NP + node] = (R)__ldg(&a.metric[((size_t)cell * 10 + i) * NP + node]);
+            for (int i = 0; i < 9; ++i) X[(L::OM + i) * NP + node] = (R)__ldg(&a.metric[((size_t)cell * 10 + i) * NP + node]);
         }
         if constexpr (!SPLIT) {
             constexpr int o = VISC ? 4 : 0;
@@ -1047,10 +1063,43 @@ template <int N1> __device__ __forceinline__ int line_node(int d, int line, int 
     return d == 0 ? node_of<N1>(pos, a, b) : d == 1 ? node_of<N1>(a, pos, b) : node_of<N1>(a, b, pos);
 }
 
-template <typename R, int N1, int CPC, bool FRA>
+// Curvilinear cells (CURV, metric rows [cell][10][NP]: C[k][d] at row k * 3 + d, 1 / det J at
+// row 9): the reference gradient r_j = D_j u + lift_j (inv_h = 1) becomes the physical one
+// q_d = (1/J) sum_j C[d][j] r_j (the curvilinear volume and face terms of the auxiliary
+// equation, strong_dg.cpp:666-1008, with the cDG weight-adjusted inverse mass 1 / (W J) at
+// GLL nodes), and the nodal viscous flux its contravariant form F~_j = sum_m C[m][j] F_m, whose
+// reference divergence and face values (F~_dn at face nodes, the metric-scaled normal flux) the
+// stage kernel takes in place of the affine ones.
+template <typename R, int N1>
+__device__ __forceinline__ void aux_curv_flux(const R un[5], const R r[5][3], const double* __restrict__ metric,
+                                              int cell, int node, int ucv, const Cst<R>& cst, R Ft[3][4]) {
+    constexpr int NP = N1 * N1 * N1;
+    const double* M = metric + (size_t)cell * 10 * NP + node;
+    double C[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) C[i] = __ldg(&M[i * NP]);
+    const double iJ = __ldg(&M[9 * NP]);
+    R g[5][3];   // the metric products in FP64 (the metric stays FP64 in the precision form)
+#pragma unroll
+    for (int s = 0; s < 5; ++s)
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            g[s][d] = (R)(iJ * (C[d * 3 + 0] * (double)r[s][0] + C[d * 3 + 1] * (double)r[s][1] +
+                                C[d * 3 + 2] * (double)r[s][2]));
+    R F[3][4];
+    viscous_flux<R>(un, g, ucv, cst, F, 7, nullptr);
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            Ft[j][k] = (R)(C[0 * 3 + j] * (double)F[0][k] + C[1 * 3 + j] * (double)F[1][k] +
+                           C[2 * 3 + j] * (double)F[2][k]);
+}
+
+template <typename R, int N1, int CPC, bool FRA, bool CURV>
 __global__ void __launch_bounds__(AuxLayout<N1, CPC, FRA>::NT)
 aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, int cell_begin, int nc, R inv_h, PhysConst pc,
-           AuxCoef<R> co, R* __restrict__ Fv) {
+           AuxCoef<R> co, R* __restrict__ Fv, const double* __restrict__ metric) {
     using L = AuxLayout<N1, CPC, FRA>;
     constexpr int NP = L::NP, NF = L::NF, NT = L::NT;
     constexpr int VT = viscous_terms_per_cell<N1>();
@@ -1147,7 +1196,12 @@ aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, int cell_b
 #pragma unroll
             for (int s = 0; s < 5; ++s) un[s] = sU[(c * 5 + s) * NP + node];
             R F[3][4];
-            viscous_flux<R>(un, g, pc.use_const_visc, cst, F, 7, nullptr);
+            if constexpr (CURV) {
+                int cell = cell0 + c; if (cell >= nc) cell = nc - 1;
+                aux_curv_flux<R, N1>(un, g, metric, cell, node, pc.use_const_visc, cst, F);
+            } else {
+                viscous_flux<R>(un, g, pc.use_const_visc, cst, F, 7, nullptr);
+            }
 #pragma unroll
             for (int d = 0; d < 3; ++d)
 #pragma unroll
@@ -1235,7 +1289,8 @@ aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, int cell_b
 #pragma unroll
             for (int s = 0; s < 5; ++s) un[s] = u[s * NP + node];
             R F[3][4];
-            viscous_flux<R>(un, g, pc.use_const_visc, cst, F, 7, nullptr);
+            if constexpr (CURV) aux_curv_flux<R, N1>(un, g, metric, cell, node, pc.use_const_visc, cst, F);
+            else viscous_flux<R>(un, g, pc.use_const_visc, cst, F, 7, nullptr);
 #pragma unroll
             for (int d = 0; d < 3; ++d)
 #pragma unroll

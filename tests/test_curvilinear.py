@@ -52,6 +52,24 @@ def test_oracle_vanishing_warp_matches_affine_path(p):
     assert np.allclose(q1, q0, rtol=1e-13, atol=0)
 
 
+@pytest.mark.parametrize("p,diss", [(2, "bassi_rebay_2"), (3, "central_visc_flux")])
+def test_oracle_vanishing_warp_matches_affine_path_navier_stokes(p, diss):
+    """The curvilinear auxiliary equation (C grad u / J, lifts by (C n)_d) and viscous terms
+    (contravariant fluxes, |C n| on faces) of the oracle reduce to the affine ones."""
+    kw = dict(poly_degree=p, n_cells=3, pde="navier_stokes", diss=diss)
+    _, affine = _oracle(kw, 0.0)
+    _, curved = _oracle(kw, 1e-300)
+    U = perturbed_tgv(affine, seed=p)
+    assert rel_max_err(curved.residual(U), affine.residual(U)) <= 1e-13
+
+
+def test_oracle_warped_mesh_preserves_free_stream_navier_stokes():
+    _, orc = _oracle(dict(poly_degree=3, n_cells=3, pde="navier_stokes", diss="bassi_rebay_2"), WARP)
+    R = orc.residual(_uniform_state(orc))
+    scale = np.max(np.abs(orc.residual(orc.initial_condition("tgv"))))
+    assert np.max(np.abs(R)) <= 1e-12 * scale
+
+
 @pytest.mark.parametrize("p,two_point,conv", [(2, "CH", "two_point_flux_with_roe_dissipation"),
                                               (3, "IR", "two_point_flux"),
                                               (4, "KG", "two_point_flux_with_lax_friedrichs_dissipation")])
@@ -174,3 +192,53 @@ def test_reference_style_curved_periodic_grid_preserves_free_stream():
     R = dg.residual_of(U)
     print(f"reference-style curved grid, uniform flow: max |R| {np.max(np.abs(R)):.3e}")
     assert np.max(np.abs(R)) <= 1e-11
+
+
+# ------------------------------------------------------------------------------- Navier-Stokes
+
+NS_CASES = [
+    ("ns_CH_roe_br2_p3_morton", dict(poly_degree=3, n_cells=4, pde="navier_stokes", diss="bassi_rebay_2")),
+    ("ns_CH_roe_br2_p5", dict(poly_degree=5, n_cells=2, pde="navier_stokes", diss="bassi_rebay_2")),
+    ("ns_IR_ec_central_p2", dict(poly_degree=2, n_cells=3, pde="navier_stokes", diss="central_visc_flux",
+                                 two_point="IR", conv="two_point_flux")),
+    ("ns_KG_lxf_br2_p4", dict(poly_degree=4, n_cells=2, pde="navier_stokes", diss="bassi_rebay_2", two_point="KG",
+                              conv="two_point_flux_with_lax_friedrichs_dissipation")),
+    ("ns_Ra_roe_br2_p1", dict(poly_degree=1, n_cells=4, pde="navier_stokes", diss="bassi_rebay_2", two_point="Ra")),
+    ("ns_CH_roe_central_p6", dict(poly_degree=6, n_cells=1, pde="navier_stokes", diss="central_visc_flux")),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,kw", NS_CASES, ids=[c[0] for c in NS_CASES])
+def test_curvilinear_navier_stokes_residual_parity(name, kw):
+    prm, orc, dg = _pair(kw)
+    U = perturbed_tgv(orc, seed=len(name))
+    err = rel_max_err(dg.residual_of(U), orc.residual(U))
+    print(f"{name}: curvilinear Navier-Stokes residual rel max err {err:.3e}")
+    assert err <= RTOL
+
+
+@pytest.mark.gpu
+def test_curvilinear_navier_stokes_free_stream_steps_and_precision_form():
+    from philip_b200 import _lib
+    from philip_b200.dg import RungeKuttaODESolver
+    kw = dict(poly_degree=3, n_cells=4, pde="navier_stokes", diss="bassi_rebay_2")
+    prm, orc, dg = _pair(kw)
+    R = dg.residual_of(_uniform_state(orc))
+    print(f"curvilinear Navier-Stokes, uniform flow: max |R| {np.max(np.abs(R)):.3e}")
+    assert np.max(np.abs(R)) <= 1e-10
+    U = orc.initial_condition("tgv")
+    dg.solution = U
+    dt = 0.1 * TWO_PI / 16 / 11.0
+    ode = RungeKuttaODESolver(dg)
+    for step in range(3):
+        orc.rk_step(U, dt)
+        ode.step_in_time(dt)
+        err = rel_max_err(dg.solution, U)
+        print(f"warped Navier-Stokes RK4 step {step}: rel err {err:.3e}")
+        assert err <= 1e-12 and dg.status() == 0
+    _, orc32, dg32 = _pair(kw, precision=_lib.PH_FP32_RESIDUAL)
+    V = perturbed_tgv(orc32, seed=3)
+    err = rel_max_err(dg32.residual_of(V), orc32.residual(V))
+    print(f"curvilinear Navier-Stokes fp32 residual rel err {err:.3e}")
+    assert err <= 1e-5

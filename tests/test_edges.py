@@ -71,9 +71,14 @@ def test_configurations_outside_the_path_are_refused(name, edit, code, text):
     assert rc == code and text in msg
 
 
-def test_curvilinear_navier_stokes_is_refused():
+def test_curvilinear_navier_stokes_with_sipg_is_refused():
+    """Curvilinear Navier-Stokes takes BR2 or the central viscous flux: the SIPG penalty uses the
+    cell's extent along the face normal (dg_base.cpp:397-413), not restated on curved cells."""
     rc, msg = _create(prm_kw=dict(pde="navier_stokes"), mesh_kw=dict(warp=0.1))
-    assert rc == _lib.PH_ERR_UNSUPPORTED and "Euler" in msg
+    assert rc == _lib.PH_ERR_UNSUPPORTED and "bassi_rebay_2" in msg
+    rc, msg = _create(prm_kw=dict(pde="navier_stokes", diss="bassi_rebay_2"), mesh_kw=dict(warp=0.1),
+                      edit=lambda p: setattr(p, "flux_reconstruction_aux", 2))
+    assert rc == _lib.PH_ERR_UNSUPPORTED and "kDG" in msg
 
 
 def test_curvilinear_gl_flux_nodes_are_refused():

@@ -99,9 +99,10 @@ CASES = [
     ("ns_const_visc_p3", dict(poly_degree=3, n_cells=4, pde="navier_stokes"), True, 0.0),
     ("ns_sutherland_p5", dict(poly_degree=5, n_cells=2, pde="navier_stokes"), False, 0.0),
     ("ns_sutherland_p6", dict(poly_degree=6, n_cells=2, pde="navier_stokes"), False, 0.0),
-    # curvilinear contexts take the Euler equations; the integrands are the Navier-Stokes
-    # physics' whatever the PDE, so the viscous quantities are still computed
+    # the integrands are the Navier-Stokes physics' whatever the PDE, so the viscous quantities
+    # are computed on the Euler context too
     ("curved_p3", dict(poly_degree=3, n_cells=3), False, 0.1),
+    ("curved_ns_br2_p4", dict(poly_degree=4, n_cells=2, pde="navier_stokes", diss="bassi_rebay_2"), False, 0.1),
     ("curved_p6", dict(poly_degree=6, n_cells=2), True, 0.1),
 ]
 
