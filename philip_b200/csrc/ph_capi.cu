@@ -263,6 +263,128 @@ bool curvilinear_cell(const std::vector<double>& x, const std::vector<double>& D
 }
 
 
+// Tensor-product evaluation on the host: out[z][y][x] = sum A_z[z][k] A_y[y][j] A_x[x][i] in[k][j][i]
+// (x first), A_e of r_e rows and n columns; in is n^3 values.
+static void host_apply3(const double* Ax, int rx, const double* Ay, int ry, const double* Az, int rz, int n,
+                        const double* in, double* out) {
+    std::vector<double> t1((size_t)rx * n * n), t2((size_t)rx * ry * n);
+    for (int k = 0; k < n; ++k)
+        for (int j = 0; j < n; ++j)
+            for (int x = 0; x < rx; ++x) {
+                double v = 0.0;
+                for (int i = 0; i < n; ++i) v += Ax[x * n + i] * in[(k * n + j) * n + i];
+                t1[(k * n + j) * rx + x] = v;
+            }
+    for (int k = 0; k < n; ++k)
+        for (int y = 0; y < ry; ++y)
+            for (int x = 0; x < rx; ++x) {
+                double v = 0.0;
+                for (int j = 0; j < n; ++j) v += Ay[y * n + j] * t1[(k * n + j) * rx + x];
+                t2[(k * ry + y) * rx + x] = v;
+            }
+    for (int z = 0; z < rz; ++z)
+        for (int y = 0; y < ry; ++y)
+            for (int x = 0; x < rx; ++x) {
+                double v = 0.0;
+                for (int k = 0; k < n; ++k) v += Az[z * n + k] * t2[(k * ry + y) * rx + x];
+                out[(z * ry + y) * rx + x] = v;
+            }
+}
+
+// Metric terms of one curvilinear cell at uncollocated flux nodes: the mapping of degree p on
+// the GLL support points (the solution's, grid_degree = poly_degree) with coordinates X
+// [3][nd^3]; the cofactor by the conservative curl form (operators.cpp:2738-2884) evaluated at
+// the nq^3 volume flux nodes and at each face's nq^2 flux nodes (operators.cpp:2444-2589), det J
+// at the volume flux nodes (operators.cpp:2591-2672). Out: vmet [10][nq^3] (C[k][d] at row
+// k * 3 + d, 1 / det J at row 9) and fnrm [6][3][nq^2] (face f's metric column C[:, f / 2]);
+// returns false on a non-positive det J.
+bool gl_curvilinear_cell(const std::vector<double>& xs, const std::vector<double>& xq, const double* X,
+                         double* vmet, double* fnrm) {
+    const int nd = (int)xs.size(), nq = (int)xq.size(), nd3 = nd * nd * nd, nq3 = nq * nq * nq, nf = nq * nq;
+    std::vector<double> Bg((size_t)nd * nd), dBg((size_t)nd * nd), Bf((size_t)nq * nd), dBf((size_t)nq * nd);
+    std::vector<double> Bs[2], dBs[2];
+    for (int a = 0; a < nd; ++a) lagrange(xs, xs[a], &Bg[a * nd], &dBg[a * nd]);
+    for (int q = 0; q < nq; ++q) lagrange(xs, xq[q], &Bf[q * nd], &dBf[q * nd]);
+    for (int side = 0; side < 2; ++side) {
+        Bs[side].assign(nd, 0.0); dBs[side].assign(nd, 0.0);
+        lagrange(xs, (double)side, Bs[side].data(), dBs[side].data());
+    }
+    // the Jacobian at the support points and the nine products X_a dX_b/dxi_j there:
+    // P[0..2] = z dy/dxi_j, P[3..5] = x dz/dxi_j, P[6..8] = y dx/dxi_j
+    std::vector<double> GX[3][3], P[9];
+    for (int m = 0; m < 3; ++m)
+        for (int j = 0; j < 3; ++j) {
+            GX[m][j].resize(nd3);
+            const double* B[3] = {Bg.data(), Bg.data(), Bg.data()};
+            B[j] = dBg.data();
+            host_apply3(B[0], nd, B[1], nd, B[2], nd, nd, X + (size_t)m * nd3, GX[m][j].data());
+        }
+    for (int j = 0; j < 3; ++j) {
+        P[j].resize(nd3); P[3 + j].resize(nd3); P[6 + j].resize(nd3);
+        for (int g = 0; g < nd3; ++g) {
+            P[j][g] = X[2 * nd3 + g] * GX[1][j][g];
+            P[3 + j][g] = X[0 * nd3 + g] * GX[2][j][g];
+            P[6 + j][g] = X[1 * nd3 + g] * GX[0][j][g];
+        }
+    }
+    // the cofactor at the points selected by A (derivatives dA): row l from the products of row l,
+    // C[l][0] = D_zeta(f_eta) - D_eta(f_zeta), C[l][1] = D_xi(f_zeta) - D_zeta(f_xi),
+    // C[l][2] = D_eta(f_xi) - D_xi(f_eta)
+    auto cofactor = [&](const double* const A[3], const double* const dA[3], const int r[3], double* C, int cs) {
+        const int npts = r[0] * r[1] * r[2];
+        std::vector<double> t1(npts), t2(npts);
+        auto D = [&](int e, const std::vector<double>& f, std::vector<double>& out) {
+            const double* B[3] = {A[0], A[1], A[2]};
+            B[e] = dA[e];
+            host_apply3(B[0], r[0], B[1], r[1], B[2], r[2], nd, f.data(), out.data());
+        };
+        for (int l = 0; l < 3; ++l) {
+            const std::vector<double>* f = &P[3 * l];
+            D(2, f[1], t1); D(1, f[2], t2);
+            for (int q = 0; q < npts; ++q) C[(l * 3 + 0) * cs + q] = t1[q] - t2[q];
+            D(0, f[2], t1); D(2, f[0], t2);
+            for (int q = 0; q < npts; ++q) C[(l * 3 + 1) * cs + q] = t1[q] - t2[q];
+            D(1, f[0], t1); D(0, f[1], t2);
+            for (int q = 0; q < npts; ++q) C[(l * 3 + 2) * cs + q] = t1[q] - t2[q];
+        }
+    };
+    {
+        const double* A[3] = {Bf.data(), Bf.data(), Bf.data()};
+        const double* dA[3] = {dBf.data(), dBf.data(), dBf.data()};
+        const int r[3] = {nq, nq, nq};
+        cofactor(A, dA, r, vmet, nq3);
+        std::vector<double> Jm[3][3];
+        for (int m = 0; m < 3; ++m)
+            for (int j = 0; j < 3; ++j) {
+                Jm[m][j].resize(nq3);
+                const double* B[3] = {Bf.data(), Bf.data(), Bf.data()};
+                B[j] = dBf.data();
+                host_apply3(B[0], nq, B[1], nq, B[2], nq, nd, X + (size_t)m * nd3, Jm[m][j].data());
+            }
+        for (int q = 0; q < nq3; ++q) {
+            double J[3][3];
+            for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) J[a][b] = Jm[a][b][q];
+            const double dj = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) -
+                              J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+                              J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+            if (!(dj > 1e-14)) return false;
+            vmet[9 * nq3 + q] = 1.0 / dj;
+        }
+    }
+    std::vector<double> Cf((size_t)9 * nf);
+    for (int f = 0; f < 6; ++f) {
+        const int dn = f / 2, side = f % 2;
+        const double* A[3] = {Bf.data(), Bf.data(), Bf.data()};
+        const double* dA[3] = {dBf.data(), dBf.data(), dBf.data()};
+        int r[3] = {nq, nq, nq};
+        A[dn] = Bs[side].data(); dA[dn] = dBs[side].data(); r[dn] = 1;
+        cofactor(A, dA, r, Cf.data(), nf);
+        for (int k = 0; k < 3; ++k)
+            for (int q = 0; q < nf; ++q) fnrm[((size_t)f * 3 + k) * nf + q] = Cf[(k * 3 + dn) * nf + q];
+    }
+    return true;
+}
+
 int check_mesh(const ph_mesh_desc* mesh) {
     const int n = mesh->n_cells_per_direction;
     if (n < 1 || !(mesh->right > mesh->left)) return fail(PH_ERR_INVALID, "bad mesh");
@@ -290,7 +412,11 @@ const char* uncollocated_reason(const ph_mesh_desc* mesh, const ph_params* prm) 
     if (prm->overintegration < 0 || prm->overintegration > 2) return "overintegration must be 0, 1 or 2";
     if (prm->poly_degree < 1 || prm->poly_degree + 1 + prm->overintegration > ph::GL_MAXQ)
         return "uncollocated flux nodes: poly_degree >= 1 and poly_degree + 1 + overintegration <= 7";
-    if (is_curvilinear(mesh)) return "uncollocated flux nodes take affine meshes";
+    if (is_curvilinear(mesh)) {
+        if (mesh->mapping_support_points == nullptr && mesh->grid_degree != prm->poly_degree)
+            return "curvilinear meshes take grid_degree = poly_degree";
+        if (prm->pde_type != 0) return "uncollocated flux nodes on curvilinear meshes take the Euler equations";
+    }
     if (prm->precision != PH_FP64) return "uncollocated flux nodes take the FP64 path";
     if (prm->runge_kutta_method > 3) return "uncollocated flux nodes take the Butcher RK methods";
     if (prm->use_relaxation_runge_kutta) return "uncollocated flux nodes: no relaxation RK";
@@ -461,6 +587,13 @@ int build_gl_operators(const ph_params* prm, ph::GlTab& t, ph::OpTab& ops) {
         }
     for (int a = 0; a < nd; ++a)
         for (int l = 0; l < nd; ++l) ops.Minv[a * ph::MAXN1 + l] = MKi[a * nd + l];
+    // the projection of the weight-adjusted inverse mass on curvilinear cells, (M+K)^-1 chi^T W
+    for (int i = 0; i < nd; ++i)
+        for (int q = 0; q < nq; ++q) {
+            double v = 0.0;
+            for (int j = 0; j < nd; ++j) v += MKi[i * nd + j] * chi[q * nd + j];
+            t.pwa[i * nq + q] = v * wq[q];
+        }
     return PH_OK;
 }
 
@@ -826,6 +959,8 @@ struct ph_ctx {
     double* d_t1 = nullptr;
     double* d_t2 = nullptr;
     double* d_vis = nullptr;
+    double* d_glvm = nullptr;           // curvilinear uncollocated: [nc][10][nq^3] cofactor + 1 / det J
+    double* d_glfn = nullptr;           // curvilinear uncollocated: [nc][6][3][nq^2] face metric columns
     // optional per-kernel timing: 1 = CUDA events around every direct launch, the stream
     // synchronised after each; 2 = event-record nodes between the kernels of the captured
     // RK step, a fresh set of events for every replay (the replays themselves are timed)
@@ -965,11 +1100,13 @@ int dispatch_aux(ph_ctx* c, const double* U, int cell_begin, int cell_end) {
 }
 
 // One kernel of the uncollocated path on the stage input a.U: 0 face values, 1 auxiliary
-// equation, 2 residual / RK stage (timing classes: other, auxiliary, stage).
+// equation, 2 residual / RK stage, 3 the curvilinear weight-adjusted inverse mass (timing classes:
+// other, auxiliary, stage, other).
 int dispatch_gl(ph_ctx* c, int kernel, const ph::StageArgs& a) {
-    static const char* const kName[] = {"face-value kernel", "auxiliary kernel", "stage kernel"};
+    static const char* const kName[] = {"face-value kernel", "auxiliary kernel", "stage kernel",
+                                        "inverse-mass kernel"};
     NvtxRange nvtx(kName[kernel]);
-    const ph::GlArgs g{c->d_gl, c->d_t1, c->d_t2, c->d_vis};
+    const ph::GlArgs g{c->d_gl, c->d_t1, c->d_t2, c->d_vis, c->d_glvm, c->d_glfn};
     cudaError_t e;
     timer_begin(c);
     switch (c->N1) {
@@ -982,7 +1119,7 @@ int dispatch_gl(ph_ctx* c, int kernel, const ph::StageArgs& a) {
     default: return fail(PH_ERR_UNSUPPORTED, "polynomial degree outside 1..6");
     }
     if (e != cudaSuccess) return fail(PH_ERR_CUDA, std::string(kName[kernel]) + " launch: " + cudaGetErrorString(e));
-    timer_end(c, kernel == 2 ? 0 : kernel == 1 ? 1 : 2);
+    timer_end(c, kernel == 2 ? 0 : kernel == 1 ? 1 : 2);   // (the inverse mass alone: other)
     return PH_OK;
 }
 
@@ -1314,6 +1451,11 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
             bad |= dalloc(&c->d_t2, faces * ph::GL_T2W);
             bad |= dalloc(&c->d_vis, (size_t)c->nc * 4 * c->NP);
         }
+        if (c->curv) {
+            const size_t q3 = (size_t)c->NQ * c->NQ * c->NQ;
+            bad |= dalloc(&c->d_glvm, (size_t)c->nc * 10 * q3);
+            bad |= dalloc(&c->d_glfn, (size_t)c->nc * 6 * 3 * c->NQ * c->NQ);
+        }
     }
     if (c->curv) bad |= dalloc(&c->d_metric, metric.size());
     if (c->curv) bad |= dalloc(&c->d_xnode, (size_t)3 * c->nc * c->NP);
@@ -1324,6 +1466,29 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
     if (e == cudaSuccess) e = cudaMemcpy(c->d_ops, &c->h_ops, sizeof(ph::OpTab), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(c->d_itab, &itab, sizeof(ph::IntegralTab), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && c->d_gl) e = cudaMemcpy(c->d_gl, &c->h_gl, sizeof(ph::GlTab), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && c->d_glvm) {   // metric terms at the uncollocated flux nodes, cell by cell
+        const int nq = c->NQ, nq3 = nq * nq * nq, nf = nq * nq, NP = c->NP;
+        std::vector<double> xq, wq;
+        if (prm->flux_nodes_type == 1) gll(nq, xq, wq); else gauss(nq, xq, wq);
+        std::vector<double> vm((size_t)c->nc * 10 * nq3), fnm((size_t)c->nc * 18 * nf);
+        std::atomic<int> ok{1};
+        const unsigned nthr = std::max(1u, std::min(32u, std::min(std::thread::hardware_concurrency(), (unsigned)c->nc)));
+        std::vector<std::thread> pool;
+        for (unsigned tI = 0; tI < nthr; ++tI)
+            pool.emplace_back([&, tI]() {
+                std::vector<double> X((size_t)3 * NP);
+                for (int cc = (int)tI; cc < c->nc; cc += (int)nthr) {
+                    for (int node = 0; node < NP; ++node)
+                        for (int d = 0; d < 3; ++d) X[(size_t)d * NP + node] = c->xyz[((size_t)cc * NP + node) * 3 + d];
+                    if (!gl_curvilinear_cell(x, xq, X.data(), &vm[(size_t)cc * 10 * nq3], &fnm[(size_t)cc * 18 * nf]))
+                        ok = 0;
+                }
+            });
+        for (auto& th : pool) th.join();
+        if (!ok) { ph_ctx_destroy(c); return fail(PH_ERR_INVALID, "non-positive det J at a flux node: the warp folds a cell"); }
+        e = cudaMemcpy(c->d_glvm, vm.data(), vm.size() * sizeof(double), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(c->d_glfn, fnm.data(), fnm.size() * sizeof(double), cudaMemcpyHostToDevice);
+    }
     if (e == cudaSuccess && c->d_ltab) {   // the FE_DGQ basis at the Gauss and Gauss-Lobatto points of p + 1
         ph::LimiterTab lt;
         std::memset(&lt, 0, sizeof(lt));
@@ -1435,7 +1600,7 @@ int ph_ctx_destroy(ph_ctx* c) {
     void* ptrs[] = {c->d_nbr, c->d_ops, c->d_itab, c->d_sol, c->d_stA, c->d_stB, c->d_acc, c->d_carry,
                     c->d_fv, c->d_comp, c->d_tmpA, c->d_tmpB, c->d_partial, c->d_status, c->d_metric, c->d_xnode, c->d_origin, c->d_err,
                     c->d_table, c->d_counter, c->d_ent, c->d_ent_cell, c->d_halo, c->d_gl, c->d_t1, c->d_t2,
-                    c->d_vis, c->d_ltab};
+                    c->d_vis, c->d_ltab, c->d_glvm, c->d_glfn};
     if (c->side) cudaStreamSynchronize(c->side);
     for (void* p : ptrs) if (p) cudaFree(p);
     if (c->side) cudaStreamDestroy(c->side);
@@ -1525,6 +1690,18 @@ int ph_apply_inverse_mass(ph_ctx* c, const double* R, double* out, int where) {
         if (int rc = ensure_tmp(c)) return rc;
         PH_CUDA(cudaMemcpyAsync(c->d_tmpA, R, c->ndofs * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         dR = c->d_tmpA; dO = c->d_tmpB;
+    }
+    if (c->gl && c->curv) {   // the weight-adjusted inverse mass at the uncollocated flux nodes
+        ph::StageArgs a = base_args(c, dR);
+        a.out = dO;
+        a.cell_begin = 0;
+        a.nc = c->nc;
+        if (int rc = dispatch_gl(c, 3, a)) return rc;
+        if (where == PH_HOST) {
+            PH_CUDA(cudaMemcpyAsync(out, dO, c->ndofs * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+            PH_CUDA(cudaStreamSynchronize(c->stream));
+        }
+        return PH_OK;
     }
     const double inv_detj = 1.0 / (c->h * c->h * c->h);
     cudaError_t e;

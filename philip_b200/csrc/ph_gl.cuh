@@ -52,6 +52,7 @@ struct GlTab {
     double minv[GL_MAXD * GL_MAXD];   // (M + K)^-1
     double minv_aux[GL_MAXD * GL_MAXD];
     double haux[GL_MAXQ * GL_MAXQ];   // chi (M + K_aux)^-1 chi^T
+    double pwa[GL_MAXD * GL_MAXQ];    // (M + K)^-1 chi^T W (nd x nq): the weight-adjusted inverse mass's projection
 };
 
 // Device buffers of the uncollocated path (per cell, reference units).
@@ -61,6 +62,11 @@ struct GlArgs {
     double* t2;    // [nc][6][8][nq^2]: the cell's F_v(u, q) . e_dn at its face nodes (4) and its face-normal
                    // volume viscous flux interpolated to them, signed by the side (4)
     double* vis;   // [nc][4][nd^3]: -chi^T W div(F_v), momentum and energy rows
+    // curvilinear cells (nullptr on affine ones): at the volume flux nodes [nc][10][nq^3] the
+    // cofactor C[k][d] (row k * 3 + d) and 1 / det J (row 9); at each face's flux nodes
+    // [nc][6][3][nq^2] the face's metric column C[:, f / 2]
+    const double* vmet;
+    const double* fnrm;
 };
 
 template <bool SPLIT> __host__ __device__ constexpr int gl_t1_width() { return SPLIT ? 10 : 5; }
@@ -578,7 +584,7 @@ gl_aux_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab T
 // ------------------------------------------------------------------------------------
 // Residual (+ mass inverse + RK epilogue)
 // ------------------------------------------------------------------------------------
-template <int ND, int NQ, bool VISC, bool SPLIT>
+template <int ND, int NQ, bool VISC, bool SPLIT, bool CURV = false>
 struct GlStageLayout {
     static constexpr int NT = gl_threads<NQ>();
     static constexpr int D3 = ND * ND * ND, Q3 = NQ * NQ * NQ, NF = NQ * NQ;
@@ -591,15 +597,23 @@ struct GlStageLayout {
     static constexpr int nT = gl_temp<ND, NQ>();
     static constexpr int oT0 = oF + 30 * NF, oT1 = oT0 + nT;
     static constexpr int oQF = oT1 + nT;                 // split: the node quantities of two faces' nodes
-    static constexpr int total = oQF + (SPLIT ? 2 * NF * 11 : 0);
+    static constexpr int oM = oQF + (SPLIT ? 2 * NF * 11 : 0);   // curvilinear: 9 NQ^3 metric cofactor
+    static constexpr int total = oM + (CURV ? 9 * Q3 : 0);
     static constexpr size_t bytes = (size_t)total * sizeof(double);
     static_assert(2 * nT >= 2 * NF * NQ * 5, "the hybrid pair fluxes of one direction fit the temporaries");
 };
 
-template <int ND, int NQ, bool VISC, bool SPLIT>
+// CURV (split or conservative Euler on curvilinear cells): the volume two-point fluxes are dotted
+// with the metric average 1/2 (C_i[:, d] + C_j[:, d]) and the conservative fluxes with C[:, d]
+// (strong_dg.cpp:1235-1578), the face fluxes use the face's unit normal C[:, dn] / |C[:, dn]|
+// scaled by |C[:, dn]| and the hybrid terms 1/2 (C_face[:, dn] + C_vol[:, dn]) (:3144-3452), and
+// the inverse mass is the weight-adjusted P diag(1 / (W det J)) P^T, P = (M+K)^-1 chi^T W
+// (dg_base.cpp:4217-4249, operators.cpp:1909-1932). The residual is then in physical units.
+template <int ND, int NQ, bool VISC, bool SPLIT, bool CURV = false>
 __global__ void __launch_bounds__(gl_threads<NQ>(), 2)
 gl_stage_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab T) {
-    using L = GlStageLayout<ND, NQ, VISC, SPLIT>;
+    static_assert(!CURV || !VISC, "curvilinear uncollocated cells: the Euler equations");
+    using L = GlStageLayout<ND, NQ, VISC, SPLIT, CURV>;
     constexpr int NT = L::NT, D3 = L::D3, Q3 = L::Q3, NF = L::NF, T1W = gl_t1_width<SPLIT>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* sm = reinterpret_cast<double*>(smem_raw);
@@ -614,8 +628,11 @@ gl_stage_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab
     const int cell = a.cell_begin + blockIdx.x;
     Cst<double> cst; cst.load(a.pc);
     const int tp = a.pc.two_point, cf = a.pc.conv_flux, df = a.pc.diss_flux, ucv = a.pc.use_const_visc;
+    double* sM = sm + L::oM;   // curvilinear: the cofactor at the flux nodes, [k * 3 + d][Q3]
     gl_load_tab(g.tab, tab, NT);
     for (int i = threadIdx.x; i < 5 * D3; i += NT) sU[i] = __ldg(&a.U[(size_t)cell * 5 * D3 + i]);
+    if constexpr (CURV)
+        for (int i = threadIdx.x; i < 9 * Q3; i += NT) sM[i] = __ldg(&g.vmet[(size_t)cell * 10 * Q3 + i]);
     __syncthreads();
     gl_apply3<NT, NQ, ND, 5>(T.chi, sU, D3, sQ, Q3, t0, t1, 1.0, false);
     if constexpr (SPLIT) {
@@ -660,31 +677,63 @@ gl_stage_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab
                 const bool valid = lseg < SPW && lt < NF;
                 const int node = gl_line_node<NQ>(rd, valid ? lt : 0, pos);
                 const int base = node - pos * st;
-                NodeQ<double> qi;
-                load_q_rot<double>(sN, Q3, node, rd, qi);
-                double accr[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+                double acc[5];
+                if constexpr (CURV) {   // the pair flux dotted with the averaged metric column
+                    NodeQ<double> qi;
+                    load_q<double>(sN, Q3, node, qi);
+                    const double mi[3] = {sM[(0 * 3 + rd) * Q3 + node], sM[(1 * 3 + rd) * Q3 + node],
+                                          sM[(2 * 3 + rd) * Q3 + node]};
 #pragma unroll
-                for (int k = 1; k <= NQ / 2; ++k) {
-                    const int jp = pos + k < NQ ? pos + k : pos + k - NQ;   // (pos + k) mod NQ
-                    const int jm = pos - k >= 0 ? pos - k : pos - k + NQ;   // (pos - k) mod NQ
-                    const bool dup = ((NQ & 1) == 0) && (2 * k == NQ);
-                    NodeQ<double> qj;
-                    load_q_rot<double>(sN, Q3, base + jp * st, rd, qj);
-                    double F[5];
-                    two_point_dir<double, 0>(qi, qj, tp, cst, F);
-                    const double cj = tab->skew[pos * NQ + jp], cr = tab->skew[pos * NQ + jm];
+                    for (int s = 0; s < 5; ++s) acc[s] = 0.0;
 #pragma unroll
-                    for (int s = 0; s < 5; ++s) {
-                        const double fr = __shfl_sync(0xffffffffu, F[s], segbase + jm);
-                        accr[s] += cj * F[s];
-                        if (!dup) accr[s] += cr * fr;
+                    for (int k = 1; k <= NQ / 2; ++k) {
+                        const int jp = pos + k < NQ ? pos + k : pos + k - NQ;
+                        const int jm = pos - k >= 0 ? pos - k : pos - k + NQ;
+                        const bool dup = ((NQ & 1) == 0) && (2 * k == NQ);
+                        const int nj = base + jp * st;
+                        NodeQ<double> qj;
+                        load_q<double>(sN, Q3, nj, qj);
+                        const double nv[3] = {0.5 * (mi[0] + sM[(0 * 3 + rd) * Q3 + nj]),
+                                              0.5 * (mi[1] + sM[(1 * 3 + rd) * Q3 + nj]),
+                                              0.5 * (mi[2] + sM[(2 * 3 + rd) * Q3 + nj])};
+                        double F[5];
+                        two_point_n<double>(qi, qj, nv, tp, cst, F);
+                        const double cj = tab->skew[pos * NQ + jp], cr = tab->skew[pos * NQ + jm];
+#pragma unroll
+                        for (int s = 0; s < 5; ++s) {
+                            const double fr = __shfl_sync(0xffffffffu, F[s], segbase + jm);
+                            acc[s] += cj * F[s];
+                            if (!dup) acc[s] += cr * fr;
+                        }
                     }
+                } else {
+                    NodeQ<double> qi;
+                    load_q_rot<double>(sN, Q3, node, rd, qi);
+                    double accr[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+                    for (int k = 1; k <= NQ / 2; ++k) {
+                        const int jp = pos + k < NQ ? pos + k : pos + k - NQ;   // (pos + k) mod NQ
+                        const int jm = pos - k >= 0 ? pos - k : pos - k + NQ;   // (pos - k) mod NQ
+                        const bool dup = ((NQ & 1) == 0) && (2 * k == NQ);
+                        NodeQ<double> qj;
+                        load_q_rot<double>(sN, Q3, base + jp * st, rd, qj);
+                        double F[5];
+                        two_point_dir<double, 0>(qi, qj, tp, cst, F);
+                        const double cj = tab->skew[pos * NQ + jp], cr = tab->skew[pos * NQ + jm];
+#pragma unroll
+                        for (int s = 0; s < 5; ++s) {
+                            const double fr = __shfl_sync(0xffffffffu, F[s], segbase + jm);
+                            accr[s] += cj * F[s];
+                            if (!dup) accr[s] += cr * fr;
+                        }
+                    }
+                    // back to (x, y, z) components by selects (a run-time index would put acc in
+                    // local memory)
+                    acc[0] = accr[0]; acc[4] = accr[4];
+                    acc[1] = rd == 0 ? accr[1] : rd == 1 ? accr[3] : accr[2];
+                    acc[2] = rd == 0 ? accr[2] : rd == 1 ? accr[1] : accr[3];
+                    acc[3] = rd == 0 ? accr[3] : rd == 1 ? accr[2] : accr[1];
                 }
-                // back to (x, y, z) components by selects (a run-time index would put acc in
-                // local memory)
-                const double acc[5] = {accr[0], rd == 0 ? accr[1] : rd == 1 ? accr[3] : accr[2],
-                                       rd == 0 ? accr[2] : rd == 1 ? accr[1] : accr[3],
-                                       rd == 0 ? accr[3] : rd == 1 ? accr[2] : accr[1], accr[4]};
                 if (valid) {
                     const int t1c = lt % NQ, t2c = lt / NQ;
                     const double wab = tab->wq[t1c] * tab->wq[t2c];
@@ -706,8 +755,10 @@ gl_stage_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab
             NodeQ<double> nq;
             node_prepare<double>(u, TP_KG, cst.gm1, nq, a.status);
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                const double nv[3] = {d == 0 ? 1.0 : 0.0, d == 1 ? 1.0 : 0.0, d == 2 ? 1.0 : 0.0};
+            for (int d = 0; d < 3; ++d) {   // affine: F . e_d; curvilinear: the contravariant F . C[:, d]
+                const double nv[3] = {CURV ? sM[(0 * 3 + d) * Q3 + q] : d == 0 ? 1.0 : 0.0,
+                                      CURV ? sM[(1 * 3 + d) * Q3 + q] : d == 1 ? 1.0 : 0.0,
+                                      CURV ? sM[(2 * 3 + d) * Q3 + q] : d == 2 ? 1.0 : 0.0};
                 double F[5];
                 conv_flux_n<double>(nq, nv, 0.0, F);
 #pragma unroll
@@ -751,7 +802,14 @@ gl_stage_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab
 #pragma unroll
             for (int s = 0; s < 5; ++s) { uo[s] = ro[s]; ue[s] = re[s]; }
         }
-        const double nv[3] = {dn == 0 ? 1.0 : 0.0, dn == 1 ? 1.0 : 0.0, dn == 2 ? 1.0 : 0.0};
+        double nv[3] = {dn == 0 ? 1.0 : 0.0, dn == 1 ? 1.0 : 0.0, dn == 2 ? 1.0 : 0.0};
+        double Jf = 1.0;
+        if constexpr (CURV) {   // the face's unit normal and |C[:, dn]|
+            const double* m = g.fnrm + ((size_t)cell * 6 + f) * 3 * NF + q2;
+            const double m0 = __ldg(&m[0]), m1 = __ldg(&m[NF]), m2 = __ldg(&m[2 * NF]);
+            Jf = sqrt(m0 * m0 + m1 * m1 + m2 * m2);
+            nv[0] = m0 / Jf; nv[1] = m1 / Jf; nv[2] = m2 / Jf;
+        }
         const double* uL = side ? uo : ue;
         const double* uR = side ? ue : uo;
         NodeQ<double> qL, qR;
@@ -761,7 +819,7 @@ gl_stage_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab
         conv_num_flux_n<double>(uL, uR, qL, qR, nv, tp, cf, cst, Fc);
         double term[5];
 #pragma unroll
-        for (int s = 0; s < 5; ++s) term[s] = -sgn * Fc[s];
+        for (int s = 0; s < 5; ++s) term[s] = -sgn * (CURV ? Jf * Fc[s] : Fc[s]);
         if constexpr (VISC) {
             // each side's F_v(u, q) . e_dn at the face node, from the auxiliary kernel
             const double* ao = g.t2 + ((size_t)cell * 6 + f) * GL_T2W * NF + q2;
@@ -841,7 +899,15 @@ gl_stage_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab
                 load_q<double>(sN, Q3, node, qv);
                 load_q<double>(sQF, 2 * NF, side * NF + q2, qf);
                 double F[5];
-                two_point_n<double>(qv, qf, nv, tp, cst, F);
+                if constexpr (CURV) {   // 1/2 (C_face[:, dn] + C_vol[:, dn])
+                    const double* m = g.fnrm + ((size_t)cell * 6 + 2 * dn + side) * 3 * NF + q2;
+                    const double mv[3] = {0.5 * (__ldg(&m[0]) + sM[(0 * 3 + dn) * Q3 + node]),
+                                          0.5 * (__ldg(&m[NF]) + sM[(1 * 3 + dn) * Q3 + node]),
+                                          0.5 * (__ldg(&m[2 * NF]) + sM[(2 * 3 + dn) * Q3 + node])};
+                    two_point_n<double>(qv, qf, mv, tp, cst, F);
+                } else {
+                    two_point_n<double>(qv, qf, nv, tp, cst, F);
+                }
 #pragma unroll
                 for (int s = 0; s < 5; ++s) s2[(size_t)it * 5 + s] = F[s];
             }
@@ -884,14 +950,25 @@ gl_stage_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab
         for (int i = threadIdx.x; i < 4 * D3; i += NT) sU[D3 + i] += __ldg(&g.vis[(size_t)cell * 4 * D3 + i]);
         __syncthreads();
     }
-    // sU = R / h^2 (the affine metric C = h^2 I and J = h^2 factored out)
+    // affine: sU = R / h^2 (the affine metric C = h^2 I and J = h^2 factored out); curvilinear: R
     if (a.mode == 0) {
-        const double h2 = a.h * a.h;
+        const double h2 = CURV ? 1.0 : a.h * a.h;
         for (int i = threadIdx.x; i < 5 * D3; i += NT) a.out[(size_t)cell * 5 * D3 + i] = h2 * sU[i];
         return;
     }
-    // k = M^-1 R = (1/h) (M+K)^-1 (x3) (R / h^2)
-    gl_apply3<NT, ND, ND, 5>(T.minv, sU, D3, sQ, D3, t0, t1, a.inv_h, false);
+    if constexpr (CURV) {   // k = P (x3) [ (1 / (W det J)) P^T (x3) R ]
+        gl_apply3<NT, NQ, ND, 5, true>(T.pwa, sU, D3, sDiv, Q3, t0, t1, 1.0, false);
+        const double* iJ = g.vmet + ((size_t)cell * 10 + 9) * Q3;
+        for (int i = threadIdx.x; i < 5 * Q3; i += NT) {
+            const int q = i % Q3;
+            sDiv[i] *= __ldg(&iJ[q]) / (tab->wq[q % NQ] * tab->wq[(q / NQ) % NQ] * tab->wq[q / NF]);
+        }
+        __syncthreads();
+        gl_apply3<NT, ND, NQ, 5>(T.pwa, sDiv, Q3, sQ, D3, t0, t1, 1.0, false);
+    } else {
+        // k = M^-1 R = (1/h) (M+K)^-1 (x3) (R / h^2)
+        gl_apply3<NT, ND, ND, 5>(T.minv, sU, D3, sQ, D3, t0, t1, a.inv_h, false);
+    }
     if (a.mode == 1) {
         for (int i = threadIdx.x; i < 5 * D3; i += NT) a.out[(size_t)cell * 5 * D3 + i] = sQ[i];
         return;
@@ -911,6 +988,48 @@ gl_stage_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab
         }
         if (a.carry_out) a.carry_out[dof] = a.a_carry * k;
     }
+}
+
+// ------------------------------------------------------------------------------------
+// The weight-adjusted inverse mass on curvilinear cells on its own (ph_apply_inverse_mass):
+// out = P (x3) [ (1 / (W det J)) P^T (x3) in ], one CTA per cell (a.U = in, a.out = out)
+// ------------------------------------------------------------------------------------
+template <int ND, int NQ>
+struct GlMinvLayout {
+    static constexpr int NT = gl_threads<NQ>();
+    static constexpr int D3 = ND * ND * ND, Q3 = NQ * NQ * NQ;
+    static constexpr int nTab = (int)(sizeof(GlTab) / sizeof(double));
+    static constexpr int oU = nTab, oQ = oU + 5 * Q3;
+    static constexpr int nT = gl_temp<ND, NQ>();
+    static constexpr int oT0 = oQ + 5 * Q3, oT1 = oT0 + nT;
+    static constexpr int total = oT1 + nT;
+    static constexpr size_t bytes = (size_t)total * sizeof(double);
+};
+
+template <int ND, int NQ>
+__global__ void __launch_bounds__(gl_threads<NQ>())
+gl_minv_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab T) {
+    using L = GlMinvLayout<ND, NQ>;
+    constexpr int NT = L::NT, D3 = L::D3, Q3 = L::Q3, NF = NQ * NQ;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* sm = reinterpret_cast<double*>(smem_raw);
+    GlTab* tab = reinterpret_cast<GlTab*>(sm);
+    double* sU = sm + L::oU;
+    double* sQ = sm + L::oQ;
+    double* t0 = sm + L::oT0;
+    double* t1 = sm + L::oT1;
+    const int cell = a.cell_begin + blockIdx.x;
+    gl_load_tab(g.tab, tab, NT);
+    for (int i = threadIdx.x; i < 5 * D3; i += NT) sU[i] = __ldg(&a.U[(size_t)cell * 5 * D3 + i]);
+    __syncthreads();
+    gl_apply3<NT, NQ, ND, 5, true>(T.pwa, sU, D3, sQ, Q3, t0, t1, 1.0, false);
+    const double* iJ = g.vmet + ((size_t)cell * 10 + 9) * Q3;
+    for (int i = threadIdx.x; i < 5 * Q3; i += NT) {
+        const int q = i % Q3;
+        sQ[i] *= __ldg(&iJ[q]) / (tab->wq[q % NQ] * tab->wq[(q / NQ) % NQ] * tab->wq[q / NF]);
+    }
+    __syncthreads();
+    gl_apply3<NT, ND, NQ, 5>(T.pwa, sQ, Q3, a.out + (size_t)cell * 5 * D3, D3, t0, t1, 1.0, false);
 }
 
 } // namespace ph

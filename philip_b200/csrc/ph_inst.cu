@@ -292,7 +292,7 @@ static cudaError_t launch_gl_nq(int kernel, const StageArgs& a, const GlArgs& g,
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     constexpr int NT = gl_threads<NQ>();
-    static bool cfg[8][64] = {};
+    static bool cfg[11][64] = {};
     if (kernel == 0) {
         if (split) return launch_gl_kernel(gl_trace_kernel<ND, NQ, true>, GlTraceLayout<ND, NQ, true>::bytes, NT, a, g, ht,
                                            cfg[0][dev], s);
@@ -304,6 +304,15 @@ static cudaError_t launch_gl_nq(int kernel, const StageArgs& a, const GlArgs& g,
                                            cfg[2][dev], s);
         return launch_gl_kernel(gl_aux_kernel<ND, NQ, false>, GlAuxLayout<ND, NQ, false>::bytes, NT, a, g, ht,
                                 cfg[3][dev], s);
+    }
+    if (kernel == 3)   // curvilinear: the weight-adjusted inverse mass alone
+        return launch_gl_kernel(gl_minv_kernel<ND, NQ>, GlMinvLayout<ND, NQ>::bytes, NT, a, g, ht, cfg[8][dev], s);
+    if (g.vmet) {      // curvilinear cells: the Euler equations (checked by the host)
+        if (visc) return cudaErrorInvalidValue;
+        if (split) return launch_gl_kernel(gl_stage_kernel<ND, NQ, false, true, true>,
+                                           GlStageLayout<ND, NQ, false, true, true>::bytes, NT, a, g, ht, cfg[9][dev], s);
+        return launch_gl_kernel(gl_stage_kernel<ND, NQ, false, false, true>,
+                                GlStageLayout<ND, NQ, false, false, true>::bytes, NT, a, g, ht, cfg[10][dev], s);
     }
     if (visc) {
         if (split) return launch_gl_kernel(gl_stage_kernel<ND, NQ, true, true>, GlStageLayout<ND, NQ, true, true>::bytes,

@@ -45,7 +45,8 @@ bool batched_shape(int fp32, bool curv, int variant, int* cpc, int* threads, siz
 // Uncollocated path (GL flux nodes / overintegration), N1 = p + 1 solution nodes and nq flux
 // nodes per direction (N1 <= nq <= min(N1 + 2, 7)): kernel 0 = face values (gl_trace_kernel),
 // 1 = auxiliary equation and viscous terms (gl_aux_kernel), 2 = residual / RK stage
-// (gl_stage_kernel); one CTA per cell of [a.cell_begin, a.nc).
+// (gl_stage_kernel), 3 = the weight-adjusted inverse mass of curvilinear cells (gl_minv_kernel,
+// a.U in, a.out out); one CTA per cell of [a.cell_begin, a.nc). g.vmet != nullptr: curvilinear.
 template <int N1>
 cudaError_t launch_gl(int kernel, int nq, const StageArgs& a, const GlArgs& g, const GlTab& ht, bool visc, bool split,
                       cudaStream_t s);

@@ -23,7 +23,12 @@ RTOL = 1e-12
 
 
 def _oracle(kw, warp):
-    prm = Parameters.from_dict(prm_dict(**kw))
+    kw = dict(kw)
+    nodes, over = kw.pop("nodes", "GLL"), kw.pop("overintegration", 0)
+    d = prm_dict(**kw)
+    d["flux_nodes_type"] = nodes
+    d["overintegration"] = over
+    prm = Parameters.from_dict(d)
     left, right = prm.grid_bounds
     return prm, Oracle(prm.oracle_cfg(), prm.n_cells, left, right, warp=warp)
 
@@ -242,3 +247,107 @@ def test_curvilinear_navier_stokes_free_stream_steps_and_precision_form():
     err = rel_max_err(dg32.residual_of(V), orc32.residual(V))
     print(f"curvilinear Navier-Stokes fp32 residual rel err {err:.3e}")
     assert err <= 1e-5
+
+
+# ------------------------------------------------------------------------------- GL flux nodes
+# The reference's own curvilinear cases run on GL flux nodes or with overintegration
+# (euler_split_inviscid_taylor_green_vortex/3D_euler_split_inviscid_taylor_green_vortex_curv.prm:
+# GL, overintegration 2, Ranocha flux, cPlus; TGV_scaling/3D_TGV_scaling_*_curv*.prm: GL, split
+# and conservative, cDG and cHU). On these the metric terms live at the flux nodes (the curl-form
+# cofactor evaluated there and at each face's flux nodes) and the inverse mass is the weight-
+# adjusted P diag(1 / (W det J)) P^T.
+
+GL_CURVED = [
+    ("gl_split_CH_roe_p3", dict(poly_degree=3, n_cells=3, nodes="GL")),
+    ("gl_overint2_split_Ra_cPlus_p3", dict(poly_degree=3, n_cells=2, nodes="GL", overintegration=2, two_point="Ra",
+                                           conv="two_point_flux", fr="cPlus")),
+    ("gl_conservative_roe_cHU_p2", dict(poly_degree=2, n_cells=3, nodes="GL", split=False, conv="roe", fr="cHU")),
+    ("gl_split_IR_ec_p5", dict(poly_degree=5, n_cells=2, nodes="GL", two_point="IR", conv="two_point_flux")),
+    ("gll_overint1_split_KG_lxf_p2", dict(poly_degree=2, n_cells=3, overintegration=1, two_point="KG",
+                                          conv="two_point_flux_with_lax_friedrichs_dissipation")),
+    ("gl_conservative_lxf_p1", dict(poly_degree=1, n_cells=4, nodes="GL", split=False, conv="lax_friedrichs")),
+]
+
+
+@pytest.mark.parametrize("kw", [dict(poly_degree=3, n_cells=2, nodes="GL"),
+                                dict(poly_degree=2, n_cells=3, nodes="GL", split=False, conv="roe", fr="cHU"),
+                                dict(poly_degree=2, n_cells=2, nodes="GL", overintegration=2)],
+                         ids=["gl_split_p3", "gl_conservative_chu_p2", "gl_overint2_p2"])
+def test_oracle_gl_vanishing_warp_and_free_stream(kw):
+    """The oracle's metric terms at uncollocated flux nodes: the vanishing-warp limit is the
+    affine GL path (pinned by the reference's GL golden energy checks), and the warped mesh
+    keeps a uniform flow uniform."""
+    _, affine = _oracle(kw, 0.0)
+    _, curved = _oracle(kw, 1e-300)
+    U = perturbed_tgv(affine, seed=3)
+    assert rel_max_err(curved.residual(U), affine.residual(U)) <= 1e-13
+    R0 = affine.residual(U)
+    if kw.get("fr", "cDG") == "cDG":
+        # with cDG the weight-adjusted inverse P W^-1 P^T / J (P = M^-1 chi^T W) is M^-1 / J on an
+        # undeformed cell; with FR it is (M+K)^-1 M (M+K)^-1 / J there, not (M+K)^-1 / J: the
+        # reference takes the weight-adjusted form on every cell of a curved manifold
+        # (dg_base.cpp:4163-4245), which the GPU parity tests hold to the oracle
+        assert rel_max_err(curved.inverse_mass(R0), affine.inverse_mass(R0)) <= 1e-13
+    _, warped = _oracle(kw, WARP)
+    R = warped.residual(_uniform_state(warped))
+    scale = np.max(np.abs(warped.residual(warped.initial_condition("tgv"))))
+    print(f"GL warped, uniform flow: max |R| {np.max(np.abs(R)):.3e} (TGV residual scale {scale:.3e})")
+    # the uniform flow's fluxes times the metric are O(300) per node: 1e-11 of the TGV residual
+    # scale is rounding of those terms (1e-13 of them)
+    assert np.max(np.abs(R)) <= 1e-11 * scale
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,kw", GL_CURVED, ids=[c[0] for c in GL_CURVED])
+def test_curvilinear_gl_residual_and_inverse_mass_parity(name, kw):
+    prm, orc, dg = _pair(kw)
+    U = perturbed_tgv(orc, seed=len(name))
+    R_orc = orc.residual(U)
+    err = rel_max_err(dg.residual_of(U), R_orc)
+    k_gpu = np.empty_like(R_orc)
+    dg.apply_inverse_global_mass_matrix(R_orc, k_gpu)
+    err_m = rel_max_err(k_gpu, orc.inverse_mass(R_orc))
+    print(f"{name}: curvilinear GL residual rel max err {err:.3e}, inverse mass {err_m:.3e}")
+    assert err <= RTOL and err_m <= RTOL
+
+
+@pytest.mark.gpu
+def test_reference_style_curved_grid_on_gl_flux_nodes():
+    """The reference-style chart map (curved_periodic_grid.cpp:64-90) given as mapping support
+    points, on GL flux nodes with overintegration 2 and cPlus as in the reference's
+    3D_euler_split_inviscid_taylor_green_vortex_curv.prm: a uniform flow stays uniform (the
+    discrete metric identities of the curl form at the flux nodes)."""
+    from philip_b200.dg import DGStrong
+    kw = dict(poly_degree=3, n_cells=2, left=0.0, right=1.0, nodes="GL", overintegration=2, two_point="Ra",
+              conv="two_point_flux", fr="cPlus")
+    prm, orc = _oracle(kw, 0.0)
+    P = orc.node_xyz().reshape(-1, 3).copy()
+    x, y, z = P[:, 0].copy(), P[:, 1].copy(), P[:, 2].copy()
+    P[:, 0] = x + 0.2 * np.sin(np.pi * y)
+    P[:, 1] = y + 0.2 * np.sin(np.pi * z)
+    P[:, 2] = z + 0.2 * np.sin(np.pi * x)
+    dg = DGStrong(prm, mapping_support_points=_support_points(P, orc.nd))
+    R = dg.residual_of(_uniform_state(orc))
+    print(f"reference-style curved grid on GL nodes, uniform flow: max |R| {np.max(np.abs(R)):.3e}")
+    assert np.max(np.abs(R)) <= 1e-10
+
+
+@pytest.mark.gpu
+def test_curvilinear_gl_free_stream_and_steps():
+    from philip_b200.dg import RungeKuttaODESolver
+    kw = dict(poly_degree=3, n_cells=2, nodes="GL", overintegration=2, two_point="Ra", conv="two_point_flux",
+              fr="cPlus")
+    prm, orc, dg = _pair(kw)
+    R = dg.residual_of(_uniform_state(orc))
+    print(f"curvilinear GL, uniform flow: max |R| {np.max(np.abs(R)):.3e}")
+    assert np.max(np.abs(R)) <= 1e-10
+    U = orc.initial_condition("tgv")
+    dg.solution = U
+    dt = 0.1 * TWO_PI / 8 / 11.0
+    ode = RungeKuttaODESolver(dg)
+    for step in range(3):
+        orc.rk_step(U, dt)
+        ode.step_in_time(dt)
+        err = rel_max_err(dg.solution, U)
+        print(f"curvilinear GL RK4 step {step}: rel err {err:.3e}")
+        assert err <= 1e-12 and dg.status() == 0

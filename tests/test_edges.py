@@ -81,9 +81,12 @@ def test_curvilinear_navier_stokes_with_sipg_is_refused():
     assert rc == _lib.PH_ERR_UNSUPPORTED and "kDG" in msg
 
 
-def test_curvilinear_gl_flux_nodes_are_refused():
-    rc, msg = _create(mesh_kw=dict(warp=0.1), edit=lambda p: setattr(p, "flux_nodes_type", 0))
-    assert rc == _lib.PH_ERR_UNSUPPORTED and "affine" in msg
+def test_curvilinear_gl_navier_stokes_is_refused():
+    """GL flux nodes on curvilinear cells take the Euler equations (no curvilinear auxiliary
+    equation at uncollocated nodes)."""
+    rc, msg = _create(prm_kw=dict(pde="navier_stokes", diss="bassi_rebay_2"), mesh_kw=dict(warp=0.1),
+                      edit=lambda p: setattr(p, "flux_nodes_type", 0))
+    assert rc == _lib.PH_ERR_UNSUPPORTED and "Euler" in msg
 
 
 def test_entry_points_without_contexts_refuse_gl_flux_nodes():
