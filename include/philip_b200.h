@@ -266,8 +266,8 @@ int ph_get_timing(ph_ctx* ctx, double out[7]);
  * ph_cell_ijk), whatever mesh->cell_order says; the state, ph_ndofs and the integrals cover
  * the owned cells only (ph_integrals / ph_integrated_quantities give this rank's share of
  * each volume average: sum them over ranks, and take the max of the wave speed). Slab
- * contexts take GLL flux nodes without overintegration and launch directly (no step graph,
- * ph_run refused); with relaxation RK they need ph_set_rank_sum; on a curvilinear mesh mapping_support_points, when given,
+ * contexts launch directly (no step graph, ph_run refused); with relaxation RK they need
+ * ph_set_rank_sum; on a curvilinear mesh mapping_support_points, when given,
  * covers the slab's own cells in the slab's state order. z_count = n is the whole mesh on one rank: its ghost layers are its own last
  * and first layers (a halo that copies send_hi to recv_lo and send_lo to recv_hi). */
 enum { PH_HALO_STATE = 0, PH_HALO_VISCOUS = 1 };   /* what is exchanged */

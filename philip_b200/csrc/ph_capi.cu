@@ -1168,6 +1168,9 @@ __global__ void halo_copy_kernel(const HaloCopy h) {
 // face, read by the first layer's z- faces) and recv_hi into the upper ghost layer (its
 // bottom face). STATE: the 5 components at the face's (p+1)^2 nodes of the state buffer U;
 // VISCOUS: the face's block of the viscous terms (4 (p+1)^2 values of the arithmetic type).
+// Uncollocated flux nodes: STATE is the face's block of the face-value buffer (the state's and
+// the projected entropy variables' face values, written by the face-value kernel), VISCOUS the
+// first four rows of the face's viscous block (each side's F_v . n).
 int halo_copy(ph_ctx* c, int what, bool pack, const double* U) {
     const int N1 = c->N1, NF = N1 * N1, NP = c->NP, L = c->layer, nc = c->nc;
     unsigned char* hb = c->d_halo;
@@ -1177,7 +1180,15 @@ int halo_copy(ph_ctx* c, int what, bool pack, const double* U) {
     const unsigned long long* vol[2];
     unsigned long long* volw[2];
     long long vpitch;
-    if (what == PH_HALO_STATE) {
+    if (c->gl) {   // uncollocated: the face blocks of the face-value / viscous buffers
+        const int NQF = c->NQ * c->NQ, T1W = c->split ? 10 : 5;
+        const size_t cw = (size_t)6 * (what == PH_HALO_STATE ? T1W : ph::GL_T2W) * NQF;   // words per cell
+        const size_t fw = cw / 6;                                                          // per face
+        auto* w = reinterpret_cast<unsigned long long*>(what == PH_HALO_STATE ? c->d_t1 : c->d_t2);
+        h.rows = L; h.width = (int)(what == PH_HALO_STATE ? fw : (size_t)4 * NQF); vpitch = (long long)cw;
+        if (pack) { vol[0] = w + 4 * fw; vol[1] = w + (size_t)(nc - L) * cw + 5 * fw; }
+        else { volw[0] = w + (size_t)nc * cw + 5 * fw; volw[1] = w + (size_t)(nc + L) * cw + 4 * fw; }
+    } else if (what == PH_HALO_STATE) {
         auto* w = reinterpret_cast<unsigned long long*>(const_cast<double*>(U));
         h.rows = 5 * L; h.width = NF; vpitch = NP;
         if (pack) { vol[0] = w; vol[1] = w + (size_t)(nc - L) * 5 * NP + (size_t)(N1 - 1) * NF; }
@@ -1277,7 +1288,21 @@ int eval_residual(ph_ctx* c, const double* in, ph::StageArgs a) {
     if (c->gl) {   // face values, (auxiliary equation,) residual: every kernel over all cells
         a.cell_begin = 0; a.nc = c->nc;
         if (int rc = dispatch_gl(c, 0, a)) return rc;
-        if (c->visc) if (int rc = dispatch_gl(c, 1, a)) return rc;
+        if (c->nc_ghost) {   // a slab: the partition faces' face values to and from the neighbours
+            if (int rc = halo_copy(c, PH_HALO_STATE, true, in)) return rc;
+            if (int rc = halo_call(c, PH_HALO_STATE, PH_HALO_BEGIN)) return rc;
+            if (int rc = halo_call(c, PH_HALO_STATE, PH_HALO_END)) return rc;
+            if (int rc = halo_copy(c, PH_HALO_STATE, false, in)) return rc;
+        }
+        if (c->visc) {
+            if (int rc = dispatch_gl(c, 1, a)) return rc;
+            if (c->nc_ghost) {
+                if (int rc = halo_copy(c, PH_HALO_VISCOUS, true, in)) return rc;
+                if (int rc = halo_call(c, PH_HALO_VISCOUS, PH_HALO_BEGIN)) return rc;
+                if (int rc = halo_call(c, PH_HALO_VISCOUS, PH_HALO_END)) return rc;
+                if (int rc = halo_copy(c, PH_HALO_VISCOUS, false, in)) return rc;
+            }
+        }
         return dispatch_gl(c, 2, a);
     }
     if (!c->nc_ghost) {
@@ -1359,7 +1384,6 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
     if (slab) {
         if (z0 < 0 || z0 >= mesh->n_cells_per_direction || nz > mesh->n_cells_per_direction)
             return fail(PH_ERR_INVALID, "slab outside the mesh: 0 <= z_first < n and 1 <= z_count <= n");
-        if (gl) return fail(PH_ERR_UNSUPPORTED, "slab contexts take GLL flux nodes without overintegration");
     }
     ph_ctx* c = new ph_ctx();
     c->prm = *prm;
@@ -1438,13 +1462,18 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
         const int NF = c->N1 * c->N1;
         c->halo_state_bytes = (size_t)c->layer * 5 * NF * sizeof(double);
         c->halo_visc_bytes = c->visc ? (size_t)c->layer * 4 * NF * (c->fp32 ? sizeof(float) : sizeof(double)) : 0;
+        if (gl) {   // the face blocks of the face-value buffer, and four rows of the viscous one
+            const int NQF = (c->N1 + prm->overintegration) * (c->N1 + prm->overintegration);
+            c->halo_state_bytes = (size_t)c->layer * (c->split ? 10 : 5) * NQF * sizeof(double);
+            c->halo_visc_bytes = c->visc ? (size_t)c->layer * 4 * NQF * sizeof(double) : 0;
+        }
         c->halo_stride = (std::max(c->halo_state_bytes, c->halo_visc_bytes) + 255) / 256 * 256;
         bad |= dalloc(&c->d_halo, 4 * c->halo_stride);
     }
     c->limiter = prm->bound_preserving_limiter;
     if (c->limiter) bad |= dalloc(&c->d_ltab, 1);
-    if (gl) {
-        const size_t faces = (size_t)c->nc * 6 * c->NQ * c->NQ;
+    if (gl) {   // (slabs: the ghost cells' face blocks too, filled by the exchange)
+        const size_t faces = (size_t)(c->nc + c->nc_ghost) * 6 * c->NQ * c->NQ;
         bad |= dalloc(&c->d_gl, 1);
         bad |= dalloc(&c->d_t1, faces * (c->split ? 10 : 5));
         if (c->visc) {

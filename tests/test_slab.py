@@ -155,8 +155,7 @@ def test_slab_refusals_without_a_gpu():
     assert create(4, 1) == _lib.PH_ERR_INVALID
     assert create(0, 0) == _lib.PH_ERR_INVALID
     assert create(1, 5) == _lib.PH_ERR_INVALID
-    assert create(0, 2, edit=lambda q: setattr(q, "flux_nodes_type", 0)) == _lib.PH_ERR_UNSUPPORTED
-    assert b"GLL" in L.ph_last_error()
+    assert create(0, 2, edit=lambda q: setattr(q, "overintegration", 3)) == _lib.PH_ERR_UNSUPPORTED
     del p
 
 
@@ -528,3 +527,54 @@ def test_relaxation_rk_on_slabs(name, kw, world):
     lonely.solution = _scatter(whole, [lonely], U0)[0]
     with pytest.raises(_lib.PhError, match="ph_set_rank_sum"):
         RungeKuttaODESolver(lonely).step_in_time(dt)
+
+
+def _gl_prm(nodes="GL", overintegration=0, **kw):
+    from philip_b200.prm import Parameters
+    from helpers import prm_dict
+    d = prm_dict(**kw)
+    d["flux_nodes_type"] = nodes
+    d["overintegration"] = overintegration
+    return Parameters.from_dict(d)
+
+
+GL_SLAB_CASES = [
+    ("gl_ns_br2_split_p3_two_slabs", dict(poly_degree=3, n_cells=4, pde="navier_stokes", diss="bassi_rebay_2"), 2, 0.0),
+    ("gl_euler_conservative_roe_p2_three_slabs", dict(poly_degree=2, n_cells=4, split=False, conv="roe"), 3, 0.0),
+    ("gll_overint1_ns_sipg_p2_two_slabs", dict(nodes="GLL", overintegration=1, poly_degree=2, n_cells=4,
+                                               pde="navier_stokes"), 2, 0.0),
+    ("gl_curvilinear_euler_p3_two_slabs", dict(poly_degree=3, n_cells=4), 2, 0.1),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,kw,world,warp", GL_SLAB_CASES, ids=[c[0] for c in GL_SLAB_CASES])
+def test_gl_slabs_are_the_whole_mesh(name, kw, world, warp):
+    """Slabs on uncollocated flux nodes: the partition faces' face values (after the face-value
+    kernel) and each side's F_v . n (after the auxiliary kernel) go through the exchange into
+    the ghost cells' face blocks, so the residual and three RK4 steps are bitwise the whole
+    mesh's."""
+    from oracle.oracle import Oracle
+    from philip_b200.dg import DGStrong, RungeKuttaODESolver
+    from helpers import TWO_PI, perturbed_tgv
+    prm = _gl_prm(**kw)
+    whole = DGStrong(prm, warp=warp)
+    U0 = perturbed_tgv(Oracle(prm.oracle_cfg(), prm.n_cells, *prm.grid_bounds), seed=len(name))
+    parts = _slabs(prm, world, warp=warp)
+    dgs = [p for p, _ in parts]
+    Us = _scatter(whole, dgs, U0)
+    Rs = _in_threads([lambda k=k: dgs[k].residual_of(Us[k]) for k in range(world)])
+    R = _gather(whole, dgs, Rs)
+    R_whole = whole.residual_of(U0)
+    print(f"{name}: max |R_slabs - R_whole| = {np.max(np.abs(R - R_whole)):.3e}")
+    assert np.array_equal(R, R_whole)
+    dt = 0.1 * TWO_PI / prm.n_cells / (prm.poly_degree + 1) / 11.0
+    whole.solution = U0
+    RungeKuttaODESolver(whole).step_in_time(dt, nsteps=3)
+    for dg, u in zip(dgs, Us):
+        dg.solution = u
+    _in_threads([lambda k=k: (RungeKuttaODESolver(dgs[k]).step_in_time(dt, nsteps=3), parts[k][1].synchronize())
+                 for k in range(world)])
+    U = _gather(whole, dgs, [dg.solution for dg in dgs])
+    print(f"{name}: max |U_slabs - U_whole| = {np.max(np.abs(U - whole.solution)):.3e}")
+    assert np.array_equal(U, whole.solution)
