@@ -114,10 +114,10 @@ typedef struct ph_mesh_desc {
      * by warp (L/2pi) sin(2pi(x-l)/L) sin(2pi(y-l)/L) sin(2pi(z-l)/L) (L = right - left,
      * l = left; zero on the cube's faces, so periodic faces still match), through a mapping
      * of degree grid_degree on GLL support points. The GPU path takes grid_degree =
-     * poly_degree and, on GLL flux nodes without overintegration, the split form and cDG
-     * (Navier-Stokes with bassi_rebay_2 or central_visc_flux and kDG); on GL flux nodes or with
-     * overintegration, the Euler equations (split or conservative, any FR type). Not a
-     * reference grid:
+     * poly_degree; split or conservative, any FR type (the weight-adjusted inverse mass);
+     * Navier-Stokes on GLL flux nodes without overintegration, with bassi_rebay_2 or
+     * central_visc_flux and kDG; the Euler equations on GL flux nodes or with overintegration.
+     * Not a reference grid:
      * the construction follows the reference's curved periodic grids
      * (src/mesh/grids/curved_periodic_grid.cpp) with this warp. */
     double warp;

@@ -435,8 +435,6 @@ const char* unsupported_reason(const ph_mesh_desc* mesh, const ph_params* prm) {
                    "extent on curved cells is not restated)";
         if (prm->pde_type != 0 && prm->flux_reconstruction_aux != 0)
             return "curvilinear Navier-Stokes takes flux_reconstruction_aux = kDG";
-        if (!prm->use_split_form) return "curvilinear meshes take the split form";
-        if (prm->flux_reconstruction != 0) return "curvilinear meshes take cDG";
     }
     return nullptr;
 }
@@ -1367,6 +1365,8 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
             return fail(PH_ERR_UNSUPPORTED, "relaxation RK: the KG two-point flux has no numerical entropy");
         if (prm->runge_kutta_method >= 7) return fail(PH_ERR_UNSUPPORTED, "relaxation RK: the Butcher methods");
         if (prm->precision != PH_FP64) return fail(PH_ERR_UNSUPPORTED, "relaxation RK: the FP64 path");
+        if (is_curvilinear(mesh) && prm->flux_reconstruction != 0)
+            return fail(PH_ERR_UNSUPPORTED, "relaxation RK on curvilinear meshes takes cDG");
         if (!(prm->relaxation_runge_kutta_root_tolerance > 0.0))
             return fail(PH_ERR_INVALID, "relaxation_runge_kutta_root_tolerance must be positive");
     }
@@ -1735,12 +1735,12 @@ int ph_apply_inverse_mass(ph_ctx* c, const double* R, double* out, int where) {
     const double inv_detj = 1.0 / (c->h * c->h * c->h);
     cudaError_t e;
     switch (c->N1) {
-    case 2: e = ph::launch_inverse_mass<2>(dR, dO, c->d_ops, c->nc, inv_detj, c->d_metric, c->stream); break;
-    case 3: e = ph::launch_inverse_mass<3>(dR, dO, c->d_ops, c->nc, inv_detj, c->d_metric, c->stream); break;
-    case 4: e = ph::launch_inverse_mass<4>(dR, dO, c->d_ops, c->nc, inv_detj, c->d_metric, c->stream); break;
-    case 5: e = ph::launch_inverse_mass<5>(dR, dO, c->d_ops, c->nc, inv_detj, c->d_metric, c->stream); break;
-    case 6: e = ph::launch_inverse_mass<6>(dR, dO, c->d_ops, c->nc, inv_detj, c->d_metric, c->stream); break;
-    case 7: e = ph::launch_inverse_mass<7>(dR, dO, c->d_ops, c->nc, inv_detj, c->d_metric, c->stream); break;
+    case 2: e = ph::launch_inverse_mass<2>(dR, dO, c->d_ops, c->nc, inv_detj, c->d_metric, c->fr ? 1 : 0, c->stream); break;
+    case 3: e = ph::launch_inverse_mass<3>(dR, dO, c->d_ops, c->nc, inv_detj, c->d_metric, c->fr ? 1 : 0, c->stream); break;
+    case 4: e = ph::launch_inverse_mass<4>(dR, dO, c->d_ops, c->nc, inv_detj, c->d_metric, c->fr ? 1 : 0, c->stream); break;
+    case 5: e = ph::launch_inverse_mass<5>(dR, dO, c->d_ops, c->nc, inv_detj, c->d_metric, c->fr ? 1 : 0, c->stream); break;
+    case 6: e = ph::launch_inverse_mass<6>(dR, dO, c->d_ops, c->nc, inv_detj, c->d_metric, c->fr ? 1 : 0, c->stream); break;
+    case 7: e = ph::launch_inverse_mass<7>(dR, dO, c->d_ops, c->nc, inv_detj, c->d_metric, c->fr ? 1 : 0, c->stream); break;
     default: return fail(PH_ERR_UNSUPPORTED, "polynomial degree");
     }
     if (e != cudaSuccess) return fail(PH_ERR_CUDA, cudaGetErrorString(e));

@@ -35,8 +35,8 @@ static cudaError_t launch_prec(const StageArgs& a, bool visc, bool split, cudaSt
     // relaxation RK's entropy estimate lives in the generic instance only
     const bool hot = split && a.pc.two_point == TP_CH && a.pc.conv_flux == CF_EC_ROE &&
                      (!visc || a.pc.diss_flux == DF_BR2) && a.ent_partial == nullptr;
-    if (a.metric) {   // curvilinear cells: the split form (checked by the host)
-        if (!split) return cudaErrorInvalidValue;
+    if (a.metric) {   // curvilinear cells
+        if (!split) return visc ? launch_one<R, N1, true, false, 0, true>(a, s) : launch_one<R, N1, false, false, 0, true>(a, s);
         if (visc) return hot ? launch_one<R, N1, true, true, 1, true>(a, s) : launch_one<R, N1, true, true, 0, true>(a, s);
         return hot ? launch_one<R, N1, false, true, 1, true>(a, s) : launch_one<R, N1, false, true, 0, true>(a, s);
     }
@@ -200,8 +200,8 @@ cudaError_t launch_aux(const double* U, const int* nbr, const OpTab& ops, int ce
 
 template <int N1>
 cudaError_t launch_inverse_mass(const double* in, double* out, const OpTab* ops, int nc, double inv_detj,
-                                const double* metric, cudaStream_t s) {
-    inverse_mass_kernel<N1><<<nc, 128, 0, s>>>(in, out, ops, nc, inv_detj, metric);
+                                const double* metric, int fr, cudaStream_t s) {
+    inverse_mass_kernel<N1><<<nc, 128, 0, s>>>(in, out, ops, nc, inv_detj, metric, fr);
     return cudaGetLastError();
 }
 
@@ -265,7 +265,7 @@ template cudaError_t launch_stage_batched<PH_N1>(const StageArgs*, const BatchTi
 template bool batched_shape<PH_N1>(int, bool, int, int*, int*, size_t*, int*);
 template cudaError_t launch_aux<PH_N1>(const double*, const int*, const OpTab&, int, int, double, const PhysConst&, int,
                                        void*, const double*, cudaStream_t);
-template cudaError_t launch_inverse_mass<PH_N1>(const double*, double*, const OpTab*, int, double, const double*,
+template cudaError_t launch_inverse_mass<PH_N1>(const double*, double*, const OpTab*, int, double, const double*, int,
                                                 cudaStream_t);
 template cudaError_t launch_integrals<PH_N1>(const double*, const double*, const double*, const IntegralTab*, int,
                                              const IntegralConst&, bool, double*, cudaStream_t);

@@ -135,7 +135,7 @@ struct Layout {
     static constexpr int NQS = 11;
     static constexpr int TR = VISC ? 9 : 5;            // trace values per face node: u (5) [+ ext viscous flux (4)]
     static constexpr int NX = (VISC ? 4 : 0) + (SPLIT ? 0 : 15) + (CURV ? 9 : 0);
-    static constexpr int OM = VISC ? 4 : 0;            // curvilinear: first metric row of X (after the viscous rows)
+    static constexpr int OM = (VISC ? 4 : 0) + (SPLIT ? 0 : 15);   // curvilinear: first metric row of X
     static constexpr int oOps = 0;                      // D, Dsk, B, w as R
     static constexpr int nOps = 3 * N1 * N1 + N1;
     static constexpr int oU = (oOps + nOps + 1) & ~1;
@@ -281,6 +281,11 @@ __device__ __forceinline__ void face_item(const Cst<R>& cst, int tp, int cf, int
         R term[5];
 #pragma unroll
         for (int s = 0; s < 5; ++s) term[s] = -sgn * J * F[s];
+        if constexpr (!SPLIT) {   // the cell's own contravariant flux F . C[:, d] at the face node
+            constexpr int o = VISC ? 4 : 0;
+#pragma unroll
+            for (int s = 0; s < 5; ++s) term[s] += sgn * X[(o + d * 5 + s) * NP + node];
+        }
         if constexpr (VISC) {
             // the metric-scaled normal viscous flux F~_d = sum_k C[k][d] F_k of both sides (the
             // auxiliary kernels' face blocks; BR2 / central: their average, strong_dg.cpp:3354-3452)
@@ -369,7 +374,7 @@ __device__ __forceinline__ void volume_dir(int d, const Cst<R>& cst, int tp, con
     const int node = node_of<N1>(d == 0 ? pos : cc[0], d == 1 ? pos : cc[1], d == 2 ? pos : cc[2]);
     const int base = node - pos * st;
     R acc[5] = {R(0), R(0), R(0), R(0), R(0)};
-    if constexpr (CURV) {
+    if constexpr (CURV && SPLIT) {
         // curvilinear: the pair flux is dotted with the averaged metric column
         // 1/2 (C_i[:, d] + C_j[:, d]), symmetric in (i, j) like the flux itself
         const R* Dq = sD + lc * NQS * NP;
@@ -605,7 +610,6 @@ __device__ __forceinline__ void prefetch_tile_l2(const StageArgs& a, int cell0) 
 // runs the tiles of many independent discretisations (a batch of solves) from a tile list.
 template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int FS, bool CURV, bool BULK = false>
 __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell0) {
-    static_assert(!CURV || SPLIT, "curvilinear cells: split form only");
     static_assert(!BULK || (std::is_same<R, double>::value && N1 % 2 == 0 && !CURV), "bulk staging: FP64, even N1");
     using L = Layout<R, N1, CPC, VISC, SPLIT, CURV>;
     constexpr int NP = L::NP, NF = L::NF, NT = L::NT, TR = L::TR, NQS = L::NQS;
@@ -734,7 +738,18 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
 #pragma unroll
             for (int i = 0; i < 9; ++i) X[(L::OM + i) * NP + node] = (R)__ldg(&a.metric[((size_t)cell * 10 + i) * NP + node]);
         }
-        if constexpr (!SPLIT) {
+        if constexpr (!SPLIT && CURV) {   // the contravariant fluxes F . C[:, d]
+            constexpr int o = VISC ? 4 : 0;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const R m[3] = {X[(L::OM + 0 * 3 + d) * NP + node], X[(L::OM + 1 * 3 + d) * NP + node],
+                                X[(L::OM + 2 * 3 + d) * NP + node]};
+                R F[5];
+                conv_flux_n<R>(q, m, cst.shift(), F);
+#pragma unroll
+                for (int s = 0; s < 5; ++s) X[(o + d * 5 + s) * NP + node] = F[s];
+            }
+        } else if constexpr (!SPLIT) {
             constexpr int o = VISC ? 4 : 0;
             R F[5];
             conv_flux_dir<R, 0>(q, cst.shift(), F);
@@ -839,22 +854,34 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
         for (int s = 0; s < 5; ++s) A[s * NP + node] = G[s];
     }
     if (a.mode != 0 && a.fr) {
-        // B (x) B (x) B applied direction by direction, ping-pong between sA and sD
+        // B (x) B (x) B applied direction by direction, ping-pong between sA and sD; curvilinear
+        // cells: the weight-adjusted inverse B (x3) [ (1 / det J) B (x3) G ] (P = (M+K)^-1 W = B on
+        // collocated GLL nodes, dg_base.cpp:4217-4249), 1 / det J applied between the two
         R* src = sA; R* dst = sD;
-        for (int d = 0; d < 3; ++d) {
-            __syncthreads();
-            const int st = (d == 0) ? 1 : (d == 1) ? N1 : N1 * N1;
-            for (int it = tid; it < CPC * NP; it += NT) {
-                const int c = it / NP, node = it % NP;
-                const int pos = (node / st) % N1;
-                const int base = node - pos * st;
-                for (int s = 0; s < 5; ++s) {
-                    R v = R(0);
-                    for (int l = 0; l < N1; ++l) v += sOpsB[pos * N1 + l] * src[(c * 5 + s) * NP + base + l * st];
-                    dst[(c * 5 + s) * NP + node] = v;
+        for (int rep = 0; rep < (CURV ? 2 : 1); ++rep) {
+            if (rep == 1) {
+                __syncthreads();
+                for (int it = tid; it < CPC * 5 * NP; it += NT) {
+                    const int c = it / (5 * NP), node = it % NP;
+                    int cell = cell0 + c; if (cell >= a.nc) cell = a.nc - 1;
+                    src[it] = (R)((double)src[it] * __ldg(&a.metric[((size_t)cell * 10 + 9) * NP + node]));
                 }
             }
-            R* t = src; src = dst; dst = t;
+            for (int d = 0; d < 3; ++d) {
+                __syncthreads();
+                const int st = (d == 0) ? 1 : (d == 1) ? N1 : N1 * N1;
+                for (int it = tid; it < CPC * NP; it += NT) {
+                    const int c = it / NP, node = it % NP;
+                    const int pos = (node / st) % N1;
+                    const int base = node - pos * st;
+                    for (int s = 0; s < 5; ++s) {
+                        R v = R(0);
+                        for (int l = 0; l < N1; ++l) v += sOpsB[pos * N1 + l] * src[(c * 5 + s) * NP + base + l * st];
+                        dst[(c * 5 + s) * NP + node] = v;
+                    }
+                }
+                R* t = src; src = dst; dst = t;
+            }
         }
         __syncthreads();
         if (src != sA) {
@@ -887,7 +914,7 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
             const int node = (it % (5 * NP)) % NP;
             const size_t dof = (size_t)cell0 * 5 * NP + it;
             const double G = (double)sA[it];
-            const double k = CURV ? G * __ldg(&a.metric[((size_t)cell * 10 + 9) * NP + node]) : G * a.inv_h;
+            const double k = CURV ? (a.fr ? G : G * __ldg(&a.metric[((size_t)cell * 10 + 9) * NP + node])) : G * a.inv_h;
             const double sum = bs[r] + a.c_acc * k;
             if (a.acc_out) a.acc_out[dof] = sum;
             if (a.final_out) {
@@ -928,7 +955,7 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
             continue;
         }
         // affine: M^-1 R = G / h; curvilinear (cDG): R / (W det J) = G / det J
-        const double k = CURV ? G * __ldg(&a.metric[((size_t)cell * 10 + 9) * NP + node]) : G * a.inv_h;
+        const double k = CURV ? (a.fr ? G : G * __ldg(&a.metric[((size_t)cell * 10 + 9) * NP + node])) : G * a.inv_h;
         if (a.mode == 1) { a.out[dof] = k; continue; }
         if (a.mode == 3) {
             // LowStorageRungeKuttaODESolver stage (low_storage_runge_kutta_ode_solver.cpp:22-100):
@@ -1373,8 +1400,9 @@ static __global__ void quotient_selftest_kernel(unsigned long long seed, int n, 
 template <int N1>
 // metric != nullptr: curvilinear cDG cells, M^-1 = 1 / (W det J) per node (the weight-adjusted
 // inverse of dg_base.cpp:4217-4249 on collocated GLL nodes)
+// (curvilinear FR cells: the weight-adjusted B (x3) [ (1 / det J) (M+K)^-1 (x3) in ], fr != 0)
 __global__ void inverse_mass_kernel(const double* __restrict__ in, double* __restrict__ out, const OpTab* ops,
-                                    int nc, double inv_detj, const double* __restrict__ metric) {
+                                    int nc, double inv_detj, const double* __restrict__ metric, int fr) {
     constexpr int NP = N1 * N1 * N1;
     __shared__ double s0[5 * NP], s1[5 * NP], sM[N1 * N1];
     const int cell = blockIdx.x;
@@ -1394,6 +1422,25 @@ __global__ void inverse_mass_kernel(const double* __restrict__ in, double* __res
         double* t = src; src = dst; dst = t;
     }
     __syncthreads();
+    if (metric && fr) {
+        for (int i = threadIdx.x; i < 5 * NP; i += blockDim.x) src[i] *= metric[((size_t)cell * 10 + 9) * NP + i % NP];
+        for (int i = threadIdx.x; i < N1 * N1; i += blockDim.x) sM[i] = ops->B[(i / N1) * MAXN1 + (i % N1)];
+        for (int d = 0; d < 3; ++d) {
+            __syncthreads();
+            const int st = (d == 0) ? 1 : (d == 1) ? N1 : N1 * N1;
+            for (int i = threadIdx.x; i < 5 * NP; i += blockDim.x) {
+                const int node = i % NP, s = i / NP;
+                const int pos = (node / st) % N1, base = node - pos * st;
+                double v = 0.0;
+                for (int l = 0; l < N1; ++l) v += sM[pos * N1 + l] * src[s * NP + base + l * st];
+                dst[i] = v;
+            }
+            double* t = src; src = dst; dst = t;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < 5 * NP; i += blockDim.x) out[(size_t)cell * 5 * NP + i] = src[i];
+        return;
+    }
     for (int i = threadIdx.x; i < 5 * NP; i += blockDim.x)
         out[(size_t)cell * 5 * NP + i] = src[i] * (metric ? metric[((size_t)cell * 10 + 9) * NP + i % NP] : inv_detj);
 }

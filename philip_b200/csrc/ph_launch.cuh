@@ -21,7 +21,7 @@ cudaError_t launch_aux(const double* U, const int* nbr, const OpTab& ops, int ce
 // DGBase::apply_inverse_global_mass_matrix on its own
 template <int N1>
 cudaError_t launch_inverse_mass(const double* in, double* out, const OpTab* ops, int nc, double inv_detj,
-                                const double* metric, cudaStream_t s);
+                                const double* metric, int fr, cudaStream_t s);
 // Taylor-Green integrals, per-cell partial sums (integral_partials<full>() per cell)
 // X: node coordinates [nc][3][NP] of curvilinear cells, nullptr on affine meshes;
 // origin: lower corner [nc][3] of affine cells (the full set's angular momentum)

@@ -351,3 +351,59 @@ def test_curvilinear_gl_free_stream_and_steps():
         err = rel_max_err(dg.solution, U)
         print(f"curvilinear GL RK4 step {step}: rel err {err:.3e}")
         assert err <= 1e-12 and dg.status() == 0
+
+
+# ------------------------------------------------------------------------------- GLL: FR and the conservative form
+
+GLL_FR_CASES = [
+    ("conservative_roe_cdg_p3", dict(poly_degree=3, n_cells=3, split=False, conv="roe")),
+    ("conservative_lxf_chu_p2", dict(poly_degree=2, n_cells=3, split=False, conv="lax_friedrichs", fr="cHU")),
+    ("split_CH_roe_chu_p4", dict(poly_degree=4, n_cells=2, fr="cHU")),
+    ("split_IR_ec_cplus_p5", dict(poly_degree=5, n_cells=2, two_point="IR", conv="two_point_flux", fr="cPlus")),
+    ("ns_split_br2_csd_p3", dict(poly_degree=3, n_cells=3, pde="navier_stokes", diss="bassi_rebay_2", fr="cSD")),
+    ("ns_conservative_central_cdg_p2", dict(poly_degree=2, n_cells=3, pde="navier_stokes", diss="central_visc_flux",
+                                            split=False, conv="roe")),
+]
+
+
+def test_oracle_conservative_form_preserves_free_stream_on_the_warped_mesh():
+    _, orc = _oracle(dict(poly_degree=3, n_cells=3, split=False, conv="roe"), WARP)
+    R = orc.residual(_uniform_state(orc))
+    scale = np.max(np.abs(orc.residual(orc.initial_condition("tgv"))))
+    assert np.max(np.abs(R)) <= 1e-11 * scale
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,kw", GLL_FR_CASES, ids=[c[0] for c in GLL_FR_CASES])
+def test_curvilinear_fr_and_conservative_parity(name, kw):
+    """FR (cHU / cSD / cPlus) on curvilinear cells takes the weight-adjusted inverse mass
+    B (x3) [(1 / det J) B (x3) G] with B = (M+K)^-1 W (dg_base.cpp:4217-4249 on collocated GLL
+    nodes); the conservative form the contravariant fluxes F . C[:, d]."""
+    prm, orc, dg = _pair(kw)
+    U = perturbed_tgv(orc, seed=len(name))
+    R_orc = orc.residual(U)
+    err = rel_max_err(dg.residual_of(U), R_orc)
+    k_gpu = np.empty_like(R_orc)
+    dg.apply_inverse_global_mass_matrix(R_orc, k_gpu)
+    err_m = rel_max_err(k_gpu, orc.inverse_mass(R_orc))
+    print(f"{name}: curvilinear residual rel max err {err:.3e}, inverse mass {err_m:.3e}")
+    assert err <= RTOL and err_m <= RTOL
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_curvilinear_fr_steps(precision):
+    from philip_b200 import _lib
+    from philip_b200.dg import RungeKuttaODESolver
+    prec = _lib.PH_FP64 if precision == "fp64" else _lib.PH_FP32_RESIDUAL
+    prm, orc, dg = _pair(dict(poly_degree=3, n_cells=3, fr="cHU"), precision=prec)
+    U = orc.initial_condition("tgv")
+    dg.solution = U
+    dt = 0.1 * TWO_PI / 12 / 11.0
+    ode = RungeKuttaODESolver(dg)
+    for step in range(3):
+        orc.rk_step(U, dt)
+        ode.step_in_time(dt)
+    err = rel_max_err(dg.solution, U)
+    print(f"curvilinear cHU {precision}: three RK4 steps rel err {err:.3e}")
+    assert err <= (1e-12 if precision == "fp64" else 1e-6)
