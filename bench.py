@@ -375,6 +375,44 @@ def one_at_a_time(reqs):
             "dof_updates_per_s_stage": work / el, "dtype": "f64", "path": "single-solve context per solve"}
 
 
+def served_sample(count: int = 24, rate: float = 50.0, budget_gb: float = 32.0, chunk: int = 16):
+    """A bounded sample of the served snapshot stream beside the default line: the first `count`
+    seeded requests of the served_stream workload arriving at its Poisson rate, served by the
+    library's native loop in the precision form, then the same solves one at a time in FP64.
+    Returns solves/s, p50 / p99 latency and the ratio to one at a time."""
+    from philip_b200 import _lib
+    from philip_b200.serve import Server, autotune, poisson_arrivals, serve_native
+    prec = _lib.PH_FP32_RESIDUAL
+    reqs = many_requests("served_stream", count)
+    arrivals = list(poisson_arrivals(rate, count, np.random.default_rng(7)))
+    tuned = {}
+    for r in reqs:   # tile shapes per (order, mesh kind) and the requests' payloads, before the clock
+        key = (r.poly_degree, r.warp != 0.0)
+        if key not in tuned:
+            tuned[key] = autotune(r.poly_degree, prec, key[1])
+        r.prepare()
+    warm = Server(1 << 28, prec, chunk=chunk)
+    serve_native(warm, [(0.0, many_requests("served_stream", 1, seed=1)[0])])
+    warm.close()
+    srv = Server(int(budget_gb * (1 << 30)), prec, chunk=chunk)
+    stats = serve_native(srv, list(zip(arrivals, reqs)))
+    srv.close()
+    lat = sorted(c.latency for c in stats.completed)
+
+    def pct(q):
+        return lat[min(len(lat) - 1, max(0, int(np.ceil(q / 100.0 * len(lat))) - 1))]
+    work = sum(c.request.ndofs * 4 * c.steps for c in stats.completed)
+    base = one_at_a_time(reqs)
+    served = {"solves_per_s": len(lat) / stats.makespan, "dof_updates_per_s_stage": work / stats.makespan,
+              "makespan_s": stats.makespan, "latency_ms": {"p50": 1e3 * pct(50), "p99": 1e3 * pct(99)},
+              "dtype": "f32-residual/f64-state", "server": "ph_server (native worker thread)"}
+    return {"workload": "served_stream", "requests": count, "arrival_rate_per_s": rate,
+            "description": "the first %d requests of the served_stream workload (%s)" % (count, MANY["served_stream"]),
+            "served": served, "one_at_a_time": base,
+            "speedup_vs_one_at_a_time": served["dof_updates_per_s_stage"] / base["dof_updates_per_s_stage"],
+            "status_flags": int(np.bitwise_or.reduce([c.status for c in stats.completed]))}
+
+
 def run_many(args, rank: int = 0, world: int = 1, local_rank: int = 0):
     """Batched (all admitted at t=0) or served (Poisson arrivals, continuous batching) form.
     With N GPUs every rank serves a cost-balanced share of the same requests (by solve; no
@@ -587,6 +625,8 @@ def main():
                     help="batched / served forms: solves in the one-at-a-time FP64 comparison (0 = all)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-served-sample", action="store_true",
+                    help="TGV workloads: skip the bounded served-stream sample reported beside the line")
     ap.add_argument("--server", default="native", choices=["native", "python"],
                     help="batched / served forms: the library's serving loop or the Python one")
     ap.add_argument("--shard", default="replicas", choices=["replicas", "slab"],
@@ -787,6 +827,11 @@ def main():
                                  "alg_bytes_per_dof": bpd, "peak_source": peak_src}},
             "clocks": clk.summary(),
         }
+        if world == 1 and not args.no_served_sample and not slab:
+            try:   # a bounded sample of the served form beside the headline (not part of `value`)
+                line["served_sample"] = served_sample()
+            except Exception as e:
+                line["served_sample"] = {"error": str(e)}
         if world == 1 and not args.no_cpu_baseline:
             try:
                 line["cpu_baseline"] = cpu_baseline(args.workload)
