@@ -399,26 +399,30 @@ struct GlAuxLayout {
     static constexpr int nTab = (int)(sizeof(GlTab) / sizeof(double));
     static constexpr int oU = nTab;                      // 5 NQ^3: the state, later the projected state
     static constexpr int oQ = oU + 5 * Q3;               // 5 NQ^3: state at the flux nodes
-    static constexpr int oG = oQ + 5 * Q3;               // 5 NQ^3: one direction's bracket [.] above
-    static constexpr int oAQ = oG + 5 * Q3;              // 15 NQ^3: lifted gradient at the flux nodes
-    static constexpr int oF = oAQ + 15 * Q3;             // 12 NQ^3: volume viscous flux (first: face terms)
+    static constexpr int oAQ = oQ + 5 * Q3;              // 15 NQ^3: lifted gradient at the flux nodes
+    static constexpr int oF = oAQ + 15 * Q3;             // 12 NQ^3: volume viscous flux
     static constexpr int nT = gl_temp<ND, NQ>();
     static constexpr int oT0 = oF + 12 * Q3, oT1 = oT0 + nT;
     static constexpr int total = oT1 + nT;
     static constexpr size_t bytes = (size_t)total * sizeof(double);
-    static_assert(12 * Q3 >= 10 * NF, "the face terms of one direction fit the flux buffer");
+    static_assert(nT >= 30 * NF, "the six faces' terms fit a temporary");
 };
 
-// one direction of the lifted gradient (see above); ends with a barrier
-template <int ND, int NQ, bool SPLIT, int D>
-__device__ __forceinline__ void gl_aux_direction(const StageArgs& a, const GlArgs& g, const GlTab& T,
-                                                 const GlTab* tab, int cell, const double* sQ, double* sG,
-                                                 double* face, double* sAQ, double* t0, double* t1) {
+// the lifted gradient of all three directions at once (see above), into sAQ[s * 3 + d][Q3]:
+// the flux-node derivatives, the six faces' terms, the brackets, then H (x) H (x) H as three
+// passes over all fifteen components in place (H is square: each line is read whole before it
+// is written). Ends with a barrier.
+template <int ND, int NQ, bool SPLIT>
+__device__ __forceinline__ void gl_aux_gradient(const StageArgs& a, const GlArgs& g, const GlTab& T,
+                                                const GlTab* tab, int cell, const double* sQ, double* face,
+                                                double* sAQ) {
     using L = GlAuxLayout<ND, NQ, SPLIT>;
     constexpr int NT = L::NT, Q3 = L::Q3, NF = L::NF, T1W = gl_t1_width<SPLIT>();
-    gl_line<NT, NQ, NQ, D, NQ, NQ, NQ, 5>(T.dphi, sQ, Q3, sG, Q3, 1.0, false);
-    for (int it = threadIdx.x; it < 2 * 5 * NF; it += NT) {   // faces 2D, 2D + 1: W_face (u* - u) n_D
-        const int f = 2 * D + it / (5 * NF), s = (it / NF) % 5, q2 = it % NF;
+    gl_line<NT, NQ, NQ, 0, NQ, NQ, NQ, 5>(T.dphi, sQ, Q3, sAQ + 0 * Q3, 3 * Q3, 1.0, false);
+    gl_line<NT, NQ, NQ, 1, NQ, NQ, NQ, 5>(T.dphi, sQ, Q3, sAQ + 1 * Q3, 3 * Q3, 1.0, false);
+    gl_line<NT, NQ, NQ, 2, NQ, NQ, NQ, 5>(T.dphi, sQ, Q3, sAQ + 2 * Q3, 3 * Q3, 1.0, false);
+    for (int it = threadIdx.x; it < 6 * 5 * NF; it += NT) {   // face[f][s][q2] = W_face (u* - u) n_{f/2}
+        const int f = it / (5 * NF), s = (it / NF) % 5, q2 = it % NF;
         const int cn = __ldg(&a.nbr[cell * 6 + f]);
         const double uo = __ldg(&g.t1[(((size_t)cell * 6 + f) * T1W + s) * NF + q2]);
         const double ue = __ldg(&g.t1[(((size_t)cn * 6 + (f ^ 1)) * T1W + s) * NF + q2]);
@@ -426,16 +430,22 @@ __device__ __forceinline__ void gl_aux_direction(const StageArgs& a, const GlArg
         face[it] = tab->wq[q2 % NQ] * tab->wq[q2 / NQ] * ((0.5 * (uo + ue) - uo) * sgn);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < 5 * Q3; i += NT) {
-        const int s = i / Q3, q = i - s * Q3;
+    for (int i = threadIdx.x; i < 15 * Q3; i += NT) {
+        const int k = i / Q3, q = i - k * Q3, s = k / 3, d = k - 3 * s;
         const int c[3] = {q % NQ, (q / NQ) % NQ, q / NF};
-        constexpr int A1 = D == 0 ? 1 : 0, A2 = D == 2 ? 1 : 2;
-        const int q2 = c[A2] * NQ + c[A1];
-        sG[i] = tab->wq[c[0]] * tab->wq[c[1]] * tab->wq[c[2]] * sG[i] + tab->phis[0][c[D]] * face[s * NF + q2] +
-                tab->phis[1][c[D]] * face[(5 + s) * NF + q2];
+        const int a1 = d == 0 ? 1 : 0, a2 = d == 2 ? 1 : 2;
+        const int q2 = c[a2] * NQ + c[a1];
+        sAQ[i] = tab->wq[c[0]] * tab->wq[c[1]] * tab->wq[c[2]] * sAQ[i] +
+                 tab->phis[0][c[d]] * face[((2 * d) * 5 + s) * NF + q2] +
+                 tab->phis[1][c[d]] * face[((2 * d + 1) * 5 + s) * NF + q2];
     }
     __syncthreads();
-    gl_apply3<NT, NQ, NQ, 5>(T.haux, sG, Q3, sAQ + D * Q3, 3 * Q3, t0, t1, a.inv_h, false);
+    gl_line<NT, NQ, NQ, 0, NQ, NQ, NQ, 15>(T.haux, sAQ, Q3, sAQ, Q3, 1.0, false);
+    __syncthreads();
+    gl_line<NT, NQ, NQ, 1, NQ, NQ, NQ, 15>(T.haux, sAQ, Q3, sAQ, Q3, 1.0, false);
+    __syncthreads();
+    gl_line<NT, NQ, NQ, 2, NQ, NQ, NQ, 15>(T.haux, sAQ, Q3, sAQ, Q3, a.inv_h, false);
+    __syncthreads();
 }
 
 template <int ND, int NQ, bool SPLIT>
@@ -448,7 +458,6 @@ gl_aux_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab T
     GlTab* tab = reinterpret_cast<GlTab*>(sm);
     double* sU = sm + L::oU;
     double* sQ = sm + L::oQ;
-    double* sG = sm + L::oG;
     double* sAQ = sm + L::oAQ;
     double* sF = sm + L::oF;
     double* t0 = sm + L::oT0;
@@ -460,9 +469,7 @@ gl_aux_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab T
     for (int i = threadIdx.x; i < 5 * D3; i += NT) sU[i] = __ldg(&a.U[(size_t)cell * 5 * D3 + i]);
     __syncthreads();
     gl_apply3<NT, NQ, ND, 5>(T.chi, sU, D3, sQ, Q3, t0, t1, 1.0, false);
-    gl_aux_direction<ND, NQ, SPLIT, 0>(a, g, T, tab, cell, sQ, sG, sF, sAQ, t0, t1);
-    gl_aux_direction<ND, NQ, SPLIT, 1>(a, g, T, tab, cell, sQ, sG, sF, sAQ, t0, t1);
-    gl_aux_direction<ND, NQ, SPLIT, 2>(a, g, T, tab, cell, sQ, sG, sF, sAQ, t0, t1);
+    gl_aux_gradient<ND, NQ, SPLIT>(a, g, T, tab, cell, sQ, t0, sAQ);
     // per face node of the cell: F_v(u, q) . e_dn with the state's and the gradient's face values
     // (each side's half of the dissipative numerical flux, strong_dg.cpp:3354-3452)
     double* tout = g.t2 + (size_t)cell * 6 * GL_T2W * NF;
