@@ -418,7 +418,6 @@ const char* uncollocated_reason(const ph_mesh_desc* mesh, const ph_params* prm) 
         if (prm->pde_type != 0) return "uncollocated flux nodes on curvilinear meshes take the Euler equations";
     }
     if (prm->precision != PH_FP64) return "uncollocated flux nodes take the FP64 path";
-    if (prm->runge_kutta_method > 3) return "uncollocated flux nodes take the Butcher RK methods";
     if (prm->use_relaxation_runge_kutta) return "uncollocated flux nodes: no relaxation RK";
     return nullptr;
 }
@@ -1797,6 +1796,7 @@ static int rk_one_step(ph_ctx* c, double dt) {
 
 // tiles (CTAs) of one stage-kernel launch
 static int stage_tiles(const ph_ctx* c) {
+    if (c->gl) return c->nc;   // the uncollocated kernels: one cell per CTA
     int threads = 0, cpc = 1;
     size_t smem = 0;
     switch (c->N1) {
@@ -2185,17 +2185,7 @@ int ph_run(ph_ctx* c, double dt, int nsteps, int record_every, double* rows) {
 int ph_rk_error_norm(ph_ctx* c, double* w) {
     if (!c || !w) return fail(PH_ERR_INVALID, "null argument");
     if (!c->lowstorage) return fail(PH_ERR_INVALID, "the error estimate belongs to the low-storage methods");
-    int threads = 0, cpc = 1;
-    size_t smem = 0;
-    switch (c->N1) {
-    case 2: ph::stage_launch_shape<2>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
-    case 3: ph::stage_launch_shape<3>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
-    case 4: ph::stage_launch_shape<4>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
-    case 5: ph::stage_launch_shape<5>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
-    case 6: ph::stage_launch_shape<6>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
-    default: ph::stage_launch_shape<7>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
-    }
-    const int tiles = (c->nc + cpc - 1) / cpc;
+    const int tiles = stage_tiles(c);   // one partial per stage-kernel tile
     std::vector<double> part(tiles);
     PH_CUDA(cudaMemcpyAsync(part.data(), c->d_err, tiles * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     PH_CUDA(cudaStreamSynchronize(c->stream));

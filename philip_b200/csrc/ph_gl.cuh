@@ -980,6 +980,12 @@ gl_stage_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab
         for (int i = threadIdx.x; i < 5 * D3; i += NT) a.out[(size_t)cell * 5 * D3 + i] = sQ[i];
         return;
     }
+    if (a.mode == 3) {   // low-storage 3S* / 3S*+ stage (as the collocated kernel's)
+        double err2 = 0.0;
+        for (int i = threadIdx.x; i < 5 * D3; i += NT) ls_stage_dof(a, (size_t)cell * 5 * D3 + i, sQ[i], err2);
+        if (a.err_partial) ls_tile_error<NT>(err2, &a.err_partial[cell]);
+        return;
+    }
     // Butcher RK stage (as the collocated kernel's epilogue)
     for (int i = threadIdx.x; i < 5 * D3; i += NT) {
         const size_t dof = (size_t)cell * 5 * D3 + i;

@@ -608,6 +608,54 @@ __device__ __forceinline__ void prefetch_tile_l2(const StageArgs& a, int cell0) 
 // residual_tile does the work of one CTA on the tile of CPC cells starting at cell0;
 // residual_kernel runs one tile per CTA of one discretisation, residual_kernel_batched
 // runs the tiles of many independent discretisations (a batch of solves) from a tile list.
+// One DOF of a low-storage 3S* / 3S*+ stage (mode 3; LowStorageRungeKuttaODESolver stage,
+// low_storage_runge_kutta_ode_solver.cpp:22-100): S2 += delta_i S1; S1 = g0 S1 + g1 S2 + g2 S3 +
+// beta dt k; S4 += bhat_i dt k; the DOF's squared scaled error added to err2.
+__device__ __forceinline__ void ls_stage_dof(const StageArgs& a, size_t dof, double k, double& err2) {
+    const double s1 = a.U[dof];
+    const double s3 = a.ls_s3[dof];
+    const double kdt = a.dt * k;
+    double e = 0.0, ref = 0.0;
+    bool have_err = false;
+    if (a.ls_s1_out) {
+        const double s2 = (a.ls_first ? 0.0 : a.ls_s2[dof]) + a.ls_delta * s1;
+        const double s1n = ((a.ls_g0 * s1 + a.ls_g1 * s2) + a.ls_g2 * s3) + a.ls_beta * kdt;
+        a.ls_s1_out[dof] = s1n;
+        if (a.ls_embedded) {   // embedded solution of the last 3S* stage
+            const double s2e = ((s2 + a.ls_delta_s * s1n) + a.ls_delta_s1 * s3) * a.ls_inv_sum_delta;
+            a.ls_s2[dof] = s2e;
+            e = s1n - s2e; ref = fmax(fabs(s1n), fabs(s2e)); have_err = true;
+        } else {
+            a.ls_s2[dof] = s2;
+        }
+    }
+    if (a.ls_s4) {
+        const double s4 = (a.ls_first ? s3 : a.ls_s4[dof]) + a.ls_bhat * kdt;
+        a.ls_s4[dof] = s4;
+        if (!a.ls_s1_out) { e = s1 - s4; ref = fmax(fabs(s1), fabs(s4)); have_err = true; }
+    }
+    if (have_err && a.err_partial) {
+        const double r = e / (a.atol + a.rtol * ref);
+        err2 += r * r;
+    }
+}
+
+// the block's sum of err2 (warp shuffles, then the warps in order) into *out: a tile's squared
+// scaled error, summed in a fixed order
+template <int NT>
+__device__ __forceinline__ void ls_tile_error(double err2, double* out) {
+    __shared__ double red[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) err2 += __shfl_down_sync(0xffffffffu, err2, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = err2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (NT + 31) / 32; ++w) t += red[w];
+        *out = t;
+    }
+}
+
 template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int FS, bool CURV, bool BULK = false>
 __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell0) {
     static_assert(!BULK || (std::is_same<R, double>::value && N1 % 2 == 0 && !CURV), "bulk staging: FP64, even N1");
@@ -954,53 +1002,16 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
             a.out[dof] = CURV ? W * G : W * a.h * a.h * G;
             continue;
         }
-        // affine: M^-1 R = G / h; curvilinear (cDG): R / (W det J) = G / det J
+        // affine: M^-1 R = G / h; curvilinear: R / (W det J) = G / det J (cDG), or the weight-adjusted
+        // passes above, which applied 1 / det J already (FR)
         const double k = CURV ? (a.fr ? G : G * __ldg(&a.metric[((size_t)cell * 10 + 9) * NP + node])) : G * a.inv_h;
         if (a.mode == 1) { a.out[dof] = k; continue; }
         if (a.mode == 3) {
-            // LowStorageRungeKuttaODESolver stage (low_storage_runge_kutta_ode_solver.cpp:22-100):
-            // S2 += delta_i S1; S1 = g0 S1 + g1 S2 + g2 S3 + beta dt k; S4 += bhat_i dt k
-            const double s1 = a.U[dof];
-            const double s3 = a.ls_s3[dof];
-            const double kdt = a.dt * k;
-            double e = 0.0, ref = 0.0;
-            bool have_err = false;
-            if (a.ls_s1_out) {
-                const double s2 = (a.ls_first ? 0.0 : a.ls_s2[dof]) + a.ls_delta * s1;
-                const double s1n = ((a.ls_g0 * s1 + a.ls_g1 * s2) + a.ls_g2 * s3) + a.ls_beta * kdt;
-                a.ls_s1_out[dof] = s1n;
-                if (a.ls_embedded) {   // embedded solution of the last 3S* stage
-                    const double s2e = ((s2 + a.ls_delta_s * s1n) + a.ls_delta_s1 * s3) * a.ls_inv_sum_delta;
-                    a.ls_s2[dof] = s2e;
-                    e = s1n - s2e; ref = fmax(fabs(s1n), fabs(s2e)); have_err = true;
-                } else {
-                    a.ls_s2[dof] = s2;
-                }
-            }
-            if (a.ls_s4) {
-                const double s4 = (a.ls_first ? s3 : a.ls_s4[dof]) + a.ls_bhat * kdt;
-                a.ls_s4[dof] = s4;
-                if (!a.ls_s1_out) { e = s1 - s4; ref = fmax(fabs(s1), fabs(s4)); have_err = true; }
-            }
-            if (have_err && a.err_partial) {
-                const double r = e / (a.atol + a.rtol * ref);
-                err2 += r * r;
-            }
+            ls_stage_dof(a, dof, k, err2);
             continue;
         }
     }
-    if (a.mode == 3 && a.err_partial) {   // tile sum of the squared scaled error, fixed order
-        __shared__ double red[32];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) err2 += __shfl_down_sync(0xffffffffu, err2, o);
-        if ((tid & 31) == 0) red[tid >> 5] = err2;
-        __syncthreads();
-        if (tid == 0) {
-            double t = 0.0;
-            for (int w = 0; w < (NT + 31) / 32; ++w) t += red[w];
-            a.err_partial[cell0 / CPC] = t;
-        }
-    }
+    if (a.mode == 3 && a.err_partial) ls_tile_error<NT>(err2, &a.err_partial[cell0 / CPC]);
 }
 
 template <typename R, int N1, int CPC, bool VISC, bool SPLIT, bool CURV>

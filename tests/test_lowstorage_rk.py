@@ -62,3 +62,34 @@ def test_lowstorage_steps_and_error_match_oracle(rk, order, visc):
         assert err <= 1e-12
         assert abs(w_gpu - w_orc) <= 1e-8 * abs(w_orc) + 1e-300
         assert dg.status() == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rk,nodes,over,visc", [("RK3_2_5F_3SStarPlus", "GL", 0, True),
+                                                ("RK4_3_5_3SStar", "GL", 0, False),
+                                                ("RK5_4_10F_3SStarPlus", "GLL", 1, True)],
+                         ids=["gl_ns_rk3_2_5f", "gl_euler_rk4_3_5", "gll_overint1_ns_rk5_4_10f"])
+def test_lowstorage_on_uncollocated_flux_nodes(rk, nodes, over, visc):
+    """The low-storage stage update and its error reduction in the uncollocated stage kernel's
+    epilogue (one tile per cell): steps and error norm against the oracle."""
+    from philip_b200.dg import DGStrong, RungeKuttaODESolver
+    d = prm_dict(rk=rk, poly_degree=3, n_cells=2, pde="navier_stokes" if visc else "euler", diss="bassi_rebay_2")
+    d["flux_nodes_type"] = nodes
+    d["overintegration"] = over
+    prm = Parameters.from_dict(d)
+    orc = Oracle(prm.oracle_cfg(), prm.n_cells, *prm.grid_bounds)
+    dg = DGStrong(prm)
+    ode = RungeKuttaODESolver(dg)
+    U = perturbed_tgv(orc, seed=6, amp=0.005)
+    dg.solution = U
+    dt = 0.1 * TWO_PI / 8 / 11.0
+    for step in range(3):
+        orc.rk_step(U, dt)
+        ode.step_in_time(dt)
+        err = rel_max_err(dg.solution, U)
+        w_gpu, w_orc = ode.error_norm(), orc.rk_error()
+        print(f"{rk} {nodes} overint {over} step {step}: state rel err {err:.3e}, error norm {w_gpu:.6e} "
+              f"vs {w_orc:.6e}")
+        assert err <= 1e-12
+        assert abs(w_gpu - w_orc) <= 1e-8 * abs(w_orc) + 1e-300
+        assert dg.status() == 0
