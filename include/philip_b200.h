@@ -115,8 +115,8 @@ typedef struct ph_mesh_desc {
      * l = left; zero on the cube's faces, so periodic faces still match), through a mapping
      * of degree grid_degree on GLL support points. The GPU path takes grid_degree =
      * poly_degree; split or conservative, any FR type (the weight-adjusted inverse mass);
-     * Navier-Stokes on GLL flux nodes without overintegration, with bassi_rebay_2 or
-     * central_visc_flux and kDG; the Euler equations on GL flux nodes or with overintegration.
+     * GLL or GL flux nodes, overintegration 0..2; Navier-Stokes with bassi_rebay_2 or
+     * central_visc_flux and flux_reconstruction_aux = kDG.
      * Not a reference grid:
      * the construction follows the reference's curved periodic grids
      * (src/mesh/grids/curved_periodic_grid.cpp) with this warp. */

@@ -415,7 +415,11 @@ const char* uncollocated_reason(const ph_mesh_desc* mesh, const ph_params* prm) 
     if (is_curvilinear(mesh)) {
         if (mesh->mapping_support_points == nullptr && mesh->grid_degree != prm->poly_degree)
             return "curvilinear meshes take grid_degree = poly_degree";
-        if (prm->pde_type != 0) return "uncollocated flux nodes on curvilinear meshes take the Euler equations";
+        if (prm->pde_type != 0 && prm->diss_num_flux == 0)
+            return "curvilinear Navier-Stokes takes bassi_rebay_2 or central_visc_flux (the SIPG penalty's cell "
+                   "extent on curved cells is not restated)";
+        if (prm->pde_type != 0 && prm->flux_reconstruction_aux != 0)
+            return "curvilinear Navier-Stokes takes flux_reconstruction_aux = kDG";
     }
     if (prm->precision != PH_FP64) return "uncollocated flux nodes take the FP64 path";
     if (prm->use_relaxation_runge_kutta) return "uncollocated flux nodes: no relaxation RK";

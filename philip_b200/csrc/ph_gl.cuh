@@ -412,7 +412,7 @@ struct GlAuxLayout {
 // the flux-node derivatives, the six faces' terms, the brackets, then H (x) H (x) H as three
 // passes over all fifteen components in place (H is square: each line is read whole before it
 // is written). Ends with a barrier.
-template <int ND, int NQ, bool SPLIT>
+template <int ND, int NQ, bool SPLIT, bool CURV = false>
 __device__ __forceinline__ void gl_aux_gradient(const StageArgs& a, const GlArgs& g, const GlTab& T,
                                                 const GlTab* tab, int cell, const double* sQ, double* face,
                                                 double* sAQ) {
@@ -430,6 +430,56 @@ __device__ __forceinline__ void gl_aux_gradient(const StageArgs& a, const GlArgs
         face[it] = tab->wq[q2 % NQ] * tab->wq[q2 / NQ] * ((0.5 * (uo + ue) - uo) * sgn);
     }
     __syncthreads();
+    if constexpr (CURV) {
+        // physical components: W sum_j C[d][j] D_j u at the volume flux nodes, and every face's
+        // lift (u* - u) (C_face[:, dn])_d (each face reaches every component on a curved cell)
+        const double* vm = g.vmet + (size_t)cell * 10 * Q3;
+        const double* fm = g.fnrm + (size_t)cell * 18 * NF;
+        for (int i = threadIdx.x; i < 5 * Q3; i += NT) {
+            const int s = i / Q3, q = i - s * Q3;
+            const int c[3] = {q % NQ, (q / NQ) % NQ, q / NF};
+            const double W = tab->wq[c[0]] * tab->wq[c[1]] * tab->wq[c[2]];
+            double r[3], b[3];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) r[j] = sAQ[(s * 3 + j) * Q3 + q];
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+                b[d] = W * (__ldg(&vm[(d * 3 + 0) * Q3 + q]) * r[0] + __ldg(&vm[(d * 3 + 1) * Q3 + q]) * r[1] +
+                            __ldg(&vm[(d * 3 + 2) * Q3 + q]) * r[2]);
+#pragma unroll
+            for (int dn = 0; dn < 3; ++dn) {
+                const int a1 = dn == 0 ? 1 : 0, a2 = dn == 2 ? 1 : 2;
+                const int q2 = c[a2] * NQ + c[a1];
+                const double l0 = tab->phis[0][c[dn]] * face[((2 * dn) * 5 + s) * NF + q2];
+                const double l1 = tab->phis[1][c[dn]] * face[((2 * dn + 1) * 5 + s) * NF + q2];
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+                    b[d] += l0 * __ldg(&fm[((2 * dn) * 3 + d) * NF + q2]) + l1 * __ldg(&fm[((2 * dn + 1) * 3 + d) * NF + q2]);
+            }
+#pragma unroll
+            for (int d = 0; d < 3; ++d) sAQ[(s * 3 + d) * Q3 + q] = b[d];
+        }
+        __syncthreads();
+        // the weight-adjusted inverse at the flux nodes: H (x3) [ (W / det J) H (x3) b ]
+        gl_line<NT, NQ, NQ, 0, NQ, NQ, NQ, 15>(T.haux, sAQ, Q3, sAQ, Q3, 1.0, false);
+        __syncthreads();
+        gl_line<NT, NQ, NQ, 1, NQ, NQ, NQ, 15>(T.haux, sAQ, Q3, sAQ, Q3, 1.0, false);
+        __syncthreads();
+        gl_line<NT, NQ, NQ, 2, NQ, NQ, NQ, 15>(T.haux, sAQ, Q3, sAQ, Q3, 1.0, false);
+        __syncthreads();
+        for (int i = threadIdx.x; i < 15 * Q3; i += NT) {
+            const int q = i % Q3;
+            sAQ[i] *= tab->wq[q % NQ] * tab->wq[(q / NQ) % NQ] * tab->wq[q / NF] * __ldg(&vm[9 * Q3 + q]);
+        }
+        __syncthreads();
+        gl_line<NT, NQ, NQ, 0, NQ, NQ, NQ, 15>(T.haux, sAQ, Q3, sAQ, Q3, 1.0, false);
+        __syncthreads();
+        gl_line<NT, NQ, NQ, 1, NQ, NQ, NQ, 15>(T.haux, sAQ, Q3, sAQ, Q3, 1.0, false);
+        __syncthreads();
+        gl_line<NT, NQ, NQ, 2, NQ, NQ, NQ, 15>(T.haux, sAQ, Q3, sAQ, Q3, 1.0, false);
+        __syncthreads();
+        return;
+    }
     for (int i = threadIdx.x; i < 15 * Q3; i += NT) {
         const int k = i / Q3, q = i - k * Q3, s = k / 3, d = k - 3 * s;
         const int c[3] = {q % NQ, (q / NQ) % NQ, q / NF};
@@ -448,7 +498,26 @@ __device__ __forceinline__ void gl_aux_gradient(const StageArgs& a, const GlArgs
     __syncthreads();
 }
 
-template <int ND, int NQ, bool SPLIT>
+// the contravariant viscous flux F~_j = sum_m C[m][j] F_m at volume flux node q (curvilinear)
+__device__ __forceinline__ void gl_contravariant(const double* vm, int q, int Q3, double F[3][4]) {
+    double C[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) C[i] = __ldg(&vm[i * Q3 + q]);
+    double Ft[3][4];
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) Ft[j][k] = C[0 * 3 + j] * F[0][k] + C[1 * 3 + j] * F[1][k] + C[2 * 3 + j] * F[2][k];
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) F[j][k] = Ft[j][k];
+}
+
+// CURV: curvilinear cells (the metric at the flux nodes, g.vmet / g.fnrm): the physical
+// gradient through the weight-adjusted inverse (gl_aux_gradient), contravariant volume fluxes,
+// and each face node's F_v . C_face[:, dn] (the metric-scaled normal flux)
+template <int ND, int NQ, bool SPLIT, bool CURV = false>
 __global__ void __launch_bounds__(gl_threads<NQ>(), 2)
 gl_aux_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab T) {
     using L = GlAuxLayout<ND, NQ, SPLIT>;
@@ -469,7 +538,8 @@ gl_aux_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab T
     for (int i = threadIdx.x; i < 5 * D3; i += NT) sU[i] = __ldg(&a.U[(size_t)cell * 5 * D3 + i]);
     __syncthreads();
     gl_apply3<NT, NQ, ND, 5>(T.chi, sU, D3, sQ, Q3, t0, t1, 1.0, false);
-    gl_aux_gradient<ND, NQ, SPLIT>(a, g, T, tab, cell, sQ, t0, sAQ);
+    gl_aux_gradient<ND, NQ, SPLIT, CURV>(a, g, T, tab, cell, sQ, t0, sAQ);
+    const double* vm = CURV ? g.vmet + (size_t)cell * 10 * Q3 : nullptr;
     // per face node of the cell: F_v(u, q) . e_dn with the state's and the gradient's face values
     // (each side's half of the dissipative numerical flux, strong_dg.cpp:3354-3452)
     double* tout = g.t2 + (size_t)cell * 6 * GL_T2W * NF;
@@ -490,6 +560,14 @@ gl_aux_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab T
             }
         }
         double F[3][4];
+        if constexpr (CURV) {   // F_v . C_face[:, dn]
+            viscous_flux<double>(r, gq, ucv, cst, F, 7, nullptr);
+            const double* m = g.fnrm + ((size_t)cell * 6 + f) * 3 * NF + q2;
+            const double m0 = __ldg(&m[0]), m1 = __ldg(&m[NF]), m2 = __ldg(&m[2 * NF]);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) tout[(f * GL_T2W + k) * NF + q2] = m0 * F[0][k] + m1 * F[1][k] + m2 * F[2][k];
+            continue;
+        }
         viscous_flux<double>(r, gq, ucv, cst, F, 1 << dn, nullptr);
 #pragma unroll
         for (int k = 0; k < 4; ++k)   // (selects, not a run-time index, keep F in registers)
@@ -530,6 +608,7 @@ gl_aux_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab T
         }
         double F[3][4];
         viscous_flux<double>(u, gq, ucv, cst, F, 7, nullptr);
+        if constexpr (CURV) gl_contravariant(vm, q, Q3, F);
 #pragma unroll
         for (int d = 0; d < 3; ++d)
 #pragma unroll
@@ -569,6 +648,7 @@ gl_aux_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab T
             }
             double F[3][4];
             viscous_flux<double>(u, gq, ucv, cst, F, 7, nullptr);
+            if constexpr (CURV) gl_contravariant(vm, q, Q3, F);
 #pragma unroll
             for (int d = 0; d < 3; ++d)
 #pragma unroll
@@ -619,7 +699,6 @@ struct GlStageLayout {
 template <int ND, int NQ, bool VISC, bool SPLIT, bool CURV = false>
 __global__ void __launch_bounds__(gl_threads<NQ>(), 2)
 gl_stage_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab T) {
-    static_assert(!CURV || !VISC, "curvilinear uncollocated cells: the Euler equations");
     using L = GlStageLayout<ND, NQ, VISC, SPLIT, CURV>;
     constexpr int NT = L::NT, D3 = L::D3, Q3 = L::Q3, NF = L::NF, T1W = gl_t1_width<SPLIT>();
     extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -292,7 +292,7 @@ static cudaError_t launch_gl_nq(int kernel, const StageArgs& a, const GlArgs& g,
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     constexpr int NT = gl_threads<NQ>();
-    static bool cfg[11][64] = {};
+    static bool cfg[15][64] = {};
     if (kernel == 0) {
         if (split) return launch_gl_kernel(gl_trace_kernel<ND, NQ, true>, GlTraceLayout<ND, NQ, true>::bytes, NT, a, g, ht,
                                            cfg[0][dev], s);
@@ -300,6 +300,12 @@ static cudaError_t launch_gl_nq(int kernel, const StageArgs& a, const GlArgs& g,
                                 cfg[1][dev], s);
     }
     if (kernel == 1) {
+        if (g.vmet) {   // curvilinear cells
+            if (split) return launch_gl_kernel(gl_aux_kernel<ND, NQ, true, true>, GlAuxLayout<ND, NQ, true>::bytes, NT, a,
+                                               g, ht, cfg[11][dev], s);
+            return launch_gl_kernel(gl_aux_kernel<ND, NQ, false, true>, GlAuxLayout<ND, NQ, false>::bytes, NT, a, g, ht,
+                                    cfg[12][dev], s);
+        }
         if (split) return launch_gl_kernel(gl_aux_kernel<ND, NQ, true>, GlAuxLayout<ND, NQ, true>::bytes, NT, a, g, ht,
                                            cfg[2][dev], s);
         return launch_gl_kernel(gl_aux_kernel<ND, NQ, false>, GlAuxLayout<ND, NQ, false>::bytes, NT, a, g, ht,
@@ -307,8 +313,14 @@ static cudaError_t launch_gl_nq(int kernel, const StageArgs& a, const GlArgs& g,
     }
     if (kernel == 3)   // curvilinear: the weight-adjusted inverse mass alone
         return launch_gl_kernel(gl_minv_kernel<ND, NQ>, GlMinvLayout<ND, NQ>::bytes, NT, a, g, ht, cfg[8][dev], s);
-    if (g.vmet) {      // curvilinear cells: the Euler equations (checked by the host)
-        if (visc) return cudaErrorInvalidValue;
+    if (g.vmet) {      // curvilinear cells
+        if (visc) {
+            if (split) return launch_gl_kernel(gl_stage_kernel<ND, NQ, true, true, true>,
+                                               GlStageLayout<ND, NQ, true, true, true>::bytes, NT, a, g, ht, cfg[13][dev],
+                                               s);
+            return launch_gl_kernel(gl_stage_kernel<ND, NQ, true, false, true>,
+                                    GlStageLayout<ND, NQ, true, false, true>::bytes, NT, a, g, ht, cfg[14][dev], s);
+        }
         if (split) return launch_gl_kernel(gl_stage_kernel<ND, NQ, false, true, true>,
                                            GlStageLayout<ND, NQ, false, true, true>::bytes, NT, a, g, ht, cfg[9][dev], s);
         return launch_gl_kernel(gl_stage_kernel<ND, NQ, false, false, true>,

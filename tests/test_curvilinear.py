@@ -407,3 +407,60 @@ def test_curvilinear_fr_steps(precision):
     err = rel_max_err(dg.solution, U)
     print(f"curvilinear cHU {precision}: three RK4 steps rel err {err:.3e}")
     assert err <= (1e-12 if precision == "fp64" else 1e-6)
+
+
+GL_NS_CURVED = [
+    ("gl_ns_split_br2_p3", dict(poly_degree=3, n_cells=2, nodes="GL", pde="navier_stokes", diss="bassi_rebay_2")),
+    ("gl_ns_conservative_central_chu_p2", dict(poly_degree=2, n_cells=3, nodes="GL", pde="navier_stokes",
+                                               diss="central_visc_flux", split=False, conv="roe", fr="cHU")),
+    ("gll_overint1_ns_split_br2_p2", dict(poly_degree=2, n_cells=3, overintegration=1, pde="navier_stokes",
+                                          diss="bassi_rebay_2")),
+    ("gl_ns_split_br2_ksd_p5", dict(poly_degree=5, n_cells=1, nodes="GL", pde="navier_stokes", diss="bassi_rebay_2",
+                                    fr_aux="kSD")),
+]
+
+
+@pytest.mark.parametrize("kw", [dict(poly_degree=3, n_cells=2, nodes="GL", pde="navier_stokes", diss="bassi_rebay_2"),
+                                dict(poly_degree=2, n_cells=3, nodes="GL", overintegration=1, pde="navier_stokes",
+                                     diss="central_visc_flux", split=False, conv="roe")],
+                         ids=["gl_ns_split_p3", "gl_overint1_ns_conservative_p2"])
+def test_oracle_gl_navier_stokes_vanishing_warp_and_free_stream(kw):
+    _, affine = _oracle(kw, 0.0)
+    _, curved = _oracle(kw, 1e-300)
+    U = perturbed_tgv(affine, seed=5)
+    assert rel_max_err(curved.residual(U), affine.residual(U)) <= 1e-13
+    _, warped = _oracle(kw, WARP)
+    R = warped.residual(_uniform_state(warped))
+    scale = np.max(np.abs(warped.residual(warped.initial_condition("tgv"))))
+    assert np.max(np.abs(R)) <= 1e-11 * scale
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,kw", GL_NS_CURVED, ids=[c[0] for c in GL_NS_CURVED])
+def test_curvilinear_gl_navier_stokes_parity(name, kw):
+    """Navier-Stokes on curvilinear cells with GL flux nodes or overintegration: the physical
+    gradient through the weight-adjusted inverse at the flux nodes, H (x3) [(W / det J) H (x3) b]
+    with H = chi (M + K_aux)^-1 chi^T, contravariant viscous fluxes, F_v . C_face on faces."""
+    prm, orc, dg = _pair(kw)
+    U = perturbed_tgv(orc, seed=len(name))
+    err = rel_max_err(dg.residual_of(U), orc.residual(U))
+    print(f"{name}: curvilinear GL Navier-Stokes residual rel max err {err:.3e}")
+    assert err <= RTOL
+
+
+@pytest.mark.gpu
+def test_curvilinear_gl_navier_stokes_steps():
+    from philip_b200.dg import RungeKuttaODESolver
+    prm, orc, dg = _pair(dict(poly_degree=3, n_cells=2, nodes="GL", pde="navier_stokes", diss="bassi_rebay_2"))
+    R = dg.residual_of(_uniform_state(orc))
+    assert np.max(np.abs(R)) <= 1e-10
+    U = orc.initial_condition("tgv")
+    dg.solution = U
+    dt = 0.1 * TWO_PI / 8 / 11.0
+    ode = RungeKuttaODESolver(dg)
+    for step in range(3):
+        orc.rk_step(U, dt)
+        ode.step_in_time(dt)
+    err = rel_max_err(dg.solution, U)
+    print(f"curvilinear GL Navier-Stokes: three RK4 steps rel err {err:.3e}, uniform flow max |R| {np.max(np.abs(R)):.3e}")
+    assert err <= 1e-12
