@@ -99,6 +99,17 @@ typedef struct ph_params {
      * pressures is off, as in the reference (Euler::check_positive_quantity). */
     int bound_preserving_limiter;
     double min_density;
+    /* Boundary conditions of a non-periodic mesh (ph_mesh_desc.boundary_type):
+     * euler/angle_of_attack and side_slip_angle in degrees (the free stream of the farfield,
+     * Riemann and inflow conditions, velocities (cos a cos b, sin a cos b, sin b); the side slip
+     * must be 0, Euler::Euler, src/physics/euler.cpp:14-70), navier_stokes/
+     * thermal_boundary_condition_type (0 adiabatic, 1 isothermal) and
+     * nondimensionalized_isothermal_wall_temperature of the no-slip wall
+     * (src/parameters/parameters_navier_stokes.cpp:21-50; the .prm default is 1.0). */
+    double angle_of_attack;
+    double side_slip_angle;
+    int thermal_boundary_condition_type;
+    double isothermal_wall_temperature;
 } ph_params;
 
 /* Periodic cube [left,right]^3 with n^3 cells (PeriodicCubeFlow::generate_grid,
@@ -128,6 +139,15 @@ typedef struct ph_mesh_desc {
      * or nonsymmetric_curved_periodic_grid with grid_degree = poly_degree) and warp is
      * ignored. The caller keeps the array alive during ph_ctx_create / ph_batch_admit. */
     const double* mapping_support_points;
+    /* Boundary condition of each side x-, x+, y-, y+, z-, z+: 0 = periodic (a pair of sides is
+     * periodic on both sides or on neither), else the boundary_id its faces carry
+     * (Euler::boundary_face_values, src/physics/euler.cpp:1508-1560): 1001 wall (Euler: slip;
+     * Navier-Stokes: no-slip, adiabatic or isothermal), 1002 pressure outflow, 1003 inflow,
+     * 1004 Riemann farfield, 1005 farfield, 1006 slip wall, 1007 extrapolation. Navier-Stokes
+     * takes 1001 and 1006 (NavierStokes::boundary_face_values_viscous_flux defines no viscous
+     * exterior state for the others). Contexts on affine meshes with collocated GLL nodes
+     * (ph_ctx_create); as a flow case's grid sets boundary ids, e.g. channel_flow.cpp:324-343. */
+    int boundary_type[6];
 } ph_mesh_desc;
 
 /* Builds host index maps, 1-D operators and device buffers (replaces DGFactory::

@@ -431,8 +431,9 @@ struct Physics {
         const double c = std::sqrt(pressure(u) * gam / rho);
         return std::sqrt(v2) + c;
     }
-    // Navier-Stokes viscous flux, "LHS" sign (navier_stokes.cpp:1198-1350)
-    void viscous_flux(const double* u, const double g[5][3], double F[5][3]) const {
+    // Navier-Stokes viscous flux, "LHS" sign (navier_stokes.cpp:1198-1350); no_heat: the heat flux
+    // set to zero (dissipative_flux_dot_normal_on_adiabatic_boundary, :1268-1317)
+    void viscous_flux(const double* u, const double g[5][3], double F[5][3], bool no_heat = false) const {
         if (prm->pde != NAVIER_STOKES) { for (int s = 0; s < 5; ++s) for (int d = 0; d < 3; ++d) F[s][d] = 0.0; return; }
         double w[5]; primitive(u, w);
         const double rho = w[0];
@@ -468,11 +469,12 @@ struct Physics {
             for (int sd = 0; sd < 3; ++sd) F[1 + sd][fd] = -tau[sd][fd];
             F[4][fd] = 0.0;
             for (int sd = 0; sd < 3; ++sd) F[4][fd] -= w[1 + sd] * tau[fd][sd];
-            F[4][fd] += q[fd];
+            F[4][fd] += no_heat ? 0.0 : q[fd];
         }
     }
-    void viscous_flux_dot_n(const double* u, const double g[5][3], const double* n, double* out) const {
-        double F[5][3]; viscous_flux(u, g, F);
+    void viscous_flux_dot_n(const double* u, const double g[5][3], const double* n, double* out,
+                            bool no_heat = false) const {
+        double F[5][3]; viscous_flux(u, g, F, no_heat);
         for (int s = 0; s < 5; ++s) { out[s] = 0.0; for (int d = 0; d < 3; ++d) out[s] += F[s][d] * n[d]; }
     }
     // convective numerical flux dot n (convective_numerical_flux.cpp:35-480)
@@ -560,6 +562,183 @@ struct Physics {
             double aL[5], aR[5];
             viscous_flux_dot_n(uL, jump, n, aL);
             viscous_flux_dot_n(uR, jump, n, aR);
+            for (int s = 0; s < 5; ++s) out[s] = out[s] - penalty * (0.5 * (aL[s] + aR[s]));
+        }
+    }
+
+    // ---- boundary conditions
+    // free-stream primitive state (Euler::Euler, euler.cpp:14-70): density 1, velocities
+    // (cos a cos b, sin a cos b, sin b) for the angle of attack a and side slip b, pressure 1/(gam M^2)
+    void free_stream(double* w) const {
+        w[0] = 1.0;
+        w[1] = std::cos(prm->angle_of_attack) * std::cos(prm->side_slip_angle);
+        w[2] = std::sin(prm->angle_of_attack) * std::cos(prm->side_slip_angle);
+        w[3] = std::sin(prm->side_slip_angle);
+        w[4] = 1.0 / (gam * mach2);
+    }
+    double entropy_measure(double rho, double p) const {   // euler.cpp:414-421
+        double rc = rho;
+        if (rc < 0.0) { positive(rc); return BIG_NUMBER; }
+        return p * std::pow(rho, -gam);
+    }
+    double sound_of(const double* u) const {   // compute_sound(conservative), euler.cpp:535-543
+        const double rho = positive(u[0]);
+        const double p = pressure(u);
+        return std::sqrt(p * gam / rho);
+    }
+    // boundary_slip_wall (euler.cpp:1171-1217): the normal velocity reflected
+    void slip_wall(const double* n, const double* u, double* ub) const {
+        double w[5], wb[5];
+        primitive(u, w);
+        wb[0] = w[0]; wb[4] = w[4];
+        const double sn[3] = {-n[0], -n[1], -n[2]};
+        double vn = 0.0;
+        for (int d = 0; d < 3; ++d) vn = vn + w[1 + d] * sn[d];
+        for (int d = 0; d < 3; ++d) wb[1 + d] = w[1 + d] - 2.0 * vn * sn[d];
+        conservative_from_primitive(wb, ub);
+    }
+    // boundary_riemann (euler.cpp:1096-1169): characteristic farfield
+    void riemann(const double* n, const double* u, double* ub) const {
+        double wi[5], we[5], wb[5];
+        primitive(u, wi);
+        free_stream(we);
+        const double ci = sound(wi[0], wi[4]), ce = sound(we[0], we[4]);
+        double vni = 0.0, vne = 0.0;
+        for (int d = 0; d < 3; ++d) { vni = vni + wi[1 + d] * n[d]; vne = vne + we[1 + d] * n[d]; }
+        const double rout = vni + 2.0 / gm1 * ci, rinc = vne - 2.0 / gm1 * ce;
+        const double vnb = 0.5 * (rout + rinc), cb = 0.25 * gm1 * (rout - rinc);
+        if (std::fabs(vnb) >= std::fabs(cb)) {          // supersonic: inlet or outlet
+            for (int s = 0; s < 5; ++s) wb[s] = vnb < 0.0 ? we[s] : wi[s];
+        } else {                                       // subsonic
+            double rb, vt[3];
+            if (vnb < 0.0) {
+                rb = std::pow(1.0 / gam * cb * cb / entropy_measure(we[0], we[4]), 1.0 / gm1);
+                for (int d = 0; d < 3; ++d) vt[d] = we[1 + d] - vne * n[d];
+            } else {
+                rb = std::pow(1.0 / gam * cb * cb / entropy_measure(wi[0], wi[4]), 1.0 / gm1);
+                for (int d = 0; d < 3; ++d) vt[d] = wi[1 + d] - vni * n[d];
+            }
+            for (int d = 0; d < 3; ++d) wb[1 + d] = vt[d] + vnb * n[d];
+            wb[4] = 1.0 / gam * cb * cb * rb;
+            wb[0] = rb;
+        }
+        conservative_from_primitive(wb, ub);
+    }
+    // boundary_pressure_outflow (euler.cpp:1287-1327), back pressure 0.99 (boundary_face_values)
+    void pressure_outflow(double total_p, double back_p, const double* u, double* ub) const {
+        double v2 = 0.0;
+        for (int d = 0; d < 3; ++d) { const double v = u[1 + d] / u[0]; v2 = v2 + v * v; }
+        const double mach = std::sqrt(v2) / sound_of(u);   // compute_mach_number, euler.cpp:555-563
+        if (mach > 1.0) { for (int s = 0; s < 5; ++s) ub[s] = u[s]; return; }
+        double wi[5], wb[5];
+        primitive(u, wi);
+        const double radicant = 1.0 + 0.5 * gm1 * mach2;
+        const double p_inlet = total_p * std::pow(radicant, -gam / gm1);
+        const double ge1 = (mach >= 1) ? 1.0 : 0.0;
+        const double p_bc = ge1 * wi[4] + (1 - ge1) * back_p * p_inlet;
+        const double t_int = gam * mach2 * (wi[4] / wi[0]);    // compute_temperature, :452-459
+        wb[0] = gam * mach2 * (p_bc / t_int);                  // compute_density_from_pressure_temperature
+        for (int d = 0; d < 3; ++d) wb[1 + d] = wi[1 + d];
+        wb[4] = p_bc;
+        conservative_from_primitive(wb, ub);
+    }
+    // boundary_inflow (euler.cpp:1329-1434), subsonic (mach_inf < 1) or supersonic
+    void inflow(double total_p, double total_t, const double* n, const double* u, double* ub) const {
+        double wi[5], wb[5];
+        primitive(u, wi);
+        const double nrm[3] = {-n[0], -n[1], -n[2]};
+        double vni = 0.0;
+        for (int d = 0; d < 3; ++d) vni += wi[1 + d] * nrm[d];
+        const double ci = sound_of(u);
+        const double mach_inf = prm->mach_inf;
+        if (mach_inf < 1.0) {
+            const double rpos = vni + 2.0 * ci / gm1;
+            const double H = u[4] / wi[0] + wi[4] / wi[0];
+            const double a = 1.0 + 2.0 / gm1;
+            const double b = -2.0 * rpos;
+            const double c = 0.5 * gm1 * (rpos * rpos - 2.0 * H);
+            const double t1 = -0.5 * b / a;
+            const double t2 = 0.5 * std::sqrt(b * b - 4.0 * a * c) / a;
+            const double cb = std::max(t1 + t2, t1 - t2);
+            const double vmag = rpos - 2.0 * cb / gm1;
+            const double mach_bc = vmag / cb;
+            const double radicant = 1.0 + 0.5 * gm1 * mach_bc * mach_bc;
+            const double p_bc = total_p * std::pow(radicant, -gam / gm1);
+            const double t_bc = total_t * std::pow(radicant, -1.0);
+            wb[0] = gam * mach2 * (p_bc / t_bc);
+            for (int d = 0; d < 3; ++d) wb[1 + d] = vmag * nrm[d];
+            wb[4] = p_bc;
+        } else {
+            const double radicant = 1.0 + 0.5 * gm1 * mach2;
+            const double p_bc = total_p * std::pow(radicant, -gam / gm1);
+            const double t_bc = total_t * std::pow(radicant, -1.0);
+            wb[0] = gam * mach2 * (p_bc / t_bc);
+            const double cb = std::sqrt(gam * p_bc / wb[0]);
+            const double vmag = mach_inf * cb;
+            for (int d = 0; d < 3; ++d) wb[1 + d] = -vmag * n[d];
+            wb[4] = p_bc;
+        }
+        conservative_from_primitive(wb, ub);
+    }
+    // Euler::boundary_face_values (euler.cpp:1508-1560): the exterior state of the convective flux
+    void boundary_state(int type, const double* n, const double* u, double* ub) const {
+        const double p_inf = 1.0 / (gam * mach2);
+        const double t_inf = gam * p_inf / 1.0 * mach2;                       // euler.cpp:44
+        const double total_p = p_inf * std::pow(1.0 + 0.5 * gm1 * mach2, gam / gm1);
+        const double total_t = t_inf * std::pow(total_p / p_inf, gm1 / gam);
+        switch (type) {
+        case BC_WALL: case BC_SLIP_WALL: slip_wall(n, u, ub); break;   // boundary_wall = slip wall
+        case BC_PRESSURE_OUTFLOW: pressure_outflow(total_p, 0.99, u, ub); break;
+        case BC_INFLOW: inflow(total_p, total_t, n, u, ub); break;
+        case BC_RIEMANN: riemann(n, u, ub); break;
+        case BC_FARFIELD: {                                            // boundary_farfield, :1436-1450
+            double w[5]; free_stream(w);
+            conservative_from_primitive(w, ub);
+            break;
+        }
+        case BC_EXTRAPOLATION: for (int s = 0; s < 5; ++s) ub[s] = u[s]; break;   // boundary_p0_extrapolation
+        default: throw std::runtime_error("oracle: boundary type not restated");
+        }
+    }
+    // NavierStokes::boundary_face_values_viscous_flux (navier_stokes.cpp:1354-1432): the exterior
+    // state and gradient of the dissipative flux. 1001: no-slip (momentum negated, gradient the
+    // interior's; adiabatic: energy gradient zero; isothermal: the exterior temperature
+    // 2 T_wall - T_int); 1006: the interior state and gradient
+    void boundary_viscous_state(int type, const double* u, const double g[5][3], double* ub, double gb[5][3]) const {
+        if (type != BC_WALL && type != BC_SLIP_WALL)
+            throw std::runtime_error("oracle: Navier-Stokes boundary type without a viscous exterior state");
+        for (int s = 0; s < 5; ++s) for (int d = 0; d < 3; ++d) gb[s][d] = g[s][d];
+        if (type == BC_SLIP_WALL) { for (int s = 0; s < 5; ++s) ub[s] = u[s]; return; }
+        ub[0] = u[0]; ub[4] = u[4];
+        for (int d = 0; d < 3; ++d) ub[1 + d] = -u[1 + d];
+        if (prm->thermal_bc == THERMAL_ADIABATIC) for (int d = 0; d < 3; ++d) gb[4][d] = 0.0;
+        if (prm->thermal_bc == THERMAL_ISOTHERMAL) {
+            double wi[5], we[5];
+            primitive(u, wi);
+            primitive(ub, we);
+            const double t_int = gam * mach2 * (wi[4] / wi[0]);
+            const double t_ext = 2.0 * prm->wall_temperature - t_int;
+            we[4] = we[0] * t_ext / (gam * mach2);   // compute_pressure_from_density_temperature
+            double w2[5]; conservative_from_primitive(we, w2);
+            ub[4] = w2[4];                          // compute_total_energy
+        }
+    }
+    // evaluate_auxiliary_flux on a boundary face (viscous_numerical_flux.cpp:66-328, on_boundary):
+    // BR2 and SIPG take the exterior gradient, the central flux the interior one; on an adiabatic
+    // 1001 wall both sides' fluxes drop the heat flux (navier_stokes.cpp:1224-1264)
+    void diss_boundary_flux(int type, const double* ui, const double* ub, const double gi[5][3],
+                            const double gb[5][3], const double* n, double penalty, double* out) const {
+        const bool ad = prm->thermal_bc == THERMAL_ADIABATIC && type == BC_WALL;
+        double fi[5], fb[5];
+        viscous_flux_dot_n(ui, gi, n, fi, ad);
+        viscous_flux_dot_n(ub, prm->diss_flux == CENTRAL_VISC ? gi : gb, n, fb, ad);
+        for (int s = 0; s < 5; ++s) out[s] = 0.5 * (fi[s] + fb[s]);
+        if (prm->diss_flux == SIPG) {
+            double jump[5][3];
+            for (int s = 0; s < 5; ++s) for (int d = 0; d < 3; ++d) jump[s][d] = (ui[s] - ub[s]) * n[d];
+            double aL[5], aR[5];
+            viscous_flux_dot_n(ui, jump, n, aL, ad);
+            viscous_flux_dot_n(ub, jump, n, aR, ad);
             for (int s = 0; s < 5; ++s) out[s] = out[s] - penalty * (0.5 * (aL[s] + aR[s]));
         }
     }
@@ -704,6 +883,7 @@ Mesh build_periodic_cube(int n, double left, double right, int order, const Ops1
     m.order = (order == ORDER_AUTO) ? (is_pow2(n) ? ORDER_MORTON : ORDER_LEXICOGRAPHIC) : order;
     m.h = (right - left) / n;
     m.ijk.resize(m.nc); m.cell_of.assign(m.nc, -1); m.nbr.resize(m.nc);
+    m.bnd.assign(m.nc, {0, 0, 0, 0, 0, 0});
     if (m.order == ORDER_MORTON) {
         int levels = 0; while ((1 << levels) < n) ++levels;
         for (int c = 0; c < m.nc; ++c) {
@@ -770,6 +950,42 @@ void Solver::init(const Params& p, int n, double left, double right, int order, 
     ndofs_cell = NSTATE * nd3;
     aux.assign(3 * ndofs(), 0.0);
     status = 0;
+}
+
+void Solver::set_boundaries(const int types[6]) {
+    if (!mesh.affine) throw std::runtime_error("oracle: boundaries on the affine cube only");
+    for (int d = 0; d < 3; ++d)
+        if ((types[2 * d] == 0) != (types[2 * d + 1] == 0))
+            throw std::runtime_error("oracle: a pair of cube sides is periodic on both sides or on neither");
+    for (int f = 0; f < 6; ++f) {
+        const int t = types[f];
+        if (t != 0 && (t < BC_WALL || t > BC_EXTRAPOLATION))
+            throw std::runtime_error("oracle: boundary type not restated");
+        // the Navier-Stokes viscous boundary state exists for 1000, 1001 and 1006 only
+        // (navier_stokes.cpp:1354-1390)
+        if (t != 0 && prm.pde == NAVIER_STOKES && t != BC_WALL && t != BC_SLIP_WALL)
+            throw std::runtime_error("oracle: Navier-Stokes takes wall (1001) and slip-wall (1006) boundaries");
+    }
+    const int n = mesh.n;
+    for (int c = 0; c < mesh.nc; ++c) {
+        const auto t = mesh.ijk[c];
+        for (int f = 0; f < 6; ++f) {
+            const int d = f / 2;
+            const bool side = (f % 2) ? t[d] == n - 1 : t[d] == 0;
+            if (types[f] != 0 && side) { mesh.nbr[c][f] = -1; mesh.bnd[c][f] = types[f]; }
+        }
+    }
+}
+
+void Solver::boundary_values(int type, const double* n, const double* u, const double* g, double* ub_conv,
+                             double* ub_visc, double* gb_visc) {
+    Physics phys(&prm, &status);
+    phys.boundary_state(type, n, u, ub_conv);
+    double gi[5][3], gb[5][3] = {};
+    for (int s = 0; s < 5; ++s) for (int d = 0; d < 3; ++d) gi[s][d] = g[s * 3 + d];
+    if (type == BC_WALL || type == BC_SLIP_WALL) phys.boundary_viscous_state(type, u, gi, ub_visc, gb);
+    else for (int s = 0; s < 5; ++s) ub_visc[s] = ub_conv[s];
+    for (int s = 0; s < 5; ++s) for (int d = 0; d < 3; ++d) gb_visc[s * 3 + d] = gb[s][d];
 }
 
 // ---------------------------------------------------------------------------------
@@ -863,17 +1079,28 @@ void Solver::assemble_residual(const double* U, double* R) {
             }
             // face part: this cell's side of each of its 6 faces (strong_dg.cpp:871-1008)
             for (int f = 0; f < 6; ++f) {
-                const int cn = mesh.nbr[c][f];
+                const int bt = mesh.bnd[c][f];
+                const int cn = bt ? c : mesh.nbr[c][f];
                 const int fn = (f % 2) ? f - 1 : f + 1;
                 const double* Un = U + (size_t)cn * ndc;
-                // int = owner (lower index) as in dg_base.cpp:417-449; this cell may be either side
-                const bool owner = c < cn;
+                // int = owner (lower index) as in dg_base.cpp:417-449; this cell may be either side.
+                // A boundary face (strong_dg.cpp:725-866): this cell is the interior side and the
+                // exterior state is the viscous boundary state of its face values
+                const bool owner = bt || c < cn;
                 const int ci = owner ? c : cn, fi = owner ? f : fn, ce = owner ? cn : c, fe = owner ? fn : f;
                 const double* Ui = owner ? Uc : Un; const double* Ue = owner ? Un : Uc;
                 std::vector<double> si(NSTATE * nf), se(NSTATE * nf);
                 for (int s = 0; s < NSTATE; ++s) {
                     surf_apply(o, chi, nq, nd, o.chi_s[fi % 2].data(), fi, Ui + s * nd3, &si[s * nf], false, 1.0);
                     surf_apply(o, chi, nq, nd, o.chi_s[fe % 2].data(), fe, Ue + s * nd3, &se[s * nf], false, 1.0);
+                }
+                if (bt) {
+                    for (int q = 0; q < nf; ++q) {
+                        double ui[5], ub[5], g0[5][3] = {}, gb[5][3];
+                        for (int s = 0; s < 5; ++s) ui[s] = si[s * nf + q];
+                        phys.boundary_viscous_state(bt, ui, g0, ub, gb);
+                        for (int s = 0; s < 5; ++s) se[s * nf + q] = ub[s];
+                    }
                 }
                 std::vector<double> term(nf);
                 for (int d = 0; d < 3; ++d) {
@@ -1009,10 +1236,15 @@ void Solver::assemble_residual(const double* U, double* R) {
 
         // ---- face terms (strong_dg.cpp:2367-3576); this cell's side of each face
         for (int f = 0; f < 6; ++f) {
-            const int cn = mesh.nbr[c][f];
+            // a boundary face (assemble_boundary_term_strong, strong_dg.cpp:1582-2366): this cell is
+            // the interior side with its own hybrid and volume-flux terms; the numerical fluxes take
+            // the boundary states at the face nodes (the "exterior" arrays below are unused)
+            const int bt = mesh.bnd[c][f];
+            const int cn = bt ? c : mesh.nbr[c][f];
             const int fn = (f % 2) ? f - 1 : f + 1;
-            const bool owner = c < cn;
-            const int ci = owner ? c : cn, fi = owner ? f : fn, ce = owner ? cn : c, fe = owner ? fn : f;
+            const bool owner = bt || c < cn;
+            const int ci = owner ? c : cn, fi = owner ? f : fn, ce = bt ? c : (owner ? cn : c);
+            const int fe = bt ? f : (owner ? fn : f);
             const double* Ui = U + (size_t)ci * ndc;
             const double* Ue = U + (size_t)ce * ndc;
             const int dni = fi / 2, dne = fe / 2;
@@ -1148,8 +1380,22 @@ void Solver::assemble_residual(const double* U, double* R) {
                 J = std::sqrt(J);
                 for (int a = 0; a < 3; ++a) np[a] /= J;
                 double cf[5], df[5] = {0, 0, 0, 0, 0};
-                phys.conv_num_flux(ui, ue, np, cf);
-                if (viscous) phys.diss_num_flux(ri, re, gi, ge, np, pen, df);
+                if (bt) {
+                    // the interior state interpolated to the face (the projected entropy variables'
+                    // state only with use_projected_entropy_variables_for_nsfr_boundary_term, off by
+                    // default, strong_dg.cpp:2255-2273); the penalty is this cell's (dg_base.cpp:563)
+                    double ub[5];
+                    phys.boundary_state(bt, np, ri, ub);
+                    phys.conv_num_flux(ri, ub, np, cf);
+                    if (viscous) {
+                        double uv[5], gv[5][3];
+                        phys.boundary_viscous_state(bt, ri, gi, uv, gv);
+                        phys.diss_boundary_flux(bt, ri, uv, gi, gv, np, penalty_of(c, f), df);
+                    }
+                } else {
+                    phys.conv_num_flux(ui, ue, np, cf);
+                    if (viscous) phys.diss_num_flux(ri, re, gi, ge, np, pen, df);
+                }
                 for (int s = 0; s < 5; ++s) { cn_[s * nf + q] = J * cf[s]; dn_[s * nf + q] = J * df[s]; }
             }
             // lift this cell's side (:3454-3576)

@@ -35,6 +35,11 @@ enum CellOrder { ORDER_AUTO = 0, ORDER_LEXICOGRAPHIC = 1, ORDER_MORTON = 2 };
 enum NonPhysical { RETURN_BIG_NUMBER = 0, ABORT_RUN = 1, PRINT_WARNING = 2 };
 // limiter/bound_preserving_limiter (parameters_limiter.cpp:17-30); the positivity-preserving ones
 enum Limiter { LIMITER_NONE = 0, LIMITER_MAXIMUM_PRINCIPLE = 1, PPL_ZHANG2010 = 2, PPL_WANG2012 = 3 };
+enum ThermalBc { THERMAL_ADIABATIC = 0, THERMAL_ISOTHERMAL = 1 };
+// boundary_id values of the boundary conditions (euler.cpp:1508-1560, navier_stokes.cpp:1354-1390);
+// 0 marks a periodic pair of cube sides here
+enum BoundaryType { BC_WALL = 1001, BC_PRESSURE_OUTFLOW = 1002, BC_INFLOW = 1003, BC_RIEMANN = 1004,
+                    BC_FARFIELD = 1005, BC_SLIP_WALL = 1006, BC_EXTRAPOLATION = 1007 };
 
 // Plain parameter block (mirrors the .prm keys of the hot path).
 struct Params {
@@ -64,6 +69,13 @@ struct Params {
     double rrk_tol = 5e-10;            // relaxation_runge_kutta_root_tolerance
     int limiter = LIMITER_NONE;        // limiter/bound_preserving_limiter
     double min_density = 1e-13;        // limiter/min_density
+    // boundary conditions: the free stream's angles in radians (euler/angle_of_attack and
+    // side_slip_angle, given in degrees, parameters_euler.cpp:39-43) and the wall's thermal
+    // condition (navier_stokes/thermal_boundary_condition_type, 0 adiabatic / 1 isothermal, and
+    // nondimensionalized_isothermal_wall_temperature, parameters_navier_stokes.cpp:21-50)
+    double angle_of_attack = 0.0, side_slip_angle = 0.0;
+    int thermal_bc = THERMAL_ADIABATIC;
+    double wall_temperature = 1.0;
 };
 
 // One-dimensional operators on the reference interval [0,1]
@@ -97,7 +109,8 @@ struct Mesh {
     double left = 0.0, right = 1.0;
     std::vector<std::array<int, 3>> ijk;        // cell -> (ix,iy,iz)
     std::vector<int> cell_of;                   // lexicographic index -> cell id
-    std::vector<std::array<int, 6>> nbr;        // cell, face -> neighbour cell
+    std::vector<std::array<int, 6>> nbr;        // cell, face -> neighbour cell (-1: boundary face)
+    std::vector<std::array<int, 6>> bnd;        // cell, face -> boundary_id of a boundary face (0 inside)
     // metric terms at volume flux nodes: C[cell][node][3][3], detJ[cell][node]
     bool affine = true;
     double h = 1.0;
@@ -129,6 +142,15 @@ struct Solver {
     void init(const Params& p, int n, double left, double right, int order,
               double warp = 0.0, int grid_degree = 1);
     std::size_t ndofs() const { return (std::size_t)mesh.nc * ndofs_cell; }
+    // non-periodic sides of the (affine) cube: types[f] for the sides x-, x+, y-, y+, z-, z+ (0 keeps
+    // a periodic pair; a pair is periodic on both sides or on neither), as the boundary_id a flow
+    // case's grid gives its boundary faces (e.g. channel_flow.cpp:324-343)
+    void set_boundaries(const int types[6]);
+    // the exterior states of boundary `type` at one face node (outward unit normal n): the
+    // convective one (boundary_face_values) and the viscous one with its gradient
+    // (boundary_face_values_viscous_flux)
+    void boundary_values(int type, const double* n, const double* u, const double* g, double* ub_conv,
+                         double* ub_visc, double* gb_visc);
     // right-hand side R(U) (before the inverse mass matrix), dg_base.cpp:2599-2915
     void assemble_residual(const double* U, double* R);
     // out = M^{-1} in (dg_base.cpp:4089-4260)

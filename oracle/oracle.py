@@ -8,6 +8,7 @@ the product library never does.
 from __future__ import annotations
 
 import ctypes
+import math
 import os
 import subprocess
 
@@ -32,6 +33,10 @@ FR_AUX = {"kDG": 0, "kSD": 1, "kHU": 2, "kNegative": 3, "kNegative2": 4, "kPlus"
 ORDER = {"auto": 0, "lexicographic": 1, "morton": 2}
 IC = {"tgv": 0, "isentropic_vortex": 1, "vortex_param": 2}
 LIMITER = {"none": 0, "maximum_principle": 1, "positivity_preservingZhang2010": 2, "positivity_preservingWang2012": 3}
+THERMAL_BC = {"adiabatic": 0, "isothermal": 1}
+# boundary_id of each boundary condition (euler.cpp:1508-1560); 0 keeps a periodic pair of sides
+BOUNDARY = {"periodic": 0, "wall": 1001, "pressure_outflow": 1002, "inflow": 1003, "riemann_farfield": 1004,
+            "farfield": 1005, "slip_wall": 1006, "extrapolation": 1007}
 
 
 class OrcParams(ctypes.Structure):
@@ -41,7 +46,9 @@ class OrcParams(ctypes.Structure):
         "non_physical", "use_rrk")] + [(n, ctypes.c_double) for n in (
         "fr_user_value", "gamma", "mach_inf", "reynolds_inf", "prandtl", "temperature_inf",
         "constant_viscosity", "sipg_penalty_factor", "atol", "rtol", "rrk_tol")] + [
-        ("limiter", ctypes.c_int), ("min_density", ctypes.c_double)]
+        ("limiter", ctypes.c_int), ("min_density", ctypes.c_double),
+        ("angle_of_attack", ctypes.c_double), ("side_slip_angle", ctypes.c_double),
+        ("thermal_bc", ctypes.c_int), ("wall_temperature", ctypes.c_double)]
 
 
 _lib = None
@@ -81,6 +88,9 @@ def lib():
         L.orc_rk_error.argtypes = [vp]; L.orc_rk_error.restype = ctypes.c_double
         L.orc_rrk_gamma.argtypes = [vp]; L.orc_rrk_gamma.restype = ctypes.c_double
         L.orc_numerical_entropy.argtypes = [vp, dp]; L.orc_numerical_entropy.restype = ctypes.c_double
+        L.orc_set_boundaries.argtypes = [vp, ip]; L.orc_set_boundaries.restype = ctypes.c_int
+        L.orc_boundary_values.argtypes = [vp, ctypes.c_int, dp, dp, dp, dp, dp, dp]
+        L.orc_boundary_values.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -121,6 +131,11 @@ def make_params(cfg: dict) -> OrcParams:
     p.rrk_tol = cfg.get("relaxation_runge_kutta_root_tolerance", 5e-10)
     p.limiter = LIMITER[cfg.get("bound_preserving_limiter", "none")]
     p.min_density = cfg.get("min_density", 1e-13)
+    pi = math.atan(1.0) * 4.0   # degrees to radians as parameters_euler.cpp:41-43
+    p.angle_of_attack = cfg.get("angle_of_attack", 0.0) * pi / 180.0
+    p.side_slip_angle = cfg.get("side_slip_angle", 0.0) * pi / 180.0
+    p.thermal_bc = THERMAL_BC[cfg.get("thermal_boundary_condition_type", "adiabatic")]
+    p.wall_temperature = cfg.get("nondimensionalized_isothermal_wall_temperature", 1.0)
     return p
 
 
@@ -128,10 +143,12 @@ class Oracle:
     """One DG discretisation on a periodic cube, evaluated on the CPU."""
 
     def __init__(self, cfg: dict, n_cells: int, left: float, right: float, order: str = "auto",
-                 warp: float = 0.0, grid_degree: int | None = None):
+                 warp: float = 0.0, grid_degree: int | None = None, boundaries=None):
         """warp != 0: the sine-warped periodic cube (every coordinate moved by
         warp (L/2pi) sin(2pi(x-l)/L) sin(2pi(y-l)/L) sin(2pi(z-l)/L)) with a mapping of degree
-        grid_degree (default: the polynomial degree)."""
+        grid_degree (default: the polynomial degree). boundaries: six boundary types (names of
+        BOUNDARY or boundary_id values) for the sides x-, x+, y-, y+, z-, z+; a pair is periodic
+        on both sides or on neither."""
         self.cfg = dict(cfg)
         self._p = make_params(cfg)
         h = ctypes.c_void_p()
@@ -149,6 +166,22 @@ class Oracle:
         self.nd = int(lib().orc_nd(h))
         self.nq = int(lib().orc_nq(h))
         self.nc = n_cells ** 3
+        if boundaries is not None:
+            t = (ctypes.c_int * 6)(*boundary_ids(boundaries))
+            if lib().orc_set_boundaries(h, t) != 0:
+                raise RuntimeError("oracle: boundaries refused")
+
+    def boundary_values(self, btype, normal, u, grad=None):
+        """The boundary states at one face node: (convective exterior state, viscous exterior
+        state, viscous exterior gradient [5][3])."""
+        n = np.ascontiguousarray(normal, dtype=np.float64)
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        g = np.zeros((5, 3)) if grad is None else np.ascontiguousarray(grad, dtype=np.float64)
+        uc, uv, gv = np.zeros(5), np.zeros(5), np.zeros((5, 3))
+        if lib().orc_boundary_values(self.h, boundary_ids([btype])[0], _dp(n), _dp(u), _dp(g), _dp(uc), _dp(uv),
+                                     _dp(gv)) != 0:
+            raise RuntimeError("oracle: boundary type refused")
+        return uc, uv, gv
 
     def __del__(self):
         if getattr(self, "h", None) is not None and _lib is not None:
@@ -231,6 +264,11 @@ class Oracle:
 
     def status(self):
         return int(lib().orc_status(self.h))
+
+
+def boundary_ids(types):
+    """boundary_id values of boundary types given by name or by id."""
+    return [BOUNDARY[t] if isinstance(t, str) else int(t) for t in types]
 
 
 def tgv_constant_dt(cfl, left, right, n_cells, poly_degree):

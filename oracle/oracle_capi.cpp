@@ -22,6 +22,9 @@ struct orc_params {
         sipg_penalty_factor, atol, rtol, rrk_tol;
     int limiter;
     double min_density;
+    double angle_of_attack, side_slip_angle;   // radians
+    int thermal_bc;
+    double wall_temperature;
 };
 
 static Params to_params(const orc_params* p) {
@@ -37,6 +40,8 @@ static Params to_params(const orc_params* p) {
     q.atol = p->atol; q.rtol = p->rtol;
     q.use_rrk = p->use_rrk; q.rrk_tol = p->rrk_tol;
     q.limiter = p->limiter; q.min_density = p->min_density;
+    q.angle_of_attack = p->angle_of_attack; q.side_slip_angle = p->side_slip_angle;
+    q.thermal_bc = p->thermal_bc; q.wall_temperature = p->wall_temperature;
     return q;
 }
 
@@ -61,6 +66,27 @@ int orc_create_curved(const orc_params* p, int n, double left, double right, int
         return 0;
     } catch (const std::exception& e) {
         std::fprintf(stderr, "orc_create_curved: %s\n", e.what());
+        return 1;
+    }
+}
+// non-periodic sides of the cube (types[6]: x-, x+, y-, y+, z-, z+; 0 periodic)
+int orc_set_boundaries(void* h, const int* types) {
+    try {
+        static_cast<Solver*>(h)->set_boundaries(types);
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "orc_set_boundaries: %s\n", e.what());
+        return 1;
+    }
+}
+// the boundary states at one face node: g and gb_visc are [5][3]
+int orc_boundary_values(void* h, int type, const double* n, const double* u, const double* g, double* ub_conv,
+                        double* ub_visc, double* gb_visc) {
+    try {
+        static_cast<Solver*>(h)->boundary_values(type, n, u, g, ub_conv, ub_visc, gb_visc);
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "orc_boundary_values: %s\n", e.what());
         return 1;
     }
 }

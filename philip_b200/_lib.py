@@ -56,14 +56,29 @@ class PhParams(ctypes.Structure):
         "prandtl_number", "temperature_inf", "nondimensionalized_constant_viscosity", "sipg_penalty_factor",
         "rk_atol", "rk_rtol", "pressure_shift")] + [
         ("use_relaxation_runge_kutta", ctypes.c_int), ("relaxation_runge_kutta_root_tolerance", ctypes.c_double),
-        ("bound_preserving_limiter", ctypes.c_int), ("min_density", ctypes.c_double)]
+        ("bound_preserving_limiter", ctypes.c_int), ("min_density", ctypes.c_double),
+        ("angle_of_attack", ctypes.c_double), ("side_slip_angle", ctypes.c_double),
+        ("thermal_boundary_condition_type", ctypes.c_int), ("isothermal_wall_temperature", ctypes.c_double)]
 
 
 class PhMeshDesc(ctypes.Structure):
     _fields_ = [("n_cells_per_direction", ctypes.c_int), ("cell_order", ctypes.c_int),
                 ("left", ctypes.c_double), ("right", ctypes.c_double),
                 ("warp", ctypes.c_double), ("grid_degree", ctypes.c_int),
-                ("mapping_support_points", ctypes.POINTER(ctypes.c_double))]
+                ("mapping_support_points", ctypes.POINTER(ctypes.c_double)),
+                ("boundary_type", ctypes.c_int * 6)]
+
+# boundary_id of each boundary condition (Euler::boundary_face_values); 0 keeps a periodic pair of sides
+BOUNDARY = {"periodic": 0, "wall": 1001, "pressure_outflow": 1002, "inflow": 1003, "riemann_farfield": 1004,
+            "farfield": 1005, "slip_wall": 1006, "extrapolation": 1007}
+
+
+def boundary_ids(types) -> list:
+    """boundary_id values of six boundary types given by name or by id."""
+    ids = [BOUNDARY[t] if isinstance(t, str) else int(t) for t in types]
+    if len(ids) != 6:
+        raise ValueError("boundaries: one type per side x-, x+, y-, y+, z-, z+")
+    return ids
 
 
 class PhError(RuntimeError):

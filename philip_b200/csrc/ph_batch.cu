@@ -334,6 +334,7 @@ int rebuild(ph_batch* b) {
 
 int check_batch_params(const ph_batch* b, const ph_mesh_desc* mesh, const ph_params* prm) {
     if (int rc = check_mesh(mesh)) return rc;
+    if (has_boundaries(mesh)) return fail(PH_ERR_UNSUPPORTED, "a batch takes periodic meshes");
     if (const char* why = unsupported_reason(mesh, prm)) return fail(PH_ERR_UNSUPPORTED, why);
     if (prm->pde_type != 0 || !prm->use_split_form)
         return fail(PH_ERR_UNSUPPORTED, "a batch takes split-form Euler solves");

@@ -392,7 +392,38 @@ int check_mesh(const ph_mesh_desc* mesh) {
     // the recursive-children order exists only for hyper_cube + refine_global: n = 2^levels
     if (mesh->cell_order == 2 && (n & (n - 1)) != 0)
         return fail(PH_ERR_INVALID, "cell_order 2 (recursive children) needs n_cells_per_direction a power of two");
+    for (int f = 0; f < 6; ++f) {
+        const int t = mesh->boundary_type[f];
+        if (t != 0 && (t < ph::BC_WALL || t > ph::BC_EXTRAPOLATION))
+            return fail(PH_ERR_INVALID, "boundary_type: 0 (periodic) or a boundary_id 1001..1007");
+    }
+    for (int d = 0; d < 3; ++d)
+        if ((mesh->boundary_type[2 * d] == 0) != (mesh->boundary_type[2 * d + 1] == 0))
+            return fail(PH_ERR_INVALID, "boundary_type: a pair of cube sides is periodic on both sides or on neither");
     return PH_OK;
+}
+
+bool has_boundaries(const ph_mesh_desc* mesh) {
+    for (int f = 0; f < 6; ++f)
+        if (mesh->boundary_type[f] != 0) return true;
+    return false;
+}
+
+// Non-periodic meshes: what the boundary terms take (nullptr when supported).
+const char* boundary_reason(const ph_mesh_desc* mesh, const ph_params* prm) {
+    if (!has_boundaries(mesh)) return nullptr;
+    if (uncollocated(prm)) return "boundary conditions: collocated GLL flux nodes without overintegration";
+    if (is_curvilinear(mesh)) return "boundary conditions: affine meshes";
+    if (prm->pde_type == 1)
+        for (int f = 0; f < 6; ++f) {
+            const int t = mesh->boundary_type[f];
+            // NavierStokes::boundary_face_values_viscous_flux defines the exterior state of 1000, 1001
+            // and 1006 only (navier_stokes.cpp:1354-1390); for the others the reference's auxiliary
+            // boundary term reads an unset state
+            if (t != 0 && t != ph::BC_WALL && t != ph::BC_SLIP_WALL)
+                return "boundary conditions: Navier-Stokes takes wall (1001) and slip wall (1006) boundaries";
+        }
+    return nullptr;
 }
 
 int check_param_ranges(const ph_params* prm) {
@@ -401,8 +432,12 @@ int check_param_ranges(const ph_params* prm) {
         prm->runge_kutta_method < 0 || prm->runge_kutta_method > 10 ||
         (prm->runge_kutta_method >= 4 && prm->runge_kutta_method <= 6) || prm->precision < 0 || prm->precision > 1 ||
         prm->flux_nodes_type < 0 || prm->flux_nodes_type > 1 || prm->flux_reconstruction_aux < 0 ||
-        prm->flux_reconstruction_aux > 6)
+        prm->flux_reconstruction_aux > 6 || prm->thermal_boundary_condition_type < 0 ||
+        prm->thermal_boundary_condition_type > 1)
         return fail(PH_ERR_INVALID, "parameter out of range");
+    // Euler::Euler aborts on a side slip (euler.cpp:47-51)
+    if (std::fabs(prm->side_slip_angle * (std::atan(1.0) * 4.0) / 180.0) >= 1e-14)
+        return fail(PH_ERR_INVALID, "side_slip_angle must be zero");
     return PH_OK;
 }
 
@@ -643,7 +678,39 @@ ph::PhysConst physics_constants(const ph_params* prm, double h, double& penalty)
     pc.sipg_pen = sipg;
     // SIPG penalty (dg_base.cpp:397-413), averaged over both (identical) cells
     penalty = (double)prm->poly_degree * (prm->poly_degree + 1) / h * sipg;
+    // boundary conditions: the free stream of Euler::Euler (euler.cpp:14-70; angles in degrees as in the
+    // .prm, parameters_euler.cpp:41-43) and the inlet totals of boundary_face_values (:1515-1516)
+    const double pi = std::atan(1.0) * 4.0;
+    const double aoa = prm->angle_of_attack * pi / 180.0, ss = prm->side_slip_angle * pi / 180.0;
+    pc.bc_v_inf[0] = std::cos(aoa) * std::cos(ss);
+    pc.bc_v_inf[1] = std::sin(aoa) * std::cos(ss);
+    pc.bc_v_inf[2] = std::sin(ss);
+    pc.bc_p_inf = 1.0 / (pc.gam * pc.mach2);
+    const double t_inf = pc.gam * pc.bc_p_inf / 1.0 * pc.mach2;
+    pc.bc_total_p = pc.bc_p_inf * std::pow(1.0 + 0.5 * pc.gm1 * pc.mach2, pc.gam / pc.gm1);
+    pc.bc_total_t = t_inf * std::pow(pc.bc_total_p / pc.bc_p_inf, pc.gm1 / pc.gam);
+    pc.bc_mach_inf = prm->mach_infinity;
+    pc.bc_t_wall = prm->isothermal_wall_temperature;
+    pc.bc_isothermal = prm->thermal_boundary_condition_type == 1;
     return pc;
+}
+
+// Boundary faces of a non-periodic cube: a cell face on a side with boundary_type[f] != 0 gets
+// nbr = -1 - k, k numbering the boundary faces cell by cell, and btype[k] = boundary_type[f]
+// (the boundary_id a flow case's grid gives those faces, e.g. channel_flow.cpp:324-343).
+void apply_boundaries(int n, const std::vector<int>& ijk, const int types[6], std::vector<int>& nbr,
+                      std::vector<int>& btype) {
+    btype.clear();
+    const int nc = (int)(ijk.size() / 3);
+    for (int cc = 0; cc < nc; ++cc)
+        for (int f = 0; f < 6; ++f) {
+            const int d = f / 2;
+            const int t = ijk[3 * cc + d];
+            if (types[f] != 0 && ((f & 1) ? t == n - 1 : t == 0)) {
+                nbr[6 * (size_t)cc + f] = -1 - (int)btype.size();
+                btype.push_back(types[f]);
+            }
+        }
 }
 
 void periodic_connectivity(int n, int order, std::vector<int>& ijk, std::vector<int>& nbr) {
@@ -998,6 +1065,11 @@ struct ph_ctx {
     // stage-input state buffer and in the viscous terms
     bool slab = false;
     int z_first = 0, z_count = 0, layer = 0, nc_ghost = 0;
+    // non-periodic mesh: boundary faces (nbr = -1 - k), their boundary_id and (Navier-Stokes) the
+    // boundary viscous fluxes of the auxiliary kernel
+    int nb = 0;
+    int* d_btype = nullptr;
+    double* d_fb = nullptr;
     size_t nalloc = 0;                  // doubles per stage-input buffer, ghost slots included
     // stage tiles [0, lo_end) and [hi_begin, nc) read ghost data (CPC-aligned, so the tiles and
     // their partial sums are those of one launch over all cells); [lo_end, hi_begin) do not
@@ -1085,14 +1157,16 @@ int dispatch_aux(ph_ctx* c, const double* U, int cell_begin, int cell_end) {
     NvtxRange nvtx("auxiliary kernel");
     cudaError_t e;
     const double inv_h = 1.0 / c->h;
+    const ph::BoundaryArgs ba{c->d_btype, c->d_fb, c->pen};
+    const ph::BoundaryArgs* bnd = c->nb ? &ba : nullptr;
     timer_begin(c);
     switch (c->N1) {
-    case 2: e = ph::launch_aux<2>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->curv ? c->d_metric : nullptr, c->stream); break;
-    case 3: e = ph::launch_aux<3>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->curv ? c->d_metric : nullptr, c->stream); break;
-    case 4: e = ph::launch_aux<4>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->curv ? c->d_metric : nullptr, c->stream); break;
-    case 5: e = ph::launch_aux<5>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->curv ? c->d_metric : nullptr, c->stream); break;
-    case 6: e = ph::launch_aux<6>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->curv ? c->d_metric : nullptr, c->stream); break;
-    case 7: e = ph::launch_aux<7>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->curv ? c->d_metric : nullptr, c->stream); break;
+    case 2: e = ph::launch_aux<2>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->curv ? c->d_metric : nullptr, c->stream, bnd); break;
+    case 3: e = ph::launch_aux<3>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->curv ? c->d_metric : nullptr, c->stream, bnd); break;
+    case 4: e = ph::launch_aux<4>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->curv ? c->d_metric : nullptr, c->stream, bnd); break;
+    case 5: e = ph::launch_aux<5>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->curv ? c->d_metric : nullptr, c->stream, bnd); break;
+    case 6: e = ph::launch_aux<6>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->curv ? c->d_metric : nullptr, c->stream, bnd); break;
+    case 7: e = ph::launch_aux<7>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->curv ? c->d_metric : nullptr, c->stream, bnd); break;
     default: return fail(PH_ERR_UNSUPPORTED, "polynomial degree outside 1..6");
     }
     if (e != cudaSuccess) return fail(PH_ERR_CUDA, std::string("aux launch: ") + cudaGetErrorString(e));
@@ -1247,6 +1321,8 @@ ph::StageArgs base_args(ph_ctx* c, const double* U) {
     a.h = c->h; a.inv_h = 1.0 / c->h; a.pen = c->pen; a.pc = c->pc; a.status = c->d_status;
     a.fr = c->fr ? 1 : 0;
     a.metric = c->d_metric;
+    a.btype = c->nb ? c->d_btype : nullptr;
+    a.Fb = c->d_fb;
     return a;
 }
 
@@ -1356,6 +1432,7 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
     if (int rc = check_mesh(mesh)) return rc;
     if (int rc = check_param_ranges(prm)) return rc;
     const bool gl = uncollocated(prm);
+    if (const char* why = boundary_reason(mesh, prm)) return fail(PH_ERR_UNSUPPORTED, why);
     if (const char* why = gl ? uncollocated_reason(mesh, prm) : unsupported_reason(mesh, prm))
         return fail(PH_ERR_UNSUPPORTED, why);
     const bool ec = prm->conv_num_flux >= 3;
@@ -1387,6 +1464,7 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
     if (slab) {
         if (z0 < 0 || z0 >= mesh->n_cells_per_direction || nz > mesh->n_cells_per_direction)
             return fail(PH_ERR_INVALID, "slab outside the mesh: 0 <= z_first < n and 1 <= z_count <= n");
+        if (has_boundaries(mesh)) return fail(PH_ERR_UNSUPPORTED, "slab contexts: periodic meshes");
     }
     ph_ctx* c = new ph_ctx();
     c->prm = *prm;
@@ -1429,9 +1507,11 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
     } else {
         rk_tableau(prm->runge_kutta_method, c->ns, c->A, c->b);
     }
-    std::vector<int> nbr;
+    std::vector<int> nbr, btype;
     if (slab) slab_connectivity(c->n, c->z_first, c->z_count, c->ijk, nbr);
     else periodic_connectivity(c->n, mesh->cell_order, c->ijk, nbr);
+    if (has_boundaries(mesh)) apply_boundaries(c->n, c->ijk, mesh->boundary_type, nbr, btype);
+    c->nb = (int)btype.size();
     std::vector<double> metric;
     if (int rc = node_geometry(c->n, c->ijk, x, D, c->left, c->right, c->warp, c->xyz, metric,
                                mesh->mapping_support_points)) { delete c; return rc; }
@@ -1475,6 +1555,13 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
     }
     c->limiter = prm->bound_preserving_limiter;
     if (c->limiter) bad |= dalloc(&c->d_ltab, 1);
+    if (c->nb) {   // boundary faces: their types, and (Navier-Stokes) their viscous fluxes in the arithmetic type
+        bad |= dalloc(&c->d_btype, (size_t)c->nb);
+        if (c->visc) {
+            const size_t fb = (size_t)c->nb * 4 * c->N1 * c->N1;
+            bad |= dalloc(&c->d_fb, c->fp32 ? (fb + 1) / 2 : fb);
+        }
+    }
     if (gl) {   // (slabs: the ghost cells' face blocks too, filled by the exchange)
         const size_t faces = (size_t)(c->nc + c->nc_ghost) * 6 * c->NQ * c->NQ;
         bad |= dalloc(&c->d_gl, 1);
@@ -1495,6 +1582,8 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
     if (bad) { ph_ctx_destroy(c); return fail(PH_ERR_NOMEM, "device allocation failed"); }
     cudaError_t e = cudaSuccess;
     e = cudaMemcpy(c->d_nbr, nbr.data(), nbr.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && c->nb)
+        e = cudaMemcpy(c->d_btype, btype.data(), btype.size() * sizeof(int), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(c->d_ops, &c->h_ops, sizeof(ph::OpTab), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(c->d_itab, &itab, sizeof(ph::IntegralTab), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && c->d_gl) e = cudaMemcpy(c->d_gl, &c->h_gl, sizeof(ph::GlTab), cudaMemcpyHostToDevice);
@@ -1632,7 +1721,7 @@ int ph_ctx_destroy(ph_ctx* c) {
     void* ptrs[] = {c->d_nbr, c->d_ops, c->d_itab, c->d_sol, c->d_stA, c->d_stB, c->d_acc, c->d_carry,
                     c->d_fv, c->d_comp, c->d_tmpA, c->d_tmpB, c->d_partial, c->d_status, c->d_metric, c->d_xnode, c->d_origin, c->d_err,
                     c->d_table, c->d_counter, c->d_ent, c->d_ent_cell, c->d_halo, c->d_gl, c->d_t1, c->d_t2,
-                    c->d_vis, c->d_ltab, c->d_glvm, c->d_glfn};
+                    c->d_vis, c->d_ltab, c->d_glvm, c->d_glfn, c->d_btype, c->d_fb};
     if (c->side) cudaStreamSynchronize(c->side);
     for (void* p : ptrs) if (p) cudaFree(p);
     if (c->side) cudaStreamDestroy(c->side);
@@ -2467,6 +2556,7 @@ extern "C" int ph_residual_noalloc(const ph_mesh_desc* mesh, const ph_params* pr
     if (int rc = check_mesh(mesh)) return rc;
     if (int rc = check_param_ranges(prm)) return rc;
     if (is_curvilinear(mesh)) return fail(PH_ERR_UNSUPPORTED, "ph_residual_noalloc: affine meshes only");
+    if (has_boundaries(mesh)) return fail(PH_ERR_UNSUPPORTED, "ph_residual_noalloc: periodic meshes only");
     if (const char* why = unsupported_reason(mesh, prm)) return fail(PH_ERR_UNSUPPORTED, why);
     if (prm->conv_num_flux >= 3 && !prm->use_split_form)
         return fail(PH_ERR_INVALID, "two point flux and not using split form are not compatible");

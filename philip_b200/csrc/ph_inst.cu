@@ -10,11 +10,11 @@ namespace ph {
 
 template <int N1> constexpr int cells_per_cta() { return N1 == 2 ? 16 : N1 == 3 ? 4 : N1 == 4 ? 2 : 1; }
 
-template <typename R, int N1, bool VISC, bool SPLIT, int FS, bool CURV = false>
+template <typename R, int N1, bool VISC, bool SPLIT, int FS, bool CURV = false, bool BND = false>
 static cudaError_t launch_one(const StageArgs& a, cudaStream_t s) {
     constexpr int CPC = cells_per_cta<N1>();
     using L = Layout<R, N1, CPC, VISC, SPLIT, CURV>;
-    auto kern = residual_kernel<R, N1, CPC, VISC, SPLIT, FS, CURV>;
+    auto kern = residual_kernel<R, N1, CPC, VISC, SPLIT, FS, CURV, BND>;
     int dev = 0;
     cudaGetDevice(&dev);
     static bool configured[64] = {false};
@@ -35,6 +35,13 @@ static cudaError_t launch_prec(const StageArgs& a, bool visc, bool split, cudaSt
     // relaxation RK's entropy estimate lives in the generic instance only
     const bool hot = split && a.pc.two_point == TP_CH && a.pc.conv_flux == CF_EC_ROE &&
                      (!visc || a.pc.diss_flux == DF_BR2) && a.ent_partial == nullptr;
+    if (a.btype) {    // boundary faces (affine cells, the generic flux set)
+        if (a.metric) return cudaErrorInvalidValue;
+        if (visc) return split ? launch_one<R, N1, true, true, 0, false, true>(a, s)
+                               : launch_one<R, N1, true, false, 0, false, true>(a, s);
+        return split ? launch_one<R, N1, false, true, 0, false, true>(a, s)
+                     : launch_one<R, N1, false, false, 0, false, true>(a, s);
+    }
     if (a.metric) {   // curvilinear cells
         if (!split) return visc ? launch_one<R, N1, true, false, 0, true>(a, s) : launch_one<R, N1, false, false, 0, true>(a, s);
         if (visc) return hot ? launch_one<R, N1, true, true, 1, true>(a, s) : launch_one<R, N1, true, true, 0, true>(a, s);
@@ -158,13 +165,14 @@ void stage_launch_shape(int fp32, bool visc, bool split, int* threads, int* cpc,
     }
 }
 
-template <typename R, int N1, bool FRA, bool CURV>
+template <typename R, int N1, bool FRA, bool CURV, bool BND = false>
 static cudaError_t launch_aux_prec(const double* U, const int* nbr, const OpTab& ops, int cell_begin, int nc,
-                                   double inv_h, const PhysConst& pc, void* Fv, const double* metric, cudaStream_t s) {
+                                   double inv_h, const PhysConst& pc, void* Fv, const double* metric, cudaStream_t s,
+                                   const BoundaryArgs* bnd = nullptr) {
     constexpr int CPC = cells_per_cta<N1>();
     using L = AuxLayout<N1, CPC, FRA>;
     constexpr size_t bytes = L::template bytes<R>();
-    auto kern = aux_kernel<R, N1, CPC, FRA, CURV>;
+    auto kern = aux_kernel<R, N1, CPC, FRA, CURV, BND>;
     int dev = 0;
     cudaGetDevice(&dev);
     static bool configured[64] = {false};
@@ -179,13 +187,23 @@ static cudaError_t launch_aux_prec(const double* U, const int* nbr, const OpTab&
     const int grid = (nc - cell_begin + CPC - 1) / CPC;
     if (grid <= 0) return cudaErrorInvalidValue;
     kern<<<grid, L::NT, bytes, s>>>(U, nbr, cell_begin, nc, CURV ? R(1) : (R)inv_h, pc, co, static_cast<R*>(Fv),
-                                    metric);
+                                    metric, bnd ? bnd->btype : nullptr, bnd ? static_cast<R*>(bnd->Fb) : nullptr,
+                                    bnd ? (R)bnd->pen : R(0));
     return cudaGetLastError();
 }
 
 template <int N1>
 cudaError_t launch_aux(const double* U, const int* nbr, const OpTab& ops, int cell_begin, int nc, double inv_h,
-                       const PhysConst& pc, int fp32, void* Fv, const double* metric, cudaStream_t s) {
+                       const PhysConst& pc, int fp32, void* Fv, const double* metric, cudaStream_t s,
+                       const BoundaryArgs* bnd) {
+    if (bnd) {      // boundary faces (affine cells)
+        if (metric) return cudaErrorInvalidValue;
+        if (ops.aux_fr)
+            return fp32 ? launch_aux_prec<float, N1, true, false, true>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, nullptr, s, bnd)
+                        : launch_aux_prec<double, N1, true, false, true>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, nullptr, s, bnd);
+        return fp32 ? launch_aux_prec<float, N1, false, false, true>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, nullptr, s, bnd)
+                    : launch_aux_prec<double, N1, false, false, true>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, nullptr, s, bnd);
+    }
     if (metric) {   // curvilinear cells (kDG, checked by the host)
         if (ops.aux_fr) return cudaErrorInvalidValue;
         return fp32 ? launch_aux_prec<float, N1, false, true>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, metric, s)
@@ -264,7 +282,7 @@ template cudaError_t launch_stage_batched<PH_N1>(const StageArgs*, const BatchTi
                                                  cudaStream_t);
 template bool batched_shape<PH_N1>(int, bool, int, int*, int*, size_t*, int*);
 template cudaError_t launch_aux<PH_N1>(const double*, const int*, const OpTab&, int, int, double, const PhysConst&, int,
-                                       void*, const double*, cudaStream_t);
+                                       void*, const double*, cudaStream_t, const BoundaryArgs*);
 template cudaError_t launch_inverse_mass<PH_N1>(const double*, double*, const OpTab*, int, double, const double*, int,
                                                 cudaStream_t);
 template cudaError_t launch_integrals<PH_N1>(const double*, const double*, const double*, const IntegralTab*, int,

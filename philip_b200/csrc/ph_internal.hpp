@@ -21,6 +21,7 @@ int fail(int code, const std::string& msg);   // records the message for ph_last
 // PH_ERR_INVALID with the message recorded (mesh size and bounds, cell_order 0..2 and the
 // recursive-children order only for a power-of-two n; enumerations within their ranges).
 int check_mesh(const ph_mesh_desc* mesh);
+bool has_boundaries(const ph_mesh_desc* mesh);
 int check_param_ranges(const ph_params* prm);
 
 // Configuration checks shared by every entry point that builds a discretisation;

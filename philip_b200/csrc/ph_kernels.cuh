@@ -116,6 +116,11 @@ struct StageArgs {
     // relaxation RK (mode 2): per-tile sums of v(u)^T M k, v the entropy variables of the
     // stage input (or nullptr; the generic flux-set kernel, FS = 0, computes them)
     double* ent_partial;
+    // non-periodic meshes: a boundary face has nbr = -1 - k, btype[k] its boundary_id, and (Navier-
+    // Stokes) Fb[k] the outward boundary viscous flux F*_v . n at its [4][NF] face nodes, in R,
+    // written by the auxiliary kernel (nullptr on periodic meshes)
+    const int* btype;
+    const void* Fb;
 };
 
 // Viscous terms per cell written by the auxiliary kernel and read by the stage kernel:
@@ -249,10 +254,12 @@ __device__ __forceinline__ void check_state_fp64(double u[5], double gm1, unsign
 // left cell is the interior side, normal +e_d) lifted into this cell with its sign.
 // The convective flux is evaluated in the frame whose x axis is the face normal.
 // fvface: this cell's face blocks of the viscous terms (viscous only).
-template <typename R, int N1, int CPC, bool VISC, bool SPLIT, bool CURV>
+// BND (non-periodic meshes): on a boundary face (bnd) the trace holds the convective boundary state
+// and, Navier-Stokes, the boundary viscous flux F*_v . e_d itself (no average, no penalty term).
+template <typename R, int N1, int CPC, bool VISC, bool SPLIT, bool CURV, bool BND = false>
 __device__ __forceinline__ void face_item(const Cst<R>& cst, int tp, int cf, int df, int ucv, const R* sU,
                                           const R* sD, R* sT, const R* sX, int c, int f, int fn, R pen,
-                                          R inv_wend, const R* __restrict__ fvface) {
+                                          R inv_wend, const R* __restrict__ fvface, bool bnd = false) {
     using L = Layout<R, N1, CPC, VISC, SPLIT, CURV>;
     constexpr int NP = L::NP, NF = L::NF, TR = L::TR, NQS = L::NQS;
     const int d = f >> 1;
@@ -324,9 +331,9 @@ __device__ __forceinline__ void face_item(const Cst<R>& cst, int tp, int cf, int
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             Fo[k] = __ldg(&fvface[(f * 4 + k) * NF + fn]);
-            Fn[k] = R(0.5) * (Fo[k] + tr[(5 + k) * NF + fn]);
+            Fn[k] = (BND && bnd) ? tr[(5 + k) * NF + fn] : R(0.5) * (Fo[k] + tr[(5 + k) * NF + fn]);
         }
-        if (df == DF_SIPG) {
+        if (df == DF_SIPG && !(BND && bnd)) {
             const R* uL = plus ? uo : ue;
             const R* uR = plus ? ue : uo;
             R gj[5][3];
@@ -656,9 +663,10 @@ __device__ __forceinline__ void ls_tile_error(double err2, double* out) {
     }
 }
 
-template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int FS, bool CURV, bool BULK = false>
+template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int FS, bool CURV, bool BULK = false, bool BND = false>
 __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell0) {
     static_assert(!BULK || (std::is_same<R, double>::value && N1 % 2 == 0 && !CURV), "bulk staging: FP64, even N1");
+    static_assert(!BND || (!BULK && !CURV), "boundary faces: affine cells, plain loads");
     using L = Layout<R, N1, CPC, VISC, SPLIT, CURV>;
     constexpr int NP = L::NP, NF = L::NF, NT = L::NT, TR = L::TR, NQS = L::NQS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -719,6 +727,28 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
         const int cn = __ldg(&a.nbr[cell * 6 + f]);
         const int nn = face_node_volume_index<N1>(f, fn, (f & 1) ? 0 : N1 - 1);
         R* tr = sT + (c * 6 + f) * TR * NF;
+        if constexpr (BND) {
+            if (cn < 0) {   // boundary face: the boundary state of this cell's face value
+                const int k = -1 - cn;
+                const int bt = __ldg(&a.btype[k]);
+                const int no = face_node_volume_index<N1>(f, fn, (f & 1) ? N1 - 1 : 0);
+                const R sg = (f & 1) ? R(1) : R(-1);
+                const int dn = f >> 1;
+                const R nrm[3] = {dn == 0 ? sg : R(0), dn == 1 ? sg : R(0), dn == 2 ? sg : R(0)};
+                R ui[5], ub[5];
+#pragma unroll
+                for (int s = 0; s < 5; ++s) ui[s] = (R)__ldg(&a.U[((size_t)cell * 5 + s) * NP + no]);
+                boundary_state<R>(bt, nrm, ui, a.pc, ub, std::is_same<R, double>::value ? a.status : nullptr);
+#pragma unroll
+                for (int s = 0; s < 5; ++s) tr[s * NF + fn] = ub[s];
+                if constexpr (VISC) {   // F*_v . e_d = sg (F*_v . n_out)
+                    const R* fb = static_cast<const R*>(a.Fb) + (size_t)k * 4 * NF;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) tr[(5 + q) * NF + fn] = sg * __ldg(&fb[q * NF + fn]);
+                }
+                continue;
+            }
+        }
         R ue[5];
 #pragma unroll
         for (int s = 0; s < 5; ++s) { ue[s] = (R)__ldg(&a.U[((size_t)cn * 5 + s) * NP + nn]); tr[s * NF + fn] = ue[s]; }
@@ -822,12 +852,11 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
             const int f = (it / NF) % 6;
             const int c = it / (NF * 6);
             const R* fvface = nullptr;
-            if constexpr (VISC) {
-                int cell = cell0 + c; if (cell >= a.nc) cell = a.nc - 1;
-                fvface = static_cast<const R*>(a.Fv) + (size_t)cell * viscous_terms_per_cell<N1>() + 4 * NP;
-            }
-            face_item<R, N1, CPC, VISC, SPLIT, CURV>(cst, tp, cf, df, ucv, sU, sD, sT, sX, c, f, fn, pen, inv_wend,
-                                                    fvface);
+            int cell = cell0 + c; if (cell >= a.nc) cell = a.nc - 1;
+            if constexpr (VISC) fvface = static_cast<const R*>(a.Fv) + (size_t)cell * viscous_terms_per_cell<N1>() + 4 * NP;
+            const bool bnd = BND && __ldg(&a.nbr[cell * 6 + f]) < 0;
+            face_item<R, N1, CPC, VISC, SPLIT, CURV, BND>(cst, tp, cf, df, ucv, sU, sD, sT, sX, c, f, fn, pen,
+                                                         inv_wend, fvface, bnd);
         }
     }
     // ---- opposite-node pair fluxes (even N1): each evaluated once, read by both lanes in phase 4
@@ -1019,10 +1048,10 @@ __host__ __device__ constexpr bool stage_bulk() {
     return PH_BULK_TILE && std::is_same<R, double>::value && N1 % 2 == 0 && !CURV && VISC;
 }
 
-template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int FS, bool CURV = false>
+template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int FS, bool CURV = false, bool BND = false>
 __global__ void __launch_bounds__(Layout<R, N1, CPC, VISC, SPLIT, CURV>::NT, Layout<R, N1, CPC, VISC, SPLIT, CURV>::MINB)
 residual_kernel(const StageArgs a) {
-    residual_tile<R, N1, CPC, VISC, SPLIT, FS, CURV, stage_bulk<R, N1, CPC, VISC, SPLIT, CURV>()>(
+    residual_tile<R, N1, CPC, VISC, SPLIT, FS, CURV, !BND && stage_bulk<R, N1, CPC, VISC, SPLIT, CURV>(), BND>(
         a, a.cell_begin + blockIdx.x * CPC);
 }
 
@@ -1134,10 +1163,70 @@ __device__ __forceinline__ void aux_curv_flux(const R un[5], const R r[5][3], co
                            C[2 * 3 + j] * (double)F[2][k]);
 }
 
-template <typename R, int N1, int CPC, bool FRA, bool CURV>
+// Boundary faces (non-periodic meshes): the outward boundary viscous flux F*_v . n at one node's
+// boundary faces (up to three at a corner), stored for the stage kernel in Fb[k][4][NF]
+// (evaluate_auxiliary_flux with on_boundary, viscous_numerical_flux.cpp:66-328, called from
+// assemble_boundary_term_strong, strong_dg.cpp:2279-2300): the exterior state is the viscous boundary
+// state; BR2 and SIPG take its gradient (the interior's, the energy gradient zero on an adiabatic
+// wall), the central flux the interior gradient; on an adiabatic 1001 wall both sides' fluxes drop
+// the heat flux (dissipative_flux_dot_normal, navier_stokes.cpp:1224-1264).
+template <typename R, int N1>
+__device__ __forceinline__ void aux_boundary_fluxes(const int* __restrict__ nbr, const int* __restrict__ btype,
+                                                    R* __restrict__ Fb, int cell, int node, const R un[5],
+                                                    const R g[5][3], const PhysConst& pc, const Cst<R>& cst, R pen) {
+    constexpr int NF = N1 * N1;
+    const int cx[3] = {node % N1, (node / N1) % N1, node / (N1 * N1)};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            if (cx[d] != (side ? N1 - 1 : 0)) continue;
+            const int cn = __ldg(&nbr[cell * 6 + 2 * d + side]);
+            if (cn >= 0) continue;
+            const int k = -1 - cn;
+            const int bt = __ldg(&btype[k]);
+            const int t1 = (d == 0) ? 1 : 0, t2 = (d == 2) ? 1 : 2;
+            const int fn = cx[t2] * N1 + cx[t1];
+            R ub[5];
+            boundary_viscous_state<R>(bt, un, pc, ub, nullptr);
+            const bool ad = bt == BC_WALL && !pc.bc_isothermal;
+            R gb[5][3];
+#pragma unroll
+            for (int s = 0; s < 5; ++s)
+#pragma unroll
+                for (int e = 0; e < 3; ++e) gb[s][e] = (ad && s == 4) ? R(0) : g[s][e];
+            const R sg = side ? R(1) : R(-1);
+            R Fi[3][4], Fe[3][4];
+            viscous_flux<R>(un, g, pc.use_const_visc, cst, Fi, 1 << d, nullptr, ad);
+            if (pc.diss_flux == DF_CENTRAL) viscous_flux<R>(ub, g, pc.use_const_visc, cst, Fe, 1 << d, nullptr, ad);
+            else viscous_flux<R>(ub, gb, pc.use_const_visc, cst, Fe, 1 << d, nullptr, ad);
+            R out[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) out[q] = R(0.5) * (sg * Fi[d][q] + sg * Fe[d][q]);
+            if (pc.diss_flux == DF_SIPG) {
+                R J[5][3];
+#pragma unroll
+                for (int s = 0; s < 5; ++s)
+#pragma unroll
+                    for (int e = 0; e < 3; ++e) J[s][e] = (e == d) ? (un[s] - ub[s]) * sg : R(0);
+                viscous_flux<R>(un, J, pc.use_const_visc, cst, Fi, 1 << d, nullptr, ad);
+                viscous_flux<R>(ub, J, pc.use_const_visc, cst, Fe, 1 << d, nullptr, ad);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) out[q] = out[q] - pen * (R(0.5) * (sg * Fi[d][q] + sg * Fe[d][q]));
+            }
+            R* dst = Fb + (size_t)k * 4 * NF + fn;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) dst[q * NF] = out[q];
+        }
+    }
+}
+
+template <typename R, int N1, int CPC, bool FRA, bool CURV, bool BND = false>
 __global__ void __launch_bounds__(AuxLayout<N1, CPC, FRA>::NT)
 aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, int cell_begin, int nc, R inv_h, PhysConst pc,
-           AuxCoef<R> co, R* __restrict__ Fv, const double* __restrict__ metric) {
+           AuxCoef<R> co, R* __restrict__ Fv, const double* __restrict__ metric, const int* __restrict__ btype,
+           R* __restrict__ Fb, R pen) {
+    static_assert(!(BND && CURV), "boundary faces: affine cells");
     using L = AuxLayout<N1, CPC, FRA>;
     constexpr int NP = L::NP, NF = L::NF, NT = L::NT;
     constexpr int VT = viscous_terms_per_cell<N1>();
@@ -1160,9 +1249,22 @@ aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, int cell_b
         const int fn = it % NF, f = (it / NF) % 6, c = it / (6 * NF);
         int cell = cell0 + c; if (cell >= nc) cell = nc - 1;
         const int cn = __ldg(&nbr[cell * 6 + f]);
+        R* dst = sT + (c * 6 + f) * 5 * NF + fn;
+        if constexpr (BND) {
+            if (cn < 0) {   // boundary face: the viscous boundary state of this cell's face value
+                const int bt = __ldg(&btype[-1 - cn]);
+                const int no = face_node_volume_index<N1>(f, fn, (f & 1) ? N1 - 1 : 0);
+                R ui[5], ub[5];
+#pragma unroll
+                for (int s = 0; s < 5; ++s) ui[s] = (R)__ldg(&U[((size_t)cell * 5 + s) * NP + no]);
+                boundary_viscous_state<R>(bt, ui, pc, ub, nullptr);
+#pragma unroll
+                for (int s = 0; s < 5; ++s) dst[s * NF] = ub[s];
+                continue;
+            }
+        }
         const int nn = face_node_volume_index<N1>(f, fn, (f & 1) ? 0 : N1 - 1);
         const double* src = U + (size_t)cn * 5 * NP + nn;
-        R* dst = sT + (c * 6 + f) * 5 * NF + fn;
 #pragma unroll
         for (int s = 0; s < 5; ++s) dst[s * NF] = (R)__ldg(&src[s * NP]);
     }
@@ -1239,6 +1341,9 @@ aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, int cell_b
                 aux_curv_flux<R, N1>(un, g, metric, cell, node, pc.use_const_visc, cst, F);
             } else {
                 viscous_flux<R>(un, g, pc.use_const_visc, cst, F, 7, nullptr);
+            }
+            if constexpr (BND) {
+                if (cell0 + c < nc) aux_boundary_fluxes<R, N1>(nbr, btype, Fb, cell0 + c, node, un, g, pc, cst, pen);
             }
 #pragma unroll
             for (int d = 0; d < 3; ++d)
@@ -1329,6 +1434,7 @@ aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, int cell_b
             R F[3][4];
             if constexpr (CURV) aux_curv_flux<R, N1>(un, g, metric, cell, node, pc.use_const_visc, cst, F);
             else viscous_flux<R>(un, g, pc.use_const_visc, cst, F, 7, nullptr);
+            if constexpr (BND) aux_boundary_fluxes<R, N1>(nbr, btype, Fb, cell, node, un, g, pc, cst, pen);
 #pragma unroll
             for (int d = 0; d < 3; ++d)
 #pragma unroll

@@ -15,9 +15,16 @@ cudaError_t launch_stage(const StageArgs& a, int fp32, bool visc, bool split, cu
 // auxiliary (lifted gradient) equation, emitting the viscous terms of the stage kernel
 // (viscous_terms_per_cell) of cells [cell_begin, nc); ops: the host copy of the operator table;
 // metric: the curvilinear cells' metric rows (nullptr on affine cells)
+// bnd: the boundary faces of a non-periodic mesh (nullptr on periodic meshes)
+struct BoundaryArgs {
+    const int* btype;   // boundary_id per boundary face
+    void* Fb;           // [nb][4][NF] boundary viscous fluxes (in the arithmetic type)
+    double pen;         // SIPG penalty of a boundary face (the cell's own)
+};
 template <int N1>
 cudaError_t launch_aux(const double* U, const int* nbr, const OpTab& ops, int cell_begin, int nc, double inv_h,
-                       const PhysConst& pc, int fp32, void* Fv, const double* metric, cudaStream_t s);
+                       const PhysConst& pc, int fp32, void* Fv, const double* metric, cudaStream_t s,
+                       const BoundaryArgs* bnd = nullptr);
 // DGBase::apply_inverse_global_mass_matrix on its own
 template <int N1>
 cudaError_t launch_inverse_mass(const double* in, double* out, const OpTab* ops, int nc, double inv_detj,

@@ -32,6 +32,11 @@ struct PhysConst {
     double gam, gm1, mach2, temp_ratio, inv_re, prandtl, const_visc, sipg_pen;
     double pressure_shift;   // precision form: reference pressure taken out of the momentum fluxes
     int use_const_visc, two_point, conv_flux, diss_flux, navier_stokes;
+    // boundary conditions: the free stream (density 1, velocities v_inf, pressure 1/(gam M^2),
+    // Euler::Euler, euler.cpp:14-70), the inlet totals of boundary_face_values (:1515-1516), the
+    // Mach number, and the wall's thermal condition (isothermal: wall temperature t_wall)
+    double bc_v_inf[3], bc_p_inf, bc_total_p, bc_total_t, bc_mach_inf, bc_t_wall;
+    int bc_isothermal;
 };
 
 template <typename R> struct Cst {
@@ -123,6 +128,15 @@ template <typename R> __device__ __forceinline__ R pressure(const R u[5], R gm1,
     R v2 = R(0);
 #pragma unroll
     for (int d = 0; d < 3; ++d) { const R v = qdiv<R>(u[1 + d], rho); v2 = v2 + v * v; }
+    return positive<R>(gm1 * (u[4] - R(0.5) * rho * v2), st);
+}
+
+// the same with IEEE division (boundary states)
+template <typename R> __device__ __forceinline__ R pressure_ieee(const R u[5], R gm1, unsigned* st) {
+    const R rho = u[0];
+    R v2 = R(0);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { const R v = u[1 + d] / rho; v2 = v2 + v * v; }
     return positive<R>(gm1 * (u[4] - R(0.5) * rho * v2), st);
 }
 
@@ -558,7 +572,8 @@ __device__ __forceinline__ void conv_num_flux_n(const R uL[5], const R uR[5], co
 // direction d; the density component is zero. `dmask` selects the directions.
 template <typename R>
 __device__ __forceinline__ void viscous_flux(const R u[5], const R g[5][3], int use_const_visc,
-                                             const Cst<R>& c, R F[3][4], int dmask, unsigned* st) {
+                                             const Cst<R>& c, R F[3][4], int dmask, unsigned* st,
+                                             bool no_heat = false) {
     const R rho_raw = u[0];
     R w[5];
 #pragma unroll
@@ -600,7 +615,190 @@ __device__ __forceinline__ void viscous_flux(const R u[5], const R g[5][3], int 
         const R q = -kappa * dT;
 #pragma unroll
         for (int k = 0; k < 3; ++k) F[d][k] = -tau_d[k];
-        F[d][3] = -(w[1] * tau_d[0] + w[2] * tau_d[1] + w[3] * tau_d[2]) + q;
+        F[d][3] = -(w[1] * tau_d[0] + w[2] * tau_d[1] + w[3] * tau_d[2]) + (no_heat ? R(0) : q);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Boundary conditions at one face node with outward unit normal n (boundary_id values of
+// euler.cpp:1508-1560). IEEE division throughout (few nodes; the flux code's quotient is for
+// the volume loops).
+// ---------------------------------------------------------------------------------------
+enum BoundaryType { BC_WALL = 1001, BC_PRESSURE_OUTFLOW = 1002, BC_INFLOW = 1003, BC_RIEMANN = 1004,
+                    BC_FARFIELD = 1005, BC_SLIP_WALL = 1006, BC_EXTRAPOLATION = 1007 };
+
+// primitive (rho, v, p) with the density and pressure checks of convert_conservative_to_primitive
+// (euler.cpp:177-198)
+template <typename R> __device__ __forceinline__ void bc_primitive(const R u[5], R gm1, R w[5], unsigned* st) {
+    const R rho = u[0];
+    R v2 = R(0);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { w[1 + d] = u[1 + d] / rho; v2 = v2 + w[1 + d] * w[1 + d]; }
+    const R p = positive<R>(gm1 * (u[4] - R(0.5) * rho * v2), st);
+    w[0] = positive<R>(rho, st);
+    w[4] = positive<R>(p, st);
+}
+// convert_primitive_to_conservative with compute_total_energy (euler.cpp:206-222, :357-374)
+template <typename R> __device__ __forceinline__ void bc_conservative(const R w[5], R gm1, R u[5]) {
+    u[0] = w[0];
+    R v2 = R(0);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { u[1 + d] = w[0] * w[1 + d]; v2 = v2 + w[1 + d] * w[1 + d]; }
+    u[4] = w[4] / gm1 + R(0.5) * w[0] * v2;
+}
+
+// Euler::boundary_face_values: the exterior state of the convective numerical flux.
+// 1001 (boundary_wall) and 1006: slip wall, the normal velocity reflected (:1171-1229);
+// 1002 pressure outflow at back pressure 0.99 (:1287-1327); 1003 inflow (:1329-1434);
+// 1004 characteristic (Riemann) farfield (:1096-1169); 1005 the free stream (:1436-1450);
+// 1007 the interior state (:1452-1464).
+template <typename R>
+__device__ void boundary_state(int type, const R n[3], const R u[5], const PhysConst& pc, R ub[5], unsigned* st) {
+    const R gam = (R)pc.gam, gm1 = (R)pc.gm1, mach2 = (R)pc.mach2;
+    R wi[5], wb[5];
+    if (type == BC_EXTRAPOLATION) {
+#pragma unroll
+        for (int s = 0; s < 5; ++s) ub[s] = u[s];
+        return;
+    }
+    if (type == BC_FARFIELD) {
+        wb[0] = R(1);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) wb[1 + d] = (R)pc.bc_v_inf[d];
+        wb[4] = R(1) / (gam * mach2);
+        bc_conservative<R>(wb, gm1, ub);
+        return;
+    }
+    if (type == BC_PRESSURE_OUTFLOW) {   // compute_mach_number (:555-563) first
+        R v2 = R(0);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) { const R v = u[1 + d] / u[0]; v2 = v2 + v * v; }
+        const R rho_c = positive<R>(u[0], st);
+        const R p_c = pressure_ieee<R>(u, gm1, st);
+        const R mach = rsqrt_<R>(v2) / rsqrt_<R>(p_c * gam / rho_c);
+        if (mach > R(1)) {
+#pragma unroll
+            for (int s = 0; s < 5; ++s) ub[s] = u[s];
+            return;
+        }
+        bc_primitive<R>(u, gm1, wi, st);
+        const R radicant = R(1) + R(0.5) * gm1 * mach2;
+        const R p_inlet = (R)pc.bc_total_p * rpow<R>(radicant, -gam / gm1);
+        const R ge1 = (mach >= R(1)) ? R(1) : R(0);
+        const R p_bc = ge1 * wi[4] + (R(1) - ge1) * R(0.99) * p_inlet;
+        const R t_int = gam * mach2 * (wi[4] / wi[0]);
+        wb[0] = gam * mach2 * (p_bc / t_int);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) wb[1 + d] = wi[1 + d];
+        wb[4] = p_bc;
+        bc_conservative<R>(wb, gm1, ub);
+        return;
+    }
+    bc_primitive<R>(u, gm1, wi, st);
+    if (type == BC_INFLOW) {
+        const R nrm[3] = {-n[0], -n[1], -n[2]};
+        R vni = R(0);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) vni += wi[1 + d] * nrm[d];
+        const R rho_c = positive<R>(u[0], st);
+        const R ci = rsqrt_<R>(pressure_ieee<R>(u, gm1, st) * gam / rho_c);   // compute_sound (:535-543)
+        const R mach_inf = (R)pc.bc_mach_inf;
+        R p_bc, t_bc, vmag;
+        if (mach_inf < R(1)) {
+            const R rpos = vni + R(2) * ci / gm1;
+            const R H = u[4] / wi[0] + wi[4] / wi[0];
+            const R a = R(1) + R(2) / gm1;
+            const R b = R(-2) * rpos;
+            const R c = R(0.5) * gm1 * (rpos * rpos - R(2) * H);
+            const R t1 = R(-0.5) * b / a;
+            const R t2 = R(0.5) * rsqrt_<R>(b * b - R(4) * a * c) / a;
+            const R cb = fmax(t1 + t2, t1 - t2);
+            vmag = rpos - R(2) * cb / gm1;
+            const R mach_bc = vmag / cb;
+            const R radicant = R(1) + R(0.5) * gm1 * mach_bc * mach_bc;
+            p_bc = (R)pc.bc_total_p * rpow<R>(radicant, -gam / gm1);
+            t_bc = (R)pc.bc_total_t * rpow<R>(radicant, R(-1));
+            wb[0] = gam * mach2 * (p_bc / t_bc);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) wb[1 + d] = vmag * nrm[d];
+        } else {
+            const R radicant = R(1) + R(0.5) * gm1 * mach2;
+            p_bc = (R)pc.bc_total_p * rpow<R>(radicant, -gam / gm1);
+            t_bc = (R)pc.bc_total_t * rpow<R>(radicant, R(-1));
+            wb[0] = gam * mach2 * (p_bc / t_bc);
+            const R cb = rsqrt_<R>(gam * p_bc / wb[0]);
+            vmag = mach_inf * cb;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) wb[1 + d] = -vmag * n[d];
+        }
+        wb[4] = p_bc;
+        bc_conservative<R>(wb, gm1, ub);
+        return;
+    }
+    if (type == BC_RIEMANN) {
+        R we[5];
+        we[0] = R(1);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) we[1 + d] = (R)pc.bc_v_inf[d];
+        we[4] = R(1) / (gam * mach2);
+        const R ci = rsqrt_<R>(wi[4] * gam / wi[0]), ce = rsqrt_<R>(we[4] * gam / we[0]);
+        R vni = R(0), vne = R(0);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) { vni = vni + wi[1 + d] * n[d]; vne = vne + we[1 + d] * n[d]; }
+        const R rout = vni + R(2) / gm1 * ci, rinc = vne - R(2) / gm1 * ce;
+        const R vnb = R(0.5) * (rout + rinc), cb = R(0.25) * gm1 * (rout - rinc);
+        if (rabs<R>(vnb) >= rabs<R>(cb)) {
+#pragma unroll
+            for (int s = 0; s < 5; ++s) wb[s] = vnb < R(0) ? we[s] : wi[s];
+        } else {
+            const R* w = vnb < R(0) ? we : wi;
+            const R vn = vnb < R(0) ? vne : vni;
+            // compute_entropy_measure (:414-421): p rho^-gam of a checked density
+            const R ent = w[0] < R(0) ? (R)BIG_NUMBER : w[4] * rpow<R>(w[0], -gam);
+            if (w[0] < R(0) && st) atomicOr(st, ST_NONPHYSICAL);
+            const R rb = rpow<R>(R(1) / gam * cb * cb / ent, R(1) / gm1);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) wb[1 + d] = (w[1 + d] - vn * n[d]) + vnb * n[d];
+            wb[4] = R(1) / gam * cb * cb * rb;
+            wb[0] = rb;
+        }
+        bc_conservative<R>(wb, gm1, ub);
+        return;
+    }
+    // slip wall (1001 in Euler::boundary_face_values, 1006)
+    wb[0] = wi[0]; wb[4] = wi[4];
+    const R sn[3] = {-n[0], -n[1], -n[2]};
+    R vn = R(0);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) vn = vn + wi[1 + d] * sn[d];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) wb[1 + d] = wi[1 + d] - R(2) * vn * sn[d];
+    bc_conservative<R>(wb, gm1, ub);
+}
+
+// NavierStokes::boundary_face_values_viscous_flux (navier_stokes.cpp:1354-1432): the exterior state
+// of the dissipative fluxes. 1001: no-slip, the momentum negated (its gradient is the interior's,
+// the energy gradient zero on an adiabatic wall; isothermal: the exterior temperature 2 T_wall - T);
+// 1006: the interior state and gradient.
+template <typename R>
+__device__ __forceinline__ void boundary_viscous_state(int type, const R u[5], const PhysConst& pc, R ub[5],
+                                                       unsigned* st) {
+#pragma unroll
+    for (int s = 0; s < 5; ++s) ub[s] = u[s];
+    if (type != BC_WALL) return;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) ub[1 + d] = -u[1 + d];
+    if (pc.bc_isothermal) {
+        const R gam = (R)pc.gam, gm1 = (R)pc.gm1, mach2 = (R)pc.mach2;
+        R wi[5], we[5];
+        bc_primitive<R>(u, gm1, wi, st);
+        bc_primitive<R>(ub, gm1, we, st);
+        const R t_int = gam * mach2 * (wi[4] / wi[0]);
+        const R t_ext = R(2) * (R)pc.bc_t_wall - t_int;
+        we[4] = we[0] * t_ext / (gam * mach2);
+        R w2[5];
+        bc_conservative<R>(we, gm1, w2);
+        ub[4] = w2[4];
     }
 }
 

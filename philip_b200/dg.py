@@ -54,8 +54,11 @@ class DGStrong:
 
     def __init__(self, parameters: Parameters, precision: int = _lib.PH_FP64, cell_order: int = 0,
                  stream: int | None = None, warp: float = 0.0, mapping_support_points: np.ndarray | None = None,
-                 slab: tuple[int, int] | None = None, halo=None, dist=None):
-        """warp != 0 gives the sine-warped (curvilinear) cube: every coordinate moves by
+                 slab: tuple[int, int] | None = None, halo=None, dist=None, boundaries=None):
+        """boundaries: six boundary conditions, for the sides x-, x+, y-, y+, z-, z+ (names of
+        _lib.BOUNDARY such as "wall", "riemann_farfield", or boundary_id values; "periodic" / 0
+        keeps a periodic pair). None: the periodic cube.
+        warp != 0 gives the sine-warped (curvilinear) cube: every coordinate moves by
         warp (L/2pi) sin(2pi(x-l)/L) sin(2pi(y-l)/L) sin(2pi(z-l)/L), mapping degree = p.
         mapping_support_points ([cell][3][(p+1)^3], GLL points) gives any other curved mapping.
         slab = (z_first, z_count): this process's layers of a mesh shared by several GPUs
@@ -73,6 +76,9 @@ class DGStrong:
         if mapping_support_points is not None:
             self._support = np.ascontiguousarray(mapping_support_points, dtype=np.float64)
             self.mesh.mapping_support_points = self._support.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        if boundaries is not None:
+            for f, t in enumerate(_lib.boundary_ids(boundaries)):
+                self.mesh.boundary_type[f] = t
         h = ctypes.c_void_p()
         st = ctypes.c_void_p(stream) if stream else None
         if slab is None:
@@ -383,12 +389,13 @@ class FlowSolver:
 
     def __init__(self, parameters: Parameters, precision: int = _lib.PH_FP64, cell_order: int = 0,
                  warp: float = 0.0, stream: int | None = None, slab: tuple[int, int] | None = None,
-                 halo=None, dist=None):
+                 halo=None, dist=None, boundaries=None):
         """slab / halo / dist: this process's share of a mesh over several GPUs (DGStrong);
-        the time steps, integrals and table rows are then the whole mesh's on every rank."""
+        the time steps, integrals and table rows are then the whole mesh's on every rank.
+        boundaries: the non-periodic sides (DGStrong)."""
         self.parameters = parameters
         self.dg = DGStrong(parameters, precision=precision, cell_order=cell_order, warp=warp, stream=stream,
-                           slab=slab, halo=halo, dist=dist)
+                           slab=slab, halo=halo, dist=dist, boundaries=boundaries)
         self.ode_solver = RungeKuttaODESolver(self.dg)
         self.flow_case = parameters.get("flow_solver/flow_case_type")
         X = self.dg.node_coordinates()

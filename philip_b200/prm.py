@@ -29,6 +29,7 @@ RK_ORDER = {"rk4_ex": 4, "ssprk3_ex": 3, "heun2_ex": 2, "euler_ex": 1, "RK4_3_5_
             "RK3_2_5F_3SStarPlus": 3, "RK4_3_9F_3SStarPlus": 4, "RK5_4_10F_3SStarPlus": 5}
 NON_PHYSICAL = {"return_big_number": 0, "abort_run": 1, "print_warning": 2}
 LIMITER = {"none": 0, "maximum_principle": 1, "positivity_preservingZhang2010": 2, "positivity_preservingWang2012": 3}
+THERMAL_BC = {"adiabatic": 0, "isothermal": 1}
 
 DEFAULTS = {
     "dimension": "-1", "pde_type": "advection", "use_weak_form": "true", "flux_nodes_type": "GL",
@@ -64,6 +65,9 @@ DEFAULTS = {
     "flow_solver/output_restart_files_every_x_steps": "1",
     "flow_solver/output_restart_files_every_dt_time_intervals": "0.0",
     "limiter/bound_preserving_limiter": "none", "limiter/min_density": "1e-13",
+    "euler/angle_of_attack": "0.0", "euler/side_slip_angle": "0.0",
+    "navier_stokes/thermal_boundary_condition_type": "adiabatic",
+    "navier_stokes/nondimensionalized_isothermal_wall_temperature": "1.0",
     "flow_solver/taylor_green_vortex/expected_kinetic_energy_at_final_time": "0",
     "flow_solver/taylor_green_vortex/expected_theoretical_dissipation_rate_at_final_time": "0",
 }
@@ -233,6 +237,10 @@ class Parameters:
         p.pressure_shift = self.reference_pressure()
         p.bound_preserving_limiter = LIMITER[self.get("limiter/bound_preserving_limiter")]
         p.min_density = float(self.get("limiter/min_density"))
+        p.angle_of_attack = float(self.get("euler/angle_of_attack"))
+        p.side_slip_angle = float(self.get("euler/side_slip_angle"))
+        p.thermal_boundary_condition_type = THERMAL_BC[self.get("navier_stokes/thermal_boundary_condition_type")]
+        p.isothermal_wall_temperature = float(self.get("navier_stokes/nondimensionalized_isothermal_wall_temperature"))
         return p
 
     def reference_pressure(self) -> float:
@@ -273,4 +281,10 @@ class Parameters:
                 self.get("ODE solver/rrk root solver/relaxation_runge_kutta_root_tolerance")),
             "bound_preserving_limiter": self.get("limiter/bound_preserving_limiter"),
             "min_density": float(self.get("limiter/min_density")),
+            "nondimensionalized_constant_viscosity": float(self.get("navier_stokes/nondimensionalized_constant_viscosity")),
+            "angle_of_attack": float(self.get("euler/angle_of_attack")),
+            "side_slip_angle": float(self.get("euler/side_slip_angle")),
+            "thermal_boundary_condition_type": self.get("navier_stokes/thermal_boundary_condition_type"),
+            "nondimensionalized_isothermal_wall_temperature": float(
+                self.get("navier_stokes/nondimensionalized_isothermal_wall_temperature")),
         }
