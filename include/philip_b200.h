@@ -110,6 +110,11 @@ typedef struct ph_params {
     double side_slip_angle;
     int thermal_boundary_condition_type;
     double isothermal_wall_temperature;
+    /* use_projected_entropy_variables_for_nsfr_boundary_term (all_parameters.cpp:399; default 0):
+     * the split form's boundary states and convective boundary flux take the face state of the
+     * projected entropy variables instead of the interpolated solution (strong_dg.cpp:2255-2273).
+     * On collocated GLL nodes the two agree to rounding. */
+    int use_projected_entropy_variables_for_nsfr_boundary_term;
 } ph_params;
 
 /* Periodic cube [left,right]^3 with n^3 cells (PeriodicCubeFlow::generate_grid,
@@ -127,7 +132,7 @@ typedef struct ph_mesh_desc {
      * of degree grid_degree on GLL support points. The GPU path takes grid_degree =
      * poly_degree; split or conservative, any FR type (the weight-adjusted inverse mass);
      * GLL or GL flux nodes, overintegration 0..2; Navier-Stokes with bassi_rebay_2 or
-     * central_visc_flux and flux_reconstruction_aux = kDG.
+     * central_visc_flux (and, on collocated GLL nodes, flux_reconstruction_aux = kDG).
      * Not a reference grid:
      * the construction follows the reference's curved periodic grids
      * (src/mesh/grids/curved_periodic_grid.cpp) with this warp. */
@@ -145,8 +150,9 @@ typedef struct ph_mesh_desc {
      * Navier-Stokes: no-slip, adiabatic or isothermal), 1002 pressure outflow, 1003 inflow,
      * 1004 Riemann farfield, 1005 farfield, 1006 slip wall, 1007 extrapolation. Navier-Stokes
      * takes 1001 and 1006 (NavierStokes::boundary_face_values_viscous_flux defines no viscous
-     * exterior state for the others). Contexts on affine meshes with collocated GLL nodes
-     * (ph_ctx_create); as a flow case's grid sets boundary ids, e.g. channel_flow.cpp:324-343. */
+     * exterior state for the others). Contexts on affine meshes (ph_ctx_create; GLL or GL flux
+     * nodes, overintegration 0..2); as a flow case's grid sets boundary ids, e.g.
+     * channel_flow.cpp:324-343. */
     int boundary_type[6];
 } ph_mesh_desc;
 

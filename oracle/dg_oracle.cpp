@@ -1381,15 +1381,18 @@ void Solver::assemble_residual(const double* U, double* R) {
                 for (int a = 0; a < 3; ++a) np[a] /= J;
                 double cf[5], df[5] = {0, 0, 0, 0, 0};
                 if (bt) {
-                    // the interior state interpolated to the face (the projected entropy variables'
-                    // state only with use_projected_entropy_variables_for_nsfr_boundary_term, off by
-                    // default, strong_dg.cpp:2255-2273); the penalty is this cell's (dg_base.cpp:563)
+                    // the interior state interpolated to the face, or with
+                    // use_projected_entropy_variables_for_nsfr_boundary_term (split form) the state of the
+                    // projected entropy variables (strong_dg.cpp:2255-2273); the dissipative flux's
+                    // interior side stays the interpolated state (:2291-2298); the penalty is this
+                    // cell's (dg_base.cpp:563)
+                    const double* us = (split && prm.bc_projected) ? ui : ri;
                     double ub[5];
-                    phys.boundary_state(bt, np, ri, ub);
-                    phys.conv_num_flux(ri, ub, np, cf);
+                    phys.boundary_state(bt, np, us, ub);
+                    phys.conv_num_flux(us, ub, np, cf);
                     if (viscous) {
                         double uv[5], gv[5][3];
-                        phys.boundary_viscous_state(bt, ri, gi, uv, gv);
+                        phys.boundary_viscous_state(bt, us, gi, uv, gv);
                         phys.diss_boundary_flux(bt, ri, uv, gi, gv, np, penalty_of(c, f), df);
                     }
                 } else {

@@ -76,6 +76,8 @@ struct Params {
     double angle_of_attack = 0.0, side_slip_angle = 0.0;
     int thermal_bc = THERMAL_ADIABATIC;
     double wall_temperature = 1.0;
+    // use_projected_entropy_variables_for_nsfr_boundary_term (all_parameters.cpp:399, default false)
+    int bc_projected = 0;
 };
 
 // One-dimensional operators on the reference interval [0,1]

@@ -48,7 +48,7 @@ class OrcParams(ctypes.Structure):
         "constant_viscosity", "sipg_penalty_factor", "atol", "rtol", "rrk_tol")] + [
         ("limiter", ctypes.c_int), ("min_density", ctypes.c_double),
         ("angle_of_attack", ctypes.c_double), ("side_slip_angle", ctypes.c_double),
-        ("thermal_bc", ctypes.c_int), ("wall_temperature", ctypes.c_double)]
+        ("thermal_bc", ctypes.c_int), ("wall_temperature", ctypes.c_double), ("bc_projected", ctypes.c_int)]
 
 
 _lib = None
@@ -136,6 +136,7 @@ def make_params(cfg: dict) -> OrcParams:
     p.side_slip_angle = cfg.get("side_slip_angle", 0.0) * pi / 180.0
     p.thermal_bc = THERMAL_BC[cfg.get("thermal_boundary_condition_type", "adiabatic")]
     p.wall_temperature = cfg.get("nondimensionalized_isothermal_wall_temperature", 1.0)
+    p.bc_projected = int(cfg.get("use_projected_entropy_variables_for_nsfr_boundary_term", False))
     return p
 
 

@@ -25,6 +25,7 @@ struct orc_params {
     double angle_of_attack, side_slip_angle;   // radians
     int thermal_bc;
     double wall_temperature;
+    int bc_projected;
 };
 
 static Params to_params(const orc_params* p) {
@@ -42,6 +43,7 @@ static Params to_params(const orc_params* p) {
     q.limiter = p->limiter; q.min_density = p->min_density;
     q.angle_of_attack = p->angle_of_attack; q.side_slip_angle = p->side_slip_angle;
     q.thermal_bc = p->thermal_bc; q.wall_temperature = p->wall_temperature;
+    q.bc_projected = p->bc_projected;
     return q;
 }
 

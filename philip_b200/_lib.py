@@ -58,7 +58,8 @@ class PhParams(ctypes.Structure):
         ("use_relaxation_runge_kutta", ctypes.c_int), ("relaxation_runge_kutta_root_tolerance", ctypes.c_double),
         ("bound_preserving_limiter", ctypes.c_int), ("min_density", ctypes.c_double),
         ("angle_of_attack", ctypes.c_double), ("side_slip_angle", ctypes.c_double),
-        ("thermal_boundary_condition_type", ctypes.c_int), ("isothermal_wall_temperature", ctypes.c_double)]
+        ("thermal_boundary_condition_type", ctypes.c_int), ("isothermal_wall_temperature", ctypes.c_double),
+        ("use_projected_entropy_variables_for_nsfr_boundary_term", ctypes.c_int)]
 
 
 class PhMeshDesc(ctypes.Structure):

@@ -412,7 +412,6 @@ bool has_boundaries(const ph_mesh_desc* mesh) {
 // Non-periodic meshes: what the boundary terms take (nullptr when supported).
 const char* boundary_reason(const ph_mesh_desc* mesh, const ph_params* prm) {
     if (!has_boundaries(mesh)) return nullptr;
-    if (uncollocated(prm)) return "boundary conditions: collocated GLL flux nodes without overintegration";
     if (is_curvilinear(mesh)) return "boundary conditions: affine meshes";
     if (prm->pde_type == 1)
         for (int f = 0; f < 6; ++f) {
@@ -453,8 +452,6 @@ const char* uncollocated_reason(const ph_mesh_desc* mesh, const ph_params* prm) 
         if (prm->pde_type != 0 && prm->diss_num_flux == 0)
             return "curvilinear Navier-Stokes takes bassi_rebay_2 or central_visc_flux (the SIPG penalty's cell "
                    "extent on curved cells is not restated)";
-        if (prm->pde_type != 0 && prm->flux_reconstruction_aux != 0)
-            return "curvilinear Navier-Stokes takes flux_reconstruction_aux = kDG";
     }
     if (prm->precision != PH_FP64) return "uncollocated flux nodes take the FP64 path";
     if (prm->use_relaxation_runge_kutta) return "uncollocated flux nodes: no relaxation RK";
@@ -692,6 +689,7 @@ ph::PhysConst physics_constants(const ph_params* prm, double h, double& penalty)
     pc.bc_mach_inf = prm->mach_infinity;
     pc.bc_t_wall = prm->isothermal_wall_temperature;
     pc.bc_isothermal = prm->thermal_boundary_condition_type == 1;
+    pc.bc_projected = prm->use_split_form && prm->use_projected_entropy_variables_for_nsfr_boundary_term;
     return pc;
 }
 
@@ -1181,7 +1179,7 @@ int dispatch_gl(ph_ctx* c, int kernel, const ph::StageArgs& a) {
     static const char* const kName[] = {"face-value kernel", "auxiliary kernel", "stage kernel",
                                         "inverse-mass kernel"};
     NvtxRange nvtx(kName[kernel]);
-    const ph::GlArgs g{c->d_gl, c->d_t1, c->d_t2, c->d_vis, c->d_glvm, c->d_glfn};
+    const ph::GlArgs g{c->d_gl, c->d_t1, c->d_t2, c->d_vis, c->d_glvm, c->d_glfn, c->d_fb};
     cudaError_t e;
     timer_begin(c);
     switch (c->N1) {
@@ -1557,8 +1555,9 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
     if (c->limiter) bad |= dalloc(&c->d_ltab, 1);
     if (c->nb) {   // boundary faces: their types, and (Navier-Stokes) their viscous fluxes in the arithmetic type
         bad |= dalloc(&c->d_btype, (size_t)c->nb);
-        if (c->visc) {
-            const size_t fb = (size_t)c->nb * 4 * c->N1 * c->N1;
+        if (c->visc) {   // per boundary face 4 values at each face flux node
+            const int nf = gl ? c->NQ * c->NQ : c->N1 * c->N1;
+            const size_t fb = (size_t)c->nb * 4 * nf;
             bad |= dalloc(&c->d_fb, c->fp32 ? (fb + 1) / 2 : fb);
         }
     }

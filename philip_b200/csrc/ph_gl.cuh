@@ -67,7 +67,60 @@ struct GlArgs {
     // [nc][6][3][nq^2] the face's metric column C[:, f / 2]
     const double* vmet;
     const double* fnrm;
+    // boundary faces of a non-periodic mesh (nbr = -1 - k, a.btype[k]): [nb][4][nq^2] the outward
+    // boundary viscous flux F*_v . n at the face nodes, written by the auxiliary kernel
+    double* fb;
 };
+
+// Boundary faces (out of line: only boundary face nodes call them, and the periodic path keeps its
+// register allocation). The viscous boundary state of a face node (component s) from the cell's own
+// face values (stride NF), for the auxiliary equation's lift.
+static __device__ __noinline__ double gl_bnd_visc_state(int bt, const double* own, int NF, int s,
+                                                        const PhysConst& pc) {
+    double u[5], ub[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) u[k] = __ldg(&own[k * NF]);
+    boundary_viscous_state<double>(bt, u, pc, ub, nullptr);
+    return s == 0 ? ub[0] : s == 1 ? ub[1] : s == 2 ? ub[2] : s == 3 ? ub[3] : ub[4];
+}
+// The outward boundary viscous flux at a face node of face f (evaluate_auxiliary_flux on a boundary,
+// viscous_numerical_flux.cpp:66-328): the viscous boundary state of us (the interpolated face state r,
+// or the projected one), BR2 / SIPG with its gradient, the central flux with the interior one, no heat
+// flux on an adiabatic 1001 wall; the interior side is r.
+static __device__ __noinline__ void gl_bnd_visc_flux(int bt, const double r[5], const double us[5],
+                                                     const double g[5][3], int f, const PhysConst& pc, double pen,
+                                                     double out[4]) {
+    Cst<double> cst; cst.load(pc);
+    const int dn = f >> 1;
+    const double sg = (f & 1) ? 1.0 : -1.0;
+    double ub[5];
+    boundary_viscous_state<double>(bt, us, pc, ub, nullptr);
+    const bool ad = bt == BC_WALL && !pc.bc_isothermal;
+    double gb[5][3];
+    for (int s = 0; s < 5; ++s)
+        for (int e = 0; e < 3; ++e) gb[s][e] = (ad && s == 4) ? 0.0 : g[s][e];
+    double Fi[3][4], Fe[3][4];
+    viscous_flux<double>(r, g, pc.use_const_visc, cst, Fi, 7, nullptr, ad);
+    viscous_flux<double>(ub, pc.diss_flux == DF_CENTRAL ? g : gb, pc.use_const_visc, cst, Fe, 7, nullptr, ad);
+    for (int k = 0; k < 4; ++k) out[k] = 0.5 * (sg * Fi[dn][k] + sg * Fe[dn][k]);
+    if (pc.diss_flux == DF_SIPG) {
+        double J[5][3];
+        for (int s = 0; s < 5; ++s)
+            for (int e = 0; e < 3; ++e) J[s][e] = (e == dn) ? (r[s] - ub[s]) * sg : 0.0;
+        viscous_flux<double>(r, J, pc.use_const_visc, cst, Fi, 7, nullptr, ad);
+        viscous_flux<double>(ub, J, pc.use_const_visc, cst, Fe, 7, nullptr, ad);
+        for (int k = 0; k < 4; ++k) out[k] = out[k] - pen * (0.5 * (sg * Fi[dn][k] + sg * Fe[dn][k]));
+    }
+}
+// The convective boundary state of a face node (Euler::boundary_face_values) for outward normal
+// sg e_dn of face f.
+static __device__ __noinline__ void gl_bnd_state(int bt, const double r[5], int f, const PhysConst& pc,
+                                                 double ub[5], unsigned* st) {
+    const int dn = f >> 1;
+    const double sg = (f & 1) ? 1.0 : -1.0;
+    const double nrm[3] = {dn == 0 ? sg : 0.0, dn == 1 ? sg : 0.0, dn == 2 ? sg : 0.0};
+    boundary_state<double>(bt, nrm, r, pc, ub, st);
+}
 
 template <bool SPLIT> __host__ __device__ constexpr int gl_t1_width() { return SPLIT ? 10 : 5; }
 constexpr int GL_T2W = 8;
@@ -425,7 +478,9 @@ __device__ __forceinline__ void gl_aux_gradient(const StageArgs& a, const GlArgs
         const int f = it / (5 * NF), s = (it / NF) % 5, q2 = it % NF;
         const int cn = __ldg(&a.nbr[cell * 6 + f]);
         const double uo = __ldg(&g.t1[(((size_t)cell * 6 + f) * T1W + s) * NF + q2]);
-        const double ue = __ldg(&g.t1[(((size_t)cn * 6 + (f ^ 1)) * T1W + s) * NF + q2]);
+        const double ue = cn >= 0 ? __ldg(&g.t1[(((size_t)cn * 6 + (f ^ 1)) * T1W + s) * NF + q2])
+                                  : gl_bnd_visc_state(__ldg(&a.btype[-1 - cn]),
+                                                      g.t1 + ((size_t)cell * 6 + f) * T1W * NF + q2, NF, s, a.pc);
         const double sgn = (f & 1) ? 1.0 : -1.0;
         face[it] = tab->wq[q2 % NQ] * tab->wq[q2 / NQ] * ((0.5 * (uo + ue) - uo) * sgn);
     }
@@ -557,6 +612,23 @@ gl_aux_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab T
 #pragma unroll
                 for (int l = 0; l < NQ; ++l) v += rw[l] * row[gl_line_node<NQ>(dn, q2, l)];
                 gq[s][d] = v;
+            }
+        }
+        if (a.btype) {   // a boundary face: its outward boundary viscous flux for the stage kernel
+            const int cn = __ldg(&a.nbr[cell * 6 + f]);
+            if (cn < 0) {
+                double us[5], out[4];
+#pragma unroll
+                for (int s = 0; s < 5; ++s) us[s] = r[s];
+                if (SPLIT && a.pc.bc_projected) {   // the face state of the projected entropy variables
+                    double v[5];
+#pragma unroll
+                    for (int s = 0; s < 5; ++s) v[s] = __ldg(&g.t1[(((size_t)cell * 6 + f) * T1W + 5 + s) * NF + q2]);
+                    gl_cons_from_entropy(v, cst.gam, cst.gm1, us);
+                }
+                gl_bnd_visc_flux(__ldg(&a.btype[-1 - cn]), r, us, gq, f, a.pc, a.pen, out);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) g.fb[((size_t)(-1 - cn) * 4 + k) * NF + q2] = out[k];
             }
         }
         double F[3][4];
@@ -873,12 +945,28 @@ gl_stage_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab
         const int dn = f >> 1, side = f & 1;
         const double sgn = side ? 1.0 : -1.0;
         const int cn = __ldg(&a.nbr[cell * 6 + f]);
+        const bool bnd = cn < 0;   // a boundary face (assemble_boundary_term_strong, strong_dg.cpp:1582-2366)
         const double* to = g.t1 + ((size_t)cell * 6 + f) * T1W * NF + q2;
-        const double* te = g.t1 + ((size_t)cn * 6 + (f ^ 1)) * T1W * NF + q2;
+        const double* te = g.t1 + ((size_t)(bnd ? cell : cn) * 6 + (f ^ 1)) * T1W * NF + q2;
         double uo[5], ue[5], ro[5], re[5];
 #pragma unroll
         for (int s = 0; s < 5; ++s) { ro[s] = __ldg(&to[s * NF]); re[s] = __ldg(&te[s * NF]); }
-        if constexpr (SPLIT) {
+        if (bnd) {
+            // the convective flux between the interpolated face state (the projected one with
+            // use_projected_entropy_variables_for_nsfr_boundary_term, :2255-2273) and its boundary state
+            double ub[5];
+#pragma unroll
+            for (int s = 0; s < 5; ++s) uo[s] = ro[s];
+            if (SPLIT && a.pc.bc_projected) {
+                double vo[5];
+#pragma unroll
+                for (int s = 0; s < 5; ++s) vo[s] = __ldg(&to[(5 + s) * NF]);
+                gl_cons_from_entropy(vo, cst.gam, cst.gm1, uo);
+            }
+            gl_bnd_state(__ldg(&a.btype[-1 - cn]), uo, f, a.pc, ub, a.status);
+#pragma unroll
+            for (int s = 0; s < 5; ++s) ue[s] = ub[s];
+        } else if constexpr (SPLIT) {
             double vo[5], ve[5];
 #pragma unroll
             for (int s = 0; s < 5; ++s) { vo[s] = __ldg(&to[(5 + s) * NF]); ve[s] = __ldg(&te[(5 + s) * NF]); }
@@ -909,7 +997,7 @@ gl_stage_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab
         if constexpr (VISC) {
             // each side's F_v(u, q) . e_dn at the face node, from the auxiliary kernel
             const double* ao = g.t2 + ((size_t)cell * 6 + f) * GL_T2W * NF + q2;
-            const double* ae = g.t2 + ((size_t)cn * 6 + (f ^ 1)) * GL_T2W * NF + q2;
+            const double* ae = g.t2 + ((size_t)(bnd ? cell : cn) * 6 + (f ^ 1)) * GL_T2W * NF + q2;
             double Fo[4], Fe[4];
 #pragma unroll
             for (int k = 0; k < 4; ++k) { Fo[k] = __ldg(&ao[k * NF]); Fe[k] = __ldg(&ae[k * NF]); }
@@ -919,8 +1007,9 @@ gl_stage_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab
             const double* FR = side ? Fe : Fo;
             double Fd[4];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) Fd[k] = 0.5 * (FL[k] + FR[k]);
-            if (df == DF_SIPG) {
+            for (int k = 0; k < 4; ++k)   // boundary: F*_v . e_dn = sgn (F*_v . n_out) of the auxiliary kernel
+                Fd[k] = bnd ? sgn * __ldg(&g.fb[((size_t)(-1 - cn) * 4 + k) * NF + q2]) : 0.5 * (FL[k] + FR[k]);
+            if (df == DF_SIPG && !bnd) {
                 double jump[5][3];
 #pragma unroll
                 for (int s = 0; s < 5; ++s)

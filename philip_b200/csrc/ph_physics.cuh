@@ -37,6 +37,7 @@ struct PhysConst {
     // Mach number, and the wall's thermal condition (isothermal: wall temperature t_wall)
     double bc_v_inf[3], bc_p_inf, bc_total_p, bc_total_t, bc_mach_inf, bc_t_wall;
     int bc_isothermal;
+    int bc_projected;   // use_projected_entropy_variables_for_nsfr_boundary_term (uncollocated split form)
 };
 
 template <typename R> struct Cst {

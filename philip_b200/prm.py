@@ -68,6 +68,7 @@ DEFAULTS = {
     "euler/angle_of_attack": "0.0", "euler/side_slip_angle": "0.0",
     "navier_stokes/thermal_boundary_condition_type": "adiabatic",
     "navier_stokes/nondimensionalized_isothermal_wall_temperature": "1.0",
+    "use_projected_entropy_variables_for_nsfr_boundary_term": "false",
     "flow_solver/taylor_green_vortex/expected_kinetic_energy_at_final_time": "0",
     "flow_solver/taylor_green_vortex/expected_theoretical_dissipation_rate_at_final_time": "0",
 }
@@ -241,6 +242,8 @@ class Parameters:
         p.side_slip_angle = float(self.get("euler/side_slip_angle"))
         p.thermal_boundary_condition_type = THERMAL_BC[self.get("navier_stokes/thermal_boundary_condition_type")]
         p.isothermal_wall_temperature = float(self.get("navier_stokes/nondimensionalized_isothermal_wall_temperature"))
+        p.use_projected_entropy_variables_for_nsfr_boundary_term = int(
+            _b(self.get("use_projected_entropy_variables_for_nsfr_boundary_term")))
         return p
 
     def reference_pressure(self) -> float:
@@ -287,4 +290,6 @@ class Parameters:
             "thermal_boundary_condition_type": self.get("navier_stokes/thermal_boundary_condition_type"),
             "nondimensionalized_isothermal_wall_temperature": float(
                 self.get("navier_stokes/nondimensionalized_isothermal_wall_temperature")),
+            "use_projected_entropy_variables_for_nsfr_boundary_term": _b(
+                self.get("use_projected_entropy_variables_for_nsfr_boundary_term")),
         }

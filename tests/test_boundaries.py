@@ -11,8 +11,14 @@ boundary term is pinned to the periodic path, which the golden energy values pin
 kept by farfield boundaries and a fluid at rest by Navier-Stokes walls.
 GPU: residuals against the oracle within 1e-12 relative max-norm (Euler: every boundary type, split
 and conservative, FR; Navier-Stokes: BR2 / SIPG / central, adiabatic and isothermal walls, slip walls,
-an FR auxiliary correction, p = 1..6), the precision form within 1e-5, three RK4 steps within 1e-11.
+FR auxiliary corrections, p = 1..6; collocated GLL nodes, GL flux nodes and overintegration, with and
+without use_projected_entropy_variables_for_nsfr_boundary_term), the precision form within 1e-5,
+three RK steps within 1e-11.
+On GL nodes the mirror test holds for the conservative form, and for the split form with
+use_projected_entropy_variables_for_nsfr_boundary_term; by default the split form's boundary flux
+takes the interpolated face state and the interior faces the projected one (pinned below).
 """
+import inspect
 import math
 
 import numpy as np
@@ -28,7 +34,10 @@ GAMMA = 1.4
 
 
 def _params(**kw):
-    extra = {k: kw.pop(k) for k in list(kw) if "/" in k}
+    """prm_dict's keywords, plus any .prm key given by its name (e.g. flux_nodes_type,
+    "euler/angle_of_attack")."""
+    named = inspect.signature(prm_dict).parameters
+    extra = {k: kw.pop(k) for k in list(kw) if k not in named}
     d = prm_dict(**kw)
     d.update(extra)
     return Parameters.from_dict(d)
@@ -166,11 +175,20 @@ def _mirror(U, n, N1):
     return B.reshape(-1)
 
 
+PROJ = "use_projected_entropy_variables_for_nsfr_boundary_term"
 MIRROR_CASES = [
     ("split_CH_roe_p2", dict(poly_degree=2, split=True, two_point="CH", conv="roe"), "wall"),
     ("split_IR_ec_p3", dict(poly_degree=3, split=True, two_point="IR", conv="two_point_flux"), "slip_wall"),
     ("conservative_roe_p3", dict(poly_degree=3, split=False, conv="roe"), "wall"),
     ("conservative_lxf_cHU_p2", dict(poly_degree=2, split=False, conv="lax_friedrichs", fr="cHU"), "slip_wall"),
+    ("gl_conservative_roe_p2", dict(poly_degree=2, split=False, conv="roe", flux_nodes_type="GL"), "wall"),
+    ("gll_overint1_conservative_roe_p2", dict(poly_degree=2, split=False, conv="roe", overintegration=1), "wall"),
+    # the uncollocated split form's interior faces take the projected entropy variables' face
+    # state: a boundary mirrors them only with the flag that gives its flux the same state
+    ("gl_split_CH_roe_p3_projected", dict(poly_degree=3, split=True, conv="roe", flux_nodes_type="GL",
+                                          **{PROJ: "true"}), "slip_wall"),
+    ("gl_overint1_split_IR_ec_p2_projected", dict(poly_degree=2, split=True, two_point="IR", conv="two_point_flux",
+                                                  flux_nodes_type="GL", overintegration=1, **{PROJ: "true"}), "wall"),
 ]
 
 
@@ -187,6 +205,22 @@ def test_oracle_slip_wall_is_the_mirrored_periodic_flow(name, kw, bt):
     err = rel_max_err(Rw, Rc)
     print(f"{name}: walls vs mirrored periodic cube {err:.2e}")
     assert err <= 1e-13
+
+
+def test_oracle_uncollocated_split_boundary_takes_the_interpolated_state_by_default():
+    """Without use_projected_entropy_variables_for_nsfr_boundary_term the boundary flux of the GL
+    split form takes the interpolated face state (strong_dg.cpp:2255-2273), which differs from the
+    projected one of the interior faces: the mirror no longer holds."""
+    prm = _params(pde="euler", poly_degree=3, split=True, conv="roe", flux_nodes_type="GL")
+    cfg = prm.oracle_cfg()
+    n, N1 = 2, 4
+    walls = Oracle(cfg, n, 0.0, 1.0, "lexicographic", boundaries=["slip_wall"] * 6)
+    cube = Oracle(cfg, 2 * n, -1.0, 1.0, "lexicographic")
+    U = perturbed_tgv(walls, seed=2, amp=0.05)
+    Rc = cube.residual(_mirror(U, n, N1)).reshape(2 * n, 2 * n, 2 * n, 5, N1 ** 3)[n:, n:, n:].reshape(-1)
+    err = rel_max_err(walls.residual(U), Rc)
+    print(f"GL split, interpolated boundary state: differs from the mirror by {err:.2e}")
+    assert err > 1e-5
 
 
 def _uniform(orc, rho, v, p):
@@ -261,6 +295,28 @@ GPU_CASES = [
     ("ns_br2_split_p6_walls_z", dict(pde="navier_stokes", poly_degree=6, diss="bassi_rebay_2", n_cells=2),
      ["periodic", "periodic", "periodic", "periodic", "wall", "wall"]),
     ("ns_sipg_split_p1_box", dict(pde="navier_stokes", poly_degree=1, n_cells=4), ["wall"] * 6),
+    # GL flux nodes (the reference's default) and overintegration
+    ("gl_euler_split_CHroe_p3_walls_y", dict(pde="euler", poly_degree=3, flux_nodes_type="GL"),
+     ["periodic", "periodic", "wall", "wall", "periodic", "periodic"]),
+    ("gl_euler_conservative_roe_p2_mixed", dict(pde="euler", poly_degree=2, split=False, conv="roe",
+                                                flux_nodes_type="GL"),
+     ["inflow", "pressure_outflow", "riemann_farfield", "riemann_farfield", "farfield", "extrapolation"]),
+    ("gl_euler_split_IR_p2_projected", dict(pde="euler", poly_degree=2, two_point="IR", conv="two_point_flux",
+                                            flux_nodes_type="GL", **{PROJ: "true"}),
+     ["slip_wall", "slip_wall", "riemann_farfield", "riemann_farfield", "periodic", "periodic"]),
+    ("gl_ns_br2_split_p3_channel", dict(pde="navier_stokes", poly_degree=3, diss="bassi_rebay_2",
+                                        flux_nodes_type="GL"),
+     ["periodic", "periodic", "wall", "wall", "periodic", "periodic"]),
+    ("gl_ns_sipg_conservative_p2_isothermal", dict(pde="navier_stokes", poly_degree=2, split=False, conv="roe",
+                                                   flux_nodes_type="GL",
+                                                   **{"navier_stokes/thermal_boundary_condition_type": "isothermal",
+                                                      "navier_stokes/nondimensionalized_isothermal_wall_temperature": 0.9}),
+     ["wall", "wall", "slip_wall", "slip_wall", "periodic", "periodic"]),
+    ("gll_overint1_ns_central_split_p2_box", dict(pde="navier_stokes", poly_degree=2, diss="central_visc_flux",
+                                                  overintegration=1), ["wall"] * 6),
+    ("gl_ns_br2_split_p4_projected_kHU", dict(pde="navier_stokes", poly_degree=4, diss="bassi_rebay_2",
+                                              flux_nodes_type="GL", fr_aux="kHU", n_cells=2, **{PROJ: "true"}),
+     ["wall", "wall", "periodic", "periodic", "slip_wall", "slip_wall"]),
 ]
 
 
@@ -293,11 +349,12 @@ def test_gpu_boundary_precision_form_close_to_oracle():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["ns_channel", "euler_riemann"])
+@pytest.mark.parametrize("case", ["ns_channel", "euler_riemann", "gl_ns_channel"])
 def test_gpu_boundary_rk_steps_match_oracle(case):
     from philip_b200.dg import DGStrong, RungeKuttaODESolver
-    if case == "ns_channel":
-        prm = _params(pde="navier_stokes", poly_degree=3, diss="bassi_rebay_2")
+    if case in ("ns_channel", "gl_ns_channel"):
+        prm = _params(pde="navier_stokes", poly_degree=3, diss="bassi_rebay_2",
+                      flux_nodes_type="GL" if case == "gl_ns_channel" else "GLL")
         bnd = ["periodic", "periodic", "wall", "wall", "periodic", "periodic"]
     else:
         prm = _params(pde="euler", poly_degree=3, split=False, conv="roe", rk="ssprk3_ex")
@@ -329,10 +386,6 @@ def _mesh(prm, bnd, **kw):
 
 WALLS_Y = ["periodic", "periodic", "wall", "wall", "periodic", "periodic"]
 REFUSED = [
-    ("gl_flux_nodes", dict(), WALLS_Y, lambda p: setattr(p, "flux_nodes_type", 0), {}, _lib.PH_ERR_UNSUPPORTED,
-     "collocated"),
-    ("overintegration", dict(), WALLS_Y, lambda p: setattr(p, "overintegration", 1), {}, _lib.PH_ERR_UNSUPPORTED,
-     "collocated"),
     ("curvilinear", dict(), WALLS_Y, None, dict(warp=0.1), _lib.PH_ERR_UNSUPPORTED, "affine"),
     ("navier_stokes_farfield", dict(pde="navier_stokes", diss="bassi_rebay_2"),
      ["riemann_farfield", "riemann_farfield", "periodic", "periodic", "periodic", "periodic"], None, {},

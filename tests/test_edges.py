@@ -84,16 +84,11 @@ def test_curvilinear_navier_stokes_with_sipg_is_refused():
 
 def test_curvilinear_gl_navier_stokes_with_sipg_is_refused():
     """GL flux nodes on curvilinear cells, like GLL ones, take BR2 or the central viscous flux
-    and kDG for the auxiliary equation."""
+    (an FR auxiliary correction is taken there: the uncollocated auxiliary kernel's weight-adjusted
+    projection carries (M + K_aux)^-1)."""
     rc, msg = _create(prm_kw=dict(pde="navier_stokes"), mesh_kw=dict(warp=0.1),
                       edit=lambda p: setattr(p, "flux_nodes_type", 0))
     assert rc == _lib.PH_ERR_UNSUPPORTED and "bassi_rebay_2" in msg
-
-    def gl_aux(p):
-        p.flux_nodes_type = 0
-        p.flux_reconstruction_aux = 2
-    rc, msg = _create(prm_kw=dict(pde="navier_stokes", diss="bassi_rebay_2"), mesh_kw=dict(warp=0.1), edit=gl_aux)
-    assert rc == _lib.PH_ERR_UNSUPPORTED and "kDG" in msg
 
 
 def test_entry_points_without_contexts_refuse_gl_flux_nodes():
