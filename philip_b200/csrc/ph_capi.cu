@@ -1068,6 +1068,10 @@ struct ph_ctx {
     int nb = 0;
     int* d_btype = nullptr;
     double* d_fb = nullptr;
+    // tile lists (first cell of each CTA's tile): the nt_int tiles without a boundary face, then
+    // the nt_bnd tiles with one
+    int* d_tiles = nullptr;
+    int nt_int = 0, nt_bnd = 0;
     size_t nalloc = 0;                  // doubles per stage-input buffer, ghost slots included
     // stage tiles [0, lo_end) and [hi_begin, nc) read ghost data (CPC-aligned, so the tiles and
     // their partial sums are those of one launch over all cells); [lo_end, hi_begin) do not
@@ -1133,7 +1137,32 @@ void timer_end(ph_ctx* c, int cls) {
     c->t_n[cls] += 1;
 }
 
+// cells per CTA of the stage and auxiliary kernels (the uncollocated ones: one)
+int cells_per_tile(const ph_ctx* c) {
+    if (c->gl) return 1;
+    int threads = 0, cpc = 1;
+    size_t smem = 0;
+    switch (c->N1) {
+    case 2: ph::stage_launch_shape<2>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
+    case 3: ph::stage_launch_shape<3>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
+    case 4: ph::stage_launch_shape<4>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
+    case 5: ph::stage_launch_shape<5>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
+    case 6: ph::stage_launch_shape<6>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
+    default: ph::stage_launch_shape<7>(c->fp32, c->visc, c->split, &threads, &cpc, &smem); break;
+    }
+    return cpc;
+}
+
 int dispatch_stage(ph_ctx* c, const ph::StageArgs& a) {
+    if (c->nb && !a.tiles) {   // non-periodic mesh: the periodic kernel on the tiles without a boundary face,
+                               // the boundary-face kernel on the others
+        if (a.cell_begin != 0 || a.nc != c->nc) return fail(PH_ERR_INVALID, "boundary faces: whole-mesh launches only");
+        ph::StageArgs ai = a, ab = a;
+        ai.btype = nullptr; ai.tiles = c->d_tiles; ai.ntiles = c->nt_int;
+        ab.btype = c->d_btype; ab.tiles = c->d_tiles + c->nt_int; ab.ntiles = c->nt_bnd;
+        if (int rc = dispatch_stage(c, ai)) return rc;
+        return dispatch_stage(c, ab);
+    }
     NvtxRange nvtx("stage kernel");
     cudaError_t e;
     timer_begin(c);
@@ -1151,12 +1180,11 @@ int dispatch_stage(ph_ctx* c, const ph::StageArgs& a) {
     return PH_OK;
 }
 
-int dispatch_aux(ph_ctx* c, const double* U, int cell_begin, int cell_end) {
+// one auxiliary-kernel launch (bnd: a tile list, with btype set the boundary-face kernel)
+static int aux_launch(ph_ctx* c, const double* U, int cell_begin, int cell_end, const ph::BoundaryArgs* bnd) {
     NvtxRange nvtx("auxiliary kernel");
     cudaError_t e;
     const double inv_h = 1.0 / c->h;
-    const ph::BoundaryArgs ba{c->d_btype, c->d_fb, c->pen};
-    const ph::BoundaryArgs* bnd = c->nb ? &ba : nullptr;
     timer_begin(c);
     switch (c->N1) {
     case 2: e = ph::launch_aux<2>(U, c->d_nbr, c->h_ops, cell_begin, cell_end, inv_h, c->pc, c->fp32, c->d_fv, c->curv ? c->d_metric : nullptr, c->stream, bnd); break;
@@ -1172,10 +1200,31 @@ int dispatch_aux(ph_ctx* c, const double* U, int cell_begin, int cell_end) {
     return PH_OK;
 }
 
+int dispatch_aux(ph_ctx* c, const double* U, int cell_begin, int cell_end) {
+    if (!c->nb) return aux_launch(c, U, cell_begin, cell_end, nullptr);
+    // non-periodic mesh: the periodic kernel on the tiles without a boundary face, then the
+    // boundary-face kernel on the others (it stores the boundary viscous fluxes)
+    if (cell_begin != 0 || cell_end != c->nc) return fail(PH_ERR_INVALID, "boundary faces: whole-mesh launches only");
+    const ph::BoundaryArgs bi{nullptr, c->d_fb, c->pen, c->d_tiles, c->nt_int};
+    const ph::BoundaryArgs bb{c->d_btype, c->d_fb, c->pen, c->d_tiles + c->nt_int, c->nt_bnd};
+    if (int rc = aux_launch(c, U, cell_begin, cell_end, &bi)) return rc;
+    return aux_launch(c, U, cell_begin, cell_end, &bb);
+}
+
 // One kernel of the uncollocated path on the stage input a.U: 0 face values, 1 auxiliary
 // equation, 2 residual / RK stage, 3 the curvilinear weight-adjusted inverse mass (timing classes:
 // other, auxiliary, stage, other).
 int dispatch_gl(ph_ctx* c, int kernel, const ph::StageArgs& a) {
+    if (c->nb && (kernel == 1 || kernel == 2) && !a.tiles) {
+        // non-periodic mesh: the periodic kernel on the cells without a boundary face, the
+        // boundary-face kernel on the others
+        if (a.cell_begin != 0 || a.nc != c->nc) return fail(PH_ERR_INVALID, "boundary faces: whole-mesh launches only");
+        ph::StageArgs ai = a, ab = a;
+        ai.btype = nullptr; ai.tiles = c->d_tiles; ai.ntiles = c->nt_int;
+        ab.btype = c->d_btype; ab.tiles = c->d_tiles + c->nt_int; ab.ntiles = c->nt_bnd;
+        if (int rc = dispatch_gl(c, kernel, ai)) return rc;
+        return dispatch_gl(c, kernel, ab);
+    }
     static const char* const kName[] = {"face-value kernel", "auxiliary kernel", "stage kernel",
                                         "inverse-mass kernel"};
     NvtxRange nvtx(kName[kernel]);
@@ -1553,6 +1602,21 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
     }
     c->limiter = prm->bound_preserving_limiter;
     if (c->limiter) bad |= dalloc(&c->d_ltab, 1);
+    std::vector<int> tiles;
+    if (c->nb) {   // the stage / auxiliary tiles without a boundary face first, then those with one
+        const int tc = cells_per_tile(c);
+        std::vector<int> tb;
+        for (int t0 = 0; t0 < c->nc; t0 += tc) {
+            bool b = false;
+            for (int cc = t0; cc < std::min(c->nc, t0 + tc); ++cc)
+                for (int f = 0; f < 6; ++f) b = b || nbr[6 * (size_t)cc + f] < 0;
+            (b ? tb : tiles).push_back(t0);
+        }
+        c->nt_int = (int)tiles.size();
+        c->nt_bnd = (int)tb.size();
+        tiles.insert(tiles.end(), tb.begin(), tb.end());
+        bad |= dalloc(&c->d_tiles, tiles.size());
+    }
     if (c->nb) {   // boundary faces: their types, and (Navier-Stokes) their viscous fluxes in the arithmetic type
         bad |= dalloc(&c->d_btype, (size_t)c->nb);
         if (c->visc) {   // per boundary face 4 values at each face flux node
@@ -1583,6 +1647,8 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
     e = cudaMemcpy(c->d_nbr, nbr.data(), nbr.size() * sizeof(int), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && c->nb)
         e = cudaMemcpy(c->d_btype, btype.data(), btype.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && c->nb)
+        e = cudaMemcpy(c->d_tiles, tiles.data(), tiles.size() * sizeof(int), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(c->d_ops, &c->h_ops, sizeof(ph::OpTab), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(c->d_itab, &itab, sizeof(ph::IntegralTab), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && c->d_gl) e = cudaMemcpy(c->d_gl, &c->h_gl, sizeof(ph::GlTab), cudaMemcpyHostToDevice);
@@ -1720,7 +1786,7 @@ int ph_ctx_destroy(ph_ctx* c) {
     void* ptrs[] = {c->d_nbr, c->d_ops, c->d_itab, c->d_sol, c->d_stA, c->d_stB, c->d_acc, c->d_carry,
                     c->d_fv, c->d_comp, c->d_tmpA, c->d_tmpB, c->d_partial, c->d_status, c->d_metric, c->d_xnode, c->d_origin, c->d_err,
                     c->d_table, c->d_counter, c->d_ent, c->d_ent_cell, c->d_halo, c->d_gl, c->d_t1, c->d_t2,
-                    c->d_vis, c->d_ltab, c->d_glvm, c->d_glfn, c->d_btype, c->d_fb};
+                    c->d_vis, c->d_ltab, c->d_glvm, c->d_glfn, c->d_btype, c->d_fb, c->d_tiles};
     if (c->side) cudaStreamSynchronize(c->side);
     for (void* p : ptrs) if (p) cudaFree(p);
     if (c->side) cudaStreamDestroy(c->side);

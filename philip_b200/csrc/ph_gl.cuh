@@ -465,7 +465,7 @@ struct GlAuxLayout {
 // the flux-node derivatives, the six faces' terms, the brackets, then H (x) H (x) H as three
 // passes over all fifteen components in place (H is square: each line is read whole before it
 // is written). Ends with a barrier.
-template <int ND, int NQ, bool SPLIT, bool CURV = false>
+template <int ND, int NQ, bool SPLIT, bool CURV = false, bool BND = false>
 __device__ __forceinline__ void gl_aux_gradient(const StageArgs& a, const GlArgs& g, const GlTab& T,
                                                 const GlTab* tab, int cell, const double* sQ, double* face,
                                                 double* sAQ) {
@@ -478,9 +478,10 @@ __device__ __forceinline__ void gl_aux_gradient(const StageArgs& a, const GlArgs
         const int f = it / (5 * NF), s = (it / NF) % 5, q2 = it % NF;
         const int cn = __ldg(&a.nbr[cell * 6 + f]);
         const double uo = __ldg(&g.t1[(((size_t)cell * 6 + f) * T1W + s) * NF + q2]);
-        const double ue = cn >= 0 ? __ldg(&g.t1[(((size_t)cn * 6 + (f ^ 1)) * T1W + s) * NF + q2])
-                                  : gl_bnd_visc_state(__ldg(&a.btype[-1 - cn]),
-                                                      g.t1 + ((size_t)cell * 6 + f) * T1W * NF + q2, NF, s, a.pc);
+        const double ue = (!BND || cn >= 0) ? __ldg(&g.t1[(((size_t)cn * 6 + (f ^ 1)) * T1W + s) * NF + q2])
+                                            : gl_bnd_visc_state(__ldg(&a.btype[-1 - cn]),
+                                                                g.t1 + ((size_t)cell * 6 + f) * T1W * NF + q2, NF, s,
+                                                                a.pc);
         const double sgn = (f & 1) ? 1.0 : -1.0;
         face[it] = tab->wq[q2 % NQ] * tab->wq[q2 / NQ] * ((0.5 * (uo + ue) - uo) * sgn);
     }
@@ -572,9 +573,12 @@ __device__ __forceinline__ void gl_contravariant(const double* vm, int q, int Q3
 // CURV: curvilinear cells (the metric at the flux nodes, g.vmet / g.fnrm): the physical
 // gradient through the weight-adjusted inverse (gl_aux_gradient), contravariant volume fluxes,
 // and each face node's F_v . C_face[:, dn] (the metric-scaled normal flux)
-template <int ND, int NQ, bool SPLIT, bool CURV = false>
+// BND: the cells with a boundary face (a tile list of them), the boundary states in the lift and the
+// boundary viscous fluxes stored for the stage kernel
+template <int ND, int NQ, bool SPLIT, bool CURV = false, bool BND = false>
 __global__ void __launch_bounds__(gl_threads<NQ>(), 2)
 gl_aux_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab T) {
+    static_assert(!(BND && CURV), "boundary faces: affine cells");
     using L = GlAuxLayout<ND, NQ, SPLIT>;
     constexpr int NT = L::NT, D3 = L::D3, Q3 = L::Q3, NF = L::NF, T1W = gl_t1_width<SPLIT>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -586,14 +590,14 @@ gl_aux_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab T
     double* sF = sm + L::oF;
     double* t0 = sm + L::oT0;
     double* t1 = sm + L::oT1;
-    const int cell = a.cell_begin + blockIdx.x;
+    const int cell = a.tiles ? __ldg(&a.tiles[blockIdx.x]) : a.cell_begin + (int)blockIdx.x;
     Cst<double> cst; cst.load(a.pc);
     const int ucv = a.pc.use_const_visc;
     gl_load_tab(g.tab, tab, NT);
     for (int i = threadIdx.x; i < 5 * D3; i += NT) sU[i] = __ldg(&a.U[(size_t)cell * 5 * D3 + i]);
     __syncthreads();
     gl_apply3<NT, NQ, ND, 5>(T.chi, sU, D3, sQ, Q3, t0, t1, 1.0, false);
-    gl_aux_gradient<ND, NQ, SPLIT, CURV>(a, g, T, tab, cell, sQ, t0, sAQ);
+    gl_aux_gradient<ND, NQ, SPLIT, CURV, BND>(a, g, T, tab, cell, sQ, t0, sAQ);
     const double* vm = CURV ? g.vmet + (size_t)cell * 10 * Q3 : nullptr;
     // per face node of the cell: F_v(u, q) . e_dn with the state's and the gradient's face values
     // (each side's half of the dissipative numerical flux, strong_dg.cpp:3354-3452)
@@ -614,7 +618,7 @@ gl_aux_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab T
                 gq[s][d] = v;
             }
         }
-        if (a.btype) {   // a boundary face: its outward boundary viscous flux for the stage kernel
+        if constexpr (BND) {   // a boundary face: its outward boundary viscous flux for the stage kernel
             const int cn = __ldg(&a.nbr[cell * 6 + f]);
             if (cn < 0) {
                 double us[5], out[4];
@@ -768,7 +772,7 @@ struct GlStageLayout {
 // scaled by |C[:, dn]| and the hybrid terms 1/2 (C_face[:, dn] + C_vol[:, dn]) (:3144-3452), and
 // the inverse mass is the weight-adjusted P diag(1 / (W det J)) P^T, P = (M+K)^-1 chi^T W
 // (dg_base.cpp:4217-4249, operators.cpp:1909-1932). The residual is then in physical units.
-template <int ND, int NQ, bool VISC, bool SPLIT, bool CURV = false>
+template <int ND, int NQ, bool VISC, bool SPLIT, bool CURV = false, bool BND = false>
 __global__ void __launch_bounds__(gl_threads<NQ>(), 2)
 gl_stage_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab T) {
     using L = GlStageLayout<ND, NQ, VISC, SPLIT, CURV>;
@@ -783,7 +787,7 @@ gl_stage_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab
     double* sF = sm + L::oF;
     double* t0 = sm + L::oT0;
     double* t1 = sm + L::oT1;
-    const int cell = a.cell_begin + blockIdx.x;
+    const int cell = a.tiles ? __ldg(&a.tiles[blockIdx.x]) : a.cell_begin + (int)blockIdx.x;
     Cst<double> cst; cst.load(a.pc);
     const int tp = a.pc.two_point, cf = a.pc.conv_flux, df = a.pc.diss_flux, ucv = a.pc.use_const_visc;
     double* sM = sm + L::oM;   // curvilinear: the cofactor at the flux nodes, [k * 3 + d][Q3]
@@ -945,7 +949,7 @@ gl_stage_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab
         const int dn = f >> 1, side = f & 1;
         const double sgn = side ? 1.0 : -1.0;
         const int cn = __ldg(&a.nbr[cell * 6 + f]);
-        const bool bnd = cn < 0;   // a boundary face (assemble_boundary_term_strong, strong_dg.cpp:1582-2366)
+        const bool bnd = BND && cn < 0;   // a boundary face (assemble_boundary_term_strong, strong_dg.cpp:1582-2366)
         const double* to = g.t1 + ((size_t)cell * 6 + f) * T1W * NF + q2;
         const double* te = g.t1 + ((size_t)(bnd ? cell : cn) * 6 + (f ^ 1)) * T1W * NF + q2;
         double uo[5], ue[5], ro[5], re[5];

@@ -23,8 +23,8 @@ static cudaError_t launch_one(const StageArgs& a, cudaStream_t s) {
         if (e != cudaSuccess) return e;
         configured[dev] = true;
     }
-    const int grid = (a.nc - a.cell_begin + CPC - 1) / CPC;
-    if (grid <= 0) return cudaErrorInvalidValue;
+    const int grid = a.tiles ? a.ntiles : (a.nc - a.cell_begin + CPC - 1) / CPC;
+    if (grid <= 0) return a.tiles ? cudaSuccess : cudaErrorInvalidValue;
     kern<<<grid, L::NT, L::bytes, s>>>(a);
     return cudaGetLastError();
 }
@@ -35,12 +35,16 @@ static cudaError_t launch_prec(const StageArgs& a, bool visc, bool split, cudaSt
     // relaxation RK's entropy estimate lives in the generic instance only
     const bool hot = split && a.pc.two_point == TP_CH && a.pc.conv_flux == CF_EC_ROE &&
                      (!visc || a.pc.diss_flux == DF_BR2) && a.ent_partial == nullptr;
-    if (a.btype) {    // boundary faces (affine cells, the generic flux set)
+    if (a.btype) {    // boundary faces (affine cells)
         if (a.metric) return cudaErrorInvalidValue;
-        if (visc) return split ? launch_one<R, N1, true, true, 0, false, true>(a, s)
-                               : launch_one<R, N1, true, false, 0, false, true>(a, s);
-        return split ? launch_one<R, N1, false, true, 0, false, true>(a, s)
-                     : launch_one<R, N1, false, false, 0, false, true>(a, s);
+        if (visc) {
+            if (split) return hot ? launch_one<R, N1, true, true, 1, false, true>(a, s)
+                                  : launch_one<R, N1, true, true, 0, false, true>(a, s);
+            return launch_one<R, N1, true, false, 0, false, true>(a, s);
+        }
+        if (split) return hot ? launch_one<R, N1, false, true, 1, false, true>(a, s)
+                              : launch_one<R, N1, false, true, 0, false, true>(a, s);
+        return launch_one<R, N1, false, false, 0, false, true>(a, s);
     }
     if (a.metric) {   // curvilinear cells
         if (!split) return visc ? launch_one<R, N1, true, false, 0, true>(a, s) : launch_one<R, N1, false, false, 0, true>(a, s);
@@ -184,11 +188,12 @@ static cudaError_t launch_aux_prec(const double* U, const int* nbr, const OpTab&
     AuxCoef<R> co{};
     for (int i = 0; i < MAXN1 * MAXN1; ++i) { co.D[i] = (R)ops.D[i]; co.Ba[i] = (R)ops.Baux[i]; }
     co.inv_wend = R(1) / (R)ops.w[0];
-    const int grid = (nc - cell_begin + CPC - 1) / CPC;
-    if (grid <= 0) return cudaErrorInvalidValue;
+    const int* tiles = bnd ? bnd->tiles : nullptr;
+    const int grid = tiles ? bnd->ntiles : (nc - cell_begin + CPC - 1) / CPC;
+    if (grid <= 0) return tiles ? cudaSuccess : cudaErrorInvalidValue;
     kern<<<grid, L::NT, bytes, s>>>(U, nbr, cell_begin, nc, CURV ? R(1) : (R)inv_h, pc, co, static_cast<R*>(Fv),
                                     metric, bnd ? bnd->btype : nullptr, bnd ? static_cast<R*>(bnd->Fb) : nullptr,
-                                    bnd ? (R)bnd->pen : R(0));
+                                    bnd ? (R)bnd->pen : R(0), tiles);
     return cudaGetLastError();
 }
 
@@ -196,7 +201,7 @@ template <int N1>
 cudaError_t launch_aux(const double* U, const int* nbr, const OpTab& ops, int cell_begin, int nc, double inv_h,
                        const PhysConst& pc, int fp32, void* Fv, const double* metric, cudaStream_t s,
                        const BoundaryArgs* bnd) {
-    if (bnd) {      // boundary faces (affine cells)
+    if (bnd && bnd->btype) {   // the boundary tiles (affine cells)
         if (metric) return cudaErrorInvalidValue;
         if (ops.aux_fr)
             return fp32 ? launch_aux_prec<float, N1, true, false, true>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, nullptr, s, bnd)
@@ -209,11 +214,11 @@ cudaError_t launch_aux(const double* U, const int* nbr, const OpTab& ops, int ce
         return fp32 ? launch_aux_prec<float, N1, false, true>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, metric, s)
                     : launch_aux_prec<double, N1, false, true>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, metric, s);
     }
-    if (ops.aux_fr)
-        return fp32 ? launch_aux_prec<float, N1, true, false>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, nullptr, s)
-                    : launch_aux_prec<double, N1, true, false>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, nullptr, s);
-    return fp32 ? launch_aux_prec<float, N1, false, false>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, nullptr, s)
-                : launch_aux_prec<double, N1, false, false>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, nullptr, s);
+    if (ops.aux_fr)   // (bnd without btype: the periodic kernel over bnd->tiles)
+        return fp32 ? launch_aux_prec<float, N1, true, false>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, nullptr, s, bnd)
+                    : launch_aux_prec<double, N1, true, false>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, nullptr, s, bnd);
+    return fp32 ? launch_aux_prec<float, N1, false, false>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, nullptr, s, bnd)
+                : launch_aux_prec<double, N1, false, false>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, nullptr, s, bnd);
 }
 
 template <int N1>
@@ -297,8 +302,8 @@ static cudaError_t launch_gl_kernel(K kern, size_t bytes, int threads, const Sta
         if (e != cudaSuccess) return e;
         configured = true;
     }
-    const int grid = a.nc - a.cell_begin;
-    if (grid <= 0) return cudaErrorInvalidValue;
+    const int grid = a.tiles ? a.ntiles : a.nc - a.cell_begin;
+    if (grid <= 0) return a.tiles ? cudaSuccess : cudaErrorInvalidValue;
     kern<<<grid, threads, bytes, s>>>(a, g, ht);
     return cudaGetLastError();
 }
@@ -310,7 +315,7 @@ static cudaError_t launch_gl_nq(int kernel, const StageArgs& a, const GlArgs& g,
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     constexpr int NT = gl_threads<NQ>();
-    static bool cfg[15][64] = {};
+    static bool cfg[21][64] = {};
     if (kernel == 0) {
         if (split) return launch_gl_kernel(gl_trace_kernel<ND, NQ, true>, GlTraceLayout<ND, NQ, true>::bytes, NT, a, g, ht,
                                            cfg[0][dev], s);
@@ -323,6 +328,12 @@ static cudaError_t launch_gl_nq(int kernel, const StageArgs& a, const GlArgs& g,
                                                g, ht, cfg[11][dev], s);
             return launch_gl_kernel(gl_aux_kernel<ND, NQ, false, true>, GlAuxLayout<ND, NQ, false>::bytes, NT, a, g, ht,
                                     cfg[12][dev], s);
+        }
+        if (a.btype) {   // the cells with a boundary face
+            if (split) return launch_gl_kernel(gl_aux_kernel<ND, NQ, true, false, true>, GlAuxLayout<ND, NQ, true>::bytes,
+                                               NT, a, g, ht, cfg[15][dev], s);
+            return launch_gl_kernel(gl_aux_kernel<ND, NQ, false, false, true>, GlAuxLayout<ND, NQ, false>::bytes, NT, a,
+                                    g, ht, cfg[16][dev], s);
         }
         if (split) return launch_gl_kernel(gl_aux_kernel<ND, NQ, true>, GlAuxLayout<ND, NQ, true>::bytes, NT, a, g, ht,
                                            cfg[2][dev], s);
@@ -343,6 +354,18 @@ static cudaError_t launch_gl_nq(int kernel, const StageArgs& a, const GlArgs& g,
                                            GlStageLayout<ND, NQ, false, true, true>::bytes, NT, a, g, ht, cfg[9][dev], s);
         return launch_gl_kernel(gl_stage_kernel<ND, NQ, false, false, true>,
                                 GlStageLayout<ND, NQ, false, false, true>::bytes, NT, a, g, ht, cfg[10][dev], s);
+    }
+    if (a.btype) {     // the cells with a boundary face
+        if (visc) {
+            if (split) return launch_gl_kernel(gl_stage_kernel<ND, NQ, true, true, false, true>,
+                                               GlStageLayout<ND, NQ, true, true>::bytes, NT, a, g, ht, cfg[17][dev], s);
+            return launch_gl_kernel(gl_stage_kernel<ND, NQ, true, false, false, true>,
+                                    GlStageLayout<ND, NQ, true, false>::bytes, NT, a, g, ht, cfg[18][dev], s);
+        }
+        if (split) return launch_gl_kernel(gl_stage_kernel<ND, NQ, false, true, false, true>,
+                                           GlStageLayout<ND, NQ, false, true>::bytes, NT, a, g, ht, cfg[19][dev], s);
+        return launch_gl_kernel(gl_stage_kernel<ND, NQ, false, false, false, true>,
+                                GlStageLayout<ND, NQ, false, false>::bytes, NT, a, g, ht, cfg[20][dev], s);
     }
     if (visc) {
         if (split) return launch_gl_kernel(gl_stage_kernel<ND, NQ, true, true>, GlStageLayout<ND, NQ, true, true>::bytes,

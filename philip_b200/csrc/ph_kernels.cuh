@@ -121,6 +121,10 @@ struct StageArgs {
     // written by the auxiliary kernel (nullptr on periodic meshes)
     const int* btype;
     const void* Fb;
+    // optional tile list: CTA b works on the tile whose first cell is tiles[b] (ntiles CTAs); the
+    // boundary-face kernels run on the tiles that touch a boundary, the periodic ones on the rest
+    const int* tiles;
+    int ntiles;
 };
 
 // Viscous terms per cell written by the auxiliary kernel and read by the stage kernel:
@@ -733,12 +737,10 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
                 const int bt = __ldg(&a.btype[k]);
                 const int no = face_node_volume_index<N1>(f, fn, (f & 1) ? N1 - 1 : 0);
                 const R sg = (f & 1) ? R(1) : R(-1);
-                const int dn = f >> 1;
-                const R nrm[3] = {dn == 0 ? sg : R(0), dn == 1 ? sg : R(0), dn == 2 ? sg : R(0)};
                 R ui[5], ub[5];
 #pragma unroll
                 for (int s = 0; s < 5; ++s) ui[s] = (R)__ldg(&a.U[((size_t)cell * 5 + s) * NP + no]);
-                boundary_state<R>(bt, nrm, ui, a.pc, ub, std::is_same<R, double>::value ? a.status : nullptr);
+                boundary_state_face<R>(bt, f, ui, a.pc, ub, std::is_same<R, double>::value ? a.status : nullptr);
 #pragma unroll
                 for (int s = 0; s < 5; ++s) tr[s * NF + fn] = ub[s];
                 if constexpr (VISC) {   // F*_v . e_d = sg (F*_v . n_out)
@@ -1052,7 +1054,7 @@ template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int FS, bool CURV 
 __global__ void __launch_bounds__(Layout<R, N1, CPC, VISC, SPLIT, CURV>::NT, Layout<R, N1, CPC, VISC, SPLIT, CURV>::MINB)
 residual_kernel(const StageArgs a) {
     residual_tile<R, N1, CPC, VISC, SPLIT, FS, CURV, !BND && stage_bulk<R, N1, CPC, VISC, SPLIT, CURV>(), BND>(
-        a, a.cell_begin + blockIdx.x * CPC);
+        a, a.tiles ? __ldg(&a.tiles[blockIdx.x]) : a.cell_begin + (int)blockIdx.x * CPC);
 }
 
 // One tile of a batch: instance index and its first cell.
@@ -1170,11 +1172,19 @@ __device__ __forceinline__ void aux_curv_flux(const R un[5], const R r[5][3], co
 // state; BR2 and SIPG take its gradient (the interior's, the energy gradient zero on an adiabatic
 // wall), the central flux the interior gradient; on an adiabatic 1001 wall both sides' fluxes drop
 // the heat flux (dissipative_flux_dot_normal, navier_stokes.cpp:1224-1264).
+// Out of line, called for the surface nodes of a boundary-face kernel only: the periodic-like
+// interior work keeps its registers (un: the node's state, g15: its gradient [5][3] row-major).
 template <typename R, int N1>
-__device__ __forceinline__ void aux_boundary_fluxes(const int* __restrict__ nbr, const int* __restrict__ btype,
-                                                    R* __restrict__ Fb, int cell, int node, const R un[5],
-                                                    const R g[5][3], const PhysConst& pc, const Cst<R>& cst, R pen) {
+__device__ __noinline__ void aux_boundary_fluxes(const int* __restrict__ nbr, const int* __restrict__ btype,
+                                                 R* __restrict__ Fb, int cell, int node, const R* un, const R* g15,
+                                                 const PhysConst& pc, R pen) {
     constexpr int NF = N1 * N1;
+    Cst<R> cst; cst.load(pc);
+    R g[5][3];
+#pragma unroll
+    for (int s = 0; s < 5; ++s)
+#pragma unroll
+        for (int e = 0; e < 3; ++e) g[s][e] = g15[s * 3 + e];
     const int cx[3] = {node % N1, (node / N1) % N1, node / (N1 * N1)};
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -1221,11 +1231,28 @@ __device__ __forceinline__ void aux_boundary_fluxes(const int* __restrict__ nbr,
     }
 }
 
+// the call above for a node on the cell's surface (a copy of its state and gradient is passed)
+template <typename R, int N1>
+__device__ __forceinline__ void aux_boundary_node(const int* __restrict__ nbr, const int* __restrict__ btype,
+                                                  R* __restrict__ Fb, int cell, int node, const R un[5],
+                                                  const R g[5][3], const PhysConst& pc, R pen) {
+    const int x = node % N1, y = (node / N1) % N1, z = node / (N1 * N1);
+    if (x != 0 && x != N1 - 1 && y != 0 && y != N1 - 1 && z != 0 && z != N1 - 1) return;
+    R uu[5], gg[15];
+#pragma unroll
+    for (int s = 0; s < 5; ++s) {
+        uu[s] = un[s];
+#pragma unroll
+        for (int e = 0; e < 3; ++e) gg[s * 3 + e] = g[s][e];
+    }
+    aux_boundary_fluxes<R, N1>(nbr, btype, Fb, cell, node, uu, gg, pc, pen);
+}
+
 template <typename R, int N1, int CPC, bool FRA, bool CURV, bool BND = false>
 __global__ void __launch_bounds__(AuxLayout<N1, CPC, FRA>::NT)
 aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, int cell_begin, int nc, R inv_h, PhysConst pc,
            AuxCoef<R> co, R* __restrict__ Fv, const double* __restrict__ metric, const int* __restrict__ btype,
-           R* __restrict__ Fb, R pen) {
+           R* __restrict__ Fb, R pen, const int* __restrict__ tiles) {
     static_assert(!(BND && CURV), "boundary faces: affine cells");
     using L = AuxLayout<N1, CPC, FRA>;
     constexpr int NP = L::NP, NF = L::NF, NT = L::NT;
@@ -1235,7 +1262,7 @@ aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, int cell_b
     R* sT = sU + CPC * 5 * NP;                // [c][face][5][NF] neighbour traces
     Cst<R> cst; cst.load(pc);
     const int tid = threadIdx.x;
-    const int cell0 = cell_begin + blockIdx.x * CPC;
+    const int cell0 = tiles ? __ldg(&tiles[blockIdx.x]) : cell_begin + (int)blockIdx.x * CPC;
     // loads unrolled so that all of a thread's loads are in flight before the first store
 #pragma unroll
     for (int it = tid; it < CPC * 5 * NP; it += NT) {
@@ -1343,7 +1370,7 @@ aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, int cell_b
                 viscous_flux<R>(un, g, pc.use_const_visc, cst, F, 7, nullptr);
             }
             if constexpr (BND) {
-                if (cell0 + c < nc) aux_boundary_fluxes<R, N1>(nbr, btype, Fb, cell0 + c, node, un, g, pc, cst, pen);
+                if (cell0 + c < nc) aux_boundary_node<R, N1>(nbr, btype, Fb, cell0 + c, node, un, g, pc, pen);
             }
 #pragma unroll
             for (int d = 0; d < 3; ++d)
@@ -1434,7 +1461,7 @@ aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, int cell_b
             R F[3][4];
             if constexpr (CURV) aux_curv_flux<R, N1>(un, g, metric, cell, node, pc.use_const_visc, cst, F);
             else viscous_flux<R>(un, g, pc.use_const_visc, cst, F, 7, nullptr);
-            if constexpr (BND) aux_boundary_fluxes<R, N1>(nbr, btype, Fb, cell, node, un, g, pc, cst, pen);
+            if constexpr (BND) aux_boundary_node<R, N1>(nbr, btype, Fb, cell, node, un, g, pc, pen);
 #pragma unroll
             for (int d = 0; d < 3; ++d)
 #pragma unroll

@@ -17,9 +17,11 @@ cudaError_t launch_stage(const StageArgs& a, int fp32, bool visc, bool split, cu
 // metric: the curvilinear cells' metric rows (nullptr on affine cells)
 // bnd: the boundary faces of a non-periodic mesh (nullptr on periodic meshes)
 struct BoundaryArgs {
-    const int* btype;   // boundary_id per boundary face
+    const int* btype;   // boundary_id per boundary face (nullptr: the periodic kernel over `tiles`)
     void* Fb;           // [nb][4][NF] boundary viscous fluxes (in the arithmetic type)
     double pen;         // SIPG penalty of a boundary face (the cell's own)
+    const int* tiles;   // first cell of each CTA's tile (ntiles CTAs)
+    int ntiles;
 };
 template <int N1>
 cudaError_t launch_aux(const double* U, const int* nbr, const OpTab& ops, int cell_begin, int nc, double inv_h,

@@ -777,6 +777,22 @@ __device__ void boundary_state(int type, const R n[3], const R u[5], const PhysC
     bc_conservative<R>(wb, gm1, ub);
 }
 
+// boundary_state for the outward normal of reference face f (+/- e_{f/2}), out of line: the kernels
+// that call it for their boundary faces keep their registers
+template <typename R>
+__device__ __noinline__ void boundary_state_face(int type, int f, const R* u, const PhysConst& pc, R* ub,
+                                                 unsigned* st) {
+    const int dn = f >> 1;
+    const R sg = (f & 1) ? R(1) : R(-1);
+    const R nrm[3] = {dn == 0 ? sg : R(0), dn == 1 ? sg : R(0), dn == 2 ? sg : R(0)};
+    R ui[5], uo[5];
+#pragma unroll
+    for (int s = 0; s < 5; ++s) ui[s] = u[s];
+    boundary_state<R>(type, nrm, ui, pc, uo, st);
+#pragma unroll
+    for (int s = 0; s < 5; ++s) ub[s] = uo[s];
+}
+
 // NavierStokes::boundary_face_values_viscous_flux (navier_stokes.cpp:1354-1432): the exterior state
 // of the dissipative fluxes. 1001: no-slip, the momentum negated (its gradient is the interior's,
 // the energy gradient zero on an adiabatic wall; isothermal: the exterior temperature 2 T_wall - T);
