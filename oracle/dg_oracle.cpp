@@ -953,7 +953,6 @@ void Solver::init(const Params& p, int n, double left, double right, int order, 
 }
 
 void Solver::set_boundaries(const int types[6]) {
-    if (!mesh.affine) throw std::runtime_error("oracle: boundaries on the affine cube only");
     for (int d = 0; d < 3; ++d)
         if ((types[2 * d] == 0) != (types[2 * d + 1] == 0))
             throw std::runtime_error("oracle: a pair of cube sides is periodic on both sides or on neither");

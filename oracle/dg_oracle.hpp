@@ -144,7 +144,7 @@ struct Solver {
     void init(const Params& p, int n, double left, double right, int order,
               double warp = 0.0, int grid_degree = 1);
     std::size_t ndofs() const { return (std::size_t)mesh.nc * ndofs_cell; }
-    // non-periodic sides of the (affine) cube: types[f] for the sides x-, x+, y-, y+, z-, z+ (0 keeps
+    // non-periodic sides of the cube: types[f] for the sides x-, x+, y-, y+, z-, z+ (0 keeps
     // a periodic pair; a pair is periodic on both sides or on neither), as the boundary_id a flow
     // case's grid gives its boundary faces (e.g. channel_flow.cpp:324-343)
     void set_boundaries(const int types[6]);

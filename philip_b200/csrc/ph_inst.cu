@@ -35,8 +35,13 @@ static cudaError_t launch_prec(const StageArgs& a, bool visc, bool split, cudaSt
     // relaxation RK's entropy estimate lives in the generic instance only
     const bool hot = split && a.pc.two_point == TP_CH && a.pc.conv_flux == CF_EC_ROE &&
                      (!visc || a.pc.diss_flux == DF_BR2) && a.ent_partial == nullptr;
+    if (a.btype && a.metric) {   // boundary faces of curvilinear cells
+        if (visc) return split ? launch_one<R, N1, true, true, 0, true, true>(a, s)
+                               : launch_one<R, N1, true, false, 0, true, true>(a, s);
+        return split ? launch_one<R, N1, false, true, 0, true, true>(a, s)
+                     : launch_one<R, N1, false, false, 0, true, true>(a, s);
+    }
     if (a.btype) {    // boundary faces (affine cells)
-        if (a.metric) return cudaErrorInvalidValue;
         if (visc) {
             if (split) return hot ? launch_one<R, N1, true, true, 1, false, true>(a, s)
                                   : launch_one<R, N1, true, true, 0, false, true>(a, s);
@@ -201,8 +206,12 @@ template <int N1>
 cudaError_t launch_aux(const double* U, const int* nbr, const OpTab& ops, int cell_begin, int nc, double inv_h,
                        const PhysConst& pc, int fp32, void* Fv, const double* metric, cudaStream_t s,
                        const BoundaryArgs* bnd) {
+    if (bnd && bnd->btype && metric) {   // the boundary tiles of curvilinear cells (kDG)
+        if (ops.aux_fr) return cudaErrorInvalidValue;
+        return fp32 ? launch_aux_prec<float, N1, false, true, true>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, metric, s, bnd)
+                    : launch_aux_prec<double, N1, false, true, true>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, metric, s, bnd);
+    }
     if (bnd && bnd->btype) {   // the boundary tiles (affine cells)
-        if (metric) return cudaErrorInvalidValue;
         if (ops.aux_fr)
             return fp32 ? launch_aux_prec<float, N1, true, false, true>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, nullptr, s, bnd)
                         : launch_aux_prec<double, N1, true, false, true>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, nullptr, s, bnd);
@@ -211,8 +220,8 @@ cudaError_t launch_aux(const double* U, const int* nbr, const OpTab& ops, int ce
     }
     if (metric) {   // curvilinear cells (kDG, checked by the host)
         if (ops.aux_fr) return cudaErrorInvalidValue;
-        return fp32 ? launch_aux_prec<float, N1, false, true>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, metric, s)
-                    : launch_aux_prec<double, N1, false, true>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, metric, s);
+        return fp32 ? launch_aux_prec<float, N1, false, true>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, metric, s, bnd)
+                    : launch_aux_prec<double, N1, false, true>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, metric, s, bnd);
     }
     if (ops.aux_fr)   // (bnd without btype: the periodic kernel over bnd->tiles)
         return fp32 ? launch_aux_prec<float, N1, true, false>(U, nbr, ops, cell_begin, nc, inv_h, pc, Fv, nullptr, s, bnd)

@@ -301,9 +301,9 @@ __device__ __forceinline__ void face_item(const Cst<R>& cst, int tp, int cf, int
             // the metric-scaled normal viscous flux F~_d = sum_k C[k][d] F_k of both sides (the
             // auxiliary kernels' face blocks; BR2 / central: their average, strong_dg.cpp:3354-3452)
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
+            for (int k = 0; k < 4; ++k) {   // (a boundary face: the trace holds the boundary flux itself)
                 const R Fo = __ldg(&fvface[(f * 4 + k) * NF + fn]);
-                const R Fn = R(0.5) * (Fo + tr[(5 + k) * NF + fn]);
+                const R Fn = (BND && bnd) ? tr[(5 + k) * NF + fn] : R(0.5) * (Fo + tr[(5 + k) * NF + fn]);
                 term[1 + k] += sgn * (Fo - Fn);
             }
         }
@@ -670,7 +670,7 @@ __device__ __forceinline__ void ls_tile_error(double err2, double* out) {
 template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int FS, bool CURV, bool BULK = false, bool BND = false>
 __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell0) {
     static_assert(!BULK || (std::is_same<R, double>::value && N1 % 2 == 0 && !CURV), "bulk staging: FP64, even N1");
-    static_assert(!BND || (!BULK && !CURV), "boundary faces: affine cells, plain loads");
+    static_assert(!BND || !BULK, "boundary faces: plain loads");
     using L = Layout<R, N1, CPC, VISC, SPLIT, CURV>;
     constexpr int NP = L::NP, NF = L::NF, NT = L::NT, TR = L::TR, NQS = L::NQS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -740,7 +740,18 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
                 R ui[5], ub[5];
 #pragma unroll
                 for (int s = 0; s < 5; ++s) ui[s] = (R)__ldg(&a.U[((size_t)cell * 5 + s) * NP + no]);
-                boundary_state_face<R>(bt, f, ui, a.pc, ub, std::is_same<R, double>::value ? a.status : nullptr);
+                unsigned* st = std::is_same<R, double>::value ? a.status : nullptr;
+                if constexpr (CURV) {   // the outward unit normal sg C[:, dn] / |C[:, dn]| at the face node
+                    const int dn = f >> 1;
+                    const double* M = a.metric + (size_t)cell * 10 * NP + no;
+                    const double m0 = __ldg(&M[(0 * 3 + dn) * NP]), m1 = __ldg(&M[(1 * 3 + dn) * NP]),
+                                 m2 = __ldg(&M[(2 * 3 + dn) * NP]);
+                    const double Jf = sqrt(m0 * m0 + m1 * m1 + m2 * m2);
+                    const R nv[3] = {(R)(sg * m0 / Jf), (R)(sg * m1 / Jf), (R)(sg * m2 / Jf)};
+                    boundary_state_normal<R>(bt, nv, ui, a.pc, ub, st);
+                } else {
+                    boundary_state_face<R>(bt, f, ui, a.pc, ub, st);
+                }
 #pragma unroll
                 for (int s = 0; s < 5; ++s) tr[s * NF + fn] = ub[s];
                 if constexpr (VISC) {   // F*_v . e_d = sg (F*_v . n_out)
@@ -1172,19 +1183,35 @@ __device__ __forceinline__ void aux_curv_flux(const R un[5], const R r[5][3], co
 // state; BR2 and SIPG take its gradient (the interior's, the energy gradient zero on an adiabatic
 // wall), the central flux the interior gradient; on an adiabatic 1001 wall both sides' fluxes drop
 // the heat flux (dissipative_flux_dot_normal, navier_stokes.cpp:1224-1264).
-// Out of line, called for the surface nodes of a boundary-face kernel only: the periodic-like
-// interior work keeps its registers (un: the node's state, g15: its gradient [5][3] row-major).
+// Out of line, called for the surface nodes of a boundary-face kernel only (un: the node's state,
+// g15: its gradient [5][3] row-major). Curvilinear cells (metric != nullptr): g15 is the reference
+// gradient, the physical one is (1/J) C g15 (as aux_curv_flux forms it), the outward unit normal is
+// sg C[:, d] / |C[:, d]| and the stored flux |C[:, d]| F*_v . n (the face Jacobian's scaling of
+// assemble_boundary_term_strong).
 template <typename R, int N1>
 __device__ __noinline__ void aux_boundary_fluxes(const int* __restrict__ nbr, const int* __restrict__ btype,
                                                  R* __restrict__ Fb, int cell, int node, const R* un, const R* g15,
-                                                 const PhysConst& pc, R pen) {
-    constexpr int NF = N1 * N1;
+                                                 const PhysConst& pc, R pen, const double* __restrict__ metric) {
+    constexpr int NF = N1 * N1, NP = N1 * N1 * N1;
     Cst<R> cst; cst.load(pc);
     R g[5][3];
 #pragma unroll
     for (int s = 0; s < 5; ++s)
 #pragma unroll
         for (int e = 0; e < 3; ++e) g[s][e] = g15[s * 3 + e];
+    double C[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (metric) {   // the physical gradient
+        const double* M = metric + (size_t)cell * 10 * NP + node;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) C[i] = __ldg(&M[i * NP]);
+        const double iJ = __ldg(&M[9 * NP]);
+#pragma unroll
+        for (int s = 0; s < 5; ++s) {
+            const double r0 = g15[s * 3 + 0], r1 = g15[s * 3 + 1], r2 = g15[s * 3 + 2];
+#pragma unroll
+            for (int e = 0; e < 3; ++e) g[s][e] = (R)(iJ * (C[e * 3 + 0] * r0 + C[e * 3 + 1] * r1 + C[e * 3 + 2] * r2));
+        }
+    }
     const int cx[3] = {node % N1, (node / N1) % N1, node / (N1 * N1)};
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -1207,6 +1234,24 @@ __device__ __noinline__ void aux_boundary_fluxes(const int* __restrict__ nbr, co
                 for (int e = 0; e < 3; ++e) gb[s][e] = (ad && s == 4) ? R(0) : g[s][e];
             const R sg = side ? R(1) : R(-1);
             R Fi[3][4], Fe[3][4];
+            if (metric) {   // curvilinear: |C[:, d]| F*_v . n with n = sg C[:, d] / |C[:, d]|
+                const double m0 = C[0 * 3 + d], m1 = C[1 * 3 + d], m2 = C[2 * 3 + d];
+                const double Jf = sqrt(m0 * m0 + m1 * m1 + m2 * m2);
+                const R nv[3] = {(R)(sg * m0 / Jf), (R)(sg * m1 / Jf), (R)(sg * m2 / Jf)};
+                viscous_flux<R>(un, g, pc.use_const_visc, cst, Fi, 7, nullptr, ad);
+                viscous_flux<R>(ub, pc.diss_flux == DF_CENTRAL ? g : gb, pc.use_const_visc, cst, Fe, 7, nullptr, ad);
+                R out[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const R fi = Fi[0][q] * nv[0] + Fi[1][q] * nv[1] + Fi[2][q] * nv[2];
+                    const R fe = Fe[0][q] * nv[0] + Fe[1][q] * nv[1] + Fe[2][q] * nv[2];
+                    out[q] = (R)Jf * (R(0.5) * (fi + fe));
+                }
+                R* dst = Fb + (size_t)k * 4 * NF + fn;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) dst[q * NF] = out[q];
+                continue;
+            }
             viscous_flux<R>(un, g, pc.use_const_visc, cst, Fi, 1 << d, nullptr, ad);
             if (pc.diss_flux == DF_CENTRAL) viscous_flux<R>(ub, g, pc.use_const_visc, cst, Fe, 1 << d, nullptr, ad);
             else viscous_flux<R>(ub, gb, pc.use_const_visc, cst, Fe, 1 << d, nullptr, ad);
@@ -1235,7 +1280,8 @@ __device__ __noinline__ void aux_boundary_fluxes(const int* __restrict__ nbr, co
 template <typename R, int N1>
 __device__ __forceinline__ void aux_boundary_node(const int* __restrict__ nbr, const int* __restrict__ btype,
                                                   R* __restrict__ Fb, int cell, int node, const R un[5],
-                                                  const R g[5][3], const PhysConst& pc, R pen) {
+                                                  const R g[5][3], const PhysConst& pc, R pen,
+                                                  const double* __restrict__ metric) {
     const int x = node % N1, y = (node / N1) % N1, z = node / (N1 * N1);
     if (x != 0 && x != N1 - 1 && y != 0 && y != N1 - 1 && z != 0 && z != N1 - 1) return;
     R uu[5], gg[15];
@@ -1245,7 +1291,7 @@ __device__ __forceinline__ void aux_boundary_node(const int* __restrict__ nbr, c
 #pragma unroll
         for (int e = 0; e < 3; ++e) gg[s * 3 + e] = g[s][e];
     }
-    aux_boundary_fluxes<R, N1>(nbr, btype, Fb, cell, node, uu, gg, pc, pen);
+    aux_boundary_fluxes<R, N1>(nbr, btype, Fb, cell, node, uu, gg, pc, pen, metric);
 }
 
 template <typename R, int N1, int CPC, bool FRA, bool CURV, bool BND = false>
@@ -1253,7 +1299,7 @@ __global__ void __launch_bounds__(AuxLayout<N1, CPC, FRA>::NT)
 aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, int cell_begin, int nc, R inv_h, PhysConst pc,
            AuxCoef<R> co, R* __restrict__ Fv, const double* __restrict__ metric, const int* __restrict__ btype,
            R* __restrict__ Fb, R pen, const int* __restrict__ tiles) {
-    static_assert(!(BND && CURV), "boundary faces: affine cells");
+
     using L = AuxLayout<N1, CPC, FRA>;
     constexpr int NP = L::NP, NF = L::NF, NT = L::NT;
     constexpr int VT = viscous_terms_per_cell<N1>();
@@ -1370,7 +1416,8 @@ aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, int cell_b
                 viscous_flux<R>(un, g, pc.use_const_visc, cst, F, 7, nullptr);
             }
             if constexpr (BND) {
-                if (cell0 + c < nc) aux_boundary_node<R, N1>(nbr, btype, Fb, cell0 + c, node, un, g, pc, pen);
+                if (cell0 + c < nc)
+                    aux_boundary_node<R, N1>(nbr, btype, Fb, cell0 + c, node, un, g, pc, pen, CURV ? metric : nullptr);
             }
 #pragma unroll
             for (int d = 0; d < 3; ++d)
@@ -1461,7 +1508,7 @@ aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, int cell_b
             R F[3][4];
             if constexpr (CURV) aux_curv_flux<R, N1>(un, g, metric, cell, node, pc.use_const_visc, cst, F);
             else viscous_flux<R>(un, g, pc.use_const_visc, cst, F, 7, nullptr);
-            if constexpr (BND) aux_boundary_node<R, N1>(nbr, btype, Fb, cell, node, un, g, pc, pen);
+            if constexpr (BND) aux_boundary_node<R, N1>(nbr, btype, Fb, cell, node, un, g, pc, pen, CURV ? metric : nullptr);
 #pragma unroll
             for (int d = 0; d < 3; ++d)
 #pragma unroll

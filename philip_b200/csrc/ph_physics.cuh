@@ -793,6 +793,19 @@ __device__ __noinline__ void boundary_state_face(int type, int f, const R* u, co
     for (int s = 0; s < 5; ++s) ub[s] = uo[s];
 }
 
+// the same for a given outward unit normal (curvilinear faces)
+template <typename R>
+__device__ __noinline__ void boundary_state_normal(int type, const R* nrm, const R* u, const PhysConst& pc, R* ub,
+                                                   unsigned* st) {
+    const R n[3] = {nrm[0], nrm[1], nrm[2]};
+    R ui[5], uo[5];
+#pragma unroll
+    for (int s = 0; s < 5; ++s) ui[s] = u[s];
+    boundary_state<R>(type, n, ui, pc, uo, st);
+#pragma unroll
+    for (int s = 0; s < 5; ++s) ub[s] = uo[s];
+}
+
 // NavierStokes::boundary_face_values_viscous_flux (navier_stokes.cpp:1354-1432): the exterior state
 // of the dissipative fluxes. 1001: no-slip, the momentum negated (its gradient is the interior's,
 // the energy gradient zero on an adiabatic wall; isothermal: the exterior temperature 2 T_wall - T);

@@ -256,6 +256,56 @@ def test_oracle_navier_stokes_wall_keeps_a_fluid_at_rest(thermal):
     assert np.max(np.abs(R)) <= 1e-13 * p
 
 
+# curvilinear cells (the sine-warped cube: the warp vanishes on the cube's sides, so boundary faces
+# stay flat while the metric varies along them)
+def _curved(kw, warp, bnd):
+    prm = _params(**kw)
+    return prm, Oracle(prm.oracle_cfg(), prm.n_cells, *prm.grid_bounds, warp=warp, boundaries=bnd)
+
+
+CURVED_PIN = [
+    ("euler_split_riemann_walls", dict(pde="euler", poly_degree=3, n_cells=3),
+     ["riemann_farfield", "riemann_farfield", "wall", "wall", "periodic", "periodic"]),
+    ("ns_br2_walls", dict(pde="navier_stokes", poly_degree=2, n_cells=3, diss="bassi_rebay_2"),
+     ["periodic", "periodic", "wall", "wall", "slip_wall", "slip_wall"]),
+    ("ns_central_isothermal", dict(pde="navier_stokes", poly_degree=3, n_cells=2, diss="central_visc_flux",
+                                   **{"navier_stokes/thermal_boundary_condition_type": "isothermal"}), ["wall"] * 6),
+]
+
+
+@pytest.mark.parametrize("name,kw,bnd", CURVED_PIN, ids=[c[0] for c in CURVED_PIN])
+def test_oracle_curvilinear_boundaries_vanishing_warp(name, kw, bnd):
+    """The curvilinear boundary terms (normals and |C n| from the face metric) reduce to the affine
+    ones as the warp vanishes."""
+    _, affine = _curved(kw, 0.0, bnd)
+    _, curved = _curved(kw, 1e-300, bnd)
+    U = _flow_state(affine, seed=3)
+    err = rel_max_err(curved.residual(U), affine.residual(U))
+    print(f"{name}: vanishing warp vs affine {err:.2e}")
+    assert err <= 1e-13
+
+
+@pytest.mark.parametrize("bt", ["farfield", "riemann_farfield"])
+def test_oracle_curvilinear_farfield_keeps_the_free_stream(bt):
+    mach, aoa = 0.4, 30.0
+    prm, orc = _curved(dict(pde="euler", poly_degree=3, n_cells=3, split=False, conv="roe", mach=mach,
+                            **{"euler/angle_of_attack": aoa}), 0.1, [bt] * 6)
+    R = orc.residual(_uniform(orc, *_free_stream(mach, aoa)))
+    scale = 1.0 / (GAMMA * mach * mach)
+    print(f"{bt}, curvilinear: max |R| / p_inf = {np.max(np.abs(R)) / scale:.2e}")
+    assert np.max(np.abs(R)) <= 1e-12 * scale
+
+
+def test_oracle_curvilinear_walls_keep_a_parallel_uniform_flow():
+    """Walls on the y sides (flat: the warp vanishes there) and a uniform flow with v_y = 0: the slip
+    wall's exterior state is the interior one, and the warped interior keeps the free stream."""
+    prm, orc = _curved(dict(pde="euler", poly_degree=3, n_cells=3), 0.1, WALLS_Y)
+    p = 1.0 / (GAMMA * 0.01)
+    R = orc.residual(_uniform(orc, 1.0, [0.6, 0.0, -0.3], p))
+    print(f"curvilinear walls, parallel uniform flow: max |R| / p = {np.max(np.abs(R)) / p:.2e}")
+    assert np.max(np.abs(R)) <= 1e-12 * p
+
+
 # ------------------------------------------------------------------------------- GPU
 def _flow_state(orc, seed):
     """Perturbed TGV with a mean flow along x (so that inflow and outflow boundaries see one)."""
@@ -335,6 +385,58 @@ def test_gpu_boundary_residual_matches_oracle(name, kw, bnd):
     assert err <= 1e-12
 
 
+CURVED_GPU = [
+    ("curved_euler_split_CHroe_p3_walls_y", dict(pde="euler", poly_degree=3),
+     ["periodic", "periodic", "wall", "wall", "periodic", "periodic"]),
+    ("curved_euler_conservative_roe_p2_riemann", dict(pde="euler", poly_degree=2, split=False, conv="roe"),
+     ["riemann_farfield", "riemann_farfield", "periodic", "periodic", "slip_wall", "slip_wall"]),
+    ("curved_euler_split_IR_p4_inflow_outflow", dict(pde="euler", poly_degree=4, two_point="IR",
+                                                     conv="two_point_flux", n_cells=2),
+     ["inflow", "pressure_outflow", "slip_wall", "slip_wall", "farfield", "extrapolation"]),
+    ("curved_ns_br2_split_p3_channel", dict(pde="navier_stokes", poly_degree=3, diss="bassi_rebay_2"),
+     ["periodic", "periodic", "wall", "wall", "periodic", "periodic"]),
+    ("curved_ns_central_split_p2_isothermal_box", dict(pde="navier_stokes", poly_degree=2, diss="central_visc_flux",
+                                                       **{"navier_stokes/thermal_boundary_condition_type":
+                                                          "isothermal"}), ["wall"] * 6),
+    ("curved_ns_br2_split_p5_slip", dict(pde="navier_stokes", poly_degree=5, diss="bassi_rebay_2", n_cells=2),
+     ["slip_wall", "slip_wall", "wall", "wall", "periodic", "periodic"]),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,kw,bnd", CURVED_GPU, ids=[c[0] for c in CURVED_GPU])
+def test_gpu_curvilinear_boundary_residual_matches_oracle(name, kw, bnd):
+    from philip_b200.dg import DGStrong
+    kw = dict(kw)
+    kw.setdefault("n_cells", 3)
+    prm, orc = _curved(kw, 0.1, bnd)
+    dg = DGStrong(prm, warp=0.1, boundaries=bnd)
+    U = _flow_state(orc, seed=len(name))
+    err = rel_max_err(dg.residual_of(U), orc.residual(U))
+    print(f"{name}: residual rel max err {err:.3e}")
+    assert err <= 1e-12
+
+
+@pytest.mark.gpu
+def test_gpu_curvilinear_boundary_steps_and_precision_form():
+    from philip_b200.dg import DGStrong, RungeKuttaODESolver
+    bnd = ["periodic", "periodic", "wall", "wall", "periodic", "periodic"]
+    prm, orc = _curved(dict(pde="navier_stokes", poly_degree=3, diss="bassi_rebay_2"), 0.1, bnd)
+    U = _flow_state(orc, seed=8)
+    dg32 = DGStrong(prm, precision=_lib.PH_FP32_RESIDUAL, warp=0.1, boundaries=bnd)
+    err32 = rel_max_err(dg32.residual_of(U), orc.residual(U))
+    dg = DGStrong(prm, warp=0.1, boundaries=bnd)
+    dg.solution = U
+    ode = RungeKuttaODESolver(dg)
+    Uo = U.copy()
+    for _ in range(3):
+        ode.step_in_time(1e-3)
+        orc.rk_step(Uo, 1e-3)
+    err = rel_max_err(dg.solution, Uo)
+    print(f"curvilinear channel: precision form {err32:.3e}, three RK4 steps {err:.3e}")
+    assert err32 <= 1e-5 and err <= 1e-11
+
+
 @pytest.mark.gpu
 def test_gpu_boundary_precision_form_close_to_oracle():
     from philip_b200.dg import DGStrong
@@ -386,7 +488,8 @@ def _mesh(prm, bnd, **kw):
 
 WALLS_Y = ["periodic", "periodic", "wall", "wall", "periodic", "periodic"]
 REFUSED = [
-    ("curvilinear", dict(), WALLS_Y, None, dict(warp=0.1), _lib.PH_ERR_UNSUPPORTED, "affine"),
+    ("curvilinear_gl", dict(), WALLS_Y, lambda p: setattr(p, "flux_nodes_type", 0), dict(warp=0.1),
+     _lib.PH_ERR_UNSUPPORTED, "collocated"),
     ("navier_stokes_farfield", dict(pde="navier_stokes", diss="bassi_rebay_2"),
      ["riemann_farfield", "riemann_farfield", "periodic", "periodic", "periodic", "periodic"], None, {},
      _lib.PH_ERR_UNSUPPORTED, "1006"),
