@@ -150,9 +150,9 @@ typedef struct ph_mesh_desc {
      * Navier-Stokes: no-slip, adiabatic or isothermal), 1002 pressure outflow, 1003 inflow,
      * 1004 Riemann farfield, 1005 farfield, 1006 slip wall, 1007 extrapolation. Navier-Stokes
      * takes 1001 and 1006 (NavierStokes::boundary_face_values_viscous_flux defines no viscous
-     * exterior state for the others). Contexts (ph_ctx_create) on affine meshes (GLL or GL flux
-     * nodes, overintegration 0..2) and on curvilinear ones (collocated GLL nodes); as a flow case's
-     * grid sets boundary ids, e.g. channel_flow.cpp:324-343. */
+     * exterior state for the others). Contexts (ph_ctx_create), affine or curvilinear, GLL or GL
+     * flux nodes, overintegration 0..2; as a flow case's grid sets boundary ids, e.g.
+     * channel_flow.cpp:324-343. */
     int boundary_type[6];
 } ph_mesh_desc;
 

@@ -412,8 +412,6 @@ bool has_boundaries(const ph_mesh_desc* mesh) {
 // Non-periodic meshes: what the boundary terms take (nullptr when supported).
 const char* boundary_reason(const ph_mesh_desc* mesh, const ph_params* prm) {
     if (!has_boundaries(mesh)) return nullptr;
-    if (is_curvilinear(mesh) && uncollocated(prm))
-        return "boundary conditions on curvilinear meshes: collocated GLL flux nodes without overintegration";
     if (prm->pde_type == 1)
         for (int f = 0; f < 6; ++f) {
             const int t = mesh->boundary_type[f];

@@ -87,14 +87,33 @@ static __device__ __noinline__ double gl_bnd_visc_state(int bt, const double* ow
 // viscous_numerical_flux.cpp:66-328): the viscous boundary state of us (the interpolated face state r,
 // or the projected one), BR2 / SIPG with its gradient, the central flux with the interior one, no heat
 // flux on an adiabatic 1001 wall; the interior side is r.
+// Curvilinear faces (m = the face's metric column C[:, f / 2] at the node, else nullptr): the outward
+// unit normal sg m / |m| and the flux scaled by |m|.
 static __device__ __noinline__ void gl_bnd_visc_flux(int bt, const double r[5], const double us[5],
                                                      const double g[5][3], int f, const PhysConst& pc, double pen,
-                                                     double out[4]) {
+                                                     double out[4], const double* m) {
     Cst<double> cst; cst.load(pc);
     const int dn = f >> 1;
     const double sg = (f & 1) ? 1.0 : -1.0;
     double ub[5];
     boundary_viscous_state<double>(bt, us, pc, ub, nullptr);
+    if (m) {
+        const double Jf = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+        const double nv[3] = {sg * m[0] / Jf, sg * m[1] / Jf, sg * m[2] / Jf};
+        const bool ad = bt == BC_WALL && !pc.bc_isothermal;
+        double gb[5][3];
+        for (int s = 0; s < 5; ++s)
+            for (int e = 0; e < 3; ++e) gb[s][e] = (ad && s == 4) ? 0.0 : g[s][e];
+        double Fi[3][4], Fe[3][4];
+        viscous_flux<double>(r, g, pc.use_const_visc, cst, Fi, 7, nullptr, ad);
+        viscous_flux<double>(ub, pc.diss_flux == DF_CENTRAL ? g : gb, pc.use_const_visc, cst, Fe, 7, nullptr, ad);
+        for (int k = 0; k < 4; ++k) {
+            const double fi = Fi[0][k] * nv[0] + Fi[1][k] * nv[1] + Fi[2][k] * nv[2];
+            const double fe = Fe[0][k] * nv[0] + Fe[1][k] * nv[1] + Fe[2][k] * nv[2];
+            out[k] = Jf * (0.5 * (fi + fe));
+        }
+        return;
+    }
     const bool ad = bt == BC_WALL && !pc.bc_isothermal;
     double gb[5][3];
     for (int s = 0; s < 5; ++s)
@@ -115,10 +134,11 @@ static __device__ __noinline__ void gl_bnd_visc_flux(int bt, const double r[5], 
 // The convective boundary state of a face node (Euler::boundary_face_values) for outward normal
 // sg e_dn of face f.
 static __device__ __noinline__ void gl_bnd_state(int bt, const double r[5], int f, const PhysConst& pc,
-                                                 double ub[5], unsigned* st) {
+                                                 double ub[5], unsigned* st, const double* nv = nullptr) {
     const int dn = f >> 1;
     const double sg = (f & 1) ? 1.0 : -1.0;
-    const double nrm[3] = {dn == 0 ? sg : 0.0, dn == 1 ? sg : 0.0, dn == 2 ? sg : 0.0};
+    double nrm[3] = {dn == 0 ? sg : 0.0, dn == 1 ? sg : 0.0, dn == 2 ? sg : 0.0};
+    if (nv) { nrm[0] = sg * nv[0]; nrm[1] = sg * nv[1]; nrm[2] = sg * nv[2]; }   // curvilinear: sg times the unit m
     boundary_state<double>(bt, nrm, r, pc, ub, st);
 }
 
@@ -578,7 +598,6 @@ __device__ __forceinline__ void gl_contravariant(const double* vm, int q, int Q3
 template <int ND, int NQ, bool SPLIT, bool CURV = false, bool BND = false>
 __global__ void __launch_bounds__(gl_threads<NQ>(), 2)
 gl_aux_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab T) {
-    static_assert(!(BND && CURV), "boundary faces: affine cells");
     using L = GlAuxLayout<ND, NQ, SPLIT>;
     constexpr int NT = L::NT, D3 = L::D3, Q3 = L::Q3, NF = L::NF, T1W = gl_t1_width<SPLIT>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -630,7 +649,12 @@ gl_aux_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab T
                     for (int s = 0; s < 5; ++s) v[s] = __ldg(&g.t1[(((size_t)cell * 6 + f) * T1W + 5 + s) * NF + q2]);
                     gl_cons_from_entropy(v, cst.gam, cst.gm1, us);
                 }
-                gl_bnd_visc_flux(__ldg(&a.btype[-1 - cn]), r, us, gq, f, a.pc, a.pen, out);
+                double mc[3];
+                if constexpr (CURV) {
+                    const double* m = g.fnrm + ((size_t)cell * 6 + f) * 3 * NF + q2;
+                    mc[0] = __ldg(&m[0]); mc[1] = __ldg(&m[NF]); mc[2] = __ldg(&m[2 * NF]);
+                }
+                gl_bnd_visc_flux(__ldg(&a.btype[-1 - cn]), r, us, gq, f, a.pc, a.pen, out, CURV ? mc : nullptr);
 #pragma unroll
                 for (int k = 0; k < 4; ++k) g.fb[((size_t)(-1 - cn) * 4 + k) * NF + q2] = out[k];
             }
@@ -967,7 +991,14 @@ gl_stage_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab
                 for (int s = 0; s < 5; ++s) vo[s] = __ldg(&to[(5 + s) * NF]);
                 gl_cons_from_entropy(vo, cst.gam, cst.gm1, uo);
             }
-            gl_bnd_state(__ldg(&a.btype[-1 - cn]), uo, f, a.pc, ub, a.status);
+            double mnv[3];
+            if constexpr (CURV) {   // the face's unit metric normal C[:, dn] / |C[:, dn]|
+                const double* m = g.fnrm + ((size_t)cell * 6 + f) * 3 * NF + q2;
+                const double m0 = __ldg(&m[0]), m1 = __ldg(&m[NF]), m2 = __ldg(&m[2 * NF]);
+                const double J = sqrt(m0 * m0 + m1 * m1 + m2 * m2);
+                mnv[0] = m0 / J; mnv[1] = m1 / J; mnv[2] = m2 / J;
+            }
+            gl_bnd_state(__ldg(&a.btype[-1 - cn]), uo, f, a.pc, ub, a.status, CURV ? mnv : nullptr);
 #pragma unroll
             for (int s = 0; s < 5; ++s) ue[s] = ub[s];
         } else if constexpr (SPLIT) {

@@ -324,7 +324,7 @@ static cudaError_t launch_gl_nq(int kernel, const StageArgs& a, const GlArgs& g,
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     constexpr int NT = gl_threads<NQ>();
-    static bool cfg[21][64] = {};
+    static bool cfg[27][64] = {};
     if (kernel == 0) {
         if (split) return launch_gl_kernel(gl_trace_kernel<ND, NQ, true>, GlTraceLayout<ND, NQ, true>::bytes, NT, a, g, ht,
                                            cfg[0][dev], s);
@@ -332,6 +332,12 @@ static cudaError_t launch_gl_nq(int kernel, const StageArgs& a, const GlArgs& g,
                                 cfg[1][dev], s);
     }
     if (kernel == 1) {
+        if (g.vmet && a.btype) {   // curvilinear cells with a boundary face
+            if (split) return launch_gl_kernel(gl_aux_kernel<ND, NQ, true, true, true>, GlAuxLayout<ND, NQ, true>::bytes,
+                                               NT, a, g, ht, cfg[21][dev], s);
+            return launch_gl_kernel(gl_aux_kernel<ND, NQ, false, true, true>, GlAuxLayout<ND, NQ, false>::bytes, NT, a,
+                                    g, ht, cfg[22][dev], s);
+        }
         if (g.vmet) {   // curvilinear cells
             if (split) return launch_gl_kernel(gl_aux_kernel<ND, NQ, true, true>, GlAuxLayout<ND, NQ, true>::bytes, NT, a,
                                                g, ht, cfg[11][dev], s);
@@ -351,6 +357,19 @@ static cudaError_t launch_gl_nq(int kernel, const StageArgs& a, const GlArgs& g,
     }
     if (kernel == 3)   // curvilinear: the weight-adjusted inverse mass alone
         return launch_gl_kernel(gl_minv_kernel<ND, NQ>, GlMinvLayout<ND, NQ>::bytes, NT, a, g, ht, cfg[8][dev], s);
+    if (g.vmet && a.btype) {   // curvilinear cells with a boundary face
+        if (visc) {
+            if (split) return launch_gl_kernel(gl_stage_kernel<ND, NQ, true, true, true, true>,
+                                               GlStageLayout<ND, NQ, true, true, true>::bytes, NT, a, g, ht, cfg[23][dev],
+                                               s);
+            return launch_gl_kernel(gl_stage_kernel<ND, NQ, true, false, true, true>,
+                                    GlStageLayout<ND, NQ, true, false, true>::bytes, NT, a, g, ht, cfg[24][dev], s);
+        }
+        if (split) return launch_gl_kernel(gl_stage_kernel<ND, NQ, false, true, true, true>,
+                                           GlStageLayout<ND, NQ, false, true, true>::bytes, NT, a, g, ht, cfg[25][dev], s);
+        return launch_gl_kernel(gl_stage_kernel<ND, NQ, false, false, true, true>,
+                                GlStageLayout<ND, NQ, false, false, true>::bytes, NT, a, g, ht, cfg[26][dev], s);
+    }
     if (g.vmet) {      // curvilinear cells
         if (visc) {
             if (split) return launch_gl_kernel(gl_stage_kernel<ND, NQ, true, true, true>,

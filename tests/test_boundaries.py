@@ -270,6 +270,10 @@ CURVED_PIN = [
      ["periodic", "periodic", "wall", "wall", "slip_wall", "slip_wall"]),
     ("ns_central_isothermal", dict(pde="navier_stokes", poly_degree=3, n_cells=2, diss="central_visc_flux",
                                    **{"navier_stokes/thermal_boundary_condition_type": "isothermal"}), ["wall"] * 6),
+    ("gl_ns_br2_walls", dict(pde="navier_stokes", poly_degree=2, n_cells=3, diss="bassi_rebay_2",
+                             flux_nodes_type="GL"), ["slip_wall"] * 2 + ["wall"] * 2 + ["periodic"] * 2),
+    ("gl_euler_conservative_riemann", dict(pde="euler", poly_degree=3, n_cells=2, split=False, conv="roe",
+                                           flux_nodes_type="GL"), ["riemann_farfield"] * 2 + ["wall"] * 4),
 ]
 
 
@@ -285,11 +289,11 @@ def test_oracle_curvilinear_boundaries_vanishing_warp(name, kw, bnd):
     assert err <= 1e-13
 
 
-@pytest.mark.parametrize("bt", ["farfield", "riemann_farfield"])
-def test_oracle_curvilinear_farfield_keeps_the_free_stream(bt):
+@pytest.mark.parametrize("bt,nodes", [("farfield", "GLL"), ("riemann_farfield", "GLL"), ("riemann_farfield", "GL")])
+def test_oracle_curvilinear_farfield_keeps_the_free_stream(bt, nodes):
     mach, aoa = 0.4, 30.0
     prm, orc = _curved(dict(pde="euler", poly_degree=3, n_cells=3, split=False, conv="roe", mach=mach,
-                            **{"euler/angle_of_attack": aoa}), 0.1, [bt] * 6)
+                            flux_nodes_type=nodes, **{"euler/angle_of_attack": aoa}), 0.1, [bt] * 6)
     R = orc.residual(_uniform(orc, *_free_stream(mach, aoa)))
     scale = 1.0 / (GAMMA * mach * mach)
     print(f"{bt}, curvilinear: max |R| / p_inf = {np.max(np.abs(R)) / scale:.2e}")
@@ -400,6 +404,19 @@ CURVED_GPU = [
                                                           "isothermal"}), ["wall"] * 6),
     ("curved_ns_br2_split_p5_slip", dict(pde="navier_stokes", poly_degree=5, diss="bassi_rebay_2", n_cells=2),
      ["slip_wall", "slip_wall", "wall", "wall", "periodic", "periodic"]),
+    # GL flux nodes and overintegration on curved cells
+    ("curved_gl_euler_split_CHroe_p3_walls_y", dict(pde="euler", poly_degree=3, flux_nodes_type="GL"),
+     ["periodic", "periodic", "wall", "wall", "periodic", "periodic"]),
+    ("curved_gl_euler_conservative_roe_p2_mixed", dict(pde="euler", poly_degree=2, split=False, conv="roe",
+                                                       flux_nodes_type="GL"),
+     ["inflow", "pressure_outflow", "riemann_farfield", "riemann_farfield", "slip_wall", "slip_wall"]),
+    ("curved_gl_ns_br2_split_p3_channel", dict(pde="navier_stokes", poly_degree=3, diss="bassi_rebay_2",
+                                               flux_nodes_type="GL"),
+     ["periodic", "periodic", "wall", "wall", "periodic", "periodic"]),
+    ("curved_gll_overint1_ns_central_split_p2_isothermal", dict(pde="navier_stokes", poly_degree=2,
+                                                                diss="central_visc_flux", overintegration=1,
+                                                                **{"navier_stokes/thermal_boundary_condition_type":
+                                                                   "isothermal"}), ["wall"] * 6),
 ]
 
 
@@ -488,8 +505,6 @@ def _mesh(prm, bnd, **kw):
 
 WALLS_Y = ["periodic", "periodic", "wall", "wall", "periodic", "periodic"]
 REFUSED = [
-    ("curvilinear_gl", dict(), WALLS_Y, lambda p: setattr(p, "flux_nodes_type", 0), dict(warp=0.1),
-     _lib.PH_ERR_UNSUPPORTED, "collocated"),
     ("navier_stokes_farfield", dict(pde="navier_stokes", diss="bassi_rebay_2"),
      ["riemann_farfield", "riemann_farfield", "periodic", "periodic", "periodic", "periodic"], None, {},
      _lib.PH_ERR_UNSUPPORTED, "1006"),
