@@ -548,3 +548,35 @@ def test_entry_points_without_boundary_terms_refuse_non_periodic_meshes():
     nbytes = ctypes.c_size_t()
     assert L.ph_batch_bytes(ctypes.byref(m), ctypes.byref(p), ctypes.byref(nbytes)) == _lib.PH_ERR_UNSUPPORTED
     assert b"periodic" in L.ph_last_error()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("method", ["RK4_3_5_3SStar", "RK3_2_5F_3SStarPlus", "relaxation"])
+def test_gpu_boundary_low_storage_and_relaxation_steps_match_oracle(method):
+    """The low-storage (3S* / 3S*+) and relaxation RK solvers on a wall-bounded mesh: the stage
+    kernels' epilogues are the periodic ones, the boundary tiles run the boundary-face instances."""
+    from philip_b200.dg import DGStrong, RungeKuttaODESolver
+    kw = dict(pde="navier_stokes", poly_degree=3, diss="bassi_rebay_2", two_point="CH", conv="two_point_flux")
+    if method == "relaxation":
+        kw["ODE solver/rrk root solver/use_relaxation_runge_kutta"] = "true"
+    else:
+        kw["rk"] = method
+    prm = _params(**kw)
+    bnd = ["periodic", "periodic", "wall", "wall", "slip_wall", "slip_wall"]
+    orc = Oracle(prm.oracle_cfg(), prm.n_cells, *prm.grid_bounds, boundaries=bnd)
+    dg = DGStrong(prm, boundaries=bnd)
+    U = _flow_state(orc, seed=5)
+    dg.solution = U
+    ode = RungeKuttaODESolver(dg)
+    Uo = U.copy()
+    for _ in range(3):
+        ode.step_in_time(1e-3)
+        orc.rk_step(Uo, 1e-3)
+    err = rel_max_err(dg.solution, Uo)
+    extra = ""
+    if method == "relaxation":
+        g_err = abs(ode.relaxation_parameter - orc.rrk_gamma()) / orc.rrk_gamma()
+        extra = f", gamma rel err {g_err:.2e}"
+        assert g_err <= 1e-5
+    print(f"walls, {method}: three steps rel err {err:.3e}{extra}")
+    assert err <= (5e-9 if method == "relaxation" else 1e-11)
