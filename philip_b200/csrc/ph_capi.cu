@@ -1071,6 +1071,7 @@ struct ph_ctx {
     // the nt_bnd tiles with one
     int* d_tiles = nullptr;
     int nt_int = 0, nt_bnd = 0;
+    std::vector<int> h_tiles;
     size_t nalloc = 0;                  // doubles per stage-input buffer, ghost slots included
     // stage tiles [0, lo_end) and [hi_begin, nc) read ghost data (CPC-aligned, so the tiles and
     // their partial sums are those of one launch over all cells); [lo_end, hi_begin) do not
@@ -1136,6 +1137,17 @@ void timer_end(ph_ctx* c, int cls) {
     c->t_n[cls] += 1;
 }
 
+// The tiles of list `list` (0: without a boundary face, 1: with one) whose first cell lies in
+// [b, e): their offset in the device tile array and their count (each list ascends; launch ranges
+// are whole tiles).
+void tile_span(const ph_ctx* c, int list, int b, int e, int* off, int* cnt) {
+    const int base = list ? c->nt_int : 0, n = list ? c->nt_bnd : c->nt_int;
+    const int* t = c->h_tiles.data() + base;
+    const int i0 = (int)(std::lower_bound(t, t + n, b) - t), i1 = (int)(std::lower_bound(t, t + n, e) - t);
+    *off = base + i0;
+    *cnt = i1 - i0;
+}
+
 // cells per CTA of the stage and auxiliary kernels (the uncollocated ones: one)
 int cells_per_tile(const ph_ctx* c) {
     if (c->gl) return 1;
@@ -1153,14 +1165,17 @@ int cells_per_tile(const ph_ctx* c) {
 }
 
 int dispatch_stage(ph_ctx* c, const ph::StageArgs& a) {
-    if (c->nb && !a.tiles) {   // non-periodic mesh: the periodic kernel on the tiles without a boundary face,
-                               // the boundary-face kernel on the others
-        if (a.cell_begin != 0 || a.nc != c->nc) return fail(PH_ERR_INVALID, "boundary faces: whole-mesh launches only");
+    if (c->nb && !a.tiles) {   // non-periodic mesh: the periodic kernel on the range's tiles without a
+                               // boundary face, the boundary-face kernel on the others
+        int oi, ni, ob, nbt;
+        tile_span(c, 0, a.cell_begin, a.nc, &oi, &ni);
+        tile_span(c, 1, a.cell_begin, a.nc, &ob, &nbt);
         ph::StageArgs ai = a, ab = a;
-        ai.btype = nullptr; ai.tiles = c->d_tiles; ai.ntiles = c->nt_int;
-        ab.btype = c->d_btype; ab.tiles = c->d_tiles + c->nt_int; ab.ntiles = c->nt_bnd;
-        if (int rc = dispatch_stage(c, ai)) return rc;
-        return dispatch_stage(c, ab);
+        ai.btype = nullptr; ai.tiles = c->d_tiles + oi; ai.ntiles = ni;
+        ab.btype = c->d_btype; ab.tiles = c->d_tiles + ob; ab.ntiles = nbt;
+        if (ni) if (int rc = dispatch_stage(c, ai)) return rc;
+        if (nbt) return dispatch_stage(c, ab);
+        return PH_OK;
     }
     NvtxRange nvtx("stage kernel");
     cudaError_t e;
@@ -1203,11 +1218,14 @@ int dispatch_aux(ph_ctx* c, const double* U, int cell_begin, int cell_end) {
     if (!c->nb) return aux_launch(c, U, cell_begin, cell_end, nullptr);
     // non-periodic mesh: the periodic kernel on the tiles without a boundary face, then the
     // boundary-face kernel on the others (it stores the boundary viscous fluxes)
-    if (cell_begin != 0 || cell_end != c->nc) return fail(PH_ERR_INVALID, "boundary faces: whole-mesh launches only");
-    const ph::BoundaryArgs bi{nullptr, c->d_fb, c->pen, c->d_tiles, c->nt_int};
-    const ph::BoundaryArgs bb{c->d_btype, c->d_fb, c->pen, c->d_tiles + c->nt_int, c->nt_bnd};
-    if (int rc = aux_launch(c, U, cell_begin, cell_end, &bi)) return rc;
-    return aux_launch(c, U, cell_begin, cell_end, &bb);
+    int oi, ni, ob, nbt;
+    tile_span(c, 0, cell_begin, cell_end, &oi, &ni);
+    tile_span(c, 1, cell_begin, cell_end, &ob, &nbt);
+    const ph::BoundaryArgs bi{nullptr, c->d_fb, c->pen, c->d_tiles + oi, ni};
+    const ph::BoundaryArgs bb{c->d_btype, c->d_fb, c->pen, c->d_tiles + ob, nbt};
+    if (ni) if (int rc = aux_launch(c, U, cell_begin, cell_end, &bi)) return rc;
+    if (nbt) return aux_launch(c, U, cell_begin, cell_end, &bb);
+    return PH_OK;
 }
 
 // One kernel of the uncollocated path on the stage input a.U: 0 face values, 1 auxiliary
@@ -1217,12 +1235,15 @@ int dispatch_gl(ph_ctx* c, int kernel, const ph::StageArgs& a) {
     if (c->nb && (kernel == 1 || kernel == 2) && !a.tiles) {
         // non-periodic mesh: the periodic kernel on the cells without a boundary face, the
         // boundary-face kernel on the others
-        if (a.cell_begin != 0 || a.nc != c->nc) return fail(PH_ERR_INVALID, "boundary faces: whole-mesh launches only");
+        int oi, ni, ob, nbt;
+        tile_span(c, 0, a.cell_begin, a.nc, &oi, &ni);
+        tile_span(c, 1, a.cell_begin, a.nc, &ob, &nbt);
         ph::StageArgs ai = a, ab = a;
-        ai.btype = nullptr; ai.tiles = c->d_tiles; ai.ntiles = c->nt_int;
-        ab.btype = c->d_btype; ab.tiles = c->d_tiles + c->nt_int; ab.ntiles = c->nt_bnd;
-        if (int rc = dispatch_gl(c, kernel, ai)) return rc;
-        return dispatch_gl(c, kernel, ab);
+        ai.btype = nullptr; ai.tiles = c->d_tiles + oi; ai.ntiles = ni;
+        ab.btype = c->d_btype; ab.tiles = c->d_tiles + ob; ab.ntiles = nbt;
+        if (ni) if (int rc = dispatch_gl(c, kernel, ai)) return rc;
+        if (nbt) return dispatch_gl(c, kernel, ab);
+        return PH_OK;
     }
     static const char* const kName[] = {"face-value kernel", "auxiliary kernel", "stage kernel",
                                         "inverse-mass kernel"};
@@ -1510,7 +1531,9 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
     if (slab) {
         if (z0 < 0 || z0 >= mesh->n_cells_per_direction || nz > mesh->n_cells_per_direction)
             return fail(PH_ERR_INVALID, "slab outside the mesh: 0 <= z_first < n and 1 <= z_count <= n");
-        if (has_boundaries(mesh)) return fail(PH_ERR_UNSUPPORTED, "slab contexts: periodic meshes");
+        // slabs cut the z direction: its sides stay periodic (the halo carries the partition faces)
+        if (mesh->boundary_type[4] || mesh->boundary_type[5])
+            return fail(PH_ERR_UNSUPPORTED, "slab contexts: boundary conditions on the x and y sides only (z periodic)");
     }
     ph_ctx* c = new ph_ctx();
     c->prm = *prm;
@@ -1614,6 +1637,7 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
         c->nt_int = (int)tiles.size();
         c->nt_bnd = (int)tb.size();
         tiles.insert(tiles.end(), tb.begin(), tb.end());
+        c->h_tiles = tiles;
         bad |= dalloc(&c->d_tiles, tiles.size());
     }
     if (c->nb) {   // boundary faces: their types, and (Navier-Stokes) their viscous fluxes in the arithmetic type

@@ -234,7 +234,7 @@ class ThreadHalo:
             return 1
 
 
-def _slabs(prm, world, precision=_lib.PH_FP64, warp=0.0):
+def _slabs(prm, world, precision=_lib.PH_FP64, warp=0.0, boundaries=None):
     import torch
     from philip_b200.dg import DGStrong
     shared = ThreadHalo.shared(world)
@@ -244,7 +244,7 @@ def _slabs(prm, world, precision=_lib.PH_FP64, warp=0.0):
         s = torch.cuda.Stream()
         halo = base.for_rank(r)
         dg = DGStrong(prm, precision=precision, stream=s.cuda_stream,
-                      slab=slab_bounds(prm.n_cells, world, r), halo=halo, warp=warp)
+                      slab=slab_bounds(prm.n_cells, world, r), halo=halo, warp=warp, boundaries=boundaries)
         out.append((dg, s))
     return out
 
@@ -561,6 +561,54 @@ def test_gl_slabs_are_the_whole_mesh(name, kw, world, warp):
     whole = DGStrong(prm, warp=warp)
     U0 = perturbed_tgv(Oracle(prm.oracle_cfg(), prm.n_cells, *prm.grid_bounds), seed=len(name))
     parts = _slabs(prm, world, warp=warp)
+    dgs = [p for p, _ in parts]
+    Us = _scatter(whole, dgs, U0)
+    Rs = _in_threads([lambda k=k: dgs[k].residual_of(Us[k]) for k in range(world)])
+    R = _gather(whole, dgs, Rs)
+    R_whole = whole.residual_of(U0)
+    print(f"{name}: max |R_slabs - R_whole| = {np.max(np.abs(R - R_whole)):.3e}")
+    assert np.array_equal(R, R_whole)
+    dt = 0.1 * TWO_PI / prm.n_cells / (prm.poly_degree + 1) / 11.0
+    whole.solution = U0
+    RungeKuttaODESolver(whole).step_in_time(dt, nsteps=3)
+    for dg, u in zip(dgs, Us):
+        dg.solution = u
+    _in_threads([lambda k=k: (RungeKuttaODESolver(dgs[k]).step_in_time(dt, nsteps=3), parts[k][1].synchronize())
+                 for k in range(world)])
+    U = _gather(whole, dgs, [dg.solution for dg in dgs])
+    print(f"{name}: max |U_slabs - U_whole| = {np.max(np.abs(U - whole.solution)):.3e}")
+    assert np.array_equal(U, whole.solution)
+
+
+WALL_SLAB_CASES = [
+    ("ns_br2_p3_walls_y_two_slabs", dict(poly_degree=3, n_cells=4, pde="navier_stokes", diss="bassi_rebay_2"), 2,
+     "GLL", ["periodic", "periodic", "wall", "wall", "periodic", "periodic"], 0.0),
+    ("euler_roe_p2_riemann_x_three_slabs", dict(poly_degree=2, n_cells=6, split=False, conv="roe"), 3, "GLL",
+     ["riemann_farfield", "riemann_farfield", "slip_wall", "slip_wall", "periodic", "periodic"], 0.0),
+    ("ns_br2_p2_walls_interior_overlap", dict(poly_degree=2, n_cells=6, pde="navier_stokes", diss="bassi_rebay_2"), 2,
+     "GLL", ["wall", "wall", "wall", "wall", "periodic", "periodic"], 0.0),
+    ("gl_ns_br2_p3_walls_y_two_slabs", dict(poly_degree=3, n_cells=4, pde="navier_stokes", diss="bassi_rebay_2"), 2,
+     "GL", ["periodic", "periodic", "wall", "wall", "periodic", "periodic"], 0.0),
+    ("curvilinear_ns_br2_p3_walls_y_two_slabs", dict(poly_degree=3, n_cells=4, pde="navier_stokes",
+                                                     diss="bassi_rebay_2"), 2, "GLL",
+     ["periodic", "periodic", "wall", "wall", "periodic", "periodic"], 0.1),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,kw,world,nodes,bnd,warp", WALL_SLAB_CASES, ids=[c[0] for c in WALL_SLAB_CASES])
+def test_slabs_with_walls_are_the_whole_mesh(name, kw, world, nodes, bnd, warp):
+    """Slabs of a mesh with boundary conditions on its x / y sides: every slab splits its launches
+    into the periodic kernel's tiles and the boundary-face kernel's, also for the interior cells
+    that run while a transfer is in flight, so the residual and three RK4 steps are bitwise the
+    whole mesh's."""
+    from oracle.oracle import Oracle
+    from philip_b200.dg import DGStrong, RungeKuttaODESolver
+    from helpers import TWO_PI, perturbed_tgv
+    prm = _gl_prm(nodes=nodes, **kw)
+    whole = DGStrong(prm, warp=warp, boundaries=bnd)
+    U0 = perturbed_tgv(Oracle(prm.oracle_cfg(), prm.n_cells, *prm.grid_bounds), seed=len(name))
+    parts = _slabs(prm, world, warp=warp, boundaries=bnd)
     dgs = [p for p, _ in parts]
     Us = _scatter(whole, dgs, U0)
     Rs = _in_threads([lambda k=k: dgs[k].residual_of(Us[k]) for k in range(world)])
