@@ -1531,9 +1531,6 @@ static int create_context(const ph_mesh_desc* mesh, const ph_params* prm, void* 
     if (slab) {
         if (z0 < 0 || z0 >= mesh->n_cells_per_direction || nz > mesh->n_cells_per_direction)
             return fail(PH_ERR_INVALID, "slab outside the mesh: 0 <= z_first < n and 1 <= z_count <= n");
-        // slabs cut the z direction: its sides stay periodic (the halo carries the partition faces)
-        if (mesh->boundary_type[4] || mesh->boundary_type[5])
-            return fail(PH_ERR_UNSUPPORTED, "slab contexts: boundary conditions on the x and y sides only (z periodic)");
     }
     ph_ctx* c = new ph_ctx();
     c->prm = *prm;

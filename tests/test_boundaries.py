@@ -533,17 +533,13 @@ def test_boundary_configurations_outside_the_path_are_refused(name, prm_kw, bnd,
 
 
 def test_entry_points_without_boundary_terms_refuse_non_periodic_meshes():
-    """Slab contexts take boundaries on the sides they do not cut (x and y); the batch and the
-    no-allocation residual take periodic meshes."""
+    """The batch and the no-allocation residual take periodic meshes."""
     import ctypes
     L = _lib.load()
     prm = Parameters.from_dict(prm_dict())
     p = prm.to_ph_params()
-    mz = _mesh(prm, ["periodic", "periodic", "periodic", "periodic", "wall", "wall"])
-    h = ctypes.c_void_p()
-    rc = L.ph_ctx_create_slab(ctypes.byref(mz), ctypes.byref(p), 0, 2, None, ctypes.byref(h))
-    assert rc == _lib.PH_ERR_UNSUPPORTED and b"z periodic" in L.ph_last_error()
     m = _mesh(prm, WALLS_Y)
+    h = ctypes.c_void_p()
     dummy = ctypes.c_void_p(16)   # never dereferenced: the checks come first
     assert L.ph_residual_noalloc(ctypes.byref(m), ctypes.byref(p), dummy, dummy, None) == _lib.PH_ERR_UNSUPPORTED
     assert b"periodic" in L.ph_last_error()

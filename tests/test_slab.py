@@ -592,6 +592,14 @@ WALL_SLAB_CASES = [
     ("curvilinear_ns_br2_p3_walls_y_two_slabs", dict(poly_degree=3, n_cells=4, pde="navier_stokes",
                                                      diss="bassi_rebay_2"), 2, "GLL",
      ["periodic", "periodic", "wall", "wall", "periodic", "periodic"], 0.1),
+    # walls on the sides the slabs cut: the first and last slab's outer faces are boundary faces
+    # (the halo's wrap-around transfer is then unused)
+    ("ns_br2_p3_walls_z_two_slabs", dict(poly_degree=3, n_cells=4, pde="navier_stokes", diss="bassi_rebay_2"), 2,
+     "GLL", ["periodic", "periodic", "periodic", "periodic", "wall", "wall"], 0.0),
+    ("gl_euler_p2_farfield_z_three_slabs", dict(poly_degree=2, n_cells=6, split=False, conv="roe"), 3, "GL",
+     ["slip_wall", "slip_wall", "periodic", "periodic", "riemann_farfield", "riemann_farfield"], 0.0),
+    ("ns_br2_p2_box_two_slabs", dict(poly_degree=2, n_cells=4, pde="navier_stokes", diss="bassi_rebay_2"), 2,
+     "GLL", ["wall"] * 6, 0.0),
 ]
 
 
