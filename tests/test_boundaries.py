@@ -578,3 +578,29 @@ def test_gpu_boundary_low_storage_and_relaxation_steps_match_oracle(method):
         assert g_err <= 1e-5
     print(f"walls, {method}: three steps rel err {err:.3e}{extra}")
     assert err <= (5e-9 if method == "relaxation" else 1e-11)
+
+
+@pytest.mark.gpu
+def test_gpu_slip_walls_run_the_mirrored_periodic_taylor_green_vortex():
+    """The inviscid Taylor-Green vortex is mirror-symmetric about the planes x, y, z = 0 and pi: on
+    [0, pi]^3 with slip walls all around it must stay the octant of the periodic run on
+    [-pi, pi]^3 (the same cells), step after step (twenty RK4 steps)."""
+    from philip_b200.dg import DGStrong, RungeKuttaODESolver
+    n, p = 3, 3
+    walls = _params(pde="euler", poly_degree=p, n_cells=n, left=0.0, right=math.pi)
+    cube = _params(pde="euler", poly_degree=p, n_cells=2 * n, left=-math.pi, right=math.pi)
+    ow = Oracle(walls.oracle_cfg(), n, 0.0, math.pi, "lexicographic", boundaries=["slip_wall"] * 6)
+    U = ow.initial_condition("tgv")
+    dw = DGStrong(walls, cell_order=1, boundaries=["slip_wall"] * 6)
+    dc = DGStrong(cube, cell_order=1)
+    dw.solution = U
+    dc.solution = _mirror(U, n, p + 1)
+    dt = 0.1 * math.pi / n / (p + 1) / 11.0
+    RungeKuttaODESolver(dw).step_in_time(dt, nsteps=20)
+    RungeKuttaODESolver(dc).step_in_time(dt, nsteps=20)
+    N1 = p + 1
+    octant = dc.solution.reshape(2 * n, 2 * n, 2 * n, 5, N1 ** 3)[n:, n:, n:].reshape(-1)
+    err = rel_max_err(dw.solution, octant)
+    change = rel_max_err(dw.solution, U)
+    print(f"slip-walled octant vs periodic cube after 20 RK4 steps: {err:.2e} (the state changed by {change:.2e})")
+    assert err <= 1e-12 and change > 1e-6
