@@ -88,7 +88,9 @@ typedef struct ph_params {
     /* Relaxation Runge-Kutta, root-finding form for the Euler / Navier-Stokes entropy
      * (ODE solver/rrk root solver: use_relaxation_runge_kutta, relaxation_runge_kutta_root_tolerance;
      * src/ode_solver/relaxation_runge_kutta/root_finding_rrk_ode_solver.cpp). The Butcher methods
-     * in FP64, two-point fluxes other than KG. */
+     * in FP64, two-point fluxes other than KG; GLL or GL flux nodes, with or without
+     * overintegration (off the solution nodes the entropy is integrated at the flux nodes and the
+     * estimate takes the entropy variables projected on the solution basis). */
     int use_relaxation_runge_kutta;
     double relaxation_runge_kutta_root_tolerance;
     /* limiter/bound_preserving_limiter (src/parameters/parameters_limiter.cpp:17-30):

@@ -1829,9 +1829,10 @@ void Solver::rk_step(double* U, double dt) {
 
 // ---- relaxation Runge-Kutta, root-finding form for the Euler / Navier-Stokes entropy
 // (RootFindingRRKODESolver, root_finding_rrk_ode_solver.cpp:15-180, :182-390;
-// RKNumEntropy::compute_entropy_vars, runge_kutta_store_entropy.cpp:27-100). GLL flux nodes:
-// the volume quadrature is the solution nodes, so the entropy variables' projection onto the
-// solution basis is the identity and the mass matrix of the M norm is diag(W det J).
+// RKNumEntropy::compute_entropy_vars, runge_kutta_store_entropy.cpp:27-100). Collocated GLL flux
+// nodes: the volume quadrature is the solution nodes, so the entropy variables' projection onto
+// the solution basis is the identity and the mass matrix of the M norm is diag(W det J); other
+// flux nodes interpolate to them and project back.
 
 // Euler::compute_entropy (euler.cpp:512-530) and compute_numerical_entropy_function (:437-447)
 static double numerical_entropy_fn(const double u[5], double gam) {
@@ -1858,8 +1859,35 @@ static double node_mass(const Mesh& mesh, const Ops1D& ops, int c, int node) {
     return W * J;
 }
 
+// W det J at flux node q of cell c (uncollocated flux nodes)
+static double flux_node_mass(const Mesh& mesh, const Ops1D& ops, int c, int q) {
+    const int nq = ops.nq;
+    const double W = ops.wq[q % nq] * ops.wq[(q / nq) % nq] * ops.wq[q / (nq * nq)];
+    const double J = mesh.affine ? mesh.h * mesh.h * mesh.h : mesh.detj[(size_t)c * nq * nq * nq + q];
+    return W * J;
+}
+
+static bool collocated(const Params& p) { return p.flux_nodes == GLL && p.overintegration == 0; }
+
 double Solver::numerical_entropy(const double* U) const {
     double sum = 0.0;
+    if (!collocated(prm)) {   // the volume quadrature: the state interpolated to the flux nodes
+        // (compute_integrated_numerical_entropy, root_finding_rrk_ode_solver.cpp:211-350)
+        const int nd = ops.nd, nq = ops.nq;
+        const double* chi = ops.chi.data();
+        std::vector<double> uq((size_t)NSTATE * nq3);
+        for (int c = 0; c < mesh.nc; ++c) {
+            for (int s = 0; s < NSTATE; ++s)
+                apply3(chi, nq, nd, chi, nq, nd, chi, nq, nd, U + (size_t)c * ndofs_cell + s * nd3, &uq[s * nq3],
+                       false, 1.0);
+            for (int q = 0; q < nq3; ++q) {
+                double u[5];
+                for (int s = 0; s < 5; ++s) u[s] = uq[s * nq3 + q];
+                sum += flux_node_mass(mesh, ops, c, q) * numerical_entropy_fn(u, prm.gamma);
+            }
+        }
+        return sum;
+    }
     for (int c = 0; c < mesh.nc; ++c)
         for (int i = 0; i < nd3; ++i) {
             double u[5];
@@ -1875,6 +1903,36 @@ double Solver::entropy_vars_dot_mass(const double* st, const double* R) {
     std::vector<double> kk((size_t)ndofs());
     apply_inverse_mass(R, kk.data());
     double sum = 0.0;
+    if (!collocated(prm)) {
+        // uncollocated flux nodes: v_hat = M^-1 chi^T W v(chi u), the entropy variables projected on
+        // the solution basis (compute_entropy_vars, runge_kutta_store_entropy.cpp:30-100), dotted with
+        // M k, M = chi^T W J chi (compute_entropy_change_estimate, root_finding_rrk_ode_solver.cpp:353-388):
+        // sum over the flux nodes of W J (chi v_hat)(chi k)
+        const int nd = ops.nd, nq = ops.nq;
+        const double* chi = ops.chi.data();
+        const double* proj = ops.proj.data();
+        std::vector<double> uq((size_t)NSTATE * nq3), vh(nd3), vq((size_t)NSTATE * nq3), kq(nq3);
+        for (int c = 0; c < mesh.nc; ++c) {
+            for (int s = 0; s < NSTATE; ++s)
+                apply3(chi, nq, nd, chi, nq, nd, chi, nq, nd, st + (size_t)c * ndofs_cell + s * nd3, &uq[s * nq3],
+                       false, 1.0);
+            for (int q = 0; q < nq3; ++q) {
+                double u[5], v[5];
+                for (int s = 0; s < 5; ++s) u[s] = uq[s * nq3 + q];
+                entropy_variables(u, prm.gamma, v);
+                for (int s = 0; s < 5; ++s) vq[s * nq3 + q] = v[s];
+            }
+            for (int s = 0; s < NSTATE; ++s) {
+                apply3(proj, nd, nq, proj, nd, nq, proj, nd, nq, &vq[s * nq3], vh.data(), false, 1.0);
+                std::vector<double> vhq(nq3);
+                apply3(chi, nq, nd, chi, nq, nd, chi, nq, nd, vh.data(), vhq.data(), false, 1.0);
+                apply3(chi, nq, nd, chi, nq, nd, chi, nq, nd, kk.data() + (size_t)c * ndofs_cell + s * nd3, kq.data(),
+                       false, 1.0);
+                for (int q = 0; q < nq3; ++q) sum += flux_node_mass(mesh, ops, c, q) * vhq[q] * kq[q];
+            }
+        }
+        return sum;
+    }
     for (int c = 0; c < mesh.nc; ++c)
         for (int i = 0; i < nd3; ++i) {
             double u[5], v[5];
@@ -1888,7 +1946,6 @@ double Solver::entropy_vars_dot_mass(const double* st, const double* R) {
 
 double Solver::relaxation_parameter(const double* un, const std::vector<std::vector<double>>& k, const double* b,
                                     int ns, double dt, double est) {
-    if (prm.flux_nodes != GLL) throw std::runtime_error("relaxation RK: GLL flux nodes only");
     const size_t N = ndofs();
     std::vector<double> d(N, 0.0), tmp(N);
     for (int i = 0; i < ns; ++i)

@@ -453,7 +453,6 @@ const char* uncollocated_reason(const ph_mesh_desc* mesh, const ph_params* prm) 
                    "extent on curved cells is not restated)";
     }
     if (prm->precision != PH_FP64) return "uncollocated flux nodes take the FP64 path";
-    if (prm->use_relaxation_runge_kutta) return "uncollocated flux nodes: no relaxation RK";
     return nullptr;
 }
 
@@ -1999,13 +1998,25 @@ static int rrk_entropy(ph_ctx* c, const double* u1, double g, double* out) {
     const double h3 = c->h * c->h * c->h;
     const double* metric = c->curv ? c->d_metric : nullptr;
     cudaError_t e;
-    switch (c->N1) {
+    if (c->gl) {   // at the flux nodes
+        const double* vm = c->curv ? c->d_glvm : nullptr;
+        switch (c->N1) {
+#define PH_RRK_GL_CASE(n) \
+        case n: e = ph::launch_gl_rrk_entropy<n>(c->NQ, c->d_sol, u1, g, c->h_gl, c->nc, h3, vm, c->prm.gamma_gas, \
+                                                 c->d_ent_cell, c->stream); break;
+        PH_RRK_GL_CASE(2) PH_RRK_GL_CASE(3) PH_RRK_GL_CASE(4) PH_RRK_GL_CASE(5) PH_RRK_GL_CASE(6) PH_RRK_GL_CASE(7)
+#undef PH_RRK_GL_CASE
+        default: return fail(PH_ERR_UNSUPPORTED, "polynomial degree");
+        }
+    } else {       // at the solution nodes
+        switch (c->N1) {
 #define PH_RRK_CASE(n) \
-    case n: e = ph::launch_rrk_entropy<n>(c->d_sol, u1, g, c->d_ops, c->nc, h3, metric, c->prm.gamma_gas, c->d_ent_cell, \
-                                          c->stream); break;
-    PH_RRK_CASE(2) PH_RRK_CASE(3) PH_RRK_CASE(4) PH_RRK_CASE(5) PH_RRK_CASE(6) PH_RRK_CASE(7)
+        case n: e = ph::launch_rrk_entropy<n>(c->d_sol, u1, g, c->d_ops, c->nc, h3, metric, c->prm.gamma_gas, \
+                                              c->d_ent_cell, c->stream); break;
+        PH_RRK_CASE(2) PH_RRK_CASE(3) PH_RRK_CASE(4) PH_RRK_CASE(5) PH_RRK_CASE(6) PH_RRK_CASE(7)
 #undef PH_RRK_CASE
-    default: return fail(PH_ERR_UNSUPPORTED, "polynomial degree");
+        default: return fail(PH_ERR_UNSUPPORTED, "polynomial degree");
+        }
     }
     if (e != cudaSuccess) return fail(PH_ERR_CUDA, cudaGetErrorString(e));
     ++c->launches;

@@ -1189,6 +1189,44 @@ gl_stage_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab
         if (a.err_partial) ls_tile_error<NT>(err2, &a.err_partial[cell]);
         return;
     }
+    if (a.ent_partial) {
+        // relaxation RK: this cell's v_hat^T M k, v_hat the entropy variables of the stage input
+        // projected on the solution basis (compute_entropy_vars, runge_kutta_store_entropy.cpp:30-100)
+        // and M = chi^T W J chi (compute_entropy_change_estimate, root_finding_rrk_ode_solver.cpp:353-388):
+        // the sum over the flux nodes of W J (chi v_hat)(chi k), chi v_hat = (chi M^-1 chi^T W) v(chi u)
+        for (int i = threadIdx.x; i < 5 * D3; i += NT) sU[i] = __ldg(&a.U[(size_t)cell * 5 * D3 + i]);
+        __syncthreads();
+        gl_apply3<NT, NQ, ND, 5>(T.chi, sU, D3, sDiv, Q3, t0, t1, 1.0, false);
+        for (int q = threadIdx.x; q < Q3; q += NT) {
+            double u[5], v[5];
+#pragma unroll
+            for (int s = 0; s < 5; ++s) u[s] = sDiv[s * Q3 + q];
+            gl_entropy_vars(u, cst.gam, cst.gm1, v, nullptr);
+#pragma unroll
+            for (int s = 0; s < 5; ++s) sDiv[s * Q3 + q] = v[s];
+        }
+        __syncthreads();
+        gl_apply3<NT, NQ, NQ, 5>(T.P, sDiv, Q3, sN, Q3, t0, t1, 1.0, false);
+        gl_apply3<NT, NQ, ND, 5>(T.chi, sQ, D3, sDiv, Q3, t0, t1, 1.0, false);
+        const double h3 = a.h * a.h * a.h;
+        double ent = 0.0;
+        for (int i = threadIdx.x; i < 5 * Q3; i += NT) {
+            const int q = i % Q3;
+            const double W = tab->wq[q % NQ] * tab->wq[(q / NQ) % NQ] * tab->wq[q / NF];
+            const double J = CURV ? 1.0 / __ldg(&g.vmet[((size_t)cell * 10 + 9) * Q3 + q]) : h3;
+            ent += W * J * sN[i] * sDiv[i];
+        }
+        __shared__ double ered[32];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) ent += __shfl_down_sync(0xffffffffu, ent, o);
+        if ((threadIdx.x & 31) == 0) ered[threadIdx.x >> 5] = ent;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int w = 0; w < (NT + 31) / 32; ++w) t += ered[w];
+            a.ent_partial[cell] = t;
+        }
+    }
     // Butcher RK stage (as the collocated kernel's epilogue)
     for (int i = threadIdx.x; i < 5 * D3; i += NT) {
         const size_t dof = (size_t)cell * 5 * D3 + i;
@@ -1203,6 +1241,57 @@ gl_stage_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab
             a.next[dof] = (cin + a.a_next * k) * a.dt + un;
         }
         if (a.carry_out) a.carry_out[dof] = a.a_carry * k;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Relaxation RK on uncollocated flux nodes: the integrated numerical entropy of
+// u_n + gamma (u_1 - u_n), the state interpolated to the flux nodes
+// (compute_integrated_numerical_entropy, root_finding_rrk_ode_solver.cpp:211-350): per-cell partials
+// ------------------------------------------------------------------------------------
+template <int ND, int NQ>
+struct GlEntropyLayout {
+    static constexpr int D3 = ND * ND * ND, Q3 = NQ * NQ * NQ, nT = gl_temp<ND, NQ>();
+    static constexpr int oU = 0, oQ = oU + 5 * D3, oT0 = oQ + 5 * Q3, oT1 = oT0 + nT, total = oT1 + nT;
+    static constexpr size_t bytes = (size_t)total * sizeof(double);
+};
+
+template <int ND, int NQ>
+__global__ void __launch_bounds__(gl_threads<NQ>())
+gl_rrk_entropy_kernel(const double* __restrict__ Un, const double* __restrict__ U1, double gamma,
+                      const __grid_constant__ GlTab T, double h3, const double* __restrict__ vmet, double gam,
+                      double* __restrict__ partial) {
+    using L = GlEntropyLayout<ND, NQ>;
+    constexpr int NT = gl_threads<NQ>(), D3 = L::D3, Q3 = L::Q3, NF = NQ * NQ;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* sm = reinterpret_cast<double*>(smem_raw);
+    double* sU = sm + L::oU;
+    double* sQ = sm + L::oQ;
+    const int cell = blockIdx.x;
+    for (int i = threadIdx.x; i < 5 * D3; i += NT) {
+        const size_t k = (size_t)cell * 5 * D3 + i;
+        sU[i] = Un[k] + gamma * (U1[k] - Un[k]);
+    }
+    __syncthreads();
+    gl_apply3<NT, NQ, ND, 5>(T.chi, sU, D3, sQ, Q3, sm + L::oT0, sm + L::oT1, 1.0, false);
+    double e = 0.0;
+    for (int q = threadIdx.x; q < Q3; q += NT) {
+        double u[5];
+#pragma unroll
+        for (int s = 0; s < 5; ++s) u[s] = sQ[s * Q3 + q];
+        const double W = T.wq[q % NQ] * T.wq[(q / NQ) % NQ] * T.wq[q / NF];
+        const double J = vmet ? 1.0 / vmet[((size_t)cell * 10 + 9) * Q3 + q] : h3;
+        e += W * J * numerical_entropy_fn(u, gam);
+    }
+    __shared__ double red[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = e;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (NT + 31) / 32; ++w) t += red[w];
+        partial[cell] = t;
     }
 }
 

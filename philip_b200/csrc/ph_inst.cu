@@ -419,6 +419,40 @@ cudaError_t launch_gl(int kernel, int nq, const StageArgs& a, const GlArgs& g, c
     }
     return cudaErrorInvalidValue;
 }
+template <int ND, int NQ>
+static cudaError_t launch_gl_rrk_entropy_nq(const double* Un, const double* U1, double gamma, const GlTab& ht, int nc,
+                                            double h3, const double* vmet, double gam, double* partial, cudaStream_t s) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    static bool configured[64] = {};
+    auto kern = gl_rrk_entropy_kernel<ND, NQ>;
+    constexpr size_t bytes = GlEntropyLayout<ND, NQ>::bytes;
+    if (!configured[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (e != cudaSuccess) return e;
+        configured[dev] = true;
+    }
+    if (nc <= 0) return cudaErrorInvalidValue;
+    kern<<<nc, gl_threads<NQ>(), bytes, s>>>(Un, U1, gamma, ht, h3, vmet, gam, partial);
+    return cudaGetLastError();
+}
+
+template <int N1>
+cudaError_t launch_gl_rrk_entropy(int nq, const double* Un, const double* U1, double gamma, const GlTab& ht, int nc,
+                                  double h3, const double* vmet, double gam, double* partial, cudaStream_t s) {
+    if (nq == N1) return launch_gl_rrk_entropy_nq<N1, N1>(Un, U1, gamma, ht, nc, h3, vmet, gam, partial, s);
+    if constexpr (N1 + 1 <= GL_MAXQ) {
+        if (nq == N1 + 1) return launch_gl_rrk_entropy_nq<N1, N1 + 1>(Un, U1, gamma, ht, nc, h3, vmet, gam, partial, s);
+    }
+    if constexpr (N1 + 2 <= GL_MAXQ) {
+        if (nq == N1 + 2) return launch_gl_rrk_entropy_nq<N1, N1 + 2>(Un, U1, gamma, ht, nc, h3, vmet, gam, partial, s);
+    }
+    return cudaErrorInvalidValue;
+}
+template cudaError_t launch_gl_rrk_entropy<PH_N1>(int, const double*, const double*, double, const GlTab&, int, double,
+                                                  const double*, double, double*, cudaStream_t);
+
 template cudaError_t launch_gl<PH_N1>(int, int, const StageArgs&, const GlArgs&, const GlTab&, bool, bool,
                                       cudaStream_t);
 

@@ -59,6 +59,11 @@ bool batched_shape(int fp32, bool curv, int variant, int* cpc, int* threads, siz
 template <int N1>
 cudaError_t launch_gl(int kernel, int nq, const StageArgs& a, const GlArgs& g, const GlTab& ht, bool visc, bool split,
                       cudaStream_t s);
+// Relaxation RK on uncollocated flux nodes (nq per direction): the integrated numerical entropy
+// of u_n + gamma (u_1 - u_n) at the flux nodes, per cell (vmet: curvilinear cells' metric rows)
+template <int N1>
+cudaError_t launch_gl_rrk_entropy(int nq, const double* Un, const double* U1, double gamma, const GlTab& ht, int nc,
+                                  double h3, const double* vmet, double gam, double* partial, cudaStream_t s);
 // dKE/dt of state U with time derivative K, per-cell partial sums (affine cells)
 template <int N1>
 cudaError_t launch_ke_rate(const double* U, const double* K, const IntegralTab* tab, int nc, double h3,

@@ -42,9 +42,6 @@ def _create(prm_kw=None, mesh_kw=None, edit=None):
 REFUSED = [
     ("gl_flux_nodes_precision_form", lambda p: (setattr(p, "flux_nodes_type", 0), setattr(p, "precision", 1)),
      _lib.PH_ERR_UNSUPPORTED, "FP64"),
-    ("gl_flux_nodes_relaxation_rk", lambda p: (setattr(p, "flux_nodes_type", 0),
-                                                setattr(p, "use_relaxation_runge_kutta", 1)),
-     _lib.PH_ERR_UNSUPPORTED, "relaxation"),
     ("overintegration_3", lambda p: setattr(p, "overintegration", 3), _lib.PH_ERR_UNSUPPORTED, "overintegration"),
     ("gl_flux_nodes_p6_overintegration", lambda p: (setattr(p, "flux_nodes_type", 0), setattr(p, "poly_degree", 6),
                                                     setattr(p, "overintegration", 1)),

@@ -468,6 +468,10 @@ def test_curvilinear_slabs_are_the_whole_curvilinear_mesh(name, kw, world, preci
 RRK_CASES = [
     ("entropy_conservative_p3_two_slabs", dict(poly_degree=3, n_cells=4, two_point="CH", conv="two_point_flux"), 2),
     ("roe_dissipation_p2_three_slabs", dict(poly_degree=2, n_cells=4), 3),
+    ("gl_entropy_conservative_p3_two_slabs", dict(poly_degree=3, n_cells=4, two_point="CH", conv="two_point_flux",
+                                                  nodes="GL"), 2),
+    ("gl_ns_ra_sipg_p2_two_slabs", dict(poly_degree=2, n_cells=4, pde="navier_stokes", fr="cPlus", two_point="Ra",
+                                        conv="two_point_flux", rk="ssprk3_ex", nodes="GL"), 2),
 ]
 
 
@@ -477,20 +481,24 @@ def test_relaxation_rk_on_slabs(name, kw, world):
     """Relaxation RK on slabs: the entropy integrals of every root iterate and the stage
     estimates are summed over the ranks (ph_set_rank_sum), so every slab takes the same
     relaxation parameter as the whole mesh up to the summation order of those integrals (the
-    bounds of the GPU-vs-oracle relaxation test: 1e-5 on gamma, 5e-9 on the state); with the
-    entropy-conservative scheme the slabs' relaxed steps conserve the mesh's numerical entropy to
-    rounding. A slab without the sum is refused at its first step."""
+    bounds of the GPU-vs-oracle relaxation test: 1e-5 on gamma, 5e-9 on the state), on GL flux
+    nodes too; with the entropy-conservative Euler scheme the slabs' relaxed steps conserve the
+    mesh's numerical entropy to rounding, and dissipative schemes lose entropy. A slab without the
+    sum is refused at its first step."""
     from oracle.oracle import Oracle
     from philip_b200.dg import DGStrong, RungeKuttaODESolver
     from philip_b200.prm import Parameters
     from philip_b200.slab import LoopbackHalo
     from helpers import prm_dict
+    kw = dict(kw)
+    nodes = kw.pop("nodes", "GLL")
     d = prm_dict(**kw)
+    d["flux_nodes_type"] = nodes
     d["ODE solver/rrk root solver/use_relaxation_runge_kutta"] = "true"
     prm = Parameters.from_dict(d)
     orc = Oracle(prm.oracle_cfg(), prm.n_cells, *prm.grid_bounds)
     U0 = orc.initial_condition("tgv")
-    dt = 0.02
+    dt = 0.02 if kw.get("pde") != "navier_stokes" else 0.01
     whole = DGStrong(prm)
     whole.solution = U0
     ode = RungeKuttaODESolver(whole)
@@ -514,7 +522,7 @@ def test_relaxation_rk_on_slabs(name, kw, world):
     assert abs(odes[0].current_time - ode.current_time) <= 1e-5 * ode.current_time
     drift = (orc.numerical_entropy(U) - e0) / abs(e0)
     print(f"{name}: entropy change over 4 relaxed slab steps {drift:.3e}")
-    if kw.get("conv") == "two_point_flux":
+    if kw.get("conv") == "two_point_flux" and kw.get("pde", "euler") == "euler":
         assert abs(drift) <= 1e-12
     else:
         assert drift < 0.0
