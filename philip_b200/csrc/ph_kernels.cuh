@@ -46,6 +46,15 @@
 #ifndef PH_PAIR_DEDUP
 #define PH_PAIR_DEDUP 0
 #endif
+// 1: at p = 5 the volume phase accumulates each direction into an array of its own (the first
+// in the state's space, two more after the layout), so the three directions run without a block
+// barrier between them and without read-modify-write of the accumulator; phase 5 sums them in
+// the order of the shared accumulator (bitwise the same). Only where the extra shared memory
+// still fits the CTAs per SM the register budget allows. Off: on B200 at 24^3 p5 the stage
+// kernel takes 0.509 ms against 0.492 in FP64 and 0.307 against 0.268 in FP32.
+#ifndef PH_SEP_ACC
+#define PH_SEP_ACC 0
+#endif
 // 1: the FP64 viscous stage kernel (even N1, affine cells) stages its tile's state and viscous
 // divergence into shared memory with bulk copies (cp.async.bulk, completion on an mbarrier),
 // issued before the neighbour gathers (B200: 24^3 p5 0.499 ms against 0.505, 32^3 p3 0.421
@@ -157,8 +166,7 @@ struct Layout {
     // even N1; in the frame of the line's direction)
     static constexpr int HP = (PH_PAIR_DEDUP && SPLIT && !CURV && (N1 % 2 == 0)) ? N1 / 2 : 0;
     static constexpr int oH = oX + CPC * NX * NP;
-    static constexpr int total = oH + 3 * CPC * NF * HP * 5;
-    static constexpr size_t bytes = (size_t)total * sizeof(R);
+    static constexpr int oA1 = oH + 3 * CPC * NF * HP * 5;   // directions 1 and 2 (SEPA)
     static constexpr int SPW = 32 / N1;                // lines per warp
     static constexpr int WARPS_LINES = (CPC * NF + SPW - 1) / SPW;
     static constexpr int NT = WARPS_LINES * 32;
@@ -171,6 +179,11 @@ struct Layout {
                                     : (N1 == 4) ? (F32 ? PH_P3_MINB_F32 : PH_P3_MINB) : 1;
     // never more CTAs than 2048 threads per SM hold (the batched tile shapes are wider)
     static constexpr int MINB = MINB_ASKED * NT > 2048 ? 2048 / NT : MINB_ASKED;
+    // separate direction accumulators where MINB CTAs (1 KB reserved each) still fit 228 KB
+    static constexpr bool SEPA = PH_SEP_ACC && N1 == 6 &&
+                                 (size_t)MINB * ((oA1 + 2 * CPC * 5 * NP) * sizeof(R) + 1024) <= 233472;
+    static constexpr int total = oA1 + (SEPA ? 2 * CPC * 5 * NP : 0);
+    static constexpr size_t bytes = (size_t)total * sizeof(R);
 };
 
 template <int N1> __device__ __forceinline__ int node_of(int x, int y, int z) { return (z * N1 + y) * N1 + x; }
@@ -480,10 +493,10 @@ __device__ __forceinline__ void volume_dir(int d, const Cst<R>& cst, int tp, con
         }
     }
     if (lvalid) {
-        R* A = sA + lc * 5 * NP;
+        R* A = sA + lc * 5 * NP;   // (SEPA: direction d's own accumulator)
 #pragma unroll
         for (int s = 0; s < 5; ++s) {
-            if (d == 0) A[s * NP + node] = acc[s];
+            if (d == 0 || L::SEPA) A[s * NP + node] = acc[s];
             else A[s * NP + node] += acc[s];
         }
     }
@@ -908,8 +921,9 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
         // constants in each copy (5-12 % faster than one runtime-indexed copy on B200)
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            __syncthreads();
-            volume_dir<R, N1, CPC, VISC, SPLIT, CURV>(d, cst, tp, sD, sX, sA, sOpsD, sOpsDsk, sm + L::oH, lc, lt, pos,
+            if (d == 0 || !L::SEPA) __syncthreads();
+            R* Ad = (L::SEPA && d > 0) ? sm + L::oA1 + (d - 1) * CPC * 5 * NP : sA;
+            volume_dir<R, N1, CPC, VISC, SPLIT, CURV>(d, cst, tp, sD, sX, Ad, sOpsD, sOpsDsk, sm + L::oH, lc, lt, pos,
                                                      seg, lvalid);
         }
         __syncthreads();
@@ -922,8 +936,15 @@ __device__ __forceinline__ void residual_tile(const StageArgs& a, const int cell
         const int cx[3] = {x, y, z};
         R* A = sA + c * 5 * NP;
         R G[5];
+        if constexpr (L::SEPA) {   // -(a0 + a1 + a2) = (-a0 - a1) - a2 exactly
+            const R* A1 = sm + L::oA1 + c * 5 * NP;
+            const R* A2 = A1 + CPC * 5 * NP;
 #pragma unroll
-        for (int s = 0; s < 5; ++s) G[s] = -A[s * NP + node];
+            for (int s = 0; s < 5; ++s) G[s] = (-A[s * NP + node] - A1[s * NP + node]) - A2[s * NP + node];
+        } else {
+#pragma unroll
+            for (int s = 0; s < 5; ++s) G[s] = -A[s * NP + node];
+        }
         if constexpr (VISC) {
             const R* X = sX + c * L::NX * NP;
 #pragma unroll
@@ -1115,10 +1136,24 @@ template <typename R, int N1, bool FRA = false> __host__ __device__ constexpr bo
     return N1 >= 5 || FRA;
 }
 
+// CTAs per SM of the periodic FP64 auxiliary kernel at p = 5 (224 threads). Timed on B200 at
+// 24^3 cells inside the RK4 steps: 3 (76 registers) 0.163 ms, 4 (70 registers) 0.147 ms, 5 (56
+// registers, 32 bytes spilled) 0.155 ms. Asked for explicitly: launch bounds naming 1 CTA per SM
+// gave 76 registers, and the allocator's choice without a count sits at 70.
+#ifndef PH_AUX_P5_MINB
+#define PH_AUX_P5_MINB 4
+#endif
+
 template <int N1, int CPC, bool FRA = false>
 struct AuxLayout {
     static constexpr int NP = N1 * N1 * N1, NF = N1 * N1;
     static constexpr int NT = ((CPC * NP + 31) / 32) * 32 > 512 ? 512 : ((CPC * NP + 31) / 32) * 32;
+    // CTAs per SM asked of the register allocator (the periodic FP64 line form at p = 5 with one
+    // cell per CTA; the other forms take what they need)
+    template <typename R, bool CURV, bool BND>
+    static constexpr int minb() {
+        return (sizeof(R) == 8 && N1 == 6 && CPC == 1 && !FRA && !CURV && !BND) ? PH_AUX_P5_MINB : 1;
+    }
     // state, neighbour traces, then (line form) the gradient / nodal flux or (node form) the
     // differentiation matrix and the nodal flux
     template <typename R>
@@ -1295,7 +1330,7 @@ __device__ __forceinline__ void aux_boundary_node(const int* __restrict__ nbr, c
 }
 
 template <typename R, int N1, int CPC, bool FRA, bool CURV, bool BND = false>
-__global__ void __launch_bounds__(AuxLayout<N1, CPC, FRA>::NT)
+__global__ void __launch_bounds__(AuxLayout<N1, CPC, FRA>::NT, AuxLayout<N1, CPC, FRA>::template minb<R, CURV, BND>())
 aux_kernel(const double* __restrict__ U, const int* __restrict__ nbr, int cell_begin, int nc, R inv_h, PhysConst pc,
            AuxCoef<R> co, R* __restrict__ Fv, const double* __restrict__ metric, const int* __restrict__ btype,
            R* __restrict__ Fb, R pen, const int* __restrict__ tiles) {
