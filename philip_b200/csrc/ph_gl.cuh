@@ -145,6 +145,55 @@ static __device__ __noinline__ void gl_bnd_state(int bt, const double r[5], int 
 template <bool SPLIT> __host__ __device__ constexpr int gl_t1_width() { return SPLIT ? 10 : 5; }
 constexpr int GL_T2W = 8;
 
+#ifndef PH_GL_PREFETCH
+#define PH_GL_PREFETCH 1
+#endif
+
+// L2 prefetch of n doubles at p, one per 128-byte line, addresses clamped inside [p, p + n)
+__device__ __forceinline__ void gl_prefetch_span(const double* p, int n, int i0, int stride) {
+    const int nl = (n + 15) / 16;
+    for (int i = i0; i < nl; i += stride) {
+        const int e = i * 16;
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(p + (e < n ? e : n - 1)));
+    }
+}
+
+// Warms L2 with the data a cell reads after its volume work: the neighbours' blocks of the
+// face-value buffer (the auxiliary kernel: their states; the stage kernel: the whole blocks), and
+// in the stage kernel its own face-value blocks, its own and its neighbours' viscous face blocks,
+// its viscous volume rows and the RK registers of the epilogue. Each block is one the kernel
+// itself reads; a prefetch writes nothing. Boundary faces (nbr < 0) have no neighbour block.
+template <int NT, int NF, int D3, int T1W, bool STAGE, bool VISC>
+__device__ __forceinline__ void gl_prefetch_l2(const StageArgs& a, const GlArgs& g, int cell) {
+    if (!PH_GL_PREFETCH) return;
+    const int w = threadIdx.x >> 5, nw = NT / 32, lane = threadIdx.x & 31;
+    // warp w takes the blocks w, w + nw, ...: 6 neighbour face-value blocks, then (stage: viscous)
+    // 6 neighbour viscous face blocks, the own blocks, (viscous) the viscous rows, the RK registers
+    constexpr int NB = STAGE ? 6 + (VISC ? 6 : 0) + 1 + (VISC ? 2 : 0) + 2 : 6;
+    for (int b = w; b < NB; b += nw) {
+        const double* p = nullptr;
+        int n = 0;
+        if (b < 6) {
+            const int cn = __ldg(&a.nbr[cell * 6 + b]);
+            if (cn >= 0) { p = g.t1 + ((size_t)cn * 6 + (b ^ 1)) * T1W * NF; n = (STAGE ? T1W : 5) * NF; }
+        } else if (STAGE && VISC && b < 12) {
+            const int f = b - 6, cn = __ldg(&a.nbr[cell * 6 + f]);
+            if (cn >= 0) { p = g.t2 + ((size_t)cn * 6 + (f ^ 1)) * GL_T2W * NF; n = GL_T2W * NF; }
+        } else {
+            const int r = b - (STAGE && VISC ? 12 : 6);
+            if (r == 0) { p = g.t1 + (size_t)cell * 6 * T1W * NF; n = 6 * T1W * NF; }
+            else if (STAGE && VISC && r == 1) { p = g.t2 + (size_t)cell * 6 * GL_T2W * NF; n = 6 * GL_T2W * NF; }
+            else if (STAGE && VISC && r == 2) { p = g.vis + (size_t)cell * 4 * D3; n = 4 * D3; }
+            else if (STAGE && a.mode == 2) {
+                const int k = r - (VISC ? 3 : 1);
+                const double* base = k == 0 ? a.Un : a.acc_in;
+                if (base) { p = base + (size_t)cell * 5 * D3; n = 5 * D3; }
+            }
+        }
+        if (p) gl_prefetch_span(p, n, lane, 32);
+    }
+}
+
 // temporaries of the sum-factorised passes on 5 components (and of the six faces' arrays)
 template <int ND, int NQ> __host__ __device__ constexpr int gl_temp() {
     constexpr int a = 5 * NQ * NQ * NQ, b = 30 * NQ * NQ, c = 30 * NQ * ND, d = 30 * ND * ND;
@@ -614,6 +663,7 @@ gl_aux_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab T
     const int ucv = a.pc.use_const_visc;
     gl_load_tab(g.tab, tab, NT);
     for (int i = threadIdx.x; i < 5 * D3; i += NT) sU[i] = __ldg(&a.U[(size_t)cell * 5 * D3 + i]);
+    gl_prefetch_l2<NT, NF, D3, T1W, false, true>(a, g, cell);
     __syncthreads();
     gl_apply3<NT, NQ, ND, 5>(T.chi, sU, D3, sQ, Q3, t0, t1, 1.0, false);
     gl_aux_gradient<ND, NQ, SPLIT, CURV, BND>(a, g, T, tab, cell, sQ, t0, sAQ);
@@ -819,6 +869,7 @@ gl_stage_kernel(const StageArgs a, const GlArgs g, const __grid_constant__ GlTab
     for (int i = threadIdx.x; i < 5 * D3; i += NT) sU[i] = __ldg(&a.U[(size_t)cell * 5 * D3 + i]);
     if constexpr (CURV)
         for (int i = threadIdx.x; i < 9 * Q3; i += NT) sM[i] = __ldg(&g.vmet[(size_t)cell * 10 * Q3 + i]);
+    gl_prefetch_l2<NT, NF, D3, T1W, true, VISC>(a, g, cell);
     __syncthreads();
     gl_apply3<NT, NQ, ND, 5>(T.chi, sU, D3, sQ, Q3, t0, t1, 1.0, false);
     if constexpr (SPLIT) {
