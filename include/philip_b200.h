@@ -27,7 +27,7 @@ typedef struct ph_ctx ph_ctx;
 enum {
     PH_OK = 0,
     PH_ERR_INVALID = 1,      /* bad argument */
-    PH_ERR_UNSUPPORTED = 2,  /* configuration outside the GPU path (e.g. GL flux nodes) */
+    PH_ERR_UNSUPPORTED = 2,  /* configuration outside the GPU path (e.g. overintegration 3, p = 7) */
     PH_ERR_CUDA = 3,         /* CUDA runtime failure */
     PH_ERR_NOMEM = 4,        /* device allocation failed */
     PH_ERR_EXCHANGE = 5      /* the halo exchange callback of a slab context failed */

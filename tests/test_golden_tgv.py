@@ -3,7 +3,8 @@
 at the final time within 1e-10 relative).
 
 The CPU oracle must reproduce all three (GL and GLL flux nodes, strong and split
-forms); the CUDA path reproduces the GLL one (it implements collocated GLL nodes).
+forms); the CUDA path reproduces the GLL one here and the two on GL flux nodes in
+test_gpu_gl.py.
 """
 import json
 import os
