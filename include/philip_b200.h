@@ -367,7 +367,9 @@ int ph_quotient_selftest(uint64_t seed, int n, double out[2]);
  * (the HBM budget); each RK stage of all admitted solves of one order runs as one persistent
  * kernel over a tile list, the stages of all orders form one CUDA graph per step, and solves
  * join and leave between steps (continuous batching). Split-form Euler, GLL, rk4_ex or
- * ssprk3_ex; affine or curvilinear meshes; one precision per batch. A solve's result is
+ * ssprk3_ex; affine or curvilinear meshes, periodic or with the Euler boundary conditions of
+ * ph_mesh_desc.boundary_type (the solves with boundary faces form groups of their own, run by
+ * the boundary-face instance of the batched kernel); one precision per batch. A solve's result is
  * bitwise the one ph_rk_step gives for it alone. Calls on one batch are not thread-safe. */
 typedef struct ph_batch ph_batch;
 int ph_batch_create(size_t hbm_budget_bytes, int precision, void* cuda_stream, ph_batch** out);

@@ -49,10 +49,19 @@ size_t align_up(size_t x) { return (x + ALIGN - 1) / ALIGN * ALIGN; }
 
 // byte offsets of one solve's arrays inside its arena range
 struct SlotLayout {
-    size_t sol, stA, stB, acc, carry, comp, metric, nbr, ops, status, total;
+    size_t sol, stA, stB, acc, carry, comp, metric, nbr, btype, ops, status, total;
 };
 
-SlotLayout slot_layout(size_t ndofs, int nc, int NP, bool curv, bool carry, bool comp) {
+// boundary faces of a mesh: n^2 on every non-periodic side
+int boundary_face_count(const ph_mesh_desc* mesh) {
+    const int n = mesh->n_cells_per_direction;
+    int nb = 0;
+    for (int f = 0; f < 6; ++f)
+        if (mesh->boundary_type[f] != 0) nb += n * n;
+    return nb;
+}
+
+SlotLayout slot_layout(size_t ndofs, int nc, int NP, bool curv, bool carry, bool comp, int nb) {
     SlotLayout L{};
     size_t o = 0;
     auto take = [&](size_t bytes) { const size_t at = o; o = align_up(o + bytes); return at; };
@@ -62,6 +71,7 @@ SlotLayout slot_layout(size_t ndofs, int nc, int NP, bool curv, bool carry, bool
     L.comp = comp ? take(vec) : SIZE_MAX;
     L.metric = curv ? take((size_t)nc * 10 * NP * sizeof(double)) : SIZE_MAX;
     L.nbr = take((size_t)nc * 6 * sizeof(int));
+    L.btype = nb > 0 ? take((size_t)nb * sizeof(int)) : SIZE_MAX;
     L.ops = take(sizeof(ph::OpTab));
     L.status = take(sizeof(unsigned));
     L.total = o;
@@ -88,14 +98,14 @@ void set_variant(int N1, int fp32, int curv, int v) {
 }
 
 cudaError_t launch_group(int N1, const ph::StageArgs* inst, const ph::BatchTile* tiles, int ntiles, int fp32,
-                         bool curv, bool hot, int variant, cudaStream_t s) {
+                         bool curv, bool hot, int variant, cudaStream_t s, bool bnd = false) {
     switch (N1) {
-    case 2: return ph::launch_stage_batched<2>(inst, tiles, ntiles, fp32, curv, hot, variant, 0, s);
-    case 3: return ph::launch_stage_batched<3>(inst, tiles, ntiles, fp32, curv, hot, variant, 0, s);
-    case 4: return ph::launch_stage_batched<4>(inst, tiles, ntiles, fp32, curv, hot, variant, 0, s);
-    case 5: return ph::launch_stage_batched<5>(inst, tiles, ntiles, fp32, curv, hot, variant, 0, s);
-    case 6: return ph::launch_stage_batched<6>(inst, tiles, ntiles, fp32, curv, hot, variant, 0, s);
-    case 7: return ph::launch_stage_batched<7>(inst, tiles, ntiles, fp32, curv, hot, variant, 0, s);
+    case 2: return ph::launch_stage_batched<2>(inst, tiles, ntiles, fp32, curv, hot, variant, 0, s, bnd);
+    case 3: return ph::launch_stage_batched<3>(inst, tiles, ntiles, fp32, curv, hot, variant, 0, s, bnd);
+    case 4: return ph::launch_stage_batched<4>(inst, tiles, ntiles, fp32, curv, hot, variant, 0, s, bnd);
+    case 5: return ph::launch_stage_batched<5>(inst, tiles, ntiles, fp32, curv, hot, variant, 0, s, bnd);
+    case 6: return ph::launch_stage_batched<6>(inst, tiles, ntiles, fp32, curv, hot, variant, 0, s, bnd);
+    case 7: return ph::launch_stage_batched<7>(inst, tiles, ntiles, fp32, curv, hot, variant, 0, s, bnd);
     }
     return cudaErrorInvalidValue;
 }
@@ -122,7 +132,7 @@ int cells_per_tile(int N1, int fp32, bool curv, int variant) {
 struct Slot {
     bool used = false, finished = false;
     int N1 = 0, NP = 0, nc = 0, ns = 0;
-    bool curv = false, hot = false;
+    bool curv = false, hot = false, bnd = false;
     size_t ndofs = 0, off = 0, bytes = 0;
     int nsteps = 0, done = 0;
     cudaEvent_t done_ev = nullptr;      // recorded after the step that finishes the solve
@@ -134,7 +144,7 @@ struct Slot {
 
 struct Group {
     int N1 = 0;
-    bool curv = false, hot = false;
+    bool curv = false, hot = false, bnd = false;
     int variant = 0, ns = 0;
     size_t tile_off = 0;
     int ntiles = 0;
@@ -260,15 +270,15 @@ int staged_upload(ph_batch* b, void* dst, const void* src, size_t bytes) {
 
 // Rebuild the tile lists of the unfinished solves and capture one RK step as a graph.
 int rebuild(ph_batch* b) {
-    std::map<std::tuple<int, int, int>, std::vector<ph::BatchTile>> lists;
-    std::map<std::tuple<int, int, int>, Group> info;
+    std::map<std::tuple<int, int, int, int>, std::vector<ph::BatchTile>> lists;
+    std::map<std::tuple<int, int, int, int>, Group> info;
     for (int s = 0; s < (int)b->slots.size(); ++s) {
         const Slot& sl = b->slots[s];
         if (!sl.used || sl.finished) continue;
-        const auto key = std::make_tuple(sl.N1, (int)sl.curv, (int)sl.hot);
+        const auto key = std::make_tuple(sl.N1, (int)sl.curv, (int)sl.hot, (int)sl.bnd);
         Group& g = info[key];
         if (g.N1 == 0) {
-            g.N1 = sl.N1; g.curv = sl.curv; g.hot = sl.hot; g.ns = sl.ns;
+            g.N1 = sl.N1; g.curv = sl.curv; g.hot = sl.hot; g.bnd = sl.bnd; g.ns = sl.ns;
             g.variant = std::max(0, variant_of(sl.N1, b->fp32, sl.curv));
         }
         g.ns = std::max(g.ns, sl.ns);
@@ -295,7 +305,7 @@ int rebuild(ph_batch* b) {
     if (int rc = staged_upload(b, b->d_tiles, all.data(), all.size() * sizeof(ph::BatchTile))) return rc;
     // configure every kernel before capture (attributes and occupancy are not stream work)
     for (const Group& g : b->groups)
-        PH_BCUDA(launch_group(g.N1, b->d_args, b->d_tiles, 0, b->fp32, g.curv, g.hot, g.variant, b->stream));
+        PH_BCUDA(launch_group(g.N1, b->d_args, b->d_tiles, 0, b->fp32, g.curv, g.hot, g.variant, b->stream, g.bnd));
     if (b->graph) { b->retired.push_back(b->graph); b->graph = nullptr; }
     b->launches_per_step = 0;
     if (!b->groups.empty()) {
@@ -308,7 +318,7 @@ int rebuild(ph_batch* b) {
             e = cudaStreamWaitEvent(st, b->ev_fork, 0);
             for (int i = 0; i < g.ns && e == cudaSuccess; ++i) {
                 e = launch_group(g.N1, b->d_args + (size_t)i * MAX_SLOTS, b->d_tiles + g.tile_off, g.ntiles, b->fp32,
-                                 g.curv, g.hot, g.variant, st);
+                                 g.curv, g.hot, g.variant, st, g.bnd);
                 ++b->launches_per_step;
             }
             if (e == cudaSuccess) e = cudaEventRecord(b->ev_join[gi], st);
@@ -334,7 +344,7 @@ int rebuild(ph_batch* b) {
 
 int check_batch_params(const ph_batch* b, const ph_mesh_desc* mesh, const ph_params* prm) {
     if (int rc = check_mesh(mesh)) return rc;
-    if (has_boundaries(mesh)) return fail(PH_ERR_UNSUPPORTED, "a batch takes periodic meshes");
+    if (const char* why = boundary_reason(mesh, prm)) return fail(PH_ERR_UNSUPPORTED, why);
     if (const char* why = unsupported_reason(mesh, prm)) return fail(PH_ERR_UNSUPPORTED, why);
     if (prm->pde_type != 0 || !prm->use_split_form)
         return fail(PH_ERR_UNSUPPORTED, "a batch takes split-form Euler solves");
@@ -421,7 +431,7 @@ int ph_batch_bytes(const ph_mesh_desc* mesh, const ph_params* prm, size_t* bytes
     if (int rc = check_batch_params(nullptr, mesh, prm)) return rc;
     const int n = mesh->n_cells_per_direction, nc = n * n * n, N1 = prm->poly_degree + 1, NP = N1 * N1 * N1;
     const SlotLayout L = slot_layout((size_t)nc * 5 * NP, nc, NP, is_curvilinear(mesh), prm->runge_kutta_method == 1,
-                                     prm->precision == PH_FP32_RESIDUAL);
+                                     prm->precision == PH_FP32_RESIDUAL, boundary_face_count(mesh));
     *bytes = L.total;
     return PH_OK;
 }
@@ -436,6 +446,8 @@ int ph_host::batch_prepare(const ph_mesh_desc* mesh, const ph_params* prm, Batch
     int rc = build_operators(prm, out.ops, out.fr, x, D);
     if (!rc) {
         periodic_connectivity(mesh->n_cells_per_direction, mesh->cell_order, ijk, out.nbr);
+        out.btype.clear();
+        if (has_boundaries(mesh)) apply_boundaries(mesh->n_cells_per_direction, ijk, mesh->boundary_type, out.nbr, out.btype);
         rc = node_geometry(mesh->n_cells_per_direction, ijk, x, D, mesh->left, mesh->right, mesh->warp, xyz,
                            out.metric, mesh->mapping_support_points);
     }
@@ -455,7 +467,8 @@ int ph_host::batch_admit_prepared(ph_batch* b, const ph_mesh_desc* mesh, const p
     int ns = 0;
     double A[4][4], bw[4];
     rk_tableau(prm->runge_kutta_method, ns, A, bw);
-    const SlotLayout L = slot_layout(ndofs, nc, NP, curv, ns == 3, b->fp32 != 0);
+    const int nb = boundary_face_count(mesh);
+    const SlotLayout L = slot_layout(ndofs, nc, NP, curv, ns == 3, b->fp32 != 0, nb);
     size_t off = 0;
     if (!arena_alloc(b, L.total, off)) return fail(PH_ERR_NOMEM, "the batch's HBM budget has no room for this solve now");
     // the tile shape of this (order, mesh kind): tuned once per process
@@ -475,7 +488,9 @@ int ph_host::batch_admit_prepared(ph_batch* b, const ph_mesh_desc* mesh, const p
     const ph::OpTab& ops = prep->ops;
     const bool fr = prep->fr;
     const std::vector<int>& nbr = prep->nbr;
+    const std::vector<int>& btype = prep->btype;
     const std::vector<double>& metric = prep->metric;
+    if ((int)btype.size() != nb) { arena_free(b, off, L.total); return fail(PH_ERR_INVALID, "the prepared mesh differs"); }
     int s = -1;
     for (int i = 0; i < (int)b->slots.size(); ++i)
         if (!b->slots[i].used) { s = i; break; }
@@ -489,7 +504,7 @@ int ph_host::batch_admit_prepared(ph_batch* b, const ph_mesh_desc* mesh, const p
     sl = Slot();
     sl.done_ev = kept_ev;
     sl.used = true;
-    sl.N1 = N1; sl.NP = NP; sl.nc = nc; sl.ns = ns; sl.curv = curv;
+    sl.N1 = N1; sl.NP = NP; sl.nc = nc; sl.ns = ns; sl.curv = curv; sl.bnd = nb > 0;
     sl.hot = prm->two_point_num_flux_type == ph::TP_CH && prm->conv_num_flux == ph::CF_EC_ROE;
     sl.ndofs = ndofs; sl.off = off; sl.bytes = L.total;
     sl.nsteps = nsteps; sl.done = 0; sl.finished = (nsteps == 0);
@@ -499,6 +514,7 @@ int ph_host::batch_admit_prepared(ph_batch* b, const ph_mesh_desc* mesh, const p
     sl.status = (unsigned*)(base + L.status);
     double* d_metric = ptr(L.metric);
     int* d_nbr = (int*)(base + L.nbr);
+    int* d_btype = nb > 0 ? (int*)(base + L.btype) : nullptr;
     ph::OpTab* d_ops = (ph::OpTab*)(base + L.ops);
     const double h = (mesh->right - mesh->left) / n;
     double pen = 0.0;
@@ -511,11 +527,13 @@ int ph_host::batch_admit_prepared(ph_batch* b, const ph_mesh_desc* mesh, const p
         a.h = h; a.inv_h = 1.0 / h; a.pen = pen; a.pc = pc; a.status = sl.status;
         a.fr = fr ? 1 : 0;
         a.metric = d_metric;
+        a.btype = d_btype;   // (Euler: no boundary viscous flux, a.Fb stays null)
         rk_stage_args(a, sl.B, i, ns, A, bw, dt, b->fp32 != 0);
     }
     // uploads through the pinned ring, ordered on the batch stream after the work already queued
     int up = staged_upload(b, sl.B.sol, U0, ndofs * sizeof(double));
     if (!up) up = staged_upload(b, d_nbr, nbr.data(), nbr.size() * sizeof(int));
+    if (!up && d_btype) up = staged_upload(b, d_btype, btype.data(), btype.size() * sizeof(int));
     if (!up) up = staged_upload(b, d_ops, &ops, sizeof(ops));
     if (!up && d_metric) up = staged_upload(b, d_metric, metric.data(), metric.size() * sizeof(double));
     for (int i = 0; i < ns && !up; ++i)

@@ -75,12 +75,12 @@ template <int N1, int V> constexpr int batched_cpc() {
     return N1 == 2 ? 16 : N1 == 3 ? (V == 0 ? 4 : 8) : N1 == 4 ? (V == 0 ? 2 : 4) : N1 == 5 ? (V == 0 ? 1 : 2) : 1;
 }
 
-template <typename R, int N1, int V, int FS, bool CURV>
+template <typename R, int N1, int V, int FS, bool CURV, bool BND>
 static cudaError_t launch_batched_one(const StageArgs* inst, const BatchTile* tiles, int ntiles, int grid,
                                       cudaStream_t s) {
     constexpr int CPC = batched_cpc<N1, V>();
     using L = Layout<R, N1, CPC, false, true, CURV>;
-    auto kern = residual_kernel_batched<R, N1, CPC, false, true, FS, CURV>;
+    auto kern = residual_kernel_batched<R, N1, CPC, false, true, FS, CURV, BND>;
     int dev = 0;
     cudaGetDevice(&dev);
     static bool configured[64] = {false};
@@ -103,30 +103,37 @@ static cudaError_t launch_batched_one(const StageArgs* inst, const BatchTile* ti
     return cudaGetLastError();
 }
 
+template <typename R, int N1, int V, bool BND>
+static cudaError_t launch_batched_vb(const StageArgs* inst, const BatchTile* tiles, int ntiles, bool curv, bool hot,
+                                     int grid, cudaStream_t s) {
+    if (curv) return hot ? launch_batched_one<R, N1, V, 1, true, BND>(inst, tiles, ntiles, grid, s)
+                         : launch_batched_one<R, N1, V, 0, true, BND>(inst, tiles, ntiles, grid, s);
+    return hot ? launch_batched_one<R, N1, V, 1, false, BND>(inst, tiles, ntiles, grid, s)
+               : launch_batched_one<R, N1, V, 0, false, BND>(inst, tiles, ntiles, grid, s);
+}
+
 template <typename R, int N1, int V>
 static cudaError_t launch_batched_v(const StageArgs* inst, const BatchTile* tiles, int ntiles, bool curv, bool hot,
-                                    int grid, cudaStream_t s) {
-    if (curv) return hot ? launch_batched_one<R, N1, V, 1, true>(inst, tiles, ntiles, grid, s)
-                         : launch_batched_one<R, N1, V, 0, true>(inst, tiles, ntiles, grid, s);
-    return hot ? launch_batched_one<R, N1, V, 1, false>(inst, tiles, ntiles, grid, s)
-               : launch_batched_one<R, N1, V, 0, false>(inst, tiles, ntiles, grid, s);
+                                    bool bnd, int grid, cudaStream_t s) {
+    return bnd ? launch_batched_vb<R, N1, V, true>(inst, tiles, ntiles, curv, hot, grid, s)
+               : launch_batched_vb<R, N1, V, false>(inst, tiles, ntiles, curv, hot, grid, s);
 }
 
 template <typename R, int N1>
 static cudaError_t launch_batched_prec(const StageArgs* inst, const BatchTile* tiles, int ntiles, bool curv, bool hot,
-                                       int variant, int grid, cudaStream_t s) {
+                                       bool bnd, int variant, int grid, cudaStream_t s) {
     if constexpr (batched_variants<N1>() > 1) {
-        if (variant == 1) return launch_batched_v<R, N1, 1>(inst, tiles, ntiles, curv, hot, grid, s);
+        if (variant == 1) return launch_batched_v<R, N1, 1>(inst, tiles, ntiles, curv, hot, bnd, grid, s);
     }
     if (variant != 0) return cudaErrorInvalidValue;
-    return launch_batched_v<R, N1, 0>(inst, tiles, ntiles, curv, hot, grid, s);
+    return launch_batched_v<R, N1, 0>(inst, tiles, ntiles, curv, hot, bnd, grid, s);
 }
 
 template <int N1>
 cudaError_t launch_stage_batched(const StageArgs* inst, const BatchTile* tiles, int ntiles, int fp32, bool curv,
-                                 bool hot, int variant, int grid, cudaStream_t s) {
-    return fp32 ? launch_batched_prec<float, N1>(inst, tiles, ntiles, curv, hot, variant, grid, s)
-                : launch_batched_prec<double, N1>(inst, tiles, ntiles, curv, hot, variant, grid, s);
+                                 bool hot, int variant, int grid, cudaStream_t s, bool bnd) {
+    return fp32 ? launch_batched_prec<float, N1>(inst, tiles, ntiles, curv, hot, bnd, variant, grid, s)
+                : launch_batched_prec<double, N1>(inst, tiles, ntiles, curv, hot, bnd, variant, grid, s);
 }
 
 template <typename R, int N1, int V, bool CURV>
@@ -293,7 +300,7 @@ template cudaError_t launch_rrk_entropy<PH_N1>(const double*, const double*, dou
 template cudaError_t launch_stage<PH_N1>(const StageArgs&, int, bool, bool, cudaStream_t);
 template void stage_launch_shape<PH_N1>(int, bool, bool, int*, int*, size_t*);
 template cudaError_t launch_stage_batched<PH_N1>(const StageArgs*, const BatchTile*, int, int, bool, bool, int, int,
-                                                 cudaStream_t);
+                                                 cudaStream_t, bool);
 template bool batched_shape<PH_N1>(int, bool, int, int*, int*, size_t*, int*);
 template cudaError_t launch_aux<PH_N1>(const double*, const int*, const OpTab&, int, int, double, const PhysConst&, int,
                                        void*, const double*, cudaStream_t, const BoundaryArgs*);

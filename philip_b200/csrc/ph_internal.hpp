@@ -22,6 +22,11 @@ int fail(int code, const std::string& msg);   // records the message for ph_last
 // recursive-children order only for a power-of-two n; enumerations within their ranges).
 int check_mesh(const ph_mesh_desc* mesh);
 bool has_boundaries(const ph_mesh_desc* mesh);
+// non-periodic meshes: nullptr when the boundary types are on the path, else the reason
+const char* boundary_reason(const ph_mesh_desc* mesh, const ph_params* prm);
+// boundary faces of the cube's non-periodic sides: nbr = -1 - k for boundary face k, btype[k] its type
+void apply_boundaries(int n, const std::vector<int>& ijk, const int types[6], std::vector<int>& nbr,
+                      std::vector<int>& btype);
 int check_param_ranges(const ph_params* prm);
 
 // Configuration checks shared by every entry point that builds a discretisation;
@@ -61,6 +66,7 @@ struct BatchPrep {
     bool fr = false;
     bool ready = false;
     std::vector<int> nbr;
+    std::vector<int> btype;   // boundary face k's type (nbr = -1 - k); empty on periodic meshes
     std::vector<double> metric;
 };
 int batch_prepare(const ph_mesh_desc* mesh, const ph_params* prm, BatchPrep& out);

@@ -1099,7 +1099,8 @@ struct BatchTile {
 // tile's discretisation (state pointers, physics, dt, RK coefficients of this stage) is
 // staged from the instance table into shared memory. The per-tile work is the same code as
 // residual_kernel, so a solve gives bitwise the same result alone and inside a batch.
-template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int FS, bool CURV = false>
+// BND: the solves of the group have boundary faces (the boundary-face instance on all their tiles).
+template <typename R, int N1, int CPC, bool VISC, bool SPLIT, int FS, bool CURV = false, bool BND = false>
 __global__ void __launch_bounds__(Layout<R, N1, CPC, VISC, SPLIT, CURV>::NT, Layout<R, N1, CPC, VISC, SPLIT, CURV>::MINB)
 residual_kernel_batched(const StageArgs* __restrict__ inst, const BatchTile* __restrict__ tiles, int ntiles) {
     static_assert(sizeof(StageArgs) % sizeof(int) == 0, "StageArgs is copied as ints");
@@ -1110,7 +1111,7 @@ residual_kernel_batched(const StageArgs* __restrict__ inst, const BatchTile* __r
         int* dst = reinterpret_cast<int*>(&sa);
         for (int i = threadIdx.x; i < (int)(sizeof(StageArgs) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
         __syncthreads();
-        residual_tile<R, N1, CPC, VISC, SPLIT, FS, CURV>(sa, tile.cell0);
+        residual_tile<R, N1, CPC, VISC, SPLIT, FS, CURV, false, BND>(sa, tile.cell0);
         __syncthreads();
     }
 }

@@ -43,10 +43,11 @@ cudaError_t launch_rrk_entropy(const double* Un, const double* U1, double gamma,
                                const double* metric, double gam, double* partial, cudaStream_t s);
 // Batched (many-solve) stage: split-form Euler tiles of several discretisations of the same
 // order. `variant` selects the cells-per-CTA tile shape (batched_shape lists them); grid <= 0
-// sizes the persistent grid to the resident CTAs of the whole GPU.
+// sizes the persistent grid to the resident CTAs of the whole GPU; bnd: solves with boundary
+// faces (the boundary-face instance).
 template <int N1>
 cudaError_t launch_stage_batched(const StageArgs* inst, const BatchTile* tiles, int ntiles, int fp32, bool curv,
-                                 bool hot, int variant, int grid, cudaStream_t s);
+                                 bool hot, int variant, int grid, cudaStream_t s, bool bnd = false);
 // tile shape of a batched variant: cells per CTA, threads, dynamic shared memory and resident
 // CTAs per SM; returns false when the variant does not exist
 template <int N1>

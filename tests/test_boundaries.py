@@ -532,20 +532,70 @@ def test_boundary_configurations_outside_the_path_are_refused(name, prm_kw, bnd,
     assert rc == code and text in msg
 
 
-def test_entry_points_without_boundary_terms_refuse_non_periodic_meshes():
-    """The batch and the no-allocation residual take periodic meshes."""
+def test_entry_points_and_non_periodic_meshes():
+    """The no-allocation residual takes periodic meshes; a batch takes boundaries on its split-form
+    Euler solves (their slot holds one boundary type per boundary face besides the periodic
+    slot's arrays) and refuses a Navier-Stokes farfield as contexts do."""
     import ctypes
     L = _lib.load()
     prm = Parameters.from_dict(prm_dict())
     p = prm.to_ph_params()
     m = _mesh(prm, WALLS_Y)
-    h = ctypes.c_void_p()
     dummy = ctypes.c_void_p(16)   # never dereferenced: the checks come first
     assert L.ph_residual_noalloc(ctypes.byref(m), ctypes.byref(p), dummy, dummy, None) == _lib.PH_ERR_UNSUPPORTED
     assert b"periodic" in L.ph_last_error()
-    nbytes = ctypes.c_size_t()
-    assert L.ph_batch_bytes(ctypes.byref(m), ctypes.byref(p), ctypes.byref(nbytes)) == _lib.PH_ERR_UNSUPPORTED
-    assert b"periodic" in L.ph_last_error()
+    walls, periodic = ctypes.c_size_t(), ctypes.c_size_t()
+    assert L.ph_batch_bytes(ctypes.byref(m), ctypes.byref(p), ctypes.byref(walls)) == _lib.PH_OK
+    mp = _mesh(prm, ["periodic"] * 6)
+    assert L.ph_batch_bytes(ctypes.byref(mp), ctypes.byref(p), ctypes.byref(periodic)) == _lib.PH_OK
+    nb = 2 * prm.n_cells ** 2
+    assert walls.value - periodic.value == (nb * 4 + 255) // 256 * 256
+    ns = Parameters.from_dict(prm_dict(pde="navier_stokes", diss="bassi_rebay_2"))
+    q = ns.to_ph_params()
+    mf = _mesh(ns, ["riemann_farfield", "riemann_farfield", "periodic", "periodic", "periodic", "periodic"])
+    assert L.ph_batch_bytes(ctypes.byref(mf), ctypes.byref(q), ctypes.byref(walls)) == _lib.PH_ERR_UNSUPPORTED
+
+
+BATCH_BND = [
+    ("walls_y", ["periodic", "periodic", "wall", "wall", "periodic", "periodic"]),
+    ("slip_farfield_outflow", ["slip_wall", "slip_wall", "farfield", "farfield", "pressure_outflow", "inflow"]),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [_lib.PH_FP64, _lib.PH_FP32_RESIDUAL], ids=["fp64", "fp32"])
+def test_batched_solves_with_boundaries_match_single_solves(precision):
+    """Split-form Euler solves with boundary faces inside a batch, beside a periodic solve of the
+    same order: the bounded solves' group runs the boundary-face instance of the batched kernel on
+    all its tiles (a context runs it on the tiles that touch a boundary and the periodic kernel on
+    the rest). The two instances evaluate an interior face alike: the results are bitwise the
+    single-solve contexts' in FP64 (measured bitwise in the precision form too; held to 1e-6 there,
+    as the periodic batch is)."""
+    from philip_b200.dg import DGStrong, RungeKuttaODESolver
+    from philip_b200.serve import Batch
+    prm = _params(poly_degree=3, n_cells=4)
+    orc = Oracle(prm.oracle_cfg(), prm.n_cells, *prm.grid_bounds)
+    U0 = orc.initial_condition("tgv")
+    dt, nsteps = 2e-3, 6
+    b = Batch(1 << 30, precision)
+    cases = BATCH_BND + [("periodic", ["periodic"] * 6)]
+    slots = [b.admit(_mesh(prm, bnd), prm.to_ph_params(precision), U0, dt, nsteps) for _, bnd in cases]
+    b.step(10 ** 6)
+    assert b.active == 0
+    tol = 0.0 if precision == _lib.PH_FP64 else 1e-6
+    for (name, bnd), s in zip(cases, slots):
+        Ub = b.state(s, U0.size)
+        dg = DGStrong(prm, precision=precision, boundaries=None if name == "periodic" else bnd)
+        dg.solution = U0
+        RungeKuttaODESolver(dg).step_in_time(dt, nsteps=nsteps)
+        Ua = dg.solution
+        err = float(np.max(np.abs(Ub - Ua)) / np.max(np.abs(Ua)))
+        print(f"{name}: batch vs context rel max err {err:.3e} (bitwise {np.array_equal(Ub, Ua)})")
+        assert b.status(s) == 0 and dg.status() == 0
+        if precision == _lib.PH_FP64:
+            assert np.array_equal(Ub, Ua)
+        assert err <= tol
+    b.close()
 
 
 @pytest.mark.gpu
